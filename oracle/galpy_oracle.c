@@ -1,0 +1,1309 @@
+/*
+ * oracle/galpy_oracle.c -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatement of galpy's batched C orbit integration for the potential
+ * types and integrators that the CUDA engine implements.  It is the checker
+ * for the CUDA kernels (tests/, __graft_entry__.smoke(), bench.py's CPU
+ * baseline leg) and is never linked into, or called by, the product path.
+ *
+ * What is restated (reference file:line in galpy):
+ *   forces   PowerSphericalPotentialwCutoff.c:9-131, MiyamotoNagaiPotential.c:
+ *            16-117, NFWPotential.c:16-106, HernquistPotential.c:15-100,
+ *            LogarithmicHaloPotential.c:5-297 (potential_c_ext/)
+ *   sums     galpy_potentials.c:120-354 (sum over components, in order)
+ *   RHS      orbit_c_ext/integrateFullOrbit.c:1307-1352 (evalRectForce,
+ *            evalRectDeriv), :1496-1681 (the dxdv variants);
+ *            orbit_c_ext/integratePlanarOrbit.c:1015-1055, :1124-1276
+ *   steppers util/bovy_symplecticode.c:132-377 (leapfrog, symplec4),
+ *            :588-809 (their step estimators), :1053-1268 (*_dxdv);
+ *            util/bovy_rk.c:66-170,328-395 (rk4 + estimator);
+ *            util/leung_dop853.c:231-517 (dop853)
+ *   drivers  integrateFullOrbit.c:1046-1150, :1234-1306;
+ *            integratePlanarOrbit.c:743-847, :940-1014
+ *   coords   util/bovy_coords.c:57-148
+ * The arithmetic of each formula follows the reference term by term so that
+ * this restatement agrees with the reference's own C (built from its sources
+ * into oracle/_ref by oracle/Makefile) to the last bit or close to it; the
+ * incomplete gamma function is the one in oracle/incgamma.c.
+ *
+ * Extras over the reference (test instrumentation only): per-orbit counts of
+ * accepted steps and of force evaluations, and an optional attempt budget.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+#include "dop853_coeffs.h"
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+double oracle_gamma_inc_P(double a, double x);
+double oracle_gamma_inc_Q(double a, double x);
+
+/* ------------------------------------------------------------------ */
+/* potentials                                                          */
+/* ------------------------------------------------------------------ */
+enum { PT_LOGHALO = 0, PT_MN = 5, PT_HERNQUIST = 8, PT_NFW = 9, PT_PSWC = 15 };
+#define OMAXPOT 32
+
+typedef struct {
+  int type;
+  double p[5]; /* the component's args as galpy passes them */
+} ocomp;
+
+typedef struct {
+  int n;
+  int planar;
+  ocomp c[OMAXPOT];
+  long long nforce; /* force evaluations (instrumentation) */
+} opot;
+
+static int nargs_of(int type, int planar)
+{
+  switch (type) {
+  case PT_LOGHALO: return 4;
+  case PT_MN: return 3;
+  case PT_HERNQUIST: return 2;
+  case PT_NFW: return 2;
+  case PT_PSWC: return planar ? 3 : 5;
+  default: return -1;
+  }
+}
+
+/* Decode galpy's (pot_type, pot_args) stream (integrateFullOrbit.c:69-1040,
+   integratePlanarOrbit.c:55-742 restricted to types 0/5/8/9/15).
+   Returns 0, or -1 for an unsupported type. */
+static int opot_decode(opot *P, int npot, const int *type, const double *args, int planar)
+{
+  if (npot > OMAXPOT || npot < 1) return -1;
+  P->n = npot;
+  P->planar = planar;
+  P->nforce = 0;
+  for (int i = 0; i < npot; i++) {
+    int na = nargs_of(type[i], planar);
+    if (na < 0) return -1;
+    P->c[i].type = type[i];
+    for (int k = 0; k < 5; k++) P->c[i].p[k] = 0.;
+    for (int k = 0; k < na; k++) P->c[i].p[k] = *args++;
+  }
+  return 0;
+}
+
+/* PowerSphericalPotentialwCutoff enclosed mass (PSwC.c:9-11) */
+static double pswc_mass(double r2, double alpha, double rc)
+{
+  return 2. * M_PI * pow(rc, 3. - alpha) *
+         (tgamma(1.5 - 0.5 * alpha) * oracle_gamma_inc_P(1.5 - 0.5 * alpha, r2 / rc / rc));
+}
+
+/* spherical force factor with the (r^2, force) cache of PSwC.c:25-46 */
+static double pswc_force_factor(ocomp *c, double r2)
+{
+  if (r2 == c->p[3]) return c->p[4];
+  double f = -c->p[0] * pswc_mass(r2, c->p[1], c->p[2]) / pow(r2, 1.5);
+  c->p[3] = r2;
+  c->p[4] = f;
+  return f;
+}
+
+static double pswc_planarRforce(const ocomp *c, double R)
+{
+  double r2 = R * R;
+  return -c->p[0] * pswc_mass(r2, c->p[1], c->p[2]) / r2;
+}
+
+static double pswc_planarR2deriv(const ocomp *c, double R)
+{
+  double amp = c->p[0], alpha = c->p[1], rc = c->p[2], r2 = R * R;
+  return amp * (4. * M_PI * pow(r2, -0.5 * alpha) * exp(-r2 / rc / rc) -
+                2. * pswc_mass(r2, alpha, rc) / pow(r2, 1.5));
+}
+
+/* LogHalo helper: R_t^2 of the triaxial form */
+static double lh_Rt2(const ocomp *c, double R, double phi)
+{
+  return R * R * (1. - c->p[3] * pow(sin(phi), 2));
+}
+
+/* ---- 3D component forces ---- */
+static double comp_Rforce(ocomp *c, double R, double Z, double phi)
+{
+  double amp = c->p[0];
+  switch (c->type) {
+  case PT_LOGHALO: {
+    double q = c->p[1], cc = c->p[2], om = c->p[3], zq = Z / q;
+    if (om < 1) {
+      double Rt2 = lh_Rt2(c, R, phi);
+      return -amp * Rt2 / R / (Rt2 + zq * zq + cc);
+    }
+    return -amp * R / (R * R + zq * zq + cc);
+  }
+  case PT_MN: {
+    double a = c->p[1], b = c->p[2];
+    return -amp * R * pow(R * R + pow(a + pow(Z * Z + b * b, 0.5), 2.), -1.5);
+  }
+  case PT_HERNQUIST: {
+    double a = c->p[1], sq = pow(R * R + Z * Z, 0.5);
+    return -amp * R / a / sq * pow(1. + sq / a, -2.) / 2. / a;
+  }
+  case PT_NFW: {
+    double a = c->p[1], Rz = R * R + Z * Z, sq = pow(Rz, 0.5);
+    return amp * R * (1. / Rz / (a + sq) - log(1. + sq / a) / sq / Rz);
+  }
+  case PT_PSWC:
+    return pswc_force_factor(c, R * R + Z * Z) * R;
+  }
+  return 0.;
+}
+
+static double comp_zforce(ocomp *c, double R, double Z, double phi)
+{
+  double amp = c->p[0];
+  switch (c->type) {
+  case PT_LOGHALO: {
+    double q = c->p[1], cc = c->p[2], om = c->p[3], zq = Z / q;
+    if (om < 1) {
+      double Rt2 = lh_Rt2(c, R, phi);
+      return -amp * zq / q / (Rt2 + zq * zq + cc);
+    }
+    return -amp * zq / q / (R * R + zq * zq + cc);
+  }
+  case PT_MN: {
+    double a = c->p[1], b = c->p[2];
+    double sqrtbz = pow(b * b + Z * Z, .5), asqrtbz = a + sqrtbz;
+    if (a == 0.) return amp * (-Z * pow(R * R + asqrtbz * asqrtbz, -1.5));
+    return amp * (-Z * asqrtbz / sqrtbz * pow(R * R + asqrtbz * asqrtbz, -1.5));
+  }
+  case PT_HERNQUIST: {
+    double a = c->p[1], sq = pow(R * R + Z * Z, 0.5);
+    return -amp * Z / a / sq * pow(1. + sq / a, -2.) / 2. / a;
+  }
+  case PT_NFW: {
+    double a = c->p[1], Rz = R * R + Z * Z, sq = pow(Rz, 0.5);
+    return amp * Z * (1. / Rz / (a + sq) - log(1. + sq / a) / sq / Rz);
+  }
+  case PT_PSWC:
+    return pswc_force_factor(c, R * R + Z * Z) * Z;
+  }
+  return 0.;
+}
+
+static double comp_phitorque(const ocomp *c, double R, double Z, double phi)
+{
+  if (c->type == PT_LOGHALO && c->p[3] < 1) {
+    double amp = c->p[0], q = c->p[1], cc = c->p[2], om = c->p[3];
+    double zq = Z / q, Rt2 = lh_Rt2(c, R, phi);
+    return amp * R * R / (Rt2 + zq * zq + cc) * sin(2 * phi) * om / 2.;
+  }
+  return 0.;
+}
+
+/* spherical potentials: Phi'(r)/amp and Phi''(r)/amp as in the reference */
+static void sph_derivs(const ocomp *c, double r, double *dphi, double *d2phi)
+{
+  double a = c->p[1];
+  if (c->type == PT_HERNQUIST) {
+    *dphi = 1. / 2. / a / a * pow(1. + r / a, -2.);
+    *d2phi = -1. / a / a / a * pow(1. + r / a, -3.);
+  } else { /* NFW */
+    *dphi = log(1. + r / a) / r / r - 1. / r / (a + r);
+    double ar = a + r;
+    *d2phi = (r * (2. * a + 3. * r) - 2. * ar * ar * log(1. + r / a)) / r / r / r / ar / ar;
+  }
+}
+
+/* 3D Hessian terms: which = 0 R2, 1 z2, 2 Rz, 3 phi2, 4 Rphi, 5 zphi */
+static double comp_hess(const ocomp *c, int which, double R, double Z, double phi)
+{
+  double amp = c->p[0];
+  switch (c->type) {
+  case PT_LOGHALO: {
+    double q = c->p[1], cc = c->p[2], om = c->p[3], zq = Z / q, q2 = q * q;
+    double Rt2, denom;
+    int tri = om < 1;
+    switch (which) {
+    case 0:
+      if (tri) {
+        Rt2 = lh_Rt2(c, R, phi);
+        denom = 1. / (Rt2 + zq * zq + cc);
+        return amp * (denom - 2. * Rt2 * denom * denom) * Rt2 / (R * R);
+      }
+      denom = 1. / (R * R + zq * zq + cc);
+      return amp * (denom - 2. * R * R * denom * denom);
+    case 1:
+      Rt2 = tri ? lh_Rt2(c, R, phi) : R * R;
+      denom = 1. / (Rt2 + zq * zq + cc);
+      return amp * (denom / q2 - 2. * Z * Z * denom * denom / (q2 * q2));
+    case 2:
+      if (tri) {
+        Rt2 = lh_Rt2(c, R, phi);
+        denom = 1. / (Rt2 + zq * zq + cc);
+        return -amp * 2. * Rt2 / R * Z / q2 * denom * denom;
+      }
+      denom = 1. / (R * R + zq * zq + cc);
+      return -amp * 2. * R * Z / q2 * denom * denom;
+    case 3:
+      if (tri) {
+        double R2 = R * R, s2phi;
+        Rt2 = R2 * (1. - om * pow(sin(phi), 2));
+        denom = 1. / (Rt2 + zq * zq + cc);
+        s2phi = sin(2. * phi);
+        return -amp * om * (0.5 * R2 * R2 * s2phi * s2phi * om * denom * denom +
+                            R2 * denom * cos(2. * phi));
+      }
+      return 0.;
+    case 4:
+      if (tri) {
+        Rt2 = lh_Rt2(c, R, phi);
+        denom = 1. / (Rt2 + zq * zq + cc);
+        return -amp * (denom - Rt2 * denom * denom) * R * sin(2. * phi) * om;
+      }
+      return 0.;
+    case 5:
+      if (tri) {
+        Rt2 = lh_Rt2(c, R, phi);
+        denom = 1. / (Rt2 + zq * zq + cc);
+        return amp * 2. * R * R * Z * sin(phi) * cos(phi) * om * denom * denom / q2;
+      }
+      return 0.;
+    }
+    return 0.;
+  }
+  case PT_MN: {
+    double a = c->p[1], b = c->p[2];
+    switch (which) {
+    case 0: {
+      double sqrtbz = pow(b * b + Z * Z, 0.5), asqrtbz = a + sqrtbz;
+      double denom = R * R + asqrtbz * asqrtbz;
+      return amp * (pow(denom, -1.5) - 3. * R * R * pow(denom, -2.5));
+    }
+    case 1: {
+      double b2 = b * b, sqrtbz = pow(b2 + Z * Z, 0.5), asqrtbz = a + sqrtbz;
+      if (a == 0.) return amp * (b2 + R * R - 2. * Z * Z) * pow(b2 + R * R + Z * Z, -2.5);
+      return amp *
+             (a * a * a * b2 + a * a * (3. * b2 - 2. * Z * Z) * sqrtbz +
+              (b2 + R * R - 2. * Z * Z) * pow(b2 + Z * Z, 1.5) +
+              a * (3. * b2 * b2 - 4. * Z * Z * Z * Z + b2 * (R * R - Z * Z))) /
+             (pow(b2 + Z * Z, 1.5) * pow(R * R + asqrtbz * asqrtbz, 2.5));
+    }
+    case 2: {
+      double sqrtbz = pow(b * b + Z * Z, 0.5), asqrtbz = a + sqrtbz;
+      if (a == 0.) return amp * (-3. * R * Z * pow(R * R + asqrtbz * asqrtbz, -2.5));
+      return amp * (-3. * R * Z * asqrtbz / sqrtbz * pow(R * R + asqrtbz * asqrtbz, -2.5));
+    }
+    }
+    return 0.;
+  }
+  case PT_HERNQUIST:
+  case PT_NFW: {
+    if (which > 2) return 0.;
+    double r = sqrt(R * R + Z * Z), dphi, d2phi;
+    sph_derivs(c, r, &dphi, &d2phi);
+    if (which == 0) return amp * (d2phi * R * R / r / r + dphi * Z * Z / r / r / r);
+    if (which == 1) return amp * (d2phi * Z * Z / r / r + dphi * R * R / r / r / r);
+    return amp * R * Z * (d2phi / r / r - dphi / r / r / r);
+  }
+  case PT_PSWC: {
+    if (which > 2) return 0.;
+    double r2 = R * R + Z * Z, r = sqrt(r2);
+    double Phipp = pswc_planarR2deriv(c, r);
+    double Phip = -pswc_planarRforce(c, r);
+    double ir2 = 1. / r2, ir3 = ir2 / r;
+    if (which == 0) return Phipp * R * R * ir2 + Phip * Z * Z * ir3;
+    if (which == 1) return Phipp * Z * Z * ir2 + Phip * R * R * ir3;
+    return R * Z * (Phipp * ir2 - Phip * ir3);
+  }
+  }
+  return 0.;
+}
+
+/* ---- planar component forces ---- */
+static double comp_planarRforce(const ocomp *c, double R, double phi)
+{
+  double amp = c->p[0];
+  switch (c->type) {
+  case PT_LOGHALO: {
+    double cc = c->p[2], om = c->p[3];
+    if (om < 1) {
+      double Rt2 = lh_Rt2(c, R, phi);
+      return -amp * Rt2 / R / (Rt2 + cc);
+    }
+    return -amp * R / (R * R + cc);
+  }
+  case PT_MN: {
+    double a = c->p[1], b = c->p[2];
+    return -amp * R * pow(R * R + pow(a + b, 2.), -1.5);
+  }
+  case PT_HERNQUIST: {
+    double a = c->p[1];
+    return -amp / a * pow(1. + R / a, -2.) / 2. / a;
+  }
+  case PT_NFW: {
+    double a = c->p[1];
+    return amp / R * (1. / (a + R) - log(1. + R / a) / R);
+  }
+  case PT_PSWC:
+    return pswc_planarRforce(c, R);
+  }
+  return 0.;
+}
+
+static double comp_planarphitorque(const ocomp *c, double R, double phi)
+{
+  if (c->type == PT_LOGHALO && c->p[3] < 1) {
+    double amp = c->p[0], cc = c->p[2], om = c->p[3], Rt2 = lh_Rt2(c, R, phi);
+    return amp * R * R / (Rt2 + cc) * sin(2 * phi) * om / 2.;
+  }
+  return 0.;
+}
+
+/* planar Hessian: which = 0 R2, 1 phi2, 2 Rphi */
+static double comp_planarhess(const ocomp *c, int which, double R, double phi)
+{
+  double amp = c->p[0];
+  switch (c->type) {
+  case PT_LOGHALO: {
+    double cc = c->p[2], om = c->p[3];
+    int tri = om < 1;
+    if (which == 0) {
+      if (tri) {
+        double Rt2 = lh_Rt2(c, R, phi);
+        return amp * (1. - 2. * Rt2 / (Rt2 + cc)) / (Rt2 + cc) * Rt2 / R / R;
+      }
+      return amp * (1. - 2. * R * R / (R * R + cc)) / (R * R + cc);
+    }
+    if (!tri) return 0.;
+    double Rt2 = lh_Rt2(c, R, phi);
+    if (which == 1)
+      return -amp * om *
+             (0.5 * pow(R * R * sin(2. * phi), 2.) * om / (Rt2 + cc) / (Rt2 + cc) +
+              R * R / (Rt2 + cc) * cos(2. * phi));
+    return -amp * cc / (Rt2 + cc) / (Rt2 + cc) * R * sin(2. * phi) * om;
+  }
+  case PT_MN: {
+    if (which) return 0.;
+    double a = c->p[1], b = c->p[2], denom = R * R + pow(a + b, 2.);
+    return amp * (pow(denom, -1.5) - 3. * R * R * pow(denom, -2.5));
+  }
+  case PT_HERNQUIST: {
+    if (which) return 0.;
+    double a = c->p[1];
+    return -amp / a / a / a * pow(1. + R / a, -3.);
+  }
+  case PT_NFW: {
+    if (which) return 0.;
+    double a = c->p[1], aR = a + R, aR2 = aR * aR;
+    return amp * (((R * (2. * a + 3. * R)) - 2. * aR2 * log(1. + R / a)) / R / R / R / aR2);
+  }
+  case PT_PSWC:
+    return which ? 0. : pswc_planarR2deriv(c, R);
+  }
+  return 0.;
+}
+
+/* ---- potential values (for energies) ---- */
+static double comp_eval(const ocomp *c, double R, double Z, double phi)
+{
+  double amp = c->p[0];
+  switch (c->type) {
+  case PT_LOGHALO: {
+    double q = c->p[1], cc = c->p[2], om = c->p[3], zq = Z / q;
+    if (om < 1) return 0.5 * amp * log(R * R * (1. - om * pow(sin(phi), 2)) + zq * zq + cc);
+    return 0.5 * amp * log(R * R + zq * zq + cc);
+  }
+  case PT_MN: {
+    double a = c->p[1], b = c->p[2];
+    return -amp * pow(R * R + pow(a + pow(Z * Z + b * b, 0.5), 2.), -0.5);
+  }
+  case PT_HERNQUIST: {
+    double a = c->p[1], sq = pow(R * R + Z * Z, 0.5);
+    return -amp / (1. + sq / a) / 2. / a;
+  }
+  case PT_NFW: {
+    double a = c->p[1], sq = pow(R * R + Z * Z, 0.5);
+    return -amp * log(1. + sq / a) / sq;
+  }
+  case PT_PSWC: {
+    double alpha = c->p[1], rc = c->p[2], r2 = R * R + Z * Z, r = sqrt(r2);
+    double a1 = 1. - 0.5 * alpha, a2 = 1.5 - 0.5 * alpha, x = r2 / rc / rc;
+    double g1 = tgamma(a1), g2 = tgamma(a2);
+    return amp * 2. * M_PI * pow(rc, 3. - alpha) / r *
+           (r / rc * (g1 - g1 * oracle_gamma_inc_Q(a1, x)) - (g2 - g2 * oracle_gamma_inc_Q(a2, x)));
+  }
+  }
+  return 0.;
+}
+
+/* ------------------------------------------------------------------ */
+/* right-hand sides                                                    */
+/* ------------------------------------------------------------------ */
+typedef struct {
+  opot *P;
+} octx;
+
+/* cylindrical angle of (x,y) as the reference computes it */
+static void cyl_of(double x, double y, double *R, double *phi, double *sp, double *cp)
+{
+  *R = sqrt(x * x + y * y);
+  *phi = acos(x / *R);
+  *sp = y / *R;
+  *cp = x / *R;
+  if (y < 0.) *phi = 2. * M_PI - *phi;
+}
+
+static void sum3(opot *P, double R, double z, double phi, double *Rf, double *zf, double *pt)
+{
+  double a = 0., b = 0., c = 0.;
+  for (int i = 0; i < P->n; i++) a += comp_Rforce(&P->c[i], R, z, phi);
+  for (int i = 0; i < P->n; i++) c += comp_phitorque(&P->c[i], R, z, phi);
+  for (int i = 0; i < P->n; i++) b += comp_zforce(&P->c[i], R, z, phi);
+  *Rf = a;
+  *zf = b;
+  *pt = c;
+  P->nforce++;
+}
+
+static void sum2(opot *P, double R, double phi, double *Rf, double *pt)
+{
+  double a = 0., c = 0.;
+  for (int i = 0; i < P->n; i++) a += comp_planarRforce(&P->c[i], R, phi);
+  for (int i = 0; i < P->n; i++) c += comp_planarphitorque(&P->c[i], R, phi);
+  *Rf = a;
+  *pt = c;
+  P->nforce++;
+}
+
+typedef void (*rhs_fn)(opot *P, const double *q, double *a);
+
+/* evalRectForce (integrateFullOrbit.c:1307) */
+static void rect_force3(opot *P, const double *q, double *a)
+{
+  double R, phi, sp, cp, Rf, zf, pt;
+  cyl_of(q[0], q[1], &R, &phi, &sp, &cp);
+  sum3(P, R, q[2], phi, &Rf, &zf, &pt);
+  a[0] = cp * Rf - 1. / R * sp * pt;
+  a[1] = sp * Rf + 1. / R * cp * pt;
+  a[2] = zf;
+}
+
+/* evalRectDeriv (integrateFullOrbit.c:1326) */
+static void rect_deriv3(opot *P, const double *q, double *a)
+{
+  a[0] = q[3];
+  a[1] = q[4];
+  a[2] = q[5];
+  rect_force3(P, q, a + 3);
+}
+
+/* evalPlanarRectForce (integratePlanarOrbit.c:1015) */
+static void rect_force2(opot *P, const double *q, double *a)
+{
+  double R, phi, sp, cp, Rf, pt;
+  cyl_of(q[0], q[1], &R, &phi, &sp, &cp);
+  sum2(P, R, phi, &Rf, &pt);
+  a[0] = cp * Rf - 1. / R * sp * pt;
+  a[1] = sp * Rf + 1. / R * cp * pt;
+}
+
+static void rect_deriv2(opot *P, const double *q, double *a)
+{
+  a[0] = q[2];
+  a[1] = q[3];
+  rect_force2(P, q, a + 2);
+}
+
+/* Cartesian tidal tensor K = -grad grad Phi in the plane, from cylindrical
+   derivatives (integratePlanarOrbit.c:1150-1174 / integrateFullOrbit.c:1570-1590) */
+static void planar_K(double R, double sp, double cp, double Rf, double pt, double R2d,
+                     double p2d, double Rpd, double *Kxx, double *Kxy, double *Kyx, double *Kyy)
+{
+  *Kxx = -cp * cp * R2d + 2. * cp * sp / R / R * pt + sp * sp / R * Rf + 2. * sp * cp / R * Rpd -
+         sp * sp / R / R * p2d;
+  *Kxy = -sp * cp * R2d + (sp * sp - cp * cp) / R / R * pt - cp * sp / R * Rf -
+         (cp * cp - sp * sp) / R * Rpd + cp * sp / R / R * p2d;
+  *Kyx = -cp * sp * R2d + (sp * sp - cp * cp) / R / R * pt + (sp * sp - cp * cp) / R * Rpd -
+         sp * cp / R * Rf + sp * cp / R / R * p2d;
+  *Kyy = -sp * sp * R2d - 2. * sp * cp / R / R * pt - 2. * sp * cp / R * Rpd + cp * cp / R * Rf -
+         cp * cp / R / R * p2d;
+}
+
+static void hess3(opot *P, double R, double z, double phi, double h[6])
+{
+  for (int w = 0; w < 6; w++) {
+    double s = 0.;
+    for (int i = 0; i < P->n; i++) s += comp_hess(&P->c[i], w, R, z, phi);
+    h[w] = s;
+  }
+}
+
+/* full 3D K (symmetric) into k[6] = xx, xy, yy, xz, yz, zz */
+static void full_K(opot *P, double R, double z, double phi, double sp, double cp, double Rf,
+                   double pt, double k[6])
+{
+  double h[6], Kyx;
+  hess3(P, R, z, phi, h); /* R2, z2, Rz, phi2, Rphi, zphi */
+  planar_K(R, sp, cp, Rf, pt, h[0], h[3], h[4], &k[0], &k[1], &Kyx, &k[2]);
+  k[3] = -cp * h[2] + sp / R * h[5];
+  k[4] = -sp * h[2] - cp / R * h[5];
+  k[5] = -h[1];
+}
+
+/* evalRectDeriv_dxdv (integrateFullOrbit.c:1496): 12-D state */
+static void rect_deriv3_dxdv(opot *P, const double *q, double *a)
+{
+  double R, phi, sp, cp, Rf, zf, pt, k[6];
+  a[0] = q[3];
+  a[1] = q[4];
+  a[2] = q[5];
+  cyl_of(q[0], q[1], &R, &phi, &sp, &cp);
+  sum3(P, R, q[2], phi, &Rf, &zf, &pt);
+  a[3] = cp * Rf - 1. / R * sp * pt;
+  a[4] = sp * Rf + 1. / R * cp * pt;
+  a[5] = zf;
+  a[6] = q[9];
+  a[7] = q[10];
+  a[8] = q[11];
+  full_K(P, R, q[2], phi, sp, cp, Rf, pt, k);
+  double dx = q[6], dy = q[7], dz = q[8];
+  a[9] = k[0] * dx + k[1] * dy + k[3] * dz;
+  a[10] = k[1] * dx + k[2] * dy + k[4] * dz;
+  a[11] = k[3] * dx + k[4] * dy + k[5] * dz;
+}
+
+/* evalRectForce_dxdv with nde = 1 (integrateFullOrbit.c:1627): q[6] = (x,y,z,dx,dy,dz) */
+static void rect_force3_dxdv(opot *P, const double *q, double *a)
+{
+  double R, phi, sp, cp, Rf, zf, pt, k[6];
+  cyl_of(q[0], q[1], &R, &phi, &sp, &cp);
+  sum3(P, R, q[2], phi, &Rf, &zf, &pt);
+  a[0] = cp * Rf - 1. / R * sp * pt;
+  a[1] = sp * Rf + 1. / R * cp * pt;
+  a[2] = zf;
+  full_K(P, R, q[2], phi, sp, cp, Rf, pt, k);
+  double dx = q[3], dy = q[4], dz = q[5];
+  a[3] = k[0] * dx + k[1] * dy + k[3] * dz;
+  a[4] = k[1] * dx + k[2] * dy + k[4] * dz;
+  a[5] = k[3] * dx + k[4] * dy + k[5] * dz;
+}
+
+static void planar_hess_sum(opot *P, double R, double phi, double *R2d, double *p2d, double *Rpd)
+{
+  double a = 0., b = 0., c = 0.;
+  for (int i = 0; i < P->n; i++) a += comp_planarhess(&P->c[i], 0, R, phi);
+  for (int i = 0; i < P->n; i++) b += comp_planarhess(&P->c[i], 1, R, phi);
+  for (int i = 0; i < P->n; i++) c += comp_planarhess(&P->c[i], 2, R, phi);
+  *R2d = a;
+  *p2d = b;
+  *Rpd = c;
+}
+
+/* evalPlanarRectDeriv_dxdv (integratePlanarOrbit.c:1124): 8-D state */
+static void rect_deriv2_dxdv(opot *P, const double *q, double *a)
+{
+  double R, phi, sp, cp, Rf, pt, R2d, p2d, Rpd, Kxx, Kxy, Kyx, Kyy;
+  a[0] = q[2];
+  a[1] = q[3];
+  cyl_of(q[0], q[1], &R, &phi, &sp, &cp);
+  sum2(P, R, phi, &Rf, &pt);
+  a[2] = cp * Rf - 1. / R * sp * pt;
+  a[3] = sp * Rf + 1. / R * cp * pt;
+  a[4] = q[6];
+  a[5] = q[7];
+  planar_hess_sum(P, R, phi, &R2d, &p2d, &Rpd);
+  planar_K(R, sp, cp, Rf, pt, R2d, p2d, Rpd, &Kxx, &Kxy, &Kyx, &Kyy);
+  a[6] = Kxx * q[4] + Kxy * q[5];
+  a[7] = Kyx * q[4] + Kyy * q[5];
+}
+
+/* evalPlanarRectForce_dxdv, nde = 1 (integratePlanarOrbit.c:1228): q = (x,y,dx,dy) */
+static void rect_force2_dxdv(opot *P, const double *q, double *a)
+{
+  double R, phi, sp, cp, Rf, pt, R2d, p2d, Rpd, Kxx, Kxy, Kyx, Kyy;
+  cyl_of(q[0], q[1], &R, &phi, &sp, &cp);
+  sum2(P, R, phi, &Rf, &pt);
+  a[0] = cp * Rf - 1. / R * sp * pt;
+  a[1] = sp * Rf + 1. / R * cp * pt;
+  planar_hess_sum(P, R, phi, &R2d, &p2d, &Rpd);
+  planar_K(R, sp, cp, Rf, pt, R2d, p2d, Rpd, &Kxx, &Kxy, &Kyx, &Kyy);
+  a[2] = Kxx * q[2] + Kxy * q[3];
+  a[3] = Kxy * q[2] + Kyy * q[3];
+}
+
+/* ------------------------------------------------------------------ */
+/* steppers                                                            */
+/* ------------------------------------------------------------------ */
+#define DT_SENTINEL -9999.99
+#define MAX_DT_REDUCE 10000.
+#define MAXD 12
+
+static const double S4C[4] = {0.6756035959798289, -0.1756035959798288, -0.1756035959798288,
+                              0.6756035959798289};
+static const double S4D[3] = {1.3512071919596578, -1.7024143839193153, 1.3512071919596578};
+
+static inline void drift(int n, const double *q, const double *p, double h, double *qn)
+{
+  for (int i = 0; i < n; i++) qn[i] = q[i] + h * p[i];
+}
+static inline void kick(int n, const double *p, double h, const double *a, double *pn)
+{
+  for (int i = 0; i < n; i++) pn[i] = p[i] + h * a[i];
+}
+
+/* log-sum-exp error scale of the symplectic / rk estimators
+   (bovy_symplecticode.c:609-624) */
+static double est_scale(int n, const double *v, double rtol, double atol)
+{
+  double m = log(fabs(v[0]));
+  for (int i = 1; i < n; i++)
+    if (log(fabs(v[i])) > m) m = log(fabs(v[i]));
+  double c = fmax(atol, rtol + m);
+  return log(exp(atol - c) + exp(rtol + m - c)) + c;
+}
+
+/* leapfrog_estimate_step (bovy_symplecticode.c:588-664) */
+static double leapfrog_est(rhs_fn f, opot *P, int dim, const double *qo, const double *po,
+                           double dt, double rtol, double atol)
+{
+  double err = 2., init_dt = dt;
+  double q11[MAXD], q12[MAXD], p11[MAXD], p12[MAXD], qt[MAXD], pt[MAXD], a[MAXD];
+  double sq = est_scale(dim, qo, rtol, atol), sp = est_scale(dim, po, rtol, atol);
+  dt *= 2.;
+  while (err > 1. && init_dt / dt < MAX_DT_REDUCE) {
+    dt /= 2.;
+    drift(dim, qo, po, dt / 2., q12);
+    f(P, q12, a);
+    kick(dim, po, dt, a, p11);
+    drift(dim, q12, p11, dt / 2., q11);
+    drift(dim, qo, po, dt / 4., q12);
+    f(P, q12, a);
+    kick(dim, po, dt / 2., a, pt);
+    drift(dim, q12, pt, dt / 2., qt);
+    f(P, qt, a);
+    kick(dim, pt, dt / 2., a, p12);
+    drift(dim, qt, p12, dt / 4., q12);
+    err = 0.;
+    for (int i = 0; i < dim; i++) {
+      err += exp(2. * log(fabs(q11[i] - q12[i])) - 2. * sq);
+      err += exp(2. * log(fabs(p11[i] - p12[i])) - 2. * sp);
+    }
+    err = sqrt(err / 2. / dim);
+  }
+  return dt;
+}
+
+/* symplec4_estimate_step (bovy_symplecticode.c:665-809) */
+static double symplec4_est(rhs_fn f, opot *P, int dim, const double *qo, const double *po,
+                           double dt, double rtol, double atol)
+{
+  const double c1 = S4C[0], c2 = S4C[1], c3 = S4C[2], c4 = S4C[3];
+  const double d1 = S4D[0], d2 = S4D[1], d3 = S4D[2];
+  double err = 2., init_dt = dt;
+  double q11[MAXD], q12[MAXD], p11[MAXD], p12[MAXD], qt[MAXD], pt[MAXD], a[MAXD];
+  double sq = est_scale(dim, qo, rtol, atol), sp = est_scale(dim, po, rtol, atol);
+  dt *= 2.;
+  while (err > 1. && init_dt / dt < MAX_DT_REDUCE) {
+    dt /= 2.;
+    /* one step of dt */
+    drift(dim, qo, po, c1 * dt, q12);
+    f(P, q12, a);
+    kick(dim, po, d1 * dt, a, p12);
+    drift(dim, q12, p12, c2 * dt, qt);
+    f(P, qt, a);
+    kick(dim, p12, d2 * dt, a, pt);
+    drift(dim, qt, pt, c3 * dt, q12);
+    f(P, q12, a);
+    kick(dim, pt, d3 * dt, a, p11);
+    drift(dim, q12, p11, c4 * dt, q11);
+    /* two steps of dt/2 */
+    drift(dim, qo, po, c1 * dt / 2., q12);
+    f(P, q12, a);
+    kick(dim, po, d1 * dt / 2., a, p12);
+    drift(dim, q12, p12, c2 * dt / 2., qt);
+    f(P, qt, a);
+    kick(dim, p12, d2 * dt / 2., a, pt);
+    drift(dim, qt, pt, c3 * dt / 2., q12);
+    f(P, q12, a);
+    kick(dim, pt, d3 * dt / 2., a, p12);
+    drift(dim, q12, p12, (c1 + c4) * dt / 2., qt);
+    f(P, qt, a);
+    kick(dim, p12, d1 * dt / 2., a, pt);
+    drift(dim, qt, pt, c2 * dt / 2., q12);
+    f(P, q12, a);
+    kick(dim, pt, d2 * dt / 2., a, p12);
+    drift(dim, q12, p12, c3 * dt / 2., qt);
+    f(P, qt, a);
+    kick(dim, p12, d3 * dt / 2., a, pt);
+    drift(dim, qt, pt, c4 * dt / 2., q12);
+    for (int i = 0; i < dim; i++) p12[i] = pt[i];
+    err = 0.;
+    for (int i = 0; i < dim; i++) {
+      err += exp(2. * log(fabs(q11[i] - q12[i])) - 2. * sq);
+      err += exp(2. * log(fabs(p11[i] - p12[i])) - 2. * sp);
+    }
+    err = sqrt(err / 2. / dim);
+  }
+  return dt;
+}
+
+/* Output ordering of a symplectic state: plain runs store [q(dim),p(dim)];
+   variational runs store [q_base,p_base,q_dev,p_dev] (save_qp_dxdv). */
+static void save_qp(int ndim, int dim_base, const double *q, const double *p, double *out)
+{
+  if (ndim == dim_base) {
+    for (int i = 0; i < ndim; i++) out[i] = q[i];
+    for (int i = 0; i < ndim; i++) out[ndim + i] = p[i];
+  } else {
+    int nb = ndim / dim_base;
+    for (int b = 0; b < nb; b++) {
+      for (int k = 0; k < dim_base; k++) *out++ = q[dim_base * b + k];
+      for (int k = 0; k < dim_base; k++) *out++ = p[dim_base * b + k];
+    }
+  }
+}
+
+typedef struct {
+  long long nsteps;
+  long long max_attempts;
+  int err;
+} ostat;
+
+/* leapfrog / symplec4 (bovy_symplecticode.c:132-377 and the *_dxdv steppers
+   :1053-1268).  f steps the ndim-vector, fb is the base force for the
+   estimator over dim_base components; yo is in save_qp layout. */
+static void symplectic(int order4, rhs_fn f, rhs_fn fb, opot *P, int ndim, int dim_base,
+                       const double *yo, int nt, double dt, const double *t, double rtol,
+                       double atol, double *result, ostat *st)
+{
+  double qo[MAXD], po[MAXD], q12[MAXD], p12[MAXD], a[MAXD];
+  int nb = ndim / dim_base;
+  for (int b = 0; b < nb; b++)
+    for (int k = 0; k < dim_base; k++) {
+      qo[dim_base * b + k] = yo[2 * dim_base * b + k];
+      po[dim_base * b + k] = yo[2 * dim_base * b + dim_base + k];
+    }
+  save_qp(ndim, dim_base, qo, po, result);
+  result += 2 * ndim;
+  st->err = 0;
+  double init_dt = t[1] - t[0];
+  if (dt == DT_SENTINEL)
+    dt = order4 ? symplec4_est(fb, P, dim_base, qo, po, init_dt, rtol, atol)
+                : leapfrog_est(fb, P, dim_base, qo, po, init_dt, rtol, atol);
+  long ndt = (long)(init_dt / dt);
+  if (!order4) {
+    for (int ii = 0; ii < nt - 1; ii++) {
+      drift(ndim, qo, po, dt / 2., q12);
+      for (long jj = 0; jj < ndt - 1; jj++) {
+        f(P, q12, a);
+        kick(ndim, po, dt, a, p12);
+        drift(ndim, q12, p12, dt, qo);
+        for (int k = 0; k < ndim; k++) {
+          q12[k] = qo[k];
+          po[k] = p12[k];
+        }
+      }
+      f(P, q12, a);
+      kick(ndim, po, dt, a, po);
+      drift(ndim, q12, po, dt / 2., qo);
+      save_qp(ndim, dim_base, qo, po, result);
+      result += 2 * ndim;
+    }
+  } else {
+    const double c1 = S4C[0], c2 = S4C[1], c3 = S4C[2], c4 = S4C[3];
+    const double d1 = S4D[0], d2 = S4D[1], d3 = S4D[2];
+    for (int ii = 0; ii < nt - 1; ii++) {
+      drift(ndim, qo, po, c1 * dt, q12);
+      for (long jj = 0; jj < ndt - 1; jj++) {
+        f(P, q12, a);
+        kick(ndim, po, d1 * dt, a, p12);
+        drift(ndim, q12, p12, c2 * dt, qo);
+        f(P, qo, a);
+        kick(ndim, p12, d2 * dt, a, po);
+        drift(ndim, qo, po, c3 * dt, q12);
+        f(P, q12, a);
+        kick(ndim, po, d3 * dt, a, p12);
+        drift(ndim, q12, p12, (c4 + c1) * dt, qo);
+        for (int k = 0; k < ndim; k++) {
+          q12[k] = qo[k];
+          po[k] = p12[k];
+        }
+      }
+      f(P, q12, a);
+      kick(ndim, po, d1 * dt, a, p12);
+      drift(ndim, q12, p12, c2 * dt, qo);
+      f(P, qo, a);
+      kick(ndim, p12, d2 * dt, a, po);
+      drift(ndim, qo, po, c3 * dt, q12);
+      f(P, q12, a);
+      kick(ndim, po, d3 * dt, a, p12);
+      drift(ndim, q12, p12, c4 * dt, qo);
+      for (int k = 0; k < ndim; k++) po[k] = p12[k];
+      save_qp(ndim, dim_base, qo, po, result);
+      result += 2 * ndim;
+    }
+  }
+  st->nsteps = (long long)ndt * (nt - 1);
+}
+
+/* bovy_rk4_onestep (bovy_rk.c:142-170) */
+static void rk4_onestep(rhs_fn f, opot *P, int dim, const double *yn, double *yn1, double dt,
+                        double *ynk, double *a)
+{
+  f(P, yn, a);
+  for (int i = 0; i < dim; i++) yn1[i] += dt * a[i] / 6.;
+  for (int i = 0; i < dim; i++) ynk[i] = yn[i] + dt * a[i] / 2.;
+  f(P, ynk, a);
+  for (int i = 0; i < dim; i++) yn1[i] += dt * a[i] / 3.;
+  for (int i = 0; i < dim; i++) ynk[i] = yn[i] + dt * a[i] / 2.;
+  f(P, ynk, a);
+  for (int i = 0; i < dim; i++) yn1[i] += dt * a[i] / 3.;
+  for (int i = 0; i < dim; i++) ynk[i] = yn[i] + dt * a[i];
+  f(P, ynk, a);
+  for (int i = 0; i < dim; i++) yn1[i] += dt * a[i] / 6.;
+}
+
+/* rk4_estimate_step (bovy_rk.c:328-395) */
+static double rk4_est(rhs_fn f, opot *P, int dim, const double *yo, double dt, double rtol,
+                      double atol)
+{
+  double err = 2., init_dt = dt;
+  double yn[MAXD], y1[MAXD], y21[MAXD], y2[MAXD], ynk[MAXD], a[MAXD];
+  double s = est_scale(dim, yo, rtol, atol);
+  while (err > 1.) {
+    for (int i = 0; i < dim; i++) yn[i] = y1[i] = y21[i] = yo[i];
+    rk4_onestep(f, P, dim, yn, y1, dt, ynk, a);
+    rk4_onestep(f, P, dim, yn, y21, dt / 2., ynk, a);
+    for (int i = 0; i < dim; i++) y2[i] = y21[i];
+    rk4_onestep(f, P, dim, y21, y2, dt / 2., ynk, a);
+    err = 0.;
+    for (int i = 0; i < dim; i++) err += exp(2. * log(fabs(y1[i] - y2[i])) - 2. * s);
+    err = sqrt(err / dim);
+    if (ceil(pow(err, 1. / 5.)) > 1. && init_dt / dt * ceil(pow(err, 1. / 5.)) < MAX_DT_REDUCE)
+      dt /= ceil(pow(err, 1. / 5.));
+    else
+      break;
+  }
+  return dt;
+}
+
+/* bovy_rk4 (bovy_rk.c:66-141) */
+static void rk4(rhs_fn f, opot *P, int dim, const double *yo, int nt, double dt, const double *t,
+                double rtol, double atol, double *result, ostat *st)
+{
+  double yn[MAXD], yn1[MAXD], ynk[MAXD], a[MAXD];
+  for (int i = 0; i < dim; i++) result[i] = yo[i];
+  result += dim;
+  st->err = 0;
+  for (int i = 0; i < dim; i++) yn[i] = yn1[i] = yo[i];
+  double init_dt = t[1] - t[0];
+  if (dt == DT_SENTINEL) dt = rk4_est(f, P, dim, yo, init_dt, rtol, atol);
+  long ndt = (long)(init_dt / dt);
+  for (int ii = 0; ii < nt - 1; ii++) {
+    for (long jj = 0; jj < ndt - 1; jj++) {
+      rk4_onestep(f, P, dim, yn, yn1, dt, ynk, a);
+      for (int k = 0; k < dim; k++) yn[k] = yn1[k];
+    }
+    rk4_onestep(f, P, dim, yn, yn1, dt, ynk, a);
+    for (int k = 0; k < dim; k++) result[k] = yn1[k];
+    result += dim;
+    for (int k = 0; k < dim; k++) yn[k] = yn1[k];
+  }
+  st->nsteps = (long long)ndt * (nt - 1);
+}
+
+#define DMAX(a, b) (((a) > (b)) ? (a) : (b))
+#define DMIN(a, b) (((a) < (b)) ? (a) : (b))
+static inline double csign(double x, double y) { return (y > 0.0) ? fabs(x) : -fabs(x); }
+
+/* dop853 (leung_dop853.c:231-517); rtol/atol arrive as logs */
+static void dop853(rhs_fn f, opot *P, int dim, const double *yin, int nt, const double *t,
+                   double rtol, double atol, double *result, ostat *st)
+{
+  rtol = exp(rtol);
+  atol = exp(atol);
+  const double safe = 0.9, expo1 = 1.0 / 8.0, facc1 = 1.0 / 0.333, facc2 = 1.0 / 6.0;
+  const double uround = 2.3e-16;
+  double facold = 1.0e-4;
+  double hmax = t[nt - 1] - t[0];
+  double pos_neg = csign(1.0, hmax);
+  double y0[MAXD], yy1[MAXD], k1[MAXD], k2[MAXD], k3[MAXD], k4[MAXD], k5[MAXD], k6[MAXD],
+      k7[MAXD], k8[MAXD], k9[MAXD], k10[MAXD];
+  double rc1[MAXD], rc2[MAXD], rc3[MAXD], rc4[MAXD], rc5[MAXD], rc6[MAXD], rc7[MAXD], rc8[MAXD];
+  int i;
+  for (i = 0; i < dim; i++) y0[i] = yin[i];
+  for (i = 0; i < dim; i++) result[i] = y0[i];
+  result += dim;
+  st->err = 0;
+  st->nsteps = 0;
+
+  f(P, y0, k1);
+  double dnf = 0.0, dny = 0.0, sk, sqr;
+  for (i = 0; i < dim; i++) {
+    sk = atol + rtol * fabs(y0[i]);
+    sqr = k1[i] / sk;
+    dnf += sqr * sqr;
+    sqr = y0[i] / sk;
+    dny += sqr * sqr;
+  }
+  double h = csign(DMIN(sqrt(dny / dnf) * 0.01, fabs(hmax)), pos_neg);
+  for (i = 0; i < dim; i++) k3[i] = y0[i] + h * k1[i];
+  f(P, k3, k2);
+  double der2 = 0.0;
+  for (i = 0; i < dim; i++) {
+    sk = atol + rtol * fabs(y0[i]);
+    sqr = (k2[i] - k1[i]) / sk;
+    der2 += sqr * sqr;
+  }
+  der2 = sqrt(der2) / h;
+  double der12 = DMAX(fabs(der2), sqrt(dnf));
+  double h1 = pow(0.01 / der12, 1.0 / 8.0);
+  h = csign(DMIN(100.0 * fabs(h), DMIN(fabs(h1), fabs(hmax))), pos_neg);
+
+  int reject = 0;
+  double t_current = t[0], t_old = t[0], t_old_older = t_old;
+  int done = 0;
+  long long attempts = 0;
+  while (done < nt - 1) {
+    if (st->max_attempts > 0 && attempts >= st->max_attempts) {
+      st->err = 2;
+      break;
+    }
+    attempts++;
+    h = pos_neg * DMAX(fabs(h), 1e3 * uround);
+    for (i = 0; i < dim; i++) yy1[i] = y0[i] + h * DP_A21 * k1[i];
+    f(P, yy1, k2);
+    for (i = 0; i < dim; i++) yy1[i] = y0[i] + h * (DP_A31 * k1[i] + DP_A32 * k2[i]);
+    f(P, yy1, k3);
+    for (i = 0; i < dim; i++) yy1[i] = y0[i] + h * (DP_A41 * k1[i] + DP_A43 * k3[i]);
+    f(P, yy1, k4);
+    for (i = 0; i < dim; i++)
+      yy1[i] = y0[i] + h * (DP_A51 * k1[i] + DP_A53 * k3[i] + DP_A54 * k4[i]);
+    f(P, yy1, k5);
+    for (i = 0; i < dim; i++)
+      yy1[i] = y0[i] + h * (DP_A61 * k1[i] + DP_A64 * k4[i] + DP_A65 * k5[i]);
+    f(P, yy1, k6);
+    for (i = 0; i < dim; i++)
+      yy1[i] = y0[i] + h * (DP_A71 * k1[i] + DP_A74 * k4[i] + DP_A75 * k5[i] + DP_A76 * k6[i]);
+    f(P, yy1, k7);
+    for (i = 0; i < dim; i++)
+      yy1[i] = y0[i] + h * (DP_A81 * k1[i] + DP_A84 * k4[i] + DP_A85 * k5[i] + DP_A86 * k6[i] +
+                            DP_A87 * k7[i]);
+    f(P, yy1, k8);
+    for (i = 0; i < dim; i++)
+      yy1[i] = y0[i] + h * (DP_A91 * k1[i] + DP_A94 * k4[i] + DP_A95 * k5[i] + DP_A96 * k6[i] +
+                            DP_A97 * k7[i] + DP_A98 * k8[i]);
+    f(P, yy1, k9);
+    for (i = 0; i < dim; i++)
+      yy1[i] = y0[i] + h * (DP_A101 * k1[i] + DP_A104 * k4[i] + DP_A105 * k5[i] +
+                            DP_A106 * k6[i] + DP_A107 * k7[i] + DP_A108 * k8[i] +
+                            DP_A109 * k9[i]);
+    f(P, yy1, k10);
+    for (i = 0; i < dim; i++)
+      yy1[i] = y0[i] + h * (DP_A111 * k1[i] + DP_A114 * k4[i] + DP_A115 * k5[i] +
+                            DP_A116 * k6[i] + DP_A117 * k7[i] + DP_A118 * k8[i] +
+                            DP_A119 * k9[i] + DP_A1110 * k10[i]);
+    f(P, yy1, k2);
+    for (i = 0; i < dim; i++)
+      yy1[i] = y0[i] + h * (DP_A121 * k1[i] + DP_A124 * k4[i] + DP_A125 * k5[i] +
+                            DP_A126 * k6[i] + DP_A127 * k7[i] + DP_A128 * k8[i] +
+                            DP_A129 * k9[i] + DP_A1210 * k10[i] + DP_A1211 * k2[i]);
+    t_old_older = t_old;
+    t_old = t_current;
+    t_current = t_current + h;
+    f(P, yy1, k3);
+    for (i = 0; i < dim; i++) {
+      k4[i] = DP_B1 * k1[i] + DP_B6 * k6[i] + DP_B7 * k7[i] + DP_B8 * k8[i] + DP_B9 * k9[i] +
+              DP_B10 * k10[i] + DP_B11 * k2[i] + DP_B12 * k3[i];
+      k5[i] = y0[i] + h * k4[i];
+    }
+    double err = 0.0, err2 = 0.0, erri;
+    for (i = 0; i < dim; i++) {
+      sk = atol + rtol * DMAX(fabs(y0[i]), fabs(k5[i]));
+      erri = k4[i] - DP_BHH1 * k1[i] - DP_BHH2 * k9[i] - DP_BHH3 * k3[i];
+      sqr = erri / sk;
+      err2 += sqr * sqr;
+      erri = DP_ER1 * k1[i] + DP_ER6 * k6[i] + DP_ER7 * k7[i] + DP_ER8 * k8[i] +
+             DP_ER9 * k9[i] + DP_ER10 * k10[i] + DP_ER11 * k2[i] + DP_ER12 * k3[i];
+      sqr = erri / sk;
+      err += sqr * sqr;
+    }
+    double deno = err + 0.01 * err2;
+    if (deno <= 0.0) deno = 1.0;
+    err = fabs(h) * err * sqrt(1.0 / (deno * (double)dim));
+    double fac11 = pow(err, expo1);
+    double fac = fac11 / pow(facold, 0.0);
+    fac = DMAX(facc2, DMIN(facc1, fac / safe));
+    double hnew = h / fac;
+    if (err <= 1.0) {
+      facold = DMAX(err, 1.0e-4);
+      st->nsteps++;
+      f(P, k5, k4);
+      for (i = 0; i < dim; i++) {
+        rc1[i] = y0[i];
+        double ydiff = k5[i] - y0[i];
+        rc2[i] = ydiff;
+        double bspl = h * k1[i] - ydiff;
+        rc3[i] = bspl;
+        rc4[i] = ydiff - h * k4[i] - bspl;
+        rc5[i] = DP_D41 * k1[i] + DP_D46 * k6[i] + DP_D47 * k7[i] + DP_D48 * k8[i] +
+                 DP_D49 * k9[i] + DP_D410 * k10[i] + DP_D411 * k2[i] + DP_D412 * k3[i];
+        rc6[i] = DP_D51 * k1[i] + DP_D56 * k6[i] + DP_D57 * k7[i] + DP_D58 * k8[i] +
+                 DP_D59 * k9[i] + DP_D510 * k10[i] + DP_D511 * k2[i] + DP_D512 * k3[i];
+        rc7[i] = DP_D61 * k1[i] + DP_D66 * k6[i] + DP_D67 * k7[i] + DP_D68 * k8[i] +
+                 DP_D69 * k9[i] + DP_D610 * k10[i] + DP_D611 * k2[i] + DP_D612 * k3[i];
+        rc8[i] = DP_D71 * k1[i] + DP_D76 * k6[i] + DP_D77 * k7[i] + DP_D78 * k8[i] +
+                 DP_D79 * k9[i] + DP_D710 * k10[i] + DP_D711 * k2[i] + DP_D712 * k3[i];
+      }
+      for (i = 0; i < dim; i++)
+        yy1[i] = y0[i] + h * (DP_A141 * k1[i] + DP_A147 * k7[i] + DP_A148 * k8[i] +
+                              DP_A149 * k9[i] + DP_A1410 * k10[i] + DP_A1411 * k2[i] +
+                              DP_A1412 * k3[i] + DP_A1413 * k4[i]);
+      f(P, yy1, k10);
+      for (i = 0; i < dim; i++)
+        yy1[i] = y0[i] + h * (DP_A151 * k1[i] + DP_A156 * k6[i] + DP_A157 * k7[i] +
+                              DP_A158 * k8[i] + DP_A1511 * k2[i] + DP_A1512 * k3[i] +
+                              DP_A1513 * k4[i] + DP_A1514 * k10[i]);
+      f(P, yy1, k2);
+      for (i = 0; i < dim; i++)
+        yy1[i] = y0[i] + h * (DP_A161 * k1[i] + DP_A166 * k6[i] + DP_A167 * k7[i] +
+                              DP_A168 * k8[i] + DP_A169 * k9[i] + DP_A1613 * k4[i] +
+                              DP_A1614 * k10[i] + DP_A1615 * k2[i]);
+      f(P, yy1, k3);
+      for (i = 0; i < dim; i++) {
+        rc5[i] = h * (rc5[i] + DP_D413 * k4[i] + DP_D414 * k10[i] + DP_D415 * k2[i] +
+                      DP_D416 * k3[i]);
+        rc6[i] = h * (rc6[i] + DP_D513 * k4[i] + DP_D514 * k10[i] + DP_D515 * k2[i] +
+                      DP_D516 * k3[i]);
+        rc7[i] = h * (rc7[i] + DP_D613 * k4[i] + DP_D614 * k10[i] + DP_D615 * k2[i] +
+                      DP_D616 * k3[i]);
+        rc8[i] = h * (rc8[i] + DP_D713 * k4[i] + DP_D714 * k10[i] + DP_D715 * k2[i] +
+                      DP_D716 * k3[i]);
+        k1[i] = k4[i];
+        y0[i] = k5[i];
+      }
+      while (done < nt - 1 && pos_neg * t[done + 1] < pos_neg * t_current) {
+        double s = (t[done + 1] - t_old) / h, s1 = 1.0 - s;
+        for (i = 0; i < dim; i++)
+          result[i] =
+              rc1[i] +
+              s * (rc2[i] +
+                   s1 * (rc3[i] +
+                         s * (rc4[i] + s1 * (rc5[i] + s * (rc6[i] + s1 * (rc7[i] + s * rc8[i]))))));
+        result += dim;
+        done++;
+      }
+      hnew = (fabs(hnew) > fabs(hmax)) ? pos_neg * hmax : hnew;
+      if (reject) hnew = pos_neg * DMIN(fabs(hnew), fabs(h));
+      reject = 0;
+    } else {
+      hnew = h / DMIN(facc1, fac11 / safe);
+      reject = 1;
+      t_current = t_old;
+      t_old = t_old_older;
+    }
+    h = hnew;
+  }
+}
+
+/* ------------------------------------------------------------------ */
+/* coordinates (bovy_coords.c:57-148)                                  */
+/* ------------------------------------------------------------------ */
+static void cyl_to_rect(double *v)
+{
+  double R = v[0], phi = v[5], cp = cos(phi), sp = sin(phi), vR = v[1], vT = v[2];
+  v[0] = R * cp;
+  v[1] = R * sp;
+  v[2] = v[3];
+  v[5] = v[4];
+  v[3] = vR * cp - vT * sp;
+  v[4] = vR * sp + vT * cp;
+}
+static void rect_to_cyl(double *v)
+{
+  double x = v[0], y = v[1], vx = v[3], vy = v[4];
+  v[3] = v[2];
+  v[4] = v[5];
+  v[5] = atan2(y, x);
+  double cp = cos(v[5]), sp = sin(v[5]);
+  v[0] = sqrt(x * x + y * y);
+  v[1] = vx * cp + vy * sp;
+  v[2] = -vx * sp + vy * cp;
+}
+static void polar_to_rect(double *v)
+{
+  double R = v[0], phi = v[3], cp = cos(phi), sp = sin(phi), vR = v[1], vT = v[2];
+  v[0] = R * cp;
+  v[1] = R * sp;
+  v[2] = vR * cp - vT * sp;
+  v[3] = vR * sp + vT * cp;
+}
+static void rect_to_polar(double *v)
+{
+  double x = v[0], y = v[1], vx = v[2], vy = v[3];
+  v[3] = atan2(y, x);
+  double cp = cos(v[3]), sp = sin(v[3]);
+  v[0] = sqrt(x * x + y * y);
+  v[1] = vx * cp + vy * sp;
+  v[2] = -vx * sp + vy * cp;
+}
+
+/* ------------------------------------------------------------------ */
+/* exported drivers                                                    */
+/* ------------------------------------------------------------------ */
+#define EXPORT __attribute__((visibility("default")))
+
+/* One orbit of the plain integration in rectangular coordinates.
+   w: [2*dim] rectangular ICs; out: nt*2*dim rectangular rows. */
+static int run_plain(opot *P, int planar, int method, const double *w, int nt, const double *t,
+                     double dt, double rtol, double atol, double *out, ostat *st)
+{
+  int dim = planar ? 2 : 3;
+  rhs_fn force = planar ? rect_force2 : rect_force3;
+  rhs_fn deriv = planar ? rect_deriv2 : rect_deriv3;
+  switch (method) {
+  case 0: symplectic(0, force, force, P, dim, dim, w, nt, dt, t, rtol, atol, out, st); return 0;
+  case 3: symplectic(1, force, force, P, dim, dim, w, nt, dt, t, rtol, atol, out, st); return 0;
+  case 1: rk4(deriv, P, 2 * dim, w, nt, dt, t, rtol, atol, out, st); return 0;
+  case 6: dop853(deriv, P, 2 * dim, w, nt, t, rtol, atol, out, st); return 0;
+  }
+  return -1;
+}
+
+/* Batched integration with galpy's layout (integrateFullOrbit.c:1046 /
+   integratePlanarOrbit.c:743): yo [nobj][6] (R,vR,vT,z,vz,phi) or [nobj][4]
+   (R,vR,vT,phi), overwritten with rectangular ICs like the reference;
+   result [nobj][nt][6|4] cylindrical.  method: 0 leapfrog, 1 rk4,
+   3 symplec4, 6 dop853.  nsteps/nforce (optional) receive per-orbit counts.
+   Returns 0, -2 unsupported method, -3 unsupported potential. */
+EXPORT int oracle_integrate(int planar, int nobj, double *yo, int nt, const double *t,
+                            int indiv_t, int npot, const int *pot_type, const double *pot_args,
+                            double dt, double rtol, double atol, double *result, int *err,
+                            int method, long long *nsteps, long long *nforce,
+                            long long max_attempts, int nthreads)
+{
+  opot P0;
+  if (opot_decode(&P0, npot, pot_type, pot_args, planar)) return -3;
+  if (method != 0 && method != 1 && method != 3 && method != 6) return -2;
+  int nv = planar ? 4 : 6;
+  int bad = 0;
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+#endif
+  for (int ii = 0; ii < nobj; ii++) {
+    opot P = P0;
+    ostat st = {0, max_attempts, 0};
+    double *w = yo + (long)nv * ii;
+    if (planar)
+      polar_to_rect(w);
+    else
+      cyl_to_rect(w);
+    double *out = result + (long)nv * nt * ii;
+    if (run_plain(&P, planar, method, w, nt, t + (long)nt * ii * indiv_t, dt, rtol, atol, out,
+                  &st))
+      bad = 1;
+    for (int jj = 0; jj < nt; jj++) {
+      if (planar)
+        rect_to_polar(out + nv * jj);
+      else
+        rect_to_cyl(out + nv * jj);
+    }
+    err[ii] = st.err;
+    if (nsteps) nsteps[ii] = st.nsteps;
+    if (nforce) nforce[ii] = P.nforce;
+  }
+  return bad ? -2 : 0;
+}
+
+/* Variational integration of nobj orbits, each with one deviation column,
+   in rectangular coordinates (integrateFullOrbit.c:1234 /
+   integratePlanarOrbit.c:940 per orbit).  yo: [nobj][4*dim] =
+   (x..., v..., dx..., dv...); result [nobj][nt][4*dim]. */
+EXPORT int oracle_integrate_dxdv(int planar, int nobj, const double *yo, int nt, const double *t,
+                                 int indiv_t, int npot, const int *pot_type,
+                                 const double *pot_args, double dt, double rtol, double atol,
+                                 double *result, int *err, int method, long long *nsteps,
+                                 int nthreads)
+{
+  opot P0;
+  if (opot_decode(&P0, npot, pot_type, pot_args, planar)) return -3;
+  if (method != 0 && method != 1 && method != 3 && method != 6) return -2;
+  int dim = planar ? 2 : 3, nv = 4 * dim;
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+#endif
+  for (int ii = 0; ii < nobj; ii++) {
+    opot P = P0;
+    ostat st = {0, 0, 0};
+    const double *w = yo + (long)nv * ii;
+    const double *tt = t + (long)nt * ii * indiv_t;
+    double *out = result + (long)nv * nt * ii;
+    rhs_fn fa = planar ? rect_force2_dxdv : rect_force3_dxdv;
+    rhs_fn fb = planar ? rect_force2 : rect_force3;
+    rhs_fn fd = planar ? rect_deriv2_dxdv : rect_deriv3_dxdv;
+    switch (method) {
+    case 0: symplectic(0, fa, fb, &P, 2 * dim, dim, w, nt, dt, tt, rtol, atol, out, &st); break;
+    case 3: symplectic(1, fa, fb, &P, 2 * dim, dim, w, nt, dt, tt, rtol, atol, out, &st); break;
+    case 1: rk4(fd, &P, nv, w, nt, dt, tt, rtol, atol, out, &st); break;
+    case 6: dop853(fd, &P, nv, w, nt, tt, rtol, atol, out, &st); break;
+    }
+    err[ii] = st.err;
+    if (nsteps) nsteps[ii] = st.nsteps;
+  }
+  return 0;
+}
+
+/* Forces and Hessian terms at n points (R, z, phi), for unit tests.
+   out[n][9] = Rforce, zforce, phitorque, R2deriv, z2deriv, Rzderiv,
+   phi2deriv, Rphideriv, zphideriv; planar: out[n][5] = planarRforce,
+   planarphitorque, planarR2deriv, planarphi2deriv, planarRphideriv. */
+EXPORT int oracle_forces(int planar, int n, const double *R, const double *z, const double *phi,
+                         int npot, const int *pot_type, const double *pot_args, double *out)
+{
+  opot P;
+  if (opot_decode(&P, npot, pot_type, pot_args, planar)) return -3;
+  for (int i = 0; i < n; i++) {
+    if (planar) {
+      double Rf, pt, h0, h1, h2;
+      sum2(&P, R[i], phi[i], &Rf, &pt);
+      planar_hess_sum(&P, R[i], phi[i], &h0, &h1, &h2);
+      double *o = out + 5L * i;
+      o[0] = Rf;
+      o[1] = pt;
+      o[2] = h0;
+      o[3] = h1;
+      o[4] = h2;
+    } else {
+      double Rf, zf, pt, h[6];
+      sum3(&P, R[i], z[i], phi[i], &Rf, &zf, &pt);
+      hess3(&P, R[i], z[i], phi[i], h);
+      double *o = out + 9L * i;
+      o[0] = Rf;
+      o[1] = zf;
+      o[2] = pt;
+      for (int w = 0; w < 6; w++) o[3 + w] = h[w];
+    }
+  }
+  return 0;
+}
+
+/* Potential energy per unit mass, summed over components (evaluatePotentials,
+   galpy_potentials.c:105-117). */
+EXPORT int oracle_potential(int n, const double *R, const double *z, const double *phi, int npot,
+                            const int *pot_type, const double *pot_args, double *out)
+{
+  opot P;
+  if (opot_decode(&P, npot, pot_type, pot_args, 0)) return -3;
+  for (int i = 0; i < n; i++) {
+    double s = 0.;
+    for (int k = 0; k < P.n; k++) s += comp_eval(&P.c[k], R[i], z[i], phi[i]);
+    out[i] = s;
+  }
+  return 0;
+}
+
+EXPORT double oracle_gammainc_P(double a, double x) { return oracle_gamma_inc_P(a, x); }
