@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Throughput of the batched orbit integrator: orbit-steps/s.
+
+Workload (the batching configuration): 1,048,576 orbits per GPU in
+MWPotential2014, DOP853 with rtol = atol = 1e-10, float64 state.  Initial
+conditions from a seeded generator: R log-uniform in [0.05, 3], vR ~ N(0,
+0.1), vT ~ 1 + N(0, 0.1), z ~ N(0, 0.05), vz ~ N(0, 0.05), phi ~ U(0, 2 pi);
+every orbit has its own end time t_end ~ LogNormal(ln 50, 0.7) and keeps 101
+snapshots (SoA float64 on the device).  One "step" is one integration of the
+whole batch; an orbit-step is one accepted DOP853 step of one orbit.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl galpy_b200|reference]
+
+value: device-resident inputs, K launches timed with CUDA events on the
+launching stream (max over ranks).  e2e: the same batch through the
+galpy-facing C ABI (integrateFullOrbit_cuda) from pinned host buffers,
+host<->device copies inside the timed region.  cpu_baseline / the reference
+arm: the reference's own C integrators (oracle/_ref, built from the
+reference's sources) -- or, where that build is absent, the CPU oracle -- on
+a bounded sample of the same workload on all host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+
+N_ORBITS = 1 << 20
+NT = 101
+RTOL = ATOL = 1e-10
+F_STEP_DOP853 = 6500.0  # nominal float64 flops per accepted DOP853 step (MWPotential2014)
+METRIC = "orbit-steps/s (MWPotential2014, dop853 rtol=atol=1e-10, ragged t_end, 1 B200)"
+WORKLOAD = ("batching: 1,048,576 orbits/GPU in MWPotential2014, dop853 rtol=atol=1e-10, "
+            "R log-uniform [0.05,3], t_end ~ LogNormal(ln 50, 0.7) per orbit, 101 snapshots "
+            "SoA float64")
+
+
+def workload(n, seed):
+    rng = np.random.default_rng(seed)
+    R = np.exp(rng.uniform(np.log(0.05), np.log(3.0), n))
+    vR = rng.normal(0, 0.1, n)
+    vT = 1 + rng.normal(0, 0.1, n)
+    z = rng.normal(0, 0.05, n)
+    vz = rng.normal(0, 0.05, n)
+    phi = rng.uniform(0, 2 * np.pi, n)
+    tend = np.exp(rng.normal(np.log(50.0), 0.7, n))
+    ics = np.stack([R, vR, vT, z, vz, phi], 1)
+    t = np.linspace(0.0, 1.0, NT)[None, :] * tend[:, None]
+    return ics, t
+
+
+def mw14_args():
+    import galpy_b200 as gb
+
+    _, pt, pa = gb.parse_pot(gb.MWPotential2014())
+    return pt, pa
+
+
+def cyl_to_rect(v):
+    R, vR, vT, z, vz, phi = v.T
+    c, s = np.cos(phi), np.sin(phi)
+    return np.stack([R * c, R * s, z, vR * c - vT * s, vR * s + vT * c, vz], 1)
+
+
+# ---------------------------------------------------------------- clocks --
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.dev)], stdout=open(self.path, "w"),
+                stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        loaded = [s for s in sm if s > 0.5 * smax] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows
+                                                         if r[3].replace(".", "").isdigit())}
+
+
+# ----------------------------------------------------------- CPU baseline --
+def cpu_reference_rate(ics, t, pt, pa, target_s=10.0, min_orbits=512):
+    """orbit-steps/s of the reference's C (oracle/_ref) or the oracle, all cores."""
+    from oracle import oracle as O
+
+    kind = "reference" if O.ref_available() else "port"
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    n = min_orbits
+    rng = np.random.default_rng(123)
+    while True:
+        idx = rng.choice(len(ics), size=min(n, len(ics)), replace=False)
+        sub_ics, sub_t = ics[idx], t[idx]
+        t0 = time.perf_counter()
+        O.integrate(sub_ics, sub_t, pt, pa, "dop853", rtol=RTOL, atol=ATOL, impl=("ref" if kind ==
+                                                                                  "reference" else "port"),
+                    nthreads=cores)
+        el = time.perf_counter() - t0
+        if el >= 0.4 * target_s or n >= len(ics):
+            break
+        n = int(n * min(8.0, max(2.0, 0.5 * target_s / max(el, 1e-3))))
+    # accepted steps of the same sample (the oracle is bit-identical to the
+    # reference's C, so its counts are the reference's)
+    _, _, ns, _ = O.integrate(sub_ics, sub_t, pt, pa, "dop853", rtol=RTOL, atol=ATOL,
+                              nthreads=cores)
+    steps = int(ns.sum())
+    return {"value": steps / el, "unit": "orbit-steps/s", "cores": cores, "kind": kind,
+            "sample": f"{len(idx)} random orbits of the workload ({steps} accepted steps, "
+                      f"{el:.1f} s), OMP threads = {cores}"}
+
+
+# ------------------------------------------------------------------ main --
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="galpy_b200", choices=["galpy_b200", "reference"])
+    ap.add_argument("--orbits", type=int, default=N_ORBITS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+
+    import torch
+
+    from galpy_b200 import _lib
+    from galpy_b200 import build as gbuild
+    import galpy_b200 as gb
+
+    gbuild.build()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=dev)
+        pg = dist
+
+    pt, pa = mw14_args()
+    ics, t = workload(args.orbits, seed=1 + 1000 * rank)
+    n = len(ics)
+    comps, ncomp = gb.compile_potential((pt, pa))
+    comps_d = torch.tensor(comps, device=dev)
+    w0 = torch.tensor(cyl_to_rect(ics).T.copy(), device=dev)
+    t_d = torch.tensor(t, device=dev)
+    out = torch.empty((6, NT, n), dtype=torch.float64, device=dev)
+    err = torch.empty(n, dtype=torch.int32, device=dev)
+    nsteps = torch.empty(n, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def run(precision="fp64"):
+        gb.integrate_device(comps_d, ncomp, w0, t_d, out, err, "dop853_cuda", nsteps=nsteps,
+                            rtol=RTOL, atol=ATOL, precision=precision, stream=stream)
+
+    def timed(precision, K, W):
+        for _ in range(W):
+            run(precision)
+        torch.cuda.synchronize()
+        steps = int(nsteps.sum().item())
+        nbad = int((err != 0).sum().item())
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(K):
+            run(precision)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if pg:
+            pg.barrier()
+        tot = torch.tensor([ms, float(steps), float(nbad)], dtype=torch.float64, device=dev)
+        if pg:
+            mx = tot.clone()
+            pg.all_reduce(mx, op=pg.ReduceOp.MAX)
+            sm = tot.clone()
+            pg.all_reduce(sm, op=pg.ReduceOp.SUM)
+            ms, steps, nbad = mx[0].item(), sm[1].item(), sm[2].item()
+        return ms, steps, nbad
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms, steps, nbad = timed("fp64", args.steps, args.warmup)
+    clk = clocks.stop()
+    value = steps * args.steps / (ms * 1e-3)
+
+    peak = ctypes_fp64_peak(_lib)
+    achieved = value / world * F_STEP_DOP853 / 1e12  # per GPU
+    result = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "orbit-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded initial conditions of the batching configuration)",
+        "config": {"workload": WORKLOAD, "orbits_per_gpu": n, "snapshots": NT,
+                   "accepted_steps_per_gpu_step": steps / world,
+                   "orbits_with_err": nbad,
+                   "l2": "no flush: inputs (0.85 GB times) and outputs (5.1 GB snapshots) "
+                         "exceed the 126 MB L2"},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                     "traffic": None,
+                     "kernel": "orbit_kernel<Dop853Machine<3,false>,3,0,false>",
+                     "flops_per_unit": F_STEP_DOP853,
+                     "peak_source": "measured in-process: float64 FMA-chain kernel "
+                                    "(galpy_cuda_fp64_peak); MEASURED_PEAKS.json has no FP64 "
+                                    "figure"},
+        "clocks": clk,
+        "gpu_launches": args.steps,
+    }
+
+    if not args.no_mixed:
+        ms32, steps32, nbad32 = timed("f32force", max(1, args.steps), 1)
+        result["mixed"] = {"precision": "f32force (float32 forces, float64 state)",
+                           "value": steps32 * max(1, args.steps) / (ms32 * 1e-3),
+                           "accepted_steps": steps32, "orbits_with_err": nbad32,
+                           "speedup_vs_fp64": (steps32 / ms32) / (steps / ms)}
+
+    if not args.no_e2e:
+        result["e2e"] = e2e(gb, ics, t, pt, pa, args.steps, pg, dev, steps)
+        result["gpu_launches"] += args.steps
+
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            result["cpu_baseline"] = cpu_reference_rate(ics, t, pt, pa)
+        except Exception as exc:  # report, do not hide
+            result["cpu_baseline"] = {"value": None, "error": repr(exc)}
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+def e2e(gb, ics, t, pt, pa, K, pg, dev, steps_total):
+    """The galpy-facing C ABI from pinned host memory (copies timed)."""
+    import torch
+
+    n = len(ics)
+    yo_pin = torch.empty((n, 6), dtype=torch.float64, pin_memory=True).numpy()
+    t_pin = torch.empty(t.shape, dtype=torch.float64, pin_memory=True).numpy()
+    res_pin = torch.empty((n, NT, 6), dtype=torch.float64, pin_memory=True).numpy()
+    t_pin[:] = t
+    import ctypes
+
+    from galpy_b200 import _lib
+
+    L = _lib.lib()
+    dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    err = np.zeros(n, np.int32)
+    pti = np.ascontiguousarray(pt, np.int32)
+    pad = np.ascontiguousarray(pa, np.float64)
+    r, a = float(np.log(RTOL)), float(np.log(ATOL))
+    opts = _lib.make_opts(device=dev.index)
+    times = []
+    for k in range(K + 1):
+        yo_pin[:] = ics  # galpy's call overwrites yo with rectangular coordinates
+        if pg:
+            pg.barrier()
+        t0 = time.perf_counter()
+        rc = L.integrateFullOrbit_cuda(n, yo_pin.ctypes.data_as(dp), NT, t_pin.ctypes.data_as(dp),
+                                       1, len(pti), pti.ctypes.data_as(ip), pad.ctypes.data_as(dp),
+                                       None, -9999.99, r, a, res_pin.ctypes.data_as(dp),
+                                       err.ctypes.data_as(ip), 6, _lib.CALLBACK(),
+                                       ctypes.byref(opts))
+        el = time.perf_counter() - t0
+        _lib.check(rc)
+        if k > 0:  # first call is a warm-up
+            times.append(el)
+    el = max(times)
+    if pg:
+        x = torch.tensor([el], dtype=torch.float64, device=dev)
+        pg.all_reduce(x, op=pg.ReduceOp.MAX)
+        el = x.item()
+    return {"value": steps_total / el, "unit": "orbit-steps/s", "seconds_per_step": el,
+            "h2d_bytes_per_step": int(yo_pin.nbytes + t_pin.nbytes),
+            "d2h_bytes_per_step": int(res_pin.nbytes + err.nbytes),
+            "api": "integrateFullOrbit_cuda (galpy layout, pinned host buffers)"}
+
+
+def ctypes_fp64_peak(_lib):
+    import ctypes
+
+    tf, ms = ctypes.c_double(0), ctypes.c_double(0)
+    rc = _lib.lib().galpy_cuda_fp64_peak(ctypes.byref(tf), ctypes.byref(ms))
+    return tf.value if rc == 0 else None
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    pt, pa = mw14_args()
+    ics, t = workload(args.orbits, seed=1)
+    vals = []
+    base = None
+    for k in range(args.warmup + args.steps):
+        b = cpu_reference_rate(ics, t, pt, pa, target_s=10.0)
+        if k >= args.warmup:
+            vals.append(b["value"])
+            base = b
+    value = statistics.mean(vals)
+    base = dict(base)
+    base["value"] = value
+    print(json.dumps({
+        "metric": METRIC, "impl": "reference", "value": value, "unit": "orbit-steps/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded initial conditions of the batching configuration)",
+        "config": {"workload": WORKLOAD, "orbits_per_gpu": args.orbits, "snapshots": NT},
+        "cpu_baseline": base,
+        "e2e": {"value": value, "unit": "orbit-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+if __name__ == "__main__":
+    main()

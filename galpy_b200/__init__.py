@@ -1,0 +1,24 @@
+"""galpy_b200 -- B200-native batched orbit integration for galpy.
+
+The engine (libgalpy_cuda.so, built from galpy_b200/csrc for sm_100a) runs
+galpy's leapfrog, symplec4, rk4 and dop853 integrators -- plain and
+variational (dxdv) -- in MWPotential2014-type potentials on the GPU.  Its
+galpy-facing entry points mirror galpy's own C wrappers
+(galpy/orbit/integrateFullOrbit.py, integratePlanarOrbit.py); ``galpy_hooks``
+plugs them into ``galpy.orbit.Orbit.integrate`` as the methods
+'leapfrog_cuda', 'rk4_cuda', 'symplec4_cuda' and 'dop853_cuda'.
+
+There is no CPU fallback: calls raise CudaLibraryMissing when the library is
+not built and CudaError when no GPU is available.
+"""
+from ._lib import (CudaError, CudaLibraryMissing, MethodNotSupported,  # noqa: F401
+                   PotentialNotSupported)
+from .integrate import (CUDA_METHODS, compile_potential, integrate_device,  # noqa: F401
+                        integrate_dxdv_batch, integrateFullOrbit_cuda,
+                        integrateFullOrbit_dxdv_cuda, integratePlanarOrbit_cuda,
+                        integratePlanarOrbit_dxdv_cuda, parse_integrator, parse_tol)
+from .potentials import (HernquistPotential, LogarithmicHaloPotential,  # noqa: F401
+                         MiyamotoNagaiPotential, MWPotential2014, NFWPotential,
+                         PowerSphericalPotentialwCutoff, parse_pot)
+
+__version__ = "0.1.0"

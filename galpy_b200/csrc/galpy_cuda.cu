@@ -1,0 +1,650 @@
+// galpy_b200/csrc/galpy_cuda.cu
+//
+// libgalpy_cuda.so: batched orbit integration on sm_100a behind the C ABI of
+// include/galpy_cuda.h.
+//
+// Execution model
+//   * One thread integrates one orbit at a time in float64 state.  Threads
+//     pull orbit indices from a device work counter (work stealing) until the
+//     batch is exhausted, so orbits with very different step counts (inner
+//     vs outer orbits, ragged integration times, adaptive DOP853) keep every
+//     lane busy instead of leaving warps waiting for their slowest orbit.
+//   * The kernel is persistent: one wave of blocks sized from the occupancy
+//     of the instantiated kernel on this device's SMs.
+//   * Every loop iteration of a thread performs exactly one force evaluation
+//     (machines.cuh), so all lanes of a warp meet at a single inlined force
+//     call whatever stage of whatever orbit they are in.
+//   * Potential parameters are compiled on the host into per-component
+//     records (compile_potential.h) read through the read-only cache; a batch
+//     may hold many parameter groups (ragged multi-potential runs).
+//   * Output rows are written directly in the requested layout: galpy's AoS
+//     cylindrical rows for the drop-in entry points, or coalesced SoA rows
+//     for device-resident batch use.
+#include <cuda_runtime.h>
+#include <signal.h>
+#include <stdio.h>
+#include <string.h>
+#include <time.h>
+
+#include <atomic>
+#include <string>
+#include <vector>
+
+#include "../../include/galpy_cuda.h"
+#include "compile_potential.h"
+#include "machines.cuh"
+
+using namespace gpc;
+
+// ----------------------------------------------------------------------------
+// error reporting
+// ----------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+
+static int set_error(int code, const std::string& msg)
+{
+  g_last_error = msg;
+  return code;
+}
+
+#define GPC_CUDA_TRY(expr)                                                              \
+  do {                                                                                  \
+    cudaError_t e_ = (expr);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return set_error(GALPY_CUDA_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+// ----------------------------------------------------------------------------
+// kernel
+// ----------------------------------------------------------------------------
+struct KArgs {
+  long long nobj;
+  int nt, indiv_t;
+  const double* t;
+  const double* w0;
+  int in_layout;
+  OutSpec out;
+  int* err;
+  long long* nsteps;
+  const GpComp* comps;
+  int ncomp;
+  const int* group;
+  double dt, rtol, atol;
+  long long max_attempts;
+  unsigned long long* counter;
+  const int* abort_flag;
+  unsigned long long* done_count;
+};
+
+template <int NV, int D, bool CYL_OK>
+struct DevRows {
+  const OutSpec* o;
+  long long i;
+  __device__ __forceinline__ void operator()(int j, const double* v) const
+  {
+    write_row<NV, D, CYL_OK>(*o, i, j, v);
+  }
+};
+
+template <class M>
+__device__ __forceinline__ void load_state(const KArgs& A, long long i, double* w)
+{
+  if (A.in_layout == GALPY_CUDA_IN_SOA) {
+#pragma unroll
+    for (int k = 0; k < M::NV; k++) w[k] = A.w0[(long long)k * A.nobj + i];
+  } else {
+#pragma unroll
+    for (int k = 0; k < M::NV; k++) w[k] = A.w0[i * M::NV + k];
+  }
+}
+
+template <class M, int D, int PREC, bool VAR>
+__global__ void __launch_bounds__(128) orbit_kernel(const KArgs A)
+{
+  constexpr bool CYL_OK = !VAR;
+  using Rows = DevRows<M::NV, D, CYL_OK>;
+  extern __shared__ double slot_store[];
+  M m;
+  m.bind(slot_store + threadIdx.x, blockDim.x);
+  long long i = 0;
+  bool active = false, aborting = false;
+  const GpComp* comps = A.comps;
+  unsigned iter = 0;
+  for (;;) {
+    if (!active) {
+      i = (long long)atomicAdd(A.counter, 1ULL);
+      if (i >= A.nobj) break;
+      if (aborting) {
+        A.err[i] = E_ABORT;
+        write_nan_rows<M::NV, D, CYL_OK>(A.out, i, 0);
+        continue;
+      }
+      double w[M::NV];
+      load_state<M>(A, i, w);
+      comps = A.comps + (A.group ? (long long)A.group[i] * A.ncomp : 0LL);
+      Rows rows{&A.out, i};
+      m.init(w, A.t + (A.indiv_t ? i * (long long)A.nt : 0LL), A.nt, A.dt, A.rtol, A.atol,
+             A.max_attempts, rows);
+      active = true;
+    }
+    if (!m.done) {
+      double y[M::NY], q[M::NA], a[M::NA];
+      m.point(y);
+      M::pos(y, q);
+      eval_force<D, PREC, VAR>(comps, A.ncomp, q, a);
+      Rows rows{&A.out, i};
+      m.consume(y, a, rows);
+    }
+    if (A.abort_flag && ((++iter & 255u) == 0u) &&
+        *reinterpret_cast<const volatile int*>(A.abort_flag)) {
+      aborting = true;
+      if (!m.done) {
+        m.err = E_ABORT;
+        m.done = true;
+      }
+    }
+    if (m.done) {
+      Rows rows{&A.out, i};
+      fill_unreached_rows(m, rows);
+      A.err[i] = m.err;
+      if (A.nsteps) A.nsteps[i] = m.nsteps;
+      if (A.done_count) atomicAdd(A.done_count, 1ULL);
+      active = false;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// launch plumbing
+// ----------------------------------------------------------------------------
+using KernelFn = void (*)(const KArgs);
+
+struct KernelInfo {
+  KernelFn fn = nullptr;
+  int slot_doubles = 0;  // per-thread shared-memory slot store (doubles)
+};
+
+template <class M, int D, int PREC, bool VAR>
+static KernelInfo info_of()
+{
+  KernelInfo k;
+  k.fn = orbit_kernel<M, D, PREC, VAR>;
+  k.slot_doubles = M::kSlotDoubles;
+  return k;
+}
+
+template <int D, int PREC, bool VAR>
+static KernelInfo pick_kernel_dim(int method)
+{
+  switch (method) {
+    case M_LEAPFROG: return info_of<SymplecticMachine<D, VAR, false>, D, PREC, VAR>();
+    case M_SYMPLEC4: return info_of<SymplecticMachine<D, VAR, true>, D, PREC, VAR>();
+    case M_RK4: return info_of<RK4Machine<D, VAR>, D, PREC, VAR>();
+    case M_DOP853: return info_of<Dop853Machine<D, VAR>, D, PREC, VAR>();
+  }
+  return KernelInfo();
+}
+
+static KernelInfo pick_kernel(int planar, int var, int prec, int method)
+{
+  if (var) {
+    if (prec != GALPY_CUDA_FP64) return KernelInfo();  // variational runs are float64 only
+    return planar ? pick_kernel_dim<2, PREC_FP64, true>(method)
+                  : pick_kernel_dim<3, PREC_FP64, true>(method);
+  }
+  if (prec == GALPY_CUDA_F32FORCE)
+    return planar ? pick_kernel_dim<2, PREC_F32, false>(method)
+                  : pick_kernel_dim<3, PREC_F32, false>(method);
+  return planar ? pick_kernel_dim<2, PREC_FP64, false>(method)
+                : pick_kernel_dim<3, PREC_FP64, false>(method);
+}
+
+static bool method_supported(int m)
+{
+  return m == M_LEAPFROG || m == M_RK4 || m == M_SYMPLEC4 || m == M_DOP853;
+}
+
+struct Scratch {  // device scratch of one launch (64 bytes)
+  unsigned long long counter;
+  unsigned long long done_count;
+  int abort_flag;
+  int pad[11];
+};
+
+// Launch on `stream`.  scratch: device Scratch (counter zeroed here).
+static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool progress,
+                         cudaStream_t stream)
+{
+  const KernelInfo ki = pick_kernel(L->planar, L->variational, L->precision, L->odeint_type);
+  KernelFn fn = ki.fn;
+  if (!fn) return set_error(GALPY_CUDA_ERR_METHOD, "method/precision combination not implemented");
+  KArgs A;
+  memset(&A, 0, sizeof(A));
+  A.nobj = L->nobj;
+  A.nt = L->nt;
+  A.indiv_t = L->indiv_t;
+  A.t = L->t;
+  A.w0 = L->w0;
+  A.in_layout = L->in_layout;
+  A.out.out = L->out;
+  A.out.layout = L->out_layout;
+  A.out.nt = L->nt;
+  A.out.row0 = L->out_row0;
+  A.out.nobj = L->nobj;
+  A.err = L->err;
+  A.nsteps = L->nsteps;
+  A.comps = static_cast<const GpComp*>(L->comps);
+  A.ncomp = L->ncomp;
+  A.group = L->group;
+  A.dt = L->dt;
+  A.rtol = L->rtol;
+  A.atol = L->atol;
+  A.max_attempts = L->max_attempts;
+  A.counter = &scratch->counter;
+  A.abort_flag = L->abort_flag ? L->abort_flag : &scratch->abort_flag;
+  A.done_count = progress ? &scratch->done_count : nullptr;
+  GPC_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(Scratch), stream));
+
+  int dev = 0;
+  GPC_CUDA_TRY(cudaGetDevice(&dev));
+  int nsm = 0;
+  GPC_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int block = L->block_size > 0 ? L->block_size : 128;
+  if (block > 128 || block % 32) return set_error(GALPY_CUDA_ERR_ARG, "block_size must be 32..128, multiple of 32");
+  const size_t smem = (size_t)ki.slot_doubles * sizeof(double) * block;
+  if (smem > 48 * 1024)
+    GPC_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  GPC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem));
+  if (per_sm < 1) per_sm = 1;
+  long long grid = L->grid_size > 0 ? L->grid_size : (long long)nsm * per_sm;
+  const long long need = (L->nobj + block - 1) / block;
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
+  fn<<<(unsigned)grid, block, smem, stream>>>(A);
+  GPC_CUDA_TRY(cudaGetLastError());
+  return GALPY_CUDA_OK;
+}
+
+static int check_launch(const galpy_cuda_launch* L)
+{
+  if (!L) return set_error(GALPY_CUDA_ERR_ARG, "launch is NULL");
+  if (!method_supported(L->odeint_type))
+    return set_error(GALPY_CUDA_ERR_METHOD, "odeint_type not implemented on the GPU");
+  if (L->nobj < 0 || L->nt < 1 || !L->t || !L->w0 || !L->out || !L->err || !L->comps ||
+      L->ncomp < 1 || L->ncomp > kMaxComp || L->out_row0 < 0 || L->out_row0 >= L->nt)
+    return set_error(GALPY_CUDA_ERR_ARG, "invalid launch arguments");
+  if (L->precision != GALPY_CUDA_FP64 && L->precision != GALPY_CUDA_F32FORCE)
+    return set_error(GALPY_CUDA_ERR_ARG, "unknown precision");
+  return GALPY_CUDA_OK;
+}
+
+// ----------------------------------------------------------------------------
+// SIGINT handling of the galpy-facing blocking calls (the reference polls a
+// process-global flag set by its handler, bovy_symplecticode.c:38-45)
+// ----------------------------------------------------------------------------
+static volatile sig_atomic_t g_sigint = 0;
+static void on_sigint(int) { g_sigint = 1; }
+
+struct SigintGuard {
+  struct sigaction old_action;
+  bool installed = false;
+  SigintGuard()
+  {
+    struct sigaction a;
+    memset(&a, 0, sizeof(a));
+    a.sa_handler = on_sigint;
+    g_sigint = 0;
+    installed = sigaction(SIGINT, &a, &old_action) == 0;
+  }
+  ~SigintGuard()
+  {
+    if (installed) sigaction(SIGINT, &old_action, nullptr);
+  }
+};
+
+// RAII device buffers for the host-pointer entry points
+struct DevBuf {
+  void* p = nullptr;
+  cudaStream_t s = nullptr;
+  ~DevBuf()
+  {
+    if (p) cudaFreeAsync(p, s);
+  }
+};
+
+static int select_device(const galpy_cuda_opts* o)
+{
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1)
+    return set_error(GALPY_CUDA_ERR_NODEVICE, "no CUDA device visible");
+  if (o && o->device >= 0) GPC_CUDA_TRY(cudaSetDevice(o->device));
+  return GALPY_CUDA_OK;
+}
+
+// Blocking host-pointer integration shared by the galpy-facing entry points.
+// w: rectangular initial states [nobj][nv]; result written in galpy's layout
+// (cylindrical rows) unless rect_out.
+static int run_host(int planar, int var, long long nobj, const double* w, int nv, int nt,
+                    const double* t, int indiv_t, int npot, const int* pot_type,
+                    const double* pot_args, double dt, double rtol, double atol, double* result,
+                    int* err, int odeint_type, galpy_cuda_callback cb, const galpy_cuda_opts* o,
+                    bool rect_out)
+{
+  int rc = select_device(o);
+  if (rc) return rc;
+  if (!method_supported(odeint_type))
+    return set_error(GALPY_CUDA_ERR_METHOD, "odeint_type not implemented on the GPU");
+  if (nobj == 0) return GALPY_CUDA_OK;
+  std::vector<GpComp> comps(npot > 0 ? npot : 1);
+  rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
+  if (rc == -3) return set_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
+  if (rc) return set_error(GALPY_CUDA_ERR_ARG, "invalid potential arguments");
+
+  cudaStream_t stream, side;
+  GPC_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  GPC_CUDA_TRY(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t a, b;
+    ~StreamGuard()
+    {
+      cudaStreamSynchronize(a);
+      cudaStreamDestroy(a);
+      cudaStreamDestroy(b);
+    }
+  } sg{stream, side};
+
+  const size_t n_w = (size_t)nobj * nv, n_t = (size_t)(indiv_t ? nobj : 1) * nt;
+  const size_t n_out = (size_t)nobj * nt * nv;
+  DevBuf dw, dt_, dout, derr, dsteps, dcomp, dscr;
+  dw.s = dt_.s = dout.s = derr.s = dsteps.s = dcomp.s = dscr.s = stream;
+  GPC_CUDA_TRY(cudaMallocAsync(&dw.p, n_w * sizeof(double), stream));
+  GPC_CUDA_TRY(cudaMallocAsync(&dt_.p, n_t * sizeof(double), stream));
+  GPC_CUDA_TRY(cudaMallocAsync(&dout.p, n_out * sizeof(double), stream));
+  GPC_CUDA_TRY(cudaMallocAsync(&derr.p, (size_t)nobj * sizeof(int), stream));
+  GPC_CUDA_TRY(cudaMallocAsync(&dcomp.p, comps.size() * sizeof(GpComp), stream));
+  GPC_CUDA_TRY(cudaMallocAsync(&dscr.p, sizeof(Scratch), stream));
+  if (o && o->nsteps) GPC_CUDA_TRY(cudaMallocAsync(&dsteps.p, (size_t)nobj * sizeof(long long), stream));
+  GPC_CUDA_TRY(cudaMemcpyAsync(dw.p, w, n_w * sizeof(double), cudaMemcpyHostToDevice, stream));
+  GPC_CUDA_TRY(cudaMemcpyAsync(dt_.p, t, n_t * sizeof(double), cudaMemcpyHostToDevice, stream));
+  GPC_CUDA_TRY(cudaMemcpyAsync(dcomp.p, comps.data(), comps.size() * sizeof(GpComp),
+                               cudaMemcpyHostToDevice, stream));
+
+  galpy_cuda_launch L;
+  memset(&L, 0, sizeof(L));
+  L.planar = planar;
+  L.variational = var;
+  L.odeint_type = odeint_type;
+  L.precision = o ? o->precision : GALPY_CUDA_FP64;
+  L.nobj = nobj;
+  L.nt = nt;
+  L.indiv_t = indiv_t;
+  L.t = static_cast<double*>(dt_.p);
+  L.w0 = static_cast<double*>(dw.p);
+  L.in_layout = GALPY_CUDA_IN_AOS;
+  L.out = static_cast<double*>(dout.p);
+  L.out_layout = rect_out ? GALPY_CUDA_OUT_AOS_RECT : GALPY_CUDA_OUT_GALPY;
+  L.out_row0 = 0;
+  L.err = static_cast<int*>(derr.p);
+  L.nsteps = static_cast<long long*>(dsteps.p);
+  L.comps = dcomp.p;
+  L.ncomp = npot;
+  L.dt = dt;
+  L.rtol = rtol;
+  L.atol = atol;
+  L.max_attempts = o ? o->max_attempts : 0;
+  L.block_size = o ? o->block_size : 0;
+  rc = check_launch(&L);
+  if (rc) return rc;
+
+  Scratch* scr = static_cast<Scratch*>(dscr.p);
+  cudaEvent_t e0, e1;
+  GPC_CUDA_TRY(cudaEventCreate(&e0));
+  GPC_CUDA_TRY(cudaEventCreate(&e1));
+  struct EvGuard {
+    cudaEvent_t a, b;
+    ~EvGuard()
+    {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+  } eg{e0, e1};
+  SigintGuard sig;
+  GPC_CUDA_TRY(cudaEventRecord(e0, stream));
+  rc = launch_kernel(&L, scr, cb != nullptr, stream);
+  if (rc) return rc;
+  GPC_CUDA_TRY(cudaEventRecord(e1, stream));
+
+  // wait: poll completion, forward SIGINT to the device, drive the progress callback
+  unsigned long long reported = 0, *pinned_done = nullptr;
+  if (cb) GPC_CUDA_TRY(cudaMallocHost(&pinned_done, sizeof(unsigned long long)));
+  bool abort_sent = false;
+  for (;;) {
+    cudaError_t q = cudaEventQuery(e1);
+    if (q == cudaSuccess) break;
+    if (q != cudaErrorNotReady) {
+      if (pinned_done) cudaFreeHost(pinned_done);
+      return set_error(GALPY_CUDA_ERR_CUDA, std::string("integration kernel: ") + cudaGetErrorString(q));
+    }
+    if (g_sigint && !abort_sent) {
+      static const int one = 1;
+      cudaMemcpyAsync(&scr->abort_flag, &one, sizeof(int), cudaMemcpyHostToDevice, side);
+      abort_sent = true;
+    }
+    if (cb) {
+      cudaMemcpyAsync(pinned_done, &scr->done_count, sizeof(unsigned long long),
+                      cudaMemcpyDeviceToHost, side);
+      cudaStreamSynchronize(side);
+      for (; reported < *pinned_done; reported++) cb();
+    }
+    struct timespec ts = {0, 2000000};
+    nanosleep(&ts, nullptr);
+  }
+  if (cb) {
+    for (; reported < (unsigned long long)nobj; reported++) cb();
+    cudaFreeHost(pinned_done);
+  }
+  if (o && o->elapsed_ms) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    *o->elapsed_ms = ms;
+  }
+  GPC_CUDA_TRY(cudaMemcpyAsync(result, dout.p, n_out * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  GPC_CUDA_TRY(cudaMemcpyAsync(err, derr.p, (size_t)nobj * sizeof(int), cudaMemcpyDeviceToHost, stream));
+  if (o && o->nsteps)
+    GPC_CUDA_TRY(cudaMemcpyAsync(o->nsteps, dsteps.p, (size_t)nobj * sizeof(long long),
+                                 cudaMemcpyDeviceToHost, stream));
+  GPC_CUDA_TRY(cudaStreamSynchronize(stream));
+  if (abort_sent) return GALPY_CUDA_ERR_INTERRUPTED;
+  return GALPY_CUDA_OK;
+}
+
+// cylindrical -> rectangular initial conditions, in place, exactly as
+// cyl_to_rect_galpy / polar_to_rect_galpy (bovy_coords.c:57-124)
+static void cyl_to_rect_inplace(int planar, long long nobj, double* yo)
+{
+  for (long long i = 0; i < nobj; i++) {
+    double* v = yo + (planar ? 4 : 6) * i;
+    if (planar) {
+      const double R = v[0], phi = v[3], cp = cos(phi), sp = sin(phi), vR = v[1], vT = v[2];
+      v[0] = R * cp;
+      v[1] = R * sp;
+      v[2] = vR * cp - vT * sp;
+      v[3] = vR * sp + vT * cp;
+    } else {
+      const double R = v[0], phi = v[5], cp = cos(phi), sp = sin(phi), vR = v[1], vT = v[2];
+      v[0] = R * cp;
+      v[1] = R * sp;
+      v[2] = v[3];
+      v[5] = v[4];
+      v[3] = vR * cp - vT * sp;
+      v[4] = vR * sp + vT * cp;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------
+// FP64 pipe peak: independent fused multiply-add chains per thread
+// ----------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) fp64_fma_peak_kernel(double* sink, int iters, double mul)
+{
+  double a0 = 1e-3 * threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4,
+         a5 = a0 + 5, a6 = a0 + 6, a7 = a0 + 7;
+  const double add = 1e-9;
+  for (int i = 0; i < iters; i++) {
+    a0 = fma(a0, mul, add);
+    a1 = fma(a1, mul, add);
+    a2 = fma(a2, mul, add);
+    a3 = fma(a3, mul, add);
+    a4 = fma(a4, mul, add);
+    a5 = fma(a5, mul, add);
+    a6 = fma(a6, mul, add);
+    a7 = fma(a7, mul, add);
+  }
+  const double s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (s == 12345.678) sink[threadIdx.x] = s;  // keeps the chains alive
+}
+
+// ----------------------------------------------------------------------------
+// exported C ABI
+// ----------------------------------------------------------------------------
+extern "C" {
+
+int galpy_cuda_fp64_peak(double* tflops, double* ms)
+{
+  int dev = 0, nsm = 0;
+  GPC_CUDA_TRY(cudaGetDevice(&dev));
+  GPC_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  double* sink = nullptr;
+  GPC_CUDA_TRY(cudaMalloc(&sink, 256 * sizeof(double)));
+  const int blocks = nsm * 8, threads = 256, iters = 1 << 16;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; rep++) {
+    cudaEventRecord(e0);
+    fp64_fma_peak_kernel<<<blocks, threads>>>(sink, iters, 0.9999999);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    if (rep > 0 && t < best) best = t;
+  }
+  cudaError_t e = cudaGetLastError();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  if (e != cudaSuccess) return set_error(GALPY_CUDA_ERR_CUDA, cudaGetErrorString(e));
+  const double flops = 2.0 * 8.0 * iters * (double)blocks * threads;
+  if (tflops) *tflops = flops / (best * 1e-3) / 1e12;
+  if (ms) *ms = best;
+  return GALPY_CUDA_OK;
+}
+
+int galpy_cuda_abi_version(void) { return GALPY_CUDA_ABI_VERSION; }
+
+const char* galpy_cuda_last_error(void) { return g_last_error.c_str(); }
+
+int galpy_cuda_device_count(void)
+{
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+int galpy_cuda_comp_size(void) { return (int)sizeof(GpComp); }
+
+int galpy_cuda_compile_potential(int planar, int npot, const int* pot_type,
+                                 const double* pot_args, int ngroup, void* out)
+{
+  if (!pot_type || !pot_args || !out || ngroup < 1)
+    return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
+  GpComp* c = static_cast<GpComp*>(out);
+  const double* p = pot_args;
+  for (int g = 0; g < ngroup; g++) {
+    int used = 0;
+    int rc = compile_group(planar, npot, pot_type, p, c + (size_t)g * npot, &used);
+    if (rc == -3) return set_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
+    if (rc) return set_error(GALPY_CUDA_ERR_ARG, "invalid potential arguments");
+    p += used;
+  }
+  return GALPY_CUDA_OK;
+}
+
+int galpy_cuda_integrate_device(const galpy_cuda_launch* L)
+{
+  int rc = check_launch(L);
+  if (rc) return rc;
+  if (L->nobj == 0) return GALPY_CUDA_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(L->stream);
+  Scratch* scr = nullptr;
+  GPC_CUDA_TRY(cudaMallocAsync((void**)&scr, sizeof(Scratch), s));
+  rc = launch_kernel(L, scr, false, s);
+  cudaFreeAsync(scr, s);
+  return rc;
+}
+
+int integrateFullOrbit_cuda(int nobj, double* yo, int nt, double* t, int indiv_t, int npot,
+                            int* pot_type, double* pot_args, void* /*pot_tfuncs*/, double dt,
+                            double rtol, double atol, double* result, int* err, int odeint_type,
+                            galpy_cuda_callback cb, const galpy_cuda_opts* opts)
+{
+  if (nobj < 0 || nt < 1 || (nobj && (!yo || !t || !result || !err)) || !pot_type || !pot_args)
+    return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
+  if (!method_supported(odeint_type))
+    return set_error(GALPY_CUDA_ERR_METHOD, "odeint_type not implemented on the GPU");
+  cyl_to_rect_inplace(0, nobj, yo);
+  return run_host(0, 0, nobj, yo, 6, nt, t, indiv_t, npot, pot_type, pot_args, dt, rtol, atol,
+                  result, err, odeint_type, cb, opts, false);
+}
+
+int integratePlanarOrbit_cuda(int nobj, double* yo, int nt, double* t, int indiv_t, int npot,
+                              int* pot_type, double* pot_args, void* /*pot_tfuncs*/, double dt,
+                              double rtol, double atol, double* result, int* err,
+                              int odeint_type, galpy_cuda_callback cb,
+                              const galpy_cuda_opts* opts)
+{
+  if (nobj < 0 || nt < 1 || (nobj && (!yo || !t || !result || !err)) || !pot_type || !pot_args)
+    return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
+  if (!method_supported(odeint_type))
+    return set_error(GALPY_CUDA_ERR_METHOD, "odeint_type not implemented on the GPU");
+  cyl_to_rect_inplace(1, nobj, yo);
+  return run_host(1, 0, nobj, yo, 4, nt, t, indiv_t, npot, pot_type, pot_args, dt, rtol, atol,
+                  result, err, odeint_type, cb, opts, false);
+}
+
+int integrateFullOrbit_dxdv_cuda(double* yo, int nt, double* t, int npot, int* pot_type,
+                                 double* pot_args, void* /*pot_tfuncs*/, double dt, double rtol,
+                                 double atol, double* result, int* err, int odeint_type,
+                                 const galpy_cuda_opts* opts)
+{
+  if (!yo || nt < 1 || !t || !result || !err || !pot_type || !pot_args)
+    return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
+  return run_host(0, 1, 1, yo, 12, nt, t, 0, npot, pot_type, pot_args, dt, rtol, atol, result,
+                  err, odeint_type, nullptr, opts, true);
+}
+
+int integratePlanarOrbit_dxdv_cuda(double* yo, int nt, double* t, int npot, int* pot_type,
+                                   double* pot_args, void* /*pot_tfuncs*/, double dt, double rtol,
+                                   double atol, double* result, int* err, int odeint_type,
+                                   galpy_cuda_callback cb, const galpy_cuda_opts* opts)
+{
+  if (!yo || nt < 1 || !t || !result || !err || !pot_type || !pot_args)
+    return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
+  return run_host(1, 1, 1, yo, 8, nt, t, 0, npot, pot_type, pot_args, dt, rtol, atol, result,
+                  err, odeint_type, cb, opts, true);
+}
+
+int integrateOrbit_dxdv_batch_cuda(int planar, int nobj, double* yo, int nt, double* t,
+                                   int indiv_t, int npot, int* pot_type, double* pot_args,
+                                   double dt, double rtol, double atol, double* result, int* err,
+                                   int odeint_type, const galpy_cuda_opts* opts)
+{
+  if (nobj < 0 || nt < 1 || (nobj && (!yo || !t || !result || !err)) || !pot_type || !pot_args)
+    return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
+  return run_host(planar ? 1 : 0, 1, nobj, yo, planar ? 8 : 12, nt, t, indiv_t, npot, pot_type,
+                  pot_args, dt, rtol, atol, result, err, odeint_type, nullptr, opts, true);
+}
+
+}  // extern "C"

@@ -1,0 +1,983 @@
+// galpy_b200/csrc/machines.cuh
+//
+// Per-orbit integrator state machines.  Each machine advances its orbit by
+// exactly one force evaluation per call:
+//
+//     m.point(y);                // state at which the next force is needed
+//     eval_force(..., y, a);     // the ONE force call site of the kernel
+//     m.consume(y, a, out);      // advance, maybe write output rows
+//
+// so that the 32 lanes of a warp always meet at the same force call, whatever
+// stage of whatever orbit each lane is in (step-size estimation, a regular
+// step, a rejected DOP853 attempt, dense-output stages, or the start of a new
+// orbit picked up by work stealing).  Orbits never diverge at the force call;
+// only the few bookkeeping instructions around it are lane-specific.
+//
+// The arithmetic of every stepper follows the reference step by step so that
+// the step sequence (and, for fixed-step methods, the chosen step size) is the
+// reference's:
+//   leapfrog / symplec4         galpy/util/bovy_symplecticode.c:132-377
+//   their step estimators       galpy/util/bovy_symplecticode.c:588-809
+//   variational (*_dxdv) forms  galpy/util/bovy_symplecticode.c:1053-1268
+//   rk4 + estimator             galpy/util/bovy_rk.c:66-170, 328-395
+//   dop853                      galpy/util/leung_dop853.c:231-517
+// Differences by design: the time variable of the reference's symplectic and
+// RK loops is not tracked (the supported potentials are static); DOP853
+// skips its three dense-output stages in steps that contain no output time
+// (their results are only used for output); every orbit has an attempt budget
+// and stops on a non-finite state instead of looping forever.
+#pragma once
+#include "dop853_tableau.cuh"
+#include "gpc_common.cuh"
+#include "potentials.cuh"
+
+namespace gpc {
+
+constexpr double kDtSentinel = -9999.99;  // galpy's "estimate the step" marker
+constexpr double kMaxDtReduce = 10000.;
+
+enum : int { M_LEAPFROG = 0, M_RK4 = 1, M_SYMPLEC4 = 3, M_DOP853 = 6 };
+// per-orbit status (the reference uses 0 and -10 for SIGINT)
+enum : int { E_OK = 0, E_BUDGET = 2, E_NONFINITE = 3, E_ABORT = -10 };
+enum : int { PREC_FP64 = 0, PREC_F32 = 1 };
+
+// symplec4 coefficients (Kinoshita et al.; bovy_symplecticode.c:96-99)
+constexpr double s4c1 = 0.6756035959798289, s4c2 = -0.1756035959798288;
+constexpr double s4c3 = -0.1756035959798288, s4c4 = 0.6756035959798289;
+constexpr double s4d1 = 1.3512071919596578, s4d2 = -1.7024143839193153;
+constexpr double s4d3 = 1.3512071919596578;
+
+// ------------------------------------------------------------------------
+// output rows
+// ------------------------------------------------------------------------
+enum : int { L_GALPY_CYL = 0, L_AOS_RECT = 1, L_SOA_RECT = 2, L_SOA_CYL = 3 };
+
+struct OutSpec {
+  double* out;
+  int layout;
+  int nt;        // rows per orbit produced by the integrator
+  int row0;      // first row stored (0 = all; nt-1 = final state only)
+  long long nobj;
+};
+
+// Write row j of orbit i.  v is the rectangular state in the reference's row
+// order: plain 3D (x,y,z,vx,vy,vz), planar (x,y,vx,vy); variational rows
+// (x, v, dx, dv) are always written rectangular.
+template <int NV, int D, bool CYL_OK>
+GPC_HD GPC_FI void write_row(const OutSpec& o, long long i, int j, const double* v)
+{
+  if (j < o.row0) return;
+  const long long nrow = o.nt - o.row0, jj = j - o.row0;
+  double w[NV];
+  const bool cyl = CYL_OK && (o.layout == L_GALPY_CYL || o.layout == L_SOA_CYL);
+  if (cyl) {
+    // rect_to_cyl_galpy / rect_to_polar_galpy (bovy_coords.c:79-148)
+    const double x = v[0], y = v[1];
+    const double vx = v[D], vy = v[D + 1];
+    const double phi = atan2(y, x), cp = cos(phi), sp = sin(phi);
+    w[0] = sqrt(x * x + y * y);
+    w[1] = vx * cp + vy * sp;
+    w[2] = -vx * sp + vy * cp;
+    if (D == 3) {
+      w[3] = v[2];
+      w[4] = v[5];
+      w[5] = phi;
+    } else {
+      w[3] = phi;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < NV; k++) w[k] = v[k];
+  }
+  if (o.layout == L_SOA_RECT || o.layout == L_SOA_CYL) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) o.out[((long long)k * nrow + jj) * o.nobj + i] = w[k];
+  } else {
+    double* p = o.out + (i * nrow + jj) * NV;
+#pragma unroll
+    for (int k = 0; k < NV; k++) p[k] = w[k];
+  }
+}
+
+template <int NV, int D, bool CYL_OK>
+GPC_HD GPC_FI void write_nan_rows(const OutSpec& o, long long i, int from)
+{
+  double v[NV];
+#pragma unroll
+  for (int k = 0; k < NV; k++) v[k] = NAN;
+  for (int j = from; j < o.nt; j++) write_row<NV, D, CYL_OK>(o, i, j, v);
+}
+
+// ------------------------------------------------------------------------
+// force adapter: positions -> accelerations (+ K . dq for variational runs)
+// ------------------------------------------------------------------------
+template <int D, int PREC, bool VAR>
+GPC_HD GPC_FI void eval_force(const GpComp* comp, int ncomp, const double* q, double* a)
+{
+  if (!VAR) {
+    if (PREC == PREC_FP64) {
+      double ax, ay, az = 0.0;
+      accel<double, D == 2>(comp, ncomp, q[0], q[1], D == 3 ? q[2] : 0.0, ax, ay, az);
+      a[0] = ax;
+      a[1] = ay;
+      if (D == 3) a[2] = az;
+    } else {
+      float ax, ay, az = 0.f;
+      accel<float, D == 2>(comp, ncomp, (float)q[0], (float)q[1], D == 3 ? (float)q[2] : 0.f, ax,
+                           ay, az);
+      a[0] = ax;
+      a[1] = ay;
+      if (D == 3) a[2] = az;
+    }
+  } else {
+    double ax, ay, az, K[6];
+    accel_tidal<D == 2>(comp, ncomp, q[0], q[1], D == 3 ? q[2] : 0.0, ax, ay, az, K);
+    a[0] = ax;
+    a[1] = ay;
+    if (D == 3) {
+      a[2] = az;
+      const double dx = q[3], dy = q[4], dz = q[5];
+      a[3] = K[0] * dx + K[1] * dy + K[3] * dz;
+      a[4] = K[1] * dx + K[2] * dy + K[4] * dz;
+      a[5] = K[3] * dx + K[4] * dy + K[5] * dz;
+    } else {
+      const double dx = q[2], dy = q[3];
+      a[2] = K[0] * dx + K[1] * dy;
+      a[3] = K[1] * dx + K[2] * dy;
+    }
+  }
+}
+
+// log-sum-exp error scale of the fixed-step estimators
+// (bovy_symplecticode.c:609-624, bovy_rk.c:346-353)
+GPC_HD GPC_FI double est_scale(const double* v, int n, int stride, double rtol, double atol)
+{
+  double m = log(fabs(v[0]));
+  for (int i = 1; i < n; i++) {
+    const double l = log(fabs(v[i * stride]));
+    if (l > m) m = l;
+  }
+  const double c = fmax(atol, rtol + m);
+  return log(exp(atol - c) + exp(rtol + m - c)) + c;
+}
+
+struct OrbitCommon {
+  const double* t;  // this orbit's output times
+  int nt;
+  int iout;         // last row written
+  int err;
+  bool done;
+  long long nsteps;    // accepted steps
+  long long attempts;  // force-consuming step attempts (budget)
+  long long max_attempts;
+};
+
+// ------------------------------------------------------------------------
+// leapfrog / symplec4 (optionally variational)
+// ------------------------------------------------------------------------
+template <int D, bool VAR, bool S4>
+struct SymplecticMachine : OrbitCommon {
+  static constexpr int NQ = VAR ? 2 * D : D;  // stepped positions
+  static constexpr int NY = NQ;               // size of the force argument
+  static constexpr int NV = 2 * NQ;           // values per output row
+  static constexpr int NA = NQ;               // force result size
+  static constexpr int kSlotDoubles = 0;      // no slot store needed
+  GPC_HD GPC_FI void bind(double*, int) {}
+  GPC_HD GPC_FI static void pos(const double* y, double* q)
+  {
+#pragma unroll
+    for (int k = 0; k < NQ; k++) q[k] = y[k];
+  }
+  enum { EST_FULL = 0, EST_HALF = 1, MAIN = 2 };
+  double qo[NQ], po[NQ];  // state at the last output
+  double qw[NQ], pw[NQ];  // state of the running advance
+  double q11[D], p11[D];  // estimator: the single-step result (base orbit)
+  double dt, init_dt, h, sq, sp, rtol, atol;
+  long long nrun, kick, nkick;
+  int sub, phase;
+
+  GPC_HD GPC_FI void start(double hh, long long nstep)
+  {
+    h = hh;
+    nrun = nstep;
+    kick = 0;
+    sub = 0;
+    nkick = (S4 ? 3 : 1) * nstep;
+    const double c = S4 ? s4c1 * h : h / 2.;
+#pragma unroll
+    for (int k = 0; k < NQ; k++) {
+      qw[k] = qo[k] + c * po[k];
+      pw[k] = po[k];
+    }
+  }
+
+  GPC_HD GPC_FI void row(double* v) const
+  {
+    // output order (x, v) for the base and (dx, dv) for the deviation
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      v[k] = qo[k];
+      v[D + k] = po[k];
+      if (VAR) {
+        v[2 * D + k] = qo[D + k];
+        v[3 * D + k] = po[D + k];
+      }
+    }
+  }
+
+  GPC_HD GPC_FI void begin_main()
+  {
+    const long long ndt = (long long)(init_dt / dt);
+    phase = MAIN;
+    start(dt, ndt < 1 ? 1 : ndt);
+  }
+
+  // w: (x, v) or (x, v, dx, dv) rectangular
+  template <class W>
+  GPC_HD void init(const double* w, const double* tt, int nt_, double dt_in, double rtol_,
+                   double atol_, long long max_att, W& out)
+  {
+    t = tt;
+    nt = nt_;
+    iout = 0;
+    err = E_OK;
+    done = false;
+    nsteps = 0;
+    attempts = 0;
+    max_attempts = max_att;
+    rtol = rtol_;
+    atol = atol_;
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      qo[k] = w[k];
+      po[k] = w[D + k];
+      if (VAR) {
+        qo[D + k] = w[2 * D + k];
+        po[D + k] = w[3 * D + k];
+      }
+    }
+    double v[NV];
+    row(v);
+    out(0, v);
+    if (nt < 2) {
+      done = true;
+      return;
+    }
+    init_dt = tt[1] - tt[0];
+    if (dt_in == kDtSentinel) {
+      dt = init_dt;
+      sq = est_scale(qo, D, 1, rtol, atol);
+      sp = est_scale(po, D, 1, rtol, atol);
+      phase = EST_FULL;
+      start(dt, 1);
+    } else {
+      dt = dt_in;
+      begin_main();
+    }
+  }
+
+  GPC_HD GPC_FI void point(double* y) const
+  {
+#pragma unroll
+    for (int k = 0; k < NQ; k++) y[k] = qw[k];
+  }
+
+  template <class W>
+  GPC_HD void consume(const double* /*y*/, const double* a, W& out)
+  {
+    const double dk = S4 ? (sub == 0 ? s4d1 * h : (sub == 1 ? s4d2 * h : s4d3 * h)) : h;
+#pragma unroll
+    for (int k = 0; k < NQ; k++) pw[k] = pw[k] + dk * a[k];
+    const bool last = (kick == nkick - 1);
+    double dc;
+    if (S4)
+      dc = sub == 0 ? s4c2 * h : (sub == 1 ? s4c3 * h : (last ? s4c4 * h : (s4c4 + s4c1) * h));
+    else
+      dc = last ? h / 2. : h;
+#pragma unroll
+    for (int k = 0; k < NQ; k++) qw[k] = qw[k] + dc * pw[k];
+    kick++;
+    sub = (S4 && sub < 2) ? sub + 1 : 0;
+    if (last) advance_done(out);
+  }
+
+  template <class W>
+  GPC_HD void advance_done(W& out)
+  {
+    if (phase == EST_FULL) {
+#pragma unroll
+      for (int k = 0; k < D; k++) {
+        q11[k] = qw[k];
+        p11[k] = pw[k];
+      }
+      phase = EST_HALF;
+      start(dt / 2., 2);
+      return;
+    }
+    if (phase == EST_HALF) {
+      double e = 0.;
+#pragma unroll
+      for (int k = 0; k < D; k++) {
+        e += exp(2. * log(fabs(q11[k] - qw[k])) - 2. * sq);
+        e += exp(2. * log(fabs(p11[k] - pw[k])) - 2. * sp);
+      }
+      e = sqrt(e / 2. / D);
+      if (e > 1. && init_dt / dt < kMaxDtReduce) {
+        dt /= 2.;
+        phase = EST_FULL;
+        start(dt, 1);
+      } else {
+        begin_main();
+      }
+      return;
+    }
+    // MAIN: one output interval completed
+    bool fin = true;
+#pragma unroll
+    for (int k = 0; k < NQ; k++) {
+      qo[k] = qw[k];
+      po[k] = pw[k];
+      fin = fin && isfinite(qw[k]) && isfinite(pw[k]);
+    }
+    nsteps += nrun;
+    attempts += nrun;
+    iout++;
+    double v[NV];
+    row(v);
+    out(iout, v);
+    if (!fin) {
+      err = E_NONFINITE;
+      done = true;
+    } else if (iout == nt - 1) {
+      done = true;
+    } else if (max_attempts > 0 && attempts >= max_attempts) {
+      err = E_BUDGET;
+      done = true;
+    } else {
+      start(dt, nrun);
+    }
+  }
+};
+
+// ------------------------------------------------------------------------
+// RK4 (optionally variational)
+// ------------------------------------------------------------------------
+template <int D, bool VAR>
+struct RK4Machine : OrbitCommon {
+  static constexpr int N = VAR ? 4 * D : 2 * D;  // ODE dimension
+  static constexpr int NY = N;
+  static constexpr int NV = N;
+  static constexpr int NA = VAR ? 2 * D : D;  // force result size
+  // force argument: positions (and deviation positions) of (x, v[, dx, dv])
+  GPC_HD GPC_FI static void pos(const double* y, double* q)
+  {
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      q[k] = y[k];
+      if (VAR) q[D + k] = y[2 * D + k];
+    }
+  }
+  static constexpr int kSlotDoubles = 0;
+  GPC_HD GPC_FI void bind(double*, int) {}
+  enum { EST_A = 0, EST_B = 1, EST_C = 2, MAIN = 3 };
+  double yo[N];    // orbit state at the last completed step
+  double yn[N], yn1[N], ynk[N];
+  double y1[N], ya[N];  // estimator: one-step result; midpoint of the two half steps
+  double dt, init_dt, h, s, rtol, atol;
+  long long nrun, step;
+  int stage, phase;
+
+  GPC_HD GPC_FI void start(const double* from, double hh)
+  {
+    h = hh;
+    stage = 0;
+#pragma unroll
+    for (int k = 0; k < N; k++) yn[k] = yn1[k] = from[k];
+  }
+
+  GPC_HD GPC_FI void begin_main()
+  {
+    const long long ndt = (long long)(init_dt / dt);
+    nrun = ndt < 1 ? 1 : ndt;
+    step = 0;
+    phase = MAIN;
+    start(yo, dt);
+  }
+
+  template <class W>
+  GPC_HD void init(const double* w, const double* tt, int nt_, double dt_in, double rtol_,
+                   double atol_, long long max_att, W& out)
+  {
+    t = tt;
+    nt = nt_;
+    iout = 0;
+    err = E_OK;
+    done = false;
+    nsteps = 0;
+    attempts = 0;
+    max_attempts = max_att;
+    rtol = rtol_;
+    atol = atol_;
+#pragma unroll
+    for (int k = 0; k < N; k++) yo[k] = w[k];
+    out(0, yo);
+    if (nt < 2) {
+      done = true;
+      return;
+    }
+    init_dt = tt[1] - tt[0];
+    if (dt_in == kDtSentinel) {
+      dt = init_dt;
+      s = est_scale(yo, N, 1, rtol, atol);
+      phase = EST_A;
+      start(yo, dt);
+    } else {
+      dt = dt_in;
+      begin_main();
+    }
+  }
+
+  GPC_HD GPC_FI void point(double* y) const
+  {
+    const bool first = stage == 0;
+#pragma unroll
+    for (int k = 0; k < N; k++) y[k] = first ? yn[k] : ynk[k];
+  }
+
+  template <class W>
+  GPC_HD void consume(const double* y, const double* a, W& out)
+  {
+    // derivative of the state at the evaluation point (x, v[, dx, dv])
+    double d[N];
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      d[k] = y[D + k];
+      d[D + k] = a[k];
+      if (VAR) {
+        d[2 * D + k] = y[3 * D + k];
+        d[3 * D + k] = a[D + k];
+      }
+    }
+    // bovy_rk4_onestep (bovy_rk.c:142-170)
+    if (stage == 0 || stage == 3) {
+#pragma unroll
+      for (int k = 0; k < N; k++) yn1[k] += h * d[k] / 6.;
+    } else {
+#pragma unroll
+      for (int k = 0; k < N; k++) yn1[k] += h * d[k] / 3.;
+    }
+    if (stage < 2) {
+#pragma unroll
+      for (int k = 0; k < N; k++) ynk[k] = yn[k] + h * d[k] / 2.;
+    } else if (stage == 2) {
+#pragma unroll
+      for (int k = 0; k < N; k++) ynk[k] = yn[k] + h * d[k];
+    }
+    if (++stage < 4) return;
+    onestep_done(out);
+  }
+
+  template <class W>
+  GPC_HD void onestep_done(W& out)
+  {
+    if (phase == EST_A) {
+#pragma unroll
+      for (int k = 0; k < N; k++) y1[k] = yn1[k];
+      phase = EST_B;
+      start(yo, dt / 2.);
+      return;
+    }
+    if (phase == EST_B) {
+#pragma unroll
+      for (int k = 0; k < N; k++) ya[k] = yn1[k];
+      phase = EST_C;
+      start(ya, dt / 2.);
+      return;
+    }
+    if (phase == EST_C) {
+      double e = 0.;
+#pragma unroll
+      for (int k = 0; k < N; k++) e += exp(2. * log(fabs(y1[k] - yn1[k])) - 2. * s);
+      e = sqrt(e / N);
+      const double c = ceil(pow(e, 1. / 5.));
+      if (c > 1. && init_dt / dt * c < kMaxDtReduce) {
+        dt /= c;
+        phase = EST_A;
+        start(yo, dt);
+      } else {
+        begin_main();
+      }
+      return;
+    }
+    bool fin = true;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+      yo[k] = yn1[k];
+      fin = fin && isfinite(yn1[k]);
+    }
+    nsteps++;
+    attempts++;
+    if (++step < nrun) {
+      if (!fin) {
+        err = E_NONFINITE;
+        done = true;
+        return;
+      }
+      start(yo, dt);
+      return;
+    }
+    step = 0;
+    iout++;
+    out(iout, yo);
+    if (!fin) {
+      err = E_NONFINITE;
+      done = true;
+    } else if (iout == nt - 1) {
+      done = true;
+    } else if (max_attempts > 0 && attempts >= max_attempts) {
+      err = E_BUDGET;
+      done = true;
+    } else {
+      start(yo, dt);
+    }
+  }
+};
+
+// ------------------------------------------------------------------------
+// DOP853 (optionally variational)
+// ------------------------------------------------------------------------
+template <int D, bool VAR>
+struct Dop853Machine : OrbitCommon {
+  static constexpr int N = VAR ? 4 * D : 2 * D;
+  static constexpr int NY = N;
+  static constexpr int NV = N;
+  static constexpr int NA = VAR ? 2 * D : D;  // force result size
+  // force argument: positions (and deviation positions) of (x, v[, dx, dv])
+  GPC_HD GPC_FI static void pos(const double* y, double* q)
+  {
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      q[k] = y[k];
+      if (VAR) q[D + k] = y[2 * D + k];
+    }
+  }
+  enum {
+    ST_INIT1 = 0, ST_INIT2 = 1,
+    // ST_S2..ST_S12 = 2..12
+    ST_FSAL = 13, ST_S14 = 14, ST_S15 = 15, ST_S16 = 16
+  };
+  // Stage slots follow the reference's use of k1..k10 (k2/k3 are reused by
+  // stages 11/12, k4/k5 hold the 8th-order increment / new state after stage
+  // 12); s14/s15 keep the first two dense-output stages so that k10/k2/k3
+  // stay available for the interpolation coefficients.  y0 and k1 (read by
+  // every stage) live in registers; k2..k10, s14, s15 live in a per-thread
+  // slot store (shared memory in the kernel, strided by the block size).
+  static constexpr int kSlots = 11;
+  double y0[N], k1[N];
+  double* ks;   // slot store: ks[(slot * N + i) * kstride]
+  int kstride;
+  // reference name k<j> (j = 2..10) or s14/s15 (j = 14, 15) -> slot
+  static constexpr int kSlotDoubles = kSlots * N;
+  GPC_HD GPC_FI void bind(double* base, int stride)
+  {
+    ks = base;
+    kstride = stride;
+  }
+  GPC_HD GPC_FI double& K(int j, int i) const { return ks[((j <= 10 ? j - 2 : j - 5) * N + i) * kstride]; }
+  double h, hnew, hmax, pos_neg, facold, rtol, atol;
+  double t_current, t_old, t_old_older, dnf;
+  int stage;
+  bool reject;
+
+  GPC_HD GPC_FI void begin_attempt()
+  {
+    h = pos_neg * dmax(fabs(h), 1e3 * 2.3e-16);
+    stage = 2;
+  }
+
+  template <class W>
+  GPC_HD void init(const double* w, const double* tt, int nt_, double /*dt*/, double rtol_,
+                   double atol_, long long max_att, W& out)
+  {
+    t = tt;
+    nt = nt_;
+    iout = 0;
+    err = E_OK;
+    done = false;
+    nsteps = 0;
+    attempts = 0;
+    max_attempts = max_att;
+    rtol = exp(rtol_);
+    atol = exp(atol_);
+    facold = 1.0e-4;
+#pragma unroll
+    for (int k = 0; k < N; k++) y0[k] = w[k];
+    out(0, y0);
+    if (nt < 2) {
+      done = true;
+      return;
+    }
+    hmax = tt[nt - 1] - tt[0];
+    pos_neg = csign(1.0, hmax);
+    reject = false;
+    t_current = t_old = t_old_older = tt[0];
+    stage = ST_INIT1;
+  }
+
+  GPC_HD GPC_FI void point(double* y) const
+  {
+    using namespace dp;
+    switch (stage) {
+      case ST_INIT1:
+#pragma unroll
+        for (int i = 0; i < N; i++) y[i] = y0[i];
+        break;
+      case ST_INIT2:  // explicit Euler step (leung_dop853.c:310)
+#pragma unroll
+        for (int i = 0; i < N; i++) y[i] = y0[i] + h * k1[i];
+        break;
+      case 2:
+#pragma unroll
+        for (int i = 0; i < N; i++) y[i] = y0[i] + h * a21 * k1[i];
+        break;
+      case 3:
+#pragma unroll
+        for (int i = 0; i < N; i++) y[i] = y0[i] + h * (a31 * k1[i] + a32 * K(2, i));
+        break;
+      case 4:
+#pragma unroll
+        for (int i = 0; i < N; i++) y[i] = y0[i] + h * (a41 * k1[i] + a43 * K(3, i));
+        break;
+      case 5:
+#pragma unroll
+        for (int i = 0; i < N; i++) y[i] = y0[i] + h * (a51 * k1[i] + a53 * K(3, i) + a54 * K(4, i));
+        break;
+      case 6:
+#pragma unroll
+        for (int i = 0; i < N; i++) y[i] = y0[i] + h * (a61 * k1[i] + a64 * K(4, i) + a65 * K(5, i));
+        break;
+      case 7:
+#pragma unroll
+        for (int i = 0; i < N; i++)
+          y[i] = y0[i] + h * (a71 * k1[i] + a74 * K(4, i) + a75 * K(5, i) + a76 * K(6, i));
+        break;
+      case 8:
+#pragma unroll
+        for (int i = 0; i < N; i++)
+          y[i] = y0[i] + h * (a81 * k1[i] + a84 * K(4, i) + a85 * K(5, i) + a86 * K(6, i) + a87 * K(7, i));
+        break;
+      case 9:
+#pragma unroll
+        for (int i = 0; i < N; i++)
+          y[i] = y0[i] + h * (a91 * k1[i] + a94 * K(4, i) + a95 * K(5, i) + a96 * K(6, i) +
+                              a97 * K(7, i) + a98 * K(8, i));
+        break;
+      case 10:
+#pragma unroll
+        for (int i = 0; i < N; i++)
+          y[i] = y0[i] + h * (a101 * k1[i] + a104 * K(4, i) + a105 * K(5, i) + a106 * K(6, i) +
+                              a107 * K(7, i) + a108 * K(8, i) + a109 * K(9, i));
+        break;
+      case 11:
+#pragma unroll
+        for (int i = 0; i < N; i++)
+          y[i] = y0[i] + h * (a111 * k1[i] + a114 * K(4, i) + a115 * K(5, i) + a116 * K(6, i) +
+                              a117 * K(7, i) + a118 * K(8, i) + a119 * K(9, i) + a1110 * K(10, i));
+        break;
+      case 12:
+#pragma unroll
+        for (int i = 0; i < N; i++)
+          y[i] = y0[i] + h * (a121 * k1[i] + a124 * K(4, i) + a125 * K(5, i) + a126 * K(6, i) +
+                              a127 * K(7, i) + a128 * K(8, i) + a129 * K(9, i) + a1210 * K(10, i) +
+                              a1211 * K(2, i));
+        break;
+      case ST_FSAL:
+#pragma unroll
+        for (int i = 0; i < N; i++) y[i] = K(5, i);
+        break;
+      case ST_S14:
+#pragma unroll
+        for (int i = 0; i < N; i++)
+          y[i] = y0[i] + h * (a141 * k1[i] + a147 * K(7, i) + a148 * K(8, i) + a149 * K(9, i) +
+                              a1410 * K(10, i) + a1411 * K(2, i) + a1412 * K(3, i) + a1413 * K(4, i));
+        break;
+      case ST_S15:
+#pragma unroll
+        for (int i = 0; i < N; i++)
+          y[i] = y0[i] + h * (a151 * k1[i] + a156 * K(6, i) + a157 * K(7, i) + a158 * K(8, i) +
+                              a1511 * K(2, i) + a1512 * K(3, i) + a1513 * K(4, i) + a1514 * K(14, i));
+        break;
+      default:  // ST_S16
+#pragma unroll
+        for (int i = 0; i < N; i++)
+          y[i] = y0[i] + h * (a161 * k1[i] + a166 * K(6, i) + a167 * K(7, i) + a168 * K(8, i) +
+                              a169 * K(9, i) + a1613 * K(4, i) + a1614 * K(14, i) + a1615 * K(15, i));
+        break;
+    }
+  }
+
+  GPC_HD GPC_FI bool output_pending() const
+  {
+    return iout < nt - 1 && pos_neg * t[iout + 1] < pos_neg * t_current;
+  }
+
+  template <class W>
+  GPC_HD void consume(const double* y, const double* a, W& out)
+  {
+    using namespace dp;
+    double d[N];
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      d[k] = y[D + k];
+      d[D + k] = a[k];
+      if (VAR) {
+        d[2 * D + k] = y[3 * D + k];
+        d[3 * D + k] = a[D + k];
+      }
+    }
+    switch (stage) {
+      case ST_INIT1: {  // leung_dop853.c:296-308
+#pragma unroll
+        for (int i = 0; i < N; i++) k1[i] = d[i];
+        double dny = 0.0;
+        dnf = 0.0;
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+          const double sk = atol + rtol * fabs(y0[i]);
+          double sqr = k1[i] / sk;
+          dnf += sqr * sqr;
+          sqr = y0[i] / sk;
+          dny += sqr * sqr;
+        }
+        h = csign(dmin(sqrt(dny / dnf) * 0.01, fabs(hmax)), pos_neg);
+        stage = ST_INIT2;
+        return;
+      }
+      case ST_INIT2: {  // leung_dop853.c:309-324
+#pragma unroll
+        for (int i = 0; i < N; i++) K(2, i) = d[i];
+        double der2 = 0.0;
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+          const double sk = atol + rtol * fabs(y0[i]);
+          const double sqr = (K(2, i) - k1[i]) / sk;
+          der2 += sqr * sqr;
+        }
+        der2 = sqrt(der2) / h;
+        const double der12 = dmax(fabs(der2), sqrt(dnf));
+        const double h1 = pow(0.01 / der12, 1.0 / 8.0);
+        h = csign(dmin(100.0 * fabs(h), dmin(fabs(h1), fabs(hmax))), pos_neg);
+        begin_attempt();
+        return;
+      }
+      case 2:
+#pragma unroll
+        for (int i = 0; i < N; i++) K(2, i) = d[i];
+        break;
+      case 3:
+#pragma unroll
+        for (int i = 0; i < N; i++) K(3, i) = d[i];
+        break;
+      case 4:
+#pragma unroll
+        for (int i = 0; i < N; i++) K(4, i) = d[i];
+        break;
+      case 5:
+#pragma unroll
+        for (int i = 0; i < N; i++) K(5, i) = d[i];
+        break;
+      case 6:
+#pragma unroll
+        for (int i = 0; i < N; i++) K(6, i) = d[i];
+        break;
+      case 7:
+#pragma unroll
+        for (int i = 0; i < N; i++) K(7, i) = d[i];
+        break;
+      case 8:
+#pragma unroll
+        for (int i = 0; i < N; i++) K(8, i) = d[i];
+        break;
+      case 9:
+#pragma unroll
+        for (int i = 0; i < N; i++) K(9, i) = d[i];
+        break;
+      case 10:
+#pragma unroll
+        for (int i = 0; i < N; i++) K(10, i) = d[i];
+        break;
+      case 11:
+#pragma unroll
+        for (int i = 0; i < N; i++) K(2, i) = d[i];
+        break;
+      case 12: {
+#pragma unroll
+        for (int i = 0; i < N; i++) K(3, i) = d[i];
+        after_stage12();
+        return;
+      }
+      case ST_FSAL: {
+#pragma unroll
+        for (int i = 0; i < N; i++) K(4, i) = d[i];
+        nsteps++;
+        if (output_pending()) {
+          stage = ST_S14;
+          return;
+        }
+        finish_step(out);
+        return;
+      }
+      case ST_S14:
+#pragma unroll
+        for (int i = 0; i < N; i++) K(14, i) = d[i];
+        stage = ST_S15;
+        return;
+      case ST_S15:
+#pragma unroll
+        for (int i = 0; i < N; i++) K(15, i) = d[i];
+        stage = ST_S16;
+        return;
+      default: {  // ST_S16: dense output (leung_dop853.c:441-474)
+        while (output_pending()) {
+          const double sv = (t[iout + 1] - t_old) / h, s1 = 1.0 - sv;
+          double v[N];
+#pragma unroll
+          for (int i = 0; i < N; i++) {
+            const double rc1 = y0[i];
+            const double ydiff = K(5, i) - y0[i];
+            const double bspl = h * k1[i] - ydiff;
+            const double rc4 = ydiff - h * K(4, i) - bspl;
+            double rc5 = d41 * k1[i] + d46 * K(6, i) + d47 * K(7, i) + d48 * K(8, i) + d49 * K(9, i) +
+                         d410 * K(10, i) + d411 * K(2, i) + d412 * K(3, i);
+            double rc6 = d51 * k1[i] + d56 * K(6, i) + d57 * K(7, i) + d58 * K(8, i) + d59 * K(9, i) +
+                         d510 * K(10, i) + d511 * K(2, i) + d512 * K(3, i);
+            double rc7 = d61 * k1[i] + d66 * K(6, i) + d67 * K(7, i) + d68 * K(8, i) + d69 * K(9, i) +
+                         d610 * K(10, i) + d611 * K(2, i) + d612 * K(3, i);
+            double rc8 = d71 * k1[i] + d76 * K(6, i) + d77 * K(7, i) + d78 * K(8, i) + d79 * K(9, i) +
+                         d710 * K(10, i) + d711 * K(2, i) + d712 * K(3, i);
+            rc5 = h * (rc5 + d413 * K(4, i) + d414 * K(14, i) + d415 * K(15, i) + d416 * d[i]);
+            rc6 = h * (rc6 + d513 * K(4, i) + d514 * K(14, i) + d515 * K(15, i) + d516 * d[i]);
+            rc7 = h * (rc7 + d613 * K(4, i) + d614 * K(14, i) + d615 * K(15, i) + d616 * d[i]);
+            rc8 = h * (rc8 + d713 * K(4, i) + d714 * K(14, i) + d715 * K(15, i) + d716 * d[i]);
+            v[i] = rc1 +
+                   sv * (ydiff +
+                         s1 * (bspl + sv * (rc4 + s1 * (rc5 + sv * (rc6 + s1 * (rc7 + sv * rc8))))));
+          }
+          iout++;
+          out(iout, v);
+        }
+        finish_step(out);
+        return;
+      }
+    }
+    stage++;
+  }
+
+  GPC_HD void after_stage12()
+  {
+    using namespace dp;
+    attempts++;
+    t_old_older = t_old;
+    t_old = t_current;
+    t_current = t_current + h;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+      K(4, i) = b1 * k1[i] + b6 * K(6, i) + b7 * K(7, i) + b8 * K(8, i) + b9 * K(9, i) + b10 * K(10, i) +
+              b11 * K(2, i) + b12 * K(3, i);
+      K(5, i) = y0[i] + h * K(4, i);
+    }
+    double e = 0.0, e2 = 0.0;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+      const double sk = atol + rtol * dmax(fabs(y0[i]), fabs(K(5, i)));
+      double erri = K(4, i) - bhh1 * k1[i] - bhh2 * K(9, i) - bhh3 * K(3, i);
+      double sqr = erri / sk;
+      e2 += sqr * sqr;
+      erri = er1 * k1[i] + er6 * K(6, i) + er7 * K(7, i) + er8 * K(8, i) + er9 * K(9, i) + er10 * K(10, i) +
+             er11 * K(2, i) + er12 * K(3, i);
+      sqr = erri / sk;
+      e += sqr * sqr;
+    }
+    double deno = e + 0.01 * e2;
+    if (deno <= 0.0) deno = 1.0;
+    e = fabs(h) * e * sqrt(1.0 / (deno * (double)N));
+    if (!isfinite(e)) {
+      err = E_NONFINITE;
+      done = true;
+      return;
+    }
+    const double fac11 = pow(e, 1.0 / 8.0);
+    double fac = fac11;  // Lund stabilisation with beta = 0: / pow(facold, 0) == / 1
+    fac = dmax(1.0 / 6.0, dmin(1.0 / 0.333, fac / 0.9));
+    hnew = h / fac;
+    if (e <= 1.0) {
+      facold = dmax(e, 1.0e-4);
+      stage = ST_FSAL;
+    } else {
+      hnew = h / dmin(1.0 / 0.333, fac11 / 0.9);
+      reject = true;
+      t_current = t_old;
+      t_old = t_old_older;
+      h = hnew;
+      if (max_attempts > 0 && attempts >= max_attempts) {
+        err = E_BUDGET;
+        done = true;
+        return;
+      }
+      begin_attempt();
+    }
+  }
+
+  template <class W>
+  GPC_HD void finish_step(W& out)
+  {
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+      k1[i] = K(4, i);
+      y0[i] = K(5, i);
+    }
+    hnew = (fabs(hnew) > fabs(hmax)) ? pos_neg * hmax : hnew;
+    if (reject) hnew = pos_neg * dmin(fabs(hnew), fabs(h));
+    reject = false;
+    h = hnew;
+    if (iout == nt - 1) {
+      done = true;
+      return;
+    }
+    if (max_attempts > 0 && attempts >= max_attempts) {
+      err = E_BUDGET;
+      done = true;
+      return;
+    }
+    begin_attempt();
+  }
+};
+
+// Rows the integrator did not reach (stopped by the budget, a non-finite
+// state or an abort) are written as NaN.
+template <class M, class W>
+GPC_HD void fill_unreached_rows(const M& m, W& out)
+{
+  if (m.err == E_OK) return;
+  double v[M::NV];
+#pragma unroll
+  for (int k = 0; k < M::NV; k++) v[k] = NAN;
+  for (int j = m.iout + 1; j < m.nt; j++) out(j, v);
+}
+
+// Per-orbit driver used by the kernels and by the host test harness: run one
+// machine to completion with the force evaluated by `force`.
+template <class M, class F, class W>
+GPC_HD void run_orbit(M& m, F& force, W& out)
+{
+  double y[M::NY], q[M::NA], a[M::NA];
+  while (!m.done) {
+    m.point(y);
+    M::pos(y, q);
+    force(q, a);
+    m.consume(y, a, out);
+  }
+  fill_unreached_rows(m, out);
+}
+
+}  // namespace gpc

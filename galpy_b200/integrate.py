@@ -1,0 +1,266 @@
+"""galpy-facing integration entry points.
+
+Each function mirrors the galpy wrapper it stands in for -- same arguments,
+same array shapes, same error behaviour -- and calls libgalpy_cuda.so through
+ctypes exactly like galpy calls libgalpy:
+
+  integrateFullOrbit_cuda         galpy/orbit/integrateFullOrbit.py:616-749
+  integratePlanarOrbit_cuda       galpy/orbit/integratePlanarOrbit.py:989
+  integrateFullOrbit_dxdv_cuda    galpy/orbit/integrateFullOrbit.py:752-856
+  integratePlanarOrbit_dxdv_cuda  galpy/orbit/integratePlanarOrbit.py:1124-1225
+
+plus ``integrate_dxdv_batch`` (all deviations of many orbits in one launch)
+and ``integrate_device`` (device-resident torch tensors, asynchronous).
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .potentials import parse_pot
+
+# galpy's odeint codes (galpy/orbit/integratePlanarOrbit.py:690-709)
+CUDA_METHODS = {"leapfrog_cuda": 0, "rk4_cuda": 1, "symplec4_cuda": 3, "dop853_cuda": 6}
+_ALIASES = {"leapfrog": 0, "rk4": 1, "symplec4": 3, "dop853": 6}
+PRECISIONS = {"fp64": _lib.FP64, "f32force": _lib.F32FORCE}
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+def parse_integrator(int_method):
+    """galpy odeint code of a method name.  Unlike galpy's _parse_integrator
+    (which maps unknown names to leapfrog), unknown names raise."""
+    m = int_method.lower()
+    if m in CUDA_METHODS:
+        return CUDA_METHODS[m]
+    for suffix in ("_cuda", "_c"):
+        if m.endswith(suffix) and m[: -len(suffix)] in _ALIASES:
+            return _ALIASES[m[: -len(suffix)]]
+    if m in _ALIASES:
+        return _ALIASES[m]
+    raise ValueError(f"{int_method} is not a method of the CUDA engine")
+
+
+def parse_tol(rtol, atol):
+    """natural logs, default 1e-12 (galpy/orbit/integratePlanarOrbit.py:712-723)."""
+    r = -12.0 * np.log(10.0) if rtol is None else np.log(rtol)
+    a = -12.0 * np.log(10.0) if atol is None else np.log(atol)
+    return float(r), float(a)
+
+
+def _precision(p):
+    if isinstance(p, int):
+        return p
+    return PRECISIONS[p.lower()]
+
+
+def _integrate_c(planar, pot, yo, t, int_method, rtol, atol, progressbar, dt, precision,
+                 max_attempts, return_nsteps, device):
+    single_obj = yo.ndim == 1
+    yo = np.atleast_2d(yo)
+    nobj = len(yo)
+    nv = 4 if planar else 6
+    rtol, atol = parse_tol(rtol, atol)
+    npot, pot_type, pot_args = parse_pot(pot, planar=planar)
+    code = parse_integrator(int_method)
+    dt = _lib.DT_SENTINEL if dt is None else float(dt)
+    t = np.asarray(t)
+    indiv_t = int(t.ndim > 1)
+    nt = t.shape[-1]
+    result = np.empty((nobj, nt, nv))
+    err = np.zeros(nobj, dtype=np.int32)
+    nsteps = np.zeros(nobj, dtype=np.int64) if return_nsteps else None
+    yo = np.require(yo, dtype=np.float64, requirements=["C", "W"])
+    t = np.require(t, dtype=np.float64, requirements=["C", "W"])
+    opts = _lib.make_opts(precision=_precision(precision), device=device,
+                          max_attempts=max_attempts, nsteps=nsteps)
+    cb = _lib.CALLBACK()
+    pbar = None
+    if progressbar and nobj > 1:
+        try:
+            import tqdm
+
+            pbar = tqdm.tqdm(total=nobj, leave=False)
+            cb = _lib.CALLBACK(pbar.update)
+        except ImportError:  # pragma: no cover
+            pass
+    fn = _lib.lib().integratePlanarOrbit_cuda if planar else _lib.lib().integrateFullOrbit_cuda
+    rc = fn(nobj, yo.ctypes.data_as(_dp), nt, t.ctypes.data_as(_dp), indiv_t, npot,
+            pot_type.ctypes.data_as(_ip), pot_args.ctypes.data_as(_dp), None, dt, rtol, atol,
+            result.ctypes.data_as(_dp), err.ctypes.data_as(_ip), code, cb, ctypes.byref(opts))
+    if pbar is not None:
+        pbar.close()
+    _lib.check(rc)
+    if np.any(err == -10):  # same behaviour as galpy (integrateFullOrbit.py:737-738)
+        raise KeyboardInterrupt("Orbit integration interrupted by CTRL-C (SIGINT)")
+    out = (result[0], err[0]) if single_obj else (result, err)
+    if return_nsteps:
+        out = out + ((nsteps[0] if single_obj else nsteps),)
+    return out
+
+
+def integrateFullOrbit_cuda(pot, yo, t, int_method, rtol=None, atol=None, progressbar=True,
+                            dt=None, precision="fp64", max_attempts=0, return_nsteps=False,
+                            device=-1):
+    """Integrate 3D orbits on the GPU.
+
+    Parameters mirror galpy's integrateFullOrbit_c: yo [N,6] or [6]
+    cylindrical (R,vR,vT,z,vz,phi) -- overwritten in place with rectangular
+    coordinates when it is a C-contiguous float64 array, as in galpy; t [nt]
+    or [N,nt]; int_method one of 'leapfrog_cuda', 'rk4_cuda', 'symplec4_cuda',
+    'dop853_cuda'.  Extra keywords: precision ('fp64' or 'f32force'),
+    max_attempts (per-orbit step-attempt budget, 0 = none), return_nsteps.
+
+    Returns (result [N,nt,6] cylindrical, err [N]) like galpy (the leading
+    axis is dropped for a single orbit), plus per-orbit accepted steps when
+    return_nsteps."""
+    return _integrate_c(False, pot, yo, t, int_method, rtol, atol, progressbar, dt, precision,
+                        max_attempts, return_nsteps, device)
+
+
+def integratePlanarOrbit_cuda(pot, yo, t, int_method, rtol=None, atol=None, progressbar=True,
+                              dt=None, precision="fp64", max_attempts=0, return_nsteps=False,
+                              device=-1):
+    """Planar counterpart of integrateFullOrbit_cuda: yo [N,4] (R,vR,vT,phi)."""
+    return _integrate_c(True, pot, yo, t, int_method, rtol, atol, progressbar, dt, precision,
+                        max_attempts, return_nsteps, device)
+
+
+def _dxdv_single(planar, pot, yo, dyo, t, int_method, dt, rtol, atol, device):
+    rtol, atol = parse_tol(rtol, atol)
+    dt = _lib.DT_SENTINEL if dt is None else float(dt)
+    npot, pot_type, pot_args = parse_pot(pot, planar=planar)
+    code = parse_integrator(int_method)
+    yo = np.require(np.concatenate((yo, dyo)), dtype=np.float64, requirements=["C", "W"])
+    t = np.require(t, dtype=np.float64, requirements=["C", "W"])
+    nv = 8 if planar else 12
+    result = np.empty((len(t), nv))
+    err = ctypes.c_int(0)
+    opts = _lib.make_opts(device=device)
+    L = _lib.lib()
+    if planar:
+        rc = L.integratePlanarOrbit_dxdv_cuda(
+            yo.ctypes.data_as(_dp), len(t), t.ctypes.data_as(_dp), npot,
+            pot_type.ctypes.data_as(_ip), pot_args.ctypes.data_as(_dp), None, dt, rtol, atol,
+            result.ctypes.data_as(_dp), ctypes.byref(err), code, _lib.CALLBACK(),
+            ctypes.byref(opts))
+    else:
+        rc = L.integrateFullOrbit_dxdv_cuda(
+            yo.ctypes.data_as(_dp), len(t), t.ctypes.data_as(_dp), npot,
+            pot_type.ctypes.data_as(_ip), pot_args.ctypes.data_as(_dp), None, dt, rtol, atol,
+            result.ctypes.data_as(_dp), ctypes.byref(err), code, ctypes.byref(opts))
+    _lib.check(rc)
+    if int(err.value) == -10:
+        raise KeyboardInterrupt("Orbit integration interrupted by CTRL-C (SIGINT)")
+    return result, err.value
+
+
+def integrateFullOrbit_dxdv_cuda(pot, yo, dyo, t, int_method, dt=None, rtol=None, atol=None,
+                                 device=-1):
+    """Mirror of galpy's integrateFullOrbit_dxdv_c: rectangular yo [6], dyo [6];
+    returns (result [nt,12], err)."""
+    return _dxdv_single(False, pot, yo, dyo, t, int_method, dt, rtol, atol, device)
+
+
+def integratePlanarOrbit_dxdv_cuda(pot, yo, dyo, t, int_method, rtol=None, atol=None, dt=None,
+                                   device=-1):
+    """Mirror of galpy's integratePlanarOrbit_dxdv_c: rectangular yo [4],
+    dyo [4]; returns (result [nt,8], err)."""
+    return _dxdv_single(True, pot, yo, dyo, t, int_method, dt, rtol, atol, device)
+
+
+def integrate_dxdv_batch(pot, w, t, int_method, planar=False, dt=None, rtol=None, atol=None,
+                         device=-1, return_nsteps=False):
+    """Variational integration of many (orbit, deviation) pairs in one launch.
+
+    w [N, 4*dim] rectangular (x, v, dx, dv); t [nt] or [N, nt].  Returns
+    (result [N, nt, 4*dim], err [N]).  Build a state-transition matrix by
+    passing the same orbit once per canonical deviation."""
+    rtol, atol = parse_tol(rtol, atol)
+    dt = _lib.DT_SENTINEL if dt is None else float(dt)
+    npot, pot_type, pot_args = parse_pot(pot, planar=planar)
+    code = parse_integrator(int_method)
+    w = np.require(np.atleast_2d(w), dtype=np.float64, requirements=["C", "W"])
+    t = np.require(t, dtype=np.float64, requirements=["C", "W"])
+    nobj, nv = w.shape
+    nt = t.shape[-1]
+    result = np.empty((nobj, nt, nv))
+    err = np.zeros(nobj, dtype=np.int32)
+    nsteps = np.zeros(nobj, dtype=np.int64) if return_nsteps else None
+    opts = _lib.make_opts(device=device, nsteps=nsteps)
+    rc = _lib.lib().integrateOrbit_dxdv_batch_cuda(
+        int(planar), nobj, w.ctypes.data_as(_dp), nt, t.ctypes.data_as(_dp), int(t.ndim > 1),
+        npot, pot_type.ctypes.data_as(_ip), pot_args.ctypes.data_as(_dp), dt, rtol, atol,
+        result.ctypes.data_as(_dp), err.ctypes.data_as(_ip), code, ctypes.byref(opts))
+    _lib.check(rc)
+    if np.any(err == -10):
+        raise KeyboardInterrupt("Orbit integration interrupted by CTRL-C (SIGINT)")
+    return (result, err, nsteps) if return_nsteps else (result, err)
+
+
+def compile_potential(pot, planar=False, ngroup=1):
+    """Compiled device records (bytes) of a potential, or of ngroup parameter
+    groups when pot is (pot_type, pot_args) with ngroup argument blocks."""
+    npot, pot_type, pot_args = parse_pot(pot, planar=planar)
+    size = _lib.lib().galpy_cuda_comp_size()
+    buf = np.zeros(size * npot * ngroup, dtype=np.uint8)
+    rc = _lib.lib().galpy_cuda_compile_potential(
+        int(planar), npot, pot_type.ctypes.data_as(_ip), pot_args.ctypes.data_as(_dp), ngroup,
+        buf.ctypes.data_as(ctypes.c_void_p))
+    _lib.check(rc)
+    return buf, npot
+
+
+def integrate_device(comps, ncomp, w0, t, out, err, int_method, planar=False, variational=False,
+                     nsteps=None, group=None, in_layout="soa", out_layout="soa_rect",
+                     out_row0=0, dt=None, rtol=None, atol=None, precision="fp64",
+                     max_attempts=0, stream=None, block_size=0, grid_size=0):
+    """Asynchronous integration of device-resident torch tensors.
+
+    comps: uint8 CUDA tensor of compiled records (compile_potential); w0
+    float64 [nv, N] (in_layout 'soa') or [N, nv] ('aos'); t float64 [nt] or
+    [N, nt]; out float64 sized for the layout ('soa_rect'/'soa_cyl':
+    [nv, nt-out_row0, N], 'aos_rect'/'galpy': [N, nt-out_row0, nv]); err int32
+    [N]; nsteps int64 [N] or None; group int32 [N] or None.  Runs on `stream`
+    (a torch.cuda.Stream, default: the current stream)."""
+    import torch
+
+    layouts_in = {"aos": _lib.IN_AOS, "soa": _lib.IN_SOA}
+    layouts_out = {"galpy": _lib.OUT_GALPY, "aos_rect": _lib.OUT_AOS_RECT,
+                   "soa_rect": _lib.OUT_SOA_RECT, "soa_cyl": _lib.OUT_SOA_CYL}
+    for name, x, dt_ in (("w0", w0, torch.float64), ("t", t, torch.float64),
+                         ("out", out, torch.float64), ("err", err, torch.int32)):
+        if not (x.is_cuda and x.dtype == dt_ and x.is_contiguous()):
+            raise ValueError(f"{name} must be a contiguous CUDA tensor of {dt_}")
+    nobj = err.shape[0]
+    rtol, atol = parse_tol(rtol, atol)
+    L = _lib.GalpyCudaLaunch()
+    L.planar = int(planar)
+    L.variational = int(variational)
+    L.odeint_type = parse_integrator(int_method)
+    L.precision = _precision(precision)
+    L.nobj = nobj
+    L.nt = t.shape[-1]
+    L.indiv_t = int(t.dim() > 1)
+    L.t = t.data_ptr()
+    L.w0 = w0.data_ptr()
+    L.in_layout = layouts_in[in_layout]
+    L.out = out.data_ptr()
+    L.out_layout = layouts_out[out_layout]
+    L.out_row0 = out_row0
+    L.err = err.data_ptr()
+    L.nsteps = nsteps.data_ptr() if nsteps is not None else None
+    L.comps = comps.data_ptr()
+    L.ncomp = ncomp
+    L.group = group.data_ptr() if group is not None else None
+    L.dt = _lib.DT_SENTINEL if dt is None else float(dt)
+    L.rtol = rtol
+    L.atol = atol
+    L.max_attempts = max_attempts
+    L.abort_flag = None
+    s = stream if stream is not None else torch.cuda.current_stream(w0.device)
+    L.stream = s.cuda_stream
+    L.block_size = block_size
+    L.grid_size = grid_size
+    _lib.check(_lib.lib().galpy_cuda_integrate_device(ctypes.byref(L)))

@@ -1,0 +1,152 @@
+/*
+ * galpy_cuda.h -- C ABI of libgalpy_cuda.so, the B200 orbit-integration engine
+ * behind galpy's Orbit.integrate methods 'leapfrog_cuda', 'rk4_cuda',
+ * 'symplec4_cuda' and 'dop853_cuda'.
+ *
+ * The galpy-facing entry points take exactly the arguments of the libgalpy
+ * functions they stand in for, with galpy's conventions: AoS arrays owned by
+ * the caller (host memory), yo overwritten with the rectangular initial
+ * conditions, t either shared (nt) or per orbit (nobj*nt, indiv_t = 1),
+ * rtol/atol as natural logarithms, dt = -9999.99 meaning "estimate the step",
+ * odeint_type 0 leapfrog, 1 rk4, 3 symplec4, 6 dop853 (galpy's numbering;
+ * 2 rk6, 4 symplec6, 5 dopr54 and 7 ias15 return GALPY_CUDA_ERR_METHOD so the
+ * caller can fall back), pot_type/pot_args as produced by galpy's _parse_pot
+ * (types 0 LogarithmicHalo, 5 MiyamotoNagai, 8 Hernquist, 9 NFW,
+ * 15 PowerSphericalwCutoff), per-orbit err[] (0 ok, -10 interrupted by
+ * SIGINT).  Two additions: every entry point returns a status code instead
+ * of void, and takes a trailing options pointer (NULL = defaults).
+ *
+ * Per-orbit err values beyond the reference's: 2 = attempt budget exhausted,
+ * 3 = the state became non-finite (the reference loops forever on NaN in
+ * DOP853; rows after the failure are NaN here).
+ */
+#ifndef GALPY_CUDA_H
+#define GALPY_CUDA_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GALPY_CUDA_ABI_VERSION 1
+
+/* return codes */
+#define GALPY_CUDA_OK 0
+#define GALPY_CUDA_ERR_ARG (-1)         /* invalid argument */
+#define GALPY_CUDA_ERR_METHOD (-2)      /* odeint_type not implemented on the GPU */
+#define GALPY_CUDA_ERR_POTENTIAL (-3)   /* a pot_type not implemented on the GPU */
+#define GALPY_CUDA_ERR_CUDA (-4)        /* CUDA runtime failure; see galpy_cuda_last_error */
+#define GALPY_CUDA_ERR_NODEVICE (-5)    /* no CUDA device visible */
+#define GALPY_CUDA_ERR_INTERRUPTED (-10) /* SIGINT during the call; err[] holds -10 */
+
+/* precision of the force evaluation (the state is always float64) */
+#define GALPY_CUDA_FP64 0
+#define GALPY_CUDA_F32FORCE 1
+
+/* array layouts of the device-pointer entry point */
+#define GALPY_CUDA_IN_AOS 0      /* [nobj][nv] rectangular */
+#define GALPY_CUDA_IN_SOA 1      /* [nv][nobj] rectangular */
+#define GALPY_CUDA_OUT_GALPY 0   /* [nobj][nrow][nv], galpy's cylindrical coordinates */
+#define GALPY_CUDA_OUT_AOS_RECT 1 /* [nobj][nrow][nv] rectangular */
+#define GALPY_CUDA_OUT_SOA_RECT 2 /* [nv][nrow][nobj] rectangular */
+#define GALPY_CUDA_OUT_SOA_CYL 3  /* [nv][nrow][nobj] cylindrical */
+
+typedef void (*galpy_cuda_callback)(void);
+
+typedef struct galpy_cuda_opts {
+  int size;                /* sizeof(galpy_cuda_opts) */
+  int device;              /* CUDA device ordinal, -1 = current */
+  int precision;           /* GALPY_CUDA_FP64 (default) or GALPY_CUDA_F32FORCE */
+  int block_size;          /* threads per block, 0 = tuned default */
+  long long max_attempts;  /* per-orbit step-attempt budget, 0 = unlimited */
+  long long *nsteps;       /* optional out, host [nobj]: accepted steps per orbit */
+  double *elapsed_ms;      /* optional out: device time of the integration kernel */
+} galpy_cuda_opts;
+
+/* Compiled potential record size in bytes (one per component). */
+int galpy_cuda_comp_size(void);
+
+/* Translate galpy's (pot_type, pot_args) for ngroup potential groups with the
+ * same component types (pot_args holds ngroup consecutive argument blocks)
+ * into compiled records written to out (host memory of
+ * ngroup*npot*galpy_cuda_comp_size() bytes).  Returns 0 or
+ * GALPY_CUDA_ERR_POTENTIAL / GALPY_CUDA_ERR_ARG. */
+int galpy_cuda_compile_potential(int planar, int npot, const int *pot_type,
+                                 const double *pot_args, int ngroup, void *out);
+
+/* Stands in for integrateFullOrbit (galpy/orbit/orbit_c_ext/integrateFullOrbit.c:1046). */
+int integrateFullOrbit_cuda(int nobj, double *yo, int nt, double *t, int indiv_t, int npot,
+                            int *pot_type, double *pot_args, void *pot_tfuncs, double dt,
+                            double rtol, double atol, double *result, int *err,
+                            int odeint_type, galpy_cuda_callback cb,
+                            const galpy_cuda_opts *opts);
+
+/* Stands in for integratePlanarOrbit (galpy/orbit/orbit_c_ext/integratePlanarOrbit.c:743). */
+int integratePlanarOrbit_cuda(int nobj, double *yo, int nt, double *t, int indiv_t, int npot,
+                              int *pot_type, double *pot_args, void *pot_tfuncs, double dt,
+                              double rtol, double atol, double *result, int *err,
+                              int odeint_type, galpy_cuda_callback cb,
+                              const galpy_cuda_opts *opts);
+
+/* Stands in for integrateFullOrbit_dxdv (integrateFullOrbit.c:1234): one
+ * orbit, yo = (x,y,z,vx,vy,vz,dx,dy,dz,dvx,dvy,dvz), result [nt][12]. */
+int integrateFullOrbit_dxdv_cuda(double *yo, int nt, double *t, int npot, int *pot_type,
+                                 double *pot_args, void *pot_tfuncs, double dt, double rtol,
+                                 double atol, double *result, int *err, int odeint_type,
+                                 const galpy_cuda_opts *opts);
+
+/* Stands in for integratePlanarOrbit_dxdv (integratePlanarOrbit.c:940): one
+ * orbit, yo = (x,y,vx,vy,dx,dy,dvx,dvy), result [nt][8]. */
+int integratePlanarOrbit_dxdv_cuda(double *yo, int nt, double *t, int npot, int *pot_type,
+                                   double *pot_args, void *pot_tfuncs, double dt, double rtol,
+                                   double atol, double *result, int *err, int odeint_type,
+                                   galpy_cuda_callback cb, const galpy_cuda_opts *opts);
+
+/* Batched variational integration (galpy runs the single-orbit functions
+ * above once per orbit from Python, galpy/orbit/Orbits.py:2445): nobj orbits
+ * with one deviation column each, yo [nobj][4*dim] rectangular, t shared or
+ * per orbit, result [nobj][nt][4*dim]. */
+int integrateOrbit_dxdv_batch_cuda(int planar, int nobj, double *yo, int nt, double *t,
+                                   int indiv_t, int npot, int *pot_type, double *pot_args,
+                                   double dt, double rtol, double atol, double *result, int *err,
+                                   int odeint_type, const galpy_cuda_opts *opts);
+
+/* Device-pointer entry point: all arrays live on the device, the call is
+ * asynchronous on `stream`.  Needs 64 bytes of device scratch for the
+ * work-stealing counter, allocated stream-ordered per call. */
+typedef struct galpy_cuda_launch {
+  int planar, variational, odeint_type, precision;
+  long long nobj;
+  int nt, indiv_t;
+  const double *t;          /* nt or nobj*nt */
+  const double *w0;         /* initial rectangular states */
+  int in_layout;            /* GALPY_CUDA_IN_* */
+  double *out;
+  int out_layout;           /* GALPY_CUDA_OUT_* */
+  int out_row0;             /* first row stored (nt-1: final state only) */
+  int *err;                 /* [nobj] */
+  long long *nsteps;        /* [nobj] or NULL */
+  const void *comps;        /* compiled potential, ngroup*ncomp records */
+  int ncomp;
+  const int *group;         /* [nobj] group of each orbit, or NULL (one group) */
+  double dt, rtol, atol;    /* galpy conventions */
+  long long max_attempts;
+  const int *abort_flag;    /* device int polled by the kernel, or NULL */
+  void *stream;             /* cudaStream_t */
+  int block_size, grid_size; /* 0 = defaults */
+} galpy_cuda_launch;
+
+int galpy_cuda_integrate_device(const galpy_cuda_launch *launch);
+
+/* Diagnostic: measured float64 fused-multiply-add throughput of the current
+ * device in TFLOP/s (2 flops per FMA), the roofline denominator of the
+ * integration kernels. */
+int galpy_cuda_fp64_peak(double *tflops, double *ms);
+
+/* Version, last error message of this thread, device count. */
+int galpy_cuda_abi_version(void);
+const char *galpy_cuda_last_error(void);
+int galpy_cuda_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GALPY_CUDA_H */

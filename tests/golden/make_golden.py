@@ -1,0 +1,149 @@
+"""Generate the golden fixtures in tests/golden/ (run in a container that has
+the reference tree and its C build, oracle/_ref/libgalpy_ref.so):
+
+    make -C oracle ref && python tests/golden/make_golden.py
+
+Two kinds of vectors are written to golden.npz:
+
+* from galpy's own Python (imported from the reference tree): the
+  MWPotential2014 argument vector galpy passes to C (_parse_pot), and the
+  Python-side forces, second derivatives and potential values of
+  MWPotential2014 / Hernquist / LogarithmicHalo (axisymmetric and
+  triaxial) at fixed points, plus galpy's pure-Python DOP853 orbits
+  (galpy/util/leung_dop853.py) in MWPotential2014;
+* from the reference's own C integrators (integrateFullOrbit /
+  integratePlanarOrbit / *_dxdv built from its sources into oracle/_ref):
+  small seeded batches for every implemented method, 3D, planar and
+  variational.
+
+The CPU oracle is checked against these in tests/test_oracle.py, so it stays
+pinned on machines that have neither the reference tree nor oracle/_ref.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.dirname(HERE))
+
+from galpy_stub import import_galpy  # noqa: E402
+
+from oracle import oracle as O  # noqa: E402
+
+
+def seeded_ics(n, seed, planar=False):
+    rng = np.random.default_rng(seed)
+    R = rng.uniform(0.5, 2.0, n)
+    vR = rng.normal(0, 0.1, n)
+    vT = 1 + rng.normal(0, 0.1, n)
+    z = rng.normal(0, 0.05, n)
+    vz = rng.normal(0, 0.05, n)
+    phi = rng.uniform(0, 2 * np.pi, n)
+    if planar:
+        return np.stack([R, vR, vT, phi], 1)
+    return np.stack([R, vR, vT, z, vz, phi], 1)
+
+
+def cyl_to_rect(v):
+    if v.shape[-1] == 4:
+        R, vR, vT, phi = v.T
+        return np.stack([R * np.cos(phi), R * np.sin(phi), vR * np.cos(phi) - vT * np.sin(phi),
+                         vR * np.sin(phi) + vT * np.cos(phi)], 1)
+    R, vR, vT, z, vz, phi = v.T
+    return np.stack([R * np.cos(phi), R * np.sin(phi), z, vR * np.cos(phi) - vT * np.sin(phi),
+                     vR * np.sin(phi) + vT * np.cos(phi), vz], 1)
+
+
+def main():
+    galpy = import_galpy()
+    if galpy is None or not O.ref_available():
+        raise SystemExit("needs the reference tree and oracle/_ref (make -C oracle ref)")
+    from galpy import potential as gp
+    from galpy.orbit import Orbit
+    from galpy.orbit.integrateFullOrbit import _parse_pot as parse3
+    from galpy.orbit.integratePlanarOrbit import _parse_pot as parse2
+
+    out = {}
+    mw = gp.MWPotential2014
+    _, pt, pa, _ = parse3(mw)
+    out["mw14_type"] = np.asarray(pt, np.int32)
+    out["mw14_args"] = np.asarray(pa)
+    _, pt2, pa2, _ = parse2(gp.toPlanarPotential(mw))
+    out["mw14_planar_type"] = np.asarray(pt2, np.int32)
+    out["mw14_planar_args"] = np.asarray(pa2)
+
+    # galpy Python forces at fixed points
+    rng = np.random.default_rng(7)
+    R = rng.uniform(0.05, 3.0, 64)
+    z = rng.normal(0, 0.4, 64)
+    phi = rng.uniform(0, 2 * np.pi, 64)
+    out["pts_R"], out["pts_z"], out["pts_phi"] = R, z, phi
+    pots = {
+        "mw14": mw,
+        "hernquist": [gp.HernquistPotential(amp=1.3, a=0.7)],
+        "loghalo": [gp.LogarithmicHaloPotential(normalize=1.0, q=0.9, core=0.2)],
+        "logtri": [gp.LogarithmicHaloPotential(normalize=1.0, q=0.9, core=0.2, b=0.8)],
+        "nfw": [gp.NFWPotential(a=3.0, normalize=0.5)],
+        "mn": [gp.MiyamotoNagaiPotential(a=0.5, b=0.1, normalize=0.7)],
+        "pswc": [gp.PowerSphericalPotentialwCutoff(alpha=1.2, rc=0.5, normalize=0.2)],
+    }
+    for name, p in pots.items():
+        _, t_, a_, _ = parse3(p)
+        out[f"{name}_type"] = np.asarray(t_, np.int32)
+        out[f"{name}_args"] = np.asarray(a_)
+        fns = (gp.evaluateRforces, gp.evaluatezforces, gp.evaluatephitorques,
+               gp.evaluateR2derivs, gp.evaluatez2derivs, gp.evaluateRzderivs,
+               gp.evaluatePotentials)
+        vals = np.stack([np.broadcast_to(np.asarray(f(p, R, z, phi=phi), float), R.shape)
+                         for f in fns], 1)
+        out[f"{name}_pyforces"] = vals
+
+    # galpy pure-Python DOP853 orbits (galpy/util/leung_dop853.py)
+    ics = seeded_ics(3, 11)
+    ts = np.linspace(0.0, 10.0, 101)
+    o = Orbit(ics)
+    o.integrate(ts, mw, method="dop853")
+    out["pydop_ics"] = ics
+    out["pydop_t"] = ts
+    out["pydop_orbit"] = np.stack([o.R(ts), o.vR(ts), o.vT(ts), o.z(ts), o.vz(ts), o.phi(ts)],
+                                  -1)
+
+    # the reference's own C integrators
+    ics = seeded_ics(8, 0)
+    ics2 = seeded_ics(8, 1, planar=True)
+    out["c_ics"], out["c_ics_planar"] = ics, ics2
+    for m in ("leapfrog", "rk4", "symplec4", "dop853"):
+        t = np.linspace(0, 5, 51)
+        res, err, _, _ = O.integrate(ics, t, pt, pa, m, impl="ref")
+        out[f"c_{m}_3d"] = res
+        res, err, _, _ = O.integrate(ics2, t, pt2, pa2, m, planar=True, impl="ref")
+        out[f"c_{m}_planar"] = res
+    # per-orbit time grids, dop853, looser tolerance
+    tend = np.linspace(3.0, 9.0, 8)
+    tt = np.linspace(0, 1, 21)[None, :] * tend[:, None]
+    out["c_indiv_t"] = tt
+    res, _, _, _ = O.integrate(ics, tt, pt, pa, "dop853", rtol=1e-10, atol=1e-10, impl="ref")
+    out["c_dop853_indiv"] = res
+    # variational
+    w = np.zeros((6, 12))
+    w[:, :6] = cyl_to_rect(ics[:6])
+    w[np.arange(6), 6 + np.arange(6)] = 1.0
+    w2 = np.zeros((4, 8))
+    w2[:, :4] = cyl_to_rect(ics2[:4])
+    w2[np.arange(4), 4 + np.arange(4)] = 1.0
+    out["c_dxdv_w3"], out["c_dxdv_w2"] = w, w2
+    t = np.linspace(0, 3, 31)
+    for m in ("leapfrog", "rk4", "symplec4", "dop853"):
+        res, _, _ = O.integrate_dxdv(w, t, pt, pa, m, impl="ref")
+        out[f"c_{m}_dxdv3"] = res
+        res, _, _ = O.integrate_dxdv(w2, t, pt2, pa2, m, planar=True, impl="ref")
+        out[f"c_{m}_dxdv2"] = res
+    np.savez_compressed(os.path.join(HERE, "golden.npz"), **out)
+    print("wrote", os.path.join(HERE, "golden.npz"), len(out), "arrays")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,142 @@
+// tests/harness/host_harness.cpp -- TEST ONLY.
+//
+// Runs the engine's own per-orbit state machines and force library
+// (galpy_b200/csrc/machines.cuh, potentials.cuh) as plain host C++, one
+// orbit after another, so the device code's logic can be compared with the
+// CPU oracle in the CPU-only test suite.  It is never part of the product:
+// the package has no CPU path and refuses to run without its CUDA library.
+#include <vector>
+
+#include "../../galpy_b200/csrc/compile_potential.h"
+#include "../../galpy_b200/csrc/machines.cuh"
+
+using namespace gpc;
+
+namespace {
+struct Rows {
+  double* out;
+  int nv, nt;
+  long long i;
+  void operator()(int j, const double* v) const
+  {
+    for (int k = 0; k < nv; k++) out[(i * nt + j) * nv + k] = v[k];
+  }
+};
+
+template <int D, int PREC, bool VAR>
+struct Force {
+  const GpComp* c;
+  int n;
+  void operator()(const double* q, double* a) const { eval_force<D, PREC, VAR>(c, n, q, a); }
+};
+
+template <class M, int D, int PREC, bool VAR>
+void run_all(int nobj, const double* w, int nt, const double* t, int indiv_t, const GpComp* comps,
+             int ncomp, double dt, double rtol, double atol, long long max_att, double* out,
+             int* err, long long* nsteps)
+{
+  Force<D, PREC, VAR> f{comps, ncomp};
+  std::vector<double> store(M::kSlotDoubles + 1);
+  for (long long i = 0; i < nobj; i++) {
+    M m;
+    m.bind(store.data(), 1);
+    Rows r{out, M::NV, nt, i};
+    m.init(w + i * M::NV, t + (indiv_t ? i * nt : 0), nt, dt, rtol, atol, max_att, r);
+    run_orbit(m, f, r);
+    err[i] = m.err;
+    if (nsteps) nsteps[i] = m.nsteps;
+  }
+}
+
+template <int D, int PREC, bool VAR>
+int dispatch(int method, int nobj, const double* w, int nt, const double* t, int indiv_t,
+             const GpComp* c, int n, double dt, double rtol, double atol, long long ma,
+             double* out, int* err, long long* ns)
+{
+  switch (method) {
+    case M_LEAPFROG:
+      run_all<SymplecticMachine<D, VAR, false>, D, PREC, VAR>(nobj, w, nt, t, indiv_t, c, n, dt,
+                                                              rtol, atol, ma, out, err, ns);
+      return 0;
+    case M_SYMPLEC4:
+      run_all<SymplecticMachine<D, VAR, true>, D, PREC, VAR>(nobj, w, nt, t, indiv_t, c, n, dt,
+                                                             rtol, atol, ma, out, err, ns);
+      return 0;
+    case M_RK4:
+      run_all<RK4Machine<D, VAR>, D, PREC, VAR>(nobj, w, nt, t, indiv_t, c, n, dt, rtol, atol,
+                                                ma, out, err, ns);
+      return 0;
+    case M_DOP853:
+      run_all<Dop853Machine<D, VAR>, D, PREC, VAR>(nobj, w, nt, t, indiv_t, c, n, dt, rtol,
+                                                   atol, ma, out, err, ns);
+      return 0;
+  }
+  return -2;
+}
+}  // namespace
+
+extern "C" int harness_integrate(int planar, int var, int method, int prec, int nobj,
+                                 const double* w, int nt, const double* t, int indiv_t,
+                                 int npot, const int* pot_type, const double* pot_args, double dt,
+                                 double rtol, double atol, long long max_att, double* out,
+                                 int* err, long long* nsteps)
+{
+  std::vector<GpComp> comps(npot);
+  int rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
+  if (rc) return rc;
+  const GpComp* c = comps.data();
+  if (planar) {
+    if (var) return dispatch<2, PREC_FP64, true>(method, nobj, w, nt, t, indiv_t, c, npot, dt,
+                                                 rtol, atol, max_att, out, err, nsteps);
+    if (prec) return dispatch<2, PREC_F32, false>(method, nobj, w, nt, t, indiv_t, c, npot, dt,
+                                                  rtol, atol, max_att, out, err, nsteps);
+    return dispatch<2, PREC_FP64, false>(method, nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol,
+                                         max_att, out, err, nsteps);
+  }
+  if (var) return dispatch<3, PREC_FP64, true>(method, nobj, w, nt, t, indiv_t, c, npot, dt, rtol,
+                                               atol, max_att, out, err, nsteps);
+  if (prec) return dispatch<3, PREC_F32, false>(method, nobj, w, nt, t, indiv_t, c, npot, dt,
+                                                rtol, atol, max_att, out, err, nsteps);
+  return dispatch<3, PREC_FP64, false>(method, nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol,
+                                       max_att, out, err, nsteps);
+}
+
+// accelerations (and tidal tensors) at points, for force-level tests
+extern "C" int harness_forces(int planar, int n, const double* x, const double* y,
+                              const double* z, int npot, const int* pot_type,
+                              const double* pot_args, double* acc /*[n][3]*/,
+                              double* tidal /*[n][6] or NULL*/, double* acc32 /*[n][3] or NULL*/)
+{
+  std::vector<GpComp> comps(npot);
+  int rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
+  if (rc) return rc;
+  for (int i = 0; i < n; i++) {
+    double ax = 0, ay = 0, az = 0, K[6];
+    if (planar)
+      accel<double, true>(comps.data(), npot, x[i], y[i], 0.0, ax, ay, az);
+    else
+      accel<double, false>(comps.data(), npot, x[i], y[i], z[i], ax, ay, az);
+    acc[3 * i] = ax;
+    acc[3 * i + 1] = ay;
+    acc[3 * i + 2] = az;
+    if (tidal) {
+      double bx, by, bz;
+      if (planar)
+        accel_tidal<true>(comps.data(), npot, x[i], y[i], 0.0, bx, by, bz, K);
+      else
+        accel_tidal<false>(comps.data(), npot, x[i], y[i], z[i], bx, by, bz, K);
+      for (int k = 0; k < 6; k++) tidal[6 * i + k] = K[k];
+    }
+    if (acc32) {
+      float fx = 0, fy = 0, fz = 0;
+      if (planar)
+        accel<float, true>(comps.data(), npot, (float)x[i], (float)y[i], 0.f, fx, fy, fz);
+      else
+        accel<float, false>(comps.data(), npot, (float)x[i], (float)y[i], (float)z[i], fx, fy, fz);
+      acc32[3 * i] = fx;
+      acc32[3 * i + 1] = fy;
+      acc32[3 * i + 2] = fz;
+    }
+  }
+  return 0;
+}

@@ -1,0 +1,64 @@
+"""Input generators and coordinate helpers shared by the tests."""
+import numpy as np
+
+
+def seeded_ics(n, seed, planar=False, r_range=(0.5, 2.0), log_r=False):
+    """Config-0 style initial conditions (R, vR, vT, z, vz, phi)."""
+    rng = np.random.default_rng(seed)
+    if log_r:
+        R = np.exp(rng.uniform(np.log(r_range[0]), np.log(r_range[1]), n))
+    else:
+        R = rng.uniform(r_range[0], r_range[1], n)
+    vR = rng.normal(0, 0.1, n)
+    vT = 1 + rng.normal(0, 0.1, n)
+    z = rng.normal(0, 0.05, n)
+    vz = rng.normal(0, 0.05, n)
+    phi = rng.uniform(0, 2 * np.pi, n)
+    if planar:
+        return np.stack([R, vR, vT, phi], 1)
+    return np.stack([R, vR, vT, z, vz, phi], 1)
+
+
+def cyl_to_rect(v):
+    """galpy's cyl_to_rect_galpy / polar_to_rect_galpy on rows."""
+    v = np.asarray(v)
+    if v.shape[-1] == 4:
+        R, vR, vT, phi = (v[..., k] for k in range(4))
+        c, s = np.cos(phi), np.sin(phi)
+        return np.stack([R * c, R * s, vR * c - vT * s, vR * s + vT * c], -1)
+    R, vR, vT, z, vz, phi = (v[..., k] for k in range(6))
+    c, s = np.cos(phi), np.sin(phi)
+    return np.stack([R * c, R * s, z, vR * c - vT * s, vR * s + vT * c, vz], -1)
+
+
+def rect_to_cyl(o):
+    o = np.asarray(o)
+    if o.shape[-1] == 4:
+        x, y, vx, vy = (o[..., k] for k in range(4))
+        phi = np.arctan2(y, x)
+        c, s = np.cos(phi), np.sin(phi)
+        return np.stack([np.hypot(x, y), vx * c + vy * s, -vx * s + vy * c, phi], -1)
+    x, y, z, vx, vy, vz = (o[..., k] for k in range(6))
+    phi = np.arctan2(y, x)
+    c, s = np.cos(phi), np.sin(phi)
+    return np.stack([np.hypot(x, y), vx * c + vy * s, -vx * s + vy * c, z, vz, phi], -1)
+
+
+def cyl_diff(a, b):
+    """|a-b| on cylindrical rows with the angle compared modulo 2 pi."""
+    d = np.abs(np.asarray(a) - np.asarray(b))
+    k = a.shape[-1] - 1
+    d[..., k] = np.abs((a[..., k] - b[..., k] + np.pi) % (2 * np.pi) - np.pi)
+    return d
+
+
+def unit_deviations(w_base, dim):
+    """One row per canonical deviation direction of each base orbit."""
+    n = len(w_base)
+    nv = 2 * dim
+    w = np.zeros((n * nv, 2 * nv))
+    for i in range(n):
+        for j in range(nv):
+            w[i * nv + j, :nv] = w_base[i]
+            w[i * nv + j, nv + j] = 1.0
+    return w

@@ -1,0 +1,99 @@
+"""The C-ABI library: exports, host-side argument handling and loud failure
+without a GPU.  No integration runs here (that needs a GPU)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import galpy_b200
+from galpy_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "galpy_cuda.h")
+
+
+def header_functions():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    txt = "\n".join(ln for ln in txt.splitlines() if not ln.lstrip().startswith("typedef"))
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(\w+)\s*\(", txt, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.lib()
+    names = header_functions()
+    assert "integrateFullOrbit_cuda" in names and "galpy_cuda_integrate_device" in names
+    for n in names:
+        assert hasattr(lib, n), n
+    # and the Python binding knows every one of them
+    assert set(names) == set(_lib.SIGNATURES), set(names) ^ set(_lib.SIGNATURES)
+
+
+def test_abi_version_and_record_size():
+    lib = _lib.lib()
+    assert lib.galpy_cuda_abi_version() == 1
+    assert lib.galpy_cuda_comp_size() == 8 + 8 * 8 + 48 * 8
+
+
+def test_compile_potential_host_only(golden):
+    buf, n = galpy_b200.compile_potential((golden["mw14_type"], golden["mw14_args"]))
+    assert n == 3 and buf.size == 3 * _lib.lib().galpy_cuda_comp_size()
+    rec = buf.reshape(3, -1)
+    assert rec[:, :4].view(np.int32).ravel().tolist() == [15, 5, 9]
+    with pytest.raises(galpy_b200.PotentialNotSupported):
+        galpy_b200.compile_potential(([1], [1.0, 0, 0, 1, 1, 0]))
+
+
+def _no_gpu():
+    return _lib.lib().galpy_cuda_device_count() == 0
+
+
+def test_fails_loudly_without_gpu(mw14):
+    if not _no_gpu():
+        pytest.skip("a GPU is present")
+    yo = np.array([[1.0, 0.1, 1.1, 0.0, 0.0, 0.0]])
+    with pytest.raises(galpy_b200.CudaError) as e:
+        galpy_b200.integrateFullOrbit_cuda(mw14, yo, np.linspace(0, 1, 11), "dop853_cuda")
+    assert e.value.code == _lib.ERR_NODEVICE
+
+
+def test_unsupported_method_is_reported(mw14):
+    lib = _lib.lib()
+    yo = np.array([[1.0, 0.1, 1.1, 0.0, 0.0, 0.0]])
+    t = np.linspace(0, 1, 11)
+    res = np.zeros((1, 11, 6))
+    err = np.zeros(1, np.int32)
+    pt = np.ascontiguousarray(mw14[0], np.int32)
+    pa = np.ascontiguousarray(mw14[1], np.float64)
+    dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    for code in (2, 4, 5, 7):  # rk6, symplec6, dopr54, ias15: galpy falls back
+        rc = lib.integrateFullOrbit_cuda(1, yo.ctypes.data_as(dp), 11, t.ctypes.data_as(dp), 0, 3,
+                                         pt.ctypes.data_as(ip), pa.ctypes.data_as(dp), None,
+                                         -9999.99, -27.6, -27.6, res.ctypes.data_as(dp),
+                                         err.ctypes.data_as(ip), code, _lib.CALLBACK(), None)
+        assert rc in (_lib.ERR_METHOD, _lib.ERR_NODEVICE)
+
+
+def test_parse_integrator_and_tolerances():
+    assert galpy_b200.parse_integrator("symplec4_cuda") == 3
+    assert galpy_b200.parse_integrator("DOP853_CUDA") == 6
+    assert galpy_b200.parse_integrator("leapfrog_c") == 0
+    assert galpy_b200.parse_integrator("rk4") == 1
+    with pytest.raises(ValueError):
+        galpy_b200.parse_integrator("dopr54_cuda")
+    r, a = galpy_b200.parse_tol(None, 1e-10)
+    assert r == pytest.approx(-12 * np.log(10)) and a == pytest.approx(np.log(1e-10))
+
+
+def test_package_has_no_cpu_path():
+    """The package never imports the oracle and has no CPU integrator."""
+    pkg = os.path.join(ROOT, "galpy_b200")
+    for dirpath, _, files in os.walk(pkg):
+        for f in files:
+            if f.endswith((".py", ".cu", ".cuh", ".h")):
+                txt = open(os.path.join(dirpath, f)).read()
+                for needle in ("import oracle", "from oracle", "liboracle", "oracle/",
+                               "libgalpy_ref", "oracle_integrate"):
+                    assert needle not in txt, (f, needle)

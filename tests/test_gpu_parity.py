@@ -1,0 +1,280 @@
+"""CUDA engine vs the CPU oracle on a B200, through the C ABI.
+
+Tolerances: fixed-step methods take the same step size per orbit as the
+reference and agree to the orbits' own conditioning (differences of 1e-16
+in the force grow to ~1e-13 over 1e4 steps; the oracle shows the same growth
+under 1e-16 perturbations of the initial conditions); DOP853 takes the same
+accepted step sequence and agrees well inside its tolerance.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+from helpers import cyl_diff, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
+
+import galpy_b200 as gb
+from galpy_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+METHODS = ["leapfrog", "rk4", "symplec4", "dop853"]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def engine():
+    from galpy_b200 import build
+
+    build.build()
+    n = _lib.lib().galpy_cuda_device_count()
+    assert n > 0, "no CUDA device: GPU tests need a GPU"
+    return _lib.lib()
+
+
+def cuda(method):
+    return method + "_cuda"
+
+
+def test_config0_symplec4_parity(oracle, mw14):
+    """symplec4, MWPotential2014, t in [0,100] with 1001 outputs (config 0
+    at 2,000 orbits so the oracle finishes in seconds)."""
+    pt, pa = mw14
+    ics = seeded_ics(2000, 0)
+    t = np.linspace(0, 100, 1001)
+    ref, eref, nref, _ = oracle.integrate(ics, t, pt, pa, "symplec4")
+    out, err, ns = gb.integrateFullOrbit_cuda((pt, pa), ics.copy(), t, "symplec4_cuda",
+                                              progressbar=False, return_nsteps=True)
+    assert not err.any()
+    same = ns == nref
+    assert same.mean() >= 0.999, same.mean()
+    per = cyl_diff(ref, out).max(axis=(1, 2))[same]
+    assert np.median(per) < 1e-12, np.median(per)
+    assert per.max() < 1e-9, per.max()
+
+
+def test_config0_full_size_energy(mw14, oracle):
+    """All 10,000 config-0 orbits: size-independent checks (energy
+    conservation per orbit, agreement with a 2x smaller step)."""
+    pt, pa = mw14
+    ics = seeded_ics(10000, 0)
+    t = np.linspace(0, 100, 1001)
+    out, err, ns = gb.integrateFullOrbit_cuda((pt, pa), ics.copy(), t, "symplec4_cuda",
+                                              progressbar=False, return_nsteps=True)
+    assert not err.any() and np.isfinite(out).all()
+    E = oracle.energy_cyl(out[:, ::50], pt, pa)
+    rel = np.abs(E / E[:, :1] - 1)
+    assert rel.max() < 1e-8, rel.max()
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("planar", [False, True])
+def test_methods_vs_oracle(oracle, mw14, mw14_planar, method, planar):
+    pt, pa = mw14_planar if planar else mw14
+    ics = seeded_ics(257, 8, planar=planar)
+    t = np.linspace(0, 20, 201)
+    ref, _, nref, _ = oracle.integrate(ics, t, pt, pa, method, planar=planar)
+    fn = gb.integratePlanarOrbit_cuda if planar else gb.integrateFullOrbit_cuda
+    out, err, ns = fn((pt, pa), ics.copy(), t, cuda(method), progressbar=False,
+                      return_nsteps=True)
+    assert not err.any()
+    assert (ns == nref).mean() >= 0.99
+    d = cyl_diff(ref, out).max(axis=(1, 2))[ns == nref]
+    assert d.max() < 1e-10, d.max()
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_golden_reference_vectors(golden, method):
+    """The committed outputs of the reference's own C build."""
+    t = np.linspace(0, 5, 51)
+    out, err = gb.integrateFullOrbit_cuda((golden["mw14_type"], golden["mw14_args"]),
+                                          golden["c_ics"].copy(), t, cuda(method),
+                                          progressbar=False)
+    assert cyl_diff(golden[f"c_{method}_3d"], out).max() < 1e-11
+    out, err = gb.integratePlanarOrbit_cuda(
+        (golden["mw14_planar_type"], golden["mw14_planar_args"]), golden["c_ics_planar"].copy(),
+        t, cuda(method), progressbar=False)
+    assert cyl_diff(golden[f"c_{method}_planar"], out).max() < 1e-11
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("planar", [False, True])
+def test_variational_vs_oracle(oracle, mw14, mw14_planar, method, planar):
+    pt, pa = mw14_planar if planar else mw14
+    dim = 2 if planar else 3
+    w = unit_deviations(cyl_to_rect(seeded_ics(4, 9, planar=planar)), dim)
+    t = np.linspace(0, 5, 51)
+    ref, _, nref = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar)
+    out, err, ns = gb.integrate_dxdv_batch((pt, pa), w, t, cuda(method), planar=planar,
+                                           return_nsteps=True)
+    assert not err.any() and np.array_equal(ns, nref)
+    scale = np.abs(ref).max(axis=1, keepdims=True)
+    assert (np.abs(out - ref) / scale).max() < 1e-10
+    # galpy's single-orbit entry points
+    single = gb.integratePlanarOrbit_dxdv_cuda if planar else gb.integrateFullOrbit_dxdv_cuda
+    res, e = single((pt, pa), w[0, :2 * dim], w[0, 2 * dim:], t, cuda(method))
+    assert e == 0 and np.allclose(res, out[0], rtol=0, atol=1e-12)
+
+
+def test_golden_variational_vectors(golden):
+    t = np.linspace(0, 3, 31)
+    for method in METHODS:
+        out, err = gb.integrate_dxdv_batch((golden["mw14_type"], golden["mw14_args"]),
+                                           golden["c_dxdv_w3"], t, cuda(method))
+        ref = golden[f"c_{method}_dxdv3"]
+        assert (np.abs(out - ref) / np.abs(ref).max(axis=1, keepdims=True)).max() < 1e-10
+
+
+def test_dop853_ragged_times(oracle, mw14):
+    """Config-1 style: log-uniform radii down to 0.05, per-orbit end times,
+    101 snapshots, rtol = atol = 1e-10."""
+    pt, pa = mw14
+    ics = seeded_ics(400, 1, r_range=(0.05, 3.0), log_r=True)
+    rng = np.random.default_rng(1)
+    tend = np.exp(rng.normal(np.log(50), 0.7, len(ics)))
+    t = np.linspace(0, 1, 101)[None, :] * tend[:, None]
+    ref, _, nref, _ = oracle.integrate(ics, t, pt, pa, "dop853", rtol=1e-10, atol=1e-10)
+    out, err, ns = gb.integrateFullOrbit_cuda((pt, pa), ics.copy(), t, "dop853_cuda",
+                                              rtol=1e-10, atol=1e-10, progressbar=False,
+                                              return_nsteps=True)
+    assert not err.any()
+    same = ns == nref
+    assert same.mean() >= 0.98, same.mean()
+    d = cyl_diff(ref, out)[same]
+    scale = np.maximum(np.abs(ref[same]), 1.0)
+    assert (d / scale).max() < 1e-7
+
+
+def test_device_api_soa_matches_galpy_layout(mw14):
+    import torch
+
+    pt, pa = mw14
+    ics = seeded_ics(1000, 21)
+    t = np.linspace(0, 10, 11)
+    res, err = gb.integrateFullOrbit_cuda((pt, pa), ics.copy(), t, "dop853_cuda",
+                                          progressbar=False)
+    comps, n = gb.compile_potential((pt, pa))
+    dev = torch.device("cuda:0")
+    w0 = torch.tensor(cyl_to_rect(ics).T.copy(), device=dev)
+    tt = torch.tensor(t, device=dev)
+    out = torch.empty((6, 11, len(ics)), dtype=torch.float64, device=dev)
+    e = torch.empty(len(ics), dtype=torch.int32, device=dev)
+    gb.integrate_device(torch.tensor(comps, device=dev), n, w0, tt, out, e, "dop853_cuda")
+    torch.cuda.synchronize()
+    got = rect_to_cyl(out.cpu().numpy().transpose(2, 1, 0))
+    assert cyl_diff(res, got).max() < 1e-14 and not e.cpu().numpy().any()
+
+
+def test_potential_groups(oracle, mw14):
+    """Ragged multi-potential batch: every orbit uses its own group's
+    parameters (config-4 style variants of MWPotential2014)."""
+    import torch
+
+    pt, pa = mw14
+    rng = np.random.default_rng(4)
+    ngroup = 5
+    args = np.tile(pa, (ngroup, 1))
+    scale = rng.uniform(0.8, 1.2, (ngroup, 6))
+    args[:, 6] *= scale[:, 0]  # MN a
+    args[:, 7] *= scale[:, 1]  # MN b
+    args[:, 9] *= scale[:, 2]  # NFW a
+    args[:, 0] *= scale[:, 3]
+    args[:, 5] *= scale[:, 4]
+    args[:, 8] *= scale[:, 5]
+    counts = rng.integers(10, 40, ngroup)
+    group = np.repeat(np.arange(ngroup), counts).astype(np.int32)
+    ics = seeded_ics(len(group), 5)
+    t = np.linspace(0, 10, 21)
+    comps, n = gb.compile_potential((pt, args.ravel()), ngroup=ngroup)
+    dev = torch.device("cuda:0")
+    out = torch.empty((6, 21, len(ics)), dtype=torch.float64, device=dev)
+    e = torch.empty(len(ics), dtype=torch.int32, device=dev)
+    gb.integrate_device(torch.tensor(comps, device=dev), n,
+                        torch.tensor(cyl_to_rect(ics).T.copy(), device=dev),
+                        torch.tensor(t, device=dev), out, e, "dop853_cuda",
+                        group=torch.tensor(group, device=dev), rtol=1e-9, atol=1e-9)
+    got = rect_to_cyl(out.cpu().numpy().transpose(2, 1, 0))
+    for g in range(ngroup):
+        sel = group == g
+        ref, _, _, _ = oracle.integrate(ics[sel], t, pt, args[g], "dop853", rtol=1e-9, atol=1e-9)
+        assert cyl_diff(ref, got[sel]).max() < 1e-8
+
+
+def test_f32_force_variant(mw14):
+    pt, pa = mw14
+    ics = seeded_ics(512, 22)
+    t = np.linspace(0, 10, 11)
+    a, _ = gb.integrateFullOrbit_cuda((pt, pa), ics.copy(), t, "symplec4_cuda", dt=0.01,
+                                      progressbar=False)
+    b, _ = gb.integrateFullOrbit_cuda((pt, pa), ics.copy(), t, "symplec4_cuda", dt=0.01,
+                                      progressbar=False, precision="f32force")
+    d = cyl_diff(a, b)[..., :5].max()
+    assert 0 < d < 1e-4, d
+
+
+def test_edge_cases(mw14, oracle):
+    pt, pa = mw14
+    t = np.linspace(0, 5, 11)
+    # no orbits
+    out, err = gb.integrateFullOrbit_cuda((pt, pa), np.zeros((0, 6)), t, "dop853_cuda")
+    assert out.shape == (0, 11, 6)
+    # one orbit given as a 1-D array; yo overwritten with rectangular coords
+    yo = seeded_ics(1, 30)[0].copy()
+    yo0 = yo.copy()
+    out, err = gb.integrateFullOrbit_cuda((pt, pa), yo, t, "symplec4_cuda")
+    assert out.shape == (11, 6) and err == 0
+    assert np.allclose(yo, cyl_to_rect(yo0[None])[0], rtol=0, atol=1e-15)
+    assert np.allclose(out[0], yo0)
+    # a single output time
+    out, err = gb.integrateFullOrbit_cuda((pt, pa), seeded_ics(3, 31), t[:1], "rk4_cuda")
+    assert out.shape == (3, 1, 6)
+    # backward integration
+    ics = seeded_ics(64, 32)
+    tb = np.linspace(0, -10, 101)
+    for m in METHODS:
+        ref, _, _, _ = oracle.integrate(ics, tb, pt, pa, m)
+        out, err = gb.integrateFullOrbit_cuda((pt, pa), ics.copy(), tb, cuda(m),
+                                              progressbar=False)
+        assert cyl_diff(ref, out).max() < 1e-10
+    # non-finite initial condition: err 3, NaN rows, neighbours unaffected
+    ics = seeded_ics(5, 33)
+    ics[2, 0] = np.nan
+    out, err = gb.integrateFullOrbit_cuda((pt, pa), ics.copy(), t, "dop853_cuda",
+                                          progressbar=False)
+    assert err.tolist() == [0, 0, 3, 0, 0] and np.isnan(out[2, 1:]).all()
+    # attempt budget
+    out, err = gb.integrateFullOrbit_cuda((pt, pa), seeded_ics(4, 34), np.linspace(0, 100, 11),
+                                          "dop853_cuda", max_attempts=30, progressbar=False)
+    assert np.all(err == 2) and np.isnan(out[:, -1]).all()
+    # unsupported method and potential: typed errors
+    with pytest.raises(ValueError):
+        gb.integrateFullOrbit_cuda((pt, pa), seeded_ics(2, 35), t, "dopr54_cuda")
+    with pytest.raises(gb.PotentialNotSupported):
+        gb.integrateFullOrbit_cuda(([14], [1.0, 1.0]), seeded_ics(2, 35), t, "dop853_cuda")
+
+
+def test_progress_callback(mw14):
+    pt, pa = mw14
+    calls = []
+    cb = _lib.CALLBACK(lambda: calls.append(1))
+    ics = seeded_ics(300, 40)
+    t = np.linspace(0, 10, 11)
+    yo = np.ascontiguousarray(ics)
+    res = np.empty((300, 11, 6))
+    err = np.zeros(300, np.int32)
+    pti = np.ascontiguousarray(pt, np.int32)
+    pad = np.ascontiguousarray(pa, np.float64)
+    dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    rc = _lib.lib().integrateFullOrbit_cuda(
+        300, yo.ctypes.data_as(dp), 11, t.ctypes.data_as(dp), 0, 3, pti.ctypes.data_as(ip),
+        pad.ctypes.data_as(dp), None, -9999.99, -27.6, -27.6, res.ctypes.data_as(dp),
+        err.ctypes.data_as(ip), 6, cb, None)
+    assert rc == 0 and len(calls) == 300
+
+
+def test_energy_conservation_gpu(oracle, mw14):
+    """galpy's energy criterion (tests/test_orbit.py:111) on GPU output."""
+    pt, pa = mw14
+    ics = seeded_ics(64, 41)
+    t = np.linspace(0, 14, 501)
+    for m in METHODS:
+        out, err = gb.integrateFullOrbit_cuda((pt, pa), ics.copy(), t, cuda(m), progressbar=False)
+        E = oracle.energy_cyl(out, pt, pa)
+        assert np.all((E.std(1) / E.mean(1)) ** 2 < 1e-10), m

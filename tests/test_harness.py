@@ -1,0 +1,128 @@
+"""The engine's device code (galpy_b200/csrc: force library + per-orbit
+stepper state machines), compiled as host C++ by the test-only harness,
+against the CPU oracle.  This checks the kernel logic on every CPU-only run;
+tests/test_gpu_parity.py checks the compiled kernels on the GPU."""
+import numpy as np
+import pytest
+from helpers import cyl_diff, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
+
+METHODS = ["leapfrog", "rk4", "symplec4", "dop853"]
+POTS = ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"]
+
+
+@pytest.mark.parametrize("name", POTS)
+def test_forces_and_tidal_tensor(harness, oracle, golden, name):
+    pt, pa = golden[f"{name}_type"], golden[f"{name}_args"]
+    R, z, phi = golden["pts_R"], golden["pts_z"], golden["pts_phi"]
+    x, y = R * np.cos(phi), R * np.sin(phi)
+    acc, K, a32 = harness.forces(x, y, z, pt, pa)
+    f = oracle.forces(R, z, phi, pt, pa)
+    Rf, zf, ptq, R2, z2, Rz, p2, Rp, zp = f.T
+    c, s = x / R, y / R
+    ref = np.stack([c * Rf - s / R * ptq, s * Rf + c / R * ptq, zf], 1)
+    # NFW at r << a cancels two terms; the reference (log(1+x)) is the less
+    # accurate side there (this code uses log1p)
+    assert (np.abs(acc - ref).max(1) / np.abs(ref).max(1)).max() < 1e-12
+    Kxx = -c * c * R2 + 2 * c * s / R / R * ptq + s * s / R * Rf + 2 * s * c / R * Rp - s * s / R / R * p2
+    Kxy = (-s * c * R2 + (s * s - c * c) / R / R * ptq - c * s / R * Rf - (c * c - s * s) / R * Rp
+           + c * s / R / R * p2)
+    Kyy = -s * s * R2 - 2 * s * c / R / R * ptq - 2 * s * c / R * Rp + c * c / R * Rf - c * c / R / R * p2
+    Kref = np.stack([Kxx, Kxy, Kyy, -c * Rz + s / R * zp, -s * Rz - c / R * zp, -z2], 1)
+    assert (np.abs(K - Kref).max(1) / np.abs(Kref).max(1)).max() < 1e-12
+    # float32 force evaluation: single-precision accuracy
+    assert (np.abs(a32 - ref).max(1) / np.abs(ref).max(1)).max() < 3e-5
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("planar", [False, True])
+def test_orbits_vs_oracle(harness, oracle, mw14, mw14_planar, method, planar):
+    pt, pa = mw14_planar if planar else mw14
+    ics = seeded_ics(24, 8, planar=planar)
+    t = np.linspace(0, 20, 201)
+    ref, eref, nref, _ = oracle.integrate(ics, t, pt, pa, method, planar=planar)
+    out, err, ns = harness.integrate(cyl_to_rect(ics), t, pt, pa, method, planar=planar)
+    assert not err.any() and not eref.any()
+    assert np.array_equal(ns, nref), "step sequence differs from the reference"
+    assert cyl_diff(ref, rect_to_cyl(out)).max() < 1e-11
+
+
+def test_config0_symplec4_conditioning(harness, oracle, mw14):
+    """t in [0,100], 1001 outputs: same step size per orbit, and differences
+    at the level of the orbits' own sensitivity to 1e-16 perturbations."""
+    pt, pa = mw14
+    ics = seeded_ics(48, 0)
+    t = np.linspace(0, 100, 1001)
+    ref, _, nref, _ = oracle.integrate(ics, t, pt, pa, "symplec4")
+    out, _, ns = harness.integrate(cyl_to_rect(ics), t, pt, pa, "symplec4")
+    assert np.array_equal(ns, nref)
+    per_orbit = cyl_diff(ref, rect_to_cyl(out)).max(axis=(1, 2))
+    assert np.median(per_orbit) < 1e-12
+    assert per_orbit.max() < 1e-10
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("planar", [False, True])
+def test_variational_vs_oracle(harness, oracle, mw14, mw14_planar, method, planar):
+    pt, pa = mw14_planar if planar else mw14
+    dim = 2 if planar else 3
+    w = unit_deviations(cyl_to_rect(seeded_ics(2, 9, planar=planar)), dim)
+    t = np.linspace(0, 5, 51)
+    ref, _, nref = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar)
+    out, err, ns = harness.integrate(w, t, pt, pa, method, planar=planar, var=True)
+    assert not err.any()
+    assert np.array_equal(ns, nref)
+    scale = np.abs(ref).max(axis=1, keepdims=True)
+    assert (np.abs(out - ref) / scale).max() < 1e-10
+
+
+def test_dop853_per_orbit_times(harness, oracle, golden):
+    pt, pa = golden["mw14_type"], golden["mw14_args"]
+    ics = golden["c_ics"]
+    out, err, _ = harness.integrate(cyl_to_rect(ics), golden["c_indiv_t"], pt, pa, "dop853",
+                                    rtol=1e-10, atol=1e-10)
+    assert not err.any()
+    assert cyl_diff(golden["c_dop853_indiv"], rect_to_cyl(out)).max() < 1e-10
+
+
+def test_backward_integration(harness, oracle, mw14):
+    pt, pa = mw14
+    ics = seeded_ics(8, 12)
+    t = np.linspace(0, -10, 101)
+    for method in METHODS:
+        ref, _, nref, _ = oracle.integrate(ics, t, pt, pa, method)
+        out, err, ns = harness.integrate(cyl_to_rect(ics), t, pt, pa, method)
+        assert np.array_equal(ns, nref)
+        assert cyl_diff(ref, rect_to_cyl(out)).max() < 1e-11
+
+
+def test_fixed_dt(harness, oracle, mw14):
+    pt, pa = mw14
+    ics = seeded_ics(8, 13)
+    t = np.linspace(0, 10, 11)
+    for method in ("leapfrog", "symplec4", "rk4"):
+        ref, _, nref, _ = oracle.integrate(ics, t, pt, pa, method, dt=0.01)
+        out, err, ns = harness.integrate(cyl_to_rect(ics), t, pt, pa, method, dt=0.01)
+        assert np.array_equal(ns, nref) and nref[0] == 1000
+        assert cyl_diff(ref, rect_to_cyl(out)).max() < 1e-11
+
+
+def test_attempt_budget_and_nonfinite(harness, mw14):
+    pt, pa = mw14
+    ics = seeded_ics(3, 14)
+    t = np.linspace(0, 50, 51)
+    out, err, ns = harness.integrate(cyl_to_rect(ics), t, pt, pa, "dop853", max_attempts=20)
+    assert np.all(err == 2)
+    assert np.isnan(out[:, -1]).all() and np.isfinite(out[:, 0]).all()
+    w = cyl_to_rect(ics)
+    w[1, 0] = np.nan
+    for method in METHODS:
+        out, err, ns = harness.integrate(w, t[:5], pt, pa, method, dt=0.01)
+        assert err[1] == 3 and err[0] == 0 and err[2] == 0
+        assert np.isnan(out[1, 1:]).all()
+
+
+def test_single_output_row(harness, mw14):
+    pt, pa = mw14
+    w = cyl_to_rect(seeded_ics(2, 15))
+    out, err, ns = harness.integrate(w, np.array([0.0]), pt, pa, "dop853")
+    assert np.array_equal(out[:, 0], w) and not err.any()

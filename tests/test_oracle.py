@@ -1,0 +1,116 @@
+"""The CPU oracle (oracle/galpy_oracle.c) pinned against the reference.
+
+* bit-for-bit against the reference's own C integrators built from its
+  sources (oracle/_ref), when that build is present;
+* against the committed golden vectors made from the reference's C build and
+  from galpy's Python (tests/golden/make_golden.py), everywhere;
+* against scipy for the incomplete gamma function of the bulge mass (the
+  reference calls GSL there, which is not part of the reference tree).
+"""
+import numpy as np
+import pytest
+from helpers import cyl_to_rect, seeded_ics
+
+METHODS = ["leapfrog", "rk4", "symplec4", "dop853"]
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("planar", [False, True])
+def test_oracle_bitwise_vs_reference_build(oracle, mw14, mw14_planar, method, planar):
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref not built here (needs the reference tree)")
+    pt, pa = mw14_planar if planar else mw14
+    ics = seeded_ics(16, 3, planar=planar)
+    t = np.linspace(0, 20, 201)
+    a, ea, _, _ = oracle.integrate(ics, t, pt, pa, method, planar=planar)
+    b, eb, _, _ = oracle.integrate(ics, t, pt, pa, method, planar=planar, impl="ref")
+    assert np.array_equal(a, b)
+    assert np.array_equal(ea, eb)
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("planar", [False, True])
+def test_oracle_dxdv_bitwise_vs_reference_build(oracle, mw14, mw14_planar, method, planar):
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref not built here (needs the reference tree)")
+    pt, pa = mw14_planar if planar else mw14
+    dim = 2 if planar else 3
+    ics = seeded_ics(2 * dim, 4, planar=planar)
+    w = np.zeros((2 * dim, 4 * dim))
+    w[:, :2 * dim] = cyl_to_rect(ics)
+    w[np.arange(2 * dim), 2 * dim + np.arange(2 * dim)] = 1.0
+    t = np.linspace(0, 4, 41)
+    a, _, _ = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar)
+    b, _, _ = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar, impl="ref")
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_oracle_matches_golden_c_vectors(oracle, golden, method):
+    pt, pa = golden["mw14_type"], golden["mw14_args"]
+    t = np.linspace(0, 5, 51)
+    a, _, _, _ = oracle.integrate(golden["c_ics"], t, pt, pa, method)
+    np.testing.assert_allclose(a, golden[f"c_{method}_3d"], rtol=0, atol=1e-13)
+    pt2, pa2 = golden["mw14_planar_type"], golden["mw14_planar_args"]
+    a, _, _, _ = oracle.integrate(golden["c_ics_planar"], t, pt2, pa2, method, planar=True)
+    np.testing.assert_allclose(a, golden[f"c_{method}_planar"], rtol=0, atol=1e-13)
+    t = np.linspace(0, 3, 31)
+    a, _, _ = oracle.integrate_dxdv(golden["c_dxdv_w3"], t, pt, pa, method)
+    np.testing.assert_allclose(a, golden[f"c_{method}_dxdv3"], rtol=0, atol=1e-12)
+    a, _, _ = oracle.integrate_dxdv(golden["c_dxdv_w2"], t, pt2, pa2, method, planar=True)
+    np.testing.assert_allclose(a, golden[f"c_{method}_dxdv2"], rtol=0, atol=1e-12)
+
+
+def test_oracle_indiv_t_golden(oracle, golden):
+    a, _, _, _ = oracle.integrate(golden["c_ics"], golden["c_indiv_t"], golden["mw14_type"],
+                                  golden["mw14_args"], "dop853", rtol=1e-10, atol=1e-10)
+    np.testing.assert_allclose(a, golden["c_dop853_indiv"], rtol=0, atol=1e-13)
+
+
+def test_incomplete_gamma_vs_scipy(oracle):
+    from scipy.special import gammainc
+
+    worst = 0.0
+    for a in (0.1, 0.6, 0.9, 1.2, 2.5, 7.0):
+        for x in np.concatenate([np.geomspace(1e-6, 300, 400), [a + 1 - 1e-12, a + 1]]):
+            ref = gammainc(a, x)
+            got = oracle.gammainc_P(a, x)
+            worst = max(worst, abs(got - ref) / max(ref, 1e-300))
+    assert worst < 5e-14, worst
+
+
+@pytest.mark.parametrize("name", ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"])
+def test_oracle_forces_vs_galpy_python(oracle, golden, name):
+    """C-side formulas restated in the oracle agree with galpy's Python
+    potentials (different code, same mathematics)."""
+    pt, pa = golden[f"{name}_type"], golden[f"{name}_args"]
+    R, z, phi = golden["pts_R"], golden["pts_z"], golden["pts_phi"]
+    py = golden[f"{name}_pyforces"]
+    f = oracle.forces(R, z, phi, pt, pa)
+    pot = oracle.potential(R, z, phi, pt, pa)
+    got = np.stack([f[:, 0], f[:, 1], f[:, 2], f[:, 3], f[:, 4], f[:, 5], pot], 1)
+    scale = np.abs(py).max(0) + 1e-300
+    err = np.abs(got - py) / scale
+    assert err.max() < 1e-11, err.max(0)
+
+
+def test_oracle_dop853_vs_galpy_python_dop853(oracle, golden):
+    """The C DOP853 (default tol 1e-12) against galpy's pure-Python DOP853."""
+    a, _, _, _ = oracle.integrate(golden["pydop_ics"], golden["pydop_t"], golden["mw14_type"],
+                                  golden["mw14_args"], "dop853")
+    d = np.abs(a - golden["pydop_orbit"])
+    d[..., 5] = np.abs((a[..., 5] - golden["pydop_orbit"][..., 5] + np.pi) % (2 * np.pi) - np.pi)
+    assert d.max() < 1e-7, d.max()
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_oracle_energy_conservation(oracle, mw14, method):
+    """galpy's test_energy_jacobi_conservation criterion
+    (tests/test_orbit.py:111, conftest.py:656): (std E / mean E)^2 < 1e-10."""
+    pt, pa = mw14
+    ics = seeded_ics(4, 5)
+    t = np.linspace(0, 14, 501)
+    res, err, _, _ = oracle.integrate(ics, t, pt, pa, method)
+    assert not err.any()
+    E = oracle.energy_cyl(res, pt, pa)
+    assert np.all((E.std(1) / E.mean(1)) ** 2 < 1e-10)
