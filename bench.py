@@ -189,6 +189,7 @@ def main():
     ics, t = workload(args.orbits, seed=1 + 1000 * rank)
     n = len(ics)
     comps, ncomp = gb.compile_potential((pt, pa))
+    sig = gb.signature((pt, pa))
     comps_d = torch.tensor(comps, device=dev)
     w0 = torch.tensor(cyl_to_rect(ics).T.copy(), device=dev)
     t_d = torch.tensor(t, device=dev)
@@ -199,7 +200,8 @@ def main():
 
     def run(precision="fp64"):
         gb.integrate_device(comps_d, ncomp, w0, t_d, out, err, "dop853_cuda", nsteps=nsteps,
-                            rtol=RTOL, atol=ATOL, precision=precision, stream=stream)
+                            rtol=RTOL, atol=ATOL, precision=precision, stream=stream,
+                            signature=sig)
 
     def timed(precision, K, W):
         for _ in range(W):

@@ -16,7 +16,8 @@ from ._lib import (CudaError, CudaLibraryMissing, MethodNotSupported,  # noqa: F
 from .integrate import (CUDA_METHODS, compile_potential, integrate_device,  # noqa: F401
                         integrate_dxdv_batch, integrateFullOrbit_cuda,
                         integrateFullOrbit_dxdv_cuda, integratePlanarOrbit_cuda,
-                        integratePlanarOrbit_dxdv_cuda, parse_integrator, parse_tol)
+                        integratePlanarOrbit_dxdv_cuda, parse_integrator, parse_tol,
+                        signature)
 from .potentials import (HernquistPotential, LogarithmicHaloPotential,  # noqa: F401
                          MiyamotoNagaiPotential, MWPotential2014, NFWPotential,
                          PowerSphericalPotentialwCutoff, parse_pot)

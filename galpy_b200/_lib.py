@@ -57,6 +57,8 @@ class GalpyCudaOpts(ctypes.Structure):
         ("max_attempts", ctypes.c_longlong),
         ("nsteps", ctypes.POINTER(ctypes.c_longlong)),
         ("elapsed_ms", ctypes.POINTER(ctypes.c_double)),
+        ("variant", ctypes.c_int),
+        ("schedule", ctypes.c_int),
     ]
 
 
@@ -88,6 +90,9 @@ class GalpyCudaLaunch(ctypes.Structure):
         ("stream", ctypes.c_void_p),
         ("block_size", ctypes.c_int),
         ("grid_size", ctypes.c_int),
+        ("signature", ctypes.c_int),
+        ("schedule", ctypes.c_int),
+        ("variant", ctypes.c_int),
     ]
 
 
@@ -108,6 +113,7 @@ SIGNATURES = {
     "galpy_cuda_last_error": (ctypes.c_char_p, []),
     "galpy_cuda_device_count": (_ci, []),
     "galpy_cuda_comp_size": (_ci, []),
+    "galpy_cuda_signature": (_ci, [_ci, _ip]),
     "galpy_cuda_compile_potential": (_ci, [_ci, _ci, _ip, _dp, _ci, _vp]),
     "integrateFullOrbit_cuda": (
         _ci,
@@ -168,7 +174,7 @@ def check(code):
 
 
 def make_opts(precision=FP64, device=-1, block_size=0, max_attempts=0, nsteps=None,
-              elapsed=None):
+              elapsed=None, variant=0, schedule=1):
     o = GalpyCudaOpts()
     o.size = ctypes.sizeof(GalpyCudaOpts)
     o.device = device
@@ -179,4 +185,6 @@ def make_opts(precision=FP64, device=-1, block_size=0, max_attempts=0, nsteps=No
         o.nsteps = nsteps.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))
     if elapsed is not None:
         o.elapsed_ms = ctypes.pointer(elapsed)
+    o.variant = variant
+    o.schedule = schedule
     return o

@@ -28,6 +28,51 @@ inline int galpy_nargs(int type, int planar)
   }
 }
 
+// gamma*(a, u) = P(a, u) / u^a = e^-u sum_n u^n / Gamma(a+n+1) in extended
+// precision (all terms positive: no cancellation).
+inline long double gamma_star_ld(long double a, long double u)
+{
+  long double term = 1.0L / tgammal(a + 1.0L), sum = term;
+  for (int n = 1; n < 2000; n++) {
+    term *= u / (a + n);
+    sum += term;
+    if (term < 1e-22L * sum) break;
+  }
+  return sum * expl(-u);
+}
+
+// Smallest integer U with Q(a, U) ~ U^(a-1) e^-U / Gamma(a) below 1e-18, so
+// that P(a, u) = 1 in double precision for u >= U.
+inline double gamma_star_cutoff(double a)
+{
+  long double U = 20.0L;
+  while (expl(-U) * powl(U, (long double)a - 1.0L) / tgammal((long double)a) > 1e-18L) U += 1.0L;
+  return (double)U;
+}
+
+// Chebyshev interpolation of gamma*(a, u) on kChebN equal intervals of
+// [0, U], kChebC nodes each (values at the Chebyshev points, coefficients
+// by the discrete cosine sums), computed in long double.
+inline void build_gamma_star_table(double a, double U, double (*cheb)[kChebC])
+{
+  const long double w = (long double)U / kChebN;
+  const long double pi = 3.141592653589793238462643383279502884L;
+  long double f[kChebC];
+  for (int k = 0; k < kChebN; k++) {
+    for (int i = 0; i < kChebC; i++) {
+      const long double x = cosl(pi * (i + 0.5L) / kChebC);
+      f[i] = gamma_star_ld((long double)a, w * (k + 0.5L * (x + 1.0L)));
+    }
+    for (int j = 0; j < kChebC; j++) {
+      long double s = 0.0L;
+      for (int i = 0; i < kChebC; i++) s += f[i] * cosl(pi * j * (i + 0.5L) / kChebC);
+      s *= 2.0L / kChebC;
+      if (j == 0) s *= 0.5L;
+      cheb[k][j] = (double)s;
+    }
+  }
+}
+
 // Compile one group.  Returns 0, -3 (unsupported type) or -1 (bad args).
 // *consumed receives the number of pot_args read.
 inline int compile_group(int planar, int npot, const int* pot_type, const double* pot_args,
@@ -49,14 +94,16 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
         const double alpha = p[1], rc = p[2];
         const double a = 1.5 - 0.5 * alpha;
         if (!(a > 0.0) || !(rc > 0.0)) return -1;
+        const double mnorm = 2.0 * M_PI * pow(rc, 3.0 - alpha) * (double)tgammal((long double)a);
         c.c[1] = 1.0 / (rc * rc);
-        c.c[2] = a;
-        c.c[3] = lgamma(a);
-        c.c[4] = 2.0 * M_PI * pow(rc, 3.0 - alpha) * tgamma(a);
-        c.c[5] = -0.5 * alpha;
-        c.c[6] = 4.0 * M_PI;
-        c.c[7] = alpha;
-        for (int n = 1; n <= kSeriesTerms; n++) c.inv_ap[n - 1] = 1.0 / (a + n);
+        c.c[2] = mnorm * pow(rc, -2.0 * a);
+        c.c[3] = -0.5 * alpha;
+        c.c[4] = mnorm;
+        const double U = gamma_star_cutoff(a);
+        c.c[5] = U;
+        c.c[6] = kChebN / U;
+        c.c[7] = 4.0 * M_PI;
+        build_gamma_star_table(a, U, c.cheb);
         break;
       }
       case T_MN:
@@ -76,9 +123,7 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
         c.c[2] = core2;
         // galpy passes 1 - 1/b^2 for a triaxial halo and 2.0 (> 1) when
         // axisymmetric (integrateFullOrbit.py:69-73)
-        const bool tri = om < 1.0;
-        c.c[3] = tri ? 1.0 - om : 1.0;
-        c.c[4] = tri ? 1.0 : 0.0;
+        c.c[3] = om < 1.0 ? 1.0 - om : 1.0;
         break;
       }
     }

@@ -20,6 +20,7 @@
 //   * Output rows are written directly in the requested layout: galpy's AoS
 //     cylindrical rows for the drop-in entry points, or coalesced SoA rows
 //     for device-resident batch use.
+#include <cub/device/device_radix_sort.cuh>
 #include <cuda_runtime.h>
 #include <signal.h>
 #include <stdio.h>
@@ -74,6 +75,8 @@ struct KArgs {
   unsigned long long* counter;
   const int* abort_flag;
   unsigned long long* done_count;
+  const int* order;  // work-queue order (longest first), or NULL
+  int variational_nv; // values per input row of variational runs (0 otherwise)
 };
 
 template <int NV, int D, bool CYL_OK>
@@ -98,8 +101,10 @@ __device__ __forceinline__ void load_state(const KArgs& A, long long i, double* 
   }
 }
 
-template <class M, int D, int PREC, bool VAR>
-__global__ void __launch_bounds__(128) orbit_kernel(const KArgs A)
+// MINB: minimum resident blocks per SM requested from the register
+// allocator (1 = no cap; larger values trade registers for occupancy).
+template <class M, int D, int PREC, bool VAR, class POT, int MINB>
+__global__ void __launch_bounds__(128, MINB) orbit_kernel(const KArgs A)
 {
   constexpr bool CYL_OK = !VAR;
   using Rows = DevRows<M::NV, D, CYL_OK>;
@@ -114,6 +119,7 @@ __global__ void __launch_bounds__(128) orbit_kernel(const KArgs A)
     if (!active) {
       i = (long long)atomicAdd(A.counter, 1ULL);
       if (i >= A.nobj) break;
+      if (A.order) i = A.order[i];
       if (aborting) {
         A.err[i] = E_ABORT;
         write_nan_rows<M::NV, D, CYL_OK>(A.out, i, 0);
@@ -127,15 +133,19 @@ __global__ void __launch_bounds__(128) orbit_kernel(const KArgs A)
              A.max_attempts, rows);
       active = true;
     }
+    // slot of the fixed stage cycle (DOP853): the iteration counter is the
+    // same in every lane of the warp
+    const int slot = (int)(iter % 15u);
     if (!m.done) {
       double y[M::NY], q[M::NA], a[M::NA];
-      m.point(y);
+      m.point(y, slot);
       M::pos(y, q);
-      eval_force<D, PREC, VAR>(comps, A.ncomp, q, a);
+      eval_force<D, PREC, VAR, POT>(comps, A.ncomp, q, a);
       Rows rows{&A.out, i};
-      m.consume(y, a, rows);
+      m.consume(y, a, rows, slot);
     }
-    if (A.abort_flag && ((++iter & 255u) == 0u) &&
+    ++iter;
+    if (A.abort_flag && ((iter & 255u) == 0u) &&
         *reinterpret_cast<const volatile int*>(A.abort_flag)) {
       aborting = true;
       if (!m.done) {
@@ -155,6 +165,41 @@ __global__ void __launch_bounds__(128) orbit_kernel(const KArgs A)
 }
 
 // ----------------------------------------------------------------------------
+// longest-first scheduling: estimated cost of each orbit
+// ----------------------------------------------------------------------------
+// cost ~ |t_end - t_0| * Omega, Omega^2 = |a . x| / |x|^2 at the initial
+// point (the local orbital frequency): the number of steps of any of the
+// integrators grows with the number of orbital periods covered.  Orbits are
+// handed out in decreasing order of this estimate so that the longest ones
+// start first and the batch does not end with a few long orbits running
+// alone.
+template <int D>
+__global__ void __launch_bounds__(256) cost_kernel(const KArgs A, float* key, int* idx)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= A.nobj) return;
+  double q[3] = {0.0, 0.0, 0.0}, a[3] = {0.0, 0.0, 0.0};
+  const int nv = 2 * D;
+  for (int k = 0; k < D; k++)
+    q[k] = A.in_layout == GALPY_CUDA_IN_SOA ? A.w0[(long long)k * A.nobj + i]
+                                             : A.w0[i * (long long)(A.variational_nv ? A.variational_nv : nv) + k];
+  const GpComp* comps = A.comps + (A.group ? (long long)A.group[i] * A.ncomp : 0LL);
+  eval_force<D, PREC_FP64, false, DynPot>(comps, A.ncomp, q, a);
+  double ax = 0.0, xx = 0.0;
+  for (int k = 0; k < D; k++) {
+    ax += a[k] * q[k];
+    xx += q[k] * q[k];
+  }
+  const double* tt = A.t + (A.indiv_t ? i * (long long)A.nt : 0LL);
+  const double span = fabs(tt[A.nt - 1] - tt[0]);
+  const double om = sqrt(fabs(ax) / (xx > 0.0 ? xx : 1e-300));
+  float k = (float)(span * om);
+  if (!isfinite(k)) k = 0.f;
+  key[i] = k;
+  idx[i] = (int)i;
+}
+
+// ----------------------------------------------------------------------------
 // launch plumbing
 // ----------------------------------------------------------------------------
 using KernelFn = void (*)(const KArgs);
@@ -164,39 +209,65 @@ struct KernelInfo {
   int slot_doubles = 0;  // per-thread shared-memory slot store (doubles)
 };
 
-template <class M, int D, int PREC, bool VAR>
-static KernelInfo info_of()
+// Register-budget variants (chosen by the autotuner, galpy_b200/autotune.py):
+// variant 0 lets the compiler use up to 255 registers; variant 1 caps them
+// so that more blocks are resident (3 blocks/SM for DOP853, whose shared
+// slot store allows at most 3; 4 blocks/SM for the lighter integrators).
+template <class M, int D, int PREC, bool VAR, class POT>
+static KernelInfo info_of(int variant)
 {
   KernelInfo k;
-  k.fn = orbit_kernel<M, D, PREC, VAR>;
+  constexpr int capped = M::kSlotDoubles > 0 ? 3 : 4;
+  if (variant == 1 && !VAR)
+    k.fn = orbit_kernel<M, D, PREC, VAR, POT, capped>;
+  else
+    k.fn = orbit_kernel<M, D, PREC, VAR, POT, 1>;
   k.slot_doubles = M::kSlotDoubles;
   return k;
 }
 
-template <int D, int PREC, bool VAR>
-static KernelInfo pick_kernel_dim(int method)
+template <int D, int PREC, bool VAR, class POT>
+static KernelInfo pick_kernel_dim(int method, int variant)
 {
   switch (method) {
-    case M_LEAPFROG: return info_of<SymplecticMachine<D, VAR, false>, D, PREC, VAR>();
-    case M_SYMPLEC4: return info_of<SymplecticMachine<D, VAR, true>, D, PREC, VAR>();
-    case M_RK4: return info_of<RK4Machine<D, VAR>, D, PREC, VAR>();
-    case M_DOP853: return info_of<Dop853Machine<D, VAR>, D, PREC, VAR>();
+    case M_LEAPFROG: return info_of<SymplecticMachine<D, VAR, false>, D, PREC, VAR, POT>(variant);
+    case M_SYMPLEC4: return info_of<SymplecticMachine<D, VAR, true>, D, PREC, VAR, POT>(variant);
+    case M_RK4: return info_of<RK4Machine<D, VAR>, D, PREC, VAR, POT>(variant);
+    case M_DOP853: return info_of<Dop853Machine<D, VAR>, D, PREC, VAR, POT>(variant);
   }
   return KernelInfo();
 }
 
-static KernelInfo pick_kernel(int planar, int var, int prec, int method)
+template <int PREC, class POT>
+static KernelInfo pick_plain(int planar, int method, int variant)
+{
+  return planar ? pick_kernel_dim<2, PREC, false, POT>(method, variant)
+                : pick_kernel_dim<3, PREC, false, POT>(method, variant);
+}
+
+// sig: GALPY_CUDA_SIG_MW14 selects the kernels with the MWPotential2014
+// component list fixed at compile time (plain runs); variational runs walk
+// the component list at run time.
+static KernelInfo pick_kernel(int planar, int var, int prec, int method, int sig, int variant)
 {
   if (var) {
     if (prec != GALPY_CUDA_FP64) return KernelInfo();  // variational runs are float64 only
-    return planar ? pick_kernel_dim<2, PREC_FP64, true>(method)
-                  : pick_kernel_dim<3, PREC_FP64, true>(method);
+    return planar ? pick_kernel_dim<2, PREC_FP64, true, DynPot>(method, 0)
+                  : pick_kernel_dim<3, PREC_FP64, true, DynPot>(method, 0);
   }
+  const bool mw14 = sig == GALPY_CUDA_SIG_MW14;
   if (prec == GALPY_CUDA_F32FORCE)
-    return planar ? pick_kernel_dim<2, PREC_F32, false>(method)
-                  : pick_kernel_dim<3, PREC_F32, false>(method);
-  return planar ? pick_kernel_dim<2, PREC_FP64, false>(method)
-                : pick_kernel_dim<3, PREC_FP64, false>(method);
+    return mw14 ? pick_plain<PREC_F32, MW14Pot>(planar, method, variant)
+                : pick_plain<PREC_F32, DynPot>(planar, method, variant);
+  return mw14 ? pick_plain<PREC_FP64, MW14Pot>(planar, method, variant)
+              : pick_plain<PREC_FP64, DynPot>(planar, method, variant);
+}
+
+static int signature_of(int npot, const int* pot_type)
+{
+  if (npot == 3 && pot_type[0] == T_PSWC && pot_type[1] == T_MN && pot_type[2] == T_NFW)
+    return GALPY_CUDA_SIG_MW14;
+  return GALPY_CUDA_SIG_GENERIC;
 }
 
 static bool method_supported(int m)
@@ -215,7 +286,9 @@ struct Scratch {  // device scratch of one launch (64 bytes)
 static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool progress,
                          cudaStream_t stream)
 {
-  const KernelInfo ki = pick_kernel(L->planar, L->variational, L->precision, L->odeint_type);
+  const KernelInfo ki =
+      pick_kernel(L->planar, L->variational, L->precision, L->odeint_type, L->signature,
+                  L->variant);
   KernelFn fn = ki.fn;
   if (!fn) return set_error(GALPY_CUDA_ERR_METHOD, "method/precision combination not implemented");
   KArgs A;
@@ -243,7 +316,39 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
   A.counter = &scratch->counter;
   A.abort_flag = L->abort_flag ? L->abort_flag : &scratch->abort_flag;
   A.done_count = progress ? &scratch->done_count : nullptr;
+  A.variational_nv = L->variational ? (L->planar ? 8 : 12) : 0;
   GPC_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(Scratch), stream));
+
+  // longest-first work queue (stream-ordered scratch, freed after the launch)
+  void* sched = nullptr;
+  if (L->schedule == GALPY_CUDA_SCHED_LONGEST_FIRST && L->nobj > 1 && L->nobj < (1LL << 31)) {
+    const int n = (int)L->nobj;
+    size_t tmp_bytes = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, (float*)nullptr, (float*)nullptr,
+                                              (int*)nullptr, (int*)nullptr, n, 0, 32, stream);
+    const size_t keys = (size_t)n * sizeof(float), vals = (size_t)n * sizeof(int);
+    const size_t off_k2 = keys, off_v1 = 2 * keys, off_v2 = 2 * keys + vals,
+                 off_tmp = (2 * keys + 2 * vals + 255) & ~(size_t)255;
+    GPC_CUDA_TRY(cudaMallocAsync(&sched, off_tmp + tmp_bytes, stream));
+    char* base = static_cast<char*>(sched);
+    float* k1 = reinterpret_cast<float*>(base);
+    float* k2 = reinterpret_cast<float*>(base + off_k2);
+    int* v1 = reinterpret_cast<int*>(base + off_v1);
+    int* v2 = reinterpret_cast<int*>(base + off_v2);
+    const unsigned cb = (unsigned)((L->nobj + 255) / 256);
+    if (L->planar)
+      cost_kernel<2><<<cb, 256, 0, stream>>>(A, k1, v1);
+    else
+      cost_kernel<3><<<cb, 256, 0, stream>>>(A, k1, v1);
+    GPC_CUDA_TRY(cudaGetLastError());
+    cudaError_t se = cub::DeviceRadixSort::SortPairsDescending(base + off_tmp, tmp_bytes, k1, k2,
+                                                               v1, v2, n, 0, 32, stream);
+    if (se != cudaSuccess) {
+      cudaFreeAsync(sched, stream);
+      return set_error(GALPY_CUDA_ERR_CUDA, std::string("radix sort: ") + cudaGetErrorString(se));
+    }
+    A.order = v2;
+  }
 
   int dev = 0;
   GPC_CUDA_TRY(cudaGetDevice(&dev));
@@ -262,7 +367,10 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
   fn<<<(unsigned)grid, block, smem, stream>>>(A);
-  GPC_CUDA_TRY(cudaGetLastError());
+  cudaError_t le = cudaGetLastError();
+  if (sched) cudaFreeAsync(sched, stream);
+  if (le != cudaSuccess)
+    return set_error(GALPY_CUDA_ERR_CUDA, std::string("orbit kernel launch: ") + cudaGetErrorString(le));
   return GALPY_CUDA_OK;
 }
 
@@ -394,6 +502,10 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
   L.atol = atol;
   L.max_attempts = o ? o->max_attempts : 0;
   L.block_size = o ? o->block_size : 0;
+  L.signature = signature_of(npot, pot_type);
+  L.schedule = o && o->size >= (int)sizeof(galpy_cuda_opts) ? o->schedule
+                                                             : GALPY_CUDA_SCHED_LONGEST_FIRST;
+  L.variant = o && o->size >= (int)sizeof(galpy_cuda_opts) ? o->variant : 0;
   rc = check_launch(&L);
   if (rc) return rc;
 
@@ -554,6 +666,12 @@ int galpy_cuda_device_count(void)
 }
 
 int galpy_cuda_comp_size(void) { return (int)sizeof(GpComp); }
+
+int galpy_cuda_signature(int npot, const int* pot_type)
+{
+  if (!pot_type || npot < 1) return GALPY_CUDA_SIG_GENERIC;
+  return signature_of(npot, pot_type);
+}
 
 int galpy_cuda_compile_potential(int planar, int npot, const int* pot_type,
                                  const double* pot_args, int ngroup, void* out)

@@ -111,20 +111,20 @@ GPC_HD GPC_FI void write_nan_rows(const OutSpec& o, long long i, int from)
 // ------------------------------------------------------------------------
 // force adapter: positions -> accelerations (+ K . dq for variational runs)
 // ------------------------------------------------------------------------
-template <int D, int PREC, bool VAR>
+template <int D, int PREC, bool VAR, class POT = DynPot>
 GPC_HD GPC_FI void eval_force(const GpComp* comp, int ncomp, const double* q, double* a)
 {
   if (!VAR) {
     if (PREC == PREC_FP64) {
       double ax, ay, az = 0.0;
-      accel<double, D == 2>(comp, ncomp, q[0], q[1], D == 3 ? q[2] : 0.0, ax, ay, az);
+      accel<double, D == 2, POT>(comp, ncomp, q[0], q[1], D == 3 ? q[2] : 0.0, ax, ay, az);
       a[0] = ax;
       a[1] = ay;
       if (D == 3) a[2] = az;
     } else {
       float ax, ay, az = 0.f;
-      accel<float, D == 2>(comp, ncomp, (float)q[0], (float)q[1], D == 3 ? (float)q[2] : 0.f, ax,
-                           ay, az);
+      accel<float, D == 2, POT>(comp, ncomp, (float)q[0], (float)q[1], D == 3 ? (float)q[2] : 0.f,
+                                ax, ay, az);
       a[0] = ax;
       a[1] = ay;
       if (D == 3) a[2] = az;
@@ -276,14 +276,14 @@ struct SymplecticMachine : OrbitCommon {
     }
   }
 
-  GPC_HD GPC_FI void point(double* y) const
+  GPC_HD GPC_FI void point(double* y, int /*slot*/) const
   {
 #pragma unroll
     for (int k = 0; k < NQ; k++) y[k] = qw[k];
   }
 
   template <class W>
-  GPC_HD void consume(const double* /*y*/, const double* a, W& out)
+  GPC_HD void consume(const double* /*y*/, const double* a, W& out, int /*slot*/)
   {
     const double dk = S4 ? (sub == 0 ? s4d1 * h : (sub == 1 ? s4d2 * h : s4d3 * h)) : h;
 #pragma unroll
@@ -437,7 +437,7 @@ struct RK4Machine : OrbitCommon {
     }
   }
 
-  GPC_HD GPC_FI void point(double* y) const
+  GPC_HD GPC_FI void point(double* y, int /*slot*/) const
   {
     const bool first = stage == 0;
 #pragma unroll
@@ -445,7 +445,7 @@ struct RK4Machine : OrbitCommon {
   }
 
   template <class W>
-  GPC_HD void consume(const double* y, const double* a, W& out)
+  GPC_HD void consume(const double* y, const double* a, W& out, int /*slot*/)
   {
     // derivative of the state at the evaluation point (x, v[, dx, dv])
     double d[N];
@@ -624,9 +624,27 @@ struct Dop853Machine : OrbitCommon {
     stage = ST_INIT1;
   }
 
-  GPC_HD GPC_FI void point(double* y) const
+  // Lanes of a warp run the stages of their (different) orbits in lock step:
+  // every step attempt is a fixed cycle of kCycle force evaluations --
+  // stages 2..12 in slots 0..10, the FSAL evaluation in slot 11 and the
+  // three dense-output stages in slots 12..14 -- driven by the kernel's
+  // iteration counter, so the stage-combination code is warp-uniform.  A
+  // lane that has nothing to compute in a slot (a rejected attempt, a step
+  // without output time, a new orbit waiting for slot 0) evaluates the force
+  // at y0 and discards it.  The two start-up evaluations of a new orbit run
+  // in whatever slots follow its pick-up.
+  static constexpr int kCycle = 15;
+  GPC_HD GPC_FI static int slot_stage(int slot) { return slot + 2; }  // 2..12, 13 FSAL, 14..16
+  GPC_HD GPC_FI bool active_in(int slot) const { return stage < 2 || stage == slot_stage(slot); }
+
+  GPC_HD GPC_FI void point(double* y, int slot) const
   {
     using namespace dp;
+    if (!active_in(slot)) {
+#pragma unroll
+      for (int i = 0; i < N; i++) y[i] = y0[i];
+      return;
+    }
     switch (stage) {
       case ST_INIT1:
 #pragma unroll
@@ -722,9 +740,10 @@ struct Dop853Machine : OrbitCommon {
   }
 
   template <class W>
-  GPC_HD void consume(const double* y, const double* a, W& out)
+  GPC_HD void consume(const double* y, const double* a, W& out, int slot)
   {
     using namespace dp;
+    if (!active_in(slot)) return;
     double d[N];
 #pragma unroll
     for (int k = 0; k < D; k++) {
@@ -971,11 +990,13 @@ template <class M, class F, class W>
 GPC_HD void run_orbit(M& m, F& force, W& out)
 {
   double y[M::NY], q[M::NA], a[M::NA];
+  unsigned iter = 0;
   while (!m.done) {
-    m.point(y);
+    const int slot = (int)(iter++ % 15u);
+    m.point(y, slot);
     M::pos(y, q);
     force(q, a);
-    m.consume(y, a, out);
+    m.consume(y, a, out, slot);
   }
   fill_unreached_rows(m, out);
 }

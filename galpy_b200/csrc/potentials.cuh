@@ -14,21 +14,25 @@
 //    R = sqrt(x^2+y^2), acos(x/R), nor the 1/R conversions of
 //    evalRectForce (integrateFullOrbit.c:1307-1325) are needed.
 //  * The host compiles galpy's (pot_type, pot_args) once into GpComp records
-//    holding the derived constants (1/rc^2, Gamma(a), b^2, 1/a ...), so no
-//    per-evaluation tgamma/pow(rc, 3-alpha) as in
-//    PowerSphericalPotentialwCutoff.c:10.
-//  * One component list per potential group; a launch may hold many groups
-//    (ragged multi-potential batches).  The component loop is warp-uniform
-//    whenever the lanes of a warp integrate orbits of the same group.
-//  * The Cartesian tidal tensor K = -grad grad Phi (for variational and
-//    adjoint integration) is built from each component's own radial /
-//    meridional derivatives, equal to the reference's cylindrical-to-
-//    Cartesian assembly (integrateFullOrbit.c:1570-1596).
-//  * The regularised incomplete gamma function of the bulge mass is this
-//    project's own implementation of the published series (Abramowitz &
-//    Stegun 6.5.29) and Legendre continued fraction (A&S 6.5.31, modified
-//    Lentz evaluation), with host-precomputed reciprocals 1/(a+n) so the
-//    series needs no division.
+//    holding the derived constants (compile_potential.h).
+//  * The bulge mass M(r) = 2 pi rc^(3-alpha) Gamma(a) P(a, r^2/rc^2),
+//    a = 1.5 - alpha/2, is evaluated as
+//        M(r) / r^3 = Mnorm rc^(-2a) (r^2)^(-alpha/2) gamma*(a, u),
+//        gamma*(a, u) = P(a, u) / u^a = e^-u sum_n u^n / Gamma(a+n+1),
+//    where gamma* -- an entire, slowly varying function -- comes from a
+//    piecewise Chebyshev table built on the host in extended precision
+//    (kChebN intervals on [0, U]; P = 1 to double precision beyond U).
+//    This replaces the reference's GSL series / continued fraction
+//    (PowerSphericalPotentialwCutoff.c:9-11), whose dependent divisions made
+//    it the latency bottleneck of every force evaluation.
+//  * A component list is walked at run time (any combination of the five
+//    types), or fixed at compile time (FixedPot) so that the components of
+//    a known potential such as MWPotential2014 are inlined side by side and
+//    their latencies overlap.
+//  * The Cartesian tidal tensor K = -grad grad Phi (variational runs) is
+//    built from each component's own radial / meridional derivatives and
+//    equals the reference's cylindrical-to-Cartesian assembly
+//    (integrateFullOrbit.c:1570-1596).
 #pragma once
 #include "gpc_common.cuh"
 
@@ -36,42 +40,37 @@ namespace gpc {
 
 enum : int { T_LOGHALO = 0, T_MN = 5, T_HERNQUIST = 8, T_NFW = 9, T_PSWC = 15 };
 
-constexpr int kMaxComp = 16;      // components per potential group
-constexpr int kSeriesTerms = 48;  // tabulated 1/(a+n), n = 1..kSeriesTerms
+constexpr int kMaxComp = 16;  // components per potential group
+constexpr int kChebN = 32;    // Chebyshev intervals of gamma*(a, u) on [0, U]
+constexpr int kChebC = 12;    // coefficients per interval (degree 11)
 
-// One compiled potential component: 8 scalars + the series table.  The
-// meaning of c[] depends on the type (see compile_potential in the host code):
-//   PSwC:      c0 amp, c1 1/rc^2, c2 a = 1.5 - alpha/2, c3 lgamma(a),
-//              c4 Mnorm = 2 pi rc^(3-alpha) Gamma(a), c5 -alpha/2,
-//              c6 4 pi, c7 alpha
+// One compiled potential component.  c[] by type:
+//   PSwC:      c0 amp, c1 1/rc^2, c2 Mnorm rc^(-2a), c3 -alpha/2,
+//              c4 Mnorm (total-mass factor, P = 1), c5 U, c6 kChebN / U,
+//              c7 4 pi
 //   MN:        c0 amp, c1 a, c2 b^2
-//   Hernquist: c0 amp, c1 a, c2 1/a
+//   Hernquist: c0 amp, c1 a
 //   NFW:       c0 amp, c1 a, c2 1/a
 //   LogHalo:   c0 amp, c1 1/q^2, c2 core^2, c3 1 - e (y-axis factor; 1 when
-//              axisymmetric), c4 triaxial flag
+//              axisymmetric)
 struct GpComp {
   int type;
   int pad;
   double c[8];
-  double inv_ap[kSeriesTerms];  // PSwC: 1/(a+n), n = 1..kSeriesTerms
+  double cheb[kChebN][kChebC];  // PSwC only
 };
 
 // ---------------------------------------------------------------- math ---
 template <typename T> struct Num;
 template <> struct Num<double> {
-  GPC_HD static double eps() { return 1.0e-16; }
-  GPC_HD static double tiny() { return 1.0e-300; }
   GPC_HD static double lg(double x) { return log(x); }
   GPC_HD static double ex(double x) { return exp(x); }
   GPC_HD static double lg1p(double x) { return log1p(x); }
   GPC_HD static double rsq(double x) { return gpc::rsq(x); }
   GPC_HD static double rcp(double x) { return 1.0 / x; }
-  GPC_HD static int maxit() { return 400; }
 };
 // FP32 evaluation: hardware approximations (SFU) for log/exp/rsqrt/rcp.
 template <> struct Num<float> {
-  GPC_HD static float eps() { return 6.0e-8f; }
-  GPC_HD static float tiny() { return 1.0e-37f; }
 #if defined(__CUDA_ARCH__)
   __device__ static float lg(float x) { return __logf(x); }
   __device__ static float ex(float x) { return __expf(x); }
@@ -83,128 +82,137 @@ template <> struct Num<float> {
 #endif
   GPC_HD static float lg1p(float x) { return log1pf(x); }
   GPC_HD static float rsq(float x) { return gpc::rsqf(x); }
-  GPC_HD static int maxit() { return 200; }
 };
 
-// Regularised lower incomplete gamma P(a, x), a > 0, x >= 0 (see header).
-// lga = lgamma(a); inv_ap[n-1] = 1/(a+n).
+// gamma*(a, u) from the component's Chebyshev table, u in [0, U)
 template <typename T>
-GPC_HD GPC_FI T inc_gamma_P(T a, T x, T lga, const double* __restrict__ inv_ap)
+GPC_HD GPC_FI T gamma_star(const GpComp* __restrict__ cp, T u)
 {
-  if (x <= T(0)) return T(0);
-  const T lpref = a * Num<T>::lg(x) - x - lga;
-  if (x < a + T(1)) {
-    // series: P = pref * sum_n x^n / (a (a+1) ... (a+n))
-    T term = Num<T>::rcp(a), sum = term;
-    int n = 0;
-    for (; n < kSeriesTerms; n++) {
-      term *= x * T(ldg(inv_ap + n));
-      sum += term;
-      if (fabs(term) < fabs(sum) * Num<T>::eps()) break;
-    }
-    if (n == kSeriesTerms) {  // only for x very close to a+1 with large a
-      T ap = a + T(kSeriesTerms);
-      for (int m = 0; m < Num<T>::maxit(); m++) {
-        ap += T(1);
-        term *= x / ap;
-        sum += term;
-        if (fabs(term) < fabs(sum) * Num<T>::eps()) break;
-      }
-    }
-    return sum * Num<T>::ex(lpref);
+  const T s = u * T(ldg(&cp->c[6]));
+  int k = (int)s;
+  k = k < kChebN - 1 ? k : kChebN - 1;
+  const T x = T(2) * (s - T(k)) - T(1);
+  const double* c = cp->cheb[k];
+  // Clenshaw recurrence
+  T b1 = T(0), b2 = T(0);
+#pragma unroll
+  for (int j = kChebC - 1; j > 0; j--) {
+    const T b0 = T(2) * x * b1 - b2 + T(ldg(c + j));
+    b2 = b1;
+    b1 = b0;
   }
-  // continued fraction for Q, modified Lentz
-  T b = x + T(1) - a, c = T(1) / Num<T>::tiny(), d = Num<T>::rcp(b), h = d;
-  for (int i = 1; i < Num<T>::maxit(); i++) {
-    const T an = -T(i) * (T(i) - a);
-    b += T(2);
-    d = an * d + b;
-    if (fabs(d) < Num<T>::tiny()) d = Num<T>::tiny();
-    c = b + an / c;
-    if (fabs(c) < Num<T>::tiny()) c = Num<T>::tiny();
-    d = Num<T>::rcp(d);
-    const T del = d * c;
-    h *= del;
-    if (fabs(del - T(1)) < Num<T>::eps()) break;
-  }
-  return T(1) - Num<T>::ex(lpref) * h;
+  return x * b1 - b2 + T(ldg(c));
 }
 
 // ------------------------------------------------------------- forces ---
-// Acceleration at (x, y, z) summed over one group's components; PLANAR
-// evaluates galpy's planar potential (the 3D potential in the plane z = 0)
-// and leaves az untouched.  T is the arithmetic type of the evaluation.
-template <typename T, bool PLANAR>
-GPC_HD GPC_FI void accel(const GpComp* __restrict__ comp, int ncomp, T x, T y, T z,
-                                      T& ax, T& ay, T& az)
+// Add one component's contribution to the radial factors: the acceleration
+// is a = (x gR, y (gR + gyx), z gz).  TYPE < 0: read the type at run time.
+template <typename T, bool PLANAR, int TYPE>
+GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, T x, T y, T z2, T R2, T r2, T& gR,
+                              T& gz, T& gyx)
+{
+  const int type = TYPE >= 0 ? TYPE : ldg(&cp->type);
+  const T amp = T(ldg(&cp->c[0]));
+  switch (type) {
+    case T_PSWC: {
+      // F = -amp M(r)/r^3 r_vec
+      const T u = r2 * T(ldg(&cp->c[1]));
+      T f;
+      if (u < T(ldg(&cp->c[5]))) {
+        const T pw = Num<T>::ex(T(ldg(&cp->c[3])) * Num<T>::lg(r2));  // (r^2)^(-alpha/2)
+        f = -amp * T(ldg(&cp->c[2])) * pw * gamma_star<T>(cp, u);
+      } else {
+        const T ir = Num<T>::rsq(r2);
+        f = -amp * T(ldg(&cp->c[4])) * (ir * ir * ir);
+      }
+      gR += f;
+      gz += f;
+      break;
+    }
+    case T_MN: {
+      const T a = T(ldg(&cp->c[1]));
+      const T zb2 = z2 + T(ldg(&cp->c[2]));
+      const T izb = Num<T>::rsq(zb2);
+      const T s = a + zb2 * izb;  // a + sqrt(z^2 + b^2)
+      const T iD = Num<T>::rsq(R2 + s * s);
+      const T iD3 = iD * iD * iD;
+      gR -= amp * iD3;
+      if (!PLANAR) gz -= amp * s * izb * iD3;
+      break;
+    }
+    case T_NFW: {
+      // Phi = -amp ln(1 + r/a)/r ; F = amp (1/(r^2 (a+r)) - ln(1+r/a)/r^3) r_vec
+      const T a = T(ldg(&cp->c[1]));
+      const T ir = Num<T>::rsq(r2);
+      const T r = r2 * ir;
+      const T f = amp * ir * ir * (Num<T>::rcp(a + r) - Num<T>::lg1p(r * T(ldg(&cp->c[2]))) * ir);
+      gR += f;
+      gz += f;
+      break;
+    }
+    case T_HERNQUIST: {
+      // Phi = -amp / (2 (r + a)) ; F = -amp / (2 r (r + a)^2) r_vec
+      const T a = T(ldg(&cp->c[1]));
+      const T ir = Num<T>::rsq(r2);
+      const T ira = Num<T>::rcp(r2 * ir + a);
+      const T f = -T(0.5) * amp * ir * ira * ira;
+      gR += f;
+      gz += f;
+      break;
+    }
+    case T_LOGHALO: {
+      // Phi = amp/2 ln(x^2 + (1-e) y^2 + z^2/q^2 + core^2)
+      const T iq2 = T(ldg(&cp->c[1]));
+      const T ye = T(ldg(&cp->c[3]));
+      const T D = x * x + ye * y * y + z2 * iq2 + T(ldg(&cp->c[2]));
+      const T g = -amp * Num<T>::rcp(D);
+      gR += g;
+      gyx += g * (ye - T(1));
+      if (!PLANAR) gz += g * iq2;
+      break;
+    }
+    default:
+      break;
+  }
+}
+
+// Run-time component list (any combination of the supported types).
+struct DynPot {
+  template <typename T, bool PLANAR>
+  GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, int ncomp, T x, T y, T z2, T R2,
+                                T r2, T& gR, T& gz, T& gyx)
+  {
+    for (int k = 0; k < ncomp; k++)
+      comp_accel<T, PLANAR, -1>(comp + k, x, y, z2, R2, r2, gR, gz, gyx);
+  }
+};
+
+// Compile-time component list: the components are inlined side by side.
+template <int... TYPES>
+struct FixedPot {
+  template <typename T, bool PLANAR>
+  GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, int /*ncomp*/, T x, T y, T z2,
+                                T R2, T r2, T& gR, T& gz, T& gyx)
+  {
+    int k = 0;
+    (comp_accel<T, PLANAR, TYPES>(comp + k++, x, y, z2, R2, r2, gR, gz, gyx), ...);
+  }
+};
+using MW14Pot = FixedPot<T_PSWC, T_MN, T_NFW>;  // galpy's MWPotential2014 order
+
+// Acceleration at (x, y, z); PLANAR evaluates galpy's planar potential (the
+// 3D potential in the plane z = 0) and leaves az untouched.
+template <typename T, bool PLANAR, class POT = DynPot>
+GPC_HD GPC_FI void accel(const GpComp* __restrict__ comp, int ncomp, T x, T y, T z, T& ax, T& ay,
+                         T& az)
 {
   const T R2 = x * x + y * y;
   const T z2 = PLANAR ? T(0) : z * z;
   const T r2 = R2 + z2;
-  T gR = T(0), gz = T(0), gy_extra = T(0);
-  for (int k = 0; k < ncomp; k++) {
-    const GpComp* cp = comp + k;
-    const int type = ldg(&cp->type);
-    const T amp = T(ldg(&cp->c[0]));
-    switch (type) {
-      case T_PSWC: {
-        // F = -amp M(r)/r^3 * r_vec, M(r) = Mnorm P(a, r^2/rc^2)
-        const T a = T(ldg(&cp->c[2]));
-        const T P = inc_gamma_P<T>(a, r2 * T(ldg(&cp->c[1])), T(ldg(&cp->c[3])), cp->inv_ap);
-        const T ir = Num<T>::rsq(r2);
-        const T f = -amp * T(ldg(&cp->c[4])) * P * (ir * ir * ir);
-        gR += f;
-        gz += f;
-        break;
-      }
-      case T_MN: {
-        const T a = T(ldg(&cp->c[1]));
-        const T zb2 = z2 + T(ldg(&cp->c[2]));
-        const T izb = Num<T>::rsq(zb2);
-        const T s = a + zb2 * izb;  // a + sqrt(z^2 + b^2)
-        const T iD = Num<T>::rsq(R2 + s * s);
-        const T iD3 = iD * iD * iD;
-        gR -= amp * iD3;
-        if (!PLANAR) gz -= amp * s * izb * iD3;
-        break;
-      }
-      case T_NFW: {
-        // Phi = -amp ln(1 + r/a)/r ; F = amp (1/(r^2 (a+r)) - ln(1+r/a)/r^3) r_vec
-        const T a = T(ldg(&cp->c[1]));
-        const T ir = Num<T>::rsq(r2);
-        const T r = r2 * ir;
-        const T f = amp * ir * ir * (Num<T>::rcp(a + r) - Num<T>::lg1p(r * T(ldg(&cp->c[2]))) * ir);
-        gR += f;
-        gz += f;
-        break;
-      }
-      case T_HERNQUIST: {
-        // Phi = -amp / (2 (r + a)) ; F = -amp / (2 r (r + a)^2) r_vec
-        const T a = T(ldg(&cp->c[1]));
-        const T ir = Num<T>::rsq(r2);
-        const T ira = Num<T>::rcp(r2 * ir + a);
-        const T f = -T(0.5) * amp * ir * ira * ira;
-        gR += f;
-        gz += f;
-        break;
-      }
-      case T_LOGHALO: {
-        // Phi = amp/2 ln(x^2 + (1-e) y^2 + z^2/q^2 + core^2)
-        const T iq2 = T(ldg(&cp->c[1]));
-        const T ye = T(ldg(&cp->c[3]));
-        const T D = x * x + ye * y * y + z2 * iq2 + T(ldg(&cp->c[2]));
-        const T g = -amp * Num<T>::rcp(D);
-        gR += g;
-        gy_extra += g * (ye - T(1));
-        if (!PLANAR) gz += g * iq2;
-        break;
-      }
-      default:
-        break;
-    }
-  }
+  T gR = T(0), gz = T(0), gyx = T(0);
+  POT::template sum<T, PLANAR>(comp, ncomp, x, y, z2, R2, r2, gR, gz, gyx);
   ax = x * gR;
-  ay = y * (gR + gy_extra);
+  ay = y * (gR + gyx);
   if (!PLANAR) az = z * gz;
 }
 
@@ -213,11 +221,9 @@ GPC_HD GPC_FI void accel(const GpComp* __restrict__ comp, int ncomp, T x, T y, T
 // (K[0]=xx, K[1]=xy, K[2]=yy, K[3]=xz, K[4]=yz, K[5]=zz), FP64.
 // Spherical components use Phi'(r), Phi''(r):
 //   K_ij = -(Phi'' - Phi'/r) x_i x_j / r^2 - Phi'/r delta_ij.
-GPC_HD GPC_FI void add_spherical(double dphi_over_r, double d2phi, double x, double y,
-                                              double z, double r2, double& gR, double& gz,
-                                              double K[6])
+GPC_HD GPC_FI void add_spherical(double dphi_over_r, double d2phi, double x, double y, double z,
+                                 double r2, double& gR, double& gz, double K[6])
 {
-  // dphi_over_r = Phi'/r, d2phi = Phi''
   const double c = (d2phi - dphi_over_r) / r2;
   gR -= dphi_over_r;
   gz -= dphi_over_r;
@@ -230,9 +236,8 @@ GPC_HD GPC_FI void add_spherical(double dphi_over_r, double d2phi, double x, dou
 }
 
 template <bool PLANAR>
-GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, double x,
-                                            double y, double z, double& ax, double& ay, double& az,
-                                            double K[6])
+GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, double x, double y,
+                               double z, double& ax, double& ay, double& az, double K[6])
 {
   if (PLANAR) z = 0.0;
   const double R2 = x * x + y * y, z2 = z * z, r2 = R2 + z2;
@@ -245,14 +250,18 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
     const double amp = ldg(&cp->c[0]);
     switch (type) {
       case T_PSWC: {
-        const double a = ldg(&cp->c[2]), irc2 = ldg(&cp->c[1]);
-        const double P = inc_gamma_P<double>(a, r2 * irc2, ldg(&cp->c[3]), cp->inv_ap);
-        const double ir = rsq(r2);
-        const double M = ldg(&cp->c[4]) * P;
-        const double dpr = amp * M * ir * ir * ir;  // Phi'/r = amp M / r^3
+        const double u = r2 * ldg(&cp->c[1]);
+        const double pw = exp(ldg(&cp->c[3]) * log(r2));  // (r^2)^(-alpha/2)
+        double Mr3;                                         // M(r) / r^3
+        if (u < ldg(&cp->c[5])) {
+          Mr3 = ldg(&cp->c[2]) * pw * gamma_star<double>(cp, u);
+        } else {
+          const double ir = rsq(r2);
+          Mr3 = ldg(&cp->c[4]) * ir * ir * ir;
+        }
+        const double dpr = amp * Mr3;  // Phi'/r
         // Phi'' = amp (4 pi r^-alpha exp(-r^2/rc^2) - 2 M / r^3)
-        const double d2 = amp * (ldg(&cp->c[6]) * pow(r2, ldg(&cp->c[5])) * exp(-r2 * irc2) -
-                                 2.0 * M * ir * ir * ir);
+        const double d2 = amp * (ldg(&cp->c[7]) * pw * exp(-u) - 2.0 * Mr3);
         add_spherical(dpr, d2, x, y, z, r2, gR, gz, K);
         break;
       }
@@ -261,7 +270,7 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
         const double ir = rsq(r2), r = r2 * ir;
         const double L = log1p(r * ldg(&cp->c[2]));
         const double iar = 1.0 / (a + r);
-        const double dpr = amp * (L * ir - iar) * ir * ir;                      // Phi'/r
+        const double dpr = amp * (L * ir - iar) * ir * ir;  // Phi'/r
         const double d2 = amp * (r * (2.0 * a + 3.0 * r) * iar * iar - 2.0 * L) * ir * ir * ir;
         add_spherical(dpr, d2, x, y, z, r2, gR, gz, K);
         break;
@@ -281,20 +290,15 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
         const double zb2 = z2 + ldg(&cp->c[2]);
         const double izb = rsq(zb2), zeta = zb2 * izb, s = a + zeta;
         const double iD = rsq(R2 + s * s), iD3 = iD * iD * iD, iD5 = iD3 * iD * iD;
-        // dPhi/dR = amp R iD3, dPhi/dz = amp z s/zeta iD3
         const double sz = s * izb;  // s / zeta
         gR -= amp * iD3;
         gz -= amp * sz * iD3;
-        // d2Phi/dR2 = amp (iD3 - 3 R^2 iD5); with x_i/R factors:
-        //   K_xx = -(amp iD3 - 3 amp x^2 iD5), K_xy = 3 amp x y iD5
         K[0] -= amp * (iD3 - 3.0 * x * x * iD5);
         K[1] += 3.0 * amp * x * y * iD5;
         K[2] -= amp * (iD3 - 3.0 * y * y * iD5);
-        // d2Phi/dRdz = -3 amp R z s/zeta iD5  -> K_xz = 3 amp x z sz iD5
         K[3] += 3.0 * amp * x * z * sz * iD5;
         K[4] += 3.0 * amp * y * z * sz * iD5;
-        // d2Phi/dz2 = amp [ iD3 (s/zeta - a z^2/zeta^3) - 3 z^2 sz^2 iD5 ]
-        //   (d/dz (z s/zeta) = s/zeta + z d(s/zeta)/dz = s/zeta - a z^2/zeta^3)
+        // d2Phi/dz2 = amp [ iD3 (s/zeta - a z^2/zeta^3) - 3 z^2 (s/zeta)^2 iD5 ]
         K[5] -= amp * (iD3 * (sz - a * z2 * izb * izb * izb) - 3.0 * z2 * sz * sz * iD5);
         break;
       }

@@ -212,18 +212,26 @@ def compile_potential(pot, planar=False, ngroup=1):
     return buf, npot
 
 
+def signature(pot, planar=False):
+    """Kernel specialisation of a potential (0 generic, 1 MWPotential2014-type)."""
+    npot, pot_type, _ = parse_pot(pot, planar=planar)
+    return _lib.lib().galpy_cuda_signature(npot, pot_type.ctypes.data_as(_ip))
+
+
 def integrate_device(comps, ncomp, w0, t, out, err, int_method, planar=False, variational=False,
                      nsteps=None, group=None, in_layout="soa", out_layout="soa_rect",
                      out_row0=0, dt=None, rtol=None, atol=None, precision="fp64",
-                     max_attempts=0, stream=None, block_size=0, grid_size=0):
+                     max_attempts=0, stream=None, block_size=0, grid_size=0, signature=0,
+                     schedule="longest_first", variant=0):
     """Asynchronous integration of device-resident torch tensors.
 
     comps: uint8 CUDA tensor of compiled records (compile_potential); w0
     float64 [nv, N] (in_layout 'soa') or [N, nv] ('aos'); t float64 [nt] or
     [N, nt]; out float64 sized for the layout ('soa_rect'/'soa_cyl':
     [nv, nt-out_row0, N], 'aos_rect'/'galpy': [N, nt-out_row0, nv]); err int32
-    [N]; nsteps int64 [N] or None; group int32 [N] or None.  Runs on `stream`
-    (a torch.cuda.Stream, default: the current stream)."""
+    [N]; nsteps int64 [N] or None; group int32 [N] or None; signature from
+    ``signature(pot)`` selects kernels specialised for the component list.
+    Runs on `stream` (a torch.cuda.Stream, default: the current stream)."""
     import torch
 
     layouts_in = {"aos": _lib.IN_AOS, "soa": _lib.IN_SOA}
@@ -263,4 +271,7 @@ def integrate_device(comps, ncomp, w0, t, out, err, int_method, planar=False, va
     L.stream = s.cuda_stream
     L.block_size = block_size
     L.grid_size = grid_size
+    L.signature = int(signature)
+    L.schedule = {"in_order": 0, "longest_first": 1}[schedule]
+    L.variant = int(variant)
     _lib.check(_lib.lib().galpy_cuda_integrate_device(ctypes.byref(L)))

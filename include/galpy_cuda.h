@@ -49,6 +49,14 @@ extern "C" {
 #define GALPY_CUDA_OUT_SOA_RECT 2 /* [nv][nrow][nobj] rectangular */
 #define GALPY_CUDA_OUT_SOA_CYL 3  /* [nv][nrow][nobj] cylindrical */
 
+/* potential signatures (kernels specialised at compile time) */
+#define GALPY_CUDA_SIG_GENERIC 0 /* any list of supported components */
+#define GALPY_CUDA_SIG_MW14 1    /* exactly (15, 5, 9): MWPotential2014's component types */
+
+/* order in which orbits are handed to the GPU threads */
+#define GALPY_CUDA_SCHED_IN_ORDER 0
+#define GALPY_CUDA_SCHED_LONGEST_FIRST 1 /* by estimated cost: integration time x orbital frequency */
+
 typedef void (*galpy_cuda_callback)(void);
 
 typedef struct galpy_cuda_opts {
@@ -59,10 +67,16 @@ typedef struct galpy_cuda_opts {
   long long max_attempts;  /* per-orbit step-attempt budget, 0 = unlimited */
   long long *nsteps;       /* optional out, host [nobj]: accepted steps per orbit */
   double *elapsed_ms;      /* optional out: device time of the integration kernel */
+  int variant;             /* register-budget variant of the kernel (see galpy_cuda_launch) */
+  int schedule;            /* GALPY_CUDA_SCHED_* (default longest-first) */
 } galpy_cuda_opts;
 
 /* Compiled potential record size in bytes (one per component). */
 int galpy_cuda_comp_size(void);
+
+/* Signature of a component-type list (GALPY_CUDA_SIG_*), for the device
+ * entry point's launch.signature. */
+int galpy_cuda_signature(int npot, const int *pot_type);
 
 /* Translate galpy's (pot_type, pot_args) for ngroup potential groups with the
  * same component types (pot_args holds ngroup consecutive argument blocks)
@@ -111,7 +125,8 @@ int integrateOrbit_dxdv_batch_cuda(int planar, int nobj, double *yo, int nt, dou
 
 /* Device-pointer entry point: all arrays live on the device, the call is
  * asynchronous on `stream`.  Needs 64 bytes of device scratch for the
- * work-stealing counter, allocated stream-ordered per call. */
+ * work-stealing counter (plus the scheduling scratch, see `schedule`),
+ * allocated stream-ordered per call. */
 typedef struct galpy_cuda_launch {
   int planar, variational, odeint_type, precision;
   long long nobj;
@@ -132,6 +147,10 @@ typedef struct galpy_cuda_launch {
   const int *abort_flag;    /* device int polled by the kernel, or NULL */
   void *stream;             /* cudaStream_t */
   int block_size, grid_size; /* 0 = defaults */
+  int signature;            /* galpy_cuda_signature(pot_type) */
+  int schedule;             /* GALPY_CUDA_SCHED_*; longest-first sorts the work queue
+                               (needs ~13 bytes/orbit of stream-ordered scratch) */
+  int variant;              /* register budget: 0 compiler default, 1 capped for occupancy */
 } galpy_cuda_launch;
 
 int galpy_cuda_integrate_device(const galpy_cuda_launch *launch);

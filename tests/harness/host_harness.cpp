@@ -23,19 +23,19 @@ struct Rows {
   }
 };
 
-template <int D, int PREC, bool VAR>
+template <int D, int PREC, bool VAR, class POT>
 struct Force {
   const GpComp* c;
   int n;
-  void operator()(const double* q, double* a) const { eval_force<D, PREC, VAR>(c, n, q, a); }
+  void operator()(const double* q, double* a) const { eval_force<D, PREC, VAR, POT>(c, n, q, a); }
 };
 
-template <class M, int D, int PREC, bool VAR>
+template <class M, int D, int PREC, bool VAR, class POT>
 void run_all(int nobj, const double* w, int nt, const double* t, int indiv_t, const GpComp* comps,
              int ncomp, double dt, double rtol, double atol, long long max_att, double* out,
              int* err, long long* nsteps)
 {
-  Force<D, PREC, VAR> f{comps, ncomp};
+  Force<D, PREC, VAR, POT> f{comps, ncomp};
   std::vector<double> store(M::kSlotDoubles + 1);
   for (long long i = 0; i < nobj; i++) {
     M m;
@@ -48,26 +48,26 @@ void run_all(int nobj, const double* w, int nt, const double* t, int indiv_t, co
   }
 }
 
-template <int D, int PREC, bool VAR>
+template <int D, int PREC, bool VAR, class POT>
 int dispatch(int method, int nobj, const double* w, int nt, const double* t, int indiv_t,
              const GpComp* c, int n, double dt, double rtol, double atol, long long ma,
              double* out, int* err, long long* ns)
 {
   switch (method) {
     case M_LEAPFROG:
-      run_all<SymplecticMachine<D, VAR, false>, D, PREC, VAR>(nobj, w, nt, t, indiv_t, c, n, dt,
+      run_all<SymplecticMachine<D, VAR, false>, D, PREC, VAR, POT>(nobj, w, nt, t, indiv_t, c, n, dt,
                                                               rtol, atol, ma, out, err, ns);
       return 0;
     case M_SYMPLEC4:
-      run_all<SymplecticMachine<D, VAR, true>, D, PREC, VAR>(nobj, w, nt, t, indiv_t, c, n, dt,
+      run_all<SymplecticMachine<D, VAR, true>, D, PREC, VAR, POT>(nobj, w, nt, t, indiv_t, c, n, dt,
                                                              rtol, atol, ma, out, err, ns);
       return 0;
     case M_RK4:
-      run_all<RK4Machine<D, VAR>, D, PREC, VAR>(nobj, w, nt, t, indiv_t, c, n, dt, rtol, atol,
+      run_all<RK4Machine<D, VAR>, D, PREC, VAR, POT>(nobj, w, nt, t, indiv_t, c, n, dt, rtol, atol,
                                                 ma, out, err, ns);
       return 0;
     case M_DOP853:
-      run_all<Dop853Machine<D, VAR>, D, PREC, VAR>(nobj, w, nt, t, indiv_t, c, n, dt, rtol,
+      run_all<Dop853Machine<D, VAR>, D, PREC, VAR, POT>(nobj, w, nt, t, indiv_t, c, n, dt, rtol,
                                                    atol, ma, out, err, ns);
       return 0;
   }
@@ -85,23 +85,38 @@ extern "C" int harness_integrate(int planar, int var, int method, int prec, int 
   int rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
   if (rc) return rc;
   const GpComp* c = comps.data();
+  // the kernels' compile-time MWPotential2014 specialisation
+  const bool mw14 = npot == 3 && pot_type[0] == T_PSWC && pot_type[1] == T_MN &&
+                    pot_type[2] == T_NFW;
+#define HARNESS_ARGS method, nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol, max_att, out, err, nsteps
+  if (var) return planar ? dispatch<2, PREC_FP64, true, DynPot>(HARNESS_ARGS)
+                         : dispatch<3, PREC_FP64, true, DynPot>(HARNESS_ARGS);
   if (planar) {
-    if (var) return dispatch<2, PREC_FP64, true>(method, nobj, w, nt, t, indiv_t, c, npot, dt,
-                                                 rtol, atol, max_att, out, err, nsteps);
-    if (prec) return dispatch<2, PREC_F32, false>(method, nobj, w, nt, t, indiv_t, c, npot, dt,
-                                                  rtol, atol, max_att, out, err, nsteps);
-    return dispatch<2, PREC_FP64, false>(method, nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol,
-                                         max_att, out, err, nsteps);
+    if (prec) return mw14 ? dispatch<2, PREC_F32, false, MW14Pot>(HARNESS_ARGS)
+                          : dispatch<2, PREC_F32, false, DynPot>(HARNESS_ARGS);
+    return mw14 ? dispatch<2, PREC_FP64, false, MW14Pot>(HARNESS_ARGS)
+                : dispatch<2, PREC_FP64, false, DynPot>(HARNESS_ARGS);
   }
-  if (var) return dispatch<3, PREC_FP64, true>(method, nobj, w, nt, t, indiv_t, c, npot, dt, rtol,
-                                               atol, max_att, out, err, nsteps);
-  if (prec) return dispatch<3, PREC_F32, false>(method, nobj, w, nt, t, indiv_t, c, npot, dt,
-                                                rtol, atol, max_att, out, err, nsteps);
-  return dispatch<3, PREC_FP64, false>(method, nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol,
-                                       max_att, out, err, nsteps);
+  if (prec) return mw14 ? dispatch<3, PREC_F32, false, MW14Pot>(HARNESS_ARGS)
+                        : dispatch<3, PREC_F32, false, DynPot>(HARNESS_ARGS);
+  return mw14 ? dispatch<3, PREC_FP64, false, MW14Pot>(HARNESS_ARGS)
+              : dispatch<3, PREC_FP64, false, DynPot>(HARNESS_ARGS);
+#undef HARNESS_ARGS
 }
 
 // accelerations (and tidal tensors) at points, for force-level tests
+// gamma*(a, u) from a compiled PowerSphericalwCutoff record (table check)
+extern "C" int harness_gamma_star(double alpha, double rc, int n, const double* u, double* out)
+{
+  const int pt = T_PSWC;
+  const double pa[3] = {1.0, alpha, rc};
+  GpComp c;
+  int rc_ = compile_group(1, 1, &pt, pa, &c, nullptr);
+  if (rc_) return rc_;
+  for (int i = 0; i < n; i++) out[i] = gamma_star<double>(&c, u[i]);
+  return 0;
+}
+
 extern "C" int harness_forces(int planar, int n, const double* x, const double* y,
                               const double* z, int npot, const int* pot_type,
                               const double* pot_args, double* acc /*[n][3]*/,

@@ -10,6 +10,32 @@ METHODS = ["leapfrog", "rk4", "symplec4", "dop853"]
 POTS = ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"]
 
 
+@pytest.mark.parametrize("alpha", [0.5, 1.2, 1.8, 2.6])
+def test_gamma_star_table_vs_mpmath(harness, alpha):
+    """The bulge's Chebyshev table of gamma*(a, u) = P(a, u) / u^a against
+    mpmath at 30 digits, a = 1.5 - alpha/2."""
+    import ctypes
+
+    import mpmath as mp
+
+    mp.mp.dps = 30
+    a = 1.5 - alpha / 2
+    u = np.concatenate([[0.0, 1e-12], np.geomspace(1e-6, 45.0, 300), np.linspace(0.1, 44.9, 300)])
+    out = np.zeros_like(u)
+    dp = ctypes.POINTER(ctypes.c_double)
+    assert harness.lib.harness_gamma_star(ctypes.c_double(alpha), ctypes.c_double(0.3), len(u),
+                                          u.ctypes.data_as(dp), out.ctypes.data_as(dp)) == 0
+    am = mp.mpf(a)
+    ref = np.array([float(1 / mp.gamma(am + 1)) if x == 0 else
+                    float(mp.gammainc(am, 0, mp.mpf(x), regularized=True) / mp.mpf(x) ** am)
+                    for x in u])
+    U = 20.0  # table cutoff, as in compile_potential.h (the kernel uses P = 1 beyond)
+    while mp.e ** -U * U ** (a - 1) / mp.gamma(a) > 1e-18:
+        U += 1.0
+    sel = u < U
+    assert (np.abs(out[sel] - ref[sel]) / ref[sel]).max() < 1e-15
+
+
 @pytest.mark.parametrize("name", POTS)
 def test_forces_and_tidal_tensor(harness, oracle, golden, name):
     pt, pa = golden[f"{name}_type"], golden[f"{name}_args"]
