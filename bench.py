@@ -58,6 +58,23 @@ def workload(n, seed):
     return ics, t
 
 
+def precision_workload(n, seed=2):
+    """The precision configuration: config-0 style initial conditions,
+    symplec4 with dt = 0.01 for 20,000 steps, final state only."""
+    rng = np.random.default_rng(seed)
+    R = rng.uniform(0.5, 2.0, n)
+    ics = np.stack([R, rng.normal(0, 0.1, n), 1 + rng.normal(0, 0.1, n),
+                    rng.normal(0, 0.05, n), rng.normal(0, 0.05, n),
+                    rng.uniform(0, 2 * np.pi, n)], 1)
+    return ics, np.array([0.0, 200.0])
+
+
+def stats(x):
+    x = np.asarray(x)
+    return {"median": float(np.median(x)), "p99": float(np.quantile(x, 0.99)),
+            "max": float(np.max(x))}
+
+
 def mw14_args():
     import galpy_b200 as gb
 
@@ -157,6 +174,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--mixed-orbits", type=int, default=1 << 22)
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -268,12 +286,18 @@ def main():
         "gpu_launches": args.steps,
     }
 
+    # energy drift of the headline run (initial state vs final snapshot)
+    E0 = torch.empty(n, dtype=torch.float64, device=dev)
+    E1 = torch.empty(n, dtype=torch.float64, device=dev)
+    gb.energy_device(comps_d, ncomp, w0, E0, stream=stream)
+    gb.energy_device(comps_d, ncomp, out[:, NT - 1, :], E1, stream=stream)
+    torch.cuda.synchronize()
+    result["energy_rel_err"] = stats((torch.abs(E1 / E0 - 1)).cpu().numpy())
+
     if not args.no_mixed:
-        ms32, steps32, nbad32 = timed("f32force", max(1, args.steps), 1)
-        result["mixed"] = {"precision": "f32force (float32 forces, float64 state)",
-                           "value": steps32 * max(1, args.steps) / (ms32 * 1e-3),
-                           "accepted_steps": steps32, "orbits_with_err": nbad32,
-                           "speedup_vs_fp64": (steps32 / ms32) / (steps / ms)}
+        result["mixed"] = mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg,
+                                    args.mixed_orbits)
+        result["gpu_launches"] += 4
 
     if not args.no_e2e:
         result["e2e"] = e2e(gb, ics, t, pt, pa, args.steps, pg, dev, steps)
@@ -289,6 +313,52 @@ def main():
         pg.destroy_process_group()
     if rank == 0:
         print(json.dumps(result), flush=True)
+
+
+def mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg, n):
+    """FP32-force / FP64-state vs all-FP64 on the precision configuration
+    (symplec4, dt = 0.01, 20,000 steps, final state only): throughput, the
+    per-orbit relative energy drift, and the final phase-space difference."""
+    ics, t = precision_workload(n)
+    w0 = torch.tensor(cyl_to_rect(ics).T.copy(), device=dev)
+    t_d = torch.tensor(t, device=dev)
+    E0 = torch.empty(n, dtype=torch.float64, device=dev)
+    gb.energy_device(comps_d, ncomp, w0, E0, stream=stream)
+    res = {}
+    outs = {}
+    for prec in ("fp64", "f32force"):
+        out = torch.empty((6, 1, n), dtype=torch.float64, device=dev)
+        err = torch.empty(n, dtype=torch.int32, device=dev)
+        ns = torch.empty(n, dtype=torch.int64, device=dev)
+        ms_list = []
+        for rep in range(2):  # warm-up + timed
+            if pg:
+                pg.barrier()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            gb.integrate_device(comps_d, ncomp, w0, t_d, out, err, "symplec4_cuda", nsteps=ns,
+                                dt=0.01, out_row0=1, precision=prec, stream=stream,
+                                signature=sig)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms_list.append(e0.elapsed_time(e1))
+        E1 = torch.empty(n, dtype=torch.float64, device=dev)
+        gb.energy_device(comps_d, ncomp, out[:, 0, :], E1, stream=stream)
+        torch.cuda.synchronize()
+        steps = float(ns.sum().item())
+        ms = ms_list[-1]
+        res[prec] = {"value": steps / (ms * 1e-3), "unit": "orbit-steps/s", "ms": ms,
+                     "energy_rel_err": stats(torch.abs(E1 / E0 - 1).cpu().numpy()),
+                     "orbits_with_err": int((err != 0).sum().item())}
+        outs[prec] = out[:, 0, :]
+    d = torch.abs(outs["f32force"] - outs["fp64"]).max(dim=0).values
+    scale = torch.abs(outs["fp64"]).max(dim=0).values
+    res["f32force"]["phase_space_rel_err_vs_fp64"] = stats((d / scale).cpu().numpy())
+    res["speedup_f32force_vs_fp64"] = res["f32force"]["value"] / res["fp64"]["value"]
+    res["workload"] = (f"precision: {n} orbits in MWPotential2014 (config-0 initial "
+                       "conditions), symplec4 dt=0.01, 20,000 steps, final state only")
+    return res
 
 
 def e2e(gb, ics, t, pt, pa, K, pg, dev, steps_total):

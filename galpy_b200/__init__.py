@@ -13,7 +13,8 @@ not built and CudaError when no GPU is available.
 """
 from ._lib import (CudaError, CudaLibraryMissing, MethodNotSupported,  # noqa: F401
                    PotentialNotSupported)
-from .integrate import (CUDA_METHODS, compile_potential, integrate_device,  # noqa: F401
+from .integrate import (CUDA_METHODS, compile_potential, energy_device,  # noqa: F401
+                        integrate_device,
                         integrate_dxdv_batch, integrateFullOrbit_cuda,
                         integrateFullOrbit_dxdv_cuda, integratePlanarOrbit_cuda,
                         integratePlanarOrbit_dxdv_cuda, parse_integrator, parse_tol,

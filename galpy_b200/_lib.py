@@ -135,6 +135,9 @@ SIGNATURES = {
     ),
     "galpy_cuda_integrate_device": (_ci, [ctypes.POINTER(GalpyCudaLaunch)]),
     "galpy_cuda_fp64_peak": (_ci, [_dp, _dp]),
+    "galpy_cuda_energy_device": (
+        _ci, [_vp, _ci, _vp, _ci, _vp, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong,
+              _vp, _vp]),
 }
 
 

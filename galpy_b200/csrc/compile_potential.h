@@ -104,6 +104,15 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
         c.c[6] = kChebN / U;
         c.c[7] = 4.0 * M_PI;
         build_gamma_star_table(a, U, c.cheb);
+        // potential energy: gamma(1 - alpha/2, u) and gamma(1.5 - alpha/2, u)
+        c.c[8] = 2.0 * M_PI * pow(rc, 3.0 - alpha);
+        c.c[9] = rc;
+        c.c[10] = 1.0 - 0.5 * alpha;
+        c.c[11] = c.c[10] > 0.0 ? tgamma(c.c[10]) : NAN;  // alpha >= 2: energy undefined here
+        c.c[12] = c.c[10] > 0.0 ? lgamma(c.c[10]) : NAN;
+        c.c[13] = a;
+        c.c[14] = tgamma(a);
+        c.c[15] = lgamma(a);
         break;
       }
       case T_MN:

@@ -596,6 +596,37 @@ static void cyl_to_rect_inplace(int planar, long long nobj, double* yo)
 }
 
 // ----------------------------------------------------------------------------
+// energies of stored states (output-side check of the integrations)
+// ----------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) energy_kernel(const GpComp* comps, int ncomp,
+                                                     const int* group, int planar,
+                                                     const double* w, long long n, long long sc,
+                                                     long long so, double* E)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* v = w + i * so;
+  const GpComp* c = comps + (group ? (long long)group[i] * ncomp : 0LL);
+  double x, y, z, vx, vy, vz;
+  if (planar) {
+    x = v[0];
+    y = v[sc];
+    z = 0.0;
+    vx = v[2 * sc];
+    vy = v[3 * sc];
+    vz = 0.0;
+  } else {
+    x = v[0];
+    y = v[sc];
+    z = v[2 * sc];
+    vx = v[3 * sc];
+    vy = v[4 * sc];
+    vz = v[5 * sc];
+  }
+  E[i] = 0.5 * (vx * vx + vy * vy + vz * vz) + potential_value(c, ncomp, x, y, z);
+}
+
+// ----------------------------------------------------------------------------
 // FP64 pipe peak: independent fused multiply-add chains per thread
 // ----------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) fp64_fma_peak_kernel(double* sink, int iters, double mul)
@@ -621,6 +652,20 @@ __global__ void __launch_bounds__(256) fp64_fma_peak_kernel(double* sink, int it
 // exported C ABI
 // ----------------------------------------------------------------------------
 extern "C" {
+
+int galpy_cuda_energy_device(const void* comps, int ncomp, const int* group, int planar,
+                             const double* w, long long n, long long comp_stride,
+                             long long orbit_stride, double* E, void* stream)
+{
+  if (!comps || !w || !E || n < 0 || ncomp < 1 || ncomp > kMaxComp)
+    return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
+  if (n == 0) return GALPY_CUDA_OK;
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  energy_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const GpComp*>(comps), ncomp, group, planar, w, n, comp_stride, orbit_stride, E);
+  GPC_CUDA_TRY(cudaGetLastError());
+  return GALPY_CUDA_OK;
+}
 
 int galpy_cuda_fp64_peak(double* tflops, double* ms)
 {

@@ -53,10 +53,13 @@ constexpr int kChebC = 12;    // coefficients per interval (degree 11)
 //   NFW:       c0 amp, c1 a, c2 1/a
 //   LogHalo:   c0 amp, c1 1/q^2, c2 core^2, c3 1 - e (y-axis factor; 1 when
 //              axisymmetric)
+//   PSwC potential (energy evaluation only): c8 2 pi rc^(3-alpha), c9 rc,
+//              c10 a1 = 1 - alpha/2, c11 Gamma(a1), c12 lgamma(a1),
+//              c13 a2 = 1.5 - alpha/2, c14 Gamma(a2), c15 lgamma(a2)
 struct GpComp {
   int type;
   int pad;
-  double c[8];
+  double c[16];
   double cheb[kChebN][kChebC];  // PSwC only
 };
 
@@ -326,6 +329,86 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
   ax = x * gR;
   ay = y * (gR + gyx);
   az = PLANAR ? 0.0 : z * gz;
+}
+
+// -------------------------------------------------- potential values ---
+// Regularised lower incomplete gamma P(a, x), a > 0 (series, A&S 6.5.29;
+// Legendre continued fraction for Q, A&S 6.5.31, modified Lentz).  Only the
+// potential-energy evaluation uses it; the integrators use the gamma* table.
+GPC_HD inline double inc_gamma_P(double a, double x, double lga)
+{
+  if (!(x > 0.0)) return 0.0;
+  const double lpref = a * log(x) - x - lga;
+  if (x < a + 1.0) {
+    double ap = a, term = 1.0 / a, sum = term;
+    for (int n = 0; n < 1000; n++) {
+      ap += 1.0;
+      term *= x / ap;
+      sum += term;
+      if (fabs(term) < fabs(sum) * 1e-17) break;
+    }
+    return sum * exp(lpref);
+  }
+  double b = x + 1.0 - a, c = 1.0 / 1e-300, d = 1.0 / b, h = d;
+  for (int i = 1; i < 1000; i++) {
+    const double an = -i * (i - a);
+    b += 2.0;
+    d = an * d + b;
+    if (fabs(d) < 1e-300) d = 1e-300;
+    c = b + an / c;
+    if (fabs(c) < 1e-300) c = 1e-300;
+    d = 1.0 / d;
+    const double del = d * c;
+    h *= del;
+    if (fabs(del - 1.0) < 1e-17) break;
+  }
+  return 1.0 - exp(lpref) * h;
+}
+
+// Potential Phi(x, y, z) summed over one group's components, FP64
+// (the *PotentialEval functions of potential_c_ext/*.c).
+GPC_HD inline double potential_value(const GpComp* __restrict__ comp, int ncomp, double x,
+                                     double y, double z)
+{
+  const double R2 = x * x + y * y, z2 = z * z, r2 = R2 + z2;
+  double phi = 0.0;
+  for (int k = 0; k < ncomp; k++) {
+    const GpComp* cp = comp + k;
+    const double amp = ldg(&cp->c[0]);
+    switch (ldg(&cp->type)) {
+      case T_PSWC: {
+        // amp 2 pi rc^(3-alpha) / r [ r/rc gamma(a1, u) - gamma(a2, u) ]
+        const double r = sqrt(r2), u = r2 * ldg(&cp->c[1]);
+        const double a1 = ldg(&cp->c[10]), a2 = ldg(&cp->c[13]);
+        const double g1 = ldg(&cp->c[11]) * inc_gamma_P(a1, u, ldg(&cp->c[12]));
+        const double g2 = ldg(&cp->c[14]) * inc_gamma_P(a2, u, ldg(&cp->c[15]));
+        phi += amp * ldg(&cp->c[8]) / r * (r / ldg(&cp->c[9]) * g1 - g2);
+        break;
+      }
+      case T_MN: {
+        const double s = ldg(&cp->c[1]) + sqrt(z2 + ldg(&cp->c[2]));
+        phi -= amp / sqrt(R2 + s * s);
+        break;
+      }
+      case T_NFW: {
+        const double r = sqrt(r2);
+        phi -= amp * log1p(r * ldg(&cp->c[2])) / r;
+        break;
+      }
+      case T_HERNQUIST: {
+        phi -= amp / (2.0 * (sqrt(r2) + ldg(&cp->c[1])));
+        break;
+      }
+      case T_LOGHALO: {
+        const double D = x * x + ldg(&cp->c[3]) * y * y + z2 * ldg(&cp->c[1]) + ldg(&cp->c[2]);
+        phi += 0.5 * amp * log(D);
+        break;
+      }
+      default:
+        break;
+    }
+  }
+  return phi;
 }
 
 }  // namespace gpc

@@ -275,3 +275,20 @@ def integrate_device(comps, ncomp, w0, t, out, err, int_method, planar=False, va
     L.schedule = {"in_order": 0, "longest_first": 1}[schedule]
     L.variant = int(variant)
     _lib.check(_lib.lib().galpy_cuda_integrate_device(ctypes.byref(L)))
+
+
+def energy_device(comps, ncomp, w, E, planar=False, layout="soa", group=None, stream=None):
+    """E = v^2/2 + Phi(x) of device-resident rectangular states (torch).
+
+    w: float64 CUDA tensor [nv, N] ('soa') or [N, nv] ('aos'), or any
+    strided view with those two axes; E: float64 [N]."""
+    import torch
+
+    if layout == "soa":
+        sc, so = w.stride(0), w.stride(1)
+    else:
+        so, sc = w.stride(0), w.stride(1)
+    s = stream if stream is not None else torch.cuda.current_stream(w.device)
+    _lib.check(_lib.lib().galpy_cuda_energy_device(
+        comps.data_ptr(), ncomp, group.data_ptr() if group is not None else None, int(planar),
+        w.data_ptr(), E.shape[0], sc, so, E.data_ptr(), s.cuda_stream))

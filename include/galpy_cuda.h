@@ -155,6 +155,15 @@ typedef struct galpy_cuda_launch {
 
 int galpy_cuda_integrate_device(const galpy_cuda_launch *launch);
 
+/* Energies E = v^2/2 + Phi(x) of n stored rectangular states on the device
+ * (galpy's Orbit.E for these potentials, galpy/orbit/Orbits.py:2902):
+ * component k of orbit i at w[i*orbit_stride + k*comp_stride]; group as in
+ * galpy_cuda_launch.  Asynchronous on `stream`.  The bulge term needs
+ * alpha < 2. */
+int galpy_cuda_energy_device(const void *comps, int ncomp, const int *group, int planar,
+                             const double *w, long long n, long long comp_stride,
+                             long long orbit_stride, double *E, void *stream);
+
 /* Diagnostic: measured float64 fused-multiply-add throughput of the current
  * device in TFLOP/s (2 flops per FMA), the roofline denominator of the
  * integration kernels. */

@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
 def test_abi_version_and_record_size():
     lib = _lib.lib()
     assert lib.galpy_cuda_abi_version() == 1
-    assert lib.galpy_cuda_comp_size() == 8 + 8 * 8 + 32 * 12 * 8
+    assert lib.galpy_cuda_comp_size() == 8 + 16 * 8 + 32 * 12 * 8
 
 
 def test_compile_potential_host_only(golden):

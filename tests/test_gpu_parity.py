@@ -280,3 +280,19 @@ def test_energy_conservation_gpu(oracle, mw14):
         out, err = gb.integrateFullOrbit_cuda((pt, pa), ics.copy(), t, cuda(m), progressbar=False)
         E = oracle.energy_cyl(out, pt, pa)
         assert np.all((E.std(1) / E.mean(1)) ** 2 < 1e-10), m
+
+
+def test_energy_kernel_vs_oracle(oracle, mw14):
+    import torch
+
+    pt, pa = mw14
+    ics = seeded_ics(5000, 50, r_range=(0.05, 3.0), log_r=True)
+    comps, n = gb.compile_potential((pt, pa))
+    dev = torch.device("cuda:0")
+    w = torch.tensor(cyl_to_rect(ics).T.copy(), device=dev)
+    E = torch.empty(len(ics), dtype=torch.float64, device=dev)
+    gb.energy_device(torch.tensor(comps, device=dev), n, w, E)
+    torch.cuda.synchronize()
+    ref = oracle.energy_cyl(ics[:, None, :], pt, pa)[:, 0]
+    # absolute on the scale of the energies (some orbits have E close to 0)
+    assert (np.abs(E.cpu().numpy() - ref) / np.abs(ref).max()).max() < 1e-14

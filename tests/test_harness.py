@@ -59,6 +59,25 @@ def test_forces_and_tidal_tensor(harness, oracle, golden, name):
     assert (np.abs(a32 - ref).max(1) / np.abs(ref).max(1)).max() < 3e-5
 
 
+@pytest.mark.parametrize("name", POTS)
+def test_potential_values(harness, oracle, golden, name):
+    """The energy kernel's potential against the oracle (reference formulas)."""
+    import ctypes
+
+    pt, pa = golden[f"{name}_type"], golden[f"{name}_args"]
+    R, z, phi = golden["pts_R"], golden["pts_z"], golden["pts_phi"]
+    x, y = R * np.cos(phi), R * np.sin(phi)
+    out = np.zeros_like(R)
+    dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    pti = np.ascontiguousarray(pt, np.int32)
+    pad = np.ascontiguousarray(pa, np.float64)
+    assert harness.lib.harness_potential(len(R), x.ctypes.data_as(dp), y.ctypes.data_as(dp),
+                                         z.ctypes.data_as(dp), len(pti), pti.ctypes.data_as(ip),
+                                         pad.ctypes.data_as(dp), out.ctypes.data_as(dp)) == 0
+    ref = oracle.potential(R, z, phi, pt, pa)
+    assert (np.abs(out - ref) / np.abs(ref).max()).max() < 1e-13
+
+
 @pytest.mark.parametrize("method", METHODS)
 @pytest.mark.parametrize("planar", [False, True])
 def test_orbits_vs_oracle(harness, oracle, mw14, mw14_planar, method, planar):
