@@ -1,0 +1,78 @@
+"""galpy's Orbit.integrate dispatching the *_cuda methods to this package.
+
+Runs galpy from the reference tree (skipped where that tree is absent).  On
+CPU machines the engine call is replaced by a recorder, so the test checks the
+dispatch and argument passing; the GPU suite checks the engine itself."""
+import numpy as np
+import pytest
+from galpy_stub import import_galpy
+
+galpy = import_galpy()
+pytestmark = pytest.mark.skipif(galpy is None, reason="galpy reference tree not available")
+
+
+@pytest.fixture()
+def hooks(monkeypatch):
+    from galpy_b200 import galpy_hooks, integrate
+
+    calls = []
+
+    def recorder(planar, pot, yo, t, int_method, rtol, atol, progressbar, dt, precision,
+                 max_attempts, return_nsteps, device):
+        calls.append(dict(planar=planar, pot=pot, yo=np.array(yo), t=np.array(t),
+                          method=int_method, rtol=rtol, atol=atol, dt=dt))
+        yo2 = np.atleast_2d(yo)
+        out = np.repeat(yo2[:, None, :], np.asarray(t).shape[-1], axis=1)
+        err = np.zeros(len(yo2), np.int32)
+        return (out[0], err[0]) if np.ndim(yo) == 1 else (out, err)
+
+    monkeypatch.setattr(integrate, "_integrate_c", recorder)
+    galpy_hooks.install()
+    yield calls
+    galpy_hooks.uninstall()
+
+
+def test_orbit_integrate_routes_cuda_methods(hooks):
+    from galpy.orbit import Orbit
+    from galpy.potential import MWPotential2014
+
+    vxvv = [[1.0, 0.1, 1.1, 0.05, 0.02, 0.3], [1.5, -0.1, 0.9, -0.02, 0.01, 2.0]]
+    o = Orbit(vxvv)
+    ts = np.linspace(0, 10, 101)
+    for method in ("leapfrog_cuda", "rk4_cuda", "symplec4_cuda", "dop853_cuda"):
+        o.integrate(ts, MWPotential2014, method=method)
+        call = hooks[-1]
+        assert call["method"] == method and not call["planar"]
+        assert call["yo"].shape == (2, 6)
+        np.testing.assert_allclose(call["yo"], np.array(vxvv))
+        np.testing.assert_allclose(call["t"], ts)
+        # the recorder returns the initial condition at every time
+        np.testing.assert_allclose(o.R(ts[-1]), [1.0, 1.5])
+    assert len(hooks) == 4
+
+
+def test_planar_orbit_routes(hooks):
+    from galpy.orbit import Orbit
+    from galpy.potential import MWPotential2014
+
+    o = Orbit([[1.0, 0.1, 1.1, 0.3]])
+    o.integrate(np.linspace(0, 5, 11), MWPotential2014, method="dop853_cuda")
+    assert hooks[-1]["planar"] and hooks[-1]["yo"].shape == (1, 4)
+
+
+def test_unsupported_potential_falls_back(hooks):
+    from galpy.orbit import Orbit
+    from galpy.potential import PlummerPotential
+
+    o = Orbit([1.0, 0.1, 1.1, 0.0, 0.1, 0.0])
+    o.integrate(np.linspace(0, 1, 11), PlummerPotential(normalize=1.0), method="dop853_cuda")
+    assert hooks == []  # galpy's own integrator ran
+
+
+def test_unknown_method_still_rejected(hooks):
+    from galpy.orbit import Orbit
+    from galpy.potential import MWPotential2014
+
+    o = Orbit([1.0, 0.1, 1.1, 0.0, 0.1, 0.0])
+    with pytest.raises(ValueError):
+        o.integrate(np.linspace(0, 1, 11), MWPotential2014, method="euler_cuda")
