@@ -134,6 +134,7 @@ SIGNATURES = {
         [_ci, _ci, _dp, _ci, _dp, _ci, _ci, _ip, _dp, _cd, _cd, _cd, _dp, _ip, _ci, _opts_p],
     ),
     "galpy_cuda_integrate_device": (_ci, [ctypes.POINTER(GalpyCudaLaunch)]),
+    "galpy_cuda_integrate_device_noalloc": (_ci, [ctypes.POINTER(GalpyCudaLaunch)]),
     "galpy_cuda_fp64_peak": (_ci, [_dp, _dp]),
     "galpy_cuda_energy_device": (
         _ci, [_vp, _ci, _vp, _ci, _vp, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong,

@@ -28,6 +28,7 @@
 #include <time.h>
 
 #include <atomic>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -649,6 +650,103 @@ __global__ void __launch_bounds__(256) fp64_fma_peak_kernel(double* sink, int it
 }
 
 // ----------------------------------------------------------------------------
+// Allocation-free variant of the device entry point
+// ----------------------------------------------------------------------------
+// galpy_cuda_integrate_device allocates its scratch (the work-stealing
+// counter and the longest-first work queue) with cudaMallocAsync on every
+// call.  Some callers cannot let a library allocate: applications that run
+// the integrator inside a loop that must not touch the CUDA allocator (an
+// allocation can implicitly synchronise the device, or grow a memory pool the
+// application has sized and locked for its own use), and embedding hosts
+// whose allocation policy forbids third-party device allocations.  For them,
+// galpy_cuda_integrate_device_noalloc keeps all of its scratch in the fixed
+// array below, which is part of the loaded module: every GPU that loads the
+// library holds these ~5 MiB until the process exits.
+constexpr long long kNoAllocMaxOrbits = 1LL << 20;  // largest batch it accepts
+constexpr int kNoAllocBuckets = 64;                 // cost buckets of the work queue
+constexpr size_t kNoAllocCtl = 0;                   // Scratch control words
+constexpr size_t kNoAllocCount = 256;               // unsigned[64] bucket sizes
+constexpr size_t kNoAllocNext = 512;                // unsigned[64] bucket fill positions
+constexpr size_t kNoAllocBucket = 1024;             // unsigned char[max] bucket of each orbit
+constexpr size_t kNoAllocOrder = kNoAllocBucket + kNoAllocMaxOrbits;  // int[max] work queue
+constexpr size_t kNoAllocBytes = kNoAllocOrder + 4 * kNoAllocMaxOrbits;
+static_assert(sizeof(Scratch) <= kNoAllocCount, "control block too large");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// Device address of g_noalloc_scratch per device, looked up once per device
+// (host code must not use the symbol itself: on the host it is only a
+// stand-in for the device object).
+static std::mutex g_noalloc_mutex;
+static void* g_noalloc_ptr[64] = {nullptr};
+
+static int noalloc_scratch(void** out)
+{
+  int dev = 0;
+  GPC_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return set_error(GALPY_CUDA_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return set_error(GALPY_CUDA_ERR_CUDA,
+                       std::string("cudaGetSymbolAddress(noalloc scratch): ") + cudaGetErrorString(e));
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return GALPY_CUDA_OK;
+}
+
+// Bucketed longest-first order without a sort: bucket = 4 log2(1 + cost)
+// (64 buckets, largest cost first), counted, scanned and scattered.
+template <int D>
+__global__ void __launch_bounds__(256) noalloc_bucket_kernel(const KArgs A, unsigned char* scr)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= A.nobj) return;
+  double q[3] = {0.0, 0.0, 0.0}, a[3] = {0.0, 0.0, 0.0};
+  const int nv = A.variational_nv ? A.variational_nv : 2 * D;
+  for (int k = 0; k < D; k++)
+    q[k] = A.in_layout == GALPY_CUDA_IN_SOA ? A.w0[(long long)k * A.nobj + i] : A.w0[i * nv + k];
+  const GpComp* comps = A.comps + (A.group ? (long long)A.group[i] * A.ncomp : 0LL);
+  eval_force<D, PREC_FP64, false, DynPot>(comps, A.ncomp, q, a);
+  double ax = 0.0, xx = 0.0;
+  for (int k = 0; k < D; k++) {
+    ax += a[k] * q[k];
+    xx += q[k] * q[k];
+  }
+  const double* tt = A.t + (A.indiv_t ? i * (long long)A.nt : 0LL);
+  const double cost = fabs(tt[A.nt - 1] - tt[0]) * sqrt(fabs(ax) / (xx > 0.0 ? xx : 1e-300));
+  int b = isfinite(cost) ? (int)(4.0 * log2(1.0 + cost)) : 0;
+  b = b < 0 ? 0 : (b > kNoAllocBuckets - 1 ? kNoAllocBuckets - 1 : b);
+  const int key = kNoAllocBuckets - 1 - b;  // descending cost
+  scr[kNoAllocBucket + i] = (unsigned char)key;
+  atomicAdd(reinterpret_cast<unsigned*>(scr + kNoAllocCount) + key, 1u);
+}
+
+__global__ void noalloc_scan_kernel(unsigned char* scr)
+{
+  if (threadIdx.x != 0) return;
+  const unsigned* count = reinterpret_cast<const unsigned*>(scr + kNoAllocCount);
+  unsigned* next = reinterpret_cast<unsigned*>(scr + kNoAllocNext);
+  unsigned s = 0;
+  for (int b = 0; b < kNoAllocBuckets; b++) {
+    next[b] = s;
+    s += count[b];
+  }
+}
+
+__global__ void __launch_bounds__(256) noalloc_scatter_kernel(long long n, unsigned char* scr)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int key = scr[kNoAllocBucket + i];
+  const unsigned pos = atomicAdd(reinterpret_cast<unsigned*>(scr + kNoAllocNext) + key, 1u);
+  reinterpret_cast<int*>(scr + kNoAllocOrder)[pos] = (int)i;
+}
+
+// ----------------------------------------------------------------------------
 // exported C ABI
 // ----------------------------------------------------------------------------
 extern "C" {
@@ -746,6 +844,89 @@ int galpy_cuda_integrate_device(const galpy_cuda_launch* L)
   rc = launch_kernel(L, scr, false, s);
   cudaFreeAsync(scr, s);
   return rc;
+}
+
+int galpy_cuda_integrate_device_noalloc(const galpy_cuda_launch* L)
+{
+  int rc = check_launch(L);
+  if (rc) return rc;
+  if (L->nobj > kNoAllocMaxOrbits)
+    return set_error(GALPY_CUDA_ERR_ARG,
+                     "galpy_cuda_integrate_device_noalloc: nobj = " + std::to_string(L->nobj) +
+                         " exceeds its fixed scratch of " + std::to_string(kNoAllocMaxOrbits) +
+                         " orbits; split the batch or use galpy_cuda_integrate_device");
+  if (L->nobj == 0) return GALPY_CUDA_OK;
+  void* base = nullptr;
+  rc = noalloc_scratch(&base);
+  if (rc) return rc;
+  unsigned char* scr = static_cast<unsigned char*>(base);
+  Scratch* ctl = reinterpret_cast<Scratch*>(scr + kNoAllocCtl);
+  cudaStream_t stream = static_cast<cudaStream_t>(L->stream);
+
+  const KernelInfo ki =
+      pick_kernel(L->planar, L->variational, L->precision, L->odeint_type, L->signature,
+                  L->variant);
+  KernelFn fn = ki.fn;
+  if (!fn) return set_error(GALPY_CUDA_ERR_METHOD, "method/precision combination not implemented");
+  KArgs A;
+  memset(&A, 0, sizeof(A));
+  A.nobj = L->nobj;
+  A.nt = L->nt;
+  A.indiv_t = L->indiv_t;
+  A.t = L->t;
+  A.w0 = L->w0;
+  A.in_layout = L->in_layout;
+  A.out.out = L->out;
+  A.out.layout = L->out_layout;
+  A.out.nt = L->nt;
+  A.out.row0 = L->out_row0;
+  A.out.nobj = L->nobj;
+  A.err = L->err;
+  A.nsteps = L->nsteps;
+  A.comps = static_cast<const GpComp*>(L->comps);
+  A.ncomp = L->ncomp;
+  A.group = L->group;
+  A.dt = L->dt;
+  A.rtol = L->rtol;
+  A.atol = L->atol;
+  A.max_attempts = L->max_attempts;
+  A.counter = &ctl->counter;
+  A.abort_flag = L->abort_flag ? L->abort_flag : &ctl->abort_flag;
+  A.done_count = nullptr;
+  A.variational_nv = L->variational ? (L->planar ? 8 : 12) : 0;
+  // the array keeps the previous call's contents: zero the control words
+  // and the bucket counters (a memset, not an allocation)
+  GPC_CUDA_TRY(cudaMemsetAsync(scr, 0, kNoAllocBucket, stream));
+  if (L->schedule == GALPY_CUDA_SCHED_LONGEST_FIRST && L->nobj > 1) {
+    const unsigned nb = (unsigned)((L->nobj + 255) / 256);
+    if (L->planar)
+      noalloc_bucket_kernel<2><<<nb, 256, 0, stream>>>(A, scr);
+    else
+      noalloc_bucket_kernel<3><<<nb, 256, 0, stream>>>(A, scr);
+    noalloc_scan_kernel<<<1, 32, 0, stream>>>(scr);
+    noalloc_scatter_kernel<<<nb, 256, 0, stream>>>(L->nobj, scr);
+    GPC_CUDA_TRY(cudaGetLastError());
+    A.order = reinterpret_cast<const int*>(scr + kNoAllocOrder);
+  }
+  int dev = 0, nsm = 0;
+  GPC_CUDA_TRY(cudaGetDevice(&dev));
+  GPC_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int block = L->block_size > 0 ? L->block_size : 128;
+  if (block > 128 || block % 32)
+    return set_error(GALPY_CUDA_ERR_ARG, "block_size must be 32..128, multiple of 32");
+  const size_t smem = (size_t)ki.slot_doubles * sizeof(double) * block;
+  if (smem > 48 * 1024)
+    GPC_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  GPC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem));
+  if (per_sm < 1) per_sm = 1;
+  long long grid = L->grid_size > 0 ? L->grid_size : (long long)nsm * per_sm;
+  const long long need = (L->nobj + block - 1) / block;
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
+  fn<<<(unsigned)grid, block, smem, stream>>>(A);
+  GPC_CUDA_TRY(cudaGetLastError());
+  return GALPY_CUDA_OK;
 }
 
 int integrateFullOrbit_cuda(int nobj, double* yo, int nt, double* t, int indiv_t, int npot,

@@ -155,6 +155,21 @@ typedef struct galpy_cuda_launch {
 
 int galpy_cuda_integrate_device(const galpy_cuda_launch *launch);
 
+/* Same integration as galpy_cuda_integrate_device, for callers that must not
+ * let a library allocate device memory while they run (an allocation can
+ * synchronise the device or grow a pool the application sized for itself).
+ * No counterpart in the reference.  It calls no cudaMalloc/cudaFree or other
+ * allocating routine: its scratch (work-stealing counter, abort word and a
+ * bucketed longest-first work queue) lives in a fixed ~5 MiB array compiled
+ * into the library, held by every GPU that loads it until the process exits.
+ * Limit: at most 1,048,576 orbits per call (GALPY_CUDA_ERR_ARG beyond that;
+ * split the batch).  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  Every call reuses the same array (the control words are cleared
+ * at the start of each call), so calls that overlap on the GPU -- on
+ * different streams or from different threads -- race: serialise them. */
+int galpy_cuda_integrate_device_noalloc(const galpy_cuda_launch *launch);
+
 /* Energies E = v^2/2 + Phi(x) of n stored rectangular states on the device
  * (galpy's Orbit.E for these potentials, galpy/orbit/Orbits.py:2902):
  * component k of orbit i at w[i*orbit_stride + k*comp_stride]; group as in
