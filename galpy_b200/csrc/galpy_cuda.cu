@@ -116,6 +116,7 @@ __global__ void __launch_bounds__(128, MINB) orbit_kernel(const KArgs A)
   bool active = false, aborting = false;
   const GpComp* comps = A.comps;
   unsigned iter = 0;
+  int slot = 0;
   for (;;) {
     if (!active) {
       i = (long long)atomicAdd(A.counter, 1ULL);
@@ -134,9 +135,6 @@ __global__ void __launch_bounds__(128, MINB) orbit_kernel(const KArgs A)
              A.max_attempts, rows);
       active = true;
     }
-    // slot of the fixed stage cycle (DOP853): the iteration counter is the
-    // same in every lane of the warp
-    const int slot = (int)(iter % 15u);
     if (!m.done) {
       double y[M::NY], q[M::NA], a[M::NA];
       m.point(y, slot);
@@ -145,6 +143,11 @@ __global__ void __launch_bounds__(128, MINB) orbit_kernel(const KArgs A)
       Rows rows{&A.out, i};
       m.consume(y, a, rows, slot);
     }
+    // advance the warp's stage slot (DOP853): the dense-output slots run only
+    // if some lane of the warp needs them
+#if defined(__CUDA_ARCH__)
+    slot = M::next_slot(slot, __any_sync(__activemask(), m.wants_dense()));
+#endif
     ++iter;
     if (A.abort_flag && ((iter & 255u) == 0u) &&
         *reinterpret_cast<const volatile int*>(A.abort_flag)) {

@@ -183,6 +183,8 @@ struct SymplecticMachine : OrbitCommon {
   static constexpr int NA = NQ;               // force result size
   static constexpr int kSlotDoubles = 0;      // no slot store needed
   GPC_HD GPC_FI void bind(double*, int) {}
+  GPC_HD GPC_FI bool wants_dense() const { return false; }
+  GPC_HD GPC_FI static int next_slot(int slot, bool) { return slot >= 14 ? 0 : slot + 1; }
   GPC_HD GPC_FI static void pos(const double* y, double* q)
   {
 #pragma unroll
@@ -379,6 +381,8 @@ struct RK4Machine : OrbitCommon {
   }
   static constexpr int kSlotDoubles = 0;
   GPC_HD GPC_FI void bind(double*, int) {}
+  GPC_HD GPC_FI bool wants_dense() const { return false; }
+  GPC_HD GPC_FI static int next_slot(int slot, bool) { return slot >= 14 ? 0 : slot + 1; }
   enum { EST_A = 0, EST_B = 1, EST_C = 2, MAIN = 3 };
   double yo[N];    // orbit state at the last completed step
   double yn[N], yn1[N], ynk[N];
@@ -546,6 +550,74 @@ struct RK4Machine : OrbitCommon {
 // ------------------------------------------------------------------------
 // DOP853 (optionally variational)
 // ------------------------------------------------------------------------
+// Stage inputs as data: stage s's input is y0 + h * sum_t coef[s][t] *
+// K[slot[s][t]] (terms in the reference's order, leung_dop853.c:351-388 and
+// :446-462), and its derivative goes to slot dst[s].  Slots: 0 k1, 1 k2, 2 k3,
+// 3 k4, 4 k5, 5 k6, 6 k7, 7 k8, 8 k9, 9 k10, 10 s14, 11 s15 -- the reference's
+// k1..k10 with its reuse (stage 11 -> k2, stage 12 -> k3, the FSAL derivative
+// -> k4, the new state -> k5), plus two slots for the first dense-output
+// stages so that k10/k2/k3 stay available for the interpolation.  Because
+// every lane of a warp is in the same stage (see kCycle below) the table
+// reads are uniform constant-cache broadcasts and one small loop serves all
+// stages.
+struct DopStageTable {
+  int nterm[17];
+  int slot[17][9];
+  double coef[17][9];
+  int dst[17];
+};
+#define GPC_DOP853_STAGE_TABLE \
+  {{0, 0, 1, 2, 2, 3, 3, 4, 5, 6, 7, 8, 9, 0, 8, 8, 8}, \
+   {{0, 0, 0, 0, 0, 0, 0, 0, 0}, \
+    {0, 0, 0, 0, 0, 0, 0, 0, 0}, \
+    {0, 0, 0, 0, 0, 0, 0, 0, 0}, \
+    {0, 1, 0, 0, 0, 0, 0, 0, 0}, \
+    {0, 2, 0, 0, 0, 0, 0, 0, 0}, \
+    {0, 2, 3, 0, 0, 0, 0, 0, 0}, \
+    {0, 3, 4, 0, 0, 0, 0, 0, 0}, \
+    {0, 3, 4, 5, 0, 0, 0, 0, 0}, \
+    {0, 3, 4, 5, 6, 0, 0, 0, 0}, \
+    {0, 3, 4, 5, 6, 7, 0, 0, 0}, \
+    {0, 3, 4, 5, 6, 7, 8, 0, 0}, \
+    {0, 3, 4, 5, 6, 7, 8, 9, 0}, \
+    {0, 3, 4, 5, 6, 7, 8, 9, 1}, \
+    {0, 0, 0, 0, 0, 0, 0, 0, 0}, \
+    {0, 6, 7, 8, 9, 1, 2, 3, 0}, \
+    {0, 5, 6, 7, 1, 2, 3, 10, 0}, \
+    {0, 5, 6, 7, 8, 3, 10, 11, 0}}, \
+   {{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, \
+    {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, \
+    {dp::a21, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, \
+    {dp::a31, dp::a32, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, \
+    {dp::a41, dp::a43, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, \
+    {dp::a51, dp::a53, dp::a54, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, \
+    {dp::a61, dp::a64, dp::a65, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, \
+    {dp::a71, dp::a74, dp::a75, dp::a76, 0.0, 0.0, 0.0, 0.0, 0.0}, \
+    {dp::a81, dp::a84, dp::a85, dp::a86, dp::a87, 0.0, 0.0, 0.0, 0.0}, \
+    {dp::a91, dp::a94, dp::a95, dp::a96, dp::a97, dp::a98, 0.0, 0.0, 0.0}, \
+    {dp::a101, dp::a104, dp::a105, dp::a106, dp::a107, dp::a108, dp::a109, 0.0, 0.0}, \
+    {dp::a111, dp::a114, dp::a115, dp::a116, dp::a117, dp::a118, dp::a119, dp::a1110, 0.0}, \
+    {dp::a121, dp::a124, dp::a125, dp::a126, dp::a127, dp::a128, dp::a129, dp::a1210, dp::a1211}, \
+    {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, \
+    {dp::a141, dp::a147, dp::a148, dp::a149, dp::a1410, dp::a1411, dp::a1412, dp::a1413, 0.0}, \
+    {dp::a151, dp::a156, dp::a157, dp::a158, dp::a1511, dp::a1512, dp::a1513, dp::a1514, 0.0}, \
+    {dp::a161, dp::a166, dp::a167, dp::a168, dp::a169, dp::a1613, dp::a1614, dp::a1615, 0.0}}, \
+   {-1, -1, 1, 2, 3, 4, 5, 6, 7, 8, 9, 1, 2, 3, 10, 11, -1}}
+
+#if defined(__CUDACC__)
+__constant__ DopStageTable kDopTableDev = GPC_DOP853_STAGE_TABLE;
+#endif
+static const DopStageTable kDopTableHost = GPC_DOP853_STAGE_TABLE;
+
+GPC_HD GPC_FI const DopStageTable& dop_table()
+{
+#if defined(__CUDA_ARCH__)
+  return kDopTableDev;
+#else
+  return kDopTableHost;
+#endif
+}
+
 template <int D, bool VAR>
 struct Dop853Machine : OrbitCommon {
   static constexpr int N = VAR ? 4 * D : 2 * D;
@@ -566,28 +638,44 @@ struct Dop853Machine : OrbitCommon {
     // ST_S2..ST_S12 = 2..12
     ST_FSAL = 13, ST_S14 = 14, ST_S15 = 15, ST_S16 = 16
   };
-  // Stage slots follow the reference's use of k1..k10 (k2/k3 are reused by
-  // stages 11/12, k4/k5 hold the 8th-order increment / new state after stage
-  // 12); s14/s15 keep the first two dense-output stages so that k10/k2/k3
-  // stay available for the interpolation coefficients.  y0 and k1 (read by
-  // every stage) live in registers; k2..k10, s14, s15 live in a per-thread
-  // slot store (shared memory in the kernel, strided by the block size).
-  static constexpr int kSlots = 11;
-  double y0[N], k1[N];
-  double* ks;   // slot store: ks[(slot * N + i) * kstride]
-  int kstride;
-  // reference name k<j> (j = 2..10) or s14/s15 (j = 14, 15) -> slot
+  enum { K1 = 0, K2 = 1, K3 = 2, K4 = 3, K5 = 4, K6 = 5, K7 = 6, K8 = 7, K9 = 8, K10 = 9,
+         S14 = 10, S15 = 11 };
+  // All stage slots live in a per-thread slot store (shared memory in the
+  // kernel, strided by the block size: bank-conflict free); only y0 stays in
+  // registers.
+  static constexpr int kSlots = 12;
   static constexpr int kSlotDoubles = kSlots * N;
+  double y0[N];
+  double* ks;  // slot store: ks[(slot * N + i) * kstride]
+  int kstride;
   GPC_HD GPC_FI void bind(double* base, int stride)
   {
     ks = base;
     kstride = stride;
   }
-  GPC_HD GPC_FI double& K(int j, int i) const { return ks[((j <= 10 ? j - 2 : j - 5) * N + i) * kstride]; }
+  GPC_HD GPC_FI double& K(int s, int i) const { return ks[(s * N + i) * kstride]; }
   double h, hnew, hmax, pos_neg, facold, rtol, atol;
   double t_current, t_old, t_old_older, dnf;
   int stage;
   bool reject;
+
+  // Lanes of a warp run the stages of their (different) orbits in lock step:
+  // an attempt occupies slots 0..10 (stages 2..12), slot 11 (the FSAL
+  // evaluation) and, only when some lane of the warp has an output time in
+  // its step, slots 12..14 (the dense-output stages); the kernel advances
+  // the slot for the whole warp (next_slot).  A lane with nothing to compute
+  // in a slot (a rejected attempt, a step without output time, a new orbit
+  // waiting for slot 0) evaluates the force at y0 and discards it.  The two
+  // start-up evaluations of a new orbit run in whatever slots follow its
+  // pick-up.
+  GPC_HD GPC_FI static int slot_stage(int slot) { return slot + 2; }
+  GPC_HD GPC_FI bool active_in(int slot) const { return stage < 2 || stage == slot_stage(slot); }
+  GPC_HD GPC_FI bool wants_dense() const { return !done && stage == ST_S14; }
+  GPC_HD GPC_FI static int next_slot(int slot, bool any_dense)
+  {
+    if (slot == 11) return any_dense ? 12 : 0;
+    return slot >= 14 ? 0 : slot + 1;
+  }
 
   GPC_HD GPC_FI void begin_attempt()
   {
@@ -624,114 +712,40 @@ struct Dop853Machine : OrbitCommon {
     stage = ST_INIT1;
   }
 
-  // Lanes of a warp run the stages of their (different) orbits in lock step:
-  // every step attempt is a fixed cycle of kCycle force evaluations --
-  // stages 2..12 in slots 0..10, the FSAL evaluation in slot 11 and the
-  // three dense-output stages in slots 12..14 -- driven by the kernel's
-  // iteration counter, so the stage-combination code is warp-uniform.  A
-  // lane that has nothing to compute in a slot (a rejected attempt, a step
-  // without output time, a new orbit waiting for slot 0) evaluates the force
-  // at y0 and discards it.  The two start-up evaluations of a new orbit run
-  // in whatever slots follow its pick-up.
-  static constexpr int kCycle = 15;
-  GPC_HD GPC_FI static int slot_stage(int slot) { return slot + 2; }  // 2..12, 13 FSAL, 14..16
-  GPC_HD GPC_FI bool active_in(int slot) const { return stage < 2 || stage == slot_stage(slot); }
-
   GPC_HD GPC_FI void point(double* y, int slot) const
   {
-    using namespace dp;
-    if (!active_in(slot)) {
+    if (!active_in(slot) || stage == ST_INIT1) {
 #pragma unroll
       for (int i = 0; i < N; i++) y[i] = y0[i];
       return;
     }
-    switch (stage) {
-      case ST_INIT1:
+    if (stage == ST_INIT2) {  // explicit Euler step (leung_dop853.c:310)
 #pragma unroll
-        for (int i = 0; i < N; i++) y[i] = y0[i];
-        break;
-      case ST_INIT2:  // explicit Euler step (leung_dop853.c:310)
-#pragma unroll
-        for (int i = 0; i < N; i++) y[i] = y0[i] + h * k1[i];
-        break;
-      case 2:
-#pragma unroll
-        for (int i = 0; i < N; i++) y[i] = y0[i] + h * a21 * k1[i];
-        break;
-      case 3:
-#pragma unroll
-        for (int i = 0; i < N; i++) y[i] = y0[i] + h * (a31 * k1[i] + a32 * K(2, i));
-        break;
-      case 4:
-#pragma unroll
-        for (int i = 0; i < N; i++) y[i] = y0[i] + h * (a41 * k1[i] + a43 * K(3, i));
-        break;
-      case 5:
-#pragma unroll
-        for (int i = 0; i < N; i++) y[i] = y0[i] + h * (a51 * k1[i] + a53 * K(3, i) + a54 * K(4, i));
-        break;
-      case 6:
-#pragma unroll
-        for (int i = 0; i < N; i++) y[i] = y0[i] + h * (a61 * k1[i] + a64 * K(4, i) + a65 * K(5, i));
-        break;
-      case 7:
-#pragma unroll
-        for (int i = 0; i < N; i++)
-          y[i] = y0[i] + h * (a71 * k1[i] + a74 * K(4, i) + a75 * K(5, i) + a76 * K(6, i));
-        break;
-      case 8:
-#pragma unroll
-        for (int i = 0; i < N; i++)
-          y[i] = y0[i] + h * (a81 * k1[i] + a84 * K(4, i) + a85 * K(5, i) + a86 * K(6, i) + a87 * K(7, i));
-        break;
-      case 9:
-#pragma unroll
-        for (int i = 0; i < N; i++)
-          y[i] = y0[i] + h * (a91 * k1[i] + a94 * K(4, i) + a95 * K(5, i) + a96 * K(6, i) +
-                              a97 * K(7, i) + a98 * K(8, i));
-        break;
-      case 10:
-#pragma unroll
-        for (int i = 0; i < N; i++)
-          y[i] = y0[i] + h * (a101 * k1[i] + a104 * K(4, i) + a105 * K(5, i) + a106 * K(6, i) +
-                              a107 * K(7, i) + a108 * K(8, i) + a109 * K(9, i));
-        break;
-      case 11:
-#pragma unroll
-        for (int i = 0; i < N; i++)
-          y[i] = y0[i] + h * (a111 * k1[i] + a114 * K(4, i) + a115 * K(5, i) + a116 * K(6, i) +
-                              a117 * K(7, i) + a118 * K(8, i) + a119 * K(9, i) + a1110 * K(10, i));
-        break;
-      case 12:
-#pragma unroll
-        for (int i = 0; i < N; i++)
-          y[i] = y0[i] + h * (a121 * k1[i] + a124 * K(4, i) + a125 * K(5, i) + a126 * K(6, i) +
-                              a127 * K(7, i) + a128 * K(8, i) + a129 * K(9, i) + a1210 * K(10, i) +
-                              a1211 * K(2, i));
-        break;
-      case ST_FSAL:
-#pragma unroll
-        for (int i = 0; i < N; i++) y[i] = K(5, i);
-        break;
-      case ST_S14:
-#pragma unroll
-        for (int i = 0; i < N; i++)
-          y[i] = y0[i] + h * (a141 * k1[i] + a147 * K(7, i) + a148 * K(8, i) + a149 * K(9, i) +
-                              a1410 * K(10, i) + a1411 * K(2, i) + a1412 * K(3, i) + a1413 * K(4, i));
-        break;
-      case ST_S15:
-#pragma unroll
-        for (int i = 0; i < N; i++)
-          y[i] = y0[i] + h * (a151 * k1[i] + a156 * K(6, i) + a157 * K(7, i) + a158 * K(8, i) +
-                              a1511 * K(2, i) + a1512 * K(3, i) + a1513 * K(4, i) + a1514 * K(14, i));
-        break;
-      default:  // ST_S16
-#pragma unroll
-        for (int i = 0; i < N; i++)
-          y[i] = y0[i] + h * (a161 * k1[i] + a166 * K(6, i) + a167 * K(7, i) + a168 * K(8, i) +
-                              a169 * K(9, i) + a1613 * K(4, i) + a1614 * K(14, i) + a1615 * K(15, i));
-        break;
+      for (int i = 0; i < N; i++) y[i] = y0[i] + h * K(K1, i);
+      return;
     }
+    if (stage == ST_FSAL) {  // the new state
+#pragma unroll
+      for (int i = 0; i < N; i++) y[i] = K(K5, i);
+      return;
+    }
+    const DopStageTable& tb = dop_table();
+    const int n = tb.nterm[stage];
+    double acc[N];
+    {
+      const int s0 = tb.slot[stage][0];
+      const double c0 = tb.coef[stage][0];
+#pragma unroll
+      for (int i = 0; i < N; i++) acc[i] = c0 * K(s0, i);
+    }
+    for (int tt = 1; tt < n; tt++) {
+      const int s = tb.slot[stage][tt];
+      const double c = tb.coef[stage][tt];
+#pragma unroll
+      for (int i = 0; i < N; i++) acc[i] += c * K(s, i);
+    }
+#pragma unroll
+    for (int i = 0; i < N; i++) y[i] = y0[i] + h * acc[i];
   }
 
   GPC_HD GPC_FI bool output_pending() const
@@ -754,142 +768,96 @@ struct Dop853Machine : OrbitCommon {
         d[3 * D + k] = a[D + k];
       }
     }
-    switch (stage) {
-      case ST_INIT1: {  // leung_dop853.c:296-308
+    if (stage == ST_INIT1) {  // leung_dop853.c:296-308
+      double dny = 0.0;
+      dnf = 0.0;
 #pragma unroll
-        for (int i = 0; i < N; i++) k1[i] = d[i];
-        double dny = 0.0;
-        dnf = 0.0;
-#pragma unroll
-        for (int i = 0; i < N; i++) {
-          const double sk = atol + rtol * fabs(y0[i]);
-          double sqr = k1[i] / sk;
-          dnf += sqr * sqr;
-          sqr = y0[i] / sk;
-          dny += sqr * sqr;
-        }
-        h = csign(dmin(sqrt(dny / dnf) * 0.01, fabs(hmax)), pos_neg);
-        stage = ST_INIT2;
-        return;
+      for (int i = 0; i < N; i++) {
+        K(K1, i) = d[i];
+        const double sk = atol + rtol * fabs(y0[i]);
+        double sqr = d[i] / sk;
+        dnf += sqr * sqr;
+        sqr = y0[i] / sk;
+        dny += sqr * sqr;
       }
-      case ST_INIT2: {  // leung_dop853.c:309-324
-#pragma unroll
-        for (int i = 0; i < N; i++) K(2, i) = d[i];
-        double der2 = 0.0;
-#pragma unroll
-        for (int i = 0; i < N; i++) {
-          const double sk = atol + rtol * fabs(y0[i]);
-          const double sqr = (K(2, i) - k1[i]) / sk;
-          der2 += sqr * sqr;
-        }
-        der2 = sqrt(der2) / h;
-        const double der12 = dmax(fabs(der2), sqrt(dnf));
-        const double h1 = pow(0.01 / der12, 1.0 / 8.0);
-        h = csign(dmin(100.0 * fabs(h), dmin(fabs(h1), fabs(hmax))), pos_neg);
-        begin_attempt();
-        return;
-      }
-      case 2:
-#pragma unroll
-        for (int i = 0; i < N; i++) K(2, i) = d[i];
-        break;
-      case 3:
-#pragma unroll
-        for (int i = 0; i < N; i++) K(3, i) = d[i];
-        break;
-      case 4:
-#pragma unroll
-        for (int i = 0; i < N; i++) K(4, i) = d[i];
-        break;
-      case 5:
-#pragma unroll
-        for (int i = 0; i < N; i++) K(5, i) = d[i];
-        break;
-      case 6:
-#pragma unroll
-        for (int i = 0; i < N; i++) K(6, i) = d[i];
-        break;
-      case 7:
-#pragma unroll
-        for (int i = 0; i < N; i++) K(7, i) = d[i];
-        break;
-      case 8:
-#pragma unroll
-        for (int i = 0; i < N; i++) K(8, i) = d[i];
-        break;
-      case 9:
-#pragma unroll
-        for (int i = 0; i < N; i++) K(9, i) = d[i];
-        break;
-      case 10:
-#pragma unroll
-        for (int i = 0; i < N; i++) K(10, i) = d[i];
-        break;
-      case 11:
-#pragma unroll
-        for (int i = 0; i < N; i++) K(2, i) = d[i];
-        break;
-      case 12: {
-#pragma unroll
-        for (int i = 0; i < N; i++) K(3, i) = d[i];
-        after_stage12();
-        return;
-      }
-      case ST_FSAL: {
-#pragma unroll
-        for (int i = 0; i < N; i++) K(4, i) = d[i];
-        nsteps++;
-        if (output_pending()) {
-          stage = ST_S14;
-          return;
-        }
-        finish_step(out);
-        return;
-      }
-      case ST_S14:
-#pragma unroll
-        for (int i = 0; i < N; i++) K(14, i) = d[i];
-        stage = ST_S15;
-        return;
-      case ST_S15:
-#pragma unroll
-        for (int i = 0; i < N; i++) K(15, i) = d[i];
-        stage = ST_S16;
-        return;
-      default: {  // ST_S16: dense output (leung_dop853.c:441-474)
-        while (output_pending()) {
-          const double sv = (t[iout + 1] - t_old) / h, s1 = 1.0 - sv;
-          double v[N];
-#pragma unroll
-          for (int i = 0; i < N; i++) {
-            const double rc1 = y0[i];
-            const double ydiff = K(5, i) - y0[i];
-            const double bspl = h * k1[i] - ydiff;
-            const double rc4 = ydiff - h * K(4, i) - bspl;
-            double rc5 = d41 * k1[i] + d46 * K(6, i) + d47 * K(7, i) + d48 * K(8, i) + d49 * K(9, i) +
-                         d410 * K(10, i) + d411 * K(2, i) + d412 * K(3, i);
-            double rc6 = d51 * k1[i] + d56 * K(6, i) + d57 * K(7, i) + d58 * K(8, i) + d59 * K(9, i) +
-                         d510 * K(10, i) + d511 * K(2, i) + d512 * K(3, i);
-            double rc7 = d61 * k1[i] + d66 * K(6, i) + d67 * K(7, i) + d68 * K(8, i) + d69 * K(9, i) +
-                         d610 * K(10, i) + d611 * K(2, i) + d612 * K(3, i);
-            double rc8 = d71 * k1[i] + d76 * K(6, i) + d77 * K(7, i) + d78 * K(8, i) + d79 * K(9, i) +
-                         d710 * K(10, i) + d711 * K(2, i) + d712 * K(3, i);
-            rc5 = h * (rc5 + d413 * K(4, i) + d414 * K(14, i) + d415 * K(15, i) + d416 * d[i]);
-            rc6 = h * (rc6 + d513 * K(4, i) + d514 * K(14, i) + d515 * K(15, i) + d516 * d[i]);
-            rc7 = h * (rc7 + d613 * K(4, i) + d614 * K(14, i) + d615 * K(15, i) + d616 * d[i]);
-            rc8 = h * (rc8 + d713 * K(4, i) + d714 * K(14, i) + d715 * K(15, i) + d716 * d[i]);
-            v[i] = rc1 +
-                   sv * (ydiff +
-                         s1 * (bspl + sv * (rc4 + s1 * (rc5 + sv * (rc6 + s1 * (rc7 + sv * rc8))))));
-          }
-          iout++;
-          out(iout, v);
-        }
-        finish_step(out);
-        return;
-      }
+      h = csign(dmin(sqrt(dny / dnf) * 0.01, fabs(hmax)), pos_neg);
+      stage = ST_INIT2;
+      return;
     }
-    stage++;
+    if (stage == ST_INIT2) {  // leung_dop853.c:309-324
+      double der2 = 0.0;
+#pragma unroll
+      for (int i = 0; i < N; i++) {
+        const double sk = atol + rtol * fabs(y0[i]);
+        const double sqr = (d[i] - K(K1, i)) / sk;
+        der2 += sqr * sqr;
+      }
+      der2 = sqrt(der2) / h;
+      const double der12 = dmax(fabs(der2), sqrt(dnf));
+      const double h1 = pow(0.01 / der12, 1.0 / 8.0);
+      h = csign(dmin(100.0 * fabs(h), dmin(fabs(h1), fabs(hmax))), pos_neg);
+      begin_attempt();
+      return;
+    }
+    const int dst = dop_table().dst[stage];
+    if (dst >= 0) {
+#pragma unroll
+      for (int i = 0; i < N; i++) K(dst, i) = d[i];
+    }
+    if (stage < 12) {
+      stage++;
+      return;
+    }
+    if (stage == 12) {
+      after_stage12();
+      return;
+    }
+    if (stage == ST_FSAL) {
+      nsteps++;
+      if (output_pending()) {
+        stage = ST_S14;
+        return;
+      }
+      finish_step(out);
+      return;
+    }
+    if (stage < ST_S16) {
+      stage++;
+      return;
+    }
+    // ST_S16: dense output (leung_dop853.c:441-474), d = stage-16 derivative
+    while (output_pending()) {
+      const double sv = (t[iout + 1] - t_old) / h, s1 = 1.0 - sv;
+      double v[N];
+#pragma unroll
+      for (int i = 0; i < N; i++) {
+        const double k1 = K(K1, i), k2 = K(K2, i), k3 = K(K3, i), k4 = K(K4, i);
+        const double k6 = K(K6, i), k7 = K(K7, i), k8 = K(K8, i), k9 = K(K9, i);
+        const double k10 = K(K10, i), s14 = K(S14, i), s15 = K(S15, i);
+        const double rc1 = y0[i];
+        const double ydiff = K(K5, i) - y0[i];
+        const double bspl = h * k1 - ydiff;
+        const double rc4 = ydiff - h * k4 - bspl;
+        double rc5 = d41 * k1 + d46 * k6 + d47 * k7 + d48 * k8 + d49 * k9 + d410 * k10 +
+                     d411 * k2 + d412 * k3;
+        double rc6 = d51 * k1 + d56 * k6 + d57 * k7 + d58 * k8 + d59 * k9 + d510 * k10 +
+                     d511 * k2 + d512 * k3;
+        double rc7 = d61 * k1 + d66 * k6 + d67 * k7 + d68 * k8 + d69 * k9 + d610 * k10 +
+                     d611 * k2 + d612 * k3;
+        double rc8 = d71 * k1 + d76 * k6 + d77 * k7 + d78 * k8 + d79 * k9 + d710 * k10 +
+                     d711 * k2 + d712 * k3;
+        rc5 = h * (rc5 + d413 * k4 + d414 * s14 + d415 * s15 + d416 * d[i]);
+        rc6 = h * (rc6 + d513 * k4 + d514 * s14 + d515 * s15 + d516 * d[i]);
+        rc7 = h * (rc7 + d613 * k4 + d614 * s14 + d615 * s15 + d616 * d[i]);
+        rc8 = h * (rc8 + d713 * k4 + d714 * s14 + d715 * s15 + d716 * d[i]);
+        v[i] = rc1 +
+               sv * (ydiff +
+                     s1 * (bspl + sv * (rc4 + s1 * (rc5 + sv * (rc6 + s1 * (rc7 + sv * rc8))))));
+      }
+      iout++;
+      out(iout, v);
+    }
+    finish_step(out);
   }
 
   GPC_HD void after_stage12()
@@ -899,21 +867,22 @@ struct Dop853Machine : OrbitCommon {
     t_old_older = t_old;
     t_old = t_current;
     t_current = t_current + h;
-#pragma unroll
-    for (int i = 0; i < N; i++) {
-      K(4, i) = b1 * k1[i] + b6 * K(6, i) + b7 * K(7, i) + b8 * K(8, i) + b9 * K(9, i) + b10 * K(10, i) +
-              b11 * K(2, i) + b12 * K(3, i);
-      K(5, i) = y0[i] + h * K(4, i);
-    }
     double e = 0.0, e2 = 0.0;
 #pragma unroll
     for (int i = 0; i < N; i++) {
-      const double sk = atol + rtol * dmax(fabs(y0[i]), fabs(K(5, i)));
-      double erri = K(4, i) - bhh1 * k1[i] - bhh2 * K(9, i) - bhh3 * K(3, i);
+      const double k1 = K(K1, i), k2 = K(K2, i), k3 = K(K3, i), k6 = K(K6, i), k7 = K(K7, i);
+      const double k8 = K(K8, i), k9 = K(K9, i), k10 = K(K10, i);
+      const double k4 =
+          b1 * k1 + b6 * k6 + b7 * k7 + b8 * k8 + b9 * k9 + b10 * k10 + b11 * k2 + b12 * k3;
+      const double k5 = y0[i] + h * k4;
+      K(K4, i) = k4;
+      K(K5, i) = k5;
+      const double sk = atol + rtol * dmax(fabs(y0[i]), fabs(k5));
+      double erri = k4 - bhh1 * k1 - bhh2 * k9 - bhh3 * k3;
       double sqr = erri / sk;
       e2 += sqr * sqr;
-      erri = er1 * k1[i] + er6 * K(6, i) + er7 * K(7, i) + er8 * K(8, i) + er9 * K(9, i) + er10 * K(10, i) +
-             er11 * K(2, i) + er12 * K(3, i);
+      erri = er1 * k1 + er6 * k6 + er7 * k7 + er8 * k8 + er9 * k9 + er10 * k10 + er11 * k2 +
+             er12 * k3;
       sqr = erri / sk;
       e += sqr * sqr;
     }
@@ -948,12 +917,12 @@ struct Dop853Machine : OrbitCommon {
   }
 
   template <class W>
-  GPC_HD void finish_step(W& out)
+  GPC_HD void finish_step(W& /*out*/)
   {
 #pragma unroll
     for (int i = 0; i < N; i++) {
-      k1[i] = K(4, i);
-      y0[i] = K(5, i);
+      K(K1, i) = K(K4, i);
+      y0[i] = K(K5, i);
     }
     hnew = (fabs(hnew) > fabs(hmax)) ? pos_neg * hmax : hnew;
     if (reject) hnew = pos_neg * dmin(fabs(hnew), fabs(h));
@@ -990,13 +959,13 @@ template <class M, class F, class W>
 GPC_HD void run_orbit(M& m, F& force, W& out)
 {
   double y[M::NY], q[M::NA], a[M::NA];
-  unsigned iter = 0;
+  int slot = 0;
   while (!m.done) {
-    const int slot = (int)(iter++ % 15u);
     m.point(y, slot);
     M::pos(y, q);
     force(q, a);
     m.consume(y, a, out, slot);
+    slot = M::next_slot(slot, m.wants_dense());
   }
   fill_unreached_rows(m, out);
 }
