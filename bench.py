@@ -69,6 +69,29 @@ def precision_workload(n, seed=2):
     return ics, np.array([0.0, 200.0])
 
 
+def ragged_workload(seed=4, ngroup=512):
+    """The ragged multi-potential configuration: 512 MWPotential2014 variants
+    (MiyamotoNagai a, b, NFW a and the three amplitudes each scaled by
+    U(0.8, 1.2)), U(1024, 16384) orbits per variant with config-0 initial
+    conditions, DOP853 rtol = 1e-9, t in [0, 50], 51 snapshots."""
+    import galpy_b200 as gb
+
+    rng = np.random.default_rng(seed)
+    _, pt, pa = gb.parse_pot(gb.MWPotential2014())
+    args = np.tile(pa, (ngroup, 1))
+    scale = rng.uniform(0.8, 1.2, (ngroup, 6))
+    args[:, 6] *= scale[:, 0]  # MiyamotoNagai a
+    args[:, 7] *= scale[:, 1]  # MiyamotoNagai b
+    args[:, 9] *= scale[:, 2]  # NFW a
+    args[:, 0] *= scale[:, 3]  # bulge amplitude
+    args[:, 5] *= scale[:, 4]  # disk amplitude
+    args[:, 8] *= scale[:, 5]  # halo amplitude
+    counts = rng.integers(1024, 16385, ngroup)
+    group = np.repeat(np.arange(ngroup), counts).astype(np.int32)
+    ics, _ = precision_workload(len(group), seed=seed)
+    return pt, args, group, ics, np.linspace(0.0, 50.0, 51)
+
+
 def stats(x):
     x = np.asarray(x)
     return {"median": float(np.median(x)), "p99": float(np.quantile(x, 0.99)),
@@ -175,6 +198,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--mixed-orbits", type=int, default=1 << 22)
+    ap.add_argument("--no-ragged", action="store_true")
+    ap.add_argument("--case", default="batching", choices=["batching", "uniform"],
+                    help="uniform: R ~ U(0.5, 2), shared t in [0, 50] (101 snapshots) "
+                         "(a throughput-bound case for profiling the same kernel)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -204,7 +231,11 @@ def main():
         pg = dist
 
     pt, pa = mw14_args()
-    ics, t = workload(args.orbits, seed=1 + 1000 * rank)
+    if args.case == "uniform":
+        ics, _ = precision_workload(args.orbits, seed=1 + 1000 * rank)
+        t = np.repeat(np.linspace(0.0, 50.0, NT)[None, :], len(ics), axis=0)
+    else:
+        ics, t = workload(args.orbits, seed=1 + 1000 * rank)
     n = len(ics)
     comps, ncomp = gb.compile_potential((pt, pa))
     sig = gb.signature((pt, pa))
@@ -219,7 +250,7 @@ def main():
     def run(precision="fp64"):
         gb.integrate_device(comps_d, ncomp, w0, t_d, out, err, "dop853_cuda", nsteps=nsteps,
                             rtol=RTOL, atol=ATOL, precision=precision, stream=stream,
-                            signature=sig)
+                            signature=sig, comps_host=comps)
 
     def timed(precision, K, W):
         for _ in range(W):
@@ -296,8 +327,12 @@ def main():
 
     if not args.no_mixed:
         result["mixed"] = mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg,
-                                    args.mixed_orbits)
+                                    args.mixed_orbits, comps)
         result["gpu_launches"] += 4
+
+    if not args.no_ragged:
+        result["ragged"] = ragged_leg(gb, torch, dev, stream, pg)
+        result["gpu_launches"] += 2
 
     if not args.no_e2e:
         result["e2e"] = e2e(gb, ics, t, pt, pa, args.steps, pg, dev, steps)
@@ -315,7 +350,45 @@ def main():
         print(json.dumps(result), flush=True)
 
 
-def mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg, n):
+def ragged_leg(gb, torch, dev, stream, pg):
+    """One launch over 512 potential-parameter groups (about 4.3 M orbits)."""
+    pt, args, group, ics, t = ragged_workload()
+    n = len(group)
+    comps, ncomp = gb.compile_potential((pt, args.ravel()), ngroup=len(args))
+    comps_d = torch.tensor(comps, device=dev)
+    sig = gb.signature((pt, args[0]))
+    w0 = torch.tensor(cyl_to_rect(ics).T.copy(), device=dev)
+    t_d = torch.tensor(t, device=dev)
+    g_d = torch.tensor(group, device=dev)
+    out = torch.empty((6, len(t), n), dtype=torch.float64, device=dev)
+    err = torch.empty(n, dtype=torch.int32, device=dev)
+    ns = torch.empty(n, dtype=torch.int64, device=dev)
+    ms = []
+    for rep in range(2):  # warm-up + timed
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        gb.integrate_device(comps_d, ncomp, w0, t_d, out, err, "dop853_cuda", nsteps=ns,
+                            group=g_d, rtol=1e-9, atol=1e-9, stream=stream, signature=sig)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    E0 = torch.empty(n, dtype=torch.float64, device=dev)
+    E1 = torch.empty(n, dtype=torch.float64, device=dev)
+    gb.energy_device(comps_d, ncomp, w0, E0, group=g_d, stream=stream)
+    gb.energy_device(comps_d, ncomp, out[:, len(t) - 1, :], E1, group=g_d, stream=stream)
+    torch.cuda.synchronize()
+    steps = float(ns.sum().item())
+    return {"workload": f"ragged: {len(args)} MWPotential2014 variants, {n} orbits, dop853 "
+                        "rtol=atol=1e-9, t in [0,50], 51 snapshots, one launch",
+            "value": steps / (ms[-1] * 1e-3), "unit": "orbit-steps/s", "ms": ms[-1],
+            "accepted_steps": steps, "orbits_with_err": int((err != 0).sum().item()),
+            "energy_rel_err": stats(torch.abs(E1 / E0 - 1).cpu().numpy())}
+
+
+def mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg, n, comps_host=None):
     """FP32-force / FP64-state vs all-FP64 on the precision configuration
     (symplec4, dt = 0.01, 20,000 steps, final state only): throughput, the
     per-orbit relative energy drift, and the final phase-space difference."""
@@ -339,7 +412,7 @@ def mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg, n):
             e0.record(stream)
             gb.integrate_device(comps_d, ncomp, w0, t_d, out, err, "symplec4_cuda", nsteps=ns,
                                 dt=0.01, out_row0=1, precision=prec, stream=stream,
-                                signature=sig)
+                                signature=sig, comps_host=comps_host)
             e1.record(stream)
             torch.cuda.synchronize()
             ms_list.append(e0.elapsed_time(e1))

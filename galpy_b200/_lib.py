@@ -93,6 +93,7 @@ class GalpyCudaLaunch(ctypes.Structure):
         ("signature", ctypes.c_int),
         ("schedule", ctypes.c_int),
         ("variant", ctypes.c_int),
+        ("comps_host", ctypes.c_void_p),
     ]
 
 

@@ -52,12 +52,21 @@ inline double gamma_star_cutoff(double a)
 
 // Chebyshev interpolation of gamma*(a, u) on kChebN equal intervals of
 // [0, U], kChebC nodes each (values at the Chebyshev points, coefficients
-// by the discrete cosine sums), computed in long double.
+// by the discrete cosine sums), converted to the power basis of the
+// interval's local variable x in [-1, 1] (T_j expanded by its three-term
+// recurrence), all in long double.
 inline void build_gamma_star_table(double a, double U, double (*cheb)[kChebC])
 {
   const long double w = (long double)U / kChebN;
   const long double pi = 3.141592653589793238462643383279502884L;
-  long double f[kChebC];
+  // power-basis coefficients of T_0 .. T_{kChebC-1}
+  long double T[kChebC][kChebC] = {};
+  T[0][0] = 1.0L;
+  if (kChebC > 1) T[1][1] = 1.0L;
+  for (int j = 2; j < kChebC; j++)
+    for (int m = 0; m < kChebC; m++)
+      T[j][m] = (m > 0 ? 2.0L * T[j - 1][m - 1] : 0.0L) - T[j - 2][m];
+  long double f[kChebC], cj[kChebC];
   for (int k = 0; k < kChebN; k++) {
     for (int i = 0; i < kChebC; i++) {
       const long double x = cosl(pi * (i + 0.5L) / kChebC);
@@ -68,7 +77,12 @@ inline void build_gamma_star_table(double a, double U, double (*cheb)[kChebC])
       for (int i = 0; i < kChebC; i++) s += f[i] * cosl(pi * j * (i + 0.5L) / kChebC);
       s *= 2.0L / kChebC;
       if (j == 0) s *= 0.5L;
-      cheb[k][j] = (double)s;
+      cj[j] = s;
+    }
+    for (int m = 0; m < kChebC; m++) {
+      long double s = 0.0L;
+      for (int j = 0; j < kChebC; j++) s += cj[j] * T[j][m];
+      cheb[k][m] = (double)s;
     }
   }
 }

@@ -78,6 +78,9 @@ struct KArgs {
   unsigned long long* done_count;
   const int* order;  // work-queue order (longest first), or NULL
   int variational_nv; // values per input row of variational runs (0 otherwise)
+  // scalar parameters of the (single) potential, read from the constant bank
+  // by the kernels whose POT takes them directly
+  double scal[kMaxComp * kScalarStride];
 };
 
 template <int NV, int D, bool CYL_OK>
@@ -105,13 +108,13 @@ __device__ __forceinline__ void load_state(const KArgs& A, long long i, double* 
 // MINB: minimum resident blocks per SM requested from the register
 // allocator (1 = no cap; larger values trade registers for occupancy).
 template <class M, int D, int PREC, bool VAR, class POT, int MINB>
-__global__ void __launch_bounds__(128, MINB) orbit_kernel(const KArgs A)
+__global__ void __launch_bounds__(128, MINB) orbit_kernel(const __grid_constant__ KArgs A)
 {
   constexpr bool CYL_OK = !VAR;
   using Rows = DevRows<M::NV, D, CYL_OK>;
   extern __shared__ double slot_store[];
   M m;
-  m.bind(slot_store + threadIdx.x, blockDim.x);
+  m.bind(slot_store + threadIdx.x);
   long long i = 0;
   bool active = false, aborting = false;
   const GpComp* comps = A.comps;
@@ -139,7 +142,7 @@ __global__ void __launch_bounds__(128, MINB) orbit_kernel(const KArgs A)
       double y[M::NY], q[M::NA], a[M::NA];
       m.point(y, slot);
       M::pos(y, q);
-      eval_force<D, PREC, VAR, POT>(comps, A.ncomp, q, a);
+      eval_force<D, PREC, VAR, POT>(comps, A.ncomp, q, a, A.scal);
       Rows rows{&A.out, i};
       m.consume(y, a, rows, slot);
     }
@@ -252,7 +255,8 @@ static KernelInfo pick_plain(int planar, int method, int variant)
 // sig: GALPY_CUDA_SIG_MW14 selects the kernels with the MWPotential2014
 // component list fixed at compile time (plain runs); variational runs walk
 // the component list at run time.
-static KernelInfo pick_kernel(int planar, int var, int prec, int method, int sig, int variant)
+static KernelInfo pick_kernel(int planar, int var, int prec, int method, int sig, int variant,
+                              bool direct)
 {
   if (var) {
     if (prec != GALPY_CUDA_FP64) return KernelInfo();  // variational runs are float64 only
@@ -260,11 +264,14 @@ static KernelInfo pick_kernel(int planar, int var, int prec, int method, int sig
                   : pick_kernel_dim<3, PREC_FP64, true, DynPot>(method, 0);
   }
   const bool mw14 = sig == GALPY_CUDA_SIG_MW14;
-  if (prec == GALPY_CUDA_F32FORCE)
-    return mw14 ? pick_plain<PREC_F32, MW14Pot>(planar, method, variant)
-                : pick_plain<PREC_F32, DynPot>(planar, method, variant);
-  return mw14 ? pick_plain<PREC_FP64, MW14Pot>(planar, method, variant)
-              : pick_plain<PREC_FP64, DynPot>(planar, method, variant);
+  if (prec == GALPY_CUDA_F32FORCE) {
+    if (!mw14) return pick_plain<PREC_F32, DynPot>(planar, method, variant);
+    return direct ? pick_plain<PREC_F32, MW14Pot>(planar, method, variant)
+                  : pick_plain<PREC_F32, MW14GroupPot>(planar, method, variant);
+  }
+  if (!mw14) return pick_plain<PREC_FP64, DynPot>(planar, method, variant);
+  return direct ? pick_plain<PREC_FP64, MW14Pot>(planar, method, variant)
+                : pick_plain<PREC_FP64, MW14GroupPot>(planar, method, variant);
 }
 
 static int signature_of(int npot, const int* pot_type)
@@ -287,12 +294,24 @@ struct Scratch {  // device scratch of one launch (64 bytes)
 };
 
 // Launch on `stream`.  scratch: device Scratch (counter zeroed here).
+// Scalars of a single-potential launch for the kernel-parameter path.
+static bool direct_scalars(const galpy_cuda_launch* L, double* scal)
+{
+  if (L->group || !L->comps_host || L->signature != GALPY_CUDA_SIG_MW14) return false;
+  const GpComp* hc = static_cast<const GpComp*>(L->comps_host);
+  for (int k = 0; k < L->ncomp && k < kMaxComp; k++)
+    for (int j = 0; j < kScalarStride; j++) scal[k * kScalarStride + j] = hc[k].c[j];
+  return true;
+}
+
 static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool progress,
                          cudaStream_t stream)
 {
+  double scal[kMaxComp * kScalarStride] = {0.0};
+  const bool direct = direct_scalars(L, scal);
   const KernelInfo ki =
       pick_kernel(L->planar, L->variational, L->precision, L->odeint_type, L->signature,
-                  L->variant);
+                  L->variant, direct);
   KernelFn fn = ki.fn;
   if (!fn) return set_error(GALPY_CUDA_ERR_METHOD, "method/precision combination not implemented");
   KArgs A;
@@ -321,6 +340,7 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
   A.abort_flag = L->abort_flag ? L->abort_flag : &scratch->abort_flag;
   A.done_count = progress ? &scratch->done_count : nullptr;
   A.variational_nv = L->variational ? (L->planar ? 8 : 12) : 0;
+  memcpy(A.scal, scal, sizeof(scal));
   GPC_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(Scratch), stream));
 
   // longest-first work queue (stream-ordered scratch, freed after the launch)
@@ -358,7 +378,8 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
   GPC_CUDA_TRY(cudaGetDevice(&dev));
   int nsm = 0;
   GPC_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  const int block = L->block_size > 0 ? L->block_size : 128;
+  // machines with a slot store run with kSlotStride threads per block
+  const int block = ki.slot_doubles > 0 ? kSlotStride : (L->block_size > 0 ? L->block_size : 128);
   if (block > 128 || block % 32) return set_error(GALPY_CUDA_ERR_ARG, "block_size must be 32..128, multiple of 32");
   const size_t smem = (size_t)ki.slot_doubles * sizeof(double) * block;
   if (smem > 48 * 1024)
@@ -500,6 +521,7 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
   L.err = static_cast<int*>(derr.p);
   L.nsteps = static_cast<long long*>(dsteps.p);
   L.comps = dcomp.p;
+  L.comps_host = comps.data();
   L.ncomp = npot;
   L.dt = dt;
   L.rtol = rtol;
@@ -866,13 +888,16 @@ int galpy_cuda_integrate_device_noalloc(const galpy_cuda_launch* L)
   Scratch* ctl = reinterpret_cast<Scratch*>(scr + kNoAllocCtl);
   cudaStream_t stream = static_cast<cudaStream_t>(L->stream);
 
+  double scal[kMaxComp * kScalarStride] = {0.0};
+  const bool direct = direct_scalars(L, scal);
   const KernelInfo ki =
       pick_kernel(L->planar, L->variational, L->precision, L->odeint_type, L->signature,
-                  L->variant);
+                  L->variant, direct);
   KernelFn fn = ki.fn;
   if (!fn) return set_error(GALPY_CUDA_ERR_METHOD, "method/precision combination not implemented");
   KArgs A;
   memset(&A, 0, sizeof(A));
+  memcpy(A.scal, scal, sizeof(scal));
   A.nobj = L->nobj;
   A.nt = L->nt;
   A.indiv_t = L->indiv_t;
@@ -914,7 +939,7 @@ int galpy_cuda_integrate_device_noalloc(const galpy_cuda_launch* L)
   int dev = 0, nsm = 0;
   GPC_CUDA_TRY(cudaGetDevice(&dev));
   GPC_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  const int block = L->block_size > 0 ? L->block_size : 128;
+  const int block = ki.slot_doubles > 0 ? kSlotStride : (L->block_size > 0 ? L->block_size : 128);
   if (block > 128 || block % 32)
     return set_error(GALPY_CUDA_ERR_ARG, "block_size must be 32..128, multiple of 32");
   const size_t smem = (size_t)ki.slot_doubles * sizeof(double) * block;

@@ -34,6 +34,10 @@
 namespace gpc {
 
 constexpr double kDtSentinel = -9999.99;  // galpy's "estimate the step" marker
+// Stride (in doubles) between consecutive values of one thread in a
+// machine's slot store: the kernel's block size, fixed at compile time so
+// that slot addresses are immediate offsets.
+constexpr int kSlotStride = 128;
 constexpr double kMaxDtReduce = 10000.;
 
 enum : int { M_LEAPFROG = 0, M_RK4 = 1, M_SYMPLEC4 = 3, M_DOP853 = 6 };
@@ -112,19 +116,20 @@ GPC_HD GPC_FI void write_nan_rows(const OutSpec& o, long long i, int from)
 // force adapter: positions -> accelerations (+ K . dq for variational runs)
 // ------------------------------------------------------------------------
 template <int D, int PREC, bool VAR, class POT = DynPot>
-GPC_HD GPC_FI void eval_force(const GpComp* comp, int ncomp, const double* q, double* a)
+GPC_HD GPC_FI void eval_force(const GpComp* comp, int ncomp, const double* q, double* a,
+                              const double* scal = nullptr)
 {
   if (!VAR) {
     if (PREC == PREC_FP64) {
       double ax, ay, az = 0.0;
-      accel<double, D == 2, POT>(comp, ncomp, q[0], q[1], D == 3 ? q[2] : 0.0, ax, ay, az);
+      accel<double, D == 2, POT>(comp, ncomp, q[0], q[1], D == 3 ? q[2] : 0.0, ax, ay, az, scal);
       a[0] = ax;
       a[1] = ay;
       if (D == 3) a[2] = az;
     } else {
       float ax, ay, az = 0.f;
       accel<float, D == 2, POT>(comp, ncomp, (float)q[0], (float)q[1], D == 3 ? (float)q[2] : 0.f,
-                                ax, ay, az);
+                                ax, ay, az, scal);
       a[0] = ax;
       a[1] = ay;
       if (D == 3) a[2] = az;
@@ -182,7 +187,7 @@ struct SymplecticMachine : OrbitCommon {
   static constexpr int NV = 2 * NQ;           // values per output row
   static constexpr int NA = NQ;               // force result size
   static constexpr int kSlotDoubles = 0;      // no slot store needed
-  GPC_HD GPC_FI void bind(double*, int) {}
+  GPC_HD GPC_FI void bind(double*) {}
   GPC_HD GPC_FI bool wants_dense() const { return false; }
   GPC_HD GPC_FI static int next_slot(int slot, bool) { return slot >= 14 ? 0 : slot + 1; }
   GPC_HD GPC_FI static void pos(const double* y, double* q)
@@ -380,7 +385,7 @@ struct RK4Machine : OrbitCommon {
     }
   }
   static constexpr int kSlotDoubles = 0;
-  GPC_HD GPC_FI void bind(double*, int) {}
+  GPC_HD GPC_FI void bind(double*) {}
   GPC_HD GPC_FI bool wants_dense() const { return false; }
   GPC_HD GPC_FI static int next_slot(int slot, bool) { return slot >= 14 ? 0 : slot + 1; }
   enum { EST_A = 0, EST_B = 1, EST_C = 2, MAIN = 3 };
@@ -646,14 +651,9 @@ struct Dop853Machine : OrbitCommon {
   static constexpr int kSlots = 12;
   static constexpr int kSlotDoubles = kSlots * N;
   double y0[N];
-  double* ks;  // slot store: ks[(slot * N + i) * kstride]
-  int kstride;
-  GPC_HD GPC_FI void bind(double* base, int stride)
-  {
-    ks = base;
-    kstride = stride;
-  }
-  GPC_HD GPC_FI double& K(int s, int i) const { return ks[(s * N + i) * kstride]; }
+  double* ks;  // slot store: ks[(slot * N + i) * kSlotStride]
+  GPC_HD GPC_FI void bind(double* base) { ks = base; }
+  GPC_HD GPC_FI double& K(int s, int i) const { return ks[(s * N + i) * kSlotStride]; }
   double h, hnew, hmax, pos_neg, facold, rtol, atol;
   double t_current, t_old, t_old_older, dnf;
   int stage;

@@ -60,7 +60,7 @@ struct GpComp {
   int type;
   int pad;
   double c[16];
-  double cheb[kChebN][kChebC];  // PSwC only
+  double cheb[kChebN][kChebC];  // PSwC only: power-basis coefficients per interval
 };
 
 // ---------------------------------------------------------------- math ---
@@ -87,54 +87,66 @@ template <> struct Num<float> {
   GPC_HD static float rsq(float x) { return gpc::rsqf(x); }
 };
 
-// gamma*(a, u) from the component's Chebyshev table, u in [0, U)
+// gamma*(a, u) from the component's table, u in [0, U): on each interval
+// the degree-11 Chebyshev interpolant is stored in the power basis of the
+// interval's local variable x in [-1, 1] and evaluated by Horner's rule (11
+// dependent FMAs, half the dependency chain of the Clenshaw recurrence; both
+// stay within ~1 ulp here, tests/test_harness.py checks against mpmath).
 template <typename T>
-GPC_HD GPC_FI T gamma_star(const GpComp* __restrict__ cp, T u)
+GPC_HD GPC_FI T gamma_star(const GpComp* __restrict__ cp, T u, T scale)
 {
-  const T s = u * T(ldg(&cp->c[6]));
+  const T s = u * scale;
   int k = (int)s;
   k = k < kChebN - 1 ? k : kChebN - 1;
   const T x = T(2) * (s - T(k)) - T(1);
   const double* c = cp->cheb[k];
-  // Clenshaw recurrence
-  T b1 = T(0), b2 = T(0);
+  T p = T(ldg(c + kChebC - 1));
 #pragma unroll
-  for (int j = kChebC - 1; j > 0; j--) {
-    const T b0 = T(2) * x * b1 - b2 + T(ldg(c + j));
-    b2 = b1;
-    b1 = b0;
-  }
-  return x * b1 - b2 + T(ldg(c));
+  for (int j = kChebC - 2; j >= 0; j--) p = p * x + T(ldg(c + j));
+  return p;
 }
 
 // ------------------------------------------------------------- forces ---
 // Add one component's contribution to the radial factors: the acceleration
 // is a = (x gR, y (gR + gyx), z gz).  TYPE < 0: read the type at run time.
-template <typename T, bool PLANAR, int TYPE>
-GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, T x, T y, T z2, T R2, T r2, T& gR,
-                              T& gz, T& gyx)
+// Scalar parameters of a component: from the compiled record in global
+// memory (read-only path), or from a copy passed as a kernel parameter
+// (constant bank: no load instruction when the index is a compile-time
+// constant) when every orbit of a launch uses the same potential.
+struct ScalarsGlobal {
+  const GpComp* cp;
+  GPC_HD GPC_FI double operator[](int j) const { return ldg(&cp->c[j]); }
+};
+struct ScalarsDirect {
+  const double* p;
+  GPC_HD GPC_FI double operator[](int j) const { return p[j]; }
+};
+
+template <typename T, bool PLANAR, int TYPE, class S>
+GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T y, T z2, T R2,
+                              T r2, T& gR, T& gz, T& gyx)
 {
   const int type = TYPE >= 0 ? TYPE : ldg(&cp->type);
-  const T amp = T(ldg(&cp->c[0]));
+  const T amp = T(sc[0]);
   switch (type) {
     case T_PSWC: {
       // F = -amp M(r)/r^3 r_vec
-      const T u = r2 * T(ldg(&cp->c[1]));
+      const T u = r2 * T(sc[1]);
       T f;
-      if (u < T(ldg(&cp->c[5]))) {
-        const T pw = Num<T>::ex(T(ldg(&cp->c[3])) * Num<T>::lg(r2));  // (r^2)^(-alpha/2)
-        f = -amp * T(ldg(&cp->c[2])) * pw * gamma_star<T>(cp, u);
+      if (u < T(sc[5])) {
+        const T pw = Num<T>::ex(T(sc[3]) * Num<T>::lg(r2));  // (r^2)^(-alpha/2)
+        f = -amp * T(sc[2]) * pw * gamma_star<T>(cp, u, T(sc[6]));
       } else {
         const T ir = Num<T>::rsq(r2);
-        f = -amp * T(ldg(&cp->c[4])) * (ir * ir * ir);
+        f = -amp * T(sc[4]) * (ir * ir * ir);
       }
       gR += f;
       gz += f;
       break;
     }
     case T_MN: {
-      const T a = T(ldg(&cp->c[1]));
-      const T zb2 = z2 + T(ldg(&cp->c[2]));
+      const T a = T(sc[1]);
+      const T zb2 = z2 + T(sc[2]);
       const T izb = Num<T>::rsq(zb2);
       const T s = a + zb2 * izb;  // a + sqrt(z^2 + b^2)
       const T iD = Num<T>::rsq(R2 + s * s);
@@ -145,17 +157,17 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, T x, T y, T z2, T R
     }
     case T_NFW: {
       // Phi = -amp ln(1 + r/a)/r ; F = amp (1/(r^2 (a+r)) - ln(1+r/a)/r^3) r_vec
-      const T a = T(ldg(&cp->c[1]));
+      const T a = T(sc[1]);
       const T ir = Num<T>::rsq(r2);
       const T r = r2 * ir;
-      const T f = amp * ir * ir * (Num<T>::rcp(a + r) - Num<T>::lg1p(r * T(ldg(&cp->c[2]))) * ir);
+      const T f = amp * ir * ir * (Num<T>::rcp(a + r) - Num<T>::lg1p(r * T(sc[2])) * ir);
       gR += f;
       gz += f;
       break;
     }
     case T_HERNQUIST: {
       // Phi = -amp / (2 (r + a)) ; F = -amp / (2 r (r + a)^2) r_vec
-      const T a = T(ldg(&cp->c[1]));
+      const T a = T(sc[1]);
       const T ir = Num<T>::rsq(r2);
       const T ira = Num<T>::rcp(r2 * ir + a);
       const T f = -T(0.5) * amp * ir * ira * ira;
@@ -165,9 +177,9 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, T x, T y, T z2, T R
     }
     case T_LOGHALO: {
       // Phi = amp/2 ln(x^2 + (1-e) y^2 + z^2/q^2 + core^2)
-      const T iq2 = T(ldg(&cp->c[1]));
-      const T ye = T(ldg(&cp->c[3]));
-      const T D = x * x + ye * y * y + z2 * iq2 + T(ldg(&cp->c[2]));
+      const T iq2 = T(sc[1]);
+      const T ye = T(sc[3]);
+      const T D = x * x + ye * y * y + z2 * iq2 + T(sc[2]);
       const T g = -amp * Num<T>::rcp(D);
       gR += g;
       gyx += g * (ye - T(1));
@@ -181,39 +193,58 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, T x, T y, T z2, T R
 
 // Run-time component list (any combination of the supported types).
 struct DynPot {
+  static constexpr bool kDirectScalars = false;
   template <typename T, bool PLANAR>
-  GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, int ncomp, T x, T y, T z2, T R2,
-                                T r2, T& gR, T& gz, T& gyx)
+  GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, const double* /*scal*/, int ncomp,
+                                T x, T y, T z2, T R2, T r2, T& gR, T& gz, T& gyx)
   {
     for (int k = 0; k < ncomp; k++)
-      comp_accel<T, PLANAR, -1>(comp + k, x, y, z2, R2, r2, gR, gz, gyx);
+      comp_accel<T, PLANAR, -1>(comp + k, ScalarsGlobal{comp + k}, x, y, z2, R2, r2, gR, gz, gyx);
   }
 };
 
 // Compile-time component list: the components are inlined side by side.
-template <int... TYPES>
+// DIRECT: the scalars come from `scal` (kScalarStride doubles per component,
+// a kernel-parameter copy), else from the records in global memory.
+constexpr int kScalarStride = 16;
+template <bool DIRECT, int... TYPES>
 struct FixedPot {
+  static constexpr bool kDirectScalars = DIRECT;
   template <typename T, bool PLANAR>
-  GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, int /*ncomp*/, T x, T y, T z2,
-                                T R2, T r2, T& gR, T& gz, T& gyx)
+  GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, const double* scal, int /*ncomp*/,
+                                T x, T y, T z2, T R2, T r2, T& gR, T& gz, T& gyx)
   {
     int k = 0;
-    (comp_accel<T, PLANAR, TYPES>(comp + k++, x, y, z2, R2, r2, gR, gz, gyx), ...);
+    if (DIRECT) {
+      ((comp_accel<T, PLANAR, TYPES>(comp + k, ScalarsDirect{scal + kScalarStride * k}, x, y, z2,
+                                     R2, r2, gR, gz, gyx),
+        ++k),
+       ...);
+    } else {
+      ((comp_accel<T, PLANAR, TYPES>(comp + k, ScalarsGlobal{comp + k}, x, y, z2, R2, r2, gR, gz,
+                                     gyx),
+        ++k),
+       ...);
+    }
   }
 };
-using MW14Pot = FixedPot<T_PSWC, T_MN, T_NFW>;  // galpy's MWPotential2014 order
+// galpy's MWPotential2014 order; MW14Pot takes the scalars as kernel
+// parameters (one potential per launch), MW14GroupPot from the records
+// (parameter groups).
+using MW14Pot = FixedPot<true, T_PSWC, T_MN, T_NFW>;
+using MW14GroupPot = FixedPot<false, T_PSWC, T_MN, T_NFW>;
 
 // Acceleration at (x, y, z); PLANAR evaluates galpy's planar potential (the
 // 3D potential in the plane z = 0) and leaves az untouched.
 template <typename T, bool PLANAR, class POT = DynPot>
 GPC_HD GPC_FI void accel(const GpComp* __restrict__ comp, int ncomp, T x, T y, T z, T& ax, T& ay,
-                         T& az)
+                         T& az, const double* scal = nullptr)
 {
   const T R2 = x * x + y * y;
   const T z2 = PLANAR ? T(0) : z * z;
   const T r2 = R2 + z2;
   T gR = T(0), gz = T(0), gyx = T(0);
-  POT::template sum<T, PLANAR>(comp, ncomp, x, y, z2, R2, r2, gR, gz, gyx);
+  POT::template sum<T, PLANAR>(comp, scal, ncomp, x, y, z2, R2, r2, gR, gz, gyx);
   ax = x * gR;
   ay = y * (gR + gyx);
   if (!PLANAR) az = z * gz;
@@ -257,7 +288,7 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
         const double pw = exp(ldg(&cp->c[3]) * log(r2));  // (r^2)^(-alpha/2)
         double Mr3;                                         // M(r) / r^3
         if (u < ldg(&cp->c[5])) {
-          Mr3 = ldg(&cp->c[2]) * pw * gamma_star<double>(cp, u);
+          Mr3 = ldg(&cp->c[2]) * pw * gamma_star<double>(cp, u, ldg(&cp->c[6]));
         } else {
           const double ir = rsq(r2);
           Mr3 = ldg(&cp->c[4]) * ir * ir * ir;

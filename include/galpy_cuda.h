@@ -151,6 +151,8 @@ typedef struct galpy_cuda_launch {
   int schedule;             /* GALPY_CUDA_SCHED_*; longest-first sorts the work queue
                                (needs ~13 bytes/orbit of stream-ordered scratch) */
   int variant;              /* register budget: 0 compiler default, 1 capped for occupancy */
+  const void *comps_host;   /* optional host copy of `comps` (ncomp records, one group):
+                               its scalars are passed as kernel parameters */
 } galpy_cuda_launch;
 
 int galpy_cuda_integrate_device(const galpy_cuda_launch *launch);

@@ -27,7 +27,11 @@ template <int D, int PREC, bool VAR, class POT>
 struct Force {
   const GpComp* c;
   int n;
-  void operator()(const double* q, double* a) const { eval_force<D, PREC, VAR, POT>(c, n, q, a); }
+  double scal[kMaxComp * kScalarStride];  // the kernel-parameter copy of the scalars
+  void operator()(const double* q, double* a) const
+  {
+    eval_force<D, PREC, VAR, POT>(c, n, q, a, scal);
+  }
 };
 
 template <class M, int D, int PREC, bool VAR, class POT>
@@ -35,11 +39,13 @@ void run_all(int nobj, const double* w, int nt, const double* t, int indiv_t, co
              int ncomp, double dt, double rtol, double atol, long long max_att, double* out,
              int* err, long long* nsteps)
 {
-  Force<D, PREC, VAR, POT> f{comps, ncomp};
-  std::vector<double> store(M::kSlotDoubles + 1);
+  Force<D, PREC, VAR, POT> f{comps, ncomp, {}};
+  for (int k = 0; k < ncomp; k++)
+    for (int j = 0; j < kScalarStride; j++) f.scal[k * kScalarStride + j] = comps[k].c[j];
+  std::vector<double> store((size_t)M::kSlotDoubles * kSlotStride + 1);
   for (long long i = 0; i < nobj; i++) {
     M m;
-    m.bind(store.data(), 1);
+    m.bind(store.data());
     Rows r{out, M::NV, nt, i};
     m.init(w + i * M::NV, t + (indiv_t ? i * nt : 0), nt, dt, rtol, atol, max_att, r);
     run_orbit(m, f, r);
@@ -113,7 +119,7 @@ extern "C" int harness_gamma_star(double alpha, double rc, int n, const double* 
   GpComp c;
   int rc_ = compile_group(1, 1, &pt, pa, &c, nullptr);
   if (rc_) return rc_;
-  for (int i = 0; i < n; i++) out[i] = gamma_star<double>(&c, u[i]);
+  for (int i = 0; i < n; i++) out[i] = gamma_star<double>(&c, u[i], c.c[6]);
   return 0;
 }
 

@@ -158,7 +158,7 @@ def test_device_api_soa_matches_galpy_layout(mw14):
     e = torch.empty(len(ics), dtype=torch.int32, device=dev)
     # same kernel specialisation as the galpy-facing call
     gb.integrate_device(torch.tensor(comps, device=dev), n, w0, tt, out, e, "dop853_cuda",
-                        signature=gb.signature((pt, pa)))
+                        signature=gb.signature((pt, pa)), comps_host=comps)
     torch.cuda.synchronize()
     got = rect_to_cyl(out.cpu().numpy().transpose(2, 1, 0))
     assert cyl_diff(res, got).max() < 1e-14 and not e.cpu().numpy().any()
