@@ -92,6 +92,27 @@ def ragged_workload(seed=4, ngroup=512):
     return pt, args, group, ics, np.linspace(0.0, 50.0, 51)
 
 
+def over_ranks(maxed, summed, pg, device):
+    """Device times are reduced with MAX and work counts with SUM over the
+    ranks of the process group (identity on one rank): the job's throughput is
+    the work of all ranks over the slowest rank's time."""
+    if pg is None:
+        return [float(v) for v in maxed], [float(v) for v in summed]
+    import torch
+
+    mx = torch.tensor([float(v) for v in maxed], dtype=torch.float64, device=device)
+    sm = torch.tensor([float(v) for v in summed], dtype=torch.float64, device=device)
+    pg.all_reduce(mx, op=pg.ReduceOp.MAX)
+    pg.all_reduce(sm, op=pg.ReduceOp.SUM)
+    return mx.tolist(), sm.tolist()
+
+
+def shard_seed(base, rank):
+    """Seed of a rank's shard: every rank integrates its own orbits (weak
+    scaling, no data exchange)."""
+    return base + 1000 * rank
+
+
 def stats(x):
     x = np.asarray(x)
     return {"median": float(np.median(x)), "p99": float(np.quantile(x, 0.99)),
@@ -232,10 +253,10 @@ def main():
 
     pt, pa = mw14_args()
     if args.case == "uniform":
-        ics, _ = precision_workload(args.orbits, seed=1 + 1000 * rank)
+        ics, _ = precision_workload(args.orbits, seed=shard_seed(1, rank))
         t = np.repeat(np.linspace(0.0, 50.0, NT)[None, :], len(ics), axis=0)
     else:
-        ics, t = workload(args.orbits, seed=1 + 1000 * rank)
+        ics, t = workload(args.orbits, seed=shard_seed(1, rank))
     n = len(ics)
     comps, ncomp = gb.compile_potential((pt, pa))
     sig = gb.signature((pt, pa))
@@ -270,13 +291,7 @@ def main():
         ms = e0.elapsed_time(e1)
         if pg:
             pg.barrier()
-        tot = torch.tensor([ms, float(steps), float(nbad)], dtype=torch.float64, device=dev)
-        if pg:
-            mx = tot.clone()
-            pg.all_reduce(mx, op=pg.ReduceOp.MAX)
-            sm = tot.clone()
-            pg.all_reduce(sm, op=pg.ReduceOp.SUM)
-            ms, steps, nbad = mx[0].item(), sm[1].item(), sm[2].item()
+        (ms,), (steps, nbad) = over_ranks([ms], [steps, nbad], pg, dev)
         return ms, steps, nbad
 
     clocks = ClockSampler(local)
@@ -469,11 +484,7 @@ def e2e(gb, ics, t, pt, pa, K, pg, dev, steps_total):
         _lib.check(rc)
         if k > 0:  # first call is a warm-up
             times.append(el)
-    el = max(times)
-    if pg:
-        x = torch.tensor([el], dtype=torch.float64, device=dev)
-        pg.all_reduce(x, op=pg.ReduceOp.MAX)
-        el = x.item()
+    (el,), _ = over_ranks([max(times)], [], pg, dev)
     return {"value": steps_total / el, "unit": "orbit-steps/s", "seconds_per_step": el,
             "h2d_bytes_per_step": int(yo_pin.nbytes + t_pin.nbytes),
             "d2h_bytes_per_step": int(res_pin.nbytes + err.nbytes),

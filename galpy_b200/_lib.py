@@ -97,6 +97,36 @@ class GalpyCudaLaunch(ctypes.Structure):
     ]
 
 
+class GalpyCudaAdjoint(ctypes.Structure):
+    _fields_ = [
+        ("size", ctypes.c_int),
+        ("planar", ctypes.c_int),
+        ("nobj", ctypes.c_longlong),
+        ("t0", ctypes.c_double),
+        ("tend", ctypes.c_double),
+        ("rtol", ctypes.c_double),
+        ("atol", ctypes.c_double),
+        ("max_attempts", ctypes.c_longlong),
+        ("comps", ctypes.c_void_p),
+        ("ncomp", ctypes.c_int),
+        ("group", ctypes.c_void_p),
+        ("signature", ctypes.c_int),
+        ("w0", ctypes.c_void_p),
+        ("yT", ctypes.c_void_p),
+        ("nsteps", ctypes.c_void_p),
+        ("err", ctypes.c_void_p),
+        ("ckpt", ctypes.c_void_p),
+        ("ckpt_cap", ctypes.c_int),
+        ("hrec", ctypes.c_void_p),
+        ("hcap", ctypes.c_longlong),
+        ("gyT", ctypes.c_void_p),
+        ("gw0", ctypes.c_void_p),
+        ("gparam", ctypes.c_void_p),
+        ("stream", ctypes.c_void_p),
+        ("block_size", ctypes.c_int),
+    ]
+
+
 CALLBACK = ctypes.CFUNCTYPE(None)
 
 _lib = None
@@ -140,6 +170,10 @@ SIGNATURES = {
     "galpy_cuda_energy_device": (
         _ci, [_vp, _ci, _vp, _ci, _vp, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong,
               _vp, _vp]),
+    "galpy_cuda_adjoint_forward": (_ci, [ctypes.POINTER(GalpyCudaAdjoint)]),
+    "galpy_cuda_adjoint_backward": (_ci, [ctypes.POINTER(GalpyCudaAdjoint)]),
+    "galpy_cuda_adjoint_replay": (_ci, [ctypes.POINTER(GalpyCudaAdjoint)]),
+    "galpy_cuda_adjoint_params": (_ci, [_ci, _ci, _ip, _ip]),
 }
 
 

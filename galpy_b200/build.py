@@ -1,6 +1,6 @@
 """In-tree build of libgalpy_cuda.so for sm_100a (B200).
 
-``build()`` compiles galpy_b200/csrc/galpy_cuda.cu with nvcc into
+``build()`` compiles galpy_b200/csrc/{galpy_cuda,adjoint}.cu with nvcc into
 galpy_b200/libgalpy_cuda.so; the library is loaded from there by
 galpy_b200._lib.  Nothing is installed outside the source tree.
 """
@@ -11,14 +11,14 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgalpy_cuda.so")
-SOURCES = ["galpy_cuda.cu"]
+SOURCES = ["galpy_cuda.cu", "adjoint.cu"]
 HEADERS = ["gpc_common.cuh", "potentials.cuh", "machines.cuh", "dop853_tableau.cuh",
-           "compile_potential.h"]
+           "compile_potential.h", "adjoint.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
 ]
 
 
@@ -39,13 +39,25 @@ def _stale():
 
 
 def build(force=False, verbose=False):
-    """Compile the engine if any source is newer than the library."""
+    """Compile the engine if any source is newer than the library (the
+    translation units in parallel, then one shared-library link)."""
     if not force and not _stale():
         return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", LIB + ".tmp"] + [os.path.join(CSRC, s) for s in SOURCES]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    procs, objs = [], []
+    for src in SOURCES:
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        cmd = [nvcc(), *NVCC_FLAGS, "-c", "-o", obj, os.path.join(CSRC, src)]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        procs.append((cmd, subprocess.Popen(cmd)))
+        objs.append(obj)
+    for cmd, p in procs:
+        if p.wait() != 0:
+            raise subprocess.CalledProcessError(p.returncode, cmd)
+    subprocess.run([nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
+                    "-o", LIB + ".tmp", *objs], check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

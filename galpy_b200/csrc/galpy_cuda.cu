@@ -49,6 +49,12 @@ static int set_error(int code, const std::string& msg)
   return code;
 }
 
+// for the library's other translation units (not exported)
+__attribute__((visibility("hidden"))) int gpc_report_error(int code, const char* msg)
+{
+  return set_error(code, msg);
+}
+
 #define GPC_CUDA_TRY(expr)                                                              \
   do {                                                                                  \
     cudaError_t e_ = (expr);                                                            \

@@ -41,8 +41,6 @@ constexpr int kSlotStride = 128;
 constexpr double kMaxDtReduce = 10000.;
 
 enum : int { M_LEAPFROG = 0, M_RK4 = 1, M_SYMPLEC4 = 3, M_DOP853 = 6 };
-// per-orbit status (the reference uses 0 and -10 for SIGINT)
-enum : int { E_OK = 0, E_BUDGET = 2, E_NONFINITE = 3, E_ABORT = -10 };
 enum : int { PREC_FP64 = 0, PREC_F32 = 1 };
 
 // symplec4 coefficients (Kinoshita et al.; bovy_symplecticode.c:96-99)

@@ -181,6 +181,74 @@ int galpy_cuda_energy_device(const void *comps, int ncomp, const int *group, int
                              const double *w, long long n, long long comp_stride,
                              long long orbit_stride, double *E, void *stream);
 
+/* ---------------------------------------------------------------------------
+ * Gradients of a loss on final states (reverse mode).  No counterpart in the
+ * reference: galpy's gradient information is the variational integration
+ * (integrate_dxdv, integratePlanarOrbit.c:940), one tangent vector per input
+ * direction; these entry points give dL/d(initial state) and
+ * dL/d(potential parameters) of a scalar loss L(y(T)) with one backward
+ * sweep per orbit.
+ *
+ * The forward pass is galpy's DOP853 (the same step sequence as
+ * odeint_type 6, y(T) from its dense output) from t0 to tend.  It saves the
+ * integrator state every 64 accepted steps (checkpoints).  The backward pass
+ * recomputes each 64-step segment from its checkpoint and applies the exact
+ * adjoint of the Runge-Kutta stages with the accepted step sizes held fixed
+ * (the discrete adjoint of the forward map).  All arrays are device memory
+ * owned by the caller; the calls are asynchronous on `stream` and allocate
+ * nothing.  nv = 4 (planar: x, y, vx, vy) or 6 (x, y, z, vx, vy, vz).
+ *
+ * Differentiable parameters, per component in pot_type order (the pot_args
+ * index of each: galpy_cuda_adjoint_params):
+ *   15 PowerSphericalwCutoff: amp, rc;  5 MiyamotoNagai: amp, a, b;
+ *   9 NFW: amp, a;  8 Hernquist: amp, a;  0 LogarithmicHalo: amp, q, core^2.
+ * ------------------------------------------------------------------------- */
+typedef struct galpy_cuda_adjoint {
+  int size;                 /* sizeof(galpy_cuda_adjoint) */
+  int planar;
+  long long nobj;
+  double t0, tend;          /* integration interval, shared by all orbits */
+  double rtol, atol;        /* natural logarithms, as galpy passes them */
+  long long max_attempts;   /* per-orbit attempt budget, 0 = unlimited */
+  const void *comps;        /* galpy_cuda_compile_potential records (device) */
+  int ncomp;
+  const int *group;         /* [nobj] group of each orbit, or NULL */
+  int signature;            /* galpy_cuda_signature(pot_type) */
+  const double *w0;         /* [nv][nobj] initial rectangular states */
+  double *yT;               /* [nv][nobj] out (forward, replay): states at tend */
+  long long *nsteps;        /* [nobj] accepted steps: out of forward, in of replay/backward */
+  int *err;                 /* [nobj] status: out of forward (0 ok, 2 budget or
+                               checkpoint capacity exhausted, 3 non-finite), in of backward */
+  double *ckpt;             /* [ckpt_cap][nv+3][nobj] checkpoints: out of forward, in of backward */
+  int ckpt_cap;             /* checkpoints per orbit: at most 64*ckpt_cap steps */
+  double *hrec;             /* [hcap][nobj] accepted step sizes: optional out of forward,
+                               in of replay; NULL to skip */
+  long long hcap;
+  const double *gyT;        /* [nv][nobj] dL/dy(tend) (backward) */
+  double *gw0;              /* [nv][nobj] out (backward): dL/dw0 */
+  double *gparam;           /* [nparam][nobj] out (backward): per-orbit dL/dparam, or NULL */
+  void *stream;             /* cudaStream_t */
+  int block_size;           /* 0 = default */
+} galpy_cuda_adjoint;
+
+/* Forward pass: yT, nsteps, err, checkpoints (and hrec if set). */
+int galpy_cuda_adjoint_forward(const galpy_cuda_adjoint *a);
+
+/* Backward pass: gw0 and gparam for gyT, from the forward pass's nsteps, err
+ * and checkpoints (same w0 interval, tolerances and potential).  Orbits with
+ * err != 0 get NaN gradients. */
+int galpy_cuda_adjoint_backward(const galpy_cuda_adjoint *a);
+
+/* The forward map with frozen steps: yT from w0 with the nsteps[i] step
+ * sizes in hrec (the function the backward pass differentiates exactly;
+ * finite differences of it check the gradients). */
+int galpy_cuda_adjoint_replay(const galpy_cuda_adjoint *a);
+
+/* Number of differentiable parameters of a component list (>= 0), or
+ * GALPY_CUDA_ERR_POTENTIAL; arg_index (may be NULL) receives the pot_args
+ * index of each parameter. */
+int galpy_cuda_adjoint_params(int planar, int npot, const int *pot_type, int *arg_index);
+
 /* Diagnostic: measured float64 fused-multiply-add throughput of the current
  * device in TFLOP/s (2 flops per FMA), the roofline denominator of the
  * integration kernels. */

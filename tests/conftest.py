@@ -105,3 +105,67 @@ class Harness:
                                      tid.ctypes.data_as(_dp), a32.ctypes.data_as(_dp))
         assert rc == 0, rc
         return acc, tid, a32
+
+    # ----------------------------------------------------------- adjoint ---
+    def _pot(self, pot_type, pot_args):
+        pt = np.ascontiguousarray(pot_type, np.int32)
+        pa = np.ascontiguousarray(pot_args, np.float64)
+        return pt, pa, len(pt), pt.ctypes.data_as(_ip), pa.ctypes.data_as(_dp)
+
+    def adj_nparam(self, pot_type, pot_args, planar=False):
+        pt, pa, n, ptp, pap = self._pot(pot_type, pot_args)
+        return self.lib.harness_adj_nparam(int(planar), n, ptp, pap)
+
+    def adj_param_vjp(self, x, y, z, lam, pot_type, pot_args, planar=False):
+        """g[i, p] = lam_i . d a(x_i) / d theta_p"""
+        x, y, z = (np.ascontiguousarray(v, np.float64) for v in (x, y, z))
+        lam = np.ascontiguousarray(lam, np.float64)
+        pt, pa, n, ptp, pap = self._pot(pot_type, pot_args)
+        g = np.zeros((len(x), self.adj_nparam(pt, pa, planar)))
+        self.lib.harness_adj_param_vjp(int(planar), len(x), x.ctypes.data_as(_dp),
+                                       y.ctypes.data_as(_dp), z.ctypes.data_as(_dp),
+                                       lam.ctypes.data_as(_dp), n, ptp, pap, g.ctypes.data_as(_dp))
+        return g
+
+    def adj_forward(self, w0, t0, tend, pot_type, pot_args, planar=False, rtol=1e-10, atol=1e-10,
+                    hcap=100000):
+        w0 = np.ascontiguousarray(w0, np.float64)
+        nobj, nv = w0.shape
+        pt, pa, n, ptp, pap = self._pot(pot_type, pot_args)
+        yT, ns, err = np.zeros((nobj, nv)), np.zeros(nobj, np.int64), np.zeros(nobj, np.int32)
+        h = np.zeros((nobj, hcap))
+        rc = self.lib.harness_adj_forward(
+            int(planar), nobj, w0.ctypes.data_as(_dp), ctypes.c_double(t0), ctypes.c_double(tend),
+            ctypes.c_double(np.log(rtol)), ctypes.c_double(np.log(atol)), n, ptp, pap,
+            yT.ctypes.data_as(_dp), ns.ctypes.data_as(_lp), err.ctypes.data_as(_ip),
+            h.ctypes.data_as(_dp), ctypes.c_longlong(hcap))
+        assert rc == 0, rc
+        return yT, ns, err, h[:, :max(int(ns.max()), 1)].copy()
+
+    def adj_replay(self, w0, t0, tend, pot_type, pot_args, h, ns, planar=False):
+        w0 = np.ascontiguousarray(w0, np.float64)
+        h = np.ascontiguousarray(h, np.float64)
+        ns = np.ascontiguousarray(ns, np.int64)
+        pt, pa, n, ptp, pap = self._pot(pot_type, pot_args)
+        yT = np.zeros_like(w0)
+        self.lib.harness_adj_replay(int(planar), len(w0), w0.ctypes.data_as(_dp),
+                                    ctypes.c_double(t0), ctypes.c_double(tend), n, ptp, pap,
+                                    h.ctypes.data_as(_dp), ctypes.c_longlong(h.shape[1]),
+                                    ns.ctypes.data_as(_lp), yT.ctypes.data_as(_dp))
+        return yT
+
+    def adj_gradient(self, w0, t0, tend, pot_type, pot_args, gyT, planar=False, rtol=1e-10,
+                     atol=1e-10):
+        """(dL/dw0, per-orbit dL/dtheta, err) for dL/dy(tend) = gyT."""
+        w0 = np.ascontiguousarray(w0, np.float64)
+        gyT = np.ascontiguousarray(gyT, np.float64)
+        pt, pa, n, ptp, pap = self._pot(pot_type, pot_args)
+        gw = np.zeros_like(w0)
+        gth = np.zeros((len(w0), self.adj_nparam(pt, pa, planar)))
+        err = np.zeros(len(w0), np.int32)
+        self.lib.harness_adj_gradient(
+            int(planar), len(w0), w0.ctypes.data_as(_dp), ctypes.c_double(t0),
+            ctypes.c_double(tend), ctypes.c_double(np.log(rtol)), ctypes.c_double(np.log(atol)),
+            n, ptp, pap, gyT.ctypes.data_as(_dp), gw.ctypes.data_as(_dp), gth.ctypes.data_as(_dp),
+            err.ctypes.data_as(_ip))
+        return gw, gth, err

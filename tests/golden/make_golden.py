@@ -141,6 +141,26 @@ def main():
         out[f"c_{m}_dxdv3"] = res
         res, _, _ = O.integrate_dxdv(w2, t, pt2, pa2, m, planar=True, impl="ref")
         out[f"c_{m}_dxdv2"] = res
+    # gradient oracle of the adjoint: Jacobians d y(T) / d y(0) from the
+    # reference's variational DOP853 (integrate{Planar,Full}Orbit_dxdv), one
+    # unit deviation column per run, t in [0, 20], rtol = atol = 1e-10
+    for planar, n, seed in ((True, 6, 3), (False, 4, 4)):
+        ics = cyl_to_rect(seeded_ics(n, seed, planar=planar))
+        nv = ics.shape[1]
+        ptp, pap = (pt2, pa2) if planar else (pt, pa)
+        jac = np.zeros((n, nv, nv))
+        yT = np.zeros((n, nv))
+        for c in range(nv):
+            w = np.zeros((n, 2 * nv))
+            w[:, :nv] = ics
+            w[:, nv + c] = 1.0
+            res, err, _ = O.integrate_dxdv(w, np.array([0.0, 20.0]), ptp, pap, "dop853",
+                                           planar=planar, rtol=1e-10, atol=1e-10, impl="ref")
+            assert not err.any()
+            jac[:, :, c] = res[:, -1, nv:]
+            yT = res[:, -1, :nv]
+        key = "adj_planar" if planar else "adj_3d"
+        out[f"{key}_w0"], out[f"{key}_jac"], out[f"{key}_yT"] = ics, jac, yT
     np.savez_compressed(os.path.join(HERE, "golden.npz"), **out)
     print("wrote", os.path.join(HERE, "golden.npz"), len(out), "arrays")
 

@@ -173,3 +173,128 @@ extern "C" int harness_forces(int planar, int n, const double* x, const double* 
   }
   return 0;
 }
+
+// ------------------------------------------------------------- adjoint ---
+#include "../../galpy_b200/csrc/adjoint.cuh"
+
+namespace {
+struct AdjPot {
+  std::vector<GpComp> comps;
+  int rc = 0;
+  AdjPot(int planar, int npot, const int* pot_type, const double* pot_args) : comps(npot)
+  {
+    rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
+  }
+  adj::Field<DynPot> field() const { return {comps.data(), (int)comps.size(), nullptr}; }
+};
+}  // namespace
+
+extern "C" int harness_adj_nparam(int planar, int npot, const int* pot_type,
+                                  const double* pot_args)
+{
+  AdjPot P(planar, npot, pot_type, pot_args);
+  if (P.rc) return P.rc;
+  return adj::group_nparam(P.comps.data(), npot);
+}
+
+// g[i][p] = lambda_i . d a(x_i) / d theta_p
+extern "C" int harness_adj_param_vjp(int planar, int n, const double* x, const double* y,
+                                     const double* z, const double* lam /*[n][3]*/, int npot,
+                                     const int* pot_type, const double* pot_args, double* g)
+{
+  AdjPot P(planar, npot, pot_type, pot_args);
+  if (P.rc) return P.rc;
+  const int np = adj::group_nparam(P.comps.data(), npot);
+  for (int i = 0; i < n; i++) {
+    double* gi = g + (size_t)i * np;
+    for (int p = 0; p < np; p++) gi[p] = 0.0;
+    if (planar)
+      adj::accel_param_vjp<true>(P.comps.data(), npot, x[i], y[i], 0.0, lam[3 * i],
+                                 lam[3 * i + 1], 0.0, gi);
+    else
+      adj::accel_param_vjp<false>(P.comps.data(), npot, x[i], y[i], z[i], lam[3 * i],
+                                  lam[3 * i + 1], lam[3 * i + 2], gi);
+  }
+  return np;
+}
+
+// Forward pass per orbit (w0, yT: [nobj][nv]); hrec [nobj][hcap] (may be
+// NULL); nsteps, err [nobj].
+extern "C" int harness_adj_forward(int planar, int nobj, const double* w0, double t0, double T,
+                                   double rtol, double atol, int npot, const int* pot_type,
+                                   const double* pot_args, double* yT, long long* nsteps,
+                                   int* err, double* hrec, long long hcap)
+{
+  AdjPot P(planar, npot, pot_type, pot_args);
+  if (P.rc) return P.rc;
+  const int nv = planar ? 4 : 6;
+  const int ccap = 4096;
+  std::vector<double> ck((size_t)ccap * (nv + 3));
+  for (int i = 0; i < nobj; i++) {
+    double* h = hrec ? hrec + (size_t)i * hcap : nullptr;
+    if (planar)
+      err[i] = adj::forward_orbit<2, DynPot>(P.field(), w0 + (size_t)i * nv, t0, T, rtol, atol, 0,
+                                             ck.data(), 1, ccap, h, 1, hcap,
+                                             yT + (size_t)i * nv, nsteps + i);
+    else
+      err[i] = adj::forward_orbit<3, DynPot>(P.field(), w0 + (size_t)i * nv, t0, T, rtol, atol, 0,
+                                             ck.data(), 1, ccap, h, 1, hcap,
+                                             yT + (size_t)i * nv, nsteps + i);
+  }
+  return 0;
+}
+
+// The forward map with frozen steps hrec [nobj][hcap], nsteps [nobj].
+extern "C" int harness_adj_replay(int planar, int nobj, const double* w0, double t0, double T,
+                                  int npot, const int* pot_type, const double* pot_args,
+                                  const double* hrec, long long hcap, const long long* nsteps,
+                                  double* yT)
+{
+  AdjPot P(planar, npot, pot_type, pot_args);
+  if (P.rc) return P.rc;
+  const int nv = planar ? 4 : 6;
+  for (int i = 0; i < nobj; i++) {
+    if (planar)
+      adj::replay_orbit<2, DynPot>(P.field(), w0 + (size_t)i * nv, t0, T, hrec + (size_t)i * hcap,
+                                   1, nsteps[i], yT + (size_t)i * nv);
+    else
+      adj::replay_orbit<3, DynPot>(P.field(), w0 + (size_t)i * nv, t0, T, hrec + (size_t)i * hcap,
+                                   1, nsteps[i], yT + (size_t)i * nv);
+  }
+  return 0;
+}
+
+// Forward + backward: gw0 [nobj][nv] = dL/dw0, gth [nobj][np] = dL/dtheta
+// for dL/dyT = gyT [nobj][nv].  Returns np.
+extern "C" int harness_adj_gradient(int planar, int nobj, const double* w0, double t0, double T,
+                                    double rtol, double atol, int npot, const int* pot_type,
+                                    const double* pot_args, const double* gyT, double* gw0,
+                                    double* gth, int* err)
+{
+  AdjPot P(planar, npot, pot_type, pot_args);
+  if (P.rc) return P.rc;
+  const int nv = planar ? 4 : 6;
+  const int np = adj::group_nparam(P.comps.data(), npot);
+  const int ccap = 4096;
+  std::vector<double> ck((size_t)ccap * (nv + 3));
+  double yT[6];
+  long long ns;
+  for (int i = 0; i < nobj; i++) {
+    double* lam = gw0 + (size_t)i * nv;
+    double* g = gth + (size_t)i * np;
+    for (int c = 0; c < nv; c++) lam[c] = gyT[(size_t)i * nv + c];
+    for (int p = 0; p < np; p++) g[p] = 0.0;
+    if (planar) {
+      err[i] = adj::forward_orbit<2, DynPot>(P.field(), w0 + (size_t)i * nv, t0, T, rtol, atol, 0,
+                                             ck.data(), 1, ccap, nullptr, 1, 0, yT, &ns);
+      if (err[i] == 0)
+        adj::backward_orbit<2, DynPot>(P.field(), t0, T, rtol, atol, ck.data(), 1, ns, lam, g);
+    } else {
+      err[i] = adj::forward_orbit<3, DynPot>(P.field(), w0 + (size_t)i * nv, t0, T, rtol, atol, 0,
+                                             ck.data(), 1, ccap, nullptr, 1, 0, yT, &ns);
+      if (err[i] == 0)
+        adj::backward_orbit<3, DynPot>(P.field(), t0, T, rtol, atol, ck.data(), 1, ns, lam, g);
+    }
+  }
+  return np;
+}

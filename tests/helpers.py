@@ -62,3 +62,42 @@ def unit_deviations(w_base, dim):
             w[i * nv + j, :nv] = w_base[i]
             w[i * nv + j, nv + j] = 1.0
     return w
+
+
+# differentiable parameters per component type and their galpy argument index
+ADJ_PARAM_ARGS = {15: (0, 2), 5: (0, 1, 2), 9: (0, 1), 8: (0, 1), 0: (0, 1, 2)}
+
+
+def galpy_nargs(t, planar):
+    return {15: 3 if planar else 5, 5: 3, 9: 2, 8: 2, 0: 4}[int(t)]
+
+
+def adj_param_index(pot_type, planar):
+    """pot_args index of every differentiable parameter, in the adjoint's order."""
+    idx, off = [], 0
+    for t in pot_type:
+        idx += [off + a for a in ADJ_PARAM_ARGS[int(t)]]
+        off += galpy_nargs(t, planar)
+    return np.array(idx, dtype=np.int64)
+
+
+def central_fd(f, x, idx, rel=1e-6, floor=1e-3):
+    """Central differences of f (array-valued) with respect to x[idx], with
+    steps rel * max(|x|, floor); returns [len(idx), *f.shape]."""
+    out = []
+    for j in idx:
+        h = rel * max(abs(x[j]), floor)
+        xp, xm = x.copy(), x.copy()
+        xp[j] += h
+        xm[j] -= h
+        out.append((f(xp) - f(xm)) / (2 * h))
+    return np.array(out)
+
+
+def differentiation_workload(n, seed=3):
+    """Planar MWPotential2014 gradient workload: config-0 style initial
+    conditions in the plane (z = vz = 0) as rectangular (x, y, vx, vy), and
+    seeded targets of the same shape for L = sum |y(20) - target|^2."""
+    w0 = cyl_to_rect(seeded_ics(n, seed, planar=True))
+    tgt = cyl_to_rect(seeded_ics(n, seed + 100, planar=True))
+    return np.ascontiguousarray(w0), np.ascontiguousarray(tgt)
