@@ -113,6 +113,25 @@ def shard_seed(base, rank):
     return base + 1000 * rank
 
 
+def differentiation_workload(n=65536, seed=3):
+    """The differentiation configuration: n planar orbits in MWPotential2014
+    (config-0 style initial conditions with z = vz = 0) as rectangular (x, y,
+    vx, vy), DOP853 rtol = atol = 1e-10 over t in [0, 20], and seeded targets
+    for L = sum |y(20) - target|^2."""
+    def planar_rect(seed_):
+        rng = np.random.default_rng(seed_)
+        R = rng.uniform(0.5, 2.0, n)
+        vR = rng.normal(0, 0.1, n)
+        vT = 1 + rng.normal(0, 0.1, n)
+        rng.normal(0, 0.05, n)  # z and vz of the 3D generator: zero in the plane
+        rng.normal(0, 0.05, n)
+        phi = rng.uniform(0, 2 * np.pi, n)
+        c, s = np.cos(phi), np.sin(phi)
+        return np.stack([R * c, R * s, vR * c - vT * s, vR * s + vT * c], 1)
+
+    return planar_rect(seed), planar_rect(seed + 100)
+
+
 def stats(x):
     x = np.asarray(x)
     return {"median": float(np.median(x)), "p99": float(np.quantile(x, 0.99)),
@@ -220,6 +239,10 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--mixed-orbits", type=int, default=1 << 22)
     ap.add_argument("--no-ragged", action="store_true")
+    ap.add_argument("--no-grad", action="store_true")
+    ap.add_argument("--grad-only", action="store_true",
+                    help="run only the differentiation leg (with --grad-orbits orbits)")
+    ap.add_argument("--grad-orbits", type=int, default=65536)
     ap.add_argument("--case", default="batching", choices=["batching", "uniform"],
                     help="uniform: R ~ U(0.5, 2), shared t in [0, 50] (101 snapshots) "
                          "(a throughput-bound case for profiling the same kernel)")
@@ -250,6 +273,17 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=dev)
         pg = dist
+
+    if args.grad_only:
+        peak = ctypes_fp64_peak(_lib)
+        res = differentiation_leg(gb, torch, dev, torch.cuda.current_stream(dev), pg, peak,
+                                  n=args.grad_orbits)
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(res), flush=True)
+        return
 
     pt, pa = mw14_args()
     if args.case == "uniform":
@@ -349,6 +383,11 @@ def main():
         result["ragged"] = ragged_leg(gb, torch, dev, stream, pg)
         result["gpu_launches"] += 2
 
+    if not args.no_grad:
+        result["differentiation"] = differentiation_leg(gb, torch, dev, stream, pg, peak,
+                                                        n=args.grad_orbits)
+        result["gpu_launches"] += 4
+
     if not args.no_e2e:
         result["e2e"] = e2e(gb, ics, t, pt, pa, args.steps, pg, dev, steps)
         result["gpu_launches"] += args.steps
@@ -363,6 +402,85 @@ def main():
         pg.destroy_process_group()
     if rank == 0:
         print(json.dumps(result), flush=True)
+
+
+F_STEP_DOP853_PLANAR = 6200.0  # 15 planar force evaluations (280) + 2000 stage flops
+F_GRAD_STEP = 3 * F_STEP_DOP853_PLANAR  # forward + backward (2 x forward: Hessian-vector products)
+
+
+def differentiation_leg(gb, torch, dev, stream, pg, peak, n=65536):
+    """Gradient of L = sum |y(20) - target|^2 over 65,536 planar orbits
+    with respect to the initial conditions and the MiyamotoNagai (amp, a,
+    b), NFW (amp, a) and bulge (amp, rc) parameters: adjoint forward +
+    backward on the GPU, timed with CUDA events; the parameter gradient is
+    checked against central differences (h = 1e-6 relative) of the loss with
+    the forward pass's step sizes frozen."""
+    from galpy_b200 import adjoint as adj
+
+    _, pt, pa = gb.parse_pot(gb.MWPotential2014(), planar=True)
+    w0, tgt = differentiation_workload(n, seed=shard_seed(3, pg.get_rank() if pg else 0))
+    comps, ncomp = gb.compile_potential((pt, pa), planar=True)
+    sig = gb.signature((pt, pa), planar=True)
+    comps_d = torch.tensor(comps, device=dev)
+    w = torch.tensor(w0.T.copy(), device=dev)
+    tg = torch.tensor(tgt.T.copy(), device=dev)
+    idx = adj.adjoint_params(pt, planar=True)
+    times = []
+    for rep in range(3):  # two warm-ups, one timed
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record(stream)
+        f = adj.adjoint_forward(comps_d, ncomp, w, 20.0, rtol=1e-10, atol=1e-10, planar=True,
+                                signature=sig, ckpt_cap=16, stream=stream)
+        ev[1].record(stream)
+        gw, gp = adj.adjoint_backward(comps_d, ncomp, f, 2 * (f["yT"] - tg), 20.0, rtol=1e-10,
+                                      atol=1e-10, planar=True, signature=sig, nparam=len(idx),
+                                      stream=stream)
+        gsum = gp.sum(dim=1)
+        ev[2].record(stream)
+        torch.cuda.synchronize()
+        times.append((ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])))
+    fwd_ms, bwd_ms = times[-1]
+    steps = float(f["nsteps"].sum().item())
+    nbad = int((f["err"] != 0).sum().item())
+    # frozen-step central differences of the total loss
+    fr = adj.adjoint_forward(comps_d, ncomp, w, 20.0, rtol=1e-10, atol=1e-10, planar=True,
+                             signature=sig, ckpt_cap=16, record_steps=int(f["nsteps"].max()),
+                             stream=stream)
+
+    def loss(p):
+        c = torch.tensor(gb.compile_potential((pt, p), planar=True)[0], device=dev)
+        y = adj.adjoint_replay(c, ncomp, w, fr["hrec"], fr["nsteps"], 20.0, planar=True,
+                               signature=sig, stream=stream)
+        return float(((y - tg) ** 2).sum().item())
+
+    fd = []
+    for j in idx:
+        h = 1e-6 * abs(pa[j])
+        pp, pm = pa.copy(), pa.copy()
+        pp[j] += h
+        pm[j] -= h
+        fd.append((loss(pp) - loss(pm)) / (2 * h))
+    fd = np.array(fd)
+    g = gsum.cpu().numpy()
+    (ms_tot,), (steps_all, nbad_all) = over_ranks([fwd_ms + bwd_ms], [steps, nbad], pg, dev)
+    value = steps_all / (ms_tot * 1e-3)
+    achieved = value / (pg.get_world_size() if pg else 1) * F_GRAD_STEP / 1e12
+    names = ["bulge amp", "bulge rc", "disk amp", "disk a", "disk b", "halo amp", "halo a"]
+    return {"workload": f"differentiation: {n} planar orbits in MWPotential2014, dop853 "
+                        "rtol=atol=1e-10, t in [0,20], L = sum |y(20) - target|^2, gradient "
+                        "w.r.t. initial conditions and 7 potential parameters",
+            "value": value, "unit": "orbit-steps/s (forward + backward)",
+            "forward_ms": fwd_ms, "backward_ms": bwd_ms, "accepted_steps": steps,
+            "max_steps_per_orbit": int(f["nsteps"].max().item()), "orbits_with_err": nbad_all,
+            "param_grad": dict(zip(names, g.tolist())),
+            "param_grad_rel_err_vs_fd": float(np.max(np.abs(g - fd) / np.abs(fd))),
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
+                         "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                         "flops_per_unit": F_GRAD_STEP,
+                         "unit_of_work": "accepted forward step (forward + backward flops)"}}
 
 
 def ragged_leg(gb, torch, dev, stream, pg):

@@ -124,6 +124,8 @@ class GalpyCudaAdjoint(ctypes.Structure):
         ("gparam", ctypes.c_void_p),
         ("stream", ctypes.c_void_p),
         ("block_size", ctypes.c_int),
+        ("order", ctypes.c_void_p),
+        ("variant", ctypes.c_int),
     ]
 
 

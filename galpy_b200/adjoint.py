@@ -9,11 +9,11 @@ differentiated with one backward sweep per orbit:
 
 * forward: galpy's DOP853 from t0 to tend on the GPU (the step sequence of
   method 'dop853_c'/'dop853_cuda', y(tend) from its dense output), saving
-  the integrator state every 64 accepted steps;
-* backward: each 64-step segment is recomputed from its checkpoint and the
-  exact adjoint of the Runge-Kutta stages is applied with the accepted step
-  sizes held fixed (tidal tensors for the state, analytic derivatives of the
-  forces for the parameters).
+  the state every 64 accepted steps with those steps' sizes (checkpoints);
+* backward: each 64-step segment is recomputed from its checkpoint with the
+  recorded step sizes and the exact adjoint of the Runge-Kutta stages is
+  applied with the step sizes held fixed (tidal tensors for the state,
+  analytic derivatives of the forces for the parameters).
 
 ``final_state`` wraps both passes in a ``torch.autograd.Function``::
 
@@ -93,8 +93,9 @@ def adjoint_forward(comps, ncomp, w0, tend, t0=0.0, rtol=None, atol=None, planar
     float64 CUDA tensor [nv, N] (SoA, rectangular).  Returns a dict with
     yT [nv, N], nsteps int64 [N], err int32 [N], ckpt, ckpt_cap and, with
     record_steps > 0, hrec [record_steps, N] (the accepted step sizes, for
-    ``adjoint_replay``).  Orbits that need more than 64*ckpt_cap steps are
-    re-run with 4x the capacity (up to twice)."""
+    ``adjoint_replay``).  Checkpoints take (nv + 65) doubles per orbit and 64
+    steps; by default the capacity starts at 512 steps and orbits that need
+    more are re-run with 4x the capacity (up to twice)."""
     import torch
 
     _require("w0", w0, torch.float64)
@@ -104,14 +105,14 @@ def adjoint_forward(comps, ncomp, w0, tend, t0=0.0, rtol=None, atol=None, planar
     rtol, atol = parse_tol(rtol, atol)
     s = stream if stream is not None else torch.cuda.current_stream(w0.device)
     dev = w0.device
-    cap = int(ckpt_cap) if ckpt_cap else 32
+    cap = int(ckpt_cap) if ckpt_cap else 8
     for attempt in range(3):
         a = _struct(planar, nobj, t0, tend, rtol, atol, comps, ncomp, group, signature, w0, s,
                     max_attempts, block_size)
         yT = torch.empty((nv, nobj), dtype=torch.float64, device=dev)
         nsteps = torch.empty(nobj, dtype=torch.int64, device=dev)
         err = torch.empty(nobj, dtype=torch.int32, device=dev)
-        ckpt = torch.empty((cap, nv + 3, nobj), dtype=torch.float64, device=dev)
+        ckpt = torch.empty((cap, nv + 1 + CKPT_EVERY, nobj), dtype=torch.float64, device=dev)
         hrec = (torch.empty((record_steps, nobj), dtype=torch.float64, device=dev)
                 if record_steps else None)
         a.yT, a.nsteps, a.err, a.ckpt = (yT.data_ptr(), nsteps.data_ptr(), err.data_ptr(),
@@ -131,10 +132,13 @@ def adjoint_forward(comps, ncomp, w0, tend, t0=0.0, rtol=None, atol=None, planar
 
 
 def adjoint_backward(comps, ncomp, fwd, gyT, tend, t0=0.0, rtol=None, atol=None, planar=False,
-                     signature=0, group=None, nparam=None, stream=None, block_size=0, w0=None):
+                     signature=0, group=None, nparam=None, stream=None, block_size=0, w0=None,
+                     sort=True, variant=0):
     """Backward pass: (gw0 [nv, N], gparam [nparam, N]) for dL/dyT = gyT
     [nv, N], from the dict returned by adjoint_forward (same potential,
-    interval and tolerances)."""
+    interval and tolerances).  sort: hand the orbits to the GPU threads by
+    decreasing step count (the forward pass's exact cost), so that the lanes
+    of a warp do similar work and the longest orbits start first."""
     import torch
 
     gyT = gyT.contiguous()
@@ -154,6 +158,11 @@ def adjoint_backward(comps, ncomp, fwd, gyT, tend, t0=0.0, rtol=None, atol=None,
     a.gyT = gyT.data_ptr()
     a.gw0 = gw0.data_ptr()
     a.gparam = gparam.data_ptr() if nparam else None
+    a.variant = int(variant)
+    order = None
+    if sort:
+        order = torch.argsort(fwd["nsteps"], descending=True).to(torch.int32)
+        a.order = order.data_ptr()
     _lib.check(_lib.lib().galpy_cuda_adjoint_backward(ctypes.byref(a)))
     return gw0, (gparam[:nparam] if nparam else None)
 

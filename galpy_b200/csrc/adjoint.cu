@@ -7,7 +7,8 @@
 // so that the 32 lanes of a warp touch consecutive addresses; the per-orbit
 // segment buffers of the backward pass (64 step start states) are
 // thread-local arrays, which the hardware interleaves across the lanes of a
-// warp the same way.  Compile-time component lists (MWPotential2014's
+// warp the same way.  A checkpoint record holds a segment's start state and
+// its 64 accepted step sizes ([ckpt_cap][nv + 1 + 64][nobj]).  Compile-time component lists (MWPotential2014's
 // PowerSphericalwCutoff + MiyamotoNagai + NFW) are inlined like in the
 // integration kernels; the tidal tensors and parameter derivatives of the
 // backward pass walk the component list at run time.
@@ -43,7 +44,14 @@ struct AdjK {
   const double* gyT;
   double* gw0;
   double* gparam;
+  const int* order;
 };
+
+// Orbit handled by thread j of the launch.
+__device__ __forceinline__ long long orbit_of(const AdjK& A, long long j)
+{
+  return A.order ? (long long)A.order[j] : j;
+}
 
 template <class POT>
 __device__ __forceinline__ adj::Field<POT> field_of(const AdjK& A, long long i)
@@ -56,8 +64,10 @@ template <int D, class POT>
 __global__ void __launch_bounds__(128) adj_forward_kernel(const AdjK A)
 {
   constexpr int N = 2 * D;
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= A.nobj) return;
+  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (j >= A.nobj) return;
+  const long long i = orbit_of(A, j);
+  if (i < 0 || i >= A.nobj) return;
   const adj::Field<POT> F = field_of<POT>(A, i);
   double w[N], y[N];
 #pragma unroll
@@ -76,8 +86,10 @@ template <int D, class POT>
 __global__ void __launch_bounds__(128) adj_replay_kernel(const AdjK A)
 {
   constexpr int N = 2 * D;
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= A.nobj) return;
+  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (j >= A.nobj) return;
+  const long long i = orbit_of(A, j);
+  if (i < 0 || i >= A.nobj) return;
   const adj::Field<POT> F = field_of<POT>(A, i);
   double w[N], y[N];
 #pragma unroll
@@ -93,25 +105,29 @@ __global__ void __launch_bounds__(128) adj_replay_kernel(const AdjK A)
   for (int c = 0; c < N; c++) A.yT[c * A.nobj + i] = y[c];
 }
 
-template <int D, class POT>
-__global__ void __launch_bounds__(128) adj_backward_kernel(const AdjK A)
+// MINB: minimum resident blocks per SM asked of the register allocator
+// (1: no cap; 4: at most 128 registers a thread at 128 threads a block).
+template <int D, class POT, int MINB>
+__global__ void __launch_bounds__(128, MINB) adj_backward_kernel(const AdjK A)
 {
   constexpr int N = 2 * D;
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= A.nobj) return;
+  const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (j >= A.nobj) return;
+  const long long i = orbit_of(A, j);
+  if (i < 0 || i >= A.nobj) return;
   const adj::Field<POT> F = field_of<POT>(A, i);
   const int np = adj::group_nparam(F.comp, F.ncomp);
   double lam[N], g[adj::kMaxParam];
   for (int p = 0; p < np; p++) g[p] = 0.0;
-  if (A.err[i] != E_OK) {
+  const long long nseg = (A.nsteps[i] + adj::kCkptEvery - 1) / adj::kCkptEvery;
+  if (A.err[i] != E_OK || A.nsteps[i] < 0 || nseg > A.ccap) {
 #pragma unroll
     for (int c = 0; c < N; c++) lam[c] = NAN;
     for (int p = 0; p < np; p++) g[p] = NAN;
   } else {
 #pragma unroll
     for (int c = 0; c < N; c++) lam[c] = A.gyT[c * A.nobj + i];
-    adj::backward_orbit<D, POT>(F, A.t0, A.T, A.rtol, A.atol, A.ckpt + i, A.nobj, A.nsteps[i],
-                                lam, g);
+    adj::backward_orbit<D, POT>(F, A.T, A.ckpt + i, A.nobj, A.nsteps[i], lam, g);
   }
 #pragma unroll
   for (int c = 0; c < N; c++) A.gw0[c * A.nobj + i] = lam[c];
@@ -122,12 +138,18 @@ __global__ void __launch_bounds__(128) adj_backward_kernel(const AdjK A)
 enum Pass { P_FORWARD, P_REPLAY, P_BACKWARD };
 
 template <int D, class POT>
-void launch_pass(Pass pass, const AdjK& K, unsigned blocks, unsigned threads, cudaStream_t s)
+void launch_pass(Pass pass, int variant, const AdjK& K, unsigned blocks, unsigned threads,
+                 cudaStream_t s)
 {
   switch (pass) {
     case P_FORWARD: adj_forward_kernel<D, POT><<<blocks, threads, 0, s>>>(K); break;
     case P_REPLAY: adj_replay_kernel<D, POT><<<blocks, threads, 0, s>>>(K); break;
-    case P_BACKWARD: adj_backward_kernel<D, POT><<<blocks, threads, 0, s>>>(K); break;
+    case P_BACKWARD:
+      if (variant == 1)
+        adj_backward_kernel<D, POT, 4><<<blocks, threads, 0, s>>>(K);
+      else
+        adj_backward_kernel<D, POT, 1><<<blocks, threads, 0, s>>>(K);
+      break;
   }
 }
 
@@ -172,18 +194,20 @@ int run_pass(Pass pass, const galpy_cuda_adjoint* a)
   K.gyT = a->gyT;
   K.gw0 = a->gw0;
   K.gparam = a->gparam;
+  K.order = a->order;
   const unsigned threads = a->block_size > 0 ? (unsigned)a->block_size : 64u;
   if (threads > 128 || threads % 32)
     return gpc_report_error(GALPY_CUDA_ERR_ARG, "adjoint: block_size must be 32..128, a multiple of 32");
   const unsigned blocks = (unsigned)((a->nobj + threads - 1) / threads);
   cudaStream_t s = static_cast<cudaStream_t>(a->stream);
   const bool mw14 = a->signature == GALPY_CUDA_SIG_MW14 && a->ncomp == 3;
+  const int v = a->variant;
   if (a->planar)
-    mw14 ? launch_pass<2, MW14Adj>(pass, K, blocks, threads, s)
-         : launch_pass<2, DynPot>(pass, K, blocks, threads, s);
+    mw14 ? launch_pass<2, MW14Adj>(pass, v, K, blocks, threads, s)
+         : launch_pass<2, DynPot>(pass, v, K, blocks, threads, s);
   else
-    mw14 ? launch_pass<3, MW14Adj>(pass, K, blocks, threads, s)
-         : launch_pass<3, DynPot>(pass, K, blocks, threads, s);
+    mw14 ? launch_pass<3, MW14Adj>(pass, v, K, blocks, threads, s)
+         : launch_pass<3, DynPot>(pass, v, K, blocks, threads, s);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     return gpc_report_error(GALPY_CUDA_ERR_CUDA, (std::string("adjoint launch: ") +

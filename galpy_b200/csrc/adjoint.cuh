@@ -17,13 +17,14 @@
 //     dense output as Dop853Machine, leung_dop853.c:231-517) from t0 to T;
 //     y(T) is the dense-output value inside the step that passes T, as in
 //     the reference (it does not shorten the last step).  Every 64 accepted
-//     steps the controller state (y, t, h, facold) is saved: a checkpoint.
+//     steps the state (y, t) is saved, a checkpoint, together with the
+//     segment's 64 accepted step sizes.
 //   * Backward, per orbit, segment by segment from the last: restore the
-//     segment's checkpoint, re-run the controller over it (bitwise the same
-//     accepted steps, since it is the same deterministic code), keep the
-//     start state of each step, then sweep the steps in reverse.  Each step
-//     recomputes its stages and applies the adjoint of an explicit
-//     Runge-Kutta step:
+//     segment's checkpoint, recompute the start state of each of its steps
+//     with the recorded step sizes (no step-size control runs again, so a
+//     marginal accept/reject decision cannot come out differently), then
+//     sweep the steps in reverse.  Each step recomputes its stages and
+//     applies the adjoint of an explicit Runge-Kutta step:
 //         kappa_i = h W_i lambda + h sum_{j>i} A_ji mu_j
 //         mu_i    = J(Y_i)^T kappa_i = (K(q_i) kappa_v, kappa_q)
 //         lambda <- lambda + sum_i mu_i,   g_theta += sum_i (da/dtheta)^T kappa_v
@@ -45,6 +46,7 @@ namespace adj {
 
 constexpr int kCkptEvery = 64;              // accepted steps per checkpointed segment
 constexpr int kMaxParam = 3 * kMaxComp;     // differentiable parameters per group
+constexpr int kMaxRejects = 1000;           // consecutive rejected attempts per step
 
 // ------------------------------------------------------- parameters ---
 // Differentiable parameters of a component, in this order:
@@ -538,10 +540,12 @@ GPC_HD GPC_FI void dense_final(const Field<POT>& F, const double* y, double h, d
   }
 }
 
-// Checkpoint record: y[N], t, h, facold.
+// Checkpoint record of a segment: y[N] and t at its start, then the step
+// sizes of its (up to) kCkptEvery accepted steps.
 template <int D>
 struct Ckpt {
-  static constexpr int W = 2 * D + 3;
+  static constexpr int H = 2 * D + 1;  // offset of the step sizes
+  static constexpr int W = H + kCkptEvery;
 };
 
 // ---------------------------------------------------------- forward ---
@@ -577,16 +581,18 @@ GPC_HD int forward_orbit(const Field<POT>& F, const double* w0, double t0, doubl
 #pragma unroll
       for (int i = 0; i < N; i++) p[i * cs] = y[i];
       p[N * cs] = c.t;
-      p[(N + 1) * cs] = c.h;
-      p[(N + 2) * cs] = c.facold;
     }
-    for (;;) {
+    for (int rej = 0;; rej++) {
+      // every rejection shrinks h by at least 1/1.11 down to the floor of
+      // begin_attempt; an orbit still rejected long after that is stopped
+      if (rej >= kMaxRejects) return E_BUDGET;
       const int r = attempt<D, POT>(F, y, k, ynew, c);
       att++;
       if (r < 0) return E_NONFINITE;
       if (r > 0) break;
       if (max_att > 0 && att >= max_att) return E_BUDGET;
     }
+    ck[((n / kCkptEvery) * CW + Ckpt<D>::H + n % kCkptEvery) * cs] = c.h;
     if (hrec) {
       if (n >= hcap) return E_BUDGET;
       hrec[n * hs] = c.h;
@@ -696,57 +702,43 @@ GPC_HD void step_vjp(const Field<POT>& F, const double* y, double h, double s, d
 // g (group_nparam entries, zeroed by the caller) accumulates dL/dtheta.
 // ck/cs: the forward pass's checkpoints; nsteps its accepted steps.
 template <int D, class POT>
-GPC_HD void backward_orbit(const Field<POT>& F, double t0, double T, double rtol_ln,
-                           double atol_ln, const double* ck, long long cs, long long nsteps,
-                           double* lam, double* g)
+GPC_HD void backward_orbit(const Field<POT>& F, double T, const double* ck, long long cs,
+                           long long nsteps, double* lam, double* g)
 {
   constexpr int N = 2 * D, CW = Ckpt<D>::W;
   if (nsteps <= 0) return;
-  double ys[kCkptEvery][N], hs[kCkptEvery], ts[kCkptEvery];
+  double ys[kCkptEvery][N], ts[kCkptEvery];
   const long long nseg = (nsteps + kCkptEvery - 1) / kCkptEvery;
   for (long long seg = nseg - 1; seg >= 0; seg--) {
-    // replay the controller over the segment
-    Ctl c;
-    init_ctl(c, t0, T, rtol_ln, atol_ln);
-    double y[N], ynew[N], k[16][N];
+    // recompute the start states of the segment's steps
     const double* p = ck + seg * CW * cs;
+    const double* hs = p + Ckpt<D>::H * cs;
+    const long long n0 = seg * kCkptEvery;
+    const int m1 = (int)((n0 + kCkptEvery < nsteps ? n0 + kCkptEvery : nsteps) - n0);
+    double y[N], ynew[N], inc[N], k[12][N];
 #pragma unroll
     for (int i = 0; i < N; i++) y[i] = p[i * cs];
-    c.t = p[N * cs];
-    c.h = p[(N + 1) * cs];
-    c.facold = p[(N + 2) * cs];
-    const long long n0 = seg * kCkptEvery;
-    const long long n1 = n0 + kCkptEvery < nsteps ? n0 + kCkptEvery : nsteps;
-    rhs<D, POT>(F, y, k[0]);
-    for (long long n = n0; n < n1; n++) {
-      // the forward pass accepted this step after finitely many attempts;
-      // the same code repeats them (bounded all the same)
-      int r = 0;
-      for (int guard = 0; guard < 100000 && r == 0; guard++) r = attempt<D, POT>(F, y, k, ynew, c);
-      if (r != 1) {
-#pragma unroll
-        for (int i = 0; i < N; i++) lam[i] = NAN;
-        return;
-      }
-      const int m = (int)(n - n0);
+    double t = p[N * cs];
+    for (int m = 0; m < m1; m++) {
 #pragma unroll
       for (int i = 0; i < N; i++) ys[m][i] = y[i];
-      hs[m] = c.h;
-      ts[m] = c.t;
-      if (n == n1 - 1) break;
-      c.t = c.t + c.h;
-      rhs<D, POT>(F, ynew, k[0]);
+      ts[m] = t;
+      if (m == m1 - 1) break;
+      const double h = hs[m * cs];
+      rhs<D, POT>(F, y, k[0]);
+      run_stages<D, POT, 1, 12>(F, y, h, k, nullptr);
+      new_state<D>(y, h, k, inc, ynew);
 #pragma unroll
       for (int i = 0; i < N; i++) y[i] = ynew[i];
-      next_step(c);
+      t = t + h;
     }
     // reverse sweep over the segment's steps
-    for (long long n = n1 - 1; n >= n0; n--) {
-      const int m = (int)(n - n0);
-      if (n == nsteps - 1)
-        step_vjp<D, POT, true>(F, ys[m], hs[m], (T - ts[m]) / hs[m], lam, g);
+    for (int m = m1 - 1; m >= 0; m--) {
+      const double h = hs[m * cs];
+      if (n0 + m == nsteps - 1)
+        step_vjp<D, POT, true>(F, ys[m], h, (T - ts[m]) / h, lam, g);
       else
-        step_vjp<D, POT, false>(F, ys[m], hs[m], 0.0, lam, g);
+        step_vjp<D, POT, false>(F, ys[m], h, 0.0, lam, g);
     }
   }
 }

@@ -191,10 +191,11 @@ int galpy_cuda_energy_device(const void *comps, int ncomp, const int *group, int
  *
  * The forward pass is galpy's DOP853 (the same step sequence as
  * odeint_type 6, y(T) from its dense output) from t0 to tend.  It saves the
- * integrator state every 64 accepted steps (checkpoints).  The backward pass
- * recomputes each 64-step segment from its checkpoint and applies the exact
- * adjoint of the Runge-Kutta stages with the accepted step sizes held fixed
- * (the discrete adjoint of the forward map).  All arrays are device memory
+ * state every 64 accepted steps together with those steps' sizes
+ * (checkpoints).  The backward pass recomputes each 64-step segment from its
+ * checkpoint with the recorded step sizes and applies the exact adjoint of
+ * the Runge-Kutta stages with the step sizes held fixed (the discrete adjoint
+ * of the forward map).  All arrays are device memory
  * owned by the caller; the calls are asynchronous on `stream` and allocate
  * nothing.  nv = 4 (planar: x, y, vx, vy) or 6 (x, y, z, vx, vy, vz).
  *
@@ -219,7 +220,8 @@ typedef struct galpy_cuda_adjoint {
   long long *nsteps;        /* [nobj] accepted steps: out of forward, in of replay/backward */
   int *err;                 /* [nobj] status: out of forward (0 ok, 2 budget or
                                checkpoint capacity exhausted, 3 non-finite), in of backward */
-  double *ckpt;             /* [ckpt_cap][nv+3][nobj] checkpoints: out of forward, in of backward */
+  double *ckpt;             /* [ckpt_cap][nv+1+64][nobj] checkpoints (segment start state and
+                               its 64 step sizes): out of forward, in of backward */
   int ckpt_cap;             /* checkpoints per orbit: at most 64*ckpt_cap steps */
   double *hrec;             /* [hcap][nobj] accepted step sizes: optional out of forward,
                                in of replay; NULL to skip */
@@ -229,6 +231,11 @@ typedef struct galpy_cuda_adjoint {
   double *gparam;           /* [nparam][nobj] out (backward): per-orbit dL/dparam, or NULL */
   void *stream;             /* cudaStream_t */
   int block_size;           /* 0 = default */
+  const int *order;         /* optional [nobj] permutation: thread j takes orbit order[j]
+                               (e.g. orbits by decreasing nsteps for the backward pass,
+                               so that the lanes of a warp have similar work), or NULL */
+  int variant;              /* backward register budget: 0 compiler default, 1 capped for
+                               occupancy (at most 128 registers a thread) */
 } galpy_cuda_adjoint;
 
 /* Forward pass: yT, nsteps, err, checkpoints (and hrec if set). */

@@ -169,3 +169,19 @@ class Harness:
             n, ptp, pap, gyT.ctypes.data_as(_dp), gw.ctypes.data_as(_dp), gth.ctypes.data_as(_dp),
             err.ctypes.data_as(_ip))
         return gw, gth, err
+
+    def adj_backward_frozen(self, w0, t0, tend, pot_type, pot_args, h, ns, gyT, planar=False):
+        """(dL/dw0, per-orbit dL/dtheta) of the map with frozen steps h [N, hcap]."""
+        w0 = np.ascontiguousarray(w0, np.float64)
+        gyT = np.ascontiguousarray(gyT, np.float64)
+        h = np.ascontiguousarray(h, np.float64)
+        ns = np.ascontiguousarray(ns, np.int64)
+        pt, pa, n, ptp, pap = self._pot(pot_type, pot_args)
+        gw = np.zeros_like(w0)
+        gth = np.zeros((len(w0), self.adj_nparam(pt, pa, planar)))
+        self.lib.harness_adj_backward_frozen(
+            int(planar), len(w0), w0.ctypes.data_as(_dp), ctypes.c_double(t0),
+            ctypes.c_double(tend), n, ptp, pap, h.ctypes.data_as(_dp),
+            ctypes.c_longlong(h.shape[1]), ns.ctypes.data_as(_lp), gyT.ctypes.data_as(_dp),
+            gw.ctypes.data_as(_dp), gth.ctypes.data_as(_dp))
+        return gw, gth

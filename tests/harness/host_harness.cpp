@@ -229,7 +229,7 @@ extern "C" int harness_adj_forward(int planar, int nobj, const double* w0, doubl
   if (P.rc) return P.rc;
   const int nv = planar ? 4 : 6;
   const int ccap = 4096;
-  std::vector<double> ck((size_t)ccap * (nv + 3));
+  std::vector<double> ck((size_t)ccap * (nv + 1 + adj::kCkptEvery));
   for (int i = 0; i < nobj; i++) {
     double* h = hrec ? hrec + (size_t)i * hcap : nullptr;
     if (planar)
@@ -276,7 +276,7 @@ extern "C" int harness_adj_gradient(int planar, int nobj, const double* w0, doub
   const int nv = planar ? 4 : 6;
   const int np = adj::group_nparam(P.comps.data(), npot);
   const int ccap = 4096;
-  std::vector<double> ck((size_t)ccap * (nv + 3));
+  std::vector<double> ck((size_t)ccap * (nv + 1 + adj::kCkptEvery));
   double yT[6];
   long long ns;
   for (int i = 0; i < nobj; i++) {
@@ -288,13 +288,66 @@ extern "C" int harness_adj_gradient(int planar, int nobj, const double* w0, doub
       err[i] = adj::forward_orbit<2, DynPot>(P.field(), w0 + (size_t)i * nv, t0, T, rtol, atol, 0,
                                              ck.data(), 1, ccap, nullptr, 1, 0, yT, &ns);
       if (err[i] == 0)
-        adj::backward_orbit<2, DynPot>(P.field(), t0, T, rtol, atol, ck.data(), 1, ns, lam, g);
+        adj::backward_orbit<2, DynPot>(P.field(), T, ck.data(), 1, ns, lam, g);
     } else {
       err[i] = adj::forward_orbit<3, DynPot>(P.field(), w0 + (size_t)i * nv, t0, T, rtol, atol, 0,
                                              ck.data(), 1, ccap, nullptr, 1, 0, yT, &ns);
       if (err[i] == 0)
-        adj::backward_orbit<3, DynPot>(P.field(), t0, T, rtol, atol, ck.data(), 1, ns, lam, g);
+        adj::backward_orbit<3, DynPot>(P.field(), T, ck.data(), 1, ns, lam, g);
     }
+  }
+  return np;
+}
+
+namespace {
+// Checkpoints of the frozen-step map (state and time at each segment start,
+// the step sizes), then the device's backward sweep.
+template <int D>
+void backward_frozen(const AdjPot& P, const double* w0, double t0, double T, const double* h,
+                     long long ns, double* lam, double* g)
+{
+  constexpr int N = 2 * D, CW = N + 1 + adj::kCkptEvery;
+  std::vector<double> ck((size_t)((ns + adj::kCkptEvery - 1) / adj::kCkptEvery + 1) * CW);
+  double y[N], k[12][N], inc[N], ynew[N], t = t0;
+  for (int c = 0; c < N; c++) y[c] = w0[c];
+  for (long long n = 0; n < ns; n++) {
+    double* p = ck.data() + (n / adj::kCkptEvery) * CW;
+    if (n % adj::kCkptEvery == 0) {
+      for (int c = 0; c < N; c++) p[c] = y[c];
+      p[N] = t;
+    }
+    p[N + 1 + n % adj::kCkptEvery] = h[n];
+    adj::rhs<D, DynPot>(P.field(), y, k[0]);
+    adj::run_stages<D, DynPot, 1, 12>(P.field(), y, h[n], k, nullptr);
+    adj::new_state<D>(y, h[n], k, inc, ynew);
+    for (int c = 0; c < N; c++) y[c] = ynew[c];
+    t = t + h[n];
+  }
+  adj::backward_orbit<D, DynPot>(P.field(), T, ck.data(), 1, ns, lam, g);
+}
+}  // namespace
+
+// Backward pass with given frozen steps hrec [nobj][hcap] (nsteps [nobj]).
+// Returns np.
+extern "C" int harness_adj_backward_frozen(int planar, int nobj, const double* w0, double t0,
+                                           double T, int npot, const int* pot_type,
+                                           const double* pot_args, const double* hrec,
+                                           long long hcap, const long long* nsteps,
+                                           const double* gyT, double* gw0, double* gth)
+{
+  AdjPot P(planar, npot, pot_type, pot_args);
+  if (P.rc) return P.rc;
+  const int nv = planar ? 4 : 6;
+  const int np = adj::group_nparam(P.comps.data(), npot);
+  for (int i = 0; i < nobj; i++) {
+    double* lam = gw0 + (size_t)i * nv;
+    double* g = gth + (size_t)i * np;
+    for (int c = 0; c < nv; c++) lam[c] = gyT[(size_t)i * nv + c];
+    for (int p = 0; p < np; p++) g[p] = 0.0;
+    if (planar)
+      backward_frozen<2>(P, w0 + (size_t)i * nv, t0, T, hrec + (size_t)i * hcap, nsteps[i], lam, g);
+    else
+      backward_frozen<3>(P, w0 + (size_t)i * nv, t0, T, hrec + (size_t)i * hcap, nsteps[i], lam, g);
   }
   return np;
 }

@@ -59,24 +59,37 @@ def _run(pt, pa, w0, T, planar, generic=False, gy=None, record=0, rtol=1e-10):
 @pytest.mark.parametrize("planar", [True, False])
 @pytest.mark.parametrize("generic", [False, True])
 def test_gpu_adjoint_matches_host_build(harness, golden, planar, generic):
+    """The same algorithm built for the host.  The step-size controller
+    amplifies rounding (its error norm is a small difference of stage
+    sums), so device and host choose step sizes that agree to ~1e-7; with
+    the device's steps frozen into the host build, forward map and gradients
+    agree to rounding."""
     pt, pa = _pot(golden, planar)
     w0 = cyl_to_rect(seeded_ics(64, 21, planar=planar))
     T = 20.0
-    yh, nh, eh, _ = harness.adj_forward(w0, 0.0, T, pt, pa, planar=planar)
+    yh, nh, eh, hh = harness.adj_forward(w0, 0.0, T, pt, pa, planar=planar)
     gy = np.random.default_rng(2).normal(size=yh.shape)
-    gwh, gth, _ = harness.adj_gradient(w0, 0.0, T, pt, pa, gy, planar=planar)
-    r = _run(pt, pa, w0, T, planar, generic, gy=gy)
+    r = _run(pt, pa, w0, T, planar, generic, gy=gy, record=hh.shape[1] + 64)
     f = r["fwd"]
     assert not f["err"].any()
     ns = f["nsteps"].cpu().numpy()
-    same = ns == nh
-    assert same.mean() >= 0.95
+    hd = np.ascontiguousarray(f["hrec"].cpu().numpy().T)
     yT = f["yT"].cpu().numpy().T
-    np.testing.assert_allclose(yT[same], yh[same], rtol=0, atol=1e-10)
-    np.testing.assert_allclose(r["gw0"][same], gwh[same], rtol=1e-8,
-                               atol=1e-8 * np.abs(gwh).max())
-    np.testing.assert_allclose(r["gparam"][same], gth[same], rtol=1e-8,
-                               atol=1e-8 * np.abs(gth).max())
+    # independent step choices: mostly the same counts and steps (a rejection
+    # taken on one side only changes the rest of an orbit's sequence), and
+    # the same results to the integration tolerance
+    k = min(hd.shape[1], hh.shape[1])
+    unused = np.arange(k)[None, :] >= nh[:, None]
+    close = (ns == nh) & np.all((np.abs(hd[:, :k] - hh[:, :k]) <= 1e-6 * np.abs(hh[:, :k])) |
+                                unused, axis=1)
+    assert close.mean() >= 0.75, close.mean()
+    np.testing.assert_allclose(yT, yh, rtol=0, atol=1e-8)
+    # the device's steps frozen into the host build
+    np.testing.assert_allclose(harness.adj_replay(w0, 0.0, T, pt, pa, hd, ns, planar=planar),
+                               yT, rtol=0, atol=1e-12)
+    gwh, gth = harness.adj_backward_frozen(w0, 0.0, T, pt, pa, hd, ns, gy, planar=planar)
+    for dev, host in ((r["gw0"], gwh), (r["gparam"], gth)):
+        np.testing.assert_allclose(dev, host, rtol=1e-10, atol=1e-10 * np.abs(host).max())
 
 
 @pytest.mark.parametrize("planar", [True, False])
