@@ -97,3 +97,18 @@ def test_package_has_no_cpu_path():
                 for needle in ("import oracle", "from oracle", "liboracle", "oracle/",
                                "libgalpy_ref", "oracle_integrate"):
                     assert needle not in txt, (f, needle)
+
+
+def test_autotune_candidates_and_keys():
+    from galpy_b200 import autotune
+
+    dop = autotune.candidates("dop853_cuda")
+    assert all(c["block_size"] == 128 and c["threads_per_orbit"] == 1 for c in dop)
+    assert {(c["variant"], c["schedule"]) for c in dop} == {
+        (v, s) for v in (0, 1) for s in ("longest_first", "in_order")}
+    assert {c["block_size"] for c in autotune.candidates("symplec4_cuda")} == {64, 128}
+    k1 = autotune.workload_key("B200", "dop853_cuda", False, "fp64", 1, False, 1 << 20, True)
+    k2 = autotune.workload_key("B200", "dop853_cuda", False, "fp64", 1, False, (1 << 20) + 5,
+                               True)
+    k3 = autotune.workload_key("B200", "dop853_cuda", True, "fp64", 1, False, 1 << 20, True)
+    assert k1 != k3 and k1.split("|n~")[0] == k2.split("|n~")[0]
