@@ -19,6 +19,7 @@ from .integrate import (CUDA_METHODS, compile_potential, energy_device,  # noqa:
                         integrateFullOrbit_dxdv_cuda, integratePlanarOrbit_cuda,
                         integratePlanarOrbit_dxdv_cuda, parse_integrator, parse_tol,
                         signature)
+from .adjoint import final_state  # noqa: F401
 from .potentials import (HernquistPotential, LogarithmicHaloPotential,  # noqa: F401
                          MiyamotoNagaiPotential, MWPotential2014, NFWPotential,
                          PowerSphericalPotentialwCutoff, parse_pot)

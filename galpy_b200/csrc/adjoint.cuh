@@ -158,23 +158,46 @@ GPC_HD void accel_param_vjp(const GpComp* __restrict__ comp, int ncomp, double x
   }
 }
 
-// mu_q = K(q) lv (K the symmetric tidal tensor) and the parameter terms.
+// The per-point force and vector-Jacobian functions are called, not
+// inlined, in device code: a DOP853 step unrolls 12-16 stages, and inlining
+// a force or tidal evaluation into every one of them made the kernels too
+// large for the instruction cache (warps stalled on instruction fetch).
+// Arguments and results travel in registers (scalars and a small struct).
+#if defined(__CUDACC__)
+#define GPC_NI __noinline__
+#else
+#define GPC_NI
+#endif
+
+struct V3 {
+  double x, y, z;
+};
+
+// mu_q = K(q) lv (K the symmetric tidal tensor); g += (da/dtheta)^T lv.
+template <bool PLANAR>
+GPC_HD GPC_NI V3 vjp_at(const GpComp* __restrict__ comp, int ncomp, double x, double y, double z,
+                        double lx, double ly, double lz, double* g)
+{
+  double ax, ay, az, K[6];
+  if (PLANAR) z = lz = 0.0;
+  accel_tidal<PLANAR>(comp, ncomp, x, y, z, ax, ay, az, K);
+  V3 r;
+  r.x = K[0] * lx + K[1] * ly + K[3] * lz;
+  r.y = K[1] * lx + K[2] * ly + K[4] * lz;
+  r.z = K[3] * lx + K[4] * ly + K[5] * lz;
+  accel_param_vjp<PLANAR>(comp, ncomp, x, y, z, lx, ly, lz, g);
+  return r;
+}
+
 template <int D>
 GPC_HD GPC_FI void accel_vjp(const GpComp* __restrict__ comp, int ncomp, const double* q,
                              const double* lv, double* Kv, double* g)
 {
-  double ax, ay, az, K[6];
-  const double z = D == 3 ? q[D - 1] : 0.0;
-  const double lz = D == 3 ? lv[D - 1] : 0.0;
-  accel_tidal<D == 2>(comp, ncomp, q[0], q[1], z, ax, ay, az, K);
-  Kv[0] = K[0] * lv[0] + K[1] * lv[1];
-  Kv[1] = K[1] * lv[0] + K[2] * lv[1];
-  if (D == 3) {
-    Kv[0] += K[3] * lz;
-    Kv[1] += K[4] * lz;
-    Kv[D - 1] = K[3] * lv[0] + K[4] * lv[1] + K[5] * lz;
-  }
-  accel_param_vjp<D == 2>(comp, ncomp, q[0], q[1], z, lv[0], lv[1], lz, g);
+  const V3 r = vjp_at<D == 2>(comp, ncomp, q[0], q[1], D == 3 ? q[D - 1] : 0.0, lv[0], lv[1],
+                              D == 3 ? lv[D - 1] : 0.0, g);
+  Kv[0] = r.x;
+  Kv[1] = r.y;
+  if (D == 3) Kv[D - 1] = r.z;
 }
 
 // ---------------------------------------------------------- tableau ---
@@ -356,18 +379,26 @@ struct Field {
   const double* scal;
 };
 
+template <bool PLANAR, class POT>
+GPC_HD GPC_NI V3 accel_at(const GpComp* __restrict__ comp, int ncomp, const double* scal,
+                          double x, double y, double z)
+{
+  V3 a = {0.0, 0.0, 0.0};
+  accel<double, PLANAR, POT>(comp, ncomp, x, y, z, a.x, a.y, a.z, scal);
+  return a;
+}
+
 // k = f(Y) = (velocities, accelerations); state (x, y[, z], vx, vy[, vz]).
 template <int D, class POT>
 GPC_HD GPC_FI void rhs(const Field<POT>& F, const double* Y, double* k)
 {
-  double ax = 0.0, ay = 0.0, az = 0.0;
-  accel<double, D == 2, POT>(F.comp, F.ncomp, Y[0], Y[1], D == 3 ? Y[D - 1] : 0.0, ax, ay, az,
-                             F.scal);
+  const V3 a = accel_at<D == 2, POT>(F.comp, F.ncomp, F.scal, Y[0], Y[1],
+                                     D == 3 ? Y[D - 1] : 0.0);
 #pragma unroll
   for (int c = 0; c < D; c++) k[c] = Y[D + c];
-  k[D] = ax;
-  k[D + 1] = ay;
-  if (D == 3) k[2 * D - 1] = az;
+  k[D] = a.x;
+  k[D + 1] = a.y;
+  if (D == 3) k[2 * D - 1] = a.z;
 }
 
 // Stages I0..I1-1 from y with step h (k[0..I0-1] given).  Q, if not null,
