@@ -13,7 +13,8 @@ not built and CudaError when no GPU is available.
 """
 from ._lib import (CudaError, CudaLibraryMissing, MethodNotSupported,  # noqa: F401
                    PotentialNotSupported)
-from .integrate import (CUDA_METHODS, compile_potential, energy_device,  # noqa: F401
+from .integrate import (CUDA_METHODS, accel_device, compile_potential,  # noqa: F401
+                        energy_device,
                         integrate_device,
                         integrate_dxdv_batch, integrateFullOrbit_cuda,
                         integrateFullOrbit_dxdv_cuda, integratePlanarOrbit_cuda,

@@ -95,7 +95,7 @@ GPC_HD void accel_param_vjp(const GpComp* __restrict__ comp, int ncomp, double x
         const double pw = exp(ldg(&cp->c[3]) * log(r2));  // (r^2)^(-alpha/2)
         double Mr3;
         if (u < ldg(&cp->c[5])) {
-          Mr3 = ldg(&cp->c[2]) * pw * gamma_star<double>(cp, u, ldg(&cp->c[6]));
+          Mr3 = ldg(&cp->c[2]) * pw * gamma_star<double>(tables(cp), u, ldg(&cp->c[6]));
         } else {
           const double ir = rsq(r2);
           Mr3 = ldg(&cp->c[4]) * ir * ir * ir;

@@ -8,6 +8,7 @@
 // precomputed once per call instead of once per force evaluation.
 #pragma once
 #include <math.h>
+#include <stddef.h>
 #include <string.h>
 
 #include "potentials.cuh"
@@ -87,6 +88,75 @@ inline void build_gamma_star_table(double a, double U, double (*cheb)[kChebC])
   }
 }
 
+// Degree-11 Chebyshev interpolants of f(m) on the eighths [1 + j/8,
+// 1 + (j+1)/8] of a binade, converted to the power basis of the local
+// variable t = 16 m - (17 + 2 j) in [-1, 1] (the binade tables of
+// potentials.cuh), in long double.
+template <class F>
+inline void build_binade_table(F f, double (*out)[kChebC])
+{
+  const long double pi = 3.141592653589793238462643383279502884L;
+  long double T[kChebC][kChebC] = {};
+  T[0][0] = 1.0L;
+  T[1][1] = 1.0L;
+  for (int j = 2; j < kChebC; j++)
+    for (int m = 0; m < kChebC; m++)
+      T[j][m] = (m > 0 ? 2.0L * T[j - 1][m - 1] : 0.0L) - T[j - 2][m];
+  for (int k = 0; k < kBinSub; k++) {
+    long double fv[kChebC], cj[kChebC];
+    for (int i = 0; i < kChebC; i++) {
+      const long double t = cosl(pi * (i + 0.5L) / kChebC);
+      fv[i] = f((17.0L + 2.0L * k + t) / 16.0L);
+    }
+    for (int j = 0; j < kChebC; j++) {
+      long double s = 0.0L;
+      for (int i = 0; i < kChebC; i++) s += fv[i] * cosl(pi * j * (i + 0.5L) / kChebC);
+      s *= 2.0L / kChebC;
+      if (j == 0) s *= 0.5L;
+      cj[j] = s;
+    }
+    for (int m = 0; m < kChebC; m++) {
+      long double s = 0.0L;
+      for (int j = 0; j < kChebC; j++) s += cj[j] * T[j][m];
+      out[k][m] = (double)s;
+    }
+  }
+}
+
+// 2^(p e) for the binade exponent e + 1024 = 64 hi + lo (PSwC power tables);
+// values beyond the double range (binades far outside any orbit) are
+// clamped to finite numbers.
+inline void build_power_exponent_tables(long double p, double* e2hi, double* e2lo)
+{
+  auto fin = [](long double v) {
+    const long double big = 1.0e300L, tiny = 1.0e-300L;
+    return (double)(v > big ? big : (v < tiny ? tiny : v));
+  };
+  for (int hi = 0; hi < 32; hi++) e2hi[hi] = fin(exp2l(p * 64.0L * (hi - 16)));
+  for (int lo = 0; lo < 64; lo++) e2lo[lo] = fin(exp2l(p * lo));
+}
+
+// Point every record at the first earlier record of the same type whose
+// tables are identical (GpComp::tab), so that parameter groups share one
+// copy of each table.
+inline void share_tables(GpComp* c, int n)
+{
+  const size_t off = offsetof(GpComp, cheb);
+  const size_t len = sizeof(GpComp) - off;
+  for (int i = 0; i < n; i++) {
+    c[i].tab = 0;
+    if (c[i].type != T_PSWC && c[i].type != T_NFW) continue;
+    for (int j = 0; j < i; j++) {
+      if (c[j].type == c[i].type && c[j].tab == 0 &&
+          memcmp(reinterpret_cast<const char*>(&c[j]) + off,
+                 reinterpret_cast<const char*>(&c[i]) + off, len) == 0) {
+        c[i].tab = j - i;
+        break;
+      }
+    }
+  }
+}
+
 // Compile one group.  Returns 0, -3 (unsupported type) or -1 (bad args).
 // *consumed receives the number of pot_args read.
 inline int compile_group(int planar, int npot, const int* pot_type, const double* pot_args,
@@ -118,6 +188,11 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
         c.c[6] = kChebN / U;
         c.c[7] = 4.0 * M_PI;
         build_gamma_star_table(a, U, c.cheb);
+        {  // (r^2)^(-alpha/2) = m^(-alpha/2) 2^(-alpha/2 e)
+          const long double pw = -0.5L * (long double)alpha;
+          build_binade_table([pw](long double m) { return powl(m, pw); }, c.bin);
+          build_power_exponent_tables(pw, c.e2hi, c.e2lo);
+        }
         // potential energy: gamma(1 - alpha/2, u) and gamma(1.5 - alpha/2, u)
         c.c[8] = 2.0 * M_PI * pow(rc, 3.0 - alpha);
         c.c[9] = rc;
@@ -138,6 +213,8 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
         if (!(p[1] > 0.0)) return -1;
         c.c[1] = p[1];
         c.c[2] = 1.0 / p[1];
+        if (type == T_NFW)  // log(m) / (m - 1); the nodes never fall on m = 1
+          build_binade_table([](long double m) { return logl(m) / (m - 1.0L); }, c.bin);
         break;
       case T_LOGHALO: {
         const double q = p[1], core2 = p[2], om = p[3];
@@ -150,6 +227,10 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
         break;
       }
     }
+    for (int i = 0; i < kChebN; i++)
+      for (int j = 0; j < kChebC; j++) c.chebf[i][j] = (float)c.cheb[i][j];
+    for (int i = 0; i < kBinSub; i++)
+      for (int j = 0; j < kChebC; j++) c.binf[i][j] = (float)c.bin[i][j];
     out[k] = c;
     p += na;
   }

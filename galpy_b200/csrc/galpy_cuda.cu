@@ -658,6 +658,28 @@ __global__ void __launch_bounds__(256) energy_kernel(const GpComp* comps, int nc
   E[i] = 0.5 * (vx * vx + vy * vy + vz * vz) + potential_value(c, ncomp, x, y, z);
 }
 
+// Accelerations at points (positions SoA [3][n], z ignored when planar) with
+// the integrators' own force code: run-time component list, or the
+// compile-time MWPotential2014 list when mw14 (the headline kernels' path).
+template <class POT, int PREC>
+__global__ void __launch_bounds__(256) accel_kernel(const GpComp* comps, int ncomp,
+                                                    const int* group, int planar,
+                                                    const double* pos, long long n, double* acc)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const GpComp* c = comps + (group ? (long long)group[i] * ncomp : 0LL);
+  const double q[3] = {pos[i], pos[n + i], planar ? 0.0 : pos[2 * n + i]};
+  double a[3] = {0.0, 0.0, 0.0};
+  if (planar)
+    eval_force<2, PREC, false, POT>(c, ncomp, q, a);
+  else
+    eval_force<3, PREC, false, POT>(c, ncomp, q, a);
+  acc[i] = a[0];
+  acc[n + i] = a[1];
+  acc[2 * n + i] = a[2];
+}
+
 // ----------------------------------------------------------------------------
 // FP64 pipe peak: independent fused multiply-add chains per thread
 // ----------------------------------------------------------------------------
@@ -796,6 +818,34 @@ int galpy_cuda_energy_device(const void* comps, int ncomp, const int* group, int
   return GALPY_CUDA_OK;
 }
 
+int galpy_cuda_accel_device(const void* comps, int ncomp, const int* group, int planar,
+                            int signature, int precision, const double* pos, long long n,
+                            double* acc, void* stream)
+{
+  if (!comps || !pos || !acc || n < 0 || ncomp < 1 || ncomp > kMaxComp)
+    return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
+  if (precision != GALPY_CUDA_FP64 && precision != GALPY_CUDA_F32FORCE)
+    return set_error(GALPY_CUDA_ERR_ARG, "unknown precision");
+  if (n == 0) return GALPY_CUDA_OK;
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const GpComp* c = static_cast<const GpComp*>(comps);
+  const bool mw14 = signature == GALPY_CUDA_SIG_MW14 && ncomp == 3;
+  if (precision == GALPY_CUDA_FP64) {
+    if (mw14)
+      accel_kernel<MW14GroupPot, PREC_FP64><<<blocks, 256, 0, s>>>(c, ncomp, group, planar, pos, n, acc);
+    else
+      accel_kernel<DynPot, PREC_FP64><<<blocks, 256, 0, s>>>(c, ncomp, group, planar, pos, n, acc);
+  } else {
+    if (mw14)
+      accel_kernel<MW14GroupPot, PREC_F32><<<blocks, 256, 0, s>>>(c, ncomp, group, planar, pos, n, acc);
+    else
+      accel_kernel<DynPot, PREC_F32><<<blocks, 256, 0, s>>>(c, ncomp, group, planar, pos, n, acc);
+  }
+  GPC_CUDA_TRY(cudaGetLastError());
+  return GALPY_CUDA_OK;
+}
+
 int galpy_cuda_fp64_peak(double* tflops, double* ms)
 {
   int dev = 0, nsm = 0;
@@ -861,6 +911,7 @@ int galpy_cuda_compile_potential(int planar, int npot, const int* pot_type,
     if (rc) return set_error(GALPY_CUDA_ERR_ARG, "invalid potential arguments");
     p += used;
   }
+  share_tables(c, ngroup * npot);
   return GALPY_CUDA_OK;
 }
 

@@ -43,6 +43,7 @@ enum : int { T_LOGHALO = 0, T_MN = 5, T_HERNQUIST = 8, T_NFW = 9, T_PSWC = 15 };
 constexpr int kMaxComp = 16;  // components per potential group
 constexpr int kChebN = 32;    // Chebyshev intervals of gamma*(a, u) on [0, U]
 constexpr int kChebC = 12;    // coefficients per interval (degree 11)
+constexpr int kBinSub = 8;    // sub-intervals of a binade [1, 2) in the binade tables
 
 // One compiled potential component.  c[] by type:
 //   PSwC:      c0 amp, c1 1/rc^2, c2 Mnorm rc^(-2a), c3 -alpha/2,
@@ -56,21 +57,98 @@ constexpr int kChebC = 12;    // coefficients per interval (degree 11)
 //   PSwC potential (energy evaluation only): c8 2 pi rc^(3-alpha), c9 rc,
 //              c10 a1 = 1 - alpha/2, c11 Gamma(a1), c12 lgamma(a1),
 //              c13 a2 = 1.5 - alpha/2, c14 Gamma(a2), c15 lgamma(a2)
+//
+// Binade tables (FP64 force path): a function of x > 0 is evaluated from
+// x = m 2^e, m in [1, 2), as g(m) * h(e), with g from a degree-11 polynomial
+// on each eighth of [1, 2) (power basis of the local variable t in [-1, 1])
+// and h(e) from two small tables indexed by e + 1024 = 64 hi + lo.
+//   PSwC: bin = m^(-alpha/2), e2hi[hi] = 2^(-alpha/2 * 64 (hi - 16)),
+//         e2lo[lo] = 2^(-alpha/2 * lo)  -> (r^2)^(-alpha/2)
+//   NFW:  bin = log(m) / (m - 1)         -> log1p(r/a)
+//
+// tab: offset, in records, of the record that holds this component's
+// tables (0: its own).  Parameter groups whose tables are identical (the
+// gamma* and power tables depend only on alpha, the NFW table on nothing)
+// share one copy, which keeps a ragged launch's table working set in L1.
 struct GpComp {
   int type;
-  int pad;
+  int tab;
   double c[16];
   double cheb[kChebN][kChebC];  // PSwC only: power-basis coefficients per interval
+  double bin[kBinSub][kChebC];  // PSwC, NFW: binade polynomial
+  double e2hi[32];              // PSwC only
+  double e2lo[64];              // PSwC only
+  float chebf[kChebN][kChebC];  // single-precision copies for the FP32 force path
+  float binf[kBinSub][kChebC];
 };
+
+// --------------------------------------------- branch-free FP64 helpers ---
+// The force of an orbit step is a dependent chain of special functions; the
+// library versions of log, exp, log1p, division and rsqrt carry branches for
+// special operands, which also keep the compiler from interleaving the
+// components of a potential.  These replacements are straight-line code for
+// the positive, normal operands of the force path (not for 0, inf, NaN or
+// subnormals).
+//
+// 1/sqrt(x) and 1/x: the hardware's approximate double-precision result
+// (PTX rsqrt.approx.f64 / rcp.approx.ftz.f64, about 2^-22 relative) as a
+// seed and one third-order Newton correction, y <- y (1 + e/2 + 3e^2/8) with
+// e = 1 - x y^2 (resp. y (1 + e + e^2), e = 1 - x y), the residual formed
+// with a fused multiply-add: error O(e^3) ~ 1e-20, so the result is within a
+// few ulp (tests/test_gpu_parity.py checks it against 1/sqrt and 1/x).
+GPC_HD GPC_FI double rsqrt_nr(double x)
+{
+#if defined(__CUDA_ARCH__)
+  double y;
+  asm("rsqrt.approx.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double e = fma(-x * y, y, 1.0);
+  return fma(y * e, fma(0.375, e, 0.5), y);
+#else
+  return 1.0 / sqrt(x);
+#endif
+}
+
+GPC_HD GPC_FI double rcp_nr(double x)
+{
+#if defined(__CUDA_ARCH__)
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double e = fma(-x, y, 1.0);
+  return fma(y, fma(e, e, e), y);
+#else
+  return 1.0 / x;
+#endif
+}
+
+GPC_HD GPC_FI long long bits_of(double x)
+{
+#if defined(__CUDA_ARCH__)
+  return __double_as_longlong(x);
+#else
+  long long b;
+  memcpy(&b, &x, sizeof(b));
+  return b;
+#endif
+}
+
+GPC_HD GPC_FI double double_of(long long b)
+{
+#if defined(__CUDA_ARCH__)
+  return __longlong_as_double(b);
+#else
+  double x;
+  memcpy(&x, &b, sizeof(x));
+  return x;
+#endif
+}
 
 // ---------------------------------------------------------------- math ---
 template <typename T> struct Num;
 template <> struct Num<double> {
   GPC_HD static double lg(double x) { return log(x); }
   GPC_HD static double ex(double x) { return exp(x); }
-  GPC_HD static double lg1p(double x) { return log1p(x); }
-  GPC_HD static double rsq(double x) { return gpc::rsq(x); }
-  GPC_HD static double rcp(double x) { return 1.0 / x; }
+  GPC_HD static double rsq(double x) { return rsqrt_nr(x); }
+  GPC_HD static double rcp(double x) { return rcp_nr(x); }
 };
 // FP32 evaluation: hardware approximations (SFU) for log/exp/rsqrt/rcp.
 template <> struct Num<float> {
@@ -83,7 +161,6 @@ template <> struct Num<float> {
   static float ex(float x) { return expf(x); }
   static float rcp(float x) { return 1.0f / x; }
 #endif
-  GPC_HD static float lg1p(float x) { return log1pf(x); }
   GPC_HD static float rsq(float x) { return gpc::rsqf(x); }
 };
 
@@ -92,18 +169,112 @@ template <> struct Num<float> {
 // interval's local variable x in [-1, 1] and evaluated by Horner's rule (11
 // dependent FMAs, half the dependency chain of the Clenshaw recurrence; both
 // stay within ~1 ulp here, tests/test_harness.py checks against mpmath).
+// The record holding a component's tables.
+GPC_HD GPC_FI const GpComp* tables(const GpComp* cp) { return cp + ldg(&cp->tab); }
+
+// tp: the component's table record (tables(cp); cp itself in a launch with a
+// single potential, where every record holds its own tables).
 template <typename T>
-GPC_HD GPC_FI T gamma_star(const GpComp* __restrict__ cp, T u, T scale)
+GPC_HD GPC_FI T gamma_star(const GpComp* __restrict__ tp, T u, T scale)
 {
   const T s = u * scale;
   int k = (int)s;
   k = k < kChebN - 1 ? k : kChebN - 1;
   const T x = T(2) * (s - T(k)) - T(1);
-  const double* c = cp->cheb[k];
-  T p = T(ldg(c + kChebC - 1));
+  // the FP32 path reads the single-precision copy (no conversions)
+  const T* c;
+  if constexpr (sizeof(T) == sizeof(double))
+    c = tp->cheb[k];
+  else
+    c = tp->chebf[k];
+  T p = ldg(c + kChebC - 1);
 #pragma unroll
-  for (int j = kChebC - 2; j >= 0; j--) p = p * x + T(ldg(c + j));
+  for (int j = kChebC - 2; j >= 0; j--) p = p * x + ldg(c + j);
   return p;
+}
+
+// x = m 2^e (x > 0 normal): the binade-table polynomial at m, e + 1024 and
+// the table row.
+struct Binade {
+  int ebias;  // e + 1024, in [1, 2047] for normal x
+  const double* row;
+  double t;   // local variable of m's eighth of [1, 2), in [-1, 1)
+  double m1;  // m - 1 (exact)
+};
+
+GPC_HD GPC_FI Binade binade(const GpComp* __restrict__ tp, double x)
+{
+  const long long b = bits_of(x);
+  Binade r;
+  r.ebias = (int)((b >> 52) & 0x7ff) + 1;
+  const int j = (int)((b >> 49) & 7);
+  const double m = double_of((b & 0x000fffffffffffffLL) | 0x3ff0000000000000LL);
+  r.t = 16.0 * m - (double)(17 + 2 * j);  // exact
+  r.m1 = m - 1.0;                          // exact
+  r.row = tp->bin[j];
+  return r;
+}
+
+GPC_HD GPC_FI double horner12(const double* c, double t)
+{
+  double p = ldg(c + kChebC - 1);
+#pragma unroll
+  for (int k = kChebC - 2; k >= 0; k--) p = fma(p, t, ldg(c + k));
+  return p;
+}
+
+// (r^2)^(-alpha/2) from the PowerSphericalwCutoff component's tables
+GPC_HD GPC_FI double pswc_power(const GpComp* __restrict__ tp, double r2)
+{
+  const Binade q = binade(tp, r2);
+  const double s = ldg(&tp->e2hi[q.ebias >> 6]) * ldg(&tp->e2lo[q.ebias & 63]);
+  return s * horner12(q.row, q.t);
+}
+
+// log1p(x), x >= 0, from the NFW component's table of log(m) / (m - 1)
+// (smooth, 1 at m = 1, so small arguments keep their relative accuracy):
+// u = 1 + x rounded, log1p(x) = log(u) + (x - (u - 1)) / u to first order in
+// the rounding of u.
+GPC_HD GPC_FI double nfw_log1p(const GpComp* __restrict__ tp, double x)
+{
+  // ln 2 = ln2_hi + ln2_lo, the head rounded to 32 significant bits so that
+  // e * ln2_hi is exact for every binade e
+  constexpr double ln2_hi = 0.6931471803691238;
+  constexpr double ln2_lo = 1.9082149292705877e-10;
+  const double u = 1.0 + x;
+  const double corr = (x - (u - 1.0)) * rcp_nr(u);
+  const Binade q = binade(tp, u);
+  const double e = (double)(q.ebias - 1024);
+  return fma(e, ln2_hi, fma(q.m1, horner12(q.row, q.t), fma(e, ln2_lo, corr)));
+}
+
+// The same log1p in single precision from the float copy of the table.
+GPC_HD GPC_FI float nfw_log1pf(const GpComp* __restrict__ tp, float x)
+{
+  const float u = 1.0f + x;
+#if defined(__CUDA_ARCH__)
+  const int b = __float_as_int(u);
+  const float corr = (x - (u - 1.0f)) * __frcp_rn(u);
+#else
+  int b;
+  memcpy(&b, &u, sizeof(b));
+  const float corr = (x - (u - 1.0f)) / u;
+#endif
+  const int e = ((b >> 23) & 0xff) - 127;
+  const int j = (b >> 20) & 7;
+  const int mb = (b & 0x7fffff) | 0x3f800000;
+  float m;
+#if defined(__CUDA_ARCH__)
+  m = __int_as_float(mb);
+#else
+  memcpy(&m, &mb, sizeof(m));
+#endif
+  const float t = 16.0f * m - (float)(17 + 2 * j);
+  const float* c = tp->binf[j];
+  float p = ldg(c + kChebC - 1);
+#pragma unroll
+  for (int k = kChebC - 2; k >= 0; k--) p = fmaf(p, t, ldg(c + k));
+  return fmaf((float)e, 0.69314718f, fmaf(m - 1.0f, p, corr));
 }
 
 // ------------------------------------------------------------- forces ---
@@ -114,10 +285,12 @@ GPC_HD GPC_FI T gamma_star(const GpComp* __restrict__ cp, T u, T scale)
 // (constant bank: no load instruction when the index is a compile-time
 // constant) when every orbit of a launch uses the same potential.
 struct ScalarsGlobal {
+  static constexpr bool kDirect = false;
   const GpComp* cp;
   GPC_HD GPC_FI double operator[](int j) const { return ldg(&cp->c[j]); }
 };
 struct ScalarsDirect {
+  static constexpr bool kDirect = true;  // one potential: records hold their own tables
   const double* p;
   GPC_HD GPC_FI double operator[](int j) const { return p[j]; }
 };
@@ -128,14 +301,23 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
 {
   const int type = TYPE >= 0 ? TYPE : ldg(&cp->type);
   const T amp = T(sc[0]);
+  constexpr bool F64 = sizeof(T) == sizeof(double);  // FP64: branch-free helpers
+  const GpComp* tp = S::kDirect ? cp : tables(cp);
   switch (type) {
     case T_PSWC: {
       // F = -amp M(r)/r^3 r_vec
       const T u = r2 * T(sc[1]);
       T f;
-      if (u < T(sc[5])) {
+      if constexpr (F64) {
+        // both forms, then a select: no branch in the force chain
+        const double ir = rsqrt_nr(r2);
+        const double inner =
+            sc[2] * pswc_power(tp, r2) * gamma_star<double>(tp, fmin(u, sc[5]), sc[6]);
+        const double outer = sc[4] * (ir * ir * ir);
+        f = -amp * (u < sc[5] ? inner : outer);
+      } else if (u < T(sc[5])) {
         const T pw = Num<T>::ex(T(sc[3]) * Num<T>::lg(r2));  // (r^2)^(-alpha/2)
-        f = -amp * T(sc[2]) * pw * gamma_star<T>(cp, u, T(sc[6]));
+        f = -amp * T(sc[2]) * pw * gamma_star<T>(tp, u, T(sc[6]));
       } else {
         const T ir = Num<T>::rsq(r2);
         f = -amp * T(sc[4]) * (ir * ir * ir);
@@ -158,9 +340,16 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
     case T_NFW: {
       // Phi = -amp ln(1 + r/a)/r ; F = amp (1/(r^2 (a+r)) - ln(1+r/a)/r^3) r_vec
       const T a = T(sc[1]);
-      const T ir = Num<T>::rsq(r2);
-      const T r = r2 * ir;
-      const T f = amp * ir * ir * (Num<T>::rcp(a + r) - Num<T>::lg1p(r * T(sc[2])) * ir);
+      T f;
+      if constexpr (F64) {
+        const double ir = rsqrt_nr(r2);
+        const double r = r2 * ir;
+        f = amp * ir * ir * (rcp_nr(a + r) - nfw_log1p(tp, r * sc[2]) * ir);
+      } else {
+        const T ir = Num<T>::rsq(r2);
+        const T r = r2 * ir;
+        f = amp * ir * ir * (Num<T>::rcp(a + r) - nfw_log1pf(tp, r * T(sc[2])) * ir);
+      }
       gR += f;
       gz += f;
       break;
@@ -288,7 +477,7 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
         const double pw = exp(ldg(&cp->c[3]) * log(r2));  // (r^2)^(-alpha/2)
         double Mr3;                                         // M(r) / r^3
         if (u < ldg(&cp->c[5])) {
-          Mr3 = ldg(&cp->c[2]) * pw * gamma_star<double>(cp, u, ldg(&cp->c[6]));
+          Mr3 = ldg(&cp->c[2]) * pw * gamma_star<double>(tables(cp), u, ldg(&cp->c[6]));
         } else {
           const double ir = rsq(r2);
           Mr3 = ldg(&cp->c[4]) * ir * ir * ir;

@@ -280,6 +280,22 @@ def integrate_device(comps, ncomp, w0, t, out, err, int_method, planar=False, va
     _lib.check(_lib.lib().galpy_cuda_integrate_device(ctypes.byref(L)))
 
 
+def accel_device(comps, ncomp, pos, acc, planar=False, signature=0, precision="fp64",
+                 group=None, stream=None):
+    """Accelerations [3, N] at positions pos [3, N] (float64 CUDA tensors,
+    z ignored when planar) with the integration kernels' force code."""
+    import torch
+
+    for name, x in (("pos", pos), ("acc", acc)):
+        if not (x.is_cuda and x.dtype == torch.float64 and x.is_contiguous()):
+            raise ValueError(f"{name} must be a contiguous CUDA tensor of float64")
+    s = stream if stream is not None else torch.cuda.current_stream(pos.device)
+    _lib.check(_lib.lib().galpy_cuda_accel_device(
+        comps.data_ptr(), ncomp, group.data_ptr() if group is not None else None, int(planar),
+        int(signature), _precision(precision), pos.data_ptr(), pos.shape[1], acc.data_ptr(),
+        s.cuda_stream))
+
+
 def energy_device(comps, ncomp, w, E, planar=False, layout="soa", group=None, stream=None):
     """E = v^2/2 + Phi(x) of device-resident rectangular states (torch).
 

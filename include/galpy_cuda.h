@@ -256,6 +256,17 @@ int galpy_cuda_adjoint_replay(const galpy_cuda_adjoint *a);
  * index of each parameter. */
 int galpy_cuda_adjoint_params(int planar, int npot, const int *pot_type, int *arg_index);
 
+/* Accelerations at n points (positions SoA [3][n] device memory, z ignored
+ * when planar) written to acc [3][n], with the integrators' own force code
+ * (galpy's evaluateRforces/zforces in Cartesian form; the acceleration that
+ * evalRectForce, integrateFullOrbit.c:1307, hands to the steppers).
+ * signature GALPY_CUDA_SIG_MW14 selects the compile-time MWPotential2014
+ * path of the integration kernels; precision as galpy_cuda_opts.
+ * Asynchronous on `stream`. */
+int galpy_cuda_accel_device(const void *comps, int ncomp, const int *group, int planar,
+                            int signature, int precision, const double *pos, long long n,
+                            double *acc, void *stream);
+
 /* Diagnostic: measured float64 fused-multiply-add throughput of the current
  * device in TFLOP/s (2 flops per FMA), the roofline denominator of the
  * integration kernels. */

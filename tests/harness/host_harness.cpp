@@ -351,3 +351,24 @@ extern "C" int harness_adj_backward_frozen(int planar, int nobj, const double* w
   }
   return np;
 }
+
+// Binade-table functions of the force path: kind 0 = (x)^(-alpha/2) from a
+// PowerSphericalwCutoff record, kind 1 = log1p(x) from an NFW record, kind 2
+// the single-precision log1p.
+extern "C" int harness_binade(int kind, double alpha, int n, const double* x, double* out)
+{
+  GpComp c;
+  if (kind == 0) {
+    const int pt = T_PSWC;
+    const double pa[3] = {1.0, alpha, 0.5};
+    if (compile_group(1, 1, &pt, pa, &c, nullptr)) return -1;
+    for (int i = 0; i < n; i++) out[i] = pswc_power(&c, x[i]);
+  } else {
+    const int pt = T_NFW;
+    const double pa[2] = {1.0, 2.0};
+    if (compile_group(1, 1, &pt, pa, &c, nullptr)) return -1;
+    for (int i = 0; i < n; i++)
+      out[i] = kind == 1 ? nfw_log1p(&c, x[i]) : (double)nfw_log1pf(&c, (float)x[i]);
+  }
+  return 0;
+}

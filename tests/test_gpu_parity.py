@@ -188,15 +188,21 @@ def test_potential_groups(oracle, mw14):
     dev = torch.device("cuda:0")
     out = torch.empty((6, 21, len(ics)), dtype=torch.float64, device=dev)
     e = torch.empty(len(ics), dtype=torch.int32, device=dev)
+    ns = torch.empty(len(ics), dtype=torch.int64, device=dev)
     gb.integrate_device(torch.tensor(comps, device=dev), n,
                         torch.tensor(cyl_to_rect(ics).T.copy(), device=dev),
-                        torch.tensor(t, device=dev), out, e, "dop853_cuda",
+                        torch.tensor(t, device=dev), out, e, "dop853_cuda", nsteps=ns,
                         group=torch.tensor(group, device=dev), rtol=1e-9, atol=1e-9)
     got = rect_to_cyl(out.cpu().numpy().transpose(2, 1, 0))
+    ns = ns.cpu().numpy()
     for g in range(ngroup):
         sel = group == g
-        ref, _, _, _ = oracle.integrate(ics[sel], t, pt, args[g], "dop853", rtol=1e-9, atol=1e-9)
-        assert cyl_diff(ref, got[sel]).max() < 1e-8
+        ref, _, nref, _ = oracle.integrate(ics[sel], t, pt, args[g], "dop853", rtol=1e-9,
+                                           atol=1e-9)
+        d = cyl_diff(ref, got[sel]).max(axis=(1, 2))
+        same = ns[sel] == nref  # an accept/reject flip at err ~ 1 changes the steps
+        assert same.mean() >= 0.9 and d[same].max() < 1e-8, (same.mean(), d.max())
+        assert d.max() < 1e-6
 
 
 def test_f32_force_variant(mw14):
@@ -296,3 +302,43 @@ def test_energy_kernel_vs_oracle(oracle, mw14):
     ref = oracle.energy_cyl(ics[:, None, :], pt, pa)[:, 0]
     # absolute on the scale of the energies (some orbits have E close to 0)
     assert (np.abs(E.cpu().numpy() - ref) / np.abs(ref).max()).max() < 1e-14
+
+
+@pytest.mark.parametrize("name", ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"])
+@pytest.mark.parametrize("planar", [False, True])
+def test_device_accelerations(golden, harness, name, planar):
+    """The kernels' force code on the device (branch-free FP64 helpers:
+    hardware-seeded 1/sqrt and 1/x with a Newton correction, binade tables
+    for the bulge power and the NFW log1p) against the same code built for
+    the host with libm's 1/sqrt and division: a few ulp of the inputs, which
+    the NFW force's cancellation at r << a amplifies (by 2a/r; 1e-12 is the
+    tolerance of the host build against the reference's formulas too)."""
+    import torch
+
+    pt, pa = golden[f"{name}_type"], np.array(golden[f"{name}_args"], float)
+    if planar and int(pt[0]) == 15:
+        pa = pa[:3]
+    if planar and name == "mw14":
+        pt, pa = golden["mw14_planar_type"], np.array(golden["mw14_planar_args"], float)
+    rng = np.random.default_rng(3)
+    n = 4096
+    R = np.exp(rng.uniform(np.log(0.01), np.log(50.0), n))
+    phi = rng.uniform(0, 2 * np.pi, n)
+    x, y, z = R * np.cos(phi), R * np.sin(phi), rng.normal(0, 0.3, n)
+    acc_h, _, acc32_h = harness.forces(x, y, z, pt, pa, planar=planar)
+    comps, nc = gb.compile_potential((pt, pa), planar=planar)
+    dev = torch.device("cuda:0")
+    pos = torch.tensor(np.stack([x, y, z]), device=dev)
+    for sig in {0, gb.signature((pt, pa), planar=planar)}:
+        for prec, ref, tol in (("fp64", acc_h, 1e-12), ("f32force", acc32_h, 1e-3)):
+            acc = torch.empty((3, n), dtype=torch.float64, device=dev)
+            gb.accel_device(torch.tensor(comps, device=dev), nc, pos, acc, planar=planar,
+                            signature=sig, precision=prec)
+            got = acc.cpu().numpy().T
+            if planar:
+                got, ref_ = got[:, :2], ref[:, :2]
+            else:
+                ref_ = ref
+            scale = np.linalg.norm(ref_, axis=1)
+            err = np.abs(got - ref_).max(axis=1) / scale
+            assert err.max() < tol, (sig, prec, err.max())

@@ -171,3 +171,36 @@ def test_single_output_row(harness, mw14):
     w = cyl_to_rect(seeded_ics(2, 15))
     out, err, ns = harness.integrate(w, np.array([0.0]), pt, pa, "dop853")
     assert np.array_equal(out[:, 0], w) and not err.any()
+
+
+def test_binade_tables_match_mpmath(harness):
+    """The FP64 force path's branch-free (r^2)^(-alpha/2) and log1p (binade
+    tables built on the host) against 120-bit references."""
+    import ctypes
+
+    mpmath = pytest.importorskip("mpmath")
+    mpmath.mp.prec = 120
+    dp = ctypes.POINTER(ctypes.c_double)
+    rng = np.random.default_rng(0)
+    x = np.exp(rng.uniform(np.log(1e-10), np.log(1e8), 4000))
+    for alpha in (1.8, 1.0, 2.5, 0.3):
+        out = np.zeros_like(x)
+        assert harness.lib.harness_binade(0, ctypes.c_double(alpha), len(x),
+                                          x.ctypes.data_as(dp), out.ctypes.data_as(dp)) == 0
+        ref = np.array([float(mpmath.mpf(v) ** (-alpha / 2)) for v in x])
+        assert np.abs(out / ref - 1).max() < 3 * 2.3e-16
+    xs = np.concatenate([np.exp(rng.uniform(np.log(1e-12), np.log(1e6), 4000)),
+                         np.linspace(0, 2, 201)])
+    out = np.zeros_like(xs)
+    assert harness.lib.harness_binade(1, ctypes.c_double(0), len(xs), xs.ctypes.data_as(dp),
+                                      out.ctypes.data_as(dp)) == 0
+    ref = np.array([float(mpmath.log1p(mpmath.mpf(v))) for v in xs])
+    pos = ref > 0
+    assert np.abs(out[pos] / ref[pos] - 1).max() < 3 * 2.3e-16
+    assert out[xs == 0].tolist() == [0.0]
+    xf = xs.astype(np.float32).astype(np.float64)
+    assert harness.lib.harness_binade(2, ctypes.c_double(0), len(xf), xf.ctypes.data_as(dp),
+                                      out.ctypes.data_as(dp)) == 0
+    ref = np.array([float(mpmath.log1p(mpmath.mpf(v))) for v in xf])
+    pos = ref > 0
+    assert np.abs(out[pos] / ref[pos] - 1).max() < 4 * 6e-8
