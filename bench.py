@@ -243,9 +243,11 @@ def main():
     ap.add_argument("--grad-only", action="store_true",
                     help="run only the differentiation leg (with --grad-orbits orbits)")
     ap.add_argument("--grad-orbits", type=int, default=65536)
-    ap.add_argument("--case", default="batching", choices=["batching", "uniform"],
+    ap.add_argument("--case", default="batching", choices=["batching", "uniform", "longest"],
                     help="uniform: R ~ U(0.5, 2), shared t in [0, 50] (101 snapshots) "
-                         "(a throughput-bound case for profiling the same kernel)")
+                         "(a throughput-bound case for profiling the same kernel); longest: "
+                         "only the --orbits longest orbits of the batching workload (by "
+                         "t_end / r0), the tail that bounds its step time")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -289,6 +291,11 @@ def main():
     if args.case == "uniform":
         ics, _ = precision_workload(args.orbits, seed=shard_seed(1, rank))
         t = np.repeat(np.linspace(0.0, 50.0, NT)[None, :], len(ics), axis=0)
+    elif args.case == "longest":
+        ics, t = workload(N_ORBITS, seed=shard_seed(1, rank))
+        r0 = np.sqrt(ics[:, 0] ** 2 + ics[:, 3] ** 2)
+        keep = np.argsort(-t[:, -1] / r0)[:args.orbits]
+        ics, t = ics[keep], t[keep]
     else:
         ics, t = workload(args.orbits, seed=shard_seed(1, rank))
     n = len(ics)

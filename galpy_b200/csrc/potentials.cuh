@@ -164,13 +164,65 @@ template <> struct Num<float> {
   GPC_HD static float rsq(float x) { return gpc::rsqf(x); }
 };
 
-// gamma*(a, u) from the component's table, u in [0, U): on each interval
-// the degree-11 Chebyshev interpolant is stored in the power basis of the
-// interval's local variable x in [-1, 1] and evaluated by Horner's rule (11
-// dependent FMAs, half the dependency chain of the Clenshaw recurrence; both
-// stay within ~1 ulp here, tests/test_harness.py checks against mpmath).
 // The record holding a component's tables.
 GPC_HD GPC_FI const GpComp* tables(const GpComp* cp) { return cp + ldg(&cp->tab); }
+
+// Interval index of s in [0, kChebN] without float<->int conversions (their
+// latency sat on the force's critical path): adding 1.5 * 2^52 (resp.
+// 1.5 * 2^23 in single precision) to s - 1/2 rounds it to an integer held in
+// the low mantissa bits; at exact ties either neighbouring interval is
+// valid.  Returns the index (clamped to the last interval) and sets the
+// interval's start as a floating-point number.
+template <typename T>
+GPC_HD GPC_FI int interval_of(T s, T& start);
+template <>
+GPC_HD GPC_FI int interval_of<double>(double s, double& start)
+{
+  constexpr double M = 6755399441055744.0;  // 1.5 * 2^52
+  const double r = (s - 0.5) + M;
+  int k = (int)(bits_of(r) & 63);
+  k = k < kChebN - 1 ? k : kChebN - 1;
+  start = fmin(r - M, (double)(kChebN - 1));
+  return k;
+}
+template <>
+GPC_HD GPC_FI int interval_of<float>(float s, float& start)
+{
+  constexpr float M = 12582912.0f;  // 1.5 * 2^23
+  const float r = (s - 0.5f) + M;
+  int b;
+#if defined(__CUDA_ARCH__)
+  b = __float_as_int(r);
+#else
+  memcpy(&b, &r, sizeof(b));
+#endif
+  int k = b & 63;
+  k = k < kChebN - 1 ? k : kChebN - 1;
+  start = fminf(r - M, (float)(kChebN - 1));
+  return k;
+}
+
+// Degree-11 polynomial sum_k c[k] x^k, |x| <= 1, by Estrin's scheme: the
+// twelve coefficients pair up as (c0 + c1 x) + x^2 (c2 + c3 x) + ... and the
+// pairs combine with x^2, x^4, x^8, so the dependency chain is 5 operations
+// deep instead of Horner's 11 (FP64 operations have long latencies and the
+// force is one dependent chain per step).  The coefficients of the tables
+// decay, and the result stays within a few ulp (tests/test_harness.py).
+template <typename T>
+GPC_HD GPC_FI T poly12(const T* __restrict__ c, T x)
+{
+  const T x2 = x * x, x4 = x2 * x2, x8 = x4 * x4;
+  const T p01 = fma(ldg(c + 1), x, ldg(c + 0)), p23 = fma(ldg(c + 3), x, ldg(c + 2));
+  const T p45 = fma(ldg(c + 5), x, ldg(c + 4)), p67 = fma(ldg(c + 7), x, ldg(c + 6));
+  const T p89 = fma(ldg(c + 9), x, ldg(c + 8)), pab = fma(ldg(c + 11), x, ldg(c + 10));
+  const T q0 = fma(p23, x2, p01), q1 = fma(p67, x2, p45), q2 = fma(pab, x2, p89);
+  return fma(q2, x8, fma(q1, x4, q0));
+}
+
+// gamma*(a, u) from the component's table, u in [0, U): on each interval
+// the degree-11 Chebyshev interpolant is stored in the power basis of the
+// interval's local variable x in [-1, 1] (tests/test_harness.py checks the
+// values against mpmath).
 
 // tp: the component's table record (tables(cp); cp itself in a launch with a
 // single potential, where every record holds its own tables).
@@ -178,19 +230,16 @@ template <typename T>
 GPC_HD GPC_FI T gamma_star(const GpComp* __restrict__ tp, T u, T scale)
 {
   const T s = u * scale;
-  int k = (int)s;
-  k = k < kChebN - 1 ? k : kChebN - 1;
-  const T x = T(2) * (s - T(k)) - T(1);
+  T start;
+  const int k = interval_of<T>(s, start);
+  const T x = T(2) * (s - start) - T(1);
   // the FP32 path reads the single-precision copy (no conversions)
   const T* c;
   if constexpr (sizeof(T) == sizeof(double))
     c = tp->cheb[k];
   else
     c = tp->chebf[k];
-  T p = ldg(c + kChebC - 1);
-#pragma unroll
-  for (int j = kChebC - 2; j >= 0; j--) p = p * x + ldg(c + j);
-  return p;
+  return poly12<T>(c, x);
 }
 
 // x = m 2^e (x > 0 normal): the binade-table polynomial at m, e + 1024 and
@@ -209,19 +258,16 @@ GPC_HD GPC_FI Binade binade(const GpComp* __restrict__ tp, double x)
   r.ebias = (int)((b >> 52) & 0x7ff) + 1;
   const int j = (int)((b >> 49) & 7);
   const double m = double_of((b & 0x000fffffffffffffLL) | 0x3ff0000000000000LL);
-  r.t = 16.0 * m - (double)(17 + 2 * j);  // exact
-  r.m1 = m - 1.0;                          // exact
+  // m with its top three fraction bits cleared: 1 + (m - (1 + j/8)), so the
+  // local variable 16 (m - 1 - j/8) - 1 needs no integer conversion
+  const double mlow = double_of((b & 0x0001ffffffffffffLL) | 0x3ff0000000000000LL);
+  r.t = 16.0 * mlow - 17.0;  // exact
+  r.m1 = m - 1.0;            // exact
   r.row = tp->bin[j];
   return r;
 }
 
-GPC_HD GPC_FI double horner12(const double* c, double t)
-{
-  double p = ldg(c + kChebC - 1);
-#pragma unroll
-  for (int k = kChebC - 2; k >= 0; k--) p = fma(p, t, ldg(c + k));
-  return p;
-}
+GPC_HD GPC_FI double horner12(const double* c, double t) { return poly12<double>(c, t); }
 
 // (r^2)^(-alpha/2) from the PowerSphericalwCutoff component's tables
 GPC_HD GPC_FI double pswc_power(const GpComp* __restrict__ tp, double r2)
@@ -244,37 +290,43 @@ GPC_HD GPC_FI double nfw_log1p(const GpComp* __restrict__ tp, double x)
   const double u = 1.0 + x;
   const double corr = (x - (u - 1.0)) * rcp_nr(u);
   const Binade q = binade(tp, u);
-  const double e = (double)(q.ebias - 1024);
+  // e as a double without a conversion: 2^52 + ebias, minus 2^52 + 1024
+  const double e = double_of(0x4330000000000000LL | (long long)q.ebias) - 4503599627371520.0;
   return fma(e, ln2_hi, fma(q.m1, horner12(q.row, q.t), fma(e, ln2_lo, corr)));
 }
 
 // The same log1p in single precision from the float copy of the table.
+GPC_HD GPC_FI float f32_of_bits(int b)
+{
+#if defined(__CUDA_ARCH__)
+  return __int_as_float(b);
+#else
+  float x;
+  memcpy(&x, &b, sizeof(x));
+  return x;
+#endif
+}
+
 GPC_HD GPC_FI float nfw_log1pf(const GpComp* __restrict__ tp, float x)
 {
   const float u = 1.0f + x;
-#if defined(__CUDA_ARCH__)
-  const int b = __float_as_int(u);
-  const float corr = (x - (u - 1.0f)) * __frcp_rn(u);
-#else
   int b;
-  memcpy(&b, &u, sizeof(b));
-  const float corr = (x - (u - 1.0f)) / u;
-#endif
-  const int e = ((b >> 23) & 0xff) - 127;
-  const int j = (b >> 20) & 7;
-  const int mb = (b & 0x7fffff) | 0x3f800000;
-  float m;
 #if defined(__CUDA_ARCH__)
-  m = __int_as_float(mb);
+  b = __float_as_int(u);
 #else
-  memcpy(&m, &mb, sizeof(m));
+  memcpy(&b, &u, sizeof(b));
 #endif
-  const float t = 16.0f * m - (float)(17 + 2 * j);
-  const float* c = tp->binf[j];
-  float p = ldg(c + kChebC - 1);
-#pragma unroll
-  for (int k = kChebC - 2; k >= 0; k--) p = fmaf(p, t, ldg(c + k));
-  return fmaf((float)e, 0.69314718f, fmaf(m - 1.0f, p, corr));
+  const int eb = (b >> 23) & 0xff;
+  // the rounding correction of u divided by u to within a factor 2
+  // (2^-e): it is below single-precision resolution of the result already
+  const float corr = (x - (u - 1.0f)) * f32_of_bits((254 - eb) << 23);
+  const int j = (b >> 20) & 7;
+  const float m = f32_of_bits((b & 0x7fffff) | 0x3f800000);
+  const float mlow = f32_of_bits((b & 0xfffff) | 0x3f800000);  // top 3 fraction bits cleared
+  const float t = 16.0f * mlow - 17.0f;
+  const float e = f32_of_bits(0x4b000000 | eb) - 8388735.0f;  // (2^23 + eb) - (2^23 + 127)
+  const float p = poly12<float>(tp->binf[j], t);
+  return fmaf(e, 0.69314718f, fmaf(m - 1.0f, p, corr));
 }
 
 // ------------------------------------------------------------- forces ---
@@ -315,12 +367,12 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
             sc[2] * pswc_power(tp, r2) * gamma_star<double>(tp, fmin(u, sc[5]), sc[6]);
         const double outer = sc[4] * (ir * ir * ir);
         f = -amp * (u < sc[5] ? inner : outer);
-      } else if (u < T(sc[5])) {
+      } else {  // single precision: hardware log2/exp2 for the power, same select
         const T pw = Num<T>::ex(T(sc[3]) * Num<T>::lg(r2));  // (r^2)^(-alpha/2)
-        f = -amp * T(sc[2]) * pw * gamma_star<T>(tp, u, T(sc[6]));
-      } else {
         const T ir = Num<T>::rsq(r2);
-        f = -amp * T(sc[4]) * (ir * ir * ir);
+        const T inner = T(sc[2]) * pw * gamma_star<T>(tp, u < T(sc[5]) ? u : T(sc[5]), T(sc[6]));
+        const T outer = T(sc[4]) * (ir * ir * ir);
+        f = -amp * (u < T(sc[5]) ? inner : outer);
       }
       gR += f;
       gz += f;
