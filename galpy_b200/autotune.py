@@ -11,8 +11,12 @@ how ragged the step counts are):
   the block size);
 * ``variant`` -- register budget: 0 = compiler default (up to 255 registers
   a thread), 1 = capped so that more blocks are resident per SM;
-* ``schedule`` -- work-queue order: in order, or longest first by the
-  estimated cost |t_end - t_0| * orbital frequency;
+* ``schedule`` -- not tuned: always longest first by the estimated cost
+  |t_end - t_0| * orbital frequency.  Its pre-pass costs about a millisecond,
+  and what it prevents -- the longest orbits starting late and running alone
+  at the end -- only shows on the whole batch: a subsample has shorter
+  longest orbits and fewer orbits per thread, and once let a noisy in-order
+  win on the sample cost the full batch 1.5x;
 * ``threads_per_orbit`` -- 1 (the only form the kernels implement: every
   lane owns a whole orbit, so that each lane's force evaluation is the
   warp's single force call site).
@@ -69,9 +73,8 @@ def candidates(int_method):
     blocks = (128,) if code == 6 else (64, 128)
     for block in blocks:
         for variant in (0, 1):
-            for schedule in ("longest_first", "in_order"):
-                shapes.append({"block_size": block, "variant": variant, "schedule": schedule,
-                               "threads_per_orbit": 1})
+            shapes.append({"block_size": block, "variant": variant,
+                           "schedule": "longest_first", "threads_per_orbit": 1})
     return shapes
 
 
