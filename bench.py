@@ -608,8 +608,9 @@ def e2e(gb, ics, t, pt, pa, K, pg, dev, steps_total):
     pti = np.ascontiguousarray(pt, np.int32)
     pad = np.ascontiguousarray(pa, np.float64)
     r, a = float(np.log(RTOL)), float(np.log(ATOL))
-    opts = _lib.make_opts(device=dev.index)
-    times = []
+    kernel_ms = ctypes.c_double(0.0)
+    opts = _lib.make_opts(device=dev.index, elapsed=kernel_ms)
+    times, kernel = [], []
     for k in range(K + 1):
         yo_pin[:] = ics  # galpy's call overwrites yo with rectangular coordinates
         if pg:
@@ -624,8 +625,10 @@ def e2e(gb, ics, t, pt, pa, K, pg, dev, steps_total):
         _lib.check(rc)
         if k > 0:  # first call is a warm-up
             times.append(el)
+            kernel.append(kernel_ms.value * 1e-3)
     (el,), _ = over_ranks([max(times)], [], pg, dev)
     return {"value": steps_total / el, "unit": "orbit-steps/s", "seconds_per_step": el,
+            "kernel_seconds_per_step": max(kernel),
             "h2d_bytes_per_step": int(yo_pin.nbytes + t_pin.nbytes),
             "d2h_bytes_per_step": int(res_pin.nbytes + err.nbytes),
             "api": "integrateFullOrbit_cuda (galpy layout, pinned host buffers)"}

@@ -452,12 +452,35 @@ struct DevBuf {
   }
 };
 
+// The blocking entry points allocate their device buffers stream-ordered
+// from the device's default memory pool.  With the pool's default release
+// threshold (0) every call would hand gigabytes back to the driver at its
+// final synchronisation and map them again on the next call; keeping them
+// in the pool (this process's pool only) makes repeated calls allocation-free
+// after the first.
+static void keep_pool_memory()
+{
+  static std::mutex m;
+  static bool done[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+  std::lock_guard<std::mutex> lock(m);
+  if (done[dev]) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    unsigned long long keep = ~0ULL;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  done[dev] = true;
+}
+
 static int select_device(const galpy_cuda_opts* o)
 {
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1)
     return set_error(GALPY_CUDA_ERR_NODEVICE, "no CUDA device visible");
   if (o && o->device >= 0) GPC_CUDA_TRY(cudaSetDevice(o->device));
+  keep_pool_memory();
   return GALPY_CUDA_OK;
 }
 
