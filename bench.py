@@ -378,7 +378,11 @@ def main():
                          "exceed the 126 MB L2"},
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
-                     "traffic": None,
+                     # DRAM read + write of a 65,536-orbit capture of this kernel
+                     # (2.239 GB), scaled by orbits x snapshots to this launch
+                     "traffic": 2.238743e9 * n / 65536,
+                     "traffic_source": "ncu capture of 65,536 orbits (uniform case), scaled "
+                                       "by orbits x snapshots",
                      "kernel": "orbit_kernel<Dop853Machine<3,false>,3,0,false>",
                      "flops_per_unit": F_STEP_DOP853,
                      "peak_source": "measured in-process: float64 FMA-chain kernel "
