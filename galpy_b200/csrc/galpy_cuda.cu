@@ -390,6 +390,12 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
   const size_t smem = (size_t)ki.slot_doubles * sizeof(double) * block;
   if (smem > 48 * 1024)
     GPC_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // slot-store machines: all of the unified L1/shared array as shared memory
+  // for the register-capped variant, so that 3 blocks' slot stores (3 x 66 KB
+  // for 3D DOP853) fit per SM; the hot potential tables are a few KB
+  if (smem > 0 && L->variant == 1)
+    GPC_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      (int)cudaSharedmemCarveoutMaxShared));
   int per_sm = 0;
   GPC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem));
   if (per_sm < 1) per_sm = 1;

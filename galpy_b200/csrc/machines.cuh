@@ -643,15 +643,15 @@ struct Dop853Machine : OrbitCommon {
   };
   enum { K1 = 0, K2 = 1, K3 = 2, K4 = 3, K5 = 4, K6 = 5, K7 = 6, K8 = 7, K9 = 8, K10 = 9,
          S14 = 10, S15 = 11 };
-  // All stage slots live in a per-thread slot store (shared memory in the
-  // kernel, strided by the block size: bank-conflict free); only y0 stays in
-  // registers.
-  static constexpr int kSlots = 12;
+  // Stage slots K2..K10, S14, S15 live in a per-thread slot store (shared
+  // memory in the kernel, strided by the block size: bank-conflict free); y0
+  // and K1 -- the first term of every stage input -- stay in registers.
+  static constexpr int kSlots = 11;
   static constexpr int kSlotDoubles = kSlots * N;
-  double y0[N];
-  double* ks;  // slot store: ks[(slot * N + i) * kSlotStride]
+  double y0[N], k1[N];
+  double* ks;  // slot store: slot s >= 1 at ks[((s - 1) * N + i) * kSlotStride]
   GPC_HD GPC_FI void bind(double* base) { ks = base; }
-  GPC_HD GPC_FI double& K(int s, int i) const { return ks[(s * N + i) * kSlotStride]; }
+  GPC_HD GPC_FI double& K(int s, int i) const { return ks[((s - 1) * N + i) * kSlotStride]; }
   double h, hnew, hmax, pos_neg, facold, rtol, atol;
   double t_current, t_old, t_old_older, dnf;
   int stage;
@@ -719,7 +719,7 @@ struct Dop853Machine : OrbitCommon {
     }
     if (stage == ST_INIT2) {  // explicit Euler step (leung_dop853.c:310)
 #pragma unroll
-      for (int i = 0; i < N; i++) y[i] = y0[i] + h * K(K1, i);
+      for (int i = 0; i < N; i++) y[i] = y0[i] + h * k1[i];
       return;
     }
     if (stage == ST_FSAL) {  // the new state
@@ -730,11 +730,10 @@ struct Dop853Machine : OrbitCommon {
     const DopStageTable& tb = dop_table();
     const int n = tb.nterm[stage];
     double acc[N];
-    {
-      const int s0 = tb.slot[stage][0];
+    {  // the first term of every stage input is K1 (table slot 0)
       const double c0 = tb.coef[stage][0];
 #pragma unroll
-      for (int i = 0; i < N; i++) acc[i] = c0 * K(s0, i);
+      for (int i = 0; i < N; i++) acc[i] = c0 * k1[i];
     }
     for (int tt = 1; tt < n; tt++) {
       const int s = tb.slot[stage][tt];
@@ -771,7 +770,7 @@ struct Dop853Machine : OrbitCommon {
       dnf = 0.0;
 #pragma unroll
       for (int i = 0; i < N; i++) {
-        K(K1, i) = d[i];
+        k1[i] = d[i];
         const double sk = atol + rtol * fabs(y0[i]);
         double sqr = d[i] / sk;
         dnf += sqr * sqr;
@@ -787,7 +786,7 @@ struct Dop853Machine : OrbitCommon {
 #pragma unroll
       for (int i = 0; i < N; i++) {
         const double sk = atol + rtol * fabs(y0[i]);
-        const double sqr = (d[i] - K(K1, i)) / sk;
+        const double sqr = (d[i] - k1[i]) / sk;
         der2 += sqr * sqr;
       }
       der2 = sqrt(der2) / h;
@@ -829,7 +828,7 @@ struct Dop853Machine : OrbitCommon {
       double v[N];
 #pragma unroll
       for (int i = 0; i < N; i++) {
-        const double k1 = K(K1, i), k2 = K(K2, i), k3 = K(K3, i), k4 = K(K4, i);
+        const double k1 = this->k1[i], k2 = K(K2, i), k3 = K(K3, i), k4 = K(K4, i);
         const double k6 = K(K6, i), k7 = K(K7, i), k8 = K(K8, i), k9 = K(K9, i);
         const double k10 = K(K10, i), s14 = K(S14, i), s15 = K(S15, i);
         const double rc1 = y0[i];
@@ -868,7 +867,7 @@ struct Dop853Machine : OrbitCommon {
     double e = 0.0, e2 = 0.0;
 #pragma unroll
     for (int i = 0; i < N; i++) {
-      const double k1 = K(K1, i), k2 = K(K2, i), k3 = K(K3, i), k6 = K(K6, i), k7 = K(K7, i);
+      const double k1 = this->k1[i], k2 = K(K2, i), k3 = K(K3, i), k6 = K(K6, i), k7 = K(K7, i);
       const double k8 = K(K8, i), k9 = K(K9, i), k10 = K(K10, i);
       const double k4 =
           b1 * k1 + b6 * k6 + b7 * k7 + b8 * k8 + b9 * k9 + b10 * k10 + b11 * k2 + b12 * k3;
@@ -919,7 +918,7 @@ struct Dop853Machine : OrbitCommon {
   {
 #pragma unroll
     for (int i = 0; i < N; i++) {
-      K(K1, i) = K(K4, i);
+      k1[i] = K(K4, i);
       y0[i] = K(K5, i);
     }
     hnew = (fabs(hnew) > fabs(hmax)) ? pos_neg * hmax : hnew;
