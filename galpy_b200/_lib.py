@@ -94,6 +94,8 @@ class GalpyCudaLaunch(ctypes.Structure):
         ("schedule", ctypes.c_int),
         ("variant", ctypes.c_int),
         ("comps_host", ctypes.c_void_p),
+        ("size_ext", ctypes.c_int),
+        ("tail_sms", ctypes.c_int),
     ]
 
 

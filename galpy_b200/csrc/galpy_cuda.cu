@@ -84,6 +84,12 @@ struct KArgs {
   unsigned long long* done_count;
   const int* order;  // work-queue order (longest first), or NULL
   int variational_nv; // values per input row of variational runs (0 otherwise)
+  // the first tail_len queue entries (the longest orbits) go to one warp on
+  // each of the SMs 0..tail_sms-1, which run nothing else (0: no reservation)
+  long long tail_len;
+  int tail_sms;
+  unsigned long long* tail_counter;
+  unsigned* sm_claim;
   // scalar parameters of the (single) potential, read from the constant bank
   // by the kernels whose POT takes them directly
   double scal[kMaxComp * kScalarStride];
@@ -111,6 +117,14 @@ __device__ __forceinline__ void load_state(const KArgs& A, long long i, double* 
   }
 }
 
+// Whether any reserved SM has taken its tail warp.
+__device__ __forceinline__ bool tail_claimed(const KArgs& A)
+{
+  for (int k = 0; k < A.tail_sms; k++)
+    if (*reinterpret_cast<const volatile unsigned*>(&A.sm_claim[k])) return true;
+  return false;
+}
+
 // MINB: minimum resident blocks per SM requested from the register
 // allocator (1 = no cap; larger values trade registers for occupancy).
 template <class M, int D, int PREC, bool VAR, class POT, int MINB>
@@ -119,6 +133,23 @@ __global__ void __launch_bounds__(128, MINB) orbit_kernel(const __grid_constant_
   constexpr bool CYL_OK = !VAR;
   using Rows = DevRows<M::NV, D, CYL_OK>;
   extern __shared__ double slot_store[];
+  // Reserved SMs for the longest orbits: the first block resident on each of
+  // SMs 0..tail_sms-1 keeps one warp, which takes the tail queue (then helps
+  // with the main queue); any other block there leaves, so those orbits do
+  // not share their SM with the bulk of the batch.  Main workers drain tail
+  // entries left unclaimed (no block landed on a reserved SM).
+  __shared__ int role;  // 0 main queue, 1 tail warp, 2 leave
+  if (threadIdx.x == 0) {
+    role = 0;
+    if (A.tail_len > 0) {
+      unsigned smid;
+      asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+      if (smid < (unsigned)A.tail_sms) role = atomicExch(&A.sm_claim[smid], 1u) == 0u ? 1 : 2;
+    }
+  }
+  __syncthreads();
+  int my_role = role;
+  if (my_role == 2 || (my_role == 1 && threadIdx.x >= 32)) return;
   M m;
   m.bind(slot_store + threadIdx.x);
   long long i = 0;
@@ -128,9 +159,28 @@ __global__ void __launch_bounds__(128, MINB) orbit_kernel(const __grid_constant_
   int slot = 0;
   for (;;) {
     if (!active) {
-      i = (long long)atomicAdd(A.counter, 1ULL);
-      if (i >= A.nobj) break;
-      if (A.order) i = A.order[i];
+      long long q = -1;
+      if (my_role == 1) {
+        q = (long long)atomicAdd(A.tail_counter, 1ULL);
+        if (q >= A.tail_len) {
+          q = -1;
+          my_role = 0;
+        }
+      }
+      if (q < 0 && A.tail_len > 0 && !tail_claimed(A)) {
+        // no reserved SM hosts a tail warp: the longest orbits go first here
+        q = (long long)atomicAdd(A.tail_counter, 1ULL);
+        if (q >= A.tail_len) q = -1;
+      }
+      if (q < 0) {
+        q = (long long)atomicAdd(A.counter, 1ULL) + A.tail_len;
+        if (q >= A.nobj) {
+          if (A.tail_len == 0) break;
+          q = (long long)atomicAdd(A.tail_counter, 1ULL);
+          if (q >= A.tail_len) break;
+        }
+      }
+      i = A.order ? A.order[q] : q;
       if (aborting) {
         A.err[i] = E_ABORT;
         write_nan_rows<M::NV, D, CYL_OK>(A.out, i, 0);
@@ -292,11 +342,14 @@ static bool method_supported(int m)
   return m == M_LEAPFROG || m == M_RK4 || m == M_SYMPLEC4 || m == M_DOP853;
 }
 
-struct Scratch {  // device scratch of one launch (64 bytes)
+constexpr int kMaxTailSms = 16;
+struct Scratch {  // device scratch of one launch (128 bytes)
   unsigned long long counter;
   unsigned long long done_count;
+  unsigned long long tail_counter;
   int abort_flag;
-  int pad[11];
+  unsigned sm_claim[kMaxTailSms];  // first block resident on each reserved SM
+  int pad[5];
 };
 
 // Launch on `stream`.  scratch: device Scratch (counter zeroed here).
@@ -343,6 +396,8 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
   A.atol = L->atol;
   A.max_attempts = L->max_attempts;
   A.counter = &scratch->counter;
+  A.tail_counter = &scratch->tail_counter;
+  A.sm_claim = scratch->sm_claim;
   A.abort_flag = L->abort_flag ? L->abort_flag : &scratch->abort_flag;
   A.done_count = progress ? &scratch->done_count : nullptr;
   A.variational_nv = L->variational ? (L->planar ? 8 : 12) : 0;
@@ -403,6 +458,16 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
   const long long need = (L->nobj + block - 1) / block;
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
+  // reserve SMs for the longest orbits of a large longest-first batch (one
+  // warp each); worthwhile only when the batch is many waves deep
+  int tail_sms = L->size_ext >= 1 && L->tail_sms >= 0 ? L->tail_sms : 2;
+  if (tail_sms > kMaxTailSms) tail_sms = kMaxTailSms;
+  if (tail_sms > nsm / 16) tail_sms = nsm / 16;
+  if (A.order && tail_sms > 0 && L->grid_size <= 0 &&
+      L->nobj >= 8LL * grid * block && grid == (long long)nsm * per_sm) {
+    A.tail_sms = tail_sms;
+    A.tail_len = 32LL * tail_sms;
+  }
   fn<<<(unsigned)grid, block, smem, stream>>>(A);
   cudaError_t le = cudaGetLastError();
   if (sched) cudaFreeAsync(sched, stream);

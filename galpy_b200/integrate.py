@@ -222,7 +222,7 @@ def integrate_device(comps, ncomp, w0, t, out, err, int_method, planar=False, va
                      nsteps=None, group=None, in_layout="soa", out_layout="soa_rect",
                      out_row0=0, dt=None, rtol=None, atol=None, precision="fp64",
                      max_attempts=0, stream=None, block_size=0, grid_size=0, signature=0,
-                     schedule="longest_first", variant=0, comps_host=None):
+                     schedule="longest_first", variant=0, comps_host=None, tail_sms=-1):
     """Asynchronous integration of device-resident torch tensors.
 
     comps: uint8 CUDA tensor of compiled records (compile_potential); w0
@@ -277,6 +277,9 @@ def integrate_device(comps, ncomp, w0, t, out, err, int_method, planar=False, va
     # host copy of the records (numpy uint8 from compile_potential): lets a
     # single-potential launch pass its scalars as kernel parameters
     L.comps_host = comps_host.ctypes.data if comps_host is not None else None
+    # SMs reserved for the longest orbits of a large longest-first batch
+    L.size_ext = 1
+    L.tail_sms = int(tail_sms)
     _lib.check(_lib.lib().galpy_cuda_integrate_device(ctypes.byref(L)))
 
 

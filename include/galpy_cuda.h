@@ -153,6 +153,9 @@ typedef struct galpy_cuda_launch {
   int variant;              /* register budget: 0 compiler default, 1 capped for occupancy */
   const void *comps_host;   /* optional host copy of `comps` (ncomp records, one group):
                                its scalars are passed as kernel parameters */
+  int size_ext;             /* 1 if the fields below are set (0: defaults) */
+  int tail_sms;             /* SMs reserved for the longest orbits of a large longest-first
+                               batch, one warp each (-1: default 2, 0: none) */
 } galpy_cuda_launch;
 
 int galpy_cuda_integrate_device(const galpy_cuda_launch *launch);
