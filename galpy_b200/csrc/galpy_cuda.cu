@@ -459,8 +459,10 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
   if (grid > need) grid = need;
   if (grid < 1) grid = 1;
   // reserve SMs for the longest orbits of a large longest-first batch (one
-  // warp each); worthwhile only when the batch is many waves deep
-  int tail_sms = L->size_ext >= 1 && L->tail_sms >= 0 ? L->tail_sms : 2;
+  // warp each); worthwhile only when the batch is many waves deep.  On the
+  // batching workload one SM was best (1,035 ms per step; 2: 1,041, 4:
+  // 1,052, 8: 1,072, none: 1,167).
+  int tail_sms = L->size_ext >= 1 && L->tail_sms >= 0 ? L->tail_sms : 1;
   if (tail_sms > kMaxTailSms) tail_sms = kMaxTailSms;
   if (tail_sms > nsm / 16) tail_sms = nsm / 16;
   if (A.order && tail_sms > 0 && L->grid_size <= 0 &&

@@ -155,7 +155,7 @@ typedef struct galpy_cuda_launch {
                                its scalars are passed as kernel parameters */
   int size_ext;             /* 1 if the fields below are set (0: defaults) */
   int tail_sms;             /* SMs reserved for the longest orbits of a large longest-first
-                               batch, one warp each (-1: default 2, 0: none) */
+                               batch, one warp each (-1: default 1, 0: none) */
 } galpy_cuda_launch;
 
 int galpy_cuda_integrate_device(const galpy_cuda_launch *launch);
