@@ -84,9 +84,30 @@ def _struct(planar, nobj, t0, tend, rtol, atol, comps, ncomp, group, signature, 
     return a
 
 
+def _cost_order(comps, ncomp, w0, planar, signature, group, stream):
+    """Orbits by decreasing estimated cost, the local orbital frequency
+    sqrt(|a . x|) / |x| at the initial point (the step count of an adaptive
+    integration over a common interval grows with it), so that the lanes of
+    a warp integrate orbits of similar length."""
+    import torch
+
+    from .integrate import accel_device
+
+    nv, n = w0.shape
+    d = nv // 2
+    pos = torch.zeros((3, n), dtype=torch.float64, device=w0.device)
+    pos[:d] = w0[:d]
+    acc = torch.empty_like(pos)
+    accel_device(comps, ncomp, pos, acc, planar=planar, signature=signature, group=group,
+                 stream=stream)
+    r2 = (pos * pos).sum(0)
+    cost = torch.sqrt(torch.abs((acc * pos).sum(0))) / torch.sqrt(r2)
+    return torch.argsort(cost, descending=True).to(torch.int32)
+
+
 def adjoint_forward(comps, ncomp, w0, tend, t0=0.0, rtol=None, atol=None, planar=False,
                     signature=0, group=None, ckpt_cap=None, record_steps=0, max_attempts=0,
-                    stream=None, block_size=0):
+                    stream=None, block_size=0, sort=True):
     """Forward pass on device-resident tensors.
 
     comps: uint8 CUDA tensor of compiled records (compile_potential); w0:
@@ -95,7 +116,9 @@ def adjoint_forward(comps, ncomp, w0, tend, t0=0.0, rtol=None, atol=None, planar
     record_steps > 0, hrec [record_steps, N] (the accepted step sizes, for
     ``adjoint_replay``).  Checkpoints take (nv + 65) doubles per orbit and 64
     steps; by default the capacity starts at 512 steps and orbits that need
-    more are re-run with 4x the capacity (up to twice)."""
+    more are re-run with 4x the capacity (up to twice).  sort: hand orbits to
+    the GPU threads by decreasing estimated cost (the results do not
+    depend on the order)."""
     import torch
 
     _require("w0", w0, torch.float64)
@@ -106,6 +129,8 @@ def adjoint_forward(comps, ncomp, w0, tend, t0=0.0, rtol=None, atol=None, planar
     s = stream if stream is not None else torch.cuda.current_stream(w0.device)
     dev = w0.device
     cap = int(ckpt_cap) if ckpt_cap else 8
+    order = _cost_order(comps, ncomp, w0, planar, signature, group, s) if sort and nobj > 1 \
+        else None
     for attempt in range(3):
         a = _struct(planar, nobj, t0, tend, rtol, atol, comps, ncomp, group, signature, w0, s,
                     max_attempts, block_size)
@@ -120,6 +145,7 @@ def adjoint_forward(comps, ncomp, w0, tend, t0=0.0, rtol=None, atol=None, planar
         a.ckpt_cap = cap
         a.hrec = hrec.data_ptr() if hrec is not None else None
         a.hcap = record_steps
+        a.order = order.data_ptr() if order is not None else None
         _lib.check(_lib.lib().galpy_cuda_adjoint_forward(ctypes.byref(a)))
         if ckpt_cap or max_attempts or record_steps:
             break
