@@ -115,3 +115,28 @@ def test_autotune_candidates_and_keys():
                                True)
     k3 = autotune.workload_key("B200", "dop853_cuda", True, "fp64", 1, False, 1 << 20, True)
     assert k1 != k3 and k1.split("|n~")[0] == k2.split("|n~")[0]
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """The ctypes mirrors of the ABI structs have the header's field offsets
+    and sizes (a mismatch would silently misplace arguments)."""
+    import subprocess
+
+    structs = {"galpy_cuda_opts": _lib.GalpyCudaOpts, "galpy_cuda_launch": _lib.GalpyCudaLaunch,
+               "galpy_cuda_adjoint": _lib.GalpyCudaAdjoint}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
+    for name, cls in structs.items():
+        lines.append(f'  printf("{name} @sizeof %zu\\n", sizeof({name}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("{name} {fname} %zu\\n", offsetof({name}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-o", str(exe), str(src)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(ln.split()[:2]): int(ln.split()[2]) for ln in out if ln}
+    for name, cls in structs.items():
+        assert got[(name, "@sizeof")] == ctypes.sizeof(cls), name
+        for fname, _ in cls._fields_:
+            assert got[(name, fname)] == getattr(cls, fname).offset, (name, fname)
