@@ -556,12 +556,17 @@ def mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg, n, comps_
     t_d = torch.tensor(t, device=dev)
     E0 = torch.empty(n, dtype=torch.float64, device=dev)
     gb.energy_device(comps_d, ncomp, w0, E0, stream=stream)
+    from galpy_b200 import autotune
+
     res = {}
     outs = {}
     for prec in ("fp64", "f32force"):
         out = torch.empty((6, 1, n), dtype=torch.float64, device=dev)
         err = torch.empty(n, dtype=torch.int32, device=dev)
         ns = torch.empty(n, dtype=torch.int64, device=dev)
+        # each form at its own best launch shape
+        tuned = autotune.tune(comps_d, ncomp, w0, t_d, out, err, "symplec4_cuda", dt=0.01,
+                              out_row0=1, precision=prec, signature=sig, comps_host=comps_host)
         ms_list = []
         for rep in range(2):  # warm-up + timed
             if pg:
@@ -571,7 +576,8 @@ def mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg, n, comps_
             e0.record(stream)
             gb.integrate_device(comps_d, ncomp, w0, t_d, out, err, "symplec4_cuda", nsteps=ns,
                                 dt=0.01, out_row0=1, precision=prec, stream=stream,
-                                signature=sig, comps_host=comps_host)
+                                signature=sig, comps_host=comps_host,
+                                **autotune.launch_kwargs(tuned))
             e1.record(stream)
             torch.cuda.synchronize()
             ms_list.append(e0.elapsed_time(e1))
@@ -581,6 +587,7 @@ def mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg, n, comps_
         steps = float(ns.sum().item())
         ms = ms_list[-1]
         res[prec] = {"value": steps / (ms * 1e-3), "unit": "orbit-steps/s", "ms": ms,
+                     "launch": autotune.launch_kwargs(tuned),
                      "energy_rel_err": stats(torch.abs(E1 / E0 - 1).cpu().numpy()),
                      "orbits_with_err": int((err != 0).sum().item())}
         outs[prec] = out[:, 0, :]
