@@ -735,6 +735,9 @@ struct Dop853Machine : OrbitCommon {
 #pragma unroll
       for (int i = 0; i < N; i++) acc[i] = c0 * k1[i];
     }
+    // unrolled by 4 (with a remainder): the table reads of later terms are
+    // issued ahead of the shared-memory loads and FMAs of earlier ones
+#pragma unroll 4
     for (int tt = 1; tt < n; tt++) {
       const int s = tb.slot[stage][tt];
       const double c = tb.coef[stage][tt];
