@@ -197,7 +197,8 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------- CPU baseline --
-def cpu_reference_rate(ics, t, pt, pa, target_s=10.0, min_orbits=512):
+def cpu_reference_rate(ics, t, pt, pa, target_s=10.0, min_orbits=512, method="dop853",
+                       rtol=RTOL, atol=ATOL):
     """orbit-steps/s of the reference's C (oracle/_ref) or the oracle, all cores."""
     from oracle import oracle as O
 
@@ -207,18 +208,17 @@ def cpu_reference_rate(ics, t, pt, pa, target_s=10.0, min_orbits=512):
     rng = np.random.default_rng(123)
     while True:
         idx = rng.choice(len(ics), size=min(n, len(ics)), replace=False)
-        sub_ics, sub_t = ics[idx], t[idx]
+        sub_ics, sub_t = ics[idx], (t[idx] if t.ndim > 1 else t)
         t0 = time.perf_counter()
-        O.integrate(sub_ics, sub_t, pt, pa, "dop853", rtol=RTOL, atol=ATOL, impl=("ref" if kind ==
-                                                                                  "reference" else "port"),
-                    nthreads=cores)
+        O.integrate(sub_ics, sub_t, pt, pa, method, rtol=rtol, atol=atol,
+                    impl=("ref" if kind == "reference" else "port"), nthreads=cores)
         el = time.perf_counter() - t0
         if el >= 0.4 * target_s or n >= len(ics):
             break
         n = int(n * min(8.0, max(2.0, 0.5 * target_s / max(el, 1e-3))))
     # accepted steps of the same sample (the oracle is bit-identical to the
     # reference's C, so its counts are the reference's)
-    _, _, ns, _ = O.integrate(sub_ics, sub_t, pt, pa, "dop853", rtol=RTOL, atol=ATOL,
+    _, _, ns, _ = O.integrate(sub_ics, sub_t, pt, pa, method, rtol=rtol, atol=atol,
                               nthreads=cores)
     steps = int(ns.sum())
     return {"value": steps / el, "unit": "orbit-steps/s", "cores": cores, "kind": kind,
@@ -243,6 +243,9 @@ def main():
     ap.add_argument("--grad-only", action="store_true",
                     help="run only the differentiation leg (with --grad-orbits orbits)")
     ap.add_argument("--grad-orbits", type=int, default=65536)
+    ap.add_argument("--methods-only", action="store_true",
+                    help="run only the integrator comparison leg: all seven integrators "
+                         "on the same batch, each beside the reference's C on a sample")
     ap.add_argument("--case", default="batching", choices=["batching", "uniform", "longest"],
                     help="uniform: R ~ U(0.5, 2), shared t in [0, 50] (101 snapshots) "
                          "(a throughput-bound case for profiling the same kernel); longest: "
@@ -280,6 +283,16 @@ def main():
         peak = ctypes_fp64_peak(_lib)
         res = differentiation_leg(gb, torch, dev, torch.cuda.current_stream(dev), pg, peak,
                                   n=args.grad_orbits)
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(res), flush=True)
+        return
+
+    if args.methods_only:
+        res = methods_leg(gb, torch, dev, torch.cuda.current_stream(dev), pg,
+                          ctypes_fp64_peak(_lib), rank, not args.no_cpu_baseline)
         if pg:
             pg.barrier()
             pg.destroy_process_group()
@@ -507,6 +520,72 @@ def differentiation_leg(gb, torch, dev, stream, pg, peak, n=65536):
                          "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                          "flops_per_unit": F_GRAD_STEP,
                          "unit_of_work": "accepted forward step (forward + backward flops)"}}
+
+
+# Nominal float64 flops per step of each integrator in MWPotential2014 (3D,
+# F_force = 300): kicks/drifts or stage combinations on top of the force
+# evaluations per step (dopr54 and dop853: per accepted step).
+METHOD_FLOPS = {"leapfrog": 318.0, "symplec4": 942.0, "symplec6": 2200.0, "rk4": 1260.0,
+                "rk6": 2250.0, "dopr54": 2050.0, "dop853": F_STEP_DOP853}
+METHODS_WORKLOAD = ("131,072 orbits/GPU in MWPotential2014, config-0 initial conditions "
+                    "(R ~ U(0.5, 2)), t in [0, 10] with 11 snapshots, galpy's default "
+                    "tolerances (rtol = atol = 1e-12) and estimated step, SoA float64 output")
+
+
+def methods_leg(gb, torch, dev, stream, pg, peak, rank, cpu=True, n=131072, K=3, W=3):
+    """Every integrator on the same batch: orbit-steps/s on the device (CUDA
+    events, max over ranks) and the reference's C on a sample of the same
+    orbits on all host cores."""
+    pt, pa = mw14_args()
+    ics, _ = precision_workload(n, seed=shard_seed(0, rank))
+    t = np.linspace(0.0, 10.0, 11)
+    comps, ncomp = gb.compile_potential((pt, pa))
+    sig = gb.signature((pt, pa))
+    comps_d = torch.tensor(comps, device=dev)
+    w0 = torch.tensor(cyl_to_rect(ics).T.copy(), device=dev)
+    t_d = torch.tensor(t, device=dev)
+    out = torch.empty((6, len(t), n), dtype=torch.float64, device=dev)
+    err = torch.empty(n, dtype=torch.int32, device=dev)
+    nsteps = torch.empty(n, dtype=torch.int64, device=dev)
+    world = pg.get_world_size() if pg else 1
+    res = {"workload": METHODS_WORKLOAD, "n_gpus": world, "steps": K, "warmup": W,
+           "per_method": {}}
+    for m, flops in METHOD_FLOPS.items():
+        def run():
+            gb.integrate_device(comps_d, ncomp, w0, t_d, out, err, m + "_cuda", nsteps=nsteps,
+                                signature=sig, comps_host=comps, stream=stream)
+
+        for _ in range(W):
+            run()
+        torch.cuda.synchronize()
+        steps = int(nsteps.sum().item())
+        nbad = int((err != 0).sum().item())
+        if pg:
+            pg.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(K):
+            run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        (ms,), (steps, nbad) = over_ranks([e0.elapsed_time(e1)], [steps, nbad], pg, dev)
+        rate = steps * K / (ms * 1e-3)
+        entry = {"value": rate, "unit": "orbit-steps/s", "ms_per_step": ms / K,
+                 "steps_per_batch": steps, "orbits_with_err": nbad,
+                 "flops_per_step": flops,
+                 "fp64_frac_of_measured_peak": rate / world * flops / 1e12 / peak if peak
+                 else None}
+        if cpu and rank == 0:
+            try:
+                c = cpu_reference_rate(ics, t, pt, pa, target_s=4.0, min_orbits=64, method=m,
+                                       rtol=None, atol=None)
+                entry["cpu_reference"] = c
+                entry["vs_cpu_reference"] = rate / c["value"]
+            except Exception as exc:  # report, do not hide
+                entry["cpu_reference"] = {"value": None, "error": repr(exc)}
+        res["per_method"][m] = entry
+    res["gpu_launches"] = 2 * (K + W) * len(METHOD_FLOPS)  # cost pass + orbit kernel per run
+    return res
 
 
 def ragged_leg(gb, torch, dev, stream, pg):

@@ -1,12 +1,13 @@
 """galpy_b200 -- B200-native batched orbit integration for galpy.
 
 The engine (libgalpy_cuda.so, built from galpy_b200/csrc for sm_100a) runs
-galpy's leapfrog, symplec4, rk4 and dop853 integrators -- plain and
-variational (dxdv) -- in MWPotential2014-type potentials on the GPU.  Its
-galpy-facing entry points mirror galpy's own C wrappers
-(galpy/orbit/integrateFullOrbit.py, integratePlanarOrbit.py); ``galpy_hooks``
-plugs them into ``galpy.orbit.Orbit.integrate`` as the methods
-'leapfrog_cuda', 'rk4_cuda', 'symplec4_cuda' and 'dop853_cuda'.
+galpy's C integrators (leapfrog, symplec4, symplec6, rk4, rk6, dopr54,
+dop853) -- plain and variational (dxdv) -- in MWPotential2014-type
+potentials on the GPU.  Its galpy-facing entry points mirror galpy's own C
+wrappers (galpy/orbit/integrateFullOrbit.py, integratePlanarOrbit.py);
+``galpy_hooks`` plugs them into ``galpy.orbit.Orbit.integrate`` as the
+methods 'leapfrog_cuda', 'symplec4_cuda', 'symplec6_cuda', 'rk4_cuda',
+'rk6_cuda', 'dopr54_cuda' and 'dop853_cuda'.
 
 There is no CPU fallback: calls raise CudaLibraryMissing when the library is
 not built and CudaError when no GPU is available.

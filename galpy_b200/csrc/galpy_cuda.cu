@@ -34,7 +34,7 @@
 
 #include "../../include/galpy_cuda.h"
 #include "compile_potential.h"
-#include "machines.cuh"
+#include "orbit_kernel.cuh"
 
 using namespace gpc;
 
@@ -61,171 +61,6 @@ __attribute__((visibility("hidden"))) int gpc_report_error(int code, const char*
     if (e_ != cudaSuccess)                                                              \
       return set_error(GALPY_CUDA_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
   } while (0)
-
-// ----------------------------------------------------------------------------
-// kernel
-// ----------------------------------------------------------------------------
-struct KArgs {
-  long long nobj;
-  int nt, indiv_t;
-  const double* t;
-  const double* w0;
-  int in_layout;
-  OutSpec out;
-  int* err;
-  long long* nsteps;
-  const GpComp* comps;
-  int ncomp;
-  const int* group;
-  double dt, rtol, atol;
-  long long max_attempts;
-  unsigned long long* counter;
-  const int* abort_flag;
-  unsigned long long* done_count;
-  const int* order;  // work-queue order (longest first), or NULL
-  int variational_nv; // values per input row of variational runs (0 otherwise)
-  // the first tail_len queue entries (the longest orbits) go to one warp on
-  // each of the SMs 0..tail_sms-1, which run nothing else (0: no reservation)
-  long long tail_len;
-  int tail_sms;
-  unsigned long long* tail_counter;
-  unsigned* sm_claim;
-  // scalar parameters of the (single) potential, read from the constant bank
-  // by the kernels whose POT takes them directly
-  double scal[kMaxComp * kScalarStride];
-};
-
-template <int NV, int D, bool CYL_OK>
-struct DevRows {
-  const OutSpec* o;
-  long long i;
-  __device__ __forceinline__ void operator()(int j, const double* v) const
-  {
-    write_row<NV, D, CYL_OK>(*o, i, j, v);
-  }
-};
-
-template <class M>
-__device__ __forceinline__ void load_state(const KArgs& A, long long i, double* w)
-{
-  if (A.in_layout == GALPY_CUDA_IN_SOA) {
-#pragma unroll
-    for (int k = 0; k < M::NV; k++) w[k] = A.w0[(long long)k * A.nobj + i];
-  } else {
-#pragma unroll
-    for (int k = 0; k < M::NV; k++) w[k] = A.w0[i * M::NV + k];
-  }
-}
-
-// Whether any reserved SM has taken its tail warp.
-__device__ __forceinline__ bool tail_claimed(const KArgs& A)
-{
-  for (int k = 0; k < A.tail_sms; k++)
-    if (*reinterpret_cast<const volatile unsigned*>(&A.sm_claim[k])) return true;
-  return false;
-}
-
-// MINB: minimum resident blocks per SM requested from the register
-// allocator (1 = no cap; larger values trade registers for occupancy).
-template <class M, int D, int PREC, bool VAR, class POT, int MINB>
-__global__ void __launch_bounds__(128, MINB) orbit_kernel(const __grid_constant__ KArgs A)
-{
-  constexpr bool CYL_OK = !VAR;
-  using Rows = DevRows<M::NV, D, CYL_OK>;
-  extern __shared__ double slot_store[];
-  // Reserved SMs for the longest orbits: the first block resident on each of
-  // SMs 0..tail_sms-1 keeps one warp, which takes the tail queue (then helps
-  // with the main queue); any other block there leaves, so those orbits do
-  // not share their SM with the bulk of the batch.  Main workers drain tail
-  // entries left unclaimed (no block landed on a reserved SM).
-  __shared__ int role;  // 0 main queue, 1 tail warp, 2 leave
-  if (threadIdx.x == 0) {
-    role = 0;
-    if (A.tail_len > 0) {
-      unsigned smid;
-      asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
-      if (smid < (unsigned)A.tail_sms) role = atomicExch(&A.sm_claim[smid], 1u) == 0u ? 1 : 2;
-    }
-  }
-  __syncthreads();
-  int my_role = role;
-  if (my_role == 2 || (my_role == 1 && threadIdx.x >= 32)) return;
-  M m;
-  m.bind(slot_store + threadIdx.x);
-  long long i = 0;
-  bool active = false, aborting = false;
-  const GpComp* comps = A.comps;
-  unsigned iter = 0;
-  int slot = 0;
-  for (;;) {
-    if (!active) {
-      long long q = -1;
-      if (my_role == 1) {
-        q = (long long)atomicAdd(A.tail_counter, 1ULL);
-        if (q >= A.tail_len) {
-          q = -1;
-          my_role = 0;
-        }
-      }
-      if (q < 0 && A.tail_len > 0 && !tail_claimed(A)) {
-        // no reserved SM hosts a tail warp: the longest orbits go first here
-        q = (long long)atomicAdd(A.tail_counter, 1ULL);
-        if (q >= A.tail_len) q = -1;
-      }
-      if (q < 0) {
-        q = (long long)atomicAdd(A.counter, 1ULL) + A.tail_len;
-        if (q >= A.nobj) {
-          if (A.tail_len == 0) break;
-          q = (long long)atomicAdd(A.tail_counter, 1ULL);
-          if (q >= A.tail_len) break;
-        }
-      }
-      i = A.order ? A.order[q] : q;
-      if (aborting) {
-        A.err[i] = E_ABORT;
-        write_nan_rows<M::NV, D, CYL_OK>(A.out, i, 0);
-        continue;
-      }
-      double w[M::NV];
-      load_state<M>(A, i, w);
-      comps = A.comps + (A.group ? (long long)A.group[i] * A.ncomp : 0LL);
-      Rows rows{&A.out, i};
-      m.init(w, A.t + (A.indiv_t ? i * (long long)A.nt : 0LL), A.nt, A.dt, A.rtol, A.atol,
-             A.max_attempts, rows);
-      active = true;
-    }
-    if (!m.done) {
-      double y[M::NY], q[M::NA], a[M::NA];
-      m.point(y, slot);
-      M::pos(y, q);
-      eval_force<D, PREC, VAR, POT>(comps, A.ncomp, q, a, A.scal);
-      Rows rows{&A.out, i};
-      m.consume(y, a, rows, slot);
-    }
-    // advance the warp's stage slot (DOP853): the dense-output slots run only
-    // if some lane of the warp needs them
-#if defined(__CUDA_ARCH__)
-    slot = M::next_slot(slot, __any_sync(__activemask(), m.wants_dense()));
-#endif
-    ++iter;
-    if (A.abort_flag && ((iter & 255u) == 0u) &&
-        *reinterpret_cast<const volatile int*>(A.abort_flag)) {
-      aborting = true;
-      if (!m.done) {
-        m.err = E_ABORT;
-        m.done = true;
-      }
-    }
-    if (m.done) {
-      Rows rows{&A.out, i};
-      fill_unreached_rows(m, rows);
-      A.err[i] = m.err;
-      if (A.nsteps) A.nsteps[i] = m.nsteps;
-      if (A.done_count) atomicAdd(A.done_count, 1ULL);
-      active = false;
-    }
-  }
-}
 
 // ----------------------------------------------------------------------------
 // longest-first scheduling: estimated cost of each orbit
@@ -265,69 +100,26 @@ __global__ void __launch_bounds__(256) cost_kernel(const KArgs A, float* key, in
 // ----------------------------------------------------------------------------
 // launch plumbing
 // ----------------------------------------------------------------------------
-using KernelFn = void (*)(const KArgs);
-
-struct KernelInfo {
-  KernelFn fn = nullptr;
-  int slot_doubles = 0;  // per-thread shared-memory slot store (doubles)
+struct CoreMethods {
+  template <int D, int PREC, bool VAR, class POT>
+  static KernelInfo pick(int method, int variant)
+  {
+    switch (method) {
+      case M_LEAPFROG: return info_of<SymplecticMachine<D, VAR, 2>, D, PREC, VAR, POT>(variant);
+      case M_SYMPLEC4: return info_of<SymplecticMachine<D, VAR, 4>, D, PREC, VAR, POT>(variant);
+      case M_RK4: return info_of<RKMachine<D, VAR, 4>, D, PREC, VAR, POT>(variant);
+      case M_DOP853: return info_of<Dop853Machine<D, VAR>, D, PREC, VAR, POT>(variant);
+    }
+    return KernelInfo();
+  }
 };
 
-// Register-budget variants (chosen by the autotuner, galpy_b200/autotune.py):
-// variant 0 lets the compiler use up to 255 registers; variant 1 caps them
-// so that more blocks are resident (3 blocks/SM for DOP853, whose shared
-// slot store allows at most 3; 4 blocks/SM for the lighter integrators).
-template <class M, int D, int PREC, bool VAR, class POT>
-static KernelInfo info_of(int variant)
-{
-  KernelInfo k;
-  constexpr int capped = M::kSlotDoubles > 0 ? 3 : 4;
-  if (variant == 1 && !VAR)
-    k.fn = orbit_kernel<M, D, PREC, VAR, POT, capped>;
-  else
-    k.fn = orbit_kernel<M, D, PREC, VAR, POT, 1>;
-  k.slot_doubles = M::kSlotDoubles;
-  return k;
-}
-
-template <int D, int PREC, bool VAR, class POT>
-static KernelInfo pick_kernel_dim(int method, int variant)
-{
-  switch (method) {
-    case M_LEAPFROG: return info_of<SymplecticMachine<D, VAR, false>, D, PREC, VAR, POT>(variant);
-    case M_SYMPLEC4: return info_of<SymplecticMachine<D, VAR, true>, D, PREC, VAR, POT>(variant);
-    case M_RK4: return info_of<RK4Machine<D, VAR>, D, PREC, VAR, POT>(variant);
-    case M_DOP853: return info_of<Dop853Machine<D, VAR>, D, PREC, VAR, POT>(variant);
-  }
-  return KernelInfo();
-}
-
-template <int PREC, class POT>
-static KernelInfo pick_plain(int planar, int method, int variant)
-{
-  return planar ? pick_kernel_dim<2, PREC, false, POT>(method, variant)
-                : pick_kernel_dim<3, PREC, false, POT>(method, variant);
-}
-
-// sig: GALPY_CUDA_SIG_MW14 selects the kernels with the MWPotential2014
-// component list fixed at compile time (plain runs); variational runs walk
-// the component list at run time.
 static KernelInfo pick_kernel(int planar, int var, int prec, int method, int sig, int variant,
                               bool direct)
 {
-  if (var) {
-    if (prec != GALPY_CUDA_FP64) return KernelInfo();  // variational runs are float64 only
-    return planar ? pick_kernel_dim<2, PREC_FP64, true, DynPot>(method, 0)
-                  : pick_kernel_dim<3, PREC_FP64, true, DynPot>(method, 0);
-  }
-  const bool mw14 = sig == GALPY_CUDA_SIG_MW14;
-  if (prec == GALPY_CUDA_F32FORCE) {
-    if (!mw14) return pick_plain<PREC_F32, DynPot>(planar, method, variant);
-    return direct ? pick_plain<PREC_F32, MW14Pot>(planar, method, variant)
-                  : pick_plain<PREC_F32, MW14GroupPot>(planar, method, variant);
-  }
-  if (!mw14) return pick_plain<PREC_FP64, DynPot>(planar, method, variant);
-  return direct ? pick_plain<PREC_FP64, MW14Pot>(planar, method, variant)
-                : pick_plain<PREC_FP64, MW14GroupPot>(planar, method, variant);
+  if (method == M_RK6 || method == M_SYMPLEC6 || method == M_DOPR54)
+    return pick_kernel_more(planar, var, prec, method, sig, variant, direct);
+  return pick_kernel_in<CoreMethods>(planar, var, prec, method, sig, variant, direct);
 }
 
 static int signature_of(int npot, const int* pot_type)
@@ -339,7 +131,7 @@ static int signature_of(int npot, const int* pot_type)
 
 static bool method_supported(int m)
 {
-  return m == M_LEAPFROG || m == M_RK4 || m == M_SYMPLEC4 || m == M_DOP853;
+  return m >= M_LEAPFROG && m <= M_DOP853;  // galpy's 0..6; 7 (ias15) is not implemented
 }
 
 constexpr int kMaxTailSms = 16;

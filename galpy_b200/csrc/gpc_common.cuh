@@ -20,8 +20,9 @@
 
 namespace gpc {
 
-// per-orbit status (the reference uses 0 and -10 for SIGINT)
-enum : int { E_OK = 0, E_BUDGET = 2, E_NONFINITE = 3, E_ABORT = -10 };
+// per-orbit status (the reference uses 0, -10 for SIGINT and, in dopr54, 1
+// for a step forced at the smallest allowed size; the orbit still completes)
+enum : int { E_OK = 0, E_MINSTEP = 1, E_BUDGET = 2, E_NONFINITE = 3, E_ABORT = -10 };
 
 template <typename T>
 GPC_HD GPC_FI T ldg(const T* p)

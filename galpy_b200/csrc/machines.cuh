@@ -16,10 +16,11 @@
 // The arithmetic of every stepper follows the reference step by step so that
 // the step sequence (and, for fixed-step methods, the chosen step size) is the
 // reference's:
-//   leapfrog / symplec4         galpy/util/bovy_symplecticode.c:132-377
-//   their step estimators       galpy/util/bovy_symplecticode.c:588-809
-//   variational (*_dxdv) forms  galpy/util/bovy_symplecticode.c:1053-1268
-//   rk4 + estimator             galpy/util/bovy_rk.c:66-170, 328-395
+//   leapfrog/symplec4/symplec6  galpy/util/bovy_symplecticode.c:132-587
+//   their step estimators       galpy/util/bovy_symplecticode.c:588-1052
+//   variational (*_dxdv) forms  galpy/util/bovy_symplecticode.c:1053-1400
+//   rk4 / rk6 + estimators      galpy/util/bovy_rk.c:66-480
+//   dopr54                      galpy/util/bovy_rk.c:501-760
 //   dop853                      galpy/util/leung_dop853.c:231-517
 // Differences by design: the time variable of the reference's symplectic and
 // RK loops is not tracked (the supported potentials are static); DOP853
@@ -40,7 +41,8 @@ constexpr double kDtSentinel = -9999.99;  // galpy's "estimate the step" marker
 constexpr int kSlotStride = 128;
 constexpr double kMaxDtReduce = 10000.;
 
-enum : int { M_LEAPFROG = 0, M_RK4 = 1, M_SYMPLEC4 = 3, M_DOP853 = 6 };
+enum : int { M_LEAPFROG = 0, M_RK4 = 1, M_RK6 = 2, M_SYMPLEC4 = 3, M_SYMPLEC6 = 4, M_DOPR54 = 5,
+             M_DOP853 = 6 };
 enum : int { PREC_FP64 = 0, PREC_F32 = 1 };
 
 // symplec4 coefficients (Kinoshita et al.; bovy_symplecticode.c:96-99)
@@ -48,6 +50,12 @@ constexpr double s4c1 = 0.6756035959798289, s4c2 = -0.1756035959798288;
 constexpr double s4c3 = -0.1756035959798288, s4c4 = 0.6756035959798289;
 constexpr double s4d1 = 1.3512071919596578, s4d2 = -1.7024143839193153;
 constexpr double s4d3 = 1.3512071919596578;
+// symplec6 coefficients (Yoshida 1990; bovy_symplecticode.c:100-107): the
+// drifts c1..c8 and kicks d1..d7 are palindromic
+constexpr double s6c1 = 0.392256805238780, s6c2 = 0.510043411918458;
+constexpr double s6c3 = -0.471053385409758, s6c4 = 0.687531682525198e-1;
+constexpr double s6d1 = 0.784513610477560, s6d2 = 0.235573213359357;
+constexpr double s6d3 = -0.117767998417887e1, s6d4 = 0.131518632068391e1;
 
 // ------------------------------------------------------------------------
 // output rows
@@ -176,10 +184,58 @@ struct OrbitCommon {
 };
 
 // ------------------------------------------------------------------------
-// leapfrog / symplec4 (optionally variational)
+// leapfrog / symplec4 / symplec6 (optionally variational)
 // ------------------------------------------------------------------------
-template <int D, bool VAR, bool S4>
+// Drift-kick compositions: ORD 2 (leapfrog: drifts h/2, h/2; kick h), 4
+// (symplec4: 4 drifts, 3 kicks) and 6 (symplec6: 8 drifts, 7 kicks).  The last
+// drift of a step merges with the first of the next, as in the reference.
+template <int ORD>
+struct Composition;
+template <>
+struct Composition<2> {
+  static constexpr int kKicks = 1;
+  GPC_HD GPC_FI static double first(double h) { return h / 2.; }
+  GPC_HD GPC_FI static double kick(int, double h) { return h; }
+  // drift after kick j: the step's last (merged with the next step's first
+  // unless `last`)
+  GPC_HD GPC_FI static double drift(int, bool last, double h) { return last ? h / 2. : h; }
+};
+template <>
+struct Composition<4> {
+  static constexpr int kKicks = 3;
+  GPC_HD GPC_FI static double first(double h) { return s4c1 * h; }
+  GPC_HD GPC_FI static double kick(int j, double h)
+  {
+    return j == 0 ? s4d1 * h : (j == 1 ? s4d2 * h : s4d3 * h);
+  }
+  GPC_HD GPC_FI static double drift(int j, bool last, double h)
+  {
+    return j == 0 ? s4c2 * h : (j == 1 ? s4c3 * h : (last ? s4c4 * h : (s4c4 + s4c1) * h));
+  }
+};
+template <>
+struct Composition<6> {
+  static constexpr int kKicks = 7;
+  GPC_HD GPC_FI static double first(double h) { return s6c1 * h; }
+  GPC_HD GPC_FI static double kick(int j, double h)
+  {
+    const int m = j < 4 ? j : 6 - j;  // d5..d7 mirror d3..d1
+    const double d = m == 0 ? s6d1 : (m == 1 ? s6d2 : (m == 2 ? s6d3 : s6d4));
+    return d * h;
+  }
+  GPC_HD GPC_FI static double drift(int j, bool last, double h)
+  {
+    // after kick j comes drift c_{j+2}; c5..c8 mirror c4..c1
+    if (j == 6) return last ? s6c1 * h : (s6c1 + s6c1) * h;  // c8 (+ c1)
+    const int m = j < 3 ? j + 1 : 6 - j;
+    const double c = m == 1 ? s6c2 : (m == 2 ? s6c3 : s6c4);
+    return c * h;
+  }
+};
+
+template <int D, bool VAR, int ORD>
 struct SymplecticMachine : OrbitCommon {
+  using C = Composition<ORD>;
   static constexpr int NQ = VAR ? 2 * D : D;  // stepped positions
   static constexpr int NY = NQ;               // size of the force argument
   static constexpr int NV = 2 * NQ;           // values per output row
@@ -207,8 +263,8 @@ struct SymplecticMachine : OrbitCommon {
     nrun = nstep;
     kick = 0;
     sub = 0;
-    nkick = (S4 ? 3 : 1) * nstep;
-    const double c = S4 ? s4c1 * h : h / 2.;
+    nkick = C::kKicks * nstep;
+    const double c = C::first(h);
 #pragma unroll
     for (int k = 0; k < NQ; k++) {
       qw[k] = qo[k] + c * po[k];
@@ -290,19 +346,15 @@ struct SymplecticMachine : OrbitCommon {
   template <class W>
   GPC_HD void consume(const double* /*y*/, const double* a, W& out, int /*slot*/)
   {
-    const double dk = S4 ? (sub == 0 ? s4d1 * h : (sub == 1 ? s4d2 * h : s4d3 * h)) : h;
+    const double dk = C::kick(sub, h);
 #pragma unroll
     for (int k = 0; k < NQ; k++) pw[k] = pw[k] + dk * a[k];
     const bool last = (kick == nkick - 1);
-    double dc;
-    if (S4)
-      dc = sub == 0 ? s4c2 * h : (sub == 1 ? s4c3 * h : (last ? s4c4 * h : (s4c4 + s4c1) * h));
-    else
-      dc = last ? h / 2. : h;
+    const double dc = C::drift(sub, last, h);
 #pragma unroll
     for (int k = 0; k < NQ; k++) qw[k] = qw[k] + dc * pw[k];
     kick++;
-    sub = (S4 && sub < 2) ? sub + 1 : 0;
+    sub = sub < C::kKicks - 1 ? sub + 1 : 0;
     if (last) advance_done(out);
   }
 
@@ -365,14 +417,119 @@ struct SymplecticMachine : OrbitCommon {
 };
 
 // ------------------------------------------------------------------------
-// RK4 (optionally variational)
+// classical RK steps as stage machines
 // ------------------------------------------------------------------------
-template <int D, bool VAR>
-struct RK4Machine : OrbitCommon {
+// Stage s of one step of size h from yn: d is the derivative at the stage's
+// point (yn for s = 0, ynk after), yn1 accumulates the step's result and ynk
+// receives the next stage's point.
+// bovy_rk4_onestep (bovy_rk.c:142-170)
+template <int N>
+GPC_HD GPC_FI void rk4_stage(int s, double h, const double* yn, double* yn1, double* ynk,
+                             const double* d)
+{
+  if (s == 0 || s == 3) {
+#pragma unroll
+    for (int k = 0; k < N; k++) yn1[k] += h * d[k] / 6.;
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; k++) yn1[k] += h * d[k] / 3.;
+  }
+  if (s < 2) {
+#pragma unroll
+    for (int k = 0; k < N; k++) ynk[k] = yn[k] + h * d[k] / 2.;
+  } else if (s == 2) {
+#pragma unroll
+    for (int k = 0; k < N; k++) ynk[k] = yn[k] + h * d[k];
+  }
+}
+
+// bovy_rk6_onestep (bovy_rk.c:256-327): weights (11, 0, 81, 81, -32, -32,
+// 11)/120; kk[0..4] hold k1..k5 (k6 is only needed for the last point)
+template <int N>
+GPC_HD GPC_FI void rk6_stage(int s, double h, const double* yn, double* yn1, double* ynk,
+                             double (*kk)[N], const double* d)
+{
+  switch (s) {
+    case 0:
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        yn1[k] += 11. * h * d[k] / 120.;
+        kk[0][k] = h * d[k];
+        ynk[k] = yn[k] + kk[0][k] / 3.;
+      }
+      break;
+    case 1:
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        kk[1][k] = h * d[k];
+        ynk[k] = yn[k] + 2. * kk[1][k] / 3.;
+      }
+      break;
+    case 2:
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        yn1[k] += 81. * h * d[k] / 120.;
+        kk[2][k] = h * d[k];
+        ynk[k] = yn[k] + (kk[0][k] + 4. * kk[1][k] - kk[2][k]) / 12.;
+      }
+      break;
+    case 3:
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        yn1[k] += 81. * h * d[k] / 120.;
+        kk[3][k] = h * d[k];
+        ynk[k] = yn[k] + (-kk[0][k] + 18. * kk[1][k] - 3. * kk[2][k] - 6. * kk[3][k]) / 16.;
+      }
+      break;
+    case 4:
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        yn1[k] -= 32. * h * d[k] / 120.;
+        kk[4][k] = h * d[k];
+        ynk[k] = yn[k] + (9. * kk[1][k] - 3. * kk[2][k] - 6. * kk[3][k] + 4. * kk[4][k]) / 8.;
+      }
+      break;
+    case 5:
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        yn1[k] -= 32. * h * d[k] / 120.;
+        const double k6 = h * d[k];
+        ynk[k] = yn[k] + (9. * kk[0][k] - 36. * kk[1][k] + 63. * kk[2][k] + 72. * kk[3][k] -
+                          64. * k6) / 44.;
+      }
+      break;
+    default:
+#pragma unroll
+      for (int k = 0; k < N; k++) yn1[k] += 11. * h * d[k] / 120.;
+  }
+}
+
+// derivative of the state y = (x, v[, dx, dv]) given the force result a
+template <int D, bool VAR, int N>
+GPC_HD GPC_FI void state_derivative(const double* y, const double* a, double* d)
+{
+#pragma unroll
+  for (int k = 0; k < D; k++) {
+    d[k] = y[D + k];
+    d[D + k] = a[k];
+    if (VAR) {
+      d[2 * D + k] = y[3 * D + k];
+      d[3 * D + k] = a[D + k];
+    }
+  }
+}
+
+// ------------------------------------------------------------------------
+// RK4 / RK6 (optionally variational)
+// ------------------------------------------------------------------------
+template <int D, bool VAR, int ORD>
+struct RKMachine : OrbitCommon {
+  static_assert(ORD == 4 || ORD == 6, "rk4 or rk6");
   static constexpr int N = VAR ? 4 * D : 2 * D;  // ODE dimension
   static constexpr int NY = N;
   static constexpr int NV = N;
   static constexpr int NA = VAR ? 2 * D : D;  // force result size
+  static constexpr int kStages = ORD == 4 ? 4 : 7;
   // force argument: positions (and deviation positions) of (x, v[, dx, dv])
   GPC_HD GPC_FI static void pos(const double* y, double* q)
   {
@@ -389,7 +546,8 @@ struct RK4Machine : OrbitCommon {
   enum { EST_A = 0, EST_B = 1, EST_C = 2, MAIN = 3 };
   double yo[N];    // orbit state at the last completed step
   double yn[N], yn1[N], ynk[N];
-  double y1[N], ya[N];  // estimator: one-step result; midpoint of the two half steps
+  double y1[N];    // estimator: the one-step result
+  double kk[ORD == 6 ? 5 : 1][N];  // rk6 stage increments k1..k5
   double dt, init_dt, h, s, rtol, atol;
   long long nrun, step;
   int stage, phase;
@@ -454,39 +612,21 @@ struct RK4Machine : OrbitCommon {
   template <class W>
   GPC_HD void consume(const double* y, const double* a, W& out, int /*slot*/)
   {
-    // derivative of the state at the evaluation point (x, v[, dx, dv])
     double d[N];
-#pragma unroll
-    for (int k = 0; k < D; k++) {
-      d[k] = y[D + k];
-      d[D + k] = a[k];
-      if (VAR) {
-        d[2 * D + k] = y[3 * D + k];
-        d[3 * D + k] = a[D + k];
-      }
-    }
-    // bovy_rk4_onestep (bovy_rk.c:142-170)
-    if (stage == 0 || stage == 3) {
-#pragma unroll
-      for (int k = 0; k < N; k++) yn1[k] += h * d[k] / 6.;
-    } else {
-#pragma unroll
-      for (int k = 0; k < N; k++) yn1[k] += h * d[k] / 3.;
-    }
-    if (stage < 2) {
-#pragma unroll
-      for (int k = 0; k < N; k++) ynk[k] = yn[k] + h * d[k] / 2.;
-    } else if (stage == 2) {
-#pragma unroll
-      for (int k = 0; k < N; k++) ynk[k] = yn[k] + h * d[k];
-    }
-    if (++stage < 4) return;
+    state_derivative<D, VAR, N>(y, a, d);
+    if (ORD == 4)
+      rk4_stage<N>(stage, h, yn, yn1, ynk, d);
+    else
+      rk6_stage<N>(stage, h, yn, yn1, ynk, kk, d);
+    if (++stage < kStages) return;
     onestep_done(out);
   }
 
   template <class W>
   GPC_HD void onestep_done(W& out)
   {
+    // rk4_estimate_step / rk6_estimate_step (bovy_rk.c:328-480): one step of
+    // dt against two of dt/2
     if (phase == EST_A) {
 #pragma unroll
       for (int k = 0; k < N; k++) y1[k] = yn1[k];
@@ -495,10 +635,8 @@ struct RK4Machine : OrbitCommon {
       return;
     }
     if (phase == EST_B) {
-#pragma unroll
-      for (int k = 0; k < N; k++) ya[k] = yn1[k];
       phase = EST_C;
-      start(ya, dt / 2.);
+      start(yn1, dt / 2.);
       return;
     }
     if (phase == EST_C) {
@@ -506,7 +644,7 @@ struct RK4Machine : OrbitCommon {
 #pragma unroll
       for (int k = 0; k < N; k++) e += exp(2. * log(fabs(y1[k] - yn1[k])) - 2. * s);
       e = sqrt(e / N);
-      const double c = ceil(pow(e, 1. / 5.));
+      const double c = ceil(pow(e, ORD == 4 ? 1. / 5. : 1. / 7.));
       if (c > 1. && init_dt / dt * c < kMaxDtReduce) {
         dt /= c;
         phase = EST_A;
@@ -547,6 +685,314 @@ struct RK4Machine : OrbitCommon {
     } else {
       start(yo, dt);
     }
+  }
+};
+
+template <int D, bool VAR>
+using RK4Machine = RKMachine<D, VAR, 4>;
+
+// ------------------------------------------------------------------------
+// DOPR54 (optionally variational)
+// ------------------------------------------------------------------------
+// Dormand-Prince 5(4) tableau (bovy_rk.c:630-665)
+namespace dp5 {
+constexpr double a21 = 0.2, a31 = 3. / 40., a32 = 9. / 40.;
+constexpr double a41 = 44. / 45., a42 = -56. / 15., a43 = 32. / 9.;
+constexpr double a51 = 19372. / 6561., a52 = -25360. / 2187., a53 = 64448. / 6561.,
+                 a54 = -212. / 729.;
+constexpr double a61 = 9017. / 3168., a62 = -355. / 33., a63 = 46732. / 5247., a64 = 49. / 176.,
+                 a65 = -5103. / 18656.;
+constexpr double b1 = 35. / 384., b3 = 500. / 1113., b4 = 125. / 192., b5 = -2187. / 6784.,
+                 b6 = 11. / 84.;
+constexpr double e1 = b1 - 5179. / 57600., e3 = b3 - 7571. / 16695., e4 = b4 - 393. / 640.,
+                 e5 = b5 + 92097. / 339200., e6 = b6 - 187. / 2100., e7 = -1. / 40.;
+}  // namespace dp5
+
+// bovy_dopr54 (bovy_rk.c:501-616) and bovy_dopr54_actualstep (:617-760):
+// adaptive steps with a first-same-as-last derivative; the step factor is
+// 0.85 err^(-1/5) rounded to a power of two in [1/8, 8] and an attempt is
+// accepted when that power is >= 0.  Each output interval ends with a step
+// clipped to its end (no interpolation).  A step that would shrink below
+// the interval's first step / 10000 (or is NaN) is taken at that size and
+// accepted, and the orbit's err becomes 1 as in the reference.  The first
+// step comes from rk4_estimate_step.  Every attempt either advances the
+// time or shrinks the step (at most 5 times in a row before a forced step),
+// and an accepted step that no longer advances the time ends the orbit
+// (err 2), so an orbit always finishes.
+template <int D, bool VAR>
+struct Dopr54Machine : OrbitCommon {
+  static constexpr int N = VAR ? 4 * D : 2 * D;
+  static constexpr int NY = N;
+  static constexpr int NV = N;
+  static constexpr int NA = VAR ? 2 * D : D;
+  GPC_HD GPC_FI static void pos(const double* y, double* q)
+  {
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      q[k] = y[k];
+      if (VAR) q[D + k] = y[2 * D + k];
+    }
+  }
+  static constexpr int kSlotDoubles = 0;
+  GPC_HD GPC_FI void bind(double*) {}
+  GPC_HD GPC_FI bool wants_dense() const { return false; }
+  GPC_HD GPC_FI static int next_slot(int slot, bool) { return slot >= 14 ? 0 : slot + 1; }
+  enum { EST_A = 0, EST_B = 1, EST_C = 2, FSAL0 = 3, MAIN = 4 };
+  double yo[N];    // state at time `to`
+  double a1[N];    // derivative at yo
+  // k1..k6 of an attempt; during the step estimation kk[0] is the RK4 step's
+  // start and kk[1] the one-step result
+  double kk[6][N];
+  double yn1[N], yerr[N], ynk[N];
+  double to, dtout, init_to, dt_one, init_dt_one, h, s, rtol, atol, est_dt, est_init;
+  int stage, phase;
+  bool forced;
+
+  GPC_HD GPC_FI void est_start(const double* from, double hh)
+  {
+    h = hh;
+    stage = 0;
+#pragma unroll
+    for (int k = 0; k < N; k++) kk[0][k] = yn1[k] = from[k];
+  }
+
+  template <class W>
+  GPC_HD void init(const double* w, const double* tt, int nt_, double dt_in, double rtol_,
+                   double atol_, long long max_att, W& out)
+  {
+    t = tt;
+    nt = nt_;
+    iout = 0;
+    err = E_OK;
+    done = false;
+    nsteps = 0;
+    attempts = 0;
+    max_attempts = max_att;
+    rtol = rtol_;
+    atol = atol_;
+#pragma unroll
+    for (int k = 0; k < N; k++) yo[k] = w[k];
+    out(0, yo);
+    if (nt < 2) {
+      done = true;
+      return;
+    }
+    dtout = tt[1] - tt[0];
+    to = tt[0];
+    if (dt_in == kDtSentinel) {
+      est_dt = est_init = dtout;
+      s = est_scale(yo, N, 1, rtol, atol);
+      phase = EST_A;
+      est_start(yo, est_dt);
+    } else {
+      dt_one = dt_in;
+      phase = FSAL0;
+    }
+  }
+
+  GPC_HD GPC_FI void point(double* y, int /*slot*/) const
+  {
+    if (phase == FSAL0) {
+#pragma unroll
+      for (int k = 0; k < N; k++) y[k] = yo[k];
+      return;
+    }
+    const bool first = phase < FSAL0 && stage == 0;
+#pragma unroll
+    for (int k = 0; k < N; k++) y[k] = first ? kk[0][k] : ynk[k];
+  }
+
+  template <class W>
+  GPC_HD void consume(const double* y, const double* a, W& out, int /*slot*/)
+  {
+    double d[N];
+    state_derivative<D, VAR, N>(y, a, d);
+    if (phase < FSAL0) {
+      rk4_stage<N>(stage, h, kk[0], yn1, ynk, d);
+      if (++stage == 4) est_step_done();
+      return;
+    }
+    if (phase == FSAL0) {
+#pragma unroll
+      for (int k = 0; k < N; k++) a1[k] = d[k];
+      phase = MAIN;
+      init_dt_one = dt_one;
+      init_to = to;
+      next_attempt(out);
+      return;
+    }
+    using namespace dp5;
+    switch (stage) {
+      case 1:
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+          kk[1][k] = h * d[k];
+          ynk[k] = yo[k] + a31 * kk[0][k] + a32 * kk[1][k];
+        }
+        break;
+      case 2:
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+          kk[2][k] = h * d[k];
+          yn1[k] += b3 * kk[2][k];
+          yerr[k] += e3 * kk[2][k];
+          ynk[k] = yo[k] + a41 * kk[0][k] + a42 * kk[1][k] + a43 * kk[2][k];
+        }
+        break;
+      case 3:
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+          kk[3][k] = h * d[k];
+          yn1[k] += b4 * kk[3][k];
+          yerr[k] += e4 * kk[3][k];
+          ynk[k] = yo[k] + a51 * kk[0][k] + a52 * kk[1][k] + a53 * kk[2][k] + a54 * kk[3][k];
+        }
+        break;
+      case 4:
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+          kk[4][k] = h * d[k];
+          yn1[k] += b5 * kk[4][k];
+          yerr[k] += e5 * kk[4][k];
+          ynk[k] = yo[k] + a61 * kk[0][k] + a62 * kk[1][k] + a63 * kk[2][k] + a64 * kk[3][k] +
+                   a65 * kk[4][k];
+        }
+        break;
+      case 5:
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+          kk[5][k] = h * d[k];
+          yn1[k] += b6 * kk[5][k];
+          yerr[k] += e6 * kk[5][k];
+          // the seventh point's a7j are the b weights (a72 = 0)
+          ynk[k] = yo[k] + b1 * kk[0][k] + b3 * kk[2][k] + b4 * kk[3][k] + b5 * kk[4][k] +
+                   b6 * kk[5][k];
+        }
+        break;
+      default:
+        attempt_done(d, out);
+        return;
+    }
+    stage++;
+  }
+
+  // rk4_estimate_step (bovy_rk.c:328-395), run on kk[0] / kk[1]
+  GPC_HD void est_step_done()
+  {
+    if (phase == EST_A) {
+#pragma unroll
+      for (int k = 0; k < N; k++) kk[1][k] = yn1[k];
+      phase = EST_B;
+      est_start(yo, est_dt / 2.);
+      return;
+    }
+    if (phase == EST_B) {
+      phase = EST_C;
+      est_start(yn1, est_dt / 2.);
+      return;
+    }
+    double e = 0.;
+#pragma unroll
+    for (int k = 0; k < N; k++) e += exp(2. * log(fabs(kk[1][k] - yn1[k])) - 2. * s);
+    e = sqrt(e / N);
+    const double c = ceil(pow(e, 1. / 5.));
+    if (c > 1. && est_init / est_dt * c < kMaxDtReduce) {
+      est_dt /= c;
+      phase = EST_A;
+      est_start(yo, est_dt);
+      return;
+    }
+    dt_one = est_dt;
+    phase = FSAL0;
+  }
+
+  // bovy_dopr54_onestep's loop (bovy_rk.c:584-616): output the intervals
+  // that are complete, then set up the next attempt (its k1 from a1)
+  template <class W>
+  GPC_HD void next_attempt(W& out)
+  {
+    for (;;) {
+      const bool more = (dtout >= 0. && to < (init_to + dtout)) ||
+                        (dtout < 0. && to > (init_to + dtout));
+      if (more) break;
+      iout++;
+      out(iout, yo);
+      if (iout == nt - 1) {
+        done = true;
+        return;
+      }
+      init_dt_one = dt_one;
+      init_to = to;
+    }
+    if (max_attempts > 0 && attempts >= max_attempts) {
+      err = E_BUDGET;
+      done = true;
+      return;
+    }
+    forced = false;
+    if (init_dt_one / dt_one > kMaxDtReduce || dt_one != dt_one) {
+      dt_one = init_dt_one / kMaxDtReduce;
+      forced = true;
+      err = E_MINSTEP;
+    }
+    if (dtout >= 0. && dt_one > (init_to + dtout - to)) dt_one = (init_to + dtout - to);
+    if (dtout < 0. && dt_one < (init_to + dtout - to)) dt_one = (init_to + dtout - to);
+    h = dt_one;
+    using namespace dp5;
+#pragma unroll
+    for (int k = 0; k < N; k++) {
+      kk[0][k] = h * a1[k];
+      yn1[k] = yo[k] + b1 * kk[0][k];
+      yerr[k] = e1 * kk[0][k];
+      ynk[k] = yo[k] + a21 * kk[0][k];
+    }
+    stage = 1;
+  }
+
+  // the seventh stage's derivative d: error norm, controller, accept
+  template <class W>
+  GPC_HD void attempt_done(const double* d, W& out)
+  {
+#pragma unroll
+    for (int k = 0; k < N; k++) yerr[k] += dp5::e7 * h * d[k];
+    const double sc = est_scale(yo, N, 1, rtol, atol);
+    double e = 0.;
+#pragma unroll
+    for (int k = 0; k < N; k++) e += exp(2. * log(fabs(yerr[k])) - 2. * sc);
+    e = sqrt(e / N);
+    const double corr = 0.85 * pow(e, -.2);
+    double p2 = round(log(corr) / log(2.));
+    if (p2 > 3.)
+      p2 = 3.;
+    else if (p2 < -3.)
+      p2 = -3.;
+    attempts++;
+    if (p2 >= 0. || forced) {
+      bool fin = true;
+#pragma unroll
+      for (int k = 0; k < N; k++) {
+        a1[k] = d[k];
+        yo[k] = yn1[k];
+        fin = fin && isfinite(yn1[k]);
+      }
+      const double to_before = to;
+      to += h;
+      nsteps++;
+      if (!fin) {
+        err = E_NONFINITE;
+        done = true;
+        return;
+      }
+      // a step below half an ulp of `to` leaves it unchanged: the reference
+      // would loop forever here; the orbit stops as out of budget instead
+      if (to == to_before) {
+        err = E_BUDGET;
+        done = true;
+        return;
+      }
+    }
+    dt_one = h * pow(2., p2);
+    next_attempt(out);
   }
 };
 

@@ -1,9 +1,9 @@
 """Plug the engine into galpy's ``Orbit.integrate``.
 
 After ``install()``, ``Orbit.integrate(ts, pot, method=m)`` accepts
-``m in ('leapfrog_cuda', 'rk4_cuda', 'symplec4_cuda', 'dop853_cuda')`` and
-runs the batch on the GPU through this package; everything else in galpy is
-untouched.  The hooks patch the four places that decide galpy's integrator
+``m`` any of galpy's C integrator names with ``_cuda`` for ``_c`` (leapfrog,
+symplec4, symplec6, rk4, rk6, dopr54, dop853; not ias15) and runs the batch
+on the GPU through this package; everything else in galpy is untouched.  The hooks patch the four places that decide galpy's integrator
 dispatch (galpy/orbit/Orbits.py):
 
 * ``Orbit.check_integrator`` (:1342-1370) -- the allow-list of method names;

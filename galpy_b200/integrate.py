@@ -20,8 +20,9 @@ from . import _lib
 from .potentials import parse_pot
 
 # galpy's odeint codes (galpy/orbit/integratePlanarOrbit.py:690-709)
-CUDA_METHODS = {"leapfrog_cuda": 0, "rk4_cuda": 1, "symplec4_cuda": 3, "dop853_cuda": 6}
-_ALIASES = {"leapfrog": 0, "rk4": 1, "symplec4": 3, "dop853": 6}
+_ALIASES = {"leapfrog": 0, "rk4": 1, "rk6": 2, "symplec4": 3, "symplec6": 4, "dopr54": 5,
+            "dop853": 6}
+CUDA_METHODS = {f"{name}_cuda": code for name, code in _ALIASES.items()}
 PRECISIONS = {"fp64": _lib.FP64, "f32force": _lib.F32FORCE}
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -108,8 +109,8 @@ def integrateFullOrbit_cuda(pot, yo, t, int_method, rtol=None, atol=None, progre
     Parameters mirror galpy's integrateFullOrbit_c: yo [N,6] or [6]
     cylindrical (R,vR,vT,z,vz,phi) -- overwritten in place with rectangular
     coordinates when it is a C-contiguous float64 array, as in galpy; t [nt]
-    or [N,nt]; int_method one of 'leapfrog_cuda', 'rk4_cuda', 'symplec4_cuda',
-    'dop853_cuda'.  Extra keywords: precision ('fp64' or 'f32force'),
+    or [N,nt]; int_method one of 'leapfrog_cuda', 'rk4_cuda', 'rk6_cuda',
+    'symplec4_cuda', 'symplec6_cuda', 'dopr54_cuda', 'dop853_cuda'.  Extra keywords: precision ('fp64' or 'f32force'),
     max_attempts (per-orbit step-attempt budget, 0 = none), return_nsteps.
 
     Returns (result [N,nt,6] cylindrical, err [N]) like galpy (the leading

@@ -1,24 +1,27 @@
 /*
  * galpy_cuda.h -- C ABI of libgalpy_cuda.so, the B200 orbit-integration engine
  * behind galpy's Orbit.integrate methods 'leapfrog_cuda', 'rk4_cuda',
- * 'symplec4_cuda' and 'dop853_cuda'.
+ * 'rk6_cuda', 'symplec4_cuda', 'symplec6_cuda', 'dopr54_cuda' and
+ * 'dop853_cuda'.
  *
  * The galpy-facing entry points take exactly the arguments of the libgalpy
  * functions they stand in for, with galpy's conventions: AoS arrays owned by
  * the caller (host memory), yo overwritten with the rectangular initial
  * conditions, t either shared (nt) or per orbit (nobj*nt, indiv_t = 1),
  * rtol/atol as natural logarithms, dt = -9999.99 meaning "estimate the step",
- * odeint_type 0 leapfrog, 1 rk4, 3 symplec4, 6 dop853 (galpy's numbering;
- * 2 rk6, 4 symplec6, 5 dopr54 and 7 ias15 return GALPY_CUDA_ERR_METHOD so the
+ * odeint_type 0 leapfrog, 1 rk4, 2 rk6, 3 symplec4, 4 symplec6, 5 dopr54,
+ * 6 dop853 (galpy's numbering; 7 ias15 returns GALPY_CUDA_ERR_METHOD so the
  * caller can fall back), pot_type/pot_args as produced by galpy's _parse_pot
  * (types 0 LogarithmicHalo, 5 MiyamotoNagai, 8 Hernquist, 9 NFW,
  * 15 PowerSphericalwCutoff), per-orbit err[] (0 ok, -10 interrupted by
- * SIGINT).  Two additions: every entry point returns a status code instead
+ * SIGINT, 1 = dopr54 forced a step at its smallest allowed size, as the
+ * reference does; the orbit is complete).  Two additions: every entry point returns a status code instead
  * of void, and takes a trailing options pointer (NULL = defaults).
  *
- * Per-orbit err values beyond the reference's: 2 = attempt budget exhausted,
- * 3 = the state became non-finite (the reference loops forever on NaN in
- * DOP853; rows after the failure are NaN here).
+ * Per-orbit err values beyond the reference's: 2 = attempt budget exhausted
+ * (or, in dopr54, a step too small to advance the time, where the reference
+ * loops forever), 3 = the state became non-finite (the reference loops
+ * forever on NaN in DOP853; rows after the failure are NaN here).
  */
 #ifndef GALPY_CUDA_H
 #define GALPY_CUDA_H

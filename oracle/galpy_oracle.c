@@ -14,10 +14,10 @@
  *   RHS      orbit_c_ext/integrateFullOrbit.c:1307-1352 (evalRectForce,
  *            evalRectDeriv), :1496-1681 (the dxdv variants);
  *            orbit_c_ext/integratePlanarOrbit.c:1015-1055, :1124-1276
- *   steppers util/bovy_symplecticode.c:132-377 (leapfrog, symplec4),
- *            :588-809 (their step estimators), :1053-1268 (*_dxdv);
- *            util/bovy_rk.c:66-170,328-395 (rk4 + estimator);
- *            util/leung_dop853.c:231-517 (dop853)
+ *   steppers util/bovy_symplecticode.c:132-587 (leapfrog, symplec4,
+ *            symplec6), :588-1052 (their step estimators), :1053-1400
+ *            (*_dxdv); util/bovy_rk.c:66-480 (rk4, rk6 + estimators),
+ *            :501-760 (dopr54); util/leung_dop853.c:231-517 (dop853)
  *   drivers  integrateFullOrbit.c:1046-1150, :1234-1306;
  *            integratePlanarOrbit.c:743-847, :940-1014
  *   coords   util/bovy_coords.c:57-148
@@ -664,91 +664,6 @@ static double est_scale(int n, const double *v, double rtol, double atol)
   return log(exp(atol - c) + exp(rtol + m - c)) + c;
 }
 
-/* leapfrog_estimate_step (bovy_symplecticode.c:588-664) */
-static double leapfrog_est(rhs_fn f, opot *P, int dim, const double *qo, const double *po,
-                           double dt, double rtol, double atol)
-{
-  double err = 2., init_dt = dt;
-  double q11[MAXD], q12[MAXD], p11[MAXD], p12[MAXD], qt[MAXD], pt[MAXD], a[MAXD];
-  double sq = est_scale(dim, qo, rtol, atol), sp = est_scale(dim, po, rtol, atol);
-  dt *= 2.;
-  while (err > 1. && init_dt / dt < MAX_DT_REDUCE) {
-    dt /= 2.;
-    drift(dim, qo, po, dt / 2., q12);
-    f(P, q12, a);
-    kick(dim, po, dt, a, p11);
-    drift(dim, q12, p11, dt / 2., q11);
-    drift(dim, qo, po, dt / 4., q12);
-    f(P, q12, a);
-    kick(dim, po, dt / 2., a, pt);
-    drift(dim, q12, pt, dt / 2., qt);
-    f(P, qt, a);
-    kick(dim, pt, dt / 2., a, p12);
-    drift(dim, qt, p12, dt / 4., q12);
-    err = 0.;
-    for (int i = 0; i < dim; i++) {
-      err += exp(2. * log(fabs(q11[i] - q12[i])) - 2. * sq);
-      err += exp(2. * log(fabs(p11[i] - p12[i])) - 2. * sp);
-    }
-    err = sqrt(err / 2. / dim);
-  }
-  return dt;
-}
-
-/* symplec4_estimate_step (bovy_symplecticode.c:665-809) */
-static double symplec4_est(rhs_fn f, opot *P, int dim, const double *qo, const double *po,
-                           double dt, double rtol, double atol)
-{
-  const double c1 = S4C[0], c2 = S4C[1], c3 = S4C[2], c4 = S4C[3];
-  const double d1 = S4D[0], d2 = S4D[1], d3 = S4D[2];
-  double err = 2., init_dt = dt;
-  double q11[MAXD], q12[MAXD], p11[MAXD], p12[MAXD], qt[MAXD], pt[MAXD], a[MAXD];
-  double sq = est_scale(dim, qo, rtol, atol), sp = est_scale(dim, po, rtol, atol);
-  dt *= 2.;
-  while (err > 1. && init_dt / dt < MAX_DT_REDUCE) {
-    dt /= 2.;
-    /* one step of dt */
-    drift(dim, qo, po, c1 * dt, q12);
-    f(P, q12, a);
-    kick(dim, po, d1 * dt, a, p12);
-    drift(dim, q12, p12, c2 * dt, qt);
-    f(P, qt, a);
-    kick(dim, p12, d2 * dt, a, pt);
-    drift(dim, qt, pt, c3 * dt, q12);
-    f(P, q12, a);
-    kick(dim, pt, d3 * dt, a, p11);
-    drift(dim, q12, p11, c4 * dt, q11);
-    /* two steps of dt/2 */
-    drift(dim, qo, po, c1 * dt / 2., q12);
-    f(P, q12, a);
-    kick(dim, po, d1 * dt / 2., a, p12);
-    drift(dim, q12, p12, c2 * dt / 2., qt);
-    f(P, qt, a);
-    kick(dim, p12, d2 * dt / 2., a, pt);
-    drift(dim, qt, pt, c3 * dt / 2., q12);
-    f(P, q12, a);
-    kick(dim, pt, d3 * dt / 2., a, p12);
-    drift(dim, q12, p12, (c1 + c4) * dt / 2., qt);
-    f(P, qt, a);
-    kick(dim, p12, d1 * dt / 2., a, pt);
-    drift(dim, qt, pt, c2 * dt / 2., q12);
-    f(P, q12, a);
-    kick(dim, pt, d2 * dt / 2., a, p12);
-    drift(dim, q12, p12, c3 * dt / 2., qt);
-    f(P, qt, a);
-    kick(dim, p12, d3 * dt / 2., a, pt);
-    drift(dim, qt, pt, c4 * dt / 2., q12);
-    for (int i = 0; i < dim; i++) p12[i] = pt[i];
-    err = 0.;
-    for (int i = 0; i < dim; i++) {
-      err += exp(2. * log(fabs(q11[i] - q12[i])) - 2. * sq);
-      err += exp(2. * log(fabs(p11[i] - p12[i])) - 2. * sp);
-    }
-    err = sqrt(err / 2. / dim);
-  }
-  return dt;
-}
-
 /* Output ordering of a symplectic state: plain runs store [q(dim),p(dim)];
    variational runs store [q_base,p_base,q_dev,p_dev] (save_qp_dxdv). */
 static void save_qp(int ndim, int dim_base, const double *q, const double *p, double *out)
@@ -771,14 +686,81 @@ typedef struct {
   int err;
 } ostat;
 
-/* leapfrog / symplec4 (bovy_symplecticode.c:132-377 and the *_dxdv steppers
-   :1053-1268).  f steps the ndim-vector, fb is the base force for the
-   estimator over dim_base components; yo is in save_qp layout. */
-static void symplectic(int order4, rhs_fn f, rhs_fn fb, opot *P, int ndim, int dim_base,
+/* Drift-kick composition schemes: nk kicks d[0..nk-1] between nk+1 drifts
+   c[0..nk] (coefficients of bovy_symplecticode.c:96-104; leapfrog is the
+   scheme c = (1/2, 1/2), d = (1), whose products with dt are the reference's
+   dt/2 and dt exactly). */
+typedef struct {
+  int nk;
+  const double *c, *d;
+} oscheme;
+static const double LFC[2] = {0.5, 0.5}, LFD[1] = {1.0};
+static const double S6C[8] = {0.392256805238780,   0.510043411918458,  -0.471053385409758,
+                              0.687531682525198e-1, 0.687531682525198e-1, -0.471053385409758,
+                              0.510043411918458,   0.392256805238780};
+static const double S6D[7] = {0.784513610477560,   0.235573213359357, -0.117767998417887e1,
+                              0.131518632068391e1, -0.117767998417887e1, 0.235573213359357,
+                              0.784513610477560};
+static const oscheme SCH_LF = {1, LFC, LFD}, SCH_S4 = {3, S4C, S4D}, SCH_S6 = {7, S6C, S6D};
+
+/* nstep steps of size h from (q0, p0) to (q, p): first drift c0 h, kicks and
+   drifts in turn, the last drift of a step merged with the first of the next
+   ((c_nk + c_0) h), the final drift c_nk h.  This is the step sequence of
+   leapfrog / symplec4 / symplec6 (bovy_symplecticode.c:132-587) and of the
+   one- and two-step trials of their estimators (:588-1052). */
+static void comp_advance(const oscheme *S, rhs_fn f, opot *P, int n, const double *q0,
+                         const double *p0, double h, long nstep, double *q, double *p)
+{
+  double a[MAXD];
+  drift(n, q0, p0, S->c[0] * h, q);
+  for (int k = 0; k < n; k++) p[k] = p0[k];
+  for (long s = 0; s < nstep; s++) {
+    for (int j = 0; j < S->nk; j++) {
+      f(P, q, a);
+      kick(n, p, S->d[j] * h, a, p);
+      double c;
+      if (j < S->nk - 1)
+        c = S->c[j + 1] * h;
+      else
+        c = (s < nstep - 1) ? (S->c[S->nk] + S->c[0]) * h : S->c[S->nk] * h;
+      drift(n, q, p, c, q);
+    }
+  }
+}
+
+/* leapfrog_estimate_step / symplec4_estimate_step / symplec6_estimate_step
+   (bovy_symplecticode.c:588-664, 665-809, 810-1052): halve dt until one step
+   and two half steps agree to the tolerance */
+static double comp_est(const oscheme *S, rhs_fn f, opot *P, int dim, const double *qo,
+                       const double *po, double dt, double rtol, double atol)
+{
+  double err = 2., init_dt = dt;
+  double q11[MAXD], q12[MAXD], p11[MAXD], p12[MAXD];
+  double sq = est_scale(dim, qo, rtol, atol), sp = est_scale(dim, po, rtol, atol);
+  dt *= 2.;
+  while (err > 1. && init_dt / dt < MAX_DT_REDUCE) {
+    dt /= 2.;
+    comp_advance(S, f, P, dim, qo, po, dt, 1, q11, p11);
+    comp_advance(S, f, P, dim, qo, po, dt / 2., 2, q12, p12);
+    err = 0.;
+    for (int i = 0; i < dim; i++) {
+      err += exp(2. * log(fabs(q11[i] - q12[i])) - 2. * sq);
+      err += exp(2. * log(fabs(p11[i] - p12[i])) - 2. * sp);
+    }
+    err = sqrt(err / 2. / dim);
+  }
+  return dt;
+}
+
+/* leapfrog / symplec4 / symplec6 (bovy_symplecticode.c:132-587 and the
+   *_dxdv steppers :1053-1400).  f steps the ndim-vector, fb is the base
+   force for the estimator over dim_base components; yo is in save_qp
+   layout. */
+static void symplectic(const oscheme *S, rhs_fn f, rhs_fn fb, opot *P, int ndim, int dim_base,
                        const double *yo, int nt, double dt, const double *t, double rtol,
                        double atol, double *result, ostat *st)
 {
-  double qo[MAXD], po[MAXD], q12[MAXD], p12[MAXD], a[MAXD];
+  double qo[MAXD], po[MAXD];
   int nb = ndim / dim_base;
   for (int b = 0; b < nb; b++)
     for (int k = 0; k < dim_base; k++) {
@@ -789,61 +771,13 @@ static void symplectic(int order4, rhs_fn f, rhs_fn fb, opot *P, int ndim, int d
   result += 2 * ndim;
   st->err = 0;
   double init_dt = t[1] - t[0];
-  if (dt == DT_SENTINEL)
-    dt = order4 ? symplec4_est(fb, P, dim_base, qo, po, init_dt, rtol, atol)
-                : leapfrog_est(fb, P, dim_base, qo, po, init_dt, rtol, atol);
+  if (dt == DT_SENTINEL) dt = comp_est(S, fb, P, dim_base, qo, po, init_dt, rtol, atol);
   long ndt = (long)(init_dt / dt);
-  if (!order4) {
-    for (int ii = 0; ii < nt - 1; ii++) {
-      drift(ndim, qo, po, dt / 2., q12);
-      for (long jj = 0; jj < ndt - 1; jj++) {
-        f(P, q12, a);
-        kick(ndim, po, dt, a, p12);
-        drift(ndim, q12, p12, dt, qo);
-        for (int k = 0; k < ndim; k++) {
-          q12[k] = qo[k];
-          po[k] = p12[k];
-        }
-      }
-      f(P, q12, a);
-      kick(ndim, po, dt, a, po);
-      drift(ndim, q12, po, dt / 2., qo);
-      save_qp(ndim, dim_base, qo, po, result);
-      result += 2 * ndim;
-    }
-  } else {
-    const double c1 = S4C[0], c2 = S4C[1], c3 = S4C[2], c4 = S4C[3];
-    const double d1 = S4D[0], d2 = S4D[1], d3 = S4D[2];
-    for (int ii = 0; ii < nt - 1; ii++) {
-      drift(ndim, qo, po, c1 * dt, q12);
-      for (long jj = 0; jj < ndt - 1; jj++) {
-        f(P, q12, a);
-        kick(ndim, po, d1 * dt, a, p12);
-        drift(ndim, q12, p12, c2 * dt, qo);
-        f(P, qo, a);
-        kick(ndim, p12, d2 * dt, a, po);
-        drift(ndim, qo, po, c3 * dt, q12);
-        f(P, q12, a);
-        kick(ndim, po, d3 * dt, a, p12);
-        drift(ndim, q12, p12, (c4 + c1) * dt, qo);
-        for (int k = 0; k < ndim; k++) {
-          q12[k] = qo[k];
-          po[k] = p12[k];
-        }
-      }
-      f(P, q12, a);
-      kick(ndim, po, d1 * dt, a, p12);
-      drift(ndim, q12, p12, c2 * dt, qo);
-      f(P, qo, a);
-      kick(ndim, p12, d2 * dt, a, po);
-      drift(ndim, qo, po, c3 * dt, q12);
-      f(P, q12, a);
-      kick(ndim, po, d3 * dt, a, p12);
-      drift(ndim, q12, p12, c4 * dt, qo);
-      for (int k = 0; k < ndim; k++) po[k] = p12[k];
-      save_qp(ndim, dim_base, qo, po, result);
-      result += 2 * ndim;
-    }
+  if (ndt < 1) ndt = 1; /* the reference's loop always makes the output step */
+  for (int ii = 0; ii < nt - 1; ii++) {
+    comp_advance(S, f, P, ndim, qo, po, dt, ndt, qo, po);
+    save_qp(ndim, dim_base, qo, po, result);
+    result += 2 * ndim;
   }
   st->nsteps = (long long)ndt * (nt - 1);
 }
@@ -865,53 +799,247 @@ static void rk4_onestep(rhs_fn f, opot *P, int dim, const double *yn, double *yn
   for (int i = 0; i < dim; i++) yn1[i] += dt * a[i] / 6.;
 }
 
-/* rk4_estimate_step (bovy_rk.c:328-395) */
-static double rk4_est(rhs_fn f, opot *P, int dim, const double *yo, double dt, double rtol,
-                      double atol)
+/* bovy_rk6_onestep (bovy_rk.c:256-327): seven stages, weights
+   (11, 0, 81, 81, -32, -32, 11)/120 accumulated into yn1 stage by stage */
+static void rk6_onestep(rhs_fn f, opot *P, int dim, const double *yn, double *yn1, double dt,
+                        double *ynk, double *a)
+{
+  double k1[MAXD], k2[MAXD], k3[MAXD], k4[MAXD], k5[MAXD];
+  f(P, yn, a);
+  for (int i = 0; i < dim; i++) {
+    yn1[i] += 11. * dt * a[i] / 120.;
+    k1[i] = dt * a[i];
+    ynk[i] = yn[i] + k1[i] / 3.;
+  }
+  f(P, ynk, a);
+  for (int i = 0; i < dim; i++) {
+    k2[i] = dt * a[i];
+    ynk[i] = yn[i] + 2. * k2[i] / 3.;
+  }
+  f(P, ynk, a);
+  for (int i = 0; i < dim; i++) {
+    yn1[i] += 81. * dt * a[i] / 120.;
+    k3[i] = dt * a[i];
+    ynk[i] = yn[i] + (k1[i] + 4. * k2[i] - k3[i]) / 12.;
+  }
+  f(P, ynk, a);
+  for (int i = 0; i < dim; i++) {
+    yn1[i] += 81. * dt * a[i] / 120.;
+    k4[i] = dt * a[i];
+    ynk[i] = yn[i] + (-k1[i] + 18. * k2[i] - 3. * k3[i] - 6. * k4[i]) / 16.;
+  }
+  f(P, ynk, a);
+  for (int i = 0; i < dim; i++) {
+    yn1[i] -= 32. * dt * a[i] / 120.;
+    k5[i] = dt * a[i];
+    ynk[i] = yn[i] + (9. * k2[i] - 3. * k3[i] - 6. * k4[i] + 4. * k5[i]) / 8.;
+  }
+  f(P, ynk, a);
+  for (int i = 0; i < dim; i++) {
+    yn1[i] -= 32. * dt * a[i] / 120.;
+    const double k6 = dt * a[i];
+    ynk[i] = yn[i] + (9. * k1[i] - 36. * k2[i] + 63. * k3[i] + 72. * k4[i] - 64. * k6) / 44.;
+  }
+  f(P, ynk, a);
+  for (int i = 0; i < dim; i++) yn1[i] += 11. * dt * a[i] / 120.;
+}
+
+typedef void (*rk_step_fn)(rhs_fn f, opot *P, int dim, const double *yn, double *yn1, double dt,
+                           double *ynk, double *a);
+
+/* rk4_estimate_step / rk6_estimate_step (bovy_rk.c:328-395, 396-480): divide
+   dt by ceil(err^(1/(order+1))) until one step and two half steps agree */
+static double rk_est(rk_step_fn onestep, double expo, rhs_fn f, opot *P, int dim,
+                     const double *yo, double dt, double rtol, double atol)
 {
   double err = 2., init_dt = dt;
   double yn[MAXD], y1[MAXD], y21[MAXD], y2[MAXD], ynk[MAXD], a[MAXD];
   double s = est_scale(dim, yo, rtol, atol);
   while (err > 1.) {
     for (int i = 0; i < dim; i++) yn[i] = y1[i] = y21[i] = yo[i];
-    rk4_onestep(f, P, dim, yn, y1, dt, ynk, a);
-    rk4_onestep(f, P, dim, yn, y21, dt / 2., ynk, a);
+    onestep(f, P, dim, yn, y1, dt, ynk, a);
+    onestep(f, P, dim, yn, y21, dt / 2., ynk, a);
     for (int i = 0; i < dim; i++) y2[i] = y21[i];
-    rk4_onestep(f, P, dim, y21, y2, dt / 2., ynk, a);
+    onestep(f, P, dim, y21, y2, dt / 2., ynk, a);
     err = 0.;
     for (int i = 0; i < dim; i++) err += exp(2. * log(fabs(y1[i] - y2[i])) - 2. * s);
     err = sqrt(err / dim);
-    if (ceil(pow(err, 1. / 5.)) > 1. && init_dt / dt * ceil(pow(err, 1. / 5.)) < MAX_DT_REDUCE)
-      dt /= ceil(pow(err, 1. / 5.));
+    if (ceil(pow(err, expo)) > 1. && init_dt / dt * ceil(pow(err, expo)) < MAX_DT_REDUCE)
+      dt /= ceil(pow(err, expo));
     else
       break;
   }
   return dt;
 }
 
-/* bovy_rk4 (bovy_rk.c:66-141) */
-static void rk4(rhs_fn f, opot *P, int dim, const double *yo, int nt, double dt, const double *t,
-                double rtol, double atol, double *result, ostat *st)
+/* bovy_rk4 / bovy_rk6 (bovy_rk.c:66-141, 171-255) */
+static void rk_fixed(int order, rhs_fn f, opot *P, int dim, const double *yo, int nt, double dt,
+                     const double *t, double rtol, double atol, double *result, ostat *st)
 {
+  rk_step_fn onestep = order == 6 ? rk6_onestep : rk4_onestep;
   double yn[MAXD], yn1[MAXD], ynk[MAXD], a[MAXD];
   for (int i = 0; i < dim; i++) result[i] = yo[i];
   result += dim;
   st->err = 0;
   for (int i = 0; i < dim; i++) yn[i] = yn1[i] = yo[i];
   double init_dt = t[1] - t[0];
-  if (dt == DT_SENTINEL) dt = rk4_est(f, P, dim, yo, init_dt, rtol, atol);
+  if (dt == DT_SENTINEL)
+    dt = rk_est(onestep, order == 6 ? 1. / 7. : 1. / 5., f, P, dim, yo, init_dt, rtol, atol);
   long ndt = (long)(init_dt / dt);
   for (int ii = 0; ii < nt - 1; ii++) {
     for (long jj = 0; jj < ndt - 1; jj++) {
-      rk4_onestep(f, P, dim, yn, yn1, dt, ynk, a);
+      onestep(f, P, dim, yn, yn1, dt, ynk, a);
       for (int k = 0; k < dim; k++) yn[k] = yn1[k];
     }
-    rk4_onestep(f, P, dim, yn, yn1, dt, ynk, a);
+    onestep(f, P, dim, yn, yn1, dt, ynk, a);
     for (int k = 0; k < dim; k++) result[k] = yn1[k];
     result += dim;
     for (int k = 0; k < dim; k++) yn[k] = yn1[k];
   }
   st->nsteps = (long long)ndt * (nt - 1);
+}
+
+/* Dormand-Prince 5(4) tableau (bovy_rk.c:630-665) */
+#define DP5_A21 0.2
+#define DP5_A31 (3. / 40.)
+#define DP5_A32 (9. / 40.)
+#define DP5_A41 (44. / 45.)
+#define DP5_A42 (-56. / 15.)
+#define DP5_A43 (32. / 9.)
+#define DP5_A51 (19372. / 6561.)
+#define DP5_A52 (-25360. / 2187.)
+#define DP5_A53 (64448. / 6561.)
+#define DP5_A54 (-212. / 729.)
+#define DP5_A61 (9017. / 3168.)
+#define DP5_A62 (-355. / 33.)
+#define DP5_A63 (46732. / 5247.)
+#define DP5_A64 (49. / 176.)
+#define DP5_A65 (-5103. / 18656.)
+#define DP5_B1 (35. / 384.)
+#define DP5_B3 (500. / 1113.)
+#define DP5_B4 (125. / 192.)
+#define DP5_B5 (-2187. / 6784.)
+#define DP5_B6 (11. / 84.)
+#define DP5_E1 (DP5_B1 - 5179. / 57600.)
+#define DP5_E3 (DP5_B3 - 7571. / 16695.)
+#define DP5_E4 (DP5_B4 - 393. / 640.)
+#define DP5_E5 (DP5_B5 + 92097. / 339200.)
+#define DP5_E6 (DP5_B6 - 187. / 2100.)
+#define DP5_E7 (-1. / 40.)
+
+/* bovy_dopr54_actualstep (bovy_rk.c:617-760): one attempt of size dt from
+   (yo, a1 = f(yo)); on acceptance (the power-of-two step factor is >= 1, or
+   the attempt is forced) yo, a1 and *to advance.  Returns the next step. */
+static double dopr54_attempt(rhs_fn f, opot *P, int dim, double *yo, double *a1, double dt,
+                             double *to, double rtol, double atol, int accept, ostat *st)
+{
+  double k1[MAXD], k2[MAXD], k3[MAXD], k4[MAXD], k5[MAXD], k6[MAXD];
+  double yn1[MAXD], yerr[MAXD], ynk[MAXD], a[MAXD];
+  int i;
+  for (i = 0; i < dim; i++) {
+    yn1[i] = yo[i];
+    k1[i] = dt * a1[i];
+    yn1[i] += DP5_B1 * k1[i];
+    yerr[i] = DP5_E1 * k1[i];
+    ynk[i] = yo[i] + DP5_A21 * k1[i];
+  }
+  f(P, ynk, a);
+  for (i = 0; i < dim; i++) {
+    k2[i] = dt * a[i];
+    ynk[i] = yo[i] + DP5_A31 * k1[i] + DP5_A32 * k2[i];
+  }
+  f(P, ynk, a);
+  for (i = 0; i < dim; i++) {
+    k3[i] = dt * a[i];
+    yn1[i] += DP5_B3 * k3[i];
+    yerr[i] += DP5_E3 * k3[i];
+    ynk[i] = yo[i] + DP5_A41 * k1[i] + DP5_A42 * k2[i] + DP5_A43 * k3[i];
+  }
+  f(P, ynk, a);
+  for (i = 0; i < dim; i++) {
+    k4[i] = dt * a[i];
+    yn1[i] += DP5_B4 * k4[i];
+    yerr[i] += DP5_E4 * k4[i];
+    ynk[i] = yo[i] + DP5_A51 * k1[i] + DP5_A52 * k2[i] + DP5_A53 * k3[i] + DP5_A54 * k4[i];
+  }
+  f(P, ynk, a);
+  for (i = 0; i < dim; i++) {
+    k5[i] = dt * a[i];
+    yn1[i] += DP5_B5 * k5[i];
+    yerr[i] += DP5_E5 * k5[i];
+    ynk[i] = yo[i] + DP5_A61 * k1[i] + DP5_A62 * k2[i] + DP5_A63 * k3[i] + DP5_A64 * k4[i] +
+             DP5_A65 * k5[i];
+  }
+  f(P, ynk, a);
+  for (i = 0; i < dim; i++) {
+    k6[i] = dt * a[i];
+    yn1[i] += DP5_B6 * k6[i];
+    yerr[i] += DP5_E6 * k6[i];
+    /* the seventh stage point uses the b weights as its a7j (a72 = 0) */
+    ynk[i] = yo[i] + DP5_B1 * k1[i] + DP5_B3 * k3[i] + DP5_B4 * k4[i] + DP5_B5 * k5[i] +
+             DP5_B6 * k6[i];
+  }
+  f(P, ynk, a);
+  for (i = 0; i < dim; i++) yerr[i] += DP5_E7 * dt * a[i];
+  double s = est_scale(dim, yo, rtol, atol);
+  double err = 0.;
+  for (i = 0; i < dim; i++) err += exp(2. * log(fabs(yerr[i])) - 2. * s);
+  err = sqrt(err / dim);
+  double corr = 0.85 * pow(err, -.2);
+  double powertwo = round(log(corr) / log(2.));
+  if (powertwo > 3.)
+    powertwo = 3.;
+  else if (powertwo < -3.)
+    powertwo = -3.;
+  if (powertwo >= 0. || accept) {
+    for (i = 0; i < dim; i++) {
+      a1[i] = a[i];
+      yo[i] = yn1[i];
+    }
+    *to += dt;
+    st->nsteps++;
+  }
+  return dt * pow(2., powertwo);
+}
+
+/* bovy_dopr54 (bovy_rk.c:501-616): adaptive steps, each output interval
+   ended by a step clipped to its end; a step that would shrink below the
+   interval's first step / 10000 (or is NaN) is forced at that size and
+   flags err = 1.  The first step comes from rk4_estimate_step. */
+static void dopr54(rhs_fn f, opot *P, int dim, const double *yin, int nt, double dt_one,
+                   const double *t, double rtol, double atol, double *result, ostat *st)
+{
+  double yo[MAXD], a1[MAXD];
+  for (int i = 0; i < dim; i++) yo[i] = result[i] = yin[i];
+  result += dim;
+  st->err = 0;
+  st->nsteps = 0;
+  double dt = t[1] - t[0];
+  if (dt_one == DT_SENTINEL) dt_one = rk_est(rk4_onestep, 1. / 5., f, P, dim, yo, dt, rtol, atol);
+  double to = t[0];
+  f(P, yo, a1);
+  long long attempts = 0;
+  for (int ii = 0; ii < nt - 1; ii++) {
+    double init_dt_one = dt_one, init_to = to;
+    while ((dt >= 0. && to < (init_to + dt)) || (dt < 0. && to > (init_to + dt))) {
+      if (st->max_attempts > 0 && attempts >= st->max_attempts) {
+        st->err = 2;
+        return;
+      }
+      attempts++;
+      int accept = 0;
+      if (init_dt_one / dt_one > MAX_DT_REDUCE || dt_one != dt_one) {
+        dt_one = init_dt_one / MAX_DT_REDUCE;
+        accept = 1;
+        if (st->err % 2 == 0) st->err += 1;
+      }
+      if (dt >= 0. && dt_one > (init_to + dt - to)) dt_one = (init_to + dt - to);
+      if (dt < 0. && dt_one < (init_to + dt - to)) dt_one = (init_to + dt - to);
+      dt_one = dopr54_attempt(f, P, dim, yo, a1, dt_one, &to, rtol, atol, accept, st);
+    }
+    for (int i = 0; i < dim; i++) result[i] = yo[i];
+    result += dim;
+  }
 }
 
 #define DMAX(a, b) (((a) > (b)) ? (a) : (b))
@@ -1164,9 +1292,12 @@ static int run_plain(opot *P, int planar, int method, const double *w, int nt, c
   rhs_fn force = planar ? rect_force2 : rect_force3;
   rhs_fn deriv = planar ? rect_deriv2 : rect_deriv3;
   switch (method) {
-  case 0: symplectic(0, force, force, P, dim, dim, w, nt, dt, t, rtol, atol, out, st); return 0;
-  case 3: symplectic(1, force, force, P, dim, dim, w, nt, dt, t, rtol, atol, out, st); return 0;
-  case 1: rk4(deriv, P, 2 * dim, w, nt, dt, t, rtol, atol, out, st); return 0;
+  case 0: symplectic(&SCH_LF, force, force, P, dim, dim, w, nt, dt, t, rtol, atol, out, st); return 0;
+  case 3: symplectic(&SCH_S4, force, force, P, dim, dim, w, nt, dt, t, rtol, atol, out, st); return 0;
+  case 4: symplectic(&SCH_S6, force, force, P, dim, dim, w, nt, dt, t, rtol, atol, out, st); return 0;
+  case 1: rk_fixed(4, deriv, P, 2 * dim, w, nt, dt, t, rtol, atol, out, st); return 0;
+  case 2: rk_fixed(6, deriv, P, 2 * dim, w, nt, dt, t, rtol, atol, out, st); return 0;
+  case 5: dopr54(deriv, P, 2 * dim, w, nt, dt, t, rtol, atol, out, st); return 0;
   case 6: dop853(deriv, P, 2 * dim, w, nt, t, rtol, atol, out, st); return 0;
   }
   return -1;
@@ -1175,8 +1306,8 @@ static int run_plain(opot *P, int planar, int method, const double *w, int nt, c
 /* Batched integration with galpy's layout (integrateFullOrbit.c:1046 /
    integratePlanarOrbit.c:743): yo [nobj][6] (R,vR,vT,z,vz,phi) or [nobj][4]
    (R,vR,vT,phi), overwritten with rectangular ICs like the reference;
-   result [nobj][nt][6|4] cylindrical.  method: 0 leapfrog, 1 rk4,
-   3 symplec4, 6 dop853.  nsteps/nforce (optional) receive per-orbit counts.
+   result [nobj][nt][6|4] cylindrical.  method: 0 leapfrog, 1 rk4, 2 rk6,
+   3 symplec4, 4 symplec6, 5 dopr54, 6 dop853.  nsteps/nforce (optional) receive per-orbit counts.
    Returns 0, -2 unsupported method, -3 unsupported potential. */
 EXPORT int oracle_integrate(int planar, int nobj, double *yo, int nt, const double *t,
                             int indiv_t, int npot, const int *pot_type, const double *pot_args,
@@ -1186,7 +1317,7 @@ EXPORT int oracle_integrate(int planar, int nobj, double *yo, int nt, const doub
 {
   opot P0;
   if (opot_decode(&P0, npot, pot_type, pot_args, planar)) return -3;
-  if (method != 0 && method != 1 && method != 3 && method != 6) return -2;
+  if (method < 0 || method > 6) return -2;
   int nv = planar ? 4 : 6;
   int bad = 0;
 #ifdef _OPENMP
@@ -1230,7 +1361,7 @@ EXPORT int oracle_integrate_dxdv(int planar, int nobj, const double *yo, int nt,
 {
   opot P0;
   if (opot_decode(&P0, npot, pot_type, pot_args, planar)) return -3;
-  if (method != 0 && method != 1 && method != 3 && method != 6) return -2;
+  if (method < 0 || method > 6) return -2;
   int dim = planar ? 2 : 3, nv = 4 * dim;
 #ifdef _OPENMP
   if (nthreads <= 0) nthreads = omp_get_max_threads();
@@ -1246,9 +1377,12 @@ EXPORT int oracle_integrate_dxdv(int planar, int nobj, const double *yo, int nt,
     rhs_fn fb = planar ? rect_force2 : rect_force3;
     rhs_fn fd = planar ? rect_deriv2_dxdv : rect_deriv3_dxdv;
     switch (method) {
-    case 0: symplectic(0, fa, fb, &P, 2 * dim, dim, w, nt, dt, tt, rtol, atol, out, &st); break;
-    case 3: symplectic(1, fa, fb, &P, 2 * dim, dim, w, nt, dt, tt, rtol, atol, out, &st); break;
-    case 1: rk4(fd, &P, nv, w, nt, dt, tt, rtol, atol, out, &st); break;
+    case 0: symplectic(&SCH_LF, fa, fb, &P, 2 * dim, dim, w, nt, dt, tt, rtol, atol, out, &st); break;
+    case 3: symplectic(&SCH_S4, fa, fb, &P, 2 * dim, dim, w, nt, dt, tt, rtol, atol, out, &st); break;
+    case 4: symplectic(&SCH_S6, fa, fb, &P, 2 * dim, dim, w, nt, dt, tt, rtol, atol, out, &st); break;
+    case 1: rk_fixed(4, fd, &P, nv, w, nt, dt, tt, rtol, atol, out, &st); break;
+    case 2: rk_fixed(6, fd, &P, nv, w, nt, dt, tt, rtol, atol, out, &st); break;
+    case 5: dopr54(fd, &P, nv, w, nt, dt, tt, rtol, atol, out, &st); break;
     case 6: dop853(fd, &P, nv, w, nt, tt, rtol, atol, out, &st); break;
     }
     err[ii] = st.err;

@@ -22,7 +22,8 @@ PORT_SO = os.path.join(_HERE, "liboracle.so")
 REF_SO = os.path.join(_HERE, "_ref", "libgalpy_ref.so")
 
 DT_SENTINEL = -9999.99
-METHODS = {"leapfrog": 0, "rk4": 1, "symplec4": 3, "dop853": 6}
+METHODS = {"leapfrog": 0, "rk4": 1, "rk6": 2, "symplec4": 3, "symplec6": 4, "dopr54": 5,
+           "dop853": 6}
 
 _port = None
 _ref = None

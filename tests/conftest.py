@@ -64,7 +64,8 @@ def harness():
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
 _lp = ctypes.POINTER(ctypes.c_longlong)
-METHOD_CODES = {"leapfrog": 0, "rk4": 1, "symplec4": 3, "dop853": 6}
+METHOD_CODES = {"leapfrog": 0, "rk4": 1, "rk6": 2, "symplec4": 3, "symplec6": 4, "dopr54": 5,
+                "dop853": 6}
 
 
 class Harness:

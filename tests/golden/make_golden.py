@@ -115,7 +115,7 @@ def main():
     ics = seeded_ics(8, 0)
     ics2 = seeded_ics(8, 1, planar=True)
     out["c_ics"], out["c_ics_planar"] = ics, ics2
-    for m in ("leapfrog", "rk4", "symplec4", "dop853"):
+    for m in ("leapfrog", "rk4", "rk6", "symplec4", "symplec6", "dopr54", "dop853"):
         t = np.linspace(0, 5, 51)
         res, err, _, _ = O.integrate(ics, t, pt, pa, m, impl="ref")
         out[f"c_{m}_3d"] = res
@@ -127,6 +127,14 @@ def main():
     out["c_indiv_t"] = tt
     res, _, _, _ = O.integrate(ics, tt, pt, pa, "dop853", rtol=1e-10, atol=1e-10, impl="ref")
     out["c_dop853_indiv"] = res
+    res, _, _, _ = O.integrate(ics, tt, pt, pa, "dopr54", rtol=1e-10, atol=1e-10, impl="ref")
+    out["c_dopr54_indiv"] = res
+    # dopr54's forced steps: one output interval of 50 started with an
+    # explicit step of 50 at an unreachable tolerance, so every orbit ends up
+    # at the smallest allowed step (interval's first step / 10000), err = 1
+    res, err, _, _ = O.integrate(ics, np.array([0.0, 50.0]), pt, pa, "dopr54", dt=50.0,
+                                 rtol=1e-20, atol=1e-20, impl="ref")
+    out["c_dopr54_forced"], out["c_dopr54_forced_err"] = res, err
     # variational
     w = np.zeros((6, 12))
     w[:, :6] = cyl_to_rect(ics[:6])
@@ -136,7 +144,7 @@ def main():
     w2[np.arange(4), 4 + np.arange(4)] = 1.0
     out["c_dxdv_w3"], out["c_dxdv_w2"] = w, w2
     t = np.linspace(0, 3, 31)
-    for m in ("leapfrog", "rk4", "symplec4", "dop853"):
+    for m in ("leapfrog", "rk4", "rk6", "symplec4", "symplec6", "dopr54", "dop853"):
         res, _, _ = O.integrate_dxdv(w, t, pt, pa, m, impl="ref")
         out[f"c_{m}_dxdv3"] = res
         res, _, _ = O.integrate_dxdv(w2, t, pt2, pa2, m, planar=True, impl="ref")

@@ -60,22 +60,19 @@ int dispatch(int method, int nobj, const double* w, int nt, const double* t, int
              double* out, int* err, long long* ns)
 {
   switch (method) {
-    case M_LEAPFROG:
-      run_all<SymplecticMachine<D, VAR, false>, D, PREC, VAR, POT>(nobj, w, nt, t, indiv_t, c, n, dt,
-                                                              rtol, atol, ma, out, err, ns);
-      return 0;
-    case M_SYMPLEC4:
-      run_all<SymplecticMachine<D, VAR, true>, D, PREC, VAR, POT>(nobj, w, nt, t, indiv_t, c, n, dt,
-                                                             rtol, atol, ma, out, err, ns);
-      return 0;
-    case M_RK4:
-      run_all<RK4Machine<D, VAR>, D, PREC, VAR, POT>(nobj, w, nt, t, indiv_t, c, n, dt, rtol, atol,
-                                                ma, out, err, ns);
-      return 0;
-    case M_DOP853:
-      run_all<Dop853Machine<D, VAR>, D, PREC, VAR, POT>(nobj, w, nt, t, indiv_t, c, n, dt, rtol,
-                                                   atol, ma, out, err, ns);
-      return 0;
+#define HARNESS_CASE(code, ...)                                                                  \
+  case code:                                                                                     \
+    run_all<__VA_ARGS__, D, PREC, VAR, POT>(nobj, w, nt, t, indiv_t, c, n, dt, rtol, atol, ma, \
+                                            out, err, ns);                                       \
+    return 0;
+    HARNESS_CASE(M_LEAPFROG, SymplecticMachine<D, VAR, 2>)
+    HARNESS_CASE(M_SYMPLEC4, SymplecticMachine<D, VAR, 4>)
+    HARNESS_CASE(M_SYMPLEC6, SymplecticMachine<D, VAR, 6>)
+    HARNESS_CASE(M_RK4, RKMachine<D, VAR, 4>)
+    HARNESS_CASE(M_RK6, RKMachine<D, VAR, 6>)
+    HARNESS_CASE(M_DOPR54, Dopr54Machine<D, VAR>)
+    HARNESS_CASE(M_DOP853, Dop853Machine<D, VAR>)
+#undef HARNESS_CASE
   }
   return -2;
 }

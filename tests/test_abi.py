@@ -71,7 +71,7 @@ def test_unsupported_method_is_reported(mw14):
     pt = np.ascontiguousarray(mw14[0], np.int32)
     pa = np.ascontiguousarray(mw14[1], np.float64)
     dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
-    for code in (2, 4, 5, 7):  # rk6, symplec6, dopr54, ias15: galpy falls back
+    for code in (7, 8, -1):  # ias15 (galpy falls back) and codes galpy does not have
         rc = lib.integrateFullOrbit_cuda(1, yo.ctypes.data_as(dp), 11, t.ctypes.data_as(dp), 0, 3,
                                          pt.ctypes.data_as(ip), pa.ctypes.data_as(dp), None,
                                          -9999.99, -27.6, -27.6, res.ctypes.data_as(dp),
@@ -84,8 +84,11 @@ def test_parse_integrator_and_tolerances():
     assert galpy_b200.parse_integrator("DOP853_CUDA") == 6
     assert galpy_b200.parse_integrator("leapfrog_c") == 0
     assert galpy_b200.parse_integrator("rk4") == 1
+    assert galpy_b200.parse_integrator("dopr54_cuda") == 5
+    assert galpy_b200.parse_integrator("symplec6_c") == 4
+    assert galpy_b200.parse_integrator("rk6") == 2
     with pytest.raises(ValueError):
-        galpy_b200.parse_integrator("dopr54_cuda")
+        galpy_b200.parse_integrator("ias15_cuda")
     r, a = galpy_b200.parse_tol(None, 1e-10)
     assert r == pytest.approx(-12 * np.log(10)) and a == pytest.approx(np.log(1e-10))
 

@@ -16,7 +16,7 @@ import galpy_b200 as gb
 from galpy_b200 import _lib
 
 pytestmark = pytest.mark.gpu
-METHODS = ["leapfrog", "rk4", "symplec4", "dop853"]
+METHODS = ["leapfrog", "rk4", "rk6", "symplec4", "symplec6", "dopr54", "dop853"]
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -142,6 +142,47 @@ def test_dop853_ragged_times(oracle, mw14):
     assert (d / scale).max() < 1e-7
 
 
+def test_dopr54_golden_vectors(golden):
+    """dopr54 against the reference's own C: per-orbit time grids, and the
+    smallest-step rule (every step forced at the interval's first step /
+    10000, err = 1 on every orbit)."""
+    pt, pa = golden["mw14_type"], golden["mw14_args"]
+    out, err, ns = gb.integrateFullOrbit_cuda((pt, pa), golden["c_ics"].copy(),
+                                              golden["c_indiv_t"], "dopr54_cuda", rtol=1e-10,
+                                              atol=1e-10, progressbar=False, return_nsteps=True)
+    assert not err.any()
+    assert cyl_diff(golden["c_dopr54_indiv"], out).max() < 1e-10
+    out, err, ns = gb.integrateFullOrbit_cuda((pt, pa), golden["c_ics"].copy(),
+                                              np.array([0.0, 50.0]), "dopr54_cuda", dt=50.0,
+                                              rtol=1e-20, atol=1e-20, progressbar=False,
+                                              return_nsteps=True)
+    assert np.array_equal(err, golden["c_dopr54_forced_err"]) and np.all(ns == 10000)
+    assert cyl_diff(golden["c_dopr54_forced"], out).max() < 1e-10
+
+
+@pytest.mark.parametrize("method", ["rk6", "symplec6", "dopr54"])
+def test_generic_potentials_and_fixed_dt(oracle, golden, method):
+    """Kernels that walk the component list at run time (a triaxial
+    logarithmic halo plus a Hernquist sphere), an explicit dt, and the
+    float32-force variant."""
+    pt = np.concatenate([golden["logtri_type"], golden["hernquist_type"]])
+    pa = np.concatenate([golden["logtri_args"], golden["hernquist_args"]])
+    ics = seeded_ics(128, 36)
+    t = np.linspace(0, 10, 41)
+    for dt in (None, 0.01):
+        ref, _, nref, _ = oracle.integrate(ics, t, pt, pa, method, dt=dt)
+        out, err, ns = gb.integrateFullOrbit_cuda((pt, pa), ics.copy(), t, cuda(method), dt=dt,
+                                                  progressbar=False, return_nsteps=True)
+        assert not err.any()
+        same = ns == nref
+        assert same.mean() >= 0.99
+        assert cyl_diff(ref, out).max(axis=(1, 2))[same].max() < 1e-10
+    f32, err = gb.integrateFullOrbit_cuda((pt, pa), ics.copy(), t, cuda(method), dt=0.01,
+                                          progressbar=False, precision="f32force")
+    d = cyl_diff(out, f32)[..., :5].max()
+    assert not err.any() and 0 < d < 1e-4, d
+
+
 def test_device_api_soa_matches_galpy_layout(mw14):
     import torch
 
@@ -251,9 +292,14 @@ def test_edge_cases(mw14, oracle):
     out, err = gb.integrateFullOrbit_cuda((pt, pa), seeded_ics(4, 34), np.linspace(0, 100, 11),
                                           "dop853_cuda", max_attempts=30, progressbar=False)
     assert np.all(err == 2) and np.isnan(out[:, -1]).all()
+    # dopr54 with a step too small to advance the time (t near 1e17): err 2
+    out, err = gb.integrateFullOrbit_cuda((pt, pa), seeded_ics(3, 36),
+                                          1e17 + np.array([0.0, 128.0, 256.0]), "dopr54_cuda",
+                                          dt=1.0, progressbar=False)
+    assert np.all(err == 2) and np.isnan(out[:, 1:]).all()
     # unsupported method and potential: typed errors
     with pytest.raises(ValueError):
-        gb.integrateFullOrbit_cuda((pt, pa), seeded_ics(2, 35), t, "dopr54_cuda")
+        gb.integrateFullOrbit_cuda((pt, pa), seeded_ics(2, 35), t, "ias15_cuda")
     with pytest.raises(gb.PotentialNotSupported):
         gb.integrateFullOrbit_cuda(([14], [1.0, 1.0]), seeded_ics(2, 35), t, "dop853_cuda")
 

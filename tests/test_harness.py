@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 from helpers import cyl_diff, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
 
-METHODS = ["leapfrog", "rk4", "symplec4", "dop853"]
+METHODS = ["leapfrog", "rk4", "rk6", "symplec4", "symplec6", "dopr54", "dop853"]
 POTS = ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"]
 
 
@@ -120,13 +120,24 @@ def test_variational_vs_oracle(harness, oracle, mw14, mw14_planar, method, plana
     assert (np.abs(out - ref) / scale).max() < 1e-10
 
 
-def test_dop853_per_orbit_times(harness, oracle, golden):
+@pytest.mark.parametrize("method", ["dop853", "dopr54"])
+def test_adaptive_per_orbit_times(harness, oracle, golden, method):
     pt, pa = golden["mw14_type"], golden["mw14_args"]
     ics = golden["c_ics"]
-    out, err, _ = harness.integrate(cyl_to_rect(ics), golden["c_indiv_t"], pt, pa, "dop853",
+    out, err, _ = harness.integrate(cyl_to_rect(ics), golden["c_indiv_t"], pt, pa, method,
                                     rtol=1e-10, atol=1e-10)
     assert not err.any()
-    assert cyl_diff(golden["c_dop853_indiv"], rect_to_cyl(out)).max() < 1e-10
+    assert cyl_diff(golden[f"c_{method}_indiv"], rect_to_cyl(out)).max() < 1e-10
+
+
+def test_dopr54_forced_steps(harness, oracle, golden):
+    """The smallest-step rule: err = 1 and 10,000 forced steps per orbit, as
+    in the reference's own C (golden vectors)."""
+    pt, pa = golden["mw14_type"], golden["mw14_args"]
+    out, err, ns = harness.integrate(cyl_to_rect(golden["c_ics"]), np.array([0.0, 50.0]), pt, pa,
+                                     "dopr54", dt=50.0, rtol=1e-20, atol=1e-20)
+    assert np.all(err == 1) and np.all(ns == 10000)
+    assert cyl_diff(golden["c_dopr54_forced"], rect_to_cyl(out)).max() < 1e-11
 
 
 def test_backward_integration(harness, oracle, mw14):
@@ -144,26 +155,44 @@ def test_fixed_dt(harness, oracle, mw14):
     pt, pa = mw14
     ics = seeded_ics(8, 13)
     t = np.linspace(0, 10, 11)
-    for method in ("leapfrog", "symplec4", "rk4"):
+    for method in ("leapfrog", "symplec4", "symplec6", "rk4", "rk6"):
         ref, _, nref, _ = oracle.integrate(ics, t, pt, pa, method, dt=0.01)
         out, err, ns = harness.integrate(cyl_to_rect(ics), t, pt, pa, method, dt=0.01)
         assert np.array_equal(ns, nref) and nref[0] == 1000
         assert cyl_diff(ref, rect_to_cyl(out)).max() < 1e-11
+    # dopr54: dt is only its first step
+    ref, _, nref, _ = oracle.integrate(ics, t, pt, pa, "dopr54", dt=0.01)
+    out, err, ns = harness.integrate(cyl_to_rect(ics), t, pt, pa, "dopr54", dt=0.01)
+    assert np.array_equal(ns, nref) and not err.any()
+    assert cyl_diff(ref, rect_to_cyl(out)).max() < 1e-11
 
 
 def test_attempt_budget_and_nonfinite(harness, mw14):
     pt, pa = mw14
     ics = seeded_ics(3, 14)
     t = np.linspace(0, 50, 51)
-    out, err, ns = harness.integrate(cyl_to_rect(ics), t, pt, pa, "dop853", max_attempts=20)
-    assert np.all(err == 2)
-    assert np.isnan(out[:, -1]).all() and np.isfinite(out[:, 0]).all()
+    for method in ("dop853", "dopr54"):
+        out, err, ns = harness.integrate(cyl_to_rect(ics), t, pt, pa, method, max_attempts=20)
+        assert np.all(err == 2)
+        assert np.isnan(out[:, -1]).all() and np.isfinite(out[:, 0]).all()
     w = cyl_to_rect(ics)
     w[1, 0] = np.nan
     for method in METHODS:
         out, err, ns = harness.integrate(w, t[:5], pt, pa, method, dt=0.01)
         assert err[1] == 3 and err[0] == 0 and err[2] == 0
         assert np.isnan(out[1, 1:]).all()
+
+
+def test_dopr54_stalled_time_ends_the_orbit(harness, mw14):
+    """Output times near 1e17 (ulp 16) and a first step of 1: the accepted
+    step leaves the time unchanged, where the reference loops forever; the
+    machine stops the orbit with err 2 after that one step."""
+    pt, pa = mw14
+    w = cyl_to_rect(seeded_ics(2, 16))
+    t = 1e17 + np.array([0.0, 128.0, 256.0])
+    out, err, ns = harness.integrate(w, t, pt, pa, "dopr54", dt=1.0)
+    assert np.all(err == 2) and np.all(ns == 1)
+    assert np.array_equal(out[:, 0], w) and np.isnan(out[:, 1:]).all()
 
 
 def test_single_output_row(harness, mw14):

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 from helpers import cyl_to_rect, seeded_ics
 
-METHODS = ["leapfrog", "rk4", "symplec4", "dop853"]
+METHODS = ["leapfrog", "rk4", "rk6", "symplec4", "symplec6", "dopr54", "dop853"]
 
 
 @pytest.mark.parametrize("method", METHODS)
@@ -61,10 +61,39 @@ def test_oracle_matches_golden_c_vectors(oracle, golden, method):
     np.testing.assert_allclose(a, golden[f"c_{method}_dxdv2"], rtol=0, atol=1e-12)
 
 
-def test_oracle_indiv_t_golden(oracle, golden):
+@pytest.mark.parametrize("method", ["dop853", "dopr54"])
+def test_oracle_indiv_t_golden(oracle, golden, method):
     a, _, _, _ = oracle.integrate(golden["c_ics"], golden["c_indiv_t"], golden["mw14_type"],
-                                  golden["mw14_args"], "dop853", rtol=1e-10, atol=1e-10)
-    np.testing.assert_allclose(a, golden["c_dop853_indiv"], rtol=0, atol=1e-13)
+                                  golden["mw14_args"], method, rtol=1e-10, atol=1e-10)
+    np.testing.assert_allclose(a, golden[f"c_{method}_indiv"], rtol=0, atol=1e-13)
+
+
+def test_oracle_dopr54_forced_steps_golden(oracle, golden):
+    """dopr54's smallest-step rule (bovy_rk.c:598-604): an unreachable
+    tolerance forces every step to the interval's first step / 10000 and
+    flags err = 1, as the reference's own C does on the same input."""
+    a, err, nsteps, _ = oracle.integrate(golden["c_ics"], np.array([0.0, 50.0]),
+                                         golden["mw14_type"], golden["mw14_args"], "dopr54",
+                                         dt=50.0, rtol=1e-20, atol=1e-20)
+    np.testing.assert_array_equal(err, golden["c_dopr54_forced_err"])
+    assert np.all(err == 1)
+    assert np.all(nsteps == 10000)
+    np.testing.assert_allclose(a, golden["c_dopr54_forced"], rtol=0, atol=1e-13)
+
+
+@pytest.mark.parametrize("method", ["rk6", "symplec6", "dopr54"])
+def test_oracle_bitwise_vs_reference_build_edge_cases(oracle, mw14, method):
+    """Backward integration over per-orbit time grids and an explicit step."""
+    if not oracle.ref_available():
+        pytest.skip("oracle/_ref not built here (needs the reference tree)")
+    pt, pa = mw14
+    ics = seeded_ics(8, 6)
+    tt = -np.linspace(0, 1, 21)[None, :] * np.linspace(3.0, 9.0, 8)[:, None]
+    for kw in ({"rtol": 1e-9, "atol": 1e-9}, {"dt": -0.01}):
+        a, ea, _, _ = oracle.integrate(ics, tt, pt, pa, method, **kw)
+        b, eb, _, _ = oracle.integrate(ics, tt, pt, pa, method, impl="ref", **kw)
+        assert np.array_equal(a, b)
+        assert np.array_equal(ea, eb)
 
 
 def test_incomplete_gamma_vs_scipy(oracle):
