@@ -528,7 +528,7 @@ def differentiation_leg(gb, torch, dev, stream, pg, peak, n=65536):
 METHOD_FLOPS = {"leapfrog": 318.0, "symplec4": 942.0, "symplec6": 2200.0, "rk4": 1260.0,
                 "rk6": 2250.0, "dopr54": 2050.0, "dop853": F_STEP_DOP853}
 METHODS_WORKLOAD = ("131,072 orbits/GPU in MWPotential2014, config-0 initial conditions "
-                    "(R ~ U(0.5, 2)), t in [0, 10] with 11 snapshots, galpy's default "
+                    "(R ~ U(0.5, 2)), t in [0, 100] with 101 snapshots, galpy's default "
                     "tolerances (rtol = atol = 1e-12) and estimated step, SoA float64 output")
 
 
@@ -538,7 +538,7 @@ def methods_leg(gb, torch, dev, stream, pg, peak, rank, cpu=True, n=131072, K=3,
     orbits on all host cores."""
     pt, pa = mw14_args()
     ics, _ = precision_workload(n, seed=shard_seed(0, rank))
-    t = np.linspace(0.0, 10.0, 11)
+    t = np.linspace(0.0, 100.0, 101)
     comps, ncomp = gb.compile_potential((pt, pa))
     sig = gb.signature((pt, pa))
     comps_d = torch.tensor(comps, device=dev)
