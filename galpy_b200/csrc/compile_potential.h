@@ -25,6 +25,10 @@ inline int galpy_nargs(int type, int planar)
     case T_HERNQUIST: return 2;
     case T_NFW: return 2;
     case T_PSWC: return planar ? 3 : 5;
+    case T_POWER: case T_JAFFE: case T_ISOCHRONE: case T_PLUMMER: case T_PSEUDOISO:
+    case T_BURKERT: case T_DEHNENCORE: return 2;
+    case T_DEHNEN: case T_HOMSPHERE: return 3;
+    case T_NULL: return 0;
     default: return -1;
   }
 }
@@ -171,7 +175,7 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
     GpComp c;
     memset(&c, 0, sizeof(c));
     c.type = type;
-    const double amp = p[0];
+    const double amp = na > 0 ? p[0] : 0.0;
     c.c[0] = amp;
     switch (type) {
       case T_PSWC: {
@@ -226,6 +230,47 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
         c.c[3] = om < 1.0 ? 1.0 - om : 1.0;
         break;
       }
+      case T_POWER:
+        c.c[1] = -0.5 * p[1];
+        c.c[2] = 1.0 - p[1];
+        c.c[3] = p[1];
+        break;
+      case T_JAFFE:
+      case T_DEHNENCORE:
+        if (!(p[1] > 0.0)) return -1;
+        c.c[1] = p[1];
+        break;
+      case T_ISOCHRONE:
+        if (!(p[1] > 0.0)) return -1;
+        c.c[1] = p[1];
+        c.c[2] = p[1] * p[1];
+        break;
+      case T_PLUMMER:
+        c.c[1] = p[1] * p[1];
+        break;
+      case T_PSEUDOISO:
+        if (!(p[1] > 0.0)) return -1;
+        c.c[1] = p[1];
+        c.c[2] = 1.0 / p[1];
+        break;
+      case T_BURKERT:
+        if (!(p[1] > 0.0)) return -1;
+        c.c[1] = p[1];
+        c.c[2] = 1.0 / p[1];
+        c.c[3] = M_PI * p[1] * p[1] * p[1];
+        break;
+      case T_DEHNEN:
+        if (!(p[1] > 0.0) || !(p[2] < 3.0)) return -1;
+        c.c[1] = p[1];
+        c.c[2] = p[2];
+        c.c[3] = 1.0 / (3.0 - p[2]);
+        break;
+      case T_HOMSPHERE:  // galpy passes R^2 and R^3
+        c.c[1] = p[1];
+        c.c[2] = p[2];
+        break;
+      case T_NULL:
+        break;
     }
     for (int i = 0; i < kChebN; i++)
       for (int j = 0; j < kChebC; j++) c.chebf[i][j] = (float)c.cheb[i][j];

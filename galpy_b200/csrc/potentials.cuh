@@ -2,11 +2,12 @@
 //
 // Device-side forces and tidal tensors of the potentials the engine supports:
 // PowerSphericalPotentialwCutoff (galpy type 15), MiyamotoNagaiPotential (5),
-// NFWPotential (9), HernquistPotential (8) and LogarithmicHaloPotential (0,
-// axisymmetric or triaxial).  Reference formulas:
-// galpy/potential/potential_c_ext/{PowerSphericalPotentialwCutoff,
-// MiyamotoNagaiPotential,NFWPotential,HernquistPotential,
-// LogarithmicHaloPotential}.c.
+// NFWPotential (9), HernquistPotential (8), LogarithmicHaloPotential (0,
+// axisymmetric or triaxial), and the spherical PowerSpherical (7), Jaffe
+// (10), Isochrone (14), Plummer (17), PseudoIsothermal (18), Burkert (20),
+// DehnenCoreSpherical (33), DehnenSpherical (34), HomogeneousSphere (35) and
+// Null (40) potentials.  Reference formulas:
+// galpy/potential/potential_c_ext/<name>.c.
 //
 // Design (not a translation of the reference's cylindrical route):
 //  * Every component is evaluated directly in Cartesian coordinates.  The
@@ -39,6 +40,12 @@
 namespace gpc {
 
 enum : int { T_LOGHALO = 0, T_MN = 5, T_HERNQUIST = 8, T_NFW = 9, T_PSWC = 15 };
+// spherical potentials (potential_c_ext/<name>.c): PowerSpherical (galpy's
+// KeplerPotential is alpha = 3), Jaffe, Isochrone, Plummer,
+// PseudoIsothermal, Burkert, DehnenCoreSpherical, DehnenSpherical,
+// HomogeneousSphere, Null (no force)
+enum : int { T_POWER = 7, T_JAFFE = 10, T_ISOCHRONE = 14, T_PLUMMER = 17, T_PSEUDOISO = 18,
+             T_BURKERT = 20, T_DEHNENCORE = 33, T_DEHNEN = 34, T_HOMSPHERE = 35, T_NULL = 40 };
 
 constexpr int kMaxComp = 16;  // components per potential group
 constexpr int kChebN = 32;    // Chebyshev intervals of gamma*(a, u) on [0, U]
@@ -54,6 +61,11 @@ constexpr int kBinSub = 8;    // sub-intervals of a binade [1, 2) in the binade 
 //   NFW:       c0 amp, c1 a, c2 1/a
 //   LogHalo:   c0 amp, c1 1/q^2, c2 core^2, c3 1 - e (y-axis factor; 1 when
 //              axisymmetric)
+//   PowerSpherical: c1 -alpha/2, c2 1 - alpha, c3 alpha
+//   Jaffe, DehnenCore: c1 a      Isochrone: c1 b, c2 b^2      Plummer: c1 b^2
+//   PseudoIsothermal: c1 a, c2 1/a       Burkert: c1 a, c2 1/a, c3 pi a^3
+//   DehnenSpherical: c1 a, c2 alpha, c3 1/(3 - alpha)
+//   HomogeneousSphere: c1 R^2, c2 R^3    Null: -
 //   PSwC potential (energy evaluation only): c8 2 pi rc^(3-alpha), c9 rc,
 //              c10 a1 = 1 - alpha/2, c11 Gamma(a1), c12 lgamma(a1),
 //              c13 a2 = 1.5 - alpha/2, c14 Gamma(a2), c15 lgamma(a2)
@@ -347,6 +359,55 @@ struct ScalarsDirect {
   GPC_HD GPC_FI double operator[](int j) const { return p[j]; }
 };
 
+// The spherical potentials' acceleration factor -Phi'(r)/r (a = f x), for
+// the run-time component list; FP32 and FP64 alike.
+template <typename T, class S>
+GPC_HD GPC_FI T sph_force_factor(int type, const S& sc, T r2)
+{
+  const T amp = T(sc[0]);
+  switch (type) {
+    case T_POWER:  // Phi' = amp r^(1-alpha)
+      return -amp * Num<T>::ex(T(sc[1]) * Num<T>::lg(r2));
+    case T_JAFFE: {  // Phi' = amp / (r (r + a))
+      const T ir = Num<T>::rsq(r2);
+      return -amp * ir * ir * Num<T>::rcp(r2 * ir + T(sc[1]));
+    }
+    case T_ISOCHRONE: {  // Phi' = amp r / (rb (b + rb)^2), rb = sqrt(r^2 + b^2)
+      const T rb2 = r2 + T(sc[2]), irb = Num<T>::rsq(rb2);
+      const T ib = Num<T>::rcp(T(sc[1]) + rb2 * irb);
+      return -amp * irb * ib * ib;
+    }
+    case T_PLUMMER: {  // Phi' = amp r (r^2 + b^2)^(-3/2)
+      const T i = Num<T>::rsq(r2 + T(sc[1]));
+      return -amp * i * i * i;
+    }
+    case T_PSEUDOISO: {  // Phi' = amp (1/r - a atan(r/a) / r^2) / a
+      const T ir = Num<T>::rsq(r2), r = r2 * ir;
+      return -amp * T(sc[2]) * ir * ir * (T(1) - T(sc[1]) * atan(r * T(sc[2])) * ir);
+    }
+    case T_BURKERT: {  // Phi' = -amp pi a^3 / r^2 (2 atan x - 2 ln(1+x) - ln(1+x^2)), x = r/a
+      const T ir = Num<T>::rsq(r2), x = r2 * ir * T(sc[2]);
+      const T B = T(2) * atan(x) - T(2) * log1p(x) - log1p(x * x);
+      return amp * T(sc[3]) * ir * ir * ir * B;
+    }
+    case T_DEHNENCORE: {  // Phi' = amp r / (3 (a + r)^3)
+      const T ia = Num<T>::rcp(r2 * Num<T>::rsq(r2) + T(sc[1]));
+      return -amp * ia * ia * ia / T(3);
+    }
+    case T_DEHNEN: {  // Phi' = amp r (1 + a/r)^alpha / ((a + r)^3 (3 - alpha))
+      const T ir = Num<T>::rsq(r2), ia = Num<T>::rcp(r2 * ir + T(sc[1]));
+      const T w = Num<T>::ex(T(sc[2]) * Num<T>::lg(T(1) + T(sc[1]) * ir));
+      return -amp * T(sc[3]) * w * ia * ia * ia;
+    }
+    case T_HOMSPHERE: {  // Phi' = 2 amp r inside R, 2 amp R^3 / r^2 outside
+      const T ir = Num<T>::rsq(r2);
+      return r2 < T(sc[1]) ? T(-2) * amp : T(-2) * amp * T(sc[2]) * ir * ir * ir;
+    }
+    default:  // T_NULL
+      return T(0);
+  }
+}
+
 template <typename T, bool PLANAR, int TYPE, class S>
 GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T y, T z2, T R2,
                               T r2, T& gR, T& gz, T& gyx)
@@ -427,8 +488,12 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
       if (!PLANAR) gz += g * iq2;
       break;
     }
-    default:
+    default: {
+      const T f = sph_force_factor<T>(type, sc, r2);
+      gR += f;
+      gz += f;
       break;
+    }
   }
 }
 
@@ -508,6 +573,75 @@ GPC_HD GPC_FI void add_spherical(double dphi_over_r, double d2phi, double x, dou
   K[3] -= c * x * z;
   K[4] -= c * y * z;
   K[5] -= c * z * z + dphi_over_r;
+}
+
+// Phi'(r)/r and Phi''(r) of the spherical potentials (zero for Null).
+GPC_HD inline void sph_derivs(const GpComp* __restrict__ cp, int type, double amp, double r2,
+                              double& dpr, double& d2)
+{
+  const double r = sqrt(r2), ir = 1.0 / r, c1 = ldg(&cp->c[1]);
+  dpr = d2 = 0.0;
+  switch (type) {
+    case T_POWER:
+      dpr = amp * exp(ldg(&cp->c[1]) * log(r2));
+      d2 = ldg(&cp->c[2]) * dpr;  // (1 - alpha) amp r^-alpha
+      break;
+    case T_JAFFE: {
+      const double ira = 1.0 / (r + c1);
+      dpr = amp * ir * ir * ira;
+      d2 = -amp * (c1 + 2.0 * r) * ir * ir * ira * ira;
+      break;
+    }
+    case T_ISOCHRONE: {
+      const double b = c1, rb = sqrt(r2 + ldg(&cp->c[2])), ib = 1.0 / (b + rb);
+      dpr = amp / rb * ib * ib;
+      const double q = 1.0 / (rb * (b + rb));
+      d2 = -amp * (-b * b * b - b * b * rb + 2.0 * r2 * rb) * q * q * q;
+      break;
+    }
+    case T_PLUMMER: {
+      const double i = 1.0 / sqrt(r2 + c1);
+      dpr = amp * i * i * i;
+      d2 = amp * (c1 - 2.0 * r2) * i * i * i * i * i;
+      break;
+    }
+    case T_PSEUDOISO: {
+      const double a = c1, at = atan(r / a);
+      dpr = amp / a * (ir * ir - a * at * ir * ir * ir);
+      d2 = amp * ir * ir * (2.0 * a * ir * at - (2.0 * a * a + r2) / (a * a + r2)) / a;
+      break;
+    }
+    case T_BURKERT: {
+      const double a = c1, x = r / a, pa3 = ldg(&cp->c[3]);
+      const double B = 2.0 * atan(x) - 2.0 * log1p(x) - log1p(x * x);
+      dpr = -amp * pa3 * ir * ir * ir * B;
+      d2 = amp * pa3 * (4.0 / ((a * a + r2) * (a + r)) + 2.0 * B * ir * ir * ir);
+      break;
+    }
+    case T_DEHNENCORE: {
+      const double ia = 1.0 / (c1 + r);
+      dpr = amp * ia * ia * ia / 3.0;
+      d2 = -amp * (2.0 * r - c1) * ia * ia * ia * ia / 3.0;
+      break;
+    }
+    case T_DEHNEN: {
+      const double a = c1, alpha = ldg(&cp->c[2]), i3a = ldg(&cp->c[3]);
+      const double ia = 1.0 / (a + r), w = pow(1.0 + a * ir, alpha);
+      dpr = amp * i3a * w * ia * ia * ia;
+      d2 = -amp * i3a * w * (2.0 * r + a * (alpha - 1.0)) * ia * ia * ia * ia;
+      break;
+    }
+    case T_HOMSPHERE:
+      if (r2 < c1) {
+        dpr = d2 = 2.0 * amp;
+      } else {
+        dpr = 2.0 * amp * ldg(&cp->c[2]) * ir * ir * ir;
+        d2 = -2.0 * dpr;
+      }
+      break;
+    default:
+      break;
+  }
 }
 
 template <bool PLANAR>
@@ -594,8 +728,12 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
         K[5] += g * iq2 + h * uz * uz;
         break;
       }
-      default:
+      default: {
+        double dpr, d2;  // Phi'/r, Phi''
+        sph_derivs(cp, type, amp, r2, dpr, d2);
+        add_spherical(dpr, d2, x, y, z, r2, gR, gz, K);
         break;
+      }
     }
   }
   ax = x * gR;
@@ -635,6 +773,42 @@ GPC_HD inline double inc_gamma_P(double a, double x, double lga)
     if (fabs(del - 1.0) < 1e-17) break;
   }
   return 1.0 - exp(lpref) * h;
+}
+
+// Potential of the spherical potentials at r^2 (0 for Null, whose constant
+// value galpy adds on the Python side only).
+GPC_HD inline double sph_value(const GpComp* __restrict__ cp, int type, double amp, double r2)
+{
+  const double r = sqrt(r2), c1 = ldg(&cp->c[1]);
+  switch (type) {
+    case T_POWER: {
+      const double alpha = ldg(&cp->c[3]);
+      if (alpha == 2.0) return 0.5 * amp * log(r2);
+      return -amp * pow(r2, 1.0 - 0.5 * alpha) / (alpha - 2.0);
+    }
+    case T_JAFFE: return -amp * log1p(c1 / r) / c1;
+    case T_ISOCHRONE: return -amp / (c1 + sqrt(r2 + ldg(&cp->c[2])));
+    case T_PLUMMER: return -amp / sqrt(r2 + c1);
+    case T_PSEUDOISO: return amp * (0.5 * log1p(r2 / (c1 * c1)) + c1 / r * atan(r / c1)) / c1;
+    case T_BURKERT: {
+      const double x = r / c1;
+      return -amp * c1 * c1 * M_PI / x *
+             (-M_PI + 2.0 * (1.0 + x) * atan(1.0 / x) + 2.0 * (1.0 + x) * log1p(x) +
+              (1.0 - x) * log1p(x * x));
+    }
+    case T_DEHNENCORE: {
+      const double u = r / (r + c1);
+      return -amp * (1.0 - u * u) / (6.0 * c1);
+    }
+    case T_DEHNEN: {
+      const double alpha = ldg(&cp->c[2]);
+      return -amp * (1.0 - pow(r / (r + c1), 2.0 - alpha)) / (c1 * (2.0 - alpha) * (3.0 - alpha));
+    }
+    case T_HOMSPHERE:
+      return r2 < c1 ? amp * (r2 - 3.0 * c1) : -2.0 * amp * ldg(&cp->c[2]) / r;
+    default:
+      return 0.0;
+  }
 }
 
 // Potential Phi(x, y, z) summed over one group's components, FP64
@@ -677,6 +851,7 @@ GPC_HD inline double potential_value(const GpComp* __restrict__ comp, int ncomp,
         break;
       }
       default:
+        phi += sph_value(cp, ldg(&cp->type), amp, r2);
         break;
     }
   }

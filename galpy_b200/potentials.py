@@ -2,8 +2,11 @@
 
 The engine integrates in the potentials galpy hands to C as pot_type codes
 0 (LogarithmicHaloPotential), 5 (MiyamotoNagaiPotential), 8
-(HernquistPotential), 9 (NFWPotential) and 15
-(PowerSphericalPotentialwCutoff) -- the parsing is
+(HernquistPotential), 9 (NFWPotential), 15 (PowerSphericalPotentialwCutoff)
+and the spherical 7 (PowerSpherical / Kepler), 10 (Jaffe), 14 (Isochrone),
+17 (Plummer), 18 (PseudoIsothermal), 20 (Burkert), 33
+(DehnenCoreSpherical), 34 (DehnenSpherical), 35 (HomogeneousSphere) and 40
+(Null) -- the parsing is
 galpy/orbit/integrateFullOrbit.py:43-614 (3D) and
 galpy/orbit/integratePlanarOrbit.py:33-663 (planar).
 
@@ -11,8 +14,8 @@ galpy/orbit/integratePlanarOrbit.py:33-663 (planar).
   * galpy potential instances (or lists of them) -- galpy's own ``_parse_pot``
     is used, so the arguments are exactly galpy's;
   * the light-weight classes below, which reproduce galpy's constructors for
-    these five potentials (amp, scale parameters and ``normalize``) for use
-    without galpy;
+    the five potentials of types 0, 5, 8, 9 and 15 (amp, scale parameters
+    and ``normalize``) for use without galpy;
   * an already-parsed ``(pot_type, pot_args)`` pair.
 """
 import math
@@ -20,7 +23,11 @@ import math
 import numpy as np
 
 T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC = 0, 5, 8, 9, 15
-SUPPORTED_TYPES = (T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC)
+# spherical: PowerSpherical (and Kepler), Jaffe, Isochrone, Plummer,
+# PseudoIsothermal, Burkert, DehnenCoreSpherical, DehnenSpherical,
+# HomogeneousSphere, Null
+SPHERICAL_TYPES = (7, 10, 14, 17, 18, 20, 33, 34, 35, 40)
+SUPPORTED_TYPES = (T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC) + SPHERICAL_TYPES
 
 
 class _Potential:

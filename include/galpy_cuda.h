@@ -13,7 +13,10 @@
  * 6 dop853 (galpy's numbering; 7 ias15 returns GALPY_CUDA_ERR_METHOD so the
  * caller can fall back), pot_type/pot_args as produced by galpy's _parse_pot
  * (types 0 LogarithmicHalo, 5 MiyamotoNagai, 8 Hernquist, 9 NFW,
- * 15 PowerSphericalwCutoff), per-orbit err[] (0 ok, -10 interrupted by
+ * 15 PowerSphericalwCutoff, and the spherical 7 PowerSpherical/Kepler,
+ * 10 Jaffe, 14 Isochrone, 17 Plummer, 18 PseudoIsothermal, 20 Burkert,
+ * 33 DehnenCoreSpherical, 34 DehnenSpherical, 35 HomogeneousSphere, 40 Null;
+ * others return GALPY_CUDA_ERR_POTENTIAL), per-orbit err[] (0 ok, -10 interrupted by
  * SIGINT, 1 = dopr54 forced a step at its smallest allowed size, as the
  * reference does; the orbit is complete).  Two additions: every entry point returns a status code instead
  * of void, and takes a trailing options pointer (NULL = defaults).

@@ -9,7 +9,10 @@
  * What is restated (reference file:line in galpy):
  *   forces   PowerSphericalPotentialwCutoff.c:9-131, MiyamotoNagaiPotential.c:
  *            16-117, NFWPotential.c:16-106, HernquistPotential.c:15-100,
- *            LogarithmicHaloPotential.c:5-297 (potential_c_ext/)
+ *            LogarithmicHaloPotential.c:5-297, and the spherical
+ *            PowerSpherical, Jaffe, Isochrone, Plummer, PseudoIsothermal,
+ *            Burkert, DehnenCore, Dehnen, HomogeneousSphere potentials and
+ *            ZeroForce (potential_c_ext/)
  *   sums     galpy_potentials.c:120-354 (sum over components, in order)
  *   RHS      orbit_c_ext/integrateFullOrbit.c:1307-1352 (evalRectForce,
  *            evalRectDeriv), :1496-1681 (the dxdv variants);
@@ -48,6 +51,19 @@ double oracle_gamma_inc_Q(double a, double x);
 /* potentials                                                          */
 /* ------------------------------------------------------------------ */
 enum { PT_LOGHALO = 0, PT_MN = 5, PT_HERNQUIST = 8, PT_NFW = 9, PT_PSWC = 15 };
+/* spherical potentials, each restated from potential_c_ext/<name>.c */
+enum {
+  PT_POWER = 7,       /* PowerSphericalPotential (KeplerPotential: alpha = 3) */
+  PT_JAFFE = 10,      /* JaffePotential */
+  PT_ISOCHRONE = 14,  /* IsochronePotential */
+  PT_PLUMMER = 17,    /* PlummerPotential */
+  PT_PSEUDOISO = 18,  /* PseudoIsothermalPotential */
+  PT_BURKERT = 20,    /* BurkertPotential */
+  PT_DEHNENCORE = 33, /* DehnenCoreSphericalPotential (DehnenCorePotential.c) */
+  PT_DEHNEN = 34,     /* DehnenSphericalPotential (DehnenPotential.c) */
+  PT_HOMSPHERE = 35,  /* HomogeneousSpherePotential */
+  PT_NULL = 40        /* NullPotential (ZeroForce) */
+};
 #define OMAXPOT 32
 
 typedef struct {
@@ -70,12 +86,246 @@ static int nargs_of(int type, int planar)
   case PT_HERNQUIST: return 2;
   case PT_NFW: return 2;
   case PT_PSWC: return planar ? 3 : 5;
+  case PT_POWER: case PT_JAFFE: case PT_ISOCHRONE: case PT_PLUMMER: case PT_PSEUDOISO:
+  case PT_BURKERT: case PT_DEHNENCORE: return 2;
+  case PT_DEHNEN: case PT_HOMSPHERE: return 3;
+  case PT_NULL: return 0;
   default: return -1;
   }
 }
 
+static int is_new_spherical(int type)
+{
+  switch (type) {
+  case PT_POWER: case PT_JAFFE: case PT_ISOCHRONE: case PT_PLUMMER: case PT_PSEUDOISO:
+  case PT_BURKERT: case PT_DEHNENCORE: case PT_DEHNEN: case PT_HOMSPHERE: case PT_NULL:
+    return 1;
+  }
+  return 0;
+}
+
+/* 3D R or z force of the spherical potentials: X is R (Rforce) or Z
+   (zforce), in the position where each reference formula has it
+   (<name>Rforce / <name>zforce in potential_c_ext/) */
+static double sph_force3(const ocomp *c, double R, double Z, double X)
+{
+  double amp = c->p[0];
+  switch (c->type) {
+  case PT_PLUMMER: { /* PlummerPotential.c:15-43 */
+    double b2 = c->p[1] * c->p[1];
+    return -amp * X * pow(R * R + Z * Z + b2, -1.5);
+  }
+  case PT_JAFFE: { /* JaffePotential.c */
+    double a = c->p[1], sqrtRz = pow(R * R + Z * Z, 0.5);
+    return -amp * X * pow(sqrtRz, -3.) / (1. + a / sqrtRz);
+  }
+  case PT_ISOCHRONE: { /* IsochronePotential.c */
+    double b = c->p[1], r2 = R * R + Z * Z, rb = sqrt(r2 + b * b);
+    return -amp * X / rb * pow(b + rb, -2.);
+  }
+  case PT_POWER: /* PowerSphericalPotential.c */
+    return -amp * X * pow(R * R + Z * Z, -0.5 * c->p[1]);
+  case PT_BURKERT: { /* BurkertPotential.c */
+    double a = c->p[1], r = sqrt(R * R + Z * Z), x = r / a;
+    return amp * a * M_PI / x / x *
+           (M_PI - 2. * atan(1. / x) - 2. * log(1. + x) - log(1. + x * x)) * X / r;
+  }
+  case PT_PSEUDOISO: { /* PseudoIsothermalPotential.c */
+    double a = c->p[1], r2 = R * R + Z * Z, r = sqrt(r2);
+    return -amp * (1. / r - a / r2 * atan(r / a)) / a * X / r;
+  }
+  case PT_DEHNENCORE: { /* DehnenCorePotential.c */
+    double a = c->p[1], sqrtRz = pow(R * R + Z * Z, 0.5);
+    return -amp * (X / pow(a + sqrtRz, 3.) / 3.);
+  }
+  case PT_DEHNEN: { /* DehnenPotential.c */
+    double a = c->p[1], alpha = c->p[2], sqrtRz = pow(R * R + Z * Z, 0.5);
+    return -amp * (X * pow(1. + a / sqrtRz, alpha) / pow(a + sqrtRz, 3.) / (3. - alpha));
+  }
+  case PT_HOMSPHERE: { /* HomogeneousSpherePotential.c */
+    double R2 = c->p[1], R3 = c->p[2], r2 = R * R + Z * Z;
+    if (r2 < R2) return -2. * amp * X;
+    return -2. * amp * R3 * X / pow(r2, 1.5);
+  }
+  }
+  return 0.;
+}
+
+/* planar R force (<name>PlanarRforce) */
+static double sph_planarRforce(const ocomp *c, double R)
+{
+  double amp = c->p[0];
+  switch (c->type) {
+  case PT_PLUMMER: {
+    double b2 = c->p[1] * c->p[1];
+    return -amp * R * pow(R * R + b2, -1.5);
+  }
+  case PT_JAFFE: {
+    double a = c->p[1];
+    return -amp * pow(R, -2.) / (1. + a / R);
+  }
+  case PT_ISOCHRONE: {
+    double b = c->p[1], r2 = R * R, rb = sqrt(r2 + b * b);
+    return -amp * R / rb * pow(b + rb, -2.);
+  }
+  case PT_POWER:
+    return -amp * pow(R, -c->p[1] + 1.);
+  case PT_BURKERT: {
+    double a = c->p[1], x = R / a;
+    return amp * a * M_PI / x / x * (M_PI - 2. * atan(1. / x) - 2. * log(1. + x) - log(1. + x * x));
+  }
+  case PT_PSEUDOISO: {
+    double a = c->p[1];
+    return -amp * (1. / R - a / R / R * atan(R / a)) / a;
+  }
+  case PT_DEHNENCORE: {
+    double a = c->p[1];
+    return -amp * (R / pow(a + R, 3.) / 3.);
+  }
+  case PT_DEHNEN: {
+    double a = c->p[1], alpha = c->p[2];
+    return -amp * (R * pow(1. + a / R, alpha) / pow(a + R, 3.) / (3. - alpha));
+  }
+  case PT_HOMSPHERE: {
+    double R2 = c->p[1], R3 = c->p[2], r2 = R * R;
+    if (r2 < R2) return -2. * amp * R;
+    return -2. * amp * R3 / r2;
+  }
+  }
+  return 0.;
+}
+
+/* planar d2Phi/dR2 (<name>PlanarR2deriv) */
+static double sph_planarR2deriv(const ocomp *c, double R)
+{
+  double amp = c->p[0];
+  switch (c->type) {
+  case PT_PLUMMER: {
+    double b2 = c->p[1] * c->p[1];
+    return amp * (b2 - 2. * R * R) * pow(R * R + b2, -2.5);
+  }
+  case PT_JAFFE: {
+    double a = c->p[1];
+    return -amp * (a + 2. * R) * pow(R, -4.) * pow(1. + a / R, -2.);
+  }
+  case PT_ISOCHRONE: {
+    double b = c->p[1], r2 = R * R, rb = sqrt(r2 + b * b);
+    return -amp * (-pow(b, 3.) - b * b * rb + 2. * r2 * rb) * pow(rb * (b + rb), -3.);
+  }
+  case PT_POWER: {
+    double alpha = c->p[1];
+    return amp * (1. - alpha) * pow(R, -alpha);
+  }
+  case PT_BURKERT: {
+    double a = c->p[1], x = R / a, R5 = pow(R, 5);
+    return -amp * M_PI * pow(a, 3) / R5 *
+           (-4. * R5 / (a * a + R * R) / (a + R) -
+            2. * R * R * (M_PI - 2. * atan(1. / x) - 2. * log(1. + x) - log(1. + x * x)));
+  }
+  case PT_PSEUDOISO: {
+    double a = c->p[1], a2 = a * a, R2 = R * R;
+    return amp / R2 * (2. * a / R * atan(R / a) - (2. * a2 + R2) / (a2 + R2)) / a;
+  }
+  case PT_DEHNENCORE: {
+    double a = c->p[1];
+    return -amp * (pow(a + R, -4.) * (2. * R - a)) / 3.;
+  }
+  case PT_DEHNEN: {
+    double a = c->p[1], alpha = c->p[2];
+    return -amp * (pow(1. + a / R, alpha) * pow(a + R, -4.) * (2. * R + a * (alpha - 1.))) /
+           (3. - alpha);
+  }
+  case PT_HOMSPHERE: {
+    double R2 = c->p[1], R3 = c->p[2], r2 = R * R;
+    if (r2 < R2) return 2. * amp;
+    return -4. * amp * R3 / pow(r2, 1.5);
+  }
+  }
+  return 0.;
+}
+
+/* 3D Hessian terms (which = 0 R2, 1 z2, 2 Rz): Plummer and Jaffe have their
+   own closed forms in the reference; the others assemble Phi'' and Phi'/r
+   from the planar functions at r (e.g. IsochronePotential.c R2deriv) */
+static double sph_hess3(const ocomp *c, int which, double R, double Z)
+{
+  double amp = c->p[0];
+  if (c->type == PT_NULL || which > 2) return 0.;
+  if (c->type == PT_PLUMMER) {
+    double b2 = c->p[1] * c->p[1];
+    if (which == 0) return amp * (b2 - 2. * R * R + Z * Z) * pow(R * R + Z * Z + b2, -2.5);
+    if (which == 1) return amp * (b2 + R * R - 2. * Z * Z) * pow(R * R + Z * Z + b2, -2.5);
+    return amp * (-3. * R * Z * pow(R * R + Z * Z + b2, -2.5));
+  }
+  if (c->type == PT_JAFFE) {
+    double a = c->p[1], r = sqrt(R * R + Z * Z);
+    double dphi = pow(r, -2.) / (1. + a / r);
+    double d2phi = -(a + 2. * r) * pow(r, -4.) * pow(1. + a / r, -2.);
+    if (which == 0) return amp * (d2phi * R * R / r / r + dphi * Z * Z / r / r / r);
+    if (which == 1) return amp * (d2phi * Z * Z / r / r + dphi * R * R / r / r / r);
+    return amp * R * Z * (d2phi / r / r - dphi / r / r / r);
+  }
+  double r2 = R * R + Z * Z, r = sqrt(r2);
+  double Phipp = sph_planarR2deriv(c, r), Phip = -sph_planarRforce(c, r);
+  double ir2 = 1. / r2, ir3 = ir2 / r;
+  if (which == 0) return Phipp * R * R * ir2 + Phip * Z * Z * ir3;
+  if (which == 1) return Phipp * Z * Z * ir2 + Phip * R * R * ir3;
+  return R * Z * (Phipp * ir2 - Phip * ir3);
+}
+
+/* potential value (<name>Eval) */
+static double sph_eval(const ocomp *c, double R, double Z)
+{
+  double amp = c->p[0];
+  switch (c->type) {
+  case PT_PLUMMER: {
+    double b2 = c->p[1] * c->p[1];
+    return -amp / sqrt(R * R + Z * Z + b2);
+  }
+  case PT_JAFFE: {
+    double a = c->p[1], sqrtRz = pow(R * R + Z * Z, 0.5);
+    return -amp * log(1. + a / sqrtRz) / a;
+  }
+  case PT_ISOCHRONE: {
+    double b = c->p[1], r2 = R * R + Z * Z;
+    return -amp / (b + sqrt(r2 + b * b));
+  }
+  case PT_POWER: {
+    double alpha = c->p[1];
+    if (alpha == 2.) return 0.5 * amp * log(R * R + Z * Z);
+    return -amp * pow(R * R + Z * Z, 1. - 0.5 * alpha) / (alpha - 2.);
+  }
+  case PT_BURKERT: {
+    double a = c->p[1], x = sqrt(R * R + Z * Z) / a;
+    return -amp * a * a * M_PI / x *
+           (-M_PI + 2. * (1. + x) * atan(1 / x) + 2. * (1. + x) * log(1. + x) +
+            (1. - x) * log(1. + x * x));
+  }
+  case PT_PSEUDOISO: {
+    double a = c->p[1], a2 = a * a, r2 = R * R + Z * Z, r = sqrt(r2);
+    return amp * (0.5 * log(1 + r2 / a2) + a / r * atan(r / a)) / a;
+  }
+  case PT_DEHNENCORE: {
+    double a = c->p[1], sqrtRz = pow(R * R + Z * Z, 0.5);
+    return -amp * (1. - pow(sqrtRz / (sqrtRz + a), 2.)) / (6. * a);
+  }
+  case PT_DEHNEN: {
+    double a = c->p[1], alpha = c->p[2], sqrtRz = pow(R * R + Z * Z, 0.5);
+    return -amp * (1. - pow(sqrtRz / (sqrtRz + a), 2. - alpha)) /
+           (a * (2. - alpha) * (3. - alpha));
+  }
+  case PT_HOMSPHERE: {
+    double R2 = c->p[1], R3 = c->p[2], r2 = R * R + Z * Z;
+    if (r2 < R2) return amp * (r2 - 3. * R2);
+    return -2. * amp * R3 / sqrt(r2);
+  }
+  }
+  return 0.;
+}
+
 /* Decode galpy's (pot_type, pot_args) stream (integrateFullOrbit.c:69-1040,
-   integratePlanarOrbit.c:55-742 restricted to types 0/5/8/9/15).
+   integratePlanarOrbit.c:55-742 restricted to types 0/5/7/8/9/10/14/15/17/
+   18/20/33/34/35/40).
    Returns 0, or -1 for an unsupported type. */
 static int opot_decode(opot *P, int npot, const int *type, const double *args, int planar)
 {
@@ -132,6 +382,7 @@ static double lh_Rt2(const ocomp *c, double R, double phi)
 /* ---- 3D component forces ---- */
 static double comp_Rforce(ocomp *c, double R, double Z, double phi)
 {
+  if (is_new_spherical(c->type)) return sph_force3(c, R, Z, R);
   double amp = c->p[0];
   switch (c->type) {
   case PT_LOGHALO: {
@@ -162,6 +413,7 @@ static double comp_Rforce(ocomp *c, double R, double Z, double phi)
 
 static double comp_zforce(ocomp *c, double R, double Z, double phi)
 {
+  if (is_new_spherical(c->type)) return sph_force3(c, R, Z, Z);
   double amp = c->p[0];
   switch (c->type) {
   case PT_LOGHALO: {
@@ -219,6 +471,7 @@ static void sph_derivs(const ocomp *c, double r, double *dphi, double *d2phi)
 /* 3D Hessian terms: which = 0 R2, 1 z2, 2 Rz, 3 phi2, 4 Rphi, 5 zphi */
 static double comp_hess(const ocomp *c, int which, double R, double Z, double phi)
 {
+  if (is_new_spherical(c->type)) return sph_hess3(c, which, R, Z);
   double amp = c->p[0];
   switch (c->type) {
   case PT_LOGHALO: {
@@ -324,6 +577,7 @@ static double comp_hess(const ocomp *c, int which, double R, double Z, double ph
 /* ---- planar component forces ---- */
 static double comp_planarRforce(const ocomp *c, double R, double phi)
 {
+  if (is_new_spherical(c->type)) return sph_planarRforce(c, R);
   double amp = c->p[0];
   switch (c->type) {
   case PT_LOGHALO: {
@@ -364,6 +618,7 @@ static double comp_planarphitorque(const ocomp *c, double R, double phi)
 /* planar Hessian: which = 0 R2, 1 phi2, 2 Rphi */
 static double comp_planarhess(const ocomp *c, int which, double R, double phi)
 {
+  if (is_new_spherical(c->type)) return which ? 0. : sph_planarR2deriv(c, R);
   double amp = c->p[0];
   switch (c->type) {
   case PT_LOGHALO: {
@@ -408,6 +663,7 @@ static double comp_planarhess(const ocomp *c, int which, double R, double phi)
 /* ---- potential values (for energies) ---- */
 static double comp_eval(const ocomp *c, double R, double Z, double phi)
 {
+  if (is_new_spherical(c->type)) return sph_eval(c, R, Z);
   double amp = c->p[0];
   switch (c->type) {
   case PT_LOGHALO: {

@@ -9,12 +9,16 @@ Two kinds of vectors are written to golden.npz:
   MWPotential2014 argument vector galpy passes to C (_parse_pot), and the
   Python-side forces, second derivatives and potential values of
   MWPotential2014 / Hernquist / LogarithmicHalo (axisymmetric and
-  triaxial) at fixed points, plus galpy's pure-Python DOP853 orbits
-  (galpy/util/leung_dop853.py) in MWPotential2014;
+  triaxial) / NFW / MiyamotoNagai / PowerSphericalwCutoff and of the
+  spherical PowerSpherical, Kepler, Jaffe, Isochrone, Plummer,
+  PseudoIsothermal, Burkert, DehnenCoreSpherical, DehnenSpherical,
+  HomogeneousSphere and Null potentials at fixed points, plus
+  galpy's pure-Python DOP853 orbits (galpy/util/leung_dop853.py) in
+  MWPotential2014;
 * from the reference's own C integrators (integrateFullOrbit /
   integratePlanarOrbit / *_dxdv built from its sources into oracle/_ref):
   small seeded batches for every implemented method, 3D, planar and
-  variational.
+  variational, and runs in each of the spherical potentials.
 
 The CPU oracle is checked against these in tests/test_oracle.py, so it stays
 pinned on machines that have neither the reference tree nor oracle/_ref.
@@ -90,6 +94,24 @@ def main():
         "mn": [gp.MiyamotoNagaiPotential(a=0.5, b=0.1, normalize=0.7)],
         "pswc": [gp.PowerSphericalPotentialwCutoff(alpha=1.2, rc=0.5, normalize=0.2)],
     }
+    # the spherical potentials added behind the same component template
+    sph = {
+        "power": [gp.PowerSphericalPotential(amp=1.0, alpha=1.8)],
+        "kepler": [gp.KeplerPotential(amp=0.9)],
+        "jaffe": [gp.JaffePotential(amp=1.2, a=0.8)],
+        "isochrone": [gp.IsochronePotential(amp=1.1, b=0.6)],
+        "plummer": [gp.PlummerPotential(amp=1.0, b=0.5)],
+        "pseudoiso": [gp.PseudoIsothermalPotential(amp=0.9, a=0.7)],
+        "burkert": [gp.BurkertPotential(amp=1.3, a=0.9)],
+        "dehnencore": [gp.DehnenCoreSphericalPotential(amp=2.5, a=0.7)],
+        "dehnen": [gp.DehnenSphericalPotential(amp=2.2, a=0.6, alpha=1.2)],
+        "homsphere": [gp.HomogeneousSpherePotential(amp=0.4, R=1.5)],
+        # galpy drops NullPotentials from combined lists before parsing, so
+        # type 40 reaches C only on its own; its Python value is the
+        # constant amp, which C never evaluates
+        "null": [gp.NullPotential()],
+    }
+    pots.update(sph)
     for name, p in pots.items():
         _, t_, a_, _ = parse3(p)
         out[f"{name}_type"] = np.asarray(t_, np.int32)
@@ -110,6 +132,25 @@ def main():
     out["pydop_t"] = ts
     out["pydop_orbit"] = np.stack([o.R(ts), o.vR(ts), o.vT(ts), o.z(ts), o.vz(ts), o.phi(ts)],
                                   -1)
+
+    # the reference's own C integrators in the spherical potentials:
+    # dop853 in 3D, symplec4 in the plane, dop853 variational in 3D
+    ics = seeded_ics(8, 0)
+    ics2 = seeded_ics(8, 1, planar=True)
+    t = np.linspace(0, 5, 51)
+    w = np.zeros((2, 12))
+    w[:, :6] = cyl_to_rect(ics[:2])
+    w[0, 6] = w[1, 10] = 1.0
+    for name, p in sph.items():
+        _, ptn, pan, _ = parse3(p)
+        _, ptn2, pan2, _ = parse2(gp.toPlanarPotential(p))
+        res, _, _, _ = O.integrate(ics, t, ptn, pan, "dop853", impl="ref")
+        out[f"sph_{name}_3d"] = res
+        res, _, _, _ = O.integrate(ics2, t, ptn2, pan2, "symplec4", planar=True, impl="ref")
+        out[f"sph_{name}_planar"] = res
+        res, _, _ = O.integrate_dxdv(w, t, ptn, pan, "dop853", impl="ref")
+        out[f"sph_{name}_dxdv3"] = res
+    out["sph_dxdv_w3"] = w
 
     # the reference's own C integrators
     ics = seeded_ics(8, 0)

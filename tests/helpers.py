@@ -101,3 +101,8 @@ def differentiation_workload(n, seed=3):
     w0 = cyl_to_rect(seeded_ics(n, seed, planar=True))
     tgt = cyl_to_rect(seeded_ics(n, seed + 100, planar=True))
     return np.ascontiguousarray(w0), np.ascontiguousarray(tgt)
+
+
+# spherical potentials behind the component template (golden-vector names)
+SPHERICAL = ["power", "kepler", "jaffe", "isochrone", "plummer", "pseudoiso", "burkert",
+             "dehnencore", "dehnen", "homsphere", "null"]

@@ -62,11 +62,21 @@ def test_planar_orbit_routes(hooks):
 
 def test_unsupported_potential_falls_back(hooks):
     from galpy.orbit import Orbit
+    from galpy.potential import KuzminDiskPotential
+
+    o = Orbit([1.0, 0.1, 1.1, 0.0, 0.1, 0.0])
+    o.integrate(np.linspace(0, 1, 11), KuzminDiskPotential(normalize=1.0), method="dop853_cuda")
+    assert hooks == []  # galpy's own integrator ran
+
+
+def test_spherical_potential_routes(hooks):
+    from galpy.orbit import Orbit
     from galpy.potential import PlummerPotential
 
     o = Orbit([1.0, 0.1, 1.1, 0.0, 0.1, 0.0])
-    o.integrate(np.linspace(0, 1, 11), PlummerPotential(normalize=1.0), method="dop853_cuda")
-    assert hooks == []  # galpy's own integrator ran
+    o.integrate(np.linspace(0, 1, 11), PlummerPotential(normalize=1.0), method="dopr54_cuda")
+    assert len(hooks) == 1 and hooks[-1]["method"] == "dopr54_cuda"
+    assert type(hooks[-1]["pot"]).__name__ == "PlummerPotential"
 
 
 def test_unknown_method_still_rejected(hooks):

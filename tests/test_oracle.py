@@ -9,7 +9,7 @@
 """
 import numpy as np
 import pytest
-from helpers import cyl_to_rect, seeded_ics
+from helpers import SPHERICAL, cyl_to_rect, seeded_ics
 
 METHODS = ["leapfrog", "rk4", "rk6", "symplec4", "symplec6", "dopr54", "dop853"]
 
@@ -108,7 +108,8 @@ def test_incomplete_gamma_vs_scipy(oracle):
     assert worst < 5e-14, worst
 
 
-@pytest.mark.parametrize("name", ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"])
+@pytest.mark.parametrize("name", ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"]
+                         + SPHERICAL)
 def test_oracle_forces_vs_galpy_python(oracle, golden, name):
     """C-side formulas restated in the oracle agree with galpy's Python
     potentials (different code, same mathematics)."""
@@ -118,9 +119,47 @@ def test_oracle_forces_vs_galpy_python(oracle, golden, name):
     f = oracle.forces(R, z, phi, pt, pa)
     pot = oracle.potential(R, z, phi, pt, pa)
     got = np.stack([f[:, 0], f[:, 1], f[:, 2], f[:, 3], f[:, 4], f[:, 5], pot], 1)
+    if name == "null":  # zero forces; galpy's Python value is the constant amp, C has none
+        assert not got[:, :6].any() and np.all(py[:, :6] == 0)
+        return
     scale = np.abs(py).max(0) + 1e-300
     err = np.abs(got - py) / scale
     assert err.max() < 1e-11, err.max(0)
+
+
+@pytest.mark.parametrize("name", SPHERICAL)
+def test_oracle_spherical_potentials(oracle, golden, name):
+    """The reference's own C in each spherical potential: golden vectors
+    (dop853 3D, symplec4 planar, dop853 variational) and, where the reference
+    build is present, bit for bit over all methods."""
+    pt, pa = golden[f"{name}_type"], golden[f"{name}_args"]
+    t = np.linspace(0, 5, 51)
+    a, _, _, _ = oracle.integrate(golden["c_ics"], t, pt, pa, "dop853")
+    np.testing.assert_allclose(a, golden[f"sph_{name}_3d"], rtol=0, atol=1e-13)
+    a, _, _, _ = oracle.integrate(golden["c_ics_planar"], t, pt, pa, "symplec4", planar=True)
+    np.testing.assert_allclose(a, golden[f"sph_{name}_planar"], rtol=0, atol=1e-13)
+    a, _, _ = oracle.integrate_dxdv(golden["sph_dxdv_w3"], t, pt, pa, "dop853")
+    np.testing.assert_allclose(a, golden[f"sph_{name}_dxdv3"], rtol=0, atol=1e-12)
+    if not oracle.ref_available():
+        return
+    ics = seeded_ics(6, 7)
+    ics2 = seeded_ics(6, 8, planar=True)
+    t = np.linspace(0, 8, 41)
+    for m in ("leapfrog", "symplec4", "symplec6", "rk4", "rk6", "dopr54", "dop853"):
+        a, ea, _, _ = oracle.integrate(ics, t, pt, pa, m, rtol=1e-10, atol=1e-10)
+        b, eb, _, _ = oracle.integrate(ics, t, pt, pa, m, rtol=1e-10, atol=1e-10, impl="ref")
+        assert np.array_equal(a, b) and np.array_equal(ea, eb), m
+        a, _, _, _ = oracle.integrate(ics2, t, pt, pa, m, planar=True, rtol=1e-10, atol=1e-10)
+        b, _, _, _ = oracle.integrate(ics2, t, pt, pa, m, planar=True, rtol=1e-10, atol=1e-10,
+                                      impl="ref")
+        assert np.array_equal(a, b), m
+    w = np.zeros((4, 8))
+    w[:, :4] = cyl_to_rect(ics2[:4])
+    w[np.arange(4), 4 + np.arange(4)] = 1.0
+    for m in ("symplec4", "dop853"):
+        a, _, _ = oracle.integrate_dxdv(w, t, pt, pa, m, planar=True)
+        b, _, _ = oracle.integrate_dxdv(w, t, pt, pa, m, planar=True, impl="ref")
+        assert np.array_equal(a, b), m
 
 
 def test_oracle_dop853_vs_galpy_python_dop853(oracle, golden):
