@@ -29,6 +29,7 @@ inline int galpy_nargs(int type, int planar)
     case T_BURKERT: case T_DEHNENCORE: return 2;
     case T_DEHNEN: case T_HOMSPHERE: return 3;
     case T_NULL: return 0;
+    case T_FLATPOWER: return planar ? 3 : 4;
     default: return -1;
   }
 }
@@ -271,6 +272,16 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
         break;
       case T_NULL:
         break;
+      case T_FLATPOWER: {  // (amp, alpha, q^2, core^2); planar (amp, alpha, core^2)
+        const double alpha = p[1], q2 = planar ? 1.0 : p[2], core2 = planar ? p[2] : p[3];
+        if (!(q2 > 0.0)) return -1;
+        c.c[1] = 1.0 / q2;
+        c.c[2] = core2;
+        c.c[3] = -0.5 * alpha - 1.0;
+        c.c[4] = alpha;
+        c.c[5] = alpha + 2.0;
+        break;
+      }
     }
     for (int i = 0; i < kChebN; i++)
       for (int j = 0; j < kChebC; j++) c.chebf[i][j] = (float)c.cheb[i][j];

@@ -6,7 +6,8 @@
 // axisymmetric or triaxial), and the spherical PowerSpherical (7), Jaffe
 // (10), Isochrone (14), Plummer (17), PseudoIsothermal (18), Burkert (20),
 // DehnenCoreSpherical (33), DehnenSpherical (34), HomogeneousSphere (35) and
-// Null (40) potentials.  Reference formulas:
+// Null (40) potentials, and the axisymmetric FlattenedPower (12).  Reference
+// formulas:
 // galpy/potential/potential_c_ext/<name>.c.
 //
 // Design (not a translation of the reference's cylindrical route):
@@ -46,6 +47,8 @@ enum : int { T_LOGHALO = 0, T_MN = 5, T_HERNQUIST = 8, T_NFW = 9, T_PSWC = 15 };
 // HomogeneousSphere, Null (no force)
 enum : int { T_POWER = 7, T_JAFFE = 10, T_ISOCHRONE = 14, T_PLUMMER = 17, T_PSEUDOISO = 18,
              T_BURKERT = 20, T_DEHNENCORE = 33, T_DEHNEN = 34, T_HOMSPHERE = 35, T_NULL = 40 };
+// axisymmetric FlattenedPowerPotential (FlattenedPowerPotential.c)
+enum : int { T_FLATPOWER = 12 };
 
 constexpr int kMaxComp = 16;  // components per potential group
 constexpr int kChebN = 32;    // Chebyshev intervals of gamma*(a, u) on [0, U]
@@ -66,6 +69,8 @@ constexpr int kBinSub = 8;    // sub-intervals of a binade [1, 2) in the binade 
 //   PseudoIsothermal: c1 a, c2 1/a       Burkert: c1 a, c2 1/a, c3 pi a^3
 //   DehnenSpherical: c1 a, c2 alpha, c3 1/(3 - alpha)
 //   HomogeneousSphere: c1 R^2, c2 R^3    Null: -
+//   FlattenedPower: c1 1/q^2 (1 in the plane), c2 core^2, c3 -alpha/2 - 1,
+//              c4 alpha, c5 alpha + 2
 //   PSwC potential (energy evaluation only): c8 2 pi rc^(3-alpha), c9 rc,
 //              c10 a1 = 1 - alpha/2, c11 Gamma(a1), c12 lgamma(a1),
 //              c13 a2 = 1.5 - alpha/2, c14 Gamma(a2), c15 lgamma(a2)
@@ -477,6 +482,16 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
       gz += f;
       break;
     }
+    case T_FLATPOWER: {
+      // Phi = -amp m^(-alpha) / alpha (alpha = 0: amp/2 ln m^2),
+      // m^2 = R^2 + z^2/q^2 + core^2: a = -amp (m^2)^(-alpha/2-1) (x, y, z/q^2)
+      const T iq2 = T(sc[1]);
+      const T m2 = R2 + z2 * iq2 + T(sc[2]);
+      const T g = -amp * Num<T>::ex(T(sc[3]) * Num<T>::lg(m2));
+      gR += g;
+      if (!PLANAR) gz += g * iq2;
+      break;
+    }
     case T_LOGHALO: {
       // Phi = amp/2 ln(x^2 + (1-e) y^2 + z^2/q^2 + core^2)
       const T iq2 = T(sc[1]);
@@ -711,6 +726,22 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
         K[5] -= amp * (iD3 * (sz - a * z2 * izb * izb * izb) - 3.0 * z2 * sz * sz * iD5);
         break;
       }
+      case T_FLATPOWER: {  // the logarithmic halo's structure with weight (alpha+2) m2^(-alpha/2-2)
+        const double iq2 = ldg(&cp->c[1]);
+        const double m2 = R2 + z2 * iq2 + ldg(&cp->c[2]);
+        const double pw = exp(ldg(&cp->c[3]) * log(m2)), g = -amp * pw;
+        const double h = amp * ldg(&cp->c[5]) * pw / m2;
+        const double ux = x, uy = y, uz = iq2 * z;
+        gR += g;
+        gz += g * iq2;
+        K[0] += g + h * ux * ux;
+        K[1] += h * ux * uy;
+        K[2] += g + h * uy * uy;
+        K[3] += h * ux * uz;
+        K[4] += h * uy * uz;
+        K[5] += g * iq2 + h * uz * uz;
+        break;
+      }
       case T_LOGHALO: {
         const double iq2 = ldg(&cp->c[1]), ye = ldg(&cp->c[3]);
         const double D = x * x + ye * y * y + z2 * iq2 + ldg(&cp->c[2]);
@@ -848,6 +879,11 @@ GPC_HD inline double potential_value(const GpComp* __restrict__ comp, int ncomp,
       case T_LOGHALO: {
         const double D = x * x + ldg(&cp->c[3]) * y * y + z2 * ldg(&cp->c[1]) + ldg(&cp->c[2]);
         phi += 0.5 * amp * log(D);
+        break;
+      }
+      case T_FLATPOWER: {
+        const double m2 = R2 + z2 * ldg(&cp->c[1]) + ldg(&cp->c[2]), alpha = ldg(&cp->c[4]);
+        phi += alpha == 0.0 ? 0.5 * amp * log(m2) : -amp * pow(m2, -0.5 * alpha) / alpha;
         break;
       }
       default:

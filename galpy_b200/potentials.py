@@ -3,7 +3,8 @@
 The engine integrates in the potentials galpy hands to C as pot_type codes
 0 (LogarithmicHaloPotential), 5 (MiyamotoNagaiPotential), 8
 (HernquistPotential), 9 (NFWPotential), 15 (PowerSphericalPotentialwCutoff)
-and the spherical 7 (PowerSpherical / Kepler), 10 (Jaffe), 14 (Isochrone),
+12 (FlattenedPower) and the spherical 7 (PowerSpherical / Kepler), 10
+(Jaffe), 14 (Isochrone),
 17 (Plummer), 18 (PseudoIsothermal), 20 (Burkert), 33
 (DehnenCoreSpherical), 34 (DehnenSpherical), 35 (HomogeneousSphere) and 40
 (Null) -- the parsing is
@@ -27,7 +28,8 @@ T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC = 0, 5, 8, 9, 15
 # PseudoIsothermal, Burkert, DehnenCoreSpherical, DehnenSpherical,
 # HomogeneousSphere, Null
 SPHERICAL_TYPES = (7, 10, 14, 17, 18, 20, 33, 34, 35, 40)
-SUPPORTED_TYPES = (T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC) + SPHERICAL_TYPES
+T_FLATPOWER = 12
+SUPPORTED_TYPES = (T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC, T_FLATPOWER) + SPHERICAL_TYPES
 
 
 class _Potential:

@@ -12,7 +12,7 @@
  *            LogarithmicHaloPotential.c:5-297, and the spherical
  *            PowerSpherical, Jaffe, Isochrone, Plummer, PseudoIsothermal,
  *            Burkert, DehnenCore, Dehnen, HomogeneousSphere potentials and
- *            ZeroForce (potential_c_ext/)
+ *            ZeroForce, FlattenedPowerPotential.c (potential_c_ext/)
  *   sums     galpy_potentials.c:120-354 (sum over components, in order)
  *   RHS      orbit_c_ext/integrateFullOrbit.c:1307-1352 (evalRectForce,
  *            evalRectDeriv), :1496-1681 (the dxdv variants);
@@ -64,6 +64,9 @@ enum {
   PT_HOMSPHERE = 35,  /* HomogeneousSpherePotential */
   PT_NULL = 40        /* NullPotential (ZeroForce) */
 };
+/* axisymmetric: FlattenedPowerPotential (FlattenedPowerPotential.c); args
+   (amp, alpha, q^2, core^2) in 3D, (amp, alpha, core^2) in the plane */
+enum { PT_FLATPOWER = 12 };
 #define OMAXPOT 32
 
 typedef struct {
@@ -90,6 +93,7 @@ static int nargs_of(int type, int planar)
   case PT_BURKERT: case PT_DEHNENCORE: return 2;
   case PT_DEHNEN: case PT_HOMSPHERE: return 3;
   case PT_NULL: return 0;
+  case PT_FLATPOWER: return planar ? 3 : 4;
   default: return -1;
   }
 }
@@ -324,8 +328,8 @@ static double sph_eval(const ocomp *c, double R, double Z)
 }
 
 /* Decode galpy's (pot_type, pot_args) stream (integrateFullOrbit.c:69-1040,
-   integratePlanarOrbit.c:55-742 restricted to types 0/5/7/8/9/10/14/15/17/
-   18/20/33/34/35/40).
+   integratePlanarOrbit.c:55-742 restricted to types 0/5/7/8/9/10/12/14/15/
+   17/18/20/33/34/35/40).
    Returns 0, or -1 for an unsupported type. */
 static int opot_decode(opot *P, int npot, const int *type, const double *args, int planar)
 {
@@ -385,6 +389,12 @@ static double comp_Rforce(ocomp *c, double R, double Z, double phi)
   if (is_new_spherical(c->type)) return sph_force3(c, R, Z, R);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_FLATPOWER: {
+    double alpha = c->p[1], q2 = c->p[2], core2 = c->p[3], m2;
+    if (alpha == 0.) return -amp * R / (R * R + Z * Z / q2 + core2);
+    m2 = core2 + R * R + Z * Z / q2;
+    return -amp * pow(m2, -0.5 * alpha - 1.) * R;
+  }
   case PT_LOGHALO: {
     double q = c->p[1], cc = c->p[2], om = c->p[3], zq = Z / q;
     if (om < 1) {
@@ -416,6 +426,12 @@ static double comp_zforce(ocomp *c, double R, double Z, double phi)
   if (is_new_spherical(c->type)) return sph_force3(c, R, Z, Z);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_FLATPOWER: {
+    double alpha = c->p[1], q2 = c->p[2], core2 = c->p[3], m2;
+    if (alpha == 0.) return -amp * Z / q2 / (R * R + Z * Z / q2 + core2);
+    m2 = core2 + R * R + Z * Z / q2;
+    return -amp * pow(m2, -0.5 * alpha - 1.) * Z / q2;
+  }
   case PT_LOGHALO: {
     double q = c->p[1], cc = c->p[2], om = c->p[3], zq = Z / q;
     if (om < 1) {
@@ -474,6 +490,21 @@ static double comp_hess(const ocomp *c, int which, double R, double Z, double ph
   if (is_new_spherical(c->type)) return sph_hess3(c, which, R, Z);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_FLATPOWER: {
+    double alpha = c->p[1], q2 = c->p[2], core2 = c->p[3], denom, m2;
+    if (which > 2) return 0.;
+    if (alpha == 0.) {
+      denom = 1. / (R * R + Z * Z / q2 + core2);
+      if (which == 0) return amp * (denom - 2. * R * R * denom * denom);
+      if (which == 1) return amp / q2 * (denom - 2. * Z * Z * denom * denom / q2);
+      return -2. * amp * R * Z / q2 * denom * denom;
+    }
+    m2 = core2 + R * R + Z * Z / q2;
+    if (which == 0) return -amp * pow(m2, -0.5 * alpha - 1.) * ((alpha + 2.) * R * R / m2 - 1.);
+    if (which == 1)
+      return -amp / q2 * pow(m2, -0.5 * alpha - 1.) * ((alpha + 2.) * Z * Z / m2 / q2 - 1.);
+    return -amp * (alpha + 2.) * R * Z / q2 * pow(m2, -0.5 * alpha - 2.);
+  }
   case PT_LOGHALO: {
     double q = c->p[1], cc = c->p[2], om = c->p[3], zq = Z / q, q2 = q * q;
     double Rt2, denom;
@@ -580,6 +611,12 @@ static double comp_planarRforce(const ocomp *c, double R, double phi)
   if (is_new_spherical(c->type)) return sph_planarRforce(c, R);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_FLATPOWER: {
+    double alpha = c->p[1], core2 = c->p[2], m2;
+    if (alpha == 0.) return -amp * R / (R * R + core2);
+    m2 = core2 + R * R;
+    return -amp * pow(m2, -0.5 * alpha - 1.) * R;
+  }
   case PT_LOGHALO: {
     double cc = c->p[2], om = c->p[3];
     if (om < 1) {
@@ -621,6 +658,13 @@ static double comp_planarhess(const ocomp *c, int which, double R, double phi)
   if (is_new_spherical(c->type)) return which ? 0. : sph_planarR2deriv(c, R);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_FLATPOWER: {
+    double alpha = c->p[1], core2 = c->p[2], m2;
+    if (which) return 0.;
+    if (alpha == 0.) return amp * (1. - 2. * R * R / (R * R + core2)) / (R * R + core2);
+    m2 = core2 + R * R;
+    return -amp * pow(m2, -0.5 * alpha - 1.) * ((alpha + 2.) * R * R / m2 - 1.);
+  }
   case PT_LOGHALO: {
     double cc = c->p[2], om = c->p[3];
     int tri = om < 1;
@@ -666,6 +710,11 @@ static double comp_eval(const ocomp *c, double R, double Z, double phi)
   if (is_new_spherical(c->type)) return sph_eval(c, R, Z);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_FLATPOWER: {
+    double alpha = c->p[1], q2 = c->p[2], core2 = c->p[3];
+    if (alpha == 0.) return 0.5 * amp * log(R * R + Z * Z / q2 + core2);
+    return -amp * pow(core2 + R * R + Z * Z / q2, -0.5 * alpha) / alpha;
+  }
   case PT_LOGHALO: {
     double q = c->p[1], cc = c->p[2], om = c->p[3], zq = Z / q;
     if (om < 1) return 0.5 * amp * log(R * R * (1. - om * pow(sin(phi), 2)) + zq * zq + cc);

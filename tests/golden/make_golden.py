@@ -110,6 +110,9 @@ def main():
         # type 40 reaches C only on its own; its Python value is the
         # constant amp, which C never evaluates
         "null": [gp.NullPotential()],
+        # axisymmetric (the same tests)
+        "flatpower": [gp.FlattenedPowerPotential(amp=1.1, alpha=0.5, q=0.8, core=0.3)],
+        "flatlog": [gp.FlattenedPowerPotential(amp=0.9, alpha=0.0, q=0.7, core=0.2)],
     }
     pots.update(sph)
     for name, p in pots.items():
@@ -144,6 +147,8 @@ def main():
     for name, p in sph.items():
         _, ptn, pan, _ = parse3(p)
         _, ptn2, pan2, _ = parse2(gp.toPlanarPotential(p))
+        out[f"{name}_planar_type"] = np.asarray(ptn2, np.int32)
+        out[f"{name}_planar_args"] = np.asarray(pan2)
         res, _, _, _ = O.integrate(ics, t, ptn, pan, "dop853", impl="ref")
         out[f"sph_{name}_3d"] = res
         res, _, _, _ = O.integrate(ics2, t, ptn2, pan2, "symplec4", planar=True, impl="ref")

@@ -103,6 +103,15 @@ def differentiation_workload(n, seed=3):
     return np.ascontiguousarray(w0), np.ascontiguousarray(tgt)
 
 
-# spherical potentials behind the component template (golden-vector names)
+# the spherical (and the axisymmetric FlattenedPower) potentials added
+# behind the component template (golden-vector names)
 SPHERICAL = ["power", "kepler", "jaffe", "isochrone", "plummer", "pseudoiso", "burkert",
-             "dehnencore", "dehnen", "homsphere", "null"]
+             "dehnencore", "dehnen", "homsphere", "null", "flatpower", "flatlog"]
+
+
+def golden_pot(golden, name, planar=False):
+    """(pot_type, pot_args) of a golden potential as galpy parses it (the
+    planar argument list where the golden file holds one)."""
+    if planar and f"{name}_planar_args" in golden:
+        return golden[f"{name}_planar_type"], golden[f"{name}_planar_args"]
+    return golden[f"{name}_type"], golden[f"{name}_args"]

@@ -10,7 +10,7 @@ import ctypes
 
 import numpy as np
 import pytest
-from helpers import SPHERICAL, cyl_diff, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
+from helpers import SPHERICAL, cyl_diff, golden_pot, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
 
 import galpy_b200 as gb
 from galpy_b200 import _lib
@@ -196,8 +196,9 @@ def test_spherical_potentials(oracle, golden, name):
     out, err = gb.integrateFullOrbit_cuda((pt, pa), golden["c_ics"].copy(), t, "dop853_cuda",
                                           progressbar=False)
     assert not err.any() and cyl_diff(golden[f"sph_{name}_3d"], out).max() < tol
-    out, err = gb.integratePlanarOrbit_cuda((pt, pa), golden["c_ics_planar"].copy(), t,
-                                            "symplec4_cuda", progressbar=False)
+    out, err = gb.integratePlanarOrbit_cuda(golden_pot(golden, name, True),
+                                            golden["c_ics_planar"].copy(), t, "symplec4_cuda",
+                                            progressbar=False)
     assert not err.any() and cyl_diff(golden[f"sph_{name}_planar"], out).max() < tol
     ref = golden[f"sph_{name}_dxdv3"]
     out, err = gb.integrate_dxdv_batch((pt, pa), golden["sph_dxdv_w3"], t, "dop853_cuda")
@@ -401,7 +402,8 @@ def test_device_accelerations(golden, harness, name, planar):
     tolerance of the host build against the reference's formulas too)."""
     import torch
 
-    pt, pa = golden[f"{name}_type"], np.array(golden[f"{name}_args"], float)
+    pt, pa = golden_pot(golden, name, planar)
+    pa = np.array(pa, float)
     if planar and int(pt[0]) == 15:
         pa = pa[:3]
     if planar and name == "mw14":

@@ -4,7 +4,7 @@ against the CPU oracle.  This checks the kernel logic on every CPU-only run;
 tests/test_gpu_parity.py checks the compiled kernels on the GPU."""
 import numpy as np
 import pytest
-from helpers import SPHERICAL, cyl_diff, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
+from helpers import SPHERICAL, cyl_diff, golden_pot, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
 
 METHODS = ["leapfrog", "rk4", "rk6", "symplec4", "symplec6", "dopr54", "dop853"]
 POTS = ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"] + SPHERICAL
@@ -99,9 +99,10 @@ def test_spherical_potential_orbits(harness, oracle, golden, name):
     """Orbits in each spherical potential: the same step sequence as the
     oracle and agreement to the orbits' conditioning, 3D, planar and
     variational."""
-    pt, pa = golden[f"{name}_type"], golden[f"{name}_args"]
+    pt, pa = golden_pot(golden, name)
     t = np.linspace(0, 8, 41)
     for planar, m in ((False, "dop853"), (False, "symplec6"), (True, "dopr54"), (True, "rk4")):
+        pt, pa = golden_pot(golden, name, planar)
         ics = seeded_ics(8, 17, planar=planar)
         ref, _, nref, _ = oracle.integrate(ics, t, pt, pa, m, planar=planar, rtol=1e-10,
                                            atol=1e-10)
@@ -118,6 +119,7 @@ def test_spherical_potential_orbits(harness, oracle, golden, name):
         else:
             assert same.all(), m
         assert d[same].max() < 1e-10, m
+    pt, pa = golden_pot(golden, name)
     w = unit_deviations(cyl_to_rect(seeded_ics(2, 18)), 3)
     ref, _, nref = oracle.integrate_dxdv(w, t, pt, pa, "dop853")
     out, err, ns = harness.integrate(w, t, pt, pa, "dop853", var=True)

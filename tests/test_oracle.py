@@ -9,7 +9,7 @@
 """
 import numpy as np
 import pytest
-from helpers import SPHERICAL, cyl_to_rect, seeded_ics
+from helpers import SPHERICAL, cyl_to_rect, golden_pot, seeded_ics
 
 METHODS = ["leapfrog", "rk4", "rk6", "symplec4", "symplec6", "dopr54", "dop853"]
 
@@ -132,11 +132,12 @@ def test_oracle_spherical_potentials(oracle, golden, name):
     """The reference's own C in each spherical potential: golden vectors
     (dop853 3D, symplec4 planar, dop853 variational) and, where the reference
     build is present, bit for bit over all methods."""
-    pt, pa = golden[f"{name}_type"], golden[f"{name}_args"]
+    pt, pa = golden_pot(golden, name)
+    pt2, pa2 = golden_pot(golden, name, planar=True)
     t = np.linspace(0, 5, 51)
     a, _, _, _ = oracle.integrate(golden["c_ics"], t, pt, pa, "dop853")
     np.testing.assert_allclose(a, golden[f"sph_{name}_3d"], rtol=0, atol=1e-13)
-    a, _, _, _ = oracle.integrate(golden["c_ics_planar"], t, pt, pa, "symplec4", planar=True)
+    a, _, _, _ = oracle.integrate(golden["c_ics_planar"], t, pt2, pa2, "symplec4", planar=True)
     np.testing.assert_allclose(a, golden[f"sph_{name}_planar"], rtol=0, atol=1e-13)
     a, _, _ = oracle.integrate_dxdv(golden["sph_dxdv_w3"], t, pt, pa, "dop853")
     np.testing.assert_allclose(a, golden[f"sph_{name}_dxdv3"], rtol=0, atol=1e-12)
@@ -149,16 +150,16 @@ def test_oracle_spherical_potentials(oracle, golden, name):
         a, ea, _, _ = oracle.integrate(ics, t, pt, pa, m, rtol=1e-10, atol=1e-10)
         b, eb, _, _ = oracle.integrate(ics, t, pt, pa, m, rtol=1e-10, atol=1e-10, impl="ref")
         assert np.array_equal(a, b) and np.array_equal(ea, eb), m
-        a, _, _, _ = oracle.integrate(ics2, t, pt, pa, m, planar=True, rtol=1e-10, atol=1e-10)
-        b, _, _, _ = oracle.integrate(ics2, t, pt, pa, m, planar=True, rtol=1e-10, atol=1e-10,
+        a, _, _, _ = oracle.integrate(ics2, t, pt2, pa2, m, planar=True, rtol=1e-10, atol=1e-10)
+        b, _, _, _ = oracle.integrate(ics2, t, pt2, pa2, m, planar=True, rtol=1e-10, atol=1e-10,
                                       impl="ref")
         assert np.array_equal(a, b), m
     w = np.zeros((4, 8))
     w[:, :4] = cyl_to_rect(ics2[:4])
     w[np.arange(4), 4 + np.arange(4)] = 1.0
     for m in ("symplec4", "dop853"):
-        a, _, _ = oracle.integrate_dxdv(w, t, pt, pa, m, planar=True)
-        b, _, _ = oracle.integrate_dxdv(w, t, pt, pa, m, planar=True, impl="ref")
+        a, _, _ = oracle.integrate_dxdv(w, t, pt2, pa2, m, planar=True)
+        b, _, _ = oracle.integrate_dxdv(w, t, pt2, pa2, m, planar=True, impl="ref")
         assert np.array_equal(a, b), m
 
 
