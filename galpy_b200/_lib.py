@@ -25,6 +25,8 @@ F32FORCE = 1
 IN_AOS, IN_SOA = 0, 1
 OUT_GALPY, OUT_AOS_RECT, OUT_SOA_RECT, OUT_SOA_CYL = 0, 1, 2, 3
 
+SYS_ORBIT, SYS_SOS = 0, 1
+
 DT_SENTINEL = -9999.99
 
 
@@ -96,6 +98,7 @@ class GalpyCudaLaunch(ctypes.Structure):
         ("comps_host", ctypes.c_void_p),
         ("size_ext", ctypes.c_int),
         ("tail_sms", ctypes.c_int),
+        ("system", ctypes.c_int),
     ]
 
 
@@ -151,6 +154,11 @@ SIGNATURES = {
     "galpy_cuda_signature": (_ci, [_ci, _ip]),
     "galpy_cuda_compile_potential": (_ci, [_ci, _ci, _ip, _dp, _ci, _vp]),
     "integrateFullOrbit_cuda": (
+        _ci,
+        [_ci, _dp, _ci, _dp, _ci, _ci, _ip, _dp, _vp, _cd, _cd, _cd, _dp, _ip, _ci, CALLBACK,
+         _opts_p],
+    ),
+    "integrateFullOrbit_sos_cuda": (
         _ci,
         [_ci, _dp, _ci, _dp, _ci, _ci, _ip, _dp, _vp, _cd, _cd, _cd, _dp, _ip, _ci, CALLBACK,
          _opts_p],

@@ -114,9 +114,16 @@ struct CoreMethods {
   }
 };
 
-static KernelInfo pick_kernel(int planar, int var, int prec, int method, int sig, int variant,
-                              bool direct)
+// The ODE system of a launch (the field exists when size_ext >= 2).
+static int launch_system(const galpy_cuda_launch* L)
 {
+  return L->size_ext >= 2 ? L->system : GALPY_CUDA_SYS_ORBIT;
+}
+
+static KernelInfo pick_kernel(int planar, int var, int prec, int method, int sig, int variant,
+                              bool direct, int system = GALPY_CUDA_SYS_ORBIT)
+{
+  if (system == GALPY_CUDA_SYS_SOS) return pick_kernel_sos(method, variant);
   if (method == M_RK6 || method == M_SYMPLEC6 || method == M_DOPR54)
     return pick_kernel_more(planar, var, prec, method, sig, variant, direct);
   return pick_kernel_in<CoreMethods>(planar, var, prec, method, sig, variant, direct);
@@ -160,9 +167,10 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
 {
   double scal[kMaxComp * kScalarStride] = {0.0};
   const bool direct = direct_scalars(L, scal);
+  const int system = launch_system(L);
   const KernelInfo ki =
       pick_kernel(L->planar, L->variational, L->precision, L->odeint_type, L->signature,
-                  L->variant, direct);
+                  L->variant, direct, system);
   KernelFn fn = ki.fn;
   if (!fn) return set_error(GALPY_CUDA_ERR_METHOD, "method/precision combination not implemented");
   KArgs A;
@@ -196,9 +204,11 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
   memcpy(A.scal, scal, sizeof(scal));
   GPC_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(Scratch), stream));
 
-  // longest-first work queue (stream-ordered scratch, freed after the launch)
+  // longest-first work queue (stream-ordered scratch, freed after the launch);
+  // surface-of-section runs go in order (the cost pass reads orbit states)
   void* sched = nullptr;
-  if (L->schedule == GALPY_CUDA_SCHED_LONGEST_FIRST && L->nobj > 1 && L->nobj < (1LL << 31)) {
+  if (L->schedule == GALPY_CUDA_SCHED_LONGEST_FIRST && L->nobj > 1 && L->nobj < (1LL << 31) &&
+      system == GALPY_CUDA_SYS_ORBIT) {
     const int n = (int)L->nobj;
     size_t tmp_bytes = 0;
     cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, (float*)nullptr, (float*)nullptr,
@@ -273,6 +283,18 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
 static int check_launch(const galpy_cuda_launch* L)
 {
   if (!L) return set_error(GALPY_CUDA_ERR_ARG, "launch is NULL");
+  const int system = launch_system(L);
+  if (system != GALPY_CUDA_SYS_ORBIT && system != GALPY_CUDA_SYS_SOS)
+    return set_error(GALPY_CUDA_ERR_ARG, "unknown system");
+  if (system == GALPY_CUDA_SYS_SOS) {
+    const int m = L->odeint_type;
+    if (m != M_RK4 && m != M_RK6 && m != M_DOPR54 && m != M_DOP853)
+      return set_error(GALPY_CUDA_ERR_METHOD,
+                       "surface-of-section integration takes rk4, rk6, dopr54 or dop853");
+    if (L->planar || L->variational || L->precision != GALPY_CUDA_FP64)
+      return set_error(GALPY_CUDA_ERR_ARG,
+                       "surface-of-section integration is 3D, plain and float64");
+  }
   if (!method_supported(L->odeint_type))
     return set_error(GALPY_CUDA_ERR_METHOD, "odeint_type not implemented on the GPU");
   if (L->nobj < 0 || L->nt < 1 || !L->t || !L->w0 || !L->out || !L->err || !L->comps ||
@@ -356,7 +378,7 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
                     const double* t, int indiv_t, int npot, const int* pot_type,
                     const double* pot_args, double dt, double rtol, double atol, double* result,
                     int* err, int odeint_type, galpy_cuda_callback cb, const galpy_cuda_opts* o,
-                    bool rect_out)
+                    bool rect_out, int system = GALPY_CUDA_SYS_ORBIT)
 {
   int rc = select_device(o);
   if (rc) return rc;
@@ -426,6 +448,9 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
   L.schedule = o && o->size >= (int)sizeof(galpy_cuda_opts) ? o->schedule
                                                              : GALPY_CUDA_SCHED_LONGEST_FIRST;
   L.variant = o && o->size >= (int)sizeof(galpy_cuda_opts) ? o->variant : 0;
+  L.size_ext = 2;
+  L.tail_sms = -1;
+  L.system = system;
   rc = check_launch(&L);
   if (rc) return rc;
 
@@ -489,6 +514,23 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
   GPC_CUDA_TRY(cudaStreamSynchronize(stream));
   if (abort_sent) return GALPY_CUDA_ERR_INTERRUPTED;
   return GALPY_CUDA_OK;
+}
+
+// (R, vR, vT, z, vz, phi, t) -> surface-of-section state (x, y, vx, vy, A,
+// t, psi), in place, exactly as cyl_to_sos_galpy (bovy_coords.c:149-163)
+static void cyl_to_sos_inplace(long long nobj, double* yo)
+{
+  for (long long i = 0; i < nobj; i++) {
+    double* v = yo + 7 * i;
+    const double R = v[0], cp = cos(v[5]), sp = sin(v[5]), vR = v[1], vT = v[2];
+    v[5] = v[6];
+    v[6] = atan2(v[3], v[4]);
+    v[4] = sqrt(v[3] * v[3] + v[4] * v[4]);
+    v[0] = R * cp;
+    v[1] = R * sp;
+    v[2] = vR * cp - vT * sp;
+    v[3] = vR * sp + vT * cp;
+  }
 }
 
 // cylindrical -> rectangular initial conditions, in place, exactly as
@@ -835,9 +877,10 @@ int galpy_cuda_integrate_device_noalloc(const galpy_cuda_launch* L)
 
   double scal[kMaxComp * kScalarStride] = {0.0};
   const bool direct = direct_scalars(L, scal);
+  const int system = launch_system(L);
   const KernelInfo ki =
       pick_kernel(L->planar, L->variational, L->precision, L->odeint_type, L->signature,
-                  L->variant, direct);
+                  L->variant, direct, system);
   KernelFn fn = ki.fn;
   if (!fn) return set_error(GALPY_CUDA_ERR_METHOD, "method/precision combination not implemented");
   KArgs A;
@@ -870,7 +913,8 @@ int galpy_cuda_integrate_device_noalloc(const galpy_cuda_launch* L)
   // the array keeps the previous call's contents: zero the control words
   // and the bucket counters (a memset, not an allocation)
   GPC_CUDA_TRY(cudaMemsetAsync(scr, 0, kNoAllocBucket, stream));
-  if (L->schedule == GALPY_CUDA_SCHED_LONGEST_FIRST && L->nobj > 1) {
+  if (L->schedule == GALPY_CUDA_SCHED_LONGEST_FIRST && L->nobj > 1 &&
+      system == GALPY_CUDA_SYS_ORBIT) {
     const unsigned nb = (unsigned)((L->nobj + 255) / 256);
     if (L->planar)
       noalloc_bucket_kernel<2><<<nb, 256, 0, stream>>>(A, scr);
@@ -914,6 +958,24 @@ int integrateFullOrbit_cuda(int nobj, double* yo, int nt, double* t, int indiv_t
   cyl_to_rect_inplace(0, nobj, yo);
   return run_host(0, 0, nobj, yo, 6, nt, t, indiv_t, npot, pot_type, pot_args, dt, rtol, atol,
                   result, err, odeint_type, cb, opts, false);
+}
+
+int integrateFullOrbit_sos_cuda(int nobj, double* yo, int npsi, double* psi, int indiv_psi,
+                                int npot, int* pot_type, double* pot_args, void* /*pot_tfuncs*/,
+                                double dpsi, double rtol, double atol, double* result, int* err,
+                                int odeint_type, galpy_cuda_callback cb,
+                                const galpy_cuda_opts* opts)
+{
+  if (nobj < 0 || npsi < 1 || (nobj && (!yo || !psi || !result || !err)) || !pot_type ||
+      !pot_args)
+    return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
+  if (odeint_type != M_RK4 && odeint_type != M_RK6 && odeint_type != M_DOPR54 &&
+      odeint_type != M_DOP853)
+    return set_error(GALPY_CUDA_ERR_METHOD,
+                     "surface-of-section integration takes rk4, rk6, dopr54 or dop853");
+  cyl_to_sos_inplace(nobj, yo);
+  return run_host(0, 0, nobj, yo, 7, npsi, psi, indiv_psi, npot, pot_type, pot_args, dpsi, rtol,
+                  atol, result, err, odeint_type, cb, opts, false, GALPY_CUDA_SYS_SOS);
 }
 
 int integratePlanarOrbit_cuda(int nobj, double* yo, int nt, double* t, int indiv_t, int npot,

@@ -80,7 +80,24 @@ GPC_HD GPC_FI void write_row(const OutSpec& o, long long i, int j, const double*
   const long long nrow = o.nt - o.row0, jj = j - o.row0;
   double w[NV];
   const bool cyl = CYL_OK && (o.layout == L_GALPY_CYL || o.layout == L_SOA_CYL);
-  if (cyl) {
+  if constexpr (NV == 7) {
+    if (cyl) {
+      // surface of section (x, y, vx, vy, A, t, psi) -> (R, vR, vT, z, vz,
+      // phi, t): sos_to_cyl_galpy (bovy_coords.c:173-189)
+      const double x = v[0], y = v[1];
+      const double phi = atan2(y, x), cp = cos(phi), sp = sin(phi);
+      w[0] = sqrt(x * x + y * y);
+      w[1] = v[2] * cp + v[3] * sp;
+      w[2] = -v[2] * sp + v[3] * cp;
+      w[3] = v[4] * sin(v[6]);
+      w[4] = v[4] * cos(v[6]);
+      w[5] = phi;
+      w[6] = v[5];
+    } else {
+#pragma unroll
+      for (int k = 0; k < NV; k++) w[k] = v[k];
+    }
+  } else if (cyl) {
     // rect_to_cyl_galpy / rect_to_polar_galpy (bovy_coords.c:79-148)
     const double x = v[0], y = v[1];
     const double vx = v[D], vy = v[D + 1];
@@ -504,32 +521,15 @@ GPC_HD GPC_FI void rk6_stage(int s, double h, const double* yn, double* yn1, dou
   }
 }
 
-// derivative of the state y = (x, v[, dx, dv]) given the force result a
-template <int D, bool VAR, int N>
-GPC_HD GPC_FI void state_derivative(const double* y, const double* a, double* d)
-{
-#pragma unroll
-  for (int k = 0; k < D; k++) {
-    d[k] = y[D + k];
-    d[D + k] = a[k];
-    if (VAR) {
-      d[2 * D + k] = y[3 * D + k];
-      d[3 * D + k] = a[D + k];
-    }
-  }
-}
-
 // ------------------------------------------------------------------------
-// RK4 / RK6 (optionally variational)
+// ODE systems of the RK-type machines
 // ------------------------------------------------------------------------
-template <int D, bool VAR, int ORD>
-struct RKMachine : OrbitCommon {
-  static_assert(ORD == 4 || ORD == 6, "rk4 or rk6");
+// An orbit: y = (x, v[, dx, dv]) in rectangular coordinates; dy/dt from the
+// force at the positions (and K . dq for the deviations).
+template <int D, bool VAR>
+struct OrbitSystem {
   static constexpr int N = VAR ? 4 * D : 2 * D;  // ODE dimension
-  static constexpr int NY = N;
-  static constexpr int NV = N;
-  static constexpr int NA = VAR ? 2 * D : D;  // force result size
-  static constexpr int kStages = ORD == 4 ? 4 : 7;
+  static constexpr int NA = VAR ? 2 * D : D;     // force argument / result size
   // force argument: positions (and deviation positions) of (x, v[, dx, dv])
   GPC_HD GPC_FI static void pos(const double* y, double* q)
   {
@@ -539,6 +539,59 @@ struct RKMachine : OrbitCommon {
       if (VAR) q[D + k] = y[2 * D + k];
     }
   }
+  GPC_HD GPC_FI static void deriv(const double* y, const double* a, double* d)
+  {
+#pragma unroll
+    for (int k = 0; k < D; k++) {
+      d[k] = y[D + k];
+      d[D + k] = a[k];
+      if (VAR) {
+        d[2 * D + k] = y[3 * D + k];
+        d[3 * D + k] = a[D + k];
+      }
+    }
+  }
+};
+
+// Surface-of-section integration (evalSOSDeriv, integrateFullOrbit.c:
+// 1353-1390): y = (x, y, vx, vy, A, t, psi) with z = A sin(psi) and
+// vz = A cos(psi); the independent variable is the increment of psi, and
+// y[6] carries the absolute angle (d y[6] = 1).  The force is evaluated at
+// (x, y, A sin psi).
+struct SosSystem {
+  static constexpr int N = 7, NA = 3;
+  GPC_HD GPC_FI static void pos(const double* y, double* q)
+  {
+    q[0] = y[0];
+    q[1] = y[1];
+    q[2] = y[4] * sin(y[6]);
+  }
+  GPC_HD GPC_FI static void deriv(const double* y, const double* a, double* d)
+  {
+    const double sp = sin(y[6]), cp = cos(y[6]);
+    const double ipd = 1.0 / (cp * cp - sp * a[2] / y[4]);  // d psi / dt = cos^2 - sin az / A
+    d[0] = y[2] * ipd;
+    d[1] = y[3] * ipd;
+    d[2] = a[0] * ipd;
+    d[3] = a[1] * ipd;
+    d[4] = cp * (y[4] * sp + a[2]) * ipd;
+    d[5] = ipd;
+    d[6] = 1.0;
+  }
+};
+
+// ------------------------------------------------------------------------
+// RK4 / RK6 (optionally variational)
+// ------------------------------------------------------------------------
+template <int D, bool VAR, int ORD, class SYS = OrbitSystem<D, VAR>>
+struct RKMachine : OrbitCommon {
+  static_assert(ORD == 4 || ORD == 6, "rk4 or rk6");
+  static constexpr int N = SYS::N;  // ODE dimension
+  static constexpr int NY = N;
+  static constexpr int NV = N;
+  static constexpr int NA = SYS::NA;  // force result size
+  static constexpr int kStages = ORD == 4 ? 4 : 7;
+  GPC_HD GPC_FI static void pos(const double* y, double* q) { SYS::pos(y, q); }
   static constexpr int kSlotDoubles = 0;
   GPC_HD GPC_FI void bind(double*) {}
   GPC_HD GPC_FI bool wants_dense() const { return false; }
@@ -613,7 +666,7 @@ struct RKMachine : OrbitCommon {
   GPC_HD void consume(const double* y, const double* a, W& out, int /*slot*/)
   {
     double d[N];
-    state_derivative<D, VAR, N>(y, a, d);
+    SYS::deriv(y, a, d);
     if (ORD == 4)
       rk4_stage<N>(stage, h, yn, yn1, ynk, d);
     else
@@ -719,20 +772,13 @@ constexpr double e1 = b1 - 5179. / 57600., e3 = b3 - 7571. / 16695., e4 = b4 - 3
 // time or shrinks the step (at most 5 times in a row before a forced step),
 // and an accepted step that no longer advances the time ends the orbit
 // (err 2), so an orbit always finishes.
-template <int D, bool VAR>
+template <int D, bool VAR, class SYS = OrbitSystem<D, VAR>>
 struct Dopr54Machine : OrbitCommon {
-  static constexpr int N = VAR ? 4 * D : 2 * D;
+  static constexpr int N = SYS::N;
   static constexpr int NY = N;
   static constexpr int NV = N;
-  static constexpr int NA = VAR ? 2 * D : D;
-  GPC_HD GPC_FI static void pos(const double* y, double* q)
-  {
-#pragma unroll
-    for (int k = 0; k < D; k++) {
-      q[k] = y[k];
-      if (VAR) q[D + k] = y[2 * D + k];
-    }
-  }
+  static constexpr int NA = SYS::NA;
+  GPC_HD GPC_FI static void pos(const double* y, double* q) { SYS::pos(y, q); }
   static constexpr int kSlotDoubles = 0;
   GPC_HD GPC_FI void bind(double*) {}
   GPC_HD GPC_FI bool wants_dense() const { return false; }
@@ -806,7 +852,7 @@ struct Dopr54Machine : OrbitCommon {
   GPC_HD void consume(const double* y, const double* a, W& out, int /*slot*/)
   {
     double d[N];
-    state_derivative<D, VAR, N>(y, a, d);
+    SYS::deriv(y, a, d);
     if (phase < FSAL0) {
       rk4_stage<N>(stage, h, kk[0], yn1, ynk, d);
       if (++stage == 4) est_step_done();
@@ -1067,21 +1113,13 @@ GPC_HD GPC_FI const DopStageTable& dop_table()
 #endif
 }
 
-template <int D, bool VAR>
+template <int D, bool VAR, class SYS = OrbitSystem<D, VAR>>
 struct Dop853Machine : OrbitCommon {
-  static constexpr int N = VAR ? 4 * D : 2 * D;
+  static constexpr int N = SYS::N;
   static constexpr int NY = N;
   static constexpr int NV = N;
-  static constexpr int NA = VAR ? 2 * D : D;  // force result size
-  // force argument: positions (and deviation positions) of (x, v[, dx, dv])
-  GPC_HD GPC_FI static void pos(const double* y, double* q)
-  {
-#pragma unroll
-    for (int k = 0; k < D; k++) {
-      q[k] = y[k];
-      if (VAR) q[D + k] = y[2 * D + k];
-    }
-  }
+  static constexpr int NA = SYS::NA;  // force result size
+  GPC_HD GPC_FI static void pos(const double* y, double* q) { SYS::pos(y, q); }
   enum {
     ST_INIT1 = 0, ST_INIT2 = 1,
     // ST_S2..ST_S12 = 2..12
@@ -1205,15 +1243,7 @@ struct Dop853Machine : OrbitCommon {
     using namespace dp;
     if (!active_in(slot)) return;
     double d[N];
-#pragma unroll
-    for (int k = 0; k < D; k++) {
-      d[k] = y[D + k];
-      d[D + k] = a[k];
-      if (VAR) {
-        d[2 * D + k] = y[3 * D + k];
-        d[3 * D + k] = a[D + k];
-      }
-    }
+    SYS::deriv(y, a, d);
     if (stage == ST_INIT1) {  // leung_dop853.c:296-308
       double dny = 0.0;
       dnf = 0.0;
@@ -1348,6 +1378,14 @@ struct Dop853Machine : OrbitCommon {
       facold = dmax(e, 1.0e-4);
       stage = ST_FSAL;
     } else {
+      // an attempt rejected at the smallest step (begin_attempt's floor)
+      // repeats exactly -- same state, same step, same error -- so the
+      // reference rejects it forever; the orbit stops as out of budget
+      if (fabs(h) <= 1e3 * 2.3e-16) {
+        err = E_BUDGET;
+        done = true;
+        return;
+      }
       hnew = h / dmin(1.0 / 0.333, fac11 / 0.9);
       reject = true;
       t_current = t_old;

@@ -246,5 +246,8 @@ static KernelInfo pick_kernel_in(int planar, int var, int prec, int method, int 
 __attribute__((visibility("hidden"))) KernelInfo pick_kernel_more(int planar, int var, int prec,
                                                                   int method, int sig,
                                                                   int variant, bool direct);
+// surface-of-section kernels: rk4, rk6, dopr54, dop853 on SosSystem, FP64,
+// run-time component list (orbit_kernels_more.cu; not exported)
+__attribute__((visibility("hidden"))) KernelInfo pick_kernel_sos(int method, int variant);
 
 }  // namespace gpc

@@ -6,7 +6,8 @@ symplec4, symplec6, rk4, rk6, dopr54, dop853; not ias15) and runs the batch
 on the GPU through this package; everything else in galpy is untouched.  The hooks patch the four places that decide galpy's integrator
 dispatch (galpy/orbit/Orbits.py):
 
-* ``Orbit.check_integrator`` (:1342-1370) -- the allow-list of method names;
+* ``Orbit.check_integrator`` (:1342-1370) -- the allow-list of method names
+  (a ``*_cuda`` name is valid where galpy's ``*_c`` name is);
 * ``Orbit._check_method_c_compatible`` (:1372-1392) -- ``"_c" in method`` is
   True for the ``*_cuda`` names; keep them when every potential component is
   one the engine implements, otherwise fall back to galpy's ``*_c`` method of
@@ -17,13 +18,17 @@ dispatch (galpy/orbit/Orbits.py):
   (``integrateFullOrbit_c`` / ``integratePlanarOrbit_c`` and, when galpy's C
   extension is not loaded, ``integrateFullOrbit`` / ``integratePlanarOrbit``)
   -- a ``*_cuda`` method is routed to ``integrateFullOrbit_cuda`` /
-  ``integratePlanarOrbit_cuda``, any other method to galpy's original.
+  ``integratePlanarOrbit_cuda``, any other method to galpy's original;
+* the same for ``Orbit.integrate_SOS`` (:2103-2278) in 3D:
+  ``integrateFullOrbit_sos_c`` / ``integrateFullOrbit_sos`` ->
+  ``integrateFullOrbit_sos_cuda``.
 
 INTEGRATION.md shows the equivalent few-line patch to galpy itself.
 """
 import numpy as np
 
-from .integrate import CUDA_METHODS, integrateFullOrbit_cuda, integratePlanarOrbit_cuda
+from .integrate import (CUDA_METHODS, integrateFullOrbit_cuda, integrateFullOrbit_sos_cuda,
+                        integratePlanarOrbit_cuda)
 from .potentials import SUPPORTED_TYPES
 
 _installed = {}
@@ -91,6 +96,28 @@ def _route_python(orig, planar):
     return integrate
 
 
+def _route_sos(orig, python_branch):
+    # Orbit.integrate_SOS (Orbits.py:2103-2278): the C branch pads orbits
+    # without phi before the call (and drops the column after), the Python
+    # branch (galpy's C extension not loaded) passes vxvv as it is
+    def integrateFullOrbit_sos(pot, yo, psi, t0, int_method, *args, **kwargs):
+        if not _is_cuda(int_method):
+            return orig(pot, yo, psi, t0, int_method, *args, **kwargs)
+        kw = {k: kwargs[k] for k in ("rtol", "atol", "progressbar", "dpsi") if k in kwargs}
+        if python_branch:
+            y, padded = _pad_phi(np.atleast_2d(yo), True)
+        else:
+            y, padded = np.copy(yo), False
+        out, err = integrateFullOrbit_sos_cuda(pot, y, psi, t0, int_method, **kw)
+        if python_branch and out.ndim == 2:
+            out = out[None]
+        if padded:
+            out = np.delete(out, 5, axis=-1)
+        return out, err
+
+    return integrateFullOrbit_sos
+
+
 def install():
     """Patch galpy (must be importable) so that Orbit.integrate accepts the
     ``*_cuda`` methods.  Idempotent."""
@@ -104,9 +131,14 @@ def install():
     orig_even = Orbit._check_array_evenlyspaced
 
     def check_integrator(method, no_symplec=False, allow_c_symplec=False):
-        if _is_cuda(method):
-            return None
-        return orig_check(method, no_symplec=no_symplec, allow_c_symplec=allow_c_symplec)
+        if not _is_cuda(method):
+            return orig_check(method, no_symplec=no_symplec, allow_c_symplec=allow_c_symplec)
+        # valid wherever galpy's *_c method of the same name is
+        try:
+            return orig_check(method[: -len("_cuda")] + "_c", no_symplec=no_symplec,
+                              allow_c_symplec=allow_c_symplec)
+        except ValueError:
+            raise ValueError(f"{method:s} is not a valid `method`") from None
 
     def _check_method_c_compatible(method, pot):
         if _is_cuda(method):
@@ -126,7 +158,9 @@ def install():
         check_integrator=orig_check, _check_method_c_compatible=orig_c_compat,
         _check_array_evenlyspaced=orig_even, integrateFullOrbit_c=O.integrateFullOrbit_c,
         integratePlanarOrbit_c=O.integratePlanarOrbit_c,
-        integrateFullOrbit=O.integrateFullOrbit, integratePlanarOrbit=O.integratePlanarOrbit)
+        integrateFullOrbit=O.integrateFullOrbit, integratePlanarOrbit=O.integratePlanarOrbit,
+        integrateFullOrbit_sos_c=O.integrateFullOrbit_sos_c,
+        integrateFullOrbit_sos=O.integrateFullOrbit_sos)
     Orbit.check_integrator = staticmethod(check_integrator)
     Orbit._check_method_c_compatible = staticmethod(_check_method_c_compatible)
     Orbit._check_array_evenlyspaced = staticmethod(_check_array_evenlyspaced)
@@ -134,6 +168,8 @@ def install():
     O.integratePlanarOrbit_c = _route_planar(_installed["integratePlanarOrbit_c"])
     O.integrateFullOrbit = _route_python(_installed["integrateFullOrbit"], False)
     O.integratePlanarOrbit = _route_python(_installed["integratePlanarOrbit"], True)
+    O.integrateFullOrbit_sos_c = _route_sos(_installed["integrateFullOrbit_sos_c"], False)
+    O.integrateFullOrbit_sos = _route_sos(_installed["integrateFullOrbit_sos"], True)
 
 
 def uninstall():
@@ -147,6 +183,6 @@ def uninstall():
     Orbit._check_method_c_compatible = staticmethod(_installed["_check_method_c_compatible"])
     Orbit._check_array_evenlyspaced = staticmethod(_installed["_check_array_evenlyspaced"])
     for name in ("integrateFullOrbit_c", "integratePlanarOrbit_c", "integrateFullOrbit",
-                 "integratePlanarOrbit"):
+                 "integratePlanarOrbit", "integrateFullOrbit_sos_c", "integrateFullOrbit_sos"):
         setattr(O, name, _installed[name])
     _installed.clear()

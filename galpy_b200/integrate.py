@@ -8,6 +8,7 @@ ctypes exactly like galpy calls libgalpy:
   integratePlanarOrbit_cuda       galpy/orbit/integratePlanarOrbit.py:989
   integrateFullOrbit_dxdv_cuda    galpy/orbit/integrateFullOrbit.py:752-856
   integratePlanarOrbit_dxdv_cuda  galpy/orbit/integratePlanarOrbit.py:1124-1225
+  integrateFullOrbit_sos_cuda     galpy/orbit/integrateFullOrbit.py:1215-1355
 
 plus ``integrate_dxdv_batch`` (all deviations of many orbits in one launch)
 and ``integrate_device`` (device-resident torch tensors, asynchronous).
@@ -126,6 +127,62 @@ def integratePlanarOrbit_cuda(pot, yo, t, int_method, rtol=None, atol=None, prog
     """Planar counterpart of integrateFullOrbit_cuda: yo [N,4] (R,vR,vT,phi)."""
     return _integrate_c(True, pot, yo, t, int_method, rtol, atol, progressbar, dt, precision,
                         max_attempts, return_nsteps, device)
+
+
+def integrateFullOrbit_sos_cuda(pot, yo, psi, t0, int_method, rtol=None, atol=None,
+                                progressbar=True, dpsi=None, max_attempts=0,
+                                return_nsteps=False, device=-1):
+    """Surface-of-section integration on the GPU (galpy's
+    integrateFullOrbit_sos_c, galpy/orbit/integrateFullOrbit.py:1215-1355).
+
+    yo [N,6] (R,vR,vT,z,vz,phi) or [6]; psi [npsi] or [N,npsi] increments of
+    the angle psi = atan2(z, vz) at which the state is wanted; t0 the initial
+    time (scalar or [N]); int_method 'rk4_cuda', 'rk6_cuda', 'dopr54_cuda' or
+    'dop853_cuda'; dpsi the step (None: estimated).  Returns (y [N,npsi,7]
+    with the time as the last column, err [N]); the leading axis is dropped
+    for a single orbit."""
+    single_obj = np.ndim(yo) == 1
+    yo = np.atleast_2d(yo)
+    nobj = len(yo)
+    rtol, atol = parse_tol(rtol, atol)
+    npot, pot_type, pot_args = parse_pot(pot)
+    code = parse_integrator(int_method)
+    dpsi = _lib.DT_SENTINEL if dpsi is None else float(dpsi)
+    t0 = np.atleast_1d(np.asarray(t0, dtype=np.float64))
+    yoo = np.empty((nobj, 7))
+    yoo[:, :6] = yo[:, :6]
+    yoo[:, 6] = t0[0] if len(t0) == 1 else t0
+    psi = np.require(np.asarray(psi, dtype=np.float64), requirements=["C", "W"])
+    indiv = int(psi.ndim > 1)
+    npsi = psi.shape[-1]
+    result = np.empty((nobj, npsi, 7))
+    err = np.zeros(nobj, dtype=np.int32)
+    nsteps = np.zeros(nobj, dtype=np.int64) if return_nsteps else None
+    opts = _lib.make_opts(precision=_lib.FP64, device=device, max_attempts=max_attempts,
+                          nsteps=nsteps)
+    cb = _lib.CALLBACK()
+    pbar = None
+    if progressbar and nobj > 1:
+        try:
+            import tqdm
+
+            pbar = tqdm.tqdm(total=nobj, leave=False)
+            cb = _lib.CALLBACK(pbar.update)
+        except ImportError:  # pragma: no cover
+            pass
+    rc = _lib.lib().integrateFullOrbit_sos_cuda(
+        nobj, yoo.ctypes.data_as(_dp), npsi, psi.ctypes.data_as(_dp), indiv, npot,
+        pot_type.ctypes.data_as(_ip), pot_args.ctypes.data_as(_dp), None, dpsi, rtol, atol,
+        result.ctypes.data_as(_dp), err.ctypes.data_as(_ip), code, cb, ctypes.byref(opts))
+    if pbar is not None:
+        pbar.close()
+    _lib.check(rc)
+    if np.any(err == -10):
+        raise KeyboardInterrupt("Orbit integration interrupted by CTRL-C (SIGINT)")
+    out = (result[0], err[0]) if single_obj else (result, err)
+    if return_nsteps:
+        out = out + ((nsteps[0] if single_obj else nsteps),)
+    return out
 
 
 def _dxdv_single(planar, pot, yo, dyo, t, int_method, dt, rtol, atol, device):

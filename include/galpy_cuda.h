@@ -61,6 +61,10 @@ extern "C" {
 #define GALPY_CUDA_SIG_MW14 1    /* exactly (15, 5, 9): MWPotential2014's component types */
 
 /* order in which orbits are handed to the GPU threads */
+/* the ODE system of a device launch (galpy_cuda_launch.system) */
+#define GALPY_CUDA_SYS_ORBIT 0 /* orbit in time: the 2*dim (or 4*dim variational) state */
+#define GALPY_CUDA_SYS_SOS 1   /* 3D surface of section: (x,y,vx,vy,A,t,psi) in the psi increment */
+
 #define GALPY_CUDA_SCHED_IN_ORDER 0
 #define GALPY_CUDA_SCHED_LONGEST_FIRST 1 /* by estimated cost: integration time x orbital frequency */
 
@@ -106,6 +110,20 @@ int integratePlanarOrbit_cuda(int nobj, double *yo, int nt, double *t, int indiv
                               double rtol, double atol, double *result, int *err,
                               int odeint_type, galpy_cuda_callback cb,
                               const galpy_cuda_opts *opts);
+
+/* Stands in for integrateFullOrbit_sos (integrateFullOrbit.c:1151-1167):
+ * yo [nobj][7] = (R,vR,vT,z,vz,phi,t0), overwritten with the surface-of-
+ * section state (x,y,vx,vy,A,t0,psi0) like the reference
+ * (cyl_to_sos_galpy); psi [npsi] or [nobj][npsi] angle increments; dpsi the
+ * step (-9999.99 = estimate); odeint_type 1 rk4, 2 rk6, 5 dopr54, 6 dop853
+ * (the symplectic ones and ias15 return GALPY_CUDA_ERR_METHOD, as the
+ * reference does not integrate them here); result [nobj][npsi][7] =
+ * (R,vR,vT,z,vz,phi,t). */
+int integrateFullOrbit_sos_cuda(int nobj, double *yo, int npsi, double *psi, int indiv_psi,
+                                int npot, int *pot_type, double *pot_args, void *pot_tfuncs,
+                                double dpsi, double rtol, double atol, double *result, int *err,
+                                int odeint_type, galpy_cuda_callback cb,
+                                const galpy_cuda_opts *opts);
 
 /* Stands in for integrateFullOrbit_dxdv (integrateFullOrbit.c:1234): one
  * orbit, yo = (x,y,z,vx,vy,vz,dx,dy,dz,dvx,dvy,dvz), result [nt][12]. */
@@ -160,9 +178,11 @@ typedef struct galpy_cuda_launch {
   int variant;              /* register budget: 0 compiler default, 1 capped for occupancy */
   const void *comps_host;   /* optional host copy of `comps` (ncomp records, one group):
                                its scalars are passed as kernel parameters */
-  int size_ext;             /* 1 if the fields below are set (0: defaults) */
+  int size_ext;             /* 1 if tail_sms is set, 2 if system is set too (0: defaults) */
   int tail_sms;             /* SMs reserved for the longest orbits of a large longest-first
                                batch, one warp each (-1: default 1, 0: none) */
+  int system;               /* GALPY_CUDA_SYS_* (size_ext >= 2; default the orbit); SOS runs
+                               are 3D, float64, rk4/rk6/dopr54/dop853, w0 rows of 7 */
 } galpy_cuda_launch;
 
 int galpy_cuda_integrate_device(const galpy_cuda_launch *launch);

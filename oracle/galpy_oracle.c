@@ -21,7 +21,8 @@
  *            symplec6), :588-1052 (their step estimators), :1053-1400
  *            (*_dxdv); util/bovy_rk.c:66-480 (rk4, rk6 + estimators),
  *            :501-760 (dopr54); util/leung_dop853.c:231-517 (dop853)
- *   drivers  integrateFullOrbit.c:1046-1150, :1234-1306;
+ *   drivers  integrateFullOrbit.c:1046-1150, :1151-1233 (surface of
+ *            section, with evalSOSDeriv :1353-1390), :1234-1306;
  *            integratePlanarOrbit.c:743-847, :940-1014
  *   coords   util/bovy_coords.c:57-148
  * The arithmetic of each formula follows the reference term by term so that
@@ -30,7 +31,9 @@
  * incomplete gamma function is the one in oracle/incgamma.c.
  *
  * Extras over the reference (test instrumentation only): per-orbit counts of
- * accepted steps and of force evaluations, and an optional attempt budget.
+ * accepted steps and of force evaluations, an optional attempt budget, and a
+ * stop (err 2) where the reference never returns (a DOP853 attempt rejected
+ * at its smallest step repeats exactly).
  */
 #include <math.h>
 #include <stdlib.h>
@@ -1532,6 +1535,12 @@ static void dop853(rhs_fn f, opot *P, int dim, const double *yin, int nt, const 
       if (reject) hnew = pos_neg * DMIN(fabs(hnew), fabs(h));
       reject = 0;
     } else {
+      /* extra over the reference: an attempt rejected at the smallest step
+         repeats exactly, where the reference loops forever; stop (err 2) */
+      if (fabs(h) <= 1e3 * uround) {
+        st->err = 2;
+        break;
+      }
       hnew = h / DMIN(facc1, fac11 / safe);
       reject = 1;
       t_current = t_old;
@@ -1584,8 +1593,96 @@ static void rect_to_polar(double *v)
 }
 
 /* ------------------------------------------------------------------ */
+/* surface of section (integrateFullOrbit.c:1151-1233, 1353-1390)       */
+/* ------------------------------------------------------------------ */
+/* evalSOSDeriv: q = (x, y, vx, vy, A, t, psi), derivative w.r.t. the psi
+   increment; the force at (x, y, A sin psi) */
+static void sos_deriv(opot *P, const double *q, double *a)
+{
+  double sinpsi = sin(q[6]), cospsi = cos(q[6]);
+  double x = q[0], y = q[1], z = q[4] * sinpsi;
+  double R = sqrt(x * x + y * y), phi = atan2(y, x);
+  double sinphi = y / R, cosphi = x / R, Rf, zf, pt;
+  sum3(P, R, z, phi, &Rf, &zf, &pt);
+  a[3] = cosphi * Rf - 1. / R * sinphi * pt;
+  a[4] = sinphi * Rf + 1. / R * cosphi * pt;
+  a[5] = zf;
+  double psidot = cospsi * cospsi - sinpsi * a[5] / q[4];
+  a[0] = q[2] / psidot;
+  a[1] = q[3] / psidot;
+  a[2] = a[3] / psidot;
+  a[3] = a[4] / psidot;
+  a[4] = cospsi * (q[4] * sinpsi + a[5]) / psidot;
+  a[5] = 1. / psidot;
+  a[6] = 1.;
+}
+
+/* cyl_to_sos_galpy / sos_to_cyl_galpy (bovy_coords.c:149-189) */
+static void cyl_to_sos(double *v)
+{
+  double R = v[0], cp = cos(v[5]), sp = sin(v[5]), vR = v[1], vT = v[2];
+  v[5] = v[6];
+  v[6] = atan2(v[3], v[4]);
+  v[4] = sqrt(v[3] * v[3] + v[4] * v[4]);
+  v[0] = R * cp;
+  v[1] = R * sp;
+  v[2] = vR * cp - vT * sp;
+  v[3] = vR * sp + vT * cp;
+}
+static void sos_to_cyl(double *v)
+{
+  double x = v[0], y = v[1], vx = v[2], vy = v[3], phi = atan2(y, x), cp = cos(phi),
+         sp = sin(phi);
+  v[0] = sqrt(x * x + y * y);
+  v[1] = vx * cp + vy * sp;
+  v[2] = -vx * sp + vy * cp;
+  v[3] = v[4] * sin(v[6]);
+  v[4] = v[4] * cos(v[6]);
+  v[6] = v[5];
+  v[5] = phi;
+}
+
+/* ------------------------------------------------------------------ */
 /* exported drivers                                                    */
 /* ------------------------------------------------------------------ */
+#define EXPORT_SOS __attribute__((visibility("default")))
+
+/* Surface-of-section integration of nobj orbits (integrateFullOrbit_sos):
+   yo [nobj][7] = (R, vR, vT, z, vz, phi, t0), overwritten with the SOS
+   state; psi [npsi] or [nobj][npsi] increments; result [nobj][npsi][7] =
+   (R, vR, vT, z, vz, phi, t).  method 1 rk4, 2 rk6, 5 dopr54, 6 dop853. */
+EXPORT_SOS int oracle_integrate_sos(int nobj, double *yo, int npsi, const double *psi,
+                                    int indiv_psi, int npot, const int *pot_type,
+                                    const double *pot_args, double dpsi, double rtol, double atol,
+                                    double *result, int *err, int method, long long *nsteps,
+                                    int nthreads)
+{
+  opot P0;
+  if (opot_decode(&P0, npot, pot_type, pot_args, 0)) return -3;
+  if (method != 1 && method != 2 && method != 5 && method != 6) return -2;
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+#endif
+  for (int ii = 0; ii < nobj; ii++) {
+    opot P = P0;
+    ostat st = {0, 0, 0};
+    double *w = yo + 7L * ii;
+    const double *ps = psi + (long)npsi * ii * indiv_psi;
+    double *out = result + 7L * npsi * ii;
+    cyl_to_sos(w);
+    switch (method) {
+    case 1: rk_fixed(4, sos_deriv, &P, 7, w, npsi, dpsi, ps, rtol, atol, out, &st); break;
+    case 2: rk_fixed(6, sos_deriv, &P, 7, w, npsi, dpsi, ps, rtol, atol, out, &st); break;
+    case 5: dopr54(sos_deriv, &P, 7, w, npsi, dpsi, ps, rtol, atol, out, &st); break;
+    case 6: dop853(sos_deriv, &P, 7, w, npsi, ps, rtol, atol, out, &st); break;
+    }
+    for (int jj = 0; jj < npsi; jj++) sos_to_cyl(out + 7L * jj);
+    err[ii] = st.err;
+    if (nsteps) nsteps[ii] = st.nsteps;
+  }
+  return 0;
+}
 #define EXPORT __attribute__((visibility("default")))
 
 /* One orbit of the plain integration in rectangular coordinates.

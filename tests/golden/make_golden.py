@@ -18,7 +18,8 @@ Two kinds of vectors are written to golden.npz:
 * from the reference's own C integrators (integrateFullOrbit /
   integratePlanarOrbit / *_dxdv built from its sources into oracle/_ref):
   small seeded batches for every implemented method, 3D, planar and
-  variational, and runs in each of the spherical potentials.
+  variational, runs in each of the spherical potentials, and surface-of-
+  section runs (integrateFullOrbit_sos).
 
 The CPU oracle is checked against these in tests/test_oracle.py, so it stays
 pinned on machines that have neither the reference tree nor oracle/_ref.
@@ -195,6 +196,21 @@ def main():
         out[f"c_{m}_dxdv3"] = res
         res, _, _ = O.integrate_dxdv(w2, t, pt2, pa2, m, planar=True, impl="ref")
         out[f"c_{m}_dxdv2"] = res
+    # surface of section (integrateFullOrbit_sos): 8 orbits in MWPotential2014,
+    # ten crossings of psi = 0 (mod 2 pi), every RK-type method; per-orbit
+    # increments with dop853
+    yo7 = np.concatenate([seeded_ics(8, 5), np.linspace(0.0, 1.0, 8)[:, None]], 1)
+    psi = np.linspace(0.0, 20.0 * np.pi, 11)
+    out["sos_yo"], out["sos_psi"] = yo7, psi
+    for m in ("rk4", "rk6", "dopr54", "dop853"):
+        res, err, _ = O.integrate_sos(yo7, psi, pt, pa, m, rtol=1e-10, atol=1e-10, impl="ref")
+        assert not err.any()
+        out[f"sos_{m}"] = res
+    psi_i = np.linspace(0.0, 1.0, 6)[None, :] * np.linspace(6.0, 30.0, 8)[:, None]
+    out["sos_psi_indiv"] = psi_i
+    res, _, _ = O.integrate_sos(yo7, psi_i, pt, pa, "dop853", rtol=1e-10, atol=1e-10, impl="ref")
+    out["sos_dop853_indiv"] = res
+
     # gradient oracle of the adjoint: Jacobians d y(T) / d y(0) from the
     # reference's variational DOP853 (integrate{Planar,Full}Orbit_dxdv), one
     # unit deviation column per run, t in [0, 20], rtol = atol = 1e-10

@@ -107,6 +107,38 @@ extern "C" int harness_integrate(int planar, int var, int method, int prec, int 
 #undef HARNESS_ARGS
 }
 
+// Surface-of-section machines (3D, FP64, run-time component list) on SOS
+// states w [nobj][7] = (x, y, vx, vy, A, t, psi); out [nobj][nt][7] raw.
+extern "C" int harness_integrate_sos(int method, int nobj, const double* w, int nt,
+                                     const double* t, int indiv_t, int npot, const int* pot_type,
+                                     const double* pot_args, double dt, double rtol, double atol,
+                                     long long max_att, double* out, int* err, long long* nsteps)
+{
+  std::vector<GpComp> comps(npot);
+  int rc = compile_group(0, npot, pot_type, pot_args, comps.data(), nullptr);
+  if (rc) return rc;
+  const GpComp* c = comps.data();
+  switch (method) {
+    case M_RK4:
+      run_all<RKMachine<3, false, 4, SosSystem>, 3, PREC_FP64, false, DynPot>(
+          nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol, max_att, out, err, nsteps);
+      return 0;
+    case M_RK6:
+      run_all<RKMachine<3, false, 6, SosSystem>, 3, PREC_FP64, false, DynPot>(
+          nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol, max_att, out, err, nsteps);
+      return 0;
+    case M_DOPR54:
+      run_all<Dopr54Machine<3, false, SosSystem>, 3, PREC_FP64, false, DynPot>(
+          nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol, max_att, out, err, nsteps);
+      return 0;
+    case M_DOP853:
+      run_all<Dop853Machine<3, false, SosSystem>, 3, PREC_FP64, false, DynPot>(
+          nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol, max_att, out, err, nsteps);
+      return 0;
+  }
+  return -2;
+}
+
 // accelerations (and tidal tensors) at points, for force-level tests
 // gamma*(a, u) from a compiled PowerSphericalwCutoff record (table check)
 extern "C" int harness_gamma_star(double alpha, double rc, int n, const double* u, double* out)

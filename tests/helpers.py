@@ -115,3 +115,31 @@ def golden_pot(golden, name, planar=False):
     if planar and f"{name}_planar_args" in golden:
         return golden[f"{name}_planar_type"], golden[f"{name}_planar_args"]
     return golden[f"{name}_type"], golden[f"{name}_args"]
+
+
+def cyl_to_sos(v):
+    """galpy's cyl_to_sos_galpy on rows (R, vR, vT, z, vz, phi, t) ->
+    (x, y, vx, vy, A, t, psi)."""
+    v = np.asarray(v, dtype=float)
+    R, vR, vT, z, vz, phi, t = (v[..., k] for k in range(7))
+    c, s = np.cos(phi), np.sin(phi)
+    return np.stack([R * c, R * s, vR * c - vT * s, vR * s + vT * c, np.sqrt(z * z + vz * vz),
+                     t, np.arctan2(z, vz)], -1)
+
+
+def sos_to_cyl(v):
+    """galpy's sos_to_cyl_galpy on rows (x, y, vx, vy, A, t, psi) ->
+    (R, vR, vT, z, vz, phi, t)."""
+    v = np.asarray(v, dtype=float)
+    x, y, vx, vy, A, t, psi = (v[..., k] for k in range(7))
+    phi = np.arctan2(y, x)
+    c, s = np.cos(phi), np.sin(phi)
+    return np.stack([np.sqrt(x * x + y * y), vx * c + vy * s, -vx * s + vy * c, A * np.sin(psi),
+                     A * np.cos(psi), phi, t], -1)
+
+
+def sos_diff(a, b):
+    """Elementwise |a - b| of (R, vR, vT, z, vz, phi, t) rows, phi wrapped."""
+    d = np.abs(np.asarray(a) - np.asarray(b))
+    d[..., 5] = np.abs((a[..., 5] - b[..., 5] + np.pi) % (2 * np.pi) - np.pi)
+    return d

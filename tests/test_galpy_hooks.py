@@ -86,3 +86,39 @@ def test_unknown_method_still_rejected(hooks):
     o = Orbit([1.0, 0.1, 1.1, 0.0, 0.1, 0.0])
     with pytest.raises(ValueError):
         o.integrate(np.linspace(0, 1, 11), MWPotential2014, method="euler_cuda")
+
+
+def test_integrate_sos_routes(monkeypatch):
+    """Orbit.integrate_SOS with a *_cuda method reaches
+    integrateFullOrbit_sos_cuda (orbits without phi padded and unpadded as
+    galpy's C branch does); symplectic *_cuda methods are refused as galpy
+    refuses symplec4_c there."""
+    from galpy.orbit import Orbit
+    from galpy.potential import MWPotential2014
+
+    from galpy_b200 import galpy_hooks
+
+    calls = []
+
+    def fake(pot, yo, psi, t0, int_method, **kw):
+        calls.append((np.array(yo).shape, int_method))
+        yo = np.atleast_2d(yo)
+        out = np.zeros((len(yo), len(psi), 7))
+        out[..., :6] = yo[:, None, :6]
+        out[..., 6] = psi  # time increasing with psi
+        return out, np.zeros(len(yo), np.int32)
+
+    monkeypatch.setattr(galpy_hooks, "integrateFullOrbit_sos_cuda", fake)
+    galpy_hooks.install()
+    try:
+        psi = np.linspace(0, 10 * np.pi, 6)
+        o = Orbit([[1.0, 0.1, 1.1, 0.05, 0.02, 0.3], [1.2, 0.0, 1.0, 0.1, 0.0, 1.0]])
+        o.integrate_SOS(psi, MWPotential2014, method="dop853_cuda")
+        assert calls[-1] == ((2, 6), "dop853_cuda") and o.orbit.shape == (2, 6, 6)
+        o5 = Orbit([[1.0, 0.1, 1.1, 0.05, 0.02]])
+        o5.integrate_SOS(psi, MWPotential2014, method="dopr54_cuda")
+        assert calls[-1][0] == (1, 6) and o5.orbit.shape == (1, 6, 5)
+        with pytest.raises(ValueError, match="symplec4_cuda"):
+            o.integrate_SOS(psi, MWPotential2014, method="symplec4_cuda")
+    finally:
+        galpy_hooks.uninstall()

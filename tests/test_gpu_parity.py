@@ -10,7 +10,7 @@ import ctypes
 
 import numpy as np
 import pytest
-from helpers import SPHERICAL, cyl_diff, golden_pot, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
+from helpers import SPHERICAL, cyl_diff, golden_pot, sos_diff, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
 
 import galpy_b200 as gb
 from galpy_b200 import _lib
@@ -221,6 +221,33 @@ def test_spherical_potentials(oracle, golden, name):
     # single-precision forces over 1,000 steps (the strong power-law orbits
     # cover the most periods)
     assert not err.any() and cyl_diff(f64, f32)[..., :5].max() < 1e-2
+
+
+@pytest.mark.parametrize("method", ["rk4", "rk6", "dopr54", "dop853"])
+def test_surface_of_section(oracle, golden, method):
+    """integrateFullOrbit_sos_cuda against the reference's C (golden) and the
+    oracle on a larger batch with per-orbit increments."""
+    pt, pa = golden["mw14_type"], golden["mw14_args"]
+    yo = golden["sos_yo"].copy()
+    out, err = gb.integrateFullOrbit_sos_cuda((pt, pa), yo[:, :6], golden["sos_psi"],
+                                              yo[:, 6], cuda(method), rtol=1e-10, atol=1e-10,
+                                              progressbar=False)
+    assert not err.any()
+    assert sos_diff(golden[f"sos_{method}"], out).max() < 1e-9
+    ics = seeded_ics(300, 38)
+    yo = np.concatenate([ics, np.zeros((300, 1))], 1)
+    psi = np.linspace(0.0, 1.0, 9)[None, :] * np.linspace(6.0, 40.0, 300)[:, None]
+    ref, _, nref = oracle.integrate_sos(yo, psi, pt, pa, method, rtol=1e-10, atol=1e-10)
+    out, err, ns = gb.integrateFullOrbit_sos_cuda((pt, pa), ics, psi, 0.0, cuda(method),
+                                                  rtol=1e-10, atol=1e-10, progressbar=False,
+                                                  return_nsteps=True)
+    same = ns == nref
+    assert not err.any() and same.mean() >= 0.95, same.mean()
+    d = sos_diff(ref, out).max(axis=(1, 2))
+    assert d[same].max() < 1e-8 and d.max() < 1e-6, d.max()
+    # the symplectic methods are not integrated in psi (as in the reference)
+    with pytest.raises(gb.MethodNotSupported):
+        gb.integrateFullOrbit_sos_cuda((pt, pa), ics[:2], psi[0], 0.0, "symplec4_cuda")
 
 
 def test_device_api_soa_matches_galpy_layout(mw14):

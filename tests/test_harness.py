@@ -4,7 +4,7 @@ against the CPU oracle.  This checks the kernel logic on every CPU-only run;
 tests/test_gpu_parity.py checks the compiled kernels on the GPU."""
 import numpy as np
 import pytest
-from helpers import SPHERICAL, cyl_diff, golden_pot, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
+from helpers import SPHERICAL, cyl_diff, cyl_to_sos, golden_pot, sos_diff, sos_to_cyl, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
 
 METHODS = ["leapfrog", "rk4", "rk6", "symplec4", "symplec6", "dopr54", "dop853"]
 POTS = ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"] + SPHERICAL
@@ -272,3 +272,18 @@ def test_binade_tables_match_mpmath(harness):
     ref = np.array([float(mpmath.log1p(mpmath.mpf(v))) for v in xf])
     pos = ref > 0
     assert np.abs(out[pos] / ref[pos] - 1).max() < 4 * 6e-8
+
+
+@pytest.mark.parametrize("method", ["rk4", "rk6", "dopr54", "dop853"])
+def test_surface_of_section_machines(harness, oracle, golden, method):
+    """The SOS system on the RK-type machines against the oracle: same step
+    sequence, agreement well inside the tolerance."""
+    for name in ("mw14", "logtri"):
+        pt, pa = golden[f"{name}_type"], golden[f"{name}_args"]
+        yo = np.concatenate([seeded_ics(8, 19), np.linspace(0, 2, 8)[:, None]], 1)
+        psi = np.linspace(0.0, 12.0 * np.pi, 7)
+        ref, _, nref = oracle.integrate_sos(yo, psi, pt, pa, method, rtol=1e-10, atol=1e-10)
+        raw, err, ns = harness.integrate_sos(cyl_to_sos(yo), psi, pt, pa, method, rtol=1e-10,
+                                             atol=1e-10)
+        assert not err.any() and np.array_equal(ns, nref), (name, ns, nref)
+        assert sos_diff(ref, sos_to_cyl(raw)).max() < 1e-10, name

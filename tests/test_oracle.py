@@ -183,3 +183,35 @@ def test_oracle_energy_conservation(oracle, mw14, method):
     assert not err.any()
     E = oracle.energy_cyl(res, pt, pa)
     assert np.all((E.std(1) / E.mean(1)) ** 2 < 1e-10)
+
+
+SOS_METHODS = ["rk4", "rk6", "dopr54", "dop853"]
+
+
+@pytest.mark.parametrize("method", SOS_METHODS)
+def test_oracle_surface_of_section(oracle, golden, method):
+    """integrateFullOrbit_sos (integrateFullOrbit.c:1151-1233, evalSOSDeriv
+    :1353-1390): golden vectors of the reference's C, and bit for bit
+    against the reference build (MWPotential2014, the triaxial logarithmic
+    halo, per-orbit increments) where it is present."""
+    pt, pa = golden["mw14_type"], golden["mw14_args"]
+    a, err, _ = oracle.integrate_sos(golden["sos_yo"], golden["sos_psi"], pt, pa, method,
+                                     rtol=1e-10, atol=1e-10)
+    assert not err.any()
+    np.testing.assert_allclose(a, golden[f"sos_{method}"], rtol=0, atol=1e-12)
+    if method == "dop853":
+        a, _, _ = oracle.integrate_sos(golden["sos_yo"], golden["sos_psi_indiv"], pt, pa,
+                                       method, rtol=1e-10, atol=1e-10)
+        np.testing.assert_allclose(a, golden["sos_dop853_indiv"], rtol=0, atol=1e-12)
+    if not oracle.ref_available():
+        return
+    # (not the Plummer sphere: one of these orbits makes the reference's
+    # dop853 reject its smallest step forever)
+    for name in ("mw14", "logtri", "flatpower"):
+        pt, pa = golden[f"{name}_type"], golden[f"{name}_args"]
+        yo = np.concatenate([seeded_ics(6, 9), np.zeros((6, 1))], 1)
+        psi = np.linspace(0.0, 12.0 * np.pi, 7)
+        for kw in ({"rtol": 1e-9, "atol": 1e-9}, {"dpsi": 0.05}):
+            a, ea, _ = oracle.integrate_sos(yo, psi, pt, pa, method, **kw)
+            b, eb, _ = oracle.integrate_sos(yo, psi, pt, pa, method, impl="ref", **kw)
+            assert np.array_equal(a, b) and np.array_equal(ea, eb), (name, kw)
