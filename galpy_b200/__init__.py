@@ -18,7 +18,7 @@ from .integrate import (CUDA_METHODS, accel_device, compile_potential,  # noqa: 
                         energy_device,
                         integrate_device,
                         integrate_dxdv_batch, integrateFullOrbit_cuda,
-                        integrateFullOrbit_sos_cuda,
+                        integrateFullOrbit_sos_cuda, integratePlanarOrbit_sos_cuda,
                         integrateFullOrbit_dxdv_cuda, integratePlanarOrbit_cuda,
                         integratePlanarOrbit_dxdv_cuda, parse_integrator, parse_tol,
                         signature)

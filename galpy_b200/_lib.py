@@ -25,7 +25,7 @@ F32FORCE = 1
 IN_AOS, IN_SOA = 0, 1
 OUT_GALPY, OUT_AOS_RECT, OUT_SOA_RECT, OUT_SOA_CYL = 0, 1, 2, 3
 
-SYS_ORBIT, SYS_SOS = 0, 1
+SYS_ORBIT, SYS_SOS, SYS_SOS_PLANAR_X, SYS_SOS_PLANAR_Y = 0, 1, 2, 3
 
 DT_SENTINEL = -9999.99
 
@@ -162,6 +162,11 @@ SIGNATURES = {
         _ci,
         [_ci, _dp, _ci, _dp, _ci, _ci, _ip, _dp, _vp, _cd, _cd, _cd, _dp, _ip, _ci, CALLBACK,
          _opts_p],
+    ),
+    "integratePlanarOrbit_sos_cuda": (
+        _ci,
+        [_ci, _dp, _ci, _dp, _ci, _ci, _ci, _ip, _dp, _vp, _cd, _cd, _cd, _dp, _ip, _ci,
+         CALLBACK, _opts_p],
     ),
     "integratePlanarOrbit_cuda": (
         _ci,

@@ -123,7 +123,7 @@ static int launch_system(const galpy_cuda_launch* L)
 static KernelInfo pick_kernel(int planar, int var, int prec, int method, int sig, int variant,
                               bool direct, int system = GALPY_CUDA_SYS_ORBIT)
 {
-  if (system == GALPY_CUDA_SYS_SOS) return pick_kernel_sos(method, variant);
+  if (system != GALPY_CUDA_SYS_ORBIT) return pick_kernel_sos(method, variant, system);
   if (method == M_RK6 || method == M_SYMPLEC6 || method == M_DOPR54)
     return pick_kernel_more(planar, var, prec, method, sig, variant, direct);
   return pick_kernel_in<CoreMethods>(planar, var, prec, method, sig, variant, direct);
@@ -284,16 +284,18 @@ static int check_launch(const galpy_cuda_launch* L)
 {
   if (!L) return set_error(GALPY_CUDA_ERR_ARG, "launch is NULL");
   const int system = launch_system(L);
-  if (system != GALPY_CUDA_SYS_ORBIT && system != GALPY_CUDA_SYS_SOS)
+  if (system < GALPY_CUDA_SYS_ORBIT || system > GALPY_CUDA_SYS_SOS_PLANAR_Y)
     return set_error(GALPY_CUDA_ERR_ARG, "unknown system");
-  if (system == GALPY_CUDA_SYS_SOS) {
+  if (system != GALPY_CUDA_SYS_ORBIT) {
     const int m = L->odeint_type;
     if (m != M_RK4 && m != M_RK6 && m != M_DOPR54 && m != M_DOP853)
       return set_error(GALPY_CUDA_ERR_METHOD,
                        "surface-of-section integration takes rk4, rk6, dopr54 or dop853");
-    if (L->planar || L->variational || L->precision != GALPY_CUDA_FP64)
+    if (L->planar != (system != GALPY_CUDA_SYS_SOS) || L->variational ||
+        L->precision != GALPY_CUDA_FP64)
       return set_error(GALPY_CUDA_ERR_ARG,
-                       "surface-of-section integration is 3D, plain and float64");
+                       "surface-of-section integration is plain float64, 3D for "
+                       "GALPY_CUDA_SYS_SOS and planar for the planar systems");
   }
   if (!method_supported(L->odeint_type))
     return set_error(GALPY_CUDA_ERR_METHOD, "odeint_type not implemented on the GPU");
@@ -530,6 +532,32 @@ static void cyl_to_sos_inplace(long long nobj, double* yo)
     v[1] = R * sp;
     v[2] = vR * cp - vT * sp;
     v[3] = vR * sp + vT * cp;
+  }
+}
+
+// (R, vR, vT, phi, t) -> planar surface-of-section state, in place, exactly
+// as polar_to_sos_galpy (bovy_coords.c:200-226): surface 1 (y = 0) gives
+// (x, vx, A, t, psi), otherwise (x = 0) (y, vy, A, t, psi)
+static void polar_to_sos_inplace(long long nobj, double* yo, int surface)
+{
+  for (long long i = 0; i < nobj; i++) {
+    double* v = yo + 5 * i;
+    const double R = v[0], cp = cos(v[3]), sp = sin(v[3]), vR = v[1], vT = v[2];
+    if (surface == 1) {
+      v[0] = R * cp;
+      v[1] = vR * cp - vT * sp;
+      const double y = R * sp, vy = vR * sp + vT * cp;
+      v[2] = sqrt(y * y + vy * vy);
+      v[3] = v[4];
+      v[4] = atan2(y, vy);
+    } else {
+      v[0] = R * sp;
+      v[1] = vR * sp + vT * cp;
+      const double x = R * cp, vx = vR * cp - vT * sp;
+      v[2] = sqrt(x * x + vx * vx);
+      v[3] = v[4];
+      v[4] = atan2(x, vx);
+    }
   }
 }
 
@@ -976,6 +1004,25 @@ int integrateFullOrbit_sos_cuda(int nobj, double* yo, int npsi, double* psi, int
   cyl_to_sos_inplace(nobj, yo);
   return run_host(0, 0, nobj, yo, 7, npsi, psi, indiv_psi, npot, pot_type, pot_args, dpsi, rtol,
                   atol, result, err, odeint_type, cb, opts, false, GALPY_CUDA_SYS_SOS);
+}
+
+int integratePlanarOrbit_sos_cuda(int nobj, double* yo, int npsi, double* psi, int indiv_psi,
+                                  int surface, int npot, int* pot_type, double* pot_args,
+                                  void* /*pot_tfuncs*/, double dpsi, double rtol, double atol,
+                                  double* result, int* err, int odeint_type,
+                                  galpy_cuda_callback cb, const galpy_cuda_opts* opts)
+{
+  if (nobj < 0 || npsi < 1 || (nobj && (!yo || !psi || !result || !err)) || !pot_type ||
+      !pot_args)
+    return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
+  if (odeint_type != M_RK4 && odeint_type != M_RK6 && odeint_type != M_DOPR54 &&
+      odeint_type != M_DOP853)
+    return set_error(GALPY_CUDA_ERR_METHOD,
+                     "surface-of-section integration takes rk4, rk6, dopr54 or dop853");
+  polar_to_sos_inplace(nobj, yo, surface);
+  return run_host(1, 0, nobj, yo, 5, npsi, psi, indiv_psi, npot, pot_type, pot_args, dpsi, rtol,
+                  atol, result, err, odeint_type, cb, opts, false,
+                  surface == 1 ? GALPY_CUDA_SYS_SOS_PLANAR_Y : GALPY_CUDA_SYS_SOS_PLANAR_X);
 }
 
 int integratePlanarOrbit_cuda(int nobj, double* yo, int nt, double* t, int indiv_t, int npot,

@@ -61,6 +61,9 @@ constexpr double s6d3 = -0.117767998417887e1, s6d4 = 0.131518632068391e1;
 // output rows
 // ------------------------------------------------------------------------
 enum : int { L_GALPY_CYL = 0, L_AOS_RECT = 1, L_SOA_RECT = 2, L_SOA_CYL = 3 };
+// what a stored state is: an orbit (rectangular), the 3D surface-of-section
+// state, or the planar one for the surface x = 0 / y = 0
+enum : int { ROW_ORBIT = 0, ROW_SOS = 1, ROW_SOS_PLANAR_X = 2, ROW_SOS_PLANAR_Y = 3 };
 
 struct OutSpec {
   double* out;
@@ -73,14 +76,33 @@ struct OutSpec {
 // Write row j of orbit i.  v is the rectangular state in the reference's row
 // order: plain 3D (x,y,z,vx,vy,vz), planar (x,y,vx,vy); variational rows
 // (x, v, dx, dv) are always written rectangular.
-template <int NV, int D, bool CYL_OK>
+template <int NV, int D, bool CYL_OK, int ROW = ROW_ORBIT>
 GPC_HD GPC_FI void write_row(const OutSpec& o, long long i, int j, const double* v)
 {
   if (j < o.row0) return;
   const long long nrow = o.nt - o.row0, jj = j - o.row0;
   double w[NV];
   const bool cyl = CYL_OK && (o.layout == L_GALPY_CYL || o.layout == L_SOA_CYL);
-  if constexpr (NV == 7) {
+  if constexpr (ROW == ROW_SOS_PLANAR_X || ROW == ROW_SOS_PLANAR_Y) {
+    if (cyl) {
+      // (u, vu, A, t, psi) -> (R, vR, vT, phi, t): sos_to_polar_galpy
+      // (bovy_coords.c:235-260)
+      const double w1 = v[2] * sin(v[4]), w2 = v[2] * cos(v[4]);
+      const double x = ROW == ROW_SOS_PLANAR_X ? w1 : v[0];
+      const double vx = ROW == ROW_SOS_PLANAR_X ? w2 : v[1];
+      const double y = ROW == ROW_SOS_PLANAR_X ? v[0] : w1;
+      const double vy = ROW == ROW_SOS_PLANAR_X ? v[1] : w2;
+      const double phi = atan2(y, x), cp = cos(phi), sp = sin(phi);
+      w[0] = sqrt(x * x + y * y);
+      w[1] = vx * cp + vy * sp;
+      w[2] = -vx * sp + vy * cp;
+      w[3] = phi;
+      w[4] = v[3];
+    } else {
+#pragma unroll
+      for (int k = 0; k < NV; k++) w[k] = v[k];
+    }
+  } else if constexpr (ROW == ROW_SOS) {
     if (cyl) {
       // surface of section (x, y, vx, vy, A, t, psi) -> (R, vR, vT, z, vz,
       // phi, t): sos_to_cyl_galpy (bovy_coords.c:173-189)
@@ -126,13 +148,13 @@ GPC_HD GPC_FI void write_row(const OutSpec& o, long long i, int j, const double*
   }
 }
 
-template <int NV, int D, bool CYL_OK>
+template <int NV, int D, bool CYL_OK, int ROW = ROW_ORBIT>
 GPC_HD GPC_FI void write_nan_rows(const OutSpec& o, long long i, int from)
 {
   double v[NV];
 #pragma unroll
   for (int k = 0; k < NV; k++) v[k] = NAN;
-  for (int j = from; j < o.nt; j++) write_row<NV, D, CYL_OK>(o, i, j, v);
+  for (int j = from; j < o.nt; j++) write_row<NV, D, CYL_OK, ROW>(o, i, j, v);
 }
 
 // ------------------------------------------------------------------------
@@ -257,6 +279,7 @@ struct SymplecticMachine : OrbitCommon {
   static constexpr int NY = NQ;               // size of the force argument
   static constexpr int NV = 2 * NQ;           // values per output row
   static constexpr int NA = NQ;               // force result size
+  static constexpr int kRow = ROW_ORBIT;
   static constexpr int kSlotDoubles = 0;      // no slot store needed
   GPC_HD GPC_FI void bind(double*) {}
   GPC_HD GPC_FI bool wants_dense() const { return false; }
@@ -530,6 +553,7 @@ template <int D, bool VAR>
 struct OrbitSystem {
   static constexpr int N = VAR ? 4 * D : 2 * D;  // ODE dimension
   static constexpr int NA = VAR ? 2 * D : D;     // force argument / result size
+  static constexpr int kRow = ROW_ORBIT;         // output row conversion
   // force argument: positions (and deviation positions) of (x, v[, dx, dv])
   GPC_HD GPC_FI static void pos(const double* y, double* q)
   {
@@ -560,6 +584,7 @@ struct OrbitSystem {
 // (x, y, A sin psi).
 struct SosSystem {
   static constexpr int N = 7, NA = 3;
+  static constexpr int kRow = ROW_SOS;
   GPC_HD GPC_FI static void pos(const double* y, double* q)
   {
     q[0] = y[0];
@@ -580,6 +605,34 @@ struct SosSystem {
   }
 };
 
+// Planar surface of section (evalPlanarSOSDerivx / evalPlanarSOSDerivy,
+// integratePlanarOrbit.c:1056-1123): y = (u, vu, A, t, psi).  SURF 0
+// (surface x = 0): (u, vu) = (y, vy), x = A sin psi, vx = A cos psi;
+// SURF 1 (y = 0): (u, vu) = (x, vx), y = A sin psi, vy = A cos psi.
+template <int SURF>
+struct PlanarSosSystem {
+  static constexpr int N = 5, NA = 2;
+  static constexpr int kRow = SURF == 0 ? ROW_SOS_PLANAR_X : ROW_SOS_PLANAR_Y;
+  GPC_HD GPC_FI static void pos(const double* y, double* q)
+  {
+    const double w = y[2] * sin(y[4]);
+    q[0] = SURF == 0 ? w : y[0];
+    q[1] = SURF == 0 ? y[0] : w;
+  }
+  GPC_HD GPC_FI static void deriv(const double* y, const double* a, double* d)
+  {
+    const double sp = sin(y[4]), cp = cos(y[4]);
+    const double aw = SURF == 0 ? a[0] : a[1];  // along the surface normal
+    const double au = SURF == 0 ? a[1] : a[0];
+    const double ipd = 1.0 / (cp * cp - sp * aw / y[2]);
+    d[0] = y[1] * ipd;
+    d[1] = au * ipd;
+    d[2] = cp * (y[2] * sp + aw) * ipd;
+    d[3] = ipd;
+    d[4] = 1.0;
+  }
+};
+
 // ------------------------------------------------------------------------
 // RK4 / RK6 (optionally variational)
 // ------------------------------------------------------------------------
@@ -590,6 +643,7 @@ struct RKMachine : OrbitCommon {
   static constexpr int NY = N;
   static constexpr int NV = N;
   static constexpr int NA = SYS::NA;  // force result size
+  static constexpr int kRow = SYS::kRow;
   static constexpr int kStages = ORD == 4 ? 4 : 7;
   GPC_HD GPC_FI static void pos(const double* y, double* q) { SYS::pos(y, q); }
   static constexpr int kSlotDoubles = 0;
@@ -778,6 +832,7 @@ struct Dopr54Machine : OrbitCommon {
   static constexpr int NY = N;
   static constexpr int NV = N;
   static constexpr int NA = SYS::NA;
+  static constexpr int kRow = SYS::kRow;
   GPC_HD GPC_FI static void pos(const double* y, double* q) { SYS::pos(y, q); }
   static constexpr int kSlotDoubles = 0;
   GPC_HD GPC_FI void bind(double*) {}
@@ -1119,6 +1174,7 @@ struct Dop853Machine : OrbitCommon {
   static constexpr int NY = N;
   static constexpr int NV = N;
   static constexpr int NA = SYS::NA;  // force result size
+  static constexpr int kRow = SYS::kRow;
   GPC_HD GPC_FI static void pos(const double* y, double* q) { SYS::pos(y, q); }
   enum {
     ST_INIT1 = 0, ST_INIT2 = 1,

@@ -47,13 +47,13 @@ struct KArgs {
   double scal[kMaxComp * kScalarStride];
 };
 
-template <int NV, int D, bool CYL_OK>
+template <int NV, int D, bool CYL_OK, int ROW>
 struct DevRows {
   const OutSpec* o;
   long long i;
   __device__ __forceinline__ void operator()(int j, const double* v) const
   {
-    write_row<NV, D, CYL_OK>(*o, i, j, v);
+    write_row<NV, D, CYL_OK, ROW>(*o, i, j, v);
   }
 };
 
@@ -83,7 +83,7 @@ template <class M, int D, int PREC, bool VAR, class POT, int MINB>
 __global__ void __launch_bounds__(128, MINB) orbit_kernel(const __grid_constant__ KArgs A)
 {
   constexpr bool CYL_OK = !VAR;
-  using Rows = DevRows<M::NV, D, CYL_OK>;
+  using Rows = DevRows<M::NV, D, CYL_OK, M::kRow>;
   extern __shared__ double slot_store[];
   // Reserved SMs for the longest orbits: the first block resident on each of
   // SMs 0..tail_sms-1 keeps one warp, which takes the tail queue (then helps
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(128, MINB) orbit_kernel(const __grid_constant_
       i = A.order ? A.order[q] : q;
       if (aborting) {
         A.err[i] = E_ABORT;
-        write_nan_rows<M::NV, D, CYL_OK>(A.out, i, 0);
+        write_nan_rows<M::NV, D, CYL_OK, M::kRow>(A.out, i, 0);
         continue;
       }
       double w[M::NV];
@@ -246,8 +246,10 @@ static KernelInfo pick_kernel_in(int planar, int var, int prec, int method, int 
 __attribute__((visibility("hidden"))) KernelInfo pick_kernel_more(int planar, int var, int prec,
                                                                   int method, int sig,
                                                                   int variant, bool direct);
-// surface-of-section kernels: rk4, rk6, dopr54, dop853 on SosSystem, FP64,
-// run-time component list (orbit_kernels_more.cu; not exported)
-__attribute__((visibility("hidden"))) KernelInfo pick_kernel_sos(int method, int variant);
+// surface-of-section kernels: rk4, rk6, dopr54, dop853 on the 3D or planar
+// (surface x = 0 / y = 0) system, FP64, run-time component list
+// (orbit_kernels_more.cu; not exported)
+__attribute__((visibility("hidden"))) KernelInfo pick_kernel_sos(int method, int variant,
+                                                                 int system);
 
 }  // namespace gpc

@@ -26,17 +26,29 @@ KernelInfo pick_kernel_more(int planar, int var, int prec, int method, int sig, 
   return pick_kernel_in<MoreMethods>(planar, var, prec, method, sig, variant, direct);
 }
 
-// Surface of section (integrateFullOrbit_sos): the RK-type machines on the
-// 7-D system, 3D and float64, any potential.
-KernelInfo pick_kernel_sos(int method, int variant)
+// Surface of section (integrateFullOrbit_sos, integratePlanarOrbit_sos): the
+// RK-type machines on the 7-D (3D) or 5-D (planar) system, float64, any
+// potential.
+template <class SYS, int D>
+static KernelInfo pick_sos_system(int method, int variant)
 {
   switch (method) {
-    case M_RK4: return info_of<RKMachine<3, false, 4, SosSystem>, 3, PREC_FP64, false, DynPot>(variant);
-    case M_RK6: return info_of<RKMachine<3, false, 6, SosSystem>, 3, PREC_FP64, false, DynPot>(variant);
+    case M_RK4: return info_of<RKMachine<D, false, 4, SYS>, D, PREC_FP64, false, DynPot>(variant);
+    case M_RK6: return info_of<RKMachine<D, false, 6, SYS>, D, PREC_FP64, false, DynPot>(variant);
     case M_DOPR54:
-      return info_of<Dopr54Machine<3, false, SosSystem>, 3, PREC_FP64, false, DynPot>(variant);
+      return info_of<Dopr54Machine<D, false, SYS>, D, PREC_FP64, false, DynPot>(variant);
     case M_DOP853:
-      return info_of<Dop853Machine<3, false, SosSystem>, 3, PREC_FP64, false, DynPot>(variant);
+      return info_of<Dop853Machine<D, false, SYS>, D, PREC_FP64, false, DynPot>(variant);
+  }
+  return KernelInfo();
+}
+
+KernelInfo pick_kernel_sos(int method, int variant, int system)
+{
+  switch (system) {
+    case GALPY_CUDA_SYS_SOS: return pick_sos_system<SosSystem, 3>(method, variant);
+    case GALPY_CUDA_SYS_SOS_PLANAR_X: return pick_sos_system<PlanarSosSystem<0>, 2>(method, variant);
+    case GALPY_CUDA_SYS_SOS_PLANAR_Y: return pick_sos_system<PlanarSosSystem<1>, 2>(method, variant);
   }
   return KernelInfo();
 }

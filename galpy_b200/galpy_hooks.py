@@ -19,16 +19,17 @@ dispatch (galpy/orbit/Orbits.py):
   extension is not loaded, ``integrateFullOrbit`` / ``integratePlanarOrbit``)
   -- a ``*_cuda`` method is routed to ``integrateFullOrbit_cuda`` /
   ``integratePlanarOrbit_cuda``, any other method to galpy's original;
-* the same for ``Orbit.integrate_SOS`` (:2103-2278) in 3D:
+* the same for ``Orbit.integrate_SOS`` (:2103-2278):
   ``integrateFullOrbit_sos_c`` / ``integrateFullOrbit_sos`` ->
-  ``integrateFullOrbit_sos_cuda``.
+  ``integrateFullOrbit_sos_cuda`` and ``integratePlanarOrbit_sos_c`` /
+  ``integratePlanarOrbit_sos`` -> ``integratePlanarOrbit_sos_cuda``.
 
 INTEGRATION.md shows the equivalent few-line patch to galpy itself.
 """
 import numpy as np
 
 from .integrate import (CUDA_METHODS, integrateFullOrbit_cuda, integrateFullOrbit_sos_cuda,
-                        integratePlanarOrbit_cuda)
+                        integratePlanarOrbit_cuda, integratePlanarOrbit_sos_cuda)
 from .potentials import SUPPORTED_TYPES
 
 _installed = {}
@@ -118,6 +119,33 @@ def _route_sos(orig, python_branch):
     return integrateFullOrbit_sos
 
 
+def _route_sos_planar(orig, python_branch):
+    # the planar counterpart (integratePlanarOrbit_sos_c / _sos); the C branch
+    # pads orbits without phi, the Python branch does not
+    def integratePlanarOrbit_sos(pot, yo, psi, t0, int_method, *args, **kwargs):
+        if not _is_cuda(int_method):
+            return orig(pot, yo, psi, t0, int_method, *args, **kwargs)
+        kw = {k: kwargs[k] for k in ("surface", "rtol", "atol", "progressbar", "dpsi")
+              if k in kwargs}
+        if kw.get("surface") is None:
+            kw.pop("surface", None)
+        if python_branch:
+            y = np.atleast_2d(yo)
+            padded = y.shape[-1] == 3
+            if padded:
+                y = np.pad(y, ((0, 0), (0, 1)), "constant", constant_values=0)
+        else:
+            y, padded = np.copy(yo), False
+        out, err = integratePlanarOrbit_sos_cuda(pot, y, psi, t0, int_method, **kw)
+        if python_branch and out.ndim == 2:
+            out = out[None]
+        if padded:
+            out = np.delete(out, 3, axis=-1)
+        return out, err
+
+    return integratePlanarOrbit_sos
+
+
 def install():
     """Patch galpy (must be importable) so that Orbit.integrate accepts the
     ``*_cuda`` methods.  Idempotent."""
@@ -160,7 +188,9 @@ def install():
         integratePlanarOrbit_c=O.integratePlanarOrbit_c,
         integrateFullOrbit=O.integrateFullOrbit, integratePlanarOrbit=O.integratePlanarOrbit,
         integrateFullOrbit_sos_c=O.integrateFullOrbit_sos_c,
-        integrateFullOrbit_sos=O.integrateFullOrbit_sos)
+        integrateFullOrbit_sos=O.integrateFullOrbit_sos,
+        integratePlanarOrbit_sos_c=O.integratePlanarOrbit_sos_c,
+        integratePlanarOrbit_sos=O.integratePlanarOrbit_sos)
     Orbit.check_integrator = staticmethod(check_integrator)
     Orbit._check_method_c_compatible = staticmethod(_check_method_c_compatible)
     Orbit._check_array_evenlyspaced = staticmethod(_check_array_evenlyspaced)
@@ -170,6 +200,9 @@ def install():
     O.integratePlanarOrbit = _route_python(_installed["integratePlanarOrbit"], True)
     O.integrateFullOrbit_sos_c = _route_sos(_installed["integrateFullOrbit_sos_c"], False)
     O.integrateFullOrbit_sos = _route_sos(_installed["integrateFullOrbit_sos"], True)
+    O.integratePlanarOrbit_sos_c = _route_sos_planar(_installed["integratePlanarOrbit_sos_c"],
+                                                     False)
+    O.integratePlanarOrbit_sos = _route_sos_planar(_installed["integratePlanarOrbit_sos"], True)
 
 
 def uninstall():
@@ -183,6 +216,7 @@ def uninstall():
     Orbit._check_method_c_compatible = staticmethod(_installed["_check_method_c_compatible"])
     Orbit._check_array_evenlyspaced = staticmethod(_installed["_check_array_evenlyspaced"])
     for name in ("integrateFullOrbit_c", "integratePlanarOrbit_c", "integrateFullOrbit",
-                 "integratePlanarOrbit", "integrateFullOrbit_sos_c", "integrateFullOrbit_sos"):
+                 "integratePlanarOrbit", "integrateFullOrbit_sos_c", "integrateFullOrbit_sos",
+                 "integratePlanarOrbit_sos_c", "integratePlanarOrbit_sos"):
         setattr(O, name, _installed[name])
     _installed.clear()

@@ -9,6 +9,7 @@ ctypes exactly like galpy calls libgalpy:
   integrateFullOrbit_dxdv_cuda    galpy/orbit/integrateFullOrbit.py:752-856
   integratePlanarOrbit_dxdv_cuda  galpy/orbit/integratePlanarOrbit.py:1124-1225
   integrateFullOrbit_sos_cuda     galpy/orbit/integrateFullOrbit.py:1215-1355
+  integratePlanarOrbit_sos_cuda   galpy/orbit/integratePlanarOrbit.py:1543-1693
 
 plus ``integrate_dxdv_batch`` (all deviations of many orbits in one launch)
 and ``integrate_device`` (device-resident torch tensors, asynchronous).
@@ -129,33 +130,24 @@ def integratePlanarOrbit_cuda(pot, yo, t, int_method, rtol=None, atol=None, prog
                         max_attempts, return_nsteps, device)
 
 
-def integrateFullOrbit_sos_cuda(pot, yo, psi, t0, int_method, rtol=None, atol=None,
-                                progressbar=True, dpsi=None, max_attempts=0,
-                                return_nsteps=False, device=-1):
-    """Surface-of-section integration on the GPU (galpy's
-    integrateFullOrbit_sos_c, galpy/orbit/integrateFullOrbit.py:1215-1355).
-
-    yo [N,6] (R,vR,vT,z,vz,phi) or [6]; psi [npsi] or [N,npsi] increments of
-    the angle psi = atan2(z, vz) at which the state is wanted; t0 the initial
-    time (scalar or [N]); int_method 'rk4_cuda', 'rk6_cuda', 'dopr54_cuda' or
-    'dop853_cuda'; dpsi the step (None: estimated).  Returns (y [N,npsi,7]
-    with the time as the last column, err [N]); the leading axis is dropped
-    for a single orbit."""
+def _integrate_sos(planar, pot, yo, psi, t0, int_method, surface, rtol, atol, progressbar,
+                   dpsi, max_attempts, return_nsteps, device):
     single_obj = np.ndim(yo) == 1
     yo = np.atleast_2d(yo)
     nobj = len(yo)
+    nv = 5 if planar else 7
     rtol, atol = parse_tol(rtol, atol)
-    npot, pot_type, pot_args = parse_pot(pot)
+    npot, pot_type, pot_args = parse_pot(pot, planar=planar)
     code = parse_integrator(int_method)
     dpsi = _lib.DT_SENTINEL if dpsi is None else float(dpsi)
     t0 = np.atleast_1d(np.asarray(t0, dtype=np.float64))
-    yoo = np.empty((nobj, 7))
-    yoo[:, :6] = yo[:, :6]
-    yoo[:, 6] = t0[0] if len(t0) == 1 else t0
+    yoo = np.empty((nobj, nv))
+    yoo[:, :nv - 1] = yo[:, :nv - 1]
+    yoo[:, nv - 1] = t0[0] if len(t0) == 1 else t0
     psi = np.require(np.asarray(psi, dtype=np.float64), requirements=["C", "W"])
     indiv = int(psi.ndim > 1)
     npsi = psi.shape[-1]
-    result = np.empty((nobj, npsi, 7))
+    result = np.empty((nobj, npsi, nv))
     err = np.zeros(nobj, dtype=np.int32)
     nsteps = np.zeros(nobj, dtype=np.int64) if return_nsteps else None
     opts = _lib.make_opts(precision=_lib.FP64, device=device, max_attempts=max_attempts,
@@ -170,10 +162,15 @@ def integrateFullOrbit_sos_cuda(pot, yo, psi, t0, int_method, rtol=None, atol=No
             cb = _lib.CALLBACK(pbar.update)
         except ImportError:  # pragma: no cover
             pass
-    rc = _lib.lib().integrateFullOrbit_sos_cuda(
-        nobj, yoo.ctypes.data_as(_dp), npsi, psi.ctypes.data_as(_dp), indiv, npot,
-        pot_type.ctypes.data_as(_ip), pot_args.ctypes.data_as(_dp), None, dpsi, rtol, atol,
-        result.ctypes.data_as(_dp), err.ctypes.data_as(_ip), code, cb, ctypes.byref(opts))
+    args = [nobj, yoo.ctypes.data_as(_dp), npsi, psi.ctypes.data_as(_dp), indiv]
+    if planar:  # galpy passes 1 for surface 'y', 0 otherwise (integratePlanarOrbit.py:1664)
+        args.append(1 if surface == "y" else 0)
+    args += [npot, pot_type.ctypes.data_as(_ip), pot_args.ctypes.data_as(_dp), None, dpsi, rtol,
+             atol, result.ctypes.data_as(_dp), err.ctypes.data_as(_ip), code, cb,
+             ctypes.byref(opts)]
+    fn = _lib.lib().integratePlanarOrbit_sos_cuda if planar else \
+        _lib.lib().integrateFullOrbit_sos_cuda
+    rc = fn(*args)
     if pbar is not None:
         pbar.close()
     _lib.check(rc)
@@ -183,6 +180,33 @@ def integrateFullOrbit_sos_cuda(pot, yo, psi, t0, int_method, rtol=None, atol=No
     if return_nsteps:
         out = out + ((nsteps[0] if single_obj else nsteps),)
     return out
+
+
+def integrateFullOrbit_sos_cuda(pot, yo, psi, t0, int_method, rtol=None, atol=None,
+                                progressbar=True, dpsi=None, max_attempts=0,
+                                return_nsteps=False, device=-1):
+    """Surface-of-section integration on the GPU (galpy's
+    integrateFullOrbit_sos_c, galpy/orbit/integrateFullOrbit.py:1215-1355).
+
+    yo [N,6] (R,vR,vT,z,vz,phi) or [6]; psi [npsi] or [N,npsi] increments of
+    the angle psi = atan2(z, vz) at which the state is wanted; t0 the initial
+    time (scalar or [N]); int_method 'rk4_cuda', 'rk6_cuda', 'dopr54_cuda' or
+    'dop853_cuda'; dpsi the step (None: estimated).  Returns (y [N,npsi,7]
+    with the time as the last column, err [N]); the leading axis is dropped
+    for a single orbit."""
+    return _integrate_sos(False, pot, yo, psi, t0, int_method, None, rtol, atol, progressbar,
+                          dpsi, max_attempts, return_nsteps, device)
+
+
+def integratePlanarOrbit_sos_cuda(pot, yo, psi, t0, int_method, surface="x", rtol=None,
+                                  atol=None, progressbar=True, dpsi=None, max_attempts=0,
+                                  return_nsteps=False, device=-1):
+    """Planar surface-of-section integration on the GPU (galpy's
+    integratePlanarOrbit_sos_c, galpy/orbit/integratePlanarOrbit.py:1543-1693):
+    yo [N,4] (R,vR,vT,phi); surface 'x' (x = 0, the default) or 'y' (y =
+    0); returns (y [N,npsi,5] = (R,vR,vT,phi,t), err [N])."""
+    return _integrate_sos(True, pot, yo, psi, t0, int_method, surface, rtol, atol, progressbar,
+                          dpsi, max_attempts, return_nsteps, device)
 
 
 def _dxdv_single(planar, pot, yo, dyo, t, int_method, dt, rtol, atol, device):

@@ -64,6 +64,8 @@ extern "C" {
 /* the ODE system of a device launch (galpy_cuda_launch.system) */
 #define GALPY_CUDA_SYS_ORBIT 0 /* orbit in time: the 2*dim (or 4*dim variational) state */
 #define GALPY_CUDA_SYS_SOS 1   /* 3D surface of section: (x,y,vx,vy,A,t,psi) in the psi increment */
+#define GALPY_CUDA_SYS_SOS_PLANAR_X 2 /* planar, surface x = 0: (y,vy,A,t,psi) */
+#define GALPY_CUDA_SYS_SOS_PLANAR_Y 3 /* planar, surface y = 0: (x,vx,A,t,psi) */
 
 #define GALPY_CUDA_SCHED_IN_ORDER 0
 #define GALPY_CUDA_SCHED_LONGEST_FIRST 1 /* by estimated cost: integration time x orbital frequency */
@@ -125,6 +127,17 @@ int integrateFullOrbit_sos_cuda(int nobj, double *yo, int npsi, double *psi, int
                                 int odeint_type, galpy_cuda_callback cb,
                                 const galpy_cuda_opts *opts);
 
+/* Stands in for integratePlanarOrbit_sos (integratePlanarOrbit.c:848-866):
+ * yo [nobj][5] = (R,vR,vT,phi,t0), overwritten with the surface-of-section
+ * state (polar_to_sos_galpy); surface 0: x = 0 (state (y,vy,A,t,psi)),
+ * 1: y = 0 (state (x,vx,A,t,psi)); result [nobj][npsi][5] =
+ * (R,vR,vT,phi,t); methods as integrateFullOrbit_sos_cuda. */
+int integratePlanarOrbit_sos_cuda(int nobj, double *yo, int npsi, double *psi, int indiv_psi,
+                                  int surface, int npot, int *pot_type, double *pot_args,
+                                  void *pot_tfuncs, double dpsi, double rtol, double atol,
+                                  double *result, int *err, int odeint_type,
+                                  galpy_cuda_callback cb, const galpy_cuda_opts *opts);
+
 /* Stands in for integrateFullOrbit_dxdv (integrateFullOrbit.c:1234): one
  * orbit, yo = (x,y,z,vx,vy,vz,dx,dy,dz,dvx,dvy,dvz), result [nt][12]. */
 int integrateFullOrbit_dxdv_cuda(double *yo, int nt, double *t, int npot, int *pot_type,
@@ -182,7 +195,8 @@ typedef struct galpy_cuda_launch {
   int tail_sms;             /* SMs reserved for the longest orbits of a large longest-first
                                batch, one warp each (-1: default 1, 0: none) */
   int system;               /* GALPY_CUDA_SYS_* (size_ext >= 2; default the orbit); SOS runs
-                               are 3D, float64, rk4/rk6/dopr54/dop853, w0 rows of 7 */
+                               are float64, rk4/rk6/dopr54/dop853, w0 rows of 7 (3D) or 5
+                               (planar) */
 } galpy_cuda_launch;
 
 int galpy_cuda_integrate_device(const galpy_cuda_launch *launch);

@@ -23,6 +23,8 @@
  *            :501-760 (dopr54); util/leung_dop853.c:231-517 (dop853)
  *   drivers  integrateFullOrbit.c:1046-1150, :1151-1233 (surface of
  *            section, with evalSOSDeriv :1353-1390), :1234-1306;
+ *            integratePlanarOrbit.c:848-939 (planar surface of section,
+ *            with evalPlanarSOSDerivx/y :1056-1123);
  *            integratePlanarOrbit.c:743-847, :940-1014
  *   coords   util/bovy_coords.c:57-148
  * The arithmetic of each formula follows the reference term by term so that
@@ -1642,10 +1644,126 @@ static void sos_to_cyl(double *v)
   v[5] = phi;
 }
 
+/* planar surface of section (integratePlanarOrbit.c:848-939, 1056-1123):
+   q = (u, vu, A, t, psi); surface x = 0: (u, vu) = (y, vy), x = A sin psi */
+static void sos_planar_derivx(opot *P, const double *q, double *a)
+{
+  double sinpsi = sin(q[4]), cospsi = cos(q[4]);
+  double x = q[2] * sinpsi, y = q[0];
+  double R = sqrt(x * x + y * y), phi = atan2(y, x), sinphi = y / R, cosphi = x / R, Rf, pt;
+  sum2(P, R, phi, &Rf, &pt);
+  a[2] = cosphi * Rf - 1. / R * sinphi * pt;
+  a[3] = sinphi * Rf + 1. / R * cosphi * pt;
+  double psidot = cospsi * cospsi - sinpsi * a[2] / q[2];
+  a[0] = q[1] / psidot;
+  a[1] = a[3] / psidot;
+  a[2] = cospsi * (q[2] * sinpsi + a[2]) / psidot;
+  a[3] = 1. / psidot;
+  a[4] = 1.;
+}
+/* surface y = 0: (u, vu) = (x, vx), y = A sin psi */
+static void sos_planar_derivy(opot *P, const double *q, double *a)
+{
+  double sinpsi = sin(q[4]), cospsi = cos(q[4]);
+  double x = q[0], y = q[2] * sinpsi;
+  double R = sqrt(x * x + y * y), phi = atan2(y, x), sinphi = y / R, cosphi = x / R, Rf, pt;
+  sum2(P, R, phi, &Rf, &pt);
+  a[2] = cosphi * Rf - 1. / R * sinphi * pt;
+  a[3] = sinphi * Rf + 1. / R * cosphi * pt;
+  double psidot = cospsi * cospsi - sinpsi * a[3] / q[2];
+  a[0] = q[1] / psidot;
+  a[1] = a[2] / psidot;
+  a[2] = cospsi * (q[2] * sinpsi + a[3]) / psidot;
+  a[3] = 1. / psidot;
+  a[4] = 1.;
+}
+/* polar_to_sos_galpy / sos_to_polar_galpy (bovy_coords.c:200-260) */
+static void polar_to_sos(double *v, int surface)
+{
+  double R = v[0], cp = cos(v[3]), sp = sin(v[3]), vR = v[1], vT = v[2], x, y, vx, vy;
+  if (surface == 1) {
+    v[0] = R * cp;
+    v[1] = vR * cp - vT * sp;
+    y = R * sp;
+    vy = vR * sp + vT * cp;
+    v[2] = sqrt(y * y + vy * vy);
+    v[3] = v[4];
+    v[4] = atan2(y, vy);
+  } else {
+    v[0] = R * sp;
+    v[1] = vR * sp + vT * cp;
+    x = R * cp;
+    vx = vR * cp - vT * sp;
+    v[2] = sqrt(x * x + vx * vx);
+    v[3] = v[4];
+    v[4] = atan2(x, vx);
+  }
+}
+static void sos_to_polar(double *v, int surface)
+{
+  double x, y, vx, vy;
+  if (surface == 1) {
+    x = v[0];
+    vx = v[1];
+    y = v[2] * sin(v[4]);
+    vy = v[2] * cos(v[4]);
+  } else {
+    y = v[0];
+    vy = v[1];
+    x = v[2] * sin(v[4]);
+    vx = v[2] * cos(v[4]);
+  }
+  double phi = atan2(y, x), cp = cos(phi), sp = sin(phi);
+  v[0] = sqrt(x * x + y * y);
+  v[1] = vx * cp + vy * sp;
+  v[2] = -vx * sp + vy * cp;
+  v[4] = v[3];
+  v[3] = phi;
+}
+
 /* ------------------------------------------------------------------ */
 /* exported drivers                                                    */
 /* ------------------------------------------------------------------ */
 #define EXPORT_SOS __attribute__((visibility("default")))
+
+/* Planar surface-of-section integration (integratePlanarOrbit_sos): yo
+   [nobj][5] = (R, vR, vT, phi, t0), overwritten with the SOS state;
+   surface 0 (x = 0) or 1 (y = 0); result [nobj][npsi][5] = (R, vR, vT, phi,
+   t). */
+EXPORT_SOS int oracle_integrate_sos_planar(int nobj, double *yo, int npsi, const double *psi,
+                                           int indiv_psi, int surface, int npot,
+                                           const int *pot_type, const double *pot_args,
+                                           double dpsi, double rtol, double atol,
+                                           double *result, int *err, int method,
+                                           long long *nsteps, int nthreads)
+{
+  opot P0;
+  if (opot_decode(&P0, npot, pot_type, pot_args, 1)) return -3;
+  if (method != 1 && method != 2 && method != 5 && method != 6) return -2;
+  rhs_fn f = surface == 1 ? sos_planar_derivy : sos_planar_derivx;
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+#endif
+  for (int ii = 0; ii < nobj; ii++) {
+    opot P = P0;
+    ostat st = {0, 0, 0};
+    double *w = yo + 5L * ii;
+    const double *ps = psi + (long)npsi * ii * indiv_psi;
+    double *out = result + 5L * npsi * ii;
+    polar_to_sos(w, surface);
+    switch (method) {
+    case 1: rk_fixed(4, f, &P, 5, w, npsi, dpsi, ps, rtol, atol, out, &st); break;
+    case 2: rk_fixed(6, f, &P, 5, w, npsi, dpsi, ps, rtol, atol, out, &st); break;
+    case 5: dopr54(f, &P, 5, w, npsi, dpsi, ps, rtol, atol, out, &st); break;
+    case 6: dop853(f, &P, 5, w, npsi, ps, rtol, atol, out, &st); break;
+    }
+    for (int jj = 0; jj < npsi; jj++) sos_to_polar(out + 5L * jj, surface);
+    err[ii] = st.err;
+    if (nsteps) nsteps[ii] = st.nsteps;
+  }
+  return 0;
+}
 
 /* Surface-of-section integration of nobj orbits (integrateFullOrbit_sos):
    yo [nobj][7] = (R, vR, vT, z, vz, phi, t0), overwritten with the SOS

@@ -70,6 +70,12 @@ def port():
             ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, _ip, ctypes.c_int, _lp,
             ctypes.c_int,
         ]
+        lib.oracle_integrate_sos_planar.restype = ctypes.c_int
+        lib.oracle_integrate_sos_planar.argtypes = [
+            ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip,
+            _dp, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, _ip, ctypes.c_int, _lp,
+            ctypes.c_int,
+        ]
         lib.oracle_forces.restype = ctypes.c_int
         lib.oracle_forces.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int,
                                       _ip, _dp, _dp]
@@ -205,40 +211,58 @@ def integrate_dxdv(w, t, pot_type, pot_args, method, planar=False, dt=None, rtol
 
 
 def integrate_sos(yo, psi, pot_type, pot_args, method, dpsi=None, rtol=None, atol=None,
-                  nthreads=0, impl="port"):
-    """Surface-of-section integration (integrateFullOrbit_sos).
+                  nthreads=0, impl="port", planar=False, surface=0):
+    """Surface-of-section integration (integrateFullOrbit_sos, or
+    integratePlanarOrbit_sos when planar with surface 0 (x = 0) or 1 (y = 0)).
 
-    yo: (nobj, 7) = (R, vR, vT, z, vz, phi, t0); psi: (npsi,) or (nobj, npsi)
-    angle increments.  Returns (result (nobj, npsi, 7) = (R, vR, vT, z, vz,
-    phi, t), err, nsteps); nsteps is None for impl="ref"."""
+    yo: (nobj, 7) = (R, vR, vT, z, vz, phi, t0), planar (nobj, 5) = (R, vR,
+    vT, phi, t0); psi: (npsi,) or (nobj, npsi) angle increments.  Returns
+    (result (nobj, npsi, 7 | 5) in the input's coordinates with the time
+    last, err, nsteps); nsteps is None for impl="ref"."""
     yo, psi, pt, pa = _prep(yo, psi, pot_type, pot_args)
-    nobj = yo.shape[0]
+    nobj, nv = yo.shape
     npsi = psi.shape[-1]
     indiv = int(psi.ndim > 1)
     r, a = _tol(rtol, atol)
     dv = DT_SENTINEL if dpsi is None else float(dpsi)
     m = METHODS[method] if isinstance(method, str) else int(method)
-    result = np.empty((nobj, npsi, 7))
+    result = np.empty((nobj, npsi, nv))
     err = np.zeros(nobj, dtype=np.int32)
     if impl == "port":
         nsteps = np.zeros(nobj, dtype=np.int64)
-        rc = port().oracle_integrate_sos(nobj, _ptr(yo, _dp), npsi, _ptr(psi, _dp), indiv,
-                                         len(pt), _ptr(pt, _ip), _ptr(pa, _dp), dv, r, a,
-                                         _ptr(result, _dp), _ptr(err, _ip), m,
-                                         _ptr(nsteps, _lp), int(nthreads))
+        if planar:
+            rc = port().oracle_integrate_sos_planar(
+                nobj, _ptr(yo, _dp), npsi, _ptr(psi, _dp), indiv, int(surface), len(pt),
+                _ptr(pt, _ip), _ptr(pa, _dp), dv, r, a, _ptr(result, _dp), _ptr(err, _ip), m,
+                _ptr(nsteps, _lp), int(nthreads))
+        else:
+            rc = port().oracle_integrate_sos(nobj, _ptr(yo, _dp), npsi, _ptr(psi, _dp), indiv,
+                                             len(pt), _ptr(pt, _ip), _ptr(pa, _dp), dv, r, a,
+                                             _ptr(result, _dp), _ptr(err, _ip), m,
+                                             _ptr(nsteps, _lp), int(nthreads))
         if rc != 0:
             raise ValueError(f"oracle_integrate_sos returned {rc}")
         return result, err, nsteps
     lib = ref()
     if lib is None:
         raise RuntimeError("reference build oracle/_ref/libgalpy_ref.so is not present")
+    if nthreads:
+        os.environ["OMP_NUM_THREADS"] = str(nthreads)
+    if planar:
+        fn = lib.integratePlanarOrbit_sos
+        fn.restype = None
+        fn.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
+                       ctypes.c_int, _ip, _dp, ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                       ctypes.c_double, _dp, _ip, ctypes.c_int, ctypes.c_void_p]
+        fn(nobj, _ptr(yo, _dp), npsi, _ptr(psi, _dp), indiv, int(surface), len(pt),
+           _ptr(pt, _ip), _ptr(pa, _dp), None, dv, r, a, _ptr(result, _dp), _ptr(err, _ip), m,
+           None)
+        return result, err, None
     fn = lib.integrateFullOrbit_sos
     fn.restype = None
     fn.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, _ip, _dp,
                    ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, _ip,
                    ctypes.c_int, ctypes.c_void_p]
-    if nthreads:
-        os.environ["OMP_NUM_THREADS"] = str(nthreads)
     fn(nobj, _ptr(yo, _dp), npsi, _ptr(psi, _dp), indiv, len(pt), _ptr(pt, _ip), _ptr(pa, _dp),
        None, dv, r, a, _ptr(result, _dp), _ptr(err, _ip), m, None)
     return result, err, None

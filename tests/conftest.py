@@ -95,13 +95,15 @@ class Harness:
         return out, err, ns
 
     def integrate_sos(self, w, psi, pot_type, pot_args, method, dpsi=None, rtol=None,
-                      atol=None, max_attempts=0):
-        """SOS machines on SOS states w [n][7]; returns raw rows [n][npsi][7]."""
+                      atol=None, max_attempts=0, surface=None):
+        """SOS machines on SOS states: 3D w [n][7], or planar w [n][5] with
+        surface 0 (x = 0) or 1 (y = 0); returns raw rows [n][npsi][7 | 5]."""
         w = np.ascontiguousarray(w, dtype=np.float64)
         psi = np.ascontiguousarray(psi, dtype=np.float64)
-        n = len(w)
+        n, nv = w.shape
         npsi = psi.shape[-1]
-        out = np.zeros((n, npsi, 7))
+        system = 1 if surface is None else 2 + int(surface)
+        out = np.zeros((n, npsi, nv))
         err = np.zeros(n, np.int32)
         ns = np.zeros(n, np.int64)
         pt = np.ascontiguousarray(pot_type, np.int32)
@@ -109,7 +111,8 @@ class Harness:
         r = -12 * np.log(10) if rtol is None else np.log(rtol)
         a = -12 * np.log(10) if atol is None else np.log(atol)
         rc = self.lib.harness_integrate_sos(
-            METHOD_CODES[method], n, w.ctypes.data_as(_dp), npsi, psi.ctypes.data_as(_dp),
+            system, METHOD_CODES[method], n, w.ctypes.data_as(_dp), npsi,
+            psi.ctypes.data_as(_dp),
             int(psi.ndim > 1), len(pt), pt.ctypes.data_as(_ip), pa.ctypes.data_as(_dp),
             ctypes.c_double(-9999.99 if dpsi is None else dpsi), ctypes.c_double(r),
             ctypes.c_double(a), ctypes.c_longlong(max_attempts), out.ctypes.data_as(_dp),

@@ -206,6 +206,15 @@ def main():
         res, err, _ = O.integrate_sos(yo7, psi, pt, pa, m, rtol=1e-10, atol=1e-10, impl="ref")
         assert not err.any()
         out[f"sos_{m}"] = res
+    # planar (integratePlanarOrbit_sos), surfaces x = 0 and y = 0
+    yo5 = np.concatenate([seeded_ics(8, 6, planar=True), np.linspace(0.0, 1.0, 8)[:, None]], 1)
+    out["sos_planar_yo"] = yo5
+    for surface in (0, 1):
+        for m in ("rk4", "rk6", "dopr54", "dop853"):
+            res, err, _ = O.integrate_sos(yo5, psi, pt2, pa2, m, rtol=1e-10, atol=1e-10,
+                                          planar=True, surface=surface, impl="ref")
+            assert not err.any()
+            out[f"sos_planar{surface}_{m}"] = res
     psi_i = np.linspace(0.0, 1.0, 6)[None, :] * np.linspace(6.0, 30.0, 8)[:, None]
     out["sos_psi_indiv"] = psi_i
     res, _, _ = O.integrate_sos(yo7, psi_i, pt, pa, "dop853", rtol=1e-10, atol=1e-10, impl="ref")

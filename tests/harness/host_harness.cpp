@@ -107,36 +107,51 @@ extern "C" int harness_integrate(int planar, int var, int method, int prec, int 
 #undef HARNESS_ARGS
 }
 
-// Surface-of-section machines (3D, FP64, run-time component list) on SOS
-// states w [nobj][7] = (x, y, vx, vy, A, t, psi); out [nobj][nt][7] raw.
-extern "C" int harness_integrate_sos(int method, int nobj, const double* w, int nt,
-                                     const double* t, int indiv_t, int npot, const int* pot_type,
-                                     const double* pot_args, double dt, double rtol, double atol,
-                                     long long max_att, double* out, int* err, long long* nsteps)
+// Surface-of-section machines (FP64, run-time component list) on SOS states:
+// system 1 (3D): w [nobj][7] = (x, y, vx, vy, A, t, psi); 2 / 3 (planar,
+// surface x = 0 / y = 0): w [nobj][5] = (u, vu, A, t, psi); out raw rows.
+template <class SYS, int D>
+static int run_sos(int method, int nobj, const double* w, int nt, const double* t, int indiv_t,
+                   const GpComp* c, int npot, double dt, double rtol, double atol,
+                   long long max_att, double* out, int* err, long long* nsteps)
 {
-  std::vector<GpComp> comps(npot);
-  int rc = compile_group(0, npot, pot_type, pot_args, comps.data(), nullptr);
-  if (rc) return rc;
-  const GpComp* c = comps.data();
   switch (method) {
     case M_RK4:
-      run_all<RKMachine<3, false, 4, SosSystem>, 3, PREC_FP64, false, DynPot>(
+      run_all<RKMachine<D, false, 4, SYS>, D, PREC_FP64, false, DynPot>(
           nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol, max_att, out, err, nsteps);
       return 0;
     case M_RK6:
-      run_all<RKMachine<3, false, 6, SosSystem>, 3, PREC_FP64, false, DynPot>(
+      run_all<RKMachine<D, false, 6, SYS>, D, PREC_FP64, false, DynPot>(
           nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol, max_att, out, err, nsteps);
       return 0;
     case M_DOPR54:
-      run_all<Dopr54Machine<3, false, SosSystem>, 3, PREC_FP64, false, DynPot>(
+      run_all<Dopr54Machine<D, false, SYS>, D, PREC_FP64, false, DynPot>(
           nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol, max_att, out, err, nsteps);
       return 0;
     case M_DOP853:
-      run_all<Dop853Machine<3, false, SosSystem>, 3, PREC_FP64, false, DynPot>(
+      run_all<Dop853Machine<D, false, SYS>, D, PREC_FP64, false, DynPot>(
           nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol, max_att, out, err, nsteps);
       return 0;
   }
   return -2;
+}
+
+extern "C" int harness_integrate_sos(int system, int method, int nobj, const double* w, int nt,
+                                     const double* t, int indiv_t, int npot, const int* pot_type,
+                                     const double* pot_args, double dt, double rtol, double atol,
+                                     long long max_att, double* out, int* err, long long* nsteps)
+{
+  const int planar = system != 1;
+  std::vector<GpComp> comps(npot);
+  int rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
+  if (rc) return rc;
+  const GpComp* c = comps.data();
+#define SOS_ARGS method, nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol, max_att, out, err, nsteps
+  if (system == 1) return run_sos<SosSystem, 3>(SOS_ARGS);
+  if (system == 2) return run_sos<PlanarSosSystem<0>, 2>(SOS_ARGS);
+  if (system == 3) return run_sos<PlanarSosSystem<1>, 2>(SOS_ARGS);
+#undef SOS_ARGS
+  return -1;
 }
 
 // accelerations (and tidal tensors) at points, for force-level tests

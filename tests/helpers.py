@@ -143,3 +143,26 @@ def sos_diff(a, b):
     d = np.abs(np.asarray(a) - np.asarray(b))
     d[..., 5] = np.abs((a[..., 5] - b[..., 5] + np.pi) % (2 * np.pi) - np.pi)
     return d
+
+
+def polar_to_sos(v, surface):
+    """galpy's polar_to_sos_galpy on rows (R, vR, vT, phi, t): surface 1
+    (y = 0) -> (x, vx, A, t, psi), otherwise (x = 0) -> (y, vy, A, t, psi)."""
+    v = np.asarray(v, dtype=float)
+    R, vR, vT, phi, t = (v[..., k] for k in range(5))
+    c, s = np.cos(phi), np.sin(phi)
+    x, y, vx, vy = R * c, R * s, vR * c - vT * s, vR * s + vT * c
+    if surface == 1:
+        return np.stack([x, vx, np.sqrt(y * y + vy * vy), t, np.arctan2(y, vy)], -1)
+    return np.stack([y, vy, np.sqrt(x * x + vx * vx), t, np.arctan2(x, vx)], -1)
+
+
+def sos_to_polar(v, surface):
+    """galpy's sos_to_polar_galpy on rows -> (R, vR, vT, phi, t)."""
+    v = np.asarray(v, dtype=float)
+    u, vu, A, t, psi = (v[..., k] for k in range(5))
+    w, vw = A * np.sin(psi), A * np.cos(psi)
+    x, vx, y, vy = (u, vu, w, vw) if surface == 1 else (w, vw, u, vu)
+    phi = np.arctan2(y, x)
+    c, s = np.cos(phi), np.sin(phi)
+    return np.stack([np.sqrt(x * x + y * y), vx * c + vy * s, -vx * s + vy * c, phi, t], -1)

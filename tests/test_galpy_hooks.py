@@ -122,3 +122,33 @@ def test_integrate_sos_routes(monkeypatch):
             o.integrate_SOS(psi, MWPotential2014, method="symplec4_cuda")
     finally:
         galpy_hooks.uninstall()
+
+
+def test_planar_integrate_sos_routes(monkeypatch):
+    from galpy.orbit import Orbit
+    from galpy.potential import MWPotential2014
+
+    from galpy_b200 import galpy_hooks
+
+    calls = []
+
+    def fake(pot, yo, psi, t0, int_method, **kw):
+        calls.append((np.array(yo).shape, int_method, kw.get("surface", "x")))
+        yo = np.atleast_2d(yo)
+        out = np.zeros((len(yo), len(psi), 5))
+        out[..., :4] = yo[:, None, :4]
+        out[..., 4] = psi
+        return out, np.zeros(len(yo), np.int32)
+
+    monkeypatch.setattr(galpy_hooks, "integratePlanarOrbit_sos_cuda", fake)
+    galpy_hooks.install()
+    try:
+        psi = np.linspace(0, 10 * np.pi, 6)
+        o = Orbit([[1.0, 0.1, 1.1, 0.3], [1.2, 0.0, 1.0, 1.0]])
+        o.integrate_SOS(psi, MWPotential2014, method="rk4_cuda", surface="y")
+        assert calls[-1] == ((2, 4), "rk4_cuda", "y") and o.orbit.shape == (2, 6, 4)
+        o3 = Orbit([[1.0, 0.1, 1.1]])
+        o3.integrate_SOS(psi, MWPotential2014, method="dop853_cuda")
+        assert calls[-1][0] == (1, 4) and calls[-1][2] == "x" and o3.orbit.shape == (1, 6, 3)
+    finally:
+        galpy_hooks.uninstall()

@@ -250,6 +250,36 @@ def test_surface_of_section(oracle, golden, method):
         gb.integrateFullOrbit_sos_cuda((pt, pa), ics[:2], psi[0], 0.0, "symplec4_cuda")
 
 
+@pytest.mark.parametrize("surface", ["x", "y"])
+@pytest.mark.parametrize("method", ["rk4", "dop853"])
+def test_planar_surface_of_section(oracle, golden, method, surface):
+    """integratePlanarOrbit_sos_cuda against the reference's C (golden) and
+    the oracle on a larger batch."""
+    pt, pa = golden["mw14_planar_type"], golden["mw14_planar_args"]
+    s = 1 if surface == "y" else 0
+    yo = golden["sos_planar_yo"]
+    out, err = gb.integratePlanarOrbit_sos_cuda((pt, pa), yo[:, :4], golden["sos_psi"],
+                                                yo[:, 4], cuda(method), surface=surface,
+                                                rtol=1e-10, atol=1e-10, progressbar=False)
+    ref = golden[f"sos_planar{s}_{method}"]
+    d = np.abs(out - ref)
+    d[..., 3] = np.abs((out[..., 3] - ref[..., 3] + np.pi) % (2 * np.pi) - np.pi)
+    assert not err.any() and d.max() < 1e-9
+    ics = seeded_ics(300, 39, planar=True)
+    yo = np.concatenate([ics, np.zeros((300, 1))], 1)
+    psi = np.linspace(0.0, 12.0 * np.pi, 7)
+    ref, _, nref = oracle.integrate_sos(yo, psi, pt, pa, method, rtol=1e-10, atol=1e-10,
+                                        planar=True, surface=s)
+    out, err, ns = gb.integratePlanarOrbit_sos_cuda((pt, pa), ics, psi, 0.0, cuda(method),
+                                                    surface=surface, rtol=1e-10, atol=1e-10,
+                                                    progressbar=False, return_nsteps=True)
+    same = ns == nref
+    d = np.abs(out - ref)
+    d[..., 3] = np.abs((out[..., 3] - ref[..., 3] + np.pi) % (2 * np.pi) - np.pi)
+    d = d.max(axis=(1, 2))
+    assert not err.any() and same.mean() >= 0.95 and d[same].max() < 1e-8 and d.max() < 1e-6
+
+
 def test_device_api_soa_matches_galpy_layout(mw14):
     import torch
 

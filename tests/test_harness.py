@@ -4,7 +4,7 @@ against the CPU oracle.  This checks the kernel logic on every CPU-only run;
 tests/test_gpu_parity.py checks the compiled kernels on the GPU."""
 import numpy as np
 import pytest
-from helpers import SPHERICAL, cyl_diff, cyl_to_sos, golden_pot, sos_diff, sos_to_cyl, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
+from helpers import SPHERICAL, cyl_diff, cyl_to_sos, golden_pot, polar_to_sos, sos_diff, sos_to_cyl, sos_to_polar, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
 
 METHODS = ["leapfrog", "rk4", "rk6", "symplec4", "symplec6", "dopr54", "dop853"]
 POTS = ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"] + SPHERICAL
@@ -287,3 +287,20 @@ def test_surface_of_section_machines(harness, oracle, golden, method):
                                              atol=1e-10)
         assert not err.any() and np.array_equal(ns, nref), (name, ns, nref)
         assert sos_diff(ref, sos_to_cyl(raw)).max() < 1e-10, name
+
+
+@pytest.mark.parametrize("surface", [0, 1])
+@pytest.mark.parametrize("method", ["rk4", "rk6", "dopr54", "dop853"])
+def test_planar_surface_of_section_machines(harness, oracle, golden, method, surface):
+    pt, pa = golden["mw14_planar_type"], golden["mw14_planar_args"]
+    yo = np.concatenate([seeded_ics(8, 20, planar=True), np.linspace(0, 2, 8)[:, None]], 1)
+    psi = np.linspace(0.0, 12.0 * np.pi, 7)
+    ref, _, nref = oracle.integrate_sos(yo, psi, pt, pa, method, rtol=1e-10, atol=1e-10,
+                                        planar=True, surface=surface)
+    raw, err, ns = harness.integrate_sos(polar_to_sos(yo, surface), psi, pt, pa, method,
+                                         rtol=1e-10, atol=1e-10, surface=surface)
+    assert not err.any() and np.array_equal(ns, nref)
+    got = sos_to_polar(raw, surface)
+    d = np.abs(got - ref)
+    d[..., 3] = np.abs((got[..., 3] - ref[..., 3] + np.pi) % (2 * np.pi) - np.pi)
+    assert d.max() < 1e-10

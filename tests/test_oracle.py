@@ -215,3 +215,29 @@ def test_oracle_surface_of_section(oracle, golden, method):
             a, ea, _ = oracle.integrate_sos(yo, psi, pt, pa, method, **kw)
             b, eb, _ = oracle.integrate_sos(yo, psi, pt, pa, method, impl="ref", **kw)
             assert np.array_equal(a, b) and np.array_equal(ea, eb), (name, kw)
+
+
+@pytest.mark.parametrize("surface", [0, 1])
+def test_oracle_planar_surface_of_section(oracle, golden, surface):
+    """integratePlanarOrbit_sos (integratePlanarOrbit.c:848-939, 1056-1123)
+    for the surfaces x = 0 and y = 0: golden vectors of the reference's C and,
+    where the reference build is present, bit for bit."""
+    pt, pa = golden["mw14_planar_type"], golden["mw14_planar_args"]
+    for m in SOS_METHODS:
+        a, err, _ = oracle.integrate_sos(golden["sos_planar_yo"], golden["sos_psi"], pt, pa, m,
+                                         rtol=1e-10, atol=1e-10, planar=True, surface=surface)
+        assert not err.any()
+        np.testing.assert_allclose(a, golden[f"sos_planar{surface}_{m}"], rtol=0, atol=1e-12)
+    if not oracle.ref_available():
+        return
+    yo = np.concatenate([seeded_ics(6, 10, planar=True), np.zeros((6, 1))], 1)
+    psi = np.linspace(0.0, 12.0 * np.pi, 7)
+    for name in ("logtri", "flatpower"):
+        ptn = golden.get(f"{name}_planar_type", golden[f"{name}_type"])
+        pan = golden.get(f"{name}_planar_args", golden[f"{name}_args"])
+        for m in SOS_METHODS:
+            a, ea, _ = oracle.integrate_sos(yo, psi, ptn, pan, m, rtol=1e-9, atol=1e-9,
+                                            planar=True, surface=surface)
+            b, eb, _ = oracle.integrate_sos(yo, psi, ptn, pan, m, rtol=1e-9, atol=1e-9,
+                                            planar=True, surface=surface, impl="ref")
+            assert np.array_equal(a, b) and np.array_equal(ea, eb), (name, m)
