@@ -1054,13 +1054,22 @@ struct Dopr54Machine : OrbitCommon {
   template <class W>
   GPC_HD void attempt_done(const double* d, W& out)
   {
+    // The reference's norm sqrt(sum_i exp(2 ln|e_i| - 2 s) / N) with the
+    // scale s from max_i ln|yo_i| (bovy_rk.c:723-738), evaluated as
+    // sqrt(sum_i e_i^2 exp(-2 s) / N) with max_i ln|yo_i| = ln max_i |yo_i|:
+    // the same values up to rounding, with 2 logs and 3 exps instead of
+    // 2N + 1 logs and N + 2 exps per attempt (which had kept the FP64 pipe
+    // busy with the controller rather than the force).
+    double ymax = fabs(yo[0]), e = 0.;
 #pragma unroll
-    for (int k = 0; k < N; k++) yerr[k] += dp5::e7 * h * d[k];
-    const double sc = est_scale(yo, N, 1, rtol, atol);
-    double e = 0.;
-#pragma unroll
-    for (int k = 0; k < N; k++) e += exp(2. * log(fabs(yerr[k])) - 2. * sc);
-    e = sqrt(e / N);
+    for (int k = 0; k < N; k++) {
+      yerr[k] += dp5::e7 * h * d[k];
+      ymax = fmax(ymax, fabs(yo[k]));
+      e += yerr[k] * yerr[k];
+    }
+    const double m = log(ymax), c = fmax(atol, rtol + m);
+    const double sc = log(exp(atol - c) + exp(rtol + m - c)) + c;
+    e = sqrt(e * exp(-2. * sc) / N);
     const double corr = 0.85 * pow(e, -.2);
     double p2 = round(log(corr) / log(2.));
     if (p2 > 3.)
