@@ -550,10 +550,18 @@ def methods_leg(gb, torch, dev, stream, pg, peak, rank, cpu=True, n=131072, K=3,
     world = pg.get_world_size() if pg else 1
     res = {"workload": METHODS_WORKLOAD, "n_gpus": world, "steps": K, "warmup": W,
            "per_method": {}}
+    from galpy_b200 import autotune
+
     for m, flops in METHOD_FLOPS.items():
+        # launch shape (orbits per block, register budget) from the autotuner,
+        # as for the headline
+        tuned = autotune.tune(comps_d, ncomp, w0, t_d, out, err, m + "_cuda", signature=sig,
+                              comps_host=comps)
+        kw = autotune.launch_kwargs(tuned)
+
         def run():
             gb.integrate_device(comps_d, ncomp, w0, t_d, out, err, m + "_cuda", nsteps=nsteps,
-                                signature=sig, comps_host=comps, stream=stream)
+                                signature=sig, comps_host=comps, stream=stream, **kw)
 
         for _ in range(W):
             run()
@@ -572,6 +580,7 @@ def methods_leg(gb, torch, dev, stream, pg, peak, rank, cpu=True, n=131072, K=3,
         rate = steps * K / (ms * 1e-3)
         entry = {"value": rate, "unit": "orbit-steps/s", "ms_per_step": ms / K,
                  "steps_per_batch": steps, "orbits_with_err": nbad,
+                 "launch": {k: tuned[k] for k in ("block_size", "variant")},
                  "flops_per_step": flops,
                  "fp64_frac_of_measured_peak": rate / world * flops / 1e12 / peak if peak
                  else None}
@@ -584,7 +593,9 @@ def methods_leg(gb, torch, dev, stream, pg, peak, rank, cpu=True, n=131072, K=3,
             except Exception as exc:  # report, do not hide
                 entry["cpu_reference"] = {"value": None, "error": repr(exc)}
         res["per_method"][m] = entry
-    res["gpu_launches"] = 2 * (K + W) * len(METHOD_FLOPS)  # cost pass + orbit kernel per run
+    # cost pass + orbit kernel per timed or warm-up run (the autotuner's trial
+    # launches come before)
+    res["gpu_launches"] = 2 * (K + W) * len(METHOD_FLOPS)
     return res
 
 

@@ -26,6 +26,11 @@ _ALIASES = {"leapfrog": 0, "rk4": 1, "rk6": 2, "symplec4": 3, "symplec6": 4, "do
             "dop853": 6}
 CUDA_METHODS = {f"{name}_cuda": code for name, code in _ALIASES.items()}
 PRECISIONS = {"fp64": _lib.FP64, "f32force": _lib.F32FORCE}
+# the ODE system of a device launch: orbits, or surface-of-section states
+# (3D rows (x, y, vx, vy, A, t, psi); planar rows (u, vu, A, t, psi) for the
+# surface x = 0 or y = 0)
+SYSTEMS = {"orbit": _lib.SYS_ORBIT, "sos": _lib.SYS_SOS, "sos_planar_x": _lib.SYS_SOS_PLANAR_X,
+           "sos_planar_y": _lib.SYS_SOS_PLANAR_Y}
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -304,7 +309,8 @@ def integrate_device(comps, ncomp, w0, t, out, err, int_method, planar=False, va
                      nsteps=None, group=None, in_layout="soa", out_layout="soa_rect",
                      out_row0=0, dt=None, rtol=None, atol=None, precision="fp64",
                      max_attempts=0, stream=None, block_size=0, grid_size=0, signature=0,
-                     schedule="longest_first", variant=0, comps_host=None, tail_sms=-1):
+                     schedule="longest_first", variant=0, comps_host=None, tail_sms=-1,
+                     system="orbit"):
     """Asynchronous integration of device-resident torch tensors.
 
     comps: uint8 CUDA tensor of compiled records (compile_potential); w0
@@ -312,7 +318,10 @@ def integrate_device(comps, ncomp, w0, t, out, err, int_method, planar=False, va
     [N, nt]; out float64 sized for the layout ('soa_rect'/'soa_cyl':
     [nv, nt-out_row0, N], 'aos_rect'/'galpy': [N, nt-out_row0, nv]); err int32
     [N]; nsteps int64 [N] or None; group int32 [N] or None; signature from
-    ``signature(pot)`` selects kernels specialised for the component list.
+    ``signature(pot)`` selects kernels specialised for the component list;
+    system 'orbit' (default), or a surface-of-section system ('sos': 3D rows
+    of 7, t holding the psi increments; 'sos_planar_x' / 'sos_planar_y':
+    planar rows of 5, planar=True) with rk4/rk6/dopr54/dop853 in float64.
     Runs on `stream` (a torch.cuda.Stream, default: the current stream)."""
     import torch
 
@@ -360,8 +369,9 @@ def integrate_device(comps, ncomp, w0, t, out, err, int_method, planar=False, va
     # single-potential launch pass its scalars as kernel parameters
     L.comps_host = comps_host.ctypes.data if comps_host is not None else None
     # SMs reserved for the longest orbits of a large longest-first batch
-    L.size_ext = 1
+    L.size_ext = 2
     L.tail_sms = int(tail_sms)
+    L.system = SYSTEMS[system] if isinstance(system, str) else int(system)
     _lib.check(_lib.lib().galpy_cuda_integrate_device(ctypes.byref(L)))
 
 

@@ -280,6 +280,58 @@ def test_planar_surface_of_section(oracle, golden, method, surface):
     assert not err.any() and same.mean() >= 0.95 and d[same].max() < 1e-8 and d.max() < 1e-6
 
 
+def test_device_api_surface_of_section(golden):
+    """The surface-of-section systems through the device-resident entry point
+    (SoA rows, galpy-coordinate output) agree with the host entry points."""
+    import torch
+
+    from helpers import cyl_to_sos, polar_to_sos
+
+    dev = torch.device("cuda:0")
+    pt, pa = golden["mw14_type"], golden["mw14_args"]
+    yo = golden["sos_yo"]
+    psi = golden["sos_psi"]
+    ref, _ = gb.integrateFullOrbit_sos_cuda((pt, pa), yo[:, :6], psi, yo[:, 6], "dop853_cuda",
+                                            rtol=1e-10, atol=1e-10, progressbar=False)
+    comps, n = gb.compile_potential((pt, pa))
+    w0 = torch.tensor(cyl_to_sos(yo).T.copy(), device=dev)
+    out = torch.empty((7, len(psi), len(yo)), dtype=torch.float64, device=dev)
+    e = torch.empty(len(yo), dtype=torch.int32, device=dev)
+    gb.integrate_device(torch.tensor(comps, device=dev), n, w0, torch.tensor(psi, device=dev),
+                        out, e, "dop853_cuda", out_layout="soa_cyl", rtol=1e-10, atol=1e-10,
+                        system="sos")
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().transpose(2, 1, 0)
+    assert not e.cpu().numpy().any() and sos_diff(ref, got).max() < 1e-13
+    # planar, surface y = 0
+    pt2, pa2 = golden["mw14_planar_type"], golden["mw14_planar_args"]
+    yo5 = golden["sos_planar_yo"]
+    ref, _ = gb.integratePlanarOrbit_sos_cuda((pt2, pa2), yo5[:, :4], psi, yo5[:, 4],
+                                              "rk4_cuda", surface="y", rtol=1e-10, atol=1e-10,
+                                              progressbar=False)
+    comps, n = gb.compile_potential((pt2, pa2), planar=True)
+    w0 = torch.tensor(polar_to_sos(yo5, 1).T.copy(), device=dev)
+    out = torch.empty((5, len(psi), len(yo5)), dtype=torch.float64, device=dev)
+    e = torch.empty(len(yo5), dtype=torch.int32, device=dev)
+    gb.integrate_device(torch.tensor(comps, device=dev), n, w0, torch.tensor(psi, device=dev),
+                        out, e, "rk4_cuda", planar=True, out_layout="soa_cyl", rtol=1e-10,
+                        atol=1e-10, system="sos_planar_y")
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().transpose(2, 1, 0)
+    d = np.abs(got - ref)
+    d[..., 3] = np.abs((got[..., 3] - ref[..., 3] + np.pi) % (2 * np.pi) - np.pi)
+    assert not e.cpu().numpy().any() and d.max() < 1e-13
+    # inconsistent requests are refused before any work
+    with pytest.raises(gb.CudaError):
+        gb.integrate_device(torch.tensor(comps, device=dev), n, w0,
+                            torch.tensor(psi, device=dev), out, e, "symplec4_cuda", planar=True,
+                            system="sos_planar_y")
+    with pytest.raises(gb.CudaError):
+        gb.integrate_device(torch.tensor(comps, device=dev), n, w0,
+                            torch.tensor(psi, device=dev), out, e, "rk4_cuda", planar=False,
+                            system="sos_planar_y")
+
+
 def test_device_api_soa_matches_galpy_layout(mw14):
     import torch
 
