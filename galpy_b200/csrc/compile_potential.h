@@ -27,7 +27,7 @@ inline int galpy_nargs(int type, int planar)
     case T_PSWC: return planar ? 3 : 5;
     case T_POWER: case T_JAFFE: case T_ISOCHRONE: case T_PLUMMER: case T_PSEUDOISO:
     case T_BURKERT: case T_DEHNENCORE: return 2;
-    case T_DEHNEN: case T_HOMSPHERE: return 3;
+    case T_DEHNEN: case T_HOMSPHERE: case T_EINASTO: return 3;
     case T_NULL: return 0;
     case T_FLATPOWER: return planar ? 3 : 4;
     default: return -1;
@@ -272,6 +272,20 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
         break;
       case T_NULL:
         break;
+      case T_EINASTO: {  // (amp, h, n)
+        const double h = p[1], n = p[2];
+        if (!(h > 0.0) || !(n > 0.0)) return -1;
+        c.c[1] = h;
+        c.c[2] = 1.0 / n;
+        c.c[3] = 3.0 * n;
+        c.c[4] = lgamma(3.0 * n);
+        c.c[5] = 4.0 * M_PI * n * h * h * h * tgamma(3.0 * n);
+        c.c[6] = 4.0 * M_PI * n * tgamma(3.0 * n);
+        c.c[7] = 2.0 * n;
+        c.c[8] = lgamma(2.0 * n);
+        c.c[9] = 4.0 * M_PI * h * h * n * tgamma(2.0 * n);
+        break;
+      }
       case T_FLATPOWER: {  // (amp, alpha, q^2, core^2); planar (amp, alpha, core^2)
         const double alpha = p[1], q2 = planar ? 1.0 : p[2], core2 = planar ? p[2] : p[3];
         if (!(q2 > 0.0)) return -1;

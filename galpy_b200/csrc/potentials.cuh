@@ -6,7 +6,8 @@
 // axisymmetric or triaxial), and the spherical PowerSpherical (7), Jaffe
 // (10), Isochrone (14), Plummer (17), PseudoIsothermal (18), Burkert (20),
 // DehnenCoreSpherical (33), DehnenSpherical (34), HomogeneousSphere (35) and
-// Null (40) potentials, and the axisymmetric FlattenedPower (12).  Reference
+// Null (40) and Einasto (41) potentials, and the axisymmetric FlattenedPower
+// (12).  Reference
 // formulas:
 // galpy/potential/potential_c_ext/<name>.c.
 //
@@ -46,7 +47,8 @@ enum : int { T_LOGHALO = 0, T_MN = 5, T_HERNQUIST = 8, T_NFW = 9, T_PSWC = 15 };
 // PseudoIsothermal, Burkert, DehnenCoreSpherical, DehnenSpherical,
 // HomogeneousSphere, Null (no force)
 enum : int { T_POWER = 7, T_JAFFE = 10, T_ISOCHRONE = 14, T_PLUMMER = 17, T_PSEUDOISO = 18,
-             T_BURKERT = 20, T_DEHNENCORE = 33, T_DEHNEN = 34, T_HOMSPHERE = 35, T_NULL = 40 };
+             T_BURKERT = 20, T_DEHNENCORE = 33, T_DEHNEN = 34, T_HOMSPHERE = 35, T_NULL = 40,
+             T_EINASTO = 41 };
 // axisymmetric FlattenedPowerPotential (FlattenedPowerPotential.c)
 enum : int { T_FLATPOWER = 12 };
 
@@ -69,6 +71,8 @@ constexpr int kBinSub = 8;    // sub-intervals of a binade [1, 2) in the binade 
 //   PseudoIsothermal: c1 a, c2 1/a       Burkert: c1 a, c2 1/a, c3 pi a^3
 //   DehnenSpherical: c1 a, c2 alpha, c3 1/(3 - alpha)
 //   HomogeneousSphere: c1 R^2, c2 R^3    Null: -
+//   Einasto: c1 h, c2 1/n, c3 3n, c4 lgamma(3n), c5 4 pi n h^3 Gamma(3n),
+//              c6 4 pi n Gamma(3n), c7 2n, c8 lgamma(2n), c9 4 pi h^2 n Gamma(2n)
 //   FlattenedPower: c1 1/q^2 (1 in the plane), c2 core^2, c3 -alpha/2 - 1,
 //              c4 alpha, c5 alpha + 2
 //   PSwC potential (energy evaluation only): c8 2 pi rc^(3-alpha), c9 rc,
@@ -346,6 +350,40 @@ GPC_HD GPC_FI float nfw_log1pf(const GpComp* __restrict__ tp, float x)
   return fmaf(e, 0.69314718f, fmaf(m - 1.0f, p, corr));
 }
 
+// Regularised lower incomplete gamma P(a, x), a > 0 (series, A&S 6.5.29;
+// Legendre continued fraction for Q, A&S 6.5.31, modified Lentz).  The
+// bulge's potential energy and the Einasto profile use it; the bulge force
+// uses the gamma* table.
+GPC_HD inline double inc_gamma_P(double a, double x, double lga)
+{
+  if (!(x > 0.0)) return 0.0;
+  const double lpref = a * log(x) - x - lga;
+  if (x < a + 1.0) {
+    double ap = a, term = 1.0 / a, sum = term;
+    for (int n = 0; n < 1000; n++) {
+      ap += 1.0;
+      term *= x / ap;
+      sum += term;
+      if (fabs(term) < fabs(sum) * 1e-17) break;
+    }
+    return sum * exp(lpref);
+  }
+  double b = x + 1.0 - a, c = 1.0 / 1e-300, d = 1.0 / b, h = d;
+  for (int i = 1; i < 1000; i++) {
+    const double an = -i * (i - a);
+    b += 2.0;
+    d = an * d + b;
+    if (fabs(d) < 1e-300) d = 1e-300;
+    c = b + an / c;
+    if (fabs(c) < 1e-300) c = 1e-300;
+    d = 1.0 / d;
+    const double del = d * c;
+    h *= del;
+    if (fabs(del - 1.0) < 1e-17) break;
+  }
+  return 1.0 - exp(lpref) * h;
+}
+
 // ------------------------------------------------------------- forces ---
 // Add one component's contribution to the radial factors: the acceleration
 // is a = (x gR, y (gR + gyx), z gz).  TYPE < 0: read the type at run time.
@@ -407,6 +445,11 @@ GPC_HD GPC_FI T sph_force_factor(int type, const S& sc, T r2)
     case T_HOMSPHERE: {  // Phi' = 2 amp r inside R, 2 amp R^3 / r^2 outside
       const T ir = Num<T>::rsq(r2);
       return r2 < T(sc[1]) ? T(-2) * amp : T(-2) * amp * T(sc[2]) * ir * ir * ir;
+    }
+    case T_EINASTO: {  // Phi'/r = amp 4 pi n h^3 gamma(3n, (r/h)^(1/n)) / r^3 (in float64)
+      const double r = sqrt((double)r2), x = pow(r / sc[1], sc[2]);
+      const double P = inc_gamma_P(sc[3], x, sc[4]);
+      return T(-(double)amp * sc[5] * P / (r * r * r));
     }
     default:  // T_NULL
       return T(0);
@@ -654,6 +697,14 @@ GPC_HD inline void sph_derivs(const GpComp* __restrict__ cp, int type, double am
         d2 = -2.0 * dpr;
       }
       break;
+    case T_EINASTO: {  // Phi'' = amp (4 pi e^-x - 2 * 4 pi n Gamma(3n) P / s^3)
+      const double x = pow(r / c1, ldg(&cp->c[2]));
+      const double P = inc_gamma_P(ldg(&cp->c[3]), x, ldg(&cp->c[4]));
+      const double s = r / c1;
+      dpr = amp * ldg(&cp->c[5]) * P * ir * ir * ir;
+      d2 = amp * (4.0 * M_PI * exp(-x) - 2.0 * ldg(&cp->c[6]) * P / (s * s * s));
+      break;
+    }
     default:
       break;
   }
@@ -773,39 +824,6 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
 }
 
 // -------------------------------------------------- potential values ---
-// Regularised lower incomplete gamma P(a, x), a > 0 (series, A&S 6.5.29;
-// Legendre continued fraction for Q, A&S 6.5.31, modified Lentz).  Only the
-// potential-energy evaluation uses it; the integrators use the gamma* table.
-GPC_HD inline double inc_gamma_P(double a, double x, double lga)
-{
-  if (!(x > 0.0)) return 0.0;
-  const double lpref = a * log(x) - x - lga;
-  if (x < a + 1.0) {
-    double ap = a, term = 1.0 / a, sum = term;
-    for (int n = 0; n < 1000; n++) {
-      ap += 1.0;
-      term *= x / ap;
-      sum += term;
-      if (fabs(term) < fabs(sum) * 1e-17) break;
-    }
-    return sum * exp(lpref);
-  }
-  double b = x + 1.0 - a, c = 1.0 / 1e-300, d = 1.0 / b, h = d;
-  for (int i = 1; i < 1000; i++) {
-    const double an = -i * (i - a);
-    b += 2.0;
-    d = an * d + b;
-    if (fabs(d) < 1e-300) d = 1e-300;
-    c = b + an / c;
-    if (fabs(c) < 1e-300) c = 1e-300;
-    d = 1.0 / d;
-    const double del = d * c;
-    h *= del;
-    if (fabs(del - 1.0) < 1e-17) break;
-  }
-  return 1.0 - exp(lpref) * h;
-}
-
 // Potential of the spherical potentials at r^2 (0 for Null, whose constant
 // value galpy adds on the Python side only).
 GPC_HD inline double sph_value(const GpComp* __restrict__ cp, int type, double amp, double r2)
@@ -837,6 +855,12 @@ GPC_HD inline double sph_value(const GpComp* __restrict__ cp, int type, double a
     }
     case T_HOMSPHERE:
       return r2 < c1 ? amp * (r2 - 3.0 * c1) : -2.0 * amp * ldg(&cp->c[2]) / r;
+    case T_EINASTO: {  // -amp 4 pi h^2 n [Gamma(3n) P(3n, x) / s + Gamma(2n) Q(2n, x)]
+      const double s = r / c1, x = pow(s, ldg(&cp->c[2]));
+      const double P3 = inc_gamma_P(ldg(&cp->c[3]), x, ldg(&cp->c[4]));
+      const double Q2 = 1.0 - inc_gamma_P(ldg(&cp->c[7]), x, ldg(&cp->c[8]));
+      return -amp * (ldg(&cp->c[6]) * c1 * c1 * P3 / s + ldg(&cp->c[9]) * Q2);
+    }
     default:
       return 0.0;
   }

@@ -67,7 +67,8 @@ enum {
   PT_DEHNENCORE = 33, /* DehnenCoreSphericalPotential (DehnenCorePotential.c) */
   PT_DEHNEN = 34,     /* DehnenSphericalPotential (DehnenPotential.c) */
   PT_HOMSPHERE = 35,  /* HomogeneousSpherePotential */
-  PT_NULL = 40        /* NullPotential (ZeroForce) */
+  PT_NULL = 40,       /* NullPotential (ZeroForce) */
+  PT_EINASTO = 41     /* EinastoPotential (through SphericalPotential.c) */
 };
 /* axisymmetric: FlattenedPowerPotential (FlattenedPowerPotential.c); args
    (amp, alpha, q^2, core^2) in 3D, (amp, alpha, core^2) in the plane */
@@ -96,7 +97,7 @@ static int nargs_of(int type, int planar)
   case PT_PSWC: return planar ? 3 : 5;
   case PT_POWER: case PT_JAFFE: case PT_ISOCHRONE: case PT_PLUMMER: case PT_PSEUDOISO:
   case PT_BURKERT: case PT_DEHNENCORE: return 2;
-  case PT_DEHNEN: case PT_HOMSPHERE: return 3;
+  case PT_DEHNEN: case PT_HOMSPHERE: case PT_EINASTO: return 3;
   case PT_NULL: return 0;
   case PT_FLATPOWER: return planar ? 3 : 4;
   default: return -1;
@@ -108,9 +109,37 @@ static int is_new_spherical(int type)
   switch (type) {
   case PT_POWER: case PT_JAFFE: case PT_ISOCHRONE: case PT_PLUMMER: case PT_PSEUDOISO:
   case PT_BURKERT: case PT_DEHNENCORE: case PT_DEHNEN: case PT_HOMSPHERE: case PT_NULL:
+  case PT_EINASTO:
     return 1;
   }
   return 0;
+}
+
+/* Einasto's radial functions (EinastoPotential.c), args (amp, h, n); the
+   reference's GSL calls restated with tgamma and the incomplete gamma of
+   incgamma.c; SphericalPotential.c applies amp */
+static double einasto_rforce(const ocomp *c, double r)
+{
+  double h = c->p[1], n = c->p[2], s = r / h;
+  double gamma_3n = tgamma(3 * n);
+  double gamma_upper_3n = oracle_gamma_inc_Q(3 * n, pow(s, 1.0 / n));
+  double s_2 = pow(s, -2.0);
+  return (4.0 * M_PI * h * n * gamma_3n) * s_2 * (gamma_upper_3n - 1.0);
+}
+static double einasto_r2deriv(const ocomp *c, double r)
+{
+  double h = c->p[1], n = c->p[2], s = r / h, s_1n = pow(s, 1.0 / n);
+  double gamma_3n = tgamma(3 * n);
+  double gamma_upper_3n = oracle_gamma_inc_Q(3 * n, s_1n);
+  return -(4.0 * M_PI * n * gamma_3n) *
+         ((-2 * pow(s, -3)) * (gamma_upper_3n - 1) - ((1 / n) * exp(-s_1n) / gamma_3n));
+}
+static double einasto_revaluate(const ocomp *c, double r)
+{
+  double h = c->p[1], n = c->p[2], s = r / h, s_1n = pow(s, 1.0 / n);
+  return (-(4.0 * M_PI * pow(h, 2) * n * tgamma(3 * n)) * pow(s, -1) *
+          (1 - oracle_gamma_inc_Q(3 * n, s_1n) +
+           s * (tgamma(2 * n) * oracle_gamma_inc_Q(2 * n, s_1n)) / tgamma(3 * n)));
 }
 
 /* 3D R or z force of the spherical potentials: X is R (Rforce) or Z
@@ -156,6 +185,10 @@ static double sph_force3(const ocomp *c, double R, double Z, double X)
     if (r2 < R2) return -2. * amp * X;
     return -2. * amp * R3 * X / pow(r2, 1.5);
   }
+  case PT_EINASTO: { /* SphericalPotentialRforce / zforce */
+    double r = sqrt(R * R + Z * Z);
+    return amp * einasto_rforce(c, r) * X / r;
+  }
   }
   return 0.;
 }
@@ -200,6 +233,8 @@ static double sph_planarRforce(const ocomp *c, double R)
     if (r2 < R2) return -2. * amp * R;
     return -2. * amp * R3 / r2;
   }
+  case PT_EINASTO:
+    return amp * einasto_rforce(c, R);
   }
   return 0.;
 }
@@ -249,6 +284,8 @@ static double sph_planarR2deriv(const ocomp *c, double R)
     if (r2 < R2) return 2. * amp;
     return -4. * amp * R3 / pow(r2, 1.5);
   }
+  case PT_EINASTO:
+    return amp * einasto_r2deriv(c, R);
   }
   return 0.;
 }
@@ -328,6 +365,8 @@ static double sph_eval(const ocomp *c, double R, double Z)
     if (r2 < R2) return amp * (r2 - 3. * R2);
     return -2. * amp * R3 / sqrt(r2);
   }
+  case PT_EINASTO:
+    return amp * einasto_revaluate(c, sqrt(R * R + Z * Z));
   }
   return 0.;
 }

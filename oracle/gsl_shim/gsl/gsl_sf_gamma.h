@@ -6,4 +6,5 @@
 double gsl_sf_gamma(double x);
 double gsl_sf_gamma_inc_P(double a, double x);
 double gsl_sf_gamma_inc(double a, double x);
+double gsl_sf_gamma_inc_Q(double a, double x);
 #endif

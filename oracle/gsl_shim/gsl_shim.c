@@ -16,6 +16,7 @@ double oracle_gamma_inc_Q(double a, double x);
 double gsl_sf_gamma(double x) { return tgamma(x); }
 double gsl_sf_gamma_inc_P(double a, double x) { return oracle_gamma_inc_P(a, x); }
 double gsl_sf_gamma_inc(double a, double x) { return tgamma(a) * oracle_gamma_inc_Q(a, x); }
+double gsl_sf_gamma_inc_Q(double a, double x) { return oracle_gamma_inc_Q(a, x); }
 
 static void shim_unreachable(const char *what)
 {

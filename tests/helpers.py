@@ -106,7 +106,7 @@ def differentiation_workload(n, seed=3):
 # the spherical (and the axisymmetric FlattenedPower) potentials added
 # behind the component template (golden-vector names)
 SPHERICAL = ["power", "kepler", "jaffe", "isochrone", "plummer", "pseudoiso", "burkert",
-             "dehnencore", "dehnen", "homsphere", "null", "flatpower", "flatlog"]
+             "dehnencore", "dehnen", "homsphere", "null", "einasto", "flatpower", "flatlog"]
 
 
 def golden_pot(golden, name, planar=False):

@@ -50,14 +50,17 @@ def test_forces_and_tidal_tensor(harness, oracle, golden, name):
     c, s = x / R, y / R
     ref = np.stack([c * Rf - s / R * ptq, s * Rf + c / R * ptq, zf], 1)
     # NFW at r << a cancels two terms; the reference (log(1+x)) is the less
-    # accurate side there (this code uses log1p)
-    assert (np.abs(acc - ref).max(1) / np.abs(ref).max(1)).max() < 1e-12
+    # accurate side there (this code uses log1p).  Einasto: the reference
+    # forms the enclosed-mass fraction as Q - 1, which loses ~eps / P digits
+    # where P(3n, (r/h)^(1/n)) is small; this code evaluates P directly.
+    tol = 1e-10 if name == "einasto" else 1e-12
+    assert (np.abs(acc - ref).max(1) / np.abs(ref).max(1)).max() < tol
     Kxx = -c * c * R2 + 2 * c * s / R / R * ptq + s * s / R * Rf + 2 * s * c / R * Rp - s * s / R / R * p2
     Kxy = (-s * c * R2 + (s * s - c * c) / R / R * ptq - c * s / R * Rf - (c * c - s * s) / R * Rp
            + c * s / R / R * p2)
     Kyy = -s * s * R2 - 2 * s * c / R / R * ptq - 2 * s * c / R * Rp + c * c / R * Rf - c * c / R / R * p2
     Kref = np.stack([Kxx, Kxy, Kyy, -c * Rz + s / R * zp, -s * Rz - c / R * zp, -z2], 1)
-    assert (np.abs(K - Kref).max(1) / np.abs(Kref).max(1)).max() < 1e-12
+    assert (np.abs(K - Kref).max(1) / np.abs(Kref).max(1)).max() < tol
     # float32 force evaluation: single-precision accuracy
     assert (np.abs(a32 - ref).max(1) / np.abs(ref).max(1)).max() < 3e-5
 
