@@ -132,6 +132,30 @@ def test_gradients_other_potentials(harness, golden, name):
     np.testing.assert_allclose(gth, fdt, rtol=1e-6, atol=1e-6 * np.abs(fdt).max())
 
 
+@pytest.mark.parametrize("name", ["plummer", "isochrone", "einasto", "flatpower", "dehnen"])
+def test_ic_gradients_added_potentials(harness, golden, name):
+    """The potentials added behind the component template have no
+    differentiable parameters; they enter the adjoint through the tidal
+    tensor: dL/dw0 against frozen-step central differences."""
+    pt, pa = golden[f"{name}_type"], np.array(golden[f"{name}_args"], float)
+    w0 = cyl_to_rect(seeded_ics(3, 5))
+    t0, T = 0.0, 10.0
+    yT, ns, err, h = harness.adj_forward(w0, t0, T, pt, pa)
+    assert not err.any()
+    tgt = np.random.default_rng(4).normal(size=yT.shape)
+
+    def loss(w):
+        return ((harness.adj_replay(w, t0, T, pt, pa, h, ns) - tgt) ** 2).sum(1)
+
+    gw, gth, err = harness.adj_gradient(w0, t0, T, pt, pa, 2 * (yT - tgt))
+    assert not err.any() and not np.any(gth)
+    nv = w0.shape[1]
+    fdw = np.stack([central_fd(lambda v: loss(np.where(np.arange(nv) == c, v[:, None], w0)),
+                               w0[:, c].copy(), range(len(w0)), floor=1.0).diagonal()
+                    for c in range(nv)], 1)
+    np.testing.assert_allclose(gw, fdw, rtol=1e-6, atol=1e-6 * np.abs(fdw).max())
+
+
 @pytest.mark.parametrize("planar", [True, False])
 def test_ic_gradient_matches_reference_variational(harness, golden, planar):
     key = "adj_planar" if planar else "adj_3d"
