@@ -30,6 +30,7 @@ inline int galpy_nargs(int type, int planar)
     case T_DEHNEN: case T_HOMSPHERE: case T_EINASTO: return 3;
     case T_NULL: return 0;
     case T_FLATPOWER: return planar ? 3 : 4;
+    case T_KKS: return 3;
     default: return -1;
   }
 }
@@ -284,6 +285,14 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
         c.c[7] = 2.0 * n;
         c.c[8] = lgamma(2.0 * n);
         c.c[9] = 4.0 * M_PI * h * h * n * tgamma(2.0 * n);
+        break;
+      }
+      case T_KKS: {  // (amp, ac, Delta)
+        const double ac = p[1], Delta = p[2];
+        if (!(Delta > 0.0) || ac == 1.0) return -1;
+        const double gamma = Delta * Delta / (1.0 - ac * ac), alpha = gamma - Delta * Delta;
+        c.c[1] = Delta * Delta;
+        c.c[2] = alpha + gamma;
         break;
       }
       case T_FLATPOWER: {  // (amp, alpha, q^2, core^2); planar (amp, alpha, core^2)

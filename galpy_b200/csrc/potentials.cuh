@@ -7,7 +7,7 @@
 // (10), Isochrone (14), Plummer (17), PseudoIsothermal (18), Burkert (20),
 // DehnenCoreSpherical (33), DehnenSpherical (34), HomogeneousSphere (35) and
 // Null (40) and Einasto (41) potentials, and the axisymmetric FlattenedPower
-// (12).  Reference
+// (12) and KuzminKutuzovStaeckel (16).  Reference
 // formulas:
 // galpy/potential/potential_c_ext/<name>.c.
 //
@@ -49,8 +49,9 @@ enum : int { T_LOGHALO = 0, T_MN = 5, T_HERNQUIST = 8, T_NFW = 9, T_PSWC = 15 };
 enum : int { T_POWER = 7, T_JAFFE = 10, T_ISOCHRONE = 14, T_PLUMMER = 17, T_PSEUDOISO = 18,
              T_BURKERT = 20, T_DEHNENCORE = 33, T_DEHNEN = 34, T_HOMSPHERE = 35, T_NULL = 40,
              T_EINASTO = 41 };
-// axisymmetric FlattenedPowerPotential (FlattenedPowerPotential.c)
-enum : int { T_FLATPOWER = 12 };
+// axisymmetric FlattenedPowerPotential (FlattenedPowerPotential.c) and
+// KuzminKutuzovStaeckelPotential (KuzminKutuzovStaeckelPotential.c)
+enum : int { T_FLATPOWER = 12, T_KKS = 16 };
 
 constexpr int kMaxComp = 16;  // components per potential group
 constexpr int kChebN = 32;    // Chebyshev intervals of gamma*(a, u) on [0, U]
@@ -75,6 +76,8 @@ constexpr int kBinSub = 8;    // sub-intervals of a binade [1, 2) in the binade 
 //              c6 4 pi n Gamma(3n), c7 2n, c8 lgamma(2n), c9 4 pi h^2 n Gamma(2n)
 //   FlattenedPower: c1 1/q^2 (1 in the plane), c2 core^2, c3 -alpha/2 - 1,
 //              c4 alpha, c5 alpha + 2
+//   KuzminKutuzovStaeckel: c1 Delta^2, c2 alpha + gamma with
+//              gamma = Delta^2 / (1 - ac^2), alpha = gamma - Delta^2
 //   PSwC potential (energy evaluation only): c8 2 pi rc^(3-alpha), c9 rc,
 //              c10 a1 = 1 - alpha/2, c11 Gamma(a1), c12 lgamma(a1),
 //              c13 a2 = 1.5 - alpha/2, c14 Gamma(a2), c15 lgamma(a2)
@@ -402,6 +405,30 @@ struct ScalarsDirect {
   GPC_HD GPC_FI double operator[](int j) const { return p[j]; }
 };
 
+// KuzminKutuzovStaeckel: Phi = -amp V, V = 1 / (sqrt(l) + sqrt(n)) with the
+// prolate spheroidal coordinates l, n = (R^2 + z^2 - alpha - gamma +- sqrt(D))
+// / 2, D = (R^2 + z^2 - Delta^2)^2 + 4 Delta^2 R^2.  kks_parts returns the
+// pieces the force and the tidal tensor share.
+struct KksParts {
+  double isd, l, n, srl, srn, isln2, dVdl, dVdn;
+};
+GPC_HD GPC_FI KksParts kks_parts(double D2, double apg, double R2, double z2)
+{
+  KksParts k;
+  const double r2 = R2 + z2, rzm = r2 - D2;
+  const double sd = sqrt(rzm * rzm + 4.0 * D2 * R2);
+  k.isd = 1.0 / sd;
+  k.l = 0.5 * (r2 - apg + sd);
+  k.n = 0.5 * (r2 - apg - sd);
+  k.srl = sqrt(k.l);
+  k.srn = sqrt(k.n);
+  const double sln = k.srl + k.srn;
+  k.isln2 = 1.0 / (sln * sln);
+  k.dVdl = 0.5 / k.srl * k.isln2;  // -dV/dl
+  k.dVdn = 0.5 / k.srn * k.isln2;  // -dV/dn
+  return k;
+}
+
 // The spherical potentials' acceleration factor -Phi'(r)/r (a = f x), for
 // the run-time component list; FP32 and FP64 alike.
 template <typename T, class S>
@@ -523,6 +550,16 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
       const T f = -T(0.5) * amp * ir * ira * ira;
       gR += f;
       gz += f;
+      break;
+    }
+    case T_KKS: {  // in float64: a = -amp (x g_R, y g_R, z g_z)
+      const double D2 = sc[1];
+      const KksParts k = kks_parts(D2, sc[2], (double)R2, (double)z2);
+      const double r2d = (double)R2 + (double)z2;
+      const double fR = (1.0 + (r2d + D2) * k.isd) * k.dVdl + (1.0 - (r2d + D2) * k.isd) * k.dVdn;
+      const double fz = (1.0 + (r2d - D2) * k.isd) * k.dVdl + (1.0 - (r2d - D2) * k.isd) * k.dVdn;
+      gR -= amp * T(fR);
+      if (!PLANAR) gz -= amp * T(fz);
       break;
     }
     case T_FLATPOWER: {
@@ -777,6 +814,44 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
         K[5] -= amp * (iD3 * (sz - a * z2 * izb * izb * izb) - 3.0 * z2 * sz * sz * iD5);
         break;
       }
+      case T_KKS: {
+        // Phi_R / R, Phi_RR, Phi_zz, Phi_Rz in (l, n) by the chain rule
+        // (KuzminKutuzovStaeckelPotential.c R2deriv / z2deriv / Rzderiv),
+        // then the axisymmetric Cartesian Hessian
+        const double D2 = ldg(&cp->c[1]);
+        const KksParts k = kks_parts(D2, ldg(&cp->c[2]), R2, z2);
+        const double r2 = R2 + z2, rzp = r2 + D2, rzm = r2 - D2, isd = k.isd;
+        const double id = isd * isd, id15 = isd * id;
+        const double isln3 = k.isln2 / (k.srl + k.srn);
+        const double d2l = (-3.0 * k.srl - k.srn) / (4.0 * k.l * k.srl) * isln3;
+        const double d2n = (-k.srl - 3.0 * k.srn) / (4.0 * k.n * k.srn) * isln3;
+        const double d2ln = -0.5 / (k.srl * k.srn) * isln3;
+        // first derivatives per unit R (resp. z) of l and n
+        const double lR = 1.0 + rzp * isd, nR = 1.0 - rzp * isd;
+        const double lz = 1.0 + rzm * isd, nz = 1.0 - rzm * isd;
+        const double gRk = -amp * (lR * k.dVdl + nR * k.dVdn);  // a_R / R
+        const double gzk = -amp * (lz * k.dVdl + nz * k.dVdn);  // a_z / z
+        const double offR = (3.0 * R2 + z2 + D2) * isd, cubR = 2.0 * R2 * rzp * rzp * id15;
+        const double offz = (R2 + 3.0 * z2 - D2) * isd, cubz = 2.0 * z2 * rzm * rzm * id15;
+        const double PRR = amp * ((1.0 + offR - cubR) * k.dVdl + (1.0 - offR + cubR) * k.dVdn +
+                                  R2 * (lR * lR * d2l + nR * nR * d2n + 2.0 * lR * nR * d2ln));
+        const double Pzz = amp * ((1.0 + offz - cubz) * k.dVdl + (1.0 - offz + cubz) * k.dVdn +
+                                  z2 * (lz * lz * d2l + nz * nz * d2n + 2.0 * lz * nz * d2ln));
+        const double mixRz = 2.0 * isd * (1.0 - (r2 * r2 - D2 * D2) * id);  // / (R z)
+        const double PRz_Rz = amp * (mixRz * (k.dVdl - k.dVdn) + lR * lz * d2l + nR * nz * d2n +
+                                     (lR * nz + lz * nR) * d2ln);  // Phi_Rz / (R z)
+        const double PR_R = -gRk;
+        gR += gRk;
+        gz += gzk;
+        const double iR2 = R2 > 0.0 ? 1.0 / R2 : 0.0;
+        K[0] -= PRR * x * x * iR2 + PR_R * y * y * iR2;
+        K[1] -= (PRR - PR_R) * x * y * iR2;
+        K[2] -= PRR * y * y * iR2 + PR_R * x * x * iR2;
+        K[3] -= PRz_Rz * x * z;
+        K[4] -= PRz_Rz * y * z;
+        K[5] -= Pzz;
+        break;
+      }
       case T_FLATPOWER: {  // the logarithmic halo's structure with weight (alpha+2) m2^(-alpha/2-2)
         const double iq2 = ldg(&cp->c[1]);
         const double m2 = R2 + z2 * iq2 + ldg(&cp->c[2]);
@@ -903,6 +978,13 @@ GPC_HD inline double potential_value(const GpComp* __restrict__ comp, int ncomp,
       case T_LOGHALO: {
         const double D = x * x + ldg(&cp->c[3]) * y * y + z2 * ldg(&cp->c[1]) + ldg(&cp->c[2]);
         phi += 0.5 * amp * log(D);
+        break;
+      }
+      case T_KKS: {  // n clipped at 0 as the reference's Eval does
+        const double D2 = ldg(&cp->c[1]), r2 = R2 + z2, rzm = r2 - D2;
+        const double sd = sqrt(rzm * rzm + 4.0 * D2 * R2);
+        const double l = 0.5 * (r2 - ldg(&cp->c[2]) + sd), n = 0.5 * (r2 - ldg(&cp->c[2]) - sd);
+        phi -= amp / (sqrt(l) + sqrt(n > 0.0 ? n : 0.0));
         break;
       }
       case T_FLATPOWER: {

@@ -3,7 +3,7 @@
 The engine integrates in the potentials galpy hands to C as pot_type codes
 0 (LogarithmicHaloPotential), 5 (MiyamotoNagaiPotential), 8
 (HernquistPotential), 9 (NFWPotential), 15 (PowerSphericalPotentialwCutoff)
-12 (FlattenedPower) and the spherical 7 (PowerSpherical / Kepler), 10
+12 (FlattenedPower), 16 (KuzminKutuzovStaeckel) and the spherical 7 (PowerSpherical / Kepler), 10
 (Jaffe), 14 (Isochrone),
 17 (Plummer), 18 (PseudoIsothermal), 20 (Burkert), 33
 (DehnenCoreSpherical), 34 (DehnenSpherical), 35 (HomogeneousSphere), 40
@@ -28,8 +28,9 @@ T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC = 0, 5, 8, 9, 15
 # PseudoIsothermal, Burkert, DehnenCoreSpherical, DehnenSpherical,
 # HomogeneousSphere, Null, Einasto
 SPHERICAL_TYPES = (7, 10, 14, 17, 18, 20, 33, 34, 35, 40, 41)
-T_FLATPOWER = 12
-SUPPORTED_TYPES = (T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC, T_FLATPOWER) + SPHERICAL_TYPES
+T_FLATPOWER, T_KKS = 12, 16
+SUPPORTED_TYPES = (T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC, T_FLATPOWER,
+                   T_KKS) + SPHERICAL_TYPES
 
 
 class _Potential:

@@ -12,7 +12,9 @@
  *            LogarithmicHaloPotential.c:5-297, and the spherical
  *            PowerSpherical, Jaffe, Isochrone, Plummer, PseudoIsothermal,
  *            Burkert, DehnenCore, Dehnen, HomogeneousSphere potentials and
- *            ZeroForce, FlattenedPowerPotential.c (potential_c_ext/)
+ *            ZeroForce, Einasto (through SphericalPotential.c),
+ *            FlattenedPowerPotential.c, KuzminKutuzovStaeckelPotential.c
+ *            (potential_c_ext/)
  *   sums     galpy_potentials.c:120-354 (sum over components, in order)
  *   RHS      orbit_c_ext/integrateFullOrbit.c:1307-1352 (evalRectForce,
  *            evalRectDeriv), :1496-1681 (the dxdv variants);
@@ -73,6 +75,10 @@ enum {
 /* axisymmetric: FlattenedPowerPotential (FlattenedPowerPotential.c); args
    (amp, alpha, q^2, core^2) in 3D, (amp, alpha, core^2) in the plane */
 enum { PT_FLATPOWER = 12 };
+/* KuzminKutuzovStaeckelPotential (KuzminKutuzovStaeckelPotential.c); args
+   (amp, ac, Delta) in 3D and in the plane */
+enum { PT_KKS = 16 };
+
 #define OMAXPOT 32
 
 typedef struct {
@@ -100,6 +106,7 @@ static int nargs_of(int type, int planar)
   case PT_DEHNEN: case PT_HOMSPHERE: case PT_EINASTO: return 3;
   case PT_NULL: return 0;
   case PT_FLATPOWER: return planar ? 3 : 4;
+  case PT_KKS: return 3;
   default: return -1;
   }
 }
@@ -113,6 +120,76 @@ static int is_new_spherical(int type)
     return 1;
   }
   return 0;
+}
+
+/* its prolate spheroidal coordinates (l, n) and the derivatives of
+   V = 1 / (sqrt(l) + sqrt(n)) the reference uses, as it writes them */
+static double kks_Rz(const ocomp *c, double R, double z, int which)
+{
+  double amp = c->p[0], ac = c->p[1], Delta = c->p[2];
+  double gamma = Delta * Delta / (1. - ac * ac);
+  double alpha = gamma - Delta * Delta;
+  double term = R * R + z * z - alpha - gamma;
+  double discr = pow(R * R + z * z - Delta * Delta, 2.) + (4. * Delta * Delta * R * R);
+  double l = 0.5 * (term + sqrt(discr));
+  double n = 0.5 * (term - sqrt(discr));
+  double dVdl = 0.5 / sqrt(l) / pow(sqrt(l) + sqrt(n), 2.);
+  double dVdn = 0.5 / sqrt(n) / pow(sqrt(l) + sqrt(n), 2.);
+  if (which == 0) { /* Rforce */
+    double dldR = R * (1. + (R * R + z * z + Delta * Delta) / sqrt(discr));
+    double dndR = R * (1. - (R * R + z * z + Delta * Delta) / sqrt(discr));
+    return -amp * (dldR * dVdl + dndR * dVdn);
+  }
+  /* zforce */
+  double dldz = z * (1. + (R * R + z * z - Delta * Delta) / sqrt(discr));
+  double dndz = z * (1. - (R * R + z * z - Delta * Delta) / sqrt(discr));
+  return -amp * (dldz * dVdl + dndz * dVdn);
+}
+
+/* second derivatives: which = 0 R2deriv, 1 z2deriv, 2 Rzderiv */
+static double kks_hess(const ocomp *c, double R, double z, int which)
+{
+  double amp = c->p[0], ac = c->p[1], Delta = c->p[2];
+  double D2 = Delta * Delta, D4 = D2 * D2;
+  double gamma = D2 / (1. - ac * ac);
+  double alpha = gamma - D2;
+  double R2 = R * R, z2 = z * z, rz2 = R2 + z2;
+  double rzD2p = rz2 + D2, rzmD2 = rz2 - D2;
+  double term = rz2 - alpha - gamma;
+  double discr = rzmD2 * rzmD2 + (4. * D2 * R2);
+  double sdiscr = sqrt(discr), isdiscr = 1. / sdiscr;
+  double idiscr15 = isdiscr / discr, idiscr = 1. / discr;
+  double l = 0.5 * (term + sdiscr), n = 0.5 * (term - sdiscr);
+  double srl = sqrt(l), srn = sqrt(n), sln = srl + srn;
+  double isln2 = 1. / (sln * sln), isln3 = isln2 / sln;
+  double dVdl = 0.5 / srl * isln2, dVdn = 0.5 / srn * isln2;
+  double d2Vdl2 = (-3. * srl - srn) / (4. * l * srl) * isln3;
+  double d2Vdn2 = (-srl - 3. * srn) / (4. * n * srn) * isln3;
+  double d2Vdln = -0.5 / (srl * srn) * isln3;
+  if (which == 0) {
+    double rzD2p_isd = rzD2p * isdiscr;
+    double dldR = R * (1. + rzD2p_isd), dndR = R * (1. - rzD2p_isd);
+    double hess_off = (3. * R2 + z2 + D2) * isdiscr;
+    double hess_cub = 2. * R2 * rzD2p * rzD2p * idiscr15;
+    double d2ldR2 = 1. + hess_off - hess_cub, d2ndR2 = 1. - hess_off + hess_cub;
+    return amp * (d2ldR2 * dVdl + d2ndR2 * dVdn + dldR * dldR * d2Vdl2 +
+                  dndR * dndR * d2Vdn2 + 2. * dldR * dndR * d2Vdln);
+  }
+  if (which == 1) {
+    double rzmD2_isd = rzmD2 * isdiscr;
+    double dldz = z * (1. + rzmD2_isd), dndz = z * (1. - rzmD2_isd);
+    double hess_off = (R2 + 3. * z2 - D2) * isdiscr;
+    double hess_cub = 2. * z2 * rzmD2 * rzmD2 * idiscr15;
+    double d2ldz2 = 1. + hess_off - hess_cub, d2ndz2 = 1. - hess_off + hess_cub;
+    return amp * (d2ldz2 * dVdl + d2ndz2 * dVdn + dldz * dldz * d2Vdl2 +
+                  dndz * dndz * d2Vdn2 + 2. * dldz * dndz * d2Vdln);
+  }
+  double rzD2p_isd = rzD2p * isdiscr, rzmD2_isd = rzmD2 * isdiscr;
+  double dldR = R * (1. + rzD2p_isd), dndR = R * (1. - rzD2p_isd);
+  double dldz = z * (1. + rzmD2_isd), dndz = z * (1. - rzmD2_isd);
+  double mix = 2. * R * z * isdiscr * (1. - (rz2 * rz2 - D4) * idiscr);
+  return amp * (mix * dVdl - mix * dVdn + dldR * dldz * d2Vdl2 + dndR * dndz * d2Vdn2 +
+                (dldR * dndz + dldz * dndR) * d2Vdln);
 }
 
 /* Einasto's radial functions (EinastoPotential.c), args (amp, h, n); the
@@ -373,7 +450,7 @@ static double sph_eval(const ocomp *c, double R, double Z)
 
 /* Decode galpy's (pot_type, pot_args) stream (integrateFullOrbit.c:69-1040,
    integratePlanarOrbit.c:55-742 restricted to types 0/5/7/8/9/10/12/14/15/
-   17/18/20/33/34/35/40).
+   16/17/18/20/33/34/35/40/41).
    Returns 0, or -1 for an unsupported type. */
 static int opot_decode(opot *P, int npot, const int *type, const double *args, int planar)
 {
@@ -433,6 +510,8 @@ static double comp_Rforce(ocomp *c, double R, double Z, double phi)
   if (is_new_spherical(c->type)) return sph_force3(c, R, Z, R);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_KKS:
+    return kks_Rz(c, R, Z, 0);
   case PT_FLATPOWER: {
     double alpha = c->p[1], q2 = c->p[2], core2 = c->p[3], m2;
     if (alpha == 0.) return -amp * R / (R * R + Z * Z / q2 + core2);
@@ -470,6 +549,8 @@ static double comp_zforce(ocomp *c, double R, double Z, double phi)
   if (is_new_spherical(c->type)) return sph_force3(c, R, Z, Z);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_KKS:
+    return kks_Rz(c, R, Z, 1);
   case PT_FLATPOWER: {
     double alpha = c->p[1], q2 = c->p[2], core2 = c->p[3], m2;
     if (alpha == 0.) return -amp * Z / q2 / (R * R + Z * Z / q2 + core2);
@@ -534,6 +615,8 @@ static double comp_hess(const ocomp *c, int which, double R, double Z, double ph
   if (is_new_spherical(c->type)) return sph_hess3(c, which, R, Z);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_KKS:
+    return which > 2 ? 0. : kks_hess(c, R, Z, which);
   case PT_FLATPOWER: {
     double alpha = c->p[1], q2 = c->p[2], core2 = c->p[3], denom, m2;
     if (which > 2) return 0.;
@@ -655,6 +738,13 @@ static double comp_planarRforce(const ocomp *c, double R, double phi)
   if (is_new_spherical(c->type)) return sph_planarRforce(c, R);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_KKS: { /* KuzminKutuzovStaeckelPotentialPlanarRforce */
+    double ac = c->p[1], Delta = c->p[2];
+    double gamma = Delta * Delta / (1. - ac * ac), alpha = gamma - Delta * Delta;
+    double l = R * R - alpha, n = -gamma, dldR = 2. * R;
+    double dVdl = 0.5 / sqrt(l) / pow(sqrt(l) + sqrt(n), 2.);
+    return -amp * dldR * dVdl;
+  }
   case PT_FLATPOWER: {
     double alpha = c->p[1], core2 = c->p[2], m2;
     if (alpha == 0.) return -amp * R / (R * R + core2);
@@ -702,6 +792,15 @@ static double comp_planarhess(const ocomp *c, int which, double R, double phi)
   if (is_new_spherical(c->type)) return which ? 0. : sph_planarR2deriv(c, R);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_KKS: { /* KuzminKutuzovStaeckelPotentialPlanarR2deriv */
+    if (which) return 0.;
+    double ac = c->p[1], Delta = c->p[2];
+    double gamma = Delta * Delta / (1. - ac * ac), alpha = gamma - Delta * Delta;
+    double l = R * R - alpha, n = -gamma, dldR = 2. * R, d2ldR2 = 2.;
+    double dVdl = 0.5 / sqrt(l) / pow(sqrt(l) + sqrt(n), 2.);
+    double d2Vdl2 = (-3. * sqrt(l) - sqrt(n)) / (4. * pow(l, 1.5) * pow(sqrt(l) + sqrt(n), 3.));
+    return amp * (d2ldR2 * dVdl + dldR * dldR * d2Vdl2);
+  }
   case PT_FLATPOWER: {
     double alpha = c->p[1], core2 = c->p[2], m2;
     if (which) return 0.;
@@ -754,6 +853,15 @@ static double comp_eval(const ocomp *c, double R, double Z, double phi)
   if (is_new_spherical(c->type)) return sph_eval(c, R, Z);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_KKS: { /* KuzminKutuzovStaeckelPotentialEval */
+    double ac = c->p[1], Delta = c->p[2];
+    double gamma = Delta * Delta / (1. - ac * ac), alpha = gamma - Delta * Delta;
+    double term = R * R + Z * Z - alpha - gamma;
+    double discr = pow(R * R + Z * Z - Delta * Delta, 2.) + (4. * Delta * Delta * R * R);
+    double l = 0.5 * (term + sqrt(discr)), n = 0.5 * (term - sqrt(discr));
+    n = ((n > 0.) ? n : 0.);
+    return -amp / (sqrt(l) + sqrt(n));
+  }
   case PT_FLATPOWER: {
     double alpha = c->p[1], q2 = c->p[2], core2 = c->p[3];
     if (alpha == 0.) return 0.5 * amp * log(R * R + Z * Z / q2 + core2);

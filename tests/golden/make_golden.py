@@ -115,6 +115,7 @@ def main():
         # axisymmetric (the same tests)
         "flatpower": [gp.FlattenedPowerPotential(amp=1.1, alpha=0.5, q=0.8, core=0.3)],
         "flatlog": [gp.FlattenedPowerPotential(amp=0.9, alpha=0.0, q=0.7, core=0.2)],
+        "kks": [gp.KuzminKutuzovStaeckelPotential(amp=1.0, ac=5.0, Delta=0.8)],
     }
     pots.update(sph)
     for name, p in pots.items():

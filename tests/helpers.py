@@ -103,10 +103,11 @@ def differentiation_workload(n, seed=3):
     return np.ascontiguousarray(w0), np.ascontiguousarray(tgt)
 
 
-# the spherical (and the axisymmetric FlattenedPower) potentials added
-# behind the component template (golden-vector names)
-SPHERICAL = ["power", "kepler", "jaffe", "isochrone", "plummer", "pseudoiso", "burkert",
-             "dehnencore", "dehnen", "homsphere", "null", "einasto", "flatpower", "flatlog"]
+# the spherical and axisymmetric (FlattenedPower, KuzminKutuzovStaeckel)
+# potentials added behind the component template (golden-vector names)
+ADDED_POTS = ["power", "kepler", "jaffe", "isochrone", "plummer", "pseudoiso", "burkert",
+             "dehnencore", "dehnen", "homsphere", "null", "einasto", "flatpower", "flatlog",
+              "kks"]
 
 
 def golden_pot(golden, name, planar=False):

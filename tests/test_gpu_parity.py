@@ -10,7 +10,7 @@ import ctypes
 
 import numpy as np
 import pytest
-from helpers import SPHERICAL, cyl_diff, golden_pot, sos_diff, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
+from helpers import ADDED_POTS, cyl_diff, golden_pot, sos_diff, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
 
 import galpy_b200 as gb
 from galpy_b200 import _lib
@@ -183,7 +183,7 @@ def test_generic_potentials_and_fixed_dt(oracle, golden, method):
     assert not err.any() and 0 < d < 1e-4, d
 
 
-@pytest.mark.parametrize("name", SPHERICAL)
+@pytest.mark.parametrize("name", ADDED_POTS)
 def test_spherical_potentials(oracle, golden, name):
     """Orbits in each spherical potential: the reference's own C (golden
     vectors: dop853 3D, symplec4 planar, dop853 variational) and the oracle
@@ -500,7 +500,7 @@ def test_energy_kernel_vs_oracle(oracle, mw14):
 
 
 @pytest.mark.parametrize("name", ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"]
-                         + SPHERICAL)
+                         + ADDED_POTS)
 @pytest.mark.parametrize("planar", [False, True])
 def test_device_accelerations(golden, harness, name, planar):
     """The kernels' force code on the device (branch-free FP64 helpers:

@@ -4,10 +4,10 @@ against the CPU oracle.  This checks the kernel logic on every CPU-only run;
 tests/test_gpu_parity.py checks the compiled kernels on the GPU."""
 import numpy as np
 import pytest
-from helpers import SPHERICAL, cyl_diff, cyl_to_sos, golden_pot, polar_to_sos, sos_diff, sos_to_cyl, sos_to_polar, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
+from helpers import ADDED_POTS, cyl_diff, cyl_to_sos, golden_pot, polar_to_sos, sos_diff, sos_to_cyl, sos_to_polar, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
 
 METHODS = ["leapfrog", "rk4", "rk6", "symplec4", "symplec6", "dopr54", "dop853"]
-POTS = ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"] + SPHERICAL
+POTS = ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"] + ADDED_POTS
 
 
 @pytest.mark.parametrize("alpha", [0.5, 1.2, 1.8, 2.6])
@@ -97,7 +97,7 @@ def test_orbits_vs_oracle(harness, oracle, mw14, mw14_planar, method, planar):
     assert cyl_diff(ref, rect_to_cyl(out)).max() < 1e-11
 
 
-@pytest.mark.parametrize("name", SPHERICAL)
+@pytest.mark.parametrize("name", ADDED_POTS)
 def test_spherical_potential_orbits(harness, oracle, golden, name):
     """Orbits in each spherical potential: the same step sequence as the
     oracle and agreement to the orbits' conditioning, 3D, planar and

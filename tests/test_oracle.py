@@ -9,7 +9,7 @@
 """
 import numpy as np
 import pytest
-from helpers import SPHERICAL, cyl_to_rect, golden_pot, seeded_ics
+from helpers import ADDED_POTS, cyl_to_rect, golden_pot, seeded_ics
 
 METHODS = ["leapfrog", "rk4", "rk6", "symplec4", "symplec6", "dopr54", "dop853"]
 
@@ -109,7 +109,7 @@ def test_incomplete_gamma_vs_scipy(oracle):
 
 
 @pytest.mark.parametrize("name", ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"]
-                         + SPHERICAL)
+                         + ADDED_POTS)
 def test_oracle_forces_vs_galpy_python(oracle, golden, name):
     """C-side formulas restated in the oracle agree with galpy's Python
     potentials (different code, same mathematics)."""
@@ -127,7 +127,7 @@ def test_oracle_forces_vs_galpy_python(oracle, golden, name):
     assert err.max() < 1e-11, err.max(0)
 
 
-@pytest.mark.parametrize("name", SPHERICAL)
+@pytest.mark.parametrize("name", ADDED_POTS)
 def test_oracle_spherical_potentials(oracle, golden, name):
     """The reference's own C in each spherical potential: golden vectors
     (dop853 3D, symplec4 planar, dop853 variational) and, where the reference
