@@ -27,7 +27,7 @@ inline int galpy_nargs(int type, int planar)
     case T_PSWC: return planar ? 3 : 5;
     case T_POWER: case T_JAFFE: case T_ISOCHRONE: case T_PLUMMER: case T_PSEUDOISO:
     case T_BURKERT: case T_DEHNENCORE: return 2;
-    case T_DEHNEN: case T_HOMSPHERE: case T_EINASTO: return 3;
+    case T_DEHNEN: case T_HOMSPHERE: case T_EINASTO: case T_EXPTRUNCNFW: return 3;
     case T_NULL: return 0;
     case T_FLATPOWER: return planar ? 3 : 4;
     case T_KKS: return 3;
@@ -273,6 +273,23 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
         break;
       case T_NULL:
         break;
+      case T_EXPTRUNCNFW: {  // (amp, a, rc); the reference's series coefficients
+        const double a = p[1], rc = p[2];
+        if (!(a > 0.0) || !(rc > 0.0)) return -1;
+        const double alpha = a / rc, ea = exp(alpha) * (1.0 + alpha);
+        c.c[1] = a;
+        c.c[2] = 1.0 / rc;
+        c.c[3] = ea;
+        c.c[4] = ea * expint_E1(alpha);
+        c.c[5] = 1e-3 * (a < rc ? a : rc);
+        c.c[6] = 0.5;
+        c.c[7] = -(1.0 / rc + 2.0 / a) / 3.0;
+        c.c[8] = (0.5 / (rc * rc) + 2.0 / (rc * a) + 3.0 / (a * a)) / 4.0;
+        c.c[9] = -(1.0 / (6.0 * rc * rc * rc) + 1.0 / (rc * rc * a) + 3.0 / (rc * a * a) +
+                   4.0 / (a * a * a)) / 5.0;
+        c.c[10] = exp(alpha) / rc;
+        break;
+      }
       case T_EINASTO: {  // (amp, h, n)
         const double h = p[1], n = p[2];
         if (!(h > 0.0) || !(n > 0.0)) return -1;

@@ -48,7 +48,7 @@ enum : int { T_LOGHALO = 0, T_MN = 5, T_HERNQUIST = 8, T_NFW = 9, T_PSWC = 15 };
 // HomogeneousSphere, Null (no force)
 enum : int { T_POWER = 7, T_JAFFE = 10, T_ISOCHRONE = 14, T_PLUMMER = 17, T_PSEUDOISO = 18,
              T_BURKERT = 20, T_DEHNENCORE = 33, T_DEHNEN = 34, T_HOMSPHERE = 35, T_NULL = 40,
-             T_EINASTO = 41 };
+             T_EINASTO = 41, T_EXPTRUNCNFW = 46 };
 // axisymmetric FlattenedPowerPotential (FlattenedPowerPotential.c) and
 // KuzminKutuzovStaeckelPotential (KuzminKutuzovStaeckelPotential.c)
 enum : int { T_FLATPOWER = 12, T_KKS = 16 };
@@ -74,6 +74,9 @@ constexpr int kBinSub = 8;    // sub-intervals of a binade [1, 2) in the binade 
 //   HomogeneousSphere: c1 R^2, c2 R^3    Null: -
 //   Einasto: c1 h, c2 1/n, c3 3n, c4 lgamma(3n), c5 4 pi n h^3 Gamma(3n),
 //              c6 4 pi n Gamma(3n), c7 2n, c8 lgamma(2n), c9 4 pi h^2 n Gamma(2n)
+//   ExpTruncNFW: c1 a, c2 1/rc, c3 e^alpha (1 + alpha), c4 c3 E1(alpha),
+//              c5 small-r threshold 1e-3 min(a, rc), c6..c9 its series
+//              coefficients, c10 e^alpha / rc (alpha = a / rc)
 //   FlattenedPower: c1 1/q^2 (1 in the plane), c2 core^2, c3 -alpha/2 - 1,
 //              c4 alpha, c5 alpha + 2
 //   KuzminKutuzovStaeckel: c1 Delta^2, c2 alpha + gamma with
@@ -387,6 +390,47 @@ GPC_HD inline double inc_gamma_P(double a, double x, double lga)
   return 1.0 - exp(lpref) * h;
 }
 
+// Exponential integral E1(x), x > 0 (ExpTruncNFW): the power series
+// -gamma_E - ln x - sum_k (-x)^k / (k k!) for x <= 1 (A&S 5.1.11), the
+// continued fraction e^-x / (x + 1 - 1 / (x + 3 - 4 / (x + 5 - ...))) for
+// x > 1 (A&S 5.1.22, modified Lentz).
+GPC_HD inline double expint_E1(double x)
+{
+  if (x <= 1.0) {
+    double term = 1.0, sum = 0.0;
+    for (int k = 1; k < 200; k++) {
+      term *= -x / k;
+      const double d = term / k;
+      sum += d;
+      if (fabs(d) < 1e-17 * fabs(sum)) break;
+    }
+    return -0.57721566490153286061 - log(x) - sum;
+  }
+  double b = x + 1.0, c = 1e300, d = 1.0 / b, h = d;
+  for (int i = 1; i < 1000; i++) {
+    const double an = -(double)i * i;
+    b += 2.0;
+    d = 1.0 / (an * d + b);
+    c = b + an / c;
+    const double del = c * d;
+    h *= del;
+    if (fabs(del - 1.0) < 1e-16) break;
+  }
+  return h * exp(-x);
+}
+
+// ExpTruncNFW's enclosed-mass function F(r) (ExpTruncNFWPotential.c): a
+// series below the small-r threshold, else e^alpha (1 + alpha) (E1(alpha) -
+// E1(beta)) - 1 + a e^(-r/rc) / (a + r), beta = (a + r) / rc.
+// S: the component's scalar accessor (sc[j] = c[j]).
+template <class S>
+GPC_HD inline double exptruncnfw_F(const S& sc, double r)
+{
+  const double a = sc[1], irc = sc[2];
+  if (r < sc[5]) return (r * r / (a * a)) * (sc[6] + r * (sc[7] + r * (sc[8] + r * sc[9])));
+  return sc[4] - sc[3] * expint_E1((a + r) * irc) - 1.0 + a * exp(-r * irc) / (a + r);
+}
+
 // ------------------------------------------------------------- forces ---
 // Add one component's contribution to the radial factors: the acceleration
 // is a = (x gR, y (gR + gyx), z gz).  TYPE < 0: read the type at run time.
@@ -472,6 +516,10 @@ GPC_HD GPC_FI T sph_force_factor(int type, const S& sc, T r2)
     case T_HOMSPHERE: {  // Phi' = 2 amp r inside R, 2 amp R^3 / r^2 outside
       const T ir = Num<T>::rsq(r2);
       return r2 < T(sc[1]) ? T(-2) * amp : T(-2) * amp * T(sc[2]) * ir * ir * ir;
+    }
+    case T_EXPTRUNCNFW: {  // Phi'/r = amp F(r) / r^3 (in float64)
+      const double r = sqrt((double)r2);
+      return T(-(double)amp * exptruncnfw_F(sc, r) / (r * r * r));
     }
     case T_EINASTO: {  // Phi'/r = amp 4 pi n h^3 gamma(3n, (r/h)^(1/n)) / r^3 (in float64)
       const double r = sqrt((double)r2), x = pow(r / sc[1], sc[2]);
@@ -734,6 +782,12 @@ GPC_HD inline void sph_derivs(const GpComp* __restrict__ cp, int type, double am
         d2 = -2.0 * dpr;
       }
       break;
+    case T_EXPTRUNCNFW: {  // Phi'' = amp (e^(-r/rc) / (r (a + r)^2) - 2 F / r^3)
+      const double F = exptruncnfw_F(ScalarsGlobal{cp}, r), ar = c1 + r;
+      dpr = amp * F * ir * ir * ir;
+      d2 = amp * (exp(-r * ldg(&cp->c[2])) * ir / (ar * ar) - 2.0 * F * ir * ir * ir);
+      break;
+    }
     case T_EINASTO: {  // Phi'' = amp (4 pi e^-x - 2 * 4 pi n Gamma(3n) P / s^3)
       const double x = pow(r / c1, ldg(&cp->c[2]));
       const double P = inc_gamma_P(ldg(&cp->c[3]), x, ldg(&cp->c[4]));
@@ -930,6 +984,11 @@ GPC_HD inline double sph_value(const GpComp* __restrict__ cp, int type, double a
     }
     case T_HOMSPHERE:
       return r2 < c1 ? amp * (r2 - 3.0 * c1) : -2.0 * amp * ldg(&cp->c[2]) / r;
+    case T_EXPTRUNCNFW: {  // -amp (F / r + e^(-r/rc) / (a + r) - e^alpha E1(beta) / rc)
+      const double irc = ldg(&cp->c[2]);
+      const double G = exp(-r * irc) / (c1 + r) - ldg(&cp->c[10]) * expint_E1((c1 + r) * irc);
+      return -amp * (exptruncnfw_F(ScalarsGlobal{cp}, r) / r + G);
+    }
     case T_EINASTO: {  // -amp 4 pi h^2 n [Gamma(3n) P(3n, x) / s + Gamma(2n) Q(2n, x)]
       const double s = r / c1, x = pow(s, ldg(&cp->c[2]));
       const double P3 = inc_gamma_P(ldg(&cp->c[3]), x, ldg(&cp->c[4]));

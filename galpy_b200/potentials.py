@@ -7,7 +7,7 @@ The engine integrates in the potentials galpy hands to C as pot_type codes
 (Jaffe), 14 (Isochrone),
 17 (Plummer), 18 (PseudoIsothermal), 20 (Burkert), 33
 (DehnenCoreSpherical), 34 (DehnenSpherical), 35 (HomogeneousSphere), 40
-(Null) and 41 (Einasto) -- the parsing is
+(Null), 41 (Einasto) and 46 (ExpTruncNFW) -- the parsing is
 galpy/orbit/integrateFullOrbit.py:43-614 (3D) and
 galpy/orbit/integratePlanarOrbit.py:33-663 (planar).
 
@@ -26,8 +26,8 @@ import numpy as np
 T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC = 0, 5, 8, 9, 15
 # spherical: PowerSpherical (and Kepler), Jaffe, Isochrone, Plummer,
 # PseudoIsothermal, Burkert, DehnenCoreSpherical, DehnenSpherical,
-# HomogeneousSphere, Null, Einasto
-SPHERICAL_TYPES = (7, 10, 14, 17, 18, 20, 33, 34, 35, 40, 41)
+# HomogeneousSphere, Null, Einasto, ExpTruncNFW
+SPHERICAL_TYPES = (7, 10, 14, 17, 18, 20, 33, 34, 35, 40, 41, 46)
 T_FLATPOWER, T_KKS = 12, 16
 SUPPORTED_TYPES = (T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC, T_FLATPOWER,
                    T_KKS) + SPHERICAL_TYPES

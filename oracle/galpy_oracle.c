@@ -12,7 +12,8 @@
  *            LogarithmicHaloPotential.c:5-297, and the spherical
  *            PowerSpherical, Jaffe, Isochrone, Plummer, PseudoIsothermal,
  *            Burkert, DehnenCore, Dehnen, HomogeneousSphere potentials and
- *            ZeroForce, Einasto (through SphericalPotential.c),
+ *            ZeroForce, Einasto and ExpTruncNFW (through
+ *            SphericalPotential.c),
  *            FlattenedPowerPotential.c, KuzminKutuzovStaeckelPotential.c
  *            (potential_c_ext/)
  *   sums     galpy_potentials.c:120-354 (sum over components, in order)
@@ -53,6 +54,7 @@
 
 double oracle_gamma_inc_P(double a, double x);
 double oracle_gamma_inc_Q(double a, double x);
+double oracle_expint_E1(double x);
 
 /* ------------------------------------------------------------------ */
 /* potentials                                                          */
@@ -70,7 +72,8 @@ enum {
   PT_DEHNEN = 34,     /* DehnenSphericalPotential (DehnenPotential.c) */
   PT_HOMSPHERE = 35,  /* HomogeneousSpherePotential */
   PT_NULL = 40,       /* NullPotential (ZeroForce) */
-  PT_EINASTO = 41     /* EinastoPotential (through SphericalPotential.c) */
+  PT_EINASTO = 41,    /* EinastoPotential (through SphericalPotential.c) */
+  PT_EXPTRUNCNFW = 46 /* ExpTruncNFWPotential (through SphericalPotential.c) */
 };
 /* axisymmetric: FlattenedPowerPotential (FlattenedPowerPotential.c); args
    (amp, alpha, q^2, core^2) in 3D, (amp, alpha, core^2) in the plane */
@@ -103,7 +106,7 @@ static int nargs_of(int type, int planar)
   case PT_PSWC: return planar ? 3 : 5;
   case PT_POWER: case PT_JAFFE: case PT_ISOCHRONE: case PT_PLUMMER: case PT_PSEUDOISO:
   case PT_BURKERT: case PT_DEHNENCORE: return 2;
-  case PT_DEHNEN: case PT_HOMSPHERE: case PT_EINASTO: return 3;
+  case PT_DEHNEN: case PT_HOMSPHERE: case PT_EINASTO: case PT_EXPTRUNCNFW: return 3;
   case PT_NULL: return 0;
   case PT_FLATPOWER: return planar ? 3 : 4;
   case PT_KKS: return 3;
@@ -116,10 +119,45 @@ static int is_new_spherical(int type)
   switch (type) {
   case PT_POWER: case PT_JAFFE: case PT_ISOCHRONE: case PT_PLUMMER: case PT_PSEUDOISO:
   case PT_BURKERT: case PT_DEHNENCORE: case PT_DEHNEN: case PT_HOMSPHERE: case PT_NULL:
-  case PT_EINASTO:
+  case PT_EINASTO: case PT_EXPTRUNCNFW:
     return 1;
   }
   return 0;
+}
+
+/* ExpTruncNFWPotential.c, args (amp, a, rc): the enclosed-mass function F
+   (a small-r series below 1e-3 min(a, rc)), G, and the radial functions;
+   GSL's E1 restated in incgamma.c; SphericalPotential.c applies amp */
+static double etnfw_F(double r, double a, double rc)
+{
+  double small_r_thresh = 1e-3 * (a < rc ? a : rc);
+  if (r < small_r_thresh) {
+    double c2 = 0.5;
+    double c3 = -(1.0 / rc + 2.0 / a) / 3.0;
+    double c4 = (0.5 / (rc * rc) + 2.0 / (rc * a) + 3.0 / (a * a)) / 4.0;
+    double c5 = -(1.0 / (6.0 * rc * rc * rc) + 1.0 / (rc * rc * a) + 3.0 / (rc * a * a) +
+                  4.0 / (a * a * a)) / 5.0;
+    return (r * r / (a * a)) * (c2 + r * (c3 + r * (c4 + r * c5)));
+  }
+  double alpha = a / rc, beta = (a + r) / rc;
+  return (exp(alpha) * (1.0 + alpha) * (oracle_expint_E1(alpha) - oracle_expint_E1(beta)) -
+          1.0 + a * exp(-r / rc) / (a + r));
+}
+static double etnfw_G(double r, double a, double rc)
+{
+  double alpha = a / rc, beta = (a + r) / rc;
+  return exp(-r / rc) / (a + r) - exp(alpha) * oracle_expint_E1(beta) / rc;
+}
+static double etnfw_rforce(const ocomp *c, double r) { return -etnfw_F(r, c->p[1], c->p[2]) / (r * r); }
+static double etnfw_r2deriv(const ocomp *c, double r)
+{
+  double a = c->p[1], rc = c->p[2];
+  double rdens = exp(-r / rc) / (4.0 * M_PI * a * a * r * pow(1.0 + r / a, 2));
+  return 4.0 * M_PI * rdens - 2.0 * etnfw_F(r, a, rc) / (r * r * r);
+}
+static double etnfw_revaluate(const ocomp *c, double r)
+{
+  return -(etnfw_F(r, c->p[1], c->p[2]) / r + etnfw_G(r, c->p[1], c->p[2]));
 }
 
 /* its prolate spheroidal coordinates (l, n) and the derivatives of
@@ -266,6 +304,10 @@ static double sph_force3(const ocomp *c, double R, double Z, double X)
     double r = sqrt(R * R + Z * Z);
     return amp * einasto_rforce(c, r) * X / r;
   }
+  case PT_EXPTRUNCNFW: {
+    double r = sqrt(R * R + Z * Z);
+    return amp * etnfw_rforce(c, r) * X / r;
+  }
   }
   return 0.;
 }
@@ -312,6 +354,8 @@ static double sph_planarRforce(const ocomp *c, double R)
   }
   case PT_EINASTO:
     return amp * einasto_rforce(c, R);
+  case PT_EXPTRUNCNFW:
+    return amp * etnfw_rforce(c, R);
   }
   return 0.;
 }
@@ -363,6 +407,8 @@ static double sph_planarR2deriv(const ocomp *c, double R)
   }
   case PT_EINASTO:
     return amp * einasto_r2deriv(c, R);
+  case PT_EXPTRUNCNFW:
+    return amp * etnfw_r2deriv(c, R);
   }
   return 0.;
 }
@@ -444,13 +490,15 @@ static double sph_eval(const ocomp *c, double R, double Z)
   }
   case PT_EINASTO:
     return amp * einasto_revaluate(c, sqrt(R * R + Z * Z));
+  case PT_EXPTRUNCNFW:
+    return amp * etnfw_revaluate(c, sqrt(R * R + Z * Z));
   }
   return 0.;
 }
 
 /* Decode galpy's (pot_type, pot_args) stream (integrateFullOrbit.c:69-1040,
    integratePlanarOrbit.c:55-742 restricted to types 0/5/7/8/9/10/12/14/15/
-   16/17/18/20/33/34/35/40/41).
+   16/17/18/20/33/34/35/40/41/46).
    Returns 0, or -1 for an unsupported type. */
 static int opot_decode(opot *P, int npot, const int *type, const double *args, int planar)
 {
@@ -2108,3 +2156,4 @@ EXPORT int oracle_potential(int n, const double *R, const double *z, const doubl
 }
 
 EXPORT double oracle_gammainc_P(double a, double x) { return oracle_gamma_inc_P(a, x); }
+EXPORT double oracle_expint(double x) { return oracle_expint_E1(x); }

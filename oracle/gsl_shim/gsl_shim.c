@@ -1,22 +1,25 @@
 /* oracle/gsl_shim/gsl_shim.c -- TEST INFRASTRUCTURE ONLY.
    Definitions behind the stand-in GSL headers, linked only into oracle/_ref
    (the reference's own C sources built by oracle/Makefile).  The gamma
-   functions are computed by oracle/incgamma.c (published series and continued
-   fraction) and C99 tgamma; the spline entry points exist only to satisfy the
+   functions and E1 are computed by oracle/incgamma.c (published series and
+   continued fractions) and C99 tgamma; the spline entry points exist only to satisfy the
    linker and abort if reached. */
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
+#include "gsl/gsl_sf_expint.h"
 #include "gsl/gsl_sf_gamma.h"
 #include "gsl/gsl_spline.h"
 
 double oracle_gamma_inc_P(double a, double x);
 double oracle_gamma_inc_Q(double a, double x);
+double oracle_expint_E1(double x);
 
 double gsl_sf_gamma(double x) { return tgamma(x); }
 double gsl_sf_gamma_inc_P(double a, double x) { return oracle_gamma_inc_P(a, x); }
 double gsl_sf_gamma_inc(double a, double x) { return tgamma(a) * oracle_gamma_inc_Q(a, x); }
 double gsl_sf_gamma_inc_Q(double a, double x) { return oracle_gamma_inc_Q(a, x); }
+double gsl_sf_expint_E1(double x) { return oracle_expint_E1(x); }
 
 static void shim_unreachable(const char *what)
 {

@@ -81,6 +81,8 @@ def port():
                                       _ip, _dp, _dp]
         lib.oracle_potential.restype = ctypes.c_int
         lib.oracle_potential.argtypes = [ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _ip, _dp, _dp]
+        lib.oracle_expint.restype = ctypes.c_double
+        lib.oracle_expint.argtypes = [ctypes.c_double]
         lib.oracle_gammainc_P.restype = ctypes.c_double
         lib.oracle_gammainc_P.argtypes = [ctypes.c_double, ctypes.c_double]
         _port = lib
@@ -300,6 +302,10 @@ def potential(R, z, phi, pot_type, pot_args):
 
 def gammainc_P(a, x):
     return port().oracle_gammainc_P(float(a), float(x))
+
+
+def expint_E1(x):
+    return port().oracle_expint(float(x))
 
 
 def energy_cyl(res, pot_type, pot_args):

@@ -12,7 +12,8 @@ Two kinds of vectors are written to golden.npz:
   triaxial) / NFW / MiyamotoNagai / PowerSphericalwCutoff and of the
   spherical PowerSpherical, Kepler, Jaffe, Isochrone, Plummer,
   PseudoIsothermal, Burkert, DehnenCoreSpherical, DehnenSpherical,
-  HomogeneousSphere, Null and Einasto potentials at fixed points, plus
+  HomogeneousSphere, Null, Einasto and ExpTruncNFW potentials at fixed
+  points, plus
   galpy's pure-Python DOP853 orbits (galpy/util/leung_dop853.py) in
   MWPotential2014;
 * from the reference's own C integrators (integrateFullOrbit /
@@ -112,6 +113,7 @@ def main():
         # constant amp, which C never evaluates
         "null": [gp.NullPotential()],
         "einasto": [gp.EinastoPotential(amp=1.5, h=1.2, n=1.8)],
+        "exptruncnfw": [gp.ExpTruncNFWPotential(amp=2.0, a=1.5, rc=6.0)],
         # axisymmetric (the same tests)
         "flatpower": [gp.FlattenedPowerPotential(amp=1.1, alpha=0.5, q=0.8, core=0.3)],
         "flatlog": [gp.FlattenedPowerPotential(amp=0.9, alpha=0.0, q=0.7, core=0.2)],

@@ -106,8 +106,8 @@ def differentiation_workload(n, seed=3):
 # the spherical and axisymmetric (FlattenedPower, KuzminKutuzovStaeckel)
 # potentials added behind the component template (golden-vector names)
 ADDED_POTS = ["power", "kepler", "jaffe", "isochrone", "plummer", "pseudoiso", "burkert",
-             "dehnencore", "dehnen", "homsphere", "null", "einasto", "flatpower", "flatlog",
-              "kks"]
+             "dehnencore", "dehnen", "homsphere", "null", "einasto", "exptruncnfw",
+              "flatpower", "flatlog", "kks"]
 
 
 def golden_pot(golden, name, planar=False):

@@ -541,11 +541,12 @@ def test_device_accelerations(golden, harness, name, planar):
                 continue
             scale = np.linalg.norm(ref_, axis=1)
             err = np.abs(got - ref_).max(axis=1) / scale
-            if name in ("pseudoiso", "burkert"):
-                # both forces cancel terms at r << a (1 - atan(x)/x, and
-                # 2 atan x - 2 ln(1+x) - ln(1+x^2) ~ -4x^3/3), in the
-                # reference's formulas as here: compare where x > 0.1 (0.5
-                # in single precision)
+            if name in ("pseudoiso", "burkert", "exptruncnfw"):
+                # these forces cancel terms at r << a (1 - atan(x)/x;
+                # 2 atan x - 2 ln(1+x) - ln(1+x^2) ~ -4x^3/3; ExpTruncNFW's
+                # F(r) ~ r^2 / (2 a^2) from O(1) terms above its series
+                # threshold), in the reference's formulas as here: compare
+                # where x = r/a > 0.1 (0.5 in single precision)
                 xr = np.sqrt(x**2 + y**2 + (0 if planar else z**2)) / float(pa[1])
                 err = err[xr > (0.1 if prec == "fp64" else 0.5)]
             assert err.max() < tol, (sig, prec, err.max())

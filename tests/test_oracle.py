@@ -108,6 +108,15 @@ def test_incomplete_gamma_vs_scipy(oracle):
     assert worst < 5e-14, worst
 
 
+def test_exponential_integral_vs_scipy(oracle):
+    """E1 for ExpTruncNFW (the reference calls GSL's gsl_sf_expint_E1)."""
+    from scipy.special import exp1
+
+    xs = np.concatenate([np.geomspace(1e-8, 1.0, 300), np.geomspace(1.0, 600.0, 300)])
+    worst = max(abs(oracle.expint_E1(x) - exp1(x)) / exp1(x) for x in xs)
+    assert worst < 2e-14, worst
+
+
 @pytest.mark.parametrize("name", ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"]
                          + ADDED_POTS)
 def test_oracle_forces_vs_galpy_python(oracle, golden, name):
