@@ -28,8 +28,8 @@
 //    This replaces the reference's GSL series / continued fraction
 //    (PowerSphericalPotentialwCutoff.c:9-11), whose dependent divisions made
 //    it the latency bottleneck of every force evaluation.
-//  * A component list is walked at run time (any combination of the five
-//    types), or fixed at compile time (FixedPot) so that the components of
+//  * A component list is walked at run time (any combination of the
+//    supported types), or fixed at compile time (FixedPot) so that the components of
 //    a known potential such as MWPotential2014 are inlined side by side and
 //    their latencies overlap.
 //  * The Cartesian tidal tensor K = -grad grad Phi (variational runs) is
