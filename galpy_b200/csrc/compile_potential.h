@@ -31,6 +31,7 @@ inline int galpy_nargs(int type, int planar)
     case T_NULL: return 0;
     case T_FLATPOWER: return planar ? 3 : 4;
     case T_KKS: return 3;
+    case T_HENONHEILES: return planar ? 1 : -1;  // (amp); a planarPotential only
     default: return -1;
   }
 }

@@ -7,8 +7,8 @@
 // (10), Isochrone (14), Plummer (17), PseudoIsothermal (18), Burkert (20),
 // DehnenCoreSpherical (33), DehnenSpherical (34), HomogeneousSphere (35) and
 // Null (40) and Einasto (41) potentials, and the axisymmetric FlattenedPower
-// (12) and KuzminKutuzovStaeckel (16).  Reference
-// formulas:
+// (12) and KuzminKutuzovStaeckel (16), and the planar HenonHeiles (29).
+// Reference formulas:
 // galpy/potential/potential_c_ext/<name>.c.
 //
 // Design (not a translation of the reference's cylindrical route):
@@ -52,6 +52,8 @@ enum : int { T_POWER = 7, T_JAFFE = 10, T_ISOCHRONE = 14, T_PLUMMER = 17, T_PSEU
 // axisymmetric FlattenedPowerPotential (FlattenedPowerPotential.c) and
 // KuzminKutuzovStaeckelPotential (KuzminKutuzovStaeckelPotential.c)
 enum : int { T_FLATPOWER = 12, T_KKS = 16 };
+// planar, non-axisymmetric HenonHeilesPotential (HenonHeilesPotential.c)
+enum : int { T_HENONHEILES = 29 };
 
 constexpr int kMaxComp = 16;  // components per potential group
 constexpr int kChebN = 32;    // Chebyshev intervals of gamma*(a, u) on [0, U]
@@ -433,7 +435,9 @@ GPC_HD inline double exptruncnfw_F(const S& sc, double r)
 
 // ------------------------------------------------------------- forces ---
 // Add one component's contribution to the radial factors: the acceleration
-// is a = (x gR, y (gR + gyx), z gz).  TYPE < 0: read the type at run time.
+// is a = (x gR, y (gR + gyx) + ay0, z gz).  ay0 only takes the terms of
+// a_y that are not proportional to y (Henon-Heiles' -amp x^2).  TYPE < 0:
+// read the type at run time.
 // Scalar parameters of a component: from the compiled record in global
 // memory (read-only path), or from a copy passed as a kernel parameter
 // (constant bank: no load instruction when the index is a compile-time
@@ -533,7 +537,7 @@ GPC_HD GPC_FI T sph_force_factor(int type, const S& sc, T r2)
 
 template <typename T, bool PLANAR, int TYPE, class S>
 GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T y, T z2, T R2,
-                              T r2, T& gR, T& gz, T& gyx)
+                              T r2, T& gR, T& gz, T& gyx, T& ay0)
 {
   const int type = TYPE >= 0 ? TYPE : ldg(&cp->type);
   const T amp = T(sc[0]);
@@ -631,6 +635,14 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
       if (!PLANAR) gz += g * iq2;
       break;
     }
+    case T_HENONHEILES: {
+      // Phi = amp ((x^2 + y^2)/2 + x^2 y - y^3/3) (planar only):
+      // a = -amp (x (1 + 2y), y (1 - y) + x^2)
+      gR -= amp * (T(1) + T(2) * y);
+      gyx += T(3) * amp * y;
+      ay0 -= amp * x * x;
+      break;
+    }
     default: {
       const T f = sph_force_factor<T>(type, sc, r2);
       gR += f;
@@ -643,12 +655,14 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
 // Run-time component list (any combination of the supported types).
 struct DynPot {
   static constexpr bool kDirectScalars = false;
+  static constexpr bool kAdditiveY = true;  // a component may add to ay0
   template <typename T, bool PLANAR>
   GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, const double* /*scal*/, int ncomp,
-                                T x, T y, T z2, T R2, T r2, T& gR, T& gz, T& gyx)
+                                T x, T y, T z2, T R2, T r2, T& gR, T& gz, T& gyx, T& ay0)
   {
     for (int k = 0; k < ncomp; k++)
-      comp_accel<T, PLANAR, -1>(comp + k, ScalarsGlobal{comp + k}, x, y, z2, R2, r2, gR, gz, gyx);
+      comp_accel<T, PLANAR, -1>(comp + k, ScalarsGlobal{comp + k}, x, y, z2, R2, r2, gR, gz, gyx,
+                                ay0);
   }
 };
 
@@ -659,19 +673,20 @@ constexpr int kScalarStride = 16;
 template <bool DIRECT, int... TYPES>
 struct FixedPot {
   static constexpr bool kDirectScalars = DIRECT;
+  static constexpr bool kAdditiveY = ((TYPES == T_HENONHEILES) || ...);
   template <typename T, bool PLANAR>
   GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, const double* scal, int /*ncomp*/,
-                                T x, T y, T z2, T R2, T r2, T& gR, T& gz, T& gyx)
+                                T x, T y, T z2, T R2, T r2, T& gR, T& gz, T& gyx, T& ay0)
   {
     int k = 0;
     if (DIRECT) {
       ((comp_accel<T, PLANAR, TYPES>(comp + k, ScalarsDirect{scal + kScalarStride * k}, x, y, z2,
-                                     R2, r2, gR, gz, gyx),
+                                     R2, r2, gR, gz, gyx, ay0),
         ++k),
        ...);
     } else {
       ((comp_accel<T, PLANAR, TYPES>(comp + k, ScalarsGlobal{comp + k}, x, y, z2, R2, r2, gR, gz,
-                                     gyx),
+                                     gyx, ay0),
         ++k),
        ...);
     }
@@ -692,10 +707,11 @@ GPC_HD GPC_FI void accel(const GpComp* __restrict__ comp, int ncomp, T x, T y, T
   const T R2 = x * x + y * y;
   const T z2 = PLANAR ? T(0) : z * z;
   const T r2 = R2 + z2;
-  T gR = T(0), gz = T(0), gyx = T(0);
-  POT::template sum<T, PLANAR>(comp, scal, ncomp, x, y, z2, R2, r2, gR, gz, gyx);
+  T gR = T(0), gz = T(0), gyx = T(0), ay0 = T(0);
+  POT::template sum<T, PLANAR>(comp, scal, ncomp, x, y, z2, R2, r2, gR, gz, gyx, ay0);
   ax = x * gR;
   ay = y * (gR + gyx);
+  if constexpr (POT::kAdditiveY) ay += ay0;  // compile-time lists without it skip the add
   if (!PLANAR) az = z * gz;
 }
 
@@ -807,7 +823,7 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
 {
   if (PLANAR) z = 0.0;
   const double R2 = x * x + y * y, z2 = z * z, r2 = R2 + z2;
-  double gR = 0.0, gz = 0.0, gyx = 0.0;
+  double gR = 0.0, gz = 0.0, gyx = 0.0, ay0 = 0.0;
 #pragma unroll
   for (int i = 0; i < 6; i++) K[i] = 0.0;
   for (int k = 0; k < ncomp; k++) {
@@ -939,6 +955,15 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
         K[5] += g * iq2 + h * uz * uz;
         break;
       }
+      case T_HENONHEILES: {  // planar only; K = -amp ((1 + 2y, 2x), (2x, 1 - 2y))
+        gR -= amp * (1.0 + 2.0 * y);
+        gyx += 3.0 * amp * y;
+        ay0 -= amp * x * x;
+        K[0] -= amp * (1.0 + 2.0 * y);
+        K[1] -= 2.0 * amp * x;
+        K[2] -= amp * (1.0 - 2.0 * y);
+        break;
+      }
       default: {
         double dpr, d2;  // Phi'/r, Phi''
         sph_derivs(cp, type, amp, r2, dpr, d2);
@@ -948,7 +973,7 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
     }
   }
   ax = x * gR;
-  ay = y * (gR + gyx);
+  ay = y * (gR + gyx) + ay0;
   az = PLANAR ? 0.0 : z * gz;
 }
 
@@ -1051,6 +1076,9 @@ GPC_HD inline double potential_value(const GpComp* __restrict__ comp, int ncomp,
         phi += alpha == 0.0 ? 0.5 * amp * log(m2) : -amp * pow(m2, -0.5 * alpha) / alpha;
         break;
       }
+      case T_HENONHEILES:  // amp (R^2/2 + R^3 sin(3 phi)/3)
+        phi += amp * (0.5 * R2 + x * x * y - y * y * y / 3.0);
+        break;
       default:
         phi += sph_value(cp, ldg(&cp->type), amp, r2);
         break;

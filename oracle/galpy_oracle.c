@@ -14,8 +14,8 @@
  *            Burkert, DehnenCore, Dehnen, HomogeneousSphere potentials and
  *            ZeroForce, Einasto and ExpTruncNFW (through
  *            SphericalPotential.c),
- *            FlattenedPowerPotential.c, KuzminKutuzovStaeckelPotential.c
- *            (potential_c_ext/)
+ *            FlattenedPowerPotential.c, KuzminKutuzovStaeckelPotential.c,
+ *            HenonHeilesPotential.c (planar) (potential_c_ext/)
  *   sums     galpy_potentials.c:120-354 (sum over components, in order)
  *   RHS      orbit_c_ext/integrateFullOrbit.c:1307-1352 (evalRectForce,
  *            evalRectDeriv), :1496-1681 (the dxdv variants);
@@ -81,6 +81,8 @@ enum { PT_FLATPOWER = 12 };
 /* KuzminKutuzovStaeckelPotential (KuzminKutuzovStaeckelPotential.c); args
    (amp, ac, Delta) in 3D and in the plane */
 enum { PT_KKS = 16 };
+/* planar only: HenonHeilesPotential (HenonHeilesPotential.c), args (amp) */
+enum { PT_HENONHEILES = 29 };
 
 #define OMAXPOT 32
 
@@ -110,6 +112,7 @@ static int nargs_of(int type, int planar)
   case PT_NULL: return 0;
   case PT_FLATPOWER: return planar ? 3 : 4;
   case PT_KKS: return 3;
+  case PT_HENONHEILES: return planar ? 1 : -1;
   default: return -1;
   }
 }
@@ -498,7 +501,7 @@ static double sph_eval(const ocomp *c, double R, double Z)
 
 /* Decode galpy's (pot_type, pot_args) stream (integrateFullOrbit.c:69-1040,
    integratePlanarOrbit.c:55-742 restricted to types 0/5/7/8/9/10/12/14/15/
-   16/17/18/20/33/34/35/40/41/46).
+   16/17/18/20/29 (planar)/33/34/35/40/41/46).
    Returns 0, or -1 for an unsupported type. */
 static int opot_decode(opot *P, int npot, const int *type, const double *args, int planar)
 {
@@ -786,6 +789,8 @@ static double comp_planarRforce(const ocomp *c, double R, double phi)
   if (is_new_spherical(c->type)) return sph_planarRforce(c, R);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_HENONHEILES: /* HenonHeilesPotentialRforce */
+    return -amp * R * (1. + R * sin(3. * phi));
   case PT_KKS: { /* KuzminKutuzovStaeckelPotentialPlanarRforce */
     double ac = c->p[1], Delta = c->p[2];
     double gamma = Delta * Delta / (1. - ac * ac), alpha = gamma - Delta * Delta;
@@ -827,6 +832,8 @@ static double comp_planarRforce(const ocomp *c, double R, double phi)
 
 static double comp_planarphitorque(const ocomp *c, double R, double phi)
 {
+  if (c->type == PT_HENONHEILES) /* HenonHeilesPotentialphitorque */
+    return -c->p[0] * pow(R, 3.) * cos(3. * phi);
   if (c->type == PT_LOGHALO && c->p[3] < 1) {
     double amp = c->p[0], cc = c->p[2], om = c->p[3], Rt2 = lh_Rt2(c, R, phi);
     return amp * R * R / (Rt2 + cc) * sin(2 * phi) * om / 2.;
@@ -840,6 +847,10 @@ static double comp_planarhess(const ocomp *c, int which, double R, double phi)
   if (is_new_spherical(c->type)) return which ? 0. : sph_planarR2deriv(c, R);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_HENONHEILES: /* HenonHeilesPotential R2deriv / phi2deriv / Rphideriv */
+    if (which == 0) return amp * (1. + 2. * R * sin(3. * phi));
+    if (which == 1) return -3. * amp * pow(R, 3.) * sin(3. * phi);
+    return 3. * amp * R * R * cos(3. * phi);
   case PT_KKS: { /* KuzminKutuzovStaeckelPotentialPlanarR2deriv */
     if (which) return 0.;
     double ac = c->p[1], Delta = c->p[2];
@@ -901,6 +912,8 @@ static double comp_eval(const ocomp *c, double R, double Z, double phi)
   if (is_new_spherical(c->type)) return sph_eval(c, R, Z);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_HENONHEILES: /* galpy's HenonHeilesPotential._evaluate (no C Eval) */
+    return amp * (0.5 * R * R + pow(R, 3.) * sin(3. * phi) / 3.);
   case PT_KKS: { /* KuzminKutuzovStaeckelPotentialEval */
     double ac = c->p[1], Delta = c->p[2];
     double gamma = Delta * Delta / (1. - ac * ac), alpha = gamma - Delta * Delta;

@@ -224,6 +224,39 @@ def main():
     res, _, _ = O.integrate_sos(yo7, psi_i, pt, pa, "dop853", rtol=1e-10, atol=1e-10, impl="ref")
     out["sos_dop853_indiv"] = res
 
+    # the planar Henon-Heiles potential (type 29, a planarPotential only):
+    # galpy's Python forces at the planar points, and the reference's C
+    # orbits (every method), variational orbits and surface of section
+    # x = 0 for bound orbits (E < 1/6 for amp = 1)
+    hh = gp.HenonHeilesPotential(amp=1.2)
+    _, pth, pah, _ = parse2([hh])
+    out["hh_type"], out["hh_args"] = np.asarray(pth, np.int32), np.asarray(pah)
+    out["hh_pyforces"] = np.stack(
+        [np.asarray([f(r, phi=q) for r, q in zip(R, phi)], float)
+         for f in (hh.Rforce, hh.phitorque, hh.R2deriv, hh.phi2deriv, hh.Rphideriv, hh)], 1)
+    hics = np.stack([np.full(8, 0.3), np.linspace(-0.2, 0.2, 8), np.full(8, 0.22),
+                     np.linspace(0.0, 6.0, 8)], 1)
+    out["hh_ics"] = hics
+    t = np.linspace(0, 30, 61)
+    for m in ("leapfrog", "rk4", "rk6", "symplec4", "symplec6", "dopr54", "dop853"):
+        res, err, _, _ = O.integrate(hics, t, pth, pah, m, planar=True, rtol=1e-10, atol=1e-10,
+                                     impl="ref")
+        assert not err.any()
+        out[f"hh_{m}"] = res
+    w2 = np.zeros((4, 8))
+    w2[:, :4] = cyl_to_rect(hics[:4])
+    w2[np.arange(4), 4 + np.arange(4)] = 1.0
+    out["hh_dxdv_w2"] = w2
+    res, _, _ = O.integrate_dxdv(w2, np.linspace(0, 10, 21), pth, pah, "dop853", planar=True,
+                                 impl="ref")
+    out["hh_dop853_dxdv2"] = res
+    hyo = np.concatenate([hics, np.zeros((8, 1))], 1)
+    for m in ("rk6", "dop853"):
+        res, err, _ = O.integrate_sos(hyo, psi, pth, pah, m, rtol=1e-10, atol=1e-10,
+                                      planar=True, surface=0, impl="ref")
+        assert not err.any()
+        out[f"hh_sos0_{m}"] = res
+
     # gradient oracle of the adjoint: Jacobians d y(T) / d y(0) from the
     # reference's variational DOP853 (integrate{Planar,Full}Orbit_dxdv), one
     # unit deviation column per run, t in [0, 20], rtol = atol = 1e-10

@@ -167,16 +167,24 @@ extern "C" int harness_gamma_star(double alpha, double rc, int n, const double* 
   return 0;
 }
 
-// potential values at points (energy kernel's device function, on the host)
+// potential values at points (energy kernel's device function, on the host),
+// from galpy's 3D or planar argument list
+extern "C" int harness_potential_in(int planar, int n, const double* x, const double* y,
+                                    const double* z, int npot, const int* pot_type,
+                                    const double* pot_args, double* out)
+{
+  std::vector<GpComp> comps(npot);
+  int rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
+  if (rc) return rc;
+  for (int i = 0; i < n; i++) out[i] = potential_value(comps.data(), npot, x[i], y[i], z[i]);
+  return 0;
+}
+
 extern "C" int harness_potential(int n, const double* x, const double* y, const double* z,
                                  int npot, const int* pot_type, const double* pot_args,
                                  double* out)
 {
-  std::vector<GpComp> comps(npot);
-  int rc = compile_group(0, npot, pot_type, pot_args, comps.data(), nullptr);
-  if (rc) return rc;
-  for (int i = 0; i < n; i++) out[i] = potential_value(comps.data(), npot, x[i], y[i], z[i]);
-  return 0;
+  return harness_potential_in(0, n, x, y, z, npot, pot_type, pot_args, out);
 }
 
 extern "C" int harness_forces(int planar, int n, const double* x, const double* y,
