@@ -231,6 +231,8 @@ int galpy_cuda_adjoint_params(int planar, int npot, const int* pot_type, int* ar
     return gpc_report_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
   int n = 0, off = 0;
   for (int k = 0; k < npot; k++) {
+    // an ellipsoidal component's argument count depends on its arguments,
+    // which this call does not take: reported as not implemented
     const int na = galpy_nargs(pot_type[k], planar);
     if (na < 0)
       return gpc_report_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");

@@ -16,9 +16,19 @@
 namespace gpc {
 
 // number of galpy arguments of a supported type (3D PowerSphericalwCutoff
-// carries two extra cache slots, integrateFullOrbit.py:178-180)
-inline int galpy_nargs(int type, int planar)
+// carries two extra cache slots, integrateFullOrbit.py:178-180); an
+// ellipsoidal component's count depends on its own arguments
+// (integrateFullOrbit.c case 21: 30 + npsi + 2 glorder), read from p
+// (-1 without them)
+inline int galpy_nargs(int type, int planar, const double* p = nullptr)
 {
+  if (is_ellipsoidal(type)) {
+    if (!p) return -1;
+    const int npsi = (int)p[16];
+    if (npsi < 0 || npsi > 16) return -1;
+    const int order = (int)p[29 + npsi];
+    return order < 1 ? -1 : 30 + npsi + 2 * order;
+  }
   switch (type) {
     case T_LOGHALO: return 4;
     case T_MN: return 3;
@@ -173,7 +183,7 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
   const double* p = pot_args;
   for (int k = 0; k < npot; k++) {
     const int type = pot_type[k];
-    const int na = galpy_nargs(type, planar);
+    const int na = galpy_nargs(type, planar, p);
     if (na < 0) return -3;
     GpComp c;
     memset(&c, 0, sizeof(c));
@@ -311,6 +321,45 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
         const double gamma = Delta * Delta / (1.0 - ac * ac), alpha = gamma - Delta * Delta;
         c.c[1] = Delta * Delta;
         c.c[2] = alpha + gamma;
+        break;
+      }
+      case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
+      case T_POWERTRI: case T_TWOPOWERTRI: {
+        // (amp, 15 cache slots, npsi, psi args, b^2, c^2, aligned, rot[9],
+        // n, x_k[n], w_k[n]), integrateFullOrbit.py:214-290; x_k are the
+        // Gauss-Legendre nodes of the integral over tau = 1/x^2 - 1
+        const int npsi = (int)p[16];
+        const double* ps = p + 17;
+        const double* e = ps + npsi;
+        const double b2 = e[0], c2 = e[1];
+        const int order = (int)e[12];
+        if (order > kEllMaxOrder) return -3;  // more nodes than the record holds
+        switch (type) {
+          case T_TWOPOWERTRI:  // (a, alpha, beta, beta - alpha, ...)
+            c.c[1] = ps[0];
+            c.c[2] = ps[1];
+            c.c[3] = ps[2];
+            c.c[4] = ps[3];
+            break;
+          case T_PERFECTELL: case T_TRIGAUSS: case T_POWERTRI:  // one parameter
+            c.c[1] = ps[0];
+            break;
+          default:  // (a, a^k)
+            c.c[1] = ps[0];
+            c.c[2] = ps[1];
+            break;
+        }
+        c.c[5] = order;
+        c.c[6] = e[2] != 0.0 ? 0.0 : 1.0;  // galpy passes "aligned"
+        for (int j = 0; j < 9; j++) c.bin[0][j] = e[3 + j];
+        double* nd = &c.cheb[0][0];
+        for (int k = 0; k < order; k++) {
+          const long double xk = e[13 + k], tau = 1.0L / (xk * xk) - 1.0L;
+          nd[4 * k] = e[13 + order + k];
+          nd[4 * k + 1] = (double)(1.0L / (1.0L + tau));
+          nd[4 * k + 2] = (double)(1.0L / ((long double)b2 + tau));
+          nd[4 * k + 3] = (double)(1.0L / ((long double)c2 + tau));
+        }
         break;
       }
       case T_FLATPOWER: {  // (amp, alpha, q^2, core^2); planar (amp, alpha, core^2)

@@ -7,8 +7,10 @@
 // (10), Isochrone (14), Plummer (17), PseudoIsothermal (18), Burkert (20),
 // DehnenCoreSpherical (33), DehnenSpherical (34), HomogeneousSphere (35) and
 // Null (40) and Einasto (41) potentials, and the axisymmetric FlattenedPower
-// (12) and KuzminKutuzovStaeckel (16), and the planar HenonHeiles (29).
-// Reference formulas:
+// (12) and KuzminKutuzovStaeckel (16), the planar HenonHeiles (29), and
+// the EllipsoidalPotential family: TriaxialHernquist (21), TriaxialNFW (22),
+// TriaxialJaffe (23), PerfectEllipsoid (30), TriaxialGaussian (37),
+// PowerTriaxial (38) and TwoPowerTriaxial (43).  Reference formulas:
 // galpy/potential/potential_c_ext/<name>.c.
 //
 // Design (not a translation of the reference's cylindrical route):
@@ -54,6 +56,17 @@ enum : int { T_POWER = 7, T_JAFFE = 10, T_ISOCHRONE = 14, T_PLUMMER = 17, T_PSEU
 enum : int { T_FLATPOWER = 12, T_KKS = 16 };
 // planar, non-axisymmetric HenonHeilesPotential (HenonHeilesPotential.c)
 enum : int { T_HENONHEILES = 29 };
+// EllipsoidalPotential.c with the density functions m -> rho(m) of
+// TwoPowerTriaxialPotential.c (TriaxialHernquist, TriaxialNFW,
+// TriaxialJaffe, TwoPowerTriaxial), PerfectEllipsoidPotential.c,
+// TriaxialGaussianPotential.c and PowerTriaxialPotential.c
+enum : int { T_TRIHERNQUIST = 21, T_TRINFW = 22, T_TRIJAFFE = 23, T_PERFECTELL = 30,
+             T_TRIGAUSS = 37, T_POWERTRI = 38, T_TWOPOWERTRI = 43 };
+GPC_HD GPC_FI constexpr bool is_ellipsoidal(int t)
+{
+  return t == T_TRIHERNQUIST || t == T_TRINFW || t == T_TRIJAFFE || t == T_PERFECTELL ||
+         t == T_TRIGAUSS || t == T_POWERTRI || t == T_TWOPOWERTRI;
+}
 
 constexpr int kMaxComp = 16;  // components per potential group
 constexpr int kChebN = 32;    // Chebyshev intervals of gamma*(a, u) on [0, U]
@@ -435,9 +448,9 @@ GPC_HD inline double exptruncnfw_F(const S& sc, double r)
 
 // ------------------------------------------------------------- forces ---
 // Add one component's contribution to the radial factors: the acceleration
-// is a = (x gR, y (gR + gyx) + ay0, z gz).  ay0 only takes the terms of
-// a_y that are not proportional to y (Henon-Heiles' -amp x^2).  TYPE < 0:
-// read the type at run time.
+// is a = (x gR, y (gR + gyx), z gz) + a0, where a0 takes the terms that are
+// not of that form (Henon-Heiles' -amp x^2 in a_y, ellipsoidal components).
+// TYPE < 0: read the type at run time.
 // Scalar parameters of a component: from the compiled record in global
 // memory (read-only path), or from a copy passed as a kernel parameter
 // (constant bank: no load instruction when the index is a compile-time
@@ -452,6 +465,143 @@ struct ScalarsDirect {
   const double* p;
   GPC_HD GPC_FI double operator[](int j) const { return p[j]; }
 };
+
+// Acceleration terms that are not of the radial-factor form (Henon-Heiles'
+// -amp x^2 in a_y, the ellipsoidal components' full vectors).
+template <typename T>
+struct AddAcc {
+  T x, y, z;
+};
+
+// ---- ellipsoidal components -------------------------------------------
+// Record: c[0] amp, c[1..4] the density's parameters (TriaxialHernquist
+// (a, a^4), TriaxialNFW (a, a^3), TriaxialJaffe (a, a^2), TwoPowerTriaxial
+// (a, alpha, beta, beta - alpha), PerfectEllipsoid (a^2), TriaxialGaussian
+// (-2 sigma^2), PowerTriaxial (alpha)), c[5] the Gauss-Legendre order n,
+// c[6] 1 if the principal axes are not the coordinate axes; the rotation
+// (row-major, x' = rot x) in bin[0][0..8]; per node k of the integral over
+// tau, cheb[] holds (w_k, 1/(1+tau_k), 1/(b^2+tau_k), 1/(c^2+tau_k)) with
+// galpy's weights w_k (the -4 pi b c / sqrt(...) factor included).
+// Force per unit amp: F' = sum_k w_k rho(m_k) (x'/(1+tau_k), y'/(b^2+tau_k),
+// z'/(c^2+tau_k)), m_k^2 = x'^2/(1+tau_k) + y'^2/(b^2+tau_k) + z'^2/(c^2+tau_k),
+// F = rot^T F'.
+constexpr int kEllMaxOrder = kChebN * kChebC / 4;
+
+GPC_HD GPC_FI double ell_rho(int type, const GpComp* cp, double m2, double& m)
+{
+  const double p1 = ldg(&cp->c[1]);
+  switch (type) {
+    case T_PERFECTELL: {
+      const double d = 1.0 / (p1 + m2);
+      return d * d;
+    }
+    case T_TRIGAUSS: return exp(m2 / p1);
+    case T_POWERTRI: return exp(-0.5 * p1 * log(m2));
+    default: break;
+  }
+  m = sqrt(m2);
+  const double mpa = m + p1, p2 = ldg(&cp->c[2]);
+  switch (type) {
+    case T_TRIHERNQUIST: return p2 / (m * mpa * mpa * mpa);
+    case T_TRINFW: return p2 / (m * mpa * mpa);
+    case T_TRIJAFFE: {
+      const double d = 1.0 / (m * mpa);
+      return p2 * p2 * d * d;
+    }
+    default:  // TwoPowerTriaxial: (a/m)^alpha (1 + m/a)^-(beta - alpha)
+      return exp(p2 * log(p1 / m) - ldg(&cp->c[4]) * log1p(m / p1));
+  }
+}
+
+// rho'(m) / m, given rho(m) and m (set by ell_rho for the types that use it)
+GPC_HD GPC_FI double ell_drho_over_m(int type, const GpComp* cp, double m2, double m, double rho)
+{
+  const double p1 = ldg(&cp->c[1]);
+  switch (type) {
+    case T_PERFECTELL: return -4.0 * rho / (p1 + m2);
+    case T_TRIGAUSS: return 2.0 * rho / p1;
+    case T_POWERTRI: return -p1 * rho / m2;
+    case T_TRIHERNQUIST: return -rho * (p1 + 4.0 * m) / (m2 * (m + p1));
+    case T_TRINFW: return -rho * (p1 + 3.0 * m) / (m2 * (m + p1));
+    case T_TRIJAFFE: return -2.0 * rho * (p1 + 2.0 * m) / (m2 * (m + p1));
+    default:  // TwoPowerTriaxial
+      return -rho * (p1 * ldg(&cp->c[2]) + ldg(&cp->c[3]) * m) / (m2 * (m + p1));
+  }
+}
+
+// Acceleration of one ellipsoidal component (amp included), FP64.
+GPC_HD GPC_FI void ell_accel(const GpComp* __restrict__ cp, int type, double x, double y,
+                             double z, double& ax, double& ay, double& az)
+{
+  const double* rot = &cp->bin[0][0];
+  const bool rotated = ldg(&cp->c[6]) != 0.0;
+  if (rotated) {
+    const double xr = ldg(rot + 0) * x + ldg(rot + 1) * y + ldg(rot + 2) * z;
+    const double yr = ldg(rot + 3) * x + ldg(rot + 4) * y + ldg(rot + 5) * z;
+    const double zr = ldg(rot + 6) * x + ldg(rot + 7) * y + ldg(rot + 8) * z;
+    x = xr;
+    y = yr;
+    z = zr;
+  }
+  const int n = (int)ldg(&cp->c[5]);
+  const double* nd = &cp->cheb[0][0];
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  for (int k = 0; k < n; k++, nd += 4) {
+    const double w = ldg(nd), i1 = ldg(nd + 1), i2 = ldg(nd + 2), i3 = ldg(nd + 3);
+    const double xs = x * i1, ys = y * i2, zs = z * i3;
+    const double m2 = x * xs + y * ys + z * zs;
+    double m = 0.0;
+    const double td = w * ell_rho(type, cp, m2, m);
+    fx += td * xs;
+    fy += td * ys;
+    fz += td * zs;
+  }
+  if (rotated) {
+    const double gx = ldg(rot + 0) * fx + ldg(rot + 3) * fy + ldg(rot + 6) * fz;
+    const double gy = ldg(rot + 1) * fx + ldg(rot + 4) * fy + ldg(rot + 7) * fz;
+    const double gz = ldg(rot + 2) * fx + ldg(rot + 5) * fy + ldg(rot + 8) * fz;
+    fx = gx;
+    fy = gy;
+    fz = gz;
+  }
+  const double amp = ldg(&cp->c[0]);
+  ax = amp * fx;
+  ay = amp * fy;
+  az = amp * fz;
+}
+
+// Tidal tensor K = -amp d^2 Phi / dx dx of one ellipsoidal component,
+// evaluated in the principal-axis form at the given (unrotated) point as
+// the reference's EllipsoidalPotential_2ndderiv_xyz_all is called; K[i] is
+// added to (xx, xy, yy, xz, yz, zz).
+GPC_HD GPC_FI void ell_tidal(const GpComp* __restrict__ cp, int type, double x, double y,
+                             double z, double K[6])
+{
+  const int n = (int)ldg(&cp->c[5]);
+  const double* nd = &cp->cheb[0][0];
+  double h[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // xx, xy, xz, yy, yz, zz per unit amp
+  for (int k = 0; k < n; k++, nd += 4) {
+    const double w = ldg(nd), i1 = ldg(nd + 1), i2 = ldg(nd + 2), i3 = ldg(nd + 3);
+    const double xs = x * i1, ys = y * i2, zs = z * i3;
+    const double m2 = x * xs + y * ys + z * zs;
+    double m = sqrt(m2);
+    const double rho = ell_rho(type, cp, m2, m);
+    const double dv = w * rho, dd = w * ell_drho_over_m(type, cp, m2, m, rho);
+    h[0] -= dd * xs * xs + dv * i1;
+    h[1] -= dd * xs * ys;
+    h[2] -= dd * xs * zs;
+    h[3] -= dd * ys * ys + dv * i2;
+    h[4] -= dd * ys * zs;
+    h[5] -= dd * zs * zs + dv * i3;
+  }
+  const double amp = ldg(&cp->c[0]);
+  K[0] -= amp * h[0];
+  K[1] -= amp * h[1];
+  K[2] -= amp * h[3];
+  K[3] -= amp * h[2];
+  K[4] -= amp * h[4];
+  K[5] -= amp * h[5];
+}
 
 // KuzminKutuzovStaeckel: Phi = -amp V, V = 1 / (sqrt(l) + sqrt(n)) with the
 // prolate spheroidal coordinates l, n = (R^2 + z^2 - alpha - gamma +- sqrt(D))
@@ -536,8 +686,8 @@ GPC_HD GPC_FI T sph_force_factor(int type, const S& sc, T r2)
 }
 
 template <typename T, bool PLANAR, int TYPE, class S>
-GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T y, T z2, T R2,
-                              T r2, T& gR, T& gz, T& gyx, T& ay0)
+GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T y, T z, T z2,
+                              T R2, T r2, T& gR, T& gz, T& gyx, AddAcc<T>& a0)
 {
   const int type = TYPE >= 0 ? TYPE : ldg(&cp->type);
   const T amp = T(sc[0]);
@@ -640,7 +790,16 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
       // a = -amp (x (1 + 2y), y (1 - y) + x^2)
       gR -= amp * (T(1) + T(2) * y);
       gyx += T(3) * amp * y;
-      ay0 -= amp * x * x;
+      a0.y -= amp * x * x;
+      break;
+    }
+    case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
+    case T_POWERTRI: case T_TWOPOWERTRI: {  // in float64
+      double ax, ay, az;
+      ell_accel(tp, type, (double)x, (double)y, PLANAR ? 0.0 : (double)z, ax, ay, az);
+      a0.x += T(ax);
+      a0.y += T(ay);
+      if (!PLANAR) a0.z += T(az);
       break;
     }
     default: {
@@ -655,14 +814,15 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
 // Run-time component list (any combination of the supported types).
 struct DynPot {
   static constexpr bool kDirectScalars = false;
-  static constexpr bool kAdditiveY = true;  // a component may add to ay0
+  static constexpr bool kAdditive = true;  // a component may add to a0
   template <typename T, bool PLANAR>
   GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, const double* /*scal*/, int ncomp,
-                                T x, T y, T z2, T R2, T r2, T& gR, T& gz, T& gyx, T& ay0)
+                                T x, T y, T z, T z2, T R2, T r2, T& gR, T& gz, T& gyx,
+                                AddAcc<T>& a0)
   {
     for (int k = 0; k < ncomp; k++)
-      comp_accel<T, PLANAR, -1>(comp + k, ScalarsGlobal{comp + k}, x, y, z2, R2, r2, gR, gz, gyx,
-                                ay0);
+      comp_accel<T, PLANAR, -1>(comp + k, ScalarsGlobal{comp + k}, x, y, z, z2, R2, r2, gR, gz,
+                                gyx, a0);
   }
 };
 
@@ -673,20 +833,21 @@ constexpr int kScalarStride = 16;
 template <bool DIRECT, int... TYPES>
 struct FixedPot {
   static constexpr bool kDirectScalars = DIRECT;
-  static constexpr bool kAdditiveY = ((TYPES == T_HENONHEILES) || ...);
+  static constexpr bool kAdditive = ((TYPES == T_HENONHEILES || is_ellipsoidal(TYPES)) || ...);
   template <typename T, bool PLANAR>
   GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, const double* scal, int /*ncomp*/,
-                                T x, T y, T z2, T R2, T r2, T& gR, T& gz, T& gyx, T& ay0)
+                                T x, T y, T z, T z2, T R2, T r2, T& gR, T& gz, T& gyx,
+                                AddAcc<T>& a0)
   {
     int k = 0;
     if (DIRECT) {
-      ((comp_accel<T, PLANAR, TYPES>(comp + k, ScalarsDirect{scal + kScalarStride * k}, x, y, z2,
-                                     R2, r2, gR, gz, gyx, ay0),
+      ((comp_accel<T, PLANAR, TYPES>(comp + k, ScalarsDirect{scal + kScalarStride * k}, x, y, z,
+                                     z2, R2, r2, gR, gz, gyx, a0),
         ++k),
        ...);
     } else {
-      ((comp_accel<T, PLANAR, TYPES>(comp + k, ScalarsGlobal{comp + k}, x, y, z2, R2, r2, gR, gz,
-                                     gyx, ay0),
+      ((comp_accel<T, PLANAR, TYPES>(comp + k, ScalarsGlobal{comp + k}, x, y, z, z2, R2, r2, gR,
+                                     gz, gyx, a0),
         ++k),
        ...);
     }
@@ -707,12 +868,17 @@ GPC_HD GPC_FI void accel(const GpComp* __restrict__ comp, int ncomp, T x, T y, T
   const T R2 = x * x + y * y;
   const T z2 = PLANAR ? T(0) : z * z;
   const T r2 = R2 + z2;
-  T gR = T(0), gz = T(0), gyx = T(0), ay0 = T(0);
-  POT::template sum<T, PLANAR>(comp, scal, ncomp, x, y, z2, R2, r2, gR, gz, gyx, ay0);
+  T gR = T(0), gz = T(0), gyx = T(0);
+  AddAcc<T> a0{T(0), T(0), T(0)};
+  POT::template sum<T, PLANAR>(comp, scal, ncomp, x, y, z, z2, R2, r2, gR, gz, gyx, a0);
   ax = x * gR;
   ay = y * (gR + gyx);
-  if constexpr (POT::kAdditiveY) ay += ay0;  // compile-time lists without it skip the add
   if (!PLANAR) az = z * gz;
+  if constexpr (POT::kAdditive) {  // compile-time lists without such terms skip the adds
+    ax += a0.x;
+    ay += a0.y;
+    if (!PLANAR) az += a0.z;
+  }
 }
 
 // ------------------------------------------------------ tidal tensor ---
@@ -823,7 +989,7 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
 {
   if (PLANAR) z = 0.0;
   const double R2 = x * x + y * y, z2 = z * z, r2 = R2 + z2;
-  double gR = 0.0, gz = 0.0, gyx = 0.0, ay0 = 0.0;
+  double gR = 0.0, gz = 0.0, gyx = 0.0, ax0 = 0.0, ay0 = 0.0, az0 = 0.0;
 #pragma unroll
   for (int i = 0; i < 6; i++) K[i] = 0.0;
   for (int k = 0; k < ncomp; k++) {
@@ -964,6 +1130,16 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
         K[2] -= amp * (1.0 - 2.0 * y);
         break;
       }
+      case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
+      case T_POWERTRI: case T_TWOPOWERTRI: {
+        double fx, fy, fz;
+        ell_accel(cp, type, x, y, z, fx, fy, fz);
+        ax0 += fx;
+        ay0 += fy;
+        az0 += fz;
+        ell_tidal(cp, type, x, y, z, K);
+        break;
+      }
       default: {
         double dpr, d2;  // Phi'/r, Phi''
         sph_derivs(cp, type, amp, r2, dpr, d2);
@@ -972,9 +1148,9 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
       }
     }
   }
-  ax = x * gR;
+  ax = x * gR + ax0;
   ay = y * (gR + gyx) + ay0;
-  az = PLANAR ? 0.0 : z * gz;
+  az = PLANAR ? 0.0 : z * gz + az0;
 }
 
 // -------------------------------------------------- potential values ---
@@ -1023,6 +1199,45 @@ GPC_HD inline double sph_value(const GpComp* __restrict__ cp, int type, double a
     default:
       return 0.0;
   }
+}
+
+// Phi of an ellipsoidal component: -amp/2 sum_k w_k psi(m_k) in the
+// rotated frame (EllipsoidalPotentialEval), psi of each density:
+// TriaxialHernquist -a^4/(m+a)^2, TriaxialNFW -2 a^3/(m+a), TriaxialJaffe
+// 2 a^2 (a/(m+a) + ln(m/(m+a))), PerfectEllipsoid -1/(a^2+m^2),
+// TriaxialGaussian s e^(m^2/s) (s = -2 sigma^2), PowerTriaxial
+// 2/(2-alpha) m^(2-alpha).
+GPC_HD inline double ell_value(const GpComp* __restrict__ cp, int type, double x, double y,
+                               double z)
+{
+  const double* rot = &cp->bin[0][0];
+  if (ldg(&cp->c[6]) != 0.0) {
+    const double xr = ldg(rot + 0) * x + ldg(rot + 1) * y + ldg(rot + 2) * z;
+    const double yr = ldg(rot + 3) * x + ldg(rot + 4) * y + ldg(rot + 5) * z;
+    const double zr = ldg(rot + 6) * x + ldg(rot + 7) * y + ldg(rot + 8) * z;
+    x = xr;
+    y = yr;
+    z = zr;
+  }
+  const int n = (int)ldg(&cp->c[5]);
+  const double* nd = &cp->cheb[0][0];
+  const double p1 = ldg(&cp->c[1]), p2 = ldg(&cp->c[2]);
+  double out = 0.0;
+  for (int k = 0; k < n; k++, nd += 4) {
+    const double m2 = x * x * ldg(nd + 1) + y * y * ldg(nd + 2) + z * z * ldg(nd + 3);
+    const double m = sqrt(m2);
+    double psi;
+    switch (type) {
+      case T_TRIHERNQUIST: psi = -p2 / ((m + p1) * (m + p1)); break;
+      case T_TRINFW: psi = -2.0 * p2 / (m + p1); break;
+      case T_TRIJAFFE: psi = 2.0 * p2 * (p1 / (m + p1) + log(m / (m + p1))); break;
+      case T_PERFECTELL: psi = -1.0 / (p1 + m2); break;
+      case T_TRIGAUSS: psi = p1 * exp(m2 / p1); break;
+      default: psi = 2.0 / (2.0 - p1) * pow(m2, 1.0 - 0.5 * p1); break;  // PowerTriaxial
+    }
+    out += ldg(nd) * psi;
+  }
+  return -0.5 * ldg(&cp->c[0]) * out;
 }
 
 // Potential Phi(x, y, z) summed over one group's components, FP64
@@ -1078,6 +1293,13 @@ GPC_HD inline double potential_value(const GpComp* __restrict__ comp, int ncomp,
       }
       case T_HENONHEILES:  // amp (R^2/2 + R^3 sin(3 phi)/3)
         phi += amp * (0.5 * R2 + x * x * y - y * y * y / 3.0);
+        break;
+      case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
+      case T_POWERTRI:
+        phi += ell_value(cp, ldg(&cp->type), x, y, z);
+        break;
+      case T_TWOPOWERTRI:  // psi needs the Gauss hypergeometric function 2F1: not carried
+        phi += NAN;
         break;
       default:
         phi += sph_value(cp, ldg(&cp->type), amp, r2);

@@ -83,12 +83,37 @@ enum { PT_FLATPOWER = 12 };
 enum { PT_KKS = 16 };
 /* planar only: HenonHeilesPotential (HenonHeilesPotential.c), args (amp) */
 enum { PT_HENONHEILES = 29 };
+/* the EllipsoidalPotential family (EllipsoidalPotential.c; densities of
+   TwoPowerTriaxialPotential.c, PerfectEllipsoidPotential.c,
+   TriaxialGaussianPotential.c, PowerTriaxialPotential.c), 3D and planar:
+   args (amp, 15 cache slots, npsi, psi args [npsi], b2, c2, aligned,
+   rot [9], glorder, glx [glorder], weights [glorder]) */
+enum { PT_TRIHERNQUIST = 21, PT_TRINFW = 22, PT_TRIJAFFE = 23, PT_PERFECTELL = 30,
+       PT_TRIGAUSS = 37, PT_POWERTRI = 38, PT_TWOPOWERTRI = 43 };
+
+static int is_ellipsoidal(int type)
+{
+  switch (type) {
+  case PT_TRIHERNQUIST: case PT_TRINFW: case PT_TRIJAFFE: case PT_PERFECTELL:
+  case PT_TRIGAUSS: case PT_POWERTRI: case PT_TWOPOWERTRI:
+    return 1;
+  }
+  return 0;
+}
+
+/* argument count of an ellipsoidal component (integrateFullOrbit.c case 21) */
+static int ell_nargs(const double *a)
+{
+  int np = (int)a[16];
+  return 30 + np + 2 * (int)a[29 + np];
+}
 
 #define OMAXPOT 32
 
 typedef struct {
   int type;
-  double p[5]; /* the component's args as galpy passes them */
+  double p[5];     /* the component's args as galpy passes them */
+  const double *ea; /* all args (ellipsoidal components: the caller's array) */
 } ocomp;
 
 typedef struct {
@@ -510,11 +535,13 @@ static int opot_decode(opot *P, int npot, const int *type, const double *args, i
   P->planar = planar;
   P->nforce = 0;
   for (int i = 0; i < npot; i++) {
-    int na = nargs_of(type[i], planar);
+    int na = is_ellipsoidal(type[i]) ? ell_nargs(args) : nargs_of(type[i], planar);
     if (na < 0) return -1;
     P->c[i].type = type[i];
+    P->c[i].ea = args;
     for (int k = 0; k < 5; k++) P->c[i].p[k] = 0.;
-    for (int k = 0; k < na; k++) P->c[i].p[k] = *args++;
+    for (int k = 0; k < na && k < 5; k++) P->c[i].p[k] = args[k];
+    args += na;
   }
   return 0;
 }
@@ -555,10 +582,195 @@ static double lh_Rt2(const ocomp *c, double R, double phi)
   return R * R * (1. - c->p[3] * pow(sin(phi), 2));
 }
 
+/* ---- the ellipsoidal family ---- */
+/* the density function m -> rho(m) (mdens), its derivative (mdensDeriv) and
+   psi of each member, from its psi args */
+static double ell_dens(int type, double m, const double *a)
+{
+  double mpa, m2;
+  switch (type) {
+  case PT_TRIHERNQUIST: mpa = m + a[0]; return a[1] * pow(mpa, -3) / m;
+  case PT_TRIJAFFE: mpa = m + a[0]; return a[1] * a[1] * pow(m * mpa, -2);
+  case PT_TRINFW: mpa = m + a[0]; return a[1] / m / mpa / mpa;
+  case PT_TWOPOWERTRI: mpa = m / a[0] + 1.0; return pow(a[0] / m, a[1]) / pow(mpa, a[3]);
+  case PT_PERFECTELL: m2 = m * m; return 1. / (a[0] + m2) / (a[0] + m2);
+  case PT_TRIGAUSS: return exp(m * m / a[0]);
+  default: m2 = m * m; return pow(m2, -a[0] / 2.); /* PowerTriaxial */
+  }
+}
+
+static double ell_densderiv(int type, double m, const double *a)
+{
+  double mpa, m2, md;
+  switch (type) {
+  case PT_TRIHERNQUIST:
+    mpa = m + a[0];
+    return -a[1] * (a[0] + 4. * m) / m / m * pow(mpa, -4);
+  case PT_TRIJAFFE:
+    mpa = m + a[0];
+    return -2. * a[1] * a[1] * (a[0] + 2. * m) * pow(m * mpa, -3);
+  case PT_TRINFW:
+    mpa = m + a[0];
+    return -a[1] * (a[0] + 3. * m) / m / m * pow(mpa, -3);
+  case PT_TWOPOWERTRI:
+    mpa = m + a[0];
+    md = pow(a[0] / m, a[1]) / pow(mpa / a[0], a[3]);
+    return -md * (a[0] * a[1] + a[2] * m) / m / mpa;
+  case PT_PERFECTELL: m2 = m * m; return -4. * m * pow(a[0] + m2, -3);
+  case PT_TRIGAUSS: return 2. * m / a[0] * exp(m * m / a[0]);
+  default: m2 = m * m; return -a[0] * pow(m2, (-a[0] - 1.) / 2.);
+  }
+}
+
+/* psi(m); TwoPowerTriaxial's needs the Gauss hypergeometric function 2F1,
+   which this restatement does not carry: NaN */
+static double ell_psi(int type, double m, const double *a)
+{
+  double mpa, m2;
+  switch (type) {
+  case PT_TRIHERNQUIST: mpa = m + a[0]; return -a[1] / mpa / mpa;
+  case PT_TRIJAFFE: mpa = m + a[0]; return 2. * a[1] * (a[0] / mpa + log(m / mpa));
+  case PT_TRINFW: mpa = m + a[0]; return -2. * a[1] / mpa;
+  case PT_PERFECTELL: m2 = m * m; return -1. / (a[0] + m2);
+  case PT_TRIGAUSS: return a[0] * exp(m * m / a[0]);
+  case PT_POWERTRI: m2 = m * m; return 2. / (2. - a[0]) * pow(m2, 1. - a[0] / 2.);
+  default: return NAN;
+  }
+}
+
+typedef struct {
+  const double *psi, *rot, *glx, *glw;
+  double b2, c2;
+  int aligned, glorder;
+} oell;
+
+static oell ell_args(const ocomp *c)
+{
+  oell e;
+  const double *a = c->ea, *p = a + 17 + (int)a[16];
+  e.psi = a + 17;
+  e.b2 = p[0];
+  e.c2 = p[1];
+  e.aligned = p[2] != 0.;
+  e.rot = p + 3;
+  e.glorder = (int)p[12];
+  e.glx = p + 13;
+  e.glw = p + 13 + e.glorder;
+  return e;
+}
+
+/* x' = rot x (galpy_potentials.c rotate) and F = rot^T F' (rotate_force) */
+static void ell_rotate(const double *r, double *x, double *y, double *z)
+{
+  double xp = r[0] * *x + r[1] * *y + r[2] * *z;
+  double yp = r[3] * *x + r[4] * *y + r[5] * *z;
+  double zp = r[6] * *x + r[7] * *y + r[8] * *z;
+  *x = xp;
+  *y = yp;
+  *z = zp;
+}
+
+static void ell_rotate_back(const double *r, double *x, double *y, double *z)
+{
+  double xp = r[0] * *x + r[3] * *y + r[6] * *z;
+  double yp = r[1] * *x + r[4] * *y + r[7] * *z;
+  double zp = r[2] * *x + r[5] * *y + r[8] * *z;
+  *x = xp;
+  *y = yp;
+  *z = zp;
+}
+
+/* Cartesian force per unit amp (EllipsoidalPotentialxyzforces_xyz) */
+static void ell_forces(const ocomp *c, double x, double y, double z, double F[3])
+{
+  oell e = ell_args(c);
+  if (!e.aligned) ell_rotate(e.rot, &x, &y, &z);
+  F[0] = F[1] = F[2] = 0.;
+  for (int i = 0; i < e.glorder; i++) {
+    double t = 1. / e.glx[i] / e.glx[i] - 1.;
+    double td = e.glw[i] * ell_dens(c->type, sqrt(x * x / (1. + t) + y * y / (e.b2 + t) +
+                                                  z * z / (e.c2 + t)), e.psi);
+    F[0] += td * x / (1. + t);
+    F[1] += td * y / (e.b2 + t);
+    F[2] += td * z / (e.c2 + t);
+  }
+  if (!e.aligned) ell_rotate_back(e.rot, &F[0], &F[1], &F[2]);
+}
+
+/* Cartesian second derivatives per unit amp (xx, xy, xz, yy, yz, zz) at the
+   unrotated point, as EllipsoidalPotential_2ndderiv_xyz_all is called */
+static void ell_hess_xyz(const ocomp *c, double x, double y, double z, double h[6])
+{
+  oell e = ell_args(c);
+  double x2 = x * x, y2 = y * y, z2 = z * z;
+  for (int k = 0; k < 6; k++) h[k] = 0.;
+  for (int i = 0; i < e.glorder; i++) {
+    double s = e.glx[i], t = 1. / s / s - 1.;
+    double t1 = 1. + t, t2 = e.b2 + t, t3 = e.c2 + t;
+    double m = sqrt(x2 / t1 + y2 / t2 + z2 / t3);
+    double dv = e.glw[i] * ell_dens(c->type, m, e.psi);
+    double dd = e.glw[i] * ell_densderiv(c->type, m, e.psi) / m;
+    double xt = x / t1, yt = y / t2, zt = z / t3;
+    h[0] -= dd * xt * xt + dv / t1;
+    h[1] -= dd * xt * yt;
+    h[2] -= dd * xt * zt;
+    h[3] -= dd * yt * yt + dv / t2;
+    h[4] -= dd * yt * zt;
+    h[5] -= dd * zt * zt + dv / t3;
+  }
+}
+
+/* which: 0 Rforce, 1 zforce, 2 phitorque (EllipsoidalPotentialRforce ...) */
+static double ell_cyl_force(const ocomp *c, int which, double R, double Z, double phi)
+{
+  double F[3];
+  ell_forces(c, R * cos(phi), R * sin(phi), Z, F);
+  if (which == 0) return c->p[0] * (cos(phi) * F[0] + sin(phi) * F[1]);
+  if (which == 1) return c->p[0] * F[2];
+  return c->p[0] * R * (-sin(phi) * F[0] + cos(phi) * F[1]);
+}
+
+/* 3D Hessian terms, which = 0 R2, 1 z2, 2 Rz, 3 phi2, 4 Rphi, 5 zphi
+   (EllipsoidalPotentialR2deriv ... zphideriv) */
+static double ell_cyl_hess(const ocomp *c, int which, double R, double Z, double phi)
+{
+  double amp = c->p[0], x = R * cos(phi), y = R * sin(phi), h[6], F[3];
+  double cp, sp;
+  ell_hess_xyz(c, x, y, Z, h);
+  cp = cos(phi);
+  sp = sin(phi);
+  switch (which) {
+  case 0: return amp * (cp * cp * h[0] + sp * sp * h[3] + 2. * cp * sp * h[1]);
+  case 1: return amp * h[5];
+  case 2: return amp * (cp * h[2] + sp * h[4]);
+  case 5: return amp * R * (cp * h[4] - sp * h[2]);
+  }
+  ell_forces(c, x, y, Z, F);
+  if (which == 3)
+    return amp * (R * R * (sp * sp * h[0] + cp * cp * h[3] - 2. * cp * sp * h[1]) +
+                  R * (cp * F[0] + sp * F[1]));
+  return amp * (R * (cp * sp * (h[3] - h[0]) + cos(2. * phi) * h[1]) + sp * F[0] - cp * F[1]);
+}
+
+/* EllipsoidalPotentialEval */
+static double ell_eval(const ocomp *c, double R, double Z, double phi)
+{
+  oell e = ell_args(c);
+  double x = R * cos(phi), y = R * sin(phi), z = Z, out = 0.;
+  if (!e.aligned) ell_rotate(e.rot, &x, &y, &z);
+  for (int i = 0; i < e.glorder; i++) {
+    double s = 1. / e.glx[i] / e.glx[i] - 1.;
+    out += e.glw[i] * ell_psi(c->type, sqrt(x * x / (1. + s) + y * y / (e.b2 + s) +
+                                            z * z / (e.c2 + s)), e.psi);
+  }
+  return -0.5 * c->p[0] * out;
+}
+
 /* ---- 3D component forces ---- */
 static double comp_Rforce(ocomp *c, double R, double Z, double phi)
 {
   if (is_new_spherical(c->type)) return sph_force3(c, R, Z, R);
+  if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 0, R, Z, phi);
   double amp = c->p[0];
   switch (c->type) {
   case PT_KKS:
@@ -598,6 +810,7 @@ static double comp_Rforce(ocomp *c, double R, double Z, double phi)
 static double comp_zforce(ocomp *c, double R, double Z, double phi)
 {
   if (is_new_spherical(c->type)) return sph_force3(c, R, Z, Z);
+  if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 1, R, Z, phi);
   double amp = c->p[0];
   switch (c->type) {
   case PT_KKS:
@@ -638,6 +851,7 @@ static double comp_zforce(ocomp *c, double R, double Z, double phi)
 
 static double comp_phitorque(const ocomp *c, double R, double Z, double phi)
 {
+  if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 2, R, Z, phi);
   if (c->type == PT_LOGHALO && c->p[3] < 1) {
     double amp = c->p[0], q = c->p[1], cc = c->p[2], om = c->p[3];
     double zq = Z / q, Rt2 = lh_Rt2(c, R, phi);
@@ -664,6 +878,7 @@ static void sph_derivs(const ocomp *c, double r, double *dphi, double *d2phi)
 static double comp_hess(const ocomp *c, int which, double R, double Z, double phi)
 {
   if (is_new_spherical(c->type)) return sph_hess3(c, which, R, Z);
+  if (is_ellipsoidal(c->type)) return ell_cyl_hess(c, which, R, Z, phi);
   double amp = c->p[0];
   switch (c->type) {
   case PT_KKS:
@@ -787,6 +1002,7 @@ static double comp_hess(const ocomp *c, int which, double R, double Z, double ph
 static double comp_planarRforce(const ocomp *c, double R, double phi)
 {
   if (is_new_spherical(c->type)) return sph_planarRforce(c, R);
+  if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 0, R, 0., phi);
   double amp = c->p[0];
   switch (c->type) {
   case PT_HENONHEILES: /* HenonHeilesPotentialRforce */
@@ -832,6 +1048,7 @@ static double comp_planarRforce(const ocomp *c, double R, double phi)
 
 static double comp_planarphitorque(const ocomp *c, double R, double phi)
 {
+  if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 2, R, 0., phi);
   if (c->type == PT_HENONHEILES) /* HenonHeilesPotentialphitorque */
     return -c->p[0] * pow(R, 3.) * cos(3. * phi);
   if (c->type == PT_LOGHALO && c->p[3] < 1) {
@@ -845,6 +1062,8 @@ static double comp_planarphitorque(const ocomp *c, double R, double phi)
 static double comp_planarhess(const ocomp *c, int which, double R, double phi)
 {
   if (is_new_spherical(c->type)) return which ? 0. : sph_planarR2deriv(c, R);
+  if (is_ellipsoidal(c->type)) /* EllipsoidalPotentialPlanarR2deriv / phi2 / Rphi */
+    return ell_cyl_hess(c, which == 0 ? 0 : which + 2, R, 0., phi);
   double amp = c->p[0];
   switch (c->type) {
   case PT_HENONHEILES: /* HenonHeilesPotential R2deriv / phi2deriv / Rphideriv */
@@ -910,6 +1129,7 @@ static double comp_planarhess(const ocomp *c, int which, double R, double phi)
 static double comp_eval(const ocomp *c, double R, double Z, double phi)
 {
   if (is_new_spherical(c->type)) return sph_eval(c, R, Z);
+  if (is_ellipsoidal(c->type)) return ell_eval(c, R, Z, phi);
   double amp = c->p[0];
   switch (c->type) {
   case PT_HENONHEILES: /* galpy's HenonHeilesPotential._evaluate (no C Eval) */

@@ -257,6 +257,51 @@ def main():
         assert not err.any()
         out[f"hh_sos0_{m}"] = res
 
+    # the EllipsoidalPotential family (aligned and rotated): galpy's Python
+    # forces (second derivatives where galpy implements them: aligned only;
+    # NaN elsewhere), and the reference's C orbits (dop853 3D, symplec4
+    # planar, dop853 variational 3D)
+    ell = {
+        "trihern": gp.TriaxialHernquistPotential(amp=1.5, a=0.8, b=0.8, c=0.6),
+        "trinfw": gp.TriaxialNFWPotential(amp=2.0, a=2.0, b=0.9, c=0.7, zvec=[0.1, 0.2, 1.0],
+                                          pa=0.3),
+        "trijaffe": gp.TriaxialJaffePotential(amp=1.2, a=0.9, b=0.85, c=0.75, pa=0.4),
+        "perfell": gp.PerfectEllipsoidPotential(amp=1.1, a=1.2, b=0.9, c=0.8),
+        "trigauss": gp.TriaxialGaussianPotential(amp=1.3, sigma=1.5, b=0.8, c=0.7),
+        "powertri": gp.PowerTriaxialPotential(amp=1.0, alpha=1.6, b=0.85, c=0.75, pa=0.2),
+        "twopowtri": gp.TwoPowerTriaxialPotential(amp=1.4, a=1.1, alpha=1.2, beta=3.6, b=0.9,
+                                                  c=0.8),
+    }
+    ics = seeded_ics(8, 0)
+    ics2 = seeded_ics(8, 1, planar=True)
+    t = np.linspace(0, 5, 51)
+    w = np.zeros((2, 12))
+    w[:, :6] = cyl_to_rect(ics[:2])
+    w[0, 6] = w[1, 10] = 1.0
+    for name, p in ell.items():
+        _, pte, pae, _ = parse3([p])
+        _, pte2, pae2, _ = parse2(gp.toPlanarPotential([p]))
+        out[f"ell_{name}_type"] = np.asarray(pte, np.int32)
+        out[f"ell_{name}_args"] = np.asarray(pae)
+        out[f"ell_{name}_planar_type"] = np.asarray(pte2, np.int32)
+        out[f"ell_{name}_planar_args"] = np.asarray(pae2)
+        cols = [np.asarray(f(p, R, z, phi=phi), float)
+                for f in (gp.evaluateRforces, gp.evaluatezforces, gp.evaluatephitorques)]
+        for fn in ("R2deriv", "z2deriv", "Rzderiv", "phi2deriv", "Rphideriv", "phizderiv"):
+            try:
+                cols.append(np.array([getattr(p, fn)(r, zz, phi=q) for r, zz, q in zip(R, z, phi)]))
+            except NotImplementedError:
+                cols.append(np.full(len(R), np.nan))
+        cols.append(np.asarray(gp.evaluatePotentials(p, R, z, phi=phi), float))
+        out[f"ell_{name}_pyforces"] = np.stack(cols, 1)
+        res, err, _, _ = O.integrate(ics, t, pte, pae, "dop853", impl="ref")
+        assert not err.any()
+        out[f"ell_{name}_3d"] = res
+        res, err, _, _ = O.integrate(ics2, t, pte2, pae2, "symplec4", planar=True, impl="ref")
+        out[f"ell_{name}_planar"] = res
+        res, _, _ = O.integrate_dxdv(w, t, pte, pae, "dop853", impl="ref")
+        out[f"ell_{name}_dxdv3"] = res
+
     # gradient oracle of the adjoint: Jacobians d y(T) / d y(0) from the
     # reference's variational DOP853 (integrate{Planar,Full}Orbit_dxdv), one
     # unit deviation column per run, t in [0, 20], rtol = atol = 1e-10
