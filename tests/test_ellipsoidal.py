@@ -190,11 +190,18 @@ def test_gpu_ellipsoidal(engine, oracle, golden, name):
     assert (np.abs(out - ref) / np.abs(ref).max(axis=(1, 2), keepdims=True)).max() < 1e-8
     ics = seeded_ics(256, 37)
     t = np.linspace(0, 6, 31)
+    # each orbit's own conditioning: the oracle's response to a 1-ulp change
+    # of the initial conditions (orbits through the PowerTriaxial cusp with
+    # a fixed rk6 step reach 1e-8)
+    ulp = 1 + np.finfo(float).eps * np.random.default_rng(1).choice([-1, 1], ics.shape)
     for m in ("rk6", "dopr54"):
         ref, _, nref, _ = oracle.integrate(ics, t, pt, pa, m, rtol=1e-10, atol=1e-10)
+        pert, _, _, _ = oracle.integrate(ics * ulp, t, pt, pa, m, rtol=1e-10, atol=1e-10)
+        bound = np.maximum(1e-9, 10 * cyl_diff(ref, pert).max(axis=(1, 2)))
         out, err, ns = gb.integrateFullOrbit_cuda((pt, pa), ics.copy(), t, m + "_cuda",
                                                   rtol=1e-10, atol=1e-10, progressbar=False,
                                                   return_nsteps=True)
         same = ns == nref
         d = cyl_diff(ref, out).max(axis=(1, 2))
-        assert not err.any() and same.mean() >= 0.9 and d[same].max() < 1e-9, m
+        assert not err.any() and same.mean() >= 0.9, m
+        assert (d[same] < bound[same]).all() and np.median(d) < 1e-11, (m, d.max())
