@@ -42,6 +42,7 @@ inline int galpy_nargs(int type, int planar, const double* p = nullptr)
     case T_FLATPOWER: return planar ? 3 : 4;
     case T_KKS: return 3;
     case T_HENONHEILES: return planar ? 1 : -1;  // (amp); a planarPotential only
+    case T_KUZMINDISK: return 2;
     default: return -1;
   }
 }
@@ -362,6 +363,9 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
         }
         break;
       }
+      case T_KUZMINDISK:  // (amp, a)
+        c.c[1] = p[1];
+        break;
       case T_FLATPOWER: {  // (amp, alpha, q^2, core^2); planar (amp, alpha, core^2)
         const double alpha = p[1], q2 = planar ? 1.0 : p[2], core2 = planar ? p[2] : p[3];
         if (!(q2 > 0.0)) return -1;

@@ -8,7 +8,8 @@
 // DehnenCoreSpherical (33), DehnenSpherical (34), HomogeneousSphere (35) and
 // Null (40) and Einasto (41) potentials, and the axisymmetric FlattenedPower
 // (12) and KuzminKutuzovStaeckel (16), the planar HenonHeiles (29), and
-// the EllipsoidalPotential family: TriaxialHernquist (21), TriaxialNFW (22),
+// KuzminDisk (19), the EllipsoidalPotential family: TriaxialHernquist (21),
+// TriaxialNFW (22),
 // TriaxialJaffe (23), PerfectEllipsoid (30), TriaxialGaussian (37),
 // PowerTriaxial (38) and TwoPowerTriaxial (43).  Reference formulas:
 // galpy/potential/potential_c_ext/<name>.c.
@@ -56,6 +57,8 @@ enum : int { T_POWER = 7, T_JAFFE = 10, T_ISOCHRONE = 14, T_PLUMMER = 17, T_PSEU
 enum : int { T_FLATPOWER = 12, T_KKS = 16 };
 // planar, non-axisymmetric HenonHeilesPotential (HenonHeilesPotential.c)
 enum : int { T_HENONHEILES = 29 };
+// KuzminDiskPotential (KuzminDiskPotential.c): Phi = -amp / sqrt(R^2 + (a + |z|)^2)
+enum : int { T_KUZMINDISK = 19 };
 // EllipsoidalPotential.c with the density functions m -> rho(m) of
 // TwoPowerTriaxialPotential.c (TriaxialHernquist, TriaxialNFW,
 // TriaxialJaffe, TwoPowerTriaxial), PerfectEllipsoidPotential.c,
@@ -793,6 +796,16 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
       a0.y -= amp * x * x;
       break;
     }
+    case T_KUZMINDISK: {
+      // a = -amp D^(-3/2) (x, y, sign(z) (a + |z|)), D = R^2 + (a + |z|)^2;
+      // a_z through a0 (sign(0) = 0, as the reference's zforce)
+      const T az = T(sc[1]) + (PLANAR ? T(0) : (z < T(0) ? -z : z));
+      const T iD = Num<T>::rsq(R2 + az * az);
+      const T g = -amp * iD * iD * iD;
+      gR += g;
+      if (!PLANAR) a0.z += z > T(0) ? g * az : (z < T(0) ? -g * az : T(0));
+      break;
+    }
     case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
     case T_POWERTRI: case T_TWOPOWERTRI: {  // in float64
       double ax, ay, az;
@@ -833,7 +846,8 @@ constexpr int kScalarStride = 16;
 template <bool DIRECT, int... TYPES>
 struct FixedPot {
   static constexpr bool kDirectScalars = DIRECT;
-  static constexpr bool kAdditive = ((TYPES == T_HENONHEILES || is_ellipsoidal(TYPES)) || ...);
+  static constexpr bool kAdditive =
+      ((TYPES == T_HENONHEILES || TYPES == T_KUZMINDISK || is_ellipsoidal(TYPES)) || ...);
   template <typename T, bool PLANAR>
   GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, const double* scal, int /*ncomp*/,
                                 T x, T y, T z, T z2, T R2, T r2, T& gR, T& gz, T& gyx,
@@ -1130,6 +1144,19 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
         K[2] -= amp * (1.0 - 2.0 * y);
         break;
       }
+      case T_KUZMINDISK: {  // Cartesian Hessian of -amp D^(-1/2), D = x^2 + y^2 + (a + |z|)^2
+        const double zs = (z > 0.0) - (z < 0.0), az = ldg(&cp->c[1]) + fabs(z);
+        const double D = R2 + az * az, iD = rsq(D), d15 = iD * iD * iD, d25 = d15 / D;
+        gR -= amp * d15;
+        az0 -= zs * amp * d15 * az;
+        K[0] -= amp * (d15 - 3.0 * x * x * d25);
+        K[1] += 3.0 * amp * x * y * d25;
+        K[2] -= amp * (d15 - 3.0 * y * y * d25);
+        K[3] += 3.0 * amp * x * az * zs * d25;
+        K[4] += 3.0 * amp * y * az * zs * d25;
+        K[5] -= amp * (d15 - 3.0 * az * az * d25);
+        break;
+      }
       case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
       case T_POWERTRI: case T_TWOPOWERTRI: {
         double fx, fy, fz;
@@ -1294,6 +1321,11 @@ GPC_HD inline double potential_value(const GpComp* __restrict__ comp, int ncomp,
       case T_HENONHEILES:  // amp (R^2/2 + R^3 sin(3 phi)/3)
         phi += amp * (0.5 * R2 + x * x * y - y * y * y / 3.0);
         break;
+      case T_KUZMINDISK: {
+        const double az = ldg(&cp->c[1]) + fabs(z);
+        phi -= amp / sqrt(R2 + az * az);
+        break;
+      }
       case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
       case T_POWERTRI:
         phi += ell_value(cp, ldg(&cp->type), x, y, z);

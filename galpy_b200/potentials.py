@@ -30,11 +30,12 @@ T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC = 0, 5, 8, 9, 15
 SPHERICAL_TYPES = (7, 10, 14, 17, 18, 20, 33, 34, 35, 40, 41, 46)
 T_FLATPOWER, T_KKS = 12, 16
 T_HENONHEILES = 29  # planar only
+T_KUZMINDISK = 19
 # EllipsoidalPotential family: TriaxialHernquist, TriaxialNFW, TriaxialJaffe,
 # PerfectEllipsoid, TriaxialGaussian, PowerTriaxial, TwoPowerTriaxial
 ELLIPSOIDAL_TYPES = (21, 22, 23, 30, 37, 38, 43)
 SUPPORTED_TYPES = (T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC, T_FLATPOWER,
-                   T_KKS, T_HENONHEILES) + SPHERICAL_TYPES + ELLIPSOIDAL_TYPES
+                   T_KKS, T_HENONHEILES, T_KUZMINDISK) + SPHERICAL_TYPES + ELLIPSOIDAL_TYPES
 
 
 class _Potential:

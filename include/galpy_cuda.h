@@ -17,7 +17,7 @@
  * 10 Jaffe, 14 Isochrone, 17 Plummer, 18 PseudoIsothermal, 20 Burkert,
  * 33 DehnenCoreSpherical, 34 DehnenSpherical, 35 HomogeneousSphere, 40 Null,
  * 41 Einasto, 46 ExpTruncNFW, and the axisymmetric 12 FlattenedPower,
- * 16 KuzminKutuzovStaeckel, the ellipsoidal 21 TriaxialHernquist, 22 TriaxialNFW,
+ * 16 KuzminKutuzovStaeckel, 19 KuzminDisk, the ellipsoidal 21 TriaxialHernquist, 22 TriaxialNFW,
  * 23 TriaxialJaffe, 30 PerfectEllipsoid, 37 TriaxialGaussian, 38 PowerTriaxial,
  * 43 TwoPowerTriaxial (at most 96 Gauss-Legendre nodes), and in the planar
  * entry points 29 HenonHeiles;

@@ -83,6 +83,8 @@ enum { PT_FLATPOWER = 12 };
 enum { PT_KKS = 16 };
 /* planar only: HenonHeilesPotential (HenonHeilesPotential.c), args (amp) */
 enum { PT_HENONHEILES = 29 };
+/* KuzminDiskPotential (KuzminDiskPotential.c), args (amp, a), 3D and planar */
+enum { PT_KUZMINDISK = 19 };
 /* the EllipsoidalPotential family (EllipsoidalPotential.c; densities of
    TwoPowerTriaxialPotential.c, PerfectEllipsoidPotential.c,
    TriaxialGaussianPotential.c, PowerTriaxialPotential.c), 3D and planar:
@@ -138,6 +140,7 @@ static int nargs_of(int type, int planar)
   case PT_FLATPOWER: return planar ? 3 : 4;
   case PT_KKS: return 3;
   case PT_HENONHEILES: return planar ? 1 : -1;
+  case PT_KUZMINDISK: return 2;
   default: return -1;
   }
 }
@@ -773,6 +776,8 @@ static double comp_Rforce(ocomp *c, double R, double Z, double phi)
   if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 0, R, Z, phi);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_KUZMINDISK: /* KuzminDiskPotentialRforce */
+    return -amp * R * pow(R * R + pow(c->p[1] + fabs(Z), 2.), -1.5);
   case PT_KKS:
     return kks_Rz(c, R, Z, 0);
   case PT_FLATPOWER: {
@@ -813,6 +818,10 @@ static double comp_zforce(ocomp *c, double R, double Z, double phi)
   if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 1, R, Z, phi);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_KUZMINDISK: { /* KuzminDiskPotentialzforce */
+    double zsign = (Z > 0) - (Z < 0), a = c->p[1];
+    return -zsign * amp * pow(R * R + pow(a + fabs(Z), 2.), -1.5) * (a + fabs(Z));
+  }
   case PT_KKS:
     return kks_Rz(c, R, Z, 1);
   case PT_FLATPOWER: {
@@ -881,6 +890,14 @@ static double comp_hess(const ocomp *c, int which, double R, double Z, double ph
   if (is_ellipsoidal(c->type)) return ell_cyl_hess(c, which, R, Z, phi);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_KUZMINDISK: { /* KuzminDiskPotentialR2deriv / z2deriv / Rzderiv */
+    double zsign = (Z > 0) - (Z < 0), az = c->p[1] + fabs(Z), denom = R * R + az * az;
+    double d15 = 1. / (denom * sqrt(denom)), d25 = 1. / (denom * denom * sqrt(denom));
+    if (which == 0) return amp * (d15 - 3. * R * R * d15 / denom);
+    if (which == 1) return amp * (d15 - 3. * az * az * d15 / denom);
+    if (which == 2) return amp * (-3. * zsign * R * az * d25);
+    return 0.;
+  }
   case PT_KKS:
     return which > 2 ? 0. : kks_hess(c, R, Z, which);
   case PT_FLATPOWER: {
@@ -1005,6 +1022,8 @@ static double comp_planarRforce(const ocomp *c, double R, double phi)
   if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 0, R, 0., phi);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_KUZMINDISK: /* KuzminDiskPotentialPlanarRforce */
+    return -amp * R * pow(R * R + c->p[1] * c->p[1], -1.5);
   case PT_HENONHEILES: /* HenonHeilesPotentialRforce */
     return -amp * R * (1. + R * sin(3. * phi));
   case PT_KKS: { /* KuzminKutuzovStaeckelPotentialPlanarRforce */
@@ -1066,6 +1085,10 @@ static double comp_planarhess(const ocomp *c, int which, double R, double phi)
     return ell_cyl_hess(c, which == 0 ? 0 : which + 2, R, 0., phi);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_KUZMINDISK: { /* KuzminDiskPotentialPlanarR2deriv */
+    double denom = R * R + c->p[1] * c->p[1];
+    return which ? 0. : amp * (-pow(denom, -1.5) + 3 * R * R * pow(denom, -2.5));
+  }
   case PT_HENONHEILES: /* HenonHeilesPotential R2deriv / phi2deriv / Rphideriv */
     if (which == 0) return amp * (1. + 2. * R * sin(3. * phi));
     if (which == 1) return -3. * amp * pow(R, 3.) * sin(3. * phi);
@@ -1132,6 +1155,8 @@ static double comp_eval(const ocomp *c, double R, double Z, double phi)
   if (is_ellipsoidal(c->type)) return ell_eval(c, R, Z, phi);
   double amp = c->p[0];
   switch (c->type) {
+  case PT_KUZMINDISK: /* KuzminDiskPotentialEval */
+    return -amp * pow(R * R + pow(c->p[1] + fabs(Z), 2.), -0.5);
   case PT_HENONHEILES: /* galpy's HenonHeilesPotential._evaluate (no C Eval) */
     return amp * (0.5 * R * R + pow(R, 3.) * sin(3. * phi) / 3.);
   case PT_KKS: { /* KuzminKutuzovStaeckelPotentialEval */

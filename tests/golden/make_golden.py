@@ -12,8 +12,9 @@ Two kinds of vectors are written to golden.npz:
   triaxial) / NFW / MiyamotoNagai / PowerSphericalwCutoff and of the
   spherical PowerSpherical, Kepler, Jaffe, Isochrone, Plummer,
   PseudoIsothermal, Burkert, DehnenCoreSpherical, DehnenSpherical,
-  HomogeneousSphere, Null, Einasto and ExpTruncNFW potentials at fixed
-  points, plus
+  HomogeneousSphere, Null, Einasto and ExpTruncNFW potentials, the
+  axisymmetric FlattenedPower, KuzminKutuzovStaeckel and KuzminDisk, the
+  planar HenonHeiles and the ellipsoidal family at fixed points, plus
   galpy's pure-Python DOP853 orbits (galpy/util/leung_dop853.py) in
   MWPotential2014;
 * from the reference's own C integrators (integrateFullOrbit /
@@ -118,6 +119,7 @@ def main():
         "flatpower": [gp.FlattenedPowerPotential(amp=1.1, alpha=0.5, q=0.8, core=0.3)],
         "flatlog": [gp.FlattenedPowerPotential(amp=0.9, alpha=0.0, q=0.7, core=0.2)],
         "kks": [gp.KuzminKutuzovStaeckelPotential(amp=1.0, ac=5.0, Delta=0.8)],
+        "kuzmindisk": [gp.KuzminDiskPotential(amp=1.3, a=0.7)],
     }
     pots.update(sph)
     for name, p in pots.items():

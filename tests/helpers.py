@@ -107,7 +107,12 @@ def differentiation_workload(n, seed=3):
 # potentials added behind the component template (golden-vector names)
 ADDED_POTS = ["power", "kepler", "jaffe", "isochrone", "plummer", "pseudoiso", "burkert",
              "dehnencore", "dehnen", "homsphere", "null", "einasto", "exptruncnfw",
-              "flatpower", "flatlog", "kks"]
+              "flatpower", "flatlog", "kks", "kuzmindisk"]
+# forces with a kink (the homogeneous sphere's surface) or a jump (the
+# Kuzmin disk's plane): an adaptive step whose stages straddle it can be
+# accepted on one side of a rounding difference and rejected on the other,
+# and dopr54 forces its smallest step there (err = 1, as the reference)
+KINKED = ("homsphere", "kuzmindisk")
 
 
 def golden_pot(golden, name, planar=False):

@@ -62,10 +62,10 @@ def test_planar_orbit_routes(hooks):
 
 def test_unsupported_potential_falls_back(hooks):
     from galpy.orbit import Orbit
-    from galpy.potential import KuzminDiskPotential
+    from galpy.potential import SCFPotential
 
     o = Orbit([1.0, 0.1, 1.1, 0.0, 0.1, 0.0])
-    o.integrate(np.linspace(0, 1, 11), KuzminDiskPotential(normalize=1.0), method="dop853_cuda")
+    o.integrate(np.linspace(0, 1, 11), SCFPotential(normalize=1.0), method="dop853_cuda")
     assert hooks == []  # galpy's own integrator ran
 
 

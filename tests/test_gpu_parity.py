@@ -10,7 +10,7 @@ import ctypes
 
 import numpy as np
 import pytest
-from helpers import ADDED_POTS, cyl_diff, golden_pot, sos_diff, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
+from helpers import ADDED_POTS, KINKED, cyl_diff, golden_pot, sos_diff, cyl_to_rect, rect_to_cyl, seeded_ics, unit_deviations
 
 import galpy_b200 as gb
 from galpy_b200 import _lib
@@ -189,9 +189,10 @@ def test_spherical_potentials(oracle, golden, name):
     vectors: dop853 3D, symplec4 planar, dop853 variational) and the oracle
     with rk6 / dopr54, FP64 and FP32 force."""
     pt, pa = golden[f"{name}_type"], golden[f"{name}_args"]
-    # the homogeneous sphere's force has a kink at its surface, where an
-    # adaptive step's accept / reject can follow a rounding difference
-    tol = 1e-8 if name == "homsphere" else 1e-10
+    # the homogeneous sphere's force has a kink at its surface and the Kuzmin
+    # disk's a jump at its plane, where an adaptive step's accept / reject can
+    # follow a rounding difference
+    tol = 1e-8 if name in KINKED else 1e-10
     t = np.linspace(0, 5, 51)
     out, err = gb.integrateFullOrbit_cuda((pt, pa), golden["c_ics"].copy(), t, "dop853_cuda",
                                           progressbar=False)
@@ -211,9 +212,20 @@ def test_spherical_potentials(oracle, golden, name):
                                                   atol=1e-10, progressbar=False,
                                                   return_nsteps=True)
         same = ns == nref
-        assert not err.any() and same.mean() >= (0.5 if name == "homsphere" else 0.9), m
         d = cyl_diff(ref, out).max(axis=(1, 2))
-        assert d[same].max() < 1e-9 and d.max() < 1e-6, (m, d.max())
+        if name in KINKED:
+            # at the kink (jump) an adaptive step's accept / reject follows
+            # rounding, and dopr54 forces its smallest step at the Kuzmin
+            # disk's plane (err 1, as the reference): each orbit is bounded
+            # by the oracle's own response to a 1-ulp change of its
+            # initial conditions
+            ulp = 1 + np.finfo(float).eps * np.random.default_rng(1).choice([-1, 1], ics.shape)
+            pert, _, _, _ = oracle.integrate(ics * ulp, t, pt, pa, m, rtol=1e-10, atol=1e-10)
+            bound = np.maximum(1e-9, 10 * cyl_diff(ref, pert).max(axis=(1, 2)))
+            assert np.isin(err, (0, 1)).all() and (d <= bound).all(), (m, d.max())
+        else:
+            assert not err.any() and same.mean() >= 0.9, m
+            assert d[same].max() < 1e-9 and d.max() < 1e-6, (m, d.max())
     f32, err = gb.integrateFullOrbit_cuda((pt, pa), ics.copy(), t, "symplec4_cuda", dt=0.01,
                                           progressbar=False, precision="f32force")
     f64, _ = gb.integrateFullOrbit_cuda((pt, pa), ics.copy(), t, "symplec4_cuda", dt=0.01,
@@ -450,7 +462,7 @@ def test_edge_cases(mw14, oracle):
     with pytest.raises(ValueError):
         gb.integrateFullOrbit_cuda((pt, pa), seeded_ics(2, 35), t, "ias15_cuda")
     with pytest.raises(gb.PotentialNotSupported):
-        gb.integrateFullOrbit_cuda(([19], [1.0, 1.0]), seeded_ics(2, 35), t, "dop853_cuda")
+        gb.integrateFullOrbit_cuda(([11], [1.0, 1.0]), seeded_ics(2, 35), t, "dop853_cuda")
 
 
 def test_progress_callback(mw14):
