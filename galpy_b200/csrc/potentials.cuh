@@ -1149,6 +1149,18 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
         const double D = R2 + az * az, iD = rsq(D), d15 = iD * iD * iD, d25 = d15 / D;
         gR -= amp * d15;
         az0 -= zs * amp * d15 * az;
+        if (PLANAR) {
+          // the reference's planar second derivative (KuzminDiskPotential.c,
+          // PlanarR2deriv) is amp (-D^(-3/2) + 3 R^2 D^(-5/2)), the opposite
+          // sign of d^2 Phi / dR^2 of its planar potential; planar
+          // variational runs follow it: K = -(Phi_RR c^2 + Phi_R/R s^2, ...)
+          const double PRR = -amp * (d15 - 3.0 * R2 * d25), PR_R = amp * d15;
+          const double iR2 = R2 > 0.0 ? 1.0 / R2 : 0.0;
+          K[0] -= (PRR * x * x + PR_R * y * y) * iR2;
+          K[1] -= (PRR - PR_R) * x * y * iR2;
+          K[2] -= (PRR * y * y + PR_R * x * x) * iR2;
+          break;
+        }
         K[0] -= amp * (d15 - 3.0 * x * x * d25);
         K[1] += 3.0 * amp * x * y * d25;
         K[2] -= amp * (d15 - 3.0 * y * y * d25);

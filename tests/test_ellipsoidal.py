@@ -156,6 +156,14 @@ def test_harness_orbits(harness, oracle, golden, name):
     out, err, ns = harness.integrate(w, t, pt, pa, "dop853", var=True)
     assert not err.any() and np.array_equal(ns, nref)
     assert (np.abs(out - ref) / np.abs(ref).max(axis=(1, 2), keepdims=True)).max() < 1e-10
+    # planar variational (the planar second derivatives of
+    # EllipsoidalPotential.c:232-410)
+    pt, pa = _pot(golden, name, planar=True)
+    w = golden["c_dxdv_w2"]
+    ref, _, nref = oracle.integrate_dxdv(w, t, pt, pa, "dop853", planar=True)
+    out, err, ns = harness.integrate(w, t, pt, pa, "dop853", planar=True, var=True)
+    assert not err.any() and np.array_equal(ns, nref)
+    assert (np.abs(out - ref) / np.abs(ref).max(axis=(1, 2), keepdims=True)).max() < 1e-10
 
 
 # ------------------------------------------------------------------ GPU ---

@@ -151,6 +151,23 @@ def test_config0_symplec4_conditioning(harness, oracle, mw14):
     assert per_orbit.max() < 1e-10
 
 
+@pytest.mark.parametrize("name", ADDED_POTS)
+def test_planar_variational_added_potentials(harness, oracle, golden, name):
+    """Planar variational runs (integratePlanarOrbit_dxdv) in each added
+    potential: the planar tidal tensor against the reference's planar second
+    derivatives, restated in the oracle (for KuzminDisk that includes the
+    reference's sign of PlanarR2deriv)."""
+    pt, pa = golden_pot(golden, name, planar=True)
+    w = unit_deviations(cyl_to_rect(seeded_ics(2, 18, planar=True)), 2)
+    t = np.linspace(0, 8, 41)
+    for m in ("rk4",) if name in KINKED else ("rk4", "dop853"):
+        ref, _, nref = oracle.integrate_dxdv(w, t, pt, pa, m, planar=True)
+        out, err, ns = harness.integrate(w, t, pt, pa, m, planar=True, var=True)
+        assert not err.any() and np.array_equal(ns, nref), m
+        rel = np.abs(out - ref) / np.abs(ref).max(axis=(1, 2), keepdims=True)
+        assert rel.max() < 1e-10, (m, rel.max())
+
+
 @pytest.mark.parametrize("method", METHODS)
 @pytest.mark.parametrize("planar", [False, True])
 def test_variational_vs_oracle(harness, oracle, mw14, mw14_planar, method, planar):
