@@ -152,3 +152,23 @@ def test_planar_integrate_sos_routes(monkeypatch):
         assert calls[-1][0] == (1, 4) and calls[-1][2] == "x" and o3.orbit.shape == (1, 6, 3)
     finally:
         galpy_hooks.uninstall()
+
+
+@pytest.mark.parametrize("pot_name, kwargs, planar", [
+    ("TriaxialNFWPotential", dict(amp=2.0, a=2.0, b=0.9, c=0.7, pa=0.3), False),
+    ("PerfectEllipsoidPotential", dict(amp=1.1, a=1.2, b=0.9, c=0.8), False),
+    ("KuzminDiskPotential", dict(amp=1.3, a=0.7), False),
+    ("HenonHeilesPotential", dict(amp=1.0), True),
+])
+def test_added_potential_types_route(hooks, pot_name, kwargs, planar):
+    """The ellipsoidal family, KuzminDisk and the planar HenonHeiles reach the
+    engine (their parsed types are in the supported set)."""
+    from galpy import potential
+    from galpy.orbit import Orbit
+
+    pot = getattr(potential, pot_name)(**kwargs)
+    vxvv = [0.3, 0.05, 0.25, 0.5] if planar else [1.0, 0.1, 1.1, 0.05, 0.02, 0.3]
+    o = Orbit(vxvv)
+    o.integrate(np.linspace(0, 1, 11), pot, method="dop853_cuda")
+    assert len(hooks) == 1 and hooks[-1]["planar"] == planar
+    assert type(hooks[-1]["pot"]).__name__ == pot_name
