@@ -213,3 +213,51 @@ def test_gpu_ellipsoidal(engine, oracle, golden, name):
         d = cyl_diff(ref, out).max(axis=(1, 2))
         assert not err.any() and same.mean() >= 0.9, m
         assert (d[same] < bound[same]).all() and np.median(d) < 1e-11, (m, d.max())
+
+
+SOS_SAFE = {  # (potential, methods) whose every orbit below completes in the oracle
+    "ell_powertri": ("rk4", "rk6", "dopr54", "dop853"),
+    "ell_trigauss": ("rk4", "rk6"),
+    "ell_perfell": ("rk4", "rk6"),
+    "ell_twopowtri": ("rk4", "rk6"),
+    "kuzmindisk": ("rk4", "rk6"),
+}
+
+
+def _sos_yo():
+    return np.concatenate([seeded_ics(6, 21), np.zeros((6, 1))], 1)
+
+
+@pytest.mark.parametrize("key", sorted(SOS_SAFE))
+def test_oracle_surface_of_section_bitwise(oracle, golden, key):
+    """integrateFullOrbit_sos in potentials symmetric about z = 0 (aligned or
+    rotated about z only), bit for bit against the reference build.  Only
+    runs whose every orbit completes in the oracle are given to the reference:
+    where the oracle stops an orbit at dop853's smallest step (err 2; here
+    orbits that escape, and tilted potentials, whose z = 0 is no symmetry
+    plane) the reference's loop never returns."""
+    pt, pa = golden[f"{key}_type"], golden[f"{key}_args"]
+    psi = np.linspace(0.0, 12.0 * np.pi, 7)
+    for m in SOS_SAFE[key]:
+        a, ea, _ = oracle.integrate_sos(_sos_yo(), psi, pt, pa, m, rtol=1e-9, atol=1e-9)
+        assert not ea.any(), m
+        if oracle.ref_available():
+            b, eb, _ = oracle.integrate_sos(_sos_yo(), psi, pt, pa, m, rtol=1e-9, atol=1e-9,
+                                            impl="ref")
+            assert np.array_equal(a, b) and np.array_equal(ea, eb), m
+
+
+@pytest.mark.parametrize("method", ["rk4", "rk6", "dopr54", "dop853"])
+def test_harness_surface_of_section(harness, oracle, golden, method):
+    """The device's SOS machine (force at (x, y, A sin psi) through the
+    ellipsoidal integral) against the oracle: same steps, same crossings."""
+    from helpers import cyl_to_sos, sos_diff, sos_to_cyl
+
+    pt, pa = golden["ell_powertri_type"], golden["ell_powertri_args"]
+    yo = _sos_yo()
+    psi = np.linspace(0.0, 12.0 * np.pi, 7)
+    ref, _, nref = oracle.integrate_sos(yo, psi, pt, pa, method, rtol=1e-9, atol=1e-9)
+    raw, err, ns = harness.integrate_sos(cyl_to_sos(yo), psi, pt, pa, method, rtol=1e-9,
+                                         atol=1e-9)
+    assert not err.any() and np.array_equal(ns, nref)
+    assert sos_diff(ref, sos_to_cyl(raw)).max() < 1e-9
