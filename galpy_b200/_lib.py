@@ -190,7 +190,7 @@ SIGNATURES = {
     "galpy_cuda_adjoint_forward": (_ci, [ctypes.POINTER(GalpyCudaAdjoint)]),
     "galpy_cuda_adjoint_backward": (_ci, [ctypes.POINTER(GalpyCudaAdjoint)]),
     "galpy_cuda_adjoint_replay": (_ci, [ctypes.POINTER(GalpyCudaAdjoint)]),
-    "galpy_cuda_adjoint_params": (_ci, [_ci, _ci, _ip, _ip]),
+    "galpy_cuda_adjoint_params": (_ci, [_ci, _ci, _ip, _dp, _ip]),
     "galpy_cuda_accel_device": (
         _ci, [_vp, _ci, _vp, _ci, _ci, _ci, _vp, ctypes.c_longlong, _vp, _vp]),
 }

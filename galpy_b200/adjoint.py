@@ -44,14 +44,19 @@ CKPT_EVERY = 64
 _ip = ctypes.POINTER(ctypes.c_int)
 
 
-def adjoint_params(pot_type, planar=False):
-    """pot_args index of every differentiable parameter of a component list."""
+def adjoint_params(pot_type, planar=False, pot_args=None):
+    """pot_args index of every differentiable parameter of a component list
+    (pot_args is needed for the ellipsoidal types, whose argument count
+    depends on their arguments)."""
     pt = np.ascontiguousarray(pot_type, dtype=np.int32)
-    n = _lib.lib().galpy_cuda_adjoint_params(int(planar), len(pt), pt.ctypes.data_as(_ip), None)
+    pa = None if pot_args is None else np.ascontiguousarray(pot_args, dtype=np.float64)
+    pap = None if pa is None else pa.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    n = _lib.lib().galpy_cuda_adjoint_params(int(planar), len(pt), pt.ctypes.data_as(_ip), pap,
+                                             None)
     if n < 0:
         _lib.check(n)
     idx = np.zeros(max(n, 1), dtype=np.int32)
-    _lib.lib().galpy_cuda_adjoint_params(int(planar), len(pt), pt.ctypes.data_as(_ip),
+    _lib.lib().galpy_cuda_adjoint_params(int(planar), len(pt), pt.ctypes.data_as(_ip), pap,
                                          idx.ctypes.data_as(_ip))
     return idx[:n]
 
@@ -250,6 +255,7 @@ def _autograd_function():
             fwd = adjoint_forward(comps, ncomp, w0s, tend, t0=t0, rtol=rtol, atol=atol,
                                   planar=planar, signature=sig)
             ctx.spec = spec
+            ctx.pa = pa
             ctx.state = (comps, ncomp, sig, fwd, w0s)
             ctx.pot_args_meta = (pot_args.shape, pot_args.device, pot_args.dtype)
             return fwd["yT"].t()
@@ -258,7 +264,7 @@ def _autograd_function():
         def backward(ctx, gy):
             planar, pot_type, t0, tend, rtol, atol, reduce = ctx.spec
             comps, ncomp, sig, fwd, w0s = ctx.state
-            idx = adjoint_params(pot_type, planar)
+            idx = adjoint_params(pot_type, planar, ctx.pa)
             gw0, gparam = adjoint_backward(comps, ncomp, fwd, gy.t().contiguous(), tend, t0=t0,
                                            rtol=rtol, atol=atol, planar=planar, signature=sig,
                                            nparam=len(idx), w0=w0s)

@@ -225,15 +225,15 @@ int galpy_cuda_adjoint_replay(const galpy_cuda_adjoint* a) { return run_pass(P_R
 
 int galpy_cuda_adjoint_backward(const galpy_cuda_adjoint* a) { return run_pass(P_BACKWARD, a); }
 
-int galpy_cuda_adjoint_params(int planar, int npot, const int* pot_type, int* arg_index)
+int galpy_cuda_adjoint_params(int planar, int npot, const int* pot_type, const double* pot_args,
+                              int* arg_index)
 {
   if (!pot_type || npot < 1 || npot > kMaxComp)
     return gpc_report_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
   int n = 0, off = 0;
   for (int k = 0; k < npot; k++) {
-    // an ellipsoidal component's argument count depends on its arguments,
-    // which this call does not take: reported as not implemented
-    const int na = galpy_nargs(pot_type[k], planar);
+    // an ellipsoidal component's argument count is read from its arguments
+    const int na = galpy_nargs(pot_type[k], planar, pot_args ? pot_args + off : nullptr);
     if (na < 0)
       return gpc_report_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
     const int np = adj::comp_nparam(pot_type[k]);

@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define GALPY_CUDA_ABI_VERSION 1
+#define GALPY_CUDA_ABI_VERSION 2
 
 /* return codes */
 #define GALPY_CUDA_OK 0
@@ -301,8 +301,12 @@ int galpy_cuda_adjoint_replay(const galpy_cuda_adjoint *a);
 
 /* Number of differentiable parameters of a component list (>= 0), or
  * GALPY_CUDA_ERR_POTENTIAL; arg_index (may be NULL) receives the pot_args
- * index of each parameter. */
-int galpy_cuda_adjoint_params(int planar, int npot, const int *pot_type, int *arg_index);
+ * index of each parameter.  pot_args (may be NULL) is needed where a
+ * component's argument count depends on its arguments (the ellipsoidal
+ * types); without it such lists return GALPY_CUDA_ERR_POTENTIAL.  (ABI 2
+ * added pot_args.) */
+int galpy_cuda_adjoint_params(int planar, int npot, const int *pot_type, const double *pot_args,
+                              int *arg_index);
 
 /* Accelerations at n points (positions SoA [3][n] device memory, z ignored
  * when planar) written to acc [3][n], with the integrators' own force code

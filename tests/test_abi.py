@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_record_size():
     lib = _lib.lib()
-    assert lib.galpy_cuda_abi_version() == 1
+    assert lib.galpy_cuda_abi_version() == 2
     # type + table offset, scalars, gamma* table, binade table, two exponent
     # tables, single-precision copies of the gamma* and binade tables
     assert lib.galpy_cuda_comp_size() == (8 + 16 * 8 + 32 * 12 * 8 + 8 * 12 * 8 + 32 * 8 + 64 * 8

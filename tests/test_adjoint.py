@@ -184,4 +184,12 @@ def test_adjoint_params_abi_matches_layout(golden):
     lib = _lib.lib()
     bad = np.array([15, 99], np.int32)
     assert lib.galpy_cuda_adjoint_params(0, 2, bad.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
-                                         None) == _lib.ERR_POTENTIAL
+                                         None, None) == _lib.ERR_POTENTIAL
+    # an ellipsoidal component ahead of a Miyamoto-Nagai disk: its argument
+    # count comes from its arguments (none of its own are differentiable)
+    pte, pae = golden["ell_trihern_type"], golden["ell_trihern_args"]
+    pt = np.concatenate([pte, golden["mn_type"]]).astype(np.int32)
+    pa = np.concatenate([pae, golden["mn_args"]])
+    np.testing.assert_array_equal(adjoint_params(pt, False, pa), len(pae) + np.arange(3))
+    with pytest.raises(_lib.PotentialNotSupported):
+        adjoint_params(pt, False)
