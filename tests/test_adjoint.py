@@ -132,11 +132,15 @@ def test_gradients_other_potentials(harness, golden, name):
     np.testing.assert_allclose(gth, fdt, rtol=1e-6, atol=1e-6 * np.abs(fdt).max())
 
 
-@pytest.mark.parametrize("name", ["plummer", "isochrone", "einasto", "flatpower", "dehnen"])
+@pytest.mark.parametrize("name", ["plummer", "isochrone", "einasto", "flatpower", "dehnen",
+                                  "ell_trihern", "ell_perfell", "ell_trigauss"])
 def test_ic_gradients_added_potentials(harness, golden, name):
     """The potentials added behind the component template have no
     differentiable parameters; they enter the adjoint through the tidal
-    tensor: dL/dw0 against frozen-step central differences."""
+    tensor: dL/dw0 against frozen-step central differences.  The ellipsoidal
+    ones are aligned: the reference's second derivatives, which the tidal
+    tensor follows, ignore any rotation, so for a rotated ellipsoid they are
+    not the derivative of its force."""
     pt, pa = golden[f"{name}_type"], np.array(golden[f"{name}_args"], float)
     w0 = cyl_to_rect(seeded_ics(3, 5))
     t0, T = 0.0, 10.0
