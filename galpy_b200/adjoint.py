@@ -250,12 +250,15 @@ def _autograd_function():
         def forward(ctx, w0, pot_args, spec):
             planar, pot_type, t0, tend, rtol, atol, reduce = spec
             pa = pot_args.detach().to("cpu", torch.float64).numpy()
+            # the parameter map first: a potential without gradients fails
+            # before any device work
+            idx = adjoint_params(pot_type, planar, pa)
             comps, ncomp, sig = _compile(pot_type, pa, planar, w0.device)
             w0s = w0.detach().t().contiguous()
             fwd = adjoint_forward(comps, ncomp, w0s, tend, t0=t0, rtol=rtol, atol=atol,
                                   planar=planar, signature=sig)
             ctx.spec = spec
-            ctx.pa = pa
+            ctx.idx = idx
             ctx.state = (comps, ncomp, sig, fwd, w0s)
             ctx.pot_args_meta = (pot_args.shape, pot_args.device, pot_args.dtype)
             return fwd["yT"].t()
@@ -264,7 +267,7 @@ def _autograd_function():
         def backward(ctx, gy):
             planar, pot_type, t0, tend, rtol, atol, reduce = ctx.spec
             comps, ncomp, sig, fwd, w0s = ctx.state
-            idx = adjoint_params(pot_type, planar, ctx.pa)
+            idx = ctx.idx
             gw0, gparam = adjoint_backward(comps, ncomp, fwd, gy.t().contiguous(), tend, t0=t0,
                                            rtol=rtol, atol=atol, planar=planar, signature=sig,
                                            nparam=len(idx), w0=w0s)

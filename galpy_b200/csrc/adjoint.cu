@@ -236,6 +236,16 @@ int galpy_cuda_adjoint_params(int planar, int npot, const int* pot_type, const d
     const int na = galpy_nargs(pot_type[k], planar, pot_args ? pot_args + off : nullptr);
     if (na < 0)
       return gpc_report_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
+    // a rotated ellipsoid: the tidal tensor follows the reference's second
+    // derivatives, which ignore the rotation, so they are not the derivative
+    // of its force and the adjoint would return wrong gradients
+    if (is_ellipsoidal(pot_type[k])) {
+      const double* e = pot_args + off + 17 + (int)pot_args[off + 16];
+      if (e[2] == 0.0)
+        return gpc_report_error(GALPY_CUDA_ERR_POTENTIAL,
+                                "gradients through a rotated ellipsoidal potential are not "
+                                "available (its second derivatives ignore the rotation)");
+    }
     const int np = adj::comp_nparam(pot_type[k]);
     for (int p = 0; p < np; p++, n++)
       if (arg_index) arg_index[n] = off + adj::comp_param_arg(pot_type[k], p);

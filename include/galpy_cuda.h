@@ -303,8 +303,11 @@ int galpy_cuda_adjoint_replay(const galpy_cuda_adjoint *a);
  * GALPY_CUDA_ERR_POTENTIAL; arg_index (may be NULL) receives the pot_args
  * index of each parameter.  pot_args (may be NULL) is needed where a
  * component's argument count depends on its arguments (the ellipsoidal
- * types); without it such lists return GALPY_CUDA_ERR_POTENTIAL.  (ABI 2
- * added pot_args.) */
+ * types); without it such lists return GALPY_CUDA_ERR_POTENTIAL.  A rotated
+ * ellipsoidal component also returns GALPY_CUDA_ERR_POTENTIAL: the tidal
+ * tensor follows the reference's second derivatives, which ignore the
+ * rotation, so the adjoint's gradients would not be those of its force.
+ * (ABI 2 added pot_args.) */
 int galpy_cuda_adjoint_params(int planar, int npot, const int *pot_type, const double *pot_args,
                               int *arg_index);
 

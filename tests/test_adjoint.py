@@ -197,3 +197,6 @@ def test_adjoint_params_abi_matches_layout(golden):
     np.testing.assert_array_equal(adjoint_params(pt, False, pa), len(pae) + np.arange(3))
     with pytest.raises(_lib.PotentialNotSupported):
         adjoint_params(pt, False)
+    # a rotated ellipsoid has no consistent second derivatives: refused
+    with pytest.raises(_lib.PotentialNotSupported, match="rotated"):
+        adjoint_params(golden["ell_trinfw_type"], False, golden["ell_trinfw_args"])
