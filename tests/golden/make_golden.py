@@ -304,6 +304,19 @@ def main():
         res, _, _ = O.integrate_dxdv(w, t, pte, pae, "dop853", impl="ref")
         out[f"ell_{name}_dxdv3"] = res
 
+    # galpy's pure-Python DOP853 (an implementation apart from its C) in the
+    # planar HenonHeiles and the 3D TriaxialHernquist potentials
+    ts = np.linspace(0.0, 10.0, 51)
+    o = Orbit(hics[:3])
+    o.integrate(ts, hh, method="dop853")
+    out["pydop_hh_orbit"] = np.stack([o.R(ts), o.vR(ts), o.vT(ts), o.phi(ts)], -1)
+    pics = seeded_ics(3, 12)
+    o = Orbit(pics)
+    o.integrate(ts, ell["trihern"], method="dop853")
+    out["pydop_trihern_ics"] = pics
+    out["pydop_trihern_orbit"] = np.stack([o.R(ts), o.vR(ts), o.vT(ts), o.z(ts), o.vz(ts),
+                                           o.phi(ts)], -1)
+
     # gradient oracle of the adjoint: Jacobians d y(T) / d y(0) from the
     # reference's variational DOP853 (integrate{Planar,Full}Orbit_dxdv), one
     # unit deviation column per run, t in [0, 20], rtol = atol = 1e-10

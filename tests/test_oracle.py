@@ -181,6 +181,24 @@ def test_oracle_dop853_vs_galpy_python_dop853(oracle, golden):
     assert d.max() < 1e-7, d.max()
 
 
+def test_oracle_dop853_vs_galpy_python_dop853_added_potentials(oracle, golden):
+    """The C DOP853 against galpy's pure-Python DOP853 in the planar
+    HenonHeiles and the 3D TriaxialHernquist potentials."""
+    ts = np.linspace(0.0, 10.0, 51)
+    a, _, _, _ = oracle.integrate(golden["hh_ics"][:3], ts, golden["hh_type"],
+                                  golden["hh_args"], "dop853", planar=True)
+    ref = golden["pydop_hh_orbit"]
+    d = np.abs(a - ref)
+    d[..., 3] = np.abs((a[..., 3] - ref[..., 3] + np.pi) % (2 * np.pi) - np.pi)
+    assert d.max() < 1e-7, d.max()
+    a, _, _, _ = oracle.integrate(golden["pydop_trihern_ics"], ts, golden["ell_trihern_type"],
+                                  golden["ell_trihern_args"], "dop853")
+    ref = golden["pydop_trihern_orbit"]
+    d = np.abs(a - ref)
+    d[..., 5] = np.abs((a[..., 5] - ref[..., 5] + np.pi) % (2 * np.pi) - np.pi)
+    assert d.max() < 1e-7, d.max()
+
+
 @pytest.mark.parametrize("method", METHODS)
 def test_oracle_energy_conservation(oracle, mw14, method):
     """galpy's test_energy_jacobi_conservation criterion
