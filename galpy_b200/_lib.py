@@ -193,6 +193,7 @@ SIGNATURES = {
     "galpy_cuda_adjoint_params": (_ci, [_ci, _ci, _ip, _dp, _ip]),
     "galpy_cuda_accel_device": (
         _ci, [_vp, _ci, _vp, _ci, _ci, _ci, _vp, ctypes.c_longlong, _vp, _vp]),
+    "galpy_cuda_trim_memory": (_ci, [_ci]),
 }
 
 

@@ -21,6 +21,7 @@
 //     cylindrical rows for the drop-in entry points, or coalesced SoA rows
 //     for device-resident batch use.
 #include <cub/device/device_radix_sort.cuh>
+#include <cuda.h>  // CUcontext and CUresult only; no driver symbol is linked
 #include <cuda_runtime.h>
 #include <signal.h>
 #include <stdio.h>
@@ -61,6 +62,25 @@ __attribute__((visibility("hidden"))) int gpc_report_error(int code, const char*
     if (e_ != cudaSuccess)                                                              \
       return set_error(GALPY_CUDA_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
   } while (0)
+
+// The context current on the calling thread: the driver's cuCtxGetCurrent,
+// reached through the runtime (cudaGetDriverEntryPoint) so that the library
+// does not link libcuda itself.  NULL when no context is current yet.
+static CUcontext current_context()
+{
+  typedef CUresult (*GetCurrentFn)(CUcontext*);
+  static const GetCurrentFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (GetCurrentFn) nullptr;
+    return reinterpret_cast<GetCurrentFn>(p);
+  }();
+  CUcontext c = nullptr;
+  if (fn && fn(&c) != CUDA_SUCCESS) c = nullptr;
+  return c;
+}
 
 // ----------------------------------------------------------------------------
 // longest-first scheduling: estimated cost of each orbit
@@ -162,18 +182,16 @@ static bool direct_scalars(const galpy_cuda_launch* L, double* scal)
   return true;
 }
 
-static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool progress,
-                         cudaStream_t stream)
+// Kernel and kernel arguments of a launch, with the control words pointed
+// into `scratch` (a Scratch in device memory, cleared by the caller).
+static int prepare_launch(const galpy_cuda_launch* L, Scratch* scratch, bool progress,
+                          KernelInfo& ki, KArgs& A)
 {
   double scal[kMaxComp * kScalarStride] = {0.0};
   const bool direct = direct_scalars(L, scal);
-  const int system = launch_system(L);
-  const KernelInfo ki =
-      pick_kernel(L->planar, L->variational, L->precision, L->odeint_type, L->signature,
-                  L->variant, direct, system);
-  KernelFn fn = ki.fn;
-  if (!fn) return set_error(GALPY_CUDA_ERR_METHOD, "method/precision combination not implemented");
-  KArgs A;
+  ki = pick_kernel(L->planar, L->variational, L->precision, L->odeint_type, L->signature,
+                   L->variant, direct, launch_system(L));
+  if (!ki.fn) return set_error(GALPY_CUDA_ERR_METHOD, "method/precision combination not implemented");
   memset(&A, 0, sizeof(A));
   A.nobj = L->nobj;
   A.nt = L->nt;
@@ -202,41 +220,16 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
   A.done_count = progress ? &scratch->done_count : nullptr;
   A.variational_nv = L->variational ? (L->planar ? 8 : 12) : 0;
   memcpy(A.scal, scal, sizeof(scal));
-  GPC_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(Scratch), stream));
+  return GALPY_CUDA_OK;
+}
 
-  // longest-first work queue (stream-ordered scratch, freed after the launch);
-  // surface-of-section runs go in order (the cost pass reads orbit states)
-  void* sched = nullptr;
-  if (L->schedule == GALPY_CUDA_SCHED_LONGEST_FIRST && L->nobj > 1 && L->nobj < (1LL << 31) &&
-      system == GALPY_CUDA_SYS_ORBIT) {
-    const int n = (int)L->nobj;
-    size_t tmp_bytes = 0;
-    cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, (float*)nullptr, (float*)nullptr,
-                                              (int*)nullptr, (int*)nullptr, n, 0, 32, stream);
-    const size_t keys = (size_t)n * sizeof(float), vals = (size_t)n * sizeof(int);
-    const size_t off_k2 = keys, off_v1 = 2 * keys, off_v2 = 2 * keys + vals,
-                 off_tmp = (2 * keys + 2 * vals + 255) & ~(size_t)255;
-    GPC_CUDA_TRY(cudaMallocAsync(&sched, off_tmp + tmp_bytes, stream));
-    char* base = static_cast<char*>(sched);
-    float* k1 = reinterpret_cast<float*>(base);
-    float* k2 = reinterpret_cast<float*>(base + off_k2);
-    int* v1 = reinterpret_cast<int*>(base + off_v1);
-    int* v2 = reinterpret_cast<int*>(base + off_v2);
-    const unsigned cb = (unsigned)((L->nobj + 255) / 256);
-    if (L->planar)
-      cost_kernel<2><<<cb, 256, 0, stream>>>(A, k1, v1);
-    else
-      cost_kernel<3><<<cb, 256, 0, stream>>>(A, k1, v1);
-    GPC_CUDA_TRY(cudaGetLastError());
-    cudaError_t se = cub::DeviceRadixSort::SortPairsDescending(base + off_tmp, tmp_bytes, k1, k2,
-                                                               v1, v2, n, 0, 32, stream);
-    if (se != cudaSuccess) {
-      cudaFreeAsync(sched, stream);
-      return set_error(GALPY_CUDA_ERR_CUDA, std::string("radix sort: ") + cudaGetErrorString(se));
-    }
-    A.order = v2;
-  }
-
+// Grid of the persistent kernel (one wave: SMs x resident blocks), its
+// shared memory and carveout, the SMs reserved for the longest orbits, and
+// the launch.  Shared by the allocating and the allocation-free entry points.
+static int launch_persistent(const galpy_cuda_launch* L, const KernelInfo& ki, KArgs& A,
+                             cudaStream_t stream)
+{
+  KernelFn fn = ki.fn;
   int dev = 0;
   GPC_CUDA_TRY(cudaGetDevice(&dev));
   int nsm = 0;
@@ -274,10 +267,63 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
   }
   fn<<<(unsigned)grid, block, smem, stream>>>(A);
   cudaError_t le = cudaGetLastError();
-  if (sched) cudaFreeAsync(sched, stream);
   if (le != cudaSuccess)
     return set_error(GALPY_CUDA_ERR_CUDA, std::string("orbit kernel launch: ") + cudaGetErrorString(le));
   return GALPY_CUDA_OK;
+}
+
+// Stream-ordered allocation from `pool`, or from the device's default pool
+// when pool is NULL (the device entry point's documented behaviour).
+static cudaError_t alloc_async(void** p, size_t bytes, cudaMemPool_t pool, cudaStream_t s)
+{
+  return pool ? cudaMallocFromPoolAsync(p, bytes, pool, s) : cudaMallocAsync(p, bytes, s);
+}
+
+static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool progress,
+                         cudaStream_t stream, cudaMemPool_t pool = nullptr)
+{
+  KernelInfo ki;
+  KArgs A;
+  int rc = prepare_launch(L, scratch, progress, ki, A);
+  if (rc) return rc;
+  const int system = launch_system(L);
+  GPC_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(Scratch), stream));
+
+  // longest-first work queue (stream-ordered scratch, freed after the launch);
+  // surface-of-section runs go in order (the cost pass reads orbit states)
+  void* sched = nullptr;
+  if (L->schedule == GALPY_CUDA_SCHED_LONGEST_FIRST && L->nobj > 1 && L->nobj < (1LL << 31) &&
+      system == GALPY_CUDA_SYS_ORBIT) {
+    const int n = (int)L->nobj;
+    size_t tmp_bytes = 0;
+    cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, (float*)nullptr, (float*)nullptr,
+                                              (int*)nullptr, (int*)nullptr, n, 0, 32, stream);
+    const size_t keys = (size_t)n * sizeof(float), vals = (size_t)n * sizeof(int);
+    const size_t off_k2 = keys, off_v1 = 2 * keys, off_v2 = 2 * keys + vals,
+                 off_tmp = (2 * keys + 2 * vals + 255) & ~(size_t)255;
+    GPC_CUDA_TRY(alloc_async(&sched, off_tmp + tmp_bytes, pool, stream));
+    char* base = static_cast<char*>(sched);
+    float* k1 = reinterpret_cast<float*>(base);
+    float* k2 = reinterpret_cast<float*>(base + off_k2);
+    int* v1 = reinterpret_cast<int*>(base + off_v1);
+    int* v2 = reinterpret_cast<int*>(base + off_v2);
+    const unsigned cb = (unsigned)((L->nobj + 255) / 256);
+    if (L->planar)
+      cost_kernel<2><<<cb, 256, 0, stream>>>(A, k1, v1);
+    else
+      cost_kernel<3><<<cb, 256, 0, stream>>>(A, k1, v1);
+    GPC_CUDA_TRY(cudaGetLastError());
+    cudaError_t se = cub::DeviceRadixSort::SortPairsDescending(base + off_tmp, tmp_bytes, k1, k2,
+                                                               v1, v2, n, 0, 32, stream);
+    if (se != cudaSuccess) {
+      cudaFreeAsync(sched, stream);
+      return set_error(GALPY_CUDA_ERR_CUDA, std::string("radix sort: ") + cudaGetErrorString(se));
+    }
+    A.order = v2;
+  }
+  rc = launch_persistent(L, ki, A, stream);
+  if (sched) cudaFreeAsync(sched, stream);
+  return rc;
 }
 
 static int check_launch(const galpy_cuda_launch* L)
@@ -342,25 +388,43 @@ struct DevBuf {
 };
 
 // The blocking entry points allocate their device buffers stream-ordered
-// from the device's default memory pool.  With the pool's default release
-// threshold (0) every call would hand gigabytes back to the driver at its
-// final synchronisation and map them again on the next call; keeping them
-// in the pool (this process's pool only) makes repeated calls allocation-free
-// after the first.
-static void keep_pool_memory()
+// from a memory pool private to the library (one per device and context),
+// whose release threshold keeps freed memory in the pool: with a threshold
+// of 0 every call would hand gigabytes back to the driver at its final
+// synchronisation and map them again on the next call (e2e 4.3e8 vs 9.7e8
+// steps/s on the batching workload).  Being private, the pool changes
+// nothing in the caller's own allocators (the device's default pool keeps
+// its settings); galpy_cuda_trim_memory returns the cached memory.
+static std::mutex g_pool_mutex;
+static cudaMemPool_t g_pool[64] = {nullptr};
+static CUcontext g_pool_ctx[64] = {nullptr};
+
+static int library_pool(cudaMemPool_t* out)
 {
-  static std::mutex m;
-  static bool done[64] = {false};
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
-  std::lock_guard<std::mutex> lock(m);
-  if (done[dev]) return;
-  cudaMemPool_t pool;
-  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-    unsigned long long keep = ~0ULL;
-    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  GPC_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return set_error(GALPY_CUDA_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  CUcontext ctx = current_context();
+  if (!ctx) {  // no context yet: cudaSetDevice initialises the primary one
+    GPC_CUDA_TRY(cudaSetDevice(dev));
+    ctx = current_context();
   }
-  done[dev] = true;
+  if (!g_pool[dev] || ctx != g_pool_ctx[dev]) {
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    GPC_CUDA_TRY(cudaMemPoolCreate(&pool, &props));
+    unsigned long long keep = ~0ULL;
+    GPC_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    g_pool[dev] = pool;
+    g_pool_ctx[dev] = ctx;
+  }
+  *out = g_pool[dev];
+  return GALPY_CUDA_OK;
 }
 
 static int select_device(const galpy_cuda_opts* o)
@@ -369,7 +433,6 @@ static int select_device(const galpy_cuda_opts* o)
   if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1)
     return set_error(GALPY_CUDA_ERR_NODEVICE, "no CUDA device visible");
   if (o && o->device >= 0) GPC_CUDA_TRY(cudaSetDevice(o->device));
-  keep_pool_memory();
   return GALPY_CUDA_OK;
 }
 
@@ -391,6 +454,9 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
   rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
   if (rc == -3) return set_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
   if (rc) return set_error(GALPY_CUDA_ERR_ARG, "invalid potential arguments");
+  cudaMemPool_t pool = nullptr;
+  rc = library_pool(&pool);
+  if (rc) return rc;
 
   cudaStream_t stream, side;
   GPC_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -409,13 +475,13 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
   const size_t n_out = (size_t)nobj * nt * nv;
   DevBuf dw, dt_, dout, derr, dsteps, dcomp, dscr;
   dw.s = dt_.s = dout.s = derr.s = dsteps.s = dcomp.s = dscr.s = stream;
-  GPC_CUDA_TRY(cudaMallocAsync(&dw.p, n_w * sizeof(double), stream));
-  GPC_CUDA_TRY(cudaMallocAsync(&dt_.p, n_t * sizeof(double), stream));
-  GPC_CUDA_TRY(cudaMallocAsync(&dout.p, n_out * sizeof(double), stream));
-  GPC_CUDA_TRY(cudaMallocAsync(&derr.p, (size_t)nobj * sizeof(int), stream));
-  GPC_CUDA_TRY(cudaMallocAsync(&dcomp.p, comps.size() * sizeof(GpComp), stream));
-  GPC_CUDA_TRY(cudaMallocAsync(&dscr.p, sizeof(Scratch), stream));
-  if (o && o->nsteps) GPC_CUDA_TRY(cudaMallocAsync(&dsteps.p, (size_t)nobj * sizeof(long long), stream));
+  GPC_CUDA_TRY(alloc_async(&dw.p, n_w * sizeof(double), pool, stream));
+  GPC_CUDA_TRY(alloc_async(&dt_.p, n_t * sizeof(double), pool, stream));
+  GPC_CUDA_TRY(alloc_async(&dout.p, n_out * sizeof(double), pool, stream));
+  GPC_CUDA_TRY(alloc_async(&derr.p, (size_t)nobj * sizeof(int), pool, stream));
+  GPC_CUDA_TRY(alloc_async(&dcomp.p, comps.size() * sizeof(GpComp), pool, stream));
+  GPC_CUDA_TRY(alloc_async(&dscr.p, sizeof(Scratch), pool, stream));
+  if (o && o->nsteps) GPC_CUDA_TRY(alloc_async(&dsteps.p, (size_t)nobj * sizeof(long long), pool, stream));
   GPC_CUDA_TRY(cudaMemcpyAsync(dw.p, w, n_w * sizeof(double), cudaMemcpyHostToDevice, stream));
   GPC_CUDA_TRY(cudaMemcpyAsync(dt_.p, t, n_t * sizeof(double), cudaMemcpyHostToDevice, stream));
   GPC_CUDA_TRY(cudaMemcpyAsync(dcomp.p, comps.data(), comps.size() * sizeof(GpComp),
@@ -470,7 +536,7 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
   } eg{e0, e1};
   SigintGuard sig;
   GPC_CUDA_TRY(cudaEventRecord(e0, stream));
-  rc = launch_kernel(&L, scr, cb != nullptr, stream);
+  rc = launch_kernel(&L, scr, cb != nullptr, stream, pool);
   if (rc) return rc;
   GPC_CUDA_TRY(cudaEventRecord(e1, stream));
 
@@ -685,11 +751,15 @@ static_assert(sizeof(Scratch) <= kNoAllocCount, "control block too large");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
-// Device address of g_noalloc_scratch per device, looked up once per device
-// (host code must not use the symbol itself: on the host it is only a
-// stand-in for the device object).
+// Device address of g_noalloc_scratch, looked up once per device and
+// context (host code must not use the symbol itself: on the host it is only
+// a stand-in for the device object).  The cache is keyed on the context as
+// well as the ordinal: after cudaDeviceReset the module is loaded again into
+// a new primary context, possibly at another address, and the next call
+// looks the array up again instead of using a stale pointer.
 static std::mutex g_noalloc_mutex;
 static void* g_noalloc_ptr[64] = {nullptr};
+static CUcontext g_noalloc_ctx[64] = {nullptr};
 
 static int noalloc_scratch(void** out)
 {
@@ -697,13 +767,15 @@ static int noalloc_scratch(void** out)
   GPC_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return set_error(GALPY_CUDA_ERR_ARG, "device ordinal out of range");
   std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-  if (!g_noalloc_ptr[dev]) {
+  CUcontext ctx = current_context();
+  if (!g_noalloc_ptr[dev] || !ctx || ctx != g_noalloc_ctx[dev]) {
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess)
       return set_error(GALPY_CUDA_ERR_CUDA,
                        std::string("cudaGetSymbolAddress(noalloc scratch): ") + cudaGetErrorString(e));
     g_noalloc_ptr[dev] = p;
+    g_noalloc_ctx[dev] = current_context();  // the lookup made the primary context current
   }
   *out = g_noalloc_ptr[dev];
   return GALPY_CUDA_OK;
@@ -847,6 +919,29 @@ int galpy_cuda_device_count(void)
   return n;
 }
 
+int galpy_cuda_trim_memory(int device)
+{
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1)
+    return set_error(GALPY_CUDA_ERR_NODEVICE, "no CUDA device visible");
+  int prev = 0;
+  GPC_CUDA_TRY(cudaGetDevice(&prev));
+  const int first = device >= 0 ? device : 0, last = device >= 0 ? device : n - 1;
+  if (first >= n) return set_error(GALPY_CUDA_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  for (int d = first; d <= last && d < 64; d++) {
+    if (!g_pool[d]) continue;
+    GPC_CUDA_TRY(cudaSetDevice(d));
+    // only the pool of the context it was made in (a reset dropped it)
+    if (current_context() == g_pool_ctx[d]) {
+      GPC_CUDA_TRY(cudaDeviceSynchronize());
+      GPC_CUDA_TRY(cudaMemPoolTrimTo(g_pool[d], 0));
+    }
+  }
+  GPC_CUDA_TRY(cudaSetDevice(prev));
+  return GALPY_CUDA_OK;
+}
+
 int galpy_cuda_comp_size(void) { return (int)sizeof(GpComp); }
 
 int galpy_cuda_signature(int npot, const int* pot_type)
@@ -902,47 +997,15 @@ int galpy_cuda_integrate_device_noalloc(const galpy_cuda_launch* L)
   unsigned char* scr = static_cast<unsigned char*>(base);
   Scratch* ctl = reinterpret_cast<Scratch*>(scr + kNoAllocCtl);
   cudaStream_t stream = static_cast<cudaStream_t>(L->stream);
-
-  double scal[kMaxComp * kScalarStride] = {0.0};
-  const bool direct = direct_scalars(L, scal);
-  const int system = launch_system(L);
-  const KernelInfo ki =
-      pick_kernel(L->planar, L->variational, L->precision, L->odeint_type, L->signature,
-                  L->variant, direct, system);
-  KernelFn fn = ki.fn;
-  if (!fn) return set_error(GALPY_CUDA_ERR_METHOD, "method/precision combination not implemented");
+  KernelInfo ki;
   KArgs A;
-  memset(&A, 0, sizeof(A));
-  memcpy(A.scal, scal, sizeof(scal));
-  A.nobj = L->nobj;
-  A.nt = L->nt;
-  A.indiv_t = L->indiv_t;
-  A.t = L->t;
-  A.w0 = L->w0;
-  A.in_layout = L->in_layout;
-  A.out.out = L->out;
-  A.out.layout = L->out_layout;
-  A.out.nt = L->nt;
-  A.out.row0 = L->out_row0;
-  A.out.nobj = L->nobj;
-  A.err = L->err;
-  A.nsteps = L->nsteps;
-  A.comps = static_cast<const GpComp*>(L->comps);
-  A.ncomp = L->ncomp;
-  A.group = L->group;
-  A.dt = L->dt;
-  A.rtol = L->rtol;
-  A.atol = L->atol;
-  A.max_attempts = L->max_attempts;
-  A.counter = &ctl->counter;
-  A.abort_flag = L->abort_flag ? L->abort_flag : &ctl->abort_flag;
-  A.done_count = nullptr;
-  A.variational_nv = L->variational ? (L->planar ? 8 : 12) : 0;
+  rc = prepare_launch(L, ctl, false, ki, A);
+  if (rc) return rc;
   // the array keeps the previous call's contents: zero the control words
   // and the bucket counters (a memset, not an allocation)
   GPC_CUDA_TRY(cudaMemsetAsync(scr, 0, kNoAllocBucket, stream));
   if (L->schedule == GALPY_CUDA_SCHED_LONGEST_FIRST && L->nobj > 1 &&
-      system == GALPY_CUDA_SYS_ORBIT) {
+      launch_system(L) == GALPY_CUDA_SYS_ORBIT) {
     const unsigned nb = (unsigned)((L->nobj + 255) / 256);
     if (L->planar)
       noalloc_bucket_kernel<2><<<nb, 256, 0, stream>>>(A, scr);
@@ -953,25 +1016,7 @@ int galpy_cuda_integrate_device_noalloc(const galpy_cuda_launch* L)
     GPC_CUDA_TRY(cudaGetLastError());
     A.order = reinterpret_cast<const int*>(scr + kNoAllocOrder);
   }
-  int dev = 0, nsm = 0;
-  GPC_CUDA_TRY(cudaGetDevice(&dev));
-  GPC_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  const int block = ki.slot_doubles > 0 ? kSlotStride : (L->block_size > 0 ? L->block_size : 128);
-  if (block > 128 || block % 32)
-    return set_error(GALPY_CUDA_ERR_ARG, "block_size must be 32..128, multiple of 32");
-  const size_t smem = (size_t)ki.slot_doubles * sizeof(double) * block;
-  if (smem > 48 * 1024)
-    GPC_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int per_sm = 0;
-  GPC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem));
-  if (per_sm < 1) per_sm = 1;
-  long long grid = L->grid_size > 0 ? L->grid_size : (long long)nsm * per_sm;
-  const long long need = (L->nobj + block - 1) / block;
-  if (grid > need) grid = need;
-  if (grid < 1) grid = 1;
-  fn<<<(unsigned)grid, block, smem, stream>>>(A);
-  GPC_CUDA_TRY(cudaGetLastError());
-  return GALPY_CUDA_OK;
+  return launch_persistent(L, ki, A, stream);
 }
 
 int integrateFullOrbit_cuda(int nobj, double* yo, int nt, double* t, int indiv_t, int npot,

@@ -24,7 +24,8 @@ dispatch (galpy/orbit/Orbits.py):
   ``integrateFullOrbit_sos_cuda`` and ``integratePlanarOrbit_sos_c`` /
   ``integratePlanarOrbit_sos`` -> ``integratePlanarOrbit_sos_cuda``.
 
-INTEGRATION.md shows the equivalent few-line patch to galpy itself.
+The same routing can be written into galpy itself as a few-line patch of the
+dispatch in ``Orbits._integrate_impl``; these hooks do it at run time.
 """
 import numpy as np
 

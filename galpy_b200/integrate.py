@@ -310,7 +310,7 @@ def integrate_device(comps, ncomp, w0, t, out, err, int_method, planar=False, va
                      out_row0=0, dt=None, rtol=None, atol=None, precision="fp64",
                      max_attempts=0, stream=None, block_size=0, grid_size=0, signature=0,
                      schedule="longest_first", variant=0, comps_host=None, tail_sms=-1,
-                     system="orbit"):
+                     system="orbit", abort_flag=None):
     """Asynchronous integration of device-resident torch tensors.
 
     comps: uint8 CUDA tensor of compiled records (compile_potential); w0
@@ -322,7 +322,12 @@ def integrate_device(comps, ncomp, w0, t, out, err, int_method, planar=False, va
     system 'orbit' (default), or a surface-of-section system ('sos': 3D rows
     of 7, t holding the psi increments; 'sos_planar_x' / 'sos_planar_y':
     planar rows of 5, planar=True) with rk4/rk6/dopr54/dop853 in float64.
-    Runs on `stream` (a torch.cuda.Stream, default: the current stream)."""
+    Runs on `stream` (a torch.cuda.Stream, default: the current stream).
+    abort_flag: optional int32 CUDA tensor (one element) that the kernel polls
+    every 256 loop iterations; once it reads non-zero, the orbits in flight
+    stop with err -10 and NaN rows after their last written one, and orbits
+    not yet started get err -10 and NaN rows (the device form of galpy's
+    SIGINT handling)."""
     import torch
 
     layouts_in = {"aos": _lib.IN_AOS, "soa": _lib.IN_SOA}
@@ -357,7 +362,12 @@ def integrate_device(comps, ncomp, w0, t, out, err, int_method, planar=False, va
     L.rtol = rtol
     L.atol = atol
     L.max_attempts = max_attempts
-    L.abort_flag = None
+    if abort_flag is not None:
+        if not (abort_flag.is_cuda and abort_flag.dtype == torch.int32):
+            raise ValueError("abort_flag must be an int32 CUDA tensor")
+        L.abort_flag = abort_flag.data_ptr()
+    else:
+        L.abort_flag = None
     s = stream if stream is not None else torch.cuda.current_stream(w0.device)
     L.stream = s.cuda_stream
     L.block_size = block_size

@@ -214,8 +214,12 @@ int galpy_cuda_integrate_device(const galpy_cuda_launch *launch);
  * into the library, held by every GPU that loads it until the process exits.
  * Limit: at most 1,048,576 orbits per call (GALPY_CUDA_ERR_ARG beyond that;
  * split the batch).  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress); make that first call before any stream
- * capture.  Every call reuses the same array (the control words are cleared
+ * address (cudaGetSymbolAddress), and so does the first call after the
+ * device's context was reset (cudaDeviceReset); make those calls before any
+ * stream capture.  The launch shape (grid, shared-memory carveout, SMs
+ * reserved for the longest orbits) is that of galpy_cuda_integrate_device;
+ * only the longest-first order differs in detail (64 cost buckets instead of
+ * a sort).  Every call reuses the same array (the control words are cleared
  * at the start of each call), so calls that overlap on the GPU -- on
  * different streams or from different threads -- race: serialise them. */
 int galpy_cuda_integrate_device_noalloc(const galpy_cuda_launch *launch);
@@ -331,6 +335,16 @@ int galpy_cuda_fp64_peak(double *tflops, double *ms);
 int galpy_cuda_abi_version(void);
 const char *galpy_cuda_last_error(void);
 int galpy_cuda_device_count(void);
+
+/* Device memory of the blocking (host-pointer) entry points.  They allocate
+ * their buffers stream-ordered from a memory pool private to this library
+ * (one per device), which keeps freed memory cached for the next call
+ * instead of unmapping and mapping it again each time; the caller's own
+ * allocators, the device's default memory pool included, are left as they
+ * are.  This returns the cached memory of `device` (-1: every device) to
+ * the driver; it synchronises those devices.  No counterpart in the
+ * reference (galpy's C allocates host memory only). */
+int galpy_cuda_trim_memory(int device);
 
 #ifdef __cplusplus
 }

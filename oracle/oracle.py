@@ -42,8 +42,9 @@ def build(ref=False):
     import subprocess
 
     subprocess.run(["make", "-s", "-C", _HERE, "all"], check=True)
-    if ref and os.path.isdir("/root/reference/galpy"):
-        subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+    tree = os.environ.get("GALPY_REFERENCE_TREE", "/root/reference")
+    if ref and os.path.isdir(os.path.join(tree, "galpy")):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", "REF=" + tree], check=True)
 
 
 def port():

@@ -1,16 +1,21 @@
-"""Import galpy from the reference tree without matplotlib (TEST ONLY).
+"""Import galpy without matplotlib (TEST ONLY).
 
 galpy imports matplotlib at module level (galpy/util/plot.py) only for
 plotting; none of the orbit or potential code used by the tests needs it.
 This installs inert stand-ins for matplotlib / mpl_toolkits before importing
-galpy from the reference checkout, when that checkout exists (it does in the
-build container; it does not on GPU machines, where the galpy-based tests
-are skipped)."""
+galpy from, in this order: the reference checkout (GALPY_REFERENCE_TREE,
+where it exists), or the pure-Python galpy installed into baseline/_ref
+(``pip install --no-deps --target baseline/_ref <galpy tree>``: git-ignored,
+but copied with the working tree to GPU machines, so galpy's own
+Orbit.integrate can drive the engine there).  Without either the galpy-based
+tests are skipped."""
 import os
 import sys
 import types
 
 REFERENCE = os.environ.get("GALPY_REFERENCE_TREE", "/root/reference")
+INSTALLED = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                         "baseline", "_ref")
 
 
 class _InertMeta(type):
@@ -51,11 +56,20 @@ _STUBS = ["matplotlib", "matplotlib.pyplot", "matplotlib.ticker", "matplotlib.cm
           "mpl_toolkits.axes_grid1", "matplotlib.gridspec"]
 
 
+def galpy_root():
+    """Directory to put on sys.path for galpy, or None."""
+    for root in (REFERENCE, INSTALLED):
+        if os.path.isfile(os.path.join(root, "galpy", "__init__.py")):
+            return root
+    return None
+
+
 def import_galpy():
-    """Return the galpy module from the reference tree, or None if absent."""
+    """Return the galpy module, or None if no copy is available."""
     if "galpy" in sys.modules:
         return sys.modules["galpy"]
-    if not os.path.isdir(os.path.join(REFERENCE, "galpy")):
+    root = galpy_root()
+    if root is None:
         return None
     try:
         import matplotlib  # noqa: F401
@@ -63,8 +77,8 @@ def import_galpy():
         for name in _STUBS:
             sys.modules.setdefault(name, _StubModule(name))
     os.environ.setdefault("HOME", "/tmp")
-    if REFERENCE not in sys.path:
-        sys.path.insert(0, REFERENCE)
+    if root not in sys.path:
+        sys.path.insert(0, root)
     import galpy
 
     return galpy

@@ -96,6 +96,62 @@ def test_noalloc_matches_allocating_entry_point(schedule):
         assert diff <= 1e-14, (call, diff)
 
 
+@pytest.mark.parametrize("case", ["planar_aos", "variational_aos"])
+def test_noalloc_other_layouts(case):
+    """The bucketed work queue reads the initial positions of planar rows
+    (4 values) and of variational rows (12 values) laid out as AoS: both
+    calls must give the allocating entry point's results bit for bit."""
+    import torch
+
+    import galpy_b200 as gb
+    from galpy_b200 import build
+
+    build.build()
+    lib = _lib.lib()
+    planar = case == "planar_aos"
+    var = case == "variational_aos"
+    pot = gb.MWPotential2014()
+    comps_np, ncomp = gb.compile_potential(pot, planar=planar)
+    sig = gb.signature(pot, planar=planar)
+    dev = torch.device("cuda:0")
+    n = 6000
+    w3, t_np = _workload(n, seed=11)
+    if planar:
+        w = np.stack([w3[0], w3[1], w3[3], w3[4]], 1)  # [n][4] rectangular
+    else:
+        w = np.zeros((n, 12))
+        w[:, :6] = w3.T
+        w[np.arange(n), 6 + np.arange(n) % 6] = 1.0  # one unit deviation per orbit
+    nv = w.shape[1]
+    comps = torch.tensor(comps_np, device=dev)
+    w0 = torch.tensor(np.ascontiguousarray(w), device=dev)
+    t = torch.tensor(t_np, device=dev)
+    method = 3 if var else 6  # variational symplec4 (tangent kicks) / dop853
+
+    def run(entry):
+        out = torch.full((nv, 21, n), float("nan"), dtype=torch.float64, device=dev)
+        err = torch.full((n,), -99, dtype=torch.int32, device=dev)
+        ns = torch.full((n,), -1, dtype=torch.int64, device=dev)
+        L = _launch(comps, ncomp, w0, t, out, err, ns, sig, 1)
+        L.planar, L.variational, L.odeint_type = int(planar), int(var), method
+        L.in_layout = _lib.IN_AOS
+        if var:
+            L.signature = 0
+            L.dt = 0.01
+        rc = entry(ctypes.byref(L))
+        assert rc == 0, _lib.last_error()
+        torch.cuda.synchronize()
+        return out, err, ns
+
+    ref_out, ref_err, ref_ns = run(lib.galpy_cuda_integrate_device)
+    assert (ref_err == 0).all()
+    for call in range(2):
+        out, err, ns = run(lib.galpy_cuda_integrate_device_noalloc)
+        assert torch.equal(err, ref_err) and torch.equal(ns, ref_ns), call
+        diff = (out - ref_out).abs().max().item()
+        assert diff <= 1e-14, (call, diff)
+
+
 def test_noalloc_rejects_oversized_batch():
     import torch
 
