@@ -246,6 +246,11 @@ def main():
     ap.add_argument("--methods-only", action="store_true",
                     help="run only the integrator comparison leg: all seven integrators "
                          "on the same batch, each beside the reference's C on a sample")
+    ap.add_argument("--profile", default=None,
+                    help="profiling case (for ncu): METHOD[:KIND], KIND one of plain, "
+                         "groups, variational, sos; runs one warm-up and one launch of that "
+                         "kernel on a small batch (--orbits, default 65,536) and prints its "
+                         "time, nothing else")
     ap.add_argument("--case", default="batching", choices=["batching", "uniform", "longest"],
                     help="uniform: R ~ U(0.5, 2), shared t in [0, 50] (101 snapshots) "
                          "(a throughput-bound case for profiling the same kernel); longest: "
@@ -278,6 +283,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=dev)
         pg = dist
+
+    if args.profile:
+        n = args.orbits if args.orbits != N_ORBITS else 65536
+        print(json.dumps(profile_leg(gb, torch, dev, args.profile, n)), flush=True)
+        return
 
     if args.grad_only:
         peak = ctypes_fp64_peak(_lib)
@@ -597,6 +607,86 @@ def methods_leg(gb, torch, dev, stream, pg, peak, rank, cpu=True, n=131072, K=3,
     # launches come before)
     res["gpu_launches"] = 2 * (K + W) * len(METHOD_FLOPS)
     return res
+
+
+def profile_leg(gb, torch, dev, spec, n):
+    """One warm-up and one timed launch of a single kernel on a small batch,
+    for profiler captures (`ncu -k regex:<machine> -s 1 -c 1`):
+
+      plain        config-0 initial conditions (R ~ U(0.5, 2)), t in [0, 20]
+                   with 101 snapshots, galpy's default tolerances 1e-12 and
+                   estimated step, MWPotential2014 (compile-time list)
+      groups       the same orbits split over 64 MWPotential2014 variants of
+                   the ragged configuration (parameter-group kernel), dop853
+                   rtol = atol = 1e-9
+      variational  3D variational integration (12-D state, one unit
+                   deviation per orbit), t in [0, 20], 21 rows
+      sos          3D surface of section, psi in [0, 20 pi] with 21 rows
+      uniform      R ~ U(0.5, 2) (seed 1), per-orbit copies of t in [0, 50]
+                   with 101 snapshots, rtol = atol = 1e-10: the batching
+                   workload's kernel on orbits of similar length
+
+    A third field selects the register variant (METHOD:KIND:VARIANT)."""
+    method, _, rest = spec.partition(":")
+    kind, _, variant = rest.partition(":")
+    kind = kind or "plain"
+    stream = torch.cuda.current_stream(dev)
+    pt, pa = mw14_args()
+    ics, _ = precision_workload(n, seed=1 if kind == "uniform" else 5)
+    kw = {"variant": int(variant or 0)}
+    group = None
+    if kind == "groups":
+        pt, args, _, _, _ = ragged_workload(ngroup=512)
+        args = args[:64]
+        comps, ncomp = gb.compile_potential((pt, args.ravel()), ngroup=len(args))
+        group = torch.tensor(np.arange(n, dtype=np.int32) % len(args), device=dev)
+        sig = gb.signature((pt, args[0]))
+        kw.update(rtol=1e-9, atol=1e-9)
+    else:
+        comps, ncomp = gb.compile_potential((pt, pa))
+        sig = gb.signature((pt, pa))
+        if kind in ("plain", "uniform"):
+            kw["comps_host"] = comps
+    comps_d = torch.tensor(comps, device=dev)
+    w = cyl_to_rect(ics)
+    nv = 6
+    t = np.linspace(0.0, 20.0, 101)
+    if kind == "uniform":
+        t = np.repeat(np.linspace(0.0, 50.0, NT)[None, :], n, axis=0)
+        kw.update(rtol=RTOL, atol=ATOL)
+    elif kind == "variational":
+        w = np.concatenate([w, np.zeros((n, 6))], 1)
+        w[np.arange(n), 6 + np.arange(n) % 6] = 1.0
+        nv, t = 12, np.linspace(0.0, 20.0, 21)
+        kw["variational"] = True
+        sig = 0
+    elif kind == "sos":
+        # (x, y, vx, vy, A, t, psi) from the cylindrical initial conditions
+        R, vR, vT, z, vz, phi = ics.T
+        c, s = np.cos(phi), np.sin(phi)
+        w = np.stack([R * c, R * s, vR * c - vT * s, vR * s + vT * c, np.hypot(z, vz),
+                      np.zeros(n), np.arctan2(z, vz)], 1)
+        nv, t = 7, np.linspace(0.0, 20 * np.pi, 21)
+        kw["system"] = "sos"
+        sig = 0
+    w0 = torch.tensor(np.ascontiguousarray(w.T), device=dev)
+    t_d = torch.tensor(t, device=dev)
+    out = torch.empty((nv, len(t), n), dtype=torch.float64, device=dev)
+    err = torch.empty(n, dtype=torch.int32, device=dev)
+    ns = torch.empty(n, dtype=torch.int64, device=dev)
+    ms = []
+    for rep in range(2):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        gb.integrate_device(comps_d, ncomp, w0, t_d, out, err, method + "_cuda", nsteps=ns,
+                            group=group, signature=sig, stream=stream, **kw)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return {"profile": spec, "orbits": n, "ms": ms[-1],
+            "accepted_steps": float(ns.sum().item()),
+            "orbits_with_err": int((err != 0).sum().item())}
 
 
 def ragged_leg(gb, torch, dev, stream, pg):

@@ -182,6 +182,13 @@ static bool direct_scalars(const galpy_cuda_launch* L, double* scal)
   return true;
 }
 
+// Stream-ordered allocation from `pool`, or from the device's default pool
+// when pool is NULL (the device entry point's documented behaviour).
+static cudaError_t alloc_async(void** p, size_t bytes, cudaMemPool_t pool, cudaStream_t s)
+{
+  return pool ? cudaMallocFromPoolAsync(p, bytes, pool, s) : cudaMallocAsync(p, bytes, s);
+}
+
 // Kernel and kernel arguments of a launch, with the control words pointed
 // into `scratch` (a Scratch in device memory, cleared by the caller).
 static int prepare_launch(const galpy_cuda_launch* L, Scratch* scratch, bool progress,
@@ -226,8 +233,12 @@ static int prepare_launch(const galpy_cuda_launch* L, Scratch* scratch, bool pro
 // Grid of the persistent kernel (one wave: SMs x resident blocks), its
 // shared memory and carveout, the SMs reserved for the longest orbits, and
 // the launch.  Shared by the allocating and the allocation-free entry points.
+// queue: give DOP853 kernels their dense-output request rings (allocated
+// stream-ordered from `pool`, or the default pool when NULL, and freed after
+// the launch); without it their dense output runs in the warps' slot cycle.
 static int launch_persistent(const galpy_cuda_launch* L, const KernelInfo& ki, KArgs& A,
-                             cudaStream_t stream)
+                             cudaStream_t stream, bool queue = false,
+                             cudaMemPool_t pool = nullptr)
 {
   KernelFn fn = ki.fn;
   int dev = 0;
@@ -265,18 +276,19 @@ static int launch_persistent(const galpy_cuda_launch* L, const KernelInfo& ki, K
     A.tail_sms = tail_sms;
     A.tail_len = 32LL * tail_sms;
   }
+  void* dq = nullptr;
+  A.dense_q = nullptr;
+  if (queue && ki.queue_doubles > 0) {
+    const size_t bytes = (size_t)grid * (block / 32) * ki.queue_doubles * sizeof(double);
+    GPC_CUDA_TRY(alloc_async(&dq, bytes, pool, stream));
+    A.dense_q = static_cast<double*>(dq);
+  }
   fn<<<(unsigned)grid, block, smem, stream>>>(A);
   cudaError_t le = cudaGetLastError();
+  if (dq) cudaFreeAsync(dq, stream);
   if (le != cudaSuccess)
     return set_error(GALPY_CUDA_ERR_CUDA, std::string("orbit kernel launch: ") + cudaGetErrorString(le));
   return GALPY_CUDA_OK;
-}
-
-// Stream-ordered allocation from `pool`, or from the device's default pool
-// when pool is NULL (the device entry point's documented behaviour).
-static cudaError_t alloc_async(void** p, size_t bytes, cudaMemPool_t pool, cudaStream_t s)
-{
-  return pool ? cudaMallocFromPoolAsync(p, bytes, pool, s) : cudaMallocAsync(p, bytes, s);
 }
 
 static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool progress,
@@ -321,7 +333,7 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
     }
     A.order = v2;
   }
-  rc = launch_persistent(L, ki, A, stream);
+  rc = launch_persistent(L, ki, A, stream, true, pool);
   if (sched) cudaFreeAsync(sched, stream);
   return rc;
 }

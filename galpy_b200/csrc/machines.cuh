@@ -1199,7 +1199,12 @@ struct Dop853Machine : OrbitCommon {
   static constexpr int kSlotDoubles = kSlots * N;
   double y0[N], k1[N];
   double* ks;  // slot store: slot s >= 1 at ks[((s - 1) * N + i) * kSlotStride]
-  GPC_HD GPC_FI void bind(double* base) { ks = base; }
+  GPC_HD GPC_FI void bind(double* base, bool queue = false)
+  {
+    ks = base;
+    queued = queue;
+    want_enqueue = false;
+  }
   GPC_HD GPC_FI double& K(int s, int i) const { return ks[((s - 1) * N + i) * kSlotStride]; }
   double h, hnew, hmax, pos_neg, facold, rtol, atol;
   double t_current, t_old, t_old_older, dnf;
@@ -1356,6 +1361,15 @@ struct Dop853Machine : OrbitCommon {
     if (stage == ST_FSAL) {
       nsteps++;
       if (output_pending()) {
+        if (queued) {
+          // the rows of this step go to the warp's queue: the kernel writes
+          // the request, then calls finish_step
+          jf = iout + 1;
+          while (output_pending()) iout++;
+          jl = iout;
+          want_enqueue = true;
+          return;
+        }
         stage = ST_S14;
         return;
       }
@@ -1368,37 +1382,157 @@ struct Dop853Machine : OrbitCommon {
     }
     // ST_S16: dense output (leung_dop853.c:441-474), d = stage-16 derivative
     while (output_pending()) {
-      const double sv = (t[iout + 1] - t_old) / h, s1 = 1.0 - sv;
+      const double sv = (t[iout + 1] - t_old) / h;
       double v[N];
 #pragma unroll
-      for (int i = 0; i < N; i++) {
-        const double k1 = this->k1[i], k2 = K(K2, i), k3 = K(K3, i), k4 = K(K4, i);
-        const double k6 = K(K6, i), k7 = K(K7, i), k8 = K(K8, i), k9 = K(K9, i);
-        const double k10 = K(K10, i), s14 = K(S14, i), s15 = K(S15, i);
-        const double rc1 = y0[i];
-        const double ydiff = K(K5, i) - y0[i];
-        const double bspl = h * k1 - ydiff;
-        const double rc4 = ydiff - h * k4 - bspl;
-        double rc5 = d41 * k1 + d46 * k6 + d47 * k7 + d48 * k8 + d49 * k9 + d410 * k10 +
-                     d411 * k2 + d412 * k3;
-        double rc6 = d51 * k1 + d56 * k6 + d57 * k7 + d58 * k8 + d59 * k9 + d510 * k10 +
-                     d511 * k2 + d512 * k3;
-        double rc7 = d61 * k1 + d66 * k6 + d67 * k7 + d68 * k8 + d69 * k9 + d610 * k10 +
-                     d611 * k2 + d612 * k3;
-        double rc8 = d71 * k1 + d76 * k6 + d77 * k7 + d78 * k8 + d79 * k9 + d710 * k10 +
-                     d711 * k2 + d712 * k3;
-        rc5 = h * (rc5 + d413 * k4 + d414 * s14 + d415 * s15 + d416 * d[i]);
-        rc6 = h * (rc6 + d513 * k4 + d514 * s14 + d515 * s15 + d516 * d[i]);
-        rc7 = h * (rc7 + d613 * k4 + d614 * s14 + d615 * s15 + d616 * d[i]);
-        rc8 = h * (rc8 + d713 * k4 + d714 * s14 + d715 * s15 + d716 * d[i]);
-        v[i] = rc1 +
-               sv * (ydiff +
-                     s1 * (bspl + sv * (rc4 + s1 * (rc5 + sv * (rc6 + s1 * (rc7 + sv * rc8))))));
-      }
+      for (int i = 0; i < N; i++)
+        v[i] = dense_value(sv, h, y0[i], K(K5, i), k1[i], K(K2, i), K(K3, i), K(K4, i),
+                           K(K6, i), K(K7, i), K(K8, i), K(K9, i), K(K10, i), K(S14, i),
+                           K(S15, i), d[i]);
       iout++;
       out(iout, v);
     }
     finish_step(out);
+  }
+
+  // One component of the dense output at s = sv of a step of size h from
+  // y0 to y1 (leung_dop853.c:441-474): k1 the step's first derivative,
+  // k2 / k3 the stage-11 / stage-12 derivatives (kept in the K2 / K3 slots,
+  // as the reference reuses k2 and k3), k4 = f(y1), k6..k10 the stage
+  // derivatives, s14..s16 the three dense-output stages.  Shared by the
+  // in-slot and the queued dense output, so both give the same rows.
+  GPC_HD GPC_FI static double dense_value(double sv, double h, double y0, double y1, double k1,
+                                          double k2, double k3, double k4, double k6,
+                                          double k7, double k8, double k9, double k10,
+                                          double s14, double s15, double s16)
+  {
+    using namespace dp;
+    const double s1 = 1.0 - sv;
+    const double rc1 = y0;
+    const double ydiff = y1 - y0;
+    const double bspl = h * k1 - ydiff;
+    const double rc4 = ydiff - h * k4 - bspl;
+    double rc5 = d41 * k1 + d46 * k6 + d47 * k7 + d48 * k8 + d49 * k9 + d410 * k10 +
+                 d411 * k2 + d412 * k3;
+    double rc6 = d51 * k1 + d56 * k6 + d57 * k7 + d58 * k8 + d59 * k9 + d510 * k10 +
+                 d511 * k2 + d512 * k3;
+    double rc7 = d61 * k1 + d66 * k6 + d67 * k7 + d68 * k8 + d69 * k9 + d610 * k10 +
+                 d611 * k2 + d612 * k3;
+    double rc8 = d71 * k1 + d76 * k6 + d77 * k7 + d78 * k8 + d79 * k9 + d710 * k10 +
+                 d711 * k2 + d712 * k3;
+    rc5 = h * (rc5 + d413 * k4 + d414 * s14 + d415 * s15 + d416 * s16);
+    rc6 = h * (rc6 + d513 * k4 + d514 * s14 + d515 * s15 + d516 * s16);
+    rc7 = h * (rc7 + d613 * k4 + d614 * s14 + d615 * s15 + d616 * s16);
+    rc8 = h * (rc8 + d713 * k4 + d714 * s14 + d715 * s15 + d716 * s16);
+    return rc1 +
+           sv * (ydiff + s1 * (bspl + sv * (rc4 + s1 * (rc5 + sv * (rc6 + s1 * (rc7 + sv * rc8))))));
+  }
+
+  // ---- queued dense output ---------------------------------------------
+  // With a request queue (the kernel's per-warp ring in global memory), a
+  // step that contains output times does not run the three dense-output
+  // stages in the warp's slot cycle, where the other lanes of the warp would
+  // sit idle for them: the lane writes the step's data to the queue and goes
+  // on with its next step, and the warp later runs the dense stages of 32
+  // queued requests side by side (one per lane).  The rows are the same as
+  // the in-slot dense output's (same arithmetic, dense_value).
+  //
+  // Request record, field-major with kQueueSlots slots per field (component
+  // i of vector field f of slot p at q[(f * N + i) * kQueueSlots + p]):
+  //   vector fields 0 y0, 1 k1, 2..10 the slot store K2..K10 (K5 = y1,
+  //   K4 = f(y1)); then scalars h, t_old, the orbit index and the row range
+  //   (first << 32 | last) at q[(11 N + k) * kQueueSlots + p], k = 0..3.
+  static constexpr int kQueueSlots = 64;
+  static constexpr int kQueueFields = 11 * N + 4;  // doubles per slot
+  static constexpr bool kQueue = SYS::kRow == ROW_ORBIT && !VAR;
+  bool queued;        // dense output through the warp's queue
+  bool want_enqueue;  // this step's dense output waits for the queue
+  int jf, jl;         // rows of the pending request
+
+  GPC_HD GPC_FI void write_request(double* q, int p, long long orbit) const
+  {
+    constexpr int QS = kQueueSlots;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+      q[(0 * N + i) * QS + p] = y0[i];
+      q[(1 * N + i) * QS + p] = k1[i];
+    }
+#pragma unroll
+    for (int s = 1; s <= 9; s++)
+#pragma unroll
+      for (int i = 0; i < N; i++) q[((1 + s) * N + i) * QS + p] = K(s, i);
+    q[(11 * N + 0) * QS + p] = h;
+    q[(11 * N + 1) * QS + p] = t_old;
+    long long* qi = reinterpret_cast<long long*>(q);
+    qi[(11 * N + 2) * QS + p] = orbit;
+    qi[(11 * N + 3) * QS + p] = ((long long)jf << 32) | (long long)(unsigned)jl;
+  }
+
+  // Slot s of request p: s = 0 its k1, 1..9 its K2..K10, 10 / 11 the dense
+  // stages S14 / S15, which the round keeps in this lane's own slot store
+  // (unused by the lane's orbit when dense output is queued).
+  GPC_HD GPC_FI double req_k(const double* q, int p, int s, int i) const
+  {
+    return s <= 9 ? q[((1 + s) * N + i) * kQueueSlots + p] : K(s, i);
+  }
+
+  // Input of dense stage `stage` (14, 15, 16) of request p: the table loop
+  // of point() over the request's slots.
+  GPC_HD GPC_FI void req_point(double* y, int stage, const double* q, int p) const
+  {
+    const DopStageTable& tb = dop_table();
+    const int n = tb.nterm[stage];
+    double acc[N];
+    {
+      const double c0 = tb.coef[stage][0];
+#pragma unroll
+      for (int i = 0; i < N; i++) acc[i] = c0 * q[(1 * N + i) * kQueueSlots + p];
+    }
+#pragma unroll 4
+    for (int tt = 1; tt < n; tt++) {
+      const int s = tb.slot[stage][tt];
+      const double c = tb.coef[stage][tt];
+#pragma unroll
+      for (int i = 0; i < N; i++) acc[i] += c * req_k(q, p, s, i);
+    }
+    const double hq = q[(11 * N) * kQueueSlots + p];
+#pragma unroll
+    for (int i = 0; i < N; i++) y[i] = q[(0 * N + i) * kQueueSlots + p] + hq * acc[i];
+  }
+
+  // Derivative of dense stage `stage` at request p: stages 14 and 15 are
+  // kept for the next stage inputs; stage 16 completes the rows.
+  template <class W>
+  GPC_HD void req_consume(const double* y, const double* a, int stage, const double* q, int p,
+                          const double* tt, W& out)
+  {
+    double d[N];
+    SYS::deriv(y, a, d);
+    if (stage < ST_S16) {
+      const int s = stage == ST_S14 ? S14 : S15;
+#pragma unroll
+      for (int i = 0; i < N; i++) K(s, i) = d[i];
+      return;
+    }
+    constexpr int QS = kQueueSlots;
+    const double hq = q[(11 * N) * QS + p], told = q[(11 * N + 1) * QS + p];
+    const long long rr = reinterpret_cast<const long long*>(q)[(11 * N + 3) * QS + p];
+    const int j0 = (int)(rr >> 32), j1 = (int)(unsigned)(rr & 0xffffffffLL);
+    for (int j = j0; j <= j1; j++) {
+      const double sv = (tt[j] - told) / hq;
+      double v[N];
+      // one component at a time: unrolled, the compiler would issue all
+      // 14 N loads of the record at once and hold them in registers
+#pragma unroll 1
+      for (int i = 0; i < N; i++)
+        v[i] = dense_value(sv, hq, q[(0 * N + i) * QS + p], q[((1 + K5) * N + i) * QS + p],
+                           q[(1 * N + i) * QS + p], q[((1 + K2) * N + i) * QS + p],
+                           q[((1 + K3) * N + i) * QS + p], q[((1 + K4) * N + i) * QS + p],
+                           q[((1 + K6) * N + i) * QS + p], q[((1 + K7) * N + i) * QS + p],
+                           q[((1 + K8) * N + i) * QS + p], q[((1 + K9) * N + i) * QS + p],
+                           q[((1 + K10) * N + i) * QS + p], K(S14, i), K(S15, i), d[i]);
+      out(j, v);
+    }
   }
 
   GPC_HD void after_stage12()
@@ -1500,6 +1634,39 @@ GPC_HD void fill_unreached_rows(const M& m, W& out)
 #pragma unroll
   for (int k = 0; k < M::NV; k++) v[k] = NAN;
   for (int j = m.iout + 1; j < m.nt; j++) out(j, v);
+}
+
+// One orbit through the queued dense output with a queue of one request
+// that is served as soon as it is written (the host test harness's check of
+// the request record and the dense rounds' arithmetic; the kernel serves 32
+// requests of a warp at a time).  m must be bound with queue = true; q holds
+// Dop853Machine::kQueueFields * kQueueSlots doubles; tt are the orbit's
+// output times.
+template <class M, class F, class W>
+GPC_HD void run_orbit_queued(M& m, F& force, W& out, double* q, const double* tt,
+                             long long orbit)
+{
+  double y[M::NY], qq[M::NA], a[M::NA];
+  int slot = 0;
+  while (!m.done) {
+    m.point(y, slot);
+    M::pos(y, qq);
+    force(qq, a);
+    m.consume(y, a, out, slot);
+    if (slot == 11 && m.want_enqueue) {
+      m.write_request(q, 0, orbit);
+      m.want_enqueue = false;
+      m.finish_step(out);
+      for (int stage = 14; stage <= 16; stage++) {
+        m.req_point(y, stage, q, 0);
+        M::pos(y, qq);
+        force(qq, a);
+        m.req_consume(y, a, stage, q, 0, tt, out);
+      }
+    }
+    slot = slot == 11 ? 0 : slot + 1;
+  }
+  fill_unreached_rows(m, out);
 }
 
 // Per-orbit driver used by the kernels and by the host test harness: run one

@@ -9,6 +9,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <type_traits>
+
 #include "../../include/galpy_cuda.h"
 #include "machines.cuh"
 
@@ -42,9 +44,22 @@ struct KArgs {
   int tail_sms;
   unsigned long long* tail_counter;
   unsigned* sm_claim;
+  // DOP853 dense-output request queues, one ring of M::kQueueSlots records
+  // per warp of the grid (NULL: dense output in the warp's slot cycle)
+  double* dense_q;
   // scalar parameters of the (single) potential, read from the constant bank
   // by the kernels whose POT takes them directly
   double scal[kMaxComp * kScalarStride];
+};
+
+// Whether machine M can queue its dense output (M::kQueue, default false).
+template <class M, class = void>
+struct QueueOf {
+  static constexpr bool value = false;
+};
+template <class M>
+struct QueueOf<M, std::void_t<decltype(M::kQueue)>> {
+  static constexpr bool value = M::kQueue;
 };
 
 template <int NV, int D, bool CYL_OK, int ROW>
@@ -77,6 +92,156 @@ __device__ __forceinline__ bool tail_claimed(const KArgs& A)
   return false;
 }
 
+// Next orbit of a worker: the reserved-SM tail queue first (tail role), then
+// the main queue; -1 when both are exhausted.
+__device__ __forceinline__ long long next_orbit(const KArgs& A, int& my_role)
+{
+  long long q = -1;
+  if (my_role == 1) {
+    q = (long long)atomicAdd(A.tail_counter, 1ULL);
+    if (q >= A.tail_len) {
+      q = -1;
+      my_role = 0;
+    }
+  }
+  if (q < 0 && A.tail_len > 0 && !tail_claimed(A)) {
+    // no reserved SM hosts a tail warp: the longest orbits go first here
+    q = (long long)atomicAdd(A.tail_counter, 1ULL);
+    if (q >= A.tail_len) q = -1;
+  }
+  if (q < 0) {
+    q = (long long)atomicAdd(A.counter, 1ULL) + A.tail_len;
+    if (q >= A.nobj) {
+      if (A.tail_len == 0) return -1;
+      q = (long long)atomicAdd(A.tail_counter, 1ULL);
+      if (q >= A.tail_len) return -1;
+    }
+  }
+  return A.order ? A.order[q] : q;
+}
+
+#if defined(__CUDACC__)
+// The persistent loop of a machine whose dense output goes through the
+// warp's request queue (Dop853Machine with KArgs::dense_q set).  The slot
+// cycle of an attempt is slots 0..10 (stages 2..12) and 11 (the FSAL
+// evaluation); after slot 11 the lanes whose step contains output times
+// append a request to the warp's ring (ballot + prefix count, so the
+// records are contiguous), and whenever 32 or more requests wait -- or the
+// warp has no orbits left -- slots 12..14 are a dense round: lane L runs the
+// three dense stages of request head + L and writes its rows.  Every lane of
+// the warp stays in the loop until the warp has no orbit and no request
+// left (the ballots need all 32 lanes), so a lane without an orbit idles
+// instead of leaving.
+template <class M, int D, int PREC, bool VAR, class POT>
+__device__ __forceinline__ void queued_loop(const KArgs& A, double* slot_store, int my_role)
+{
+  constexpr bool CYL_OK = !VAR;
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr int QS = M::kQueueSlots;
+  using Rows = DevRows<M::NV, D, CYL_OK, M::kRow>;
+  const int lane = threadIdx.x & 31;
+  const long long warp_id = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  double* const q = A.dense_q + warp_id * (long long)(M::kQueueFields * QS);
+  M m;
+  m.bind(slot_store + threadIdx.x, true);
+  long long i = 0;
+  bool active = false, aborting = false, idle = false;
+  const GpComp* comps = A.comps;
+  unsigned iter = 0;
+  int slot = 0, qhead = 0, qcount = 0, nround = 0;
+  for (;;) {
+    const bool dense = slot >= 12;
+    if (!dense && !active && !idle) {
+      const long long o = next_orbit(A, my_role);
+      if (o < 0) {
+        idle = true;
+      } else if (aborting) {
+        A.err[o] = E_ABORT;
+        write_nan_rows<M::NV, D, CYL_OK, M::kRow>(A.out, o, 0);
+      } else {
+        i = o;
+        double w[M::NV];
+        load_state<M>(A, i, w);
+        comps = A.comps + (A.group ? (long long)A.group[i] * A.ncomp : 0LL);
+        Rows rows{&A.out, i};
+        m.init(w, A.t + (A.indiv_t ? i * (long long)A.nt : 0LL), A.nt, A.dt, A.rtol, A.atol,
+               A.max_attempts, rows);
+        active = true;
+      }
+    }
+    const int p = (qhead + lane) & (QS - 1);
+    if (dense ? lane < nround : (active && !m.done)) {
+      double y[M::NY], qq[M::NA], a[M::NA];
+      long long o = i;
+      const GpComp* cp = comps;
+      if (dense) {  // the request's orbit and its parameter group
+        o = reinterpret_cast<const long long*>(q)[(11 * M::N + 2) * QS + p];
+        cp = A.comps + (A.group ? (long long)A.group[o] * A.ncomp : 0LL);
+        m.req_point(y, slot + 2, q, p);
+      } else {
+        m.point(y, slot);
+      }
+      M::pos(y, qq);
+      eval_force<D, PREC, VAR, POT>(cp, A.ncomp, qq, a, A.scal);
+      Rows rows{&A.out, o};
+      if (dense)
+        m.req_consume(y, a, slot + 2, q, p, A.t + (A.indiv_t ? o * (long long)A.nt : 0LL), rows);
+      else
+        m.consume(y, a, rows, slot);
+    }
+    // the requests of this slot's accepted steps (only the FSAL slot makes any)
+    if (slot == 11) {
+      const unsigned want = __ballot_sync(FULL, m.want_enqueue);
+      if (m.want_enqueue) {
+        const int rank = __popc(want & ((1u << lane) - 1u));
+        m.write_request(q, (qhead + qcount + rank) & (QS - 1), i);
+        m.want_enqueue = false;
+        Rows rows{&A.out, i};
+        m.finish_step(rows);
+      }
+      qcount += __popc(want);
+    }
+    const bool all_idle = __all_sync(FULL, idle);
+    // next slot (uniform over the warp)
+    if (slot == 14) {
+      __syncwarp();  // every lane has read its request before the slots are reused
+      qhead = (qhead + nround) & (QS - 1);
+      qcount -= nround;
+      nround = 0;
+    }
+    if (slot == 11 || slot == 14 || (all_idle && !dense)) {
+      if (qcount >= 32 || (all_idle && qcount > 0)) {
+        __syncwarp();  // the records of the ring are visible to every lane
+        nround = qcount < 32 ? qcount : 32;
+        slot = 12;
+      } else {
+        slot = 0;
+      }
+    } else {
+      slot++;
+    }
+    if (all_idle && qcount == 0 && nround == 0) break;
+    ++iter;
+    if (A.abort_flag && ((iter & 255u) == 0u) &&
+        *reinterpret_cast<const volatile int*>(A.abort_flag)) {
+      aborting = true;
+      if (active && !m.done) {
+        m.err = E_ABORT;
+        m.done = true;
+      }
+    }
+    if (active && m.done) {
+      Rows rows{&A.out, i};
+      fill_unreached_rows(m, rows);
+      A.err[i] = m.err;
+      if (A.nsteps) A.nsteps[i] = m.nsteps;
+      if (A.done_count) atomicAdd(A.done_count, 1ULL);
+      active = false;
+    }
+  }
+}
+#endif
+
 // MINB: minimum resident blocks per SM requested from the register
 // allocator (1 = no cap; larger values trade registers for occupancy).
 template <class M, int D, int PREC, bool VAR, class POT, int MINB>
@@ -102,6 +267,12 @@ __global__ void __launch_bounds__(128, MINB) orbit_kernel(const __grid_constant_
   __syncthreads();
   int my_role = role;
   if (my_role == 2 || (my_role == 1 && threadIdx.x >= 32)) return;
+  if constexpr (QueueOf<M>::value) {
+    if (A.dense_q) {
+      queued_loop<M, D, PREC, VAR, POT>(A, slot_store, my_role);
+      return;
+    }
+  }
   M m;
   m.bind(slot_store + threadIdx.x);
   long long i = 0;
@@ -186,8 +357,18 @@ using KernelFn = void (*)(const KArgs);
 
 struct KernelInfo {
   KernelFn fn = nullptr;
-  int slot_doubles = 0;  // per-thread shared-memory slot store (doubles)
+  int slot_doubles = 0;   // per-thread shared-memory slot store (doubles)
+  int queue_doubles = 0;  // per-warp dense-output request ring (doubles; 0: none)
 };
+
+template <class M>
+constexpr int queue_doubles_of()
+{
+  if constexpr (QueueOf<M>::value)
+    return M::kQueueFields * M::kQueueSlots;
+  else
+    return 0;
+}
 
 // Register-budget variants (chosen by the autotuner, galpy_b200/autotune.py):
 // variant 0 lets the compiler use up to 255 registers; variant 1 caps them
@@ -207,6 +388,7 @@ static KernelInfo info_of(int variant)
       k.fn = orbit_kernel<M, D, PREC, VAR, POT, 1>;
   }
   k.slot_doubles = M::kSlotDoubles;
+  k.queue_doubles = queue_doubles_of<M>();
   return k;
 }
 

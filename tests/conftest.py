@@ -94,6 +94,29 @@ class Harness:
         assert rc == 0, rc
         return out, err, ns
 
+    def dop853_queued(self, w, t, pot_type, pot_args, planar=False, rtol=None, atol=None,
+                      max_attempts=0):
+        """DOP853 with its dense output through the kernels' request record
+        (served one request at a time); same return values as integrate."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        t = np.ascontiguousarray(t, dtype=np.float64)
+        n, nv = w.shape
+        nt = t.shape[-1]
+        out = np.zeros((n, nt, nv))
+        err = np.zeros(n, np.int32)
+        ns = np.zeros(n, np.int64)
+        pt = np.ascontiguousarray(pot_type, np.int32)
+        pa = np.ascontiguousarray(pot_args, np.float64)
+        r = -12 * np.log(10) if rtol is None else np.log(rtol)
+        a = -12 * np.log(10) if atol is None else np.log(atol)
+        rc = self.lib.harness_dop853_queued(
+            int(planar), n, w.ctypes.data_as(_dp), nt, t.ctypes.data_as(_dp), int(t.ndim > 1),
+            len(pt), pt.ctypes.data_as(_ip), pa.ctypes.data_as(_dp), ctypes.c_double(r),
+            ctypes.c_double(a), ctypes.c_longlong(max_attempts), out.ctypes.data_as(_dp),
+            err.ctypes.data_as(_ip), ns.ctypes.data_as(_lp))
+        assert rc == 0, rc
+        return out, err, ns
+
     def integrate_sos(self, w, psi, pot_type, pot_args, method, dpsi=None, rtol=None,
                       atol=None, max_attempts=0, surface=None):
         """SOS machines on SOS states: 3D w [n][7], or planar w [n][5] with

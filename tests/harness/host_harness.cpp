@@ -107,6 +107,60 @@ extern "C" int harness_integrate(int planar, int var, int method, int prec, int 
 #undef HARNESS_ARGS
 }
 
+// DOP853 with its dense output through the request record (the kernels'
+// queued dense output, served one request at a time): same outputs as
+// harness_integrate's in-slot dense output, bit for bit.
+template <int D, class POT>
+static void run_dop853_queued(int nobj, const double* w, int nt, const double* t, int indiv_t,
+                              const GpComp* comps, int ncomp, double rtol, double atol,
+                              long long max_att, double* out, int* err, long long* nsteps)
+{
+  using M = Dop853Machine<D, false>;
+  Force<D, PREC_FP64, false, POT> f{comps, ncomp, {}};
+  for (int k = 0; k < ncomp; k++)
+    for (int j = 0; j < kScalarStride; j++) f.scal[k * kScalarStride + j] = comps[k].c[j];
+  std::vector<double> store((size_t)M::kSlotDoubles * kSlotStride + 1);
+  std::vector<double> q((size_t)M::kQueueFields * M::kQueueSlots);
+  for (long long i = 0; i < nobj; i++) {
+    M m;
+    m.bind(store.data(), true);
+    Rows r{out, M::NV, nt, i};
+    const double* tt = t + (indiv_t ? i * nt : 0);
+    m.init(w + i * M::NV, tt, nt, kDtSentinel, rtol, atol, max_att, r);
+    run_orbit_queued(m, f, r, q.data(), tt, i);
+    err[i] = m.err;
+    if (nsteps) nsteps[i] = m.nsteps;
+  }
+}
+
+extern "C" int harness_dop853_queued(int planar, int nobj, const double* w, int nt,
+                                     const double* t, int indiv_t, int npot, const int* pot_type,
+                                     const double* pot_args, double rtol, double atol,
+                                     long long max_att, double* out, int* err, long long* nsteps)
+{
+  std::vector<GpComp> comps(npot);
+  int rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
+  if (rc) return rc;
+  const bool mw14 = npot == 3 && pot_type[0] == T_PSWC && pot_type[1] == T_MN &&
+                    pot_type[2] == T_NFW;
+  if (planar) {
+    if (mw14)
+      run_dop853_queued<2, MW14Pot>(nobj, w, nt, t, indiv_t, comps.data(), npot, rtol, atol,
+                                    max_att, out, err, nsteps);
+    else
+      run_dop853_queued<2, DynPot>(nobj, w, nt, t, indiv_t, comps.data(), npot, rtol, atol,
+                                   max_att, out, err, nsteps);
+  } else {
+    if (mw14)
+      run_dop853_queued<3, MW14Pot>(nobj, w, nt, t, indiv_t, comps.data(), npot, rtol, atol,
+                                    max_att, out, err, nsteps);
+    else
+      run_dop853_queued<3, DynPot>(nobj, w, nt, t, indiv_t, comps.data(), npot, rtol, atol,
+                                   max_att, out, err, nsteps);
+  }
+  return 0;
+}
+
 // Surface-of-section machines (FP64, run-time component list) on SOS states:
 // system 1 (3D): w [nobj][7] = (x, y, vx, vy, A, t, psi); 2 / 3 (planar,
 // surface x = 0 / y = 0): w [nobj][5] = (u, vu, A, t, psi); out raw rows.

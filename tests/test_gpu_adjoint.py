@@ -65,7 +65,7 @@ def test_gpu_adjoint_matches_host_build(harness, golden, planar, generic):
     the device's steps frozen into the host build, forward map and gradients
     agree to rounding."""
     pt, pa = _pot(golden, planar)
-    w0 = cyl_to_rect(seeded_ics(64, 21, planar=planar))
+    w0 = cyl_to_rect(seeded_ics(256, 21, planar=planar))
     T = 20.0
     yh, nh, eh, hh = harness.adj_forward(w0, 0.0, T, pt, pa, planar=planar)
     gy = np.random.default_rng(2).normal(size=yh.shape)
@@ -75,14 +75,27 @@ def test_gpu_adjoint_matches_host_build(harness, golden, planar, generic):
     ns = f["nsteps"].cpu().numpy()
     hd = np.ascontiguousarray(f["hrec"].cpu().numpy().T)
     yT = f["yT"].cpu().numpy().T
-    # independent step choices: mostly the same counts and steps (a rejection
-    # taken on one side only changes the rest of an orbit's sequence), and
-    # the same results to the integration tolerance
-    k = min(hd.shape[1], hh.shape[1])
-    unused = np.arange(k)[None, :] >= nh[:, None]
-    close = (ns == nh) & np.all((np.abs(hd[:, :k] - hh[:, :k]) <= 1e-6 * np.abs(hh[:, :k])) |
-                                unused, axis=1)
-    assert close.mean() >= 0.5, close.mean()
+    # independent step choices: the same accepted-step counts, and step sizes
+    # that differ no more than the host build's own step sizes move under a
+    # one-ulp change of the initial conditions (the controller's error norm
+    # is a small difference of stage sums: on this workload that response
+    # alone is ~2e-8 median, ~6e-7 at the 90th percentile, measured on a
+    # B200 together with the device's differences, which match it)
+    assert (ns == nh).mean() >= 0.99, (ns == nh).mean()
+    ulp = 1 + np.finfo(float).eps * np.random.default_rng(7).choice([-1, 1], w0.shape)
+    _, nh1, _, hh1 = harness.adj_forward(w0 * ulp, 0.0, T, pt, pa, planar=planar)
+
+    def step_rel_diff(a, b, n):
+        k = min(a.shape[1], b.shape[1])
+        used = np.arange(k)[None, :] < n[:, None]
+        return np.where(used, np.abs(a[:, :k] - b[:, :k]) / np.abs(b[:, :k]).clip(1e-300),
+                        0.0).max(axis=1)
+
+    dev = step_rel_diff(hd, hh, nh)[ns == nh]
+    resp = step_rel_diff(hh1, hh, nh)[nh1 == nh]
+    for qtl in (0.5, 0.9):
+        assert np.quantile(dev, qtl) <= 3 * np.quantile(resp, qtl) + 1e-12, (
+            qtl, np.quantile(dev, qtl), np.quantile(resp, qtl))
     np.testing.assert_allclose(yT, yh, rtol=0, atol=1e-8)
     # the device's steps frozen into the host build
     np.testing.assert_allclose(harness.adj_replay(w0, 0.0, T, pt, pa, hd, ns, planar=planar),

@@ -46,9 +46,14 @@ def test_device_abort_word(oracle, mw14, method):
     pt, pa = mw14
     n = 4096
     ics = seeded_ics(n, 50)
-    # early output times so that some rows are written before the kernel
-    # first reads the flag, then a long stretch it never reaches
-    t = np.concatenate([np.linspace(0.0, 0.02, 5), [2000.0]])
+    if method == "dop853":
+        # early output times so that some rows are written before the kernel
+        # first reads the flag, then a long stretch it never reaches
+        t = np.concatenate([np.linspace(0.0, 0.02, 5), [2000.0]])
+    else:
+        # galpy's fixed-step integrators take evenly spaced output times
+        # (the number of steps per output comes from the first interval)
+        t = np.linspace(0.0, 2000.0, 6)
     comps, ncomp = gb.compile_potential((pt, pa))
     dev = torch.device("cuda", 0)
     d_comps = torch.from_numpy(comps).to(dev)

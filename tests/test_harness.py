@@ -331,3 +331,37 @@ def test_planar_surface_of_section_machines(harness, oracle, golden, method, sur
     d = np.abs(got - ref)
     d[..., 3] = np.abs((got[..., 3] - ref[..., 3] + np.pi) % (2 * np.pi) - np.pi)
     assert d.max() < 1e-10
+
+
+@pytest.mark.parametrize("planar", [False, True])
+def test_dop853_queued_dense_output(harness, oracle, golden, planar):
+    """The kernels' queued dense output (request record written at the
+    accepted step, dense stages run later from the record) gives the in-slot
+    dense output's rows bit for bit: shared grids, ragged per-orbit grids
+    with several outputs in one step, backward integration, a generic
+    component list, and orbits stopped by the attempt budget."""
+    pt, pa = ((golden["mw14_planar_type"], golden["mw14_planar_args"]) if planar
+              else (golden["mw14_type"], golden["mw14_args"]))
+    ics = seeded_ics(24, 61, planar=planar, r_range=(0.05, 3.0), log_r=True)
+    w = cyl_to_rect(ics)
+    rng = np.random.default_rng(61)
+    grids = [np.linspace(0, 20, 201), np.linspace(0, -15, 31),
+             np.sort(rng.uniform(0, 1, (len(w), 41)), axis=1) * rng.uniform(2, 30, (len(w), 1))]
+    grids[2][:, 0] = 0.0
+    for t in grids:
+        ref, eref, nref = harness.integrate(w, t, pt, pa, "dop853", planar=planar, rtol=1e-10,
+                                            atol=1e-10)
+        out, err, ns = harness.dop853_queued(w, t, pt, pa, planar=planar, rtol=1e-10, atol=1e-10)
+        assert np.array_equal(err, eref) and np.array_equal(ns, nref)
+        assert np.array_equal(out, ref)
+    # a generic list (triaxial halo + Hernquist) and the attempt budget
+    pt2 = np.concatenate([golden["logtri_type"], golden["hernquist_type"]])
+    pa2 = np.concatenate([golden["logtri_args"], golden["hernquist_args"]])
+    t = np.linspace(0, 50, 51)
+    for ma in (0, 40):
+        ref, eref, nref = harness.integrate(w, t, pt2, pa2, "dop853", planar=planar,
+                                            max_attempts=ma)
+        out, err, ns = harness.dop853_queued(w, t, pt2, pa2, planar=planar, max_attempts=ma)
+        assert np.array_equal(err, eref) and np.array_equal(ns, nref)
+        assert np.array_equal(out, ref, equal_nan=True)
+    assert (eref == 2).all()  # the budget stops every orbit
