@@ -198,7 +198,7 @@ class ClockSampler:
 
 # ----------------------------------------------------------- CPU baseline --
 def cpu_reference_rate(ics, t, pt, pa, target_s=10.0, min_orbits=512, method="dop853",
-                       rtol=RTOL, atol=ATOL):
+                       rtol=RTOL, atol=ATOL, dt=None, planar=False):
     """orbit-steps/s of the reference's C (oracle/_ref) or the oracle, all cores."""
     from oracle import oracle as O
 
@@ -210,7 +210,7 @@ def cpu_reference_rate(ics, t, pt, pa, target_s=10.0, min_orbits=512, method="do
         idx = rng.choice(len(ics), size=min(n, len(ics)), replace=False)
         sub_ics, sub_t = ics[idx], (t[idx] if t.ndim > 1 else t)
         t0 = time.perf_counter()
-        O.integrate(sub_ics, sub_t, pt, pa, method, rtol=rtol, atol=atol,
+        O.integrate(sub_ics, sub_t, pt, pa, method, rtol=rtol, atol=atol, dt=dt, planar=planar,
                     impl=("ref" if kind == "reference" else "port"), nthreads=cores)
         el = time.perf_counter() - t0
         if el >= 0.4 * target_s or n >= len(ics):
@@ -218,12 +218,108 @@ def cpu_reference_rate(ics, t, pt, pa, target_s=10.0, min_orbits=512, method="do
         n = int(n * min(8.0, max(2.0, 0.5 * target_s / max(el, 1e-3))))
     # accepted steps of the same sample (the oracle is bit-identical to the
     # reference's C, so its counts are the reference's)
-    _, _, ns, _ = O.integrate(sub_ics, sub_t, pt, pa, method, rtol=rtol, atol=atol,
-                              nthreads=cores)
+    _, _, ns, _ = O.integrate(sub_ics, sub_t, pt, pa, method, rtol=rtol, atol=atol, dt=dt,
+                              planar=planar, nthreads=cores)
     steps = int(ns.sum())
     return {"value": steps / el, "unit": "orbit-steps/s", "cores": cores, "kind": kind,
             "sample": f"{len(idx)} random orbits of the workload ({steps} accepted steps, "
                       f"{el:.1f} s), OMP threads = {cores}"}
+
+
+def cpu_reference_rate_groups(pt, args, group, ics, t, target_s=10.0, ngroups=8, rtol=1e-9,
+                              atol=1e-9):
+    """The reference's C on the ragged multi-potential workload: it takes one
+    potential per call, so a random sample of the parameter groups is
+    integrated group by group (all cores inside each call)."""
+    from oracle import oracle as O
+
+    kind = "reference" if O.ref_available() else "port"
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    rng = np.random.default_rng(321)
+    gsel = rng.choice(len(args), size=ngroups, replace=False)
+    per = 64
+    while True:
+        el, steps, norb = 0.0, 0, 0
+        for g in gsel:
+            idx = np.flatnonzero(group == g)
+            idx = rng.choice(idx, size=min(per, len(idx)), replace=False)
+            t0 = time.perf_counter()
+            O.integrate(ics[idx], t, pt, args[g], "dop853", rtol=rtol, atol=atol,
+                        impl=("ref" if kind == "reference" else "port"), nthreads=cores)
+            el += time.perf_counter() - t0
+            _, _, ns, _ = O.integrate(ics[idx], t, pt, args[g], "dop853", rtol=rtol, atol=atol,
+                                      nthreads=cores)
+            steps += int(ns.sum())
+            norb += len(idx)
+        if el >= 0.4 * target_s or per >= 16384:
+            break
+        per = int(per * min(8.0, max(2.0, 0.5 * target_s / max(el, 1e-3))))
+    return {"value": steps / el, "unit": "orbit-steps/s", "cores": cores, "kind": kind,
+            "sample": f"{norb} random orbits of {ngroups} random parameter groups, one call per "
+                      f"group ({steps} accepted steps, {el:.1f} s), OMP threads = {cores}"}
+
+
+def cpu_reference_gradient_rate(w0, tgt, pt, pa, idx, target_s=10.0):
+    """What the reference needs for the same gradients on a sample of the
+    differentiation workload: dL/d(initial state) from its variational
+    integrator (integratePlanarOrbit_dxdv, one call per orbit and deviation
+    direction: the 4 columns of the state-transition matrix), and
+    dL/d(parameters) by central differences (2 integrations of every orbit
+    per parameter).  Threads over orbits for the single-orbit dxdv calls
+    (ctypes releases the interpreter lock); the batched calls use OpenMP.
+    Returns orbit-steps/s in the differentiation leg's unit: accepted
+    forward steps of the sample over that time."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import oracle as O
+
+    kind = "reference" if O.ref_available() else "port"
+    impl = "ref" if kind == "reference" else "port"
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    t = np.array([0.0, 20.0])
+    rng = np.random.default_rng(77)
+
+    def cyl(w):
+        x, y, vx, vy = w.T
+        phi = np.arctan2(y, x)
+        c, s = np.cos(phi), np.sin(phi)
+        return np.stack([np.hypot(x, y), vx * c + vy * s, -vx * s + vy * c, phi], 1)
+
+    n = 32
+    while True:
+        sel = rng.choice(len(w0), size=min(n, len(w0)), replace=False)
+        w, ics = w0[sel], cyl(w0[sel])
+        t0 = time.perf_counter()
+        # state-transition matrix columns: one variational run per direction
+        rows = [np.concatenate([w[i], np.eye(4)[k]]) for i in range(len(w)) for k in range(4)]
+
+        def one(r):
+            return O.integrate_dxdv(r[None], t, pt, pa, "dop853", planar=True, rtol=1e-10,
+                                    atol=1e-10, impl=impl)[0]
+
+        with ThreadPoolExecutor(max_workers=cores) as ex:
+            list(ex.map(one, rows))
+        # parameters: central differences of the whole sample's loss
+        for j in idx:
+            for sgn in (1, -1):
+                p = np.array(pa, float)
+                p[j] += sgn * 1e-6 * abs(pa[j])
+                O.integrate(ics, t, pt, p, "dop853", planar=True, rtol=1e-10, atol=1e-10,
+                            impl=impl, nthreads=cores)
+        el = time.perf_counter() - t0
+        if el >= 0.4 * target_s or n >= len(w0):
+            break
+        n = int(n * min(8.0, max(2.0, 0.5 * target_s / max(el, 1e-3))))
+    _, _, ns, _ = O.integrate(ics, t, pt, pa, "dop853", planar=True, rtol=1e-10, atol=1e-10,
+                              nthreads=cores)
+    steps = int(ns.sum())
+    return {"value": steps / el, "unit": "orbit-steps/s (forward + backward)", "cores": cores,
+            "kind": kind,
+            "sample": f"{len(sel)} random orbits: 4 variational dop853 runs per orbit "
+                      f"(integratePlanarOrbit_dxdv, {cores} threads over orbits) and "
+                      f"{2 * len(idx)} perturbed integrations of the sample for the "
+                      f"{len(idx)} parameters (central differences), {steps} accepted forward "
+                      f"steps, {el:.1f} s"}
 
 
 # ------------------------------------------------------------------ main --
@@ -425,16 +521,22 @@ def main():
 
     if not args.no_mixed:
         result["mixed"] = mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg,
-                                    args.mixed_orbits, comps)
+                                    args.mixed_orbits, comps,
+                                    cpu=rank == 0 and not args.no_cpu_baseline)
+        result["gpu_launches"] += 4
+        # the FP32-force form of the batching workload's DOP853, on a sample
+        result["f32force_sample"] = f32force_dop853_sample(gb, torch, dev, stream, "batching")
         result["gpu_launches"] += 4
 
     if not args.no_ragged:
-        result["ragged"] = ragged_leg(gb, torch, dev, stream, pg)
-        result["gpu_launches"] += 2
+        result["ragged"] = ragged_leg(gb, torch, dev, stream, pg,
+                                      cpu=rank == 0 and not args.no_cpu_baseline)
+        result["gpu_launches"] += result["ragged"]["gpu_launches"]
 
     if not args.no_grad:
-        result["differentiation"] = differentiation_leg(gb, torch, dev, stream, pg, peak,
-                                                        n=args.grad_orbits)
+        result["differentiation"] = differentiation_leg(
+            gb, torch, dev, stream, pg, peak, n=args.grad_orbits,
+            cpu=rank == 0 and not args.no_cpu_baseline)
         result["gpu_launches"] += 4
 
     if not args.no_e2e:
@@ -457,7 +559,7 @@ F_STEP_DOP853_PLANAR = 6200.0  # 15 planar force evaluations (280) + 2000 stage 
 F_GRAD_STEP = 3 * F_STEP_DOP853_PLANAR  # forward + backward (2 x forward: Hessian-vector products)
 
 
-def differentiation_leg(gb, torch, dev, stream, pg, peak, n=65536):
+def differentiation_leg(gb, torch, dev, stream, pg, peak, n=65536, cpu=False):
     """Gradient of L = sum |y(20) - target|^2 over 65,536 planar orbits
     with respect to the initial conditions and the MiyamotoNagai (amp, a,
     b), NFW (amp, a) and bulge (amp, rc) parameters: adjoint forward +
@@ -518,18 +620,24 @@ def differentiation_leg(gb, torch, dev, stream, pg, peak, n=65536):
     value = steps_all / (ms_tot * 1e-3)
     achieved = value / (pg.get_world_size() if pg else 1) * F_GRAD_STEP / 1e12
     names = ["bulge amp", "bulge rc", "disk amp", "disk a", "disk b", "halo amp", "halo a"]
-    return {"workload": f"differentiation: {n} planar orbits in MWPotential2014, dop853 "
-                        "rtol=atol=1e-10, t in [0,20], L = sum |y(20) - target|^2, gradient "
-                        "w.r.t. initial conditions and 7 potential parameters",
-            "value": value, "unit": "orbit-steps/s (forward + backward)",
-            "forward_ms": fwd_ms, "backward_ms": bwd_ms, "accepted_steps": steps,
-            "max_steps_per_orbit": int(f["nsteps"].max().item()), "orbits_with_err": nbad_all,
-            "param_grad": dict(zip(names, g.tolist())),
-            "param_grad_rel_err_vs_fd": float(np.max(np.abs(g - fd) / np.abs(fd))),
-            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
-                         "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
-                         "flops_per_unit": F_GRAD_STEP,
-                         "unit_of_work": "accepted forward step (forward + backward flops)"}}
+    res = {"workload": f"differentiation: {n} planar orbits in MWPotential2014, dop853 "
+                       "rtol=atol=1e-10, t in [0,20], L = sum |y(20) - target|^2, gradient "
+                       "w.r.t. initial conditions and 7 potential parameters",
+           "value": value, "unit": "orbit-steps/s (forward + backward)",
+           "forward_ms": fwd_ms, "backward_ms": bwd_ms, "accepted_steps": steps,
+           "max_steps_per_orbit": int(f["nsteps"].max().item()), "orbits_with_err": nbad_all,
+           "param_grad": dict(zip(names, g.tolist())),
+           "param_grad_rel_err_vs_fd": float(np.max(np.abs(g - fd) / np.abs(fd))),
+           "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
+                        "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                        "flops_per_unit": F_GRAD_STEP,
+                        "unit_of_work": "accepted forward step (forward + backward flops)"}}
+    if cpu:
+        try:
+            res["cpu_baseline"] = cpu_reference_gradient_rate(w0, tgt, pt, pa, idx)
+        except Exception as exc:  # report, do not hide
+            res["cpu_baseline"] = {"value": None, "error": repr(exc)}
+    return res
 
 
 # Nominal float64 flops per step of each integrator in MWPotential2014 (3D,
@@ -689,8 +797,16 @@ def profile_leg(gb, torch, dev, spec, n):
             "orbits_with_err": int((err != 0).sum().item())}
 
 
-def ragged_leg(gb, torch, dev, stream, pg):
-    """One launch over 512 potential-parameter groups (about 4.3 M orbits)."""
+def ragged_leg(gb, torch, dev, stream, pg, K=3, W=2, cpu=False):
+    """One launch over 512 potential-parameter groups (about 4.3 M orbits):
+    the launch shape from the autotuner (on a subsample, parameter groups
+    included), the integration captured in a CUDA graph, W warm-up and K
+    timed replays (CUDA events, max over ranks).  Also: the FP32-force
+    variant on a sample of 8 groups, and the reference's C on a sample of
+    groups (cpu)."""
+    from galpy_b200 import autotune
+    from galpy_b200.graph import IntegrationGraph
+
     pt, args, group, ics, t = ragged_workload()
     n = len(group)
     comps, ncomp = gb.compile_potential((pt, args.ravel()), ngroup=len(args))
@@ -702,32 +818,57 @@ def ragged_leg(gb, torch, dev, stream, pg):
     out = torch.empty((6, len(t), n), dtype=torch.float64, device=dev)
     err = torch.empty(n, dtype=torch.int32, device=dev)
     ns = torch.empty(n, dtype=torch.int64, device=dev)
-    ms = []
-    for rep in range(2):  # warm-up + timed
-        if pg:
-            pg.barrier()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        gb.integrate_device(comps_d, ncomp, w0, t_d, out, err, "dop853_cuda", nsteps=ns,
-                            group=g_d, rtol=1e-9, atol=1e-9, stream=stream, signature=sig)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        ms.append(e0.elapsed_time(e1))
+    tuned = autotune.tune(comps_d, ncomp, w0, t_d, out, err, "dop853_cuda", rtol=1e-9, atol=1e-9,
+                          signature=sig, group=g_d)
+    graph = IntegrationGraph(comps_d, ncomp, w0, t_d, out, err, "dop853_cuda", nsteps=ns,
+                             group=g_d, rtol=1e-9, atol=1e-9, signature=sig,
+                             **autotune.launch_kwargs(tuned))
+    for _ in range(W):
+        graph.replay()
+    torch.cuda.synchronize()
+    steps = float(ns.sum().item())
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(K):
+        graph.replay()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    (ms,), (steps_all,) = over_ranks([e0.elapsed_time(e1) / K], [steps], pg, dev)
     E0 = torch.empty(n, dtype=torch.float64, device=dev)
     E1 = torch.empty(n, dtype=torch.float64, device=dev)
     gb.energy_device(comps_d, ncomp, w0, E0, group=g_d, stream=stream)
     gb.energy_device(comps_d, ncomp, out[:, len(t) - 1, :], E1, group=g_d, stream=stream)
     torch.cuda.synchronize()
-    steps = float(ns.sum().item())
-    return {"workload": f"ragged: {len(args)} MWPotential2014 variants, {n} orbits, dop853 "
-                        "rtol=atol=1e-9, t in [0,50], 51 snapshots, one launch",
-            "value": steps / (ms[-1] * 1e-3), "unit": "orbit-steps/s", "ms": ms[-1],
-            "accepted_steps": steps, "orbits_with_err": int((err != 0).sum().item()),
-            "energy_rel_err": stats(torch.abs(E1 / E0 - 1).cpu().numpy())}
+    rel = torch.abs(E1 / E0 - 1).cpu().numpy()
+    E0h = E0.cpu().numpy()
+    res = {"workload": f"ragged: {len(args)} MWPotential2014 variants, {n} orbits, dop853 "
+                       "rtol=atol=1e-9, t in [0,50], 51 snapshots, one launch",
+           "value": steps_all / (ms * 1e-3), "unit": "orbit-steps/s", "ms": ms, "steps": K,
+           "warmup": W, "launch": {"graph": "CUDA graph replay",
+                                   **autotune.launch_kwargs(tuned)},
+           "accepted_steps": steps, "orbits_with_err": int((err != 0).sum().item()),
+           "energy_rel_err": stats(rel),
+           # the largest relative drifts belong to orbits whose energy is
+           # close to zero (|E0| small makes |E1/E0 - 1| large for the same
+           # absolute error): the absolute drift of the worst orbits
+           "energy_worst": {"rel": float(rel.max()), "E0": float(E0h[rel.argmax()]),
+                            "abs_err_max": float(np.abs(rel * E0h).max())},
+           "gpu_launches": 2 * (K + W)}
+    res["f32force_sample"] = f32force_dop853_sample(gb, torch, dev, stream, "ragged")
+    if cpu:
+        try:
+            res["cpu_baseline"] = cpu_reference_rate_groups(pt, args, group, ics, t)
+        except Exception as exc:  # report, do not hide
+            res["cpu_baseline"] = {"value": None, "error": repr(exc)}
+    graph.reset()
+    return res
 
 
-def mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg, n, comps_host=None):
+def mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg, n, comps_host=None,
+              cpu=False):
     """FP32-force / FP64-state vs all-FP64 on the precision configuration
     (symplec4, dt = 0.01, 20,000 steps, final state only): throughput, the
     per-orbit relative energy drift, and the final phase-space difference."""
@@ -777,6 +918,111 @@ def mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg, n, comps_
     res["speedup_f32force_vs_fp64"] = res["f32force"]["value"] / res["fp64"]["value"]
     res["workload"] = (f"precision: {n} orbits in MWPotential2014 (config-0 initial "
                        "conditions), symplec4 dt=0.01, 20,000 steps, final state only")
+    # both forms against the FP64 oracle (the reference's arithmetic) on a
+    # sample: final phase-space difference and the oracle's own energy drift
+    from oracle import oracle as O
+
+    m = min(n, 1024)
+    ref, eref, _, _ = O.integrate(ics[:m], t, pt, pa, "symplec4", dt=0.01)
+    ref_rect = cyl_to_rect(ref[:, -1])
+    for prec in ("fp64", "f32force"):
+        g = outs[prec][:, :m].cpu().numpy().T
+        dd = np.abs(g - ref_rect).max(axis=1) / np.abs(ref_rect).max(axis=1)
+        res[prec]["phase_space_rel_err_vs_oracle"] = stats(dd)
+    e0 = O.energy_cyl(ics[:m, None], pt, pa)[:, 0]
+    e1 = O.energy_cyl(ref[:, -1:], pt, pa)[:, 0]
+    res["oracle_sample"] = {"orbits": m, "energy_rel_err": stats(np.abs(e1 / e0 - 1)),
+                            "kind": "oracle (C restatement of galpy's symplec4, bit-identical "
+                                    "to the reference's C)"}
+    if cpu:  # the reference's C symplec4 (float64) on a sample, all cores
+        try:
+            res["cpu_baseline"] = cpu_reference_rate(ics, t, pt, pa, method="symplec4",
+                                                     dt=0.01, min_orbits=64)
+        except Exception as exc:  # report, do not hide
+            res["cpu_baseline"] = {"value": None, "error": repr(exc)}
+    return res
+
+
+def rect_to_cyl(w):
+    x, y, z, vx, vy, vz = w.T
+    phi = np.arctan2(y, x)
+    c, s = np.cos(phi), np.sin(phi)
+    return np.stack([np.hypot(x, y), vx * c + vy * s, -vx * s + vy * c, z, vz, phi], 1)
+
+
+def f32force_dop853_sample(gb, torch, dev, stream, kind, n_sample=4096, budget=2_000_000):
+    """The FP32-force variant of DOP853 beside FP64 on a random sample of the
+    batching (kind "batching": rtol = atol = 1e-10) or ragged ("ragged":
+    1e-9, 8 parameter groups) workload.  DOP853's error estimate sees the
+    single-precision force rounding, so the step count grows: the line gives
+    the accepted-step ratio, both forms' relative energy drift and the final
+    phase-space difference.  A per-orbit attempt budget bounds the run; orbits
+    that exhaust it (err 2) are counted and left out of the error statistics."""
+    rng = np.random.default_rng(99)
+    group_d = None
+    if kind == "batching":
+        pt, pa = mw14_args()
+        ics, t = workload(N_ORBITS, seed=1)
+        sel = rng.choice(len(ics), size=n_sample, replace=False)
+        ics, t = ics[sel], t[sel]
+        comps, ncomp = gb.compile_potential((pt, pa))
+        sig = gb.signature((pt, pa))
+        tol = RTOL
+        last = NT - 1
+    else:
+        pt, args, group, ics_all, t = ragged_workload()
+        gsel = rng.choice(len(args), size=8, replace=False)
+        idx = np.concatenate([rng.choice(np.flatnonzero(group == g),
+                                         size=n_sample // 8, replace=False) for g in gsel])
+        ics = ics_all[idx]
+        slot_of = {int(g): k for k, g in enumerate(gsel)}
+        grp = np.array([slot_of[int(g)] for g in group[idx]], np.int32)
+        comps, ncomp = gb.compile_potential((pt, args[gsel].ravel()), ngroup=len(gsel))
+        sig = gb.signature((pt, args[0]))
+        group_d = torch.tensor(grp, device=dev)
+        tol = 1e-9
+        last = len(t) - 1
+    n = len(ics)
+    comps_d = torch.tensor(comps, device=dev)
+    w0 = torch.tensor(cyl_to_rect(ics).T.copy(), device=dev)
+    t_d = torch.tensor(t, device=dev)
+    E0 = torch.empty(n, dtype=torch.float64, device=dev)
+    gb.energy_device(comps_d, ncomp, w0, E0, group=group_d, stream=stream)
+    res, fin, steps, errs, ms = {}, {}, {}, {}, {}
+    for prec in ("fp64", "f32force"):
+        out = torch.empty((6, 1, n), dtype=torch.float64, device=dev)
+        err = torch.empty(n, dtype=torch.int32, device=dev)
+        ns = torch.empty(n, dtype=torch.int64, device=dev)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        gb.integrate_device(comps_d, ncomp, w0, t_d, out, err, "dop853_cuda", nsteps=ns,
+                            group=group_d, out_row0=last, rtol=tol, atol=tol, precision=prec,
+                            max_attempts=budget, signature=sig, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms[prec] = e0.elapsed_time(e1)
+        fin[prec] = out[:, 0, :]
+        steps[prec] = ns.cpu().numpy()
+        errs[prec] = err.cpu().numpy()
+    ok = (errs["fp64"] == 0) & (errs["f32force"] == 0)
+    for prec in ("fp64", "f32force"):
+        E1 = torch.empty(n, dtype=torch.float64, device=dev)
+        gb.energy_device(comps_d, ncomp, fin[prec], E1, group=group_d, stream=stream)
+        torch.cuda.synchronize()
+        rel = torch.abs(E1 / E0 - 1).cpu().numpy()
+        res[prec] = {"accepted_steps": float(steps[prec].sum()), "ms": ms[prec],
+                     "orbits_with_err": int((errs[prec] != 0).sum()),
+                     "energy_rel_err": stats(rel[ok]) if ok.any() else None}
+    d = (torch.abs(fin["f32force"] - fin["fp64"]).max(dim=0).values /
+         torch.abs(fin["fp64"]).max(dim=0).values).cpu().numpy()
+    res["f32force"]["phase_space_rel_err_vs_fp64"] = stats(d[ok]) if ok.any() else None
+    r = steps["f32force"][ok].sum() / max(1, steps["fp64"][ok].sum())
+    res["accepted_step_ratio_f32force_vs_fp64"] = float(r)
+    res["speed_ratio_f32force_vs_fp64_orbits_per_s"] = ms["fp64"] / ms["f32force"]
+    res["sample"] = (f"{n} random orbits of the {kind} workload" +
+                     (" (8 random parameter groups)" if kind == "ragged" else "") +
+                     f", dop853 rtol = atol = {tol:g}, attempt budget {budget} per orbit")
     return res
 
 

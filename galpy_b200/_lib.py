@@ -194,6 +194,9 @@ SIGNATURES = {
     "galpy_cuda_accel_device": (
         _ci, [_vp, _ci, _vp, _ci, _ci, _ci, _vp, ctypes.c_longlong, _vp, _vp]),
     "galpy_cuda_trim_memory": (_ci, [_ci]),
+    "galpy_cuda_jacobi_device": (
+        _ci, [_vp, _ci, _vp, _ci, _vp, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong,
+              _dp, _vp, _vp]),
 }
 
 

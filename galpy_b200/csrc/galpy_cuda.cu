@@ -666,10 +666,13 @@ static void cyl_to_rect_inplace(int planar, long long nobj, double* yo)
 // ----------------------------------------------------------------------------
 // energies of stored states (output-side check of the integrations)
 // ----------------------------------------------------------------------------
+// E = v^2/2 + Phi(x), minus Omega . (x cross v) when Omega is not zero (the
+// Jacobi integral in a frame rotating with pattern speed Omega).
 __global__ void __launch_bounds__(256) energy_kernel(const GpComp* comps, int ncomp,
                                                      const int* group, int planar,
                                                      const double* w, long long n, long long sc,
-                                                     long long so, double* E)
+                                                     long long so, double ox, double oy,
+                                                     double oz, double* E)
 {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -691,7 +694,10 @@ __global__ void __launch_bounds__(256) energy_kernel(const GpComp* comps, int nc
     vy = v[4 * sc];
     vz = v[5 * sc];
   }
-  E[i] = 0.5 * (vx * vx + vy * vy + vz * vz) + potential_value(c, ncomp, x, y, z);
+  double e = 0.5 * (vx * vx + vy * vy + vz * vz) + potential_value(c, ncomp, x, y, z);
+  if (ox != 0.0 || oy != 0.0 || oz != 0.0)
+    e -= ox * (y * vz - z * vy) + oy * (z * vx - x * vz) + oz * (x * vy - y * vx);
+  E[i] = e;
 }
 
 // Accelerations at points (positions SoA [3][n], z ignored when planar) with
@@ -855,7 +861,25 @@ int galpy_cuda_energy_device(const void* comps, int ncomp, const int* group, int
   if (n == 0) return GALPY_CUDA_OK;
   const unsigned blocks = (unsigned)((n + 255) / 256);
   energy_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
-      static_cast<const GpComp*>(comps), ncomp, group, planar, w, n, comp_stride, orbit_stride, E);
+      static_cast<const GpComp*>(comps), ncomp, group, planar, w, n, comp_stride, orbit_stride,
+      0.0, 0.0, 0.0, E);
+  GPC_CUDA_TRY(cudaGetLastError());
+  return GALPY_CUDA_OK;
+}
+
+int galpy_cuda_jacobi_device(const void* comps, int ncomp, const int* group, int planar,
+                             const double* w, long long n, long long comp_stride,
+                             long long orbit_stride, const double* omega, double* J,
+                             void* stream)
+{
+  if (!comps || !w || !J || !omega || n < 0 || ncomp < 1 || ncomp > kMaxComp)
+    return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
+  if (n == 0) return GALPY_CUDA_OK;
+  const unsigned blocks = (unsigned)((n + 255) / 256);
+  // planar states have no z: only the z component of Omega acts on them
+  energy_kernel<<<blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+      static_cast<const GpComp*>(comps), ncomp, group, planar, w, n, comp_stride, orbit_stride,
+      planar ? 0.0 : omega[0], planar ? 0.0 : omega[1], omega[2], J);
   GPC_CUDA_TRY(cudaGetLastError());
   return GALPY_CUDA_OK;
 }

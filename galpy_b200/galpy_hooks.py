@@ -147,6 +147,187 @@ def _route_sos_planar(orig, python_branch):
     return integratePlanarOrbit_sos
 
 
+def _cyl_to_rect_state(yo, planar):
+    """galpy's rows (R, vR, vT[, z, vz], phi) -> (x, y[, z], vx, vy[, vz])."""
+    R, vR, vT, phi = yo[:, 0], yo[:, 1], yo[:, 2], yo[:, -1]
+    c, s = np.cos(phi), np.sin(phi)
+    if planar:
+        return np.stack([R * c, R * s, vR * c - vT * s, vR * s + vT * c], 1)
+    return np.stack([R * c, R * s, yo[:, 3], vR * c - vT * s, vR * s + vT * c, yo[:, 4]], 1)
+
+
+def _cyl_to_rect_dev(yo, dyo, planar):
+    """Deviations (dR, dvR, dvT[, dz, dvz], dphi) at the rows yo -> the
+    rectangular deviations, through the Jacobian of the cylindrical ->
+    rectangular map (the conversion of galpy/orbit/integratePlanarOrbit.py:
+    1463-1484 and integrateFullOrbit.py:935-944)."""
+    R, vR, vT, phi = yo[:, 0], yo[:, 1], yo[:, 2], yo[:, -1]
+    c, s = np.cos(phi), np.sin(phi)
+    dR, dvR, dvT, dphi = dyo[:, 0], dyo[:, 1], dyo[:, 2], dyo[:, -1]
+    dx = c * dR - R * s * dphi
+    dy = s * dR + R * c * dphi
+    dvx = c * dvR - s * dvT - (vR * s + vT * c) * dphi
+    dvy = s * dvR + c * dvT + (vR * c - vT * s) * dphi
+    if planar:
+        return np.stack([dx, dy, dvx, dvy], 1)
+    return np.stack([dx, dy, dyo[:, 3], dvx, dvy, dyo[:, 4]], 1)
+
+
+def _rect_to_cyl_rows(out, planar):
+    """Rectangular (x, v, dx, dv) rows in place -> galpy's cylindrical base
+    state; returns (R, vR, vT, phi) for the deviation conversion.  The planar
+    driver's angle is arccos(x/R) mapped to [0, 2 pi), the 3D one's atan2
+    (the two galpy wrappers differ; both are kept)."""
+    d = 2 if planar else 3
+    x, y = out[..., 0], out[..., 1]
+    vx, vy = out[..., d], out[..., d + 1]
+    R = np.sqrt(x * x + y * y)
+    if planar:
+        phi = np.arccos(x / R)
+        phi = np.where(y < 0.0, 2.0 * np.pi - phi, phi)
+    else:
+        phi = np.arctan2(y, x)
+    c, s = np.cos(phi), np.sin(phi)
+    vR = vx * c + vy * s
+    vT = vy * c - vx * s
+    if planar:
+        out[..., 0], out[..., 1], out[..., 2], out[..., 3] = R, vR, vT, phi
+    else:
+        z, vz = np.copy(out[..., 2]), np.copy(out[..., 5])
+        out[..., 0], out[..., 1], out[..., 2] = R, vR, vT
+        out[..., 3], out[..., 4], out[..., 5] = z, vz, phi
+    return R, vR, vT, phi, c, s
+
+
+def _rect_to_cyl_dev(out, planar, R, vR, vT, c, s):
+    """Rectangular deviations in out[..., 2*dim:] -> (dR, dvR, dvT[, dz,
+    dvz], dphi), the inverse of the Jacobian above."""
+    d = 2 if planar else 3
+    k = 2 * d
+    dx, dy = out[..., k], out[..., k + 1]
+    dvx, dvy = out[..., k + d], out[..., k + d + 1]
+    dR = c * dx + s * dy
+    dphi = (c * dy - s * dx) / R
+    dvR = c * dvx + s * dvy + vT * dphi
+    dvT = c * dvy - s * dvx - vR * dphi
+    if planar:
+        out[..., k], out[..., k + 1], out[..., k + 2], out[..., k + 3] = dR, dvR, dvT, dphi
+    else:
+        dz, dvz = np.copy(out[..., k + 2]), np.copy(out[..., k + 5])
+        out[..., k], out[..., k + 1], out[..., k + 2] = dR, dvR, dvT
+        out[..., k + 3], out[..., k + 4], out[..., k + 5] = dz, dvz, dphi
+
+
+def _route_dxdv(orig, planar):
+    """galpy's integrate{Full,Planar}Orbit_dxdv (integrateFullOrbit.py:859,
+    integratePlanarOrbit.py:1393) maps its single-orbit C integrator over the
+    orbits in Python; for a *_cuda method all (orbit, deviation) pairs go to
+    the GPU in one batched launch instead, with the same coordinate
+    conversions around it."""
+    def integrate_dxdv(pot, yo, dyo, t, int_method, rectIn, rectOut, *args, **kwargs):
+        if not _is_cuda(int_method):
+            return orig(pot, yo, dyo, t, int_method, rectIn, rectOut, *args, **kwargs)
+        from .integrate import integrate_dxdv_batch
+
+        yo = np.atleast_2d(np.asarray(yo, dtype=np.float64))
+        dyo = np.atleast_2d(np.asarray(dyo, dtype=np.float64))
+        w = _cyl_to_rect_state(yo, planar)
+        dw = dyo if rectIn else _cyl_to_rect_dev(yo, dyo, planar)
+        out, err = integrate_dxdv_batch(pot, np.hstack([w, dw]), np.asarray(t, np.float64),
+                                        int_method, planar=planar, dt=kwargs.get("dt"),
+                                        rtol=kwargs.get("rtol"), atol=kwargs.get("atol"))
+        if np.any(err == -10):
+            raise KeyboardInterrupt("Orbit integration interrupted by CTRL-C (SIGINT)")
+        R, vR, vT, phi, c, s = _rect_to_cyl_rows(out, planar)
+        if not rectOut:
+            _rect_to_cyl_dev(out, planar, R, vR, vT, c, s)
+        return out, err
+
+    return integrate_dxdv
+
+
+class _EngineAsC:
+    """Inside integrate_dxdv / lyapunov with a *_cuda method, galpy decides
+    between its C path and odeint from ``ext_loaded`` and ``_check_c``
+    (Orbits.py:2418-2445, 2616-2634); this context lets that decision see
+    the engine (it runs the potentials the check is about) and restores
+    galpy's values afterwards."""
+
+    def __init__(self, O):
+        self.O = O
+
+    def __enter__(self):
+        self.saved = (self.O.ext_loaded, self.O._check_c)
+        self.O.ext_loaded = True
+        self.O._check_c = lambda *a, **k: True
+
+    def __exit__(self, *exc):
+        self.O.ext_loaded, self.O._check_c = self.saved
+        return False
+
+
+def _wrap_variational(orig, O):
+    """Orbit.integrate_dxdv / Orbit.lyapunov: a *_cuda method with supported
+    potentials runs galpy's own code with the engine taken as its C path
+    (the dxdv mapper above does the integration); otherwise galpy's *_c
+    method of the same integrator (and galpy's own fallbacks from there)."""
+    import inspect
+
+    sig = inspect.signature(orig)
+
+    def wrapper(self, *args, **kwargs):
+        ba = sig.bind(self, *args, **kwargs)
+        ba.apply_defaults()
+        method = ba.arguments.get("method")
+        if not _is_cuda(method):
+            return orig(self, *args, **kwargs)
+        pot = ba.arguments.get("pot")
+        if pot is None:
+            pot = getattr(self, "_pot", None)
+        planar = self.dim() == 2
+        if pot is not None and _supported(O.toPlanarPotential(pot) if planar else pot, planar):
+            with _EngineAsC(O):
+                return orig(*ba.args, **ba.kwargs)
+        ba.arguments["method"] = method[: -len("_cuda")] + "_c"
+        return orig(*ba.args, **ba.kwargs)
+
+    wrapper.__doc__ = orig.__doc__
+    wrapper.__name__ = orig.__name__
+    return wrapper
+
+
+# Smallest number of points for which the potential sums of Orbit.E /
+# Orbit.Jacobi go to the GPU (below it the launch latency dominates).
+DEVICE_POTENTIAL_MIN_POINTS = 4096
+
+
+def _route_potential_sum(orig, planar):
+    """evaluatePotentials / evaluateplanarPotentials as Orbit.E (Orbits.py:
+    2902) and Orbit.Jacobi (:3298, through E) call them: plain potential
+    values of a supported static potential at many points run on the GPU
+    (galpy_cuda_energy_device with zero velocities); anything else -- a
+    derivative, a time-dependent or unsupported potential, physical output,
+    a few points -- goes to galpy's own function."""
+    def evaluate(pot, R, *args, **kwargs):
+        plain = (not args[1:] if planar else len(args) <= 1) and not any(
+            kwargs.get(k) for k in ("dR", "dphi", "use_physical")) and set(kwargs) <= {
+            "phi", "t", "dR", "dphi", "use_physical", "z"}
+        if not plain or np.size(R) < DEVICE_POTENTIAL_MIN_POINTS:
+            return orig(pot, R, *args, **kwargs)
+        try:
+            if not _supported(pot, planar):
+                return orig(pot, R, *args, **kwargs)
+        except Exception:
+            return orig(pot, R, *args, **kwargs)
+        from .orbit_quantities import potential_values
+
+        z = 0.0 if planar else (args[0] if args else kwargs.get("z", 0.0))
+        phi = kwargs.get("phi", args[0] if planar and args else 0.0)
+        return potential_values(pot, R, z, phi, planar=planar)
+
+    return evaluate
+
+
 def install():
     """Patch galpy (must be importable) so that Orbit.integrate accepts the
     ``*_cuda`` methods.  Idempotent."""
@@ -204,6 +385,21 @@ def install():
     O.integratePlanarOrbit_sos_c = _route_sos_planar(_installed["integratePlanarOrbit_sos_c"],
                                                      False)
     O.integratePlanarOrbit_sos = _route_sos_planar(_installed["integratePlanarOrbit_sos"], True)
+    # variational integration (integrate_dxdv, lyapunov) and the potential
+    # sums of Orbit.E / Orbit.Jacobi
+    _installed.update(
+        integrate_dxdv=Orbit.integrate_dxdv, lyapunov=Orbit.lyapunov,
+        integrateFullOrbit_dxdv=O.integrateFullOrbit_dxdv,
+        integratePlanarOrbit_dxdv=O.integratePlanarOrbit_dxdv,
+        evaluatePotentials=O.evaluatePotentials,
+        evaluateplanarPotentials=O.evaluateplanarPotentials)
+    Orbit.integrate_dxdv = _wrap_variational(_installed["integrate_dxdv"], O)
+    Orbit.lyapunov = _wrap_variational(_installed["lyapunov"], O)
+    O.integrateFullOrbit_dxdv = _route_dxdv(_installed["integrateFullOrbit_dxdv"], False)
+    O.integratePlanarOrbit_dxdv = _route_dxdv(_installed["integratePlanarOrbit_dxdv"], True)
+    O.evaluatePotentials = _route_potential_sum(_installed["evaluatePotentials"], False)
+    O.evaluateplanarPotentials = _route_potential_sum(_installed["evaluateplanarPotentials"],
+                                                      True)
 
 
 def uninstall():
@@ -216,8 +412,12 @@ def uninstall():
     Orbit.check_integrator = staticmethod(_installed["check_integrator"])
     Orbit._check_method_c_compatible = staticmethod(_installed["_check_method_c_compatible"])
     Orbit._check_array_evenlyspaced = staticmethod(_installed["_check_array_evenlyspaced"])
+    Orbit.integrate_dxdv = _installed["integrate_dxdv"]
+    Orbit.lyapunov = _installed["lyapunov"]
     for name in ("integrateFullOrbit_c", "integratePlanarOrbit_c", "integrateFullOrbit",
                  "integratePlanarOrbit", "integrateFullOrbit_sos_c", "integrateFullOrbit_sos",
-                 "integratePlanarOrbit_sos_c", "integratePlanarOrbit_sos"):
+                 "integratePlanarOrbit_sos_c", "integratePlanarOrbit_sos",
+                 "integrateFullOrbit_dxdv", "integratePlanarOrbit_dxdv", "evaluatePotentials",
+                 "evaluateplanarPotentials"):
         setattr(O, name, _installed[name])
     _installed.clear()

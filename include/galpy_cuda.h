@@ -233,6 +233,17 @@ int galpy_cuda_energy_device(const void *comps, int ncomp, const int *group, int
                              const double *w, long long n, long long comp_stride,
                              long long orbit_stride, double *E, void *stream);
 
+/* The Jacobi integral J = v^2/2 + Phi(x) - Omega . (x cross v) of n stored
+ * rectangular states on the device (galpy's Orbit.Jacobi, E - OmegaP . L,
+ * galpy/orbit/Orbits.py:3298-3375), states and group as in
+ * galpy_cuda_energy_device; omega: host double[3], the pattern-speed vector
+ * (planar states use its z component).  Omega = 0 gives the energy.
+ * Asynchronous on `stream`. */
+int galpy_cuda_jacobi_device(const void *comps, int ncomp, const int *group, int planar,
+                             const double *w, long long n, long long comp_stride,
+                             long long orbit_stride, const double *omega, double *J,
+                             void *stream);
+
 /* ---------------------------------------------------------------------------
  * Gradients of a loss on final states (reverse mode).  No counterpart in the
  * reference: galpy's gradient information is the variational integration

@@ -172,3 +172,113 @@ def test_added_potential_types_route(hooks, pot_name, kwargs, planar):
     o.integrate(np.linspace(0, 1, 11), pot, method="dop853_cuda")
     assert len(hooks) == 1 and hooks[-1]["planar"] == planar
     assert type(hooks[-1]["pot"]).__name__ == pot_name
+
+
+@pytest.fixture()
+def host_engine(monkeypatch, harness, oracle):
+    """The hooks with the engine's variational integration run by the host
+    build of the device code (tests/harness) and the potential sums by the
+    oracle: galpy's own integrate_dxdv, lyapunov and E then run the routed
+    paths on the CPU with real numbers."""
+    from galpy_b200 import galpy_hooks, integrate, orbit_quantities
+    from galpy_b200.potentials import parse_pot
+
+    calls = []
+
+    def batch(pot, w, t, int_method, planar=False, dt=None, rtol=None, atol=None, **kw):
+        _, pt, pa = parse_pot(pot, planar=planar)
+        calls.append(("dxdv", int_method, np.shape(w)))
+        out, err, _ = harness.integrate(w, t, pt, pa, int_method[: -len("_cuda")],
+                                        planar=planar, var=True, dt=dt, rtol=rtol, atol=atol)
+        return out, err
+
+    def potvals(pot, R, z=0.0, phi=0.0, planar=False):
+        _, pt, pa = parse_pot(pot, planar=planar)
+        calls.append(("phi", np.size(R)))
+        R, z, phi = np.broadcast_arrays(R, z, phi)
+        return oracle.potential(R.ravel(), z.ravel(), phi.ravel(), pt, pa).reshape(R.shape)
+
+    monkeypatch.setattr(integrate, "integrate_dxdv_batch", batch)
+    monkeypatch.setattr(orbit_quantities, "potential_values", potvals)
+    galpy_hooks.install()
+    yield calls
+    galpy_hooks.uninstall()
+
+
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("rect", [False, True])
+def test_integrate_dxdv_routes(host_engine, planar, rect):
+    """Orbit.integrate_dxdv with dop853_cuda: one batched call for all
+    orbits, galpy's coordinate conventions around it (cylindrical or
+    rectangular deviations in and out), the same numbers as galpy's own
+    pure-Python dop853 variational integration."""
+    from galpy.orbit import Orbit
+    from galpy.potential import MWPotential2014
+
+    vxvv = ([[1.0, 0.1, 1.1, 0.3], [1.3, -0.05, 0.9, 2.0], [0.8, 0.02, 1.2, -1.0]] if planar
+            else [[1.0, 0.1, 1.1, 0.05, 0.02, 0.3], [1.3, -0.05, 0.9, -0.1, 0.03, 2.0]])
+    n, nv = len(vxvv), len(vxvv[0])
+    dxdv = np.random.default_rng(5).normal(size=(n, nv)) * 1e-3
+    ts = np.linspace(0, 5, 51)
+    o = Orbit(vxvv)
+    o.integrate_dxdv(dxdv, ts, MWPotential2014, method="dop853_cuda", rectIn=rect,
+                     rectOut=rect, rtol=1e-12, atol=1e-12)
+    assert [c[0] for c in host_engine] == ["dxdv"]  # one batched call
+    assert host_engine[0][2] == (n, 2 * nv)
+    ref = Orbit(vxvv)
+    ref.integrate_dxdv(dxdv, ts, MWPotential2014, method="dop853", rectIn=rect, rectOut=rect,
+                       rtol=1e-12, atol=1e-12)
+    got, want = o.getOrbit_dxdv(), ref.getOrbit_dxdv()
+    assert got.shape == want.shape
+    d = np.abs(got - want)
+    k = nv - 1  # phi of the base orbit, compared modulo 2 pi
+    d[..., k] = np.abs((got[..., k] - want[..., k] + np.pi) % (2 * np.pi) - np.pi)
+    scale = np.abs(want).max(axis=1, keepdims=True)
+    assert (d / scale).max() < 1e-8, (d / scale).max()
+
+
+def test_lyapunov_routes(host_engine):
+    """Orbit.lyapunov with dop853_cuda runs its renormalisation segments
+    through the routed integrate_dxdv and agrees with galpy's pure-Python
+    dop853 estimate."""
+    from galpy.orbit import Orbit
+    from galpy.potential import MWPotential2014
+
+    vxvv = [[1.0, 0.1, 1.1, 0.05, 0.02, 0.3], [1.3, -0.05, 0.9, -0.1, 0.03, 2.0]]
+    ts = np.linspace(0, 20, 41)
+    lam = Orbit(vxvv).lyapunov(ts, MWPotential2014, method="dop853_cuda", renorm_every=10,
+                               rtol=1e-12, atol=1e-12)
+    assert sum(c[0] == "dxdv" for c in host_engine) == 4  # one call per segment
+    ref = Orbit(vxvv).lyapunov(ts, MWPotential2014, method="dop853", renorm_every=10,
+                               rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(lam[:, 1:], ref[:, 1:], rtol=1e-7, atol=1e-10)
+
+
+def test_energy_and_jacobi_route_potential_sums(host_engine):
+    """Orbit.E and Orbit.Jacobi over many stored points take the potential
+    sum from the engine (here its oracle stand-in); few points stay with
+    galpy."""
+    from galpy.orbit import Orbit
+    from galpy.potential import MWPotential2014
+
+    from galpy_b200 import galpy_hooks
+
+    rng = np.random.default_rng(9)
+    n = 64
+    vxvv = np.stack([rng.uniform(0.5, 2, n), rng.normal(0, 0.1, n), 1 + rng.normal(0, 0.1, n),
+                     rng.normal(0, 0.05, n), rng.normal(0, 0.05, n),
+                     rng.uniform(0, 2 * np.pi, n)], 1)
+    ts = np.linspace(0, 2, 101)  # 64 x 101 = 6,464 points: above the threshold
+    o = Orbit(vxvv)
+    o.integrate(ts, MWPotential2014, method="dop853")  # galpy's own integrator
+    E = o.E(ts)
+    J = o.Jacobi(ts, OmegaP=0.3)
+    assert sum(c[0] == "phi" for c in host_engine) == 2
+    galpy_hooks.uninstall()
+    Eref, Jref = o.E(ts), o.Jacobi(ts, OmegaP=0.3)
+    galpy_hooks.install()
+    np.testing.assert_allclose(E, Eref, rtol=1e-13)
+    np.testing.assert_allclose(J, Jref, rtol=1e-13)
+    host_engine.clear()
+    o.E(ts[:2])  # 128 points: galpy's own sum
+    assert not host_engine

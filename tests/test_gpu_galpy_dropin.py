@@ -26,7 +26,7 @@ err ~ 1, where the two results still agree inside the integrator tolerance.
 import numpy as np
 import pytest
 from galpy_stub import import_galpy
-from helpers import cyl_diff, seeded_ics
+from helpers import cyl_diff, cyl_to_rect, rect_to_cyl, seeded_ics
 
 galpy = import_galpy()
 pytestmark = [pytest.mark.gpu,
@@ -156,3 +156,68 @@ def test_unsupported_potential_keeps_galpy_path():
     o.integrate(np.linspace(0, 1, 11), SCFPotential(normalize=1.0), method="dop853_cuda",
                 progressbar=False)
     assert np.isfinite(o.getOrbit()).all()
+
+
+@pytest.mark.parametrize("planar", [False, True])
+def test_orbit_integrate_dxdv_cuda(oracle, planar):
+    """Orbit.integrate_dxdv(method='dop853_cuda'): every (orbit, deviation)
+    pair in one GPU launch (galpy maps its single-orbit C integrator over
+    the orbits in Python, Orbits.py:2445), against the reference's own
+    variational C integrator run orbit by orbit (oracle/_ref) where present,
+    else the oracle (bit-identical to it)."""
+    from galpy.orbit import Orbit
+    from galpy.potential import MWPotential2014
+
+    ics = seeded_ics(128, 49, planar=planar)
+    n, nv = ics.shape
+    dxdv = np.random.default_rng(49).normal(size=(n, nv)) * 1e-4
+    ts = np.linspace(0, 10, 101)
+    o = Orbit(ics)
+    o.integrate_dxdv(dxdv, ts, MWPotential2014, method="dop853_cuda", rectIn=True,
+                     rectOut=True, rtol=1e-11, atol=1e-11, progressbar=False)
+    got = o.getOrbit_dxdv()
+    pt, pa = parsed(MWPotential2014, planar)
+    w = np.hstack([cyl_to_rect(ics), dxdv])
+    impl = "ref" if oracle.ref_available() else "port"
+    ref, err, _ = oracle.integrate_dxdv(w, ts, pt, pa, "dop853", planar=planar, rtol=1e-11,
+                                        atol=1e-11, impl=impl)
+    assert not err.any()
+    d = np.abs(got[..., nv:] - ref[..., nv:]) / np.abs(ref[..., nv:]).max(axis=1, keepdims=True)
+    assert np.quantile(d.max(axis=(1, 2)), 0.97) < 1e-9 and d.max() < 1e-6, d.max()
+    assert cyl_diff(rect_to_cyl(ref[..., :nv]), got[..., :nv]).max() < 1e-6
+
+
+def test_orbit_lyapunov_cuda():
+    """Orbit.lyapunov(method='dop853_cuda') against galpy's own pure-Python
+    dop853 estimate (same algorithm, renormalisation every 10 outputs)."""
+    from galpy.orbit import Orbit
+    from galpy.potential import MWPotential2014
+
+    ics = seeded_ics(8, 50)
+    ts = np.linspace(0, 20, 41)
+    lam = Orbit(ics).lyapunov(ts, MWPotential2014, method="dop853_cuda", rtol=1e-12,
+                              atol=1e-12)
+    ref = Orbit(ics).lyapunov(ts, MWPotential2014, method="dop853", rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(lam[:, 1:], ref[:, 1:], rtol=1e-6, atol=1e-9)
+
+
+def test_orbit_energy_and_jacobi_on_device():
+    """Orbit.E and Orbit.Jacobi after a dop853_cuda integration: the routed
+    potential sums (GPU) against galpy's own (hooks removed)."""
+    from galpy.orbit import Orbit
+    from galpy.potential import MWPotential2014
+
+    from galpy_b200 import galpy_hooks
+
+    ics = seeded_ics(256, 51)
+    ts = np.linspace(0, 10, 51)
+    o = Orbit(ics)
+    o.integrate(ts, MWPotential2014, method="dop853_cuda", progressbar=False)
+    E, J = o.E(ts), o.Jacobi(ts, OmegaP=0.4)
+    galpy_hooks.uninstall()
+    try:
+        Eref, Jref = o.E(ts), o.Jacobi(ts, OmegaP=0.4)
+    finally:
+        galpy_hooks.install()
+    np.testing.assert_allclose(E, Eref, rtol=1e-13)
+    np.testing.assert_allclose(J, Jref, rtol=1e-13)

@@ -558,6 +558,48 @@ def test_energy_kernel_vs_oracle(oracle, mw14):
     assert (np.abs(E.cpu().numpy() - ref) / np.abs(ref).max()).max() < 1e-14
 
 
+@pytest.mark.parametrize("planar", [False, True])
+def test_jacobi_kernel_vs_oracle(oracle, mw14, mw14_planar, planar):
+    """galpy_cuda_jacobi_device: E - Omega . L (galpy's Orbit.Jacobi,
+    Orbits.py:3298-3375) against the oracle's energies and the angular
+    momentum from the same states, for a scalar pattern speed and a
+    pattern-speed vector; Omega = 0 gives galpy_cuda_energy_device's E."""
+    import torch
+
+    from galpy_b200.orbit_quantities import jacobi_device
+
+    pt, pa = mw14_planar if planar else mw14
+    ics = seeded_ics(4000, 52, planar=planar)
+    comps, n = gb.compile_potential((pt, pa), planar=planar)
+    dev = torch.device("cuda:0")
+    cd = torch.tensor(comps, device=dev)
+    w_np = cyl_to_rect(ics)
+    w = torch.tensor(w_np.T.copy(), device=dev)
+    if planar:
+        x, y, vx, vy = w_np.T
+        L = np.stack([np.zeros_like(x), np.zeros_like(x), x * vy - y * vx], 1)
+        # the planar potential is the 3D one in the plane z = 0
+        rows = np.insert(np.insert(ics, 3, 0.0, 1), 4, 0.0, 1)
+        Eref = oracle.energy_cyl(rows[:, None], *mw14)[:, 0]
+    else:
+        L = np.cross(w_np[:, :3], w_np[:, 3:])
+        Eref = oracle.energy_cyl(ics[:, None, :], pt, pa)[:, 0]
+    E0 = torch.empty(len(ics), dtype=torch.float64, device=dev)
+    if not planar:
+        gb.energy_device(cd, n, w, E0)
+    for omega in (0.0, 0.55, (0.1, -0.2, 0.7)):
+        J = torch.empty(len(ics), dtype=torch.float64, device=dev)
+        jacobi_device(cd, n, w, J, omega=omega, planar=planar)
+        torch.cuda.synchronize()
+        om = np.array([0.0, 0.0, omega]) if np.ndim(omega) == 0 else np.array(omega)
+        if planar:
+            om[:2] = 0.0  # planar states: only the z component acts
+        ref = Eref - L @ om
+        assert (np.abs(J.cpu().numpy() - ref) / np.abs(ref).max()).max() < 1e-14, omega
+        if omega == 0.0 and not planar:
+            assert torch.equal(J, E0)
+
+
 @pytest.mark.parametrize("name", ["mw14", "hernquist", "loghalo", "logtri", "nfw", "mn", "pswc"]
                          + ADDED_POTS)
 @pytest.mark.parametrize("planar", [False, True])
