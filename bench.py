@@ -867,11 +867,22 @@ def ragged_leg(gb, torch, dev, stream, pg, K=3, W=2, cpu=False):
     return res
 
 
+# the precision forms of the engine (include/galpy_cuda.h), in the order
+# the mixed leg reports them; the first is the plain float64 reference form
+PRECISION_FORMS = ("fp64", "f32force", "f64tail32", "f32bulge", "f32force_df")
+
+
 def mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg, n, comps_host=None,
               cpu=False):
-    """FP32-force / FP64-state vs all-FP64 on the precision configuration
-    (symplec4, dt = 0.01, 20,000 steps, final state only): throughput, the
-    per-orbit relative energy drift, and the final phase-space difference."""
+    """The precision forms on the precision configuration (symplec4, dt =
+    0.01, 20,000 steps, final state only), each at its own autotuned launch
+    shape: throughput and its ratio to the plain float64 kernel, the
+    per-orbit relative energy drift, and the final phase-space difference
+    from the float64 kernel and from the float64 oracle (on a sample).
+    Forms: fp64 (float64 force and state), f32force (float32 force, float64
+    state), f64tail32 (float64 force with float32 tails of its table
+    polynomials), f32bulge (f64tail32 with the bulge term in float32),
+    f32force_df (float32 force, double-float state)."""
     ics, t = precision_workload(n)
     w0 = torch.tensor(cyl_to_rect(ics).T.copy(), device=dev)
     t_d = torch.tensor(t, device=dev)
@@ -881,7 +892,7 @@ def mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg, n, comps_
 
     res = {}
     outs = {}
-    for prec in ("fp64", "f32force"):
+    for prec in PRECISION_FORMS:
         out = torch.empty((6, 1, n), dtype=torch.float64, device=dev)
         err = torch.empty(n, dtype=torch.int32, device=dev)
         ns = torch.empty(n, dtype=torch.int64, device=dev)
@@ -906,26 +917,28 @@ def mixed_leg(gb, torch, dev, stream, comps_d, ncomp, sig, pt, pa, pg, n, comps_
         gb.energy_device(comps_d, ncomp, out[:, 0, :], E1, stream=stream)
         torch.cuda.synchronize()
         steps = float(ns.sum().item())
-        ms = ms_list[-1]
+        (ms,), (steps,) = over_ranks([ms_list[-1]], [steps], pg, dev)
         res[prec] = {"value": steps / (ms * 1e-3), "unit": "orbit-steps/s", "ms": ms,
                      "launch": autotune.launch_kwargs(tuned),
                      "energy_rel_err": stats(torch.abs(E1 / E0 - 1).cpu().numpy()),
                      "orbits_with_err": int((err != 0).sum().item())}
         outs[prec] = out[:, 0, :]
-    d = torch.abs(outs["f32force"] - outs["fp64"]).max(dim=0).values
     scale = torch.abs(outs["fp64"]).max(dim=0).values
-    res["f32force"]["phase_space_rel_err_vs_fp64"] = stats((d / scale).cpu().numpy())
-    res["speedup_f32force_vs_fp64"] = res["f32force"]["value"] / res["fp64"]["value"]
+    for prec in PRECISION_FORMS[1:]:
+        d = torch.abs(outs[prec] - outs["fp64"]).max(dim=0).values
+        res[prec]["phase_space_rel_err_vs_fp64"] = stats((d / scale).cpu().numpy())
+        res[prec]["speedup_vs_fp64"] = res[prec]["value"] / res["fp64"]["value"]
+    res["speedup_f32force_vs_fp64"] = res["f32force"]["speedup_vs_fp64"]
     res["workload"] = (f"precision: {n} orbits in MWPotential2014 (config-0 initial "
                        "conditions), symplec4 dt=0.01, 20,000 steps, final state only")
-    # both forms against the FP64 oracle (the reference's arithmetic) on a
+    # every form against the FP64 oracle (the reference's arithmetic) on a
     # sample: final phase-space difference and the oracle's own energy drift
     from oracle import oracle as O
 
     m = min(n, 1024)
     ref, eref, _, _ = O.integrate(ics[:m], t, pt, pa, "symplec4", dt=0.01)
     ref_rect = cyl_to_rect(ref[:, -1])
-    for prec in ("fp64", "f32force"):
+    for prec in PRECISION_FORMS:
         g = outs[prec][:, :m].cpu().numpy().T
         dd = np.abs(g - ref_rect).max(axis=1) / np.abs(ref_rect).max(axis=1)
         res[prec]["phase_space_rel_err_vs_oracle"] = stats(dd)
@@ -951,13 +964,15 @@ def rect_to_cyl(w):
 
 
 def f32force_dop853_sample(gb, torch, dev, stream, kind, n_sample=4096, budget=2_000_000):
-    """The FP32-force variant of DOP853 beside FP64 on a random sample of the
+    """The precision forms of DOP853 beside float64 on a random sample of the
     batching (kind "batching": rtol = atol = 1e-10) or ragged ("ragged":
-    1e-9, 8 parameter groups) workload.  DOP853's error estimate sees the
-    single-precision force rounding, so the step count grows: the line gives
-    the accepted-step ratio, both forms' relative energy drift and the final
-    phase-space difference.  A per-orbit attempt budget bounds the run; orbits
-    that exhaust it (err 2) are counted and left out of the error statistics."""
+    1e-9, 8 parameter groups) workload: f32force (float32 force; DOP853's
+    error estimate sees the single-precision force rounding, so its step
+    count grows), f64tail32 and f32bulge.  Per form: the accepted-step ratio
+    and speed ratio to float64, the relative energy drift and the final
+    phase-space difference.  A per-orbit attempt budget bounds the run;
+    orbits that exhaust it (err 2) in any form are counted and left out of
+    the error statistics."""
     rng = np.random.default_rng(99)
     group_d = None
     if kind == "batching":
@@ -989,7 +1004,8 @@ def f32force_dop853_sample(gb, torch, dev, stream, kind, n_sample=4096, budget=2
     E0 = torch.empty(n, dtype=torch.float64, device=dev)
     gb.energy_device(comps_d, ncomp, w0, E0, group=group_d, stream=stream)
     res, fin, steps, errs, ms = {}, {}, {}, {}, {}
-    for prec in ("fp64", "f32force"):
+    forms = ("fp64", "f32force", "f64tail32", "f32bulge")
+    for prec in forms:
         out = torch.empty((6, 1, n), dtype=torch.float64, device=dev)
         err = torch.empty(n, dtype=torch.int32, device=dev)
         ns = torch.empty(n, dtype=torch.int64, device=dev)
@@ -1005,8 +1021,8 @@ def f32force_dop853_sample(gb, torch, dev, stream, kind, n_sample=4096, budget=2
         fin[prec] = out[:, 0, :]
         steps[prec] = ns.cpu().numpy()
         errs[prec] = err.cpu().numpy()
-    ok = (errs["fp64"] == 0) & (errs["f32force"] == 0)
-    for prec in ("fp64", "f32force"):
+    ok = np.logical_and.reduce([errs[p] == 0 for p in forms])
+    for prec in forms:
         E1 = torch.empty(n, dtype=torch.float64, device=dev)
         gb.energy_device(comps_d, ncomp, fin[prec], E1, group=group_d, stream=stream)
         torch.cuda.synchronize()
@@ -1014,12 +1030,15 @@ def f32force_dop853_sample(gb, torch, dev, stream, kind, n_sample=4096, budget=2
         res[prec] = {"accepted_steps": float(steps[prec].sum()), "ms": ms[prec],
                      "orbits_with_err": int((errs[prec] != 0).sum()),
                      "energy_rel_err": stats(rel[ok]) if ok.any() else None}
-    d = (torch.abs(fin["f32force"] - fin["fp64"]).max(dim=0).values /
-         torch.abs(fin["fp64"]).max(dim=0).values).cpu().numpy()
-    res["f32force"]["phase_space_rel_err_vs_fp64"] = stats(d[ok]) if ok.any() else None
-    r = steps["f32force"][ok].sum() / max(1, steps["fp64"][ok].sum())
-    res["accepted_step_ratio_f32force_vs_fp64"] = float(r)
-    res["speed_ratio_f32force_vs_fp64_orbits_per_s"] = ms["fp64"] / ms["f32force"]
+        if prec == "fp64":
+            continue
+        d = (torch.abs(fin[prec] - fin["fp64"]).max(dim=0).values /
+             torch.abs(fin["fp64"]).max(dim=0).values).cpu().numpy()
+        res[prec]["phase_space_rel_err_vs_fp64"] = stats(d[ok]) if ok.any() else None
+        res[prec]["accepted_step_ratio_vs_fp64"] = float(
+            steps[prec][ok].sum() / max(1, steps["fp64"][ok].sum()))
+        res[prec]["speed_ratio_vs_fp64_orbits_per_s"] = ms["fp64"] / ms[prec]
+    res["accepted_step_ratio_f32force_vs_fp64"] = res["f32force"]["accepted_step_ratio_vs_fp64"]
     res["sample"] = (f"{n} random orbits of the {kind} workload" +
                      (" (8 random parameter groups)" if kind == "ragged" else "") +
                      f", dop853 rtol = atol = {tol:g}, attempt budget {budget} per orbit")

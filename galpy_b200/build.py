@@ -1,6 +1,6 @@
 """In-tree build of libgalpy_cuda.so for sm_100a (B200).
 
-``build()`` compiles galpy_b200/csrc/{galpy_cuda,orbit_kernels_more,adjoint}.cu
+``build()`` compiles galpy_b200/csrc/{galpy_cuda,orbit_kernels_more,orbit_kernels_prec,adjoint}.cu
 with nvcc into galpy_b200/libgalpy_cuda.so; the library is loaded from there
 by galpy_b200._lib.  Nothing is installed outside the source tree.
 """
@@ -11,7 +11,7 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgalpy_cuda.so")
-SOURCES = ["galpy_cuda.cu", "orbit_kernels_more.cu", "adjoint.cu"]
+SOURCES = ["galpy_cuda.cu", "orbit_kernels_more.cu", "orbit_kernels_prec.cu", "adjoint.cu"]
 HEADERS = ["gpc_common.cuh", "potentials.cuh", "machines.cuh", "dop853_tableau.cuh",
            "compile_potential.h", "adjoint.cuh", "orbit_kernel.cuh"]
 

@@ -144,6 +144,8 @@ static KernelInfo pick_kernel(int planar, int var, int prec, int method, int sig
                               bool direct, int system = GALPY_CUDA_SYS_ORBIT)
 {
   if (system != GALPY_CUDA_SYS_ORBIT) return pick_kernel_sos(method, variant, system);
+  if (prec >= GALPY_CUDA_F64_TAIL32)
+    return pick_kernel_prec(planar, var, prec, method, sig, variant, direct);
   if (method == M_RK6 || method == M_SYMPLEC6 || method == M_DOPR54)
     return pick_kernel_more(planar, var, prec, method, sig, variant, direct);
   return pick_kernel_in<CoreMethods>(planar, var, prec, method, sig, variant, direct);
@@ -360,7 +362,7 @@ static int check_launch(const galpy_cuda_launch* L)
   if (L->nobj < 0 || L->nt < 1 || !L->t || !L->w0 || !L->out || !L->err || !L->comps ||
       L->ncomp < 1 || L->ncomp > kMaxComp || L->out_row0 < 0 || L->out_row0 >= L->nt)
     return set_error(GALPY_CUDA_ERR_ARG, "invalid launch arguments");
-  if (L->precision != GALPY_CUDA_FP64 && L->precision != GALPY_CUDA_F32FORCE)
+  if (L->precision < GALPY_CUDA_FP64 || L->precision > GALPY_CUDA_F32FORCE_DF)
     return set_error(GALPY_CUDA_ERR_ARG, "unknown precision");
   return GALPY_CUDA_OK;
 }
@@ -890,14 +892,23 @@ int galpy_cuda_accel_device(const void* comps, int ncomp, const int* group, int 
 {
   if (!comps || !pos || !acc || n < 0 || ncomp < 1 || ncomp > kMaxComp)
     return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
-  if (precision != GALPY_CUDA_FP64 && precision != GALPY_CUDA_F32FORCE)
+  if (precision < GALPY_CUDA_FP64 || precision > GALPY_CUDA_F32FORCE_DF)
     return set_error(GALPY_CUDA_ERR_ARG, "unknown precision");
+  const bool mw14 = signature == GALPY_CUDA_SIG_MW14 && ncomp == 3;
+  if ((precision == GALPY_CUDA_F64_TAIL32 || precision == GALPY_CUDA_F32BULGE) && !mw14)
+    return set_error(GALPY_CUDA_ERR_METHOD,
+                     "the mixed float64/float32 forces are built for MWPotential2014 only");
   if (n == 0) return GALPY_CUDA_OK;
   const unsigned blocks = (unsigned)((n + 255) / 256);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const GpComp* c = static_cast<const GpComp*>(comps);
-  const bool mw14 = signature == GALPY_CUDA_SIG_MW14 && ncomp == 3;
-  if (precision == GALPY_CUDA_FP64) {
+  if (precision == GALPY_CUDA_F64_TAIL32) {
+    accel_kernel<MW14MixedPot<false, MIX_TAIL32>, PREC_FP64>
+        <<<blocks, 256, 0, s>>>(c, ncomp, group, planar, pos, n, acc);
+  } else if (precision == GALPY_CUDA_F32BULGE) {
+    accel_kernel<MW14MixedPot<false, MIX_F32BULGE>, PREC_FP64>
+        <<<blocks, 256, 0, s>>>(c, ncomp, group, planar, pos, n, acc);
+  } else if (precision == GALPY_CUDA_FP64) {
     if (mw14)
       accel_kernel<MW14GroupPot, PREC_FP64><<<blocks, 256, 0, s>>>(c, ncomp, group, planar, pos, n, acc);
     else

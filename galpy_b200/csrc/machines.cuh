@@ -28,6 +28,8 @@
 // (their results are only used for output); every orbit has an attempt budget
 // and stops on a non-finite state instead of looping forever.
 #pragma once
+#include <type_traits>
+
 #include "dop853_tableau.cuh"
 #include "gpc_common.cuh"
 #include "potentials.cuh"
@@ -272,9 +274,52 @@ struct Composition<6> {
   }
 };
 
-template <int D, bool VAR, int ORD>
+// ------------------------------------------------------------------------
+// double-float numbers (head + tail floats, ~48 significant bits): the
+// compensated state of the symplectic machines' FP32-force form.  Sums by
+// Knuth's TwoSum, products by Dekker's with a fused multiply-add for the
+// rounding error of the heads' product, each renormalised with Fast2Sum.
+// ------------------------------------------------------------------------
+struct DFloat {
+  float hi, lo;
+};
+GPC_HD GPC_FI DFloat df_of(double x)
+{
+  const float h = (float)x;
+  return {h, (float)(x - (double)h)};
+}
+GPC_HD GPC_FI double df_val(DFloat a) { return (double)a.hi + (double)a.lo; }
+GPC_HD GPC_FI DFloat df_add(DFloat a, DFloat b)
+{
+  const float s = a.hi + b.hi;
+  const float bb = s - a.hi;
+  const float e = ((a.hi - (s - bb)) + (b.hi - bb)) + (a.lo + b.lo);
+  const float h = s + e;
+  return {h, e - (h - s)};
+}
+GPC_HD GPC_FI DFloat df_mul(DFloat a, DFloat b)
+{
+  const float p = a.hi * b.hi;
+  const float e = fmaf(a.hi, b.hi, -p) + (a.hi * b.lo + a.lo * b.hi);
+  const float h = p + e;
+  return {h, e - (h - p)};
+}
+GPC_HD GPC_FI DFloat df_mulf(DFloat a, float f)
+{
+  const float p = a.hi * f;
+  const float e = fmaf(a.hi, f, -p) + a.lo * f;
+  const float h = p + e;
+  return {h, e - (h - p)};
+}
+
+// Running state of a symplectic advance: float64, or double-float (DFloat).
+GPC_HD GPC_FI double state_val(double x) { return x; }
+GPC_HD GPC_FI double state_val(DFloat x) { return df_val(x); }
+
+template <int D, bool VAR, int ORD, class S = double>
 struct SymplecticMachine : OrbitCommon {
   using C = Composition<ORD>;
+  static constexpr bool kDF = !std::is_same<S, double>::value;  // double-float state
   static constexpr int NQ = VAR ? 2 * D : D;  // stepped positions
   static constexpr int NY = NQ;               // size of the force argument
   static constexpr int NV = 2 * NQ;           // values per output row
@@ -291,11 +336,19 @@ struct SymplecticMachine : OrbitCommon {
   }
   enum { EST_FULL = 0, EST_HALF = 1, MAIN = 2 };
   double qo[NQ], po[NQ];  // state at the last output
-  double qw[NQ], pw[NQ];  // state of the running advance
+  S qw[NQ], pw[NQ];       // state of the running advance
   double q11[D], p11[D];  // estimator: the single-step result (base orbit)
   double dt, init_dt, h, sq, sp, rtol, atol;
   long long nrun, kick, nkick;
   int sub, phase;
+  // double-float form: the step's kick and drift coefficients, converted
+  // once per advance (the drift after the last kick of the advance is dlast)
+  DFloat kc0, kc1, kc2, dc0, dc1, dc2, dlast;
+
+  GPC_HD GPC_FI static DFloat pick3(int j, DFloat a, DFloat b, DFloat c)
+  {
+    return j == 0 ? a : (j == 1 ? b : c);
+  }
 
   GPC_HD GPC_FI void start(double hh, long long nstep)
   {
@@ -305,10 +358,27 @@ struct SymplecticMachine : OrbitCommon {
     sub = 0;
     nkick = C::kKicks * nstep;
     const double c = C::first(h);
+    if constexpr (kDF) {
+      static_assert(C::kKicks <= 3, "double-float state: leapfrog and symplec4");
+      kc0 = df_of(C::kick(0, h));
+      kc1 = df_of(C::kick(C::kKicks > 1 ? 1 : 0, h));
+      kc2 = df_of(C::kick(C::kKicks > 2 ? 2 : 0, h));
+      dc0 = df_of(C::drift(0, false, h));
+      dc1 = df_of(C::drift(C::kKicks > 1 ? 1 : 0, false, h));
+      dc2 = df_of(C::drift(C::kKicks > 2 ? 2 : 0, false, h));
+      dlast = df_of(C::drift(C::kKicks - 1, true, h));
+      const DFloat cd = df_of(c);
 #pragma unroll
-    for (int k = 0; k < NQ; k++) {
-      qw[k] = qo[k] + c * po[k];
-      pw[k] = po[k];
+      for (int k = 0; k < NQ; k++) {
+        qw[k] = df_add(df_of(qo[k]), df_mul(cd, df_of(po[k])));
+        pw[k] = df_of(po[k]);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < NQ; k++) {
+        qw[k] = qo[k] + c * po[k];
+        pw[k] = po[k];
+      }
     }
   }
 
@@ -379,20 +449,35 @@ struct SymplecticMachine : OrbitCommon {
 
   GPC_HD GPC_FI void point(double* y, int /*slot*/) const
   {
+    // the double-float form hands its head to the single-precision force
 #pragma unroll
-    for (int k = 0; k < NQ; k++) y[k] = qw[k];
+    for (int k = 0; k < NQ; k++) {
+      if constexpr (kDF)
+        y[k] = (double)qw[k].hi;
+      else
+        y[k] = qw[k];
+    }
   }
 
   template <class W>
   GPC_HD void consume(const double* /*y*/, const double* a, W& out, int /*slot*/)
   {
-    const double dk = C::kick(sub, h);
-#pragma unroll
-    for (int k = 0; k < NQ; k++) pw[k] = pw[k] + dk * a[k];
     const bool last = (kick == nkick - 1);
-    const double dc = C::drift(sub, last, h);
+    if constexpr (kDF) {
+      const DFloat dk = pick3(sub, kc0, kc1, kc2);
 #pragma unroll
-    for (int k = 0; k < NQ; k++) qw[k] = qw[k] + dc * pw[k];
+      for (int k = 0; k < NQ; k++) pw[k] = df_add(pw[k], df_mulf(dk, (float)a[k]));
+      const DFloat dd = last ? dlast : pick3(sub, dc0, dc1, dc2);
+#pragma unroll
+      for (int k = 0; k < NQ; k++) qw[k] = df_add(qw[k], df_mul(dd, pw[k]));
+    } else {
+      const double dk = C::kick(sub, h);
+#pragma unroll
+      for (int k = 0; k < NQ; k++) pw[k] = pw[k] + dk * a[k];
+      const double dc = C::drift(sub, last, h);
+#pragma unroll
+      for (int k = 0; k < NQ; k++) qw[k] = qw[k] + dc * pw[k];
+    }
     kick++;
     sub = sub < C::kKicks - 1 ? sub + 1 : 0;
     if (last) advance_done(out);
@@ -404,8 +489,8 @@ struct SymplecticMachine : OrbitCommon {
     if (phase == EST_FULL) {
 #pragma unroll
       for (int k = 0; k < D; k++) {
-        q11[k] = qw[k];
-        p11[k] = pw[k];
+        q11[k] = state_val(qw[k]);
+        p11[k] = state_val(pw[k]);
       }
       phase = EST_HALF;
       start(dt / 2., 2);
@@ -415,8 +500,8 @@ struct SymplecticMachine : OrbitCommon {
       double e = 0.;
 #pragma unroll
       for (int k = 0; k < D; k++) {
-        e += exp(2. * log(fabs(q11[k] - qw[k])) - 2. * sq);
-        e += exp(2. * log(fabs(p11[k] - pw[k])) - 2. * sp);
+        e += exp(2. * log(fabs(q11[k] - state_val(qw[k]))) - 2. * sq);
+        e += exp(2. * log(fabs(p11[k] - state_val(pw[k]))) - 2. * sp);
       }
       e = sqrt(e / 2. / D);
       if (e > 1. && init_dt / dt < kMaxDtReduce) {
@@ -432,9 +517,9 @@ struct SymplecticMachine : OrbitCommon {
     bool fin = true;
 #pragma unroll
     for (int k = 0; k < NQ; k++) {
-      qo[k] = qw[k];
-      po[k] = pw[k];
-      fin = fin && isfinite(qw[k]) && isfinite(pw[k]);
+      qo[k] = state_val(qw[k]);
+      po[k] = state_val(pw[k]);
+      fin = fin && isfinite(qo[k]) && isfinite(po[k]);
     }
     nsteps += nrun;
     attempts += nrun;

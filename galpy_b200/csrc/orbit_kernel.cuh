@@ -428,6 +428,12 @@ static KernelInfo pick_kernel_in(int planar, int var, int prec, int method, int 
 __attribute__((visibility("hidden"))) KernelInfo pick_kernel_more(int planar, int var, int prec,
                                                                   int method, int sig,
                                                                   int variant, bool direct);
+// the mixed-precision forms (GALPY_CUDA_F64_TAIL32, _F32BULGE,
+// _F32FORCE_DF) of the MWPotential2014 kernels (orbit_kernels_prec.cu; not
+// exported)
+__attribute__((visibility("hidden"))) KernelInfo pick_kernel_prec(int planar, int var, int prec,
+                                                                  int method, int sig,
+                                                                  int variant, bool direct);
 // surface-of-section kernels: rk4, rk6, dopr54, dop853 on the 3D or planar
 // (surface x = 0 / y = 0) system, FP64, run-time component list
 // (orbit_kernels_more.cu; not exported)

@@ -291,6 +291,7 @@ GPC_HD GPC_FI T gamma_star(const GpComp* __restrict__ tp, T u, T scale)
 // the table row.
 struct Binade {
   int ebias;  // e + 1024, in [1, 2047] for normal x
+  int j;      // m's eighth of [1, 2): the table row
   const double* row;
   double t;   // local variable of m's eighth of [1, 2), in [-1, 1)
   double m1;  // m - 1 (exact)
@@ -308,24 +309,69 @@ GPC_HD GPC_FI Binade binade(const GpComp* __restrict__ tp, double x)
   const double mlow = double_of((b & 0x0001ffffffffffffLL) | 0x3ff0000000000000LL);
   r.t = 16.0 * mlow - 17.0;  // exact
   r.m1 = m - 1.0;            // exact
+  r.j = j;
   r.row = tp->bin[j];
   return r;
 }
 
 GPC_HD GPC_FI double horner12(const double* c, double t) { return poly12<double>(c, t); }
 
+// The same polynomial with its tail in single precision:
+//   p(x) = sum_{k<K} c_k x^k + x^K q(x),  q = sum_{k>=K} c_k x^(k-K),
+// the leading K terms in float64 and q (from the single-precision copy of
+// the coefficients, cf) in float32.  K = 4 on the binade tables (local
+// variable over an eighth of [1, 2): |c4 / c0| ~ 1e-5, so q's rounding moves
+// p by ~1e-12 relative), K = 6 on the wider gamma* intervals (|c6 / c0|
+// ~ 1e-5); tests/test_harness.py bounds the resulting force against the
+// float64 one.  Six (K = 4) or nine (K = 6) float64 operations instead of
+// fourteen.
+template <int K>
+GPC_HD GPC_FI double poly12_tail32(const double* __restrict__ c, const float* __restrict__ cf,
+                                   double x)
+{
+  static_assert(K == 4 || K == 6, "float64 head of 4 or 6 terms");
+  const double x2 = x * x;
+  const float xf = (float)x, x2f = xf * xf;
+  if constexpr (K == 4) {
+    const double lead = fma(fma(ldg(c + 3), x, ldg(c + 2)), x2, fma(ldg(c + 1), x, ldg(c + 0)));
+    const float x4f = x2f * x2f;
+    const float q01 = fmaf(ldg(cf + 5), xf, ldg(cf + 4));
+    const float q23 = fmaf(ldg(cf + 7), xf, ldg(cf + 6));
+    const float q45 = fmaf(ldg(cf + 9), xf, ldg(cf + 8));
+    const float q67 = fmaf(ldg(cf + 11), xf, ldg(cf + 10));
+    const float q = fmaf(fmaf(q67, x2f, q45), x4f, fmaf(q23, x2f, q01));
+    return fma(x2 * x2, (double)q, lead);
+  } else {
+    const double x4 = x2 * x2;
+    const double p01 = fma(ldg(c + 1), x, ldg(c + 0)), p23 = fma(ldg(c + 3), x, ldg(c + 2));
+    const double p45 = fma(ldg(c + 5), x, ldg(c + 4));
+    const double lead = fma(p45, x4, fma(p23, x2, p01));
+    const float q01 = fmaf(ldg(cf + 7), xf, ldg(cf + 6));
+    const float q23 = fmaf(ldg(cf + 9), xf, ldg(cf + 8));
+    const float q45 = fmaf(ldg(cf + 11), xf, ldg(cf + 10));
+    const float q = fmaf(q45, x2f * x2f, fmaf(q23, x2f, q01));
+    return fma(x4 * x2, (double)q, lead);
+  }
+}
+
 // (r^2)^(-alpha/2) from the PowerSphericalwCutoff component's tables
+// (TAIL32: the polynomial's tail in single precision, poly12_tail32)
+template <bool TAIL32 = false>
 GPC_HD GPC_FI double pswc_power(const GpComp* __restrict__ tp, double r2)
 {
   const Binade q = binade(tp, r2);
   const double s = ldg(&tp->e2hi[q.ebias >> 6]) * ldg(&tp->e2lo[q.ebias & 63]);
-  return s * horner12(q.row, q.t);
+  if constexpr (TAIL32)
+    return s * poly12_tail32<4>(q.row, tp->binf[q.j], q.t);
+  else
+    return s * horner12(q.row, q.t);
 }
 
 // log1p(x), x >= 0, from the NFW component's table of log(m) / (m - 1)
 // (smooth, 1 at m = 1, so small arguments keep their relative accuracy):
 // u = 1 + x rounded, log1p(x) = log(u) + (x - (u - 1)) / u to first order in
 // the rounding of u.
+template <bool TAIL32 = false>
 GPC_HD GPC_FI double nfw_log1p(const GpComp* __restrict__ tp, double x)
 {
   // ln 2 = ln2_hi + ln2_lo, the head rounded to 32 significant bits so that
@@ -337,7 +383,12 @@ GPC_HD GPC_FI double nfw_log1p(const GpComp* __restrict__ tp, double x)
   const Binade q = binade(tp, u);
   // e as a double without a conversion: 2^52 + ebias, minus 2^52 + 1024
   const double e = double_of(0x4330000000000000LL | (long long)q.ebias) - 4503599627371520.0;
-  return fma(e, ln2_hi, fma(q.m1, horner12(q.row, q.t), fma(e, ln2_lo, corr)));
+  double p;
+  if constexpr (TAIL32)
+    p = poly12_tail32<4>(q.row, tp->binf[q.j], q.t);
+  else
+    p = horner12(q.row, q.t);
+  return fma(e, ln2_hi, fma(q.m1, p, fma(e, ln2_lo, corr)));
 }
 
 // The same log1p in single precision from the float copy of the table.
@@ -688,7 +739,22 @@ GPC_HD GPC_FI T sph_force_factor(int type, const S& sc, T r2)
   }
 }
 
-template <typename T, bool PLANAR, int TYPE, class S>
+// MIX (float64 path only): 0 plain float64; MIX_TAIL32 the table
+// polynomials' tails in float32 (poly12_tail32); MIX_F32BULGE in addition the
+// whole bulge (PowerSphericalwCutoff) term in float32.
+enum : int { MIX_NONE = 0, MIX_TAIL32 = 1, MIX_F32BULGE = 2 };
+
+// gamma*(a, u) with the interpolant's tail in float32 (poly12_tail32).
+GPC_HD GPC_FI double gamma_star_tail32(const GpComp* __restrict__ tp, double u, double scale)
+{
+  const double s = u * scale;
+  double start;
+  const int k = interval_of<double>(s, start);
+  const double x = 2.0 * (s - start) - 1.0;
+  return poly12_tail32<6>(tp->cheb[k], tp->chebf[k], x);
+}
+
+template <typename T, bool PLANAR, int TYPE, class S, int MIX = MIX_NONE>
 GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T y, T z, T z2,
                               T R2, T r2, T& gR, T& gz, T& gyx, AddAcc<T>& a0)
 {
@@ -701,11 +767,23 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
       // F = -amp M(r)/r^3 r_vec
       const T u = r2 * T(sc[1]);
       T f;
-      if constexpr (F64) {
+      if constexpr (F64 && MIX == MIX_F32BULGE) {
+        // the bulge term in float32 (as the FP32-force path), the rest of the
+        // force in float64
+        const float r2f = (float)r2, uf = (float)u;
+        const float pw = Num<float>::ex((float)sc[3] * Num<float>::lg(r2f));
+        const float ir = Num<float>::rsq(r2f);
+        const float inner = (float)sc[2] * pw *
+                            gamma_star<float>(tp, uf < (float)sc[5] ? uf : (float)sc[5],
+                                              (float)sc[6]);
+        const float outer = (float)sc[4] * (ir * ir * ir);
+        f = -amp * (double)(uf < (float)sc[5] ? inner : outer);
+      } else if constexpr (F64) {
         // both forms, then a select: no branch in the force chain
         const double ir = rsqrt_nr(r2);
-        const double inner =
-            sc[2] * pswc_power(tp, r2) * gamma_star<double>(tp, fmin(u, sc[5]), sc[6]);
+        const double g = MIX == MIX_TAIL32 ? gamma_star_tail32(tp, fmin(u, sc[5]), sc[6])
+                                           : gamma_star<double>(tp, fmin(u, sc[5]), sc[6]);
+        const double inner = sc[2] * pswc_power<MIX == MIX_TAIL32>(tp, r2) * g;
         const double outer = sc[4] * (ir * ir * ir);
         f = -amp * (u < sc[5] ? inner : outer);
       } else {  // single precision: hardware log2/exp2 for the power, same select
@@ -737,7 +815,7 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
       if constexpr (F64) {
         const double ir = rsqrt_nr(r2);
         const double r = r2 * ir;
-        f = amp * ir * ir * (rcp_nr(a + r) - nfw_log1p(tp, r * sc[2]) * ir);
+        f = amp * ir * ir * (rcp_nr(a + r) - nfw_log1p<(MIX > MIX_NONE)>(tp, r * sc[2]) * ir);
       } else {
         const T ir = Num<T>::rsq(r2);
         const T r = r2 * ir;
@@ -872,6 +950,35 @@ struct FixedPot {
 // (parameter groups).
 using MW14Pot = FixedPot<true, T_PSWC, T_MN, T_NFW>;
 using MW14GroupPot = FixedPot<false, T_PSWC, T_MN, T_NFW>;
+
+// A compile-time list evaluated in one of the mixed float64 / float32 forms
+// (MIX_TAIL32, MIX_F32BULGE; float64 state and force accumulation).
+template <bool DIRECT, int MIX, int... TYPES>
+struct MixedPot {
+  static constexpr bool kDirectScalars = DIRECT;
+  static constexpr bool kAdditive = false;
+  template <typename T, bool PLANAR>
+  GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, const double* scal, int /*ncomp*/,
+                                T x, T y, T z, T z2, T R2, T r2, T& gR, T& gz, T& gyx,
+                                AddAcc<T>& a0)
+  {
+    int k = 0;
+    if (DIRECT) {
+      ((comp_accel<T, PLANAR, TYPES, ScalarsDirect, MIX>(
+            comp + k, ScalarsDirect{scal + kScalarStride * k}, x, y, z, z2, R2, r2, gR, gz, gyx,
+            a0),
+        ++k),
+       ...);
+    } else {
+      ((comp_accel<T, PLANAR, TYPES, ScalarsGlobal, MIX>(comp + k, ScalarsGlobal{comp + k}, x,
+                                                         y, z, z2, R2, r2, gR, gz, gyx, a0),
+        ++k),
+       ...);
+    }
+  }
+};
+template <bool DIRECT, int MIX>
+using MW14MixedPot = MixedPot<DIRECT, MIX, T_PSWC, T_MN, T_NFW>;
 
 // Acceleration at (x, y, z); PLANAR evaluates galpy's planar potential (the
 // 3D potential in the plane z = 0) and leaves az untouched.

@@ -25,7 +25,12 @@ from .potentials import parse_pot
 _ALIASES = {"leapfrog": 0, "rk4": 1, "rk6": 2, "symplec4": 3, "symplec6": 4, "dopr54": 5,
             "dop853": 6}
 CUDA_METHODS = {f"{name}_cuda": code for name, code in _ALIASES.items()}
-PRECISIONS = {"fp64": _lib.FP64, "f32force": _lib.F32FORCE}
+# precision forms (include/galpy_cuda.h): float64; float32 force with
+# float64 state; float64 force with float32 tails of its table polynomials;
+# that with the bulge term in float32; float32 force with a double-float
+# state (the last three for MWPotential2014-type potentials)
+PRECISIONS = {"fp64": _lib.FP64, "f32force": _lib.F32FORCE, "f64tail32": 2, "f32bulge": 3,
+              "f32force_df": 4}
 # the ODE system of a device launch: orbits, or surface-of-section states
 # (3D rows (x, y, vx, vy, A, t, psi); planar rows (u, vu, A, t, psi) for the
 # surface x = 0 or y = 0)

@@ -48,9 +48,20 @@ extern "C" {
 #define GALPY_CUDA_ERR_NODEVICE (-5)    /* no CUDA device visible */
 #define GALPY_CUDA_ERR_INTERRUPTED (-10) /* SIGINT during the call; err[] holds -10 */
 
-/* precision of the force evaluation (the state is always float64) */
-#define GALPY_CUDA_FP64 0
-#define GALPY_CUDA_F32FORCE 1
+/* precision of the force evaluation and the state.  FP64 and F32FORCE apply
+ * to every method and potential; the three mixed forms to plain (not
+ * variational) runs in MWPotential2014-type potentials
+ * (GALPY_CUDA_SIG_MW14), other combinations return GALPY_CUDA_ERR_METHOD. */
+#define GALPY_CUDA_FP64 0       /* float64 force and state */
+#define GALPY_CUDA_F32FORCE 1   /* float32 force, float64 state */
+#define GALPY_CUDA_F64_TAIL32 2 /* float64 force with the high-order terms of its special-
+                                   function table polynomials in float32 (~1e-11 relative
+                                   force error), float64 state; leapfrog, symplec4, rk4,
+                                   dop853 */
+#define GALPY_CUDA_F32BULGE 3   /* as F64_TAIL32 with the bulge (PowerSphericalwCutoff) term in
+                                   float32; leapfrog, symplec4, rk4, dop853 */
+#define GALPY_CUDA_F32FORCE_DF 4 /* float32 force, compensated double-float (two float32)
+                                    state; leapfrog, symplec4 */
 
 /* array layouts of the device-pointer entry point */
 #define GALPY_CUDA_IN_AOS 0      /* [nobj][nv] rectangular */

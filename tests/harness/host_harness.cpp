@@ -280,6 +280,40 @@ extern "C" int harness_forces(int planar, int n, const double* x, const double* 
   return 0;
 }
 
+// The mixed float64 / float32 MWPotential2014 forces (MIX_TAIL32 = 1,
+// MIX_F32BULGE = 2) at n points, [n][3].
+extern "C" int harness_forces_mixed(int mix, int planar, int n, const double* x, const double* y,
+                                    const double* z, const double* pot_args, double* acc)
+{
+  const int pot_type[3] = {T_PSWC, T_MN, T_NFW};
+  std::vector<GpComp> comps(3);
+  int rc = compile_group(planar, 3, pot_type, pot_args, comps.data(), nullptr);
+  if (rc) return rc;
+  for (int i = 0; i < n; i++) {
+    double ax = 0, ay = 0, az = 0;
+    const double zi = planar ? 0.0 : z[i];
+    if (mix == MIX_TAIL32) {
+      if (planar)
+        accel<double, true, MW14MixedPot<false, MIX_TAIL32>>(comps.data(), 3, x[i], y[i], zi,
+                                                            ax, ay, az);
+      else
+        accel<double, false, MW14MixedPot<false, MIX_TAIL32>>(comps.data(), 3, x[i], y[i], zi,
+                                                             ax, ay, az);
+    } else {
+      if (planar)
+        accel<double, true, MW14MixedPot<false, MIX_F32BULGE>>(comps.data(), 3, x[i], y[i], zi,
+                                                              ax, ay, az);
+      else
+        accel<double, false, MW14MixedPot<false, MIX_F32BULGE>>(comps.data(), 3, x[i], y[i],
+                                                               zi, ax, ay, az);
+    }
+    acc[3 * i] = ax;
+    acc[3 * i + 1] = ay;
+    acc[3 * i + 2] = az;
+  }
+  return 0;
+}
+
 // ------------------------------------------------------------- adjoint ---
 #include "../../galpy_b200/csrc/adjoint.cuh"
 

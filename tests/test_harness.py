@@ -365,3 +365,37 @@ def test_dop853_queued_dense_output(harness, oracle, golden, planar):
         assert np.array_equal(err, eref) and np.array_equal(ns, nref)
         assert np.array_equal(out, ref, equal_nan=True)
     assert (eref == 2).all()  # the budget stops every orbit
+
+
+@pytest.mark.parametrize("planar", [False, True])
+def test_mixed_precision_forces(harness, golden, planar):
+    """The mixed float64 / float32 MWPotential2014 forces against the
+    float64 force over the radii the integrations visit (0.01 to 30, all
+    polynomial intervals of the tables): the float32 tails of the table
+    polynomials (F64_TAIL32) move the force by < 1e-11 relative; the float32
+    bulge term (F32BULGE) by the single-precision log2 / exp2 of its power
+    law, up to ~1e-6 of the total where the bulge dominates (r < 0.1)."""
+    import ctypes
+
+    pt, pa = ((golden["mw14_planar_type"], golden["mw14_planar_args"]) if planar
+              else (golden["mw14_type"], golden["mw14_args"]))
+    rng = np.random.default_rng(17)
+    n = 20000
+    r = np.exp(rng.uniform(np.log(0.01), np.log(30.0), n))
+    th = np.arccos(rng.uniform(-1, 1, n)) if not planar else np.full(n, np.pi / 2)
+    ph = rng.uniform(0, 2 * np.pi, n)
+    x, y, z = r * np.sin(th) * np.cos(ph), r * np.sin(th) * np.sin(ph), r * np.cos(th)
+    ref, _, _ = harness.forces(x, y, z, pt, pa, planar=planar)
+    pa_c = np.ascontiguousarray(pa, np.float64)
+    dp = ctypes.POINTER(ctypes.c_double)
+    for mix, tol in ((1, 1e-11), (2, 3e-6)):
+        acc = np.zeros((n, 3))
+        rc = harness.lib.harness_forces_mixed(
+            mix, int(planar), n, np.ascontiguousarray(x).ctypes.data_as(dp),
+            np.ascontiguousarray(y).ctypes.data_as(dp), np.ascontiguousarray(z).ctypes.data_as(dp),
+            pa_c.ctypes.data_as(dp), acc.ctypes.data_as(dp))
+        assert rc == 0
+        rel = np.abs(acc - ref).max(axis=1) / np.abs(ref).max(axis=1)
+        assert rel.max() < tol, (mix, rel.max())
+        if mix == 1:
+            assert rel.max() > 0  # the tails are in float32 indeed
