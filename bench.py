@@ -347,6 +347,9 @@ def main():
                          "groups, variational, sos; runs one warm-up and one launch of that "
                          "kernel on a small batch (--orbits, default 65,536) and prints its "
                          "time, nothing else")
+    ap.add_argument("--variant", type=int, default=None,
+                    help="pin the register variant of the headline kernel (0 compiler "
+                         "budget, 1 capped) instead of the autotuner's choice")
     ap.add_argument("--case", default="batching", choices=["batching", "uniform", "longest"],
                     help="uniform: R ~ U(0.5, 2), shared t in [0, 50] (101 snapshots) "
                          "(a throughput-bound case for profiling the same kernel); longest: "
@@ -436,6 +439,8 @@ def main():
 
     tuned = autotune.tune(comps_d, ncomp, w0, t_d, out, err, "dop853_cuda", rtol=RTOL,
                           atol=ATOL, signature=sig, comps_host=comps)
+    if args.variant is not None:
+        tuned = dict(tuned, variant=args.variant, pinned_variant=True)
     graph = IntegrationGraph(comps_d, ncomp, w0, t_d, out, err, "dop853_cuda", nsteps=nsteps,
                              rtol=RTOL, atol=ATOL, precision="fp64", signature=sig,
                              comps_host=comps, **autotune.launch_kwargs(tuned))
@@ -779,7 +784,7 @@ def profile_leg(gb, torch, dev, spec, n):
         sig = 0
     w0 = torch.tensor(np.ascontiguousarray(w.T), device=dev)
     t_d = torch.tensor(t, device=dev)
-    out = torch.empty((nv, len(t), n), dtype=torch.float64, device=dev)
+    out = torch.empty((nv, t.shape[-1], n), dtype=torch.float64, device=dev)
     err = torch.empty(n, dtype=torch.int32, device=dev)
     ns = torch.empty(n, dtype=torch.int64, device=dev)
     ms = []

@@ -61,6 +61,7 @@ class GalpyCudaOpts(ctypes.Structure):
         ("elapsed_ms", ctypes.POINTER(ctypes.c_double)),
         ("variant", ctypes.c_int),
         ("schedule", ctypes.c_int),
+        ("stream_rows", ctypes.c_int),
     ]
 
 
@@ -236,7 +237,7 @@ def check(code):
 
 
 def make_opts(precision=FP64, device=-1, block_size=0, max_attempts=0, nsteps=None,
-              elapsed=None, variant=0, schedule=1):
+              elapsed=None, variant=0, schedule=1, stream_rows=-1):
     o = GalpyCudaOpts()
     o.size = ctypes.sizeof(GalpyCudaOpts)
     o.device = device
@@ -249,4 +250,5 @@ def make_opts(precision=FP64, device=-1, block_size=0, max_attempts=0, nsteps=No
         o.elapsed_ms = ctypes.pointer(elapsed)
     o.variant = variant
     o.schedule = schedule
+    o.stream_rows = stream_rows
     return o

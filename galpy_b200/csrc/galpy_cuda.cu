@@ -24,13 +24,17 @@
 #include <cuda.h>  // CUcontext and CUresult only; no driver symbol is linked
 #include <cuda_runtime.h>
 #include <signal.h>
+#include <stddef.h>
 #include <stdio.h>
 #include <string.h>
 #include <time.h>
 
+#include <algorithm>
 #include <atomic>
+#include <condition_variable>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/galpy_cuda.h"
@@ -168,9 +172,19 @@ struct Scratch {  // device scratch of one launch (128 bytes)
   unsigned long long counter;
   unsigned long long done_count;
   unsigned long long tail_counter;
+  unsigned long long stage_claim;  // staging slots taken (streaming of finished orbits)
   int abort_flag;
   unsigned sm_claim[kMaxTailSms];  // first block resident on each reserved SM
-  int pad[5];
+  int pad[7];
+};
+static_assert(sizeof(Scratch) == 128, "Scratch layout");
+
+// Device buffers of the streaming of finished orbits (RowStreamer).
+struct Staging {
+  double* rows = nullptr;     // [nobj][row] in completion order
+  int* idx = nullptr;         // [nobj] orbit of each slot
+  unsigned* ready = nullptr;  // [nchunk] staged slots per chunk
+  int* pend = nullptr;        // [nobj] unfinished row writers per orbit
 };
 
 // Launch on `stream`.  scratch: device Scratch (counter zeroed here).
@@ -194,7 +208,7 @@ static cudaError_t alloc_async(void** p, size_t bytes, cudaMemPool_t pool, cudaS
 // Kernel and kernel arguments of a launch, with the control words pointed
 // into `scratch` (a Scratch in device memory, cleared by the caller).
 static int prepare_launch(const galpy_cuda_launch* L, Scratch* scratch, bool progress,
-                          KernelInfo& ki, KArgs& A)
+                          KernelInfo& ki, KArgs& A, const Staging* stg = nullptr)
 {
   double scal[kMaxComp * kScalarStride] = {0.0};
   const bool direct = direct_scalars(L, scal);
@@ -229,6 +243,13 @@ static int prepare_launch(const galpy_cuda_launch* L, Scratch* scratch, bool pro
   A.done_count = progress ? &scratch->done_count : nullptr;
   A.variational_nv = L->variational ? (L->planar ? 8 : 12) : 0;
   memcpy(A.scal, scal, sizeof(scal));
+  if (stg) {
+    A.stage_rows = stg->rows;
+    A.stage_idx = stg->idx;
+    A.stage_ready = stg->ready;
+    A.pend = stg->pend;
+    A.stage_claim = &scratch->stage_claim;
+  }
   return GALPY_CUDA_OK;
 }
 
@@ -294,11 +315,12 @@ static int launch_persistent(const galpy_cuda_launch* L, const KernelInfo& ki, K
 }
 
 static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool progress,
-                         cudaStream_t stream, cudaMemPool_t pool = nullptr)
+                         cudaStream_t stream, cudaMemPool_t pool = nullptr,
+                         const Staging* stg = nullptr)
 {
   KernelInfo ki;
   KArgs A;
-  int rc = prepare_launch(L, scratch, progress, ki, A);
+  int rc = prepare_launch(L, scratch, progress, ki, A, stg);
   if (rc) return rc;
   const int system = launch_system(L);
   GPC_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(Scratch), stream));
@@ -450,6 +472,208 @@ static int select_device(const galpy_cuda_opts* o)
   return GALPY_CUDA_OK;
 }
 
+// ----------------------------------------------------------------------------
+// streaming of finished orbits to the host
+// ----------------------------------------------------------------------------
+// The blocking entry points return galpy's AoS result rows in host memory
+// (pinned or pageable numpy arrays).  Copying the whole result after the
+// kernel would add the full device->host transfer (5 GB for the batching
+// workload) to the call.  Instead the kernel copies every finished orbit's
+// rows to a staging array in completion order (stage_orbit), and while it
+// runs this streamer copies the finished 4096-orbit chunks of the staging
+// array through pinned bounce buffers on a copy stream, and worker threads
+// scatter their rows to the orbits' places in the caller's result array.
+// Pinned bounce buffers of RowStreamer, kept for later calls (pinning host
+// memory is slow); at most kBounceCache of them stay cached.
+static std::mutex g_bounce_mu;
+static std::vector<void*> g_bounce_free;
+constexpr size_t kBounceCache = 8;
+
+static cudaError_t bounce_get(void** p, size_t bytes)
+{
+  {
+    std::lock_guard<std::mutex> lk(g_bounce_mu);
+    if (!g_bounce_free.empty()) {
+      *p = g_bounce_free.back();
+      g_bounce_free.pop_back();
+      return cudaSuccess;
+    }
+  }
+  return cudaMallocHost(p, bytes);
+}
+
+static void bounce_put(void* p)
+{
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(g_bounce_mu);
+  if (g_bounce_free.size() < kBounceCache)
+    g_bounce_free.push_back(p);
+  else
+    cudaFreeHost(p);
+}
+
+class RowStreamer {
+ public:
+  static constexpr size_t kBounceBytes = 32u << 20;
+  static constexpr int kBuffers = 4;
+
+  RowStreamer(const Staging& st, long long nobj, size_t row, double* result,
+              cudaStream_t side)
+      : st_(st), nobj_(nobj), row_(row), result_(result), side_(side)
+  {
+    nchunk_ = (int)((nobj + kStageChunk - 1) / kStageChunk);
+    per_buf_ = (long long)(kBounceBytes / (row * sizeof(double)));
+    if (per_buf_ < 1) per_buf_ = 1;
+    if (per_buf_ > kStageChunk) per_buf_ = kStageChunk;
+  }
+
+  ~RowStreamer()
+  {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : workers_) t.join();
+    if (copy_) cudaStreamDestroy(copy_);
+    for (auto& b : buf_) {
+      if (b.ev) cudaEventDestroy(b.ev);
+      bounce_put(b.rows);
+      if (b.idx) cudaFreeHost(b.idx);
+    }
+    if (ready_h_) cudaFreeHost(ready_h_);
+  }
+
+  cudaError_t start()
+  {
+    cudaError_t e = cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMallocHost(&ready_h_, nchunk_ * sizeof(unsigned))) != cudaSuccess) return e;
+    for (auto& b : buf_) {
+      void* p = nullptr;
+      if ((e = bounce_get(&p, kBounceBytes)) != cudaSuccess) return e;
+      b.rows = static_cast<double*>(p);
+      if ((e = cudaMallocHost(&b.idx, per_buf_ * sizeof(int))) != cudaSuccess) return e;
+      if ((e = cudaEventCreateWithFlags(&b.ev, cudaEventDisableTiming)) != cudaSuccess) return e;
+    }
+    unsigned nt = std::thread::hardware_concurrency();
+    nworkers_ = nt < 2 ? 1 : (nt > 16 ? 16 : (int)nt);
+    for (int k = 0; k < nworkers_; k++) workers_.emplace_back([this] { work(); });
+    return cudaSuccess;
+  }
+
+  // Issue the copies of finished chunks and hand finished copies to the
+  // workers; returns whether every orbit has been delivered.
+  cudaError_t poll(bool& all_done)
+  {
+    cudaError_t e;
+    if (next_slot_ < nobj_) {
+      if ((e = cudaMemcpyAsync(ready_h_, st_.ready, nchunk_ * sizeof(unsigned),
+                               cudaMemcpyDeviceToHost, side_)) != cudaSuccess)
+        return e;
+      if ((e = cudaStreamSynchronize(side_)) != cudaSuccess) return e;
+    }
+    for (auto& b : buf_) {
+      if (b.state != 1) continue;
+      e = cudaEventQuery(b.ev);
+      if (e == cudaErrorNotReady) continue;
+      if (e != cudaSuccess) return e;
+      b.state = 2;
+      enqueue(b);
+    }
+    // copies, in slot order, of the slots whose chunk is complete
+    for (auto& b : buf_) {
+      if (next_slot_ >= nobj_) break;
+      if (b.state != 0) continue;
+      const int c = (int)(next_slot_ / kStageChunk);
+      const long long csize = std::min<long long>(kStageChunk, nobj_ - (long long)c * kStageChunk);
+      if (ready_h_[c] < (unsigned)csize) break;
+      const long long chunk_end = (long long)c * kStageChunk + csize;
+      const long long n = std::min(per_buf_, chunk_end - next_slot_);
+      if ((e = cudaMemcpyAsync(b.rows, st_.rows + next_slot_ * row_, n * row_ * sizeof(double),
+                               cudaMemcpyDeviceToHost, copy_)) != cudaSuccess)
+        return e;
+      if ((e = cudaMemcpyAsync(b.idx, st_.idx + next_slot_, n * sizeof(int),
+                               cudaMemcpyDeviceToHost, copy_)) != cudaSuccess)
+        return e;
+      if ((e = cudaEventRecord(b.ev, copy_)) != cudaSuccess) return e;
+      b.count = n;
+      b.state = 1;
+      next_slot_ += n;
+    }
+    all_done = next_slot_ >= nobj_ && delivered_.load() >= nobj_;
+    return cudaSuccess;
+  }
+
+ private:
+  struct Buf {
+    double* rows = nullptr;
+    int* idx = nullptr;
+    cudaEvent_t ev = nullptr;
+    long long count = 0;
+    std::atomic<int> state{0};  // 0 free, 1 copying, 2 scattering (workers free it)
+    std::atomic<int> parts{0};
+  };
+  struct Job {
+    Buf* b;
+    long long k0, k1;
+  };
+
+  void enqueue(Buf& b)
+  {
+    const int parts = (int)std::min<long long>(nworkers_, b.count);
+    b.parts.store(parts);
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      for (int p = 0; p < parts; p++)
+        jobs_.push_back({&b, b.count * p / parts, b.count * (p + 1) / parts});
+    }
+    cv_.notify_all();
+  }
+
+  void work()
+  {
+    for (;;) {
+      Job j;
+      {
+        std::unique_lock<std::mutex> lk(mu_);
+        cv_.wait(lk, [this] { return stop_ || !jobs_.empty(); });
+        if (jobs_.empty()) return;
+        j = jobs_.back();
+        jobs_.pop_back();
+      }
+      for (long long k = j.k0; k < j.k1; k++)
+        memcpy(result_ + (size_t)j.b->idx[k] * row_, j.b->rows + (size_t)k * row_,
+               row_ * sizeof(double));
+      delivered_.fetch_add(j.k1 - j.k0);
+      if (j.b->parts.fetch_sub(1) == 1) j.b->state = 0;  // the buffer is free again
+    }
+  }
+
+  Staging st_;
+  long long nobj_;
+  size_t row_;
+  double* result_;
+  cudaStream_t side_, copy_ = nullptr;
+  int nchunk_ = 0, nworkers_ = 1;
+  long long per_buf_ = 1, next_slot_ = 0;
+  unsigned* ready_h_ = nullptr;
+  Buf buf_[kBuffers];
+  std::vector<std::thread> workers_;
+  std::vector<Job> jobs_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  bool stop_ = false;
+  std::atomic<long long> delivered_{0};
+};
+
+// Streaming pays off when the result is large (its transfer is then a
+// sizeable part of the call) and spans several chunks.
+static bool stream_rows_for(long long nobj, size_t n_out)
+{
+  return nobj >= 4LL * kStageChunk && n_out * sizeof(double) >= (size_t)(256u << 20);
+}
+
 // Blocking host-pointer integration shared by the galpy-facing entry points.
 // w: rectangular initial states [nobj][nv]; result written in galpy's layout
 // (cylindrical rows) unless rect_out.
@@ -496,6 +720,28 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
   GPC_CUDA_TRY(alloc_async(&dcomp.p, comps.size() * sizeof(GpComp), pool, stream));
   GPC_CUDA_TRY(alloc_async(&dscr.p, sizeof(Scratch), pool, stream));
   if (o && o->nsteps) GPC_CUDA_TRY(alloc_async(&dsteps.p, (size_t)nobj * sizeof(long long), pool, stream));
+  // streaming of finished orbits (RowStreamer): staging rows, slot orbits,
+  // per-chunk ready counts, per-orbit writer counts
+  const int stream_opt =
+      o && o->size >= (int)(offsetof(galpy_cuda_opts, stream_rows) + sizeof(int))
+          ? o->stream_rows
+          : -1;
+  const bool stream_rows = stream_opt == 1 || (stream_opt < 0 && stream_rows_for(nobj, n_out));
+  DevBuf srows, sidx, sready, spend;
+  srows.s = sidx.s = sready.s = spend.s = stream;
+  Staging stg;
+  if (stream_rows) {
+    const size_t nchunk = (size_t)((nobj + kStageChunk - 1) / kStageChunk);
+    GPC_CUDA_TRY(alloc_async(&srows.p, n_out * sizeof(double), pool, stream));
+    GPC_CUDA_TRY(alloc_async(&sidx.p, (size_t)nobj * sizeof(int), pool, stream));
+    GPC_CUDA_TRY(alloc_async(&sready.p, nchunk * sizeof(unsigned), pool, stream));
+    GPC_CUDA_TRY(alloc_async(&spend.p, (size_t)nobj * sizeof(int), pool, stream));
+    GPC_CUDA_TRY(cudaMemsetAsync(sready.p, 0, nchunk * sizeof(unsigned), stream));
+    stg.rows = static_cast<double*>(srows.p);
+    stg.idx = static_cast<int*>(sidx.p);
+    stg.ready = static_cast<unsigned*>(sready.p);
+    stg.pend = static_cast<int*>(spend.p);
+  }
   GPC_CUDA_TRY(cudaMemcpyAsync(dw.p, w, n_w * sizeof(double), cudaMemcpyHostToDevice, stream));
   GPC_CUDA_TRY(cudaMemcpyAsync(dt_.p, t, n_t * sizeof(double), cudaMemcpyHostToDevice, stream));
   GPC_CUDA_TRY(cudaMemcpyAsync(dcomp.p, comps.data(), comps.size() * sizeof(GpComp),
@@ -527,9 +773,9 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
   L.max_attempts = o ? o->max_attempts : 0;
   L.block_size = o ? o->block_size : 0;
   L.signature = signature_of(npot, pot_type);
-  L.schedule = o && o->size >= (int)sizeof(galpy_cuda_opts) ? o->schedule
-                                                             : GALPY_CUDA_SCHED_LONGEST_FIRST;
-  L.variant = o && o->size >= (int)sizeof(galpy_cuda_opts) ? o->variant : 0;
+  const bool has_sched = o && o->size >= (int)(offsetof(galpy_cuda_opts, schedule) + sizeof(int));
+  L.schedule = has_sched ? o->schedule : GALPY_CUDA_SCHED_LONGEST_FIRST;
+  L.variant = has_sched ? o->variant : 0;
   L.size_ext = 2;
   L.tail_sms = -1;
   L.system = system;
@@ -549,46 +795,65 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
     }
   } eg{e0, e1};
   SigintGuard sig;
+  RowStreamer streamer(stg, nobj, (size_t)nt * nv, result, side);
+  if (stream_rows) GPC_CUDA_TRY(streamer.start());
   GPC_CUDA_TRY(cudaEventRecord(e0, stream));
-  rc = launch_kernel(&L, scr, cb != nullptr, stream, pool);
+  rc = launch_kernel(&L, scr, cb != nullptr, stream, pool, stream_rows ? &stg : nullptr);
   if (rc) return rc;
   GPC_CUDA_TRY(cudaEventRecord(e1, stream));
 
-  // wait: poll completion, forward SIGINT to the device, drive the progress callback
+  // wait: poll completion, forward SIGINT to the device, drive the progress
+  // callback, stream the finished orbits' rows to the result
   unsigned long long reported = 0, *pinned_done = nullptr;
   if (cb) GPC_CUDA_TRY(cudaMallocHost(&pinned_done, sizeof(unsigned long long)));
-  bool abort_sent = false;
-  for (;;) {
-    cudaError_t q = cudaEventQuery(e1);
-    if (q == cudaSuccess) break;
-    if (q != cudaErrorNotReady) {
-      if (pinned_done) cudaFreeHost(pinned_done);
-      return set_error(GALPY_CUDA_ERR_CUDA, std::string("integration kernel: ") + cudaGetErrorString(q));
+  struct PinGuard {
+    unsigned long long* p;
+    ~PinGuard()
+    {
+      if (p) cudaFreeHost(p);
     }
+  } pg{pinned_done};
+  bool abort_sent = false, kernel_done = false, rows_done = !stream_rows;
+  for (;;) {
+    if (!kernel_done) {
+      cudaError_t q = cudaEventQuery(e1);
+      if (q == cudaSuccess)
+        kernel_done = true;
+      else if (q != cudaErrorNotReady)
+        return set_error(GALPY_CUDA_ERR_CUDA,
+                         std::string("integration kernel: ") + cudaGetErrorString(q));
+    }
+    if (stream_rows && !rows_done) {
+      cudaError_t q = streamer.poll(rows_done);
+      if (q != cudaSuccess)
+        return set_error(GALPY_CUDA_ERR_CUDA,
+                         std::string("result streaming: ") + cudaGetErrorString(q));
+    }
+    if (kernel_done && rows_done) break;
     if (g_sigint && !abort_sent) {
       static const int one = 1;
       cudaMemcpyAsync(&scr->abort_flag, &one, sizeof(int), cudaMemcpyHostToDevice, side);
       abort_sent = true;
     }
-    if (cb) {
+    if (cb && !kernel_done) {
       cudaMemcpyAsync(pinned_done, &scr->done_count, sizeof(unsigned long long),
                       cudaMemcpyDeviceToHost, side);
       cudaStreamSynchronize(side);
       for (; reported < *pinned_done; reported++) cb();
     }
-    struct timespec ts = {0, 2000000};
+    struct timespec ts = {0, stream_rows ? 500000 : 2000000};
     nanosleep(&ts, nullptr);
   }
-  if (cb) {
+  if (cb)
     for (; reported < (unsigned long long)nobj; reported++) cb();
-    cudaFreeHost(pinned_done);
-  }
   if (o && o->elapsed_ms) {
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
     *o->elapsed_ms = ms;
   }
-  GPC_CUDA_TRY(cudaMemcpyAsync(result, dout.p, n_out * sizeof(double), cudaMemcpyDeviceToHost, stream));
+  if (!stream_rows)
+    GPC_CUDA_TRY(cudaMemcpyAsync(result, dout.p, n_out * sizeof(double), cudaMemcpyDeviceToHost,
+                                 stream));
   GPC_CUDA_TRY(cudaMemcpyAsync(err, derr.p, (size_t)nobj * sizeof(int), cudaMemcpyDeviceToHost, stream));
   if (o && o->nsteps)
     GPC_CUDA_TRY(cudaMemcpyAsync(o->nsteps, dsteps.p, (size_t)nobj * sizeof(long long),

@@ -47,6 +47,19 @@ struct KArgs {
   // DOP853 dense-output request queues, one ring of M::kQueueSlots records
   // per warp of the grid (NULL: dense output in the warp's slot cycle)
   double* dense_q;
+  // Streaming of finished orbits (blocking host entry points, AoS output):
+  // when an orbit's last row is written, its rows are copied to
+  // stage_rows[slot] with slot taken in completion order, stage_idx[slot]
+  // records the orbit, and stage_ready[slot / kStageChunk] counts the staged
+  // slots of each chunk, so that the host can copy finished chunks while the
+  // kernel runs.  pend[i] counts the writers of orbit i's rows that have not
+  // finished (its own lane, and its queued dense-output requests).  NULL:
+  // no streaming.
+  double* stage_rows;
+  int* stage_idx;
+  unsigned long long* stage_claim;
+  unsigned* stage_ready;
+  int* pend;
   // scalar parameters of the (single) potential, read from the constant bank
   // by the kernels whose POT takes them directly
   double scal[kMaxComp * kScalarStride];
@@ -91,6 +104,42 @@ __device__ __forceinline__ bool tail_claimed(const KArgs& A)
     if (*reinterpret_cast<const volatile unsigned*>(&A.sm_claim[k])) return true;
   return false;
 }
+
+// Staged slots per chunk of the streaming of finished orbits.
+constexpr int kStageChunk = 4096;
+
+#if defined(__CUDACC__)
+// Orbit i is complete (all of its rows written, by whichever lanes wrote
+// them, and made visible with __threadfence): copy its rows (AoS, nrow * nv
+// contiguous doubles) to the next staging slot and publish it.
+static __device__ __noinline__ void stage_orbit(const KArgs& A, long long i, int nv)
+{
+  const long long slot = (long long)atomicAdd(A.stage_claim, 1ULL);
+  const long long row = (long long)(A.out.nt - A.out.row0) * nv;
+  const double* src = A.out.out + i * row;
+  double* dst = A.stage_rows + slot * row;
+  if ((row & 1) == 0) {
+    const double2* s2 = reinterpret_cast<const double2*>(src);
+    double2* d2 = reinterpret_cast<double2*>(dst);
+    for (long long k = 0; k < row / 2; k++) d2[k] = s2[k];
+  } else {
+    for (long long k = 0; k < row; k++) dst[k] = src[k];
+  }
+  A.stage_idx[slot] = (int)i;
+  __threadfence();
+  atomicAdd(&A.stage_ready[slot / kStageChunk], 1u);
+}
+
+// One writer of orbit i's rows has finished: the last one stages the orbit.
+__device__ __forceinline__ void release_orbit(const KArgs& A, long long i, int nv)
+{
+  __threadfence();  // this writer's rows before the count
+  if (atomicSub(&A.pend[i], 1) == 1) {
+    __threadfence();  // the other writers' rows before the copy
+    stage_orbit(A, i, nv);
+  }
+}
+#endif
 
 // Next orbit of a worker: the reserved-SM tail queue first (tail role), then
 // the main queue; -1 when both are exhausted.
@@ -158,8 +207,13 @@ __device__ __forceinline__ void queued_loop(const KArgs& A, double* slot_store, 
       } else if (aborting) {
         A.err[o] = E_ABORT;
         write_nan_rows<M::NV, D, CYL_OK, M::kRow>(A.out, o, 0);
+        if (A.stage_rows) {
+          __threadfence();
+          stage_orbit(A, o, M::NV);
+        }
       } else {
         i = o;
+        if (A.pend) A.pend[i] = 1;  // its own lane writes rows until it is done
         double w[M::NV];
         load_state<M>(A, i, w);
         comps = A.comps + (A.group ? (long long)A.group[i] * A.ncomp : 0LL);
@@ -184,16 +238,19 @@ __device__ __forceinline__ void queued_loop(const KArgs& A, double* slot_store, 
       M::pos(y, qq);
       eval_force<D, PREC, VAR, POT>(cp, A.ncomp, qq, a, A.scal);
       Rows rows{&A.out, o};
-      if (dense)
+      if (dense) {
         m.req_consume(y, a, slot + 2, q, p, A.t + (A.indiv_t ? o * (long long)A.nt : 0LL), rows);
-      else
+        if (A.stage_rows && slot == 14) release_orbit(A, o, M::NV);  // its rows are written
+      } else {
         m.consume(y, a, rows, slot);
+      }
     }
     // the requests of this slot's accepted steps (only the FSAL slot makes any)
     if (slot == 11) {
       const unsigned want = __ballot_sync(FULL, m.want_enqueue);
       if (m.want_enqueue) {
         const int rank = __popc(want & ((1u << lane) - 1u));
+        if (A.pend) atomicAdd(&A.pend[i], 1);  // the request writes rows of orbit i
         m.write_request(q, (qhead + qcount + rank) & (QS - 1), i);
         m.want_enqueue = false;
         Rows rows{&A.out, i};
@@ -236,6 +293,7 @@ __device__ __forceinline__ void queued_loop(const KArgs& A, double* slot_store, 
       A.err[i] = m.err;
       if (A.nsteps) A.nsteps[i] = m.nsteps;
       if (A.done_count) atomicAdd(A.done_count, 1ULL);
+      if (A.stage_rows) release_orbit(A, i, M::NV);
       active = false;
     }
   }
@@ -307,6 +365,10 @@ __global__ void __launch_bounds__(128, MINB) orbit_kernel(const __grid_constant_
       if (aborting) {
         A.err[i] = E_ABORT;
         write_nan_rows<M::NV, D, CYL_OK, M::kRow>(A.out, i, 0);
+        if (A.stage_rows) {
+          __threadfence();
+          stage_orbit(A, i, M::NV);
+        }
         continue;
       }
       double w[M::NV];
@@ -345,6 +407,10 @@ __global__ void __launch_bounds__(128, MINB) orbit_kernel(const __grid_constant_
       A.err[i] = m.err;
       if (A.nsteps) A.nsteps[i] = m.nsteps;
       if (A.done_count) atomicAdd(A.done_count, 1ULL);
+      if (A.stage_rows) {
+        __threadfence();
+        stage_orbit(A, i, M::NV);
+      }
       active = false;
     }
   }

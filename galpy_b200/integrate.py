@@ -69,7 +69,7 @@ def _precision(p):
 
 
 def _integrate_c(planar, pot, yo, t, int_method, rtol, atol, progressbar, dt, precision,
-                 max_attempts, return_nsteps, device):
+                 max_attempts, return_nsteps, device, stream_rows=-1):
     single_obj = yo.ndim == 1
     yo = np.atleast_2d(yo)
     nobj = len(yo)
@@ -87,7 +87,7 @@ def _integrate_c(planar, pot, yo, t, int_method, rtol, atol, progressbar, dt, pr
     yo = np.require(yo, dtype=np.float64, requirements=["C", "W"])
     t = np.require(t, dtype=np.float64, requirements=["C", "W"])
     opts = _lib.make_opts(precision=_precision(precision), device=device,
-                          max_attempts=max_attempts, nsteps=nsteps)
+                          max_attempts=max_attempts, nsteps=nsteps, stream_rows=stream_rows)
     cb = _lib.CALLBACK()
     pbar = None
     if progressbar and nobj > 1:
@@ -115,29 +115,32 @@ def _integrate_c(planar, pot, yo, t, int_method, rtol, atol, progressbar, dt, pr
 
 def integrateFullOrbit_cuda(pot, yo, t, int_method, rtol=None, atol=None, progressbar=True,
                             dt=None, precision="fp64", max_attempts=0, return_nsteps=False,
-                            device=-1):
+                            device=-1, stream_rows=-1):
     """Integrate 3D orbits on the GPU.
 
     Parameters mirror galpy's integrateFullOrbit_c: yo [N,6] or [6]
     cylindrical (R,vR,vT,z,vz,phi) -- overwritten in place with rectangular
     coordinates when it is a C-contiguous float64 array, as in galpy; t [nt]
     or [N,nt]; int_method one of 'leapfrog_cuda', 'rk4_cuda', 'rk6_cuda',
-    'symplec4_cuda', 'symplec6_cuda', 'dopr54_cuda', 'dop853_cuda'.  Extra keywords: precision ('fp64' or 'f32force'),
-    max_attempts (per-orbit step-attempt budget, 0 = none), return_nsteps.
+    'symplec4_cuda', 'symplec6_cuda', 'dopr54_cuda', 'dop853_cuda'.  Extra
+    keywords: precision (a key of PRECISIONS), max_attempts (per-orbit
+    step-attempt budget, 0 = none), return_nsteps, stream_rows (the result
+    transfer: -1 automatic, 0 one copy after the kernel, 1 the rows of
+    finished orbits copied while the kernel runs).
 
     Returns (result [N,nt,6] cylindrical, err [N]) like galpy (the leading
     axis is dropped for a single orbit), plus per-orbit accepted steps when
     return_nsteps."""
     return _integrate_c(False, pot, yo, t, int_method, rtol, atol, progressbar, dt, precision,
-                        max_attempts, return_nsteps, device)
+                        max_attempts, return_nsteps, device, stream_rows)
 
 
 def integratePlanarOrbit_cuda(pot, yo, t, int_method, rtol=None, atol=None, progressbar=True,
                               dt=None, precision="fp64", max_attempts=0, return_nsteps=False,
-                              device=-1):
+                              device=-1, stream_rows=-1):
     """Planar counterpart of integrateFullOrbit_cuda: yo [N,4] (R,vR,vT,phi)."""
     return _integrate_c(True, pot, yo, t, int_method, rtol, atol, progressbar, dt, precision,
-                        max_attempts, return_nsteps, device)
+                        max_attempts, return_nsteps, device, stream_rows)
 
 
 def _integrate_sos(planar, pot, yo, psi, t0, int_method, surface, rtol, atol, progressbar,

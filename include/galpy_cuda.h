@@ -90,13 +90,17 @@ typedef void (*galpy_cuda_callback)(void);
 typedef struct galpy_cuda_opts {
   int size;                /* sizeof(galpy_cuda_opts) */
   int device;              /* CUDA device ordinal, -1 = current */
-  int precision;           /* GALPY_CUDA_FP64 (default) or GALPY_CUDA_F32FORCE */
+  int precision;           /* a GALPY_CUDA_* precision form (default GALPY_CUDA_FP64) */
   int block_size;          /* threads per block, 0 = tuned default */
   long long max_attempts;  /* per-orbit step-attempt budget, 0 = unlimited */
   long long *nsteps;       /* optional out, host [nobj]: accepted steps per orbit */
   double *elapsed_ms;      /* optional out: device time of the integration kernel */
   int variant;             /* register-budget variant of the kernel (see galpy_cuda_launch) */
   int schedule;            /* GALPY_CUDA_SCHED_* (default longest-first) */
+  int stream_rows;         /* the blocking entry points' result transfer: -1 (or a shorter
+                              struct) automatic -- for large results the rows of finished
+                              orbits are copied to the host while the kernel runs; 0 one copy
+                              after the kernel; 1 streamed whatever the size */
 } galpy_cuda_opts;
 
 /* Compiled potential record size in bytes (one per component). */

@@ -1208,14 +1208,31 @@ typedef struct {
   opot *P;
 } octx;
 
+/* How the angle of the Cartesian force routes is formed: 0 (default) as the
+ * reference, acos(x/R) mapped to [0, 2 pi) (integrateFullOrbit.c:1313,
+ * integratePlanarOrbit.c:1022); 1 atan2(y, x).  acos is ill-conditioned
+ * where x/R is near +-1: a step that lands within ~1e-8 rad of the x axis
+ * gets its angle wrong by up to sqrt(2 eps) ~ 2e-8, which in a
+ * non-axisymmetric potential moves that force by as much.  The tests use
+ * mode 1 to tell that reference-side error from the engine's (the engine
+ * evaluates the force in Cartesian form, with no angle at all).  Test
+ * infrastructure; not thread-safe against concurrent integrations. */
+static int g_phi_mode = 0;
+void oracle_set_phi_mode(int mode) { g_phi_mode = mode; }
+
 /* cylindrical angle of (x,y) as the reference computes it */
 static void cyl_of(double x, double y, double *R, double *phi, double *sp, double *cp)
 {
   *R = sqrt(x * x + y * y);
-  *phi = acos(x / *R);
+  if (g_phi_mode == 1) {
+    *phi = atan2(y, x);
+    if (*phi < 0.) *phi += 2. * M_PI;
+  } else {
+    *phi = acos(x / *R);
+  }
   *sp = y / *R;
   *cp = x / *R;
-  if (y < 0.) *phi = 2. * M_PI - *phi;
+  if (g_phi_mode == 0 && y < 0.) *phi = 2. * M_PI - *phi;
 }
 
 static void sum3(opot *P, double R, double z, double phi, double *Rf, double *zf, double *pt)

@@ -84,6 +84,8 @@ def port():
         lib.oracle_potential.argtypes = [ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _ip, _dp, _dp]
         lib.oracle_expint.restype = ctypes.c_double
         lib.oracle_expint.argtypes = [ctypes.c_double]
+        lib.oracle_set_phi_mode.restype = None
+        lib.oracle_set_phi_mode.argtypes = [ctypes.c_int]
         lib.oracle_gammainc_P.restype = ctypes.c_double
         lib.oracle_gammainc_P.argtypes = [ctypes.c_double, ctypes.c_double]
         _port = lib
@@ -299,6 +301,21 @@ def potential(R, z, phi, pot_type, pot_args):
     if rc:
         raise ValueError(f"oracle_potential returned {rc}")
     return out
+
+
+class phi_from_atan2:
+    """Within the block the oracle's Cartesian force routes take the angle
+    from atan2(y, x) instead of the reference's acos(x / R), which is
+    ill-conditioned near the x axis (galpy_oracle.c, cyl_of).  Used by tests
+    to separate that reference-side rounding from the engine's (whose forces
+    are Cartesian)."""
+
+    def __enter__(self):
+        port().oracle_set_phi_mode(1)
+
+    def __exit__(self, *exc):
+        port().oracle_set_phi_mode(0)
+        return False
 
 
 def gammainc_P(a, x):

@@ -109,13 +109,26 @@ def test_methods_vs_oracle(oracle, golden, method, planar, potname):
     d = cyl_diff(ref, out).max(axis=(1, 2))
     far = same & (d >= 1e-10)
     if far.any():
-        # orbits that amplify rounding (e.g. box orbits of the triaxial
-        # halo): bounded by the oracle's own response to a one-ulp change of
-        # their initial conditions
-        ulp = 1 + np.finfo(float).eps * np.random.default_rng(3).choice([-1, 1], ics.shape)
-        pert, _, _, _ = oracle.integrate(ics[far] * ulp[far], t, pt, pa, method, planar=planar)
-        resp = cyl_diff(ref[far], pert).max(axis=(1, 2))
-        assert (d[far] <= np.maximum(1e-10, 30 * resp)).all(), (d[far], resp)
+        # The reference takes the angle of its Cartesian force routes as
+        # acos(x / R) (integratePlanarOrbit.c:1022, integrateFullOrbit.c:1313),
+        # ill-conditioned near the x axis: in the triaxial halo a step that
+        # lands within ~1e-8 rad of the axis moves its force by up to ~1e-8,
+        # and the orbit by ~1e-10 after it.  The engine's force is Cartesian
+        # (no angle); with the angle from atan2 -- the only change -- the
+        # oracle agrees with it again.  What is left beyond 1e-10 is bounded
+        # by that oracle's response to a one-ulp change of the orbit's
+        # initial conditions.
+        with oracle.phi_from_atan2():
+            ref2, _, nref2, _ = oracle.integrate(ics[far], t, pt, pa, method, planar=planar)
+            d2 = cyl_diff(ref2, out[far]).max(axis=(1, 2))
+            still = (d2 >= 1e-10) | (nref2 != ns[far])
+            if still.any():
+                ulp = 1 + np.finfo(float).eps * np.random.default_rng(3).choice(
+                    [-1, 1], ics[far][still].shape)
+                pert, _, _, _ = oracle.integrate(ics[far][still] * ulp, t, pt, pa, method,
+                                                 planar=planar)
+                resp = cyl_diff(ref2[still], pert).max(axis=(1, 2))
+                assert (d2[still] <= np.maximum(1e-10, 30 * resp)).all(), (d2[still], resp)
 
 
 @pytest.mark.parametrize("method", METHODS)
