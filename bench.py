@@ -350,11 +350,16 @@ def main():
     ap.add_argument("--variant", type=int, default=None,
                     help="pin the register variant of the headline kernel (0 compiler "
                          "budget, 1 capped) instead of the autotuner's choice")
-    ap.add_argument("--case", default="batching", choices=["batching", "uniform", "longest"],
+    ap.add_argument("--out-layout", default="soa_rect", choices=["soa_rect", "aos_rect"],
+                    help="snapshot layout of the headline and --profile runs: [6][nt][N] "
+                         "(soa_rect) or [N][nt][6] (aos_rect, galpy's row order)")
+    ap.add_argument("--case", default="batching",
+                    choices=["batching", "uniform", "longest", "bulk"],
                     help="uniform: R ~ U(0.5, 2), shared t in [0, 50] (101 snapshots) "
                          "(a throughput-bound case for profiling the same kernel); longest: "
                          "only the --orbits longest orbits of the batching workload (by "
-                         "t_end / r0), the tail that bounds its step time")
+                         "t_end / r0), the tail that bounds its step time; bulk: the "
+                         "batching workload without its --orbits longest orbits")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -385,7 +390,8 @@ def main():
 
     if args.profile:
         n = args.orbits if args.orbits != N_ORBITS else 65536
-        print(json.dumps(profile_leg(gb, torch, dev, args.profile, n)), flush=True)
+        print(json.dumps(profile_leg(gb, torch, dev, args.profile, n, args.out_layout)),
+              flush=True)
         return
 
     if args.grad_only:
@@ -418,6 +424,11 @@ def main():
         r0 = np.sqrt(ics[:, 0] ** 2 + ics[:, 3] ** 2)
         keep = np.argsort(-t[:, -1] / r0)[:args.orbits]
         ics, t = ics[keep], t[keep]
+    elif args.case == "bulk":
+        ics, t = workload(N_ORBITS, seed=shard_seed(1, rank))
+        r0 = np.sqrt(ics[:, 0] ** 2 + ics[:, 3] ** 2)
+        keep = np.sort(np.argsort(-t[:, -1] / r0)[args.orbits:])
+        ics, t = ics[keep], t[keep]
     else:
         ics, t = workload(args.orbits, seed=shard_seed(1, rank))
     n = len(ics)
@@ -426,7 +437,8 @@ def main():
     comps_d = torch.tensor(comps, device=dev)
     w0 = torch.tensor(cyl_to_rect(ics).T.copy(), device=dev)
     t_d = torch.tensor(t, device=dev)
-    out = torch.empty((6, NT, n), dtype=torch.float64, device=dev)
+    aos = args.out_layout == "aos_rect"
+    out = torch.empty((n, NT, 6) if aos else (6, NT, n), dtype=torch.float64, device=dev)
     err = torch.empty(n, dtype=torch.int32, device=dev)
     nsteps = torch.empty(n, dtype=torch.int64, device=dev)
     stream = torch.cuda.current_stream(dev)
@@ -438,12 +450,14 @@ def main():
     from galpy_b200.graph import IntegrationGraph
 
     tuned = autotune.tune(comps_d, ncomp, w0, t_d, out, err, "dop853_cuda", rtol=RTOL,
-                          atol=ATOL, signature=sig, comps_host=comps)
+                          atol=ATOL, signature=sig, comps_host=comps,
+                          out_layout=args.out_layout)
     if args.variant is not None:
         tuned = dict(tuned, variant=args.variant, pinned_variant=True)
     graph = IntegrationGraph(comps_d, ncomp, w0, t_d, out, err, "dop853_cuda", nsteps=nsteps,
                              rtol=RTOL, atol=ATOL, precision="fp64", signature=sig,
-                             comps_host=comps, **autotune.launch_kwargs(tuned))
+                             comps_host=comps, out_layout=args.out_layout,
+                             **autotune.launch_kwargs(tuned))
 
     def run(precision="fp64"):
         graph.replay()
@@ -520,7 +534,8 @@ def main():
     E0 = torch.empty(n, dtype=torch.float64, device=dev)
     E1 = torch.empty(n, dtype=torch.float64, device=dev)
     gb.energy_device(comps_d, ncomp, w0, E0, stream=stream)
-    gb.energy_device(comps_d, ncomp, out[:, NT - 1, :], E1, stream=stream)
+    gb.energy_device(comps_d, ncomp, out[:, NT - 1, :], E1, layout="aos" if aos else "soa",
+                     stream=stream)
     torch.cuda.synchronize()
     result["energy_rel_err"] = stats((torch.abs(E1 / E0 - 1)).cpu().numpy())
 
@@ -722,7 +737,7 @@ def methods_leg(gb, torch, dev, stream, pg, peak, rank, cpu=True, n=131072, K=3,
     return res
 
 
-def profile_leg(gb, torch, dev, spec, n):
+def profile_leg(gb, torch, dev, spec, n, out_layout="soa_rect"):
     """One warm-up and one timed launch of a single kernel on a small batch,
     for profiler captures (`ncu -k regex:<machine> -s 1 -c 1`):
 
@@ -739,7 +754,8 @@ def profile_leg(gb, torch, dev, spec, n):
                    with 101 snapshots, rtol = atol = 1e-10: the batching
                    workload's kernel on orbits of similar length
 
-    A third field selects the register variant (METHOD:KIND:VARIANT)."""
+    A third field selects the register variant (METHOD:KIND:VARIANT).
+    out_layout: the snapshot layout ('soa_rect' or 'aos_rect')."""
     method, _, rest = spec.partition(":")
     kind, _, variant = rest.partition(":")
     kind = kind or "plain"
@@ -784,7 +800,9 @@ def profile_leg(gb, torch, dev, spec, n):
         sig = 0
     w0 = torch.tensor(np.ascontiguousarray(w.T), device=dev)
     t_d = torch.tensor(t, device=dev)
-    out = torch.empty((nv, t.shape[-1], n), dtype=torch.float64, device=dev)
+    shape = (n, t.shape[-1], nv) if out_layout == "aos_rect" else (nv, t.shape[-1], n)
+    out = torch.empty(shape, dtype=torch.float64, device=dev)
+    kw["out_layout"] = out_layout
     err = torch.empty(n, dtype=torch.int32, device=dev)
     ns = torch.empty(n, dtype=torch.int64, device=dev)
     ms = []

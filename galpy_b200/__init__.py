@@ -21,7 +21,7 @@ from .integrate import (CUDA_METHODS, accel_device, compile_potential,  # noqa: 
                         integrateFullOrbit_sos_cuda, integratePlanarOrbit_sos_cuda,
                         integrateFullOrbit_dxdv_cuda, integratePlanarOrbit_cuda,
                         integratePlanarOrbit_dxdv_cuda, parse_integrator, parse_tol,
-                        signature)
+                        shard_of, signature, split_orbits)
 from .adjoint import final_state  # noqa: F401
 from .potentials import (HernquistPotential, LogarithmicHaloPotential,  # noqa: F401
                          MiyamotoNagaiPotential, MWPotential2014, NFWPotential,

@@ -62,6 +62,8 @@ class GalpyCudaOpts(ctypes.Structure):
         ("variant", ctypes.c_int),
         ("schedule", ctypes.c_int),
         ("stream_rows", ctypes.c_int),
+        ("ndevices", ctypes.c_int),
+        ("devices", ctypes.POINTER(ctypes.c_int)),
     ]
 
 
@@ -194,6 +196,9 @@ SIGNATURES = {
     "galpy_cuda_adjoint_params": (_ci, [_ci, _ci, _ip, _dp, _ip]),
     "galpy_cuda_accel_device": (
         _ci, [_vp, _ci, _vp, _ci, _ci, _ci, _vp, ctypes.c_longlong, _vp, _vp]),
+    "galpy_cuda_split_orbits": (
+        _ci, [_ci, ctypes.c_longlong, _dp, _ci, _ci, _dp, _ci, _ci, _ip, _dp, _ci, _ip, _ci,
+              ctypes.POINTER(ctypes.c_longlong)]),
     "galpy_cuda_trim_memory": (_ci, [_ci]),
     "galpy_cuda_jacobi_device": (
         _ci, [_vp, _ci, _vp, _ci, _vp, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong,
@@ -237,7 +242,9 @@ def check(code):
 
 
 def make_opts(precision=FP64, device=-1, block_size=0, max_attempts=0, nsteps=None,
-              elapsed=None, variant=0, schedule=1, stream_rows=-1):
+              elapsed=None, variant=0, schedule=1, stream_rows=-1, devices=None):
+    """devices: None (one device, `device`), -1 (every visible device) or a
+    sequence of device ordinals the call spreads its orbits over."""
     o = GalpyCudaOpts()
     o.size = ctypes.sizeof(GalpyCudaOpts)
     o.device = device
@@ -251,4 +258,15 @@ def make_opts(precision=FP64, device=-1, block_size=0, max_attempts=0, nsteps=No
     o.variant = variant
     o.schedule = schedule
     o.stream_rows = stream_rows
+    if devices is None:
+        o.ndevices = 0
+    elif isinstance(devices, int):
+        if devices != -1:
+            raise ValueError("devices: -1 (every visible device) or a sequence of ordinals")
+        o.ndevices = -1
+    else:
+        arr = (ctypes.c_int * len(devices))(*[int(d) for d in devices])
+        o._devices_keep = arr  # the array lives as long as the opts
+        o.ndevices = len(devices)
+        o.devices = ctypes.cast(arr, ctypes.POINTER(ctypes.c_int))
     return o

@@ -95,19 +95,23 @@ def workload_key(device_name, int_method, planar, precision, signature, variatio
 
 def tune(comps, ncomp, w0, t, out, err, int_method, planar=False, variational=False,
          precision="fp64", signature=0, group=None, out_row0=0, dt=None, rtol=None, atol=None,
-         comps_host=None, sample=131072, seed=0, use_cache=True, key_extra="", verbose=False):
+         comps_host=None, sample=131072, seed=0, use_cache=True, key_extra="", verbose=False,
+         out_layout="soa_rect"):
     """Best launch shape for this batch (dict of integrate_device keyword
     arguments, plus ``threads_per_orbit`` and the measured ``ms``).
 
     Arguments as for integrate_device with device tensors w0 [nv, N]
-    (SoA), t [nt] or [N, nt], out [nv, nt - out_row0, N] and err [N].  At
-    most ``sample`` orbits, drawn at random, are timed per candidate."""
+    (SoA), t [nt] or [N, nt], out [nv, nt - out_row0, N] (out_layout
+    'soa_rect' / 'soa_cyl') or [N, nt - out_row0, nv] ('aos_rect' /
+    'galpy') and err [N].  At most ``sample`` orbits, drawn at random, are
+    timed per candidate."""
     import torch
 
     nobj = err.shape[0]
     dev = w0.device
     key = workload_key(torch.cuda.get_device_name(dev), int_method, planar, precision,
-                       signature, variational, nobj, t.dim() > 1, key_extra)
+                       signature, variational, nobj, t.dim() > 1,
+                       key_extra + ("" if out_layout == "soa_rect" else f"|out={out_layout}"))
     with _lock:
         if use_cache:
             if key in _memo:
@@ -121,7 +125,10 @@ def tune(comps, ncomp, w0, t, out, err, int_method, planar=False, variational=Fa
     idx = torch.randperm(nobj, generator=g)[:m].to(dev)
     w_s = w0[:, idx].contiguous()
     t_s = t[idx].contiguous() if t.dim() > 1 else t
-    out_s = torch.empty((out.shape[0], out.shape[1], m), dtype=out.dtype, device=dev)
+    if out_layout in ("aos_rect", "galpy"):
+        out_s = torch.empty((m, out.shape[1], out.shape[2]), dtype=out.dtype, device=dev)
+    else:
+        out_s = torch.empty((out.shape[0], out.shape[1], m), dtype=out.dtype, device=dev)
     err_s = torch.empty(m, dtype=torch.int32, device=dev)
     grp_s = group[idx].contiguous() if group is not None else None
     stream = torch.cuda.current_stream(dev)
@@ -132,7 +139,7 @@ def tune(comps, ncomp, w0, t, out, err, int_method, planar=False, variational=Fa
                          rtol=rtol, atol=atol, precision=precision, stream=stream,
                          signature=signature, comps_host=comps_host,
                          block_size=cfg["block_size"], variant=cfg["variant"],
-                         schedule=cfg["schedule"])
+                         schedule=cfg["schedule"], out_layout=out_layout)
 
     results = []
     cands = candidates(int_method)

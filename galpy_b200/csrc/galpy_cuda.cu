@@ -31,6 +31,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <condition_variable>
 #include <mutex>
 #include <string>
@@ -399,8 +400,9 @@ static void on_sigint(int) { g_sigint = 1; }
 struct SigintGuard {
   struct sigaction old_action;
   bool installed = false;
-  SigintGuard()
+  explicit SigintGuard(bool install = true)
   {
+    if (!install) return;
     struct sigaction a;
     memset(&a, 0, sizeof(a));
     a.sa_handler = on_sigint;
@@ -674,6 +676,15 @@ static bool stream_rows_for(long long nobj, size_t n_out)
   return nobj >= 4LL * kStageChunk && n_out * sizeof(double) >= (size_t)(256u << 20);
 }
 
+// One device's share of a multi-device blocking call.  The caller's thread
+// holds the SIGINT handler and drives the progress callback from the orbit
+// counts each device reports; a device that fails raises `stop`, which the
+// others forward to their kernels like a SIGINT.
+struct SplitCtl {
+  std::atomic<unsigned long long> done{0};
+  std::atomic<int>* stop = nullptr;
+};
+
 // Blocking host-pointer integration shared by the galpy-facing entry points.
 // w: rectangular initial states [nobj][nv]; result written in galpy's layout
 // (cylindrical rows) unless rect_out.
@@ -681,7 +692,7 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
                     const double* t, int indiv_t, int npot, const int* pot_type,
                     const double* pot_args, double dt, double rtol, double atol, double* result,
                     int* err, int odeint_type, galpy_cuda_callback cb, const galpy_cuda_opts* o,
-                    bool rect_out, int system = GALPY_CUDA_SYS_ORBIT)
+                    bool rect_out, int system = GALPY_CUDA_SYS_ORBIT, SplitCtl* ctl = nullptr)
 {
   int rc = select_device(o);
   if (rc) return rc;
@@ -794,18 +805,19 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
       cudaEventDestroy(b);
     }
   } eg{e0, e1};
-  SigintGuard sig;
+  SigintGuard sig(ctl == nullptr);
   RowStreamer streamer(stg, nobj, (size_t)nt * nv, result, side);
   if (stream_rows) GPC_CUDA_TRY(streamer.start());
+  const bool track = cb != nullptr || ctl != nullptr;
   GPC_CUDA_TRY(cudaEventRecord(e0, stream));
-  rc = launch_kernel(&L, scr, cb != nullptr, stream, pool, stream_rows ? &stg : nullptr);
+  rc = launch_kernel(&L, scr, track, stream, pool, stream_rows ? &stg : nullptr);
   if (rc) return rc;
   GPC_CUDA_TRY(cudaEventRecord(e1, stream));
 
   // wait: poll completion, forward SIGINT to the device, drive the progress
   // callback, stream the finished orbits' rows to the result
   unsigned long long reported = 0, *pinned_done = nullptr;
-  if (cb) GPC_CUDA_TRY(cudaMallocHost(&pinned_done, sizeof(unsigned long long)));
+  if (track) GPC_CUDA_TRY(cudaMallocHost(&pinned_done, sizeof(unsigned long long)));
   struct PinGuard {
     unsigned long long* p;
     ~PinGuard()
@@ -830,21 +842,26 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
                          std::string("result streaming: ") + cudaGetErrorString(q));
     }
     if (kernel_done && rows_done) break;
-    if (g_sigint && !abort_sent) {
+    if ((g_sigint || (ctl && ctl->stop->load())) && !abort_sent) {
       static const int one = 1;
       cudaMemcpyAsync(&scr->abort_flag, &one, sizeof(int), cudaMemcpyHostToDevice, side);
       abort_sent = true;
     }
-    if (cb && !kernel_done) {
+    if (track && !kernel_done) {
       cudaMemcpyAsync(pinned_done, &scr->done_count, sizeof(unsigned long long),
                       cudaMemcpyDeviceToHost, side);
       cudaStreamSynchronize(side);
-      for (; reported < *pinned_done; reported++) cb();
+      if (ctl)
+        ctl->done.store(*pinned_done);
+      else
+        for (; reported < *pinned_done; reported++) cb();
     }
     struct timespec ts = {0, stream_rows ? 500000 : 2000000};
     nanosleep(&ts, nullptr);
   }
-  if (cb)
+  if (ctl)
+    ctl->done.store((unsigned long long)nobj);
+  else if (cb)
     for (; reported < (unsigned long long)nobj; reported++) cb();
   if (o && o->elapsed_ms) {
     float ms = 0.f;
@@ -860,6 +877,192 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
                                  cudaMemcpyDeviceToHost, stream));
   GPC_CUDA_TRY(cudaStreamSynchronize(stream));
   if (abort_sent) return GALPY_CUDA_ERR_INTERRUPTED;
+  return GALPY_CUDA_OK;
+}
+
+// ----------------------------------------------------------------------------
+// one blocking call over several devices
+// ----------------------------------------------------------------------------
+// The orbits of a batch are independent, so a batch spread over devices needs
+// no exchange: each device integrates a contiguous range of orbits, whose
+// states, times and result rows are contiguous slices of the caller's arrays.
+// The ranges hold equal shares of the estimated cost -- the longest-first
+// estimate |t_end - t_0| * Omega(x_0) of cost_kernel, evaluated here on the
+// host with the same force code -- rather than equal orbit counts, so that a
+// batch ordered by energy or radius (a grid of orbits, say) still loads the
+// devices evenly.  Within its range each device schedules longest-first as a
+// one-device call does.
+
+// Estimated cost of each orbit (cost_kernel's estimate; 1 for every orbit of
+// a surface-of-section run, whose states are not positions).  group: the
+// potential group of each orbit (comps holds ngroup * ncomp records), or null.
+static void orbit_costs(int planar, long long nobj, const double* w, int nv, int nt,
+                        const double* t, int indiv_t, const GpComp* comps, int ncomp,
+                        const int* group, int system, double* cost)
+{
+  const int D = planar ? 2 : 3;
+  auto one = [&](long long i) {
+    if (system != GALPY_CUDA_SYS_ORBIT) return 1.0;
+    double q[3] = {0.0, 0.0, 0.0}, a[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < D; k++) q[k] = w[i * nv + k];
+    const GpComp* c = comps + (group ? (long long)group[i] * ncomp : 0LL);
+    if (D == 3)
+      eval_force<3, PREC_FP64, false, DynPot>(c, ncomp, q, a);
+    else
+      eval_force<2, PREC_FP64, false, DynPot>(c, ncomp, q, a);
+    double ax = 0.0, xx = 0.0;
+    for (int k = 0; k < D; k++) {
+      ax += a[k] * q[k];
+      xx += q[k] * q[k];
+    }
+    const double* tt = t + (indiv_t ? i * (long long)nt : 0LL);
+    const double est = fabs(tt[nt - 1] - tt[0]) * sqrt(fabs(ax) / (xx > 0.0 ? xx : 1e-300));
+    // a floor keeps orbits with a zero estimate (at the centre, or of zero
+    // duration) from being free: each still costs its launch share
+    return std::isfinite(est) ? est + 1e-3 : 1e-3;
+  };
+  const long long per = 1 << 15;
+  const int nthr = (int)std::min<long long>(
+      std::max(1u, std::min(std::thread::hardware_concurrency(), 32u)), (nobj + per - 1) / per);
+  if (nthr <= 1) {
+    for (long long i = 0; i < nobj; i++) cost[i] = one(i);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int k = 0; k < nthr; k++)
+    th.emplace_back([&, k] {
+      const long long a = nobj * k / nthr, b = nobj * (k + 1) / nthr;
+      for (long long i = a; i < b; i++) cost[i] = one(i);
+    });
+  for (auto& x : th) x.join();
+}
+
+// Cut [0, nobj) into nparts contiguous ranges of equal cost: bounds[k] is the
+// first orbit of part k (bounds[0] = 0, bounds[nparts] = nobj).  Part k ends
+// where the running cost first reaches k+1 nparts-ths of the total; a part
+// may be empty when single orbits dominate the cost.
+static void cut_ranges(long long nobj, const double* cost, int nparts, long long* bounds)
+{
+  double total = 0.0;
+  for (long long i = 0; i < nobj; i++) total += cost[i];
+  bounds[0] = 0;
+  long long i = 0;
+  double run = 0.0;
+  for (int k = 1; k < nparts; k++) {
+    const double target = total * k / nparts;
+    // take orbit i while that brings the running cost closer to the target
+    while (i < nobj && run + 0.5 * cost[i] <= target) run += cost[i++];
+    bounds[k] = i;
+  }
+  bounds[nparts] = nobj;
+}
+
+// The devices of a multi-device call (empty: one device, opts.device).
+static int device_list(const galpy_cuda_opts* o, std::vector<int>& devs)
+{
+  devs.clear();
+  const bool has = o && o->size >= (int)(offsetof(galpy_cuda_opts, devices) + sizeof(o->devices));
+  if (!has || o->ndevices == 0 || o->ndevices == 1) return GALPY_CUDA_OK;
+  if (o->ndevices < -1) return set_error(GALPY_CUDA_ERR_ARG, "invalid ndevices");
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1)
+    return set_error(GALPY_CUDA_ERR_NODEVICE, "no CUDA device visible");
+  const int want = o->ndevices < 0 ? n : o->ndevices;
+  for (int k = 0; k < want; k++) {
+    const int d = o->ndevices > 0 && o->devices ? o->devices[k] : k;
+    if (d < 0 || d >= n) return set_error(GALPY_CUDA_ERR_ARG, "device ordinal out of range");
+    devs.push_back(d);  // a repeated ordinal runs several ranges concurrently on that device
+  }
+  return GALPY_CUDA_OK;
+}
+
+// run_host over the devices opts names: one thread per device, each running
+// the one-device path on its range; this thread forwards SIGINT, reports
+// progress and collects the first error.
+static int run_host_split(int planar, int var, long long nobj, const double* w, int nv, int nt,
+                          const double* t, int indiv_t, int npot, const int* pot_type,
+                          const double* pot_args, double dt, double rtol, double atol,
+                          double* result, int* err, int odeint_type, galpy_cuda_callback cb,
+                          const galpy_cuda_opts* o, bool rect_out,
+                          int system = GALPY_CUDA_SYS_ORBIT)
+{
+  std::vector<int> devs;
+  int rc = device_list(o, devs);
+  if (rc) return rc;
+  if (devs.size() < 2 || nobj < (long long)devs.size())
+    return run_host(planar, var, nobj, w, nv, nt, t, indiv_t, npot, pot_type, pot_args, dt, rtol,
+                    atol, result, err, odeint_type, cb, o, rect_out, system);
+  if (!method_supported(odeint_type))
+    return set_error(GALPY_CUDA_ERR_METHOD, "odeint_type not implemented on the GPU");
+  std::vector<GpComp> comps(npot > 0 ? npot : 1);
+  rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
+  if (rc == -3) return set_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
+  if (rc) return set_error(GALPY_CUDA_ERR_ARG, "invalid potential arguments");
+
+  const int nd = (int)devs.size();
+  std::vector<double> cost((size_t)nobj);
+  orbit_costs(planar, nobj, w, nv, nt, t, indiv_t, comps.data(), npot, nullptr, system,
+              cost.data());
+  std::vector<long long> bounds(nd + 1);
+  cut_ranges(nobj, cost.data(), nd, bounds.data());
+
+  std::atomic<int> stop{0};
+  std::vector<SplitCtl> ctl(nd);
+  std::vector<int> rcs(nd, GALPY_CUDA_OK);
+  std::vector<std::string> msgs(nd);
+  std::vector<double> ms(nd, 0.0);
+  std::vector<std::atomic<int>> finished(nd);
+  SigintGuard sig;
+  std::vector<std::thread> th;
+  for (int k = 0; k < nd; k++) {
+    ctl[k].stop = &stop;
+    finished[k].store(0);
+    th.emplace_back([&, k] {
+      const long long a = bounds[k], n = bounds[k + 1] - a;
+      galpy_cuda_opts ok = *o;
+      ok.size = (int)sizeof(galpy_cuda_opts);
+      ok.device = devs[k];
+      ok.ndevices = 0;
+      ok.devices = nullptr;
+      ok.nsteps = o->nsteps ? o->nsteps + a : nullptr;
+      ok.elapsed_ms = &ms[k];
+      int r = GALPY_CUDA_OK;
+      if (n > 0)
+        r = run_host(planar, var, n, w + a * nv, nv, nt, t + (indiv_t ? a * nt : 0), indiv_t,
+                     npot, pot_type, pot_args, dt, rtol, atol, result + a * (long long)nt * nv,
+                     err + a, odeint_type, nullptr, &ok, rect_out, system, &ctl[k]);
+      ctl[k].done.store((unsigned long long)n);
+      if (r != GALPY_CUDA_OK && r != GALPY_CUDA_ERR_INTERRUPTED) {
+        msgs[k] = g_last_error;
+        stop.store(1);
+      }
+      rcs[k] = r;
+      finished[k].store(1);
+    });
+  }
+  unsigned long long reported = 0;
+  for (;;) {
+    bool all = true;
+    unsigned long long done = 0;
+    for (int k = 0; k < nd; k++) {
+      all = all && finished[k].load();
+      done += ctl[k].done.load();
+    }
+    if (cb)
+      for (; reported < done; reported++) cb();
+    if (all) break;
+    struct timespec ts = {0, 2000000};
+    nanosleep(&ts, nullptr);
+  }
+  for (auto& x : th) x.join();
+  if (cb)
+    for (; reported < (unsigned long long)nobj; reported++) cb();
+  if (o->elapsed_ms) *o->elapsed_ms = *std::max_element(ms.begin(), ms.end());
+  for (int k = 0; k < nd; k++)
+    if (rcs[k] != GALPY_CUDA_OK && rcs[k] != GALPY_CUDA_ERR_INTERRUPTED)
+      return set_error(rcs[k], "device " + std::to_string(devs[k]) + ": " + msgs[k]);
+  for (int k = 0; k < nd; k++)
+    if (rcs[k] == GALPY_CUDA_ERR_INTERRUPTED) return GALPY_CUDA_ERR_INTERRUPTED;
   return GALPY_CUDA_OK;
 }
 
@@ -1280,6 +1483,36 @@ int galpy_cuda_compile_potential(int planar, int npot, const int* pot_type,
   return GALPY_CUDA_OK;
 }
 
+int galpy_cuda_split_orbits(int planar, long long nobj, const double* w, int nv, int nt,
+                            const double* t, int indiv_t, int npot, const int* pot_type,
+                            const double* pot_args, int ngroup, const int* group, int nparts,
+                            long long* bounds)
+{
+  if (nobj < 0 || nt < 1 || nparts < 1 || nv < (planar ? 4 : 6) || !bounds ||
+      (nobj && (!w || !t)) || npot < 1 || !pot_type || !pot_args || ngroup < 1 ||
+      (ngroup > 1 && !group))
+    return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
+  if (group)
+    for (long long i = 0; i < nobj; i++)
+      if (group[i] < 0 || group[i] >= ngroup)
+        return set_error(GALPY_CUDA_ERR_ARG, "group index out of range");
+  std::vector<GpComp> comps((size_t)npot * ngroup);
+  const double* p = pot_args;
+  for (int g = 0; g < ngroup; g++) {
+    int used = 0;
+    int rc = compile_group(planar, npot, pot_type, p, comps.data() + (size_t)g * npot, &used);
+    if (rc == -3)
+      return set_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
+    if (rc) return set_error(GALPY_CUDA_ERR_ARG, "invalid potential arguments");
+    p += used;
+  }
+  std::vector<double> cost((size_t)nobj);
+  orbit_costs(planar, nobj, w, nv, nt, t, indiv_t, comps.data(), npot, group,
+              GALPY_CUDA_SYS_ORBIT, cost.data());
+  cut_ranges(nobj, cost.data(), nparts, bounds);
+  return GALPY_CUDA_OK;
+}
+
 int galpy_cuda_integrate_device(const galpy_cuda_launch* L)
 {
   int rc = check_launch(L);
@@ -1341,7 +1574,7 @@ int integrateFullOrbit_cuda(int nobj, double* yo, int nt, double* t, int indiv_t
   if (!method_supported(odeint_type))
     return set_error(GALPY_CUDA_ERR_METHOD, "odeint_type not implemented on the GPU");
   cyl_to_rect_inplace(0, nobj, yo);
-  return run_host(0, 0, nobj, yo, 6, nt, t, indiv_t, npot, pot_type, pot_args, dt, rtol, atol,
+  return run_host_split(0, 0, nobj, yo, 6, nt, t, indiv_t, npot, pot_type, pot_args, dt, rtol, atol,
                   result, err, odeint_type, cb, opts, false);
 }
 
@@ -1359,7 +1592,7 @@ int integrateFullOrbit_sos_cuda(int nobj, double* yo, int npsi, double* psi, int
     return set_error(GALPY_CUDA_ERR_METHOD,
                      "surface-of-section integration takes rk4, rk6, dopr54 or dop853");
   cyl_to_sos_inplace(nobj, yo);
-  return run_host(0, 0, nobj, yo, 7, npsi, psi, indiv_psi, npot, pot_type, pot_args, dpsi, rtol,
+  return run_host_split(0, 0, nobj, yo, 7, npsi, psi, indiv_psi, npot, pot_type, pot_args, dpsi, rtol,
                   atol, result, err, odeint_type, cb, opts, false, GALPY_CUDA_SYS_SOS);
 }
 
@@ -1377,7 +1610,7 @@ int integratePlanarOrbit_sos_cuda(int nobj, double* yo, int npsi, double* psi, i
     return set_error(GALPY_CUDA_ERR_METHOD,
                      "surface-of-section integration takes rk4, rk6, dopr54 or dop853");
   polar_to_sos_inplace(nobj, yo, surface);
-  return run_host(1, 0, nobj, yo, 5, npsi, psi, indiv_psi, npot, pot_type, pot_args, dpsi, rtol,
+  return run_host_split(1, 0, nobj, yo, 5, npsi, psi, indiv_psi, npot, pot_type, pot_args, dpsi, rtol,
                   atol, result, err, odeint_type, cb, opts, false,
                   surface == 1 ? GALPY_CUDA_SYS_SOS_PLANAR_Y : GALPY_CUDA_SYS_SOS_PLANAR_X);
 }
@@ -1393,7 +1626,7 @@ int integratePlanarOrbit_cuda(int nobj, double* yo, int nt, double* t, int indiv
   if (!method_supported(odeint_type))
     return set_error(GALPY_CUDA_ERR_METHOD, "odeint_type not implemented on the GPU");
   cyl_to_rect_inplace(1, nobj, yo);
-  return run_host(1, 0, nobj, yo, 4, nt, t, indiv_t, npot, pot_type, pot_args, dt, rtol, atol,
+  return run_host_split(1, 0, nobj, yo, 4, nt, t, indiv_t, npot, pot_type, pot_args, dt, rtol, atol,
                   result, err, odeint_type, cb, opts, false);
 }
 
@@ -1426,7 +1659,7 @@ int integrateOrbit_dxdv_batch_cuda(int planar, int nobj, double* yo, int nt, dou
 {
   if (nobj < 0 || nt < 1 || (nobj && (!yo || !t || !result || !err)) || !pot_type || !pot_args)
     return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
-  return run_host(planar ? 1 : 0, 1, nobj, yo, planar ? 8 : 12, nt, t, indiv_t, npot, pot_type,
+  return run_host_split(planar ? 1 : 0, 1, nobj, yo, planar ? 8 : 12, nt, t, indiv_t, npot, pot_type,
                   pot_args, dt, rtol, atol, result, err, odeint_type, nullptr, opts, true);
 }
 

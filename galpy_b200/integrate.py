@@ -69,7 +69,7 @@ def _precision(p):
 
 
 def _integrate_c(planar, pot, yo, t, int_method, rtol, atol, progressbar, dt, precision,
-                 max_attempts, return_nsteps, device, stream_rows=-1):
+                 max_attempts, return_nsteps, device, stream_rows=-1, devices=None):
     single_obj = yo.ndim == 1
     yo = np.atleast_2d(yo)
     nobj = len(yo)
@@ -87,7 +87,8 @@ def _integrate_c(planar, pot, yo, t, int_method, rtol, atol, progressbar, dt, pr
     yo = np.require(yo, dtype=np.float64, requirements=["C", "W"])
     t = np.require(t, dtype=np.float64, requirements=["C", "W"])
     opts = _lib.make_opts(precision=_precision(precision), device=device,
-                          max_attempts=max_attempts, nsteps=nsteps, stream_rows=stream_rows)
+                          max_attempts=max_attempts, nsteps=nsteps, stream_rows=stream_rows,
+                          devices=devices)
     cb = _lib.CALLBACK()
     pbar = None
     if progressbar and nobj > 1:
@@ -115,7 +116,7 @@ def _integrate_c(planar, pot, yo, t, int_method, rtol, atol, progressbar, dt, pr
 
 def integrateFullOrbit_cuda(pot, yo, t, int_method, rtol=None, atol=None, progressbar=True,
                             dt=None, precision="fp64", max_attempts=0, return_nsteps=False,
-                            device=-1, stream_rows=-1):
+                            device=-1, stream_rows=-1, devices=None):
     """Integrate 3D orbits on the GPU.
 
     Parameters mirror galpy's integrateFullOrbit_c: yo [N,6] or [6]
@@ -126,25 +127,28 @@ def integrateFullOrbit_cuda(pot, yo, t, int_method, rtol=None, atol=None, progre
     keywords: precision (a key of PRECISIONS), max_attempts (per-orbit
     step-attempt budget, 0 = none), return_nsteps, stream_rows (the result
     transfer: -1 automatic, 0 one copy after the kernel, 1 the rows of
-    finished orbits copied while the kernel runs).
+    finished orbits copied while the kernel runs), devices (None: the one
+    device `device`; a sequence of ordinals, or -1 for every visible device:
+    the orbits are cut into contiguous ranges of equal estimated cost, one
+    per device, integrated concurrently).
 
     Returns (result [N,nt,6] cylindrical, err [N]) like galpy (the leading
     axis is dropped for a single orbit), plus per-orbit accepted steps when
     return_nsteps."""
     return _integrate_c(False, pot, yo, t, int_method, rtol, atol, progressbar, dt, precision,
-                        max_attempts, return_nsteps, device, stream_rows)
+                        max_attempts, return_nsteps, device, stream_rows, devices)
 
 
 def integratePlanarOrbit_cuda(pot, yo, t, int_method, rtol=None, atol=None, progressbar=True,
                               dt=None, precision="fp64", max_attempts=0, return_nsteps=False,
-                              device=-1, stream_rows=-1):
+                              device=-1, stream_rows=-1, devices=None):
     """Planar counterpart of integrateFullOrbit_cuda: yo [N,4] (R,vR,vT,phi)."""
     return _integrate_c(True, pot, yo, t, int_method, rtol, atol, progressbar, dt, precision,
-                        max_attempts, return_nsteps, device, stream_rows)
+                        max_attempts, return_nsteps, device, stream_rows, devices)
 
 
 def _integrate_sos(planar, pot, yo, psi, t0, int_method, surface, rtol, atol, progressbar,
-                   dpsi, max_attempts, return_nsteps, device):
+                   dpsi, max_attempts, return_nsteps, device, devices=None):
     single_obj = np.ndim(yo) == 1
     yo = np.atleast_2d(yo)
     nobj = len(yo)
@@ -164,7 +168,7 @@ def _integrate_sos(planar, pot, yo, psi, t0, int_method, surface, rtol, atol, pr
     err = np.zeros(nobj, dtype=np.int32)
     nsteps = np.zeros(nobj, dtype=np.int64) if return_nsteps else None
     opts = _lib.make_opts(precision=_lib.FP64, device=device, max_attempts=max_attempts,
-                          nsteps=nsteps)
+                          nsteps=nsteps, devices=devices)
     cb = _lib.CALLBACK()
     pbar = None
     if progressbar and nobj > 1:
@@ -197,7 +201,7 @@ def _integrate_sos(planar, pot, yo, psi, t0, int_method, surface, rtol, atol, pr
 
 def integrateFullOrbit_sos_cuda(pot, yo, psi, t0, int_method, rtol=None, atol=None,
                                 progressbar=True, dpsi=None, max_attempts=0,
-                                return_nsteps=False, device=-1):
+                                return_nsteps=False, device=-1, devices=None):
     """Surface-of-section integration on the GPU (galpy's
     integrateFullOrbit_sos_c, galpy/orbit/integrateFullOrbit.py:1215-1355).
 
@@ -206,20 +210,21 @@ def integrateFullOrbit_sos_cuda(pot, yo, psi, t0, int_method, rtol=None, atol=No
     time (scalar or [N]); int_method 'rk4_cuda', 'rk6_cuda', 'dopr54_cuda' or
     'dop853_cuda'; dpsi the step (None: estimated).  Returns (y [N,npsi,7]
     with the time as the last column, err [N]); the leading axis is dropped
-    for a single orbit."""
+    for a single orbit.  devices: as for integrateFullOrbit_cuda (equal orbit
+    counts per device)."""
     return _integrate_sos(False, pot, yo, psi, t0, int_method, None, rtol, atol, progressbar,
-                          dpsi, max_attempts, return_nsteps, device)
+                          dpsi, max_attempts, return_nsteps, device, devices)
 
 
 def integratePlanarOrbit_sos_cuda(pot, yo, psi, t0, int_method, surface="x", rtol=None,
                                   atol=None, progressbar=True, dpsi=None, max_attempts=0,
-                                  return_nsteps=False, device=-1):
+                                  return_nsteps=False, device=-1, devices=None):
     """Planar surface-of-section integration on the GPU (galpy's
     integratePlanarOrbit_sos_c, galpy/orbit/integratePlanarOrbit.py:1543-1693):
     yo [N,4] (R,vR,vT,phi); surface 'x' (x = 0, the default) or 'y' (y =
     0); returns (y [N,npsi,5] = (R,vR,vT,phi,t), err [N])."""
     return _integrate_sos(True, pot, yo, psi, t0, int_method, surface, rtol, atol, progressbar,
-                          dpsi, max_attempts, return_nsteps, device)
+                          dpsi, max_attempts, return_nsteps, device, devices)
 
 
 def _dxdv_single(planar, pot, yo, dyo, t, int_method, dt, rtol, atol, device):
@@ -266,7 +271,7 @@ def integratePlanarOrbit_dxdv_cuda(pot, yo, dyo, t, int_method, rtol=None, atol=
 
 
 def integrate_dxdv_batch(pot, w, t, int_method, planar=False, dt=None, rtol=None, atol=None,
-                         device=-1, return_nsteps=False):
+                         device=-1, return_nsteps=False, devices=None):
     """Variational integration of many (orbit, deviation) pairs in one launch.
 
     w [N, 4*dim] rectangular (x, v, dx, dv); t [nt] or [N, nt].  Returns
@@ -283,7 +288,7 @@ def integrate_dxdv_batch(pot, w, t, int_method, planar=False, dt=None, rtol=None
     result = np.empty((nobj, nt, nv))
     err = np.zeros(nobj, dtype=np.int32)
     nsteps = np.zeros(nobj, dtype=np.int64) if return_nsteps else None
-    opts = _lib.make_opts(device=device, nsteps=nsteps)
+    opts = _lib.make_opts(device=device, nsteps=nsteps, devices=devices)
     rc = _lib.lib().integrateOrbit_dxdv_batch_cuda(
         int(planar), nobj, w.ctypes.data_as(_dp), nt, t.ctypes.data_as(_dp), int(t.ndim > 1),
         npot, pot_type.ctypes.data_as(_ip), pot_args.ctypes.data_as(_dp), dt, rtol, atol,
@@ -311,6 +316,45 @@ def signature(pot, planar=False):
     """Kernel specialisation of a potential (0 generic, 1 MWPotential2014-type)."""
     npot, pot_type, _ = parse_pot(pot, planar=planar)
     return _lib.lib().galpy_cuda_signature(npot, pot_type.ctypes.data_as(_ip))
+
+
+def split_orbits(pot, w, t, nparts, planar=False, group=None, ngroup=1):
+    """Contiguous orbit ranges of equal estimated cost (the cut a call with
+    ``devices=`` makes), for spreading a batch over processes, one per
+    device: part k is orbits [bounds[k], bounds[k+1]).
+
+    w [N, nv] RECTANGULAR states, positions first (x, y[, z], ...); t [nt]
+    or [N, nt]; for parameter groups, pot = (pot_type, pot_args) with
+    ngroup argument blocks and group [N] each orbit's block.  The cost of an
+    orbit is |t_end - t_0| * Omega(x_0), Omega^2 = |a.x| / |x|^2 in its
+    group's potential.  Runs on the host; needs no GPU."""
+    npot, pot_type, pot_args = parse_pot(pot, planar=planar)
+    w = np.require(np.atleast_2d(w), dtype=np.float64, requirements=["C"])
+    t = np.require(t, dtype=np.float64, requirements=["C"])
+    if t.ndim > 1 and t.shape[0] != w.shape[0]:
+        raise ValueError("per-orbit times need one row per orbit")
+    gp = None
+    if group is not None:
+        group = np.require(group, dtype=np.int32, requirements=["C"])
+        if group.shape != (w.shape[0],):
+            raise ValueError("group needs one entry per orbit")
+        gp = group.ctypes.data_as(_ip)
+    bounds = np.zeros(int(nparts) + 1, dtype=np.int64)
+    rc = _lib.lib().galpy_cuda_split_orbits(
+        int(planar), w.shape[0], w.ctypes.data_as(_dp), w.shape[1], t.shape[-1],
+        t.ctypes.data_as(_dp), int(t.ndim > 1), npot, pot_type.ctypes.data_as(_ip),
+        pot_args.ctypes.data_as(_dp), int(ngroup), gp, int(nparts),
+        bounds.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)))
+    _lib.check(rc)
+    return bounds
+
+
+def shard_of(pot, w, t, rank, world, planar=False, group=None, ngroup=1):
+    """This rank's orbit range (start, stop) of a batch spread over `world`
+    processes by split_orbits.  The ranks share nothing but the inputs: each
+    computes the same cut."""
+    b = split_orbits(pot, w, t, world, planar=planar, group=group, ngroup=ngroup)
+    return int(b[rank]), int(b[rank + 1])
 
 
 def integrate_device(comps, ncomp, w0, t, out, err, int_method, planar=False, variational=False,

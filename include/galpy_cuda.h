@@ -101,6 +101,16 @@ typedef struct galpy_cuda_opts {
                               struct) automatic -- for large results the rows of finished
                               orbits are copied to the host while the kernel runs; 0 one copy
                               after the kernel; 1 streamed whatever the size */
+  int ndevices;            /* devices one blocking call spreads its orbits over: 0 or 1 (or a
+                              shorter struct) one device (`device`); n > 1 the first n of
+                              `devices` (or ordinals 0..n-1 when `devices` is NULL); -1 every
+                              visible device.  The orbits are cut into contiguous ranges of
+                              equal estimated cost (the longest-first estimate), one per
+                              device, integrated concurrently, each range's results written
+                              straight into its rows of the caller's arrays; no data crosses
+                              between devices.  elapsed_ms then reports the slowest device. */
+  const int *devices;      /* optional device ordinals for ndevices > 1; an ordinal may
+                              repeat (its ranges then run concurrently on that device) */
 } galpy_cuda_opts;
 
 /* Compiled potential record size in bytes (one per component). */
@@ -117,6 +127,21 @@ int galpy_cuda_signature(int npot, const int *pot_type);
  * GALPY_CUDA_ERR_POTENTIAL / GALPY_CUDA_ERR_ARG. */
 int galpy_cuda_compile_potential(int planar, int npot, const int *pot_type,
                                  const double *pot_args, int ngroup, void *out);
+
+/* Contiguous orbit ranges of equal estimated cost, as a multi-device call
+ * (galpy_cuda_opts.ndevices) cuts them; for callers that spread a batch over
+ * processes themselves (one per device, e.g. torch.distributed ranks).
+ * w [nobj][nv] rectangular states (positions first), t [nt] or [nobj][nt];
+ * pot_args holds ngroup consecutive argument blocks (as for
+ * galpy_cuda_compile_potential) and group [nobj] each orbit's block (NULL
+ * when ngroup is 1); writes bounds[nparts+1]: part k is orbits
+ * [bounds[k], bounds[k+1]).  The cost of an orbit is |t_end - t_0| *
+ * Omega(x_0), Omega^2 = |a.x|/|x|^2 in its group's potential (the
+ * longest-first schedule's estimate).  Host only: needs no device. */
+int galpy_cuda_split_orbits(int planar, long long nobj, const double *w, int nv, int nt,
+                            const double *t, int indiv_t, int npot, const int *pot_type,
+                            const double *pot_args, int ngroup, const int *group, int nparts,
+                            long long *bounds);
 
 /* Stands in for integrateFullOrbit (galpy/orbit/orbit_c_ext/integrateFullOrbit.c:1046). */
 int integrateFullOrbit_cuda(int nobj, double *yo, int nt, double *t, int indiv_t, int npot,

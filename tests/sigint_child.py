@@ -5,7 +5,10 @@ reports how it ended; the parent sends SIGINT while the kernel runs.  The
 same pattern as the reference's tests/orbitint4sigint.py driven by
 test_orbit_c_sigint_full / _planar (tests/test_orbit.py:12211-12420).
 
-usage: python sigint_child.py <method> full|planar
+usage: python sigint_child.py <method> full|planar [split]
+
+With `split` the call spreads its orbits over two ranges on device 0
+(devices=[0, 0]), whose threads the calling thread's handler stops.
 """
 import os
 import sys
@@ -24,6 +27,7 @@ def main():
     from helpers import seeded_ics
 
     method, kind = sys.argv[1], sys.argv[2]
+    devices = [0, 0] if len(sys.argv) > 3 and sys.argv[3] == "split" else None
     planar = kind == "planar"
     pot = potentials.MWPotential2014()
     fn = gb.integratePlanarOrbit_cuda if planar else gb.integrateFullOrbit_cuda
@@ -36,7 +40,8 @@ def main():
     print("Starting long integration ...", flush=True)
     t0 = time.time()
     try:
-        fn(pot, ics, t, method, progressbar=False, dt=0.001 if "dop" not in method else None)
+        fn(pot, ics, t, method, progressbar=False, dt=0.001 if "dop" not in method else None,
+           devices=devices)
     except KeyboardInterrupt:
         print(f"KeyboardInterrupt after {time.time() - t0:.3f} s", flush=True)
         return 0

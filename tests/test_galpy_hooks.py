@@ -18,7 +18,7 @@ def hooks(monkeypatch):
     calls = []
 
     def recorder(planar, pot, yo, t, int_method, rtol, atol, progressbar, dt, precision,
-                 max_attempts, return_nsteps, device, stream_rows=-1):
+                 max_attempts, return_nsteps, device, stream_rows=-1, devices=None):
         calls.append(dict(planar=planar, pot=pot, yo=np.array(yo), t=np.array(t),
                           method=int_method, rtol=rtol, atol=atol, dt=dt))
         yo2 = np.atleast_2d(yo)

@@ -175,7 +175,10 @@ def test_orbit_integrate_dxdv_cuda(oracle, planar):
     o = Orbit(ics)
     o.integrate_dxdv(dxdv, ts, MWPotential2014, method="dop853_cuda", rectIn=True,
                      rectOut=True, rtol=1e-11, atol=1e-11, progressbar=False)
-    got = o.getOrbit_dxdv()
+    # orbit_dxdv: orbit (cylindrical) then deviation (rectangular, rectOut)
+    # columns; getOrbit_dxdv() returns the deviation columns alone
+    got = o.orbit_dxdv
+    assert np.array_equal(o.getOrbit_dxdv(), got[..., nv:])
     pt, pa = parsed(MWPotential2014, planar)
     w = np.hstack([cyl_to_rect(ics), dxdv])
     impl = "ref" if oracle.ref_available() else "port"

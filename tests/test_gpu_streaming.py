@@ -76,11 +76,13 @@ def test_streamed_rows_into_pinned_memory(golden):
     dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
     opts = _lib.make_opts(stream_rows=1)
     tt = np.ascontiguousarray(t)
+    # the wrapper's default tolerances (-12 ln 10, one ulp away from ln 1e-12)
+    lr, la = gb.parse_tol(None, None)
     rc = lib.integrateFullOrbit_cuda(n, yo.ctypes.data_as(dp), len(t), tt.ctypes.data_as(dp), 0,
                                      3, pti.ctypes.data_as(ip), pad.ctypes.data_as(dp), None,
-                                     -9999.99, float(np.log(1e-12)), float(np.log(1e-12)),
-                                     res.ctypes.data_as(dp), er.ctypes.data_as(ip), 6,
-                                     _lib.CALLBACK(), ctypes.byref(opts))
+                                     -9999.99, lr, la, res.ctypes.data_as(dp),
+                                     er.ctypes.data_as(ip), 6, _lib.CALLBACK(),
+                                     ctypes.byref(opts))
     assert rc == 0 and not er.any()
     assert np.array_equal(res, ref)
 
