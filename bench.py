@@ -1106,11 +1106,35 @@ def e2e(gb, ics, t, pt, pa, K, pg, dev, steps_total):
             times.append(el)
             kernel.append(kernel_ms.value * 1e-3)
     (el,), _ = over_ranks([max(times)], [], pg, dev)
+    # the same call with pageable numpy arrays, as galpy passes them
+    # (integrateFullOrbit.py:708-712)
+    yo_pg = np.empty((n, 6))
+    t_pg = np.ascontiguousarray(t, dtype=np.float64)
+    res_pg = np.empty((n, NT, 6))
+    ptimes = []
+    for k in range(K + 1):
+        yo_pg[:] = ics
+        if pg:
+            pg.barrier()
+        t0 = time.perf_counter()
+        rc = L.integrateFullOrbit_cuda(n, yo_pg.ctypes.data_as(dp), NT, t_pg.ctypes.data_as(dp),
+                                       1, len(pti), pti.ctypes.data_as(ip), pad.ctypes.data_as(dp),
+                                       None, -9999.99, r, a, res_pg.ctypes.data_as(dp),
+                                       err.ctypes.data_as(ip), 6, _lib.CALLBACK(),
+                                       ctypes.byref(opts))
+        pel = time.perf_counter() - t0
+        _lib.check(rc)
+        if k > 0:
+            ptimes.append(pel)
+    (pel,), _ = over_ranks([max(ptimes)], [], pg, dev)
     return {"value": steps_total / el, "unit": "orbit-steps/s", "seconds_per_step": el,
             "kernel_seconds_per_step": max(kernel),
             "h2d_bytes_per_step": int(yo_pin.nbytes + t_pin.nbytes),
             "d2h_bytes_per_step": int(res_pin.nbytes + err.nbytes),
-            "api": "integrateFullOrbit_cuda (galpy layout, pinned host buffers)"}
+            "api": "integrateFullOrbit_cuda (galpy layout, pinned host buffers)",
+            "pageable": {"value": steps_total / pel, "seconds_per_step": pel,
+                         "api": "integrateFullOrbit_cuda (galpy layout, pageable numpy "
+                                "arrays as galpy passes them)"}}
 
 
 def ctypes_fp64_peak(_lib):

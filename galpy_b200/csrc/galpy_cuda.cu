@@ -160,7 +160,21 @@ static int signature_of(int npot, const int* pot_type)
 {
   if (npot == 3 && pot_type[0] == T_PSWC && pot_type[1] == T_MN && pot_type[2] == T_NFW)
     return GALPY_CUDA_SIG_MW14;
-  return GALPY_CUDA_SIG_GENERIC;
+  for (int k = 0; k < npot; k++)
+    if (is_ellipsoidal(pot_type[k])) return GALPY_CUDA_SIG_GENERIC;
+  return GALPY_CUDA_SIG_COMMON;
+}
+
+// The signature a launch runs with: GALPY_CUDA_SIG_COMMON falls back to the
+// full run-time list when the host copy of the records shows an ellipsoidal
+// component.
+static int launch_signature(const galpy_cuda_launch* L)
+{
+  if (L->signature != GALPY_CUDA_SIG_COMMON || !L->comps_host) return L->signature;
+  const GpComp* hc = static_cast<const GpComp*>(L->comps_host);
+  for (int k = 0; k < L->ncomp; k++)
+    if (is_ellipsoidal(hc[k].type)) return GALPY_CUDA_SIG_GENERIC;
+  return GALPY_CUDA_SIG_COMMON;
 }
 
 static bool method_supported(int m)
@@ -173,19 +187,19 @@ struct Scratch {  // device scratch of one launch (128 bytes)
   unsigned long long counter;
   unsigned long long done_count;
   unsigned long long tail_counter;
-  unsigned long long stage_claim;  // staging slots taken (streaming of finished orbits)
+  unsigned long long spare;
   int abort_flag;
   unsigned sm_claim[kMaxTailSms];  // first block resident on each reserved SM
   int pad[7];
 };
 static_assert(sizeof(Scratch) == 128, "Scratch layout");
 
-// Device buffers of the streaming of finished orbits (RowStreamer).
+// Device buffers of the streaming of finished orbits (RowStreamer); the
+// launch's output then holds the rows in work-queue order.
 struct Staging {
-  double* rows = nullptr;     // [nobj][row] in completion order
-  int* idx = nullptr;         // [nobj] orbit of each slot
-  unsigned* ready = nullptr;  // [nchunk] staged slots per chunk
-  int* pend = nullptr;        // [nobj] unfinished row writers per orbit
+  int* idx = nullptr;         // [nobj] orbit at each output position
+  unsigned* ready = nullptr;  // [nchunk] complete positions per chunk
+  int* pend = nullptr;        // [nobj] unfinished row writers per position
 };
 
 // Launch on `stream`.  scratch: device Scratch (counter zeroed here).
@@ -213,7 +227,7 @@ static int prepare_launch(const galpy_cuda_launch* L, Scratch* scratch, bool pro
 {
   double scal[kMaxComp * kScalarStride] = {0.0};
   const bool direct = direct_scalars(L, scal);
-  ki = pick_kernel(L->planar, L->variational, L->precision, L->odeint_type, L->signature,
+  ki = pick_kernel(L->planar, L->variational, L->precision, L->odeint_type, launch_signature(L),
                    L->variant, direct, launch_system(L));
   if (!ki.fn) return set_error(GALPY_CUDA_ERR_METHOD, "method/precision combination not implemented");
   memset(&A, 0, sizeof(A));
@@ -245,11 +259,9 @@ static int prepare_launch(const galpy_cuda_launch* L, Scratch* scratch, bool pro
   A.variational_nv = L->variational ? (L->planar ? 8 : 12) : 0;
   memcpy(A.scal, scal, sizeof(scal));
   if (stg) {
-    A.stage_rows = stg->rows;
     A.stage_idx = stg->idx;
     A.stage_ready = stg->ready;
     A.pend = stg->pend;
-    A.stage_claim = &scratch->stage_claim;
   }
   return GALPY_CUDA_OK;
 }
@@ -480,11 +492,14 @@ static int select_device(const galpy_cuda_opts* o)
 // The blocking entry points return galpy's AoS result rows in host memory
 // (pinned or pageable numpy arrays).  Copying the whole result after the
 // kernel would add the full device->host transfer (5 GB for the batching
-// workload) to the call.  Instead the kernel copies every finished orbit's
-// rows to a staging array in completion order (stage_orbit), and while it
-// runs this streamer copies the finished 4096-orbit chunks of the staging
-// array through pinned bounce buffers on a copy stream, and worker threads
-// scatter their rows to the orbits' places in the caller's result array.
+// workload) to the call.  Instead the kernel writes the rows in work-queue
+// order (the orbit at queue position q at output position q) and publishes
+// each position once its rows are complete; while it runs, this streamer
+// copies every 4096-position chunk whose positions are all published
+// through pinned bounce buffers on a copy stream, in any order, and worker
+// threads scatter the rows to the orbits' places in the caller's result
+// array.  Positions are taken in longest-first order, so a chunk holds
+// orbits of similar length, which finish at similar times.
 // Pinned bounce buffers of RowStreamer, kept for later calls (pinning host
 // memory is slow); at most kBounceCache of them stay cached.
 static std::mutex g_bounce_mu;
@@ -519,11 +534,13 @@ class RowStreamer {
   static constexpr size_t kBounceBytes = 32u << 20;
   static constexpr int kBuffers = 4;
 
-  RowStreamer(const Staging& st, long long nobj, size_t row, double* result,
+  // rows: the launch's output, [nobj][row] in work-queue order
+  RowStreamer(const Staging& st, const double* rows, long long nobj, size_t row, double* result,
               cudaStream_t side)
-      : st_(st), nobj_(nobj), row_(row), result_(result), side_(side)
+      : st_(st), rows_(rows), nobj_(nobj), row_(row), result_(result), side_(side)
   {
     nchunk_ = (int)((nobj + kStageChunk - 1) / kStageChunk);
+    issued_.assign(nchunk_, 0);
     per_buf_ = (long long)(kBounceBytes / (row * sizeof(double)));
     if (per_buf_ < 1) per_buf_ = 1;
     if (per_buf_ > kStageChunk) per_buf_ = kStageChunk;
@@ -569,7 +586,7 @@ class RowStreamer {
   cudaError_t poll(bool& all_done)
   {
     cudaError_t e;
-    if (next_slot_ < nobj_) {
+    if (issued_total_ < nobj_) {
       if ((e = cudaMemcpyAsync(ready_h_, st_.ready, nchunk_ * sizeof(unsigned),
                                cudaMemcpyDeviceToHost, side_)) != cudaSuccess)
         return e;
@@ -583,31 +600,39 @@ class RowStreamer {
       b.state = 2;
       enqueue(b);
     }
-    // copies, in slot order, of the slots whose chunk is complete
+    // copies of complete chunks, lowest chunk first
+    while (scan_ < nchunk_ && issued_[scan_] == chunk_size(scan_)) scan_++;
+    int c = scan_;
     for (auto& b : buf_) {
-      if (next_slot_ >= nobj_) break;
+      if (issued_total_ >= nobj_) break;
       if (b.state != 0) continue;
-      const int c = (int)(next_slot_ / kStageChunk);
-      const long long csize = std::min<long long>(kStageChunk, nobj_ - (long long)c * kStageChunk);
-      if (ready_h_[c] < (unsigned)csize) break;
-      const long long chunk_end = (long long)c * kStageChunk + csize;
-      const long long n = std::min(per_buf_, chunk_end - next_slot_);
-      if ((e = cudaMemcpyAsync(b.rows, st_.rows + next_slot_ * row_, n * row_ * sizeof(double),
+      while (c < nchunk_ && (issued_[c] == chunk_size(c) || ready_h_[c] < (unsigned)chunk_size(c)))
+        c++;
+      if (c >= nchunk_) break;
+      const long long first = (long long)c * kStageChunk + issued_[c];
+      const long long n = std::min<long long>(per_buf_, chunk_size(c) - issued_[c]);
+      if ((e = cudaMemcpyAsync(b.rows, rows_ + first * row_, n * row_ * sizeof(double),
                                cudaMemcpyDeviceToHost, copy_)) != cudaSuccess)
         return e;
-      if ((e = cudaMemcpyAsync(b.idx, st_.idx + next_slot_, n * sizeof(int),
+      if ((e = cudaMemcpyAsync(b.idx, st_.idx + first, n * sizeof(int),
                                cudaMemcpyDeviceToHost, copy_)) != cudaSuccess)
         return e;
       if ((e = cudaEventRecord(b.ev, copy_)) != cudaSuccess) return e;
       b.count = n;
       b.state = 1;
-      next_slot_ += n;
+      issued_[c] += (int)n;
+      issued_total_ += n;
     }
-    all_done = next_slot_ >= nobj_ && delivered_.load() >= nobj_;
+    all_done = issued_total_ >= nobj_ && delivered_.load() >= nobj_;
     return cudaSuccess;
   }
 
  private:
+  int chunk_size(int c) const
+  {
+    return (int)std::min<long long>(kStageChunk, nobj_ - (long long)c * kStageChunk);
+  }
+
   struct Buf {
     double* rows = nullptr;
     int* idx = nullptr;
@@ -653,12 +678,15 @@ class RowStreamer {
   }
 
   Staging st_;
+  const double* rows_;
   long long nobj_;
   size_t row_;
   double* result_;
   cudaStream_t side_, copy_ = nullptr;
   int nchunk_ = 0, nworkers_ = 1;
-  long long per_buf_ = 1, next_slot_ = 0;
+  long long per_buf_ = 1, issued_total_ = 0;
+  std::vector<int> issued_;  // positions of each chunk whose copy is issued
+  int scan_ = 0;             // chunks below are fully issued
   unsigned* ready_h_ = nullptr;
   Buf buf_[kBuffers];
   std::vector<std::thread> workers_;
@@ -731,24 +759,23 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
   GPC_CUDA_TRY(alloc_async(&dcomp.p, comps.size() * sizeof(GpComp), pool, stream));
   GPC_CUDA_TRY(alloc_async(&dscr.p, sizeof(Scratch), pool, stream));
   if (o && o->nsteps) GPC_CUDA_TRY(alloc_async(&dsteps.p, (size_t)nobj * sizeof(long long), pool, stream));
-  // streaming of finished orbits (RowStreamer): staging rows, slot orbits,
-  // per-chunk ready counts, per-orbit writer counts
+  // streaming of finished orbits (RowStreamer; the output then holds the
+  // rows in work-queue order): the orbit at each output position, per-chunk
+  // counts of complete positions, per-position writer counts
   const int stream_opt =
       o && o->size >= (int)(offsetof(galpy_cuda_opts, stream_rows) + sizeof(int))
           ? o->stream_rows
           : -1;
   const bool stream_rows = stream_opt == 1 || (stream_opt < 0 && stream_rows_for(nobj, n_out));
-  DevBuf srows, sidx, sready, spend;
-  srows.s = sidx.s = sready.s = spend.s = stream;
+  DevBuf sidx, sready, spend;
+  sidx.s = sready.s = spend.s = stream;
   Staging stg;
   if (stream_rows) {
     const size_t nchunk = (size_t)((nobj + kStageChunk - 1) / kStageChunk);
-    GPC_CUDA_TRY(alloc_async(&srows.p, n_out * sizeof(double), pool, stream));
     GPC_CUDA_TRY(alloc_async(&sidx.p, (size_t)nobj * sizeof(int), pool, stream));
     GPC_CUDA_TRY(alloc_async(&sready.p, nchunk * sizeof(unsigned), pool, stream));
     GPC_CUDA_TRY(alloc_async(&spend.p, (size_t)nobj * sizeof(int), pool, stream));
     GPC_CUDA_TRY(cudaMemsetAsync(sready.p, 0, nchunk * sizeof(unsigned), stream));
-    stg.rows = static_cast<double*>(srows.p);
     stg.idx = static_cast<int*>(sidx.p);
     stg.ready = static_cast<unsigned*>(sready.p);
     stg.pend = static_cast<int*>(spend.p);
@@ -806,7 +833,8 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
     }
   } eg{e0, e1};
   SigintGuard sig(ctl == nullptr);
-  RowStreamer streamer(stg, nobj, (size_t)nt * nv, result, side);
+  RowStreamer streamer(stg, static_cast<const double*>(dout.p), nobj, (size_t)nt * nv, result,
+                       side);
   if (stream_rows) GPC_CUDA_TRY(streamer.start());
   const bool track = cb != nullptr || ctl != nullptr;
   GPC_CUDA_TRY(cudaEventRecord(e0, stream));
@@ -1066,21 +1094,39 @@ static int run_host_split(int planar, int var, long long nobj, const double* w, 
   return GALPY_CUDA_OK;
 }
 
+// f(i0, i1) over [0, n) in contiguous pieces on up to 16 host threads (one
+// thread below 65,536 items): the per-orbit coordinate conversions of large
+// batches (1M orbits: ~40 ms of sin/cos on one core).
+template <class F>
+static void host_parallel_for(long long n, F f)
+{
+  const int nthr = n < 65536 ? 1 : (int)std::max(1u, std::min(std::thread::hardware_concurrency(), 16u));
+  if (nthr <= 1) {
+    f(0LL, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int k = 0; k < nthr; k++) th.emplace_back([&, k] { f(n * k / nthr, n * (k + 1) / nthr); });
+  for (auto& x : th) x.join();
+}
+
 // (R, vR, vT, z, vz, phi, t) -> surface-of-section state (x, y, vx, vy, A,
 // t, psi), in place, exactly as cyl_to_sos_galpy (bovy_coords.c:149-163)
 static void cyl_to_sos_inplace(long long nobj, double* yo)
 {
-  for (long long i = 0; i < nobj; i++) {
-    double* v = yo + 7 * i;
-    const double R = v[0], cp = cos(v[5]), sp = sin(v[5]), vR = v[1], vT = v[2];
-    v[5] = v[6];
-    v[6] = atan2(v[3], v[4]);
-    v[4] = sqrt(v[3] * v[3] + v[4] * v[4]);
-    v[0] = R * cp;
-    v[1] = R * sp;
-    v[2] = vR * cp - vT * sp;
-    v[3] = vR * sp + vT * cp;
-  }
+  host_parallel_for(nobj, [yo](long long i0, long long i1) {
+    for (long long i = i0; i < i1; i++) {
+      double* v = yo + 7 * i;
+      const double R = v[0], cp = cos(v[5]), sp = sin(v[5]), vR = v[1], vT = v[2];
+      v[5] = v[6];
+      v[6] = atan2(v[3], v[4]);
+      v[4] = sqrt(v[3] * v[3] + v[4] * v[4]);
+      v[0] = R * cp;
+      v[1] = R * sp;
+      v[2] = vR * cp - vT * sp;
+      v[3] = vR * sp + vT * cp;
+    }
+  });
 }
 
 // (R, vR, vT, phi, t) -> planar surface-of-section state, in place, exactly
@@ -1088,49 +1134,53 @@ static void cyl_to_sos_inplace(long long nobj, double* yo)
 // (x, vx, A, t, psi), otherwise (x = 0) (y, vy, A, t, psi)
 static void polar_to_sos_inplace(long long nobj, double* yo, int surface)
 {
-  for (long long i = 0; i < nobj; i++) {
-    double* v = yo + 5 * i;
-    const double R = v[0], cp = cos(v[3]), sp = sin(v[3]), vR = v[1], vT = v[2];
-    if (surface == 1) {
-      v[0] = R * cp;
-      v[1] = vR * cp - vT * sp;
-      const double y = R * sp, vy = vR * sp + vT * cp;
-      v[2] = sqrt(y * y + vy * vy);
-      v[3] = v[4];
-      v[4] = atan2(y, vy);
-    } else {
-      v[0] = R * sp;
-      v[1] = vR * sp + vT * cp;
-      const double x = R * cp, vx = vR * cp - vT * sp;
-      v[2] = sqrt(x * x + vx * vx);
-      v[3] = v[4];
-      v[4] = atan2(x, vx);
+  host_parallel_for(nobj, [yo, surface](long long i0, long long i1) {
+    for (long long i = i0; i < i1; i++) {
+      double* v = yo + 5 * i;
+      const double R = v[0], cp = cos(v[3]), sp = sin(v[3]), vR = v[1], vT = v[2];
+      if (surface == 1) {
+        v[0] = R * cp;
+        v[1] = vR * cp - vT * sp;
+        const double y = R * sp, vy = vR * sp + vT * cp;
+        v[2] = sqrt(y * y + vy * vy);
+        v[3] = v[4];
+        v[4] = atan2(y, vy);
+      } else {
+        v[0] = R * sp;
+        v[1] = vR * sp + vT * cp;
+        const double x = R * cp, vx = vR * cp - vT * sp;
+        v[2] = sqrt(x * x + vx * vx);
+        v[3] = v[4];
+        v[4] = atan2(x, vx);
+      }
     }
-  }
+  });
 }
 
 // cylindrical -> rectangular initial conditions, in place, exactly as
 // cyl_to_rect_galpy / polar_to_rect_galpy (bovy_coords.c:57-124)
 static void cyl_to_rect_inplace(int planar, long long nobj, double* yo)
 {
-  for (long long i = 0; i < nobj; i++) {
-    double* v = yo + (planar ? 4 : 6) * i;
-    if (planar) {
-      const double R = v[0], phi = v[3], cp = cos(phi), sp = sin(phi), vR = v[1], vT = v[2];
-      v[0] = R * cp;
-      v[1] = R * sp;
-      v[2] = vR * cp - vT * sp;
-      v[3] = vR * sp + vT * cp;
-    } else {
-      const double R = v[0], phi = v[5], cp = cos(phi), sp = sin(phi), vR = v[1], vT = v[2];
-      v[0] = R * cp;
-      v[1] = R * sp;
-      v[2] = v[3];
-      v[5] = v[4];
-      v[3] = vR * cp - vT * sp;
-      v[4] = vR * sp + vT * cp;
+  host_parallel_for(nobj, [yo, planar](long long i0, long long i1) {
+    for (long long i = i0; i < i1; i++) {
+      double* v = yo + (planar ? 4 : 6) * i;
+      if (planar) {
+        const double R = v[0], phi = v[3], cp = cos(phi), sp = sin(phi), vR = v[1], vT = v[2];
+        v[0] = R * cp;
+        v[1] = R * sp;
+        v[2] = vR * cp - vT * sp;
+        v[3] = vR * sp + vT * cp;
+      } else {
+        const double R = v[0], phi = v[5], cp = cos(phi), sp = sin(phi), vR = v[1], vT = v[2];
+        v[0] = R * cp;
+        v[1] = R * sp;
+        v[2] = v[3];
+        v[5] = v[4];
+        v[3] = vR * cp - vT * sp;
+        v[4] = vR * sp + vT * cp;
+      }
     }
-  }
+  });
 }
 
 // ----------------------------------------------------------------------------

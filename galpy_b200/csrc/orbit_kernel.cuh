@@ -48,16 +48,15 @@ struct KArgs {
   // per warp of the grid (NULL: dense output in the warp's slot cycle)
   double* dense_q;
   // Streaming of finished orbits (blocking host entry points, AoS output):
-  // when an orbit's last row is written, its rows are copied to
-  // stage_rows[slot] with slot taken in completion order, stage_idx[slot]
-  // records the orbit, and stage_ready[slot / kStageChunk] counts the staged
-  // slots of each chunk, so that the host can copy finished chunks while the
-  // kernel runs.  pend[i] counts the writers of orbit i's rows that have not
-  // finished (its own lane, and its queued dense-output requests).  NULL:
-  // no streaming.
-  double* stage_rows;
+  // the rows of the orbit at work-queue position q are written at output
+  // position q (the output holds the rows in queue order); once they are
+  // all written, stage_idx[q] records the orbit and stage_ready[q /
+  // kStageChunk] counts the complete positions of each chunk, so that the
+  // host can copy finished chunks while the kernel runs.  pend[q] counts
+  // the writers of those rows that have not finished (the orbit's own lane,
+  // and its queued dense-output requests).  NULL: no streaming (rows at the
+  // orbit's index).
   int* stage_idx;
-  unsigned long long* stage_claim;
   unsigned* stage_ready;
   int* pend;
   // scalar parameters of the (single) potential, read from the constant bank
@@ -108,41 +107,44 @@ __device__ __forceinline__ bool tail_claimed(const KArgs& A)
 // Staged slots per chunk of the streaming of finished orbits.
 constexpr int kStageChunk = 4096;
 
-#if defined(__CUDACC__)
-// Orbit i is complete (all of its rows written, by whichever lanes wrote
-// them, and made visible with __threadfence): copy its rows (AoS, nrow * nv
-// contiguous doubles) to the next staging slot and publish it.
-static __device__ __noinline__ void stage_orbit(const KArgs& A, long long i, int nv)
+// Output position of the orbit i at work-queue position q: q when rows are
+// streamed (the output then holds them in queue order), else i.
+__device__ __forceinline__ long long out_pos(const KArgs& A, long long q, long long i)
 {
-  const long long slot = (long long)atomicAdd(A.stage_claim, 1ULL);
-  const long long row = (long long)(A.out.nt - A.out.row0) * nv;
-  const double* src = A.out.out + i * row;
-  double* dst = A.stage_rows + slot * row;
-  if ((row & 1) == 0) {
-    const double2* s2 = reinterpret_cast<const double2*>(src);
-    double2* d2 = reinterpret_cast<double2*>(dst);
-    for (long long k = 0; k < row / 2; k++) d2[k] = s2[k];
-  } else {
-    for (long long k = 0; k < row; k++) dst[k] = src[k];
-  }
-  A.stage_idx[slot] = (int)i;
-  __threadfence();
-  atomicAdd(&A.stage_ready[slot / kStageChunk], 1u);
+  return A.stage_idx ? q : i;
 }
 
-// One writer of orbit i's rows has finished: the last one stages the orbit.
-__device__ __forceinline__ void release_orbit(const KArgs& A, long long i, int nv)
+// The orbit whose rows are at output position p.
+__device__ __forceinline__ long long orbit_at(const KArgs& A, long long p)
+{
+  return A.stage_idx && A.order ? (long long)A.order[p] : p;
+}
+
+#if defined(__CUDACC__)
+// The rows at output position p (orbit i) are all written, by whichever lanes
+// wrote them, and made visible with __threadfence: publish the position.
+__device__ __forceinline__ void publish_rows(const KArgs& A, long long p, long long i)
+{
+  A.stage_idx[p] = (int)i;
+  __threadfence();
+  atomicAdd(&A.stage_ready[p / kStageChunk], 1u);
+}
+
+// One writer of the rows at output position p has finished: the last one
+// publishes them.
+__device__ __forceinline__ void release_rows(const KArgs& A, long long p)
 {
   __threadfence();  // this writer's rows before the count
-  if (atomicSub(&A.pend[i], 1) == 1) {
-    __threadfence();  // the other writers' rows before the copy
-    stage_orbit(A, i, nv);
+  if (atomicSub(&A.pend[p], 1) == 1) {
+    __threadfence();  // the other writers' rows before the publication
+    publish_rows(A, p, orbit_at(A, p));
   }
 }
 #endif
 
-// Next orbit of a worker: the reserved-SM tail queue first (tail role), then
-// the main queue; -1 when both are exhausted.
+// Next work-queue position of a worker: the reserved-SM tail queue first
+// (tail role), then the main queue; -1 when both are exhausted.  The orbit
+// at position q is order[q] (q without an order).
 __device__ __forceinline__ long long next_orbit(const KArgs& A, int& my_role)
 {
   long long q = -1;
@@ -166,7 +168,7 @@ __device__ __forceinline__ long long next_orbit(const KArgs& A, int& my_role)
       if (q >= A.tail_len) return -1;
     }
   }
-  return A.order ? A.order[q] : q;
+  return q;
 }
 
 #if defined(__CUDACC__)
@@ -193,7 +195,7 @@ __device__ __forceinline__ void queued_loop(const KArgs& A, double* slot_store, 
   double* const q = A.dense_q + warp_id * (long long)(M::kQueueFields * QS);
   M m;
   m.bind(slot_store + threadIdx.x, true);
-  long long i = 0;
+  long long i = 0, pos = 0;  // the active orbit and its output position
   bool active = false, aborting = false, idle = false;
   const GpComp* comps = A.comps;
   unsigned iter = 0;
@@ -201,35 +203,39 @@ __device__ __forceinline__ void queued_loop(const KArgs& A, double* slot_store, 
   for (;;) {
     const bool dense = slot >= 12;
     if (!dense && !active && !idle) {
-      const long long o = next_orbit(A, my_role);
-      if (o < 0) {
+      const long long qpos = next_orbit(A, my_role);
+      if (qpos < 0) {
         idle = true;
-      } else if (aborting) {
-        A.err[o] = E_ABORT;
-        write_nan_rows<M::NV, D, CYL_OK, M::kRow>(A.out, o, 0);
-        if (A.stage_rows) {
-          __threadfence();
-          stage_orbit(A, o, M::NV);
-        }
       } else {
-        i = o;
-        if (A.pend) A.pend[i] = 1;  // its own lane writes rows until it is done
-        double w[M::NV];
-        load_state<M>(A, i, w);
-        comps = A.comps + (A.group ? (long long)A.group[i] * A.ncomp : 0LL);
-        Rows rows{&A.out, i};
-        m.init(w, A.t + (A.indiv_t ? i * (long long)A.nt : 0LL), A.nt, A.dt, A.rtol, A.atol,
-               A.max_attempts, rows);
-        active = true;
+        i = A.order ? (long long)A.order[qpos] : qpos;
+        pos = out_pos(A, qpos, i);
+        if (aborting) {
+          A.err[i] = E_ABORT;
+          write_nan_rows<M::NV, D, CYL_OK, M::kRow>(A.out, pos, 0);
+          if (A.stage_idx) {
+            __threadfence();
+            publish_rows(A, pos, i);
+          }
+        } else {
+          if (A.pend) A.pend[pos] = 1;  // its own lane writes rows until it is done
+          double w[M::NV];
+          load_state<M>(A, i, w);
+          comps = A.comps + (A.group ? (long long)A.group[i] * A.ncomp : 0LL);
+          Rows rows{&A.out, pos};
+          m.init(w, A.t + (A.indiv_t ? i * (long long)A.nt : 0LL), A.nt, A.dt, A.rtol, A.atol,
+                 A.max_attempts, rows);
+          active = true;
+        }
       }
     }
     const int p = (qhead + lane) & (QS - 1);
     if (dense ? lane < nround : (active && !m.done)) {
       double y[M::NY], qq[M::NA], a[M::NA];
-      long long o = i;
+      long long o = i, opos = pos;
       const GpComp* cp = comps;
-      if (dense) {  // the request's orbit and its parameter group
-        o = reinterpret_cast<const long long*>(q)[(11 * M::N + 2) * QS + p];
+      if (dense) {  // the request's output position, orbit and parameter group
+        opos = reinterpret_cast<const long long*>(q)[(11 * M::N + 2) * QS + p];
+        o = orbit_at(A, opos);
         cp = A.comps + (A.group ? (long long)A.group[o] * A.ncomp : 0LL);
         m.req_point(y, slot + 2, q, p);
       } else {
@@ -237,10 +243,10 @@ __device__ __forceinline__ void queued_loop(const KArgs& A, double* slot_store, 
       }
       M::pos(y, qq);
       eval_force<D, PREC, VAR, POT>(cp, A.ncomp, qq, a, A.scal);
-      Rows rows{&A.out, o};
+      Rows rows{&A.out, opos};
       if (dense) {
         m.req_consume(y, a, slot + 2, q, p, A.t + (A.indiv_t ? o * (long long)A.nt : 0LL), rows);
-        if (A.stage_rows && slot == 14) release_orbit(A, o, M::NV);  // its rows are written
+        if (A.stage_idx && slot == 14) release_rows(A, opos);  // its rows are written
       } else {
         m.consume(y, a, rows, slot);
       }
@@ -250,10 +256,10 @@ __device__ __forceinline__ void queued_loop(const KArgs& A, double* slot_store, 
       const unsigned want = __ballot_sync(FULL, m.want_enqueue);
       if (m.want_enqueue) {
         const int rank = __popc(want & ((1u << lane) - 1u));
-        if (A.pend) atomicAdd(&A.pend[i], 1);  // the request writes rows of orbit i
-        m.write_request(q, (qhead + qcount + rank) & (QS - 1), i);
+        if (A.pend) atomicAdd(&A.pend[pos], 1);  // the request writes rows at pos
+        m.write_request(q, (qhead + qcount + rank) & (QS - 1), pos);
         m.want_enqueue = false;
-        Rows rows{&A.out, i};
+        Rows rows{&A.out, pos};
         m.finish_step(rows);
       }
       qcount += __popc(want);
@@ -288,12 +294,12 @@ __device__ __forceinline__ void queued_loop(const KArgs& A, double* slot_store, 
       }
     }
     if (active && m.done) {
-      Rows rows{&A.out, i};
+      Rows rows{&A.out, pos};
       fill_unreached_rows(m, rows);
       A.err[i] = m.err;
       if (A.nsteps) A.nsteps[i] = m.nsteps;
       if (A.done_count) atomicAdd(A.done_count, 1ULL);
-      if (A.stage_rows) release_orbit(A, i, M::NV);
+      if (A.stage_idx) release_rows(A, pos);
       active = false;
     }
   }
@@ -333,48 +339,30 @@ __global__ void __launch_bounds__(128, MINB) orbit_kernel(const __grid_constant_
   }
   M m;
   m.bind(slot_store + threadIdx.x);
-  long long i = 0;
+  long long i = 0, pos = 0;  // the active orbit and its output position
   bool active = false, aborting = false;
   const GpComp* comps = A.comps;
   unsigned iter = 0;
   int slot = 0;
   for (;;) {
     if (!active) {
-      long long q = -1;
-      if (my_role == 1) {
-        q = (long long)atomicAdd(A.tail_counter, 1ULL);
-        if (q >= A.tail_len) {
-          q = -1;
-          my_role = 0;
-        }
-      }
-      if (q < 0 && A.tail_len > 0 && !tail_claimed(A)) {
-        // no reserved SM hosts a tail warp: the longest orbits go first here
-        q = (long long)atomicAdd(A.tail_counter, 1ULL);
-        if (q >= A.tail_len) q = -1;
-      }
-      if (q < 0) {
-        q = (long long)atomicAdd(A.counter, 1ULL) + A.tail_len;
-        if (q >= A.nobj) {
-          if (A.tail_len == 0) break;
-          q = (long long)atomicAdd(A.tail_counter, 1ULL);
-          if (q >= A.tail_len) break;
-        }
-      }
-      i = A.order ? A.order[q] : q;
+      const long long qpos = next_orbit(A, my_role);
+      if (qpos < 0) break;
+      i = A.order ? (long long)A.order[qpos] : qpos;
+      pos = out_pos(A, qpos, i);
       if (aborting) {
         A.err[i] = E_ABORT;
-        write_nan_rows<M::NV, D, CYL_OK, M::kRow>(A.out, i, 0);
-        if (A.stage_rows) {
+        write_nan_rows<M::NV, D, CYL_OK, M::kRow>(A.out, pos, 0);
+        if (A.stage_idx) {
           __threadfence();
-          stage_orbit(A, i, M::NV);
+          publish_rows(A, pos, i);
         }
         continue;
       }
       double w[M::NV];
       load_state<M>(A, i, w);
       comps = A.comps + (A.group ? (long long)A.group[i] * A.ncomp : 0LL);
-      Rows rows{&A.out, i};
+      Rows rows{&A.out, pos};
       m.init(w, A.t + (A.indiv_t ? i * (long long)A.nt : 0LL), A.nt, A.dt, A.rtol, A.atol,
              A.max_attempts, rows);
       active = true;
@@ -384,7 +372,7 @@ __global__ void __launch_bounds__(128, MINB) orbit_kernel(const __grid_constant_
       m.point(y, slot);
       M::pos(y, q);
       eval_force<D, PREC, VAR, POT>(comps, A.ncomp, q, a, A.scal);
-      Rows rows{&A.out, i};
+      Rows rows{&A.out, pos};
       m.consume(y, a, rows, slot);
     }
     // advance the warp's stage slot (DOP853): the dense-output slots run only
@@ -402,14 +390,14 @@ __global__ void __launch_bounds__(128, MINB) orbit_kernel(const __grid_constant_
       }
     }
     if (m.done) {
-      Rows rows{&A.out, i};
+      Rows rows{&A.out, pos};
       fill_unreached_rows(m, rows);
       A.err[i] = m.err;
       if (A.nsteps) A.nsteps[i] = m.nsteps;
       if (A.done_count) atomicAdd(A.done_count, 1ULL);
-      if (A.stage_rows) {
+      if (A.stage_idx) {
         __threadfence();
-        stage_orbit(A, i, M::NV);
+        publish_rows(A, pos, i);
       }
       active = false;
     }
@@ -468,8 +456,9 @@ static KernelInfo pick_plain(int planar, int method, int variant)
 }
 
 // sig: GALPY_CUDA_SIG_MW14 selects the kernels with the MWPotential2014
-// component list fixed at compile time (plain runs); variational runs walk
-// the component list at run time.
+// component list fixed at compile time (plain runs), GALPY_CUDA_SIG_COMMON
+// the float64 kernels whose run-time list leaves out the ellipsoidal family;
+// variational runs and float32 forces walk the full list at run time.
 template <class Set>
 static KernelInfo pick_kernel_in(int planar, int var, int prec, int method, int sig,
                                  int variant, bool direct)
@@ -485,6 +474,8 @@ static KernelInfo pick_kernel_in(int planar, int var, int prec, int method, int 
     return direct ? pick_plain<Set, PREC_F32, MW14Pot>(planar, method, variant)
                   : pick_plain<Set, PREC_F32, MW14GroupPot>(planar, method, variant);
   }
+  if (sig == GALPY_CUDA_SIG_COMMON)
+    return pick_plain<Set, PREC_FP64, DynPotCommon>(planar, method, variant);
   if (!mw14) return pick_plain<Set, PREC_FP64, DynPot>(planar, method, variant);
   return direct ? pick_plain<Set, PREC_FP64, MW14Pot>(planar, method, variant)
                 : pick_plain<Set, PREC_FP64, MW14GroupPot>(planar, method, variant);

@@ -504,7 +504,9 @@ GPC_HD inline double exptruncnfw_F(const S& sc, double r)
 // Add one component's contribution to the radial factors: the acceleration
 // is a = (x gR, y (gR + gyx), z gz) + a0, where a0 takes the terms that are
 // not of that form (Henon-Heiles' -amp x^2 in a_y, ellipsoidal components).
-// TYPE < 0: read the type at run time.
+// TYPE < 0: read the type at run time, any supported type (kRunTimeAll) or
+// any but the ellipsoidal family (kRunTimeCommon).
+constexpr int kRunTimeAll = -1, kRunTimeCommon = -2;
 // Scalar parameters of a component: from the compiled record in global
 // memory (read-only path), or from a copy passed as a kernel parameter
 // (constant bank: no load instruction when the index is a compile-time
@@ -886,11 +888,17 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
     }
     case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
     case T_POWERTRI: case T_TWOPOWERTRI: {  // in float64
-      double ax, ay, az;
-      ell_accel(tp, type, (double)x, (double)y, PLANAR ? 0.0 : (double)z, ax, ay, az);
-      a0.x += T(ax);
-      a0.y += T(ay);
-      if (!PLANAR) a0.z += T(az);
+      if constexpr (TYPE == kRunTimeCommon) {
+        // not carried by the common run-time list (the host never selects it
+        // for such a potential): a non-finite force stops the orbit, err 3
+        gR = T(NAN);
+      } else {
+        double ax, ay, az;
+        ell_accel(tp, type, (double)x, (double)y, PLANAR ? 0.0 : (double)z, ax, ay, az);
+        a0.x += T(ax);
+        a0.y += T(ay);
+        if (!PLANAR) a0.z += T(az);
+      }
       break;
     }
     default: {
@@ -912,8 +920,26 @@ struct DynPot {
                                 AddAcc<T>& a0)
   {
     for (int k = 0; k < ncomp; k++)
-      comp_accel<T, PLANAR, -1>(comp + k, ScalarsGlobal{comp + k}, x, y, z, z2, R2, r2, gR, gz,
-                                gyx, a0);
+      comp_accel<T, PLANAR, kRunTimeAll>(comp + k, ScalarsGlobal{comp + k}, x, y, z, z2, R2, r2,
+                                         gR, gz, gyx, a0);
+  }
+};
+
+// Run-time component list without the ellipsoidal family, whose
+// Gauss-Legendre shell integral costs every kernel of the full list 5-30
+// registers (and some kernels a resident block): the host selects it for
+// potentials without such a component (GALPY_CUDA_SIG_COMMON).
+struct DynPotCommon {
+  static constexpr bool kDirectScalars = false;
+  static constexpr bool kAdditive = true;
+  template <typename T, bool PLANAR>
+  GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, const double* /*scal*/, int ncomp,
+                                T x, T y, T z, T z2, T R2, T r2, T& gR, T& gz, T& gyx,
+                                AddAcc<T>& a0)
+  {
+    for (int k = 0; k < ncomp; k++)
+      comp_accel<T, PLANAR, kRunTimeCommon>(comp + k, ScalarsGlobal{comp + k}, x, y, z, z2, R2,
+                                            r2, gR, gz, gyx, a0);
   }
 };
 

@@ -74,6 +74,13 @@ extern "C" {
 /* potential signatures (kernels specialised at compile time) */
 #define GALPY_CUDA_SIG_GENERIC 0 /* any list of supported components */
 #define GALPY_CUDA_SIG_MW14 1    /* exactly (15, 5, 9): MWPotential2014's component types */
+#define GALPY_CUDA_SIG_COMMON 2  /* a list without ellipsoidal components (types 21, 22, 23,
+                                    30, 37, 38, 43): float64 kernels whose run-time list
+                                    leaves that family out (fewer registers).  Orbits of a
+                                    launch given this signature for a potential with such a
+                                    component stop with err 3 (non-finite force); when the
+                                    launch carries comps_host the engine checks the types and
+                                    uses the full list instead. */
 
 /* order in which orbits are handed to the GPU threads */
 /* the ODE system of a device launch (galpy_cuda_launch.system) */

@@ -37,12 +37,23 @@ def _ptr(a, t):
     return a.ctypes.data_as(t) if a is not None else None
 
 
+def reference_tree():
+    """The reference checkout the oracle's recipe reads (its REF: the
+    GALPY_REFERENCE_TREE environment variable, else the recipe's default);
+    it need not exist."""
+    import subprocess
+
+    r = subprocess.run(["make", "-s", "-C", _HERE, "print-ref"], stdout=subprocess.PIPE,
+                       text=True, check=True)
+    return r.stdout.strip()
+
+
 def build(ref=False):
     """Compile the oracle (and, if asked and the reference is present, _ref)."""
     import subprocess
 
     subprocess.run(["make", "-s", "-C", _HERE, "all"], check=True)
-    tree = os.environ.get("GALPY_REFERENCE_TREE", "/root/reference")
+    tree = reference_tree()
     if ref and os.path.isdir(os.path.join(tree, "galpy")):
         subprocess.run(["make", "-s", "-C", _HERE, "ref", "REF=" + tree], check=True)
 

@@ -10,10 +10,24 @@ but copied with the working tree to GPU machines, so galpy's own
 Orbit.integrate can drive the engine there).  Without either the galpy-based
 tests are skipped."""
 import os
+import subprocess
 import sys
 import types
 
-REFERENCE = os.environ.get("GALPY_REFERENCE_TREE", "/root/reference")
+
+def _reference_tree():
+    """The reference checkout the oracle's recipe reads (oracle/Makefile's
+    REF: GALPY_REFERENCE_TREE, else its default); it need not exist."""
+    here = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    try:
+        r = subprocess.run(["make", "-s", "-C", os.path.join(here, "oracle"), "print-ref"],
+                           stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        return r.stdout.strip()
+    except OSError:  # no make: only the installed copy can serve
+        return ""
+
+
+REFERENCE = _reference_tree()
 INSTALLED = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
                          "baseline", "_ref")
 

@@ -49,6 +49,22 @@ def test_compile_potential_host_only(golden):
         galpy_b200.compile_potential(([1], [1.0, 0, 0, 1, 1, 0]))
 
 
+def test_signatures_of_component_lists():
+    """MWPotential2014's exact list gets the compile-time kernels; lists
+    without an ellipsoidal component the lighter run-time list; any list with
+    one the full run-time list."""
+    sig = _lib.lib().galpy_cuda_signature
+
+    def s(types):
+        t = np.ascontiguousarray(types, np.int32)
+        return sig(len(t), t.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+
+    assert s([15, 5, 9]) == 1
+    assert s([15, 9, 5]) == 2 and s([13]) == 2 and s([5, 19, 29]) == 2
+    for ell in (21, 22, 23, 30, 37, 38, 43):
+        assert s([ell]) == 0 and s([15, 5, ell]) == 0
+
+
 def _no_gpu():
     return _lib.lib().galpy_cuda_device_count() == 0
 
