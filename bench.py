@@ -6,7 +6,7 @@ MWPotential2014, DOP853 with rtol = atol = 1e-10, float64 state.  Initial
 conditions from a seeded generator: R log-uniform in [0.05, 3], vR ~ N(0,
 0.1), vT ~ 1 + N(0, 0.1), z ~ N(0, 0.05), vz ~ N(0, 0.05), phi ~ U(0, 2 pi);
 every orbit has its own end time t_end ~ LogNormal(ln 50, 0.7) and keeps 101
-snapshots (SoA float64 on the device).  One "step" is one integration of the
+snapshots (float64 on the device, one orbit's rows contiguous).  One "step" is one integration of the
 whole batch; an orbit-step is one accepted DOP853 step of one orbit.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl galpy_b200|reference]
@@ -41,7 +41,7 @@ F_STEP_DOP853 = 6500.0  # nominal float64 flops per accepted DOP853 step (MWPote
 METRIC = "orbit-steps/s (MWPotential2014, dop853 rtol=atol=1e-10, ragged t_end, 1 B200)"
 WORKLOAD = ("batching: 1,048,576 orbits/GPU in MWPotential2014, dop853 rtol=atol=1e-10, "
             "R log-uniform [0.05,3], t_end ~ LogNormal(ln 50, 0.7) per orbit, 101 snapshots "
-            "SoA float64")
+            "float64")
 
 
 def workload(n, seed):
@@ -350,9 +350,12 @@ def main():
     ap.add_argument("--variant", type=int, default=None,
                     help="pin the register variant of the headline kernel (0 compiler "
                          "budget, 1 capped) instead of the autotuner's choice")
-    ap.add_argument("--out-layout", default="soa_rect", choices=["soa_rect", "aos_rect"],
-                    help="snapshot layout of the headline and --profile runs: [6][nt][N] "
-                         "(soa_rect) or [N][nt][6] (aos_rect, galpy's row order)")
+    ap.add_argument("--out-layout", default="aos_rect", choices=["soa_rect", "aos_rect"],
+                    help="snapshot layout of the headline and --profile runs: [N][nt][6] "
+                         "(aos_rect, galpy's row order: one orbit's rows are contiguous, so "
+                         "its partial 32-byte sectors merge in L2; the default) or "
+                         "[6][nt][N] (soa_rect: four orbits share each sector, written at "
+                         "different times, 4.7x the DRAM traffic)")
     ap.add_argument("--case", default="batching",
                     choices=["batching", "uniform", "longest", "bulk"],
                     help="uniform: R ~ U(0.5, 2), shared t in [0, 50] (101 snapshots) "
@@ -517,10 +520,14 @@ def main():
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                      # DRAM read + write of a 65,536-orbit capture of this kernel
-                     # (2.239 GB), scaled by orbits x snapshots to this launch
-                     "traffic": 2.238743e9 * n / 65536,
-                     "traffic_source": "ncu capture of 65,536 orbits (uniform case), scaled "
-                                       "by orbits x snapshots",
+                     # with 101 snapshots per orbit (AoS rows: 0.821 GB; SoA rows:
+                     # 3.833 GB), scaled by orbits x snapshots to this launch
+                     "traffic": (0.820831e9 if aos else 3.833354e9) * n / 65536,
+                     "traffic_algorithmic": n * NT * 6 * 8 + t.size * 8 + n * 6 * 8,
+                     "traffic_source": "ncu capture of 65,536 orbits (uniform case, "
+                                       f"{args.out_layout} snapshots), scaled by orbits x "
+                                       "snapshots",
+                     "out_layout": args.out_layout,
                      "kernel": "orbit_kernel<Dop853Machine<3,false>,3,0,false>",
                      "flops_per_unit": F_STEP_DOP853,
                      "peak_source": "measured in-process: float64 FMA-chain kernel "

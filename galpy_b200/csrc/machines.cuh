@@ -122,11 +122,22 @@ GPC_HD GPC_FI void write_row(const OutSpec& o, long long i, int j, const double*
       for (int k = 0; k < NV; k++) w[k] = v[k];
     }
   } else if (cyl) {
-    // rect_to_cyl_galpy / rect_to_polar_galpy (bovy_coords.c:79-148)
+    // rect_to_cyl_galpy / rect_to_polar_galpy (bovy_coords.c:79-148), with
+    // (cos phi, sin phi) = (x, y) / R instead of two more special functions
+    // (the same values to an ulp or two; atan2's own convention at R = 0)
     const double x = v[0], y = v[1];
     const double vx = v[D], vy = v[D + 1];
-    const double phi = atan2(y, x), cp = cos(phi), sp = sin(phi);
-    w[0] = sqrt(x * x + y * y);
+    const double phi = atan2(y, x), R = sqrt(x * x + y * y);
+    double cp, sp;
+    if (R > 0.0) {
+      const double iR = 1.0 / R;
+      cp = x * iR;
+      sp = y * iR;
+    } else {
+      cp = cos(phi);
+      sp = sin(phi);
+    }
+    w[0] = R;
     w[1] = vx * cp + vy * sp;
     w[2] = -vx * sp + vy * cp;
     if (D == 3) {
