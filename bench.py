@@ -350,6 +350,9 @@ def main():
     ap.add_argument("--variant", type=int, default=None,
                     help="pin the register variant of the headline kernel (0 compiler "
                          "budget, 1 capped) instead of the autotuner's choice")
+    ap.add_argument("--block", type=int, default=None,
+                    help="pin the headline kernel's orbits per block (DOP853: 128 or 96) "
+                         "instead of the autotuner's choice")
     ap.add_argument("--out-layout", default="aos_rect", choices=["soa_rect", "aos_rect"],
                     help="snapshot layout of the headline and --profile runs: [N][nt][6] "
                          "(aos_rect, galpy's row order: one orbit's rows are contiguous, so "
@@ -457,6 +460,8 @@ def main():
                           out_layout=args.out_layout)
     if args.variant is not None:
         tuned = dict(tuned, variant=args.variant, pinned_variant=True)
+    if args.block is not None:
+        tuned = dict(tuned, block_size=args.block, pinned_block=True)
     graph = IntegrationGraph(comps_d, ncomp, w0, t_d, out, err, "dop853_cuda", nsteps=nsteps,
                              rtol=RTOL, atol=ATOL, precision="fp64", signature=sig,
                              comps_host=comps, out_layout=args.out_layout,
@@ -761,15 +766,17 @@ def profile_leg(gb, torch, dev, spec, n, out_layout="soa_rect"):
                    with 101 snapshots, rtol = atol = 1e-10: the batching
                    workload's kernel on orbits of similar length
 
-    A third field selects the register variant (METHOD:KIND:VARIANT).
-    out_layout: the snapshot layout ('soa_rect' or 'aos_rect')."""
+    A third field selects the register variant and a fourth the orbits per
+    block (METHOD:KIND:VARIANT[:BLOCK]).  out_layout: the snapshot layout
+    ('soa_rect' or 'aos_rect')."""
     method, _, rest = spec.partition(":")
     kind, _, variant = rest.partition(":")
+    variant, _, block = variant.partition(":")
     kind = kind or "plain"
     stream = torch.cuda.current_stream(dev)
     pt, pa = mw14_args()
     ics, _ = precision_workload(n, seed=1 if kind == "uniform" else 5)
-    kw = {"variant": int(variant or 0)}
+    kw = {"variant": int(variant or 0), "block_size": int(block or 0)}
     group = None
     if kind == "groups":
         pt, args, _, _, _ = ragged_workload(ngroup=512)

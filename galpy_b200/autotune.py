@@ -6,9 +6,11 @@ launch shape, and the best choice differs between integrators, dimensions,
 precisions and potentials (register pressure, shared-memory slot stores,
 how ragged the step counts are):
 
-* ``block_size`` -- orbits per block (the fixed-step integrators; DOP853 runs
-  128 orbits per block because its shared-memory slot store is strided by
-  the block size);
+* ``block_size`` -- orbits per block (64 or 128 for the fixed-step
+  integrators; DOP853 runs 128: at its ~214 registers each SM sub-partition
+  holds two warps whatever the block, and blocks of 96 -- which a sample of
+  the batching workload preferred -- left 6 warps per SM and made the full
+  batch 22 % slower);
 * ``variant`` -- register budget: 0 = compiler default (up to 255 registers
   a thread), 1 = capped so that more blocks are resident per SM;
 * ``schedule`` -- not tuned: always longest first by the estimated cost
@@ -70,11 +72,13 @@ def candidates(int_method):
     """Launch shapes to try for an integrator."""
     code = parse_integrator(int_method)
     shapes = []
-    blocks = (128,) if code == 6 else (64, 128)
-    for block in blocks:
-        for variant in (0, 1):
-            shapes.append({"block_size": block, "variant": variant,
-                           "schedule": "longest_first", "threads_per_orbit": 1})
+    if code == 6:
+        pairs = ((128, 0), (128, 1))
+    else:
+        pairs = tuple((b, v) for b in (64, 128) for v in (0, 1))
+    for block, variant in pairs:
+        shapes.append({"block_size": block, "variant": variant,
+                       "schedule": "longest_first", "threads_per_orbit": 1})
     return shapes
 
 

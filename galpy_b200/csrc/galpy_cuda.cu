@@ -281,18 +281,23 @@ static int launch_persistent(const galpy_cuda_launch* L, const KernelInfo& ki, K
   GPC_CUDA_TRY(cudaGetDevice(&dev));
   int nsm = 0;
   GPC_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  // machines with a slot store run with kSlotStride threads per block
-  const int block = ki.slot_doubles > 0 ? kSlotStride : (L->block_size > 0 ? L->block_size : 128);
+  const int block = L->block_size > 0 ? L->block_size : 128;
   if (block > 128 || block % 32) return set_error(GALPY_CUDA_ERR_ARG, "block_size must be 32..128, multiple of 32");
-  const size_t smem = (size_t)ki.slot_doubles * sizeof(double) * block;
+  // machines with a slot store keep it strided by kSlotStride threads
+  // whatever the block size (smaller blocks leave part of it unused)
+  const size_t smem = (size_t)ki.slot_doubles * sizeof(double) * kSlotStride;
   if (smem > 48 * 1024)
     GPC_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   // slot-store machines: all of the unified L1/shared array as shared memory
-  // for the register-capped variant, so that 3 blocks' slot stores (3 x 66 KB
-  // for 3D DOP853) fit per SM; the hot potential tables are a few KB
-  if (smem > 0 && L->variant == 1)
-    GPC_CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                      (int)cudaSharedmemCarveoutMaxShared));
+  // for the register-capped variant and for blocks below 128, so that 3
+  // blocks' slot stores (3 x 66 KB for 3D DOP853) fit per SM; the hot
+  // potential tables are a few KB
+  // (the attribute belongs to the kernel, so it is set on every launch)
+  if (smem > 0)
+    GPC_CUDA_TRY(cudaFuncSetAttribute(
+        fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+        (int)(L->variant == 1 || block < kSlotStride ? cudaSharedmemCarveoutMaxShared
+                                                     : cudaSharedmemCarveoutDefault)));
   int per_sm = 0;
   GPC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem));
   if (per_sm < 1) per_sm = 1;

@@ -1302,10 +1302,15 @@ struct Dop853Machine : OrbitCommon {
     want_enqueue = false;
   }
   GPC_HD GPC_FI double& K(int s, int i) const { return ks[((s - 1) * N + i) * kSlotStride]; }
-  double h, hnew, hmax, pos_neg, facold, rtol, atol;
-  double t_current, t_old, t_old_older, dnf;
+  double h, hnew, rtol, atol;
+  double t_current, t_old;
   int stage;
   bool reject;
+  // The span t_end - t_0 and its sign, from the orbit's times when needed
+  // (once per attempt) instead of two more doubles held in registers across
+  // every force evaluation.
+  GPC_HD GPC_FI double hmax() const { return t[nt - 1] - t[0]; }
+  GPC_HD GPC_FI double pos_neg() const { return csign(1.0, hmax()); }
 
   // Lanes of a warp run the stages of their (different) orbits in lock step:
   // an attempt occupies slots 0..10 (stages 2..12), slot 11 (the FSAL
@@ -1327,7 +1332,7 @@ struct Dop853Machine : OrbitCommon {
 
   GPC_HD GPC_FI void begin_attempt()
   {
-    h = pos_neg * dmax(fabs(h), 1e3 * 2.3e-16);
+    h = pos_neg() * dmax(fabs(h), 1e3 * 2.3e-16);
     stage = 2;
   }
 
@@ -1345,7 +1350,6 @@ struct Dop853Machine : OrbitCommon {
     max_attempts = max_att;
     rtol = exp(rtol_);
     atol = exp(atol_);
-    facold = 1.0e-4;
 #pragma unroll
     for (int k = 0; k < N; k++) y0[k] = w[k];
     out(0, y0);
@@ -1353,10 +1357,8 @@ struct Dop853Machine : OrbitCommon {
       done = true;
       return;
     }
-    hmax = tt[nt - 1] - tt[0];
-    pos_neg = csign(1.0, hmax);
     reject = false;
-    t_current = t_old = t_old_older = tt[0];
+    t_current = t_old = tt[0];
     stage = ST_INIT1;
   }
 
@@ -1400,7 +1402,8 @@ struct Dop853Machine : OrbitCommon {
 
   GPC_HD GPC_FI bool output_pending() const
   {
-    return iout < nt - 1 && pos_neg * t[iout + 1] < pos_neg * t_current;
+    const double pn = pos_neg();
+    return iout < nt - 1 && pn * t[iout + 1] < pn * t_current;
   }
 
   template <class W>
@@ -1411,8 +1414,7 @@ struct Dop853Machine : OrbitCommon {
     double d[N];
     SYS::deriv(y, a, d);
     if (stage == ST_INIT1) {  // leung_dop853.c:296-308
-      double dny = 0.0;
-      dnf = 0.0;
+      double dny = 0.0, dnf = 0.0;
 #pragma unroll
       for (int i = 0; i < N; i++) {
         k1[i] = d[i];
@@ -1422,7 +1424,8 @@ struct Dop853Machine : OrbitCommon {
         sqr = y0[i] / sk;
         dny += sqr * sqr;
       }
-      h = csign(dmin(sqrt(dny / dnf) * 0.01, fabs(hmax)), pos_neg);
+      h = csign(dmin(sqrt(dny / dnf) * 0.01, fabs(hmax())), pos_neg());
+      hnew = dnf;  // kept for the second start-up evaluation (hnew is free until the first step)
       stage = ST_INIT2;
       return;
     }
@@ -1435,9 +1438,9 @@ struct Dop853Machine : OrbitCommon {
         der2 += sqr * sqr;
       }
       der2 = sqrt(der2) / h;
-      const double der12 = dmax(fabs(der2), sqrt(dnf));
+      const double der12 = dmax(fabs(der2), sqrt(hnew));  // hnew: dnf of the first evaluation
       const double h1 = pow(0.01 / der12, 1.0 / 8.0);
-      h = csign(dmin(100.0 * fabs(h), dmin(fabs(h1), fabs(hmax))), pos_neg);
+      h = csign(dmin(100.0 * fabs(h), dmin(fabs(h1), fabs(hmax()))), pos_neg());
       begin_attempt();
       return;
     }
@@ -1635,9 +1638,6 @@ struct Dop853Machine : OrbitCommon {
   {
     using namespace dp;
     attempts++;
-    t_old_older = t_old;
-    t_old = t_current;
-    t_current = t_current + h;
     double e = 0.0, e2 = 0.0;
 #pragma unroll
     for (int i = 0; i < N; i++) {
@@ -1666,11 +1666,16 @@ struct Dop853Machine : OrbitCommon {
       return;
     }
     const double fac11 = pow(e, 1.0 / 8.0);
-    double fac = fac11;  // Lund stabilisation with beta = 0: / pow(facold, 0) == / 1
+    // Lund stabilisation with beta = 0 divides by pow(facold, 0) == 1, so the
+    // reference's facold (max(e, 1e-4) of the last accepted step) drops out
+    double fac = fac11;
     fac = dmax(1.0 / 6.0, dmin(1.0 / 0.333, fac / 0.9));
     hnew = h / fac;
     if (e <= 1.0) {
-      facold = dmax(e, 1.0e-4);
+      // accepted: the step runs from t_old to t_current (the reference
+      // advances both before the test and restores them on rejection)
+      t_old = t_current;
+      t_current = t_current + h;
       stage = ST_FSAL;
     } else {
       // an attempt rejected at the smallest step (begin_attempt's floor)
@@ -1683,8 +1688,6 @@ struct Dop853Machine : OrbitCommon {
       }
       hnew = h / dmin(1.0 / 0.333, fac11 / 0.9);
       reject = true;
-      t_current = t_old;
-      t_old = t_old_older;
       h = hnew;
       if (max_attempts > 0 && attempts >= max_attempts) {
         err = E_BUDGET;
@@ -1703,8 +1706,9 @@ struct Dop853Machine : OrbitCommon {
       k1[i] = K(K4, i);
       y0[i] = K(K5, i);
     }
-    hnew = (fabs(hnew) > fabs(hmax)) ? pos_neg * hmax : hnew;
-    if (reject) hnew = pos_neg * dmin(fabs(hnew), fabs(h));
+    const double hm = hmax(), pn = csign(1.0, hm);
+    hnew = (fabs(hnew) > fabs(hm)) ? pn * hm : hnew;
+    if (reject) hnew = pn * dmin(fabs(hnew), fabs(h));
     reject = false;
     h = hnew;
     if (iout == nt - 1) {

@@ -125,9 +125,8 @@ def test_autotune_candidates_and_keys():
     from galpy_b200 import autotune
 
     dop = autotune.candidates("dop853_cuda")
-    assert all(c["block_size"] == 128 and c["threads_per_orbit"] == 1 for c in dop)
-    assert {(c["variant"], c["schedule"]) for c in dop} == {(0, "longest_first"),
-                                                             (1, "longest_first")}
+    assert all(c["threads_per_orbit"] == 1 and c["schedule"] == "longest_first" for c in dop)
+    assert {(c["block_size"], c["variant"]) for c in dop} == {(128, 0), (128, 1)}
     assert {c["block_size"] for c in autotune.candidates("symplec4_cuda")} == {64, 128}
     k1 = autotune.workload_key("B200", "dop853_cuda", False, "fp64", 1, False, 1 << 20, True)
     k2 = autotune.workload_key("B200", "dop853_cuda", False, "fp64", 1, False, (1 << 20) + 5,
