@@ -1302,15 +1302,10 @@ struct Dop853Machine : OrbitCommon {
     want_enqueue = false;
   }
   GPC_HD GPC_FI double& K(int s, int i) const { return ks[((s - 1) * N + i) * kSlotStride]; }
-  double h, hnew, rtol, atol;
+  double h, hnew, hmax, pos_neg, rtol, atol;
   double t_current, t_old;
   int stage;
   bool reject;
-  // The span t_end - t_0 and its sign, from the orbit's times when needed
-  // (once per attempt) instead of two more doubles held in registers across
-  // every force evaluation.
-  GPC_HD GPC_FI double hmax() const { return t[nt - 1] - t[0]; }
-  GPC_HD GPC_FI double pos_neg() const { return csign(1.0, hmax()); }
 
   // Lanes of a warp run the stages of their (different) orbits in lock step:
   // an attempt occupies slots 0..10 (stages 2..12), slot 11 (the FSAL
@@ -1332,7 +1327,7 @@ struct Dop853Machine : OrbitCommon {
 
   GPC_HD GPC_FI void begin_attempt()
   {
-    h = pos_neg() * dmax(fabs(h), 1e3 * 2.3e-16);
+    h = pos_neg * dmax(fabs(h), 1e3 * 2.3e-16);
     stage = 2;
   }
 
@@ -1357,6 +1352,8 @@ struct Dop853Machine : OrbitCommon {
       done = true;
       return;
     }
+    hmax = tt[nt - 1] - tt[0];
+    pos_neg = csign(1.0, hmax);
     reject = false;
     t_current = t_old = tt[0];
     stage = ST_INIT1;
@@ -1402,8 +1399,7 @@ struct Dop853Machine : OrbitCommon {
 
   GPC_HD GPC_FI bool output_pending() const
   {
-    const double pn = pos_neg();
-    return iout < nt - 1 && pn * t[iout + 1] < pn * t_current;
+    return iout < nt - 1 && pos_neg * t[iout + 1] < pos_neg * t_current;
   }
 
   template <class W>
@@ -1424,7 +1420,7 @@ struct Dop853Machine : OrbitCommon {
         sqr = y0[i] / sk;
         dny += sqr * sqr;
       }
-      h = csign(dmin(sqrt(dny / dnf) * 0.01, fabs(hmax())), pos_neg());
+      h = csign(dmin(sqrt(dny / dnf) * 0.01, fabs(hmax)), pos_neg);
       hnew = dnf;  // kept for the second start-up evaluation (hnew is free until the first step)
       stage = ST_INIT2;
       return;
@@ -1440,7 +1436,7 @@ struct Dop853Machine : OrbitCommon {
       der2 = sqrt(der2) / h;
       const double der12 = dmax(fabs(der2), sqrt(hnew));  // hnew: dnf of the first evaluation
       const double h1 = pow(0.01 / der12, 1.0 / 8.0);
-      h = csign(dmin(100.0 * fabs(h), dmin(fabs(h1), fabs(hmax()))), pos_neg());
+      h = csign(dmin(100.0 * fabs(h), dmin(fabs(h1), fabs(hmax))), pos_neg);
       begin_attempt();
       return;
     }
@@ -1620,16 +1616,28 @@ struct Dop853Machine : OrbitCommon {
     for (int j = j0; j <= j1; j++) {
       const double sv = (tt[j] - told) / hq;
       double v[N];
+#pragma unroll
+      for (int k = 0; k < N; k++) v[k] = 0.0;
       // one component at a time: unrolled, the compiler would issue all
-      // 14 N loads of the record at once and hold them in registers
+      // 14 N loads of the record at once and hold them in registers.  The
+      // component index of this loop is a run-time value, so d and v are
+      // read and written through selects over compile-time indices: indexed
+      // by it they would live in local memory.
 #pragma unroll 1
-      for (int i = 0; i < N; i++)
-        v[i] = dense_value(sv, hq, q[(0 * N + i) * QS + p], q[((1 + K5) * N + i) * QS + p],
-                           q[(1 * N + i) * QS + p], q[((1 + K2) * N + i) * QS + p],
-                           q[((1 + K3) * N + i) * QS + p], q[((1 + K4) * N + i) * QS + p],
-                           q[((1 + K6) * N + i) * QS + p], q[((1 + K7) * N + i) * QS + p],
-                           q[((1 + K8) * N + i) * QS + p], q[((1 + K9) * N + i) * QS + p],
-                           q[((1 + K10) * N + i) * QS + p], K(S14, i), K(S15, i), d[i]);
+      for (int i = 0; i < N; i++) {
+        double di = d[0];
+#pragma unroll
+        for (int k = 1; k < N; k++) di = i == k ? d[k] : di;
+        const double vi =
+            dense_value(sv, hq, q[(0 * N + i) * QS + p], q[((1 + K5) * N + i) * QS + p],
+                        q[(1 * N + i) * QS + p], q[((1 + K2) * N + i) * QS + p],
+                        q[((1 + K3) * N + i) * QS + p], q[((1 + K4) * N + i) * QS + p],
+                        q[((1 + K6) * N + i) * QS + p], q[((1 + K7) * N + i) * QS + p],
+                        q[((1 + K8) * N + i) * QS + p], q[((1 + K9) * N + i) * QS + p],
+                        q[((1 + K10) * N + i) * QS + p], K(S14, i), K(S15, i), di);
+#pragma unroll
+        for (int k = 0; k < N; k++) v[k] = i == k ? vi : v[k];
+      }
       out(j, v);
     }
   }
@@ -1706,9 +1714,8 @@ struct Dop853Machine : OrbitCommon {
       k1[i] = K(K4, i);
       y0[i] = K(K5, i);
     }
-    const double hm = hmax(), pn = csign(1.0, hm);
-    hnew = (fabs(hnew) > fabs(hm)) ? pn * hm : hnew;
-    if (reject) hnew = pn * dmin(fabs(hnew), fabs(h));
+    hnew = (fabs(hnew) > fabs(hmax)) ? pos_neg * hmax : hnew;
+    if (reject) hnew = pos_neg * dmin(fabs(hnew), fabs(h));
     reject = false;
     h = hnew;
     if (iout == nt - 1) {
