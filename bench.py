@@ -525,9 +525,9 @@ def main():
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                      # DRAM read + write of a 65,536-orbit capture of this kernel
-                     # with 101 snapshots per orbit (AoS rows: 0.821 GB; SoA rows:
+                     # with 101 snapshots per orbit (AoS rows: 0.549 GB; SoA rows:
                      # 3.833 GB), scaled by orbits x snapshots to this launch
-                     "traffic": (0.820831e9 if aos else 3.833354e9) * n / 65536,
+                     "traffic": (0.549170e9 if aos else 3.833354e9) * n / 65536,
                      "traffic_algorithmic": n * NT * 6 * 8 + t.size * 8 + n * 6 * 8,
                      "traffic_source": "ncu capture of 65,536 orbits (uniform case, "
                                        f"{args.out_layout} snapshots), scaled by orbits x "
