@@ -199,6 +199,8 @@ SIGNATURES = {
     "galpy_cuda_split_orbits": (
         _ci, [_ci, ctypes.c_longlong, _dp, _ci, _ci, _dp, _ci, _ci, _ip, _dp, _ci, _ip, _ci,
               ctypes.POINTER(ctypes.c_longlong)]),
+    "galpy_cuda_orbit_interp_device": (
+        _ci, [_ci, ctypes.c_longlong, _ci, _vp, _ci, _vp, _ci, _vp, _ci, _vp, _vp]),
     "galpy_cuda_trim_memory": (_ci, [_ci]),
     "galpy_cuda_jacobi_device": (
         _ci, [_vp, _ci, _vp, _ci, _vp, ctypes.c_longlong, ctypes.c_longlong, ctypes.c_longlong,

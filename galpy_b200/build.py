@@ -11,7 +11,8 @@ import subprocess
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgalpy_cuda.so")
-SOURCES = ["galpy_cuda.cu", "orbit_kernels_more.cu", "orbit_kernels_prec.cu", "adjoint.cu"]
+SOURCES = ["galpy_cuda.cu", "orbit_kernels_more.cu", "orbit_kernels_prec.cu", "adjoint.cu",
+           "orbit_interp.cu"]
 HEADERS = ["gpc_common.cuh", "potentials.cuh", "machines.cuh", "dop853_tableau.cuh",
            "compile_potential.h", "adjoint.cuh", "orbit_kernel.cuh"]
 

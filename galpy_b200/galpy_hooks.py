@@ -24,6 +24,13 @@ dispatch (galpy/orbit/Orbits.py):
   ``integrateFullOrbit_sos_cuda`` and ``integratePlanarOrbit_sos_c`` /
   ``integratePlanarOrbit_sos`` -> ``integratePlanarOrbit_sos_cuda``.
 
+Beyond the dispatch they route ``Orbit.integrate_dxdv`` and ``Orbit.lyapunov``
+(every orbit's deviations in one batched launch), the potential sums of
+``Orbit.E`` / ``Orbit.Jacobi`` over many points, and ``Orbit._call_internal``
+(``Orbit.__call__``, ``o.R(t)``, ... between integration times: the spline
+interpolation on the GPU) -- each only where it applies, galpy's own code
+otherwise.
+
 The same routing can be written into galpy itself as a few-line patch of the
 dispatch in ``Orbits._integrate_impl``; these hooks do it at run time.
 """
@@ -328,6 +335,45 @@ def _route_potential_sum(orig, planar):
     return evaluate
 
 
+# Orbit.__call__ between integration times: at least this many (orbit,
+# time) pairs are interpolated on the GPU
+DEVICE_INTERP_MIN_POINTS = 4096
+
+
+def _wrap_call_internal(orig):
+    """Orbit._call_internal (Orbits.py:6460-6575), behind Orbit.__call__
+    and the coordinate methods (o.R(t), o.x(t), ...): at times that are not
+    the integration times of an Orbit integrated on one shared time grid,
+    galpy fits scipy splines to every orbit (_setupOrbitInterp, :6739) and
+    evaluates them in Python; here the same interpolants (not-a-knot cubics
+    of x, y and the other components per orbit) are built and evaluated on
+    the GPU (galpy_cuda_orbit_interp_device) for at least
+    DEVICE_INTERP_MIN_POINTS (orbit, time) pairs of a 4- or 6-D orbit.
+    Everything else -- the integration times themselves, per-orbit time
+    grids, times outside the integrated range (galpy raises), quantities,
+    small requests -- is galpy's own."""
+    def _call_internal(self, *args, **kwargs):
+        if len(args) != 1 or kwargs or not hasattr(self, "t") or np.ndim(self.t) != 1:
+            return orig(self, *args, **kwargs)
+        t = args[0]
+        if hasattr(t, "unit") or np.ndim(t) != 1 or self.phasedim() not in (4, 6) or \
+                self.__dict__.get("_integrate_t_asQuantity"):
+            return orig(self, *args, **kwargs)
+        tq = np.asarray(t, dtype=np.float64)
+        self_t = np.asarray(self.t, dtype=np.float64)
+        if (tq.size * self.size < DEVICE_INTERP_MIN_POINTS or np.isnan(self_t).any()
+                or (tq.size == self_t.size and np.all(tq == self_t))
+                or np.any(tq > self_t.max()) or np.any(tq < self_t.min())
+                or self_t.size < 2):
+            return orig(self, *args, **kwargs)
+        from .orbit_quantities import interpolate
+
+        out = interpolate(self.orbit, self_t, tq).transpose(2, 1, 0)  # [phasedim, nq, N]
+        return out[:, 0] if tq.size == 1 else out
+
+    return _call_internal
+
+
 def install():
     """Patch galpy (must be importable) so that Orbit.integrate accepts the
     ``*_cuda`` methods.  Idempotent."""
@@ -400,6 +446,9 @@ def install():
     O.evaluatePotentials = _route_potential_sum(_installed["evaluatePotentials"], False)
     O.evaluateplanarPotentials = _route_potential_sum(_installed["evaluateplanarPotentials"],
                                                       True)
+    # interpolation between integration times (Orbit.__call__ and friends)
+    _installed.update(_call_internal=Orbit._call_internal)
+    Orbit._call_internal = _wrap_call_internal(_installed["_call_internal"])
 
 
 def uninstall():
@@ -414,6 +463,7 @@ def uninstall():
     Orbit._check_array_evenlyspaced = staticmethod(_installed["_check_array_evenlyspaced"])
     Orbit.integrate_dxdv = _installed["integrate_dxdv"]
     Orbit.lyapunov = _installed["lyapunov"]
+    Orbit._call_internal = _installed["_call_internal"]
     for name in ("integrateFullOrbit_c", "integratePlanarOrbit_c", "integrateFullOrbit",
                  "integratePlanarOrbit", "integrateFullOrbit_sos_c", "integrateFullOrbit_sos",
                  "integratePlanarOrbit_sos_c", "integratePlanarOrbit_sos",

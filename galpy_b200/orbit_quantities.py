@@ -103,3 +103,53 @@ def energies(pot, rows, planar=False, omega=0.0):
     Jd = torch.empty(len(r), dtype=torch.float64, device=dev)
     jacobi_device(comps, ncomp, wd, Jd, omega=omega, planar=planar)
     return Jd.cpu().numpy().reshape(shape)
+
+
+def interpolate_device(rows, t, tq, out, stream=None):
+    """Orbits between their stored rows, on the device: rows float64 CUDA
+    tensor [N, nt, nv] in galpy's cylindrical layout (nv 6 or 4), t [nt] or
+    [N, nt] increasing, tq [nq] or [N, nq], out [N, nq, nv] (all contiguous
+    float64 CUDA tensors).  Per orbit and component (x = R cos phi and
+    y = R sin phi in place of R and phi) the interpolating cubic spline with
+    not-a-knot ends -- the spline galpy's Orbit.__call__ evaluates between
+    integration times (Orbits.py:6739) -- then back to (R, phi).  Queries
+    outside [t_0, t_end] extrapolate the end pieces."""
+    import torch
+
+    for name, x in (("rows", rows), ("t", t), ("tq", tq), ("out", out)):
+        if not (x.is_cuda and x.dtype == torch.float64 and x.is_contiguous()):
+            raise ValueError(f"{name} must be a contiguous float64 CUDA tensor")
+    n, nt, nv = rows.shape
+    nq = tq.shape[-1]
+    if t.shape[-1] != nt or out.shape != (n, nq, nv) or (t.dim() > 1 and t.shape[0] != n) or \
+            (tq.dim() > 1 and tq.shape[0] != n):
+        raise ValueError("inconsistent shapes")
+    s = stream if stream is not None else torch.cuda.current_stream(rows.device)
+    _lib.check(_lib.lib().galpy_cuda_orbit_interp_device(
+        nv, n, nt, t.data_ptr(), int(t.dim() > 1), rows.data_ptr(), nq, tq.data_ptr(),
+        int(tq.dim() > 1), out.data_ptr(), s.cuda_stream))
+
+
+def interpolate(rows, t, tq):
+    """interpolate_device for host arrays: rows [N, nt, nv] galpy-layout
+    cylindrical rows, t [nt] or [N, nt] (increasing or decreasing), tq [nq]
+    or [N, nq]; returns [N, nq, nv] (numpy)."""
+    import torch
+
+    rows = np.asarray(rows, dtype=np.float64)
+    t = np.asarray(t, dtype=np.float64)
+    tq = np.asarray(tq, dtype=np.float64)
+    if t.ndim == 1 and t.size > 1 and t[1] < t[0]:  # a backward integration
+        t, rows = t[::-1], rows[:, ::-1]
+    elif t.ndim == 2 and t.shape[1] > 1:
+        back = t[:, 1] < t[:, 0]
+        if back.any():
+            t, rows = t.copy(), rows.copy()
+            t[back], rows[back] = t[back, ::-1], rows[back, ::-1]
+    dev = _device()
+    n, _, nv = rows.shape
+    out = torch.empty((n, tq.shape[-1], nv), dtype=torch.float64, device=dev)
+    interpolate_device(torch.from_numpy(np.ascontiguousarray(rows)).to(dev),
+                       torch.from_numpy(np.ascontiguousarray(t)).to(dev),
+                       torch.from_numpy(np.ascontiguousarray(tq)).to(dev), out)
+    return out.cpu().numpy()

@@ -291,6 +291,23 @@ int galpy_cuda_jacobi_device(const void *comps, int ncomp, const int *group, int
                              long long orbit_stride, const double *omega, double *J,
                              void *stream);
 
+/* Orbits between their stored rows (galpy's Orbit.__call__ at times that are
+ * not integration times, galpy/orbit/Orbits.py:6460-6575, through the
+ * interpolants of _setupOrbitInterp, :6739-6830): per orbit and component --
+ * x = R cos(phi), y = R sin(phi) in place of R and phi -- the interpolating
+ * cubic spline through the rows with not-a-knot ends (FITPACK's s = 0, k = 3
+ * spline, which galpy's InterpolatedUnivariateSpline / RectBivariateSpline
+ * evaluate; degree nt - 1 below 4 rows), then R = sqrt(x^2 + y^2), phi =
+ * atan2(y, x).  nv 6 (R,vR,vT,z,vz,phi) or 4 (R,vR,vT,phi); rows [n][nt][nv]
+ * (galpy's result layout); t [nt] or [n][nt] (indiv_t), increasing; tq [nq]
+ * or [n][nq] (indiv_q); out [n][nq][nv].  Queries outside [t_0, t_end]
+ * extrapolate the end pieces (galpy refuses them before it interpolates).
+ * Device pointers, asynchronous on `stream`; scratch of n*nt*nv doubles
+ * (plus n*nt with per-orbit times) allocated stream-ordered on it. */
+int galpy_cuda_orbit_interp_device(int nv, long long n, int nt, const double *t, int indiv_t,
+                                   const double *rows, int nq, const double *tq, int indiv_q,
+                                   double *out, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Gradients of a loss on final states (reverse mode).  No counterpart in the
  * reference: galpy's gradient information is the variational integration

@@ -198,8 +198,18 @@ def host_engine(monkeypatch, harness, oracle):
         R, z, phi = np.broadcast_arrays(R, z, phi)
         return oracle.potential(R.ravel(), z.ravel(), phi.ravel(), pt, pa).reshape(R.shape)
 
+    def interp(rows, t, tq):
+        from oracle import spline
+
+        calls.append(("interp", np.shape(rows), np.size(tq)))
+        t = np.asarray(t)
+        if t.size > 1 and t[1] < t[0]:
+            t, rows = t[::-1], np.asarray(rows)[:, ::-1]
+        return spline.interpolate(rows, t, tq)
+
     monkeypatch.setattr(integrate, "integrate_dxdv_batch", batch)
     monkeypatch.setattr(orbit_quantities, "potential_values", potvals)
+    monkeypatch.setattr(orbit_quantities, "interpolate", interp)
     galpy_hooks.install()
     yield calls
     galpy_hooks.uninstall()
@@ -281,4 +291,53 @@ def test_energy_and_jacobi_route_potential_sums(host_engine):
     np.testing.assert_allclose(J, Jref, rtol=1e-13)
     host_engine.clear()
     o.E(ts[:2])  # 128 points: galpy's own sum
+    assert not host_engine
+
+
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("backward", [False, True])
+def test_orbit_call_between_times_routes_interpolation(host_engine, planar, backward):
+    """Orbit.__call__ (and o.R(t), o.phi(t), ...) at times between the
+    integration times of many orbits takes the interpolation from the engine
+    (here its oracle stand-in, pinned against scipy's FITPACK in
+    tests/test_oracle.py); the integration times themselves, times outside
+    the integrated range and small requests stay with galpy."""
+    from galpy.orbit import Orbit
+    from galpy.potential import MWPotential2014
+
+    from galpy_b200 import galpy_hooks
+
+    rng = np.random.default_rng(12)
+    n = 64
+    vxvv = np.stack([rng.uniform(0.5, 2, n), rng.normal(0, 0.1, n), 1 + rng.normal(0, 0.1, n),
+                     rng.normal(0, 0.05, n), rng.normal(0, 0.05, n),
+                     rng.uniform(0, 2 * np.pi, n)], 1)
+    if planar:
+        vxvv = vxvv[:, [0, 1, 2, 5]]
+    ts = np.linspace(0, 3, 61)
+    if backward:
+        ts = -ts
+    o = Orbit(vxvv)
+    pot = MWPotential2014 if not planar else [p.toPlanar() for p in MWPotential2014]
+    o.integrate(ts, pot, method="dop853")  # galpy's own integrator
+    tq = np.sort(rng.uniform(ts.min(), ts.max(), 80))  # 64 x 80 = 5,120 pairs
+    host_engine.clear()
+    got = o._call_internal(tq)
+    R, phi = o.R(tq), o.phi(tq)
+    assert [c[0] for c in host_engine] == ["interp"] * 3
+    galpy_hooks.uninstall()
+    ref = o._call_internal(tq)
+    Rref, phiref = o.R(tq), o.phi(tq)
+    galpy_hooks.install()
+    assert got.shape == ref.shape == ((4 if planar else 6), 80, n)
+    np.testing.assert_allclose(got[:-1], ref[:-1], rtol=1e-10, atol=1e-12)
+    dphi = np.mod(got[-1] - ref[-1] + np.pi, 2 * np.pi) - np.pi
+    assert np.abs(dphi).max() < 1e-10
+    np.testing.assert_allclose(R, Rref, rtol=1e-10)
+    assert np.abs(np.mod(phi - phiref + np.pi, 2 * np.pi) - np.pi).max() < 1e-10
+    host_engine.clear()
+    o._call_internal(ts)  # the integration times: galpy's fast path
+    o._call_internal(tq[:10])  # 640 pairs: galpy's own splines
+    with pytest.raises(ValueError):
+        o._call_internal(np.array([ts.max() + 1.0, 0.5]) * (-1 if backward else 1) * 10)
     assert not host_engine

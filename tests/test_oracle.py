@@ -268,3 +268,52 @@ def test_oracle_planar_surface_of_section(oracle, golden, surface):
             b, eb, _ = oracle.integrate_sos(yo, psi, ptn, pan, m, rtol=1e-9, atol=1e-9,
                                             planar=True, surface=surface, impl="ref")
             assert np.array_equal(a, b) and np.array_equal(ea, eb), (name, m)
+
+
+# --- orbit interpolation between stored rows (oracle/spline.py) ----------
+
+@pytest.mark.parametrize("m", [2, 3, 4, 5, 11, 101])
+def test_spline_oracle_vs_scipy_fitpack(m):
+    """The restated interpolant against scipy's FITPACK splines, which
+    galpy's Orbit.__call__ evaluates: InterpolatedUnivariateSpline with
+    k = min(3, m - 1) (per-orbit grids) and RectBivariateSpline(kx=3, ky=1,
+    s=0) at integer orbit indices (shared grids, m >= 4)."""
+    from scipy import interpolate as si
+
+    from oracle import spline
+
+    rng = np.random.default_rng(m)
+    t = np.sort(rng.uniform(0, 10, m)) if m > 4 else np.linspace(0, 3, m)
+    ys = np.stack([np.sin(1.3 * t + k) * (1 + 0.1 * k) for k in range(5)])
+    tq = np.concatenate([rng.uniform(t[0], t[-1], 40), t, [t[0], t[-1]]])
+    for y in ys:
+        ref = si.InterpolatedUnivariateSpline(t, y, k=min(3, m - 1))(tq)
+        got = spline.interp1(t, y, tq)
+        assert np.allclose(got, ref, rtol=1e-12, atol=1e-12 * np.abs(y).max()), m
+    if m >= 4:
+        rb = si.RectBivariateSpline(t, np.arange(5), ys.T, ky=1, s=0.0)
+        ref2 = rb(np.sort(tq), np.arange(5))
+        got2 = np.stack([spline.interp1(t, y, np.sort(tq)) for y in ys], 1)
+        assert np.allclose(got2, ref2, rtol=1e-11, atol=1e-12)
+
+
+def test_spline_oracle_unpacks_like_galpy():
+    """R and phi are interpolated as x = R cos phi and y = R sin phi and
+    unpacked with sqrt and atan2, as Orbit.__call__ does (phase wrapping of
+    phi between rows does not matter)."""
+    from scipy import interpolate as si
+
+    from oracle import spline
+
+    t = np.linspace(0, 5, 21)
+    R = 1 + 0.2 * np.sin(t)
+    phi = np.mod(1.7 * t, 2 * np.pi) - np.pi  # wraps
+    rows = np.stack([R, 0.1 * np.cos(t), R * 1.7, phi], 1)[None]
+    tq = np.linspace(0.05, 4.95, 33)
+    got = spline.interpolate(rows, t, tq)[0]
+    x = si.InterpolatedUnivariateSpline(t, R * np.cos(phi), k=3)(tq)
+    y = si.InterpolatedUnivariateSpline(t, R * np.sin(phi), k=3)(tq)
+    assert np.allclose(got[:, 0], np.sqrt(x * x + y * y), rtol=1e-12)
+    assert np.allclose(got[:, 3], np.arctan2(y, x), atol=1e-12)
+    assert np.allclose(got[:, 1], si.InterpolatedUnivariateSpline(t, rows[0, :, 1], k=3)(tq),
+                       atol=1e-13)
