@@ -122,6 +122,42 @@ __global__ void __launch_bounds__(256) cost_kernel(const KArgs A, float* key, in
   idx[i] = (int)i;
 }
 
+// Parameter-group launches: the cost estimate in 64 logarithmic buckets
+// (4 log2(1 + cost): each a factor 2^(1/4) wide) as the high bits of the key
+// and the orbit's group (complemented) as the low bits, so that the
+// descending sort still hands out the longest orbits first, while the orbits
+// of one bucket come group by group: the lanes of a warp then read the same
+// potential records (on the ragged workload, 512 groups: 1,235 ms per launch
+// with the plain cost order, 1,026 ms in index order, where groups are
+// contiguous).
+constexpr int kCostBuckets = 64;
+template <int D>
+__global__ void __launch_bounds__(256) cost_group_kernel(const KArgs A, unsigned* key, int* idx)
+{
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= A.nobj) return;
+  double q[3] = {0.0, 0.0, 0.0}, a[3] = {0.0, 0.0, 0.0};
+  const int nv = 2 * D;
+  for (int k = 0; k < D; k++)
+    q[k] = A.in_layout == GALPY_CUDA_IN_SOA ? A.w0[(long long)k * A.nobj + i]
+                                             : A.w0[i * (long long)(A.variational_nv ? A.variational_nv : nv) + k];
+  const int g = A.group[i];
+  const GpComp* comps = A.comps + (long long)g * A.ncomp;
+  eval_force<D, PREC_FP64, false, DynPot>(comps, A.ncomp, q, a);
+  double ax = 0.0, xx = 0.0;
+  for (int k = 0; k < D; k++) {
+    ax += a[k] * q[k];
+    xx += q[k] * q[k];
+  }
+  const double* tt = A.t + (A.indiv_t ? i * (long long)A.nt : 0LL);
+  const double cost = fabs(tt[A.nt - 1] - tt[0]) * sqrt(fabs(ax) / (xx > 0.0 ? xx : 1e-300));
+  int b = isfinite(cost) ? (int)(4.0 * log2(1.0 + cost)) : 0;
+  b = b < 0 ? 0 : (b > kCostBuckets - 1 ? kCostBuckets - 1 : b);
+  const unsigned gl = (unsigned)(g < 0 ? 0 : (g > 0xffffff ? 0xffffff : g));
+  key[i] = ((unsigned)b << 24) | (0xffffffu - gl);
+  idx[i] = (int)i;
+}
+
 // ----------------------------------------------------------------------------
 // launch plumbing
 // ----------------------------------------------------------------------------
@@ -352,6 +388,13 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
     size_t tmp_bytes = 0;
     cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, (float*)nullptr, (float*)nullptr,
                                               (int*)nullptr, (int*)nullptr, n, 0, 32, stream);
+    if (A.group) {  // parameter groups sort 32-bit unsigned keys (cost_group_kernel)
+      size_t ubytes = 0;
+      cub::DeviceRadixSort::SortPairsDescending(nullptr, ubytes, (unsigned*)nullptr,
+                                                (unsigned*)nullptr, (int*)nullptr, (int*)nullptr,
+                                                n, 0, 32, stream);
+      tmp_bytes = std::max(tmp_bytes, ubytes);
+    }
     const size_t keys = (size_t)n * sizeof(float), vals = (size_t)n * sizeof(int);
     const size_t off_k2 = keys, off_v1 = 2 * keys, off_v2 = 2 * keys + vals,
                  off_tmp = (2 * keys + 2 * vals + 255) & ~(size_t)255;
@@ -362,13 +405,26 @@ static int launch_kernel(const galpy_cuda_launch* L, Scratch* scratch, bool prog
     int* v1 = reinterpret_cast<int*>(base + off_v1);
     int* v2 = reinterpret_cast<int*>(base + off_v2);
     const unsigned cb = (unsigned)((L->nobj + 255) / 256);
-    if (L->planar)
-      cost_kernel<2><<<cb, 256, 0, stream>>>(A, k1, v1);
-    else
-      cost_kernel<3><<<cb, 256, 0, stream>>>(A, k1, v1);
-    GPC_CUDA_TRY(cudaGetLastError());
-    cudaError_t se = cub::DeviceRadixSort::SortPairsDescending(base + off_tmp, tmp_bytes, k1, k2,
-                                                               v1, v2, n, 0, 32, stream);
+    cudaError_t se;
+    if (A.group) {  // bucketed cost, then group (cost_group_kernel)
+      unsigned* u1 = reinterpret_cast<unsigned*>(k1);
+      unsigned* u2 = reinterpret_cast<unsigned*>(k2);
+      if (L->planar)
+        cost_group_kernel<2><<<cb, 256, 0, stream>>>(A, u1, v1);
+      else
+        cost_group_kernel<3><<<cb, 256, 0, stream>>>(A, u1, v1);
+      GPC_CUDA_TRY(cudaGetLastError());
+      se = cub::DeviceRadixSort::SortPairsDescending(base + off_tmp, tmp_bytes, u1, u2, v1, v2, n,
+                                                     0, 32, stream);
+    } else {
+      if (L->planar)
+        cost_kernel<2><<<cb, 256, 0, stream>>>(A, k1, v1);
+      else
+        cost_kernel<3><<<cb, 256, 0, stream>>>(A, k1, v1);
+      GPC_CUDA_TRY(cudaGetLastError());
+      se = cub::DeviceRadixSort::SortPairsDescending(base + off_tmp, tmp_bytes, k1, k2, v1, v2, n,
+                                                     0, 32, stream);
+    }
     if (se != cudaSuccess) {
       cudaFreeAsync(sched, stream);
       return set_error(GALPY_CUDA_ERR_CUDA, std::string("radix sort: ") + cudaGetErrorString(se));
