@@ -336,6 +336,8 @@ def main():
     ap.add_argument("--mixed-orbits", type=int, default=1 << 22)
     ap.add_argument("--no-ragged", action="store_true")
     ap.add_argument("--no-grad", action="store_true")
+    ap.add_argument("--no-interp", action="store_true",
+                    help="skip the orbit-interpolation leg (Orbit.__call__ between times)")
     ap.add_argument("--grad-only", action="store_true",
                     help="run only the differentiation leg (with --grad-orbits orbits)")
     ap.add_argument("--grad-orbits", type=int, default=65536)
@@ -575,6 +577,11 @@ def main():
         result["e2e"] = e2e(gb, ics, t, pt, pa, args.steps, pg, dev, steps)
         result["gpu_launches"] += args.steps
 
+    if not args.no_interp:
+        result["interp"] = interp_leg(gb, torch, dev, stream, pg,
+                                      cpu=rank == 0 and not args.no_cpu_baseline)
+        result["gpu_launches"] += result["interp"]["gpu_launches"]
+
     if rank == 0 and not args.no_cpu_baseline:
         try:
             result["cpu_baseline"] = cpu_reference_rate(ics, t, pt, pa)
@@ -589,6 +596,82 @@ def main():
 
 F_STEP_DOP853_PLANAR = 6200.0  # 15 planar force evaluations (280) + 2000 stage flops
 F_GRAD_STEP = 3 * F_STEP_DOP853_PLANAR  # forward + backward (2 x forward: Hessian-vector products)
+
+
+def interp_leg(gb, torch, dev, stream, pg, n=1 << 20, nt=NT, nq=NT - 1, K=3, W=3, cpu=False):
+    """Orbits between their stored rows (galpy's Orbit.__call__ at times
+    between the integration times): n orbits with nt galpy-layout rows on a
+    shared grid t in [0, 50], evaluated at the nq midpoints of the grid, on
+    the device (galpy_cuda_orbit_interp_device: not-a-knot cubic splines of
+    x, y and the other components per orbit).  HBM bound: the algorithmic
+    bytes are the rows read once and the outputs written once.  cpu: galpy's
+    own route (scipy's RectBivariateSpline per component over (t, orbit
+    index), then evaluation) on a sample, one host thread."""
+    from galpy_b200.orbit_quantities import interpolate_device
+
+    rng = np.random.default_rng(7)
+    t = np.linspace(0.0, 50.0, nt)
+    tq = 0.5 * (t[1:] + t[:-1])[:nq]
+    # smooth synthetic rows of the batching workload's shape (the cost does
+    # not depend on the values)
+    f = rng.uniform(0.2, 2.0, (n, 1))
+    ph = rng.uniform(0, 2 * np.pi, (n, 1))
+    rows_h = np.empty((n, nt, 6))
+    rows_h[..., 0] = 1.0 + 0.3 * np.sin(f * t[None, :] + ph)
+    rows_h[..., 1] = 0.3 * f * np.cos(f * t[None, :] + ph)
+    rows_h[..., 2] = 1.0 + 0.1 * np.cos(f * t[None, :])
+    rows_h[..., 3] = 0.05 * np.sin(2 * f * t[None, :] + ph)
+    rows_h[..., 4] = 0.1 * f * np.cos(2 * f * t[None, :] + ph)
+    rows_h[..., 5] = np.mod(f * t[None, :] + ph, 2 * np.pi) - np.pi
+    rows = torch.from_numpy(rows_h).to(dev)
+    t_d = torch.from_numpy(t).to(dev)
+    tq_d = torch.from_numpy(tq).to(dev)
+    out = torch.empty((n, nq, 6), dtype=torch.float64, device=dev)
+    for _ in range(W):
+        interpolate_device(rows, t_d, tq_d, out, stream=stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(K):
+        interpolate_device(rows, t_d, tq_d, out, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / K
+    (ms,), _ = over_ranks([ms], [], pg, dev)
+    algo_bytes = n * (nt + nq) * 6 * 8
+    res = {"workload": f"interpolation: {n} orbits x {nt} rows (6 components, shared t in "
+                       f"[0, 50]) at the {nq} midpoints",
+           "value": n * nq / (ms * 1e-3), "unit": "interpolated rows/s", "ms": ms,
+           "algorithmic_bytes": algo_bytes,
+           "achieved_GBs": algo_bytes / (ms * 1e-3) / 1e9,
+           "gpu_launches": 3 * K}
+    if cpu:
+        try:
+            from scipy import interpolate as si
+
+            m = 4096
+            sub = rows_h[:m]
+            c0 = time.perf_counter()
+            x = sub[..., 0] * np.cos(sub[..., 5])
+            y = sub[..., 0] * np.sin(sub[..., 5])
+            comps = [x, sub[..., 1], sub[..., 2], sub[..., 3], sub[..., 4], y]
+            idx = np.arange(m)
+            vals = [si.RectBivariateSpline(t, idx, c.T, ky=1, s=0.0)(tq, idx) for c in comps]
+            el = time.perf_counter() - c0
+            ref = np.stack([np.sqrt(vals[0] ** 2 + vals[5] ** 2), vals[1], vals[2], vals[3],
+                            vals[4], np.arctan2(vals[5], vals[0])], -1).transpose(1, 0, 2)
+            got = out[:m].cpu().numpy()
+            d = np.abs(got - ref)
+            d[..., 5] = np.abs(np.mod(got[..., 5] - ref[..., 5] + np.pi, 2 * np.pi) - np.pi)
+            res["cpu_baseline"] = {"value": m * nq / el, "unit": "interpolated rows/s",
+                                   "cores": 1, "kind": "reference",
+                                   "sample": f"{m} orbits through galpy's route (scipy "
+                                             "RectBivariateSpline(kx=3, ky=1, s=0) per "
+                                             f"component), {el:.2f} s",
+                                   "max_abs_diff_vs_device": float(d.max())}
+        except ImportError:
+            res["cpu_baseline"] = {"unavailable": "scipy not importable"}
+    return res
 
 
 def differentiation_leg(gb, torch, dev, stream, pg, peak, n=65536, cpu=False):

@@ -25,15 +25,21 @@
 // parabola.  Queries outside [t_0, t_{m-1}] extrapolate the end pieces (as
 // FITPACK's splev does by default; galpy refuses them before interpolating).
 //
-// Three passes, all one thread per item:
-//   sweep_kernel     per orbit (one thread for shared times): the Thomas
-//                    factors c'_i, which depend on the times only
-//   moments_kernel   per (orbit, component): the right-hand side, forward
-//                    elimination and back substitution -> M_i
-//   eval_kernel      per (orbit, query): interval search, the cubic of each
-//                    component, conversion back to (R, phi), one output row
-// Moments are stored component-major [nv][nt][n] and the Thomas factors
-// [nt][n], so that consecutive threads (orbits) touch consecutive doubles.
+// Four passes:
+//   transpose_kernel  the rows [n][nt][nv] to component-major values
+//                     X[nv][nt][n] (x, y in place of R, phi), through a
+//                     shared-memory tile: each orbit's rows are read as one
+//                     contiguous run and the values written orbit-contiguous
+//   sweep_kernel      per orbit (one thread for shared times): the Thomas
+//                     factors c'_i, which depend on the times only
+//   moments_kernel    per (orbit, component): the right-hand side, forward
+//                     elimination and back substitution -> M_i
+//   eval_kernel       per (orbit, block of queries): interval search, the
+//                     cubic of each component, conversion back to (R, phi);
+//                     the thread writes its orbit's consecutive output rows
+// X, the moments M[nv][nt][n] and the Thomas factors [nt][n] are
+// orbit-contiguous, so that consecutive threads (orbits) touch consecutive
+// doubles.
 #include <cuda_runtime.h>
 #include <stddef.h>
 
@@ -50,15 +56,44 @@ __device__ __forceinline__ double tq_of(const double* t, int indiv, long long i,
   return t[(indiv ? i * (long long)nt : 0LL) + j];
 }
 
-// Component k of row j of orbit i as splined: x, y for R, phi (k = 0 and
-// k = nv - 1), the stored value otherwise.
-template <int NV>
-__device__ __forceinline__ double comp_value(const double* rows, long long i, int nt, int j, int k)
+// Value of component k at row j of orbit i in the component-major array X.
+__device__ __forceinline__ double xval(const double* X, long long n, int nt, int k, int j,
+                                       long long i)
 {
-  const double* r = rows + (i * nt + j) * NV;
-  if (k == 0) return r[0] * cos(r[NV - 1]);
-  if (k == NV - 1) return r[0] * sin(r[NV - 1]);
-  return r[k];
+  return X[((long long)k * nt + j) * n + i];
+}
+
+// Rows [n][nt][NV] (galpy cylindrical) -> X[NV][nt][n] with x = R cos(phi),
+// y = R sin(phi) in the places of R and phi.  Block: kTileO orbits x kTileJ
+// rows; the load walks each orbit's kTileJ * NV contiguous doubles, the
+// store walks orbits.
+constexpr int kTileO = 32, kTileJ = 8;
+template <int NV>
+__global__ void __launch_bounds__(256) transpose_kernel(long long n, int nt, const double* rows,
+                                                        double* X)
+{
+  constexpr int W = kTileJ * NV + 1;  // padded row of the tile (bank spread)
+  __shared__ double tile[kTileO * W];
+  const long long i0 = (long long)blockIdx.x * kTileO;
+  const int j0 = blockIdx.y * kTileJ;
+  const int jn = nt - j0 < kTileJ ? nt - j0 : kTileJ;
+  for (int e = threadIdx.x; e < kTileO * kTileJ * NV; e += blockDim.x) {
+    const int o = e / (kTileJ * NV), r = e - o * (kTileJ * NV);
+    if (i0 + o < n && r < jn * NV) tile[o * W + r] = rows[((i0 + o) * nt + j0) * NV + r];
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < kTileO * kTileJ * NV; e += blockDim.x) {
+    const int o = e % kTileO, rest = e / kTileO;
+    const int jj = rest % kTileJ, k = rest / kTileJ;
+    if (i0 + o >= n || jj >= jn) continue;
+    const double* v = tile + o * W + jj * NV;
+    double val = v[k];
+    if (k == 0)
+      val = v[0] * cos(v[NV - 1]);
+    else if (k == NV - 1)
+      val = v[0] * sin(v[NV - 1]);
+    X[((long long)k * nt + j0 + jj) * n + i0 + o] = val;
+  }
 }
 
 // Coefficients of row i (1 <= i <= m-2) of the reduced system
@@ -102,7 +137,7 @@ __global__ void sweep_kernel(long long n, int nt, const double* t, int indiv, do
 
 template <int NV>
 __global__ void moments_kernel(long long n, int nt, const double* t, int indiv,
-                               const double* rows, const double* cp, long long ncp, double* M)
+                               const double* X, const double* cp, long long ncp, double* M)
 {
   const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (g >= n * NV) return;
@@ -113,10 +148,10 @@ __global__ void moments_kernel(long long n, int nt, const double* t, int indiv,
   const int m = nt;
   double* Mk = M + (long long)k * nt * n;
   // forward elimination: d'_r stored in M_r
-  double ym = comp_value<NV>(rows, i, nt, 0, k), y0 = comp_value<NV>(rows, i, nt, 1, k);
+  double ym = xval(X, n, nt, k, 0, i), y0 = xval(X, n, nt, k, 1, i);
   double dprev = 0.0, cprev = 0.0;
   for (int r = 1; r <= m - 2; r++) {
-    const double yp = comp_value<NV>(rows, i, nt, r + 1, k);
+    const double yp = xval(X, n, nt, k, r + 1, i);
     const double h0 = tt[r] - tt[r - 1], h1 = tt[r + 1] - tt[r];
     const double rhs = 6.0 * ((yp - y0) / h1 - (y0 - ym) / h0);
     double a, b, c;
@@ -160,58 +195,65 @@ __device__ __forceinline__ int interval(const double* tt, int m, double tq)
   return lo;
 }
 
+// Queries per thread of eval_kernel: a thread writes kQueryBlock
+// consecutive output rows of its orbit, whose partial 32-byte sectors then
+// merge in L2.
+constexpr int kQueryBlock = 16;
 template <int NV>
-__global__ void eval_kernel(long long n, int nt, const double* t, int indiv, const double* rows,
-                            const double* M, int nq, const double* tq, int indiv_q, double* out)
+__global__ void __launch_bounds__(128) eval_kernel(long long n, int nt, const double* t, int indiv,
+                                                   const double* X, const double* M, int nq,
+                                                   const double* tq, int indiv_q, double* out)
 {
   const long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (g >= n * (long long)nq) return;
   const long long i = g % n;  // consecutive threads: consecutive orbits
-  const int q = (int)(g / n);
+  const long long qb = g / n;
+  const int q0 = (int)(qb * kQueryBlock);
+  if (q0 >= nq) return;
+  const int q1 = nq - q0 < kQueryBlock ? nq : q0 + kQueryBlock;
   const double* tt = t + (indiv ? i * (long long)nt : 0LL);
-  const double x = tq_of(tq, indiv_q, i, nq, q);
   const int m = nt;
-  double v[NV];
-  if (m == 1) {
+  for (int q = q0; q < q1; q++) {
+    const double x = tq_of(tq, indiv_q, i, nq, q);
+    double v[NV];
+    if (m == 1) {
 #pragma unroll
-    for (int k = 0; k < NV; k++) v[k] = comp_value<NV>(rows, i, nt, 0, k);
-  } else if (m == 2) {  // the line through both rows
-    const double s = (x - tt[0]) / (tt[1] - tt[0]);
+      for (int k = 0; k < NV; k++) v[k] = xval(X, n, nt, k, 0, i);
+    } else if (m == 2) {  // the line through both rows
+      const double s = (x - tt[0]) / (tt[1] - tt[0]);
 #pragma unroll
-    for (int k = 0; k < NV; k++) {
-      const double a = comp_value<NV>(rows, i, nt, 0, k), b = comp_value<NV>(rows, i, nt, 1, k);
-      v[k] = a + s * (b - a);
+      for (int k = 0; k < NV; k++) {
+        const double a = xval(X, n, nt, k, 0, i), b = xval(X, n, nt, k, 1, i);
+        v[k] = a + s * (b - a);
+      }
+    } else if (m == 3) {  // the parabola through the three rows (Newton form)
+      const double t0 = tt[0], t1 = tt[1], t2 = tt[2];
+#pragma unroll
+      for (int k = 0; k < NV; k++) {
+        const double y0 = xval(X, n, nt, k, 0, i), y1 = xval(X, n, nt, k, 1, i);
+        const double y2 = xval(X, n, nt, k, 2, i);
+        const double d01 = (y1 - y0) / (t1 - t0), d12 = (y2 - y1) / (t2 - t1);
+        const double d012 = (d12 - d01) / (t2 - t0);
+        v[k] = y0 + (x - t0) * (d01 + (x - t1) * d012);
+      }
+    } else {
+      const int j = interval(tt, m, x);
+      const double h = tt[j + 1] - tt[j], A = tt[j + 1] - x, B = x - tt[j];
+#pragma unroll
+      for (int k = 0; k < NV; k++) {
+        const double Mj = xval(M, n, nt, k, j, i), Mj1 = xval(M, n, nt, k, j + 1, i);
+        const double yj = xval(X, n, nt, k, j, i), yj1 = xval(X, n, nt, k, j + 1, i);
+        v[k] = (Mj * A * A * A + Mj1 * B * B * B) / (6.0 * h) + (yj / h - Mj * h / 6.0) * A +
+               (yj1 / h - Mj1 * h / 6.0) * B;
+      }
     }
-  } else if (m == 3) {  // the parabola through the three rows (Newton form)
-    const double t0 = tt[0], t1 = tt[1], t2 = tt[2];
+    // (x, y) -> (R, phi), galpy's unpacking of the interpolated x and y
+    const double px = v[0], py = v[NV - 1];
+    double* o = out + (i * nq + q) * NV;
+    o[0] = sqrt(px * px + py * py);
 #pragma unroll
-    for (int k = 0; k < NV; k++) {
-      const double y0 = comp_value<NV>(rows, i, nt, 0, k), y1 = comp_value<NV>(rows, i, nt, 1, k);
-      const double y2 = comp_value<NV>(rows, i, nt, 2, k);
-      const double d01 = (y1 - y0) / (t1 - t0), d12 = (y2 - y1) / (t2 - t1);
-      const double d012 = (d12 - d01) / (t2 - t0);
-      v[k] = y0 + (x - t0) * (d01 + (x - t1) * d012);
-    }
-  } else {
-    const int j = interval(tt, m, x);
-    const double h = tt[j + 1] - tt[j], A = tt[j + 1] - x, B = x - tt[j];
-#pragma unroll
-    for (int k = 0; k < NV; k++) {
-      const double* Mk = M + (long long)k * nt * n;
-      const double Mj = Mk[(long long)j * n + i], Mj1 = Mk[(long long)(j + 1) * n + i];
-      const double yj = comp_value<NV>(rows, i, nt, j, k);
-      const double yj1 = comp_value<NV>(rows, i, nt, j + 1, k);
-      v[k] = (Mj * A * A * A + Mj1 * B * B * B) / (6.0 * h) + (yj / h - Mj * h / 6.0) * A +
-             (yj1 / h - Mj1 * h / 6.0) * B;
-    }
+    for (int k = 1; k < NV - 1; k++) o[k] = v[k];
+    o[NV - 1] = atan2(py, px);
   }
-  // (x, y) -> (R, phi), galpy's unpacking of the interpolated x and y
-  const double px = v[0], py = v[NV - 1];
-  double* o = out + (i * nq + q) * NV;
-  o[0] = sqrt(px * px + py * py);
-#pragma unroll
-  for (int k = 1; k < NV - 1; k++) o[k] = v[k];
-  o[NV - 1] = atan2(py, px);
 }
 
 int fail(const char* what, cudaError_t e)
@@ -223,25 +265,32 @@ template <int NV>
 int run(long long n, int nt, const double* t, int indiv_t, const double* rows, int nq,
         const double* tq, int indiv_q, double* out, cudaStream_t s)
 {
+  double* X = nullptr;
   double* M = nullptr;
   double* cp = nullptr;
   cudaError_t e;
   const long long ncp = indiv_t ? n : 1;
+  const size_t vals = (size_t)NV * nt * n;
+  if ((e = cudaMallocAsync((void**)&X, vals * sizeof(double), s)) != cudaSuccess)
+    return fail("interpolation scratch: ", e);
+  const dim3 tgrid((unsigned)((n + kTileO - 1) / kTileO), (unsigned)((nt + kTileJ - 1) / kTileJ));
+  transpose_kernel<NV><<<tgrid, 256, 0, s>>>(n, nt, rows, X);
   if (nt >= 4) {
-    if ((e = cudaMallocAsync((void**)&M, (size_t)NV * nt * n * sizeof(double), s)) != cudaSuccess)
-      return fail("interpolation scratch: ", e);
-    if ((e = cudaMallocAsync((void**)&cp, (size_t)nt * ncp * sizeof(double), s)) != cudaSuccess) {
-      cudaFreeAsync(M, s);
+    if ((e = cudaMallocAsync((void**)&M, vals * sizeof(double), s)) != cudaSuccess ||
+        (e = cudaMallocAsync((void**)&cp, (size_t)nt * ncp * sizeof(double), s)) != cudaSuccess) {
+      if (M) cudaFreeAsync(M, s);
+      cudaFreeAsync(X, s);
       return fail("interpolation scratch: ", e);
     }
     sweep_kernel<<<(unsigned)((ncp + 127) / 128), 128, 0, s>>>(ncp, nt, t, indiv_t, cp);
-    moments_kernel<NV><<<(unsigned)((n * NV + 127) / 128), 128, 0, s>>>(n, nt, t, indiv_t, rows,
-                                                                         cp, ncp, M);
+    moments_kernel<NV><<<(unsigned)((n * NV + 127) / 128), 128, 0, s>>>(n, nt, t, indiv_t, X, cp,
+                                                                         ncp, M);
   }
-  const long long items = n * (long long)nq;
-  eval_kernel<NV><<<(unsigned)((items + 127) / 128), 128, 0, s>>>(n, nt, t, indiv_t, rows, M, nq,
-                                                                   tq, indiv_q, out);
+  const long long items = n * (long long)((nq + kQueryBlock - 1) / kQueryBlock);
+  eval_kernel<NV><<<(unsigned)((items + 127) / 128), 128, 0, s>>>(n, nt, t, indiv_t, X, M, nq, tq,
+                                                                   indiv_q, out);
   e = cudaGetLastError();
+  cudaFreeAsync(X, s);
   if (M) cudaFreeAsync(M, s);
   if (cp) cudaFreeAsync(cp, s);
   if (e != cudaSuccess) return fail("interpolation kernels: ", e);

@@ -302,8 +302,9 @@ int galpy_cuda_jacobi_device(const void *comps, int ncomp, const int *group, int
  * (galpy's result layout); t [nt] or [n][nt] (indiv_t), increasing; tq [nq]
  * or [n][nq] (indiv_q); out [n][nq][nv].  Queries outside [t_0, t_end]
  * extrapolate the end pieces (galpy refuses them before it interpolates).
- * Device pointers, asynchronous on `stream`; scratch of n*nt*nv doubles
- * (plus n*nt with per-orbit times) allocated stream-ordered on it. */
+ * Device pointers, asynchronous on `stream`; scratch of 2*n*nt*nv doubles
+ * (n*nt*nv below 4 rows; plus n*nt with per-orbit times) allocated
+ * stream-ordered on it. */
 int galpy_cuda_orbit_interp_device(int nv, long long n, int nt, const double *t, int indiv_t,
                                    const double *rows, int nq, const double *tq, int indiv_q,
                                    double *out, void *stream);
