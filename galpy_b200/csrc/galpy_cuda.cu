@@ -538,6 +538,13 @@ static int library_pool(cudaMemPool_t* out)
   return GALPY_CUDA_OK;
 }
 
+// The same pool for the library's other translation units (the orbit
+// interpolation's scratch).
+__attribute__((visibility("hidden"))) int gpc_library_pool(cudaMemPool_t* out)
+{
+  return library_pool(out);
+}
+
 static int select_device(const galpy_cuda_opts* o)
 {
   int n = 0;

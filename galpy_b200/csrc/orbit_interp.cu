@@ -48,6 +48,7 @@
 #include "../../include/galpy_cuda.h"
 
 int gpc_report_error(int code, const char* msg);  // galpy_cuda.cu
+int gpc_library_pool(cudaMemPool_t* out);         // galpy_cuda.cu
 
 namespace {
 
@@ -269,15 +270,22 @@ int run(long long n, int nt, const double* t, int indiv_t, const double* rows, i
   double* M = nullptr;
   double* cp = nullptr;
   cudaError_t e;
+  // scratch from the library's private pool, which keeps freed memory
+  // mapped for the next call (galpy_cuda_trim_memory returns it): with a
+  // release threshold of 0 every call would map its gigabytes again
+  cudaMemPool_t pool = nullptr;
+  const int prc = gpc_library_pool(&pool);
+  if (prc) return prc;
   const long long ncp = indiv_t ? n : 1;
   const size_t vals = (size_t)NV * nt * n;
-  if ((e = cudaMallocAsync((void**)&X, vals * sizeof(double), s)) != cudaSuccess)
+  if ((e = cudaMallocFromPoolAsync((void**)&X, vals * sizeof(double), pool, s)) != cudaSuccess)
     return fail("interpolation scratch: ", e);
   const dim3 tgrid((unsigned)((n + kTileO - 1) / kTileO), (unsigned)((nt + kTileJ - 1) / kTileJ));
   transpose_kernel<NV><<<tgrid, 256, 0, s>>>(n, nt, rows, X);
   if (nt >= 4) {
-    if ((e = cudaMallocAsync((void**)&M, vals * sizeof(double), s)) != cudaSuccess ||
-        (e = cudaMallocAsync((void**)&cp, (size_t)nt * ncp * sizeof(double), s)) != cudaSuccess) {
+    if ((e = cudaMallocFromPoolAsync((void**)&M, vals * sizeof(double), pool, s)) != cudaSuccess ||
+        (e = cudaMallocFromPoolAsync((void**)&cp, (size_t)nt * ncp * sizeof(double), pool, s)) !=
+            cudaSuccess) {
       if (M) cudaFreeAsync(M, s);
       cudaFreeAsync(X, s);
       return fail("interpolation scratch: ", e);

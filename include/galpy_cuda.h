@@ -304,7 +304,8 @@ int galpy_cuda_jacobi_device(const void *comps, int ncomp, const int *group, int
  * extrapolate the end pieces (galpy refuses them before it interpolates).
  * Device pointers, asynchronous on `stream`; scratch of 2*n*nt*nv doubles
  * (n*nt*nv below 4 rows; plus n*nt with per-orbit times) allocated
- * stream-ordered on it. */
+ * stream-ordered on it from the library's private memory pool (kept for the
+ * next call; galpy_cuda_trim_memory returns it). */
 int galpy_cuda_orbit_interp_device(int nv, long long n, int nt, const double *t, int indiv_t,
                                    const double *rows, int nq, const double *tq, int indiv_q,
                                    double *out, void *stream);
