@@ -338,6 +338,10 @@ def main():
     ap.add_argument("--no-grad", action="store_true")
     ap.add_argument("--no-interp", action="store_true",
                     help="skip the orbit-interpolation leg (Orbit.__call__ between times)")
+    ap.add_argument("--interp-only", action="store_true",
+                    help="run only the orbit-interpolation leg (with --interp-orbits "
+                         "orbits, --steps timed calls after --warmup)")
+    ap.add_argument("--interp-orbits", type=int, default=1 << 20)
     ap.add_argument("--grad-only", action="store_true",
                     help="run only the differentiation leg (with --grad-orbits orbits)")
     ap.add_argument("--grad-orbits", type=int, default=65536)
@@ -406,6 +410,17 @@ def main():
         peak = ctypes_fp64_peak(_lib)
         res = differentiation_leg(gb, torch, dev, torch.cuda.current_stream(dev), pg, peak,
                                   n=args.grad_orbits)
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        if rank == 0:
+            print(json.dumps(res), flush=True)
+        return
+
+    if args.interp_only:
+        res = interp_leg(gb, torch, dev, torch.cuda.current_stream(dev), pg,
+                         n=args.interp_orbits, K=args.steps, W=args.warmup,
+                         cpu=rank == 0 and not args.no_cpu_baseline)
         if pg:
             pg.barrier()
             pg.destroy_process_group()
@@ -644,7 +659,7 @@ def interp_leg(gb, torch, dev, stream, pg, n=1 << 20, nt=NT, nq=NT - 1, K=3, W=3
            "value": n * nq / (ms * 1e-3), "unit": "interpolated rows/s", "ms": ms,
            "algorithmic_bytes": algo_bytes,
            "achieved_GBs": algo_bytes / (ms * 1e-3) / 1e9,
-           "gpu_launches": 3 * K}
+           "gpu_launches": 4 * K}  # transpose, sweep, moments, evaluation
     if cpu:
         try:
             from scipy import interpolate as si
