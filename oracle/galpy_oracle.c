@@ -15,7 +15,10 @@
  *            ZeroForce, Einasto and ExpTruncNFW (through
  *            SphericalPotential.c),
  *            FlattenedPowerPotential.c, KuzminKutuzovStaeckelPotential.c,
- *            HenonHeilesPotential.c (planar) (potential_c_ext/)
+ *            HenonHeilesPotential.c (planar), the time-dependent
+            DehnenBarPotential.c and SCFPotential.c (static coefficients;
+            the Gegenbauer and Legendre arrays by this file's own
+            recurrences) (potential_c_ext/)
  *   sums     galpy_potentials.c:120-354 (sum over components, in order)
  *   RHS      orbit_c_ext/integrateFullOrbit.c:1307-1352 (evalRectForce,
  *            evalRectDeriv), :1496-1681 (the dxdv variants);
@@ -30,6 +33,9 @@
  *            with evalPlanarSOSDerivx/y :1056-1123);
  *            integratePlanarOrbit.c:743-847, :940-1014
  *   coords   util/bovy_coords.c:57-148
+ * Each force evaluation gets the time the reference's stepper hands it (its
+ * own bookkeeping of `to`, t_current, t_old, or the state's time in a
+ * surface of section), which only the time-dependent components read.
  * The arithmetic of each formula follows the reference term by term so that
  * this restatement agrees with the reference's own C (built from its sources
  * into oracle/_ref by oracle/Makefile) to the last bit or close to it; the
@@ -92,6 +98,12 @@ enum { PT_KUZMINDISK = 19 };
    rot [9], glorder, glx [glorder], weights [glorder]) */
 enum { PT_TRIHERNQUIST = 21, PT_TRINFW = 22, PT_TRIJAFFE = 23, PT_PERFECTELL = 30,
        PT_TRIGAUSS = 37, PT_POWERTRI = 38, PT_TWOPOWERTRI = 43 };
+/* time-dependent DehnenBarPotential (DehnenBarPotential.c), args (amp * af,
+   tform, tsteady, rb, omegab, barphi), 3D and planar */
+enum { PT_DEHNENBAR = 1 };
+/* SCFPotential (SCFPotential.c), static coefficients: args (a, isNonAxi, N,
+   L, M, Nt = 0, Acos [N][L][M], Asin [N][L][M] if isNonAxi, 11 cache slots) */
+enum { PT_SCF = 24 };
 
 static int is_ellipsoidal(int type)
 {
@@ -110,12 +122,26 @@ static int ell_nargs(const double *a)
   return 30 + np + 2 * (int)a[29 + np];
 }
 
+/* argument count of an SCF component (integrateFullOrbit.c case 24) with
+   static coefficients (Nt = 0; time-dependent coefficients are not
+   restated); -1 otherwise */
+#define SCF_MAXN 64
+#define SCF_MAXL 32
+static int scf_nargs(const double *a)
+{
+  int nonaxi = (int)a[1], N = (int)a[2], L = (int)a[3], M = (int)a[4], Nt = (int)a[5];
+  if (Nt != 0 || N < 1 || L < 1 || M < 1 || N > SCF_MAXN || L > SCF_MAXL) return -1;
+  if (nonaxi && M != L) return -1; /* the reference sums m <= l over an [N][L][L] array */
+  return 6 + (1 + nonaxi) * N * L * M + 11;
+}
+
 #define OMAXPOT 32
 
 typedef struct {
   int type;
-  double p[5];     /* the component's args as galpy passes them */
-  const double *ea; /* all args (ellipsoidal components: the caller's array) */
+  double p[8];     /* the component's args as galpy passes them */
+  const double *ea; /* all args (ellipsoidal and SCF components: the caller's array) */
+  double t;        /* time of the current evaluation (time-dependent types) */
 } ocomp;
 
 typedef struct {
@@ -123,6 +149,7 @@ typedef struct {
   int planar;
   ocomp c[OMAXPOT];
   long long nforce; /* force evaluations (instrumentation) */
+  double t;         /* time at which the stepper evaluates the next force */
 } opot;
 
 static int nargs_of(int type, int planar)
@@ -141,6 +168,7 @@ static int nargs_of(int type, int planar)
   case PT_KKS: return 3;
   case PT_HENONHEILES: return planar ? 1 : -1;
   case PT_KUZMINDISK: return 2;
+  case PT_DEHNENBAR: return 6;
   default: return -1;
   }
 }
@@ -537,13 +565,17 @@ static int opot_decode(opot *P, int npot, const int *type, const double *args, i
   P->n = npot;
   P->planar = planar;
   P->nforce = 0;
+  P->t = 0.;
   for (int i = 0; i < npot; i++) {
-    int na = is_ellipsoidal(type[i]) ? ell_nargs(args) : nargs_of(type[i], planar);
+    int na = is_ellipsoidal(type[i]) ? ell_nargs(args)
+             : type[i] == PT_SCF      ? scf_nargs(args)
+                                      : nargs_of(type[i], planar);
     if (na < 0) return -1;
     P->c[i].type = type[i];
     P->c[i].ea = args;
-    for (int k = 0; k < 5; k++) P->c[i].p[k] = 0.;
-    for (int k = 0; k < na && k < 5; k++) P->c[i].p[k] = args[k];
+    P->c[i].t = 0.;
+    for (int k = 0; k < 8; k++) P->c[i].p[k] = 0.;
+    for (int k = 0; k < na && k < 8; k++) P->c[i].p[k] = args[k];
     args += na;
   }
   return 0;
@@ -769,9 +801,327 @@ static double ell_eval(const ocomp *c, double R, double Z, double phi)
   return -0.5 * c->p[0] * out;
 }
 
+/* ---- DehnenBarPotential (DehnenBarPotential.c:5-314) ---- */
+/* bar growth factor (dehnenBarSmooth): 0 before tform, the quintic
+   3/16 xi^5 - 5/8 xi^3 + 15/16 xi + 1/2 of xi = 2 (t - tform) / (tsteady -
+   tform) - 1 until tsteady, 1 after */
+static double dbar_smooth(double t, double tform, double tsteady)
+{
+  if (t < tform) return 0.;
+  if (t < tsteady) {
+    double xi = 2. * (t - tform) / (tsteady - tform) - 1.;
+    return 3. / 16. * pow(xi, 5.) - 5. / 8. * pow(xi, 3.) + 15. / 16. * xi + .5;
+  }
+  return 1.;
+}
+
+/* args: p0 amp, p1 tform, p2 tsteady, p3 rb, p4 omegab, p5 barphi;
+   which: 0 Rforce, 1 zforce, 2 phitorque (3D) */
+static double dbar_force3(const ocomp *c, int which, double R, double z, double phi)
+{
+  double amp = c->p[0], rb = c->p[3], t = c->t;
+  double sm = dbar_smooth(t, c->p[1], c->p[2]);
+  double ang = 2. * (phi - c->p[4] * t - c->p[5]);
+  double r2 = R * R + z * z, r = sqrt(r2);
+  if (which == 0) {
+    if (r <= rb)
+      return -amp * sm * cos(ang) * (pow(r / rb, 3.) * R * (3. * R * R + 2. * z * z) - 4. * R * z * z) /
+             pow(r, 4.);
+    return -amp * sm * cos(ang) * pow(rb / r, 3.) * R / pow(r, 4) * (3. * R * R - 2. * z * z);
+  }
+  if (which == 1) {
+    if (r <= rb) return -amp * sm * cos(ang) * (pow(r / rb, 3.) + 4.) * R * R * z / pow(r, 4.);
+    return -5. * amp * sm * cos(ang) * pow(rb / r, 3.) * R * R * z / pow(r, 4);
+  }
+  if (r <= rb) return 2. * amp * sm * sin(ang) * (pow(r / rb, 3.) - 2.) * R * R / r2;
+  return -2. * amp * sm * sin(ang) * pow(rb / r, 3.) * R * R / r2;
+}
+
+/* planar: which 0 Rforce, 2 phitorque */
+static double dbar_force2(const ocomp *c, int which, double R, double phi)
+{
+  double amp = c->p[0], rb = c->p[3], t = c->t;
+  double sm = dbar_smooth(t, c->p[1], c->p[2]);
+  double ang = 2. * (phi - c->p[4] * t - c->p[5]);
+  if (which == 0) {
+    if (R <= rb) return -3. * amp * sm * cos(ang) * pow(R / rb, 3.) / R;
+    return -3. * amp * sm * cos(ang) * pow(rb / R, 3.) / R;
+  }
+  if (R <= rb) return 2. * amp * sm * sin(ang) * (pow(R / rb, 3.) - 2.);
+  return -2. * amp * sm * sin(ang) * pow(rb / R, 3.);
+}
+
+/* planar second derivatives of the potential: which 0 R2, 1 phi2, 2 Rphi */
+static double dbar_hess2(const ocomp *c, int which, double R, double phi)
+{
+  double amp = c->p[0], rb = c->p[3], t = c->t;
+  double sm = dbar_smooth(t, c->p[1], c->p[2]);
+  double ang = 2. * (phi - c->p[4] * t - c->p[5]);
+  int in = R <= rb;
+  if (which == 0)
+    return in ? 6. * amp * sm * cos(ang) * pow(R / rb, 3.) / R / R
+              : -12. * amp * sm * cos(ang) * pow(rb / R, 3.) / R / R;
+  if (which == 1)
+    return in ? -4. * amp * sm * cos(ang) * (pow(R / rb, 3.) - 2.)
+              : 4. * amp * sm * cos(ang) * pow(rb / R, 3.);
+  return in ? -6. * amp * sm * sin(ang) * pow(R / rb, 3.) / R
+            : -6. * amp * sm * sin(ang) * pow(rb / R, 3.) / R;
+}
+
+/* 3D second derivatives: which 0 R2, 1 z2, 2 Rz, 3 phi2, 4 Rphi, 5 zphi */
+static double dbar_hess3(const ocomp *c, int which, double R, double z, double phi)
+{
+  double amp = c->p[0], rb = c->p[3], t = c->t;
+  double sm = dbar_smooth(t, c->p[1], c->p[2]);
+  double ang = 2. * (phi - c->p[4] * t - c->p[5]);
+  double R2 = R * R, z2 = z * z, r2 = R2 + z2, r4 = r2 * r2, r6 = r4 * r2;
+  int in = r2 <= rb * rb;
+  double pre;
+  switch (which) {
+  case 0:
+    pre = amp * sm * cos(ang);
+    if (in)
+      return pre * (pow(r2, 1.5) / (rb * rb * rb) * ((9. * R2 + 2. * z2) / r4 - R2 / r6 * (3. * R2 + 2. * z2)) +
+                    4. * z2 / r6 * (4. * R2 - r2));
+    return pre * pow(rb, 3.) * pow(r2, -1.5) / r6 * ((r2 - 7. * R2) * (3. * R2 - 2. * z2) + 6. * R2 * r2);
+  case 1:
+    pre = amp * sm * cos(ang);
+    if (in) return pre * R2 / r6 * (pow(r2, 1.5) / (rb * rb * rb) * (r2 - z2) + 4. * (r2 - 4. * z2));
+    return pre * 5. * pow(rb, 3.) * pow(r2, -1.5) * R2 / r6 * (r2 - 7. * z2);
+  case 2:
+    pre = amp * sm * cos(ang);
+    if (in) return pre * R * z / r6 * (pow(r2, 1.5) / (rb * rb * rb) * (2. * r2 - R2) + 8. * (r2 - 2. * R2));
+    return pre * 5. * pow(rb, 3.) * pow(r2, -1.5) * R * z / r6 * (2. * r2 - 7. * R2);
+  case 3:
+    pre = 4. * amp * sm * cos(ang);
+    if (in) return -pre * (pow(r2, 1.5) / (rb * rb * rb) - 2.) * R2 / r2;
+    return pre * pow(rb, 3.) * pow(r2, -1.5) * R2 / r2;
+  case 4:
+    pre = -2. * amp * sm * sin(ang);
+    if (in) return pre * (pow(r2, 1.5) / (rb * rb * rb) * R * (3. * R2 + 2. * z2) - 4. * R * z2) / r4;
+    return pre * pow(rb, 3.) * pow(r2, -1.5) * R / r4 * (3. * R2 - 2. * z2);
+  default:
+    pre = -2. * amp * sm * sin(ang);
+    if (in) return pre * (pow(r2, 1.5) / (rb * rb * rb) + 4.) * R2 * z / r4;
+    return pre * 5. * pow(rb, 3.) * pow(r2, -1.5) * R2 * z / r4;
+  }
+}
+
+/* ---- SCFPotential (SCFPotential.c:181-1025), static coefficients ---- */
+/* Hernquist-Ostriker expansion Phi = sqrt(4 pi) sum_{nlm} (Acos cos m phi +
+   Asin sin m phi) phiTilde_nl(r) P_l^m(cos theta) with phiTilde_nl =
+   -(a r)^l / (a + r)^(2l+1) C_n^(2l+3/2)(xi), xi = (r - a)/(r + a).  The
+   Gegenbauer and associated Legendre functions (GSL's in the reference) are
+   this file's own three-term recurrences (DLMF 18.9.1, 14.10.3), checked
+   against scipy in the tests. */
+/* C_n^lam(x), n = 0..nmax: (n+1) C_{n+1} = 2 (n + lam) x C_n - (n + 2 lam - 1) C_{n-1} */
+static void scf_gegen(int nmax, double lam, double x, double *C)
+{
+  C[0] = 1.;
+  if (nmax >= 1) C[1] = 2. * lam * x;
+  for (int n = 1; n < nmax; n++)
+    C[n + 1] = (2. * (n + lam) * x * C[n] - (n + 2. * lam - 1.) * C[n - 1]) / (n + 1.);
+}
+
+/* P_l^m(x) with the Condon-Shortley phase for 0 <= m <= l < L (m < M) in
+   the triangle layout l (l + 1) / 2 + m, and dP/dx, by the upward
+   recurrences (l - m) P_l^m = (2l - 1) x P_{l-1}^m - (l + m - 1) P_{l-2}^m
+   from P_m^m = (-1)^m (2m - 1)!! (1 - x^2)^(m/2), and (x^2 - 1) dP_l^m/dx =
+   l x P_l^m - (l + m) P_{l-1}^m */
+static void scf_legendre(double x, int L, int M, double *P, double *dP)
+{
+  double s = sqrt((1. - x) * (1. + x)), pmm = 1.;
+  for (int m = 0; m < M && m < L; m++) {
+    if (m > 0) pmm *= -(2. * m - 1.) * s;
+    double pm2 = 0., pm1 = pmm;
+    for (int l = m; l < L; l++) {
+      double p;
+      if (l == m)
+        p = pmm;
+      else if (l == m + 1)
+        p = x * (2. * m + 1.) * pmm;
+      else
+        p = ((2. * l - 1.) * x * pm1 - (l + m - 1.) * pm2) / (l - m);
+      double prev = l == m ? 0. : pm1;
+      int i = l * (l + 1) / 2 + m;
+      P[i] = p;
+      if (dP) dP[i] = (l * x * p - (l + m) * prev) / (x * x - 1.);
+      if (l > m) {
+        pm2 = pm1;
+        pm1 = p;
+      }
+    }
+  }
+}
+
+typedef struct {
+  double a;
+  int nonaxi, N, L, M;
+  const double *Acos, *Asin;
+} oscf;
+
+static oscf scf_args(const ocomp *c)
+{
+  oscf d;
+  const double *a = c->ea;
+  d.a = a[0];
+  d.nonaxi = (int)a[1];
+  d.N = (int)a[2];
+  d.L = (int)a[3];
+  d.M = (int)a[4];
+  d.Acos = a + 6;
+  d.Asin = d.nonaxi ? a + 6 + d.N * d.L * d.M : NULL;
+  return d;
+}
+
+/* Spherical quantities at (r, theta, phi), summed as the reference sums
+   them (sum_spher_forces, sum_expansion, sum_spher_full): F[0..2] the forces
+   -dPhi/dr, -dPhi/dtheta, -dPhi/dphi, F[3] Phi and, if hess, H[0..7] =
+   dPhi/dr, dPhi/dtheta, d2/dr2, d2/dtheta2, d2/drdtheta, d2/dphi2,
+   d2/drdphi, d2/dthetadphi */
+static void scf_spher(const ocomp *c, double r, double theta, double phi, int hess, double *F,
+                      double *H)
+{
+  oscf d = scf_args(c);
+  int N = d.N, L = d.L, M = d.M, Me = d.nonaxi ? M : 1;
+  double a = d.a, xi = (r - a) / (r + a), ar = a + r;
+  double C[SCF_MAXL][SCF_MAXN], dC[SCF_MAXL][SCF_MAXN], d2C[SCF_MAXL][SCF_MAXN];
+  double phiT[SCF_MAXL][SCF_MAXN], dphiT[SCF_MAXL][SCF_MAXN], d2phiT[SCF_MAXL][SCF_MAXN];
+  for (int l = 0; l < L; l++) {
+    double tmp[SCF_MAXN];
+    scf_gegen(N - 1, 1.5 + 2 * l, xi, C[l]);
+    dC[l][0] = 0.;
+    if (N > 1) {
+      scf_gegen(N - 2, 2.5 + 2 * l, xi, tmp);
+      for (int n = 1; n < N; n++) dC[l][n] = tmp[n - 1];
+    }
+    for (int n = 0; n < N; n++) dC[l][n] *= 2.0 * (2 * l + 1.5);
+    d2C[l][0] = 0.;
+    if (N > 1) d2C[l][1] = 0.;
+    if (N > 2) {
+      scf_gegen(N - 3, 3.5 + 2 * l, xi, tmp);
+      for (int n = 2; n < N; n++) d2C[l][n] = tmp[n - 2];
+    }
+    for (int n = 0; n < N; n++) d2C[l][n] *= 4.0 * (2 * l + 1.5) * (2 * l + 2.5);
+  }
+  /* radial functions (compute_phiTilde, compute_dphiTilde, compute_d2phiTilde) */
+  double rt = -1.0 / (r + a), rt1 = 1.0 / (r * ar * ar * ar);
+  double rt2 = 1.0 / (r * r * ar * ar * ar * ar * ar);
+  for (int l = 0; l < L; l++) {
+    if (l > 0) {
+      rt *= r * a / ((a + r) * (a + r));
+      rt1 *= a * r / (ar * ar);
+      rt2 *= a * r / (ar * ar);
+    }
+    for (int n = 0; n < N; n++) {
+      double ar2 = ar * ar, ar3 = ar2 * ar, ar4 = ar3 * ar;
+      phiT[l][n] = rt * C[l][n];
+      dphiT[l][n] = rt1 * (((2 * l + 1) * r * ar - l * ar * ar) * C[l][n] - 2.0 * a * r * dC[l][n]);
+      d2phiT[l][n] = rt2 * (C[l][n] * (l * (1 - l) * ar4 - (4.0 * l * l + 6.0 * l + 2.0) * r * r * ar2 +
+                                       l * (4 * l + 2) * r * ar3) +
+                            a * r *
+                                ((4.0 * r * r + 4.0 * a * r + (8 * l + 4) * r * ar - 4 * l * ar2) * dC[l][n] -
+                                 4.0 * a * r * d2C[l][n]));
+    }
+  }
+  /* angular functions; theta derivatives as legendre_theta_from_x */
+  double P[SCF_MAXL * (SCF_MAXL + 1) / 2], dPx[SCF_MAXL * (SCF_MAXL + 1) / 2];
+  double x = cos(theta), st = sin(theta), is2 = 1.0 / (st * st);
+  scf_legendre(x, L, Me, P, dPx);
+  double f0 = 0., f1 = 0., f2 = 0., pot = 0.;
+  if (hess)
+    for (int k = 0; k < 8; k++) H[k] = 0.;
+  for (int l = 0; l < L; l++) {
+    for (int m = 0; m <= l && m < Me; m++) {
+      double mc = cos(m * phi), ms = sin(m * phi);
+      int pi = l * (l + 1) / 2 + m;
+      double dPt = -st * dPx[pi];
+      double d2Pt = x * dPx[pi] - l * (l + 1) * P[pi] + (m ? m * m * is2 * P[pi] : 0.0);
+      for (int n = 0; n < N; n++) {
+        int ci = n * L * M + l * M + m;
+        double ac = d.Acos[ci], as = d.nonaxi ? d.Asin[ci] : 0.;
+        double cs = ac * mc + as * ms, sd = ac * ms - as * mc;
+        f0 -= cs * P[pi] * dphiT[l][n];
+        f1 -= cs * dPx[pi] * phiT[l][n];
+        f2 += m * sd * P[pi] * phiT[l][n];
+        pot += cs * P[pi] * phiT[l][n];
+        if (hess) {
+          double dsum = m * (as * mc - ac * ms);
+          H[0] += cs * P[pi] * dphiT[l][n];
+          H[1] += cs * dPt * phiT[l][n];
+          H[2] += cs * P[pi] * d2phiT[l][n];
+          H[3] += cs * d2Pt * phiT[l][n];
+          H[4] += cs * dPt * dphiT[l][n];
+          H[5] -= m * m * cs * P[pi] * phiT[l][n];
+          H[6] += dsum * P[pi] * dphiT[l][n];
+          H[7] += dsum * dPt * phiT[l][n];
+        }
+      }
+    }
+  }
+  double s4 = sqrt(4.0 * M_PI);
+  F[0] = f0 * s4;
+  F[1] = f1 * (s4 * (-st));
+  F[2] = f2 * s4;
+  F[3] = pot * s4;
+  if (hess)
+    for (int k = 0; k < 8; k++) H[k] *= s4;
+}
+
+/* which: 0 Rforce, 1 zforce, 2 phitorque (SCFPotentialRforce / zforce / phitorque) */
+static double scf_force3(const ocomp *c, int which, double R, double Z, double phi)
+{
+  double r = sqrt(R * R + Z * Z), theta = atan2(R, Z), F[4];
+  scf_spher(c, r, theta, phi, 0, F, NULL);
+  if (which == 0) return F[0] * (R / r) + F[1] * (Z / (r * r));
+  if (which == 1) return F[0] * (Z / r) + F[1] * (-R / (r * r));
+  return F[2];
+}
+
+/* 3D second derivatives (compute_scf_hessian_cyl): 0 R2, 1 z2, 2 Rz, 3 phi2, 4 Rphi, 5 zphi */
+static double scf_hess3(const ocomp *c, int which, double R, double Z, double phi)
+{
+  double r = sqrt(R * R + Z * Z), theta = atan2(R, Z), F[4], S[8];
+  scf_spher(c, r, theta, phi, 1, F, S);
+  double Pr = S[0], Pth = S[1], Prr = S[2], Pthth = S[3], Prth = S[4];
+  double Ppp = S[5], Prp = S[6], Pthp = S[7];
+  double ir = 1.0 / r, ir2 = ir * ir, ir3 = ir2 * ir, ir4 = ir2 * ir2;
+  double rR = R * ir, rz = Z * ir, thR = Z * ir2, thz = -R * ir2;
+  double rRR = Z * Z * ir3, rzz = R * R * ir3, rRz = -R * Z * ir3;
+  double thRR = -2.0 * R * Z * ir4, thzz = 2.0 * R * Z * ir4, thRz = (R * R - Z * Z) * ir4;
+  switch (which) {
+  case 0: return Prr * rR * rR + 2.0 * Prth * rR * thR + Pthth * thR * thR + Pr * rRR + Pth * thRR;
+  case 1: return Prr * rz * rz + 2.0 * Prth * rz * thz + Pthth * thz * thz + Pr * rzz + Pth * thzz;
+  case 2:
+    return Prr * rR * rz + Prth * (rR * thz + rz * thR) + Pthth * thR * thz + Pr * rRz + Pth * thRz;
+  case 3: return Ppp;
+  case 4: return Prp * rR + Pthp * thR;
+  default: return Prp * rz + Pthp * thz;
+  }
+}
+
+/* planar second derivatives (compute_spher_2nd_derivs at Z = 0): 0 R2, 1 phi2, 2 Rphi */
+static double scf_hess2(const ocomp *c, int which, double R, double phi)
+{
+  double F[4], S[8];
+  scf_spher(c, R, atan2(R, 0.0), phi, 1, F, S);
+  if (which == 0) return S[2];
+  if (which == 1) return S[5];
+  return S[6];
+}
+
+static double scf_eval(const ocomp *c, double R, double Z, double phi)
+{
+  double F[4];
+  scf_spher(c, sqrt(R * R + Z * Z), atan2(R, Z), phi, 0, F, NULL);
+  return F[3];
+}
+
 /* ---- 3D component forces ---- */
 static double comp_Rforce(ocomp *c, double R, double Z, double phi)
 {
+  if (c->type == PT_DEHNENBAR) return dbar_force3(c, 0, R, Z, phi);
+  if (c->type == PT_SCF) return scf_force3(c, 0, R, Z, phi);
   if (is_new_spherical(c->type)) return sph_force3(c, R, Z, R);
   if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 0, R, Z, phi);
   double amp = c->p[0];
@@ -814,6 +1164,8 @@ static double comp_Rforce(ocomp *c, double R, double Z, double phi)
 
 static double comp_zforce(ocomp *c, double R, double Z, double phi)
 {
+  if (c->type == PT_DEHNENBAR) return dbar_force3(c, 1, R, Z, phi);
+  if (c->type == PT_SCF) return scf_force3(c, 1, R, Z, phi);
   if (is_new_spherical(c->type)) return sph_force3(c, R, Z, Z);
   if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 1, R, Z, phi);
   double amp = c->p[0];
@@ -860,6 +1212,8 @@ static double comp_zforce(ocomp *c, double R, double Z, double phi)
 
 static double comp_phitorque(const ocomp *c, double R, double Z, double phi)
 {
+  if (c->type == PT_DEHNENBAR) return dbar_force3(c, 2, R, Z, phi);
+  if (c->type == PT_SCF) return scf_force3(c, 2, R, Z, phi);
   if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 2, R, Z, phi);
   if (c->type == PT_LOGHALO && c->p[3] < 1) {
     double amp = c->p[0], q = c->p[1], cc = c->p[2], om = c->p[3];
@@ -886,6 +1240,8 @@ static void sph_derivs(const ocomp *c, double r, double *dphi, double *d2phi)
 /* 3D Hessian terms: which = 0 R2, 1 z2, 2 Rz, 3 phi2, 4 Rphi, 5 zphi */
 static double comp_hess(const ocomp *c, int which, double R, double Z, double phi)
 {
+  if (c->type == PT_DEHNENBAR) return dbar_hess3(c, which, R, Z, phi);
+  if (c->type == PT_SCF) return scf_hess3(c, which, R, Z, phi);
   if (is_new_spherical(c->type)) return sph_hess3(c, which, R, Z);
   if (is_ellipsoidal(c->type)) return ell_cyl_hess(c, which, R, Z, phi);
   double amp = c->p[0];
@@ -1018,6 +1374,8 @@ static double comp_hess(const ocomp *c, int which, double R, double Z, double ph
 /* ---- planar component forces ---- */
 static double comp_planarRforce(const ocomp *c, double R, double phi)
 {
+  if (c->type == PT_DEHNENBAR) return dbar_force2(c, 0, R, phi);
+  if (c->type == PT_SCF) return scf_force3(c, 0, R, 0.0, phi); /* SCFPotentialPlanarRforce */
   if (is_new_spherical(c->type)) return sph_planarRforce(c, R);
   if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 0, R, 0., phi);
   double amp = c->p[0];
@@ -1067,6 +1425,8 @@ static double comp_planarRforce(const ocomp *c, double R, double phi)
 
 static double comp_planarphitorque(const ocomp *c, double R, double phi)
 {
+  if (c->type == PT_DEHNENBAR) return dbar_force2(c, 2, R, phi);
+  if (c->type == PT_SCF) return scf_force3(c, 2, R, 0.0, phi);
   if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 2, R, 0., phi);
   if (c->type == PT_HENONHEILES) /* HenonHeilesPotentialphitorque */
     return -c->p[0] * pow(R, 3.) * cos(3. * phi);
@@ -1080,6 +1440,8 @@ static double comp_planarphitorque(const ocomp *c, double R, double phi)
 /* planar Hessian: which = 0 R2, 1 phi2, 2 Rphi */
 static double comp_planarhess(const ocomp *c, int which, double R, double phi)
 {
+  if (c->type == PT_DEHNENBAR) return dbar_hess2(c, which, R, phi);
+  if (c->type == PT_SCF) return scf_hess2(c, which, R, phi);
   if (is_new_spherical(c->type)) return which ? 0. : sph_planarR2deriv(c, R);
   if (is_ellipsoidal(c->type)) /* EllipsoidalPotentialPlanarR2deriv / phi2 / Rphi */
     return ell_cyl_hess(c, which == 0 ? 0 : which + 2, R, 0., phi);
@@ -1151,6 +1513,8 @@ static double comp_planarhess(const ocomp *c, int which, double R, double phi)
 /* ---- potential values (for energies) ---- */
 static double comp_eval(const ocomp *c, double R, double Z, double phi)
 {
+  if (c->type == PT_SCF) return scf_eval(c, R, Z, phi);
+  if (c->type == PT_DEHNENBAR) return NAN; /* no C evaluation in the reference */
   if (is_new_spherical(c->type)) return sph_eval(c, R, Z);
   if (is_ellipsoidal(c->type)) return ell_eval(c, R, Z, phi);
   double amp = c->p[0];
@@ -1235,9 +1599,16 @@ static void cyl_of(double x, double y, double *R, double *phi, double *sp, doubl
   if (g_phi_mode == 0 && y < 0.) *phi = 2. * M_PI - *phi;
 }
 
+/* the stepper's evaluation time, handed to the time-dependent components */
+static void stamp_time(opot *P)
+{
+  for (int i = 0; i < P->n; i++) P->c[i].t = P->t;
+}
+
 static void sum3(opot *P, double R, double z, double phi, double *Rf, double *zf, double *pt)
 {
   double a = 0., b = 0., c = 0.;
+  stamp_time(P);
   for (int i = 0; i < P->n; i++) a += comp_Rforce(&P->c[i], R, z, phi);
   for (int i = 0; i < P->n; i++) c += comp_phitorque(&P->c[i], R, z, phi);
   for (int i = 0; i < P->n; i++) b += comp_zforce(&P->c[i], R, z, phi);
@@ -1250,6 +1621,7 @@ static void sum3(opot *P, double R, double z, double phi, double *Rf, double *zf
 static void sum2(opot *P, double R, double phi, double *Rf, double *pt)
 {
   double a = 0., c = 0.;
+  stamp_time(P);
   for (int i = 0; i < P->n; i++) a += comp_planarRforce(&P->c[i], R, phi);
   for (int i = 0; i < P->n; i++) c += comp_planarphitorque(&P->c[i], R, phi);
   *Rf = a;
@@ -1313,6 +1685,7 @@ static void planar_K(double R, double sp, double cp, double Rf, double pt, doubl
 
 static void hess3(opot *P, double R, double z, double phi, double h[6])
 {
+  stamp_time(P);
   for (int w = 0; w < 6; w++) {
     double s = 0.;
     for (int i = 0; i < P->n; i++) s += comp_hess(&P->c[i], w, R, z, phi);
@@ -1373,6 +1746,7 @@ static void rect_force3_dxdv(opot *P, const double *q, double *a)
 static void planar_hess_sum(opot *P, double R, double phi, double *R2d, double *p2d, double *Rpd)
 {
   double a = 0., b = 0., c = 0.;
+  stamp_time(P);
   for (int i = 0; i < P->n; i++) a += comp_planarhess(&P->c[i], 0, R, phi);
   for (int i = 0; i < P->n; i++) b += comp_planarhess(&P->c[i], 1, R, phi);
   for (int i = 0; i < P->n; i++) c += comp_planarhess(&P->c[i], 2, R, phi);
@@ -1488,14 +1862,29 @@ static const oscheme SCH_LF = {1, LFC, LFD}, SCH_S4 = {3, S4C, S4D}, SCH_S6 = {7
    ((c_nk + c_0) h), the final drift c_nk h.  This is the step sequence of
    leapfrog / symplec4 / symplec6 (bovy_symplecticode.c:132-587) and of the
    one- and two-step trials of their estimators (:588-1052). */
+/* Force times, as the reference keeps its time `to`: TM_DRIFTS (symplec4,
+   symplec6 and their estimators) adds each drift's length to *to and kicks
+   at *to; TM_LEAP (leapfrog) kicks at *to + h/2 and adds h after each step;
+   TM_LEAP_EST (leapfrog_estimate_step) kicks at to + dt/2 (one step of dt)
+   or to + dt/4 and to + 3 dt/4 (two of dt/2), *to unchanged. */
+enum { TM_DRIFTS = 0, TM_LEAP = 1, TM_LEAP_EST = 2 };
+
 static void comp_advance(const oscheme *S, rhs_fn f, opot *P, int n, const double *q0,
-                         const double *p0, double h, long nstep, double *q, double *p)
+                         const double *p0, double h, long nstep, double *q, double *p,
+                         double *to, int tmode)
 {
   double a[MAXD];
   drift(n, q0, p0, S->c[0] * h, q);
+  if (tmode == TM_DRIFTS) *to += S->c[0] * h;
   for (int k = 0; k < n; k++) p[k] = p0[k];
   for (long s = 0; s < nstep; s++) {
     for (int j = 0; j < S->nk; j++) {
+      if (tmode == TM_DRIFTS)
+        P->t = *to;
+      else if (tmode == TM_LEAP || nstep == 1)
+        P->t = *to + h / 2.;
+      else /* the estimator's two half steps, dt = 2 h */
+        P->t = s == 0 ? *to + (2. * h) / 4. : *to + 3. * (2. * h) / 4.;
       f(P, q, a);
       kick(n, p, S->d[j] * h, a, p);
       double c;
@@ -1504,7 +1893,9 @@ static void comp_advance(const oscheme *S, rhs_fn f, opot *P, int n, const doubl
       else
         c = (s < nstep - 1) ? (S->c[S->nk] + S->c[0]) * h : S->c[S->nk] * h;
       drift(n, q, p, c, q);
+      if (tmode == TM_DRIFTS) *to += c;
     }
+    if (tmode == TM_LEAP) *to = *to + h;
   }
 }
 
@@ -1512,16 +1903,19 @@ static void comp_advance(const oscheme *S, rhs_fn f, opot *P, int n, const doubl
    (bovy_symplecticode.c:588-664, 665-809, 810-1052): halve dt until one step
    and two half steps agree to the tolerance */
 static double comp_est(const oscheme *S, rhs_fn f, opot *P, int dim, const double *qo,
-                       const double *po, double dt, double rtol, double atol)
+                       const double *po, double dt, double t0, double rtol, double atol)
 {
-  double err = 2., init_dt = dt;
+  double err = 2., init_dt = dt, to = t0;
+  int tmode = S == &SCH_LF ? TM_LEAP_EST : TM_DRIFTS;
   double q11[MAXD], q12[MAXD], p11[MAXD], p12[MAXD];
   double sq = est_scale(dim, qo, rtol, atol), sp = est_scale(dim, po, rtol, atol);
   dt *= 2.;
   while (err > 1. && init_dt / dt < MAX_DT_REDUCE) {
     dt /= 2.;
-    comp_advance(S, f, P, dim, qo, po, dt, 1, q11, p11);
-    comp_advance(S, f, P, dim, qo, po, dt / 2., 2, q12, p12);
+    comp_advance(S, f, P, dim, qo, po, dt, 1, q11, p11, &to, tmode);
+    if (tmode == TM_DRIFTS) to -= dt;
+    comp_advance(S, f, P, dim, qo, po, dt / 2., 2, q12, p12, &to, tmode);
+    if (tmode == TM_DRIFTS) to -= dt;
     err = 0.;
     for (int i = 0; i < dim; i++) {
       err += exp(2. * log(fabs(q11[i] - q12[i])) - 2. * sq);
@@ -1551,11 +1945,12 @@ static void symplectic(const oscheme *S, rhs_fn f, rhs_fn fb, opot *P, int ndim,
   result += 2 * ndim;
   st->err = 0;
   double init_dt = t[1] - t[0];
-  if (dt == DT_SENTINEL) dt = comp_est(S, fb, P, dim_base, qo, po, init_dt, rtol, atol);
+  if (dt == DT_SENTINEL) dt = comp_est(S, fb, P, dim_base, qo, po, init_dt, t[0], rtol, atol);
   long ndt = (long)(init_dt / dt);
   if (ndt < 1) ndt = 1; /* the reference's loop always makes the output step */
+  double to = t[0];
   for (int ii = 0; ii < nt - 1; ii++) {
-    comp_advance(S, f, P, ndim, qo, po, dt, ndt, qo, po);
+    comp_advance(S, f, P, ndim, qo, po, dt, ndt, qo, po, &to, S == &SCH_LF ? TM_LEAP : TM_DRIFTS);
     save_qp(ndim, dim_base, qo, po, result);
     result += 2 * ndim;
   }
@@ -1563,84 +1958,95 @@ static void symplectic(const oscheme *S, rhs_fn f, rhs_fn fb, opot *P, int ndim,
 }
 
 /* bovy_rk4_onestep (bovy_rk.c:142-170) */
-static void rk4_onestep(rhs_fn f, opot *P, int dim, const double *yn, double *yn1, double dt,
-                        double *ynk, double *a)
+static void rk4_onestep(rhs_fn f, opot *P, int dim, const double *yn, double *yn1, double tn,
+                        double dt, double *ynk, double *a)
 {
+  P->t = tn;
   f(P, yn, a);
   for (int i = 0; i < dim; i++) yn1[i] += dt * a[i] / 6.;
   for (int i = 0; i < dim; i++) ynk[i] = yn[i] + dt * a[i] / 2.;
+  P->t = tn + dt / 2.;
   f(P, ynk, a);
   for (int i = 0; i < dim; i++) yn1[i] += dt * a[i] / 3.;
   for (int i = 0; i < dim; i++) ynk[i] = yn[i] + dt * a[i] / 2.;
+  P->t = tn + dt / 2.;
   f(P, ynk, a);
   for (int i = 0; i < dim; i++) yn1[i] += dt * a[i] / 3.;
   for (int i = 0; i < dim; i++) ynk[i] = yn[i] + dt * a[i];
+  P->t = tn + dt;
   f(P, ynk, a);
   for (int i = 0; i < dim; i++) yn1[i] += dt * a[i] / 6.;
 }
 
 /* bovy_rk6_onestep (bovy_rk.c:256-327): seven stages, weights
    (11, 0, 81, 81, -32, -32, 11)/120 accumulated into yn1 stage by stage */
-static void rk6_onestep(rhs_fn f, opot *P, int dim, const double *yn, double *yn1, double dt,
-                        double *ynk, double *a)
+static void rk6_onestep(rhs_fn f, opot *P, int dim, const double *yn, double *yn1, double tn,
+                        double dt, double *ynk, double *a)
 {
   double k1[MAXD], k2[MAXD], k3[MAXD], k4[MAXD], k5[MAXD];
+  P->t = tn;
   f(P, yn, a);
   for (int i = 0; i < dim; i++) {
     yn1[i] += 11. * dt * a[i] / 120.;
     k1[i] = dt * a[i];
     ynk[i] = yn[i] + k1[i] / 3.;
   }
+  P->t = tn + dt / 3.;
   f(P, ynk, a);
   for (int i = 0; i < dim; i++) {
     k2[i] = dt * a[i];
     ynk[i] = yn[i] + 2. * k2[i] / 3.;
   }
+  P->t = tn + 2. * dt / 3.;
   f(P, ynk, a);
   for (int i = 0; i < dim; i++) {
     yn1[i] += 81. * dt * a[i] / 120.;
     k3[i] = dt * a[i];
     ynk[i] = yn[i] + (k1[i] + 4. * k2[i] - k3[i]) / 12.;
   }
+  P->t = tn + dt / 3.;
   f(P, ynk, a);
   for (int i = 0; i < dim; i++) {
     yn1[i] += 81. * dt * a[i] / 120.;
     k4[i] = dt * a[i];
     ynk[i] = yn[i] + (-k1[i] + 18. * k2[i] - 3. * k3[i] - 6. * k4[i]) / 16.;
   }
+  P->t = tn + dt / 2.;
   f(P, ynk, a);
   for (int i = 0; i < dim; i++) {
     yn1[i] -= 32. * dt * a[i] / 120.;
     k5[i] = dt * a[i];
     ynk[i] = yn[i] + (9. * k2[i] - 3. * k3[i] - 6. * k4[i] + 4. * k5[i]) / 8.;
   }
+  P->t = tn + dt / 2.;
   f(P, ynk, a);
   for (int i = 0; i < dim; i++) {
     yn1[i] -= 32. * dt * a[i] / 120.;
     const double k6 = dt * a[i];
     ynk[i] = yn[i] + (9. * k1[i] - 36. * k2[i] + 63. * k3[i] + 72. * k4[i] - 64. * k6) / 44.;
   }
+  P->t = tn + dt;
   f(P, ynk, a);
   for (int i = 0; i < dim; i++) yn1[i] += 11. * dt * a[i] / 120.;
 }
 
-typedef void (*rk_step_fn)(rhs_fn f, opot *P, int dim, const double *yn, double *yn1, double dt,
-                           double *ynk, double *a);
+typedef void (*rk_step_fn)(rhs_fn f, opot *P, int dim, const double *yn, double *yn1, double tn,
+                           double dt, double *ynk, double *a);
 
 /* rk4_estimate_step / rk6_estimate_step (bovy_rk.c:328-395, 396-480): divide
    dt by ceil(err^(1/(order+1))) until one step and two half steps agree */
 static double rk_est(rk_step_fn onestep, double expo, rhs_fn f, opot *P, int dim,
-                     const double *yo, double dt, double rtol, double atol)
+                     const double *yo, double dt, double to, double rtol, double atol)
 {
   double err = 2., init_dt = dt;
   double yn[MAXD], y1[MAXD], y21[MAXD], y2[MAXD], ynk[MAXD], a[MAXD];
   double s = est_scale(dim, yo, rtol, atol);
   while (err > 1.) {
     for (int i = 0; i < dim; i++) yn[i] = y1[i] = y21[i] = yo[i];
-    onestep(f, P, dim, yn, y1, dt, ynk, a);
-    onestep(f, P, dim, yn, y21, dt / 2., ynk, a);
+    onestep(f, P, dim, yn, y1, to, dt, ynk, a);
+    onestep(f, P, dim, yn, y21, to, dt / 2., ynk, a);
     for (int i = 0; i < dim; i++) y2[i] = y21[i];
-    onestep(f, P, dim, y21, y2, dt / 2., ynk, a);
+    onestep(f, P, dim, y21, y2, to + dt / 2., dt / 2., ynk, a);
     err = 0.;
     for (int i = 0; i < dim; i++) err += exp(2. * log(fabs(y1[i] - y2[i])) - 2. * s);
     err = sqrt(err / dim);
@@ -1664,14 +2070,18 @@ static void rk_fixed(int order, rhs_fn f, opot *P, int dim, const double *yo, in
   for (int i = 0; i < dim; i++) yn[i] = yn1[i] = yo[i];
   double init_dt = t[1] - t[0];
   if (dt == DT_SENTINEL)
-    dt = rk_est(onestep, order == 6 ? 1. / 7. : 1. / 5., f, P, dim, yo, init_dt, rtol, atol);
+    dt = rk_est(onestep, order == 6 ? 1. / 7. : 1. / 5., f, P, dim, yo, init_dt, t[0], rtol,
+                atol);
   long ndt = (long)(init_dt / dt);
+  double to = t[0];
   for (int ii = 0; ii < nt - 1; ii++) {
     for (long jj = 0; jj < ndt - 1; jj++) {
-      onestep(f, P, dim, yn, yn1, dt, ynk, a);
+      onestep(f, P, dim, yn, yn1, to, dt, ynk, a);
+      to += dt;
       for (int k = 0; k < dim; k++) yn[k] = yn1[k];
     }
-    onestep(f, P, dim, yn, yn1, dt, ynk, a);
+    onestep(f, P, dim, yn, yn1, to, dt, ynk, a);
+    to += dt;
     for (int k = 0; k < dim; k++) result[k] = yn1[k];
     result += dim;
     for (int k = 0; k < dim; k++) yn[k] = yn1[k];
@@ -1723,11 +2133,13 @@ static double dopr54_attempt(rhs_fn f, opot *P, int dim, double *yo, double *a1,
     yerr[i] = DP5_E1 * k1[i];
     ynk[i] = yo[i] + DP5_A21 * k1[i];
   }
+  P->t = *to + 0.2 * dt;
   f(P, ynk, a);
   for (i = 0; i < dim; i++) {
     k2[i] = dt * a[i];
     ynk[i] = yo[i] + DP5_A31 * k1[i] + DP5_A32 * k2[i];
   }
+  P->t = *to + 0.3 * dt;
   f(P, ynk, a);
   for (i = 0; i < dim; i++) {
     k3[i] = dt * a[i];
@@ -1735,6 +2147,7 @@ static double dopr54_attempt(rhs_fn f, opot *P, int dim, double *yo, double *a1,
     yerr[i] += DP5_E3 * k3[i];
     ynk[i] = yo[i] + DP5_A41 * k1[i] + DP5_A42 * k2[i] + DP5_A43 * k3[i];
   }
+  P->t = *to + 0.8 * dt;
   f(P, ynk, a);
   for (i = 0; i < dim; i++) {
     k4[i] = dt * a[i];
@@ -1742,6 +2155,7 @@ static double dopr54_attempt(rhs_fn f, opot *P, int dim, double *yo, double *a1,
     yerr[i] += DP5_E4 * k4[i];
     ynk[i] = yo[i] + DP5_A51 * k1[i] + DP5_A52 * k2[i] + DP5_A53 * k3[i] + DP5_A54 * k4[i];
   }
+  P->t = *to + 8. / 9. * dt;
   f(P, ynk, a);
   for (i = 0; i < dim; i++) {
     k5[i] = dt * a[i];
@@ -1750,6 +2164,7 @@ static double dopr54_attempt(rhs_fn f, opot *P, int dim, double *yo, double *a1,
     ynk[i] = yo[i] + DP5_A61 * k1[i] + DP5_A62 * k2[i] + DP5_A63 * k3[i] + DP5_A64 * k4[i] +
              DP5_A65 * k5[i];
   }
+  P->t = *to + dt;
   f(P, ynk, a);
   for (i = 0; i < dim; i++) {
     k6[i] = dt * a[i];
@@ -1759,6 +2174,7 @@ static double dopr54_attempt(rhs_fn f, opot *P, int dim, double *yo, double *a1,
     ynk[i] = yo[i] + DP5_B1 * k1[i] + DP5_B3 * k3[i] + DP5_B4 * k4[i] + DP5_B5 * k5[i] +
              DP5_B6 * k6[i];
   }
+  P->t = *to + dt;
   f(P, ynk, a);
   for (i = 0; i < dim; i++) yerr[i] += DP5_E7 * dt * a[i];
   double s = est_scale(dim, yo, rtol, atol);
@@ -1795,8 +2211,10 @@ static void dopr54(rhs_fn f, opot *P, int dim, const double *yin, int nt, double
   st->err = 0;
   st->nsteps = 0;
   double dt = t[1] - t[0];
-  if (dt_one == DT_SENTINEL) dt_one = rk_est(rk4_onestep, 1. / 5., f, P, dim, yo, dt, rtol, atol);
+  if (dt_one == DT_SENTINEL)
+    dt_one = rk_est(rk4_onestep, 1. / 5., f, P, dim, yo, dt, t[0], rtol, atol);
   double to = t[0];
+  P->t = to;
   f(P, yo, a1);
   long long attempts = 0;
   for (int ii = 0; ii < nt - 1; ii++) {
@@ -1847,6 +2265,7 @@ static void dop853(rhs_fn f, opot *P, int dim, const double *yin, int nt, const 
   st->err = 0;
   st->nsteps = 0;
 
+  P->t = t[0];
   f(P, y0, k1);
   double dnf = 0.0, dny = 0.0, sk, sqr;
   for (i = 0; i < dim; i++) {
@@ -1858,6 +2277,7 @@ static void dop853(rhs_fn f, opot *P, int dim, const double *yin, int nt, const 
   }
   double h = csign(DMIN(sqrt(dny / dnf) * 0.01, fabs(hmax)), pos_neg);
   for (i = 0; i < dim; i++) k3[i] = y0[i] + h * k1[i];
+  P->t = t[0] + h;
   f(P, k3, k2);
   double der2 = 0.0;
   for (i = 0; i < dim; i++) {
@@ -1882,37 +2302,47 @@ static void dop853(rhs_fn f, opot *P, int dim, const double *yin, int nt, const 
     attempts++;
     h = pos_neg * DMAX(fabs(h), 1e3 * uround);
     for (i = 0; i < dim; i++) yy1[i] = y0[i] + h * DP_A21 * k1[i];
+    P->t = t_current + DP_C2 * h;
     f(P, yy1, k2);
     for (i = 0; i < dim; i++) yy1[i] = y0[i] + h * (DP_A31 * k1[i] + DP_A32 * k2[i]);
+    P->t = t_current + DP_C3 * h;
     f(P, yy1, k3);
     for (i = 0; i < dim; i++) yy1[i] = y0[i] + h * (DP_A41 * k1[i] + DP_A43 * k3[i]);
+    P->t = t_current + DP_C4 * h;
     f(P, yy1, k4);
     for (i = 0; i < dim; i++)
       yy1[i] = y0[i] + h * (DP_A51 * k1[i] + DP_A53 * k3[i] + DP_A54 * k4[i]);
+    P->t = t_current + DP_C5 * h;
     f(P, yy1, k5);
     for (i = 0; i < dim; i++)
       yy1[i] = y0[i] + h * (DP_A61 * k1[i] + DP_A64 * k4[i] + DP_A65 * k5[i]);
+    P->t = t_current + DP_C6 * h;
     f(P, yy1, k6);
     for (i = 0; i < dim; i++)
       yy1[i] = y0[i] + h * (DP_A71 * k1[i] + DP_A74 * k4[i] + DP_A75 * k5[i] + DP_A76 * k6[i]);
+    P->t = t_current + DP_C7 * h;
     f(P, yy1, k7);
     for (i = 0; i < dim; i++)
       yy1[i] = y0[i] + h * (DP_A81 * k1[i] + DP_A84 * k4[i] + DP_A85 * k5[i] + DP_A86 * k6[i] +
                             DP_A87 * k7[i]);
+    P->t = t_current + DP_C8 * h;
     f(P, yy1, k8);
     for (i = 0; i < dim; i++)
       yy1[i] = y0[i] + h * (DP_A91 * k1[i] + DP_A94 * k4[i] + DP_A95 * k5[i] + DP_A96 * k6[i] +
                             DP_A97 * k7[i] + DP_A98 * k8[i]);
+    P->t = t_current + DP_C9 * h;
     f(P, yy1, k9);
     for (i = 0; i < dim; i++)
       yy1[i] = y0[i] + h * (DP_A101 * k1[i] + DP_A104 * k4[i] + DP_A105 * k5[i] +
                             DP_A106 * k6[i] + DP_A107 * k7[i] + DP_A108 * k8[i] +
                             DP_A109 * k9[i]);
+    P->t = t_current + DP_C10 * h;
     f(P, yy1, k10);
     for (i = 0; i < dim; i++)
       yy1[i] = y0[i] + h * (DP_A111 * k1[i] + DP_A114 * k4[i] + DP_A115 * k5[i] +
                             DP_A116 * k6[i] + DP_A117 * k7[i] + DP_A118 * k8[i] +
                             DP_A119 * k9[i] + DP_A1110 * k10[i]);
+    P->t = t_current + DP_C11 * h;
     f(P, yy1, k2);
     for (i = 0; i < dim; i++)
       yy1[i] = y0[i] + h * (DP_A121 * k1[i] + DP_A124 * k4[i] + DP_A125 * k5[i] +
@@ -1921,6 +2351,7 @@ static void dop853(rhs_fn f, opot *P, int dim, const double *yin, int nt, const 
     t_old_older = t_old;
     t_old = t_current;
     t_current = t_current + h;
+    P->t = t_current;
     f(P, yy1, k3);
     for (i = 0; i < dim; i++) {
       k4[i] = DP_B1 * k1[i] + DP_B6 * k6[i] + DP_B7 * k7[i] + DP_B8 * k8[i] + DP_B9 * k9[i] +
@@ -1948,6 +2379,7 @@ static void dop853(rhs_fn f, opot *P, int dim, const double *yin, int nt, const 
     if (err <= 1.0) {
       facold = DMAX(err, 1.0e-4);
       st->nsteps++;
+      P->t = t_current;
       f(P, k5, k4);
       for (i = 0; i < dim; i++) {
         rc1[i] = y0[i];
@@ -1969,16 +2401,19 @@ static void dop853(rhs_fn f, opot *P, int dim, const double *yin, int nt, const 
         yy1[i] = y0[i] + h * (DP_A141 * k1[i] + DP_A147 * k7[i] + DP_A148 * k8[i] +
                               DP_A149 * k9[i] + DP_A1410 * k10[i] + DP_A1411 * k2[i] +
                               DP_A1412 * k3[i] + DP_A1413 * k4[i]);
+      P->t = t_old + DP_C14 * h;
       f(P, yy1, k10);
       for (i = 0; i < dim; i++)
         yy1[i] = y0[i] + h * (DP_A151 * k1[i] + DP_A156 * k6[i] + DP_A157 * k7[i] +
                               DP_A158 * k8[i] + DP_A1511 * k2[i] + DP_A1512 * k3[i] +
                               DP_A1513 * k4[i] + DP_A1514 * k10[i]);
+      P->t = t_old + DP_C15 * h;
       f(P, yy1, k2);
       for (i = 0; i < dim; i++)
         yy1[i] = y0[i] + h * (DP_A161 * k1[i] + DP_A166 * k6[i] + DP_A167 * k7[i] +
                               DP_A168 * k8[i] + DP_A169 * k9[i] + DP_A1613 * k4[i] +
                               DP_A1614 * k10[i] + DP_A1615 * k2[i]);
+      P->t = t_old + DP_C16 * h;
       f(P, yy1, k3);
       for (i = 0; i < dim; i++) {
         rc5[i] = h * (rc5[i] + DP_D413 * k4[i] + DP_D414 * k10[i] + DP_D415 * k2[i] +
@@ -2075,6 +2510,7 @@ static void sos_deriv(opot *P, const double *q, double *a)
   double x = q[0], y = q[1], z = q[4] * sinpsi;
   double R = sqrt(x * x + y * y), phi = atan2(y, x);
   double sinphi = y / R, cosphi = x / R, Rf, zf, pt;
+  P->t = q[5]; /* the state carries the time */
   sum3(P, R, z, phi, &Rf, &zf, &pt);
   a[3] = cosphi * Rf - 1. / R * sinphi * pt;
   a[4] = sinphi * Rf + 1. / R * cosphi * pt;
@@ -2121,6 +2557,7 @@ static void sos_planar_derivx(opot *P, const double *q, double *a)
   double sinpsi = sin(q[4]), cospsi = cos(q[4]);
   double x = q[2] * sinpsi, y = q[0];
   double R = sqrt(x * x + y * y), phi = atan2(y, x), sinphi = y / R, cosphi = x / R, Rf, pt;
+  P->t = q[3];
   sum2(P, R, phi, &Rf, &pt);
   a[2] = cosphi * Rf - 1. / R * sinphi * pt;
   a[3] = sinphi * Rf + 1. / R * cosphi * pt;
@@ -2137,6 +2574,7 @@ static void sos_planar_derivy(opot *P, const double *q, double *a)
   double sinpsi = sin(q[4]), cospsi = cos(q[4]);
   double x = q[0], y = q[2] * sinpsi;
   double R = sqrt(x * x + y * y), phi = atan2(y, x), sinphi = y / R, cosphi = x / R, Rf, pt;
+  P->t = q[3];
   sum2(P, R, phi, &Rf, &pt);
   a[2] = cosphi * Rf - 1. / R * sinphi * pt;
   a[3] = sinphi * Rf + 1. / R * cosphi * pt;
@@ -2384,12 +2822,15 @@ EXPORT int oracle_integrate_dxdv(int planar, int nobj, const double *yo, int nt,
 /* Forces and Hessian terms at n points (R, z, phi), for unit tests.
    out[n][9] = Rforce, zforce, phitorque, R2deriv, z2deriv, Rzderiv,
    phi2deriv, Rphideriv, zphideriv; planar: out[n][5] = planarRforce,
-   planarphitorque, planarR2deriv, planarphi2deriv, planarRphideriv. */
+   planarphitorque, planarR2deriv, planarphi2deriv, planarRphideriv; t the
+   time (time-dependent components). */
 EXPORT int oracle_forces(int planar, int n, const double *R, const double *z, const double *phi,
-                         int npot, const int *pot_type, const double *pot_args, double *out)
+                         int npot, const int *pot_type, const double *pot_args, double *out,
+                         double t)
 {
   opot P;
   if (opot_decode(&P, npot, pot_type, pot_args, planar)) return -3;
+  P.t = t;
   for (int i = 0; i < n; i++) {
     if (planar) {
       double Rf, pt, h0, h1, h2;

@@ -90,7 +90,7 @@ def port():
         ]
         lib.oracle_forces.restype = ctypes.c_int
         lib.oracle_forces.argtypes = [ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_int,
-                                      _ip, _dp, _dp]
+                                      _ip, _dp, _dp, ctypes.c_double]
         lib.oracle_potential.restype = ctypes.c_int
         lib.oracle_potential.argtypes = [ctypes.c_int, _dp, _dp, _dp, ctypes.c_int, _ip, _dp, _dp]
         lib.oracle_expint.restype = ctypes.c_double
@@ -284,9 +284,9 @@ def integrate_sos(yo, psi, pot_type, pot_args, method, dpsi=None, rtol=None, ato
     return result, err, None
 
 
-def forces(R, z, phi, pot_type, pot_args, planar=False):
+def forces(R, z, phi, pot_type, pot_args, planar=False, t=0.0):
     """Per-point (Rforce, zforce, phitorque, R2, z2, Rz, phi2, Rphi, zphi)
-    (3D) or (Rforce, phitorque, R2, phi2, Rphi) (planar)."""
+    (3D) or (Rforce, phitorque, R2, phi2, Rphi) (planar), at time t."""
     R = np.ascontiguousarray(R, dtype=np.float64)
     z = np.ascontiguousarray(np.broadcast_to(z, R.shape), dtype=np.float64)
     phi = np.ascontiguousarray(np.broadcast_to(phi, R.shape), dtype=np.float64)
@@ -294,7 +294,7 @@ def forces(R, z, phi, pot_type, pot_args, planar=False):
     pa = np.ascontiguousarray(pot_args, dtype=np.float64)
     out = np.empty((R.size, 5 if planar else 9))
     rc = port().oracle_forces(int(planar), R.size, _ptr(R, _dp), _ptr(z, _dp), _ptr(phi, _dp),
-                              len(pt), _ptr(pt, _ip), _ptr(pa, _dp), _ptr(out, _dp))
+                              len(pt), _ptr(pt, _ip), _ptr(pa, _dp), _ptr(out, _dp), float(t))
     if rc:
         raise ValueError(f"oracle_forces returned {rc}")
     return out

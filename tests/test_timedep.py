@@ -1,0 +1,142 @@
+"""The oracle's DehnenBarPotential (time-dependent) and SCFPotential against
+the reference's own C (oracle/_ref, built from DehnenBarPotential.c and
+SCFPotential.c with the stand-in Gegenbauer / Legendre arrays) and against
+galpy's Python potentials (scipy's special functions).
+
+The time the reference hands each force evaluation follows its steppers'
+own bookkeeping (leapfrog's to + dt/2, the symplectic drifts summed into
+`to`, the RK stage offsets tn + c dt, dop853's t_current + c h and t_old +
+c h, the state's time in a surface of section); the oracle restates it, so
+the comparison is bit for bit."""
+import numpy as np
+import pytest
+
+import timedep_pots as TP
+from oracle import oracle
+
+METHODS = ["leapfrog", "rk4", "rk6", "symplec4", "symplec6", "dopr54", "dop853"]
+needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
+
+
+def ics(n, planar, seed=11):
+    rng = np.random.default_rng(seed)
+    R = rng.uniform(0.5, 1.5, n)
+    vR = rng.normal(0, 0.1, n)
+    vT = rng.uniform(0.8, 1.1, n)
+    phi = rng.uniform(0, 2 * np.pi, n)
+    if planar:
+        return np.stack([R, vR, vT, phi], 1)
+    return np.stack([R, vR, vT, rng.normal(0, 0.1, n), rng.normal(0, 0.1, n), phi], 1)
+
+
+def tol(method):
+    return dict(rtol=1e-10, atol=1e-10) if method in ("dopr54", "dop853") else {}
+
+
+@needs_ref
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", TP.NAMES)
+@pytest.mark.parametrize("method", METHODS)
+def test_orbits_bit_exact_vs_reference_build(name, planar, method):
+    pt, pa = TP.potential(name, planar)
+    yo = ics(8, planar)
+    t = np.linspace(0.0, 8.0, 41)
+    a, ea, _, _ = oracle.integrate(yo, t, pt, pa, method, planar=planar, **tol(method))
+    b, eb, _, _ = oracle.integrate(yo, t, pt, pa, method, planar=planar, impl="ref", **tol(method))
+    np.testing.assert_array_equal(ea, eb)
+    np.testing.assert_array_equal(a, b)
+
+
+@needs_ref
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", ["bar_growing+mw14", "scf_nonaxi"])
+@pytest.mark.parametrize("method", METHODS)
+def test_dxdv_bit_exact_vs_reference_build(name, planar, method):
+    pt, pa = TP.potential(name, planar)
+    dim = 2 if planar else 3
+    rng = np.random.default_rng(5)
+    w = np.concatenate([rng.uniform(0.6, 1.2, (4, dim)), rng.normal(0, 0.2, (4, dim)),
+                        rng.normal(0, 1, (4, 2 * dim))], 1)
+    w[:, dim + 1] += 1.0
+    t = np.linspace(0.0, 4.0, 17)
+    a = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar, **tol(method))[0]
+    b = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar, impl="ref", **tol(method))[0]
+    np.testing.assert_array_equal(a, b)
+
+
+@needs_ref
+@pytest.mark.parametrize("method", ["rk4", "dop853"])
+def test_sos_time_from_state_vs_reference_build(method):
+    """The surface of section's force time is the state's (integrated) time."""
+    pt, pa = TP.potential("bar_growing+mw14")
+    yo = np.concatenate([ics(4, False), np.full((4, 1), 0.5)], 1)
+    psi = np.linspace(0.0, 6 * np.pi, 25)
+    a, _, _ = oracle.integrate_sos(yo, psi, pt, pa, method, **tol(method))
+    b, _, _ = oracle.integrate_sos(yo, psi, pt, pa, method, impl="ref", **tol(method))
+    np.testing.assert_array_equal(a, b)
+
+
+def test_bar_force_follows_time():
+    """The bar's force at a point changes with its pattern rotation and its
+    growth; zero before tform."""
+    pt, pa = TP.potential("bar_growing+mw14")
+    R, z, phi = np.array([0.7]), np.array([0.1]), np.array([0.3])
+    f_early = oracle.forces(R, z, phi, pt[3:], pa[-6:], t=0.5)
+    assert np.all(f_early == 0.0)
+    f1 = oracle.forces(R, z, phi, pt[3:], pa[-6:], t=2.0)
+    f2 = oracle.forces(R, z, phi, pt[3:], pa[-6:], t=2.3)
+    assert np.all(np.abs(f1[0, :3]) > 0) and not np.allclose(f1, f2)
+
+
+def galpy_or_skip():
+    import galpy_stub
+
+    if galpy_stub.import_galpy() is None:
+        pytest.skip("galpy not importable")
+    from galpy import potential as P
+
+    return P
+
+
+@pytest.mark.parametrize("planar", [False, True])
+def test_argument_layouts_match_galpy(planar):
+    P = galpy_or_skip()
+    if planar:
+        from galpy.orbit.integratePlanarOrbit import _parse_pot
+    else:
+        from galpy.orbit.integrateFullOrbit import _parse_pot
+    bar = P.DehnenBarPotential(omegab=1.85, rb=0.8, Af=0.01, tform=-2.0, tsteady=3.0, barphi=0.4)
+    pots = [bar] if not planar else [P.toPlanarPotential(bar)]
+    _, pt, pa, _ = _parse_pot(pots)
+    assert list(pt) == [1]
+    # galpy keeps tform / tsteady in absolute times (given in bar periods)
+    np.testing.assert_array_equal(
+        pa, TP.dehnen_bar_args(bar._amp * bar._af, bar._tform, bar._tsteady, bar._rb,
+                               bar._omegab, bar._barphi))
+    Acos, Asin = TP.scf_coefficients(nonaxi=True)
+    scf = P.SCFPotential(amp=1.0, Acos=Acos, Asin=Asin, a=1.1)
+    _, pt, pa, _ = _parse_pot([scf] if not planar else [P.toPlanarPotential(scf)])
+    assert list(pt) == [24]
+    # galpy folds its spherical-harmonic normalisation into the coefficients
+    np.testing.assert_array_equal(np.asarray(pa),
+                                  TP.scf_args(scf._Acos, scf._Asin, a=scf._a, amp=scf._amp))
+
+
+@pytest.mark.parametrize("nonaxi", [True, False])
+def test_scf_forces_vs_galpy_python(nonaxi):
+    """Forces and second derivatives of the oracle's SCF (own Gegenbauer and
+    Legendre recurrences) against galpy's Python SCFPotential (scipy)."""
+    P = galpy_or_skip()
+    Acos, Asin = TP.scf_coefficients(nonaxi=nonaxi)
+    pot = P.SCFPotential(amp=1.0, Acos=Acos, Asin=Asin, a=1.1)
+    rng = np.random.default_rng(2)
+    R, z, phi = rng.uniform(0.3, 2, 60), rng.normal(0, 0.5, 60), rng.uniform(0, 6.2, 60)
+    args = TP.scf_args(pot._Acos, pot._Asin if nonaxi else None, a=pot._a, amp=pot._amp)
+    got = oracle.forces(R, z, phi, np.array([24], np.int32), np.array(args))
+    names = ["Rforce", "zforce", "phitorque", "R2deriv", "z2deriv", "Rzderiv", "phi2deriv",
+             "Rphideriv", "phizderiv"]
+    for k, nm in enumerate(names):
+        ref = np.array([getattr(pot, nm)(R[i], z[i], phi=phi[i], use_physical=False)
+                        for i in range(R.size)])
+        scale = max(np.abs(ref).max(), 1e-300)
+        assert np.abs(got[:, k] - ref).max() <= 1e-13 * scale, nm

@@ -1,0 +1,69 @@
+"""galpy's (pot_type, pot_args) for the time-dependent DehnenBarPotential and
+the SCFPotential, built without galpy (TEST ONLY): the layouts of
+galpy/orbit/integrateFullOrbit.py (DehnenBar: type 1, (amp * af, tform,
+tsteady, rb, omegab, barphi); SCF: type 24 through _parse_scf_pot in
+integratePlanarOrbit.py, (a, isNonAxi, N, L, M, Nt = 0, amp * Acos,
+amp * Asin if non-axisymmetric, 11 cache slots)).  tests/test_timedep.py
+checks them against galpy's own _parse_pot where galpy is importable."""
+import numpy as np
+
+
+def mw14(planar=False):
+    """MWPotential2014's (types, args) as galpy marshals them, from the
+    package's galpy-free parser."""
+    import galpy_b200 as gb
+
+    _, pt, pa = gb.parse_pot(gb.MWPotential2014(), planar=planar)
+    return [int(x) for x in pt], [float(x) for x in pa]
+
+
+def dehnen_bar_args(amp_af=0.01, tform=-2.0, tsteady=3.0, rb=0.8, omegab=1.85, barphi=0.4):
+    return [amp_af, tform, tsteady, rb, omegab, barphi]
+
+
+def scf_coefficients(N=6, L=5, nonaxi=True, seed=3):
+    """Coefficients (Acos, Asin) of a smooth Hernquist-like expansion: the
+    (0, 0, 0) term 1, the others small; m <= l only, Asin[..., 0] = 0."""
+    rng = np.random.default_rng(seed)
+    M = L if nonaxi else 1
+    Acos = rng.normal(size=(N, L, M)) * 0.05
+    Acos[0, 0, 0] = 1.0
+    Asin = rng.normal(size=(N, L, M)) * 0.05 if nonaxi else None
+    for l in range(L):
+        Acos[:, l, l + 1:] = 0.0
+        if nonaxi:
+            Asin[:, l, l + 1:] = 0.0
+    if nonaxi:
+        Asin[:, :, 0] = 0.0
+    return Acos, Asin
+
+
+def scf_args(Acos, Asin=None, a=1.1, amp=1.0):
+    N, L, M = Acos.shape
+    nonaxi = Asin is not None
+    out = [a, float(nonaxi), float(N), float(L), float(M), 0.0]
+    out.extend((amp * Acos).ravel().tolist())
+    if nonaxi:
+        out.extend((amp * Asin).ravel().tolist())
+    out.extend([-1.0] + [0.0] * 10)
+    return out
+
+
+def potential(name, planar=False):
+    """(pot_type int32, pot_args float64) of a named test potential."""
+    mw_t, mw_a = mw14(planar)
+    if name == "bar+mw14":
+        t, a = mw_t + [1], mw_a + dehnen_bar_args()
+    elif name == "bar_growing+mw14":  # the bar grows during the integration
+        t, a = mw_t + [1], mw_a + dehnen_bar_args(amp_af=0.02, tform=1.0, tsteady=6.0)
+    elif name == "scf_nonaxi":
+        t, a = [24], scf_args(*scf_coefficients(nonaxi=True), a=1.1)
+    elif name == "scf_axi+mn":
+        nb = 3 if planar else 5  # the bulge's argument count
+        t, a = [24, 5], scf_args(*scf_coefficients(nonaxi=False), a=0.9) + mw_a[nb:nb + 3]
+    else:
+        raise KeyError(name)
+    return np.asarray(t, np.int32), np.asarray(a, np.float64)
+
+
+NAMES = ["bar+mw14", "bar_growing+mw14", "scf_nonaxi", "scf_axi+mn"]
