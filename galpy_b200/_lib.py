@@ -154,6 +154,7 @@ SIGNATURES = {
     "galpy_cuda_last_error": (ctypes.c_char_p, []),
     "galpy_cuda_device_count": (_ci, []),
     "galpy_cuda_comp_size": (_ci, []),
+    "galpy_cuda_comp_records": (_ci, [_ci, _ci, _ip, _dp]),
     "galpy_cuda_signature": (_ci, [_ci, _ip]),
     "galpy_cuda_compile_potential": (_ci, [_ci, _ci, _ip, _dp, _ci, _vp]),
     "integrateFullOrbit_cuda": (

@@ -11,6 +11,8 @@
 #include <stddef.h>
 #include <string.h>
 
+#include <vector>
+
 #include "potentials.cuh"
 
 namespace gpc {
@@ -22,6 +24,13 @@ namespace gpc {
 // (-1 without them)
 inline int galpy_nargs(int type, int planar, const double* p = nullptr)
 {
+  if (type == T_SCF) {  // (a, isNonAxi, N, L, M, Nt, coefficients, 11 cache slots)
+    if (!p) return -1;
+    const int nonaxi = (int)p[1], N = (int)p[2], L = (int)p[3], M = (int)p[4];
+    if ((int)p[5] != 0 || N < 1 || L < 1 || M < 1) return -1;  // time-dependent coefficients
+    if (nonaxi && M != L) return -1;
+    return 6 + (1 + nonaxi) * N * L * M + 11;
+  }
   if (is_ellipsoidal(type)) {
     if (!p) return -1;
     const int npsi = (int)p[16];
@@ -43,6 +52,7 @@ inline int galpy_nargs(int type, int planar, const double* p = nullptr)
     case T_KKS: return 3;
     case T_HENONHEILES: return planar ? 1 : -1;  // (amp); a planarPotential only
     case T_KUZMINDISK: return 2;
+    case T_DEHNENBAR: return 6;
     default: return -1;
   }
 }
@@ -175,17 +185,56 @@ inline void share_tables(GpComp* c, int n)
   }
 }
 
-// Compile one group.  Returns 0, -3 (unsupported type) or -1 (bad args).
-// *consumed receives the number of pot_args read.
+// Payload doubles of an SCF component (coefficients with m <= l of the
+// summed orders, then the Gegenbauer recurrence table), from galpy's args.
+inline int scf_payload_len(const double* p)
+{
+  const int nonaxi = (int)p[1], N = (int)p[2], L = (int)p[3];
+  const int Me = nonaxi ? L : 1;
+  int pairs = 0;
+  for (int m = 0; m < Me; m++) pairs += L - m;
+  return pairs * N * (1 + nonaxi) + 4 * L * (N - 1);
+}
+
+// Records one component takes: 1, plus continuation records for an SCF
+// expansion's payload.
+inline int comp_records(int type, const double* p)
+{
+  if (type != T_SCF) return 1;
+  const int len = scf_payload_len(p);
+  return 1 + (len + kPayloadDoubles - 1) / kPayloadDoubles;
+}
+
+// Records of one group (the stride of a parameter group in the device
+// array); -3 (unsupported type) or -1 (bad args).
+inline int group_records(int planar, int npot, const int* pot_type, const double* pot_args)
+{
+  if (npot < 1 || npot > kMaxComp) return -1;
+  const double* p = pot_args;
+  int n = 0;
+  for (int k = 0; k < npot; k++) {
+    const int na = galpy_nargs(pot_type[k], planar, p);
+    if (na < 0) return -3;
+    n += comp_records(pot_type[k], p);
+    p += na;
+  }
+  return n;
+}
+
+// Compile one group into group_records(...) records.  Returns 0, -3
+// (unsupported type) or -1 (bad args).  *consumed receives the number of
+// pot_args read.
 inline int compile_group(int planar, int npot, const int* pot_type, const double* pot_args,
                          GpComp* out, int* consumed)
 {
   if (npot < 1 || npot > kMaxComp) return -1;
   const double* p = pot_args;
+  int rec = 0;  // next record
   for (int k = 0; k < npot; k++) {
     const int type = pot_type[k];
     const int na = galpy_nargs(type, planar, p);
     if (na < 0) return -3;
+    const int nrec = comp_records(type, p);
     GpComp c;
     memset(&c, 0, sizeof(c));
     c.type = type;
@@ -366,6 +415,57 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
       case T_KUZMINDISK:  // (amp, a)
         c.c[1] = p[1];
         break;
+      case T_DEHNENBAR: {  // (amp * af, tform, tsteady, rb, omegab, barphi)
+        if (!(p[3] > 0.0) || p[2] < p[1]) return -1;
+        for (int j = 1; j < 6; j++) c.c[j] = p[j];
+        c.c[6] = p[3] * p[3] * p[3];
+        c.c[7] = p[2] > p[1] ? 1.0 / (p[2] - p[1]) : 0.0;
+        break;
+      }
+      case T_SCF: {  // (a, isNonAxi, N, L, M, 0, Acos[N][L][M], Asin, cache)
+        const int nonaxi = (int)p[1], N = (int)p[2], L = (int)p[3], M = (int)p[4];
+        const int Me = nonaxi ? L : 1;
+        if (!(p[0] > 0.0)) return -1;
+        c.c[0] = p[0];
+        c.c[1] = nonaxi;
+        c.c[2] = N;
+        c.c[3] = L;
+        c.c[4] = Me;
+        std::vector<double> pay;
+        pay.reserve(scf_payload_len(p));
+        const double s4 = sqrt(4.0 * M_PI);
+        const double* Ac = p + 6;
+        const double* As = p + 6 + N * L * M;
+        for (int m = 0; m < Me; m++)
+          for (int l = m; l < L; l++)
+            for (int n = 0; n < N; n++) {
+              const int ci = (n * L + l) * M + m;
+              pay.push_back(s4 * Ac[ci]);
+              if (nonaxi) pay.push_back(s4 * As[ci]);
+            }
+        c.c[5] = (double)pay.size();  // the recurrence table's offset
+        for (int l = 0; l < L; l++) {
+          const long double al = 2.0L * l + 1.5L;
+          for (int n = 0; n + 1 < N; n++) {
+            const long double n1 = n + 1.0L;
+            pay.push_back((double)(2.0L * (n + al) / n1));
+            pay.push_back((double)((n + 2.0L * al - 1.0L) / n1));
+            pay.push_back((double)(2.0L * (n + al + 1.0L) / n1));
+            pay.push_back((double)((n + 2.0L * al + 1.0L) / n1));
+          }
+        }
+        for (int r = 1; r < nrec; r++) {  // continuation records
+          GpComp& q = out[rec + r];
+          memset(&q, 0, sizeof(q));
+          q.type = T_PAYLOAD;
+          double* d = &q.c[0];
+          for (int j = 0; j < kPayloadDoubles; j++) {
+            const size_t i = (size_t)(r - 1) * kPayloadDoubles + j;
+            d[j] = i < pay.size() ? pay[i] : 0.0;
+          }
+        }
+        break;
+      }
       case T_FLATPOWER: {  // (amp, alpha, q^2, core^2); planar (amp, alpha, core^2)
         const double alpha = p[1], q2 = planar ? 1.0 : p[2], core2 = planar ? p[2] : p[3];
         if (!(q2 > 0.0)) return -1;
@@ -381,7 +481,8 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
       for (int j = 0; j < kChebC; j++) c.chebf[i][j] = (float)c.cheb[i][j];
     for (int i = 0; i < kBinSub; i++)
       for (int j = 0; j < kChebC; j++) c.binf[i][j] = (float)c.bin[i][j];
-    out[k] = c;
+    out[rec] = c;
+    rec += nrec;
     p += na;
   }
   if (consumed) *consumed = (int)(p - pot_args);

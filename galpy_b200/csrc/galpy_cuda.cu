@@ -197,19 +197,19 @@ static int signature_of(int npot, const int* pot_type)
   if (npot == 3 && pot_type[0] == T_PSWC && pot_type[1] == T_MN && pot_type[2] == T_NFW)
     return GALPY_CUDA_SIG_MW14;
   for (int k = 0; k < npot; k++)
-    if (is_ellipsoidal(pot_type[k])) return GALPY_CUDA_SIG_GENERIC;
+    if (needs_full_list(pot_type[k])) return GALPY_CUDA_SIG_GENERIC;
   return GALPY_CUDA_SIG_COMMON;
 }
 
 // The signature a launch runs with: GALPY_CUDA_SIG_COMMON falls back to the
-// full run-time list when the host copy of the records shows an ellipsoidal
-// component.
+// full run-time list when the host copy of the records shows a component
+// only that list carries (ellipsoidal, DehnenBar, SCF).
 static int launch_signature(const galpy_cuda_launch* L)
 {
   if (L->signature != GALPY_CUDA_SIG_COMMON || !L->comps_host) return L->signature;
   const GpComp* hc = static_cast<const GpComp*>(L->comps_host);
   for (int k = 0; k < L->ncomp; k++)
-    if (is_ellipsoidal(hc[k].type)) return GALPY_CUDA_SIG_GENERIC;
+    if (needs_full_list(hc[k].type)) return GALPY_CUDA_SIG_GENERIC;
   return GALPY_CUDA_SIG_COMMON;
 }
 
@@ -782,6 +782,27 @@ struct SplitCtl {
 };
 
 // Blocking host-pointer integration shared by the galpy-facing entry points.
+// One potential's records (a component may take continuation records: an
+// SCF expansion's coefficients).  Variational runs need the tidal tensor,
+// which the device does not evaluate for an SCF expansion.
+static int compile_records(int planar, int var, int npot, const int* pot_type,
+                           const double* pot_args, std::vector<GpComp>& comps)
+{
+  const int n = group_records(planar, npot, pot_type, pot_args);
+  if (n == -3) return set_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
+  if (n < 1) return set_error(GALPY_CUDA_ERR_ARG, "invalid potential arguments");
+  if (var)
+    for (int k = 0; k < npot; k++)
+      if (pot_type[k] == T_SCF)
+        return set_error(GALPY_CUDA_ERR_POTENTIAL,
+                         "variational runs in an SCF potential are not implemented on the GPU");
+  comps.assign((size_t)n, GpComp{});
+  const int rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
+  if (rc == -3) return set_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
+  if (rc) return set_error(GALPY_CUDA_ERR_ARG, "invalid potential arguments");
+  return GALPY_CUDA_OK;
+}
+
 // w: rectangular initial states [nobj][nv]; result written in galpy's layout
 // (cylindrical rows) unless rect_out.
 static int run_host(int planar, int var, long long nobj, const double* w, int nv, int nt,
@@ -795,10 +816,9 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
   if (!method_supported(odeint_type))
     return set_error(GALPY_CUDA_ERR_METHOD, "odeint_type not implemented on the GPU");
   if (nobj == 0) return GALPY_CUDA_OK;
-  std::vector<GpComp> comps(npot > 0 ? npot : 1);
-  rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
-  if (rc == -3) return set_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
-  if (rc) return set_error(GALPY_CUDA_ERR_ARG, "invalid potential arguments");
+  std::vector<GpComp> comps;
+  rc = compile_records(planar, var, npot, pot_type, pot_args, comps);
+  if (rc) return rc;
   cudaMemPool_t pool = nullptr;
   rc = library_pool(&pool);
   if (rc) return rc;
@@ -872,7 +892,7 @@ static int run_host(int planar, int var, long long nobj, const double* w, int nv
   L.nsteps = static_cast<long long*>(dsteps.p);
   L.comps = dcomp.p;
   L.comps_host = comps.data();
-  L.ncomp = npot;
+  L.ncomp = (int)comps.size();
   L.dt = dt;
   L.rtol = rtol;
   L.atol = atol;
@@ -1090,14 +1110,13 @@ static int run_host_split(int planar, int var, long long nobj, const double* w, 
                     atol, result, err, odeint_type, cb, o, rect_out, system);
   if (!method_supported(odeint_type))
     return set_error(GALPY_CUDA_ERR_METHOD, "odeint_type not implemented on the GPU");
-  std::vector<GpComp> comps(npot > 0 ? npot : 1);
-  rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
-  if (rc == -3) return set_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
-  if (rc) return set_error(GALPY_CUDA_ERR_ARG, "invalid potential arguments");
+  std::vector<GpComp> comps;
+  rc = compile_records(planar, var, npot, pot_type, pot_args, comps);
+  if (rc) return rc;
 
   const int nd = (int)devs.size();
   std::vector<double> cost((size_t)nobj);
-  orbit_costs(planar, nobj, w, nv, nt, t, indiv_t, comps.data(), npot, nullptr, system,
+  orbit_costs(planar, nobj, w, nv, nt, t, indiv_t, comps.data(), (int)comps.size(), nullptr, system,
               cost.data());
   std::vector<long long> bounds(nd + 1);
   cut_ranges(nobj, cost.data(), nd, bounds.data());
@@ -1583,6 +1602,15 @@ int galpy_cuda_signature(int npot, const int* pot_type)
   return signature_of(npot, pot_type);
 }
 
+int galpy_cuda_comp_records(int planar, int npot, const int* pot_type, const double* pot_args)
+{
+  if (!pot_type || !pot_args) return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
+  const int n = group_records(planar, npot, pot_type, pot_args);
+  if (n == -3) return set_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
+  if (n < 1) return set_error(GALPY_CUDA_ERR_ARG, "invalid potential arguments");
+  return n;
+}
+
 int galpy_cuda_compile_potential(int planar, int npot, const int* pot_type,
                                  const double* pot_args, int ngroup, void* out)
 {
@@ -1590,14 +1618,19 @@ int galpy_cuda_compile_potential(int planar, int npot, const int* pot_type,
     return set_error(GALPY_CUDA_ERR_ARG, "invalid arguments");
   GpComp* c = static_cast<GpComp*>(out);
   const double* p = pot_args;
+  const int nrec = group_records(planar, npot, pot_type, pot_args);
+  if (nrec == -3) return set_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
+  if (nrec < 1) return set_error(GALPY_CUDA_ERR_ARG, "invalid potential arguments");
   for (int g = 0; g < ngroup; g++) {
     int used = 0;
-    int rc = compile_group(planar, npot, pot_type, p, c + (size_t)g * npot, &used);
+    if (group_records(planar, npot, pot_type, p) != nrec)  // groups share one stride
+      return set_error(GALPY_CUDA_ERR_ARG, "parameter groups of different sizes");
+    int rc = compile_group(planar, npot, pot_type, p, c + (size_t)g * nrec, &used);
     if (rc == -3) return set_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
     if (rc) return set_error(GALPY_CUDA_ERR_ARG, "invalid potential arguments");
     p += used;
   }
-  share_tables(c, ngroup * npot);
+  share_tables(c, ngroup * nrec);
   return GALPY_CUDA_OK;
 }
 
@@ -1614,18 +1647,14 @@ int galpy_cuda_split_orbits(int planar, long long nobj, const double* w, int nv,
     for (long long i = 0; i < nobj; i++)
       if (group[i] < 0 || group[i] >= ngroup)
         return set_error(GALPY_CUDA_ERR_ARG, "group index out of range");
-  std::vector<GpComp> comps((size_t)npot * ngroup);
-  const double* p = pot_args;
-  for (int g = 0; g < ngroup; g++) {
-    int used = 0;
-    int rc = compile_group(planar, npot, pot_type, p, comps.data() + (size_t)g * npot, &used);
-    if (rc == -3)
-      return set_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
-    if (rc) return set_error(GALPY_CUDA_ERR_ARG, "invalid potential arguments");
-    p += used;
-  }
+  const int nrec = galpy_cuda_comp_records(planar, npot, pot_type, pot_args);
+  if (nrec < 0) return nrec;
+  std::vector<GpComp> comps((size_t)nrec * ngroup);
+  const int rc = galpy_cuda_compile_potential(planar, npot, pot_type, pot_args, ngroup,
+                                              comps.data());
+  if (rc) return rc;
   std::vector<double> cost((size_t)nobj);
-  orbit_costs(planar, nobj, w, nv, nt, t, indiv_t, comps.data(), npot, group,
+  orbit_costs(planar, nobj, w, nv, nt, t, indiv_t, comps.data(), nrec, group,
               GALPY_CUDA_SYS_ORBIT, cost.data());
   cut_ranges(nobj, cost.data(), nparts, bounds);
   return GALPY_CUDA_OK;

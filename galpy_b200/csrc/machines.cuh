@@ -22,11 +22,14 @@
 //   rk4 / rk6 + estimators      galpy/util/bovy_rk.c:66-480
 //   dopr54                      galpy/util/bovy_rk.c:501-760
 //   dop853                      galpy/util/leung_dop853.c:231-517
-// Differences by design: the time variable of the reference's symplectic and
-// RK loops is not tracked (the supported potentials are static); DOP853
-// skips its three dense-output stages in steps that contain no output time
-// (their results are only used for output); every orbit has an attempt budget
-// and stops on a non-finite state instead of looping forever.
+// Each machine also reports the time at which the reference evaluates the
+// force of its current point (tpoint: the reference stepper's own
+// bookkeeping, so that a time-dependent potential sees the same times); the
+// kernel asks for it only when the component list reads the time.
+// Differences by design: DOP853 skips its three dense-output stages in
+// steps that contain no output time (their results are only used for
+// output); every orbit has an attempt budget and stops on a non-finite
+// state instead of looping forever.
 #pragma once
 #include <type_traits>
 
@@ -175,26 +178,27 @@ GPC_HD GPC_FI void write_nan_rows(const OutSpec& o, long long i, int from)
 // ------------------------------------------------------------------------
 template <int D, int PREC, bool VAR, class POT = DynPot>
 GPC_HD GPC_FI void eval_force(const GpComp* comp, int ncomp, const double* q, double* a,
-                              const double* scal = nullptr)
+                              const double* scal = nullptr, double t = 0.0)
 {
   if (!VAR) {
     if (PREC == PREC_FP64) {
       double ax, ay, az = 0.0;
-      accel<double, D == 2, POT>(comp, ncomp, q[0], q[1], D == 3 ? q[2] : 0.0, ax, ay, az, scal);
+      accel<double, D == 2, POT>(comp, ncomp, q[0], q[1], D == 3 ? q[2] : 0.0, ax, ay, az, scal,
+                                 t);
       a[0] = ax;
       a[1] = ay;
       if (D == 3) a[2] = az;
     } else {
       float ax, ay, az = 0.f;
       accel<float, D == 2, POT>(comp, ncomp, (float)q[0], (float)q[1], D == 3 ? (float)q[2] : 0.f,
-                                ax, ay, az, scal);
+                                ax, ay, az, scal, t);
       a[0] = ax;
       a[1] = ay;
       if (D == 3) a[2] = az;
     }
   } else {
     double ax, ay, az, K[6];
-    accel_tidal<D == 2>(comp, ncomp, q[0], q[1], D == 3 ? q[2] : 0.0, ax, ay, az, K);
+    accel_tidal<D == 2>(comp, ncomp, q[0], q[1], D == 3 ? q[2] : 0.0, ax, ay, az, K, t);
     a[0] = ax;
     a[1] = ay;
     if (D == 3) {
@@ -350,6 +354,11 @@ struct SymplecticMachine : OrbitCommon {
   S qw[NQ], pw[NQ];       // state of the running advance
   double q11[D], p11[D];  // estimator: the single-step result (base orbit)
   double dt, init_dt, h, sq, sp, rtol, atol;
+  // the reference's time `to` (bovy_symplecticode.c): symplec4 / symplec6
+  // add each drift's length to it and kick at it (their estimators take it
+  // back by dt after each trial); leapfrog kicks at to + dt/2 and adds dt
+  // per step (its estimator kicks at t0 + dt/2, t0 + dt/4, t0 + 3 dt/4)
+  double tk;
   long long nrun, kick, nkick;
   int sub, phase;
   // double-float form: the step's kick and drift coefficients, converted
@@ -369,6 +378,7 @@ struct SymplecticMachine : OrbitCommon {
     sub = 0;
     nkick = C::kKicks * nstep;
     const double c = C::first(h);
+    if (ORD != 2) tk += c;
     if constexpr (kDF) {
       static_assert(C::kKicks <= 3, "double-float state: leapfrog and symplec4");
       kc0 = df_of(C::kick(0, h));
@@ -411,7 +421,17 @@ struct SymplecticMachine : OrbitCommon {
   {
     const long long ndt = (long long)(init_dt / dt);
     phase = MAIN;
+    tk = t[0];
     start(dt, ndt < 1 ? 1 : ndt);
+  }
+
+  // time of the force evaluation of the current kick
+  GPC_HD GPC_FI double tpoint(const double* /*y*/, int /*slot*/) const
+  {
+    if (ORD != 2) return tk;
+    if (phase == MAIN) return tk + dt / 2.;
+    if (phase == EST_FULL) return t[0] + dt / 2.;
+    return kick == 0 ? t[0] + dt / 4. : t[0] + 3. * dt / 4.;
   }
 
   // w: (x, v) or (x, v, dx, dv) rectangular
@@ -446,6 +466,7 @@ struct SymplecticMachine : OrbitCommon {
       return;
     }
     init_dt = tt[1] - tt[0];
+    tk = tt[0];
     if (dt_in == kDtSentinel) {
       dt = init_dt;
       sq = est_scale(qo, D, 1, rtol, atol);
@@ -489,6 +510,10 @@ struct SymplecticMachine : OrbitCommon {
 #pragma unroll
       for (int k = 0; k < NQ; k++) qw[k] = qw[k] + dc * pw[k];
     }
+    if (ORD != 2)
+      tk += C::drift(sub, last, h);
+    else if (phase == MAIN)
+      tk = tk + dt;
     kick++;
     sub = sub < C::kKicks - 1 ? sub + 1 : 0;
     if (last) advance_done(out);
@@ -497,6 +522,7 @@ struct SymplecticMachine : OrbitCommon {
   template <class W>
   GPC_HD void advance_done(W& out)
   {
+    if (phase != MAIN && ORD != 2) tk -= dt;  // the estimator's `to -= dt`
     if (phase == EST_FULL) {
 #pragma unroll
       for (int k = 0; k < D; k++) {
@@ -650,6 +676,7 @@ struct OrbitSystem {
   static constexpr int N = VAR ? 4 * D : 2 * D;  // ODE dimension
   static constexpr int NA = VAR ? 2 * D : D;     // force argument / result size
   static constexpr int kRow = ROW_ORBIT;         // output row conversion
+  static constexpr int kTimeIndex = -1;          // the time is the machine's, not in y
   // force argument: positions (and deviation positions) of (x, v[, dx, dv])
   GPC_HD GPC_FI static void pos(const double* y, double* q)
   {
@@ -681,6 +708,7 @@ struct OrbitSystem {
 struct SosSystem {
   static constexpr int N = 7, NA = 3;
   static constexpr int kRow = ROW_SOS;
+  static constexpr int kTimeIndex = 5;  // the force's time is the state's
   GPC_HD GPC_FI static void pos(const double* y, double* q)
   {
     q[0] = y[0];
@@ -709,6 +737,7 @@ template <int SURF>
 struct PlanarSosSystem {
   static constexpr int N = 5, NA = 2;
   static constexpr int kRow = SURF == 0 ? ROW_SOS_PLANAR_X : ROW_SOS_PLANAR_Y;
+  static constexpr int kTimeIndex = 3;
   GPC_HD GPC_FI static void pos(const double* y, double* q)
   {
     const double w = y[2] * sin(y[4]);
@@ -752,8 +781,29 @@ struct RKMachine : OrbitCommon {
   double y1[N];    // estimator: the one-step result
   double kk[ORD == 6 ? 5 : 1][N];  // rk6 stage increments k1..k5
   double dt, init_dt, h, s, rtol, atol;
+  double tk;  // the reference's `to` of the main loop (bovy_rk.c: += dt per step)
   long long nrun, step;
   int stage, phase;
+
+  // time of the current stage's force evaluation: the step's start tb
+  // (rk4_estimate_step's to, to, to + dt/2 for its three trial steps) plus
+  // the stage offset of bovy_rk4_onestep / bovy_rk6_onestep
+  GPC_HD GPC_FI double tpoint(const double* y, int /*slot*/) const
+  {
+    if constexpr (SYS::kTimeIndex >= 0) {
+      return y[SYS::kTimeIndex];
+    } else {
+      const double tb = phase == MAIN ? tk : (phase == EST_C ? t[0] + dt / 2. : t[0]);
+      if (stage == 0) return tb;
+      if (ORD == 4) return stage == 3 ? tb + h : tb + h / 2.;
+      switch (stage) {
+        case 1: case 3: return tb + h / 3.;
+        case 2: return tb + 2. * h / 3.;
+        case 4: case 5: return tb + h / 2.;
+        default: return tb + h;
+      }
+    }
+  }
 
   GPC_HD GPC_FI void start(const double* from, double hh)
   {
@@ -769,6 +819,7 @@ struct RKMachine : OrbitCommon {
     nrun = ndt < 1 ? 1 : ndt;
     step = 0;
     phase = MAIN;
+    tk = t[0];
     start(yo, dt);
   }
 
@@ -863,6 +914,7 @@ struct RKMachine : OrbitCommon {
       yo[k] = yn1[k];
       fin = fin && isfinite(yn1[k]);
     }
+    tk += dt;
     nsteps++;
     attempts++;
     if (++step < nrun) {
@@ -944,6 +996,30 @@ struct Dopr54Machine : OrbitCommon {
   double to, dtout, init_to, dt_one, init_dt_one, h, s, rtol, atol, est_dt, est_init;
   int stage, phase;
   bool forced;
+
+  // time of the current force evaluation: the step estimation's rk4 trial
+  // steps from to (to + est_dt/2 for the third), the first derivative at to,
+  // then bovy_dopr54_actualstep's to + c_i dt (c = 1/5, 3/10, 4/5, 8/9, 1, 1)
+  GPC_HD GPC_FI double tpoint(const double* y, int /*slot*/) const
+  {
+    if constexpr (SYS::kTimeIndex >= 0) {
+      return y[SYS::kTimeIndex];
+    } else {
+      if (phase < FSAL0) {
+        const double tb = phase == EST_C ? to + est_dt / 2. : to;
+        if (stage == 0) return tb;
+        return stage == 3 ? tb + h : tb + h / 2.;
+      }
+      if (phase == FSAL0) return to;
+      switch (stage) {
+        case 1: return to + 0.2 * h;
+        case 2: return to + 0.3 * h;
+        case 3: return to + 0.8 * h;
+        case 4: return to + 8. / 9. * h;
+        default: return to + h;
+      }
+    }
+  }
 
   GPC_HD GPC_FI void est_start(const double* from, double hh)
   {
@@ -1402,6 +1478,44 @@ struct Dop853Machine : OrbitCommon {
     return iout < nt - 1 && pos_neg * t[iout + 1] < pos_neg * t_current;
   }
 
+  // c_s of the stage whose input is evaluated (leung_dop853.c:351-462)
+  GPC_HD GPC_FI static double stage_c(int stage)
+  {
+    using namespace dp;
+    switch (stage) {
+      case 2: return c2;
+      case 3: return c3;
+      case 4: return c4;
+      case 5: return c5;
+      case 6: return c6;
+      case 7: return c7;
+      case 8: return c8;
+      case 9: return c9;
+      case 10: return c10;
+      case 11: return c11;
+      case ST_S14: return c14;
+      case ST_S15: return c15;
+      default: return c16;
+    }
+  }
+
+  // time of the current force evaluation as the reference passes it:
+  // t0 and t0 + h for the start-up, t_current + c_s h for stages 2..11,
+  // t_current + h for stage 12, the new t_current for the FSAL derivative,
+  // t_old + c_s h for the dense-output stages (a lane idle in the slot:
+  // any time, its result is discarded)
+  GPC_HD GPC_FI double tpoint(const double* y, int slot) const
+  {
+    if constexpr (SYS::kTimeIndex >= 0) {
+      return y[SYS::kTimeIndex];
+    } else {
+      if (!active_in(slot) || stage == ST_INIT1 || stage == ST_FSAL) return t_current;
+      if (stage == ST_INIT2 || stage == 12) return t_current + h;
+      if (stage >= ST_S14) return t_old + stage_c(stage) * h;
+      return t_current + stage_c(stage) * h;
+    }
+  }
+
   template <class W>
   GPC_HD void consume(const double* y, const double* a, W& out, int slot)
   {
@@ -1595,6 +1709,16 @@ struct Dop853Machine : OrbitCommon {
     for (int i = 0; i < N; i++) y[i] = q[(0 * N + i) * kQueueSlots + p] + hq * acc[i];
   }
 
+  // Time of dense stage `stage` of request p (t_old + c_s h of its step).
+  GPC_HD GPC_FI double req_tpoint(const double* y, int stage, const double* q, int p) const
+  {
+    if constexpr (SYS::kTimeIndex >= 0) {
+      return y[SYS::kTimeIndex];
+    } else {
+      return q[(11 * N + 1) * kQueueSlots + p] + stage_c(stage) * q[(11 * N) * kQueueSlots + p];
+    }
+  }
+
   // Derivative of dense stage `stage` at request p: stages 14 and 15 are
   // kept for the next stage inputs; stage 16 completes the rows.
   template <class W>
@@ -1758,7 +1882,7 @@ GPC_HD void run_orbit_queued(M& m, F& force, W& out, double* q, const double* tt
   while (!m.done) {
     m.point(y, slot);
     M::pos(y, qq);
-    force(qq, a);
+    force(qq, a, m.tpoint(y, slot));
     m.consume(y, a, out, slot);
     if (slot == 11 && m.want_enqueue) {
       m.write_request(q, 0, orbit);
@@ -1767,7 +1891,7 @@ GPC_HD void run_orbit_queued(M& m, F& force, W& out, double* q, const double* tt
       for (int stage = 14; stage <= 16; stage++) {
         m.req_point(y, stage, q, 0);
         M::pos(y, qq);
-        force(qq, a);
+        force(qq, a, m.req_tpoint(y, stage, q, 0));
         m.req_consume(y, a, stage, q, 0, tt, out);
       }
     }
@@ -1776,8 +1900,8 @@ GPC_HD void run_orbit_queued(M& m, F& force, W& out, double* q, const double* tt
   fill_unreached_rows(m, out);
 }
 
-// Per-orbit driver used by the kernels and by the host test harness: run one
-// machine to completion with the force evaluated by `force`.
+// Per-orbit driver used by the host test harness: run one machine to
+// completion with the force evaluated by `force` (positions, result, time).
 template <class M, class F, class W>
 GPC_HD void run_orbit(M& m, F& force, W& out)
 {
@@ -1786,7 +1910,7 @@ GPC_HD void run_orbit(M& m, F& force, W& out)
   while (!m.done) {
     m.point(y, slot);
     M::pos(y, q);
-    force(q, a);
+    force(q, a, m.tpoint(y, slot));
     m.consume(y, a, out, slot);
     slot = M::next_slot(slot, m.wants_dense());
   }

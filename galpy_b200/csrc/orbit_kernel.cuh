@@ -233,16 +233,19 @@ __device__ __forceinline__ void queued_loop(const KArgs& A, double* slot_store, 
       double y[M::NY], qq[M::NA], a[M::NA];
       long long o = i, opos = pos;
       const GpComp* cp = comps;
+      double tf = 0.0;  // the force's time (read by time-dependent component lists only)
       if (dense) {  // the request's output position, orbit and parameter group
         opos = reinterpret_cast<const long long*>(q)[(11 * M::N + 2) * QS + p];
         o = orbit_at(A, opos);
         cp = A.comps + (A.group ? (long long)A.group[o] * A.ncomp : 0LL);
         m.req_point(y, slot + 2, q, p);
+        if constexpr (POT::kTimeDep) tf = m.req_tpoint(y, slot + 2, q, p);
       } else {
         m.point(y, slot);
+        if constexpr (POT::kTimeDep) tf = m.tpoint(y, slot);
       }
       M::pos(y, qq);
-      eval_force<D, PREC, VAR, POT>(cp, A.ncomp, qq, a, A.scal);
+      eval_force<D, PREC, VAR, POT>(cp, A.ncomp, qq, a, A.scal, tf);
       Rows rows{&A.out, opos};
       if (dense) {
         m.req_consume(y, a, slot + 2, q, p, A.t + (A.indiv_t ? o * (long long)A.nt : 0LL), rows);
@@ -370,8 +373,10 @@ __global__ void __launch_bounds__(128, MINB) orbit_kernel(const __grid_constant_
     if (!m.done) {
       double y[M::NY], q[M::NA], a[M::NA];
       m.point(y, slot);
+      double tf = 0.0;
+      if constexpr (POT::kTimeDep) tf = m.tpoint(y, slot);
       M::pos(y, q);
-      eval_force<D, PREC, VAR, POT>(comps, A.ncomp, q, a, A.scal);
+      eval_force<D, PREC, VAR, POT>(comps, A.ncomp, q, a, A.scal, tf);
       Rows rows{&A.out, pos};
       m.consume(y, a, rows, slot);
     }

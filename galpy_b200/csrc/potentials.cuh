@@ -747,6 +747,10 @@ GPC_HD GPC_FI T sph_force_factor(int type, const S& sc, T r2)
 enum : int { MIX_NONE = 0, MIX_TAIL32 = 1, MIX_F32BULGE = 2 };
 
 // gamma*(a, u) with the interpolant's tail in float32 (poly12_tail32).
+}  // namespace gpc
+#include "potentials_td.cuh"
+namespace gpc {
+
 GPC_HD GPC_FI double gamma_star_tail32(const GpComp* __restrict__ tp, double u, double scale)
 {
   const double s = u * scale;
@@ -758,7 +762,7 @@ GPC_HD GPC_FI double gamma_star_tail32(const GpComp* __restrict__ tp, double u, 
 
 template <typename T, bool PLANAR, int TYPE, class S, int MIX = MIX_NONE>
 GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T y, T z, T z2,
-                              T R2, T r2, T& gR, T& gz, T& gyx, AddAcc<T>& a0)
+                              T R2, T r2, T& gR, T& gz, T& gyx, AddAcc<T>& a0, double t)
 {
   const int type = TYPE >= 0 ? TYPE : ldg(&cp->type);
   const T amp = T(sc[0]);
@@ -886,6 +890,24 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
       if (!PLANAR) a0.z += z > T(0) ? g * az : (z < T(0) ? -g * az : T(0));
       break;
     }
+    case T_PAYLOAD:  // an SCF component's coefficients
+      break;
+    case T_DEHNENBAR:
+    case T_SCF: {  // in float64; carried by the full run-time list only
+      if constexpr (TYPE == kRunTimeAll) {
+        double ax, ay, az;
+        if (type == T_DEHNENBAR)
+          dbar_accel<PLANAR>(cp, t, (double)x, (double)y, (double)z, ax, ay, az);
+        else
+          scf_accel<PLANAR>(cp, (double)x, (double)y, (double)z, ax, ay, az);
+        a0.x += T(ax);
+        a0.y += T(ay);
+        if (!PLANAR) a0.z += T(az);
+      } else {
+        gR = T(NAN);
+      }
+      break;
+    }
     case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
     case T_POWERTRI: case T_TWOPOWERTRI: {  // in float64
       if constexpr (TYPE == kRunTimeCommon) {
@@ -911,17 +933,20 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
 }
 
 // Run-time component list (any combination of the supported types).
+// The full list also carries the time-dependent DehnenBar and the SCF
+// expansion: its force reads the evaluation time (kTimeDep).
 struct DynPot {
   static constexpr bool kDirectScalars = false;
   static constexpr bool kAdditive = true;  // a component may add to a0
+  static constexpr bool kTimeDep = true;
   template <typename T, bool PLANAR>
   GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, const double* /*scal*/, int ncomp,
                                 T x, T y, T z, T z2, T R2, T r2, T& gR, T& gz, T& gyx,
-                                AddAcc<T>& a0)
+                                AddAcc<T>& a0, double t)
   {
     for (int k = 0; k < ncomp; k++)
       comp_accel<T, PLANAR, kRunTimeAll>(comp + k, ScalarsGlobal{comp + k}, x, y, z, z2, R2, r2,
-                                         gR, gz, gyx, a0);
+                                         gR, gz, gyx, a0, t);
   }
 };
 
@@ -932,14 +957,15 @@ struct DynPot {
 struct DynPotCommon {
   static constexpr bool kDirectScalars = false;
   static constexpr bool kAdditive = true;
+  static constexpr bool kTimeDep = false;
   template <typename T, bool PLANAR>
   GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, const double* /*scal*/, int ncomp,
                                 T x, T y, T z, T z2, T R2, T r2, T& gR, T& gz, T& gyx,
-                                AddAcc<T>& a0)
+                                AddAcc<T>& a0, double /*t*/)
   {
     for (int k = 0; k < ncomp; k++)
       comp_accel<T, PLANAR, kRunTimeCommon>(comp + k, ScalarsGlobal{comp + k}, x, y, z, z2, R2,
-                                            r2, gR, gz, gyx, a0);
+                                            r2, gR, gz, gyx, a0, 0.0);
   }
 };
 
@@ -952,20 +978,21 @@ struct FixedPot {
   static constexpr bool kDirectScalars = DIRECT;
   static constexpr bool kAdditive =
       ((TYPES == T_HENONHEILES || TYPES == T_KUZMINDISK || is_ellipsoidal(TYPES)) || ...);
+  static constexpr bool kTimeDep = false;
   template <typename T, bool PLANAR>
   GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, const double* scal, int /*ncomp*/,
                                 T x, T y, T z, T z2, T R2, T r2, T& gR, T& gz, T& gyx,
-                                AddAcc<T>& a0)
+                                AddAcc<T>& a0, double /*t*/)
   {
     int k = 0;
     if (DIRECT) {
       ((comp_accel<T, PLANAR, TYPES>(comp + k, ScalarsDirect{scal + kScalarStride * k}, x, y, z,
-                                     z2, R2, r2, gR, gz, gyx, a0),
+                                     z2, R2, r2, gR, gz, gyx, a0, 0.0),
         ++k),
        ...);
     } else {
       ((comp_accel<T, PLANAR, TYPES>(comp + k, ScalarsGlobal{comp + k}, x, y, z, z2, R2, r2, gR,
-                                     gz, gyx, a0),
+                                     gz, gyx, a0, 0.0),
         ++k),
        ...);
     }
@@ -983,21 +1010,22 @@ template <bool DIRECT, int MIX, int... TYPES>
 struct MixedPot {
   static constexpr bool kDirectScalars = DIRECT;
   static constexpr bool kAdditive = false;
+  static constexpr bool kTimeDep = false;
   template <typename T, bool PLANAR>
   GPC_HD GPC_FI static void sum(const GpComp* __restrict__ comp, const double* scal, int /*ncomp*/,
                                 T x, T y, T z, T z2, T R2, T r2, T& gR, T& gz, T& gyx,
-                                AddAcc<T>& a0)
+                                AddAcc<T>& a0, double /*t*/)
   {
     int k = 0;
     if (DIRECT) {
       ((comp_accel<T, PLANAR, TYPES, ScalarsDirect, MIX>(
             comp + k, ScalarsDirect{scal + kScalarStride * k}, x, y, z, z2, R2, r2, gR, gz, gyx,
-            a0),
+            a0, 0.0),
         ++k),
        ...);
     } else {
       ((comp_accel<T, PLANAR, TYPES, ScalarsGlobal, MIX>(comp + k, ScalarsGlobal{comp + k}, x,
-                                                         y, z, z2, R2, r2, gR, gz, gyx, a0),
+                                                         y, z, z2, R2, r2, gR, gz, gyx, a0, 0.0),
         ++k),
        ...);
     }
@@ -1006,18 +1034,19 @@ struct MixedPot {
 template <bool DIRECT, int MIX>
 using MW14MixedPot = MixedPot<DIRECT, MIX, T_PSWC, T_MN, T_NFW>;
 
-// Acceleration at (x, y, z); PLANAR evaluates galpy's planar potential (the
-// 3D potential in the plane z = 0) and leaves az untouched.
+// Acceleration at (x, y, z) and time t (read by time-dependent components
+// only); PLANAR evaluates galpy's planar potential (the 3D potential in the
+// plane z = 0) and leaves az untouched.
 template <typename T, bool PLANAR, class POT = DynPot>
 GPC_HD GPC_FI void accel(const GpComp* __restrict__ comp, int ncomp, T x, T y, T z, T& ax, T& ay,
-                         T& az, const double* scal = nullptr)
+                         T& az, const double* scal = nullptr, double t = 0.0)
 {
   const T R2 = x * x + y * y;
   const T z2 = PLANAR ? T(0) : z * z;
   const T r2 = R2 + z2;
   T gR = T(0), gz = T(0), gyx = T(0);
   AddAcc<T> a0{T(0), T(0), T(0)};
-  POT::template sum<T, PLANAR>(comp, scal, ncomp, x, y, z, z2, R2, r2, gR, gz, gyx, a0);
+  POT::template sum<T, PLANAR>(comp, scal, ncomp, x, y, z, z2, R2, r2, gR, gz, gyx, a0, t);
   ax = x * gR;
   ay = y * (gR + gyx);
   if (!PLANAR) az = z * gz;
@@ -1132,7 +1161,8 @@ GPC_HD inline void sph_derivs(const GpComp* __restrict__ cp, int type, double am
 
 template <bool PLANAR>
 GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, double x, double y,
-                               double z, double& ax, double& ay, double& az, double K[6])
+                               double z, double& ax, double& ay, double& az, double K[6],
+                               double t = 0.0)
 {
   if (PLANAR) z = 0.0;
   const double R2 = x * x + y * y, z2 = z * z, r2 = R2 + z2;
@@ -1302,6 +1332,14 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
         K[5] -= amp * (d15 - 3.0 * az * az * d25);
         break;
       }
+      case T_PAYLOAD:
+        break;
+      case T_DEHNENBAR:
+        dbar_tidal<PLANAR>(cp, t, x, y, z, ax0, ay0, az0, K);
+        break;
+      case T_SCF:  // no tidal tensor on the device: the host refuses such runs
+        gR = NAN;
+        break;
       case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
       case T_POWERTRI: case T_TWOPOWERTRI: {
         double fx, fy, fz;
@@ -1476,6 +1514,17 @@ GPC_HD inline double potential_value(const GpComp* __restrict__ comp, int ncomp,
         phi += ell_value(cp, ldg(&cp->type), x, y, z);
         break;
       case T_TWOPOWERTRI:  // psi needs the Gauss hypergeometric function 2F1: not carried
+        phi += NAN;
+        break;
+      case T_PAYLOAD:
+        break;
+      case T_SCF: {
+        double ax, ay, az, p;
+        scf_accel<false>(cp, x, y, z, ax, ay, az, &p);
+        phi += p;
+        break;
+      }
+      case T_DEHNENBAR:  // time-dependent: not evaluated here (the host refuses it)
         phi += NAN;
         break;
       default:

@@ -1,0 +1,253 @@
+// galpy_b200/csrc/potentials_td.cuh
+//
+// Device forces of the time-dependent DehnenBarPotential (galpy type 1,
+// potential_c_ext/DehnenBarPotential.c) and of the SCFPotential with static
+// coefficients (type 24, potential_c_ext/SCFPotential.c), evaluated in
+// Cartesian form.  Included by potentials.cuh; used by the full run-time
+// component list only.
+//
+// DehnenBar.  Phi = A s(t) cos 2(phi - Omega t - phi_b) (R/r)^2 g(r), with
+// g = (r/rb)^3 - 2 inside rb and -(rb/r)^3 outside, and s(t) the quintic
+// growth factor between tform and tsteady.  Since R^2 cos 2(phi - B/2) =
+// cB (x^2 - y^2) + 2 sB x y with B = 2 (Omega t + phi_b), the potential is
+// A s h(r) Q(x, y): h = g / r^2 (r/rb^3 - 2/r^2 inside, -rb^3/r^5 outside)
+// times a quadratic form -- no angle, no division by R, and its Cartesian
+// gradient and Hessian follow in closed form.
+//
+// SCF.  Phi = sum_{n,l,m} (Acos cos m phi + Asin sin m phi) P_l^m(cos theta)
+// phiTilde_nl(r), phiTilde_nl = -(a r)^l / (a + r)^(2l+1) C_n^(2l+3/2)(xi),
+// xi = (r - a) / (r + a) (Hernquist & Ostriker 1992).  The sums run m
+// outer, l inner, n innermost, each family by its three-term recurrence, so
+// no array is held per thread: cos / sin m phi by the angle-addition
+// recurrence from (x, y) / R; P_l^m and dP_l^m / dtheta upward in l from
+// P_m^m = -(2m - 1) sin(theta) P_{m-1}^{m-1} (Condon-Shortley phase) and its
+// theta derivative; C_n^alpha and C_n^(alpha+1) (dC_n^alpha / dxi = 2 alpha
+// C_{n-1}^(alpha+1)) upward in n with the coefficients tabulated on the host.
+#pragma once
+#include <cstddef>
+
+namespace gpc {
+
+enum : int { T_DEHNENBAR = 1, T_SCF = 24 };
+// Continuation record of a component whose data does not fit one record
+// (an SCF expansion's coefficients): skipped by every component loop.
+enum : int { T_PAYLOAD = -100 };
+
+// Types that only the full run-time component list carries.
+GPC_HD GPC_FI constexpr bool needs_full_list(int t)
+{
+  return is_ellipsoidal(t) || t == T_DEHNENBAR || t == T_SCF || t == T_PAYLOAD;
+}
+
+// Doubles of payload per continuation record: the record after its
+// (type, tab) header.
+constexpr int kPayloadDoubles = (int)((sizeof(GpComp) - offsetof(GpComp, c)) / sizeof(double));
+static_assert(offsetof(GpComp, c) == 8 && (sizeof(GpComp) - 8) % sizeof(double) == 0,
+              "continuation records are read as a run of doubles");
+
+// Payload value j of the component record cp (its continuation records
+// follow it).
+GPC_HD GPC_FI double payload(const GpComp* __restrict__ cp, int j)
+{
+  const int rec = j / kPayloadDoubles, off = j - rec * kPayloadDoubles;
+  return ldg(&cp[1 + rec].c[0] + off);
+}
+
+// ---- DehnenBar ------------------------------------------------------------
+// Record: c0 amp (galpy's amp * af), c1 tform, c2 tsteady, c3 rb, c4 omegab,
+// c5 barphi, c6 rb^3, c7 1 / (tsteady - tform).
+struct BarParts {
+  double A;           // amp * s(t)
+  double cB, sB;      // cos, sin of 2 (omegab t + barphi)
+  double h, hp_r;     // h(r), h'(r) / r
+  double hpp;         // h''(r)
+};
+
+GPC_HD GPC_FI BarParts dbar_parts(const GpComp* __restrict__ cp, double t, double r2)
+{
+  BarParts b;
+  const double tform = ldg(&cp->c[1]), tsteady = ldg(&cp->c[2]);
+  double s = 1.0;
+  if (t < tform) {
+    s = 0.0;
+  } else if (t < tsteady) {
+    const double xi = 2.0 * (t - tform) * ldg(&cp->c[7]) - 1.0, x2 = xi * xi;
+    s = ((3.0 / 16.0 * x2 - 5.0 / 8.0) * x2 + 15.0 / 16.0) * xi + 0.5;
+  }
+  b.A = ldg(&cp->c[0]) * s;
+  sincos(2.0 * (ldg(&cp->c[4]) * t + ldg(&cp->c[5])), &b.sB, &b.cB);
+  const double rb = ldg(&cp->c[3]), rb3 = ldg(&cp->c[6]);
+  const double ir2 = 1.0 / r2, ir = sqrt(ir2), ir4 = ir2 * ir2;
+  if (r2 <= rb * rb) {
+    const double r = r2 * ir;
+    b.h = r / rb3 - 2.0 * ir2;
+    b.hp_r = ir / rb3 + 4.0 * ir4;
+    b.hpp = -12.0 * ir4;
+  } else {
+    const double ir5 = ir4 * ir;
+    b.h = -rb3 * ir5;
+    b.hp_r = 5.0 * rb3 * ir5 * ir2;
+    b.hpp = -30.0 * rb3 * ir5 * ir2;
+  }
+  return b;
+}
+
+// Acceleration -grad Phi at time t (PLANAR: the 3D potential at z = 0).
+template <bool PLANAR>
+GPC_HD GPC_FI void dbar_accel(const GpComp* __restrict__ cp, double t, double x, double y,
+                              double z, double& ax, double& ay, double& az)
+{
+  const double zz = PLANAR ? 0.0 : z;
+  const BarParts b = dbar_parts(cp, t, x * x + y * y + zz * zz);
+  const double Q = b.cB * (x * x - y * y) + 2.0 * b.sB * x * y;
+  const double Qx = 2.0 * (b.cB * x + b.sB * y), Qy = 2.0 * (b.sB * x - b.cB * y);
+  const double f = -b.A * b.hp_r * Q;
+  ax = f * x - b.A * b.h * Qx;
+  ay = f * y - b.A * b.h * Qy;
+  az = PLANAR ? 0.0 : f * zz;
+}
+
+// Acceleration and K = -grad grad Phi (K[0] xx, 1 xy, 2 yy, 3 xz, 4 yz, 5 zz),
+// added to ax.. and K.
+template <bool PLANAR>
+GPC_HD GPC_FI void dbar_tidal(const GpComp* __restrict__ cp, double t, double x, double y,
+                              double z, double& ax, double& ay, double& az, double K[6])
+{
+  const double zz = PLANAR ? 0.0 : z;
+  const double r2 = x * x + y * y + zz * zz;
+  const BarParts b = dbar_parts(cp, t, r2);
+  const double Q = b.cB * (x * x - y * y) + 2.0 * b.sB * x * y;
+  const double Qx = 2.0 * (b.cB * x + b.sB * y), Qy = 2.0 * (b.sB * x - b.cB * y);
+  const double f = -b.A * b.hp_r * Q;
+  ax += f * x - b.A * b.h * Qx;
+  ay += f * y - b.A * b.h * Qy;
+  if (!PLANAR) az += f * zz;
+  // Hessian: A [(h'' - h'/r) x_i x_j / r^2 Q + h'/r (delta_ij Q + x_i Q_j +
+  // x_j Q_i) + h Q_ij], Q_xx = 2 cB, Q_xy = 2 sB, Q_yy = -2 cB
+  const double c = b.A * (b.hpp - b.hp_r) * Q / r2, d = b.A * b.hp_r, e = b.A * b.h;
+  const double dQ = d * Q;
+  K[0] -= c * x * x + dQ + 2.0 * d * x * Qx + 2.0 * e * b.cB;
+  K[1] -= c * x * y + d * (x * Qy + y * Qx) + 2.0 * e * b.sB;
+  K[2] -= c * y * y + dQ + 2.0 * d * y * Qy - 2.0 * e * b.cB;
+  if (!PLANAR) {
+    K[3] -= c * x * zz + d * zz * Qx;
+    K[4] -= c * y * zz + d * zz * Qy;
+    K[5] -= c * zz * zz + dQ;
+  }
+}
+
+// ---- SCF --------------------------------------------------------------------
+// Record: c0 a, c1 1 if non-axisymmetric, c2 N, c3 L, c4 the number of m
+// orders summed (L if non-axisymmetric, else 1), c5 the payload offset of
+// the recurrence table.  Payload (continuation records): for m < c4, l in
+// [m, L), n < N: sqrt(4 pi) Acos_nlm (and sqrt(4 pi) Asin_nlm next to it if
+// non-axisymmetric); then for l < L, n < N - 1 the Gegenbauer recurrence
+// C_{n+1} = p0 xi C_n - p1 C_{n-1} of alpha = 2l + 3/2 (p0, p1) and of
+// alpha + 1 (p2, p3), 4 doubles.
+struct ScfSums {
+  double pot;           // Phi
+  double dr, dth, dph;  // dPhi/dr, dPhi/dtheta, dPhi/dphi
+};
+
+GPC_HD inline ScfSums scf_sums(const GpComp* __restrict__ cp, double r, double ct, double st,
+                               double cph, double sph)
+{
+  const double a = ldg(&cp->c[0]);
+  const bool nonaxi = ldg(&cp->c[1]) != 0.0;
+  const int N = (int)ldg(&cp->c[2]), L = (int)ldg(&cp->c[3]), Me = (int)ldg(&cp->c[4]);
+  const int rec0 = (int)ldg(&cp->c[5]);
+  const double ar = a + r, iar = 1.0 / ar, xi = (r - a) * iar;
+  const double q = r * a * iar * iar;  // the factor between l and l + 1
+  ScfSums S{0.0, 0.0, 0.0, 0.0};
+  double cm = 1.0, sm = 0.0;                         // cos, sin m phi
+  double pmm = 1.0, dmm = 0.0;                       // P_m^m, dP_m^m / dtheta
+  double rtm = -iar, rt1m = iar * iar * iar / r;     // radial prefactors at l = m
+  int j = 0;                                         // payload cursor (coefficients)
+  for (int m = 0; m < Me; m++) {
+    if (m > 0) {
+      const double f = -(2.0 * m - 1.0);
+      const double pn = f * st * pmm, dn = f * (ct * pmm + st * dmm);
+      pmm = pn;
+      dmm = dn;
+      const double cn = cm * cph - sm * sph;
+      sm = sm * cph + cm * sph;
+      cm = cn;
+      rtm *= q;
+      rt1m *= q;
+    }
+    double p1 = 0.0, d1 = 0.0, p0 = pmm, d0 = dmm;  // P_{l-1}, P_l (and d/dtheta)
+    double rt = rtm, rt1 = rt1m;
+    for (int l = m; l < L; l++) {
+      if (l > m) {
+        double pn, dn;
+        if (l == m + 1) {
+          pn = (2.0 * m + 1.0) * ct * p0;
+          dn = (2.0 * m + 1.0) * (ct * d0 - st * p0);
+        } else {
+          const double il = 1.0 / (double)(l - m), c2 = 2.0 * l - 1.0, c3 = l + m - 1.0;
+          pn = (c2 * ct * p0 - c3 * p1) * il;
+          dn = (c2 * (ct * d0 - st * p0) - c3 * d1) * il;
+        }
+        p1 = p0;
+        d1 = d0;
+        p0 = pn;
+        d0 = dn;
+        rt *= q;
+        rt1 *= q;
+      }
+      // radial sums over n with the Gegenbauer recurrences of alpha = 2l + 3/2
+      const double alpha2 = 4.0 * l + 3.0;  // 2 alpha
+      const int tb = rec0 + 4 * l * (N - 1);
+      double Cp = 0.0, C = 1.0, Ep = 0.0, E = 1.0;
+      double ac = payload(cp, j), as = nonaxi ? payload(cp, j + 1) : 0.0;
+      j += nonaxi ? 2 : 1;
+      double Sc = ac, Ss = as, Dc = 0.0, Ds = 0.0;
+      for (int n = 1; n < N; n++) {
+        const int k = tb + 4 * (n - 1);
+        const double Cn = payload(cp, k) * xi * C - payload(cp, k + 1) * Cp;
+        const double dC = alpha2 * E;  // 2 alpha C_{n-1}^(alpha+1)
+        const double En = payload(cp, k + 2) * xi * E - payload(cp, k + 3) * Ep;
+        Cp = C;
+        C = Cn;
+        Ep = E;
+        E = En;
+        ac = payload(cp, j);
+        as = nonaxi ? payload(cp, j + 1) : 0.0;
+        j += nonaxi ? 2 : 1;
+        Sc += ac * Cn;
+        Ss += as * Cn;
+        Dc += ac * dC;
+        Ds += as * dC;
+      }
+      const double U = cm * Sc + sm * Ss, V = cm * Dc + sm * Ds;
+      const double W = (double)m * (cm * Ss - sm * Sc);
+      const double rad = ((2.0 * l + 1.0) * r * ar - l * ar * ar) * U - 2.0 * a * r * V;
+      S.pot += p0 * rt * U;
+      S.dr += p0 * rt1 * rad;
+      S.dth += d0 * rt * U;
+      S.dph += p0 * rt * W;
+    }
+  }
+  return S;
+}
+
+// Acceleration -grad Phi (PLANAR: at z = 0); pot receives Phi if non-null.
+template <bool PLANAR>
+GPC_HD inline void scf_accel(const GpComp* __restrict__ cp, double x, double y, double z,
+                             double& ax, double& ay, double& az, double* pot = nullptr)
+{
+  const double zz = PLANAR ? 0.0 : z;
+  const double R2 = x * x + y * y, r2 = R2 + zz * zz, R = sqrt(R2), r = sqrt(r2);
+  const double iR = R > 0.0 ? 1.0 / R : 0.0, ir = 1.0 / r;
+  const double cph = R > 0.0 ? x * iR : 1.0, sph = R > 0.0 ? y * iR : 0.0;
+  const ScfSums S = scf_sums(cp, r, zz * ir, R * ir, cph, sph);
+  if (pot) *pot = S.pot;
+  // dPhi/dx_i = Phi_r x_i / r + Phi_theta dtheta/dx_i + Phi_phi dphi/dx_i,
+  // theta = atan2(R, z): dtheta/dR = z / r^2, dtheta/dz = -R / r^2
+  const double gr = S.dr * ir, gth = S.dth * ir * ir, gph = S.dph * iR;
+  ax = -(gr * x + gth * zz * cph - gph * sph);
+  ay = -(gr * y + gth * zz * sph + gph * cph);
+  az = PLANAR ? 0.0 : -(gr * zz - gth * R);
+}
+
+}  // namespace gpc

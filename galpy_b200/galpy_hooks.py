@@ -38,7 +38,7 @@ import numpy as np
 
 from .integrate import (CUDA_METHODS, integrateFullOrbit_cuda, integrateFullOrbit_sos_cuda,
                         integratePlanarOrbit_cuda, integratePlanarOrbit_sos_cuda)
-from .potentials import SUPPORTED_TYPES
+from .potentials import SUPPORTED_TYPES, T_SCF, TIME_DEPENDENT_TYPES
 
 _installed = {}
 
@@ -47,16 +47,35 @@ def _is_cuda(method):
     return isinstance(method, str) and method.lower() in CUDA_METHODS
 
 
-def _supported(pot, planar):
+def _supported(pot, planar, purpose="integrate"):
+    """Whether the engine carries this potential for `purpose`: "integrate"
+    (orbits, surfaces of section), "variational" (no SCF expansion: the
+    device has no tidal tensor for it) or "potential" (values at points,
+    evaluated without a time: no time-dependent component).  An SCF
+    expansion must have static coefficients."""
     try:
         if planar:
             from galpy.orbit.integratePlanarOrbit import _parse_pot
         else:
             from galpy.orbit.integrateFullOrbit import _parse_pot
-        npot, pot_type, _, tfuncs = _parse_pot(pot)
+        npot, pot_type, pot_args, tfuncs = _parse_pot(pot)
     except Exception:
         return False
-    return len(tfuncs) == 0 and all(int(t) in SUPPORTED_TYPES for t in pot_type)
+    types = [int(t) for t in pot_type]
+    if len(tfuncs) or not all(t in SUPPORTED_TYPES for t in types):
+        return False
+    if purpose == "variational" and T_SCF in types:
+        return False
+    if purpose == "potential" and any(t in TIME_DEPENDENT_TYPES for t in types):
+        return False
+    if T_SCF in types:  # time-dependent SCF coefficients are not carried
+        from . import _lib
+
+        pt = np.ascontiguousarray(types, np.int32)
+        pa = np.ascontiguousarray(pot_args, np.float64)
+        return _lib.lib().galpy_cuda_comp_records(
+            int(planar), len(types), pt.ctypes.data_as(_lib._ip), pa.ctypes.data_as(_lib._dp)) > 0
+    return True
 
 
 def _pad_phi(yo, full_dim):
@@ -292,7 +311,8 @@ def _wrap_variational(orig, O):
         if pot is None:
             pot = getattr(self, "_pot", None)
         planar = self.dim() == 2
-        if pot is not None and _supported(O.toPlanarPotential(pot) if planar else pot, planar):
+        if pot is not None and _supported(O.toPlanarPotential(pot) if planar else pot, planar,
+                                          "variational"):
             with _EngineAsC(O):
                 return orig(*ba.args, **ba.kwargs)
         ba.arguments["method"] = method[: -len("_cuda")] + "_c"
@@ -322,7 +342,7 @@ def _route_potential_sum(orig, planar):
         if not plain or np.size(R) < DEVICE_POTENTIAL_MIN_POINTS:
             return orig(pot, R, *args, **kwargs)
         try:
-            if not _supported(pot, planar):
+            if not _supported(pot, planar, "potential"):
                 return orig(pot, R, *args, **kwargs)
         except Exception:
             return orig(pot, R, *args, **kwargs)

@@ -301,15 +301,21 @@ def integrate_dxdv_batch(pot, w, t, int_method, planar=False, dt=None, rtol=None
 
 def compile_potential(pot, planar=False, ngroup=1):
     """Compiled device records (bytes) of a potential, or of ngroup parameter
-    groups when pot is (pot_type, pot_args) with ngroup argument blocks."""
+    groups when pot is (pot_type, pot_args) with ngroup argument blocks, and
+    the number of records per group (the launches' ncomp)."""
     npot, pot_type, pot_args = parse_pot(pot, planar=planar)
     size = _lib.lib().galpy_cuda_comp_size()
-    buf = np.zeros(size * npot * ngroup, dtype=np.uint8)
+    # records per group: one per component, plus an SCF expansion's
+    # continuation records (the launch's ncomp)
+    nrec = _lib.lib().galpy_cuda_comp_records(int(planar), npot, pot_type.ctypes.data_as(_ip),
+                                              pot_args.ctypes.data_as(_dp))
+    _lib.check(min(nrec, 0))
+    buf = np.zeros(size * nrec * ngroup, dtype=np.uint8)
     rc = _lib.lib().galpy_cuda_compile_potential(
         int(planar), npot, pot_type.ctypes.data_as(_ip), pot_args.ctypes.data_as(_dp), ngroup,
         buf.ctypes.data_as(ctypes.c_void_p))
     _lib.check(rc)
-    return buf, npot
+    return buf, nrec
 
 
 def signature(pot, planar=False):

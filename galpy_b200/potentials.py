@@ -7,7 +7,8 @@ The engine integrates in the potentials galpy hands to C as pot_type codes
 (Jaffe), 14 (Isochrone),
 17 (Plummer), 18 (PseudoIsothermal), 20 (Burkert), 33
 (DehnenCoreSpherical), 34 (DehnenSpherical), 35 (HomogeneousSphere), 40
-(Null), 41 (Einasto) and 46 (ExpTruncNFW) -- the parsing is
+(Null), 41 (Einasto) and 46 (ExpTruncNFW), the time-dependent 1
+(DehnenBar) and 24 (SCF, static coefficients) -- the parsing is
 galpy/orbit/integrateFullOrbit.py:43-614 (3D) and
 galpy/orbit/integratePlanarOrbit.py:33-663 (planar).
 
@@ -34,8 +35,13 @@ T_KUZMINDISK = 19
 # EllipsoidalPotential family: TriaxialHernquist, TriaxialNFW, TriaxialJaffe,
 # PerfectEllipsoid, TriaxialGaussian, PowerTriaxial, TwoPowerTriaxial
 ELLIPSOIDAL_TYPES = (21, 22, 23, 30, 37, 38, 43)
+# DehnenBarPotential (its force depends on the time) and SCFPotential (the
+# Hernquist-Ostriker expansion; static coefficients only)
+T_DEHNENBAR, T_SCF = 1, 24
+TIME_DEPENDENT_TYPES = (T_DEHNENBAR,)
 SUPPORTED_TYPES = (T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC, T_FLATPOWER,
-                   T_KKS, T_HENONHEILES, T_KUZMINDISK) + SPHERICAL_TYPES + ELLIPSOIDAL_TYPES
+                   T_KKS, T_HENONHEILES, T_KUZMINDISK, T_DEHNENBAR, T_SCF) + SPHERICAL_TYPES + \
+    ELLIPSOIDAL_TYPES
 
 
 class _Potential:

@@ -120,8 +120,15 @@ typedef struct galpy_cuda_opts {
                               repeat (its ranges then run concurrently on that device) */
 } galpy_cuda_opts;
 
-/* Compiled potential record size in bytes (one per component). */
+/* Compiled potential record size in bytes. */
 int galpy_cuda_comp_size(void);
+
+/* Records one potential group compiles to: one per component, plus
+ * continuation records that hold an SCF expansion's coefficients (galpy
+ * type 24); the stride of a parameter group in the compiled array and the
+ * launch's ncomp.  Returns the count, or GALPY_CUDA_ERR_POTENTIAL /
+ * GALPY_CUDA_ERR_ARG. */
+int galpy_cuda_comp_records(int planar, int npot, const int *pot_type, const double *pot_args);
 
 /* Signature of a component-type list (GALPY_CUDA_SIG_*), for the device
  * entry point's launch.signature. */
@@ -129,8 +136,9 @@ int galpy_cuda_signature(int npot, const int *pot_type);
 
 /* Translate galpy's (pot_type, pot_args) for ngroup potential groups with the
  * same component types (pot_args holds ngroup consecutive argument blocks)
- * into compiled records written to out (host memory of
- * ngroup*npot*galpy_cuda_comp_size() bytes).  Returns 0 or
+ * into compiled records written to out (host memory of ngroup *
+ * galpy_cuda_comp_records(...) * galpy_cuda_comp_size() bytes; every group
+ * must compile to the same number of records).  Returns 0 or
  * GALPY_CUDA_ERR_POTENTIAL / GALPY_CUDA_ERR_ARG. */
 int galpy_cuda_compile_potential(int planar, int npot, const int *pot_type,
                                  const double *pot_args, int ngroup, void *out);

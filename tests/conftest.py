@@ -143,16 +143,16 @@ class Harness:
         assert rc == 0, rc
         return out, err, ns
 
-    def forces(self, x, y, z, pot_type, pot_args, planar=False):
+    def forces(self, x, y, z, pot_type, pot_args, planar=False, t=0.0):
         x, y, z = (np.ascontiguousarray(v, np.float64) for v in (x, y, z))
         n = len(x)
         acc, tid, a32 = np.zeros((n, 3)), np.zeros((n, 6)), np.zeros((n, 3))
         pt = np.ascontiguousarray(pot_type, np.int32)
         pa = np.ascontiguousarray(pot_args, np.float64)
-        rc = self.lib.harness_forces(int(planar), n, x.ctypes.data_as(_dp), y.ctypes.data_as(_dp),
-                                     z.ctypes.data_as(_dp), len(pt), pt.ctypes.data_as(_ip),
-                                     pa.ctypes.data_as(_dp), acc.ctypes.data_as(_dp),
-                                     tid.ctypes.data_as(_dp), a32.ctypes.data_as(_dp))
+        rc = self.lib.harness_forces_at(
+            int(planar), n, x.ctypes.data_as(_dp), y.ctypes.data_as(_dp), z.ctypes.data_as(_dp),
+            ctypes.c_double(t), len(pt), pt.ctypes.data_as(_ip), pa.ctypes.data_as(_dp),
+            acc.ctypes.data_as(_dp), tid.ctypes.data_as(_dp), a32.ctypes.data_as(_dp))
         assert rc == 0, rc
         return acc, tid, a32
 

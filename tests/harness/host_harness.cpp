@@ -13,6 +13,16 @@
 using namespace gpc;
 
 namespace {
+// one group's compiled records (a component may take continuation records)
+int records(int planar, int npot, const int* pot_type, const double* pot_args,
+            std::vector<GpComp>& comps)
+{
+  const int n = group_records(planar, npot, pot_type, pot_args);
+  if (n < 1) return n < 0 ? n : -1;
+  comps.assign((size_t)n, GpComp{});
+  return compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
+}
+
 struct Rows {
   double* out;
   int nv, nt;
@@ -28,9 +38,9 @@ struct Force {
   const GpComp* c;
   int n;
   double scal[kMaxComp * kScalarStride];  // the kernel-parameter copy of the scalars
-  void operator()(const double* q, double* a) const
+  void operator()(const double* q, double* a, double t) const
   {
-    eval_force<D, PREC, VAR, POT>(c, n, q, a, scal);
+    eval_force<D, PREC, VAR, POT>(c, n, q, a, scal, t);
   }
 };
 
@@ -40,7 +50,7 @@ void run_all(int nobj, const double* w, int nt, const double* t, int indiv_t, co
              int* err, long long* nsteps)
 {
   Force<D, PREC, VAR, POT> f{comps, ncomp, {}};
-  for (int k = 0; k < ncomp; k++)
+  for (int k = 0; k < ncomp && k < kMaxComp; k++)
     for (int j = 0; j < kScalarStride; j++) f.scal[k * kScalarStride + j] = comps[k].c[j];
   std::vector<double> store((size_t)M::kSlotDoubles * kSlotStride + 1);
   for (long long i = 0; i < nobj; i++) {
@@ -84,14 +94,15 @@ extern "C" int harness_integrate(int planar, int var, int method, int prec, int 
                                  double rtol, double atol, long long max_att, double* out,
                                  int* err, long long* nsteps)
 {
-  std::vector<GpComp> comps(npot);
-  int rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
+  std::vector<GpComp> comps;
+  int rc = records(planar, npot, pot_type, pot_args, comps);
   if (rc) return rc;
   const GpComp* c = comps.data();
   // the kernels' compile-time MWPotential2014 specialisation
   const bool mw14 = npot == 3 && pot_type[0] == T_PSWC && pot_type[1] == T_MN &&
                     pot_type[2] == T_NFW;
-#define HARNESS_ARGS method, nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol, max_att, out, err, nsteps
+  const int nrec = (int)comps.size();
+#define HARNESS_ARGS method, nobj, w, nt, t, indiv_t, c, nrec, dt, rtol, atol, max_att, out, err, nsteps
   if (var) return planar ? dispatch<2, PREC_FP64, true, DynPot>(HARNESS_ARGS)
                          : dispatch<3, PREC_FP64, true, DynPot>(HARNESS_ARGS);
   if (planar) {
@@ -117,7 +128,7 @@ static void run_dop853_queued(int nobj, const double* w, int nt, const double* t
 {
   using M = Dop853Machine<D, false>;
   Force<D, PREC_FP64, false, POT> f{comps, ncomp, {}};
-  for (int k = 0; k < ncomp; k++)
+  for (int k = 0; k < ncomp && k < kMaxComp; k++)
     for (int j = 0; j < kScalarStride; j++) f.scal[k * kScalarStride + j] = comps[k].c[j];
   std::vector<double> store((size_t)M::kSlotDoubles * kSlotStride + 1);
   std::vector<double> q((size_t)M::kQueueFields * M::kQueueSlots);
@@ -138,24 +149,24 @@ extern "C" int harness_dop853_queued(int planar, int nobj, const double* w, int 
                                      const double* pot_args, double rtol, double atol,
                                      long long max_att, double* out, int* err, long long* nsteps)
 {
-  std::vector<GpComp> comps(npot);
-  int rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
+  std::vector<GpComp> comps;
+  int rc = records(planar, npot, pot_type, pot_args, comps);
   if (rc) return rc;
   const bool mw14 = npot == 3 && pot_type[0] == T_PSWC && pot_type[1] == T_MN &&
                     pot_type[2] == T_NFW;
   if (planar) {
     if (mw14)
-      run_dop853_queued<2, MW14Pot>(nobj, w, nt, t, indiv_t, comps.data(), npot, rtol, atol,
+      run_dop853_queued<2, MW14Pot>(nobj, w, nt, t, indiv_t, comps.data(), (int)comps.size(), rtol, atol,
                                     max_att, out, err, nsteps);
     else
-      run_dop853_queued<2, DynPot>(nobj, w, nt, t, indiv_t, comps.data(), npot, rtol, atol,
+      run_dop853_queued<2, DynPot>(nobj, w, nt, t, indiv_t, comps.data(), (int)comps.size(), rtol, atol,
                                    max_att, out, err, nsteps);
   } else {
     if (mw14)
-      run_dop853_queued<3, MW14Pot>(nobj, w, nt, t, indiv_t, comps.data(), npot, rtol, atol,
+      run_dop853_queued<3, MW14Pot>(nobj, w, nt, t, indiv_t, comps.data(), (int)comps.size(), rtol, atol,
                                     max_att, out, err, nsteps);
     else
-      run_dop853_queued<3, DynPot>(nobj, w, nt, t, indiv_t, comps.data(), npot, rtol, atol,
+      run_dop853_queued<3, DynPot>(nobj, w, nt, t, indiv_t, comps.data(), (int)comps.size(), rtol, atol,
                                    max_att, out, err, nsteps);
   }
   return 0;
@@ -196,11 +207,12 @@ extern "C" int harness_integrate_sos(int system, int method, int nobj, const dou
                                      long long max_att, double* out, int* err, long long* nsteps)
 {
   const int planar = system != 1;
-  std::vector<GpComp> comps(npot);
-  int rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
+  std::vector<GpComp> comps;
+  int rc = records(planar, npot, pot_type, pot_args, comps);
   if (rc) return rc;
   const GpComp* c = comps.data();
-#define SOS_ARGS method, nobj, w, nt, t, indiv_t, c, npot, dt, rtol, atol, max_att, out, err, nsteps
+  const int nrec = (int)comps.size();
+#define SOS_ARGS method, nobj, w, nt, t, indiv_t, c, nrec, dt, rtol, atol, max_att, out, err, nsteps
   if (system == 1) return run_sos<SosSystem, 3>(SOS_ARGS);
   if (system == 2) return run_sos<PlanarSosSystem<0>, 2>(SOS_ARGS);
   if (system == 3) return run_sos<PlanarSosSystem<1>, 2>(SOS_ARGS);
@@ -227,10 +239,11 @@ extern "C" int harness_potential_in(int planar, int n, const double* x, const do
                                     const double* z, int npot, const int* pot_type,
                                     const double* pot_args, double* out)
 {
-  std::vector<GpComp> comps(npot);
-  int rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
+  std::vector<GpComp> comps;
+  int rc = records(planar, npot, pot_type, pot_args, comps);
   if (rc) return rc;
-  for (int i = 0; i < n; i++) out[i] = potential_value(comps.data(), npot, x[i], y[i], z[i]);
+  const int nrec = (int)comps.size();
+  for (int i = 0; i < n; i++) out[i] = potential_value(comps.data(), nrec, x[i], y[i], z[i]);
   return 0;
 }
 
@@ -241,43 +254,55 @@ extern "C" int harness_potential(int n, const double* x, const double* y, const 
   return harness_potential_in(0, n, x, y, z, npot, pot_type, pot_args, out);
 }
 
-extern "C" int harness_forces(int planar, int n, const double* x, const double* y,
-                              const double* z, int npot, const int* pot_type,
-                              const double* pot_args, double* acc /*[n][3]*/,
-                              double* tidal /*[n][6] or NULL*/, double* acc32 /*[n][3] or NULL*/)
+// accelerations (tidal tensors, FP32 accelerations) at points at time t
+extern "C" int harness_forces_at(int planar, int n, const double* x, const double* y,
+                                 const double* z, double t, int npot, const int* pot_type,
+                                 const double* pot_args, double* acc /*[n][3]*/,
+                                 double* tidal /*[n][6] or NULL*/,
+                                 double* acc32 /*[n][3] or NULL*/)
 {
-  std::vector<GpComp> comps(npot);
-  int rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
+  std::vector<GpComp> comps;
+  int rc = records(planar, npot, pot_type, pot_args, comps);
   if (rc) return rc;
+  const int nrec = (int)comps.size();
   for (int i = 0; i < n; i++) {
     double ax = 0, ay = 0, az = 0, K[6];
     if (planar)
-      accel<double, true>(comps.data(), npot, x[i], y[i], 0.0, ax, ay, az);
+      accel<double, true>(comps.data(), nrec, x[i], y[i], 0.0, ax, ay, az, nullptr, t);
     else
-      accel<double, false>(comps.data(), npot, x[i], y[i], z[i], ax, ay, az);
+      accel<double, false>(comps.data(), nrec, x[i], y[i], z[i], ax, ay, az, nullptr, t);
     acc[3 * i] = ax;
     acc[3 * i + 1] = ay;
     acc[3 * i + 2] = az;
     if (tidal) {
       double bx, by, bz;
       if (planar)
-        accel_tidal<true>(comps.data(), npot, x[i], y[i], 0.0, bx, by, bz, K);
+        accel_tidal<true>(comps.data(), nrec, x[i], y[i], 0.0, bx, by, bz, K, t);
       else
-        accel_tidal<false>(comps.data(), npot, x[i], y[i], z[i], bx, by, bz, K);
+        accel_tidal<false>(comps.data(), nrec, x[i], y[i], z[i], bx, by, bz, K, t);
       for (int k = 0; k < 6; k++) tidal[6 * i + k] = K[k];
     }
     if (acc32) {
       float fx = 0, fy = 0, fz = 0;
       if (planar)
-        accel<float, true>(comps.data(), npot, (float)x[i], (float)y[i], 0.f, fx, fy, fz);
+        accel<float, true>(comps.data(), nrec, (float)x[i], (float)y[i], 0.f, fx, fy, fz,
+                           nullptr, t);
       else
-        accel<float, false>(comps.data(), npot, (float)x[i], (float)y[i], (float)z[i], fx, fy, fz);
+        accel<float, false>(comps.data(), nrec, (float)x[i], (float)y[i], (float)z[i], fx, fy,
+                            fz, nullptr, t);
       acc32[3 * i] = fx;
       acc32[3 * i + 1] = fy;
       acc32[3 * i + 2] = fz;
     }
   }
   return 0;
+}
+
+extern "C" int harness_forces(int planar, int n, const double* x, const double* y,
+                              const double* z, int npot, const int* pot_type,
+                              const double* pot_args, double* acc, double* tidal, double* acc32)
+{
+  return harness_forces_at(planar, n, x, y, z, 0.0, npot, pot_type, pot_args, acc, tidal, acc32);
 }
 
 // The mixed float64 / float32 MWPotential2014 forces (MIX_TAIL32 = 1,

@@ -45,8 +45,32 @@ def test_compile_potential_host_only(golden):
     assert n == 3 and buf.size == 3 * _lib.lib().galpy_cuda_comp_size()
     rec = buf.reshape(3, -1)
     assert rec[:, :4].view(np.int32).ravel().tolist() == [15, 5, 9]
+    with pytest.raises(galpy_b200.PotentialNotSupported):  # SpiralArmsPotential
+        galpy_b200.compile_potential(([27], [1.0, 0, 0, 1, 1, 0]))
+
+
+def test_scf_continuation_records():
+    """An SCF expansion compiles to its record and continuation records
+    (type -100) holding its coefficients; the count is the launch's ncomp.
+    Time-dependent SCF coefficients are not carried."""
+    import timedep_pots as TP
+
+    pt, pa = TP.potential("scf_nonaxi")
+    size = _lib.lib().galpy_cuda_comp_size()
+    buf, n = galpy_b200.compile_potential((pt, pa))
+    N, L = 6, 5
+    payload = (L * (L + 1) // 2) * N * 2 + 4 * L * (N - 1)
+    per = (size - 8) // 8
+    assert n == 1 + -(-payload // per) and buf.size == n * size
+    types = buf.reshape(n, -1)[:, :4].view(np.int32).ravel().tolist()
+    assert types == [24] + [-100] * (n - 1)
+    pt2, pa2 = TP.potential("scf_axi+mn")
+    buf2, n2 = galpy_b200.compile_potential((pt2, pa2))
+    assert buf2.reshape(n2, -1)[:, :4].view(np.int32).ravel().tolist() == [24, -100, 5]
+    tdep = pa.copy()
+    tdep[5] = 3.0  # Nt > 0: coefficients interpolated in time
     with pytest.raises(galpy_b200.PotentialNotSupported):
-        galpy_b200.compile_potential(([1], [1.0, 0, 0, 1, 1, 0]))
+        galpy_b200.compile_potential((pt, tdep))
 
 
 def test_signatures_of_component_lists():
@@ -63,6 +87,8 @@ def test_signatures_of_component_lists():
     assert s([15, 9, 5]) == 2 and s([13]) == 2 and s([5, 19, 29]) == 2
     for ell in (21, 22, 23, 30, 37, 38, 43):
         assert s([ell]) == 0 and s([15, 5, ell]) == 0
+    # DehnenBar (time-dependent) and SCF: the full run-time list
+    assert s([15, 5, 9, 1]) == 0 and s([24]) == 0 and s([24, 5]) == 0
 
 
 def _no_gpu():

@@ -62,11 +62,34 @@ def test_planar_orbit_routes(hooks):
 
 def test_unsupported_potential_falls_back(hooks):
     from galpy.orbit import Orbit
-    from galpy.potential import SCFPotential
+    from galpy.potential import SpiralArmsPotential
 
     o = Orbit([1.0, 0.1, 1.1, 0.0, 0.1, 0.0])
-    o.integrate(np.linspace(0, 1, 11), SCFPotential(normalize=1.0), method="dop853_cuda")
+    o.integrate(np.linspace(0, 1, 11), SpiralArmsPotential(), method="dop853_cuda")
     assert hooks == []  # galpy's own integrator ran
+
+
+def test_bar_and_scf_route(hooks):
+    """The time-dependent DehnenBarPotential and a static SCFPotential go to
+    the engine; an SCF expansion with time-dependent coefficients stays with
+    galpy."""
+    from galpy.orbit import Orbit
+    from galpy.potential import DehnenBarPotential, MWPotential2014, SCFPotential
+
+    o = Orbit([1.0, 0.1, 1.1, 0.0, 0.1, 0.0])
+    o.integrate(np.linspace(0, 1, 11), [*MWPotential2014, DehnenBarPotential()],
+                method="dop853_cuda")
+    assert len(hooks) == 1
+    o.integrate(np.linspace(0, 1, 11), SCFPotential(normalize=1.0), method="rk4_cuda")
+    assert len(hooks) == 2 and hooks[-1]["method"] == "rk4_cuda"
+    Acos = np.zeros((2, 1, 1, 1))
+    Acos[:, 0, 0, 0] = [1.0, 1.2]
+    try:
+        tdep = SCFPotential(Acos=Acos, tgrid=np.array([0.0, 2.0]))
+    except TypeError:  # a galpy without time-dependent SCF coefficients
+        return
+    o.integrate(np.linspace(0, 1, 11), tdep, method="rk4_cuda")
+    assert len(hooks) == 2
 
 
 def test_spherical_potential_routes(hooks):

@@ -1,0 +1,145 @@
+"""The CUDA engine in the time-dependent DehnenBarPotential and the
+SCFPotential against the oracle (bit-exact with the reference's C for these
+potentials: tests/test_timedep.py), through galpy's C-ABI entry points.
+
+Force times follow the reference steppers' bookkeeping, so the engine takes
+the reference's step sizes; its force is Cartesian (the bar as a quadratic
+form, the SCF sums by recurrences), so results differ by the force's
+rounding, which each orbit amplifies by its own conditioning: the bound per
+orbit is the oracle's response to a one-ulp change of its initial
+conditions (times 30), never looser than 1e-10.  DOP853 orbits that cross
+the bar radius (a jump of the potential's second derivative) may flip
+accept / reject decisions at that rounding level; they agree to the
+tolerance's scale instead."""
+import numpy as np
+import pytest
+from helpers import cyl_diff, cyl_to_rect, sos_diff, unit_deviations
+
+import galpy_b200 as gb
+import timedep_pots as TP
+from galpy_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+METHODS = ["leapfrog", "rk4", "rk6", "symplec4", "symplec6", "dopr54", "dop853"]
+
+
+@pytest.fixture(scope="module", autouse=True)
+def engine():
+    from galpy_b200 import build
+
+    build.build()
+    assert _lib.lib().galpy_cuda_device_count() > 0, "GPU tests need a GPU"
+
+
+def ics(n, planar, seed):
+    rng = np.random.default_rng(seed)
+    R = rng.uniform(0.5, 1.5, n)
+    vR, vT, phi = rng.normal(0, 0.1, n), rng.uniform(0.8, 1.1, n), rng.uniform(0, 2 * np.pi, n)
+    if planar:
+        return np.stack([R, vR, vT, phi], 1)
+    return np.stack([R, vR, vT, rng.normal(0, 0.1, n), rng.normal(0, 0.1, n), phi], 1)
+
+
+def tol(method):
+    return dict(rtol=1e-10, atol=1e-10) if method in ("dopr54", "dop853") else {}
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", TP.NAMES)
+def test_orbits_vs_oracle(oracle, name, planar, method):
+    pt, pa = TP.potential(name, planar)
+    y0 = ics(128, planar, 17 + TP.NAMES.index(name))
+    t = np.linspace(0.0, 10.0, 41)
+    with oracle.phi_from_atan2():
+        ref, eref, nref, _ = oracle.integrate(y0, t, pt, pa, method, planar=planar, **tol(method))
+    fn = gb.integratePlanarOrbit_cuda if planar else gb.integrateFullOrbit_cuda
+    out, err, ns = fn((pt, pa), y0.copy(), t, method + "_cuda", progressbar=False,
+                      return_nsteps=True, **tol(method))
+    assert not err.any() and not eref.any()
+    d = cyl_diff(ref, out).max(axis=(1, 2))
+    same = ns == nref
+    kink = TP.crosses_bar_radius(ref) if name.startswith("bar") and method == "dop853" else \
+        np.zeros(len(ns), bool)
+    assert same[~kink].mean() >= 0.99, same[~kink].mean()
+    far = same & (d > 1e-10)
+    if far.any():
+        with oracle.phi_from_atan2():
+            resp = TP.ulp_response(oracle, y0[far], t, pt, pa, method, planar, ref[far],
+                                   **tol(method))
+        assert (d[far] <= 30 * resp).all(), (d[far], resp)
+    assert (d[~same] < 1e-6).all(), d[~same]
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("planar", [False, True])
+def test_variational_in_growing_bar(oracle, method, planar):
+    pt, pa = TP.potential("bar_growing+mw14", planar)
+    dim = 2 if planar else 3
+    w = unit_deviations(cyl_to_rect(ics(6, planar, 5)), dim)
+    t = np.linspace(0.0, 6.0, 25)
+    with oracle.phi_from_atan2():
+        ref, _, nref = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar, **tol(method))
+    out, err, ns = gb.integrate_dxdv_batch((pt, pa), w, t, method + "_cuda", planar=planar,
+                                           return_nsteps=True, **tol(method))
+    assert not err.any() and np.array_equal(ns, nref)
+    scale = np.abs(ref).max(axis=1, keepdims=True)
+    assert (np.abs(out - ref) / scale).max() < 1e-9
+
+
+def test_variational_scf_refused():
+    """No tidal tensor of an SCF expansion on the device: the call reports
+    the potential unsupported (galpy then keeps its own C path)."""
+    pt, pa = TP.potential("scf_nonaxi")
+    w = unit_deviations(cyl_to_rect(ics(2, False, 1)), 3)
+    with pytest.raises(gb.PotentialNotSupported):
+        gb.integrate_dxdv_batch((pt, pa), w, np.linspace(0, 1, 5), "rk4_cuda")
+
+
+@pytest.mark.parametrize("method", ["rk4", "dop853"])
+def test_surface_of_section_in_growing_bar(oracle, method):
+    """The surface of section's force time is the integrated time in the
+    state."""
+    pt, pa = TP.potential("bar_growing+mw14")
+    y0 = ics(64, False, 9)
+    yo = np.concatenate([y0, np.full((64, 1), 0.5)], 1)
+    psi = np.linspace(0.0, 6 * np.pi, 13)
+    with oracle.phi_from_atan2():
+        ref, _, nref = oracle.integrate_sos(yo, psi, pt, pa, method, rtol=1e-10, atol=1e-10)
+    out, err, ns = gb.integrateFullOrbit_sos_cuda((pt, pa), y0, psi, 0.5, method + "_cuda",
+                                                  rtol=1e-10, atol=1e-10, progressbar=False,
+                                                  return_nsteps=True)
+    assert not err.any()
+    same = ns == nref
+    assert same.mean() >= 0.8, same.mean()
+    d = sos_diff(ref, out).max(axis=(1, 2))
+    assert np.median(d) < 1e-10 and d.max() < 1e-6, (np.median(d), d.max())
+
+
+def test_device_forces_and_potential(oracle):
+    """Accelerations of the device kernel (galpy_cuda_accel_device) and SCF
+    potential values (galpy_cuda_energy_device) against the oracle."""
+    import torch
+
+    rng = np.random.default_rng(4)
+    R, z, phi = rng.uniform(0.2, 2.0, 500), rng.normal(0, 0.4, 500), rng.uniform(0, 6.28, 500)
+    for name in ["scf_nonaxi", "scf_axi+mn"]:
+        pt, pa = TP.potential(name)
+        comps, nrec = gb.compile_potential((pt, pa))
+        dev = torch.device("cuda", 0)
+        pos = torch.tensor(np.stack([R * np.cos(phi), R * np.sin(phi), z]), device=dev)
+        acc = torch.empty_like(pos)
+        gb.accel_device(torch.from_numpy(comps).to(dev), nrec, pos, acc)
+        f = oracle.forces(R, z, phi, pt, pa)
+        ax = np.cos(phi) * f[:, 0] - np.sin(phi) * f[:, 2] / R
+        ay = np.sin(phi) * f[:, 0] + np.cos(phi) * f[:, 2] / R
+        a = acc.cpu().numpy()
+        scale = np.abs(np.stack([ax, ay, f[:, 1]])).max()
+        assert np.abs(a - np.stack([ax, ay, f[:, 1]])).max() < 1e-13 * scale, name
+        # potential: the energy at rest
+        w = torch.zeros((6, R.size), dtype=torch.float64, device=dev)
+        w[:3] = pos
+        E = torch.empty(R.size, dtype=torch.float64, device=dev)
+        gb.energy_device(torch.from_numpy(comps).to(dev), nrec, w, E)
+        ref = oracle.potential(R, z, phi, pt, pa)
+        assert np.abs(E.cpu().numpy() - ref).max() < 1e-13 * np.abs(ref).max(), name

@@ -140,3 +140,88 @@ def test_scf_forces_vs_galpy_python(nonaxi):
                         for i in range(R.size)])
         scale = max(np.abs(ref).max(), 1e-300)
         assert np.abs(got[:, k] - ref).max() <= 1e-13 * scale, nm
+
+
+# ---- the engine's machines and forces, compiled as host C++ (harness) -------
+def c2r(v, planar):
+    if planar:
+        R, vR, vT, p = v.T
+        c, s = np.cos(p), np.sin(p)
+        return np.stack([R * c, R * s, vR * c - vT * s, vR * s + vT * c], 1)
+    R, vR, vT, z, vz, p = v.T
+    c, s = np.cos(p), np.sin(p)
+    return np.stack([R * c, R * s, z, vR * c - vT * s, vR * s + vT * c, vz], 1)
+
+
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", TP.NAMES)
+def test_engine_forces_at_times(harness, name, planar):
+    """The engine's Cartesian forces (the bar's quadratic form, the SCF
+    recurrences) against the oracle's cylindrical restatement at several
+    times."""
+    pt, pa = TP.potential(name, planar)
+    rng = np.random.default_rng(6)
+    R = rng.uniform(0.3, 2.0, 200)
+    z = np.zeros(200) if planar else rng.normal(0, 0.4, 200)
+    phi = rng.uniform(0, 2 * np.pi, 200)
+    for t in (0.0, 2.5, 7.0):
+        f = oracle.forces(R, z, phi, pt, pa, planar=planar, t=t)
+        tq = f[:, 1] if planar else f[:, 2]
+        ax = np.cos(phi) * f[:, 0] - np.sin(phi) * tq / R
+        ay = np.sin(phi) * f[:, 0] + np.cos(phi) * tq / R
+        acc, _, _ = harness.forces(R * np.cos(phi), R * np.sin(phi), z, pt, pa, planar=planar,
+                                   t=t)
+        ref = np.stack([ax, ay] + ([] if planar else [f[:, 1]]), 1)
+        scale = np.abs(ref).max()
+        assert np.abs(acc[:, :ref.shape[1]] - ref).max() < 1e-14 * scale, t
+
+
+@pytest.mark.parametrize("planar", [False, True])
+def test_engine_bar_tidal_tensor(harness, planar):
+    """K = -grad grad Phi of the bar (engine: Cartesian closed form) against
+    the oracle's cylindrical second derivatives."""
+    pt, pa = np.array([1], np.int32), np.array(TP.dehnen_bar_args())
+    rng = np.random.default_rng(8)
+    R = rng.uniform(0.3, 2.0, 100)
+    z = np.zeros(100) if planar else rng.normal(0, 0.4, 100)
+    phi = rng.uniform(0, 2 * np.pi, 100)
+    x, y = R * np.cos(phi), R * np.sin(phi)
+    _, K, _ = harness.forces(x, y, z, pt, pa, planar=planar, t=1.3)
+    # central differences of the engine's own accelerations
+    h = 1e-6
+    cols = [(0, 0), (0, 1), (1, 1)] + ([] if planar else [(0, 2), (1, 2), (2, 2)])
+    for k, (i, j) in enumerate(cols):
+        dp = [x, y, z]
+        dm = [x, y, z]
+        dp = [v + (h if m == j else 0) for m, v in enumerate(dp)]
+        dm = [v - (h if m == j else 0) for m, v in enumerate(dm)]
+        ap, _, _ = harness.forces(*dp, pt, pa, planar=planar, t=1.3)
+        am, _, _ = harness.forces(*dm, pt, pa, planar=planar, t=1.3)
+        fd = (ap[:, i] - am[:, i]) / (2 * h)
+        assert np.abs(K[:, k] - fd).max() < 1e-6 * max(np.abs(fd).max(), 1e-3), (i, j)
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", ["bar+mw14", "bar_growing+mw14", "scf_axi+mn"])
+def test_engine_machines_vs_oracle(harness, name, planar, method):
+    """The engine's stepper machines with their force times (host build)
+    against the oracle: same step sizes; DOP853 the same steps on orbits
+    that stay on one side of the bar radius."""
+    pt, pa = TP.potential(name, planar)
+    y0 = ics(24, planar, seed=21)
+    t = np.linspace(0.0, 10.0, 41)
+    with oracle.phi_from_atan2():
+        ref, _, nref, _ = oracle.integrate(y0, t, pt, pa, method, planar=planar, **tol(method))
+    out, err, ns = harness.integrate(c2r(y0, planar), t, pt, pa, method, planar=planar,
+                                     **tol(method))
+    assert not err.any()
+    ref_r = np.stack([c2r(ref[:, j], planar) for j in range(len(t))], 1)
+    d = np.abs(out - ref_r).reshape(len(y0), -1).max(1)
+    same = ns == nref
+    kink = TP.crosses_bar_radius(ref) if name.startswith("bar") and method == "dop853" else \
+        np.zeros(len(ns), bool)
+    assert same[~kink].all()
+    strict = same & ~kink
+    assert np.median(d[strict]) < 1e-12 and d[strict].max() < 1e-9, d[strict].max()
+    assert (d < 1e-6).all()

@@ -67,3 +67,24 @@ def potential(name, planar=False):
 
 
 NAMES = ["bar+mw14", "bar_growing+mw14", "scf_nonaxi", "scf_axi+mn"]
+
+
+def crosses_bar_radius(ref_cyl, rb=0.8):
+    """Orbits (cylindrical rows [n][nt][6|4]) whose radius r crosses the bar
+    radius, where the bar potential's second derivative jumps: there
+    DOP853's error estimate sits near 1 more often, and accept / reject
+    decisions flip on rounding-level differences of the force."""
+    R = ref_cyl[..., 0]
+    z = ref_cyl[..., 3] if ref_cyl.shape[-1] == 6 else 0.0 * R
+    r = np.sqrt(R * R + z * z)
+    return (r.min(axis=1) < rb) & (r.max(axis=1) > rb)
+
+
+def ulp_response(oracle, ics, t, pt, pa, method, planar, ref, seed=3, **kw):
+    """Per-orbit change of the oracle's orbit under a one-ulp change of its
+    initial conditions: the orbit's own conditioning."""
+    from helpers import cyl_diff
+
+    ulp = 1 + np.finfo(float).eps * np.random.default_rng(seed).choice([-1, 1], ics.shape)
+    pert, _, _, _ = oracle.integrate(ics * ulp, t, pt, pa, method, planar=planar, **kw)
+    return cyl_diff(ref, pert).max(axis=(1, 2))
