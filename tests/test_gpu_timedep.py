@@ -7,10 +7,13 @@ the reference's step sizes; its force is Cartesian (the bar as a quadratic
 form, the SCF sums by recurrences), so results differ by the force's
 rounding, which each orbit amplifies by its own conditioning: the bound per
 orbit is the oracle's response to a one-ulp change of its initial
-conditions (times 30), never looser than 1e-10.  DOP853 orbits that cross
-the bar radius (a jump of the potential's second derivative) may flip
-accept / reject decisions at that rounding level; they agree to the
-tolerance's scale instead."""
+conditions (times 30, the larger of two such responses), never looser
+than 1e-10.  DOP853 orbits that cross the bar radius (a jump of the
+potential's second derivative) may flip accept / reject decisions at that
+rounding level; they agree to the tolerance's scale instead.  The random
+non-axisymmetric SCF expansion makes many orbits chaotic (the oracle's own
+orbits move by O(1) at t = 10 under a one-ulp change of their initial
+conditions), so it is compared over t <= 3."""
 import numpy as np
 import pytest
 from helpers import cyl_diff, cyl_to_rect, sos_diff, unit_deviations
@@ -44,13 +47,16 @@ def tol(method):
     return dict(rtol=1e-10, atol=1e-10) if method in ("dopr54", "dop853") else {}
 
 
+T_END = {"scf_nonaxi": 3.0}  # chaotic orbits: a short window
+
+
 @pytest.mark.parametrize("method", METHODS)
 @pytest.mark.parametrize("planar", [False, True])
 @pytest.mark.parametrize("name", TP.NAMES)
 def test_orbits_vs_oracle(oracle, name, planar, method):
     pt, pa = TP.potential(name, planar)
     y0 = ics(128, planar, 17 + TP.NAMES.index(name))
-    t = np.linspace(0.0, 10.0, 41)
+    t = np.linspace(0.0, T_END.get(name, 10.0), 41)
     with oracle.phi_from_atan2():
         ref, eref, nref, _ = oracle.integrate(y0, t, pt, pa, method, planar=planar, **tol(method))
     fn = gb.integratePlanarOrbit_cuda if planar else gb.integrateFullOrbit_cuda
@@ -62,13 +68,14 @@ def test_orbits_vs_oracle(oracle, name, planar, method):
     kink = TP.crosses_bar_radius(ref) if name.startswith("bar") and method == "dop853" else \
         np.zeros(len(ns), bool)
     assert same[~kink].mean() >= 0.99, same[~kink].mean()
-    far = same & (d > 1e-10)
+    far = same & ~kink & (d > 1e-10)
     if far.any():
         with oracle.phi_from_atan2():
-            resp = TP.ulp_response(oracle, y0[far], t, pt, pa, method, planar, ref[far],
-                                   **tol(method))
+            resp = np.maximum(*[TP.ulp_response(oracle, y0[far], t, pt, pa, method, planar,
+                                                ref[far], seed=sd, **tol(method))
+                                for sd in (3, 4)])
         assert (d[far] <= 30 * resp).all(), (d[far], resp)
-    assert (d[~same] < 1e-6).all(), d[~same]
+    assert (d[~same | kink] < 1e-6).all(), d[~same | kink]
 
 
 @pytest.mark.parametrize("method", METHODS)
@@ -79,12 +86,18 @@ def test_variational_in_growing_bar(oracle, method, planar):
     w = unit_deviations(cyl_to_rect(ics(6, planar, 5)), dim)
     t = np.linspace(0.0, 6.0, 25)
     with oracle.phi_from_atan2():
-        ref, _, nref = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar, **tol(method))
+        ref, eref, nref = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar,
+                                                **tol(method))
     out, err, ns = gb.integrate_dxdv_batch((pt, pa), w, t, method + "_cuda", planar=planar,
                                            return_nsteps=True, **tol(method))
-    assert not err.any() and np.array_equal(ns, nref)
-    scale = np.abs(ref).max(axis=1, keepdims=True)
-    assert (np.abs(out - ref) / scale).max() < 1e-9
+    # err 1: dopr54's forced smallest step, flagged by the reference too
+    assert np.array_equal(err, eref)
+    r = np.sqrt((ref[..., :dim] ** 2).sum(-1))
+    kink = (r.min(axis=1) < 0.8) & (r.max(axis=1) > 0.8) if method == "dop853" else \
+        np.zeros(len(ns), bool)
+    assert np.array_equal(ns[~kink], nref[~kink])
+    rel = (np.abs(out - ref) / np.abs(ref).max(axis=1, keepdims=True)).max(axis=(1, 2))
+    assert rel[~kink].max() < 1e-9 and (rel[kink] < 1e-5).all(), rel
 
 
 def test_variational_scf_refused():
