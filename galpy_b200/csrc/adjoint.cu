@@ -236,6 +236,12 @@ int galpy_cuda_adjoint_params(int planar, int npot, const int* pot_type, const d
     const int na = galpy_nargs(pot_type[k], planar, pot_args ? pot_args + off : nullptr);
     if (na < 0)
       return gpc_report_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
+    // the adjoint's DOP853 evaluates static forces and needs the tidal
+    // tensor, which the device does not have for an SCF expansion
+    if (pot_type[k] == T_DEHNENBAR || pot_type[k] == T_SCF)
+      return gpc_report_error(GALPY_CUDA_ERR_POTENTIAL,
+                              "gradients through a time-dependent or SCF potential are not "
+                              "available");
     // a rotated ellipsoid: the tidal tensor follows the reference's second
     // derivatives, which ignore the rotation, so they are not the derivative
     // of its force and the adjoint would return wrong gradients

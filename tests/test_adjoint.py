@@ -200,3 +200,17 @@ def test_adjoint_params_abi_matches_layout(golden):
     # a rotated ellipsoid has no consistent second derivatives: refused
     with pytest.raises(_lib.PotentialNotSupported, match="rotated"):
         adjoint_params(golden["ell_trinfw_type"], False, golden["ell_trinfw_args"])
+
+
+def test_adjoint_refuses_bar_and_scf():
+    """The adjoint's forward pass evaluates static forces, and the device has
+    no tidal tensor of an SCF expansion: both potentials are refused."""
+    import timedep_pots as TP
+
+    from galpy_b200 import _lib
+    from galpy_b200.adjoint import adjoint_params
+
+    for name in ("bar+mw14", "scf_axi+mn"):
+        pt, pa = TP.potential(name, planar=True)
+        with pytest.raises(_lib.PotentialNotSupported, match="time-dependent or SCF"):
+            adjoint_params(pt, True, pa)
