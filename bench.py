@@ -847,6 +847,22 @@ def methods_leg(gb, torch, dev, stream, pg, peak, rank, cpu=True, n=131072, K=3,
     return res
 
 
+def scf_expansion_args(N=8, L=6, a=1.1, seed=3):
+    """galpy's SCFPotential arguments (a, isNonAxi, N, L, M, Nt = 0, Acos,
+    Asin, 11 cache slots) of a seeded non-axisymmetric expansion: the
+    (0, 0, 0) term 1, the m <= l others ~N(0, 0.05)."""
+    rng = np.random.default_rng(seed)
+    Acos = rng.normal(size=(N, L, L)) * 0.05
+    Asin = rng.normal(size=(N, L, L)) * 0.05
+    Acos[0, 0, 0] = 1.0
+    for l in range(L):
+        Acos[:, l, l + 1:] = 0.0
+        Asin[:, l, l + 1:] = 0.0
+    Asin[:, :, 0] = 0.0
+    return np.concatenate([[a, 1.0, N, L, L, 0.0], Acos.ravel(), Asin.ravel(),
+                           [-1.0] + [0.0] * 10])
+
+
 def profile_leg(gb, torch, dev, spec, n, out_layout="soa_rect"):
     """One warm-up and one timed launch of a single kernel on a small batch,
     for profiler captures (`ncu -k regex:<machine> -s 1 -c 1`):
@@ -863,6 +879,11 @@ def profile_leg(gb, torch, dev, spec, n, out_layout="soa_rect"):
       uniform      R ~ U(0.5, 2) (seed 1), per-orbit copies of t in [0, 50]
                    with 101 snapshots, rtol = atol = 1e-10: the batching
                    workload's kernel on orbits of similar length
+      bar          as plain, in MWPotential2014 plus a rotating
+                   DehnenBarPotential (the full run-time list, whose force
+                   reads the time)
+      scf          as plain, in a non-axisymmetric SCF expansion (N = 8,
+                   L = 6) plus MWPotential2014's disk (full run-time list)
 
     A third field selects the register variant and a fourth the orbits per
     block (METHOD:KIND:VARIANT[:BLOCK]).  out_layout: the snapshot layout
@@ -873,6 +894,12 @@ def profile_leg(gb, torch, dev, spec, n, out_layout="soa_rect"):
     kind = kind or "plain"
     stream = torch.cuda.current_stream(dev)
     pt, pa = mw14_args()
+    if kind == "bar":
+        pt = np.append(pt, 1).astype(np.int32)
+        pa = np.concatenate([pa, [0.01, -2.0, 3.0, 0.8, 1.85, 0.4]])
+    elif kind == "scf":
+        pt = np.array([24, 5], np.int32)
+        pa = np.concatenate([scf_expansion_args(), pa[5:8]])
     ics, _ = precision_workload(n, seed=1 if kind == "uniform" else 5)
     kw = {"variant": int(variant or 0), "block_size": int(block or 0)}
     group = None

@@ -193,7 +193,7 @@ inline int scf_payload_len(const double* p)
   const int Me = nonaxi ? L : 1;
   int pairs = 0;
   for (int m = 0; m < Me; m++) pairs += L - m;
-  return pairs * N * (1 + nonaxi) + 4 * L * (N - 1);
+  return pairs * N * (1 + nonaxi) + kScfTable * L * (N - 1);
 }
 
 // Records one component takes: 1, plus continuation records for an SCF
@@ -452,6 +452,8 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
             pay.push_back((double)((n + 2.0L * al - 1.0L) / n1));
             pay.push_back((double)(2.0L * (n + al + 1.0L) / n1));
             pay.push_back((double)((n + 2.0L * al + 1.0L) / n1));
+            pay.push_back((double)(2.0L * (n + al + 2.0L) / n1));
+            pay.push_back((double)((n + 2.0L * al + 3.0L) / n1));
           }
         }
         for (int r = 1; r < nrec; r++) {  // continuation records

@@ -783,19 +783,13 @@ struct SplitCtl {
 
 // Blocking host-pointer integration shared by the galpy-facing entry points.
 // One potential's records (a component may take continuation records: an
-// SCF expansion's coefficients).  Variational runs need the tidal tensor,
-// which the device does not evaluate for an SCF expansion.
-static int compile_records(int planar, int var, int npot, const int* pot_type,
+// SCF expansion's coefficients).
+static int compile_records(int planar, int /*var*/, int npot, const int* pot_type,
                            const double* pot_args, std::vector<GpComp>& comps)
 {
   const int n = group_records(planar, npot, pot_type, pot_args);
   if (n == -3) return set_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");
   if (n < 1) return set_error(GALPY_CUDA_ERR_ARG, "invalid potential arguments");
-  if (var)
-    for (int k = 0; k < npot; k++)
-      if (pot_type[k] == T_SCF)
-        return set_error(GALPY_CUDA_ERR_POTENTIAL,
-                         "variational runs in an SCF potential are not implemented on the GPU");
   comps.assign((size_t)n, GpComp{});
   const int rc = compile_group(planar, npot, pot_type, pot_args, comps.data(), nullptr);
   if (rc == -3) return set_error(GALPY_CUDA_ERR_POTENTIAL, "potential type not implemented on the GPU");

@@ -1337,8 +1337,8 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
       case T_DEHNENBAR:
         dbar_tidal<PLANAR>(cp, t, x, y, z, ax0, ay0, az0, K);
         break;
-      case T_SCF:  // no tidal tensor on the device: the host refuses such runs
-        gR = NAN;
+      case T_SCF:
+        scf_tidal<PLANAR>(cp, x, y, z, ax0, ay0, az0, K);
         break;
       case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
       case T_POWERTRI: case T_TWOPOWERTRI: {

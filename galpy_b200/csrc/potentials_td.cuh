@@ -142,13 +142,20 @@ GPC_HD GPC_FI void dbar_tidal(const GpComp* __restrict__ cp, double t, double x,
 // the recurrence table.  Payload (continuation records): for m < c4, l in
 // [m, L), n < N: sqrt(4 pi) Acos_nlm (and sqrt(4 pi) Asin_nlm next to it if
 // non-axisymmetric); then for l < L, n < N - 1 the Gegenbauer recurrence
-// C_{n+1} = p0 xi C_n - p1 C_{n-1} of alpha = 2l + 3/2 (p0, p1) and of
-// alpha + 1 (p2, p3), 4 doubles.
+// C_{n+1} = p0 xi C_n - p1 C_{n-1} of alpha = 2l + 3/2 (p0, p1), of
+// alpha + 1 (p2, p3) and of alpha + 2 (p4, p5): kScfTable doubles.
+constexpr int kScfTable = 6;
+
+// Derivatives of Phi in spherical coordinates (r, theta, phi); the second
+// ones only with HESS.
 struct ScfSums {
-  double pot;           // Phi
-  double dr, dth, dph;  // dPhi/dr, dPhi/dtheta, dPhi/dphi
+  double pot;                  // Phi
+  double dr, dth, dph;         // first derivatives
+  double drr, dthth, dphph;    // second derivatives
+  double drth, drph, dthph;
 };
 
+template <bool HESS>
 GPC_HD inline ScfSums scf_sums(const GpComp* __restrict__ cp, double r, double ct, double st,
                                double cph, double sph)
 {
@@ -158,15 +165,18 @@ GPC_HD inline ScfSums scf_sums(const GpComp* __restrict__ cp, double r, double c
   const int rec0 = (int)ldg(&cp->c[5]);
   const double ar = a + r, iar = 1.0 / ar, xi = (r - a) * iar;
   const double q = r * a * iar * iar;  // the factor between l and l + 1
-  ScfSums S{0.0, 0.0, 0.0, 0.0};
-  double cm = 1.0, sm = 0.0;                         // cos, sin m phi
-  double pmm = 1.0, dmm = 0.0;                       // P_m^m, dP_m^m / dtheta
-  double rtm = -iar, rt1m = iar * iar * iar / r;     // radial prefactors at l = m
-  int j = 0;                                         // payload cursor (coefficients)
+  const double ar2 = ar * ar, ar3 = ar2 * ar, ar4 = ar2 * ar2;
+  ScfSums S{0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  double cm = 1.0, sm = 0.0;                   // cos, sin m phi
+  double pmm = 1.0, dmm = 0.0, emm = 0.0;      // P_m^m and its first, second theta derivative
+  // radial prefactors at l = m: -1/(a+r), 1/(r (a+r)^3), 1/(r^2 (a+r)^5), times q^m
+  double rtm = -iar, rt1m = iar * iar * iar / r, rt2m = HESS ? rt1m * iar * iar / r : 0.0;
+  int j = 0;  // payload cursor (coefficients)
   for (int m = 0; m < Me; m++) {
     if (m > 0) {
       const double f = -(2.0 * m - 1.0);
       const double pn = f * st * pmm, dn = f * (ct * pmm + st * dmm);
+      if (HESS) emm = f * (-st * pmm + 2.0 * ct * dmm + st * emm);
       pmm = pn;
       dmm = dn;
       const double cn = cm * cph - sm * sph;
@@ -174,38 +184,48 @@ GPC_HD inline ScfSums scf_sums(const GpComp* __restrict__ cp, double r, double c
       cm = cn;
       rtm *= q;
       rt1m *= q;
+      rt2m *= q;
     }
-    double p1 = 0.0, d1 = 0.0, p0 = pmm, d0 = dmm;  // P_{l-1}, P_l (and d/dtheta)
-    double rt = rtm, rt1 = rt1m;
+    // P_l^m (p0), P_{l-1}^m (p1) and their theta derivatives (d, e)
+    double p1 = 0.0, d1 = 0.0, e1 = 0.0, p0 = pmm, d0 = dmm, e0 = emm;
+    double rt = rtm, rt1 = rt1m, rt2 = rt2m;
     for (int l = m; l < L; l++) {
       if (l > m) {
-        double pn, dn;
+        double pn, dn, en = 0.0;
         if (l == m + 1) {
-          pn = (2.0 * m + 1.0) * ct * p0;
-          dn = (2.0 * m + 1.0) * (ct * d0 - st * p0);
+          const double c2 = 2.0 * m + 1.0;
+          pn = c2 * ct * p0;
+          dn = c2 * (ct * d0 - st * p0);
+          if (HESS) en = c2 * (ct * e0 - 2.0 * st * d0 - ct * p0);
         } else {
           const double il = 1.0 / (double)(l - m), c2 = 2.0 * l - 1.0, c3 = l + m - 1.0;
           pn = (c2 * ct * p0 - c3 * p1) * il;
           dn = (c2 * (ct * d0 - st * p0) - c3 * d1) * il;
+          if (HESS) en = (c2 * (ct * e0 - 2.0 * st * d0 - ct * p0) - c3 * e1) * il;
         }
         p1 = p0;
         d1 = d0;
+        e1 = e0;
         p0 = pn;
         d0 = dn;
+        e0 = en;
         rt *= q;
         rt1 *= q;
+        rt2 *= q;
       }
-      // radial sums over n with the Gegenbauer recurrences of alpha = 2l + 3/2
-      const double alpha2 = 4.0 * l + 3.0;  // 2 alpha
-      const int tb = rec0 + 4 * l * (N - 1);
-      double Cp = 0.0, C = 1.0, Ep = 0.0, E = 1.0;
+      // radial sums over n with the Gegenbauer recurrences of alpha = 2l + 3/2:
+      // C_n, dC_n = 2 alpha C_{n-1}^(alpha+1), d2C_n = 4 alpha (alpha+1) C_{n-2}^(alpha+2)
+      const double alpha2 = 4.0 * l + 3.0;                         // 2 alpha
+      const double alpha4 = (4.0 * l + 3.0) * (4.0 * l + 5.0);     // 4 alpha (alpha + 1)
+      const int tb = rec0 + kScfTable * l * (N - 1);
+      double Cp = 0.0, C = 1.0, Ep = 0.0, E = 1.0, Fp = 0.0, F = 1.0;
       double ac = payload(cp, j), as = nonaxi ? payload(cp, j + 1) : 0.0;
       j += nonaxi ? 2 : 1;
-      double Sc = ac, Ss = as, Dc = 0.0, Ds = 0.0;
+      double Sc = ac, Ss = as, Dc = 0.0, Ds = 0.0, Hc = 0.0, Hs = 0.0;
       for (int n = 1; n < N; n++) {
-        const int k = tb + 4 * (n - 1);
+        const int k = tb + kScfTable * (n - 1);
         const double Cn = payload(cp, k) * xi * C - payload(cp, k + 1) * Cp;
-        const double dC = alpha2 * E;  // 2 alpha C_{n-1}^(alpha+1)
+        const double dC = alpha2 * E;
         const double En = payload(cp, k + 2) * xi * E - payload(cp, k + 3) * Ep;
         Cp = C;
         C = Cn;
@@ -218,14 +238,39 @@ GPC_HD inline ScfSums scf_sums(const GpComp* __restrict__ cp, double r, double c
         Ss += as * Cn;
         Dc += ac * dC;
         Ds += as * dC;
+        if (HESS && n >= 2) {
+          const double d2C = alpha4 * F;  // F = C_{n-2}^(alpha+2)
+          Hc += ac * d2C;
+          Hs += as * d2C;
+          const int k2 = tb + kScfTable * (n - 2);
+          const double Fn = payload(cp, k2 + 4) * xi * F - payload(cp, k2 + 5) * Fp;
+          Fp = F;
+          F = Fn;
+        }
       }
+      // azimuthal combinations and their phi derivatives
       const double U = cm * Sc + sm * Ss, V = cm * Dc + sm * Ds;
-      const double W = (double)m * (cm * Ss - sm * Sc);
-      const double rad = ((2.0 * l + 1.0) * r * ar - l * ar * ar) * U - 2.0 * a * r * V;
+      const double Uf = (double)m * (cm * Ss - sm * Sc);
+      const double c1 = (2.0 * l + 1.0) * r * ar - l * ar2, c0 = 2.0 * a * r;
+      const double R1 = rt1 * (c1 * U - c0 * V);  // d/dr of the radial factor times U
       S.pot += p0 * rt * U;
-      S.dr += p0 * rt1 * rad;
+      S.dr += p0 * R1;
       S.dth += d0 * rt * U;
-      S.dph += p0 * rt * W;
+      S.dph += p0 * rt * Uf;
+      if (HESS) {
+        const double H = cm * Hc + sm * Hs, Vf = (double)m * (cm * Ds - sm * Dc);
+        const double u2 = l * (1.0 - l) * ar4 - (4.0 * l * l + 6.0 * l + 2.0) * r * r * ar2 +
+                          l * (4.0 * l + 2.0) * r * ar3;
+        const double v2 = a * r * (4.0 * r * r + 4.0 * a * r + (8.0 * l + 4.0) * r * ar -
+                                   4.0 * l * ar2);
+        const double w2 = 4.0 * a * a * r * r;
+        S.drr += p0 * rt2 * (u2 * U + v2 * V - w2 * H);
+        S.dthth += e0 * rt * U;
+        S.dphph -= (double)(m * m) * p0 * rt * U;
+        S.drth += d0 * R1;
+        S.drph += p0 * rt1 * (c1 * Uf - c0 * Vf);
+        S.dthph += d0 * rt * Uf;
+      }
     }
   }
   return S;
@@ -240,7 +285,7 @@ GPC_HD inline void scf_accel(const GpComp* __restrict__ cp, double x, double y, 
   const double R2 = x * x + y * y, r2 = R2 + zz * zz, R = sqrt(R2), r = sqrt(r2);
   const double iR = R > 0.0 ? 1.0 / R : 0.0, ir = 1.0 / r;
   const double cph = R > 0.0 ? x * iR : 1.0, sph = R > 0.0 ? y * iR : 0.0;
-  const ScfSums S = scf_sums(cp, r, zz * ir, R * ir, cph, sph);
+  const ScfSums S = scf_sums<false>(cp, r, zz * ir, R * ir, cph, sph);
   if (pot) *pot = S.pot;
   // dPhi/dx_i = Phi_r x_i / r + Phi_theta dtheta/dx_i + Phi_phi dphi/dx_i,
   // theta = atan2(R, z): dtheta/dR = z / r^2, dtheta/dz = -R / r^2
@@ -248,6 +293,49 @@ GPC_HD inline void scf_accel(const GpComp* __restrict__ cp, double x, double y, 
   ax = -(gr * x + gth * zz * cph - gph * sph);
   ay = -(gr * y + gth * zz * sph + gph * cph);
   az = PLANAR ? 0.0 : -(gr * zz - gth * R);
+}
+
+// Acceleration and K = -grad grad Phi added to ax.. and K (PLANAR: at
+// z = 0): the spherical second derivatives, then the cylindrical ones by the
+// chain rule through r = sqrt(R^2 + z^2), theta = atan2(R, z) (as the
+// reference's compute_scf_hessian_cyl), then the Cartesian tensor from the
+// cylindrical derivatives (R > 0).
+template <bool PLANAR>
+GPC_HD inline void scf_tidal(const GpComp* __restrict__ cp, double x, double y, double z,
+                             double& ax, double& ay, double& az, double K[6])
+{
+  const double zz = PLANAR ? 0.0 : z;
+  const double R2 = x * x + y * y, r2 = R2 + zz * zz, R = sqrt(R2), r = sqrt(r2);
+  const double iR = 1.0 / R, ir = 1.0 / r;
+  const double c = x * iR, s = y * iR;
+  const ScfSums S = scf_sums<true>(cp, r, zz * ir, R * ir, c, s);
+  const double ir2 = ir * ir, ir3 = ir2 * ir, ir4 = ir2 * ir2;
+  const double rR = R * ir, rz = zz * ir, thR = zz * ir2, thz = -R * ir2;
+  const double rRR = zz * zz * ir3, rzz = R2 * ir3, rRz = -R * zz * ir3;
+  const double thRR = -2.0 * R * zz * ir4, thzz = -thRR, thRz = (R2 - zz * zz) * ir4;
+  const double PR = S.dr * rR + S.dth * thR, Pz = S.dr * rz + S.dth * thz, Pf = S.dph;
+  const double HRR = S.drr * rR * rR + 2.0 * S.drth * rR * thR + S.dthth * thR * thR +
+                     S.dr * rRR + S.dth * thRR;
+  const double Hzz = S.drr * rz * rz + 2.0 * S.drth * rz * thz + S.dthth * thz * thz +
+                     S.dr * rzz + S.dth * thzz;
+  const double HRz = S.drr * rR * rz + S.drth * (rR * thz + rz * thR) + S.dthth * thR * thz +
+                     S.dr * rRz + S.dth * thRz;
+  const double Hff = S.dphph, HRf = S.drph * rR + S.dthph * thR, Hzf = S.drph * rz + S.dthph * thz;
+  // gradient and Hessian of Phi(R, phi, z) in Cartesian coordinates
+  ax -= c * PR - s * iR * Pf;
+  ay -= s * PR + c * iR * Pf;
+  if (!PLANAR) az -= Pz;
+  const double iR2 = iR * iR, cs = c * s, c2s2 = c * c - s * s;
+  K[0] -= c * c * HRR - 2.0 * cs * iR * HRf + s * s * iR2 * Hff + s * s * iR * PR +
+          2.0 * cs * iR2 * Pf;
+  K[1] -= cs * HRR + c2s2 * iR * HRf - cs * iR2 * Hff - cs * iR * PR - c2s2 * iR2 * Pf;
+  K[2] -= s * s * HRR + 2.0 * cs * iR * HRf + c * c * iR2 * Hff + c * c * iR * PR -
+          2.0 * cs * iR2 * Pf;
+  if (!PLANAR) {
+    K[3] -= c * HRz - s * iR * Hzf;
+    K[4] -= s * HRz + c * iR * Hzf;
+    K[5] -= Hzz;
+  }
 }
 
 }  // namespace gpc

@@ -49,10 +49,9 @@ def _is_cuda(method):
 
 def _supported(pot, planar, purpose="integrate"):
     """Whether the engine carries this potential for `purpose`: "integrate"
-    (orbits, surfaces of section), "variational" (no SCF expansion: the
-    device has no tidal tensor for it) or "potential" (values at points,
-    evaluated without a time: no time-dependent component).  An SCF
-    expansion must have static coefficients."""
+    (orbits, surfaces of section, variational runs) or "potential" (values
+    at points, evaluated without a time: no time-dependent component).  An
+    SCF expansion must have static coefficients."""
     try:
         if planar:
             from galpy.orbit.integratePlanarOrbit import _parse_pot
@@ -63,8 +62,6 @@ def _supported(pot, planar, purpose="integrate"):
         return False
     types = [int(t) for t in pot_type]
     if len(tfuncs) or not all(t in SUPPORTED_TYPES for t in types):
-        return False
-    if purpose == "variational" and T_SCF in types:
         return False
     if purpose == "potential" and any(t in TIME_DEPENDENT_TYPES for t in types):
         return False
@@ -311,8 +308,7 @@ def _wrap_variational(orig, O):
         if pot is None:
             pot = getattr(self, "_pot", None)
         planar = self.dim() == 2
-        if pot is not None and _supported(O.toPlanarPotential(pot) if planar else pot, planar,
-                                          "variational"):
+        if pot is not None and _supported(O.toPlanarPotential(pot) if planar else pot, planar):
             with _EngineAsC(O):
                 return orig(*ba.args, **ba.kwargs)
         ba.arguments["method"] = method[: -len("_cuda")] + "_c"

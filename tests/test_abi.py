@@ -59,7 +59,7 @@ def test_scf_continuation_records():
     size = _lib.lib().galpy_cuda_comp_size()
     buf, n = galpy_b200.compile_potential((pt, pa))
     N, L = 6, 5
-    payload = (L * (L + 1) // 2) * N * 2 + 4 * L * (N - 1)
+    payload = (L * (L + 1) // 2) * N * 2 + 6 * L * (N - 1)
     per = (size - 8) // 8
     assert n == 1 + -(-payload // per) and buf.size == n * size
     types = buf.reshape(n, -1)[:, :4].view(np.int32).ravel().tolist()

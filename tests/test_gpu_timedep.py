@@ -100,13 +100,25 @@ def test_variational_in_growing_bar(oracle, method, planar):
     assert rel[~kink].max() < 1e-9 and (rel[kink] < 1e-5).all(), rel
 
 
-def test_variational_scf_refused():
-    """No tidal tensor of an SCF expansion on the device: the call reports
-    the potential unsupported (galpy then keeps its own C path)."""
-    pt, pa = TP.potential("scf_nonaxi")
-    w = unit_deviations(cyl_to_rect(ics(2, False, 1)), 3)
-    with pytest.raises(gb.PotentialNotSupported):
-        gb.integrate_dxdv_batch((pt, pa), w, np.linspace(0, 1, 5), "rk4_cuda")
+@pytest.mark.parametrize("method", ["leapfrog", "rk4", "symplec4", "dop853"])
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", ["scf_axi+mn", "scf_nonaxi"])
+def test_variational_in_scf(oracle, name, method, planar):
+    """The SCF expansion's tidal tensor (second derivatives by the
+    recurrences, the reference's spherical-to-cylindrical chain rule, then
+    Cartesian) drives the deviations like the reference's."""
+    pt, pa = TP.potential(name, planar)
+    dim = 2 if planar else 3
+    w = unit_deviations(cyl_to_rect(ics(6, planar, 7)), dim)
+    t = np.linspace(0.0, 2.0, 17)
+    with oracle.phi_from_atan2():
+        ref, eref, nref = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar,
+                                                **tol(method))
+    out, err, ns = gb.integrate_dxdv_batch((pt, pa), w, t, method + "_cuda", planar=planar,
+                                           return_nsteps=True, **tol(method))
+    assert np.array_equal(err, eref) and np.array_equal(ns, nref)
+    rel = (np.abs(out - ref) / np.abs(ref).max(axis=1, keepdims=True)).max()
+    assert rel < 1e-9, rel
 
 
 @pytest.mark.parametrize("method", ["rk4", "dop853"])

@@ -225,3 +225,59 @@ def test_engine_machines_vs_oracle(harness, name, planar, method):
     strict = same & ~kink
     assert np.median(d[strict]) < 1e-12 and d[strict].max() < 1e-9, d[strict].max()
     assert (d < 1e-6).all()
+
+
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", ["scf_nonaxi", "scf_axi+mn"])
+def test_engine_scf_tidal_tensor(harness, name, planar):
+    """K = -grad grad Phi of the SCF expansion (engine: second derivatives
+    by the recurrences, chain rule to cylindrical, then Cartesian) against
+    the oracle's cylindrical second derivatives (the reference's
+    compute_scf_hessian_cyl, bit-exact with it)."""
+    pt, pa = TP.potential(name, planar)
+    rng = np.random.default_rng(12)
+    R = rng.uniform(0.3, 2.0, 150)
+    z = np.zeros(150) if planar else rng.normal(0, 0.4, 150)
+    phi = rng.uniform(0, 2 * np.pi, 150)
+    c, s = np.cos(phi), np.sin(phi)
+    _, K, _ = harness.forces(R * c, R * s, z, pt, pa, planar=planar)
+    f = oracle.forces(R, z, phi, pt, pa, planar=planar)
+    if planar:
+        Rf, tq, R2, p2, Rp = f.T
+        z2 = Rz = zp = np.zeros_like(R)
+    else:
+        Rf, zf, tq, R2, z2, Rz, p2, Rp, zp = f.T
+    # Cartesian -Hessian from the cylindrical derivatives (Rf = -Phi_R, tq = -Phi_phi)
+    PR, Pf = -Rf, -tq
+    Kxx = -(c * c * R2 - 2 * c * s / R * Rp + s * s / R**2 * p2 + s * s / R * PR +
+            2 * c * s / R**2 * Pf)
+    Kxy = -(c * s * R2 + (c * c - s * s) / R * Rp - c * s / R**2 * p2 - c * s / R * PR -
+            (c * c - s * s) / R**2 * Pf)
+    Kyy = -(s * s * R2 + 2 * c * s / R * Rp + c * c / R**2 * p2 + c * c / R * PR -
+            2 * c * s / R**2 * Pf)
+    ref = [Kxx, Kxy, Kyy]
+    if not planar:
+        ref += [-(c * Rz - s / R * zp), -(s * Rz + c / R * zp), -z2]
+    ref = np.stack(ref, 1)
+    scale = np.abs(ref).max()
+    assert np.abs(K[:, :ref.shape[1]] - ref).max() < 1e-12 * scale
+
+
+@pytest.mark.parametrize("method", ["leapfrog", "rk4", "symplec4", "dopr54", "dop853"])
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", ["scf_axi+mn", "scf_nonaxi", "bar_growing+mw14"])
+def test_engine_variational_vs_oracle(harness, name, planar, method):
+    from helpers import unit_deviations
+
+    pt, pa = TP.potential(name, planar)
+    dim = 2 if planar else 3
+    w = unit_deviations(c2r(ics(6, planar, seed=7), planar), dim)
+    t = np.linspace(0.0, 2.0, 17)
+    with oracle.phi_from_atan2():
+        ref, eref, nref = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar,
+                                                **tol(method))
+    out, err, ns = harness.integrate(w, t, pt, pa, method, planar=planar, var=True,
+                                     **tol(method))
+    assert np.array_equal(err, eref) and np.array_equal(ns, nref)
+    rel = (np.abs(out - ref) / np.abs(ref).max(axis=1, keepdims=True)).max()
+    assert rel < 1e-10, rel
