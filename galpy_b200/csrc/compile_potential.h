@@ -205,33 +205,78 @@ inline int comp_records(int type, const double* p)
   return 1 + (len + kPayloadDoubles - 1) / kPayloadDoubles;
 }
 
+// Arguments of a wrapper after its wrapped entries.
+inline int wrapper_nargs(int type) { return type == T_WRAP_SMOOTH ? 4 : 3; }
+
+// Records of n entries of galpy's (type, args) streams, advancing both; a
+// wrapper (one level deep) is its record plus its wrapped entries' records.
+// -3 (unsupported type, nested wrapper) or -1 (bad args).
+inline int count_entries(int planar, int n, const int*& tp, const double*& p, int depth)
+{
+  int rec = 0;
+  for (int k = 0; k < n; k++) {
+    const int type = *tp++;
+    if (is_wrapper(type)) {
+      if (depth > 0) return -3;
+      const int nw = (int)*p++;
+      if (nw < 1 || nw > kMaxComp) return -1;
+      const int inner = count_entries(planar, nw, tp, p, depth + 1);
+      if (inner < 0) return inner;
+      rec += 1 + inner;
+      p += wrapper_nargs(type);
+      continue;
+    }
+    const int na = galpy_nargs(type, planar, p);
+    if (na < 0) return -3;
+    rec += comp_records(type, p);
+    p += na;
+  }
+  return rec;
+}
+
 // Records of one group (the stride of a parameter group in the device
-// array); -3 (unsupported type) or -1 (bad args).
+// array, the launch's ncomp); -3 (unsupported type) or -1 (bad args).
 inline int group_records(int planar, int npot, const int* pot_type, const double* pot_args)
 {
   if (npot < 1 || npot > kMaxComp) return -1;
+  const int* tp = pot_type;
   const double* p = pot_args;
-  int n = 0;
-  for (int k = 0; k < npot; k++) {
-    const int na = galpy_nargs(pot_type[k], planar, p);
-    if (na < 0) return -3;
-    n += comp_records(pot_type[k], p);
-    p += na;
-  }
-  return n;
+  return count_entries(planar, npot, tp, p, 0);
 }
 
-// Compile one group into group_records(...) records.  Returns 0, -3
-// (unsupported type) or -1 (bad args).  *consumed receives the number of
-// pot_args read.
-inline int compile_group(int planar, int npot, const int* pot_type, const double* pot_args,
-                         GpComp* out, int* consumed)
+// Compile n entries of galpy's streams into out from record `rec` on
+// (advancing the streams and rec).
+inline int compile_entries(int planar, int n, const int*& tp, const double*& p, GpComp* out,
+                           int& rec, int depth)
 {
-  if (npot < 1 || npot > kMaxComp) return -1;
-  const double* p = pot_args;
-  int rec = 0;  // next record
-  for (int k = 0; k < npot; k++) {
-    const int type = pot_type[k];
+  for (int k = 0; k < n; k++) {
+    const int type = *tp++;
+    if (is_wrapper(type)) {
+      // the wrapper's record, then its wrapped entries' records; galpy's
+      // stream: (nwrapped, wrapped args, the wrapper's own args)
+      if (depth > 0) return -3;  // nested wrappers are not carried
+      const int nw = (int)*p++;
+      if (nw < 1 || nw > kMaxComp) return -1;
+      const int w = rec++;
+      const int rc = compile_entries(planar, nw, tp, p, out, rec, depth + 1);
+      if (rc) return rc;
+      GpComp& c = out[w];
+      memset(&c, 0, sizeof(c));
+      c.type = type;
+      c.c[0] = p[0];
+      c.c[1] = p[1];
+      c.c[2] = p[2];
+      if (type == T_WRAP_SMOOTH) {  // (amp, tform, tsteady, grow)
+        if (p[2] < p[1]) return -1;
+        c.c[3] = p[3];
+        c.c[4] = p[2] > p[1] ? 1.0 / (p[2] - p[1]) : 0.0;
+      } else if (type == T_WRAP_GAUSS && !(p[2] > 0.0)) {  // (amp, to, sigma^2)
+        return -1;
+      }
+      c.c[15] = rec - w - 1;
+      p += wrapper_nargs(type);
+      continue;
+    }
     const int na = galpy_nargs(type, planar, p);
     if (na < 0) return -3;
     const int nrec = comp_records(type, p);
@@ -487,6 +532,21 @@ inline int compile_group(int planar, int npot, const int* pot_type, const double
     rec += nrec;
     p += na;
   }
+  return 0;
+}
+
+// Compile one group (npot top-level entries of galpy's streams) into its
+// group_records(...) records.  Returns 0, -3 (unsupported type) or -1 (bad
+// args).  *consumed receives the number of pot_args read.
+inline int compile_group(int planar, int npot, const int* pot_type, const double* pot_args,
+                         GpComp* out, int* consumed)
+{
+  if (npot < 1 || npot > kMaxComp) return -1;
+  const int* tp = pot_type;
+  const double* p = pot_args;
+  int rec = 0;
+  const int rc = compile_entries(planar, npot, tp, p, out, rec, 0);
+  if (rc) return rc;
   if (consumed) *consumed = (int)(p - pot_args);
   return 0;
 }

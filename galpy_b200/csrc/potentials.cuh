@@ -892,6 +892,11 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
     }
     case T_PAYLOAD:  // an SCF component's coefficients
       break;
+    case T_WRAP_SMOOTH:
+    case T_WRAP_ROTATE:
+    case T_WRAP_GAUSS:  // opened by the full list's loop; no other list carries one
+      gR = T(NAN);
+      break;
     case T_DEHNENBAR:
     case T_SCF: {  // in float64; carried by the full run-time list only
       if constexpr (TYPE == kRunTimeAll) {
@@ -933,8 +938,13 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
 }
 
 // Run-time component list (any combination of the supported types).
-// The full list also carries the time-dependent DehnenBar and the SCF
-// expansion: its force reads the evaluation time (kTimeDep).
+// The full list also carries the time-dependent DehnenBar, the SCF
+// expansion and the wrappers: its force reads the evaluation time
+// (kTimeDep).  A wrapper opens a frame over the records it wraps: the
+// accumulators are set aside, the wrapped components are evaluated at the
+// point rotated by -alpha, and at the frame's end their acceleration,
+// rotated back by alpha and scaled by the wrapper's factor, joins a0 (R^2
+// and r^2 do not change under the rotation about z).
 struct DynPot {
   static constexpr bool kDirectScalars = false;
   static constexpr bool kAdditive = true;  // a component may add to a0
@@ -944,9 +954,42 @@ struct DynPot {
                                 T x, T y, T z, T z2, T R2, T r2, T& gR, T& gz, T& gyx,
                                 AddAcc<T>& a0, double t)
   {
-    for (int k = 0; k < ncomp; k++)
-      comp_accel<T, PLANAR, kRunTimeAll>(comp + k, ScalarsGlobal{comp + k}, x, y, z, z2, R2, r2,
-                                         gR, gz, gyx, a0, t);
+    int wend = -1;  // one past the open frame's last record
+    T xw = x, yw = y, sR = T(0), sz = T(0), syx = T(0);
+    AddAcc<T> sa{T(0), T(0), T(0)};
+    WrapFrame fr{1.0, 1.0, 0.0};
+    for (int k = 0; k <= ncomp; k++) {
+      if (k == wend) {  // close the frame
+        const T fc = T(fr.c), fs = T(fr.s), ff = T(fr.fac);
+        const T axw = xw * gR + a0.x, ayw = yw * (gR + gyx) + a0.y, azw = z * gz + a0.z;
+        gR = sR;
+        gz = sz;
+        gyx = syx;
+        a0.x = sa.x + ff * (fc * axw - fs * ayw);
+        a0.y = sa.y + ff * (fs * axw + fc * ayw);
+        if (!PLANAR) a0.z = sa.z + ff * azw;
+        xw = x;
+        yw = y;
+        wend = -1;
+      }
+      if (k == ncomp) break;
+      const int type = ldg(&comp[k].type);
+      if (is_wrapper(type)) {  // open a frame (wrappers do not nest)
+        fr = wrap_frame(comp + k, type, t);
+        wend = k + 1 + (int)ldg(&comp[k].c[15]);
+        sR = gR;
+        sz = gz;
+        syx = gyx;
+        sa = a0;
+        gR = gz = gyx = T(0);
+        a0 = AddAcc<T>{T(0), T(0), T(0)};
+        xw = T(fr.c) * x + T(fr.s) * y;
+        yw = T(fr.c) * y - T(fr.s) * x;
+        continue;
+      }
+      comp_accel<T, PLANAR, kRunTimeAll>(comp + k, ScalarsGlobal{comp + k}, xw, yw, z, z2, R2,
+                                         r2, gR, gz, gyx, a0, t);
+    }
   }
 };
 
@@ -1159,6 +1202,201 @@ GPC_HD inline void sph_derivs(const GpComp* __restrict__ cp, int type, double am
   }
 }
 
+// One component's acceleration terms and its part of K = d a / d x at
+// (x, y, z) (the full list's cases; wrappers are opened by accel_tidal).
+template <bool PLANAR>
+GPC_HD GPC_FI void comp_tidal(const GpComp* __restrict__ cp, int type, double x, double y,
+                              double z, double R2, double z2, double r2, double& gR, double& gz,
+                              double& gyx, double& ax0, double& ay0, double& az0, double K[6],
+                              double t)
+{
+  const double amp = ldg(&cp->c[0]);
+  switch (type) {
+    case T_PSWC: {
+      const double u = r2 * ldg(&cp->c[1]);
+      const double pw = exp(ldg(&cp->c[3]) * log(r2));  // (r^2)^(-alpha/2)
+      double Mr3;                                         // M(r) / r^3
+      if (u < ldg(&cp->c[5])) {
+        Mr3 = ldg(&cp->c[2]) * pw * gamma_star<double>(tables(cp), u, ldg(&cp->c[6]));
+      } else {
+        const double ir = rsq(r2);
+        Mr3 = ldg(&cp->c[4]) * ir * ir * ir;
+      }
+      const double dpr = amp * Mr3;  // Phi'/r
+      // Phi'' = amp (4 pi r^-alpha exp(-r^2/rc^2) - 2 M / r^3)
+      const double d2 = amp * (ldg(&cp->c[7]) * pw * exp(-u) - 2.0 * Mr3);
+      add_spherical(dpr, d2, x, y, z, r2, gR, gz, K);
+      break;
+    }
+    case T_NFW: {
+      const double a = ldg(&cp->c[1]);
+      const double ir = rsq(r2), r = r2 * ir;
+      const double L = log1p(r * ldg(&cp->c[2]));
+      const double iar = 1.0 / (a + r);
+      const double dpr = amp * (L * ir - iar) * ir * ir;  // Phi'/r
+      const double d2 = amp * (r * (2.0 * a + 3.0 * r) * iar * iar - 2.0 * L) * ir * ir * ir;
+      add_spherical(dpr, d2, x, y, z, r2, gR, gz, K);
+      break;
+    }
+    case T_HERNQUIST: {
+      const double a = ldg(&cp->c[1]);
+      const double ir = rsq(r2), r = r2 * ir;
+      const double ira = 1.0 / (r + a);
+      const double dpr = 0.5 * amp * ir * ira * ira;  // Phi'/r
+      const double d2 = -amp * ira * ira * ira;       // Phi''
+      add_spherical(dpr, d2, x, y, z, r2, gR, gz, K);
+      break;
+    }
+    case T_MN: {
+      // Phi = -amp (R^2 + s^2)^-1/2, s = a + zeta, zeta = sqrt(z^2 + b^2)
+      const double a = ldg(&cp->c[1]);
+      const double zb2 = z2 + ldg(&cp->c[2]);
+      const double izb = rsq(zb2), zeta = zb2 * izb, s = a + zeta;
+      const double iD = rsq(R2 + s * s), iD3 = iD * iD * iD, iD5 = iD3 * iD * iD;
+      const double sz = s * izb;  // s / zeta
+      gR -= amp * iD3;
+      gz -= amp * sz * iD3;
+      K[0] -= amp * (iD3 - 3.0 * x * x * iD5);
+      K[1] += 3.0 * amp * x * y * iD5;
+      K[2] -= amp * (iD3 - 3.0 * y * y * iD5);
+      K[3] += 3.0 * amp * x * z * sz * iD5;
+      K[4] += 3.0 * amp * y * z * sz * iD5;
+      // d2Phi/dz2 = amp [ iD3 (s/zeta - a z^2/zeta^3) - 3 z^2 (s/zeta)^2 iD5 ]
+      K[5] -= amp * (iD3 * (sz - a * z2 * izb * izb * izb) - 3.0 * z2 * sz * sz * iD5);
+      break;
+    }
+    case T_KKS: {
+      // Phi_R / R, Phi_RR, Phi_zz, Phi_Rz in (l, n) by the chain rule
+      // (KuzminKutuzovStaeckelPotential.c R2deriv / z2deriv / Rzderiv),
+      // then the axisymmetric Cartesian Hessian
+      const double D2 = ldg(&cp->c[1]);
+      const KksParts k = kks_parts(D2, ldg(&cp->c[2]), R2, z2);
+      const double r2 = R2 + z2, rzp = r2 + D2, rzm = r2 - D2, isd = k.isd;
+      const double id = isd * isd, id15 = isd * id;
+      const double isln3 = k.isln2 / (k.srl + k.srn);
+      const double d2l = (-3.0 * k.srl - k.srn) / (4.0 * k.l * k.srl) * isln3;
+      const double d2n = (-k.srl - 3.0 * k.srn) / (4.0 * k.n * k.srn) * isln3;
+      const double d2ln = -0.5 / (k.srl * k.srn) * isln3;
+      // first derivatives per unit R (resp. z) of l and n
+      const double lR = 1.0 + rzp * isd, nR = 1.0 - rzp * isd;
+      const double lz = 1.0 + rzm * isd, nz = 1.0 - rzm * isd;
+      const double gRk = -amp * (lR * k.dVdl + nR * k.dVdn);  // a_R / R
+      const double gzk = -amp * (lz * k.dVdl + nz * k.dVdn);  // a_z / z
+      const double offR = (3.0 * R2 + z2 + D2) * isd, cubR = 2.0 * R2 * rzp * rzp * id15;
+      const double offz = (R2 + 3.0 * z2 - D2) * isd, cubz = 2.0 * z2 * rzm * rzm * id15;
+      const double PRR = amp * ((1.0 + offR - cubR) * k.dVdl + (1.0 - offR + cubR) * k.dVdn +
+                                R2 * (lR * lR * d2l + nR * nR * d2n + 2.0 * lR * nR * d2ln));
+      const double Pzz = amp * ((1.0 + offz - cubz) * k.dVdl + (1.0 - offz + cubz) * k.dVdn +
+                                z2 * (lz * lz * d2l + nz * nz * d2n + 2.0 * lz * nz * d2ln));
+      const double mixRz = 2.0 * isd * (1.0 - (r2 * r2 - D2 * D2) * id);  // / (R z)
+      const double PRz_Rz = amp * (mixRz * (k.dVdl - k.dVdn) + lR * lz * d2l + nR * nz * d2n +
+                                   (lR * nz + lz * nR) * d2ln);  // Phi_Rz / (R z)
+      const double PR_R = -gRk;
+      gR += gRk;
+      gz += gzk;
+      const double iR2 = R2 > 0.0 ? 1.0 / R2 : 0.0;
+      K[0] -= PRR * x * x * iR2 + PR_R * y * y * iR2;
+      K[1] -= (PRR - PR_R) * x * y * iR2;
+      K[2] -= PRR * y * y * iR2 + PR_R * x * x * iR2;
+      K[3] -= PRz_Rz * x * z;
+      K[4] -= PRz_Rz * y * z;
+      K[5] -= Pzz;
+      break;
+    }
+    case T_FLATPOWER: {  // the logarithmic halo's structure with weight (alpha+2) m2^(-alpha/2-2)
+      const double iq2 = ldg(&cp->c[1]);
+      const double m2 = R2 + z2 * iq2 + ldg(&cp->c[2]);
+      const double pw = exp(ldg(&cp->c[3]) * log(m2)), g = -amp * pw;
+      const double h = amp * ldg(&cp->c[5]) * pw / m2;
+      const double ux = x, uy = y, uz = iq2 * z;
+      gR += g;
+      gz += g * iq2;
+      K[0] += g + h * ux * ux;
+      K[1] += h * ux * uy;
+      K[2] += g + h * uy * uy;
+      K[3] += h * ux * uz;
+      K[4] += h * uy * uz;
+      K[5] += g * iq2 + h * uz * uz;
+      break;
+    }
+    case T_LOGHALO: {
+      const double iq2 = ldg(&cp->c[1]), ye = ldg(&cp->c[3]);
+      const double D = x * x + ye * y * y + z2 * iq2 + ldg(&cp->c[2]);
+      const double iDl = 1.0 / D, g = -amp * iDl;
+      const double ux = x, uy = ye * y, uz = iq2 * z;  // grad of D / 2
+      gR += g;
+      gyx += g * (ye - 1.0);
+      gz += g * iq2;
+      const double h = 2.0 * amp * iDl * iDl;
+      K[0] += g + h * ux * ux;
+      K[1] += h * ux * uy;
+      K[2] += g * ye + h * uy * uy;
+      K[3] += h * ux * uz;
+      K[4] += h * uy * uz;
+      K[5] += g * iq2 + h * uz * uz;
+      break;
+    }
+    case T_HENONHEILES: {  // planar only; K = -amp ((1 + 2y, 2x), (2x, 1 - 2y))
+      gR -= amp * (1.0 + 2.0 * y);
+      gyx += 3.0 * amp * y;
+      ay0 -= amp * x * x;
+      K[0] -= amp * (1.0 + 2.0 * y);
+      K[1] -= 2.0 * amp * x;
+      K[2] -= amp * (1.0 - 2.0 * y);
+      break;
+    }
+    case T_KUZMINDISK: {  // Cartesian Hessian of -amp D^(-1/2), D = x^2 + y^2 + (a + |z|)^2
+      const double zs = (z > 0.0) - (z < 0.0), az = ldg(&cp->c[1]) + fabs(z);
+      const double D = R2 + az * az, iD = rsq(D), d15 = iD * iD * iD, d25 = d15 / D;
+      gR -= amp * d15;
+      az0 -= zs * amp * d15 * az;
+      if (PLANAR) {
+        // the reference's planar second derivative (KuzminDiskPotential.c,
+        // PlanarR2deriv) is amp (-D^(-3/2) + 3 R^2 D^(-5/2)), the opposite
+        // sign of d^2 Phi / dR^2 of its planar potential; planar
+        // variational runs follow it: K = -(Phi_RR c^2 + Phi_R/R s^2, ...)
+        const double PRR = -amp * (d15 - 3.0 * R2 * d25), PR_R = amp * d15;
+        const double iR2 = R2 > 0.0 ? 1.0 / R2 : 0.0;
+        K[0] -= (PRR * x * x + PR_R * y * y) * iR2;
+        K[1] -= (PRR - PR_R) * x * y * iR2;
+        K[2] -= (PRR * y * y + PR_R * x * x) * iR2;
+        break;
+      }
+      K[0] -= amp * (d15 - 3.0 * x * x * d25);
+      K[1] += 3.0 * amp * x * y * d25;
+      K[2] -= amp * (d15 - 3.0 * y * y * d25);
+      K[3] += 3.0 * amp * x * az * zs * d25;
+      K[4] += 3.0 * amp * y * az * zs * d25;
+      K[5] -= amp * (d15 - 3.0 * az * az * d25);
+      break;
+    }
+    case T_PAYLOAD:
+      break;
+    case T_DEHNENBAR:
+      dbar_tidal<PLANAR>(cp, t, x, y, z, ax0, ay0, az0, K);
+      break;
+    case T_SCF:
+      scf_tidal<PLANAR>(cp, x, y, z, ax0, ay0, az0, K);
+      break;
+    case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
+    case T_POWERTRI: case T_TWOPOWERTRI: {
+      double fx, fy, fz;
+      ell_accel(cp, type, x, y, z, fx, fy, fz);
+      ax0 += fx;
+      ay0 += fy;
+      az0 += fz;
+      ell_tidal(cp, type, x, y, z, K);
+      break;
+    }
+    default: {
+      double dpr, d2;  // Phi'/r, Phi''
+      sph_derivs(cp, type, amp, r2, dpr, d2);
+      add_spherical(dpr, d2, x, y, z, r2, gR, gz, K);
+      break;
+    }
+  }
+}
+
 template <bool PLANAR>
 GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, double x, double y,
                                double z, double& ax, double& ay, double& az, double K[6],
@@ -1169,194 +1407,55 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
   double gR = 0.0, gz = 0.0, gyx = 0.0, ax0 = 0.0, ay0 = 0.0, az0 = 0.0;
 #pragma unroll
   for (int i = 0; i < 6; i++) K[i] = 0.0;
-  for (int k = 0; k < ncomp; k++) {
+  // wrapper frames as in DynPot::sum; K of the wrapped records, taken in the
+  // rotated frame, returns as fac R(alpha) K' R(alpha)^T
+  int wend = -1;
+  double xw = x, yw = y, sR = 0.0, sz = 0.0, syx = 0.0, sx0 = 0.0, sy0 = 0.0, sz0 = 0.0, sK[6];
+  WrapFrame fr{1.0, 1.0, 0.0};
+  for (int k = 0; k <= ncomp; k++) {
+    if (k == wend) {
+      const double c = fr.c, s = fr.s, f = fr.fac;
+      const double axw = xw * gR + ax0, ayw = yw * (gR + gyx) + ay0, azw = z * gz + az0;
+      gR = sR;
+      gz = sz;
+      gyx = syx;
+      ax0 = sx0 + f * (c * axw - s * ayw);
+      ay0 = sy0 + f * (s * axw + c * ayw);
+      az0 = sz0 + (PLANAR ? 0.0 : f * azw);
+      const double kxx = K[0], kxy = K[1], kyy = K[2], kxz = K[3], kyz = K[4], kzz = K[5];
+      K[0] = sK[0] + f * (c * c * kxx - 2.0 * c * s * kxy + s * s * kyy);
+      K[1] = sK[1] + f * (c * s * (kxx - kyy) + (c * c - s * s) * kxy);
+      K[2] = sK[2] + f * (s * s * kxx + 2.0 * c * s * kxy + c * c * kyy);
+      K[3] = sK[3] + f * (c * kxz - s * kyz);
+      K[4] = sK[4] + f * (s * kxz + c * kyz);
+      K[5] = sK[5] + f * kzz;
+      xw = x;
+      yw = y;
+      wend = -1;
+    }
+    if (k == ncomp) break;
     const GpComp* cp = comp + k;
     const int type = ldg(&cp->type);
-    const double amp = ldg(&cp->c[0]);
-    switch (type) {
-      case T_PSWC: {
-        const double u = r2 * ldg(&cp->c[1]);
-        const double pw = exp(ldg(&cp->c[3]) * log(r2));  // (r^2)^(-alpha/2)
-        double Mr3;                                         // M(r) / r^3
-        if (u < ldg(&cp->c[5])) {
-          Mr3 = ldg(&cp->c[2]) * pw * gamma_star<double>(tables(cp), u, ldg(&cp->c[6]));
-        } else {
-          const double ir = rsq(r2);
-          Mr3 = ldg(&cp->c[4]) * ir * ir * ir;
-        }
-        const double dpr = amp * Mr3;  // Phi'/r
-        // Phi'' = amp (4 pi r^-alpha exp(-r^2/rc^2) - 2 M / r^3)
-        const double d2 = amp * (ldg(&cp->c[7]) * pw * exp(-u) - 2.0 * Mr3);
-        add_spherical(dpr, d2, x, y, z, r2, gR, gz, K);
-        break;
+    if (is_wrapper(type)) {
+      fr = wrap_frame(cp, type, t);
+      wend = k + 1 + (int)ldg(&cp->c[15]);
+      sR = gR;
+      sz = gz;
+      syx = gyx;
+      sx0 = ax0;
+      sy0 = ay0;
+      sz0 = az0;
+#pragma unroll
+      for (int i = 0; i < 6; i++) {
+        sK[i] = K[i];
+        K[i] = 0.0;
       }
-      case T_NFW: {
-        const double a = ldg(&cp->c[1]);
-        const double ir = rsq(r2), r = r2 * ir;
-        const double L = log1p(r * ldg(&cp->c[2]));
-        const double iar = 1.0 / (a + r);
-        const double dpr = amp * (L * ir - iar) * ir * ir;  // Phi'/r
-        const double d2 = amp * (r * (2.0 * a + 3.0 * r) * iar * iar - 2.0 * L) * ir * ir * ir;
-        add_spherical(dpr, d2, x, y, z, r2, gR, gz, K);
-        break;
-      }
-      case T_HERNQUIST: {
-        const double a = ldg(&cp->c[1]);
-        const double ir = rsq(r2), r = r2 * ir;
-        const double ira = 1.0 / (r + a);
-        const double dpr = 0.5 * amp * ir * ira * ira;  // Phi'/r
-        const double d2 = -amp * ira * ira * ira;       // Phi''
-        add_spherical(dpr, d2, x, y, z, r2, gR, gz, K);
-        break;
-      }
-      case T_MN: {
-        // Phi = -amp (R^2 + s^2)^-1/2, s = a + zeta, zeta = sqrt(z^2 + b^2)
-        const double a = ldg(&cp->c[1]);
-        const double zb2 = z2 + ldg(&cp->c[2]);
-        const double izb = rsq(zb2), zeta = zb2 * izb, s = a + zeta;
-        const double iD = rsq(R2 + s * s), iD3 = iD * iD * iD, iD5 = iD3 * iD * iD;
-        const double sz = s * izb;  // s / zeta
-        gR -= amp * iD3;
-        gz -= amp * sz * iD3;
-        K[0] -= amp * (iD3 - 3.0 * x * x * iD5);
-        K[1] += 3.0 * amp * x * y * iD5;
-        K[2] -= amp * (iD3 - 3.0 * y * y * iD5);
-        K[3] += 3.0 * amp * x * z * sz * iD5;
-        K[4] += 3.0 * amp * y * z * sz * iD5;
-        // d2Phi/dz2 = amp [ iD3 (s/zeta - a z^2/zeta^3) - 3 z^2 (s/zeta)^2 iD5 ]
-        K[5] -= amp * (iD3 * (sz - a * z2 * izb * izb * izb) - 3.0 * z2 * sz * sz * iD5);
-        break;
-      }
-      case T_KKS: {
-        // Phi_R / R, Phi_RR, Phi_zz, Phi_Rz in (l, n) by the chain rule
-        // (KuzminKutuzovStaeckelPotential.c R2deriv / z2deriv / Rzderiv),
-        // then the axisymmetric Cartesian Hessian
-        const double D2 = ldg(&cp->c[1]);
-        const KksParts k = kks_parts(D2, ldg(&cp->c[2]), R2, z2);
-        const double r2 = R2 + z2, rzp = r2 + D2, rzm = r2 - D2, isd = k.isd;
-        const double id = isd * isd, id15 = isd * id;
-        const double isln3 = k.isln2 / (k.srl + k.srn);
-        const double d2l = (-3.0 * k.srl - k.srn) / (4.0 * k.l * k.srl) * isln3;
-        const double d2n = (-k.srl - 3.0 * k.srn) / (4.0 * k.n * k.srn) * isln3;
-        const double d2ln = -0.5 / (k.srl * k.srn) * isln3;
-        // first derivatives per unit R (resp. z) of l and n
-        const double lR = 1.0 + rzp * isd, nR = 1.0 - rzp * isd;
-        const double lz = 1.0 + rzm * isd, nz = 1.0 - rzm * isd;
-        const double gRk = -amp * (lR * k.dVdl + nR * k.dVdn);  // a_R / R
-        const double gzk = -amp * (lz * k.dVdl + nz * k.dVdn);  // a_z / z
-        const double offR = (3.0 * R2 + z2 + D2) * isd, cubR = 2.0 * R2 * rzp * rzp * id15;
-        const double offz = (R2 + 3.0 * z2 - D2) * isd, cubz = 2.0 * z2 * rzm * rzm * id15;
-        const double PRR = amp * ((1.0 + offR - cubR) * k.dVdl + (1.0 - offR + cubR) * k.dVdn +
-                                  R2 * (lR * lR * d2l + nR * nR * d2n + 2.0 * lR * nR * d2ln));
-        const double Pzz = amp * ((1.0 + offz - cubz) * k.dVdl + (1.0 - offz + cubz) * k.dVdn +
-                                  z2 * (lz * lz * d2l + nz * nz * d2n + 2.0 * lz * nz * d2ln));
-        const double mixRz = 2.0 * isd * (1.0 - (r2 * r2 - D2 * D2) * id);  // / (R z)
-        const double PRz_Rz = amp * (mixRz * (k.dVdl - k.dVdn) + lR * lz * d2l + nR * nz * d2n +
-                                     (lR * nz + lz * nR) * d2ln);  // Phi_Rz / (R z)
-        const double PR_R = -gRk;
-        gR += gRk;
-        gz += gzk;
-        const double iR2 = R2 > 0.0 ? 1.0 / R2 : 0.0;
-        K[0] -= PRR * x * x * iR2 + PR_R * y * y * iR2;
-        K[1] -= (PRR - PR_R) * x * y * iR2;
-        K[2] -= PRR * y * y * iR2 + PR_R * x * x * iR2;
-        K[3] -= PRz_Rz * x * z;
-        K[4] -= PRz_Rz * y * z;
-        K[5] -= Pzz;
-        break;
-      }
-      case T_FLATPOWER: {  // the logarithmic halo's structure with weight (alpha+2) m2^(-alpha/2-2)
-        const double iq2 = ldg(&cp->c[1]);
-        const double m2 = R2 + z2 * iq2 + ldg(&cp->c[2]);
-        const double pw = exp(ldg(&cp->c[3]) * log(m2)), g = -amp * pw;
-        const double h = amp * ldg(&cp->c[5]) * pw / m2;
-        const double ux = x, uy = y, uz = iq2 * z;
-        gR += g;
-        gz += g * iq2;
-        K[0] += g + h * ux * ux;
-        K[1] += h * ux * uy;
-        K[2] += g + h * uy * uy;
-        K[3] += h * ux * uz;
-        K[4] += h * uy * uz;
-        K[5] += g * iq2 + h * uz * uz;
-        break;
-      }
-      case T_LOGHALO: {
-        const double iq2 = ldg(&cp->c[1]), ye = ldg(&cp->c[3]);
-        const double D = x * x + ye * y * y + z2 * iq2 + ldg(&cp->c[2]);
-        const double iDl = 1.0 / D, g = -amp * iDl;
-        const double ux = x, uy = ye * y, uz = iq2 * z;  // grad of D / 2
-        gR += g;
-        gyx += g * (ye - 1.0);
-        gz += g * iq2;
-        const double h = 2.0 * amp * iDl * iDl;
-        K[0] += g + h * ux * ux;
-        K[1] += h * ux * uy;
-        K[2] += g * ye + h * uy * uy;
-        K[3] += h * ux * uz;
-        K[4] += h * uy * uz;
-        K[5] += g * iq2 + h * uz * uz;
-        break;
-      }
-      case T_HENONHEILES: {  // planar only; K = -amp ((1 + 2y, 2x), (2x, 1 - 2y))
-        gR -= amp * (1.0 + 2.0 * y);
-        gyx += 3.0 * amp * y;
-        ay0 -= amp * x * x;
-        K[0] -= amp * (1.0 + 2.0 * y);
-        K[1] -= 2.0 * amp * x;
-        K[2] -= amp * (1.0 - 2.0 * y);
-        break;
-      }
-      case T_KUZMINDISK: {  // Cartesian Hessian of -amp D^(-1/2), D = x^2 + y^2 + (a + |z|)^2
-        const double zs = (z > 0.0) - (z < 0.0), az = ldg(&cp->c[1]) + fabs(z);
-        const double D = R2 + az * az, iD = rsq(D), d15 = iD * iD * iD, d25 = d15 / D;
-        gR -= amp * d15;
-        az0 -= zs * amp * d15 * az;
-        if (PLANAR) {
-          // the reference's planar second derivative (KuzminDiskPotential.c,
-          // PlanarR2deriv) is amp (-D^(-3/2) + 3 R^2 D^(-5/2)), the opposite
-          // sign of d^2 Phi / dR^2 of its planar potential; planar
-          // variational runs follow it: K = -(Phi_RR c^2 + Phi_R/R s^2, ...)
-          const double PRR = -amp * (d15 - 3.0 * R2 * d25), PR_R = amp * d15;
-          const double iR2 = R2 > 0.0 ? 1.0 / R2 : 0.0;
-          K[0] -= (PRR * x * x + PR_R * y * y) * iR2;
-          K[1] -= (PRR - PR_R) * x * y * iR2;
-          K[2] -= (PRR * y * y + PR_R * x * x) * iR2;
-          break;
-        }
-        K[0] -= amp * (d15 - 3.0 * x * x * d25);
-        K[1] += 3.0 * amp * x * y * d25;
-        K[2] -= amp * (d15 - 3.0 * y * y * d25);
-        K[3] += 3.0 * amp * x * az * zs * d25;
-        K[4] += 3.0 * amp * y * az * zs * d25;
-        K[5] -= amp * (d15 - 3.0 * az * az * d25);
-        break;
-      }
-      case T_PAYLOAD:
-        break;
-      case T_DEHNENBAR:
-        dbar_tidal<PLANAR>(cp, t, x, y, z, ax0, ay0, az0, K);
-        break;
-      case T_SCF:
-        scf_tidal<PLANAR>(cp, x, y, z, ax0, ay0, az0, K);
-        break;
-      case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
-      case T_POWERTRI: case T_TWOPOWERTRI: {
-        double fx, fy, fz;
-        ell_accel(cp, type, x, y, z, fx, fy, fz);
-        ax0 += fx;
-        ay0 += fy;
-        az0 += fz;
-        ell_tidal(cp, type, x, y, z, K);
-        break;
-      }
-      default: {
-        double dpr, d2;  // Phi'/r, Phi''
-        sph_derivs(cp, type, amp, r2, dpr, d2);
-        add_spherical(dpr, d2, x, y, z, r2, gR, gz, K);
-        break;
-      }
+      gR = gz = gyx = ax0 = ay0 = az0 = 0.0;
+      xw = fr.c * x + fr.s * y;
+      yw = fr.c * y - fr.s * x;
+      continue;
     }
+    comp_tidal<PLANAR>(cp, type, xw, yw, z, R2, z2, r2, gR, gz, gyx, ax0, ay0, az0, K, t);
   }
   ax = x * gR + ax0;
   ay = y * (gR + gyx) + ay0;
@@ -1452,6 +1551,90 @@ GPC_HD inline double ell_value(const GpComp* __restrict__ cp, int type, double x
 
 // Potential Phi(x, y, z) summed over one group's components, FP64
 // (the *PotentialEval functions of potential_c_ext/*.c).
+// One component's potential at (x, y, z) (wrappers are opened by
+// potential_value).
+GPC_HD inline double comp_value(const GpComp* __restrict__ cp, double x, double y, double z,
+                                double R2, double z2, double r2)
+{
+  const double amp = ldg(&cp->c[0]);
+  double phi = 0.0;
+  switch (ldg(&cp->type)) {
+    case T_PSWC: {
+      // amp 2 pi rc^(3-alpha) / r [ r/rc gamma(a1, u) - gamma(a2, u) ]
+      const double r = sqrt(r2), u = r2 * ldg(&cp->c[1]);
+      const double a1 = ldg(&cp->c[10]), a2 = ldg(&cp->c[13]);
+      const double g1 = ldg(&cp->c[11]) * inc_gamma_P(a1, u, ldg(&cp->c[12]));
+      const double g2 = ldg(&cp->c[14]) * inc_gamma_P(a2, u, ldg(&cp->c[15]));
+      phi += amp * ldg(&cp->c[8]) / r * (r / ldg(&cp->c[9]) * g1 - g2);
+      break;
+    }
+    case T_MN: {
+      const double s = ldg(&cp->c[1]) + sqrt(z2 + ldg(&cp->c[2]));
+      phi -= amp / sqrt(R2 + s * s);
+      break;
+    }
+    case T_NFW: {
+      const double r = sqrt(r2);
+      phi -= amp * log1p(r * ldg(&cp->c[2])) / r;
+      break;
+    }
+    case T_HERNQUIST: {
+      phi -= amp / (2.0 * (sqrt(r2) + ldg(&cp->c[1])));
+      break;
+    }
+    case T_LOGHALO: {
+      const double D = x * x + ldg(&cp->c[3]) * y * y + z2 * ldg(&cp->c[1]) + ldg(&cp->c[2]);
+      phi += 0.5 * amp * log(D);
+      break;
+    }
+    case T_KKS: {  // n clipped at 0 as the reference's Eval does
+      const double D2 = ldg(&cp->c[1]), r2 = R2 + z2, rzm = r2 - D2;
+      const double sd = sqrt(rzm * rzm + 4.0 * D2 * R2);
+      const double l = 0.5 * (r2 - ldg(&cp->c[2]) + sd), n = 0.5 * (r2 - ldg(&cp->c[2]) - sd);
+      phi -= amp / (sqrt(l) + sqrt(n > 0.0 ? n : 0.0));
+      break;
+    }
+    case T_FLATPOWER: {
+      const double m2 = R2 + z2 * ldg(&cp->c[1]) + ldg(&cp->c[2]), alpha = ldg(&cp->c[4]);
+      phi += alpha == 0.0 ? 0.5 * amp * log(m2) : -amp * pow(m2, -0.5 * alpha) / alpha;
+      break;
+    }
+    case T_HENONHEILES:  // amp (R^2/2 + R^3 sin(3 phi)/3)
+      phi += amp * (0.5 * R2 + x * x * y - y * y * y / 3.0);
+      break;
+    case T_KUZMINDISK: {
+      const double az = ldg(&cp->c[1]) + fabs(z);
+      phi -= amp / sqrt(R2 + az * az);
+      break;
+    }
+    case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
+    case T_POWERTRI:
+      phi += ell_value(cp, ldg(&cp->type), x, y, z);
+      break;
+    case T_TWOPOWERTRI:  // psi needs the Gauss hypergeometric function 2F1: not carried
+      phi += NAN;
+      break;
+    case T_PAYLOAD:
+      break;
+    case T_SCF: {
+      double ax, ay, az, p;
+      scf_accel<false>(cp, x, y, z, ax, ay, az, &p);
+      phi += p;
+      break;
+    }
+    case T_DEHNENBAR:  // time-dependent: not evaluated here (the host refuses it)
+      phi += NAN;
+      break;
+    default:
+      phi += sph_value(cp, ldg(&cp->type), amp, r2);
+      break;
+  }
+  return phi;
+}
+
+// Potential summed over one group's records; a wrapper scales the sum over
+// the records it wraps (evaluated at t = 0 as the reference's potential
+// evaluation does; the rotation wrapper has none: NaN).
 GPC_HD inline double potential_value(const GpComp* __restrict__ comp, int ncomp, double x,
                                      double y, double z)
 {
@@ -1459,78 +1642,17 @@ GPC_HD inline double potential_value(const GpComp* __restrict__ comp, int ncomp,
   double phi = 0.0;
   for (int k = 0; k < ncomp; k++) {
     const GpComp* cp = comp + k;
-    const double amp = ldg(&cp->c[0]);
-    switch (ldg(&cp->type)) {
-      case T_PSWC: {
-        // amp 2 pi rc^(3-alpha) / r [ r/rc gamma(a1, u) - gamma(a2, u) ]
-        const double r = sqrt(r2), u = r2 * ldg(&cp->c[1]);
-        const double a1 = ldg(&cp->c[10]), a2 = ldg(&cp->c[13]);
-        const double g1 = ldg(&cp->c[11]) * inc_gamma_P(a1, u, ldg(&cp->c[12]));
-        const double g2 = ldg(&cp->c[14]) * inc_gamma_P(a2, u, ldg(&cp->c[15]));
-        phi += amp * ldg(&cp->c[8]) / r * (r / ldg(&cp->c[9]) * g1 - g2);
-        break;
-      }
-      case T_MN: {
-        const double s = ldg(&cp->c[1]) + sqrt(z2 + ldg(&cp->c[2]));
-        phi -= amp / sqrt(R2 + s * s);
-        break;
-      }
-      case T_NFW: {
-        const double r = sqrt(r2);
-        phi -= amp * log1p(r * ldg(&cp->c[2])) / r;
-        break;
-      }
-      case T_HERNQUIST: {
-        phi -= amp / (2.0 * (sqrt(r2) + ldg(&cp->c[1])));
-        break;
-      }
-      case T_LOGHALO: {
-        const double D = x * x + ldg(&cp->c[3]) * y * y + z2 * ldg(&cp->c[1]) + ldg(&cp->c[2]);
-        phi += 0.5 * amp * log(D);
-        break;
-      }
-      case T_KKS: {  // n clipped at 0 as the reference's Eval does
-        const double D2 = ldg(&cp->c[1]), r2 = R2 + z2, rzm = r2 - D2;
-        const double sd = sqrt(rzm * rzm + 4.0 * D2 * R2);
-        const double l = 0.5 * (r2 - ldg(&cp->c[2]) + sd), n = 0.5 * (r2 - ldg(&cp->c[2]) - sd);
-        phi -= amp / (sqrt(l) + sqrt(n > 0.0 ? n : 0.0));
-        break;
-      }
-      case T_FLATPOWER: {
-        const double m2 = R2 + z2 * ldg(&cp->c[1]) + ldg(&cp->c[2]), alpha = ldg(&cp->c[4]);
-        phi += alpha == 0.0 ? 0.5 * amp * log(m2) : -amp * pow(m2, -0.5 * alpha) / alpha;
-        break;
-      }
-      case T_HENONHEILES:  // amp (R^2/2 + R^3 sin(3 phi)/3)
-        phi += amp * (0.5 * R2 + x * x * y - y * y * y / 3.0);
-        break;
-      case T_KUZMINDISK: {
-        const double az = ldg(&cp->c[1]) + fabs(z);
-        phi -= amp / sqrt(R2 + az * az);
-        break;
-      }
-      case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
-      case T_POWERTRI:
-        phi += ell_value(cp, ldg(&cp->type), x, y, z);
-        break;
-      case T_TWOPOWERTRI:  // psi needs the Gauss hypergeometric function 2F1: not carried
-        phi += NAN;
-        break;
-      case T_PAYLOAD:
-        break;
-      case T_SCF: {
-        double ax, ay, az, p;
-        scf_accel<false>(cp, x, y, z, ax, ay, az, &p);
-        phi += p;
-        break;
-      }
-      case T_DEHNENBAR:  // time-dependent: not evaluated here (the host refuses it)
-        phi += NAN;
-        break;
-      default:
-        phi += sph_value(cp, ldg(&cp->type), amp, r2);
-        break;
+    const int type = ldg(&cp->type);
+    if (is_wrapper(type)) {
+      const int nw = (int)ldg(&cp->c[15]);
+      const WrapFrame fr = wrap_frame(cp, type, 0.0);
+      double w = 0.0;
+      for (int j = 1; j <= nw; j++) w += comp_value(cp + j, x, y, z, R2, z2, r2);
+      phi += type == T_WRAP_ROTATE ? NAN : fr.fac * w;
+      k += nw;
+      continue;
     }
+    phi += comp_value(cp, x, y, z, R2, z2, r2);
   }
   return phi;
 }

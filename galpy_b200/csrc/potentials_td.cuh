@@ -29,6 +29,14 @@
 namespace gpc {
 
 enum : int { T_DEHNENBAR = 1, T_SCF = 24 };
+// Wrappers (DehnenSmoothWrapperPotential.c, SolidBodyRotationWrapperPotential.c,
+// GaussianAmplitudeWrapperPotential.c): a wrapper record is followed by the
+// records of the components it wraps (c15 holds their count).
+enum : int { T_WRAP_SMOOTH = -1, T_WRAP_ROTATE = -2, T_WRAP_GAUSS = -5 };
+GPC_HD GPC_FI constexpr bool is_wrapper(int t)
+{
+  return t == T_WRAP_SMOOTH || t == T_WRAP_ROTATE || t == T_WRAP_GAUSS;
+}
 // Continuation record of a component whose data does not fit one record
 // (an SCF expansion's coefficients): skipped by every component loop.
 enum : int { T_PAYLOAD = -100 };
@@ -36,7 +44,7 @@ enum : int { T_PAYLOAD = -100 };
 // Types that only the full run-time component list carries.
 GPC_HD GPC_FI constexpr bool needs_full_list(int t)
 {
-  return is_ellipsoidal(t) || t == T_DEHNENBAR || t == T_SCF || t == T_PAYLOAD;
+  return is_ellipsoidal(t) || t == T_DEHNENBAR || t == T_SCF || t == T_PAYLOAD || is_wrapper(t);
 }
 
 // Doubles of payload per continuation record: the record after its
@@ -56,6 +64,44 @@ GPC_HD GPC_FI double payload(const GpComp* __restrict__ cp, int j)
 // ---- DehnenBar ------------------------------------------------------------
 // Record: c0 amp (galpy's amp * af), c1 tform, c2 tsteady, c3 rb, c4 omegab,
 // c5 barphi, c6 rb^3, c7 1 / (tsteady - tform).
+// Growth factor of the bar and of DehnenSmoothWrapper (dehnenBarSmooth,
+// dehnenSmooth): 0 before tform, the quintic 3/16 xi^5 - 5/8 xi^3 + 15/16 xi
+// + 1/2 of xi = 2 (t - tform) / (tsteady - tform) - 1 until tsteady, 1 after
+// (inv: 1 / (tsteady - tform)).
+GPC_HD GPC_FI double dehnen_smooth(double t, double tform, double tsteady, double inv)
+{
+  if (t < tform) return 0.0;
+  if (t >= tsteady) return 1.0;
+  const double xi = 2.0 * (t - tform) * inv - 1.0, x2 = xi * xi;
+  return ((3.0 / 16.0 * x2 - 5.0 / 8.0) * x2 + 15.0 / 16.0) * xi + 0.5;
+}
+
+// A wrapper's effect at time t: the wrapped components' forces are scaled
+// by fac and evaluated in a frame rotated by alpha (cos c, sin s): at
+// phi - alpha, rotated back by alpha.  DehnenSmooth: fac = amp s(t) (1 - s
+// when not growing); GaussianAmplitude: amp exp(-(t - to)^2 / (2 sigma^2));
+// SolidBodyRotation: amp, alpha = omega t + pa.
+// Records: c0 amp; smooth c1 tform, c2 tsteady, c3 grow, c4 1/(tsteady -
+// tform); Gaussian c1 to, c2 sigma^2; rotation c1 omega, c2 pa.
+struct WrapFrame {
+  double fac, c, s;
+};
+
+GPC_HD GPC_FI WrapFrame wrap_frame(const GpComp* __restrict__ cp, int type, double t)
+{
+  WrapFrame f{ldg(&cp->c[0]), 1.0, 0.0};
+  if (type == T_WRAP_SMOOTH) {
+    const double sm = dehnen_smooth(t, ldg(&cp->c[1]), ldg(&cp->c[2]), ldg(&cp->c[4]));
+    f.fac *= ldg(&cp->c[3]) != 0.0 ? sm : 1.0 - sm;
+  } else if (type == T_WRAP_GAUSS) {
+    const double d = t - ldg(&cp->c[1]);
+    f.fac *= exp(-0.5 * d * d / ldg(&cp->c[2]));
+  } else {
+    sincos(ldg(&cp->c[1]) * t + ldg(&cp->c[2]), &f.s, &f.c);
+  }
+  return f;
+}
+
 struct BarParts {
   double A;           // amp * s(t)
   double cB, sB;      // cos, sin of 2 (omegab t + barphi)
@@ -66,15 +112,7 @@ struct BarParts {
 GPC_HD GPC_FI BarParts dbar_parts(const GpComp* __restrict__ cp, double t, double r2)
 {
   BarParts b;
-  const double tform = ldg(&cp->c[1]), tsteady = ldg(&cp->c[2]);
-  double s = 1.0;
-  if (t < tform) {
-    s = 0.0;
-  } else if (t < tsteady) {
-    const double xi = 2.0 * (t - tform) * ldg(&cp->c[7]) - 1.0, x2 = xi * xi;
-    s = ((3.0 / 16.0 * x2 - 5.0 / 8.0) * x2 + 15.0 / 16.0) * xi + 0.5;
-  }
-  b.A = ldg(&cp->c[0]) * s;
+  b.A = ldg(&cp->c[0]) * dehnen_smooth(t, ldg(&cp->c[1]), ldg(&cp->c[2]), ldg(&cp->c[7]));
   sincos(2.0 * (ldg(&cp->c[4]) * t + ldg(&cp->c[5])), &b.sB, &b.cB);
   const double rb = ldg(&cp->c[3]), rb3 = ldg(&cp->c[6]);
   const double ir2 = 1.0 / r2, ir = sqrt(ir2), ir4 = ir2 * ir2;

@@ -65,13 +65,14 @@ def _supported(pot, planar, purpose="integrate"):
         return False
     if purpose == "potential" and any(t in TIME_DEPENDENT_TYPES for t in types):
         return False
-    if T_SCF in types:  # time-dependent SCF coefficients are not carried
+    if T_SCF in types or any(t < 0 for t in types):
+        # time-dependent SCF coefficients and nested wrappers are not carried
         from . import _lib
 
         pt = np.ascontiguousarray(types, np.int32)
         pa = np.ascontiguousarray(pot_args, np.float64)
         return _lib.lib().galpy_cuda_comp_records(
-            int(planar), len(types), pt.ctypes.data_as(_lib._ip), pa.ctypes.data_as(_lib._dp)) > 0
+            int(planar), int(npot), pt.ctypes.data_as(_lib._ip), pa.ctypes.data_as(_lib._dp)) > 0
     return True
 
 

@@ -8,7 +8,9 @@ The engine integrates in the potentials galpy hands to C as pot_type codes
 17 (Plummer), 18 (PseudoIsothermal), 20 (Burkert), 33
 (DehnenCoreSpherical), 34 (DehnenSpherical), 35 (HomogeneousSphere), 40
 (Null), 41 (Einasto) and 46 (ExpTruncNFW), the time-dependent 1
-(DehnenBar) and 24 (SCF, static coefficients) -- the parsing is
+(DehnenBar) and 24 (SCF, static coefficients), and the wrappers -1
+(DehnenSmooth), -2 (SolidBodyRotation) and -5 (GaussianAmplitude) around
+them -- the parsing is
 galpy/orbit/integrateFullOrbit.py:43-614 (3D) and
 galpy/orbit/integratePlanarOrbit.py:33-663 (planar).
 
@@ -38,10 +40,13 @@ ELLIPSOIDAL_TYPES = (21, 22, 23, 30, 37, 38, 43)
 # DehnenBarPotential (its force depends on the time) and SCFPotential (the
 # Hernquist-Ostriker expansion; static coefficients only)
 T_DEHNENBAR, T_SCF = 1, 24
-TIME_DEPENDENT_TYPES = (T_DEHNENBAR,)
+# wrappers around other components (one level deep): DehnenSmooth,
+# SolidBodyRotation, GaussianAmplitude
+WRAPPER_TYPES = (-1, -2, -5)
+TIME_DEPENDENT_TYPES = (T_DEHNENBAR,) + WRAPPER_TYPES
 SUPPORTED_TYPES = (T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC, T_FLATPOWER,
                    T_KKS, T_HENONHEILES, T_KUZMINDISK, T_DEHNENBAR, T_SCF) + SPHERICAL_TYPES + \
-    ELLIPSOIDAL_TYPES
+    ELLIPSOIDAL_TYPES + WRAPPER_TYPES
 
 
 class _Potential:
@@ -173,11 +178,14 @@ def _is_galpy(p):
 
 
 def parse_pot(pot, planar=False):
-    """(npot, pot_type int32[], pot_args float64[]) for the C ABI."""
-    if isinstance(pot, tuple) and len(pot) == 2 and not isinstance(pot[0], _Potential):
+    """(npot, pot_type int32[], pot_args float64[]) for the C ABI.  An
+    already-parsed potential is (pot_type, pot_args), or (pot_type,
+    pot_args, npot) when a wrapper's wrapped types make galpy's count of
+    top-level entries npot differ from len(pot_type)."""
+    if isinstance(pot, tuple) and len(pot) in (2, 3) and not isinstance(pot[0], _Potential):
         pt = np.ascontiguousarray(pot[0], dtype=np.int32)
         pa = np.ascontiguousarray(pot[1], dtype=np.float64)
-        return len(pt), pt, pa
+        return (int(pot[2]) if len(pot) == 3 else len(pt)), pt, pa
     plist = pot if isinstance(pot, (list, tuple)) else [pot]
     if any(_is_galpy(p) for p in plist):
         if planar:

@@ -104,6 +104,11 @@ enum { PT_DEHNENBAR = 1 };
 /* SCFPotential (SCFPotential.c), static coefficients: args (a, isNonAxi, N,
    L, M, Nt = 0, Acos [N][L][M], Asin [N][L][M] if isNonAxi, 11 cache slots) */
 enum { PT_SCF = 24 };
+/* wrappers (DehnenSmoothWrapperPotential.c, SolidBodyRotationWrapperPotential.c,
+   GaussianAmplitudeWrapperPotential.c): type followed by the wrapped
+   components' types; args (nwrapped, the wrapped components' args, then
+   (amp, tform, tsteady, grow), (amp, omega, pa) or (amp, to, sigma^2)) */
+enum { PT_WRAP_SMOOTH = -1, PT_WRAP_ROTATE = -2, PT_WRAP_GAUSS = -5 };
 
 static int is_ellipsoidal(int type)
 {
@@ -142,6 +147,7 @@ typedef struct {
   double p[8];     /* the component's args as galpy passes them */
   const double *ea; /* all args (ellipsoidal and SCF components: the caller's array) */
   double t;        /* time of the current evaluation (time-dependent types) */
+  int nsub;        /* a wrapper: the entries it wraps, which follow it */
 } ocomp;
 
 typedef struct {
@@ -559,25 +565,55 @@ static double sph_eval(const ocomp *c, double R, double Z)
    integratePlanarOrbit.c:55-742 restricted to types 0/5/7/8/9/10/12/14/15/
    16/17/18/20/29 (planar)/33/34/35/40/41/46).
    Returns 0, or -1 for an unsupported type. */
+static int is_wrapper(int type)
+{
+  return type == PT_WRAP_SMOOTH || type == PT_WRAP_ROTATE || type == PT_WRAP_GAUSS;
+}
+
+/* n entries of the (type, args) streams into P->c from *idx on; a wrapper
+   (parse_leapFuncArgs_Full's nwrapped recursion, integrateFullOrbit.c:
+   1010-1018) is followed by its wrapped entries and records their count */
+static int decode_entries(opot *P, int *idx, int n, const int **type, const double **args,
+                          int planar)
+{
+  for (int e = 0; e < n; e++) {
+    if (*idx >= OMAXPOT) return -1;
+    const int t = *(*type)++;
+    ocomp *c = &P->c[(*idx)++];
+    c->type = t;
+    c->t = 0.;
+    c->nsub = 0;
+    for (int k = 0; k < 8; k++) c->p[k] = 0.;
+    if (is_wrapper(t)) {
+      const int nw = (int)*(*args)++;
+      const int first = *idx;
+      if (nw < 1 || decode_entries(P, idx, nw, type, args, planar)) return -1;
+      c->nsub = *idx - first;
+      const int na = t == PT_WRAP_SMOOTH ? 4 : 3;
+      for (int k = 0; k < na; k++) c->p[k] = (*args)[k];
+      c->ea = *args;
+      *args += na;
+      continue;
+    }
+    const double *a = *args;
+    int na = is_ellipsoidal(t) ? ell_nargs(a) : t == PT_SCF ? scf_nargs(a) : nargs_of(t, planar);
+    if (na < 0) return -1;
+    c->ea = a;
+    for (int k = 0; k < na && k < 8; k++) c->p[k] = a[k];
+    *args += na;
+  }
+  return 0;
+}
+
 static int opot_decode(opot *P, int npot, const int *type, const double *args, int planar)
 {
   if (npot > OMAXPOT || npot < 1) return -1;
-  P->n = npot;
   P->planar = planar;
   P->nforce = 0;
   P->t = 0.;
-  for (int i = 0; i < npot; i++) {
-    int na = is_ellipsoidal(type[i]) ? ell_nargs(args)
-             : type[i] == PT_SCF      ? scf_nargs(args)
-                                      : nargs_of(type[i], planar);
-    if (na < 0) return -1;
-    P->c[i].type = type[i];
-    P->c[i].ea = args;
-    P->c[i].t = 0.;
-    for (int k = 0; k < 8; k++) P->c[i].p[k] = 0.;
-    for (int k = 0; k < na && k < 8; k++) P->c[i].p[k] = args[k];
-    args += na;
-  }
+  int idx = 0;
+  if (decode_entries(P, &idx, npot, &type, &args, planar)) return -1;
+  P->n = idx;
   return 0;
 }
 
@@ -1565,6 +1601,58 @@ static double comp_eval(const ocomp *c, double R, double Z, double phi)
   return 0.;
 }
 
+/* ---- sums over components, through wrappers ---- */
+/* Quantities summed over a range of entries: 3D forces and second
+   derivatives, planar forces and second derivatives, potential values. */
+enum { Q_RF, Q_ZF, Q_PT, Q_H0, Q_H1, Q_H2, Q_H3, Q_H4, Q_H5, Q_PRF, Q_PPT, Q_PH0, Q_PH1,
+       Q_PH2, Q_EVAL };
+
+static double comp_quantity(ocomp *c, int q, double R, double z, double phi)
+{
+  switch (q) {
+  case Q_RF: return comp_Rforce(c, R, z, phi);
+  case Q_ZF: return comp_zforce(c, R, z, phi);
+  case Q_PT: return comp_phitorque(c, R, z, phi);
+  case Q_PRF: return comp_planarRforce(c, R, phi);
+  case Q_PPT: return comp_planarphitorque(c, R, phi);
+  case Q_PH0: case Q_PH1: case Q_PH2: return comp_planarhess(c, q - Q_PH0, R, phi);
+  case Q_EVAL: return comp_eval(c, R, z, phi);
+  default: return comp_hess(c, q - Q_H0, R, z, phi);
+  }
+}
+
+/* sum of quantity q over entries [i0, i1), in order; a wrapper contributes
+   its factor times the sum over its entries (at phi - omega t - pa for the
+   rotation wrapper): DehnenSmooth amp s(t) (1 - s(t) if not growing),
+   GaussianAmplitude amp exp(-(t - to)^2 / (2 sigma^2)), SolidBodyRotation
+   amp (galpy_potentials.c calc* over the wrapped list) */
+static double range_sum(opot *P, int i0, int i1, int q, double R, double z, double phi)
+{
+  double sum = 0.;
+  for (int i = i0; i < i1; i++) {
+    ocomp *c = &P->c[i];
+    if (!is_wrapper(c->type)) {
+      sum += comp_quantity(c, q, R, z, phi);
+      continue;
+    }
+    const double *a = c->p, t = c->t;
+    double fac, ph = phi;
+    if (c->type == PT_WRAP_SMOOTH) {
+      double sm = dbar_smooth(t, a[1], a[2]); /* dehnenSmooth: the same quintic */
+      fac = a[0] * ((int)a[3] ? sm : 1. - sm);
+    } else if (c->type == PT_WRAP_GAUSS) {
+      fac = a[0] * exp(-0.5 * (t - a[1]) * (t - a[1]) / a[2]);
+    } else {
+      fac = a[0];
+      ph = phi - a[1] * t - a[2];
+      if (q == Q_EVAL) fac = NAN; /* no C evaluation in the reference */
+    }
+    sum += fac * range_sum(P, i + 1, i + 1 + c->nsub, q, R, z, ph);
+    i += c->nsub;
+  }
+  return sum;
+}
+
 /* ------------------------------------------------------------------ */
 /* right-hand sides                                                    */
 /* ------------------------------------------------------------------ */
@@ -1609,9 +1697,9 @@ static void sum3(opot *P, double R, double z, double phi, double *Rf, double *zf
 {
   double a = 0., b = 0., c = 0.;
   stamp_time(P);
-  for (int i = 0; i < P->n; i++) a += comp_Rforce(&P->c[i], R, z, phi);
-  for (int i = 0; i < P->n; i++) c += comp_phitorque(&P->c[i], R, z, phi);
-  for (int i = 0; i < P->n; i++) b += comp_zforce(&P->c[i], R, z, phi);
+  a = range_sum(P, 0, P->n, Q_RF, R, z, phi);
+  c = range_sum(P, 0, P->n, Q_PT, R, z, phi);
+  b = range_sum(P, 0, P->n, Q_ZF, R, z, phi);
   *Rf = a;
   *zf = b;
   *pt = c;
@@ -1622,8 +1710,8 @@ static void sum2(opot *P, double R, double phi, double *Rf, double *pt)
 {
   double a = 0., c = 0.;
   stamp_time(P);
-  for (int i = 0; i < P->n; i++) a += comp_planarRforce(&P->c[i], R, phi);
-  for (int i = 0; i < P->n; i++) c += comp_planarphitorque(&P->c[i], R, phi);
+  a = range_sum(P, 0, P->n, Q_PRF, R, 0., phi);
+  c = range_sum(P, 0, P->n, Q_PPT, R, 0., phi);
   *Rf = a;
   *pt = c;
   P->nforce++;
@@ -1688,7 +1776,7 @@ static void hess3(opot *P, double R, double z, double phi, double h[6])
   stamp_time(P);
   for (int w = 0; w < 6; w++) {
     double s = 0.;
-    for (int i = 0; i < P->n; i++) s += comp_hess(&P->c[i], w, R, z, phi);
+    s = range_sum(P, 0, P->n, Q_H0 + w, R, z, phi);
     h[w] = s;
   }
 }
@@ -1747,9 +1835,9 @@ static void planar_hess_sum(opot *P, double R, double phi, double *R2d, double *
 {
   double a = 0., b = 0., c = 0.;
   stamp_time(P);
-  for (int i = 0; i < P->n; i++) a += comp_planarhess(&P->c[i], 0, R, phi);
-  for (int i = 0; i < P->n; i++) b += comp_planarhess(&P->c[i], 1, R, phi);
-  for (int i = 0; i < P->n; i++) c += comp_planarhess(&P->c[i], 2, R, phi);
+  a = range_sum(P, 0, P->n, Q_PH0, R, 0., phi);
+  b = range_sum(P, 0, P->n, Q_PH1, R, 0., phi);
+  c = range_sum(P, 0, P->n, Q_PH2, R, 0., phi);
   *R2d = a;
   *p2d = b;
   *Rpd = c;
@@ -2865,7 +2953,7 @@ EXPORT int oracle_potential(int n, const double *R, const double *z, const doubl
   if (opot_decode(&P, npot, pot_type, pot_args, 0)) return -3;
   for (int i = 0; i < n; i++) {
     double s = 0.;
-    for (int k = 0; k < P.n; k++) s += comp_eval(&P.c[k], R[i], z[i], phi[i]);
+    s = range_sum(&P, 0, P.n, Q_EVAL, R[i], z[i], phi[i]);
     out[i] = s;
   }
   return 0;

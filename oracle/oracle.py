@@ -123,6 +123,9 @@ def _tol(rtol, atol):
     return float(r), float(a)
 
 
+# npot (every function below): galpy's count of top-level potential entries,
+# which differs from len(pot_type) when a wrapper (negative type) carries
+# wrapped components; default len(pot_type).
 def _prep(yo, t, pot_type, pot_args):
     yo = np.array(yo, dtype=np.float64, order="C", copy=True)
     t = np.ascontiguousarray(t, dtype=np.float64)
@@ -132,7 +135,7 @@ def _prep(yo, t, pot_type, pot_args):
 
 
 def integrate(yo, t, pot_type, pot_args, method, planar=False, dt=None, rtol=None, atol=None,
-              nthreads=0, max_attempts=0, impl="port"):
+              nthreads=0, max_attempts=0, impl="port", npot=None):
     """Integrate nobj orbits with galpy's conventions.
 
     yo: (nobj, 6) cylindrical (R,vR,vT,z,vz,phi), or (nobj, 4) (R,vR,vT,phi)
@@ -152,7 +155,7 @@ def integrate(yo, t, pot_type, pot_args, method, planar=False, dt=None, rtol=Non
         nsteps = np.zeros(nobj, dtype=np.int64)
         nforce = np.zeros(nobj, dtype=np.int64)
         rc = port().oracle_integrate(
-            int(planar), nobj, _ptr(yo, _dp), nt, _ptr(t, _dp), indiv_t, len(pt), _ptr(pt, _ip),
+            int(planar), nobj, _ptr(yo, _dp), nt, _ptr(t, _dp), indiv_t, (len(pt) if npot is None else int(npot)), _ptr(pt, _ip),
             _ptr(pa, _dp), dtv, r, a, _ptr(result, _dp), _ptr(err, _ip), m, _ptr(nsteps, _lp),
             _ptr(nforce, _lp), int(max_attempts), int(nthreads))
         if rc != 0:
@@ -168,13 +171,13 @@ def integrate(yo, t, pot_type, pot_args, method, planar=False, dt=None, rtol=Non
                    ctypes.c_int, ctypes.c_void_p]
     if nthreads:
         os.environ["OMP_NUM_THREADS"] = str(nthreads)
-    fn(nobj, _ptr(yo, _dp), nt, _ptr(t, _dp), indiv_t, len(pt), _ptr(pt, _ip), _ptr(pa, _dp),
+    fn(nobj, _ptr(yo, _dp), nt, _ptr(t, _dp), indiv_t, (len(pt) if npot is None else int(npot)), _ptr(pt, _ip), _ptr(pa, _dp),
        None, dtv, r, a, _ptr(result, _dp), _ptr(err, _ip), m, None)
     return result, err, None, None
 
 
 def integrate_dxdv(w, t, pot_type, pot_args, method, planar=False, dt=None, rtol=None,
-                   atol=None, nthreads=0, impl="port"):
+                   atol=None, nthreads=0, impl="port", npot=None):
     """Variational integration, rectangular in and out.
 
     w: (nobj, 4*dim) = (x, v, dx, dv) per orbit; returns (result (nobj, nt,
@@ -192,7 +195,7 @@ def integrate_dxdv(w, t, pot_type, pot_args, method, planar=False, dt=None, rtol
     if impl == "port":
         nsteps = np.zeros(nobj, dtype=np.int64)
         rc = port().oracle_integrate_dxdv(
-            int(planar), nobj, _ptr(w, _dp), nt, _ptr(t, _dp), indiv_t, len(pt), _ptr(pt, _ip),
+            int(planar), nobj, _ptr(w, _dp), nt, _ptr(t, _dp), indiv_t, (len(pt) if npot is None else int(npot)), _ptr(pt, _ip),
             _ptr(pa, _dp), dtv, r, a, _ptr(result, _dp), _ptr(err, _ip), m, _ptr(nsteps, _lp),
             int(nthreads))
         if rc != 0:
@@ -216,7 +219,7 @@ def integrate_dxdv(w, t, pot_type, pot_args, method, planar=False, dt=None, rtol
         ti = np.ascontiguousarray(t[i] if indiv_t else t)
         res = np.empty((nt, nv))
         e = np.zeros(1, dtype=np.int32)
-        args = [_ptr(wi, _dp), nt, _ptr(ti, _dp), len(pt), _ptr(pt, _ip), _ptr(pa, _dp), None,
+        args = [_ptr(wi, _dp), nt, _ptr(ti, _dp), (len(pt) if npot is None else int(npot)), _ptr(pt, _ip), _ptr(pa, _dp), None,
                 dtv, r, a, _ptr(res, _dp), _ptr(e, _ip), m]
         if planar:
             args.append(None)
@@ -227,7 +230,7 @@ def integrate_dxdv(w, t, pot_type, pot_args, method, planar=False, dt=None, rtol
 
 
 def integrate_sos(yo, psi, pot_type, pot_args, method, dpsi=None, rtol=None, atol=None,
-                  nthreads=0, impl="port", planar=False, surface=0):
+                  nthreads=0, impl="port", planar=False, surface=0, npot=None):
     """Surface-of-section integration (integrateFullOrbit_sos, or
     integratePlanarOrbit_sos when planar with surface 0 (x = 0) or 1 (y = 0)).
 
@@ -248,12 +251,12 @@ def integrate_sos(yo, psi, pot_type, pot_args, method, dpsi=None, rtol=None, ato
         nsteps = np.zeros(nobj, dtype=np.int64)
         if planar:
             rc = port().oracle_integrate_sos_planar(
-                nobj, _ptr(yo, _dp), npsi, _ptr(psi, _dp), indiv, int(surface), len(pt),
+                nobj, _ptr(yo, _dp), npsi, _ptr(psi, _dp), indiv, int(surface), (len(pt) if npot is None else int(npot)),
                 _ptr(pt, _ip), _ptr(pa, _dp), dv, r, a, _ptr(result, _dp), _ptr(err, _ip), m,
                 _ptr(nsteps, _lp), int(nthreads))
         else:
             rc = port().oracle_integrate_sos(nobj, _ptr(yo, _dp), npsi, _ptr(psi, _dp), indiv,
-                                             len(pt), _ptr(pt, _ip), _ptr(pa, _dp), dv, r, a,
+                                             (len(pt) if npot is None else int(npot)), _ptr(pt, _ip), _ptr(pa, _dp), dv, r, a,
                                              _ptr(result, _dp), _ptr(err, _ip), m,
                                              _ptr(nsteps, _lp), int(nthreads))
         if rc != 0:
@@ -270,7 +273,7 @@ def integrate_sos(yo, psi, pot_type, pot_args, method, dpsi=None, rtol=None, ato
         fn.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int,
                        ctypes.c_int, _ip, _dp, ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
                        ctypes.c_double, _dp, _ip, ctypes.c_int, ctypes.c_void_p]
-        fn(nobj, _ptr(yo, _dp), npsi, _ptr(psi, _dp), indiv, int(surface), len(pt),
+        fn(nobj, _ptr(yo, _dp), npsi, _ptr(psi, _dp), indiv, int(surface), (len(pt) if npot is None else int(npot)),
            _ptr(pt, _ip), _ptr(pa, _dp), None, dv, r, a, _ptr(result, _dp), _ptr(err, _ip), m,
            None)
         return result, err, None
@@ -279,12 +282,12 @@ def integrate_sos(yo, psi, pot_type, pot_args, method, dpsi=None, rtol=None, ato
     fn.argtypes = [ctypes.c_int, _dp, ctypes.c_int, _dp, ctypes.c_int, ctypes.c_int, _ip, _dp,
                    ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, _ip,
                    ctypes.c_int, ctypes.c_void_p]
-    fn(nobj, _ptr(yo, _dp), npsi, _ptr(psi, _dp), indiv, len(pt), _ptr(pt, _ip), _ptr(pa, _dp),
+    fn(nobj, _ptr(yo, _dp), npsi, _ptr(psi, _dp), indiv, (len(pt) if npot is None else int(npot)), _ptr(pt, _ip), _ptr(pa, _dp),
        None, dv, r, a, _ptr(result, _dp), _ptr(err, _ip), m, None)
     return result, err, None
 
 
-def forces(R, z, phi, pot_type, pot_args, planar=False, t=0.0):
+def forces(R, z, phi, pot_type, pot_args, planar=False, t=0.0, npot=None):
     """Per-point (Rforce, zforce, phitorque, R2, z2, Rz, phi2, Rphi, zphi)
     (3D) or (Rforce, phitorque, R2, phi2, Rphi) (planar), at time t."""
     R = np.ascontiguousarray(R, dtype=np.float64)
@@ -294,20 +297,20 @@ def forces(R, z, phi, pot_type, pot_args, planar=False, t=0.0):
     pa = np.ascontiguousarray(pot_args, dtype=np.float64)
     out = np.empty((R.size, 5 if planar else 9))
     rc = port().oracle_forces(int(planar), R.size, _ptr(R, _dp), _ptr(z, _dp), _ptr(phi, _dp),
-                              len(pt), _ptr(pt, _ip), _ptr(pa, _dp), _ptr(out, _dp), float(t))
+                              (len(pt) if npot is None else int(npot)), _ptr(pt, _ip), _ptr(pa, _dp), _ptr(out, _dp), float(t))
     if rc:
         raise ValueError(f"oracle_forces returned {rc}")
     return out
 
 
-def potential(R, z, phi, pot_type, pot_args):
+def potential(R, z, phi, pot_type, pot_args, npot=None):
     R = np.ascontiguousarray(R, dtype=np.float64)
     z = np.ascontiguousarray(np.broadcast_to(z, R.shape), dtype=np.float64)
     phi = np.ascontiguousarray(np.broadcast_to(phi, R.shape), dtype=np.float64)
     pt = np.ascontiguousarray(pot_type, dtype=np.int32)
     pa = np.ascontiguousarray(pot_args, dtype=np.float64)
     out = np.empty(R.size)
-    rc = port().oracle_potential(R.size, _ptr(R, _dp), _ptr(z, _dp), _ptr(phi, _dp), len(pt),
+    rc = port().oracle_potential(R.size, _ptr(R, _dp), _ptr(z, _dp), _ptr(phi, _dp), (len(pt) if npot is None else int(npot)),
                                  _ptr(pt, _ip), _ptr(pa, _dp), _ptr(out, _dp))
     if rc:
         raise ValueError(f"oracle_potential returned {rc}")

@@ -69,11 +69,15 @@ METHOD_CODES = {"leapfrog": 0, "rk4": 1, "rk6": 2, "symplec4": 3, "symplec6": 4,
 
 
 class Harness:
+    """npot (integrate, dop853_queued, integrate_sos, forces): galpy's count
+    of top-level potential entries when a wrapper carries wrapped ones
+    (default len(pot_type))."""
+
     def __init__(self, lib):
         self.lib = lib
 
     def integrate(self, w, t, pot_type, pot_args, method, planar=False, var=False, f32=False,
-                  dt=None, rtol=None, atol=None, max_attempts=0):
+                  dt=None, rtol=None, atol=None, max_attempts=0, npot=None):
         w = np.ascontiguousarray(w, dtype=np.float64)
         t = np.ascontiguousarray(t, dtype=np.float64)
         n, nv = w.shape
@@ -87,7 +91,7 @@ class Harness:
         a = -12 * np.log(10) if atol is None else np.log(atol)
         rc = self.lib.harness_integrate(
             int(planar), int(var), METHOD_CODES[method], int(f32), n, w.ctypes.data_as(_dp), nt,
-            t.ctypes.data_as(_dp), int(t.ndim > 1), len(pt), pt.ctypes.data_as(_ip),
+            t.ctypes.data_as(_dp), int(t.ndim > 1), (len(pt) if npot is None else npot), pt.ctypes.data_as(_ip),
             pa.ctypes.data_as(_dp), ctypes.c_double(-9999.99 if dt is None else dt),
             ctypes.c_double(r), ctypes.c_double(a), ctypes.c_longlong(max_attempts),
             out.ctypes.data_as(_dp), err.ctypes.data_as(_ip), ns.ctypes.data_as(_lp))
@@ -95,7 +99,7 @@ class Harness:
         return out, err, ns
 
     def dop853_queued(self, w, t, pot_type, pot_args, planar=False, rtol=None, atol=None,
-                      max_attempts=0):
+                      max_attempts=0, npot=None):
         """DOP853 with its dense output through the kernels' request record
         (served one request at a time); same return values as integrate."""
         w = np.ascontiguousarray(w, dtype=np.float64)
@@ -111,14 +115,14 @@ class Harness:
         a = -12 * np.log(10) if atol is None else np.log(atol)
         rc = self.lib.harness_dop853_queued(
             int(planar), n, w.ctypes.data_as(_dp), nt, t.ctypes.data_as(_dp), int(t.ndim > 1),
-            len(pt), pt.ctypes.data_as(_ip), pa.ctypes.data_as(_dp), ctypes.c_double(r),
+            (len(pt) if npot is None else npot), pt.ctypes.data_as(_ip), pa.ctypes.data_as(_dp), ctypes.c_double(r),
             ctypes.c_double(a), ctypes.c_longlong(max_attempts), out.ctypes.data_as(_dp),
             err.ctypes.data_as(_ip), ns.ctypes.data_as(_lp))
         assert rc == 0, rc
         return out, err, ns
 
     def integrate_sos(self, w, psi, pot_type, pot_args, method, dpsi=None, rtol=None,
-                      atol=None, max_attempts=0, surface=None):
+                      atol=None, max_attempts=0, surface=None, npot=None):
         """SOS machines on SOS states: 3D w [n][7], or planar w [n][5] with
         surface 0 (x = 0) or 1 (y = 0); returns raw rows [n][npsi][7 | 5]."""
         w = np.ascontiguousarray(w, dtype=np.float64)
@@ -136,14 +140,14 @@ class Harness:
         rc = self.lib.harness_integrate_sos(
             system, METHOD_CODES[method], n, w.ctypes.data_as(_dp), npsi,
             psi.ctypes.data_as(_dp),
-            int(psi.ndim > 1), len(pt), pt.ctypes.data_as(_ip), pa.ctypes.data_as(_dp),
+            int(psi.ndim > 1), (len(pt) if npot is None else npot), pt.ctypes.data_as(_ip), pa.ctypes.data_as(_dp),
             ctypes.c_double(-9999.99 if dpsi is None else dpsi), ctypes.c_double(r),
             ctypes.c_double(a), ctypes.c_longlong(max_attempts), out.ctypes.data_as(_dp),
             err.ctypes.data_as(_ip), ns.ctypes.data_as(_lp))
         assert rc == 0, rc
         return out, err, ns
 
-    def forces(self, x, y, z, pot_type, pot_args, planar=False, t=0.0):
+    def forces(self, x, y, z, pot_type, pot_args, planar=False, t=0.0, npot=None):
         x, y, z = (np.ascontiguousarray(v, np.float64) for v in (x, y, z))
         n = len(x)
         acc, tid, a32 = np.zeros((n, 3)), np.zeros((n, 6)), np.zeros((n, 3))
@@ -151,7 +155,7 @@ class Harness:
         pa = np.ascontiguousarray(pot_args, np.float64)
         rc = self.lib.harness_forces_at(
             int(planar), n, x.ctypes.data_as(_dp), y.ctypes.data_as(_dp), z.ctypes.data_as(_dp),
-            ctypes.c_double(t), len(pt), pt.ctypes.data_as(_ip), pa.ctypes.data_as(_dp),
+            ctypes.c_double(t), (len(pt) if npot is None else npot), pt.ctypes.data_as(_ip), pa.ctypes.data_as(_dp),
             acc.ctypes.data_as(_dp), tid.ctypes.data_as(_dp), a32.ctypes.data_as(_dp))
         assert rc == 0, rc
         return acc, tid, a32

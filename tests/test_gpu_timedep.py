@@ -168,3 +168,53 @@ def test_device_forces_and_potential(oracle):
         gb.energy_device(torch.from_numpy(comps).to(dev), nrec, w, E)
         ref = oracle.potential(R, z, phi, pt, pa)
         assert np.abs(E.cpu().numpy() - ref).max() < 1e-13 * np.abs(ref).max(), name
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", TP.WRAPPED)
+def test_wrapped_orbits_vs_oracle(oracle, name, planar, method):
+    """Wrappers (DehnenSmooth, SolidBodyRotation, GaussianAmplitude) around
+    a bar or a triaxial halo, next to MWPotential2014, through galpy's entry
+    points with galpy's (pot_type, pot_args, npot)."""
+    pt, pa, npot = TP.wrapped(name, planar)
+    y0 = ics(128, planar, 31 + TP.WRAPPED.index(name))
+    t = np.linspace(0.0, 10.0, 41)
+    with oracle.phi_from_atan2():
+        ref, eref, nref, _ = oracle.integrate(y0, t, pt, pa, method, planar=planar, npot=npot,
+                                              **tol(method))
+    fn = gb.integratePlanarOrbit_cuda if planar else gb.integrateFullOrbit_cuda
+    out, err, ns = fn((pt, pa, npot), y0.copy(), t, method + "_cuda", progressbar=False,
+                      return_nsteps=True, **tol(method))
+    assert not err.any() and not eref.any()
+    d = cyl_diff(ref, out).max(axis=(1, 2))
+    same = ns == nref
+    kink = TP.crosses_bar_radius(ref) if "bar" in name and method == "dop853" else \
+        np.zeros(len(ns), bool)
+    assert same[~kink].mean() >= 0.99, same[~kink].mean()
+    far = same & ~kink & (d > 1e-10)
+    if far.any():
+        with oracle.phi_from_atan2():
+            resp = np.maximum(*[TP.ulp_response(oracle, y0[far], t, pt, pa, method, planar,
+                                                ref[far], seed=sd, npot=npot, **tol(method))
+                                for sd in (3, 4)])
+        assert (d[far] <= 30 * resp).all(), (d[far], resp)
+    assert (d[~same | kink] < 1e-6).all(), d[~same | kink]
+
+
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", ["smooth(bar)+mw14", "rotate(loghalo)+mw14"])
+def test_wrapped_variational(oracle, name, planar):
+    pt, pa, npot = TP.wrapped(name, planar)
+    dim = 2 if planar else 3
+    w = unit_deviations(cyl_to_rect(ics(6, planar, 5)), dim)
+    t = np.linspace(0.0, 4.0, 17)
+    for method in ("rk4", "symplec4"):
+        with oracle.phi_from_atan2():
+            ref, eref, nref = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar,
+                                                    npot=npot)
+        out, err, ns = gb.integrate_dxdv_batch((pt, pa, npot), w, t, method + "_cuda",
+                                               planar=planar, return_nsteps=True)
+        assert np.array_equal(err, eref) and np.array_equal(ns, nref)
+        rel = (np.abs(out - ref) / np.abs(ref).max(axis=1, keepdims=True)).max()
+        assert rel < 1e-9, (method, rel)

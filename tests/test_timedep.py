@@ -281,3 +281,115 @@ def test_engine_variational_vs_oracle(harness, name, planar, method):
     assert np.array_equal(err, eref) and np.array_equal(ns, nref)
     rel = (np.abs(out - ref) / np.abs(ref).max(axis=1, keepdims=True)).max()
     assert rel < 1e-10, rel
+
+
+# ---- wrappers: DehnenSmooth, SolidBodyRotation, GaussianAmplitude ----------
+@needs_ref
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", TP.WRAPPED)
+@pytest.mark.parametrize("method", ["leapfrog", "rk6", "symplec6", "dopr54", "dop853"])
+def test_wrapped_orbits_bit_exact_vs_reference_build(name, planar, method):
+    pt, pa, npot = TP.wrapped(name, planar)
+    yo = ics(8, planar)
+    t = np.linspace(0.0, 8.0, 41)
+    a, ea, _, _ = oracle.integrate(yo, t, pt, pa, method, planar=planar, npot=npot, **tol(method))
+    b, eb, _, _ = oracle.integrate(yo, t, pt, pa, method, planar=planar, npot=npot, impl="ref",
+                                   **tol(method))
+    np.testing.assert_array_equal(ea, eb)
+    np.testing.assert_array_equal(a, b)
+
+
+@needs_ref
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", ["smooth(bar)+mw14", "rotate(loghalo)+mw14"])
+def test_wrapped_dxdv_bit_exact_vs_reference_build(name, planar):
+    pt, pa, npot = TP.wrapped(name, planar)
+    dim = 2 if planar else 3
+    rng = np.random.default_rng(5)
+    w = np.concatenate([rng.uniform(0.6, 1.2, (4, dim)), rng.normal(0, 0.2, (4, dim)),
+                        rng.normal(0, 1, (4, 2 * dim))], 1)
+    w[:, dim + 1] += 1.0
+    t = np.linspace(0.0, 4.0, 17)
+    for method in ("rk4", "symplec4", "dop853"):
+        a = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar, npot=npot,
+                                  **tol(method))[0]
+        b = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar, npot=npot, impl="ref",
+                                  **tol(method))[0]
+        np.testing.assert_array_equal(a, b)
+
+
+def cyl_to_K(f, R, phi, planar):
+    """Cartesian K = -grad grad Phi from the oracle's cylindrical forces and
+    second derivatives (Rf = -Phi_R, tq = -Phi_phi)."""
+    c, s = np.cos(phi), np.sin(phi)
+    if planar:
+        Rf, tq, R2, p2, Rp = f.T
+    else:
+        Rf, zf, tq, R2, z2, Rz, p2, Rp, zp = f.T
+    PR, Pf = -Rf, -tq
+    K = [-(c * c * R2 - 2 * c * s / R * Rp + s * s / R**2 * p2 + s * s / R * PR +
+           2 * c * s / R**2 * Pf),
+         -(c * s * R2 + (c * c - s * s) / R * Rp - c * s / R**2 * p2 - c * s / R * PR -
+           (c * c - s * s) / R**2 * Pf),
+         -(s * s * R2 + 2 * c * s / R * Rp + c * c / R**2 * p2 + c * c / R * PR -
+           2 * c * s / R**2 * Pf)]
+    if not planar:
+        K += [-(c * Rz - s / R * zp), -(s * Rz + c / R * zp), -z2]
+    return np.stack(K, 1)
+
+
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", TP.WRAPPED)
+def test_engine_wrapped_forces_and_tidal(harness, name, planar):
+    """The engine's wrapper frames (records evaluated at the rotated point,
+    rotated back and scaled) against the oracle's wrapped sums, at several
+    times."""
+    pt, pa, npot = TP.wrapped(name, planar)
+    rng = np.random.default_rng(14)
+    R = rng.uniform(0.3, 2.0, 120)
+    z = np.zeros(120) if planar else rng.normal(0, 0.4, 120)
+    phi = rng.uniform(0, 2 * np.pi, 120)
+    for t in (0.2, 2.5, 7.0):
+        f = oracle.forces(R, z, phi, pt, pa, planar=planar, t=t, npot=npot)
+        tq = f[:, 1] if planar else f[:, 2]
+        ax = np.cos(phi) * f[:, 0] - np.sin(phi) * tq / R
+        ay = np.sin(phi) * f[:, 0] + np.cos(phi) * tq / R
+        acc, K, _ = harness.forces(R * np.cos(phi), R * np.sin(phi), z, pt, pa, planar=planar,
+                                   t=t, npot=npot)
+        ref = np.stack([ax, ay] + ([] if planar else [f[:, 1]]), 1)
+        assert np.abs(acc[:, :ref.shape[1]] - ref).max() < 1e-14 * np.abs(ref).max(), t
+        Kref = cyl_to_K(f, R, phi, planar)
+        assert np.abs(K[:, :Kref.shape[1]] - Kref).max() < 1e-12 * np.abs(Kref).max(), t
+
+
+@pytest.mark.parametrize("method", ["leapfrog", "symplec4", "rk4", "dopr54", "dop853"])
+@pytest.mark.parametrize("name", TP.WRAPPED)
+def test_engine_wrapped_machines_vs_oracle(harness, name, method):
+    pt, pa, npot = TP.wrapped(name)
+    y0 = ics(24, False, seed=23)
+    t = np.linspace(0.0, 8.0, 33)
+    with oracle.phi_from_atan2():
+        ref, _, nref, _ = oracle.integrate(y0, t, pt, pa, method, npot=npot, **tol(method))
+    out, err, ns = harness.integrate(c2r(y0, False), t, pt, pa, method, npot=npot,
+                                     **tol(method))
+    assert not err.any()
+    ref_r = np.stack([c2r(ref[:, j], False) for j in range(len(t))], 1)
+    d = np.abs(out - ref_r).reshape(len(y0), -1).max(1)
+    same = ns == nref
+    kink = TP.crosses_bar_radius(ref) if "bar" in name and method == "dop853" else \
+        np.zeros(len(ns), bool)
+    assert same[~kink].all()
+    strict = same & ~kink
+    assert np.median(d[strict]) < 1e-12 and d[strict].max() < 1e-9, d[strict].max()
+    assert (d < 1e-6).all()
+
+
+def test_nested_wrappers_refused():
+    import galpy_b200 as gb
+
+    mt, ma = TP.mw14()
+    inner = [1] + TP.loghalo_triaxial_args() + [1.0, 0.6, 0.3]  # a rotating halo
+    pt = np.array(mt + [-1, -2, 0], np.int32)
+    pa = np.array(ma + [1] + inner + [1.0, 0.5, 4.0, 1.0])  # ... smoothly grown
+    with pytest.raises(gb.PotentialNotSupported):
+        gb.compile_potential((pt, pa, len(mt) + 1))

@@ -69,6 +69,32 @@ def potential(name, planar=False):
 NAMES = ["bar+mw14", "bar_growing+mw14", "scf_nonaxi", "scf_axi+mn"]
 
 
+def loghalo_triaxial_args():
+    """galpy's LogarithmicHaloPotential args (amp, q, core^2, 1 - 1/b^2), b = 0.8."""
+    return [0.5, 0.9, 0.01, 1.0 - 1.0 / 0.64]
+
+
+def wrapped(name, planar=False):
+    """(pot_type, pot_args, npot) of a wrapper around one component, next to
+    MWPotential2014: galpy's layout (type, wrapped types; nwrapped, wrapped
+    args, wrapper args), npot counting top-level entries."""
+    mw_t, mw_a = mw14(planar)
+    if name == "smooth(bar)+mw14":  # a bar that grows, then a wrapper that grows it again
+        t, a = [-1, 1], [1] + dehnen_bar_args(amp_af=0.02) + [1.0, 0.5, 4.0, 1.0]
+    elif name == "decay(bar)+mw14":  # DehnenSmooth with grow = 0: decaying
+        t, a = [-1, 1], [1] + dehnen_bar_args(amp_af=0.02) + [1.0, 0.5, 4.0, 0.0]
+    elif name == "rotate(loghalo)+mw14":  # a triaxial halo in solid-body rotation
+        t, a = [-2, 0], [1] + loghalo_triaxial_args() + [1.0, 0.6, 0.3]
+    elif name == "gauss(loghalo)+mw14":  # a triaxial halo with a Gaussian amplitude in time
+        t, a = [-5, 0], [1] + loghalo_triaxial_args() + [1.0, 3.0, 4.0]
+    else:
+        raise KeyError(name)
+    return (np.asarray(mw_t + t, np.int32), np.asarray(mw_a + a, np.float64), len(mw_t) + 1)
+
+
+WRAPPED = ["smooth(bar)+mw14", "decay(bar)+mw14", "rotate(loghalo)+mw14", "gauss(loghalo)+mw14"]
+
+
 def crosses_bar_radius(ref_cyl, rb=0.8):
     """Orbits (cylindrical rows [n][nt][6|4]) whose radius r crosses the bar
     radius, where the bar potential's second derivative jumps: there
