@@ -102,6 +102,28 @@ def test_spherical_potential_routes(hooks):
     assert type(hooks[-1]["pot"]).__name__ == "PlummerPotential"
 
 
+def test_wrappers_route(hooks):
+    """Wrapped potentials go to the engine; a wrapper inside a wrapper stays
+    with galpy."""
+    from galpy.orbit import Orbit
+    from galpy.potential import (DehnenBarPotential, DehnenSmoothWrapperPotential,
+                                 LogarithmicHaloPotential, MWPotential2014,
+                                 SolidBodyRotationWrapperPotential)
+
+    o = Orbit([1.0, 0.1, 1.1, 0.0, 0.1, 0.0])
+    ts = np.linspace(0, 1, 11)
+    bar = DehnenSmoothWrapperPotential(pot=DehnenBarPotential(), tform=0.5, tsteady=2.0)
+    o.integrate(ts, [*MWPotential2014, bar], method="dop853_cuda")
+    assert len(hooks) == 1
+    halo = SolidBodyRotationWrapperPotential(
+        pot=LogarithmicHaloPotential(normalize=0.5, b=0.8, q=0.9), omega=0.6)
+    o.integrate(ts, [*MWPotential2014, halo], method="rk4_cuda")
+    assert len(hooks) == 2
+    nested = DehnenSmoothWrapperPotential(pot=halo, tform=0.5, tsteady=2.0)
+    o.integrate(ts, [*MWPotential2014, nested], method="rk4_cuda")
+    assert len(hooks) == 2
+
+
 def test_unknown_method_still_rejected(hooks):
     from galpy.orbit import Orbit
     from galpy.potential import MWPotential2014
