@@ -53,6 +53,10 @@ inline int galpy_nargs(int type, int planar, const double* p = nullptr)
     case T_HENONHEILES: return planar ? 1 : -1;  // (amp); a planarPotential only
     case T_KUZMINDISK: return 2;
     case T_DEHNENBAR: return 6;
+    case T_TRANSPIRAL: case T_STEADYSPIRAL: return planar ? 8 : -1;  // planarPotentials only
+    case T_ELLDISK: return planar ? 6 : -1;
+    case T_LOPSIDED: return planar ? 4 : -1;
+    case T_COSMPHI: return planar ? 9 : -1;
     default: return -1;
   }
 }
@@ -460,6 +464,14 @@ inline int compile_entries(int planar, int n, const int*& tp, const double*& p, 
       case T_KUZMINDISK:  // (amp, a)
         c.c[1] = p[1];
         break;
+      case T_TRANSPIRAL: case T_STEADYSPIRAL: case T_ELLDISK: case T_LOPSIDED:
+      case T_COSMPHI: {  // galpy's args as they are; the growth factor's 1 / (tsteady - tform)
+        for (int j = 1; j < na; j++) c.c[j] = p[j];
+        if ((type == T_STEADYSPIRAL || type == T_ELLDISK) && p[1] == p[1])
+          c.c[9] = p[2] > p[1] ? 1.0 / (p[2] - p[1]) : 0.0;
+        if (type == T_COSMPHI && (int)p[4] == 0) return -1;
+        break;
+      }
       case T_DEHNENBAR: {  // (amp * af, tform, tsteady, rb, omegab, barphi)
         if (!(p[3] > 0.0) || p[2] < p[1]) return -1;
         for (int j = 1; j < 6; j++) c.c[j] = p[j];

@@ -897,6 +897,18 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
     case T_WRAP_GAUSS:  // opened by the full list's loop; no other list carries one
       gR = T(NAN);
       break;
+    case T_TRANSPIRAL: case T_STEADYSPIRAL: case T_ELLDISK: case T_LOPSIDED:
+    case T_COSMPHI: {  // planar only, in float64, full list only
+      if constexpr (TYPE == kRunTimeAll && PLANAR) {
+        double ax = 0.0, ay = 0.0;
+        disk_pert_accel(cp, type, (double)x, (double)y, t, ax, ay, nullptr);
+        a0.x += T(ax);
+        a0.y += T(ay);
+      } else {
+        gR = T(NAN);
+      }
+      break;
+    }
     case T_DEHNENBAR:
     case T_SCF: {  // in float64; carried by the full run-time list only
       if constexpr (TYPE == kRunTimeAll) {
@@ -1378,6 +1390,12 @@ GPC_HD GPC_FI void comp_tidal(const GpComp* __restrict__ cp, int type, double x,
     case T_SCF:
       scf_tidal<PLANAR>(cp, x, y, z, ax0, ay0, az0, K);
       break;
+    case T_TRANSPIRAL: case T_STEADYSPIRAL: case T_ELLDISK: case T_LOPSIDED: case T_COSMPHI:
+      if (PLANAR)
+        disk_pert_accel(cp, type, x, y, t, ax0, ay0, K);
+      else
+        gR = NAN;
+      break;
     case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
     case T_POWERTRI: case T_TWOPOWERTRI: {
       double fx, fy, fz;
@@ -1622,7 +1640,8 @@ GPC_HD inline double comp_value(const GpComp* __restrict__ cp, double x, double 
       phi += p;
       break;
     }
-    case T_DEHNENBAR:  // time-dependent: not evaluated here (the host refuses it)
+    case T_TRANSPIRAL: case T_STEADYSPIRAL: case T_ELLDISK: case T_LOPSIDED: case T_COSMPHI:
+    case T_DEHNENBAR:  // no evaluation in the reference's C (the hooks keep galpy's)
       phi += NAN;
       break;
     default:

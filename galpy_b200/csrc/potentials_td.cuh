@@ -37,6 +37,15 @@ GPC_HD GPC_FI constexpr bool is_wrapper(int t)
 {
   return t == T_WRAP_SMOOTH || t == T_WRAP_ROTATE || t == T_WRAP_GAUSS;
 }
+// Planar-only disk perturbations: TransientLogSpiral, SteadyLogSpiral,
+// EllipticalDisk, LopsidedDisk, CosmphiDisk (potential_c_ext/<name>.c)
+enum : int { T_TRANSPIRAL = 2, T_STEADYSPIRAL = 3, T_ELLDISK = 4, T_LOPSIDED = 6,
+             T_COSMPHI = 28 };
+GPC_HD GPC_FI constexpr bool is_disk_pert(int t)
+{
+  return t == T_TRANSPIRAL || t == T_STEADYSPIRAL || t == T_ELLDISK || t == T_LOPSIDED ||
+         t == T_COSMPHI;
+}
 // Continuation record of a component whose data does not fit one record
 // (an SCF expansion's coefficients): skipped by every component loop.
 enum : int { T_PAYLOAD = -100 };
@@ -44,7 +53,8 @@ enum : int { T_PAYLOAD = -100 };
 // Types that only the full run-time component list carries.
 GPC_HD GPC_FI constexpr bool needs_full_list(int t)
 {
-  return is_ellipsoidal(t) || t == T_DEHNENBAR || t == T_SCF || t == T_PAYLOAD || is_wrapper(t);
+  return is_ellipsoidal(t) || t == T_DEHNENBAR || t == T_SCF || t == T_PAYLOAD || is_wrapper(t) ||
+         is_disk_pert(t);
 }
 
 // Doubles of payload per continuation record: the record after its
@@ -171,6 +181,115 @@ GPC_HD GPC_FI void dbar_tidal(const GpComp* __restrict__ cp, double t, double x,
     K[3] -= c * x * zz + d * zz * Qx;
     K[4] -= c * y * zz + d * zz * Qy;
     K[5] -= c * zz * zz + dQ;
+  }
+}
+
+// ---- planar disk perturbations ------------------------------------------
+// Record: galpy's args in c0..c8 (TransientLogSpiral amp, A, to, sigma^2,
+// alpha, m, omegas, gamma; SteadyLogSpiral amp, tform, tsteady, A, alpha, m,
+// omegas, gamma; EllipticalDisk amp, tform, tsteady, twophio, p, phib;
+// LopsidedDisk amp, phio, p, phib; CosmphiDisk amp, mphio, p, mphib, m, rb,
+// rb^p, rb^2p, r1^p), c9 1 / (tsteady - tform).  Each is R-power (or log R)
+// times a harmonic in phi; the parts below are -dPhi/dR (FR), -dPhi/dphi
+// (tq) and the second derivatives (R2, p2, Rp), as the reference writes them.
+struct CylParts {
+  double FR, tq, R2, p2, Rp;
+};
+
+GPC_HD inline CylParts disk_pert_parts(const GpComp* __restrict__ cp, int type, double R,
+                                       double phi, double t)
+{
+  double a[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) a[k] = ldg(&cp->c[k]);
+  const double amp = a[0];
+  CylParts P;
+  if (type == T_TRANSPIRAL || type == T_STEADYSPIRAL) {
+    double g, A, alpha, m, om, gam;
+    if (type == T_TRANSPIRAL) {
+      const double d = t - a[2];
+      A = a[1];
+      g = amp * A * exp(-0.5 * d * d / a[3]);
+      alpha = a[4], m = a[5], om = a[6], gam = a[7];
+    } else {  // tform NaN: always on
+      A = a[3];
+      const double sm = a[1] != a[1] ? 1.0 : dehnen_smooth(t, a[1], a[2], ldg(&cp->c[9]));
+      g = amp * sm * A;
+      alpha = a[4], m = a[5], om = a[6], gam = a[7];
+    }
+    double sc, cc;
+    sincos(alpha * log(R) - m * (phi - om * t - gam), &sc, &cc);
+    const double iR = 1.0 / R;
+    P.FR = g * iR * sc;
+    P.tq = -g / alpha * m * sc;
+    P.R2 = g * iR * iR * (sc - alpha * cc);
+    P.p2 = -g / alpha * m * m * cc;
+    P.Rp = g * m * iR * cc;
+    return P;
+  }
+  if (type == T_ELLDISK || type == T_LOPSIDED) {
+    double k, p, harm;
+    if (type == T_ELLDISK) {
+      const double sm = a[1] != a[1] ? 1.0 : dehnen_smooth(t, a[1], a[2], ldg(&cp->c[9]));
+      k = amp * sm * a[3];
+      p = a[4];
+      harm = 2.0;
+    } else {
+      k = amp * a[1];
+      p = a[2];
+      harm = 1.0;
+    }
+    const double phib = type == T_ELLDISK ? a[5] : a[3];
+    double sn, cs;
+    sincos(harm * (phi - phib), &sn, &cs);
+    const double Rp1 = pow(R, p - 1.0), Rp0 = Rp1 * R;
+    const double h = type == T_ELLDISK ? 0.5 : 1.0;  // the R-part's factor: twophio / 2, phio
+    P.FR = -k * h * p * Rp1 * cs;
+    P.tq = k * h * harm * Rp0 * sn;
+    P.R2 = k * h * p * (p - 1.0) * Rp1 / R * cs;
+    P.p2 = -k * h * harm * harm * Rp0 * cs;
+    P.Rp = -k * h * harm * p * Rp1 * sn;
+    return P;
+  }
+  // CosmphiDisk
+  const double mphio = a[1], p = a[2], mphib = a[3], m = (double)(int)a[4], rb = a[5];
+  const double rbp = a[6], rb2p = a[7], r1p = a[8];
+  double sn, cs;
+  sincos(m * phi - mphib, &sn, &cs);
+  if (R <= rb) {
+    const double iRp = pow(R, -p), inner = rbp * (2.0 * r1p - rbp * iRp);
+    P.FR = -amp * p * mphio / m * rb2p * iRp / R * cs;
+    P.tq = amp * mphio * inner * sn;
+    P.R2 = -amp * p * (p + 1.0) * mphio / m * rb2p * iRp / (R * R) * cs;
+    P.p2 = -amp * m * mphio * inner * cs;
+    P.Rp = -amp * p * mphio / m * rb2p * iRp / R * sn;
+  } else {
+    const double Rp1 = pow(R, p - 1.0), Rp0 = Rp1 * R;
+    P.FR = -amp * p * mphio / m * Rp1 * cs;
+    P.tq = amp * mphio * Rp0 * sn;
+    P.R2 = amp * p * (p - 1.0) * mphio / m * Rp1 / R * cs;
+    P.p2 = -amp * m * mphio * Rp0 * cs;
+    P.Rp = -amp * p * mphio * Rp1 * sn;
+  }
+  return P;
+}
+
+// Cartesian acceleration (and K = -grad grad Phi if K) in the plane from
+// the cylindrical parts at (x, y), R > 0.
+GPC_HD GPC_FI void disk_pert_accel(const GpComp* __restrict__ cp, int type, double x, double y,
+                                   double t, double& ax, double& ay, double* K)
+{
+  const double R = sqrt(x * x + y * y), iR = 1.0 / R, c = x * iR, s = y * iR;
+  const CylParts P = disk_pert_parts(cp, type, R, atan2(y, x), t);
+  ax += c * P.FR - s * iR * P.tq;
+  ay += s * P.FR + c * iR * P.tq;
+  if (K) {
+    const double PR = -P.FR, Pf = -P.tq, iR2 = iR * iR, cs = c * s, c2s2 = c * c - s * s;
+    K[0] -= c * c * P.R2 - 2.0 * cs * iR * P.Rp + s * s * iR2 * P.p2 + s * s * iR * PR +
+            2.0 * cs * iR2 * Pf;
+    K[1] -= cs * P.R2 + c2s2 * iR * P.Rp - cs * iR2 * P.p2 - cs * iR * PR - c2s2 * iR2 * Pf;
+    K[2] -= s * s * P.R2 + 2.0 * cs * iR * P.Rp + c * c * iR2 * P.p2 + c * c * iR * PR -
+            2.0 * cs * iR2 * Pf;
   }
 }
 

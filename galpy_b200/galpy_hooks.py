@@ -50,8 +50,9 @@ def _is_cuda(method):
 def _supported(pot, planar, purpose="integrate"):
     """Whether the engine carries this potential for `purpose`: "integrate"
     (orbits, surfaces of section, variational runs) or "potential" (values
-    at points, evaluated without a time: no time-dependent component).  An
-    SCF expansion must have static coefficients."""
+    at points, evaluated without a time: no time-dependent component and no
+    planar disk perturbation, which the reference's C does not evaluate).
+    An SCF expansion must have static coefficients."""
     try:
         if planar:
             from galpy.orbit.integratePlanarOrbit import _parse_pot

@@ -10,7 +10,8 @@ The engine integrates in the potentials galpy hands to C as pot_type codes
 (Null), 41 (Einasto) and 46 (ExpTruncNFW), the time-dependent 1
 (DehnenBar) and 24 (SCF, static coefficients), and the wrappers -1
 (DehnenSmooth), -2 (SolidBodyRotation) and -5 (GaussianAmplitude) around
-them -- the parsing is
+them, and in the plane 2, 3, 4, 6 and 28 (the log spirals and the
+elliptical, lopsided and cos(m phi) disks) -- the parsing is
 galpy/orbit/integrateFullOrbit.py:43-614 (3D) and
 galpy/orbit/integratePlanarOrbit.py:33-663 (planar).
 
@@ -43,10 +44,13 @@ T_DEHNENBAR, T_SCF = 1, 24
 # wrappers around other components (one level deep): DehnenSmooth,
 # SolidBodyRotation, GaussianAmplitude
 WRAPPER_TYPES = (-1, -2, -5)
-TIME_DEPENDENT_TYPES = (T_DEHNENBAR,) + WRAPPER_TYPES
+# planar disk perturbations: TransientLogSpiral, SteadyLogSpiral,
+# EllipticalDisk, LopsidedDisk, CosmphiDisk (no potential evaluation in C)
+DISK_PERTURBATION_TYPES = (2, 3, 4, 6, 28)
+TIME_DEPENDENT_TYPES = (T_DEHNENBAR,) + WRAPPER_TYPES + DISK_PERTURBATION_TYPES
 SUPPORTED_TYPES = (T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC, T_FLATPOWER,
                    T_KKS, T_HENONHEILES, T_KUZMINDISK, T_DEHNENBAR, T_SCF) + SPHERICAL_TYPES + \
-    ELLIPSOIDAL_TYPES + WRAPPER_TYPES
+    ELLIPSOIDAL_TYPES + WRAPPER_TYPES + DISK_PERTURBATION_TYPES
 
 
 class _Potential:

@@ -109,6 +109,13 @@ enum { PT_SCF = 24 };
    components' types; args (nwrapped, the wrapped components' args, then
    (amp, tform, tsteady, grow), (amp, omega, pa) or (amp, to, sigma^2)) */
 enum { PT_WRAP_SMOOTH = -1, PT_WRAP_ROTATE = -2, PT_WRAP_GAUSS = -5 };
+/* planar-only disk perturbations: TransientLogSpiral (2; amp, A, to,
+   sigma^2, alpha, m, omegas, gamma), SteadyLogSpiral (3; amp, tform,
+   tsteady, A, alpha, m, omegas, gamma; tform NaN: no growth), EllipticalDisk
+   (4; amp, tform, tsteady, twophio, p, phib), LopsidedDisk (6; amp, phio, p,
+   phib), CosmphiDisk (28; amp, mphio, p, mphib, m, rb, rb^p, rb^2p, r1^p) */
+enum { PT_TRANSPIRAL = 2, PT_STEADYSPIRAL = 3, PT_ELLDISK = 4, PT_LOPSIDED = 6,
+       PT_COSMPHI = 28 };
 
 static int is_ellipsoidal(int type)
 {
@@ -144,7 +151,7 @@ static int scf_nargs(const double *a)
 
 typedef struct {
   int type;
-  double p[8];     /* the component's args as galpy passes them */
+  double p[9];     /* the component's args as galpy passes them */
   const double *ea; /* all args (ellipsoidal and SCF components: the caller's array) */
   double t;        /* time of the current evaluation (time-dependent types) */
   int nsub;        /* a wrapper: the entries it wraps, which follow it */
@@ -175,6 +182,10 @@ static int nargs_of(int type, int planar)
   case PT_HENONHEILES: return planar ? 1 : -1;
   case PT_KUZMINDISK: return 2;
   case PT_DEHNENBAR: return 6;
+  case PT_TRANSPIRAL: case PT_STEADYSPIRAL: return planar ? 8 : -1;
+  case PT_ELLDISK: return planar ? 6 : -1;
+  case PT_LOPSIDED: return planar ? 4 : -1;
+  case PT_COSMPHI: return planar ? 9 : -1;
   default: return -1;
   }
 }
@@ -583,7 +594,7 @@ static int decode_entries(opot *P, int *idx, int n, const int **type, const doub
     c->type = t;
     c->t = 0.;
     c->nsub = 0;
-    for (int k = 0; k < 8; k++) c->p[k] = 0.;
+    for (int k = 0; k < 9; k++) c->p[k] = 0.;
     if (is_wrapper(t)) {
       const int nw = (int)*(*args)++;
       const int first = *idx;
@@ -599,7 +610,7 @@ static int decode_entries(opot *P, int *idx, int n, const int **type, const doub
     int na = is_ellipsoidal(t) ? ell_nargs(a) : t == PT_SCF ? scf_nargs(a) : nargs_of(t, planar);
     if (na < 0) return -1;
     c->ea = a;
-    for (int k = 0; k < na && k < 8; k++) c->p[k] = a[k];
+    for (int k = 0; k < na && k < 9; k++) c->p[k] = a[k];
     *args += na;
   }
   return 0;
@@ -1153,6 +1164,97 @@ static double scf_eval(const ocomp *c, double R, double Z, double phi)
   return F[3];
 }
 
+/* ---- planar disk perturbations (TransientLogSpiralPotential.c,
+   SteadyLogSpiralPotential.c, EllipticalDiskPotential.c,
+   LopsidedDiskPotential.c, CosmphiDiskPotential.c) ---- */
+static int is_disk_pert(int type)
+{
+  return type == PT_TRANSPIRAL || type == PT_STEADYSPIRAL || type == PT_ELLDISK ||
+         type == PT_LOPSIDED || type == PT_COSMPHI;
+}
+
+/* growth of the steady spiral and the elliptical disk (dehnenSpiralSmooth,
+   EllipticalDiskSmooth): 1 when tform is NaN */
+static double pert_smooth(double t, double tform, double tsteady)
+{
+  if (isnan(tform)) return 1.;
+  return dbar_smooth(t, tform, tsteady);
+}
+
+/* which: 0 Rforce, 1 phitorque, 2 R2deriv, 3 phi2deriv, 4 Rphideriv */
+static double disk_pert(const ocomp *c, int which, double R, double phi)
+{
+  const double *a = c->p, t = c->t, amp = a[0];
+  switch (c->type) {
+  case PT_TRANSPIRAL: {
+    double A = a[1], to = a[2], sigma2 = a[3], alpha = a[4], m = a[5], om = a[6], gam = a[7];
+    double g = exp(-pow(t - to, 2.) / 2. / sigma2);
+    double chi = alpha * log(R) - m * (phi - om * t - gam);
+    switch (which) {
+    case 0: return amp * A * g / R * sin(chi);
+    case 1: return -amp * A * g / alpha * m * sin(chi);
+    case 2: return amp * A * g / R / R * (sin(chi) - alpha * cos(chi));
+    case 3: return -amp * A * g / alpha * m * m * cos(chi);
+    default: return amp * A * g * m / R * cos(chi);
+    }
+  }
+  case PT_STEADYSPIRAL: {
+    double A = a[3], alpha = a[4], m = a[5], om = a[6], gam = a[7];
+    double sm = pert_smooth(t, a[1], a[2]);
+    double chi = alpha * log(R) - m * (phi - om * t - gam);
+    switch (which) {
+    case 0: return amp * sm * A / R * sin(chi);
+    case 1: return -amp * sm * A / alpha * m * sin(chi);
+    case 2: return amp * sm * A / R / R * (sin(chi) - alpha * cos(chi));
+    case 3: return -amp * sm * A / alpha * m * m * cos(chi);
+    default: return amp * sm * A * m / R * cos(chi);
+    }
+  }
+  case PT_ELLDISK: {
+    double twophio = a[3], p = a[4], phib = a[5], sm = pert_smooth(t, a[1], a[2]);
+    switch (which) {
+    case 0: return -amp * sm * p * twophio / 2. * pow(R, p - 1.) * cos(2. * (phi - phib));
+    case 1: return amp * sm * twophio * pow(R, p) * sin(2. * (phi - phib));
+    case 2: return amp * sm * p * (p - 1) * twophio / 2. * pow(R, p - 2.) * cos(2. * (phi - phib));
+    case 3: return -2. * amp * sm * twophio * pow(R, p) * cos(2. * (phi - phib));
+    default: return -amp * sm * p * twophio * pow(R, p - 1.) * sin(2. * (phi - phib));
+    }
+  }
+  case PT_LOPSIDED: {
+    double phio = a[1], p = a[2], phib = a[3];
+    switch (which) {
+    case 0: return -amp * p * phio * pow(R, p - 1.) * cos(phi - phib);
+    case 1: return amp * phio * pow(R, p) * sin(phi - phib);
+    case 2: return amp * p * (p - 1) * phio * pow(R, p - 2.) * cos(phi - phib);
+    case 3: return -amp * phio * pow(R, p) * cos(phi - phib);
+    default: return -amp * p * phio * pow(R, p - 1.) * sin(phi - phib);
+    }
+  }
+  default: { /* PT_COSMPHI */
+    double mphio = a[1], p = a[2], mphib = a[3], rb = a[5], rbp = a[6], rb2p = a[7], r1p = a[8];
+    int m = (int)a[4];
+    int in = R <= rb;
+    switch (which) {
+    case 0:
+      return in ? -amp * p * mphio / m * rb2p / pow(R, p + 1.) * cos(m * phi - mphib)
+                : -amp * p * mphio / m * pow(R, p - 1.) * cos(m * phi - mphib);
+    case 1:
+      return in ? amp * mphio * rbp * (2. * r1p - rbp / pow(R, p)) * sin(m * phi - mphib)
+                : amp * mphio * pow(R, p) * sin(m * phi - mphib);
+    case 2:
+      return in ? -amp * p * (p + 1) * mphio / m * rb2p / pow(R, p + 2.) * cos(m * phi - mphib)
+                : amp * p * (p - 1) * mphio / m * pow(R, p - 2.) * cos(m * phi - mphib);
+    case 3:
+      return in ? -amp * m * mphio * rbp * (2. * r1p - rbp / pow(R, p)) * cos(m * phi - mphib)
+                : -amp * m * mphio * pow(R, p) * cos(m * phi - mphib);
+    default:
+      return in ? -amp * p * mphio / m * rb2p / pow(R, p + 1) * sin(m * phi - mphib)
+                : -amp * p * mphio * pow(R, p - 1.) * sin(m * phi - mphib);
+    }
+  }
+  }
+}
+
 /* ---- 3D component forces ---- */
 static double comp_Rforce(ocomp *c, double R, double Z, double phi)
 {
@@ -1410,6 +1512,7 @@ static double comp_hess(const ocomp *c, int which, double R, double Z, double ph
 /* ---- planar component forces ---- */
 static double comp_planarRforce(const ocomp *c, double R, double phi)
 {
+  if (is_disk_pert(c->type)) return disk_pert(c, 0, R, phi);
   if (c->type == PT_DEHNENBAR) return dbar_force2(c, 0, R, phi);
   if (c->type == PT_SCF) return scf_force3(c, 0, R, 0.0, phi); /* SCFPotentialPlanarRforce */
   if (is_new_spherical(c->type)) return sph_planarRforce(c, R);
@@ -1461,6 +1564,7 @@ static double comp_planarRforce(const ocomp *c, double R, double phi)
 
 static double comp_planarphitorque(const ocomp *c, double R, double phi)
 {
+  if (is_disk_pert(c->type)) return disk_pert(c, 1, R, phi);
   if (c->type == PT_DEHNENBAR) return dbar_force2(c, 2, R, phi);
   if (c->type == PT_SCF) return scf_force3(c, 2, R, 0.0, phi);
   if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 2, R, 0., phi);
@@ -1476,6 +1580,7 @@ static double comp_planarphitorque(const ocomp *c, double R, double phi)
 /* planar Hessian: which = 0 R2, 1 phi2, 2 Rphi */
 static double comp_planarhess(const ocomp *c, int which, double R, double phi)
 {
+  if (is_disk_pert(c->type)) return disk_pert(c, 2 + which, R, phi);
   if (c->type == PT_DEHNENBAR) return dbar_hess2(c, which, R, phi);
   if (c->type == PT_SCF) return scf_hess2(c, which, R, phi);
   if (is_new_spherical(c->type)) return which ? 0. : sph_planarR2deriv(c, R);

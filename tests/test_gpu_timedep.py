@@ -222,3 +222,50 @@ def test_wrapped_variational(oracle, name, planar):
         assert np.array_equal(err, eref) and np.array_equal(ns, nref)
         rel = (np.abs(out - ref) / np.abs(ref).max(axis=1, keepdims=True)).max()
         assert rel < 1e-9, (method, rel)
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("name", TP.PLANAR_PERTURBATIONS)
+def test_planar_perturbation_orbits_vs_oracle(oracle, name, method):
+    """galpy's planar disk perturbations (log spirals, elliptical, lopsided
+    and cos(m phi) disks) over MWPotential2014 in the plane.  CosmphiDisk's
+    second derivative jumps at its break radius rb = 0.6: DOP853 orbits
+    crossing it may flip decisions at the rounding level."""
+    pt, pa = TP.planar_perturbation(name)
+    y0 = ics(128, True, 41 + TP.PLANAR_PERTURBATIONS.index(name))
+    t = np.linspace(0.0, 10.0, 41)
+    with oracle.phi_from_atan2():
+        ref, eref, nref, _ = oracle.integrate(y0, t, pt, pa, method, planar=True, **tol(method))
+    out, err, ns = gb.integratePlanarOrbit_cuda((pt, pa), y0.copy(), t, method + "_cuda",
+                                                progressbar=False, return_nsteps=True,
+                                                **tol(method))
+    assert not err.any() and not eref.any()
+    d = cyl_diff(ref, out).max(axis=(1, 2))
+    same = ns == nref
+    R = ref[..., 0]
+    kink = ((R.min(axis=1) < 0.6) & (R.max(axis=1) > 0.6)) if (
+        name.startswith("cosmphi") and method == "dop853") else np.zeros(len(ns), bool)
+    assert same[~kink].mean() >= 0.98, same[~kink].mean()
+    far = same & ~kink & (d > 1e-10)
+    if far.any():
+        with oracle.phi_from_atan2():
+            resp = np.maximum(*[TP.ulp_response(oracle, y0[far], t, pt, pa, method, True,
+                                                ref[far], seed=sd, **tol(method))
+                                for sd in (3, 4)])
+        assert (d[far] <= 30 * resp).all(), (d[far], resp)
+    assert (d[~same | kink] < 1e-6).all(), d[~same | kink]
+
+
+@pytest.mark.parametrize("name", TP.PLANAR_PERTURBATIONS)
+def test_planar_perturbation_variational(oracle, name):
+    pt, pa = TP.planar_perturbation(name)
+    w = unit_deviations(cyl_to_rect(ics(6, True, 5)), 2)
+    t = np.linspace(0.0, 4.0, 17)
+    for method in ("rk4", "symplec4"):
+        with oracle.phi_from_atan2():
+            ref, eref, nref = oracle.integrate_dxdv(w, t, pt, pa, method, planar=True)
+        out, err, ns = gb.integrate_dxdv_batch((pt, pa), w, t, method + "_cuda", planar=True,
+                                               return_nsteps=True)
+        assert np.array_equal(err, eref) and np.array_equal(ns, nref)
+        rel = (np.abs(out - ref) / np.abs(ref).max(axis=1, keepdims=True)).max()
+        assert rel < 1e-9, (method, rel)

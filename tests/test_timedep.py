@@ -393,3 +393,81 @@ def test_nested_wrappers_refused():
     pa = np.array(ma + [1] + inner + [1.0, 0.5, 4.0, 1.0])  # ... smoothly grown
     with pytest.raises(gb.PotentialNotSupported):
         gb.compile_potential((pt, pa, len(mt) + 1))
+
+
+# ---- planar disk perturbations: log spirals, elliptical / lopsided / cos(m phi) disks
+def pert_kink(name, ref):
+    """Orbits crossing a radius where the potential's second derivative
+    jumps: CosmphiDisk's break radius rb = 0.6."""
+    if not name.startswith("cosmphi"):
+        return np.zeros(len(ref), bool)
+    R = ref[..., 0]
+    return (R.min(axis=1) < 0.6) & (R.max(axis=1) > 0.6)
+
+
+@needs_ref
+@pytest.mark.parametrize("name", TP.PLANAR_PERTURBATIONS)
+@pytest.mark.parametrize("method", METHODS)
+def test_perturbation_orbits_bit_exact_vs_reference_build(name, method):
+    pt, pa = TP.planar_perturbation(name)
+    yo = ics(8, True)
+    t = np.linspace(0.0, 8.0, 41)
+    a, ea, _, _ = oracle.integrate(yo, t, pt, pa, method, planar=True, **tol(method))
+    b, eb, _, _ = oracle.integrate(yo, t, pt, pa, method, planar=True, impl="ref", **tol(method))
+    np.testing.assert_array_equal(ea, eb)
+    np.testing.assert_array_equal(a, b)
+
+
+@needs_ref
+@pytest.mark.parametrize("name", TP.PLANAR_PERTURBATIONS)
+def test_perturbation_dxdv_bit_exact_vs_reference_build(name):
+    pt, pa = TP.planar_perturbation(name)
+    rng = np.random.default_rng(5)
+    w = np.concatenate([rng.uniform(0.6, 1.2, (4, 2)), rng.normal(0, 0.2, (4, 2)),
+                        rng.normal(0, 1, (4, 4))], 1)
+    w[:, 3] += 1.0
+    t = np.linspace(0.0, 4.0, 17)
+    for method in ("rk4", "symplec4", "dop853"):
+        a = oracle.integrate_dxdv(w, t, pt, pa, method, planar=True, **tol(method))[0]
+        b = oracle.integrate_dxdv(w, t, pt, pa, method, planar=True, impl="ref",
+                                  **tol(method))[0]
+        np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("name", TP.PLANAR_PERTURBATIONS)
+def test_engine_perturbation_forces_and_tidal(harness, name):
+    pt, pa = TP.planar_perturbation(name)
+    rng = np.random.default_rng(15)
+    R, phi = rng.uniform(0.3, 2.0, 120), rng.uniform(0, 2 * np.pi, 120)
+    z = np.zeros(120)
+    for t in (0.2, 3.0, 7.0):
+        f = oracle.forces(R, z, phi, pt, pa, planar=True, t=t)
+        ax = np.cos(phi) * f[:, 0] - np.sin(phi) * f[:, 1] / R
+        ay = np.sin(phi) * f[:, 0] + np.cos(phi) * f[:, 1] / R
+        acc, K, _ = harness.forces(R * np.cos(phi), R * np.sin(phi), z, pt, pa, planar=True,
+                                   t=t)
+        ref = np.stack([ax, ay], 1)
+        assert np.abs(acc[:, :2] - ref).max() < 1e-14 * np.abs(ref).max(), t
+        Kref = cyl_to_K(f, R, phi, True)
+        assert np.abs(K[:, :3] - Kref).max() < 1e-12 * np.abs(Kref).max(), t
+
+
+@pytest.mark.parametrize("method", ["leapfrog", "symplec4", "rk4", "dopr54", "dop853"])
+@pytest.mark.parametrize("name", TP.PLANAR_PERTURBATIONS)
+def test_engine_perturbation_machines_vs_oracle(harness, name, method):
+    pt, pa = TP.planar_perturbation(name)
+    y0 = ics(24, True, seed=29)
+    t = np.linspace(0.0, 10.0, 41)
+    with oracle.phi_from_atan2():
+        ref, _, nref, _ = oracle.integrate(y0, t, pt, pa, method, planar=True, **tol(method))
+    out, err, ns = harness.integrate(c2r(y0, True), t, pt, pa, method, planar=True,
+                                     **tol(method))
+    assert not err.any()
+    ref_r = np.stack([c2r(ref[:, j], True) for j in range(len(t))], 1)
+    d = np.abs(out - ref_r).reshape(len(y0), -1).max(1)
+    same = ns == nref
+    kink = pert_kink(name, ref) if method == "dop853" else np.zeros(len(ns), bool)
+    assert same[~kink].all()
+    strict = same & ~kink
+    assert np.median(d[strict]) < 1e-12 and d[strict].max() < 1e-9, d[strict].max()
+    assert (d < 1e-6).all()

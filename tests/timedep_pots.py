@@ -114,3 +114,32 @@ def ulp_response(oracle, ics, t, pt, pa, method, planar, ref, seed=3, **kw):
     ulp = 1 + np.finfo(float).eps * np.random.default_rng(seed).choice([-1, 1], ics.shape)
     pert, _, _, _ = oracle.integrate(ics * ulp, t, pt, pa, method, planar=planar, **kw)
     return cyl_diff(ref, pert).max(axis=(1, 2))
+
+
+def planar_perturbation(name):
+    """(pot_type, pot_args) of MWPotential2014 in the plane plus one of
+    galpy's planar disk perturbations (the layouts of integratePlanarOrbit.py):
+    TransientLogSpiral (2), SteadyLogSpiral (3, grown or always on),
+    EllipticalDisk (4), LopsidedDisk (6), CosmphiDisk (28)."""
+    mw_t, mw_a = mw14(True)
+    gam = np.pi / 4
+    if name == "transspiral+mw14":
+        t, a = [2], [1.0, -0.035, 5.0, 4.0, -7.0, 2.0, 0.65, gam]
+    elif name == "steadyspiral+mw14":
+        t, a = [3], [1.0, 1.0, 5.0, -0.035, -7.0, 2.0, 0.65, gam]
+    elif name == "steadyspiral_on+mw14":
+        t, a = [3], [1.0, float("nan"), float("nan"), -0.035, -7.0, 2.0, 0.65, gam]
+    elif name == "elldisk+mw14":
+        t, a = [4], [1.0, 0.5, 3.0, 0.02, 1.0, 0.4]
+    elif name == "lopsided+mw14":
+        t, a = [6], [1.0, 0.02, 1.0, 0.4]
+    elif name == "cosmphi+mw14":
+        rb, p = 0.6, 1.0
+        t, a = [28], [1.0, 0.02, p, 0.8, 3.0, rb, rb**p, rb**(2 * p), 1.0]
+    else:
+        raise KeyError(name)
+    return np.asarray(mw_t + t, np.int32), np.asarray(mw_a + a, np.float64)
+
+
+PLANAR_PERTURBATIONS = ["transspiral+mw14", "steadyspiral+mw14", "steadyspiral_on+mw14",
+                        "elldisk+mw14", "lopsided+mw14", "cosmphi+mw14"]
