@@ -53,6 +53,8 @@ inline int galpy_nargs(int type, int planar, const double* p = nullptr)
     case T_HENONHEILES: return planar ? 1 : -1;  // (amp); a planarPotential only
     case T_KUZMINDISK: return 2;
     case T_DEHNENBAR: return 6;
+    case T_SPIRALARMS:  // (nCs, amp, N, sin alpha, tan alpha, r_ref, phi_ref, Rs, H, omega, Cs)
+      return p && (int)p[0] >= 1 && (int)p[0] <= kSpiralMaxTerms ? 10 + (int)p[0] : -1;
     case T_TRANSPIRAL: case T_STEADYSPIRAL: return planar ? 8 : -1;  // planarPotentials only
     case T_ELLDISK: return planar ? 6 : -1;
     case T_LOPSIDED: return planar ? 4 : -1;
@@ -470,6 +472,13 @@ inline int compile_entries(int planar, int n, const int*& tp, const double*& p, 
         if ((type == T_STEADYSPIRAL || type == T_ELLDISK) && p[1] == p[1])
           c.c[9] = p[2] > p[1] ? 1.0 / (p[2] - p[1]) : 0.0;
         if (type == T_COSMPHI && (int)p[4] == 0) return -1;
+        break;
+      }
+      case T_SPIRALARMS: {
+        for (int j = 0; j < 9; j++) c.c[j] = p[1 + j];
+        c.c[9] = p[0];
+        for (int n = 0; n < (int)p[0]; n++) c.c[10 + n] = p[10 + n];
+        if (!(p[3] != 0.0) || !(p[4] != 0.0) || !(p[7] > 0.0)) return -1;
         break;
       }
       case T_DEHNENBAR: {  // (amp * af, tform, tsteady, rb, omegab, barphi)

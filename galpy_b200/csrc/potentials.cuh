@@ -897,6 +897,18 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
     case T_WRAP_GAUSS:  // opened by the full list's loop; no other list carries one
       gR = T(NAN);
       break;
+    case T_SPIRALARMS: {  // in float64, full list only
+      if constexpr (TYPE == kRunTimeAll) {
+        double ax = 0.0, ay = 0.0, az = 0.0;
+        spiral_accel<PLANAR>(cp, (double)x, (double)y, (double)z, t, ax, ay, az, nullptr);
+        a0.x += T(ax);
+        a0.y += T(ay);
+        if (!PLANAR) a0.z += T(az);
+      } else {
+        gR = T(NAN);
+      }
+      break;
+    }
     case T_TRANSPIRAL: case T_STEADYSPIRAL: case T_ELLDISK: case T_LOPSIDED:
     case T_COSMPHI: {  // planar only, in float64, full list only
       if constexpr (TYPE == kRunTimeAll && PLANAR) {
@@ -1396,6 +1408,9 @@ GPC_HD GPC_FI void comp_tidal(const GpComp* __restrict__ cp, int type, double x,
       else
         gR = NAN;
       break;
+    case T_SPIRALARMS:
+      spiral_accel<PLANAR>(cp, x, y, z, t, ax0, ay0, az0, K);
+      break;
     case T_TRIHERNQUIST: case T_TRINFW: case T_TRIJAFFE: case T_PERFECTELL: case T_TRIGAUSS:
     case T_POWERTRI: case T_TWOPOWERTRI: {
       double fx, fy, fz;
@@ -1640,6 +1655,9 @@ GPC_HD inline double comp_value(const GpComp* __restrict__ cp, double x, double 
       phi += p;
       break;
     }
+    case T_SPIRALARMS:  // at t = 0 (time-dependent: the hooks keep galpy's path)
+      phi += spiral_potential<false>(cp, sqrt(R2), z, atan2(y, x), 0.0).v;
+      break;
     case T_TRANSPIRAL: case T_STEADYSPIRAL: case T_ELLDISK: case T_LOPSIDED: case T_COSMPHI:
     case T_DEHNENBAR:  // no evaluation in the reference's C (the hooks keep galpy's)
       phi += NAN;

@@ -41,6 +41,10 @@ GPC_HD GPC_FI constexpr bool is_wrapper(int t)
 // EllipticalDisk, LopsidedDisk, CosmphiDisk (potential_c_ext/<name>.c)
 enum : int { T_TRANSPIRAL = 2, T_STEADYSPIRAL = 3, T_ELLDISK = 4, T_LOPSIDED = 6,
              T_COSMPHI = 28 };
+// SpiralArmsPotential (SpiralArmsPotential.c): 3D and planar
+enum : int { T_SPIRALARMS = 27 };
+constexpr int kSpiralMaxTerms = 6;  // Cn terms a record holds
+
 GPC_HD GPC_FI constexpr bool is_disk_pert(int t)
 {
   return t == T_TRANSPIRAL || t == T_STEADYSPIRAL || t == T_ELLDISK || t == T_LOPSIDED ||
@@ -54,7 +58,7 @@ enum : int { T_PAYLOAD = -100 };
 GPC_HD GPC_FI constexpr bool needs_full_list(int t)
 {
   return is_ellipsoidal(t) || t == T_DEHNENBAR || t == T_SCF || t == T_PAYLOAD || is_wrapper(t) ||
-         is_disk_pert(t);
+         is_disk_pert(t) || t == T_SPIRALARMS;
 }
 
 // Doubles of payload per continuation record: the record after its
@@ -290,6 +294,197 @@ GPC_HD GPC_FI void disk_pert_accel(const GpComp* __restrict__ cp, int type, doub
     K[1] -= cs * P.R2 + c2s2 * iR * P.Rp - cs * iR2 * P.p2 - cs * iR * PR - c2s2 * iR2 * Pf;
     K[2] -= s * s * P.R2 + 2.0 * cs * iR * P.Rp + c * c * iR2 * P.p2 + c * c * iR * PR -
             2.0 * cs * iR2 * Pf;
+  }
+}
+
+// ---- second-order forward differentiation over (R, z, phi) --------------
+// A value with its gradient and (HESS) Hessian in three variables: the
+// spiral arms' potential is written once, and its forces and second
+// derivatives follow by the chain rule of each operation.
+template <bool HESS>
+struct Dual3 {
+  double v, g[3], h[3][3];
+};
+
+template <bool HESS>
+GPC_HD GPC_FI Dual3<HESS> dual_var(double v, int i)
+{
+  Dual3<HESS> r;
+  r.v = v;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    r.g[a] = a == i ? 1.0 : 0.0;
+#pragma unroll
+    for (int b = 0; b < 3; b++) r.h[a][b] = 0.0;
+  }
+  return r;
+}
+
+// f(u) from f(u.v), f'(u.v), f''(u.v)
+template <bool HESS>
+GPC_HD GPC_FI Dual3<HESS> dual_apply(const Dual3<HESS>& u, double f, double f1, double f2)
+{
+  Dual3<HESS> r;
+  r.v = f;
+#pragma unroll
+  for (int a = 0; a < 3; a++) r.g[a] = f1 * u.g[a];
+  if (HESS) {
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int b = 0; b < 3; b++) r.h[a][b] = f1 * u.h[a][b] + f2 * u.g[a] * u.g[b];
+  }
+  return r;
+}
+
+template <bool HESS>
+GPC_HD GPC_FI Dual3<HESS> dual_mul(const Dual3<HESS>& x, const Dual3<HESS>& y)
+{
+  Dual3<HESS> r;
+  r.v = x.v * y.v;
+#pragma unroll
+  for (int a = 0; a < 3; a++) r.g[a] = x.g[a] * y.v + x.v * y.g[a];
+  if (HESS) {
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int b = 0; b < 3; b++)
+        r.h[a][b] = x.h[a][b] * y.v + x.g[a] * y.g[b] + x.g[b] * y.g[a] + x.v * y.h[a][b];
+  }
+  return r;
+}
+
+template <bool HESS>
+GPC_HD GPC_FI Dual3<HESS> dual_lin(double ca, const Dual3<HESS>& x, double c0)  // ca x + c0
+{
+  Dual3<HESS> r;
+  r.v = ca * x.v + c0;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    r.g[a] = ca * x.g[a];
+    if (HESS)
+#pragma unroll
+      for (int b = 0; b < 3; b++) r.h[a][b] = ca * x.h[a][b];
+  }
+  return r;
+}
+
+template <bool HESS>
+GPC_HD GPC_FI Dual3<HESS> dual_rcp(const Dual3<HESS>& u)
+{
+  const double i = 1.0 / u.v;
+  return dual_apply(u, i, -i * i, 2.0 * i * i * i);
+}
+
+template <bool HESS>
+GPC_HD GPC_FI Dual3<HESS> dual_exp(const Dual3<HESS>& u)
+{
+  const double e = exp(u.v);
+  return dual_apply(u, e, e, e);
+}
+
+template <bool HESS>
+GPC_HD GPC_FI Dual3<HESS> dual_log(const Dual3<HESS>& u)
+{
+  const double i = 1.0 / u.v;
+  return dual_apply(u, log(u.v), i, -i * i);
+}
+
+template <bool HESS>
+GPC_HD GPC_FI Dual3<HESS> dual_cos(const Dual3<HESS>& u)
+{
+  double s, c;
+  sincos(u.v, &s, &c);
+  return dual_apply(u, c, -s, -c);
+}
+
+template <bool HESS>
+GPC_HD GPC_FI Dual3<HESS> dual_cosh(const Dual3<HESS>& u)
+{
+  const double c = cosh(u.v);
+  return dual_apply(u, c, sinh(u.v), c);
+}
+
+// ---- SpiralArms -------------------------------------------------------------
+// Phi = -amp H exp(-(R - r_ref)/Rs) sum_n Cn / (Kn Dn) cos(n gamma)
+//       / cosh(Kn z / Bn)^Bn,  gamma = N (phi - omega t - phi_ref - ln(R/r_ref)
+//       / tan alpha), Kn = n N / (R sin alpha), Bn = Kn H (1 + 0.4 Kn H),
+//       Dn = (1 + Kn H + 0.3 (Kn H)^2) / (1 + 0.3 Kn H)
+// (Cox & Gomez 2002).  Record: c0 amp, c1 N, c2 sin alpha, c3 tan alpha, c4
+// r_ref, c5 phi_ref, c6 Rs, c7 H, c8 omega, c9 the number of terms, c10.. Cn.
+template <bool HESS>
+GPC_HD inline Dual3<HESS> spiral_potential(const GpComp* __restrict__ cp, double R, double z,
+                                           double phi, double t)
+{
+  const double amp = ldg(&cp->c[0]), N = ldg(&cp->c[1]), sa = ldg(&cp->c[2]);
+  const double ta = ldg(&cp->c[3]), rref = ldg(&cp->c[4]), phiref = ldg(&cp->c[5]);
+  const double Rs = ldg(&cp->c[6]), H = ldg(&cp->c[7]), om = ldg(&cp->c[8]);
+  const int nC = (int)ldg(&cp->c[9]);
+  const Dual3<HESS> vR = dual_var<HESS>(R, 0), vz = dual_var<HESS>(z, 1);
+  const Dual3<HESS> vf = dual_var<HESS>(phi, 2);
+  const Dual3<HESS> iR = dual_rcp(vR);
+  // gamma = N (phi - omega t - phi_ref) - N / tan(alpha) ln(R / r_ref)
+  Dual3<HESS> gam = dual_lin(-N / ta, dual_log(dual_lin(1.0 / rref, vR, 0.0)), 0.0);
+#pragma unroll
+  for (int a = 0; a < 3; a++) gam.g[a] += N * vf.g[a];
+  gam.v += N * (phi - om * t - phiref);
+  Dual3<HESS> sum = dual_lin(0.0, vR, 0.0);
+  for (int n = 1; n <= nC && n <= kSpiralMaxTerms; n++) {
+    const double Cn = ldg(&cp->c[9 + n]);
+    const Dual3<HESS> Kn = dual_lin(n * N / sa, iR, 0.0);   // n N / (R sin alpha)
+    const Dual3<HESS> KH = dual_lin(H, Kn, 0.0);
+    const Dual3<HESS> Bn = dual_mul(KH, dual_lin(0.4, KH, 1.0));
+    const Dual3<HESS> Dn = dual_mul(dual_lin(1.0, dual_mul(KH, dual_lin(0.3, KH, 1.0)), 1.0),
+                                    dual_rcp(dual_lin(0.3, KH, 1.0)));
+    const Dual3<HESS> c = dual_cos(dual_lin((double)n, gam, 0.0));
+    // cosh(Kn z / Bn)^(-Bn) = exp(-Bn log cosh(Kn z / Bn))
+    const Dual3<HESS> arg = dual_mul(dual_mul(Kn, vz), dual_rcp(Bn));
+    const Dual3<HESS> sech = dual_exp(dual_mul(dual_lin(-1.0, Bn, 0.0), dual_log(dual_cosh(arg))));
+    const Dual3<HESS> term = dual_mul(dual_mul(c, sech), dual_rcp(dual_mul(Kn, Dn)));
+    sum.v += Cn * term.v;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      sum.g[a] += Cn * term.g[a];
+      if (HESS)
+#pragma unroll
+        for (int b = 0; b < 3; b++) sum.h[a][b] += Cn * term.h[a][b];
+    }
+  }
+  const Dual3<HESS> pre = dual_exp(dual_lin(-1.0 / Rs, vR, rref / Rs));
+  return dual_lin(-amp * H, dual_mul(pre, sum), 0.0);
+}
+
+// Acceleration (and K if K) of the spiral arms at (x, y, z), time t, R > 0.
+template <bool PLANAR>
+GPC_HD inline void spiral_accel(const GpComp* __restrict__ cp, double x, double y, double z,
+                                double t, double& ax, double& ay, double& az, double* K)
+{
+  const double zz = PLANAR ? 0.0 : z;
+  const double R = sqrt(x * x + y * y), iR = 1.0 / R, c = x * iR, s = y * iR;
+  const double phi = atan2(y, x);
+  if (!K) {
+    const Dual3<false> P = spiral_potential<false>(cp, R, zz, phi, t);
+    const double FR = -P.g[0], tq = -P.g[2];
+    ax += c * FR - s * iR * tq;
+    ay += s * FR + c * iR * tq;
+    if (!PLANAR) az += -P.g[1];
+    return;
+  }
+  const Dual3<true> P = spiral_potential<true>(cp, R, zz, phi, t);
+  const double FR = -P.g[0], tq = -P.g[2];
+  ax += c * FR - s * iR * tq;
+  ay += s * FR + c * iR * tq;
+  if (!PLANAR) az += -P.g[1];
+  const double R2 = P.h[0][0], p2 = P.h[2][2], Rp = P.h[0][2];
+  const double PR = -FR, Pf = -tq, iR2 = iR * iR, cs = c * s, c2s2 = c * c - s * s;
+  K[0] -= c * c * R2 - 2.0 * cs * iR * Rp + s * s * iR2 * p2 + s * s * iR * PR + 2.0 * cs * iR2 * Pf;
+  K[1] -= cs * R2 + c2s2 * iR * Rp - cs * iR2 * p2 - cs * iR * PR - c2s2 * iR2 * Pf;
+  K[2] -= s * s * R2 + 2.0 * cs * iR * Rp + c * c * iR2 * p2 + c * c * iR * PR - 2.0 * cs * iR2 * Pf;
+  if (!PLANAR) {
+    const double Rz = P.h[0][1], zp = P.h[1][2];
+    K[3] -= c * Rz - s * iR * zp;
+    K[4] -= s * Rz + c * iR * zp;
+    K[5] -= P.h[1][1];
   }
 }
 

@@ -38,7 +38,7 @@ import numpy as np
 
 from .integrate import (CUDA_METHODS, integrateFullOrbit_cuda, integrateFullOrbit_sos_cuda,
                         integratePlanarOrbit_cuda, integratePlanarOrbit_sos_cuda)
-from .potentials import SUPPORTED_TYPES, T_SCF, TIME_DEPENDENT_TYPES
+from .potentials import SUPPORTED_TYPES, T_SCF, T_SPIRALARMS, TIME_DEPENDENT_TYPES
 
 _installed = {}
 
@@ -66,8 +66,9 @@ def _supported(pot, planar, purpose="integrate"):
         return False
     if purpose == "potential" and any(t in TIME_DEPENDENT_TYPES for t in types):
         return False
-    if T_SCF in types or any(t < 0 for t in types):
-        # time-dependent SCF coefficients and nested wrappers are not carried
+    if T_SCF in types or T_SPIRALARMS in types or any(t < 0 for t in types):
+        # time-dependent SCF coefficients, nested wrappers and spiral arms
+        # with more than six terms are not carried
         from . import _lib
 
         pt = np.ascontiguousarray(types, np.int32)

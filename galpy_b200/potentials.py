@@ -47,9 +47,12 @@ WRAPPER_TYPES = (-1, -2, -5)
 # planar disk perturbations: TransientLogSpiral, SteadyLogSpiral,
 # EllipticalDisk, LopsidedDisk, CosmphiDisk (no potential evaluation in C)
 DISK_PERTURBATION_TYPES = (2, 3, 4, 6, 28)
-TIME_DEPENDENT_TYPES = (T_DEHNENBAR,) + WRAPPER_TYPES + DISK_PERTURBATION_TYPES
+# SpiralArmsPotential (Cox & Gomez arms rotating at omega; up to six terms)
+T_SPIRALARMS = 27
+TIME_DEPENDENT_TYPES = (T_DEHNENBAR, T_SPIRALARMS) + WRAPPER_TYPES + DISK_PERTURBATION_TYPES
 SUPPORTED_TYPES = (T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC, T_FLATPOWER,
-                   T_KKS, T_HENONHEILES, T_KUZMINDISK, T_DEHNENBAR, T_SCF) + SPHERICAL_TYPES + \
+                   T_KKS, T_HENONHEILES, T_KUZMINDISK, T_DEHNENBAR, T_SCF,
+                   T_SPIRALARMS) + SPHERICAL_TYPES + \
     ELLIPSOIDAL_TYPES + WRAPPER_TYPES + DISK_PERTURBATION_TYPES
 
 

@@ -116,6 +116,9 @@ enum { PT_WRAP_SMOOTH = -1, PT_WRAP_ROTATE = -2, PT_WRAP_GAUSS = -5 };
    phib), CosmphiDisk (28; amp, mphio, p, mphib, m, rb, rb^p, rb^2p, r1^p) */
 enum { PT_TRANSPIRAL = 2, PT_STEADYSPIRAL = 3, PT_ELLDISK = 4, PT_LOPSIDED = 6,
        PT_COSMPHI = 28 };
+/* SpiralArmsPotential (SpiralArmsPotential.c), 3D and planar: args (nCs,
+   amp, N, sin alpha, tan alpha, r_ref, phi_ref, Rs, H, omega, Cs[nCs]) */
+enum { PT_SPIRALARMS = 27 };
 
 static int is_ellipsoidal(int type)
 {
@@ -607,7 +610,10 @@ static int decode_entries(opot *P, int *idx, int n, const int **type, const doub
       continue;
     }
     const double *a = *args;
-    int na = is_ellipsoidal(t) ? ell_nargs(a) : t == PT_SCF ? scf_nargs(a) : nargs_of(t, planar);
+    int na = is_ellipsoidal(t)    ? ell_nargs(a)
+             : t == PT_SCF         ? scf_nargs(a)
+             : t == PT_SPIRALARMS  ? 10 + (int)a[0]
+                                   : nargs_of(t, planar);
     if (na < 0) return -1;
     c->ea = a;
     for (int k = 0; k < na && k < 9; k++) c->p[k] = a[k];
@@ -1255,9 +1261,96 @@ static double disk_pert(const ocomp *c, int which, double R, double phi)
   }
 }
 
+/* ---- SpiralArmsPotential: the potential (SpiralArmsPotentialEval) with
+   its derivatives by second-order forward differentiation over (R, z, phi)
+   (this file's own dual arithmetic); the reference differentiates by hand,
+   so the two agree to rounding, not bit for bit ---- */
+typedef struct {
+  double v, g[3], h[3][3];
+} odual;
+
+static odual od_var(double v, int i)
+{
+  odual r;
+  memset(&r, 0, sizeof(r));
+  r.v = v;
+  r.g[i] = 1.;
+  return r;
+}
+
+static odual od_apply(odual u, double f, double f1, double f2)
+{
+  odual r;
+  r.v = f;
+  for (int a = 0; a < 3; a++) r.g[a] = f1 * u.g[a];
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) r.h[a][b] = f1 * u.h[a][b] + f2 * u.g[a] * u.g[b];
+  return r;
+}
+
+static odual od_mul(odual x, odual y)
+{
+  odual r;
+  r.v = x.v * y.v;
+  for (int a = 0; a < 3; a++) r.g[a] = x.g[a] * y.v + x.v * y.g[a];
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++)
+      r.h[a][b] = x.h[a][b] * y.v + x.g[a] * y.g[b] + x.g[b] * y.g[a] + x.v * y.h[a][b];
+  return r;
+}
+
+static odual od_lin(double ca, odual x, double c0)
+{
+  odual r = x;
+  r.v = ca * x.v + c0;
+  for (int a = 0; a < 3; a++) {
+    r.g[a] = ca * x.g[a];
+    for (int b = 0; b < 3; b++) r.h[a][b] = ca * x.h[a][b];
+  }
+  return r;
+}
+
+static odual od_rcp(odual u) { double i = 1. / u.v; return od_apply(u, i, -i * i, 2. * i * i * i); }
+static odual od_exp(odual u) { double e = exp(u.v); return od_apply(u, e, e, e); }
+static odual od_log(odual u) { double i = 1. / u.v; return od_apply(u, log(u.v), i, -i * i); }
+static odual od_cos(odual u) { return od_apply(u, cos(u.v), -sin(u.v), -cos(u.v)); }
+static odual od_cosh(odual u) { return od_apply(u, cosh(u.v), sinh(u.v), cosh(u.v)); }
+
+/* Phi = -amp H exp(-(R - r_ref)/Rs) sum_n Cn / (Kn Dn) cos(n gamma) /
+   cosh(Kn z / Bn)^Bn with the reference's gam, K, B, D */
+static odual spiral_pot(const ocomp *c, double R, double z, double phi)
+{
+  const double *a = c->ea;
+  int nC = (int)a[0];
+  double amp = a[1], N = a[2], sa = a[3], ta = a[4], rref = a[5], phiref = a[6], Rs = a[7];
+  double H = a[8], om = a[9], t = c->t;
+  odual vR = od_var(R, 0), vz = od_var(z, 1), iR = od_rcp(vR);
+  odual gam = od_lin(-N / ta, od_log(od_lin(1. / rref, vR, 0.)), 0.);
+  gam.g[2] += N;
+  gam.v += N * (phi - om * t - phiref);
+  odual sum = od_lin(0., vR, 0.);
+  for (int n = 1; n <= nC; n++) {
+    double Cn = a[9 + n];
+    odual Kn = od_lin(n * N / sa, iR, 0.), KH = od_lin(H, Kn, 0.);
+    odual Bn = od_mul(KH, od_lin(0.4, KH, 1.));
+    odual Dn = od_mul(od_lin(1., od_mul(KH, od_lin(0.3, KH, 1.)), 1.), od_rcp(od_lin(0.3, KH, 1.)));
+    odual cs = od_cos(od_lin((double)n, gam, 0.));
+    odual arg = od_mul(od_mul(Kn, vz), od_rcp(Bn));
+    odual sech = od_exp(od_mul(od_lin(-1., Bn, 0.), od_log(od_cosh(arg))));
+    odual term = od_mul(od_mul(cs, sech), od_rcp(od_mul(Kn, Dn)));
+    sum.v += Cn * term.v;
+    for (int i = 0; i < 3; i++) {
+      sum.g[i] += Cn * term.g[i];
+      for (int j = 0; j < 3; j++) sum.h[i][j] += Cn * term.h[i][j];
+    }
+  }
+  return od_lin(-amp * H, od_mul(od_exp(od_lin(-1. / Rs, vR, rref / Rs)), sum), 0.);
+}
+
 /* ---- 3D component forces ---- */
 static double comp_Rforce(ocomp *c, double R, double Z, double phi)
 {
+  if (c->type == PT_SPIRALARMS) return -spiral_pot(c, R, Z, phi).g[0];
   if (c->type == PT_DEHNENBAR) return dbar_force3(c, 0, R, Z, phi);
   if (c->type == PT_SCF) return scf_force3(c, 0, R, Z, phi);
   if (is_new_spherical(c->type)) return sph_force3(c, R, Z, R);
@@ -1302,6 +1395,7 @@ static double comp_Rforce(ocomp *c, double R, double Z, double phi)
 
 static double comp_zforce(ocomp *c, double R, double Z, double phi)
 {
+  if (c->type == PT_SPIRALARMS) return -spiral_pot(c, R, Z, phi).g[1];
   if (c->type == PT_DEHNENBAR) return dbar_force3(c, 1, R, Z, phi);
   if (c->type == PT_SCF) return scf_force3(c, 1, R, Z, phi);
   if (is_new_spherical(c->type)) return sph_force3(c, R, Z, Z);
@@ -1350,6 +1444,7 @@ static double comp_zforce(ocomp *c, double R, double Z, double phi)
 
 static double comp_phitorque(const ocomp *c, double R, double Z, double phi)
 {
+  if (c->type == PT_SPIRALARMS) return -spiral_pot(c, R, Z, phi).g[2];
   if (c->type == PT_DEHNENBAR) return dbar_force3(c, 2, R, Z, phi);
   if (c->type == PT_SCF) return scf_force3(c, 2, R, Z, phi);
   if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 2, R, Z, phi);
@@ -1378,6 +1473,11 @@ static void sph_derivs(const ocomp *c, double r, double *dphi, double *d2phi)
 /* 3D Hessian terms: which = 0 R2, 1 z2, 2 Rz, 3 phi2, 4 Rphi, 5 zphi */
 static double comp_hess(const ocomp *c, int which, double R, double Z, double phi)
 {
+  if (c->type == PT_SPIRALARMS) { /* R2, z2, Rz, phi2, Rphi, zphi */
+    odual P = spiral_pot(c, R, Z, phi);
+    static const int ia[6] = {0, 1, 0, 2, 0, 1}, ib[6] = {0, 1, 1, 2, 2, 2};
+    return P.h[ia[which]][ib[which]];
+  }
   if (c->type == PT_DEHNENBAR) return dbar_hess3(c, which, R, Z, phi);
   if (c->type == PT_SCF) return scf_hess3(c, which, R, Z, phi);
   if (is_new_spherical(c->type)) return sph_hess3(c, which, R, Z);
@@ -1512,6 +1612,7 @@ static double comp_hess(const ocomp *c, int which, double R, double Z, double ph
 /* ---- planar component forces ---- */
 static double comp_planarRforce(const ocomp *c, double R, double phi)
 {
+  if (c->type == PT_SPIRALARMS) return -spiral_pot(c, R, 0., phi).g[0];
   if (is_disk_pert(c->type)) return disk_pert(c, 0, R, phi);
   if (c->type == PT_DEHNENBAR) return dbar_force2(c, 0, R, phi);
   if (c->type == PT_SCF) return scf_force3(c, 0, R, 0.0, phi); /* SCFPotentialPlanarRforce */
@@ -1564,6 +1665,7 @@ static double comp_planarRforce(const ocomp *c, double R, double phi)
 
 static double comp_planarphitorque(const ocomp *c, double R, double phi)
 {
+  if (c->type == PT_SPIRALARMS) return -spiral_pot(c, R, 0., phi).g[2];
   if (is_disk_pert(c->type)) return disk_pert(c, 1, R, phi);
   if (c->type == PT_DEHNENBAR) return dbar_force2(c, 2, R, phi);
   if (c->type == PT_SCF) return scf_force3(c, 2, R, 0.0, phi);
@@ -1580,6 +1682,10 @@ static double comp_planarphitorque(const ocomp *c, double R, double phi)
 /* planar Hessian: which = 0 R2, 1 phi2, 2 Rphi */
 static double comp_planarhess(const ocomp *c, int which, double R, double phi)
 {
+  if (c->type == PT_SPIRALARMS) { /* R2, phi2, Rphi */
+    odual P = spiral_pot(c, R, 0., phi);
+    return which == 0 ? P.h[0][0] : which == 1 ? P.h[2][2] : P.h[0][2];
+  }
   if (is_disk_pert(c->type)) return disk_pert(c, 2 + which, R, phi);
   if (c->type == PT_DEHNENBAR) return dbar_hess2(c, which, R, phi);
   if (c->type == PT_SCF) return scf_hess2(c, which, R, phi);
@@ -1654,6 +1760,7 @@ static double comp_planarhess(const ocomp *c, int which, double R, double phi)
 /* ---- potential values (for energies) ---- */
 static double comp_eval(const ocomp *c, double R, double Z, double phi)
 {
+  if (c->type == PT_SPIRALARMS) return spiral_pot(c, R, Z, phi).v;
   if (c->type == PT_SCF) return scf_eval(c, R, Z, phi);
   if (c->type == PT_DEHNENBAR) return NAN; /* no C evaluation in the reference */
   if (is_new_spherical(c->type)) return sph_eval(c, R, Z);

@@ -62,10 +62,10 @@ def test_planar_orbit_routes(hooks):
 
 def test_unsupported_potential_falls_back(hooks):
     from galpy.orbit import Orbit
-    from galpy.potential import SpiralArmsPotential
+    from galpy.potential import SoftenedNeedleBarPotential
 
     o = Orbit([1.0, 0.1, 1.1, 0.0, 0.1, 0.0])
-    o.integrate(np.linspace(0, 1, 11), SpiralArmsPotential(), method="dop853_cuda")
+    o.integrate(np.linspace(0, 1, 11), SoftenedNeedleBarPotential(), method="dop853_cuda")
     assert hooks == []  # galpy's own integrator ran
 
 
@@ -90,6 +90,20 @@ def test_bar_and_scf_route(hooks):
         return
     o.integrate(np.linspace(0, 1, 11), tdep, method="rk4_cuda")
     assert len(hooks) == 2
+
+
+def test_spiral_arms_route(hooks):
+    """SpiralArmsPotential goes to the engine with up to six Fourier terms;
+    more stay with galpy."""
+    from galpy.orbit import Orbit
+    from galpy.potential import MWPotential2014, SpiralArmsPotential
+
+    o = Orbit([1.0, 0.1, 1.1, 0.0, 0.1, 0.0])
+    arms = SpiralArmsPotential(N=4, omega=0.6, Cs=[1.0, 0.5, 0.2])
+    o.integrate(np.linspace(0, 1, 11), [*MWPotential2014, arms], method="dop853_cuda")
+    assert len(hooks) == 1
+    o.integrate(np.linspace(0, 1, 11), SpiralArmsPotential(Cs=[1.0] * 7), method="dop853_cuda")
+    assert len(hooks) == 1
 
 
 def test_spherical_potential_routes(hooks):

@@ -471,3 +471,131 @@ def test_engine_perturbation_machines_vs_oracle(harness, name, method):
     strict = same & ~kink
     assert np.median(d[strict]) < 1e-12 and d[strict].max() < 1e-9, d[strict].max()
     assert (d < 1e-6).all()
+
+
+# ---- SpiralArmsPotential: the oracle differentiates its potential by dual numbers
+@pytest.mark.parametrize("planar", [False, True])
+def test_spiral_arms_layout_and_forces_vs_galpy_python(planar):
+    """The argument layout galpy's integrators build, and the oracle's forces
+    and second derivatives against galpy's Python SpiralArmsPotential (its
+    hand-written derivatives), at two times."""
+    P = galpy_or_skip()
+    pot = P.SpiralArmsPotential(amp=0.8, N=4, alpha=np.deg2rad(12), r_ref=1.1, phi_ref=0.3,
+                                Rs=0.4, H=0.1, omega=0.55, Cs=[8 / (3 * np.pi), 0.5,
+                                                              8 / (15 * np.pi)])
+    if planar:
+        from galpy.orbit.integratePlanarOrbit import _parse_pot
+        gp = P.toPlanarPotential(pot)
+    else:
+        from galpy.orbit.integrateFullOrbit import _parse_pot
+        gp = pot
+    _, pt, pa, _ = _parse_pot([gp])
+    assert list(pt) == [27]
+    _, ref_a = TP.spiral_arms("spiral3+mw14", planar)
+    np.testing.assert_allclose(pa, ref_a[-len(pa):], rtol=1e-15, atol=0)
+    rng = np.random.default_rng(4)
+    R, phi = rng.uniform(0.3, 2.0, 50), rng.uniform(0, 2 * np.pi, 50)
+    z = np.zeros(50) if planar else rng.normal(0, 0.3, 50)
+    names = (["Rforce", "phitorque", "R2deriv", "phi2deriv", "Rphideriv"] if planar else
+             ["Rforce", "zforce", "phitorque", "R2deriv", "z2deriv", "Rzderiv", "phi2deriv",
+              "Rphideriv", "phizderiv"])
+    for t in (0.0, 1.7):
+        got = oracle.forces(R, z, phi, np.array([27], np.int32), np.asarray(pa), planar=planar,
+                            t=t)
+        for k, nm in enumerate(names):
+            ref = np.array([getattr(gp, nm)(R[i], *([] if planar else [z[i]]), phi=phi[i], t=t,
+                                            use_physical=False) for i in range(R.size)])
+            assert np.abs(got[:, k] - ref).max() <= 5e-14 * np.abs(ref).max(), (nm, t)
+    if not planar:
+        pv = oracle.potential(R, z, phi, np.array([27], np.int32), np.asarray(pa))
+        ref = np.array([pot(R[i], z[i], phi=phi[i], use_physical=False) for i in range(50)])
+        assert np.abs(pv - ref).max() <= 1e-14 * np.abs(ref).max()
+
+
+@needs_ref
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", TP.SPIRAL_ARMS)
+@pytest.mark.parametrize("method", METHODS)
+def test_spiral_orbits_vs_reference_build(name, planar, method):
+    """The reference differentiates the spiral potential by hand, the oracle
+    by dual numbers: orbits agree to each orbit's own one-ulp response."""
+    from helpers import cyl_diff
+
+    pt, pa = TP.spiral_arms(name, planar)
+    yo = ics(8, planar)
+    t = np.linspace(0.0, 8.0, 41)
+    a, ea, _, _ = oracle.integrate(yo, t, pt, pa, method, planar=planar, **tol(method))
+    b, eb, _, _ = oracle.integrate(yo, t, pt, pa, method, planar=planar, impl="ref",
+                                   **tol(method))
+    np.testing.assert_array_equal(ea, eb)
+    u = TP.ulp_response(oracle, yo, t, pt, pa, method, planar, a, **tol(method))
+    d = cyl_diff(a, b).max(axis=(1, 2))
+    assert (d <= 30 * np.maximum(u, 1e-15)).all(), (d / np.maximum(u, 1e-15)).max()
+
+
+@needs_ref
+@pytest.mark.parametrize("planar", [False, True])
+def test_spiral_dxdv_vs_reference_build(planar):
+    pt, pa = TP.spiral_arms("spiral3+mw14", planar)
+    dim = 2 if planar else 3
+    rng = np.random.default_rng(5)
+    w = np.concatenate([rng.uniform(0.6, 1.2, (4, dim)), rng.normal(0, 0.2, (4, dim)),
+                        rng.normal(0, 1, (4, 2 * dim))], 1)
+    w[:, dim + 1] += 1.0
+    t = np.linspace(0.0, 4.0, 17)
+    for method in ("rk4", "symplec4", "dop853"):
+        a = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar, **tol(method))[0]
+        b = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar, impl="ref",
+                                  **tol(method))[0]
+        assert np.abs(a - b).max() < 1e-9 * max(1.0, np.abs(a).max()), method
+
+
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", TP.SPIRAL_ARMS)
+def test_engine_spiral_forces_and_tidal(harness, name, planar):
+    """The engine's spiral arms (second-order forward differentiation in
+    Cartesian form) against the oracle's cylindrical derivatives."""
+    pt, pa = TP.spiral_arms(name, planar)
+    rng = np.random.default_rng(16)
+    R = rng.uniform(0.3, 2.0, 120)
+    z = np.zeros(120) if planar else rng.normal(0, 0.4, 120)
+    phi = rng.uniform(0, 2 * np.pi, 120)
+    for t in (0.0, 2.5, 7.0):
+        f = oracle.forces(R, z, phi, pt, pa, planar=planar, t=t)
+        tq = f[:, 1] if planar else f[:, 2]
+        ax = np.cos(phi) * f[:, 0] - np.sin(phi) * tq / R
+        ay = np.sin(phi) * f[:, 0] + np.cos(phi) * tq / R
+        acc, K, _ = harness.forces(R * np.cos(phi), R * np.sin(phi), z, pt, pa, planar=planar,
+                                   t=t)
+        ref = np.stack([ax, ay] + ([] if planar else [f[:, 1]]), 1)
+        assert np.abs(acc[:, :ref.shape[1]] - ref).max() < 1e-14 * np.abs(ref).max(), t
+        Kref = cyl_to_K(f, R, phi, planar)
+        assert np.abs(K[:, :Kref.shape[1]] - Kref).max() < 1e-12 * np.abs(Kref).max(), t
+
+
+@pytest.mark.parametrize("method", ["leapfrog", "symplec4", "rk4", "dopr54", "dop853"])
+@pytest.mark.parametrize("planar", [False, True])
+def test_engine_spiral_machines_vs_oracle(harness, planar, method):
+    pt, pa = TP.spiral_arms("spiral3+mw14", planar)
+    y0 = ics(24, planar, seed=31)
+    t = np.linspace(0.0, 10.0, 41)
+    with oracle.phi_from_atan2():
+        ref, _, nref, _ = oracle.integrate(y0, t, pt, pa, method, planar=planar, **tol(method))
+    out, err, ns = harness.integrate(c2r(y0, planar), t, pt, pa, method, planar=planar,
+                                     **tol(method))
+    assert not err.any()
+    ref_r = np.stack([c2r(ref[:, j], planar) for j in range(len(t))], 1)
+    d = np.abs(out - ref_r).reshape(len(y0), -1).max(1)
+    same = ns == nref
+    assert same.mean() > 0.9
+    assert np.median(d[same]) < 1e-12 and d[same].max() < 1e-9, d[same].max()
+    assert (d < 1e-6).all()
+
+
+def test_spiral_arms_term_limit():
+    import galpy_b200 as gb
+
+    mt, ma = TP.mw14()
+    a = TP.spiral_arms_args(Cs=[1.0] * 7)
+    with pytest.raises(gb.PotentialNotSupported):
+        gb.compile_potential((np.array(mt + [27], np.int32), np.array(ma + a)))

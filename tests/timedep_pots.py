@@ -143,3 +143,32 @@ def planar_perturbation(name):
 
 PLANAR_PERTURBATIONS = ["transspiral+mw14", "steadyspiral+mw14", "steadyspiral_on+mw14",
                         "elldisk+mw14", "lopsided+mw14", "cosmphi+mw14"]
+
+
+def spiral_arms_args(Cs=(1.0,), amp=1.0, N=2, alpha=0.2, r_ref=1.0, phi_ref=0.0, Rs=0.3,
+                     H=0.125, omega=0.0):
+    """SpiralArmsPotential's argument list (integrateFullOrbit.py's layout:
+    nCs, amp, N, sin alpha, tan alpha, r_ref, phi_ref, Rs, H, omega, Cs) for
+    the constructor's N and alpha, which galpy stores negated (trailing
+    arms)."""
+    return [float(len(Cs)), amp, float(-N), np.sin(-alpha), np.tan(-alpha), r_ref, phi_ref, Rs,
+            H, omega] + [float(c) for c in Cs]
+
+
+def spiral_arms(name, planar=False):
+    """(pot_type, pot_args) of MWPotential2014 plus one SpiralArmsPotential
+    (type 27): galpy's defaults set rotating, or four arms with three
+    Fourier terms (the Cox & Gomez sinusoidal-density coefficients)."""
+    mw_t, mw_a = mw14(planar)
+    if name == "spiral+mw14":
+        a = spiral_arms_args(omega=0.65)
+    elif name == "spiral3+mw14":
+        a = spiral_arms_args(Cs=(8 / (3 * np.pi), 0.5, 8 / (15 * np.pi)), amp=0.8, N=4,
+                             alpha=np.deg2rad(12), r_ref=1.1, phi_ref=0.3, Rs=0.4, H=0.1,
+                             omega=0.55)
+    else:
+        raise KeyError(name)
+    return np.asarray(mw_t + [27], np.int32), np.asarray(mw_a + a, np.float64)
+
+
+SPIRAL_ARMS = ["spiral+mw14", "spiral3+mw14"]
