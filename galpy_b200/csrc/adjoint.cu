@@ -239,6 +239,7 @@ int galpy_cuda_adjoint_params(int planar, int npot, const int* pot_type, const d
     // the adjoint's DOP853 evaluates static forces and needs the tidal
     // tensor, which the device does not have for an SCF expansion
     if (pot_type[k] == T_DEHNENBAR || pot_type[k] == T_SCF || pot_type[k] == T_SPIRALARMS ||
+        pot_type[k] == T_NEEDLEBAR ||
         is_wrapper(pot_type[k]) || is_disk_pert(pot_type[k]))
       return gpc_report_error(GALPY_CUDA_ERR_POTENTIAL,
                               "gradients through a time-dependent or SCF potential are not "

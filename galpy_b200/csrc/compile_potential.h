@@ -53,6 +53,7 @@ inline int galpy_nargs(int type, int planar, const double* p = nullptr)
     case T_HENONHEILES: return planar ? 1 : -1;  // (amp); a planarPotential only
     case T_KUZMINDISK: return 2;
     case T_DEHNENBAR: return 6;
+    case T_NEEDLEBAR: return 13;  // (amp, a, b, c^2, pa, omegab, 7 cache slots)
     case T_SPIRALARMS:  // (nCs, amp, N, sin alpha, tan alpha, r_ref, phi_ref, Rs, H, omega, Cs)
       return p && (int)p[0] >= 1 && (int)p[0] <= kSpiralMaxTerms ? 10 + (int)p[0] : -1;
     case T_TRANSPIRAL: case T_STEADYSPIRAL: return planar ? 8 : -1;  // planarPotentials only
@@ -479,6 +480,12 @@ inline int compile_entries(int planar, int n, const int*& tp, const double*& p, 
         c.c[9] = p[0];
         for (int n = 0; n < (int)p[0]; n++) c.c[10 + n] = p[10 + n];
         if (!(p[3] != 0.0) || !(p[4] != 0.0) || !(p[7] > 0.0)) return -1;
+        break;
+      }
+      case T_NEEDLEBAR: {  // (amp, a, b, c^2, pa, omegab, cache)
+        if (!(p[1] > 0.0) || !(p[3] >= 0.0) || !(p[2] >= 0.0)) return -1;
+        for (int j = 0; j < 6; j++) c.c[j] = p[j];
+        c.c[6] = 0.5 / p[1];
         break;
       }
       case T_DEHNENBAR: {  // (amp * af, tform, tsteady, rb, omegab, barphi)

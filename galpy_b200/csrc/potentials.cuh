@@ -922,12 +922,16 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
       break;
     }
     case T_DEHNENBAR:
+    case T_NEEDLEBAR:
     case T_SCF: {  // in float64; carried by the full run-time list only
       if constexpr (TYPE == kRunTimeAll) {
         double ax, ay, az;
-        if (type == T_DEHNENBAR)
+        if (type == T_DEHNENBAR) {
           dbar_accel<PLANAR>(cp, t, (double)x, (double)y, (double)z, ax, ay, az);
-        else
+        } else if (type == T_NEEDLEBAR) {
+          ax = ay = az = 0.0;
+          needle_accel<PLANAR>(cp, t, (double)x, (double)y, (double)z, ax, ay, az, nullptr);
+        } else
           scf_accel<PLANAR>(cp, (double)x, (double)y, (double)z, ax, ay, az);
         a0.x += T(ax);
         a0.y += T(ay);
@@ -1399,6 +1403,9 @@ GPC_HD GPC_FI void comp_tidal(const GpComp* __restrict__ cp, int type, double x,
     case T_DEHNENBAR:
       dbar_tidal<PLANAR>(cp, t, x, y, z, ax0, ay0, az0, K);
       break;
+    case T_NEEDLEBAR:
+      needle_accel<PLANAR>(cp, t, x, y, z, ax0, ay0, az0, K);
+      break;
     case T_SCF:
       scf_tidal<PLANAR>(cp, x, y, z, ax0, ay0, az0, K);
       break;
@@ -1657,6 +1664,9 @@ GPC_HD inline double comp_value(const GpComp* __restrict__ cp, double x, double 
     }
     case T_SPIRALARMS:  // at t = 0 (time-dependent: the hooks keep galpy's path)
       phi += spiral_potential<false>(cp, sqrt(R2), z, atan2(y, x), 0.0).v;
+      break;
+    case T_NEEDLEBAR:  // at t = 0, likewise
+      phi += needle_value(cp, 0.0, x, y, z);
       break;
     case T_TRANSPIRAL: case T_STEADYSPIRAL: case T_ELLDISK: case T_LOPSIDED: case T_COSMPHI:
     case T_DEHNENBAR:  // no evaluation in the reference's C (the hooks keep galpy's)

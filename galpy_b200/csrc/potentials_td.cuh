@@ -44,6 +44,8 @@ enum : int { T_TRANSPIRAL = 2, T_STEADYSPIRAL = 3, T_ELLDISK = 4, T_LOPSIDED = 6
 // SpiralArmsPotential (SpiralArmsPotential.c): 3D and planar
 enum : int { T_SPIRALARMS = 27 };
 constexpr int kSpiralMaxTerms = 6;  // Cn terms a record holds
+// SoftenedNeedleBarPotential (SoftenedNeedleBarPotential.c): 3D and planar
+enum : int { T_NEEDLEBAR = 25 };
 
 GPC_HD GPC_FI constexpr bool is_disk_pert(int t)
 {
@@ -58,7 +60,7 @@ enum : int { T_PAYLOAD = -100 };
 GPC_HD GPC_FI constexpr bool needs_full_list(int t)
 {
   return is_ellipsoidal(t) || t == T_DEHNENBAR || t == T_SCF || t == T_PAYLOAD || is_wrapper(t) ||
-         is_disk_pert(t) || t == T_SPIRALARMS;
+         is_disk_pert(t) || t == T_SPIRALARMS || t == T_NEEDLEBAR;
 }
 
 // Doubles of payload per continuation record: the record after its
@@ -486,6 +488,71 @@ GPC_HD inline void spiral_accel(const GpComp* __restrict__ cp, double x, double 
     K[4] -= s * Rz + c * iR * zp;
     K[5] -= P.h[1][1];
   }
+}
+
+// ---- SoftenedNeedleBar ------------------------------------------------------
+// In the frame turning with the bar (angle pa + omegab t):
+// Phi = amp ln[(x - a + T-) / (x + a + T+)] / (2a), T+- = sqrt((a +- x)^2 +
+// y^2 + u^2), u = b + sqrt(z^2 + c^2) (Long & Murali 1992).  Its gradient
+// per amplitude, with G = (a - x)/T- + (a + x)/T+ and T+ - T- = 4ax/(T+ + T-)
+// (no cancellation near x = 0):
+//   dPhi/dx = 2x / (T+ T- (T+ + T-)),  G/(2a) = (S - 4x^2/S) / (2 T+ T-), S = T+ + T-,
+//   dPhi/dy = y G/(2a s2),  dPhi/dz = w G/(2a s2),  s2 = y^2 + u^2, w = z u / sqrt(z^2 + c^2).
+// The Hessian adds h = ((a - x)/T-^3 + (a + x)/T+^3)/(2a) and k = (1/T-^3 -
+// 1/T+^3)/(2a) = 2x (T+^2 + T+ T- + T-^2) / (S T+^3 T-^3):
+//   xx h, xy -y k, xz -w k, yy g (s2 - 2y^2)/s2^2 - y^2 h/s2,
+//   yz -y w (2g/s2^2 + h/s2), zz (1 + b c^2/zc^3) g/s2 - w^2 (h/s2 + 2g/s2^2)
+// with g = G/(2a).  Record: c0 amp, c1 a, c2 b, c3 c^2, c4 pa, c5 omegab,
+// c6 1/(2a).
+template <bool PLANAR>
+GPC_HD inline void needle_accel(const GpComp* __restrict__ cp, double t, double X, double Y,
+                                double Z, double& ax, double& ay, double& az, double* K)
+{
+  const double amp = ldg(&cp->c[0]), a = ldg(&cp->c[1]), b = ldg(&cp->c[2]);
+  const double c2 = ldg(&cp->c[3]);
+  double sn, cs;
+  sincos(ldg(&cp->c[4]) + ldg(&cp->c[5]) * t, &sn, &cs);
+  const double x = cs * X + sn * Y, y = cs * Y - sn * X, z = PLANAR ? 0.0 : Z;
+  const double zc = sqrt(z * z + c2), u = b + zc, s2 = y * y + u * u, is2 = 1.0 / s2;
+  const double Tp = sqrt((a + x) * (a + x) + s2), Tm = sqrt((a - x) * (a - x) + s2);
+  const double S = Tp + Tm, iS = 1.0 / S, iPM = 1.0 / (Tp * Tm);
+  const double g = 0.5 * (S - 4.0 * x * x * iS) * iPM;  // G / (2a)
+  const double px = 2.0 * x * iPM * iS, py = y * g * is2;
+  const double fx = -amp * px, fy = -amp * py;
+  ax += cs * fx - sn * fy;
+  ay += sn * fx + cs * fy;
+  const double w = z * u / zc;
+  if (!PLANAR) az -= amp * w * g * is2;
+  if (!K) return;
+  const double iP3 = iPM * iPM * iPM, i2a = ldg(&cp->c[6]);
+  const double h = ((a - x) * Tp * Tp * Tp + (a + x) * Tm * Tm * Tm) * iP3 * i2a;
+  const double k = 2.0 * x * (Tp * Tp + Tp * Tm + Tm * Tm) * iS * iP3;
+  const double pxx = h, pxy = -y * k, pyy = g * (s2 - 2.0 * y * y) * is2 * is2 - y * y * h * is2;
+  // rotate the bar-frame Hessian back: R H R^T with R = [[cs, -sn], [sn, cs]]
+  const double c2r = cs * cs, s2r = sn * sn, csr = cs * sn;
+  K[0] -= amp * (c2r * pxx - 2.0 * csr * pxy + s2r * pyy);
+  K[1] -= amp * (csr * (pxx - pyy) + (c2r - s2r) * pxy);
+  K[2] -= amp * (s2r * pxx + 2.0 * csr * pxy + c2r * pyy);
+  if (!PLANAR) {
+    const double pxz = -w * k, pyz = -y * w * (2.0 * g * is2 * is2 + h * is2);
+    const double pzz = (1.0 + b * c2 / (zc * zc * zc)) * g * is2 - w * w * (h * is2 + 2.0 * g * is2 * is2);
+    K[3] -= amp * (cs * pxz - sn * pyz);
+    K[4] -= amp * (sn * pxz + cs * pyz);
+    K[5] -= amp * pzz;
+  }
+}
+
+// Potential of the needle bar at time t.
+GPC_HD inline double needle_value(const GpComp* __restrict__ cp, double t, double X, double Y,
+                                  double Z)
+{
+  const double amp = ldg(&cp->c[0]), a = ldg(&cp->c[1]), b = ldg(&cp->c[2]);
+  double sn, cs;
+  sincos(ldg(&cp->c[4]) + ldg(&cp->c[5]) * t, &sn, &cs);
+  const double x = cs * X + sn * Y, y = cs * Y - sn * X;
+  const double u = b + sqrt(Z * Z + ldg(&cp->c[3])), s2 = y * y + u * u;
+  const double Tp = sqrt((a + x) * (a + x) + s2), Tm = sqrt((a - x) * (a - x) + s2);
+  return amp * ldg(&cp->c[6]) * log((x - a + Tm) / (x + a + Tp));
 }
 
 // ---- SCF --------------------------------------------------------------------

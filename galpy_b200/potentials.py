@@ -48,11 +48,13 @@ WRAPPER_TYPES = (-1, -2, -5)
 # EllipticalDisk, LopsidedDisk, CosmphiDisk (no potential evaluation in C)
 DISK_PERTURBATION_TYPES = (2, 3, 4, 6, 28)
 # SpiralArmsPotential (Cox & Gomez arms rotating at omega; up to six terms)
-T_SPIRALARMS = 27
-TIME_DEPENDENT_TYPES = (T_DEHNENBAR, T_SPIRALARMS) + WRAPPER_TYPES + DISK_PERTURBATION_TYPES
+# and the rotating SoftenedNeedleBarPotential
+T_SPIRALARMS, T_NEEDLEBAR = 27, 25
+TIME_DEPENDENT_TYPES = (T_DEHNENBAR, T_SPIRALARMS, T_NEEDLEBAR) + WRAPPER_TYPES + \
+    DISK_PERTURBATION_TYPES
 SUPPORTED_TYPES = (T_LOGHALO, T_MN, T_HERNQUIST, T_NFW, T_PSWC, T_FLATPOWER,
                    T_KKS, T_HENONHEILES, T_KUZMINDISK, T_DEHNENBAR, T_SCF,
-                   T_SPIRALARMS) + SPHERICAL_TYPES + \
+                   T_SPIRALARMS, T_NEEDLEBAR) + SPHERICAL_TYPES + \
     ELLIPSOIDAL_TYPES + WRAPPER_TYPES + DISK_PERTURBATION_TYPES
 
 

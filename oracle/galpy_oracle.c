@@ -119,6 +119,9 @@ enum { PT_TRANSPIRAL = 2, PT_STEADYSPIRAL = 3, PT_ELLDISK = 4, PT_LOPSIDED = 6,
 /* SpiralArmsPotential (SpiralArmsPotential.c), 3D and planar: args (nCs,
    amp, N, sin alpha, tan alpha, r_ref, phi_ref, Rs, H, omega, Cs[nCs]) */
 enum { PT_SPIRALARMS = 27 };
+/* SoftenedNeedleBarPotential (SoftenedNeedleBarPotential.c), 3D and planar:
+   args (amp, a, b, c^2, pa, omegab, 7 cache slots the reference fills) */
+enum { PT_NEEDLEBAR = 25 };
 
 static int is_ellipsoidal(int type)
 {
@@ -185,6 +188,7 @@ static int nargs_of(int type, int planar)
   case PT_HENONHEILES: return planar ? 1 : -1;
   case PT_KUZMINDISK: return 2;
   case PT_DEHNENBAR: return 6;
+  case PT_NEEDLEBAR: return 13;
   case PT_TRANSPIRAL: case PT_STEADYSPIRAL: return planar ? 8 : -1;
   case PT_ELLDISK: return planar ? 6 : -1;
   case PT_LOPSIDED: return planar ? 4 : -1;
@@ -1347,11 +1351,105 @@ static odual spiral_pot(const ocomp *c, double R, double z, double phi)
   return od_lin(-amp * H, od_mul(od_exp(od_lin(-1. / Rs, vR, rref / Rs)), sum), 0.);
 }
 
+/* ---- SoftenedNeedleBar: Phi = amp ln[(x - a + T-) / (x + a + T+)] / (2a)
+   in the frame turning with the bar (angle pa + omegab t), T+- = sqrt((a +-
+   x)^2 + y^2 + (b + sqrt(z^2 + c^2))^2).  Restated in the reference's
+   arithmetic order (SoftenedNeedleBarPotential.c:5-72, 143-205) so results
+   are bit-identical; its force cache only repeats the same values ---- */
+typedef struct {
+  double x, y, z, zc, Tp, Tm, cd, sd;
+} oneedle;
+
+static oneedle needle_frame(const ocomp *c, double R, double z, double phi)
+{
+  const double a = c->p[1], b = c->p[2], c2 = c->p[3], pa = c->p[4], om = c->p[5];
+  oneedle f;
+  double phid = phi - pa - om * c->t;
+  f.cd = cos(phid);
+  f.sd = sin(phid);
+  f.x = R * f.cd;
+  f.y = R * f.sd;
+  f.z = z;
+  double rest = f.y * f.y + pow(b + sqrt(z * z + c2), 2);
+  f.Tp = sqrt(pow(a + f.x, 2) + rest);
+  f.Tm = sqrt(pow(a - f.x, 2) + rest);
+  f.zc = sqrt(z * z + c2);
+  return f;
+}
+
+/* the force per unit amplitude in the inertial frame: out[0] x, [1] y, [2] z */
+static void needle_xyz(const ocomp *c, double R, double z, double phi, double *out)
+{
+  const double b = c->p[2], pa = c->p[4], om = c->p[5];
+  oneedle f = needle_frame(c, R, z, phi);
+  double S = f.Tp + f.Tm;
+  double fx = -2. * f.x / f.Tp / f.Tm / S;
+  double fy = -f.y / 2. / f.Tp / f.Tm * (S - 4. * f.x * f.x / S) / (f.y * f.y + pow(b + f.zc, 2));
+  double fz = -f.z / 2. / f.Tp / f.Tm * (S - 4. * f.x * f.x / S) /
+              (f.y * f.y + pow(b + f.zc, 2)) * (b + f.zc) / f.zc;
+  double ca = cos(pa + om * c->t), sa = sin(pa + om * c->t);
+  out[0] = ca * fx - sa * fy;
+  out[1] = sa * fx + ca * fy;
+  out[2] = fz;
+}
+
+/* which: 0 Rforce, 1 zforce, 2 phitorque */
+static double needle_force(const ocomp *c, int which, double R, double z, double phi)
+{
+  double F[3];
+  needle_xyz(c, R, z, phi, F);
+  if (which == 0) return c->p[0] * (cos(phi) * F[0] + sin(phi) * F[1]);
+  if (which == 1) return c->p[0] * F[2];
+  return c->p[0] * R * (-sin(phi) * F[0] + cos(phi) * F[1]);
+}
+
+/* cylindrical second derivatives (amp times): 0 R2, 1 z2, 2 phi2, 3 Rz,
+   4 Rphi, 5 zphi, from the bar-frame Cartesian Hessian */
+static double needle_hess(const ocomp *c, int which, double R, double z, double phi)
+{
+  const double amp = c->p[0], a = c->p[1], b = c->p[2], c2 = c->p[3];
+  oneedle f = needle_frame(c, R, z, phi);
+  double cd = f.cd, sd = f.sd, x = R * cd, y = R * sd;
+  double zc = sqrt(z * z + c2), u = b + zc, s2 = y * y + u * u;
+  double Tp3 = f.Tp * f.Tp * f.Tp, Tm3 = f.Tm * f.Tm * f.Tm;
+  double G = (a - x) / f.Tm + (a + x) / f.Tp;
+  double H = (a - x) / Tm3 + (a + x) / Tp3;
+  double K = 1. / Tm3 - 1. / Tp3;
+  double w = z * u / zc;
+  double px = (1. / f.Tm - 1. / f.Tp) / 2. / a, py = y * G / 2. / a / s2;
+  double pxx = H / 2. / a, pxy = -y * K / 2. / a, pxz = -w * K / 2. / a;
+  double pyy = (G * (s2 - 2. * y * y) / s2 / s2 - y * y * H / s2) / 2. / a;
+  double pyz = -y * w * (2. * G / s2 / s2 + H / s2) / 2. / a;
+  double pzz = ((1. + b * c2 / zc / zc / zc) * G / s2 - w * w * (H / s2 + 2. * G / s2 / s2)) / 2. / a;
+  double h;
+  switch (which) {
+  case 0: h = cd * cd * pxx + 2. * cd * sd * pxy + sd * sd * pyy; break;
+  case 1: h = pzz; break;
+  case 2:
+    h = R * R * (sd * sd * pxx - 2. * sd * cd * pxy + cd * cd * pyy) - R * (cd * px + sd * py);
+    break;
+  case 3: h = cd * pxz + sd * pyz; break;
+  case 4:
+    h = R * (-sd * cd * pxx + (cd * cd - sd * sd) * pxy + sd * cd * pyy) - sd * px + cd * py;
+    break;
+  default: h = R * (-sd * pxz + cd * pyz); break;
+  }
+  return amp * h;
+}
+
+static double needle_eval(const ocomp *c, double R, double z, double phi)
+{
+  const double a = c->p[1];
+  oneedle f = needle_frame(c, R, z, phi);
+  return 0.5 * c->p[0] * log((f.x - a + f.Tm) / (f.x + a + f.Tp)) / a;
+}
+
 /* ---- 3D component forces ---- */
 static double comp_Rforce(ocomp *c, double R, double Z, double phi)
 {
   if (c->type == PT_SPIRALARMS) return -spiral_pot(c, R, Z, phi).g[0];
   if (c->type == PT_DEHNENBAR) return dbar_force3(c, 0, R, Z, phi);
+  if (c->type == PT_NEEDLEBAR) return needle_force(c, 0, R, Z, phi);
   if (c->type == PT_SCF) return scf_force3(c, 0, R, Z, phi);
   if (is_new_spherical(c->type)) return sph_force3(c, R, Z, R);
   if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 0, R, Z, phi);
@@ -1397,6 +1495,7 @@ static double comp_zforce(ocomp *c, double R, double Z, double phi)
 {
   if (c->type == PT_SPIRALARMS) return -spiral_pot(c, R, Z, phi).g[1];
   if (c->type == PT_DEHNENBAR) return dbar_force3(c, 1, R, Z, phi);
+  if (c->type == PT_NEEDLEBAR) return needle_force(c, 1, R, Z, phi);
   if (c->type == PT_SCF) return scf_force3(c, 1, R, Z, phi);
   if (is_new_spherical(c->type)) return sph_force3(c, R, Z, Z);
   if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 1, R, Z, phi);
@@ -1446,6 +1545,7 @@ static double comp_phitorque(const ocomp *c, double R, double Z, double phi)
 {
   if (c->type == PT_SPIRALARMS) return -spiral_pot(c, R, Z, phi).g[2];
   if (c->type == PT_DEHNENBAR) return dbar_force3(c, 2, R, Z, phi);
+  if (c->type == PT_NEEDLEBAR) return needle_force(c, 2, R, Z, phi);
   if (c->type == PT_SCF) return scf_force3(c, 2, R, Z, phi);
   if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 2, R, Z, phi);
   if (c->type == PT_LOGHALO && c->p[3] < 1) {
@@ -1479,6 +1579,10 @@ static double comp_hess(const ocomp *c, int which, double R, double Z, double ph
     return P.h[ia[which]][ib[which]];
   }
   if (c->type == PT_DEHNENBAR) return dbar_hess3(c, which, R, Z, phi);
+  if (c->type == PT_NEEDLEBAR) { /* R2, z2, Rz, phi2, Rphi, zphi -> its order */
+    static const int map[6] = {0, 1, 3, 2, 4, 5};
+    return needle_hess(c, map[which], R, Z, phi);
+  }
   if (c->type == PT_SCF) return scf_hess3(c, which, R, Z, phi);
   if (is_new_spherical(c->type)) return sph_hess3(c, which, R, Z);
   if (is_ellipsoidal(c->type)) return ell_cyl_hess(c, which, R, Z, phi);
@@ -1615,6 +1719,7 @@ static double comp_planarRforce(const ocomp *c, double R, double phi)
   if (c->type == PT_SPIRALARMS) return -spiral_pot(c, R, 0., phi).g[0];
   if (is_disk_pert(c->type)) return disk_pert(c, 0, R, phi);
   if (c->type == PT_DEHNENBAR) return dbar_force2(c, 0, R, phi);
+  if (c->type == PT_NEEDLEBAR) return needle_force(c, 0, R, 0., phi);
   if (c->type == PT_SCF) return scf_force3(c, 0, R, 0.0, phi); /* SCFPotentialPlanarRforce */
   if (is_new_spherical(c->type)) return sph_planarRforce(c, R);
   if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 0, R, 0., phi);
@@ -1668,6 +1773,7 @@ static double comp_planarphitorque(const ocomp *c, double R, double phi)
   if (c->type == PT_SPIRALARMS) return -spiral_pot(c, R, 0., phi).g[2];
   if (is_disk_pert(c->type)) return disk_pert(c, 1, R, phi);
   if (c->type == PT_DEHNENBAR) return dbar_force2(c, 2, R, phi);
+  if (c->type == PT_NEEDLEBAR) return needle_force(c, 2, R, 0., phi);
   if (c->type == PT_SCF) return scf_force3(c, 2, R, 0.0, phi);
   if (is_ellipsoidal(c->type)) return ell_cyl_force(c, 2, R, 0., phi);
   if (c->type == PT_HENONHEILES) /* HenonHeilesPotentialphitorque */
@@ -1688,6 +1794,7 @@ static double comp_planarhess(const ocomp *c, int which, double R, double phi)
   }
   if (is_disk_pert(c->type)) return disk_pert(c, 2 + which, R, phi);
   if (c->type == PT_DEHNENBAR) return dbar_hess2(c, which, R, phi);
+  if (c->type == PT_NEEDLEBAR) return needle_hess(c, which == 0 ? 0 : which == 1 ? 2 : 4, R, 0., phi);
   if (c->type == PT_SCF) return scf_hess2(c, which, R, phi);
   if (is_new_spherical(c->type)) return which ? 0. : sph_planarR2deriv(c, R);
   if (is_ellipsoidal(c->type)) /* EllipsoidalPotentialPlanarR2deriv / phi2 / Rphi */
@@ -1763,6 +1870,7 @@ static double comp_eval(const ocomp *c, double R, double Z, double phi)
   if (c->type == PT_SPIRALARMS) return spiral_pot(c, R, Z, phi).v;
   if (c->type == PT_SCF) return scf_eval(c, R, Z, phi);
   if (c->type == PT_DEHNENBAR) return NAN; /* no C evaluation in the reference */
+  if (c->type == PT_NEEDLEBAR) return needle_eval(c, R, Z, phi);
   if (is_new_spherical(c->type)) return sph_eval(c, R, Z);
   if (is_ellipsoidal(c->type)) return ell_eval(c, R, Z, phi);
   double amp = c->p[0];

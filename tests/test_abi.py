@@ -45,8 +45,8 @@ def test_compile_potential_host_only(golden):
     assert n == 3 and buf.size == 3 * _lib.lib().galpy_cuda_comp_size()
     rec = buf.reshape(3, -1)
     assert rec[:, :4].view(np.int32).ravel().tolist() == [15, 5, 9]
-    with pytest.raises(galpy_b200.PotentialNotSupported):  # SoftenedNeedleBarPotential
-        galpy_b200.compile_potential(([25], [1.0, 0, 0, 1, 1, 0, 0, 0]))
+    with pytest.raises(galpy_b200.PotentialNotSupported):  # TwoPowerSphericalPotential
+        galpy_b200.compile_potential(([42], [1.0, 1.0, 1.5, 3.5]))
 
 
 def test_scf_continuation_records():

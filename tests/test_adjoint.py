@@ -214,10 +214,10 @@ def test_adjoint_refuses_bar_and_scf():
         pt, pa = TP.potential(name, planar=True)
         with pytest.raises(_lib.PotentialNotSupported, match="time-dependent or SCF"):
             adjoint_params(pt, True, pa)
-    for planar in (False, True):  # rotating spiral arms
-        pt, pa = TP.spiral_arms("spiral+mw14", planar)
-        with pytest.raises(_lib.PotentialNotSupported, match="time-dependent or SCF"):
-            adjoint_params(pt, planar, pa)
+    for planar in (False, True):  # rotating spiral arms and needle bar
+        for pt, pa in (TP.spiral_arms("spiral+mw14", planar), TP.needle_bar("needle+mw14", planar)):
+            with pytest.raises(_lib.PotentialNotSupported, match="time-dependent or SCF"):
+                adjoint_params(pt, planar, pa)
     pt, pa = TP.planar_perturbation("lopsided+mw14")
     with pytest.raises(_lib.PotentialNotSupported, match="time-dependent or SCF"):
         adjoint_params(pt, True, pa)

@@ -62,10 +62,11 @@ def test_planar_orbit_routes(hooks):
 
 def test_unsupported_potential_falls_back(hooks):
     from galpy.orbit import Orbit
-    from galpy.potential import SoftenedNeedleBarPotential
+    from galpy.potential import TwoPowerSphericalPotential
 
     o = Orbit([1.0, 0.1, 1.1, 0.0, 0.1, 0.0])
-    o.integrate(np.linspace(0, 1, 11), SoftenedNeedleBarPotential(), method="dop853_cuda")
+    o.integrate(np.linspace(0, 1, 11), TwoPowerSphericalPotential(alpha=1.5, beta=3.5),
+                method="dop853_cuda")
     assert hooks == []  # galpy's own integrator ran
 
 
@@ -104,6 +105,16 @@ def test_spiral_arms_route(hooks):
     assert len(hooks) == 1
     o.integrate(np.linspace(0, 1, 11), SpiralArmsPotential(Cs=[1.0] * 7), method="dop853_cuda")
     assert len(hooks) == 1
+
+
+def test_needle_bar_routes(hooks):
+    from galpy.orbit import Orbit
+    from galpy.potential import MWPotential2014, SoftenedNeedleBarPotential
+
+    o = Orbit([1.0, 0.1, 1.1, 0.0, 0.1, 0.0])
+    bar = SoftenedNeedleBarPotential(amp=0.05, a=0.5, c=0.125, omegab=1.8)
+    o.integrate(np.linspace(0, 1, 11), [*MWPotential2014, bar], method="rk4_cuda")
+    assert len(hooks) == 1 and hooks[-1]["method"] == "rk4_cuda"
 
 
 def test_spherical_potential_routes(hooks):

@@ -340,3 +340,72 @@ def test_spiral_arms_device_forces_and_potential(oracle):
     gb.energy_device(torch.from_numpy(comps).to(dev), nrec, w, E)
     pv = oracle.potential(R, z, phi, pt, pa)
     assert np.abs(E.cpu().numpy() - pv).max() < 1e-13 * np.abs(pv).max()
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", TP.NEEDLE_BARS)
+def test_needle_bar_orbits_vs_oracle(oracle, name, planar, method):
+    """A rotating softened needle bar (galpy's default shape, and a thick
+    one) over MWPotential2014: a smooth potential, every orbit takes the
+    oracle's steps."""
+    pt, pa = TP.needle_bar(name, planar)
+    y0 = ics(128, planar, 61 + TP.NEEDLE_BARS.index(name))
+    t = np.linspace(0.0, 10.0, 41)
+    with oracle.phi_from_atan2():
+        ref, eref, nref, _ = oracle.integrate(y0, t, pt, pa, method, planar=planar,
+                                              **tol(method))
+    fn = gb.integratePlanarOrbit_cuda if planar else gb.integrateFullOrbit_cuda
+    out, err, ns = fn((pt, pa), y0.copy(), t, method + "_cuda", progressbar=False,
+                      return_nsteps=True, **tol(method))
+    assert not err.any() and not eref.any()
+    d = cyl_diff(ref, out).max(axis=(1, 2))
+    same = ns == nref
+    assert same.mean() >= 0.98, same.mean()
+    far = same & (d > 1e-10)
+    if far.any():
+        with oracle.phi_from_atan2():
+            resp = np.maximum(*[TP.ulp_response(oracle, y0[far], t, pt, pa, method, planar,
+                                                ref[far], seed=sd, **tol(method))
+                                for sd in (3, 4)])
+        assert (d[far] <= 30 * resp).all(), (d[far], resp)
+    assert (d[~same] < 1e-6).all(), d[~same]
+
+
+@pytest.mark.parametrize("planar", [False, True])
+def test_needle_bar_variational(oracle, planar):
+    pt, pa = TP.needle_bar("needle_thick+mw14", planar)
+    dim = 2 if planar else 3
+    w = unit_deviations(cyl_to_rect(ics(6, planar, 5)), dim)
+    t = np.linspace(0.0, 4.0, 17)
+    for method in ("rk4", "symplec4"):
+        with oracle.phi_from_atan2():
+            ref, eref, nref = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar)
+        out, err, ns = gb.integrate_dxdv_batch((pt, pa), w, t, method + "_cuda",
+                                               planar=planar, return_nsteps=True)
+        assert np.array_equal(err, eref) and np.array_equal(ns, nref)
+        rel = (np.abs(out - ref) / np.abs(ref).max(axis=1, keepdims=True)).max()
+        assert rel < 1e-9, (method, rel)
+
+
+def test_needle_bar_device_forces_and_potential(oracle):
+    import torch
+
+    rng = np.random.default_rng(9)
+    R, z, phi = rng.uniform(0.2, 2.0, 500), rng.normal(0, 0.4, 500), rng.uniform(0, 6.28, 500)
+    pt, pa = TP.needle_bar("needle_thick+mw14")
+    comps, nrec = gb.compile_potential((pt, pa))
+    dev = torch.device("cuda", 0)
+    pos = torch.tensor(np.stack([R * np.cos(phi), R * np.sin(phi), z]), device=dev)
+    acc = torch.empty_like(pos)
+    gb.accel_device(torch.from_numpy(comps).to(dev), nrec, pos, acc)
+    f = oracle.forces(R, z, phi, pt, pa)
+    ref = np.stack([np.cos(phi) * f[:, 0] - np.sin(phi) * f[:, 2] / R,
+                    np.sin(phi) * f[:, 0] + np.cos(phi) * f[:, 2] / R, f[:, 1]])
+    assert np.abs(acc.cpu().numpy() - ref).max() < 1e-13 * np.abs(ref).max()
+    w = torch.zeros((6, R.size), dtype=torch.float64, device=dev)
+    w[:3] = pos
+    E = torch.empty(R.size, dtype=torch.float64, device=dev)
+    gb.energy_device(torch.from_numpy(comps).to(dev), nrec, w, E)
+    pv = oracle.potential(R, z, phi, pt, pa)
+    assert np.abs(E.cpu().numpy() - pv).max() < 1e-13 * np.abs(pv).max()

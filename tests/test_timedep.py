@@ -599,3 +599,127 @@ def test_spiral_arms_term_limit():
     a = TP.spiral_arms_args(Cs=[1.0] * 7)
     with pytest.raises(gb.PotentialNotSupported):
         gb.compile_potential((np.array(mt + [27], np.int32), np.array(ma + a)))
+
+
+# ---- SoftenedNeedleBarPotential: a rotating softened needle ------------------
+@pytest.mark.parametrize("planar", [False, True])
+def test_needle_bar_layout_and_forces_vs_galpy_python(planar):
+    """galpy's argument layout, and the oracle's forces and second
+    derivatives against galpy's Python SoftenedNeedleBarPotential, at two
+    times."""
+    P = galpy_or_skip()
+    pot = P.SoftenedNeedleBarPotential(amp=0.08, a=0.4, b=0.1, c=0.2, pa=-0.3, omegab=1.5)
+    if planar:
+        from galpy.orbit.integratePlanarOrbit import _parse_pot
+        gp = P.toPlanarPotential(pot)
+    else:
+        from galpy.orbit.integrateFullOrbit import _parse_pot
+        gp = pot
+    _, pt, pa, _ = _parse_pot([gp])
+    assert list(pt) == [25]
+    _, ref_a = TP.needle_bar("needle_thick+mw14", planar)
+    np.testing.assert_allclose(pa, ref_a[-len(pa):], rtol=1e-15, atol=0)
+    rng = np.random.default_rng(8)
+    R, phi = rng.uniform(0.2, 2.0, 50), rng.uniform(0, 2 * np.pi, 50)
+    z = np.zeros(50) if planar else rng.normal(0, 0.3, 50)
+    names = (["Rforce", "phitorque", "R2deriv", "phi2deriv", "Rphideriv"] if planar else
+             ["Rforce", "zforce", "phitorque", "R2deriv", "z2deriv", "Rzderiv", "phi2deriv",
+              "Rphideriv", "phizderiv"])
+    for t in (0.0, 1.3):
+        got = oracle.forces(R, z, phi, np.array([25], np.int32), np.asarray(pa), planar=planar,
+                            t=t)
+        for k, nm in enumerate(names):
+            ref = np.array([getattr(gp, nm)(R[i], *([] if planar else [z[i]]), phi=phi[i], t=t,
+                                            use_physical=False) for i in range(R.size)])
+            assert np.abs(got[:, k] - ref).max() <= 1e-12 * np.abs(ref).max(), (nm, t)
+    if not planar:
+        pv = oracle.potential(R, z, phi, np.array([25], np.int32), np.asarray(pa))
+        ref = np.array([pot(R[i], z[i], phi=phi[i], use_physical=False) for i in range(50)])
+        assert np.abs(pv - ref).max() <= 1e-14 * np.abs(ref).max()
+
+
+@needs_ref
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", TP.NEEDLE_BARS)
+@pytest.mark.parametrize("method", METHODS)
+def test_needle_orbits_bit_exact_vs_reference_build(name, planar, method):
+    pt, pa = TP.needle_bar(name, planar)
+    yo = ics(8, planar)
+    t = np.linspace(0.0, 8.0, 41)
+    a, ea, _, _ = oracle.integrate(yo, t, pt, pa, method, planar=planar, **tol(method))
+    b, eb, _, _ = oracle.integrate(yo, t, pt, pa, method, planar=planar, impl="ref",
+                                   **tol(method))
+    np.testing.assert_array_equal(ea, eb)
+    np.testing.assert_array_equal(a, b)
+
+
+@needs_ref
+@pytest.mark.parametrize("planar", [False, True])
+def test_needle_dxdv_bit_exact_vs_reference_build(planar):
+    pt, pa = TP.needle_bar("needle_thick+mw14", planar)
+    dim = 2 if planar else 3
+    rng = np.random.default_rng(5)
+    w = np.concatenate([rng.uniform(0.6, 1.2, (4, dim)), rng.normal(0, 0.2, (4, dim)),
+                        rng.normal(0, 1, (4, 2 * dim))], 1)
+    w[:, dim + 1] += 1.0
+    t = np.linspace(0.0, 4.0, 17)
+    for method in ("rk4", "symplec4", "dop853"):
+        a = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar, **tol(method))[0]
+        b = oracle.integrate_dxdv(w, t, pt, pa, method, planar=planar, impl="ref",
+                                  **tol(method))[0]
+        np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("planar", [False, True])
+@pytest.mark.parametrize("name", TP.NEEDLE_BARS)
+def test_engine_needle_forces_and_tidal(harness, name, planar):
+    """The engine's needle bar (bar-frame Cartesian gradient and Hessian in
+    cancellation-free forms, rotated back) against the oracle."""
+    pt, pa = TP.needle_bar(name, planar)
+    rng = np.random.default_rng(18)
+    R = rng.uniform(0.2, 2.0, 120)
+    z = np.zeros(120) if planar else rng.normal(0, 0.4, 120)
+    phi = rng.uniform(0, 2 * np.pi, 120)
+    for t in (0.0, 2.5, 7.0):
+        f = oracle.forces(R, z, phi, pt, pa, planar=planar, t=t)
+        tq = f[:, 1] if planar else f[:, 2]
+        ax = np.cos(phi) * f[:, 0] - np.sin(phi) * tq / R
+        ay = np.sin(phi) * f[:, 0] + np.cos(phi) * tq / R
+        acc, K, _ = harness.forces(R * np.cos(phi), R * np.sin(phi), z, pt, pa, planar=planar,
+                                   t=t)
+        ref = np.stack([ax, ay] + ([] if planar else [f[:, 1]]), 1)
+        assert np.abs(acc[:, :ref.shape[1]] - ref).max() < 1e-14 * np.abs(ref).max(), t
+        Kref = cyl_to_K(f, R, phi, planar)
+        assert np.abs(K[:, :Kref.shape[1]] - Kref).max() < 1e-12 * np.abs(Kref).max(), t
+
+
+@pytest.mark.parametrize("method", ["leapfrog", "symplec4", "rk4", "dopr54", "dop853"])
+@pytest.mark.parametrize("planar", [False, True])
+def test_engine_needle_machines_vs_oracle(harness, planar, method):
+    pt, pa = TP.needle_bar("needle_thick+mw14", planar)
+    y0 = ics(24, planar, seed=37)
+    t = np.linspace(0.0, 10.0, 41)
+    with oracle.phi_from_atan2():
+        ref, _, nref, _ = oracle.integrate(y0, t, pt, pa, method, planar=planar, **tol(method))
+    out, err, ns = harness.integrate(c2r(y0, planar), t, pt, pa, method, planar=planar,
+                                     **tol(method))
+    assert not err.any()
+    ref_r = np.stack([c2r(ref[:, j], planar) for j in range(len(t))], 1)
+    d = np.abs(out - ref_r).reshape(len(y0), -1).max(1)
+    same = ns == nref
+    assert same.mean() > 0.9
+    assert np.median(d[same]) < 1e-12 and d[same].max() < 1e-9, d[same].max()
+    assert (d < 1e-6).all()
+
+
+def test_needle_bar_arguments_checked():
+    """A needle of zero length is refused; an unsoftened one (b = c = 0,
+    singular on the needle only, as in the reference) compiles."""
+    import galpy_b200 as gb
+    from galpy_b200 import _lib
+
+    mt, ma = TP.mw14()
+    pt = np.array(mt + [25], np.int32)
+    with pytest.raises(_lib.CudaError, match="invalid potential arguments"):
+        gb.compile_potential((pt, np.array(ma + TP.needle_bar_args(a=0.0))))
+    gb.compile_potential((pt, np.array(ma + TP.needle_bar_args(b=0.0, c=0.0))))

@@ -172,3 +172,25 @@ def spiral_arms(name, planar=False):
 
 
 SPIRAL_ARMS = ["spiral+mw14", "spiral3+mw14"]
+
+
+def needle_bar_args(amp=0.05, a=0.5, b=0.0, c=0.125, pa=0.4, omegab=1.8):
+    """SoftenedNeedleBarPotential's argument list (amp, a, b, c^2, pa,
+    omegab, and seven cache slots galpy passes as zeros)."""
+    return [amp, a, b, c * c, pa, omegab] + [0.0] * 7
+
+
+def needle_bar(name, planar=False):
+    """(pot_type, pot_args) of MWPotential2014 plus a rotating softened
+    needle bar (type 25): galpy's default shape, or a thick bar (b > 0)."""
+    mw_t, mw_a = mw14(planar)
+    if name == "needle+mw14":
+        a = needle_bar_args()
+    elif name == "needle_thick+mw14":
+        a = needle_bar_args(amp=0.08, a=0.4, b=0.1, c=0.2, pa=-0.3, omegab=1.5)
+    else:
+        raise KeyError(name)
+    return np.asarray(mw_t + [25], np.int32), np.asarray(mw_a + a, np.float64)
+
+
+NEEDLE_BARS = ["needle+mw14", "needle_thick+mw14"]
