@@ -279,6 +279,8 @@ inline int compile_entries(int planar, int n, const int*& tp, const double*& p, 
         c.c[4] = p[2] > p[1] ? 1.0 / (p[2] - p[1]) : 0.0;
       } else if (type == T_WRAP_GAUSS && !(p[2] > 0.0)) {  // (amp, to, sigma^2)
         return -1;
+      } else if (type == T_WRAP_KUZMIN && !(p[1] >= 0.0 && p[2] >= 0.0)) {  // (amp, a, b^2)
+        return -1;
       }
       c.c[15] = rec - w - 1;
       p += wrapper_nargs(type);

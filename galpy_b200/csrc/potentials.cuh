@@ -972,7 +972,8 @@ GPC_HD GPC_FI void comp_accel(const GpComp* __restrict__ cp, const S& sc, T x, T
 // accumulators are set aside, the wrapped components are evaluated at the
 // point rotated by -alpha, and at the frame's end their acceleration,
 // rotated back by alpha and scaled by the wrapper's factor, joins a0 (R^2
-// and r^2 do not change under the rotation about z).
+// and r^2 do not change under the rotation about z).  A KuzminLike frame
+// evaluates them at (xi, 0, 0) instead and adds fac a_x' grad xi.
 struct DynPot {
   static constexpr bool kDirectScalars = false;
   static constexpr bool kAdditive = true;  // a component may add to a0
@@ -983,21 +984,32 @@ struct DynPot {
                                 AddAcc<T>& a0, double t)
   {
     int wend = -1;  // one past the open frame's last record
-    T xw = x, yw = y, sR = T(0), sz = T(0), syx = T(0);
+    T xw = x, yw = y, zw = z, z2w = z2, R2w = R2, r2w = r2, sR = T(0), sz = T(0), syx = T(0);
     AddAcc<T> sa{T(0), T(0), T(0)};
-    WrapFrame fr{1.0, 1.0, 0.0};
+    WrapFrame fr{1.0, 1.0, 0.0, false, 0.0, 0.0, 0.0};
     for (int k = 0; k <= ncomp; k++) {
       if (k == wend) {  // close the frame
         const T fc = T(fr.c), fs = T(fr.s), ff = T(fr.fac);
-        const T axw = xw * gR + a0.x, ayw = yw * (gR + gyx) + a0.y, azw = z * gz + a0.z;
+        const T axw = xw * gR + a0.x, ayw = yw * (gR + gyx) + a0.y, azw = zw * gz + a0.z;
         gR = sR;
         gz = sz;
         gyx = syx;
-        a0.x = sa.x + ff * (fc * axw - fs * ayw);
-        a0.y = sa.y + ff * (fs * axw + fc * ayw);
-        if (!PLANAR) a0.z = sa.z + ff * azw;
+        if (fr.kz) {  // fac dPhi/dxi grad xi, the wrapped force taken along x'
+          const T g = ff * axw / T(fr.xi);
+          a0.x = sa.x + g * x;
+          a0.y = sa.y + g * y;
+          if (!PLANAR) a0.z = sa.z + g * T(fr.q);
+        } else {
+          a0.x = sa.x + ff * (fc * axw - fs * ayw);
+          a0.y = sa.y + ff * (fs * axw + fc * ayw);
+          if (!PLANAR) a0.z = sa.z + ff * azw;
+        }
         xw = x;
         yw = y;
+        zw = z;
+        z2w = z2;
+        R2w = R2;
+        r2w = r2;
         wend = -1;
       }
       if (k == ncomp) break;
@@ -1011,12 +1023,19 @@ struct DynPot {
         sa = a0;
         gR = gz = gyx = T(0);
         a0 = AddAcc<T>{T(0), T(0), T(0)};
-        xw = T(fr.c) * x + T(fr.s) * y;
-        yw = T(fr.c) * y - T(fr.s) * x;
+        if (fr.kz) {
+          kuzmin_map<PLANAR>(comp + k, (double)R2, (double)z, fr);
+          xw = T(fr.xi);
+          yw = zw = z2w = T(0);
+          R2w = r2w = xw * xw;
+        } else {
+          xw = T(fr.c) * x + T(fr.s) * y;
+          yw = T(fr.c) * y - T(fr.s) * x;
+        }
         continue;
       }
-      comp_accel<T, PLANAR, kRunTimeAll>(comp + k, ScalarsGlobal{comp + k}, xw, yw, z, z2, R2,
-                                         r2, gR, gz, gyx, a0, t);
+      comp_accel<T, PLANAR, kRunTimeAll>(comp + k, ScalarsGlobal{comp + k}, xw, yw, zw, z2w, R2w,
+                                         r2w, gR, gz, gyx, a0, t);
     }
   }
 };
@@ -1450,27 +1469,49 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
   // wrapper frames as in DynPot::sum; K of the wrapped records, taken in the
   // rotated frame, returns as fac R(alpha) K' R(alpha)^T
   int wend = -1;
-  double xw = x, yw = y, sR = 0.0, sz = 0.0, syx = 0.0, sx0 = 0.0, sy0 = 0.0, sz0 = 0.0, sK[6];
-  WrapFrame fr{1.0, 1.0, 0.0};
+  double xw = x, yw = y, zw = z, z2w = z2, R2w = R2, r2w = r2;
+  double sR = 0.0, sz = 0.0, syx = 0.0, sx0 = 0.0, sy0 = 0.0, sz0 = 0.0, sK[6];
+  WrapFrame fr{1.0, 1.0, 0.0, false, 0.0, 0.0, 0.0};
   for (int k = 0; k <= ncomp; k++) {
     if (k == wend) {
       const double c = fr.c, s = fr.s, f = fr.fac;
-      const double axw = xw * gR + ax0, ayw = yw * (gR + gyx) + ay0, azw = z * gz + az0;
+      const double axw = xw * gR + ax0, ayw = yw * (gR + gyx) + ay0, azw = zw * gz + az0;
       gR = sR;
       gz = sz;
       gyx = syx;
-      ax0 = sx0 + f * (c * axw - s * ayw);
-      ay0 = sy0 + f * (s * axw + c * ayw);
-      az0 = sz0 + (PLANAR ? 0.0 : f * azw);
-      const double kxx = K[0], kxy = K[1], kyy = K[2], kxz = K[3], kyz = K[4], kzz = K[5];
-      K[0] = sK[0] + f * (c * c * kxx - 2.0 * c * s * kxy + s * s * kyy);
-      K[1] = sK[1] + f * (c * s * (kxx - kyy) + (c * c - s * s) * kxy);
-      K[2] = sK[2] + f * (s * s * kxx + 2.0 * c * s * kxy + c * c * kyy);
-      K[3] = sK[3] + f * (c * kxz - s * kyz);
-      K[4] = sK[4] + f * (s * kxz + c * kyz);
-      K[5] = sK[5] + f * kzz;
+      if (fr.kz) {
+        // Phi = fac f(xi): -Hessian = fac (K'_xx g g^T + a'_x grad grad xi),
+        // g = grad xi = (x, y, q) / xi, grad grad xi = (I' - g g^T) / xi with
+        // I' = diag(1, 1, dq)
+        const double ix = 1.0 / fr.xi, gx = x * ix, gy = y * ix, gz3 = fr.q * ix;
+        const double kp = K[0], ap = axw * ix;
+        ax0 = sx0 + f * axw * gx;
+        ay0 = sy0 + f * axw * gy;
+        az0 = sz0 + (PLANAR ? 0.0 : f * axw * gz3);
+        K[0] = sK[0] + f * ((kp - ap) * gx * gx + ap);
+        K[1] = sK[1] + f * (kp - ap) * gx * gy;
+        K[2] = sK[2] + f * ((kp - ap) * gy * gy + ap);
+        K[3] = sK[3] + f * (kp - ap) * gx * gz3;
+        K[4] = sK[4] + f * (kp - ap) * gy * gz3;
+        K[5] = sK[5] + f * ((kp - ap) * gz3 * gz3 + ap * fr.dq);
+      } else {
+        ax0 = sx0 + f * (c * axw - s * ayw);
+        ay0 = sy0 + f * (s * axw + c * ayw);
+        az0 = sz0 + (PLANAR ? 0.0 : f * azw);
+        const double kxx = K[0], kxy = K[1], kyy = K[2], kxz = K[3], kyz = K[4], kzz = K[5];
+        K[0] = sK[0] + f * (c * c * kxx - 2.0 * c * s * kxy + s * s * kyy);
+        K[1] = sK[1] + f * (c * s * (kxx - kyy) + (c * c - s * s) * kxy);
+        K[2] = sK[2] + f * (s * s * kxx + 2.0 * c * s * kxy + c * c * kyy);
+        K[3] = sK[3] + f * (c * kxz - s * kyz);
+        K[4] = sK[4] + f * (s * kxz + c * kyz);
+        K[5] = sK[5] + f * kzz;
+      }
       xw = x;
       yw = y;
+      zw = z;
+      z2w = z2;
+      R2w = R2;
+      r2w = r2;
       wend = -1;
     }
     if (k == ncomp) break;
@@ -1491,11 +1532,18 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
         K[i] = 0.0;
       }
       gR = gz = gyx = ax0 = ay0 = az0 = 0.0;
-      xw = fr.c * x + fr.s * y;
-      yw = fr.c * y - fr.s * x;
+      if (fr.kz) {
+        kuzmin_map<PLANAR>(cp, R2, z, fr);
+        xw = fr.xi;
+        yw = zw = z2w = 0.0;
+        R2w = r2w = xw * xw;
+      } else {
+        xw = fr.c * x + fr.s * y;
+        yw = fr.c * y - fr.s * x;
+      }
       continue;
     }
-    comp_tidal<PLANAR>(cp, type, xw, yw, z, R2, z2, r2, gR, gz, gyx, ax0, ay0, az0, K, t);
+    comp_tidal<PLANAR>(cp, type, xw, yw, zw, R2w, z2w, r2w, gR, gz, gyx, ax0, ay0, az0, K, t);
   }
   ax = x * gR + ax0;
   ay = y * (gR + gyx) + ay0;
@@ -1692,9 +1740,15 @@ GPC_HD inline double potential_value(const GpComp* __restrict__ comp, int ncomp,
     const int type = ldg(&cp->type);
     if (is_wrapper(type)) {
       const int nw = (int)ldg(&cp->c[15]);
-      const WrapFrame fr = wrap_frame(cp, type, 0.0);
+      WrapFrame fr = wrap_frame(cp, type, 0.0);
       double w = 0.0;
-      for (int j = 1; j <= nw; j++) w += comp_value(cp + j, x, y, z, R2, z2, r2);
+      if (fr.kz) {  // the wrapped list at (xi, 0, 0)
+        kuzmin_map<false>(cp, R2, z, fr);
+        const double xi2 = fr.xi * fr.xi;
+        for (int j = 1; j <= nw; j++) w += comp_value(cp + j, fr.xi, 0.0, 0.0, xi2, 0.0, xi2);
+      } else {
+        for (int j = 1; j <= nw; j++) w += comp_value(cp + j, x, y, z, R2, z2, r2);
+      }
       phi += type == T_WRAP_ROTATE ? NAN : fr.fac * w;
       k += nw;
       continue;

@@ -32,10 +32,12 @@ enum : int { T_DEHNENBAR = 1, T_SCF = 24 };
 // Wrappers (DehnenSmoothWrapperPotential.c, SolidBodyRotationWrapperPotential.c,
 // GaussianAmplitudeWrapperPotential.c): a wrapper record is followed by the
 // records of the components it wraps (c15 holds their count).
-enum : int { T_WRAP_SMOOTH = -1, T_WRAP_ROTATE = -2, T_WRAP_GAUSS = -5 };
+// KuzminLikeWrapperPotential.c: the wrapped list on the plane at
+// xi = sqrt(R^2 + (a + sqrt(z^2 + b^2))^2).
+enum : int { T_WRAP_SMOOTH = -1, T_WRAP_ROTATE = -2, T_WRAP_GAUSS = -5, T_WRAP_KUZMIN = -10 };
 GPC_HD GPC_FI constexpr bool is_wrapper(int t)
 {
-  return t == T_WRAP_SMOOTH || t == T_WRAP_ROTATE || t == T_WRAP_GAUSS;
+  return t == T_WRAP_SMOOTH || t == T_WRAP_ROTATE || t == T_WRAP_GAUSS || t == T_WRAP_KUZMIN;
 }
 // Planar-only disk perturbations: TransientLogSpiral, SteadyLogSpiral,
 // EllipticalDisk, LopsidedDisk, CosmphiDisk (potential_c_ext/<name>.c)
@@ -99,14 +101,22 @@ GPC_HD GPC_FI double dehnen_smooth(double t, double tform, double tsteady, doubl
 // SolidBodyRotation: amp, alpha = omega t + pa.
 // Records: c0 amp; smooth c1 tform, c2 tsteady, c3 grow, c4 1/(tsteady -
 // tform); Gaussian c1 to, c2 sigma^2; rotation c1 omega, c2 pa.
+// A wrapper's frame: its factor and, for the rotation, cos / sin of the
+// angle; for KuzminLike (kz) the point map x -> (xi, 0, 0) with
+// grad xi = (x, y, q) / xi, q = (a + zeta) z / zeta, zeta = sqrt(z^2 + b^2),
+// and dq = dq/dz = 1 + a b^2 / zeta^3 (for the tidal tensor).
 struct WrapFrame {
   double fac, c, s;
+  bool kz;
+  double xi, q, dq;
 };
 
 GPC_HD GPC_FI WrapFrame wrap_frame(const GpComp* __restrict__ cp, int type, double t)
 {
-  WrapFrame f{ldg(&cp->c[0]), 1.0, 0.0};
-  if (type == T_WRAP_SMOOTH) {
+  WrapFrame f{ldg(&cp->c[0]), 1.0, 0.0, false, 0.0, 0.0, 0.0};
+  if (type == T_WRAP_KUZMIN) {
+    f.kz = true;
+  } else if (type == T_WRAP_SMOOTH) {
     const double sm = dehnen_smooth(t, ldg(&cp->c[1]), ldg(&cp->c[2]), ldg(&cp->c[4]));
     f.fac *= ldg(&cp->c[3]) != 0.0 ? sm : 1.0 - sm;
   } else if (type == T_WRAP_GAUSS) {
@@ -116,6 +126,17 @@ GPC_HD GPC_FI WrapFrame wrap_frame(const GpComp* __restrict__ cp, int type, doub
     sincos(ldg(&cp->c[1]) * t + ldg(&cp->c[2]), &f.s, &f.c);
   }
   return f;
+}
+
+// The KuzminLike point map at (R^2, z) (z = 0 in the plane).
+template <bool PLANAR>
+GPC_HD GPC_FI void kuzmin_map(const GpComp* __restrict__ cp, double R2, double z, WrapFrame& f)
+{
+  const double a = ldg(&cp->c[1]), b2 = ldg(&cp->c[2]);
+  const double zeta = sqrt((PLANAR ? 0.0 : z * z) + b2), A = a + zeta;
+  f.xi = sqrt(R2 + A * A);
+  f.q = PLANAR ? 0.0 : A * z / zeta;
+  f.dq = 1.0 + a * b2 / (zeta * zeta * zeta);
 }
 
 struct BarParts {

@@ -109,6 +109,9 @@ enum { PT_SCF = 24 };
    components' types; args (nwrapped, the wrapped components' args, then
    (amp, tform, tsteady, grow), (amp, omega, pa) or (amp, to, sigma^2)) */
 enum { PT_WRAP_SMOOTH = -1, PT_WRAP_ROTATE = -2, PT_WRAP_GAUSS = -5 };
+/* KuzminLikeWrapperPotential.c: the wrapped potential at xi(R, z) =
+   sqrt(R^2 + (a + sqrt(z^2 + b^2))^2) on the plane, args (amp, a, b^2) */
+enum { PT_WRAP_KUZMIN = -10 };
 /* planar-only disk perturbations: TransientLogSpiral (2; amp, A, to,
    sigma^2, alpha, m, omegas, gamma), SteadyLogSpiral (3; amp, tform,
    tsteady, A, alpha, m, omegas, gamma; tform NaN: no growth), EllipticalDisk
@@ -585,7 +588,8 @@ static double sph_eval(const ocomp *c, double R, double Z)
    Returns 0, or -1 for an unsupported type. */
 static int is_wrapper(int type)
 {
-  return type == PT_WRAP_SMOOTH || type == PT_WRAP_ROTATE || type == PT_WRAP_GAUSS;
+  return type == PT_WRAP_SMOOTH || type == PT_WRAP_ROTATE || type == PT_WRAP_GAUSS ||
+         type == PT_WRAP_KUZMIN;
 }
 
 /* n entries of the (type, args) streams into P->c from *idx on; a wrapper
@@ -1941,6 +1945,51 @@ static double comp_quantity(ocomp *c, int q, double R, double z, double phi)
   }
 }
 
+/* xi and its derivatives, in the reference's forms
+   (KuzminLikeWrapperPotential.c:5-40): d[0] xi, d[1] dxi/dR, d[2] dxi/dz,
+   d[3] d2xi/dR2, d[4] d2xi/dz2, d[5] d2xi/dRdz */
+static void kuzmin_xi(double R, double z, double a, double b2, double *d)
+{
+  double sbz = sqrt(z * z + b2), asbz = a + sbz;
+  d[0] = sqrt(R * R + asbz * asbz);
+  d[1] = R / sqrt(R * R + asbz * asbz);
+  d[2] = asbz * z / sqrt(R * R + asbz * asbz) / sbz;
+  d[3] = asbz * asbz / pow(R * R + asbz * asbz, 1.5);
+  d[4] = (a * a * a * b2 + 3. * a * a * b2 * sbz + a * b2 * (3. * b2 + R * R + 3. * z * z) +
+          (b2 + R * R) * pow(sbz, 3.0)) / pow(sbz, 3.0) / pow(d[0], 3.0);
+  d[5] = -R * z * asbz / sbz / pow(R * R + asbz * asbz, 1.5);
+}
+
+static double range_sum(opot *P, int i0, int i1, int q, double R, double z, double phi);
+
+/* a KuzminLike wrapper's contribution to quantity q: the chain rule of the
+   wrapped list's in-plane radial force and second derivative at (xi, 0, 0)
+   (the wrapper is axisymmetric: its torque and phi derivatives are 0) */
+static double kuzmin_quantity(opot *P, const ocomp *c, int i, int q, double R, double z)
+{
+  const double amp = c->p[0], a = c->p[1], b2 = c->p[2];
+  const int j0 = i + 1, j1 = i + 1 + c->nsub;
+  const int planar = q == Q_PRF || q == Q_PPT || q == Q_PH0 || q == Q_PH1 || q == Q_PH2;
+  double d[6];
+  kuzmin_xi(R, planar ? 0.0 : z, a, b2, d);
+  const int qf = planar ? Q_PRF : Q_RF;
+  switch (q) {
+  case Q_RF: case Q_PRF: return amp * range_sum(P, j0, j1, qf, d[0], 0.0, 0.0) * d[1];
+  case Q_ZF: return amp * range_sum(P, j0, j1, Q_RF, d[0], 0.0, 0.0) * d[2];
+  case Q_H0: case Q_PH0:
+    return amp * (range_sum(P, j0, j1, planar ? Q_PH0 : Q_H0, d[0], 0.0, 0.0) * d[1] * d[1] -
+                  range_sum(P, j0, j1, qf, d[0], 0.0, 0.0) * d[3]);
+  case Q_H1:
+    return amp * (range_sum(P, j0, j1, Q_H0, d[0], 0.0, 0.0) * d[2] * d[2] -
+                  range_sum(P, j0, j1, Q_RF, d[0], 0.0, 0.0) * d[4]);
+  case Q_H2:
+    return amp * (range_sum(P, j0, j1, Q_H0, d[0], 0.0, 0.0) * d[1] * d[2] -
+                  range_sum(P, j0, j1, Q_RF, d[0], 0.0, 0.0) * d[5]);
+  case Q_EVAL: return amp * range_sum(P, j0, j1, Q_EVAL, d[0], 0.0, 0.0);
+  default: return 0.0;
+  }
+}
+
 /* sum of quantity q over entries [i0, i1), in order; a wrapper contributes
    its factor times the sum over its entries (at phi - omega t - pa for the
    rotation wrapper): DehnenSmooth amp s(t) (1 - s(t) if not growing),
@@ -1953,6 +2002,11 @@ static double range_sum(opot *P, int i0, int i1, int q, double R, double z, doub
     ocomp *c = &P->c[i];
     if (!is_wrapper(c->type)) {
       sum += comp_quantity(c, q, R, z, phi);
+      continue;
+    }
+    if (c->type == PT_WRAP_KUZMIN) {
+      sum += kuzmin_quantity(P, c, i, q, R, z);
+      i += c->nsub;
       continue;
     }
     const double *a = c->p, t = c->t;

@@ -147,6 +147,11 @@ def test_wrappers_route(hooks):
     nested = DehnenSmoothWrapperPotential(pot=halo, tform=0.5, tsteady=2.0)
     o.integrate(ts, [*MWPotential2014, nested], method="rk4_cuda")
     assert len(hooks) == 2
+    from galpy.potential import KuzminLikeWrapperPotential, PlummerPotential
+
+    disk = KuzminLikeWrapperPotential(pot=PlummerPotential(amp=0.5, b=0.4), a=0.3, b=0.1)
+    o.integrate(ts, [*MWPotential2014, disk], method="dopr54_cuda")
+    assert len(hooks) == 3
 
 
 def test_unknown_method_still_rejected(hooks):

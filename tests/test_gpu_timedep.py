@@ -207,7 +207,8 @@ def test_wrapped_orbits_vs_oracle(oracle, name, planar, method):
 
 
 @pytest.mark.parametrize("planar", [False, True])
-@pytest.mark.parametrize("name", ["smooth(bar)+mw14", "rotate(loghalo)+mw14"])
+@pytest.mark.parametrize("name", ["smooth(bar)+mw14", "rotate(loghalo)+mw14",
+                                  "kuzmin(plummer)+mw14"])
 def test_wrapped_variational(oracle, name, planar):
     pt, pa, npot = TP.wrapped(name, planar)
     dim = 2 if planar else 3
@@ -408,4 +409,28 @@ def test_needle_bar_device_forces_and_potential(oracle):
     E = torch.empty(R.size, dtype=torch.float64, device=dev)
     gb.energy_device(torch.from_numpy(comps).to(dev), nrec, w, E)
     pv = oracle.potential(R, z, phi, pt, pa)
+    assert np.abs(E.cpu().numpy() - pv).max() < 1e-13 * np.abs(pv).max()
+
+
+def test_kuzmin_like_device_forces_and_potential(oracle):
+    """KuzminLike frames on the device: accelerations and potential values
+    (the wrapped list at (xi, 0, 0)) against the oracle."""
+    import torch
+
+    rng = np.random.default_rng(12)
+    R, z, phi = rng.uniform(0.1, 2.0, 500), rng.normal(0, 0.4, 500), rng.uniform(0, 6.28, 500)
+    pt, pa, npot = TP.wrapped("kuzmin(hernquist,plummer)")
+    comps, nrec = gb.compile_potential((pt, pa, npot))
+    dev = torch.device("cuda", 0)
+    pos = torch.tensor(np.stack([R * np.cos(phi), R * np.sin(phi), z]), device=dev)
+    acc = torch.empty_like(pos)
+    gb.accel_device(torch.from_numpy(comps).to(dev), nrec, pos, acc)
+    f = oracle.forces(R, z, phi, pt, pa, npot=npot)
+    ref = np.stack([np.cos(phi) * f[:, 0], np.sin(phi) * f[:, 0], f[:, 1]])
+    assert np.abs(acc.cpu().numpy() - ref).max() < 1e-13 * np.abs(ref).max()
+    w = torch.zeros((6, R.size), dtype=torch.float64, device=dev)
+    w[:3] = pos
+    E = torch.empty(R.size, dtype=torch.float64, device=dev)
+    gb.energy_device(torch.from_numpy(comps).to(dev), nrec, w, E)
+    pv = oracle.potential(R, z, phi, pt, pa, npot=npot)
     assert np.abs(E.cpu().numpy() - pv).max() < 1e-13 * np.abs(pv).max()

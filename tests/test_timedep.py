@@ -301,7 +301,8 @@ def test_wrapped_orbits_bit_exact_vs_reference_build(name, planar, method):
 
 @needs_ref
 @pytest.mark.parametrize("planar", [False, True])
-@pytest.mark.parametrize("name", ["smooth(bar)+mw14", "rotate(loghalo)+mw14"])
+@pytest.mark.parametrize("name", ["smooth(bar)+mw14", "rotate(loghalo)+mw14",
+                                  "kuzmin(plummer)+mw14"])
 def test_wrapped_dxdv_bit_exact_vs_reference_build(name, planar):
     pt, pa, npot = TP.wrapped(name, planar)
     dim = 2 if planar else 3
@@ -723,3 +724,37 @@ def test_needle_bar_arguments_checked():
     with pytest.raises(_lib.CudaError, match="invalid potential arguments"):
         gb.compile_potential((pt, np.array(ma + TP.needle_bar_args(a=0.0))))
     gb.compile_potential((pt, np.array(ma + TP.needle_bar_args(b=0.0, c=0.0))))
+
+
+@pytest.mark.parametrize("planar", [False, True])
+def test_kuzmin_like_layout_and_forces_vs_galpy_python(planar):
+    """galpy's layout of a KuzminLikeWrapperPotential around a Plummer
+    sphere, and the oracle's forces, second derivatives and potential
+    against galpy's Python wrapper."""
+    P = galpy_or_skip()
+    pot = P.KuzminLikeWrapperPotential(pot=P.PlummerPotential(amp=0.8, b=0.5), a=0.3,
+                                       b=np.sqrt(0.4))
+    if planar:
+        from galpy.orbit.integratePlanarOrbit import _parse_pot
+        gp = P.toPlanarPotential(pot)
+    else:
+        from galpy.orbit.integrateFullOrbit import _parse_pot
+        gp = pot
+    npot, pt, pa, _ = _parse_pot([gp])
+    assert npot == 1 and list(pt) == [-10, 17]
+    np.testing.assert_allclose(pa, [1, 0.8, 0.5, 1.0, 0.3, 0.4], rtol=1e-15)
+    rng = np.random.default_rng(10)
+    R, phi = rng.uniform(0.1, 2.0, 40), rng.uniform(0, 2 * np.pi, 40)
+    z = np.zeros(40) if planar else rng.normal(0, 0.4, 40)
+    names = (["Rforce", "phitorque", "R2deriv"] if planar else
+             ["Rforce", "zforce", "phitorque", "R2deriv", "z2deriv", "Rzderiv"])
+    cols = [0, 1, 2] if planar else [0, 1, 2, 3, 4, 5]
+    got = oracle.forces(R, z, phi, pt, np.asarray(pa), planar=planar, npot=1)
+    for k, nm in zip(cols, names):
+        ref = np.array([getattr(gp, nm)(R[i], *([] if planar else [z[i]]), phi=phi[i],
+                                        use_physical=False) for i in range(R.size)])
+        assert np.abs(got[:, k] - ref).max() <= 1e-13 * max(np.abs(ref).max(), 1e-300), nm
+    if not planar:
+        pv = oracle.potential(R, z, phi, pt, np.asarray(pa), npot=1)
+        ref = np.array([pot(R[i], z[i], phi=phi[i], use_physical=False) for i in range(40)])
+        assert np.abs(pv - ref).max() <= 1e-14 * np.abs(ref).max()

@@ -87,12 +87,18 @@ def wrapped(name, planar=False):
         t, a = [-2, 0], [1] + loghalo_triaxial_args() + [1.0, 0.6, 0.3]
     elif name == "gauss(loghalo)+mw14":  # a triaxial halo with a Gaussian amplitude in time
         t, a = [-5, 0], [1] + loghalo_triaxial_args() + [1.0, 3.0, 4.0]
+    elif name == "kuzmin(plummer)+mw14":  # KuzminLike: a flattened Plummer (amp, a, b^2)
+        t, a = [-10, 17], [1, 0.3, 0.4] + [0.8, 0.5, 0.05]
+    elif name == "kuzmin(hernquist,plummer)":  # two wrapped spheres, no other component
+        mw_t, mw_a = [], []
+        t, a = [-10, 8, 17], [2, 0.6, 0.7, 0.3, 0.2] + [1.2, 0.4, 0.01]
     else:
         raise KeyError(name)
     return (np.asarray(mw_t + t, np.int32), np.asarray(mw_a + a, np.float64), len(mw_t) + 1)
 
 
-WRAPPED = ["smooth(bar)+mw14", "decay(bar)+mw14", "rotate(loghalo)+mw14", "gauss(loghalo)+mw14"]
+WRAPPED = ["smooth(bar)+mw14", "decay(bar)+mw14", "rotate(loghalo)+mw14", "gauss(loghalo)+mw14",
+           "kuzmin(plummer)+mw14", "kuzmin(hernquist,plummer)"]
 
 
 def crosses_bar_radius(ref_cyl, rb=0.8):
