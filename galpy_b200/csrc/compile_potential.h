@@ -213,7 +213,10 @@ inline int comp_records(int type, const double* p)
 }
 
 // Arguments of a wrapper after its wrapped entries.
-inline int wrapper_nargs(int type) { return type == T_WRAP_SMOOTH ? 4 : 3; }
+inline int wrapper_nargs(int type)
+{
+  return type == T_WRAP_SMOOTH ? 4 : type == T_WRAP_COROT ? 5 : 3;
+}
 
 // Records of n entries of galpy's (type, args) streams, advancing both; a
 // wrapper (one level deep) is its record plus its wrapped entries' records.
@@ -273,6 +276,10 @@ inline int compile_entries(int planar, int n, const int*& tp, const double*& p, 
       c.c[0] = p[0];
       c.c[1] = p[1];
       c.c[2] = p[2];
+      if (type == T_WRAP_COROT) {  // (amp, vpo, beta, pa, to)
+        c.c[3] = p[3];
+        c.c[4] = p[4];
+      }
       if (type == T_WRAP_SMOOTH) {  // (amp, tform, tsteady, grow)
         if (p[2] < p[1]) return -1;
         c.c[3] = p[3];

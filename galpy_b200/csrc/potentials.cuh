@@ -986,7 +986,7 @@ struct DynPot {
     int wend = -1;  // one past the open frame's last record
     T xw = x, yw = y, zw = z, z2w = z2, R2w = R2, r2w = r2, sR = T(0), sz = T(0), syx = T(0);
     AddAcc<T> sa{T(0), T(0), T(0)};
-    WrapFrame fr{1.0, 1.0, 0.0, false, 0.0, 0.0, 0.0};
+    WrapFrame fr{1.0, 1.0, 0.0, false, false, 0.0, 0.0, 0.0};
     for (int k = 0; k <= ncomp; k++) {
       if (k == wend) {  // close the frame
         const T fc = T(fr.c), fs = T(fr.s), ff = T(fr.fac);
@@ -1000,8 +1000,11 @@ struct DynPot {
           a0.y = sa.y + g * y;
           if (!PLANAR) a0.z = sa.z + g * T(fr.q);
         } else {
-          a0.x = sa.x + ff * (fc * axw - fs * ayw);
-          a0.y = sa.y + ff * (fs * axw + fc * ayw);
+          // a rotation by alpha(R) adds -fac tau' grad alpha, tau' the wrapped
+          // torque about z, grad alpha = (alpha'/R) (x, y, 0)
+          const T tq = fr.co ? ff * T(fr.q) * (xw * ayw - yw * axw) : T(0);
+          a0.x = sa.x + ff * (fc * axw - fs * ayw) - tq * x;
+          a0.y = sa.y + ff * (fs * axw + fc * ayw) - tq * y;
           if (!PLANAR) a0.z = sa.z + ff * azw;
         }
         xw = x;
@@ -1029,6 +1032,7 @@ struct DynPot {
           yw = zw = z2w = T(0);
           R2w = r2w = xw * xw;
         } else {
+          if (fr.co) corot_map(comp + k, (double)R2, t, fr);
           xw = T(fr.c) * x + T(fr.s) * y;
           yw = T(fr.c) * y - T(fr.s) * x;
         }
@@ -1471,7 +1475,7 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
   int wend = -1;
   double xw = x, yw = y, zw = z, z2w = z2, R2w = R2, r2w = r2;
   double sR = 0.0, sz = 0.0, syx = 0.0, sx0 = 0.0, sy0 = 0.0, sz0 = 0.0, sK[6];
-  WrapFrame fr{1.0, 1.0, 0.0, false, 0.0, 0.0, 0.0};
+  WrapFrame fr{1.0, 1.0, 0.0, false, false, 0.0, 0.0, 0.0};
   for (int k = 0; k <= ncomp; k++) {
     if (k == wend) {
       const double c = fr.c, s = fr.s, f = fr.fac;
@@ -1505,6 +1509,27 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
         K[3] = sK[3] + f * (c * kxz - s * kyz);
         K[4] = sK[4] + f * (s * kxz + c * kyz);
         K[5] = sK[5] + f * kzz;
+        if (fr.co) {
+          // Phi = fac Phi'(R(-alpha) x), alpha = alpha(R): with tau' = -dPhi'/dphi',
+          // u = R(alpha) grad'(dPhi'/dphi'), P2 = d2Phi'/dphi'2 and g = grad alpha,
+          // -Hessian gains fac (u g^T + g u^T - P2 g g^T - tau' grad grad alpha),
+          // grad grad alpha = (alpha'' - alpha'/R) R^ R^T + (alpha'/R) I_2; the
+          // acceleration gains -fac tau' g.  Primed Hessian H' = -K'.
+          const double hxx = -kxx, hxy = -kxy, hyy = -kyy, hxz = -kxz, hyz = -kyz;
+          const double px = -axw, py = -ayw, tq = xw * ayw - yw * axw;
+          const double ux = py + xw * hxy - yw * hxx, uy = xw * hyy - px - yw * hxy;
+          const double uz = xw * hyz - yw * hxz;
+          const double P2 = xw * xw * hyy - 2.0 * xw * yw * hxy + yw * yw * hxx - xw * px - yw * py;
+          const double uix = c * ux - s * uy, uiy = s * ux + c * uy;
+          const double gx = fr.q * x, gy = fr.q * y, iR2 = 1.0 / R2, e = fr.dq - fr.q;
+          ax0 -= f * tq * gx;
+          ay0 -= f * tq * gy;
+          K[0] += f * (2.0 * uix * gx - P2 * gx * gx - tq * (e * x * x * iR2 + fr.q));
+          K[1] += f * (uix * gy + uiy * gx - P2 * gx * gy - tq * e * x * y * iR2);
+          K[2] += f * (2.0 * uiy * gy - P2 * gy * gy - tq * (e * y * y * iR2 + fr.q));
+          K[3] += f * uz * gx;
+          K[4] += f * uz * gy;
+        }
       }
       xw = x;
       yw = y;
@@ -1538,6 +1563,7 @@ GPC_HD GPC_FI void accel_tidal(const GpComp* __restrict__ comp, int ncomp, doubl
         yw = zw = z2w = 0.0;
         R2w = r2w = xw * xw;
       } else {
+        if (fr.co) corot_map(cp, R2, t, fr);
         xw = fr.c * x + fr.s * y;
         yw = fr.c * y - fr.s * x;
       }
@@ -1749,7 +1775,7 @@ GPC_HD inline double potential_value(const GpComp* __restrict__ comp, int ncomp,
       } else {
         for (int j = 1; j <= nw; j++) w += comp_value(cp + j, x, y, z, R2, z2, r2);
       }
-      phi += type == T_WRAP_ROTATE ? NAN : fr.fac * w;
+      phi += type == T_WRAP_ROTATE || type == T_WRAP_COROT ? NAN : fr.fac * w;
       k += nw;
       continue;
     }

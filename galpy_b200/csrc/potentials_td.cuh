@@ -34,10 +34,14 @@ enum : int { T_DEHNENBAR = 1, T_SCF = 24 };
 // records of the components it wraps (c15 holds their count).
 // KuzminLikeWrapperPotential.c: the wrapped list on the plane at
 // xi = sqrt(R^2 + (a + sqrt(z^2 + b^2))^2).
-enum : int { T_WRAP_SMOOTH = -1, T_WRAP_ROTATE = -2, T_WRAP_GAUSS = -5, T_WRAP_KUZMIN = -10 };
+// CorotatingRotationWrapperPotential.c: the wrapped list rotated by
+// alpha(R, t) = vpo R^(beta - 1) (t - to) + pa.
+enum : int { T_WRAP_SMOOTH = -1, T_WRAP_ROTATE = -2, T_WRAP_COROT = -4, T_WRAP_GAUSS = -5,
+             T_WRAP_KUZMIN = -10 };
 GPC_HD GPC_FI constexpr bool is_wrapper(int t)
 {
-  return t == T_WRAP_SMOOTH || t == T_WRAP_ROTATE || t == T_WRAP_GAUSS || t == T_WRAP_KUZMIN;
+  return t == T_WRAP_SMOOTH || t == T_WRAP_ROTATE || t == T_WRAP_GAUSS || t == T_WRAP_KUZMIN ||
+         t == T_WRAP_COROT;
 }
 // Planar-only disk perturbations: TransientLogSpiral, SteadyLogSpiral,
 // EllipticalDisk, LopsidedDisk, CosmphiDisk (potential_c_ext/<name>.c)
@@ -101,21 +105,25 @@ GPC_HD GPC_FI double dehnen_smooth(double t, double tform, double tsteady, doubl
 // SolidBodyRotation: amp, alpha = omega t + pa.
 // Records: c0 amp; smooth c1 tform, c2 tsteady, c3 grow, c4 1/(tsteady -
 // tform); Gaussian c1 to, c2 sigma^2; rotation c1 omega, c2 pa.
-// A wrapper's frame: its factor and, for the rotation, cos / sin of the
+// A wrapper's frame: its factor and, for the rotations, cos / sin of the
 // angle; for KuzminLike (kz) the point map x -> (xi, 0, 0) with
 // grad xi = (x, y, q) / xi, q = (a + zeta) z / zeta, zeta = sqrt(z^2 + b^2),
-// and dq = dq/dz = 1 + a b^2 / zeta^3 (for the tidal tensor).
+// and dq = dq/dz = 1 + a b^2 / zeta^3 (for the tidal tensor); for
+// CorotatingRotation (co) the angle at the point's R, with q = alpha'(R) / R
+// and dq = alpha''(R).
 struct WrapFrame {
   double fac, c, s;
-  bool kz;
+  bool kz, co;
   double xi, q, dq;
 };
 
 GPC_HD GPC_FI WrapFrame wrap_frame(const GpComp* __restrict__ cp, int type, double t)
 {
-  WrapFrame f{ldg(&cp->c[0]), 1.0, 0.0, false, 0.0, 0.0, 0.0};
+  WrapFrame f{ldg(&cp->c[0]), 1.0, 0.0, false, false, 0.0, 0.0, 0.0};
   if (type == T_WRAP_KUZMIN) {
     f.kz = true;
+  } else if (type == T_WRAP_COROT) {
+    f.co = true;
   } else if (type == T_WRAP_SMOOTH) {
     const double sm = dehnen_smooth(t, ldg(&cp->c[1]), ldg(&cp->c[2]), ldg(&cp->c[4]));
     f.fac *= ldg(&cp->c[3]) != 0.0 ? sm : 1.0 - sm;
@@ -137,6 +145,18 @@ GPC_HD GPC_FI void kuzmin_map(const GpComp* __restrict__ cp, double R2, double z
   f.xi = sqrt(R2 + A * A);
   f.q = PLANAR ? 0.0 : A * z / zeta;
   f.dq = 1.0 + a * b2 / (zeta * zeta * zeta);
+}
+
+// The CorotatingRotation angle at R^2, time t (record c1 vpo, c2 beta,
+// c3 pa, c4 to): alpha = w R^(beta-1) + pa, alpha'/R = w (beta-1) R^(beta-3),
+// alpha'' = w (beta-1) (beta-2) R^(beta-3), w = vpo (t - to).
+GPC_HD GPC_FI void corot_map(const GpComp* __restrict__ cp, double R2, double t, WrapFrame& f)
+{
+  const double beta = ldg(&cp->c[2]), w = ldg(&cp->c[1]) * (t - ldg(&cp->c[4]));
+  const double Rb = pow(R2, 0.5 * (beta - 3.0));
+  sincos(w * Rb * R2 + ldg(&cp->c[3]), &f.s, &f.c);
+  f.q = w * (beta - 1.0) * Rb;
+  f.dq = f.q * (beta - 2.0);
 }
 
 struct BarParts {

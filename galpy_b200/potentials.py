@@ -42,8 +42,8 @@ ELLIPSOIDAL_TYPES = (21, 22, 23, 30, 37, 38, 43)
 # Hernquist-Ostriker expansion; static coefficients only)
 T_DEHNENBAR, T_SCF = 1, 24
 # wrappers around other components (one level deep): DehnenSmooth,
-# SolidBodyRotation, GaussianAmplitude, KuzminLike
-WRAPPER_TYPES = (-1, -2, -5, -10)
+# SolidBodyRotation, CorotatingRotation, GaussianAmplitude, KuzminLike
+WRAPPER_TYPES = (-1, -2, -4, -5, -10)
 # planar disk perturbations: TransientLogSpiral, SteadyLogSpiral,
 # EllipticalDisk, LopsidedDisk, CosmphiDisk (no potential evaluation in C)
 DISK_PERTURBATION_TYPES = (2, 3, 4, 6, 28)

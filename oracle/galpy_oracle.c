@@ -112,6 +112,9 @@ enum { PT_WRAP_SMOOTH = -1, PT_WRAP_ROTATE = -2, PT_WRAP_GAUSS = -5 };
 /* KuzminLikeWrapperPotential.c: the wrapped potential at xi(R, z) =
    sqrt(R^2 + (a + sqrt(z^2 + b^2))^2) on the plane, args (amp, a, b^2) */
 enum { PT_WRAP_KUZMIN = -10 };
+/* CorotatingRotationWrapperPotential.c: the wrapped list at phi - vpo
+   R^(beta - 1) (t - to) - pa, args (amp, vpo, beta, pa, to) */
+enum { PT_WRAP_COROT = -4 };
 /* planar-only disk perturbations: TransientLogSpiral (2; amp, A, to,
    sigma^2, alpha, m, omegas, gamma), SteadyLogSpiral (3; amp, tform,
    tsteady, A, alpha, m, omegas, gamma; tform NaN: no growth), EllipticalDisk
@@ -589,7 +592,7 @@ static double sph_eval(const ocomp *c, double R, double Z)
 static int is_wrapper(int type)
 {
   return type == PT_WRAP_SMOOTH || type == PT_WRAP_ROTATE || type == PT_WRAP_GAUSS ||
-         type == PT_WRAP_KUZMIN;
+         type == PT_WRAP_KUZMIN || type == PT_WRAP_COROT;
 }
 
 /* n entries of the (type, args) streams into P->c from *idx on; a wrapper
@@ -611,7 +614,7 @@ static int decode_entries(opot *P, int *idx, int n, const int **type, const doub
       const int first = *idx;
       if (nw < 1 || decode_entries(P, idx, nw, type, args, planar)) return -1;
       c->nsub = *idx - first;
-      const int na = t == PT_WRAP_SMOOTH ? 4 : 3;
+      const int na = t == PT_WRAP_SMOOTH ? 4 : t == PT_WRAP_COROT ? 5 : 3;
       for (int k = 0; k < na; k++) c->p[k] = (*args)[k];
       c->ea = *args;
       *args += na;
@@ -1990,6 +1993,41 @@ static double kuzmin_quantity(opot *P, const ocomp *c, int i, int q, double R, d
   }
 }
 
+/* a CorotatingRotation wrapper's contribution to quantity q: the wrapped
+   list at phi' = phi - s(R, t), radial derivatives through the chain rule
+   d/dR -> d/dR - s_R d/dphi' (CorotatingRotationWrapperPotential.c: each
+   quantity in the reference's own grouping) */
+static double corot_quantity(opot *P, const ocomp *c, int i, int q, double R, double z,
+                             double phi)
+{
+  const double amp = c->p[0], vpo = c->p[1], beta = c->p[2], pa = c->p[3], to = c->p[4];
+  const double t = c->t;
+  const int j0 = i + 1, j1 = i + 1 + c->nsub;
+  const double ph = phi - vpo * pow(R, beta - 1) * (t - to) - pa;
+  const double dR = -vpo * (beta - 1) * pow(R, beta - 2) * (t - to);
+#define CQ(Q) range_sum(P, j0, j1, (Q), R, z, ph)
+  switch (q) {
+  case Q_RF:
+    return amp * (CQ(Q_RF) - CQ(Q_PT) * vpo * (beta - 1) * pow(R, beta - 2) * (t - to));
+  case Q_PRF:
+    return amp * (CQ(Q_PRF) - CQ(Q_PPT) * vpo * (beta - 1) * pow(R, beta - 2) * (t - to));
+  case Q_ZF: case Q_PT: case Q_PPT: case Q_H1: case Q_H3: case Q_H5: case Q_PH1:
+    return amp * CQ(q);
+  case Q_H0:
+    return amp * (CQ(Q_H0) + 2. * dR * CQ(Q_H4) + dR * dR * CQ(Q_H3) +
+                  CQ(Q_PT) * vpo * (beta - 1) * (beta - 2) * pow(R, beta - 3) * (t - to));
+  case Q_PH0:
+    return amp * (CQ(Q_PH0) + 2. * dR * CQ(Q_PH2) + dR * dR * CQ(Q_PH1) +
+                  CQ(Q_PPT) * vpo * (beta - 1) * (beta - 2) * pow(R, beta - 3) * (t - to));
+  case Q_H2: return amp * (CQ(Q_H2) + dR * CQ(Q_H5));
+  case Q_H4: return amp * (CQ(Q_H4) + dR * CQ(Q_H3));
+  case Q_PH2:
+    return amp * (CQ(Q_PH2) - CQ(Q_PH1) * vpo * (beta - 1) * pow(R, beta - 2) * (t - to));
+  default: return NAN; /* no potential evaluation in the reference's C */
+  }
+#undef CQ
+}
+
 /* sum of quantity q over entries [i0, i1), in order; a wrapper contributes
    its factor times the sum over its entries (at phi - omega t - pa for the
    rotation wrapper): DehnenSmooth amp s(t) (1 - s(t) if not growing),
@@ -2004,8 +2042,9 @@ static double range_sum(opot *P, int i0, int i1, int q, double R, double z, doub
       sum += comp_quantity(c, q, R, z, phi);
       continue;
     }
-    if (c->type == PT_WRAP_KUZMIN) {
-      sum += kuzmin_quantity(P, c, i, q, R, z);
+    if (c->type == PT_WRAP_KUZMIN || c->type == PT_WRAP_COROT) {
+      sum += c->type == PT_WRAP_KUZMIN ? kuzmin_quantity(P, c, i, q, R, z)
+                                        : corot_quantity(P, c, i, q, R, z, phi);
       i += c->nsub;
       continue;
     }

@@ -152,6 +152,11 @@ def test_wrappers_route(hooks):
     disk = KuzminLikeWrapperPotential(pot=PlummerPotential(amp=0.5, b=0.4), a=0.3, b=0.1)
     o.integrate(ts, [*MWPotential2014, disk], method="dopr54_cuda")
     assert len(hooks) == 3
+    from galpy.potential import CorotatingRotationWrapperPotential
+
+    wound = CorotatingRotationWrapperPotential(pot=DehnenBarPotential(), vpo=1.0, beta=0.1)
+    o.integrate(ts, [*MWPotential2014, wound], method="dop853_cuda")
+    assert len(hooks) == 4
 
 
 def test_unknown_method_still_rejected(hooks):

@@ -208,7 +208,7 @@ def test_wrapped_orbits_vs_oracle(oracle, name, planar, method):
 
 @pytest.mark.parametrize("planar", [False, True])
 @pytest.mark.parametrize("name", ["smooth(bar)+mw14", "rotate(loghalo)+mw14",
-                                  "kuzmin(plummer)+mw14"])
+                                  "kuzmin(plummer)+mw14", "corot(needle)+mw14"])
 def test_wrapped_variational(oracle, name, planar):
     pt, pa, npot = TP.wrapped(name, planar)
     dim = 2 if planar else 3

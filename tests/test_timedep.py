@@ -302,7 +302,7 @@ def test_wrapped_orbits_bit_exact_vs_reference_build(name, planar, method):
 @needs_ref
 @pytest.mark.parametrize("planar", [False, True])
 @pytest.mark.parametrize("name", ["smooth(bar)+mw14", "rotate(loghalo)+mw14",
-                                  "kuzmin(plummer)+mw14"])
+                                  "kuzmin(plummer)+mw14", "corot(needle)+mw14"])
 def test_wrapped_dxdv_bit_exact_vs_reference_build(name, planar):
     pt, pa, npot = TP.wrapped(name, planar)
     dim = 2 if planar else 3
@@ -758,3 +758,34 @@ def test_kuzmin_like_layout_and_forces_vs_galpy_python(planar):
         pv = oracle.potential(R, z, phi, pt, np.asarray(pa), npot=1)
         ref = np.array([pot(R[i], z[i], phi=phi[i], use_physical=False) for i in range(40)])
         assert np.abs(pv - ref).max() <= 1e-14 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("planar", [False, True])
+def test_corotating_rotation_layout_and_forces_vs_galpy_python(planar):
+    """galpy's layout of a CorotatingRotationWrapperPotential around a
+    triaxial halo, and the oracle's forces and second derivatives against
+    galpy's Python wrapper, at two times."""
+    P = galpy_or_skip()
+    halo = P.LogarithmicHaloPotential(amp=0.5, q=0.9, core=0.1, b=0.8)
+    pot = P.CorotatingRotationWrapperPotential(pot=halo, vpo=0.7, beta=0.8, pa=0.2, to=0.5)
+    if planar:
+        from galpy.orbit.integratePlanarOrbit import _parse_pot
+        gp = P.toPlanarPotential(pot)
+    else:
+        from galpy.orbit.integrateFullOrbit import _parse_pot
+        gp = pot
+    npot, pt, pa, _ = _parse_pot([gp])
+    assert npot == 1 and list(pt) == [-4, 0]
+    np.testing.assert_allclose(pa[-5:], [1.0, 0.7, 0.8, 0.2, 0.5], rtol=1e-15)
+    rng = np.random.default_rng(13)
+    R, phi = rng.uniform(0.3, 2.0, 40), rng.uniform(0, 2 * np.pi, 40)
+    z = np.zeros(40) if planar else rng.normal(0, 0.4, 40)
+    names = (["Rforce", "phitorque", "R2deriv", "phi2deriv", "Rphideriv"] if planar else
+             ["Rforce", "zforce", "phitorque", "R2deriv", "z2deriv", "Rzderiv", "phi2deriv",
+              "Rphideriv", "phizderiv"])
+    for t in (0.0, 2.3):
+        got = oracle.forces(R, z, phi, pt, np.asarray(pa), planar=planar, t=t, npot=1)
+        for k, nm in enumerate(names):
+            ref = np.array([getattr(gp, nm)(R[i], *([] if planar else [z[i]]), phi=phi[i],
+                                            t=t, use_physical=False) for i in range(R.size)])
+            assert np.abs(got[:, k] - ref).max() <= 1e-12 * np.abs(ref).max(), (nm, t)

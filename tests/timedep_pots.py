@@ -87,6 +87,11 @@ def wrapped(name, planar=False):
         t, a = [-2, 0], [1] + loghalo_triaxial_args() + [1.0, 0.6, 0.3]
     elif name == "gauss(loghalo)+mw14":  # a triaxial halo with a Gaussian amplitude in time
         t, a = [-5, 0], [1] + loghalo_triaxial_args() + [1.0, 3.0, 4.0]
+    elif name == "corot(needle)+mw14":  # a needle bar winding up with the rotation curve
+        t, a = [-4, 25], [1] + needle_bar_args(amp=0.08, b=0.05, omegab=0.0) + \
+            [1.0, 1.0, 0.1, 0.3, -1.0]
+    elif name == "corot(loghalo)+mw14":  # a triaxial halo in differential rotation
+        t, a = [-4, 0], [1] + loghalo_triaxial_args() + [1.0, 0.7, 0.8, 0.2, 0.5]
     elif name == "kuzmin(plummer)+mw14":  # KuzminLike: a flattened Plummer (amp, a, b^2)
         t, a = [-10, 17], [1, 0.3, 0.4] + [0.8, 0.5, 0.05]
     elif name == "kuzmin(hernquist,plummer)":  # two wrapped spheres, no other component
@@ -98,7 +103,8 @@ def wrapped(name, planar=False):
 
 
 WRAPPED = ["smooth(bar)+mw14", "decay(bar)+mw14", "rotate(loghalo)+mw14", "gauss(loghalo)+mw14",
-           "kuzmin(plummer)+mw14", "kuzmin(hernquist,plummer)"]
+           "kuzmin(plummer)+mw14", "kuzmin(hernquist,plummer)", "corot(needle)+mw14",
+           "corot(loghalo)+mw14"]
 
 
 def crosses_bar_radius(ref_cyl, rb=0.8):
