@@ -150,11 +150,11 @@ def test_unsupported_potential_keeps_galpy_path():
     """A potential the engine does not implement runs galpy's own
     integrator (the hooks fall back to galpy's method of the same name)."""
     from galpy.orbit import Orbit
-    from galpy.potential import SCFPotential
+    from galpy.potential import TwoPowerSphericalPotential
 
     o = Orbit([1.0, 0.1, 1.1, 0.0, 0.1, 0.0])
-    o.integrate(np.linspace(0, 1, 11), SCFPotential(normalize=1.0), method="dop853_cuda",
-                progressbar=False)
+    o.integrate(np.linspace(0, 1, 11), TwoPowerSphericalPotential(alpha=1.5, beta=3.5),
+                method="dop853_cuda", progressbar=False)
     assert np.isfinite(o.getOrbit()).all()
 
 
